@@ -1,0 +1,337 @@
+"""Benchmark of the march: particle-pushes/s including the field solve, one B200 per rank.
+
+Workload (default): the oblique plane wave on a dense bunch, plain FP64 form: 128 x 128 Fourier modes,
+1024 zeta slices (h = 0.1), 1,048,576 macro-electrons, a0 = 0.5 p-polarised plane wave at 20 mrad with a
+flat top of 60 and sin^2 ramps of 10, s-step 2, sponge 6 (0.1 L). One step = push (RK4 in the grid fields
+and the analytic wave) + deposit + zeta filter + forward FFT pair + per-mode march + sponge + real fields +
+window centroid: Simulation::step of the reference. Inputs (a state of 4.6 GB) are larger than L2.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl g3d|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica (the march is one serial chain in zeta;
+replicas only), timed on the device, max over ranks; value = pushes of all ranks / that time.
+--impl reference times the reference GEM-PIC-3D CPU/OpenMP build (oracle/_ref) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "gem-pic-3d_b200"))
+
+METRIC = "particle-pushes/s incl. field solve (FP64 plain form)"
+UNIT = "pushes/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="g3d", choices=["g3d", "reference"])
+    ap.add_argument("--workload", type=int, default=2, choices=[1, 2])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(k):
+    from g3d import configs
+    return configs.baseline(k)
+
+
+def config_json(cfg, k):
+    return {"workload": f"{k}: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, "
+                        f"{cfg.particles} macro-electrons, FP64",
+            "nx": cfg.nx, "ny": cfg.ny, "nzeta": cfg.nzeta, "particles": cfg.particles,
+            "grid_points": cfg.grid_points, "dz": cfg.params["dz"], "sponge": cfg.params.get("sponge", 0),
+            "laser_envelope": "flattop" if cfg.params.get("laser_envelope") == 1 else "gaussian",
+            "l2": "inputs larger than L2 (field state 4.6 GB, F 0.4 GB)", "parallelism": "replicas"}
+
+
+# ------------------------------------------------------------------ algorithmic bytes per launch (FP64)
+def algorithmic_bytes(name, cfg):
+    """Per-launch algorithmic bytes of each kernel: the per-unit figures (bytes per grid point G and per
+    beam particle P per s-step) of the reference's march, split over the kernels that do each part."""
+    G, P, nk, N = cfg.grid_points, cfg.particles, cfg.nx * cfg.ny, cfg.nzeta
+    table = {
+        "push": 112 * P + 24 * G,          # particle read 64 + write 48; F read 24 per grid point
+        "deposit": 56 * P + 24 * G,        # particle read 56; raw current write 24 per grid point
+        "cur_cols": 24 * G + 32 * G,       # raw currents read 24; two complex planes written 32
+        "cur_rows": 32 * G + 48 * G,       # two complex planes read 32; jkx, jky, jkz written 48
+        "march": 272 * G,                  # state read 96 + j0 32 + jk 48, state write 96
+        "real_cols": 96 * G + 48 * G,      # state read 96; three complex planes written 48
+        "real_rows": 48 * G + 24 * G,      # three complex planes read 48; F written 24
+        "sponge_rows": 32 * G + 16 * G + 32 * G,   # R read 32, j_z read 16; packed R - R_b and psi written 32
+        "sponge_cols": 32 * G,             # one complex plane read and written
+        "sponge_rowpairs": 32 * G + 32 * G,        # packed plane and psi read 32; R written 32
+    }
+    return table.get(name)
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+class ClockSampler:
+    def __init__(self, bus_id=None):
+        self.bus_id = (bus_id or "").lower()
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        rows = self.rows
+        if self.bus_id:
+            mine = [r for r in rows if r and self.bus_id.endswith(r[0].lower()[-12:])]
+            rows = mine or rows
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU baseline: the reference build
+def reference_rate(cfg, steps, threads):
+    """Reference CPU/OpenMP build on `threads` host threads: init (untimed), then `steps` s-steps timed."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref
+    if not ref.available():
+        return None, "oracle/_ref/libg3dref.so not built"
+    from g3d import abi
+    rcfg = cfg
+    if cfg.params.get("laser_envelope") == abi.G3D_ENV_FLATTOP:
+        # the reference has only the Gaussian envelope: same pulse centre, FWHM = the plateau length
+        import copy
+        rcfg = copy.deepcopy(cfg)
+        rcfg.params.update(laser_envelope=abi.G3D_ENV_GAUSSIAN, tau=cfg.params.get("flat_length", 60.0))
+    r = ref.RefSimulation(rcfg, threads=threads)
+    r.load_bunch()
+    r.init_fields()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.step()
+    dt = time.perf_counter() - t0
+    n = cfg.particles
+    r.close()
+    return n * steps / dt, None
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ the reference arm
+def run_reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = workload(a.workload)
+    cores = host_cores()
+    steps = max(1, min(a.steps, 5))
+    v, why = reference_rate(cfg, steps, cores)
+    if v is None:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    sample = (f"init untimed, then {steps} s-steps of the full workload (Gaussian envelope of FWHM 60 in place of "
+              f"the flat top, which the reference lacks), OpenMP on {cores} threads")
+    ms = cfg.particles / v * 1e3
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+                      "steps": steps, "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bunch sampler of the reference)",
+                      "config": config_json(cfg, a.workload),
+                      "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+                      "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ------------------------------------------------------------------ our arm
+def run_g3d(a):
+    import numpy as np
+    import torch
+    import g3d
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg = workload(a.workload)
+    sim = g3d.Simulation(cfg)
+    sim.init()
+    P = int(sim.status().np)
+    stream = torch.cuda.ExternalStream(sim.stream_ptr())
+    for _ in range(max(a.warmup, 3)):
+        sim.step()
+
+    # ---------------- timed region: K steps, per-kernel events on the same stream
+    props = torch.cuda.get_device_properties(local)
+    bus = getattr(props, "pci_bus_id", None)
+    bus = f"{bus:02x}:00.0" if isinstance(bus, int) else None
+    clocks = ClockSampler(bus)
+    sim.profile(True)
+    l0 = sim.launch_count()
+    clocks.start()
+    time.sleep(0.6)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        sim.step_async()
+    e1.record(stream)
+    e1.synchronize()
+    sim.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clk = clocks.stop()
+    launches = sim.launch_count() - l0
+    prof = sim.profile_results()
+    sim.profile(False)
+    value = P * a.steps * world / (ms * 1e-3)
+
+    # ---------------- roofline of the dominant kernel
+    import json as _json
+    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    top = max(prof.items(), key=lambda kv: kv[1][1])
+    name, (n_launch, tot_ms) = top
+    avg_ms = tot_ms / max(1, n_launch)
+    ab = algorithmic_bytes(name, cfg)
+    achieved = ab / (avg_ms * 1e-3) / 1e9 if ab else None
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = _json.load(open(tpath)).get(f"{a.workload}:{name}")
+    kernels = {k: {"launches": n, "avg_ms": round(t / max(1, n), 5), "share": round(t / sum(v[1] for v in prof.values()), 4),
+                   "GB/s": (round(algorithmic_bytes(k, cfg) / (t / max(1, n) * 1e-3) / 1e9, 1)
+                            if algorithmic_bytes(k, cfg) else None)}
+               for k, (n, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+
+    # ---------------- end to end through the C-ABI with host buffers
+    e2e = None
+    if a.e2e_steps > 0:
+        host = torch.empty(P * g3d.PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
+        parts = host.numpy().view(g3d.PARTICLE_DTYPE)
+        parts[:] = sim.host_particles()
+        out = torch.empty_like(host)
+        outp = out.numpy().view(g3d.PARTICLE_DTYPE)
+        lib, ctx = sim.lib, sim.ctx
+        diag = (__import__("ctypes").c_double * 19)()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x0 = torch.cuda.Event(enable_timing=True)
+        x1 = torch.cuda.Event(enable_timing=True)
+        x0.record(stream)
+        got = __import__("ctypes").c_int64()
+        for _ in range(a.e2e_steps):
+            sim._c(lib.g3d_set_particles(ctx, parts.ctypes.data, P))          # inputs: H2D from pinned memory
+            sim._c(lib.g3d_step(ctx))
+            sim._c(lib.g3d_get_particles(ctx, outp.ctypes.data, P, __import__("ctypes").byref(got)))  # result D2H
+            sim._c(lib.g3d_diagnostics(ctx, diag))
+            parts, outp = outp, parts
+        x1.record(stream)
+        x1.synchronize()
+        wall = time.perf_counter() - t0
+        ems = max(x0.elapsed_time(x1), wall * 1e3)
+        if dist:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": P * a.e2e_steps * world / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": P * 104, "d2h_bytes_per_step": P * 104 + 19 * 8,
+               "steps": a.e2e_steps,
+               "path": "g3d_set_particles (pinned host records) -> g3d_step -> g3d_get_particles + g3d_diagnostics"}
+
+    # ---------------- CPU baseline on rank 0 at N = 1
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cores = host_cores()
+        steps = 3
+        v, why = reference_rate(cfg, steps, cores)
+        if v is not None:
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"the full workload, init untimed then {steps} s-steps, reference OpenMP build on {cores} "
+                             f"threads (Gaussian envelope FWHM 60 in place of the flat top)"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", "sample": why}
+
+    if dist:
+        dist.barrier()
+    sim.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bunch sampler of the reference)",
+                "config": config_json(cfg, a.workload),
+                "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak if achieved else None, "traffic": traffic,
+                             "peak_source": peak_src, "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_ms},
+                "kernels": kernels, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+    else:
+        run_g3d(a)
+
+
+if __name__ == "__main__":
+    main()

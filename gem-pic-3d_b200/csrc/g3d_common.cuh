@@ -1,0 +1,86 @@
+// Common device/host definitions of libg3d: complex arithmetic on double2/float2, the zeta and
+// y axis lookup, TSC weights, and the error plumbing of the C-ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#define G3D_HD __host__ __device__ __forceinline__
+
+// ---------------------------------------------------------------- errors
+// Host-side failures travel as g3d::Error (with the status code of include/g3d.h) up to the
+// extern "C" layer, which turns them into a status and a message.
+namespace g3d {
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+}  // namespace g3d
+
+#define G3D_CUDA(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            throw g3d::Error(1, std::string(#call) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + \
+                                    ":" + std::to_string(__LINE__) + ")");                             \
+    } while (0)
+
+// ---------------------------------------------------------------- complex numbers
+// cpx is a double2 = {re, im}, the layout of the reference's `struct cpx` (src/portable.hpp:25).
+typedef double2 cpx;
+G3D_HD cpx C(double r, double i = 0.0) { return make_double2(r, i); }
+G3D_HD cpx operator+(cpx a, cpx b) { return make_double2(a.x + b.x, a.y + b.y); }
+G3D_HD cpx operator-(cpx a, cpx b) { return make_double2(a.x - b.x, a.y - b.y); }
+G3D_HD cpx operator-(cpx a) { return make_double2(-a.x, -a.y); }
+G3D_HD cpx operator*(cpx a, cpx b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+G3D_HD cpx operator*(double s, cpx a) { return make_double2(s * a.x, s * a.y); }
+G3D_HD cpx operator*(cpx a, double s) { return make_double2(s * a.x, s * a.y); }
+G3D_HD cpx operator/(cpx a, double s) { return make_double2(a.x / s, a.y / s); }
+G3D_HD cpx cdiv(cpx a, cpx b) {
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+G3D_HD cpx conj(cpx a) { return make_double2(a.x, -a.y); }
+// i k * z for a real k (the derivative factor of a spectral mode)
+G3D_HD cpx ik(double k, cpx z) { return make_double2(-k * z.y, k * z.x); }
+G3D_HD cpx mul_i(cpx z) { return make_double2(-z.y, z.x); }          // i z
+G3D_HD cpx mul_mi(cpx z) { return make_double2(z.y, -z.x); }         // -i z
+
+// ---------------------------------------------------------------- axes
+// Location of a coordinate on a grid of nodes (uniform: direct; else binary search), with the end
+// cells continued beyond the ends. Same contract as the reference's Axis::locate (src/grid.hpp:325-341).
+struct AxisDev {
+    const double* X;            // nodes (device), n of them
+    int n, uniform;
+    double x0, ih;
+    G3D_HD void locate(double x, int& i, double& f) const {
+        if (uniform) { const double t = (x - x0) * ih; i = int(floor(t)); f = t - i; return; }
+        if (x < X[0]) { const double t = (x - X[0]) / (X[1] - X[0]); i = int(floor(t)); f = t - i; return; }
+        if (x >= X[n - 1]) {
+            const double t = (x - X[n - 1]) / (X[n - 1] - X[n - 2]);
+            const int k = int(floor(t));
+            i = n - 1 + k; f = t - k; return;
+        }
+        int lo = 0, hi = n - 1;
+        while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (X[m] <= x) lo = m; else hi = m; }
+        i = lo; f = (x - X[lo]) / (X[lo + 1] - X[lo]);
+    }
+};
+
+// Quadratic (TSC) weights of the three points around the nearest integer of the index coordinate
+// (reference tsc_index, src/sim_kernels.hpp:21-26).
+G3D_HD void tsc_weights(double xi, int idx[3], double w[3]) {
+    const int i0 = int(floor(xi + 0.5));
+    const double f = xi - i0;
+    w[0] = 0.5 * (0.5 - f) * (0.5 - f);
+    w[1] = 0.75 - f * f;
+    w[2] = 0.5 * (0.5 + f) * (0.5 + f);
+    idx[0] = i0 - 1; idx[1] = i0; idx[2] = i0 + 1;
+}
+// TSC on a periodic uniform grid with nodes at i*d (reference tsc, src/sim_kernels.hpp:28-31).
+G3D_HD void tsc_periodic(double x, double d, int n, int idx[3], double w[3]) {
+    tsc_weights(x / d, idx, w);
+    for (int k = 0; k < 3; ++k) idx[k] = (idx[k] % n + n) % n;
+}

@@ -1,0 +1,181 @@
+// Host context of libg3d and the plain structs its kernels take by value.
+#pragma once
+#include <array>
+#include <deque>
+#include <string>
+#include <vector>
+#include "g3d.h"
+#include "g3d_common.cuh"
+
+namespace g3d {
+
+// ---------------------------------------------------------------- device structs (kernel arguments)
+// Grid, k-tables, zeta weights and FFT twiddles. Tables follow the reference's set-up
+// (Simulation::Simulation, setup_y_fourier, setup_zeta: src/sim_setup.cpp:17-35, 63-82, 148-164).
+struct Geo {
+    int nx, ny, nk, N, a, b, ns, nh;     // nh = ns + 3 planes of the raw deposit
+    int yf, zeta_uniform;
+    double dx, dy, Lx, Ly;
+    const double *kxd, *kxs, *filt, *maskx;
+    const double *kyd, *kys, *filty, *masky_n, *masky_h, *iD, *iA;
+    const double *zs, *hcg, *wlo, *whi, *wsl;
+    AxisDev zax, yax;
+    const cpx *twx, *twy;               // exp(-2 pi i s / nx), exp(-2 pi i s / ny)
+};
+
+// Particles as structure of arrays (the reference keeps an array of 104-byte records).
+struct PartsDev {
+    double *x, *y, *zeta, *px, *py, *pz, *w, *rem, *z, *q, *qm;
+    int32_t *alive, *sp;
+    uint64_t* id;
+};
+
+// Analytic plane wave A = a0 g(eta) cos(kL (eta - eta_c) + cep) (reference struct Laser,
+// src/sim.hpp:191-210), with the Gaussian envelope of the reference and a flat-top envelope with
+// sin^2 ramps added here.
+struct LaserDev {
+    int on, pol, env;
+    double a0, kL, tau, cep, eta_c, kx, kz, flat, ramp;
+    G3D_HD double eta(double x, double z, double t) const { return t - kx * x - kz * z; }
+    // envelope g and dg/dxi at xi = eta - eta_c; false outside the pulse
+    G3D_HD bool envelope(double xi, double& g, double& gp) const {
+        if (env == G3D_ENV_GAUSSIAN) {
+            if (fabs(xi) > 5 * tau) return false;
+            g = exp(-1.3862943611198906 * xi * xi / (tau * tau));       // 2 ln 2
+            gp = -2.7725887222397811 * xi / (tau * tau) * g;             // 4 ln 2
+            return true;
+        }
+        const double ax = fabs(xi), hf = 0.5 * flat;
+        if (ax <= hf) { g = 1; gp = 0; return true; }
+        if (ax >= hf + ramp) return false;
+        const double u = (hf + ramp - ax) / ramp;                       // 1 at the plateau edge, 0 outside
+        const double sn = sin(1.5707963267948966 * u), cs = cos(1.5707963267948966 * u);
+        g = sn * sn;
+        gp = (xi > 0 ? -1.0 : 1.0) * (3.1415926535897932 / ramp) * sn * cs;
+        return true;
+    }
+    G3D_HD void field(double x, double z, double t, double E[3], double B[3]) const {
+        E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
+        if (!on) return;
+        const double xi = eta(x, z, t) - eta_c;
+        double g, gp;
+        if (!envelope(xi, g, gp)) return;
+        const double ph = kL * xi + cep, c = cos(ph), s = sin(ph);
+        const double d1 = a0 * (gp * c - kL * g * s), d2 = a0 * (gp * s + kL * g * c);
+        if (pol == 0) { E[1] = -d1; }
+        else if (pol == 1) { E[0] = -d1 * kz; E[2] = d1 * kx; }
+        else { E[0] = -d1 * kz; E[2] = d1 * kx; E[1] = -d2; }
+        B[0] = -kz * E[1]; B[1] = kz * E[0] - kx * E[2]; B[2] = kx * E[1];
+    }
+};
+
+// ---------------------------------------------------------------- device buffers
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void alloc(size_t count, cudaStream_t s) {
+        release();
+        n = count;
+        if (n) {
+            G3D_CUDA(cudaMalloc(&p, n * sizeof(T)));
+            G3D_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+        }
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    void zero(cudaStream_t s) { if (n) G3D_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+    void upload(const std::vector<T>& v, cudaStream_t s) {
+        if (v.size() != n) alloc(v.size(), s);
+        if (n) G3D_CUDA(cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------- profiling
+struct ProfEntry { std::string name; long launches = 0; double ms = 0; };
+struct PendingEvent { int entry; cudaEvent_t e0, e1; };
+
+// ---------------------------------------------------------------- the context
+struct Ctx {
+    // grid (single rank: a = 0, b = ns = N)
+    int nx = 0, ny = 0, N = 0, a = 0, b = 0, ns = 0, nk = 0;
+    double dx = 0, dy = 0;
+    bool yf = true;
+    g3d_params P{};
+    std::vector<double> zeta;
+    std::vector<double> hcg_h, wlo_h, whi_h, wsl_h, kxd_h, kyd_h;
+    // tables
+    DevBuf<double> kxd, kxs, filt, maskx, kyd, kys, filty, masky_n, masky_h, iD, iA;
+    DevBuf<double> zs, hcg, wlo, whi, wsl;
+    DevBuf<cpx> twx, twy;
+    // field state (reference layouts, src/sim.hpp:265-276)
+    DevBuf<cpx> Rx, Ry, Ez, Bz, Lx, Ly;          // ns planes
+    DevBuf<cpx> j0x, j0y, jkx, jky, jkz;         // ns+1 half-cell planes
+    DevBuf<cpx> jzg;                             // 2 ghost planes of filtered j_z (zero on one rank)
+    DevBuf<double> jw;                           // 3 x (ns+3) planes
+    DevBuf<float> F;                             // 6 x (ns+2) planes
+    DevBuf<cpx> S1, S2, S3;                      // FFT scratch, ns+1 planes each
+    DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns planes
+    bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
+    // particles
+    DevBuf<double> pbuf_d;                       // 11 double columns
+    DevBuf<int32_t> pbuf_i;                      // 2 int columns
+    DevBuf<uint64_t> pbuf_u;                     // ids
+    DevBuf<g3d_particle> pstage;                 // device staging of the 104-byte records
+    PartsDev parts{};
+    long np = 0, pcap = 0;
+    // reductions
+    DevBuf<double> red;                          // per-block partial sums
+    std::vector<double> red_h;
+    // scalars (reference members)
+    double s = 0, X0 = 0, Y0 = 0, beta_b = 1, gm2_b = 0, field_energy = 0, hmin = 1e300;
+    long istep = 0, lost_total = 0;
+    bool stop_ = false, starting_ = false, comoving_c_ = false;
+    LaserDev laser{};
+    AxisDev zax{}, yax{};
+    std::deque<std::array<double, 3>> cent_;     // centroid sums awaiting their step (window lag)
+    // stream, launches, profiling
+    cudaStream_t stream = nullptr;
+    long launches = 0;
+    bool profiling = false;
+    std::vector<ProfEntry> prof;
+    std::vector<PendingEvent> pending;
+    std::vector<cudaEvent_t> event_pool;
+    std::string err;
+
+    Geo geo() const;
+    // kernel launch bookkeeping: call before/after each launch
+    int prof_begin(const char* name);
+    void prof_end(int token);
+    void prof_collect();
+    void check_launch(const char* what);
+};
+
+// ---------------------------------------------------------------- launchers (k_*.cu)
+void launch_deposit(Ctx& c);
+void launch_cur_fft(Ctx& c, bool keep0);
+void launch_march(Ctx& c, double D);
+void launch_sponge(Ctx& c);
+void launch_real_fields(Ctx& c);
+void launch_comoving(Ctx& c, double beta, double gm2);
+void launch_push(Ctx& c, double s0, double s1);
+void launch_zero_c(Ctx& c, cpx* p, size_t n);
+void launch_axpy_c(Ctx& c, cpx* y, const cpx* x, double a, size_t n);   // y = y + a x
+void launch_copy_c(Ctx& c, cpx* y, const cpx* x, size_t n);
+void launch_beta_sums(Ctx& c, double out[2]);
+void launch_centroid(Ctx& c, double out[3]);
+void launch_diag(Ctx& c, double S[19]);
+double launch_field_energy(Ctx& c);
+void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy);
+void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
+void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)
+
+}  // namespace g3d
+
+struct g3d_ctx {
+    g3d::Ctx c;
+};

@@ -1,0 +1,722 @@
+// Host side of libg3d: the context (grids, tables, buffers), the orchestration of a step, the bunch
+// loader, checkpoints and the extern "C" entry points of include/g3d.h.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <random>
+#include "g3d_ctx.hpp"
+
+namespace g3d {
+
+namespace {
+constexpr double c_SI = 299792458.0, e_SI = 1.602176634e-19, me_SI = 9.1093837015e-31, eps0 = 8.8541878128e-12;
+thread_local std::string g_create_err;
+
+bool pow2_ok(int n) { return n >= 4 && n <= 512 && (n & (n - 1)) == 0; }
+}  // namespace
+
+// ---------------------------------------------------------------- context plumbing
+Geo Ctx::geo() const {
+    Geo g;
+    g.nx = nx; g.ny = ny; g.nk = nk; g.N = N; g.a = a; g.b = b; g.ns = ns; g.nh = ns + 3;
+    g.yf = yf ? 1 : 0; g.zeta_uniform = zax.uniform;
+    g.dx = dx; g.dy = dy; g.Lx = nx * dx; g.Ly = ny * dy;
+    g.kxd = kxd.p; g.kxs = kxs.p; g.filt = filt.p; g.maskx = maskx.p;
+    g.kyd = kyd.p; g.kys = kys.p; g.filty = filty.p; g.masky_n = masky_n.p; g.masky_h = masky_h.p; g.iD = iD.p; g.iA = iA.p;
+    g.zs = zs.p; g.hcg = hcg.p; g.wlo = wlo.p; g.whi = whi.p; g.wsl = wsl.p;
+    g.zax = zax; g.yax = yax;
+    g.twx = twx.p; g.twy = twy.p;
+    return g;
+}
+
+int Ctx::prof_begin(const char* name) {
+    if (!profiling) return -1;
+    int e = -1;
+    for (size_t k = 0; k < prof.size(); ++k) if (prof[k].name == name) { e = int(k); break; }
+    if (e < 0) { prof.push_back(ProfEntry{name, 0, 0}); e = int(prof.size()) - 1; }
+    PendingEvent pe{e, nullptr, nullptr};
+    for (cudaEvent_t* ev : {&pe.e0, &pe.e1}) {
+        if (!event_pool.empty()) { *ev = event_pool.back(); event_pool.pop_back(); }
+        else G3D_CUDA(cudaEventCreate(ev));
+    }
+    G3D_CUDA(cudaEventRecord(pe.e0, stream));
+    pending.push_back(pe);
+    return int(pending.size()) - 1;
+}
+void Ctx::prof_end(int tok) {
+    if (tok < 0) return;
+    G3D_CUDA(cudaEventRecord(pending[size_t(tok)].e1, stream));
+}
+void Ctx::prof_collect() {
+    if (pending.empty()) return;
+    G3D_CUDA(cudaStreamSynchronize(stream));
+    for (auto& pe : pending) {
+        float ms = 0;
+        G3D_CUDA(cudaEventElapsedTime(&ms, pe.e0, pe.e1));
+        prof[size_t(pe.entry)].ms += ms;
+        prof[size_t(pe.entry)].launches += 1;
+        event_pool.push_back(pe.e0); event_pool.push_back(pe.e1);
+    }
+    pending.clear();
+}
+void Ctx::check_launch(const char* what) {
+    ++launches;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error(G3D_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------- set-up (reference sim_setup.cpp:5-164)
+static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
+    if (!G.y_fourier) throw Error(G3D_ERR_ARG, "free-hand y grids are not supported by this release (y_fourier = 1)");
+    if (!pow2_ok(G.nx) || !pow2_ok(G.ny) || G.nx < 8)
+        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512 and ny one in 4..512");
+    if (G.nzeta < 4 || !G.zeta) throw Error(G3D_ERR_ARG, "nzeta must be >= 4 with a zeta table");
+    if (!(G.Lx > 0) || !(G.Ly > 0)) throw Error(G3D_ERR_ARG, "Lx, Ly must be positive");
+    if (P.precision != G3D_FP64) throw Error(G3D_ERR_ARG, "only the FP64 form is built in this release");
+    if (!(P.dz > 0) || !(P.dz_push > 0) || !(P.lambda0 > 0)) throw Error(G3D_ERR_ARG, "dz, dz_push, lambda0 must be positive");
+    for (int m = 0; m + 1 < G.nzeta; ++m)
+        if (!(G.zeta[m + 1] > G.zeta[m])) throw Error(G3D_ERR_ARG, "zeta slices must increase");
+    c.P = P;
+    c.N = G.nzeta; c.nx = G.nx; c.ny = G.ny; c.nk = c.nx * c.ny;
+    c.a = 0; c.ns = c.N; c.b = c.N;
+    c.dx = G.Lx / c.nx;
+    c.yf = true;
+    c.zeta.assign(G.zeta, G.zeta + G.nzeta);
+    cudaStream_t s = c.stream;
+
+    // x: Fourier modes; Nyquist zeroed for derivatives, kept for the shift; cos^2 current filter; sponge
+    const int nx = c.nx, ny = c.ny;
+    std::vector<double> hkx(nx), hsx(nx), hf(nx), hm(nx);
+    auto prof = [&](double dd, double w) {
+        if (w <= 0 || dd >= w) return 1.0;
+        const double r = 1 - dd / w;
+        return 1 - P.sponge_rate * r * r;
+    };
+    for (int ixx = 0; ixx < nx; ++ixx) {
+        const int mx = ixx <= nx / 2 ? ixx : ixx - nx;
+        hsx[ixx] = 2 * M_PI * mx / G.Lx;
+        hkx[ixx] = (2 * ixx == nx) ? 0 : hsx[ixx];
+        hf[ixx] = P.k_filter ? std::pow(std::cos(0.5 * hsx[ixx] * c.dx), 2) : 1.0;
+        if (2 * ixx == nx) hf[ixx] = 0;
+        hm[ixx] = prof(std::min(ixx * c.dx, G.Lx - ixx * c.dx), P.sponge);
+    }
+    c.kxd.upload(hkx, s); c.kxs.upload(hsx, s); c.filt.upload(hf, s); c.maskx.upload(hm, s);
+    c.kxd_h = hkx;
+    // y: Fourier modes (reference setup_y_fourier, sim_setup.cpp:63-82)
+    c.dy = G.Ly / ny;
+    std::vector<double> hky(ny), hsy(ny), hfy(ny), hmy(ny), hi(ny, 1 / c.dy);
+    for (int j = 0; j < ny; ++j) {
+        const int my = j <= ny / 2 ? j : j - ny;
+        hsy[j] = 2 * M_PI * my / G.Ly;
+        hky[j] = (2 * j == ny) ? 0 : hsy[j];
+        hfy[j] = P.k_filter ? std::pow(std::cos(0.5 * hsy[j] * c.dy), 2) : 1.0;
+        if (2 * j == ny) hfy[j] = 0;
+        const double dd = std::min(j * c.dy, G.Ly - j * c.dy), w = P.sponge_y;
+        double m = 1;
+        if (w > 0 && dd < w) { const double r = 1 - dd / w; m = 1 - P.sponge_rate * r * r; }
+        hmy[j] = m;
+    }
+    c.kyd.upload(hky, s); c.kys.upload(hsy, s); c.filty.upload(hfy, s); c.masky_n.upload(hmy, s); c.masky_h.upload(hmy, s);
+    c.iD.upload(hi, s); c.iA.upload(hi, s);
+    c.kyd_h = hky;
+    c.yax = AxisDev{nullptr, ny + 1, 1, 0.0, 1 / c.dy};
+    // zeta (reference setup_zeta, sim_setup.cpp:148-164)
+    const int N = c.N;
+    const std::vector<double>& Z = c.zeta;
+    std::vector<double> hh(N - 1);
+    for (int m = 0; m < N - 1; ++m) hh[m] = Z[m + 1] - Z[m];
+    bool uni = true;
+    for (int m = 0; m < N - 1; ++m) uni = uni && hh[m] == hh[0];
+    if (uni) for (double& v : hh) v = Z.back() / (N - 1);
+    std::vector<double> g(N + 3), lo(N), hi2(N), ws(N);
+    for (int m = -2; m <= N; ++m) g[m + 2] = hh[std::min(std::max(m, 0), N - 2)];
+    for (int n = 0; n < N; ++n) {
+        const double hmn = g[n - 1 + 2], hpn = g[n + 2];
+        lo[n] = hpn / (hmn + hpn); hi2[n] = hmn / (hmn + hpn);
+        ws[n] = 0.5 * ((n > 0 ? hh[n - 1] : 0) + (n < N - 1 ? hh[n] : 0));
+    }
+    c.zs.upload(Z, s); c.hcg.upload(g, s); c.wlo.upload(lo, s); c.whi.upload(hi2, s); c.wsl.upload(ws, s);
+    c.hcg_h = g; c.wlo_h = lo; c.whi_h = hi2; c.wsl_h = ws;
+    c.zax = AxisDev{c.zs.p, N, uni ? 1 : 0, 0.0, 1 / hh[0]};
+    c.hmin = 1e300;
+    for (int m = 0; m + 1 < N; ++m) c.hmin = std::min(c.hmin, Z[m + 1] - Z[m]);
+    // twiddles exp(-2 pi i s / n)
+    auto tw = [&](int n) {
+        std::vector<cpx> t(n);
+        for (int k = 0; k < n; ++k) { const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / n); t[k] = C(w.real(), w.imag()); }
+        return t;
+    };
+    c.twx.upload(tw(nx), s); c.twy.upload(tw(ny), s);
+    // field buffers (reference layouts)
+    const size_t pl = size_t(c.nk), ns = size_t(c.ns);
+    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly, &c.S3}) p->alloc(ns * pl, s);
+    for (DevBuf<cpx>* p : {&c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz, &c.S1, &c.S2}) p->alloc((ns + 1) * pl, s);
+    c.jzg.alloc(2 * pl, s);
+    c.jw.alloc(3 * (ns + 3) * pl, s);
+    c.F.alloc(6 * (ns + 2) * pl, s);
+    c.rscratch.alloc(ns * pl, s);
+    c.red.alloc(size_t(297) * 17, s);
+    // the plane wave (reference sim_setup.cpp:51-54; eta_c given directly)
+    c.laser.on = P.laser_on; c.laser.pol = P.laser_pol; c.laser.env = P.laser_envelope;
+    c.laser.a0 = P.a0; c.laser.kL = P.kL; c.laser.tau = P.tau; c.laser.cep = P.cep; c.laser.eta_c = P.eta_c;
+    c.laser.kx = std::sin(P.theta); c.laser.kz = std::cos(P.theta);
+    c.laser.flat = P.flat_length; c.laser.ramp = P.ramp_length;
+    if (P.laser_on && P.laser_envelope == G3D_ENV_FLATTOP && !(P.ramp_length > 0))
+        throw Error(G3D_ERR_ARG, "flat-top envelope needs ramp_length > 0");
+    G3D_CUDA(cudaStreamSynchronize(s));
+}
+
+// ---------------------------------------------------------------- particles
+static void reserve_particles(Ctx& c, long n) {
+    if (n <= c.pcap && c.pcap <= 2 * n + 1024) return;
+    const long cap = n + n / 4 + 64;
+    c.pbuf_d.alloc(size_t(cap) * 11, c.stream);
+    c.pbuf_i.alloc(size_t(cap) * 2, c.stream);
+    c.pbuf_u.alloc(size_t(cap), c.stream);
+    double* d = c.pbuf_d.p;
+    PartsDev& P = c.parts;
+    double** cols[11] = {&P.x, &P.y, &P.zeta, &P.px, &P.py, &P.pz, &P.w, &P.rem, &P.z, &P.q, &P.qm};
+    for (int k = 0; k < 11; ++k) *cols[k] = d + size_t(k) * cap;
+    P.alive = c.pbuf_i.p; P.sp = c.pbuf_i.p + cap;
+    P.id = c.pbuf_u.p;
+    c.pcap = cap;
+}
+
+// Host records (104-byte AoS) <-> device columns: one DMA of the records into a device staging buffer
+// and a transposition kernel (k_parts_unpack / k_parts_pack, k_parts.cu).
+static void set_particles(Ctx& c, const g3d_particle* v, long n) {
+    reserve_particles(c, n);
+    c.np = n;
+    if (!n) return;
+    if (c.pstage.n < size_t(n)) c.pstage.alloc(size_t(n) + size_t(n) / 4 + 64, c.stream);
+    G3D_CUDA(cudaMemcpyAsync(c.pstage.p, v, size_t(n) * sizeof(g3d_particle), cudaMemcpyHostToDevice, c.stream));
+    launch_parts_unpack(c, n);
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+static void get_particles_into(Ctx& c, g3d_particle* out) {
+    const long n = c.np;
+    if (!n) return;
+    if (c.pstage.n < size_t(n)) c.pstage.alloc(size_t(n) + size_t(n) / 4 + 64, c.stream);
+    launch_parts_pack(c, n);
+    G3D_CUDA(cudaMemcpyAsync(out, c.pstage.p, size_t(n) * sizeof(g3d_particle), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+static std::vector<g3d_particle> get_particles(Ctx& c) {
+    std::vector<g3d_particle> out(static_cast<size_t>(c.np));
+    get_particles_into(c, out.data());
+    return out;
+}
+
+// Bunch sampling with the reference's random sequence for the built-in profiles (sim_bunches.cpp:92-217,
+// shot_noise = random): per particle G for x, y, (U or G) for z, G for px and py when sigma > 0, G for pz.
+// Host code only: it needs the grid, not a device.
+static void sample_bunches(const g3d_grid& G, const g3d_params& P, const g3d_bunch* list, int count,
+                           std::vector<g3d_particle>& mine, long& lost, double& X0, double& Y0) {
+    const double Lu = P.lambda0 / (2 * M_PI), w0 = c_SI / Lu;
+    const double nc = eps0 * me_SI * w0 * w0 / (e_SI * e_SI);
+    const double yoff = 0.5 * G.Ly;                   // Fourier y: box coordinate, physical y = p.y + Y0
+    const int N = G.nzeta;
+    // the zeta axis as the set-up builds it (uniform: direct location with 1 / h)
+    bool uni = true;
+    const double h0 = G.zeta[1] - G.zeta[0];
+    for (int m = 0; m + 1 < N; ++m) uni = uni && (G.zeta[m + 1] - G.zeta[m]) == h0;
+    const AxisDev zax{G.zeta, N, uni ? 1 : 0, 0.0, 1 / (uni ? G.zeta[N - 1] / (N - 1) : h0)};
+    lost = 0;
+    for (int kb = 0; kb < count; ++kb) {
+        const g3d_bunch& B = list[kb];
+        if (!(B.gamma > 1)) throw Error(G3D_ERR_ARG, "bunch gamma must be > 1");
+        std::mt19937_64 rng(B.seed);
+        std::normal_distribution<double> Gs(0, 1);
+        std::uniform_real_distribution<double> U(-0.5, 0.5);
+        const double Ne = B.charge_C / e_SI;
+        const double W = (B.nmacro > 0 ? Ne / double(B.nmacro) : 0) / (nc * std::pow(Lu, 3));
+        const double p0 = std::sqrt(B.gamma * B.gamma - 1);
+        mine.reserve(mine.size() + size_t(B.nmacro));
+        for (long ib = 0; ib < B.nmacro; ++ib) {
+            const double x = B.x0 + B.sigx * Gs(rng);
+            const double y = B.y0 + B.sigy * Gs(rng);
+            const double z = B.length > 0 ? B.length * U(rng) : B.sigz * Gs(rng);
+            const double px = B.sigx > 0 ? B.emitx / B.sigx * Gs(rng) : 0;
+            const double py = B.sigy > 0 ? B.emity / B.sigy * Gs(rng) : 0;
+            const double pz = p0 * (1 + B.espread * Gs(rng));
+            const double g = std::sqrt(1 + px * px + py * py + pz * pz);
+            const double vx = px / g, vy = py / g, vz = pz / g;
+            const double zz = z;
+            g3d_particle p{};
+            p.x = x - vx * zz / vz + 0.5 * G.Lx; p.y = y - vy * zz / vz + yoff;
+            p.zeta = B.zeta_center + zz / vz;
+            p.px = px; p.py = py; p.pz = pz; p.w = W; p.alive = 1;
+            p.q = B.q; p.qm = B.q; p.sp = -kb; p.z = 0;
+            int hc; double f;
+            zax.locate(p.zeta, hc, f);
+            if (p.zeta < 0 || hc > N - 2) { ++lost; continue; }
+            mine.push_back(p);
+        }
+    }
+    X0 = -0.5 * G.Lx; Y0 = -yoff;
+}
+
+static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int count) {
+    std::vector<g3d_particle> mine;
+    long lost = 0;
+    sample_bunches(G, c.P, list, count, mine, lost, c.X0, c.Y0);
+    set_particles(c, mine.data(), long(mine.size()));
+    c.lost_total += lost;
+}
+
+// ---------------------------------------------------------------- the march path
+static void currents(Ctx& c) {
+    c.jk_is_j0 = false;
+    launch_deposit(c);
+    const bool keep0 = false;            // no plasma in this release: the k = 0 current is removed (sim_particles.cpp:145)
+    launch_cur_fft(c, keep0);
+    // one rank: the filtered j_z ghosts of the neighbours are zero (exchange_jz_ghosts, sim_particles.cpp:210-226)
+}
+static void march(Ctx& c, double D) {
+    if (c.jk_is_j0) throw Error(G3D_ERR_STATE, "march needs the currents of level s1 (call currents first)");
+    launch_march(c, D);
+}
+static void sponge_and_real_fields(Ctx& c) {
+    if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge(c);
+    launch_real_fields(c);
+}
+// j0 <- jk (sim_fields.cpp:313-315): the buffers are swapped; until the next deposit jk reads as j0.
+static void j0_from_jk(Ctx& c) {
+    std::swap(c.j0x.p, c.jkx.p);
+    std::swap(c.j0y.p, c.jky.p);
+    c.jk_is_j0 = true;
+}
+static void materialize_jk(Ctx& c) {
+    if (!c.jk_is_j0) return;
+    launch_copy_c(c, c.jkx.p, c.j0x.p, c.jkx.n);
+    launch_copy_c(c, c.jky.p, c.j0y.p, c.jky.n);
+    c.jk_is_j0 = false;
+}
+static void solve_fields(Ctx& c, double D) {
+    currents(c);
+    march(c, D);
+    sponge_and_real_fields(c);
+    j0_from_jk(c);
+}
+static void comoving_field(Ctx& c) {
+    double sums[2];
+    launch_beta_sums(c, sums);
+    const double beta = c.comoving_c_ ? 1 : sums[1] > 0 ? sums[0] / sums[1] : 1;
+    const double gm2 = 1 - beta * beta;
+    if (!c.comoving_c_) { c.beta_b = beta; c.gm2_b = gm2; }
+    launch_comoving(c, beta, gm2);
+}
+static void relax_start_field(Ctx& c) {
+    const size_t n = size_t(c.ns) * c.nk, nj = size_t(c.ns + 1) * c.nk;
+    cpx* dxr = c.S1.p; cpx* dyr = c.S3.p;          // R of the bunch's beta (S1 and S3 are free here)
+    launch_copy_c(c, dxr, c.Rx.p, n);
+    launch_copy_c(c, dyr, c.Ry.p, n);
+    c.comoving_c_ = true; comoving_field(c); c.comoving_c_ = false;
+    launch_axpy_c(c, dxr, c.Rx.p, -1.0, n);
+    launch_axpy_c(c, dyr, c.Ry.p, -1.0, n);
+    const double D = 100 * c.P.dz;
+    for (int it = 0; it < 3; ++it) {
+        launch_zero_c(c, c.Ez.p, n); launch_zero_c(c, c.Bz.p, n);
+        launch_zero_c(c, c.j0x.p, nj); launch_zero_c(c, c.j0y.p, nj);
+        march(c, D);
+    }
+    launch_axpy_c(c, c.Rx.p, dxr, 1.0, n);
+    launch_axpy_c(c, c.Ry.p, dyr, 1.0, n);
+}
+static void shift_window(Ctx& c, int nxs, int nys) {
+    materialize_jk(c);
+    c.X0 += nxs * c.dx; c.Y0 += nys * c.dy;
+    launch_shift(c, nxs, nys, nxs * c.dx, nys * c.dy);
+}
+static void window_shift_post(Ctx& c) {
+    if (!c.P.move_x && !(c.yf && c.P.move_y)) return;
+    double a[3];
+    launch_centroid(c, a);
+    c.cent_.push_back({a[0], a[1], a[2]});
+}
+static void window_shift_start(Ctx& c) {
+    if (!c.P.move_x && !(c.yf && c.P.move_y)) return;
+    if (long(c.cent_.size()) < c.P.window_lag) return;
+    const std::array<double, 3> v = c.cent_.front();
+    c.cent_.pop_front();
+    if (v[2] <= 0) return;
+    const double Lx = c.nx * c.dx, Ly = c.ny * c.dy;
+    const int nxs = c.P.move_x ? int(std::lround((v[0] / v[2] - (c.X0 + 0.5 * Lx)) / c.dx)) : 0;
+    const int nys = c.yf && c.P.move_y ? int(std::lround((v[1] / v[2] - (c.Y0 + 0.5 * Ly)) / c.dy)) : 0;
+    if (std::abs(nxs) >= 2 || std::abs(nys) >= 2) shift_window(c, nxs, nys);
+}
+static void init_fields(Ctx& c) {
+    c.s = 0; c.istep = 0;
+    if (c.P.self_fields) {
+        c.starting_ = true;
+        currents(c);
+        comoving_field(c);
+        if (c.P.start_relax) relax_start_field(c);
+        march(c, 0.0);
+        c.starting_ = false;
+        sponge_and_real_fields(c);
+        j0_from_jk(c);
+    }
+    window_shift_post(c);
+}
+static void step(Ctx& c, bool sync) {
+    window_shift_start(c);
+    launch_push(c, c.s, c.s + c.P.dz);
+    c.s += c.P.dz; ++c.istep;
+    if (c.P.self_fields) solve_fields(c, 0.5 * c.P.dz);
+    window_shift_post(c);
+    if (sync) G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+static bool finished(const Ctx& c) { return c.s >= c.P.z_end - 1e-9 || c.stop_; }
+
+// ---------------------------------------------------------------- arrays
+static void* array_ptr(Ctx& c, int which, size_t& count, size_t& eb) {
+    DevBuf<cpx>* cb = nullptr;
+    switch (which) {
+        case G3D_A_RX: cb = &c.Rx; break; case G3D_A_RY: cb = &c.Ry; break;
+        case G3D_A_EZ: cb = &c.Ez; break; case G3D_A_BZ: cb = &c.Bz; break;
+        case G3D_A_LX: cb = &c.Lx; break; case G3D_A_LY: cb = &c.Ly; break;
+        case G3D_A_J0X: cb = &c.j0x; break; case G3D_A_J0Y: cb = &c.j0y; break;
+        case G3D_A_JKX: cb = c.jk_is_j0 ? &c.j0x : &c.jkx; break;
+        case G3D_A_JKY: cb = c.jk_is_j0 ? &c.j0y : &c.jky; break;
+        case G3D_A_JKZ: cb = &c.jkz; break;
+        case G3D_A_JW: count = c.jw.n; eb = sizeof(double); return c.jw.p;
+        case G3D_A_F: count = c.F.n; eb = sizeof(float); return c.F.p;
+        default: throw Error(G3D_ERR_ARG, "unknown array id " + std::to_string(which));
+    }
+    count = cb->n; eb = sizeof(cpx);
+    return cb->p;
+}
+
+// ---------------------------------------------------------------- checkpoints (sim_checkpoint.cpp:9-58)
+namespace {
+const char MAGIC[8] = {'G', '3', 'D', 'C', 'K', 'P', 'T', '1'};
+struct CkptHeader {                  // the reference's native struct layout (128 bytes on x86-64)
+    char magic[8];
+    int32_t ranks, rank, N, a, b, ns, nk, nx, ny, plasma;
+    int64_t istep, lost, trapped, restreamed;
+    double s, X0, Y0, beta_b, gm2_b;
+    int32_t stop, ncent;
+};
+static_assert(sizeof(CkptHeader) == 128, "checkpoint header layout");
+template <class T>
+void put(FILE* f, const T* p, uint64_t n) {
+    if (std::fwrite(&n, sizeof n, 1, f) != 1 || (n && std::fwrite(p, sizeof(T), n, f) != n)) throw Error(G3D_ERR_IO, "checkpoint: write error");
+}
+template <class T>
+std::vector<T> get(FILE* f) {
+    uint64_t n = 0;
+    if (std::fread(&n, sizeof n, 1, f) != 1) throw Error(G3D_ERR_IO, "checkpoint: file too short");
+    if (n > (uint64_t(1) << 40)) throw Error(G3D_ERR_IO, "checkpoint: corrupt array length");
+    std::vector<T> v(n);
+    if (n && std::fread(v.data(), sizeof(T), n, f) != n) throw Error(G3D_ERR_IO, "checkpoint: file too short");
+    return v;
+}
+template <class T>
+std::vector<T> d2h(Ctx& c, const T* p, size_t n) {
+    std::vector<T> v(n);
+    if (n) G3D_CUDA(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return v;
+}
+}  // namespace
+
+static void write_checkpoint(Ctx& c, const char* path) {
+    CkptHeader h{};
+    std::memcpy(h.magic, MAGIC, 8);
+    h.ranks = 1; h.rank = 0; h.N = c.N; h.a = c.a; h.b = c.b; h.ns = c.ns; h.nk = c.nk; h.nx = c.nx; h.ny = c.ny; h.plasma = 0;
+    h.istep = c.istep; h.lost = c.lost_total; h.trapped = 0; h.restreamed = 0;
+    h.s = c.s; h.X0 = c.X0; h.Y0 = c.Y0; h.beta_b = c.beta_b; h.gm2_b = c.gm2_b; h.stop = c.stop_; h.ncent = int(c.cent_.size());
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) throw Error(G3D_ERR_IO, "cannot write " + tmp);
+    try {
+        if (std::fwrite(&h, sizeof h, 1, f) != 1) throw Error(G3D_ERR_IO, "checkpoint: write error");
+        for (int w : {G3D_A_RX, G3D_A_RY, G3D_A_EZ, G3D_A_BZ, G3D_A_LX, G3D_A_LY, G3D_A_J0X, G3D_A_J0Y}) {
+            size_t n, eb;
+            const cpx* p = static_cast<const cpx*>(array_ptr(c, w, n, eb));
+            const std::vector<cpx> v = d2h(c, p, n);
+            put(f, v.data(), v.size());
+        }
+        for (int k = 0; k < 3; ++k) put<cpx>(f, nullptr, 0);      // js0x, js0y, js0z: no plasma
+        const std::vector<float> fv = d2h(c, c.F.p, c.F.n);
+        put(f, fv.data(), fv.size());
+        const std::vector<g3d_particle> pv = get_particles(c);
+        put(f, pv.data(), pv.size());
+        put<g3d_particle>(f, nullptr, 0);                          // joining: no plasma
+        for (const auto& v : c.cent_) put(f, v.data(), 3);
+    } catch (...) { std::fclose(f); throw; }
+    std::fclose(f);
+    if (std::rename(tmp.c_str(), path) != 0) throw Error(G3D_ERR_IO, std::string("cannot rename to ") + path);
+}
+
+static void read_checkpoint(Ctx& c, const char* path) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) throw Error(G3D_ERR_IO, std::string("cannot read ") + path);
+    try {
+        CkptHeader h{};
+        if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, MAGIC, 8))
+            throw Error(G3D_ERR_IO, std::string(path) + ": not a GEM-PIC-3D checkpoint");
+        if (h.ranks != 1) throw Error(G3D_ERR_IO, std::string(path) + ": written by " + std::to_string(h.ranks) + " ranks; restart with as many");
+        if (h.N != c.N || h.a != c.a || h.b != c.b || h.nx != c.nx || h.ny != c.ny || h.plasma != 0)
+            throw Error(G3D_ERR_IO, std::string(path) + ": the grid (nx, ny, zeta slices) or the plasma differ");
+        std::vector<std::vector<cpx>> arrays;
+        for (int k = 0; k < 11; ++k) arrays.push_back(get<cpx>(f));
+        const std::vector<float> fv = get<float>(f);
+        const std::vector<g3d_particle> pv = get<g3d_particle>(f);
+        const std::vector<g3d_particle> jv = get<g3d_particle>(f);
+        std::deque<std::array<double, 3>> cent;
+        for (int k = 0; k < h.ncent; ++k) {
+            const std::vector<double> v = get<double>(f);
+            if (v.size() != 3) throw Error(G3D_ERR_IO, std::string(path) + ": bad centroid record");
+            cent.push_back({v[0], v[1], v[2]});
+        }
+        std::fclose(f);
+        f = nullptr;
+        if (fv.size() != c.F.n) throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
+        c.jk_is_j0 = false;
+        DevBuf<cpx>* dst[8] = {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly, &c.j0x, &c.j0y};
+        for (int k = 0; k < 8; ++k) {
+            if (arrays[size_t(k)].size() != dst[k]->n) throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
+            G3D_CUDA(cudaMemcpyAsync(dst[k]->p, arrays[size_t(k)].data(), dst[k]->bytes(), cudaMemcpyHostToDevice, c.stream));
+        }
+        for (int k = 8; k < 11; ++k)
+            if (!arrays[size_t(k)].empty()) throw Error(G3D_ERR_IO, std::string(path) + ": streaming currents present but no plasma");
+        if (!jv.empty()) throw Error(G3D_ERR_IO, std::string(path) + ": joining particles present but no plasma");
+        G3D_CUDA(cudaMemcpyAsync(c.F.p, fv.data(), c.F.bytes(), cudaMemcpyHostToDevice, c.stream));
+        set_particles(c, pv.data(), long(pv.size()));
+        c.istep = h.istep; c.lost_total = h.lost; c.s = h.s; c.X0 = h.X0; c.Y0 = h.Y0;
+        c.beta_b = h.beta_b; c.gm2_b = h.gm2_b; c.stop_ = h.stop != 0;
+        c.cent_ = cent;
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    } catch (...) {
+        if (f) std::fclose(f);
+        throw;
+    }
+}
+
+}  // namespace g3d
+
+// ================================================================ extern "C"
+using g3d::Ctx;
+using g3d::Error;
+
+namespace {
+template <class Fn>
+int guarded(g3d_ctx* ctx, Fn&& fn) {
+    try {
+        fn();
+        if (ctx) ctx->c.err.clear();
+        return G3D_OK;
+    } catch (const Error& e) {
+        if (ctx) ctx->c.err = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->c.err = e.what();
+        return G3D_ERR_ARG;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* g3d_version(void) { return "libg3d 0.1 (sm_100a, FP64 march, Fourier y)"; }
+
+int g3d_create(const g3d_grid* grid, const g3d_params* params, g3d_ctx** out) {
+    if (!grid || !params || !out) { g3d::g_create_err = "null argument"; return G3D_ERR_ARG; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g3d::g_create_err = "no CUDA device visible";
+        return G3D_ERR_NODEV;
+    }
+    g3d_ctx* ctx = new g3d_ctx();
+    try {
+        G3D_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        g3d::setup(ctx->c, *grid, *params);
+    } catch (const Error& e) {
+        g3d::g_create_err = e.what();
+        g3d_destroy(ctx);
+        return e.code;
+    } catch (const std::exception& e) {
+        g3d::g_create_err = e.what();
+        g3d_destroy(ctx);
+        return G3D_ERR_ARG;
+    }
+    *out = ctx;
+    return G3D_OK;
+}
+
+void g3d_destroy(g3d_ctx* ctx) {
+    if (!ctx) return;
+    Ctx& c = ctx->c;
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (auto& pe : c.pending) { cudaEventDestroy(pe.e0); cudaEventDestroy(pe.e1); }
+    for (auto e : c.event_pool) cudaEventDestroy(e);
+    cudaStream_t s = c.stream;
+    delete ctx;                      // DevBuf destructors free the device memory
+    if (s) cudaStreamDestroy(s);
+}
+
+const char* g3d_last_error(const g3d_ctx* ctx) { return ctx ? ctx->c.err.c_str() : g3d::g_create_err.c_str(); }
+
+int g3d_set_particles(g3d_ctx* ctx, const g3d_particle* parts, int64_t n) {
+    return guarded(ctx, [&] {
+        if (n < 0 || (n > 0 && !parts)) throw Error(G3D_ERR_ARG, "bad particle array");
+        g3d::set_particles(ctx->c, parts, long(n));
+    });
+}
+int g3d_get_particles(g3d_ctx* ctx, g3d_particle* out, int64_t capacity, int64_t* n) {
+    return guarded(ctx, [&] {
+        if (n) *n = ctx->c.np;
+        if (capacity < ctx->c.np) throw Error(G3D_ERR_CAPACITY, "output capacity below the particle count");
+        g3d::get_particles_into(ctx->c, out);
+    });
+}
+int g3d_load_bunches(g3d_ctx* ctx, const g3d_bunch* b, int32_t count) {
+    return guarded(ctx, [&] {
+        if (count < 0 || (count > 0 && !b)) throw Error(G3D_ERR_ARG, "bad bunch list");
+        if (count > 1) throw Error(G3D_ERR_ARG, "one bunch block per run in this release");
+        Ctx& c = ctx->c;
+        const g3d_grid G{c.nx, c.ny, c.N, 1, c.nx * c.dx, c.ny * c.dy, c.zeta.data(), nullptr};
+        g3d::load_bunches(c, G, b, count);
+    });
+}
+int g3d_sample_bunches(const g3d_grid* grid, const g3d_params* params, const g3d_bunch* b, int32_t count,
+                       g3d_particle* out, int64_t capacity, int64_t* n, int64_t* lost, double* X0, double* Y0) {
+    try {
+        if (!grid || !params || !n || count < 0 || (count > 0 && !b) || grid->nzeta < 4 || !grid->zeta)
+            throw Error(G3D_ERR_ARG, "bad arguments");
+        std::vector<g3d_particle> v;
+        long ls = 0;
+        double x0 = 0, y0 = 0;
+        g3d::sample_bunches(*grid, *params, b, count, v, ls, x0, y0);
+        *n = int64_t(v.size());
+        if (lost) *lost = ls;
+        if (X0) *X0 = x0;
+        if (Y0) *Y0 = y0;
+        if (int64_t(v.size()) > capacity) throw Error(G3D_ERR_CAPACITY, "output capacity below the particle count");
+        if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(g3d_particle));
+        return G3D_OK;
+    } catch (const Error& e) {
+        g3d::g_create_err = e.what();
+        return e.code;
+    }
+}
+int g3d_init(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::init_fields(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); }); }
+int g3d_step(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::step(ctx->c, true); ctx->c.prof_collect(); }); }
+int g3d_step_async(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::step(ctx->c, false); }); }
+int g3d_solve_fields(g3d_ctx* ctx, double D) {
+    return guarded(ctx, [&] { g3d::solve_fields(ctx->c, D); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+int g3d_currents(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::currents(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); }); }
+int g3d_march(g3d_ctx* ctx, double D) {
+    return guarded(ctx, [&] { g3d::materialize_jk(ctx->c); g3d::march(ctx->c, D); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+int g3d_sponge_and_real_fields(g3d_ctx* ctx) {
+    return guarded(ctx, [&] { g3d::sponge_and_real_fields(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+int g3d_push(g3d_ctx* ctx, double s0, double s1) {
+    return guarded(ctx, [&] { g3d::launch_push(ctx->c, s0, s1); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+int g3d_comoving_field(g3d_ctx* ctx) {
+    return guarded(ctx, [&] { g3d::comoving_field(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+}
+int g3d_relax_start_field(g3d_ctx* ctx) {
+    return guarded(ctx, [&] {
+        g3d::materialize_jk(ctx->c);
+        g3d::relax_start_field(ctx->c);
+        G3D_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ctx, [&] { g3d::shift_window(ctx->c, nxs, nys); }); }
+
+int g3d_diagnostics(g3d_ctx* ctx, double out[19]) {
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        double S[19] = {0};
+        g3d::launch_diag(c, S);
+        S[15] = c.P.self_fields ? g3d::launch_field_energy(c) : 0;
+        S[16] = double(c.lost_total);
+        c.field_energy = S[15];
+        // stop condition of the analytic laser (sim_output.cpp:30-31)
+        const double w = S[0] > 0 ? S[0] : 1;
+        if (c.laser.on && c.P.stop_fwhm > 0 && c.laser.tau > 0 && (S[13] / w - c.laser.eta_c) / c.laser.tau > c.P.stop_fwhm)
+            c.stop_ = true;
+        std::memcpy(out, S, sizeof S);
+    });
+}
+int g3d_field_energy(g3d_ctx* ctx, double* out) {
+    return guarded(ctx, [&] { *out = ctx->c.P.self_fields ? g3d::launch_field_energy(ctx->c) : 0; });
+}
+int g3d_get_status(const g3d_ctx* ctx, g3d_status* o) {
+    if (!ctx || !o) return G3D_ERR_ARG;
+    const Ctx& c = ctx->c;
+    o->s = c.s; o->X0 = c.X0; o->Y0 = c.Y0; o->beta_b = c.beta_b; o->gm2_b = c.gm2_b; o->field_energy = c.field_energy;
+    o->istep = c.istep; o->np = c.np; o->lost = c.lost_total; o->stop = g3d::finished(c) ? 1 : 0;
+    return G3D_OK;
+}
+
+int g3d_array_info(const g3d_ctx* ctx, int32_t which, size_t* count, size_t* eb) {
+    return guarded(const_cast<g3d_ctx*>(ctx), [&] {
+        size_t n, e;
+        g3d::array_ptr(const_cast<g3d_ctx*>(ctx)->c, which, n, e);
+        *count = n; *eb = e;
+    });
+}
+int g3d_get_array(g3d_ctx* ctx, int32_t which, void* host, size_t count) {
+    return guarded(ctx, [&] {
+        size_t n, e;
+        void* p = g3d::array_ptr(ctx->c, which, n, e);
+        if (count != n) throw Error(G3D_ERR_ARG, "count differs from the array size " + std::to_string(n));
+        if (n) G3D_CUDA(cudaMemcpyAsync(host, p, n * e, cudaMemcpyDeviceToHost, ctx->c.stream));
+        G3D_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+int g3d_set_array(g3d_ctx* ctx, int32_t which, const void* host, size_t count) {
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (which == G3D_A_JKX || which == G3D_A_JKY || which == G3D_A_J0X || which == G3D_A_J0Y) g3d::materialize_jk(c);
+        size_t n, e;
+        void* p = g3d::array_ptr(c, which, n, e);
+        if (count != n) throw Error(G3D_ERR_ARG, "count differs from the array size " + std::to_string(n));
+        if (n) G3D_CUDA(cudaMemcpyAsync(p, host, n * e, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+void* g3d_device_ptr(g3d_ctx* ctx, int32_t which) {
+    void* p = nullptr;
+    guarded(ctx, [&] { size_t n, e; p = g3d::array_ptr(ctx->c, which, n, e); });
+    return p;
+}
+
+int g3d_write_checkpoint(g3d_ctx* ctx, const char* path) { return guarded(ctx, [&] { g3d::write_checkpoint(ctx->c, path); }); }
+int g3d_read_checkpoint(g3d_ctx* ctx, const char* path) { return guarded(ctx, [&] { g3d::read_checkpoint(ctx->c, path); }); }
+
+void* g3d_stream(g3d_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
+int g3d_synchronize(g3d_ctx* ctx) {
+    return guarded(ctx, [&] { G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); ctx->c.prof_collect(); });
+}
+int g3d_profile_enable(g3d_ctx* ctx, int32_t on) {
+    return guarded(ctx, [&] {
+        ctx->c.prof_collect();
+        ctx->c.profiling = on != 0;
+        ctx->c.prof.clear();
+    });
+}
+int32_t g3d_profile_count(const g3d_ctx* ctx) { return ctx ? int32_t(ctx->c.prof.size()) : 0; }
+int g3d_profile_get(g3d_ctx* ctx, int32_t k, const char** name, int64_t* launches, double* total_ms) {
+    return guarded(ctx, [&] {
+        ctx->c.prof_collect();
+        if (k < 0 || size_t(k) >= ctx->c.prof.size()) throw Error(G3D_ERR_ARG, "profile index out of range");
+        const g3d::ProfEntry& e = ctx->c.prof[size_t(k)];
+        *name = e.name.c_str(); *launches = e.launches; *total_ms = e.ms;
+    });
+}
+int64_t g3d_launch_count(const g3d_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+}  // extern "C"

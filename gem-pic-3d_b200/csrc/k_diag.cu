@@ -1,0 +1,148 @@
+// Device reductions of the diagnostics (src/sim_output.cpp:5-77), of the window centroid
+// (src/sim_setup.cpp:222-235) and of the mean beta of the bunch (src/sim_fields.cpp:45-51).
+//
+// The reference copies every particle to the host (or sums with atomics); here each reduction is a
+// fixed-order two-level tree: a persistent grid of RB blocks accumulates grid-stride partial sums,
+// each block reduces them in shared memory, and one block sums the block results in index order. The
+// result depends only on the input, never on the thread schedule, so reruns are bit-identical.
+#include "g3d_ctx.hpp"
+
+namespace g3d {
+
+namespace {
+constexpr int RB = 296;     // blocks of the first level (2 per SM)
+constexpr int RT = 256;     // threads per block
+
+template <int NV>
+__device__ void block_store(double (&acc)[NV], double* __restrict__ out) {
+    __shared__ double sh[RT];
+    for (int v = 0; v < NV; ++v) {
+        sh[threadIdx.x] = acc[v];
+        __syncthreads();
+        for (int s = RT / 2; s > 0; s >>= 1) {
+            if (int(threadIdx.x) < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[long(blockIdx.x) * NV + v] = sh[0];
+        __syncthreads();
+    }
+}
+
+template <int NV>
+__global__ void __launch_bounds__(RT) k_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    double acc[NV];
+    for (int v = 0; v < NV; ++v) acc[v] = 0;
+    for (int b = threadIdx.x; b < nb; b += RT)
+        for (int v = 0; v < NV; ++v) acc[v] += part[long(b) * NV + v];
+    block_store<NV>(acc, out);
+}
+
+// ------------------------------------------------ particle sums of diag.txt
+struct DiagArgs { LaserDev laser; double X0, Y0, s, zc; };
+constexpr int NDIAG = 17;    // S[0..14], trapped count, trapped charge
+__global__ void __launch_bounds__(RT) k_diag(PartsDev P, long np, DiagArgs d, double* __restrict__ part) {
+    double acc[NDIAG];
+    for (int v = 0; v < NDIAG; ++v) acc[v] = 0;
+    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < np; i += long(gridDim.x) * RT) {
+        if (P.alive[i] != 1) continue;
+        const double w = P.w[i];
+        if (P.sp[i] > 0) { acc[15] += 1; acc[16] += P.q[i] * w; continue; }     // trapped plasma electrons
+        const double px = P.px[i], py = P.py[i], pz = P.pz[i], zeta = P.zeta[i];
+        const double g = sqrt(1 + px * px + py * py + pz * pz);
+        const double X = P.x[i] + d.X0, Y = P.y[i] + d.Y0;
+        const double et = d.laser.eta(X, d.s, d.s - (zeta - d.zc));
+        const double v[14] = {1, X, Y, zeta, X * X, Y * Y, zeta * zeta, px, py, pz, g, px * d.laser.kx + pz * d.laser.kz, pz * pz, et};
+        for (int k = 0; k < 14; ++k) acc[k] += w * v[k];
+        acc[14] += 1;
+    }
+    block_store<NDIAG>(acc, part);
+}
+
+// ------------------------------------------------ field energy: sum over slices of 1/2 w E^2 (dual cells)
+__global__ void __launch_bounds__(RT) k_energy(Geo g, const float* __restrict__ F, double* __restrict__ part) {
+    double acc[1] = {0};
+    const long nk = g.nk, fpl = long(g.ns + 2) * nk;
+    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < nk; i += long(gridDim.x) * RT) {
+        const int j = int(i / g.nx);
+        const double wn = 1 / g.iA[j], wh = 1 / g.iD[j];
+        double e = 0;
+        for (int l = 0; l < g.ns; ++l) {
+            const double w = g.wsl[g.a + l];
+            for (int comp = 0; comp < 6; ++comp) {
+                const double v = F[comp * fpl + l * nk + i];
+                const bool half = comp == 1 || comp == 3 || comp == 5;
+                e += 0.5 * w * (half ? wh : wn) * v * v;
+            }
+        }
+        acc[0] += e;
+    }
+    block_store<1>(acc, part);
+}
+
+// ------------------------------------------------ centroid of the bunch (window shift)
+__global__ void __launch_bounds__(RT) k_centroid(PartsDev P, long np, double X0, double Y0, double* __restrict__ part) {
+    double acc[3] = {0, 0, 0};
+    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < np; i += long(gridDim.x) * RT) {
+        if (P.alive[i] != 1 || P.sp[i] > 0) continue;
+        const double w = P.w[i];
+        acc[0] += w * (P.x[i] + X0); acc[1] += w * (P.y[i] + Y0); acc[2] += w;
+    }
+    block_store<3>(acc, part);
+}
+
+// ------------------------------------------------ mean beta of the alive particles (co-moving field)
+__global__ void __launch_bounds__(RT) k_beta(PartsDev P, long np, double* __restrict__ part) {
+    double acc[2] = {0, 0};
+    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < np; i += long(gridDim.x) * RT) {
+        if (P.alive[i] != 1) continue;
+        const double px = P.px[i], py = P.py[i], pz = P.pz[i], w = P.w[i];
+        acc[0] += w * pz / sqrt(1 + px * px + py * py + pz * pz);
+        acc[1] += w;
+    }
+    block_store<2>(acc, part);
+}
+
+template <int NV>
+void finish(Ctx& c, double* out) {
+    k_final<NV><<<1, RT, 0, c.stream>>>(c.red.p, RB, c.red.p + RB * NV);
+    c.check_launch("k_final");
+    G3D_CUDA(cudaMemcpyAsync(out, c.red.p + RB * NV, NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+}  // namespace
+
+void launch_diag(Ctx& c, double S[19]) {
+    double r[NDIAG];
+    DiagArgs d{c.laser, c.X0, c.Y0, c.s, c.P.zeta_center};
+    const int tok = c.prof_begin("diag");
+    k_diag<<<RB, RT, 0, c.stream>>>(c.parts, c.np, d, c.red.p);
+    c.check_launch("k_diag");
+    c.prof_end(tok);
+    finish<NDIAG>(c, r);
+    for (int k = 0; k < 15; ++k) S[k] = r[k];
+    S[17] = r[15]; S[18] = r[16];
+}
+
+double launch_field_energy(Ctx& c) {
+    double r[1];
+    const int tok = c.prof_begin("field_energy");
+    k_energy<<<RB, RT, 0, c.stream>>>(c.geo(), c.F.p, c.red.p);
+    c.check_launch("k_energy");
+    c.prof_end(tok);
+    finish<1>(c, r);
+    return r[0] * c.dx;
+}
+
+void launch_centroid(Ctx& c, double out[3]) {
+    k_centroid<<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.X0, c.Y0, c.red.p);
+    c.check_launch("k_centroid");
+    finish<3>(c, out);
+}
+
+void launch_beta_sums(Ctx& c, double out[2]) {
+    k_beta<<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.red.p);
+    c.check_launch("k_beta");
+    finish<2>(c, out);
+}
+
+}  // namespace g3d

@@ -1,0 +1,117 @@
+// Hand-written batched FFT of power-of-two lengths 4..512 on lines held in shared memory.
+//
+// Algorithm: self-sorting Stockham, decimation in time. A length-N transform is a sequence of passes
+// with radices R (the product of the radices of the earlier passes is L, m = N / (L R)); butterfly
+// b = j L + k of a pass reads x[(q m + j) L + k], q < R, multiplies by exp(-2 pi i q k / (L R)), takes the
+// length-R DFT and writes y[(j R + r) L + k], r < R. The passes here are one radix-2 or radix-4 pass
+// (when log2 N is not a multiple of 3; it comes first, where the twiddles are all 1) followed by radix-8
+// passes. Every thread owns E = min(N, 8) values of a line in registers during a pass; a line is worked
+// by N / E threads. The pass reads its inputs, synchronises the CTA, writes its outputs and synchronises
+// again, so a line is transformed in place.
+//
+// The forward transform has the sign -1 and is unnormalised; the inverse is taken as
+// conj(forward(conj(x))) by the callers, who also apply the 1/N factors (the reference's convention,
+// src/fftmany.hpp:39-119: forward sign -1, inverse normalised).
+#pragma once
+#include "g3d_common.cuh"
+
+namespace g3d {
+
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
+template <int N>
+struct FftShape {
+    static_assert(N >= 4 && N <= 512 && (N & (N - 1)) == 0, "FFT length must be a power of two in 4..512");
+    static constexpr int E = N < 8 ? N : 8;                 // values per thread
+    static constexpr int T = N / E;                         // threads per line
+    static constexpr int LOG = ilog2(N);
+    static constexpr int REM = N < 8 ? N : (1 << (LOG % 3));   // radix of the first pass (1: none)
+    static constexpr int NR8 = N < 8 ? 0 : LOG / 3;            // radix-8 passes
+};
+
+// ---------------------------------------------------------------- small DFTs (forward, sign -1)
+__device__ __forceinline__ void dft2(cpx* v) {
+    const cpx a = v[0], b = v[1];
+    v[0] = a + b; v[1] = a - b;
+}
+__device__ __forceinline__ void dft4(cpx* v) {
+    const cpx s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = mul_mi(v[1] - v[3]);
+    v[0] = s02 + s13; v[1] = d02 + d13; v[2] = s02 - s13; v[3] = d02 - d13;
+}
+__device__ __forceinline__ void dft8(cpx* v) {
+    // even / odd split into two DFT4, combined with the eighth roots of unity
+    const double r = 0.70710678118654752440;
+    const cpx a0 = v[0] + v[4], a1 = v[0] - v[4], a2 = v[2] + v[6], a3 = mul_mi(v[2] - v[6]);
+    const cpx a4 = v[1] + v[5], a5 = v[1] - v[5], a6 = v[3] + v[7], a7 = mul_mi(v[3] - v[7]);
+    const cpx b0 = a0 + a2, b2 = a0 - a2, b1 = a1 + a3, b3 = a1 - a3;
+    const cpx c0 = a4 + a6, c2 = a4 - a6, c1 = a5 + a7, c3 = a5 - a7;
+    const cpx w1 = C(r * (c1.x + c1.y), r * (c1.y - c1.x));          // exp(-i pi/4) c1
+    const cpx w2 = mul_mi(c2);                                        // -i c2
+    const cpx w3 = C(r * (c3.y - c3.x), -r * (c3.x + c3.y));         // exp(-3i pi/4) c3
+    v[0] = b0 + c0; v[4] = b0 - c0;
+    v[1] = b1 + w1; v[5] = b1 - w1;
+    v[2] = b2 + w2; v[6] = b2 - w2;
+    v[3] = b3 + w3; v[7] = b3 - w3;
+}
+template <int R>
+__device__ __forceinline__ void dft(cpx* v) {
+    if constexpr (R == 2) dft2(v);
+    else if constexpr (R == 4) dft4(v);
+    else dft8(v);
+}
+
+// One Stockham pass of radix R over a line. `A(p)` maps the position p of the line to its shared
+// memory index; `t` is the thread's index among the T threads of the line; tw[s] = exp(-2 pi i s / N).
+template <int N, int R, class Addr>
+__device__ __forceinline__ void fft_pass(cpx* sm, const Addr& A, int t, int L, const cpx* __restrict__ tw) {
+    constexpr int E = FftShape<N>::E, T = FftShape<N>::T, BPT = E / R;
+    const int m = N / (L * R);
+    cpx v[E];
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int b = t + u * T, j = b / L, k = b - j * L;
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[u * R + q] = sm[A((q * m + j) * L + k)];
+        if (L > 1) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[u * R + q] = v[u * R + q] * __ldg(&tw[q * k * m]);
+        }
+        dft<R>(&v[u * R]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int b = t + u * T, j = b / L, k = b - j * L;
+#pragma unroll
+        for (int r = 0; r < R; ++r) sm[A((j * R + r) * L + k)] = v[u * R + r];
+    }
+    __syncthreads();
+}
+
+// The whole forward transform of one line in shared memory (every thread of the CTA must call it
+// the same number of times: the passes synchronise the CTA).
+template <int N, class Addr>
+__device__ __forceinline__ void fft_line(cpx* sm, const Addr& A, int t, const cpx* __restrict__ tw) {
+    using S = FftShape<N>;
+    int L = 1;
+    if constexpr (S::REM > 1) { fft_pass<N, S::REM>(sm, A, t, L, tw); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR8; ++s) { fft_pass<N, 8>(sm, A, t, L, tw); L *= 8; }
+}
+
+// Shared-memory addressing of a row line: one padding slot per 8 values keeps the strided
+// Stockham accesses free of bank conflicts.
+struct RowAddr {
+    int base;
+    __device__ __forceinline__ int operator()(int p) const { return base + p + (p >> 3); }
+};
+template <int N>
+constexpr int row_stride() { return N + N / 8 + 1; }
+// Shared-memory addressing of a column line inside a tile of CW columns stored row-major.
+template <int CW>
+struct ColAddr {
+    int c;
+    __device__ __forceinline__ int operator()(int p) const { return p * CW + c; }
+};
+
+}  // namespace g3d

@@ -1,0 +1,139 @@
+// Push of the beam list to the next plane s1 (Simulation::push, src/sim_particles.cpp:6-24): characteristics
+// with z as the independent variable, dr/dz = p/p_z, dzeta/dz = -(gamma - p_z)/p_z, dp/dz = q (gamma E + p x B)/p_z,
+// integrated by RK4 (src/sim_kernels.hpp:73-149). The fields are the grid fields of level s0 (float F, TSC in x
+// and y, linear in zeta between the slices; gather, sim_kernels.hpp:44-72) plus the analytic plane wave.
+// A sub-step is at most dz_push, at most push_phase of the laser phase and moves the particle by at most
+// hmin/2 in zeta. One thread per particle, FP64 arithmetic on the float field data.
+#include "g3d_ctx.hpp"
+
+namespace g3d {
+
+struct PushArgs {
+    const float* __restrict__ F;
+    Geo g;
+    LaserDev laser;
+    double X0, Y0, zc, dz_push, push_phase, zhand, zmax, ylo, yhi, s1, vz_min, hmin;
+    int freeze, self;
+};
+
+struct St { double x, y, zeta, px, py, pz; };
+
+__device__ __forceinline__ void gather(const PushArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
+    E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
+    if (!c.self) return;
+    const Geo& g = c.g;
+    int n; double fz;
+    g.zax.locate(zeta, n, fz);
+    if (n == g.a - 1 && fz > 1 - 1e-9) { n = g.a; fz = 0; }    // on the lowest slice (rounding of locate)
+    const int fl = n - g.a;
+    if (fl < 0 || fl > g.ns) return;
+    int ix[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    const long nk = g.nk;
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) {
+        const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
+        const float* p1 = p0 + nk;
+        double v = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const long k = long(jn[j]) * g.nx + ix[i];
+                v += wx[i] * wn[j] * ((1 - fz) * double(__ldg(p0 + k)) + fz * double(__ldg(p1 + k)));
+            }
+        if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+    }
+}
+
+__device__ __forceinline__ bool rhs(const PushArgs& c, const St& Y, double z, double qm, St& d) {
+    const double g = sqrt(1 + Y.px * Y.px + Y.py * Y.py + Y.pz * Y.pz);
+    if (Y.pz < 0.3 * g) return false;
+    const double gm = (1 + Y.px * Y.px + Y.py * Y.py) / (g + Y.pz);
+    double E[3], B[3], Ee[3], Be[3];
+    gather(c, fmod(fmod(Y.x, c.g.Lx) + c.g.Lx, c.g.Lx), fmod(fmod(Y.y, c.g.Ly) + c.g.Ly, c.g.Ly), Y.zeta, E, B);
+    c.laser.field(Y.x + c.X0, z, z - (Y.zeta - c.zc), Ee, Be);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+    const double ip = 1 / Y.pz;
+    d.x = Y.px * ip; d.y = Y.py * ip; d.zeta = -gm * ip;
+    d.px = qm * (g * E[0] + Y.py * B[2] - Y.pz * B[1]) * ip;
+    d.py = qm * (g * E[1] + Y.pz * B[0] - Y.px * B[2]) * ip;
+    d.pz = qm * (g * E[2] + Y.px * B[1] - Y.py * B[0]) * ip;
+    return true;
+}
+__device__ __forceinline__ St axpy(const St& a, double h, const St& b) {
+    return St{a.x + h * b.x, a.y + h * b.y, a.zeta + h * b.zeta, a.px + h * b.px, a.py + h * b.py, a.pz + h * b.pz};
+}
+
+// RK4 from z0 to the plane s1 (reference push_one, src/sim_kernels.hpp:98-149).
+__global__ void __launch_bounds__(128) k_push(PushArgs c, PartsDev P, long np, double s0) {
+    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ip >= np) return;
+    const int alive = P.alive[ip];
+    if (alive != 1 && alive != 3) return;
+    const double s1 = c.s1;
+    if (c.freeze && P.sp[ip] <= 0) { P.z[ip] = s1; return; }       // numerics.freeze_bunch: rigid bunch
+    St Y{P.x[ip], P.y[ip], P.zeta[ip], P.px[ip], P.py[ip], P.pz[ip]};
+    const double qm = P.qm[ip];
+    double z = alive == 1 ? s0 : s1 - P.rem[ip];
+    while (z < s1 - 1e-12 * fabs(s1)) {
+        if (Y.zeta < c.zhand) {          // handed to the rank below with the rest of the step
+            P.x[ip] = Y.x; P.y[ip] = Y.y; P.zeta[ip] = Y.zeta; P.px[ip] = Y.px; P.py[ip] = Y.py; P.pz[ip] = Y.pz;
+            P.alive[ip] = 2; P.rem[ip] = s1 - z;
+            return;
+        }
+        if (c.vz_min > 0 && Y.pz < c.vz_min * sqrt(1 + Y.px * Y.px + Y.py * Y.py + Y.pz * Y.pz)) {
+            // too slow for the beam list: streams in the current march from (z, zeta)
+            P.x[ip] = Y.x; P.y[ip] = Y.y; P.zeta[ip] = Y.zeta; P.px[ip] = Y.px; P.py[ip] = Y.py; P.pz[ip] = Y.pz;
+            P.z[ip] = z; P.alive[ip] = 4;
+            return;
+        }
+        double ds = c.dz_push < s1 - z ? c.dz_push : s1 - z;
+        {
+            const double g = sqrt(1 + Y.px * Y.px + Y.py * Y.py + Y.pz * Y.pz);
+            const double lz = 0.5 * c.hmin * Y.pz * (g + Y.pz) / (1 + Y.px * Y.px + Y.py * Y.py);
+            if (lz < ds) ds = (s1 - z) / ceil((s1 - z) / lz);
+        }
+        if (c.laser.on) {
+            const double g = sqrt(1 + Y.px * Y.px + Y.py * Y.py + Y.pz * Y.pz);
+            const double hl = g - Y.px * c.laser.kx - Y.pz * c.laser.kz;
+            const double lim = c.push_phase * Y.pz / (c.laser.kL * (hl > 1e-12 ? hl : 1e-12));
+            if (lim < ds) ds = (s1 - z) / ceil((s1 - z) / lim);
+        }
+        St k1, k2, k3, k4;
+        if (!(rhs(c, Y, z, qm, k1) && rhs(c, axpy(Y, 0.5 * ds, k1), z + 0.5 * ds, qm, k2) &&
+              rhs(c, axpy(Y, 0.5 * ds, k2), z + 0.5 * ds, qm, k3) && rhs(c, axpy(Y, ds, k3), z + ds, qm, k4))) {
+            P.alive[ip] = 0;
+            return;
+        }
+        const double w = ds / 6;
+        Y.x += w * (k1.x + 2 * k2.x + 2 * k3.x + k4.x); Y.y += w * (k1.y + 2 * k2.y + 2 * k3.y + k4.y);
+        Y.zeta += w * (k1.zeta + 2 * k2.zeta + 2 * k3.zeta + k4.zeta);
+        Y.px += w * (k1.px + 2 * k2.px + 2 * k3.px + k4.px); Y.py += w * (k1.py + 2 * k2.py + 2 * k3.py + k4.py);
+        Y.pz += w * (k1.pz + 2 * k2.pz + 2 * k3.pz + k4.pz);
+        z += ds;
+    }
+    P.x[ip] = Y.x; P.y[ip] = Y.y; P.zeta[ip] = Y.zeta; P.px[ip] = Y.px; P.py[ip] = Y.py; P.pz[ip] = Y.pz; P.z[ip] = s1;
+    // lost: out of the window in zeta, or within one cell of a wall in y
+    int al = (Y.zeta < 0 || Y.zeta >= c.zmax || Y.y < c.ylo || Y.y > c.yhi) ? 0 : 1;
+    if (al == 1 && Y.zeta < c.zhand) { al = 2; P.rem[ip] = 0; }
+    P.alive[ip] = al;
+}
+
+void launch_push(Ctx& c, double s0, double s1) {
+    if (c.np == 0) return;
+    PushArgs a;
+    a.F = c.F.p; a.g = c.geo(); a.laser = c.laser;
+    a.X0 = c.X0; a.Y0 = c.Y0; a.zc = c.P.zeta_center; a.dz_push = c.P.dz_push; a.push_phase = c.P.push_phase;
+    a.zhand = -1e300;                                   // one rank: nothing is handed over
+    a.zmax = c.zeta[c.N - 1]; a.ylo = -1e300; a.yhi = 1e300; a.s1 = s1; a.vz_min = 0; a.hmin = c.hmin;
+    a.freeze = c.P.freeze_bunch; a.self = c.P.self_fields;
+    const int tok = c.prof_begin("push");
+    k_push<<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.parts, c.np, s0);
+    c.check_launch("k_push");
+    c.prof_end(tok);
+}
+
+}  // namespace g3d

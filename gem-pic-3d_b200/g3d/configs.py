@@ -1,0 +1,143 @@
+"""Run configurations in code units (the reference's deck keys, docs/input_deck.md, set in code the way
+the reference's tests do with `base()`, tests/test_util.hpp:36-43).
+
+`baseline(k)` builds the five benchmark workloads of this project (k = 1..5) by their sizes:
+  1  frozen-bunch wake in vacuum: 64x64 modes, 256 slices (h = 0.5), 262,144 macro-electrons, 10 s-steps
+  2  oblique plane wave on a bunch: 128x128 modes, 1024 slices (h = 0.1), 1,048,576 macro-electrons,
+     a0 = 0.5, p polarisation, 20 mrad, flat top 60 with sin^2 ramps 10, 100 s-steps of 2
+  3-5 plasma runs (not built by this release; `baseline` raises for them)
+Every size can be reduced with keyword overrides for tests.
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+C_SI, E_SI, ME_SI, EPS0 = 299792458.0, 1.602176634e-19, 9.1093837015e-31, 8.8541878128e-12
+
+
+def units(lambda0):
+    """Unit of length Lu = lambda0 / 2 pi [m] and the critical density n_c [m^-3] (sim_config.cpp:5-11)."""
+    Lu = lambda0 / (2 * math.pi)
+    w0 = C_SI / Lu
+    nc = EPS0 * ME_SI * w0 * w0 / (E_SI * E_SI)
+    return Lu, nc
+
+
+def charge_for_peak_density(n_peak, sigx, sigy, sigz, lambda0):
+    """|charge| [C] of a Gaussian bunch with the peak density n_peak (units of n_c), sizes in 1/k0."""
+    Lu, nc = units(lambda0)
+    ne = n_peak * (2 * math.pi) ** 1.5 * sigx * sigy * sigz * nc * Lu ** 3
+    return ne * E_SI
+
+
+@dataclass
+class RunConfig:
+    name: str
+    nx: int
+    ny: int
+    nzeta: int
+    Lx: float
+    Ly: float
+    h: float                       # uniform slice step
+    params: dict = field(default_factory=dict)
+    bunches: list = field(default_factory=list)
+    steps: int = 10
+
+    @property
+    def zeta(self):
+        return np.arange(self.nzeta, dtype=np.float64) * self.h
+
+    def grid_struct(self):
+        z = np.ascontiguousarray(self.zeta)
+        g = abi.Grid(self.nx, self.ny, self.nzeta, 1, self.Lx, self.Ly,
+                     z.ctypes.data_as(abi.C.POINTER(abi.C.c_double)), None)
+        return g, z            # keep z alive while g is used
+
+    def params_struct(self):
+        p = abi.Params()
+        d = default_params()
+        d.update(self.params)
+        for k, v in d.items():
+            setattr(p, k, v)
+        return p
+
+    def bunch_structs(self):
+        arr = (abi.Bunch * max(1, len(self.bunches)))()
+        for i, b in enumerate(self.bunches):
+            d = default_bunch()
+            d.update(b)
+            for k, v in d.items():
+                setattr(arr[i], k, v)
+        return arr, len(self.bunches)
+
+    @property
+    def grid_points(self):
+        return self.nx * self.ny * self.nzeta
+
+    @property
+    def particles(self):
+        return sum(int(b.get("nmacro", 0)) for b in self.bunches)
+
+
+def default_params():
+    """Deck defaults of the reference (sim_config.cpp:69-343) for the keys of g3d_params."""
+    return dict(lambda0=0.8e-6, dz=1.0, dz_push=1.0, z_end=10.0, sponge=0.0, sponge_y=0.0, sponge_rate=0.1,
+                move_x=1, move_y=1, window_lag=4, self_fields=1, zeta_filter=1, k_filter=1, push_phase=0.05,
+                laser_on=0, laser_pol=abi.G3D_POL_S, laser_envelope=abi.G3D_ENV_GAUSSIAN, reserved0=0,
+                a0=0.0, kL=1.0, theta=0.0, tau=1.0, cep=0.0, eta_c=0.0, stop_fwhm=0.0,
+                flat_length=0.0, ramp_length=0.0, zeta_center=0.0,
+                freeze_bunch=0, start_relax=1, box_mean=1, precision=abi.G3D_FP64)
+
+
+def default_bunch():
+    return dict(charge_C=0.0, gamma=2.0, sigx=1.0, sigy=1.0, sigz=1.0, length=0.0, emitx=0.0, emity=0.0,
+                espread=0.0, zeta_center=0.0, x0=0.0, y0=0.0, q=-1.0, nmacro=0, seed=1)
+
+
+def config1(nx=64, ny=64, nzeta=256, nmacro=262144, steps=10):
+    """Plain FP64 frozen-bunch wake in vacuum (the CPU-runnable case)."""
+    lam = 0.8e-6
+    h = 0.5 * (255 / (nzeta - 1))       # keeps the 127.5 window when nzeta is reduced
+    dz = 5.0
+    sig, sigz = 2.0, 4.0
+    q = charge_for_peak_density(0.01, sig, sig, sigz, lam)
+    b = dict(charge_C=q, gamma=math.sqrt(1 + 1000.0 ** 2), sigx=sig, sigy=sig, sigz=sigz,
+             emitx=0.2, emity=0.2, espread=0.0, zeta_center=64.0, nmacro=nmacro, seed=1)
+    p = dict(lambda0=lam, dz=dz, dz_push=dz, z_end=dz * steps, sponge=0.0, sponge_y=0.0,
+             move_x=0, move_y=0, zeta_center=64.0)
+    return RunConfig("frozen-bunch wake, vacuum", nx, ny, nzeta, 40.0, 40.0, h, p, [b], steps)
+
+
+def config2(nx=128, ny=128, nzeta=1024, nmacro=1048576, steps=100, envelope=abi.G3D_ENV_FLATTOP):
+    """Plain FP64 oblique plane wave on a dense bunch (the headline single-GPU workload)."""
+    lam = 0.8e-6
+    h = 0.1 * (1023 / (nzeta - 1))
+    dz = 2.0
+    L = 60.0
+    sig, sigz = 3.0, 6.0
+    q = charge_for_peak_density(0.05, sig, sig, sigz, lam)
+    window = h * (nzeta - 1)
+    zc = 0.75 * window                  # reference default bunch.zeta_center (sim_bunches.cpp:49)
+    b = dict(charge_C=q, gamma=500.0, sigx=sig, sigy=sig, sigz=sigz, emitx=1.0, emity=1.0, espread=1e-3,
+             zeta_center=zc, nmacro=nmacro, seed=1)
+    p = dict(lambda0=lam, dz=dz, dz_push=dz, z_end=dz * steps, sponge=0.1 * L, sponge_y=0.1 * L,
+             zeta_center=zc, laser_on=1, laser_pol=abi.G3D_POL_P, a0=0.5, kL=1.0, theta=0.02, cep=0.0)
+    if envelope == abi.G3D_ENV_FLATTOP:
+        # plateau 60, sin^2 ramps 10; the bunch sits in the plateau (eta_c = 0)
+        p.update(laser_envelope=abi.G3D_ENV_FLATTOP, flat_length=60.0, ramp_length=10.0, tau=60.0, eta_c=0.0,
+                 stop_fwhm=0.0)
+    else:
+        # the reference's Gaussian envelope with the same intensity FWHM, centred on the bunch
+        p.update(laser_envelope=abi.G3D_ENV_GAUSSIAN, tau=60.0, eta_c=0.0, stop_fwhm=0.0)
+    return RunConfig("oblique plane wave on a bunch", nx, ny, nzeta, L, L, h, p, [b], steps)
+
+
+def baseline(k, **kw):
+    if k == 1:
+        return config1(**kw)
+    if k == 2:
+        return config2(**kw)
+    raise NotImplementedError(f"workload {k} needs the plasma march, which this release does not build")

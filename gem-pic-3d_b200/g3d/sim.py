@@ -1,0 +1,206 @@
+"""Host-side mirror of the reference's `class Simulation` (src/sim.hpp:222-360) over the C-ABI.
+
+Same method names, argument meaning and error behaviour: a failing call raises G3DError (a
+RuntimeError, as the reference throws std::runtime_error), carrying the C-ABI status code.
+Arrays come back in the reference layouts (spectra [l][j][ix] complex128, F [comp][fl][j][ix] float32,
+particles as the 104-byte records of PARTICLE_DTYPE).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+
+class G3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"g3d error {code}: {msg}")
+        self.code = code
+
+
+def _check(lib, ctx, rc):
+    if rc != abi.G3D_OK:
+        raise G3DError(rc, lib.g3d_last_error(ctx).decode(errors="replace"))
+
+
+def sample_bunches(cfg, lib=None):
+    """The bunch of the configuration as the reference loads it (src/sim_bunches.cpp:92-217), sampled on
+    the host without a device. Returns (particles, lost, X0, Y0)."""
+    lib = lib or abi.load_library()
+    g, z = cfg.grid_struct()
+    p = cfg.params_struct()
+    b, nb = cfg.bunch_structs()
+    cap = max(1, cfg.particles)
+    out = np.zeros(cap, dtype=abi.PARTICLE_DTYPE)
+    n, lost, x0, y0 = C.c_int64(), C.c_int64(), C.c_double(), C.c_double()
+    rc = lib.g3d_sample_bunches(C.byref(g), C.byref(p), b, nb, out.ctypes.data, cap, C.byref(n), C.byref(lost),
+                                C.byref(x0), C.byref(y0))
+    if rc != abi.G3D_OK:
+        raise G3DError(rc, lib.g3d_last_error(None).decode(errors="replace"))
+    return out[: n.value], lost.value, x0.value, y0.value
+
+
+class Simulation:
+    """One march context on the current CUDA device."""
+
+    def __init__(self, cfg, lib=None):
+        self.lib = lib or abi.load_library()
+        self.cfg = cfg
+        g, self._zeta = cfg.grid_struct()
+        p = cfg.params_struct()
+        h = C.c_void_p()
+        rc = self.lib.g3d_create(C.byref(g), C.byref(p), C.byref(h))
+        if rc != abi.G3D_OK:
+            raise G3DError(rc, self.lib.g3d_last_error(None).decode(errors="replace"))
+        self.ctx = h
+        self.N, self.nx, self.ny = cfg.nzeta, cfg.nx, cfg.ny
+        self.nk = cfg.nx * cfg.ny
+        self.ns = cfg.nzeta
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.g3d_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _c(self, rc):
+        _check(self.lib, self.ctx, rc)
+
+    # ------------------------------------------------------------ particles
+    def load_bunch(self):
+        arr, n = self.cfg.bunch_structs()
+        self._c(self.lib.g3d_load_bunches(self.ctx, arr, n))
+
+    def set_particles(self, parts):
+        parts = np.ascontiguousarray(parts, dtype=abi.PARTICLE_DTYPE)
+        self._c(self.lib.g3d_set_particles(self.ctx, parts.ctypes.data, len(parts)))
+
+    def host_particles(self):
+        n = self.status().np
+        out = np.zeros(n, dtype=abi.PARTICLE_DTYPE)
+        got = C.c_int64()
+        self._c(self.lib.g3d_get_particles(self.ctx, out.ctypes.data, n, C.byref(got)))
+        return out
+
+    # ------------------------------------------------------------ the march path
+    def init(self):
+        """Simulation::init: the bunch of the configuration, then the start fields."""
+        self.load_bunch()
+        self.init_fields()
+
+    def init_fields(self):
+        self._c(self.lib.g3d_init(self.ctx))
+
+    def step(self):
+        self._c(self.lib.g3d_step(self.ctx))
+
+    def step_async(self):
+        self._c(self.lib.g3d_step_async(self.ctx))
+
+    def solve_fields(self, D):
+        self._c(self.lib.g3d_solve_fields(self.ctx, D))
+
+    def currents(self):
+        self._c(self.lib.g3d_currents(self.ctx))
+
+    def march(self, D):
+        self._c(self.lib.g3d_march(self.ctx, D))
+
+    def sponge_and_real_fields(self):
+        self._c(self.lib.g3d_sponge_and_real_fields(self.ctx))
+
+    def push(self, s0, s1):
+        self._c(self.lib.g3d_push(self.ctx, s0, s1))
+
+    def comoving_field(self):
+        self._c(self.lib.g3d_comoving_field(self.ctx))
+
+    def relax_start_field(self):
+        self._c(self.lib.g3d_relax_start_field(self.ctx))
+
+    def shift_window(self, nxs, nys):
+        self._c(self.lib.g3d_shift_window(self.ctx, nxs, nys))
+
+    # ------------------------------------------------------------ diagnostics
+    def diagnostics_sums(self):
+        out = (C.c_double * 19)()
+        self._c(self.lib.g3d_diagnostics(self.ctx, out))
+        return np.array(out[:], dtype=np.float64)
+
+    def field_energy(self):
+        v = C.c_double()
+        self._c(self.lib.g3d_field_energy(self.ctx, C.byref(v)))
+        return v.value
+
+    def status(self):
+        st = abi.Status()
+        self._c(self.lib.g3d_get_status(self.ctx, C.byref(st)))
+        return st
+
+    @property
+    def s(self):
+        return self.status().s
+
+    @property
+    def istep(self):
+        return self.status().istep
+
+    def finished(self):
+        return bool(self.status().stop)
+
+    # ------------------------------------------------------------ arrays
+    def array_info(self, name):
+        n, eb = C.c_size_t(), C.c_size_t()
+        self._c(self.lib.g3d_array_info(self.ctx, abi.ARRAYS[name], C.byref(n), C.byref(eb)))
+        return n.value, eb.value
+
+    def array(self, name):
+        n, eb = self.array_info(name)
+        dt = {16: np.complex128, 8: np.float64, 4: np.float32}[eb]
+        out = np.empty(n, dtype=dt)
+        self._c(self.lib.g3d_get_array(self.ctx, abi.ARRAYS[name], out.ctypes.data, n))
+        return out
+
+    def set_array(self, name, values):
+        n, eb = self.array_info(name)
+        dt = {16: np.complex128, 8: np.float64, 4: np.float32}[eb]
+        v = np.ascontiguousarray(values, dtype=dt).ravel()
+        if v.size != n:
+            raise ValueError(f"{name}: {v.size} values for an array of {n}")
+        self._c(self.lib.g3d_set_array(self.ctx, abi.ARRAYS[name], v.ctypes.data, n))
+
+    def device_ptr(self, name):
+        return self.lib.g3d_device_ptr(self.ctx, abi.ARRAYS[name])
+
+    # ------------------------------------------------------------ checkpoints
+    def write_checkpoint(self, path):
+        self._c(self.lib.g3d_write_checkpoint(self.ctx, str(path).encode()))
+
+    def read_checkpoint(self, path):
+        self._c(self.lib.g3d_read_checkpoint(self.ctx, str(path).encode()))
+
+    # ------------------------------------------------------------ stream, timing
+    def stream_ptr(self):
+        return self.lib.g3d_stream(self.ctx)
+
+    def synchronize(self):
+        self._c(self.lib.g3d_synchronize(self.ctx))
+
+    def profile(self, on=True):
+        self._c(self.lib.g3d_profile_enable(self.ctx, 1 if on else 0))
+
+    def profile_results(self):
+        out = {}
+        for k in range(self.lib.g3d_profile_count(self.ctx)):
+            name, n, ms = C.c_char_p(), C.c_int64(), C.c_double()
+            self._c(self.lib.g3d_profile_get(self.ctx, k, C.byref(name), C.byref(n), C.byref(ms)))
+            out[name.value.decode()] = (n.value, ms.value)
+        return out
+
+    def launch_count(self):
+        return self.lib.g3d_launch_count(self.ctx)

@@ -1,0 +1,200 @@
+/*
+ * g3d.h -- C-ABI of the B200-native per-zeta-slice march of GEM-PIC-3D.
+ *
+ * The library (libg3d.so, hand-written sm_100a CUDA) replaces from below the reference's
+ * `class Simulation` (src/sim.hpp:222-360) for the hot path: push, current deposit,
+ * zeta filter, transverse FFTs, per-mode march, sponge, real fields, window shift and the
+ * diagnostics reductions. Every entry point is `extern "C"`, takes plain pointers and
+ * sizes, and returns an int status (G3D_OK = 0). A non-zero status leaves a message in
+ * g3d_last_error(). Calls are synchronous at the ABI: they return after the work queued on
+ * the context's own CUDA stream has finished, unless the name ends in `_async`.
+ * One context = one GPU = one host thread (the reference runs one host thread per rank).
+ *
+ * Units are the reference's code units (README.md:43-45): c = 1, lengths 1/k0, times
+ * 1/omega0, momenta m c, fields m c omega0 / e, densities n_c.
+ */
+#ifndef G3D_H
+#define G3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque context: one march on one GPU. */
+struct g3d_ctx;
+typedef struct g3d_ctx g3d_ctx;
+
+/* ------------------------------------------------------------------ status codes */
+#define G3D_OK            0
+#define G3D_ERR_CUDA      1   /* a CUDA call failed (reference: gpu_check, src/portable.hpp:43-49) */
+#define G3D_ERR_TIMEOUT   2   /* a bounded device-side wait gave up */
+#define G3D_ERR_CAPACITY  3   /* a fixed-capacity list overflowed */
+#define G3D_ERR_ARG       4   /* an invalid argument (sizes, grid, unknown array id) */
+#define G3D_ERR_STATE     5   /* an entry point called in the wrong state */
+#define G3D_ERR_IO        6   /* checkpoint file missing, truncated or not a checkpoint */
+#define G3D_ERR_NODEV     7   /* no CUDA device visible to this process */
+
+/* ------------------------------------------------------------------ forms */
+#define G3D_FP64   0          /* plain form: FP64 throughout, float F as in the reference */
+#define G3D_MIXED  1          /* mixed FP32/FP64 form */
+
+/* laser envelope of the analytic plane wave */
+#define G3D_ENV_GAUSSIAN 0    /* reference Laser::envelope, src/sim.hpp:195 */
+#define G3D_ENV_FLATTOP  1    /* flat top with sin^2 ramps (no counterpart in the reference) */
+
+/* polarisation of the analytic plane wave (reference Laser::pol, src/sim.hpp:192) */
+#define G3D_POL_S        0    /* E along y */
+#define G3D_POL_P        1    /* E in the x-z plane */
+#define G3D_POL_CIRCULAR 2
+
+/* ------------------------------------------------------------------ records */
+/* One macro-particle, byte for byte the reference's `struct Particle` (src/sim.hpp:217, 104 B):
+ * this is the layout of checkpoints and of g3d_set/get_particles. On the device the library
+ * keeps the particles as structure-of-arrays. */
+typedef struct g3d_particle {
+    double x, y, zeta, px, py, pz, w, rem, z, q, qm;
+    int32_t alive, sp;
+    uint64_t id;
+} g3d_particle;
+
+/* Grid (reference Config grid fields, src/sim.hpp:38-44). */
+typedef struct g3d_grid {
+    int32_t nx, ny, nzeta;
+    int32_t y_fourier;          /* 1: Fourier y (the only form of this release); 0: free-hand y */
+    double Lx, Ly;
+    const double* zeta;         /* nzeta slice positions, zeta[0] = 0 (rear) ... zeta[nzeta-1] = window */
+    const double* ynode;        /* ny+1 node positions of the free-hand y grid, NULL for Fourier y */
+} g3d_grid;
+
+/* Run parameters (reference Config, src/sim.hpp:36-187, the subset on the march path). */
+typedef struct g3d_params {
+    double lambda0;             /* reference wavelength [m] (sets the unit of length 1/k0) */
+    double dz, dz_push, z_end;  /* s-step, longest particle sub-step, end of the run */
+    double sponge, sponge_y, sponge_rate;
+    int32_t move_x, move_y, window_lag;
+    int32_t self_fields, zeta_filter, k_filter;
+    double push_phase;          /* rad of laser phase per RK4 sub-step */
+    /* analytic plane-wave laser (reference Laser, src/sim.hpp:191-210) */
+    int32_t laser_on, laser_pol, laser_envelope, reserved0;
+    double a0, kL, theta, tau, cep;
+    double eta_c;               /* pulse centre in eta (reference: start_fwhm * tau, sim_setup.cpp:54) */
+    double stop_fwhm;           /* stop when <eta> - eta_c > stop_fwhm * tau (0: never) */
+    double flat_length, ramp_length;   /* G3D_ENV_FLATTOP: plateau length and sin^2 ramp length */
+    double zeta_center;         /* zeta of the bunch centre (time origin of the push, PushCtx.zc) */
+    int32_t freeze_bunch, start_relax, box_mean, precision;
+} g3d_params;
+
+/* A Gaussian or flat-top bunch block (reference Config::Bunch, src/sim.hpp:61-81, the built-in
+ * profiles of sim_bunches.cpp:151-158; shot_noise = random). */
+typedef struct g3d_bunch {
+    double charge_C;            /* |charge| [C] */
+    double gamma, sigx, sigy, sigz, length;   /* length > 0: flat top in z instead of sigz */
+    double emitx, emity, espread, zeta_center, x0, y0;
+    double q;                   /* charge number: -1 electrons, +1 positrons */
+    int64_t nmacro;
+    uint64_t seed;
+} g3d_bunch;
+
+/* Scalars of the run (reference members s, istep, X0, Y0, beta_b, gm2_b, np, lost_total). */
+typedef struct g3d_status {
+    double s, X0, Y0, beta_b, gm2_b, field_energy;
+    int64_t istep, np, lost, stop;
+} g3d_status;
+
+/* Array ids for g3d_array_info / g3d_get_array / g3d_set_array / g3d_device_ptr.
+ * Layouts are the reference's (src/sim.hpp:265-301): spectra [l][j][ix] complex128
+ * (l = slice 0..N-1 or half-cell plane 0..N), jw [comp][hw][j][ix] double (3 x (N+3) planes),
+ * F [comp][fl][j][ix] float (6 x (N+2) planes). */
+#define G3D_A_RX   0
+#define G3D_A_RY   1
+#define G3D_A_EZ   2
+#define G3D_A_BZ   3
+#define G3D_A_LX   4
+#define G3D_A_LY   5
+#define G3D_A_J0X  6
+#define G3D_A_J0Y  7
+#define G3D_A_JKX  8
+#define G3D_A_JKY  9
+#define G3D_A_JKZ  10
+#define G3D_A_JW   11
+#define G3D_A_F    12
+#define G3D_A_COUNT 13
+
+/* ------------------------------------------------------------------ lifetime */
+/* Creates a context on the current CUDA device: device buffers of the reference layouts,
+ * k-tables, zeta weights. Replaces Simulation::Simulation (src/sim_setup.cpp:5-60). */
+int g3d_create(const g3d_grid* grid, const g3d_params* params, struct g3d_ctx** out);
+void g3d_destroy(struct g3d_ctx* ctx);
+/* Message of the last failed call on this context (or of the last failed g3d_create when
+ * ctx is NULL). Never NULL. */
+const char* g3d_last_error(const struct g3d_ctx* ctx);
+/* Library version string. */
+const char* g3d_version(void);
+
+/* ------------------------------------------------------------------ particles */
+/* Replaces Simulation::set_particles / host_particles (src/sim_setup.cpp:166-175). */
+int g3d_set_particles(struct g3d_ctx* ctx, const g3d_particle* parts, int64_t n);
+int g3d_get_particles(struct g3d_ctx* ctx, g3d_particle* out, int64_t capacity, int64_t* n);
+/* Bunch loading on the host with the reference's random sequence (std::mt19937_64 with
+ * std::normal_distribution, src/sim_bunches.cpp:92-217), then uploaded. Sets X0, Y0. */
+int g3d_load_bunches(struct g3d_ctx* ctx, const g3d_bunch* bunches, int32_t count);
+/* The same sampling without a context or a device: fills `out` (capacity records) with the loaded
+ * particles, `n` their count, `lost` those outside the window, X0/Y0 the box origin. The message of a
+ * failure is g3d_last_error(NULL). */
+int g3d_sample_bunches(const g3d_grid* grid, const g3d_params* params, const g3d_bunch* bunches, int32_t count,
+                       g3d_particle* out, int64_t capacity, int64_t* n, int64_t* lost, double* X0, double* Y0);
+
+/* ------------------------------------------------------------------ the march path */
+int g3d_init(struct g3d_ctx* ctx);                  /* Simulation::init, sim_setup.cpp:178-197 (after loading) */
+int g3d_step(struct g3d_ctx* ctx);                  /* Simulation::step, sim_setup.cpp:199-217 */
+int g3d_step_async(struct g3d_ctx* ctx);            /* the same, without the final stream synchronisation */
+int g3d_solve_fields(struct g3d_ctx* ctx, double D);/* Simulation::solve_fields, sim_fields.cpp:309-317 */
+int g3d_currents(struct g3d_ctx* ctx);              /* Simulation::currents, sim_particles.cpp:56-207 */
+int g3d_march(struct g3d_ctx* ctx, double D);       /* Simulation::march, sim_fields.cpp:7-39 */
+int g3d_sponge_and_real_fields(struct g3d_ctx* ctx);/* sim_fields.cpp:156-307 */
+int g3d_push(struct g3d_ctx* ctx, double s0, double s1);   /* Simulation::push, sim_particles.cpp:6-24 */
+int g3d_comoving_field(struct g3d_ctx* ctx);        /* Simulation::comoving_field, sim_fields.cpp:44-151 */
+int g3d_relax_start_field(struct g3d_ctx* ctx);     /* sim_fields.cpp:384-410 */
+int g3d_shift_window(struct g3d_ctx* ctx, int32_t nxs, int32_t nys);  /* sim_setup.cpp:249-281 */
+
+/* ------------------------------------------------------------------ diagnostics */
+/* The 19 weighted sums of Simulation::diagnostics (src/sim_output.cpp:10-26) before the
+ * rank reduction: S[0..13] weighted moments of the alive bunch particles (1, X, Y, zeta, X^2,
+ * Y^2, zeta^2, px, py, pz, gamma, p.khat, pz^2, eta), S[14] their count, S[15] field energy
+ * (code units), S[16] lost particles, S[17] count and S[18] charge of trapped particles. */
+int g3d_diagnostics(struct g3d_ctx* ctx, double out[19]);
+/* Field energy of the slices in code units (Simulation::local_field_energy, sim_output.cpp:55-77). */
+int g3d_field_energy(struct g3d_ctx* ctx, double* out);
+int g3d_get_status(const struct g3d_ctx* ctx, g3d_status* out);
+
+/* ------------------------------------------------------------------ arrays (reference layouts) */
+int g3d_array_info(const struct g3d_ctx* ctx, int32_t which, size_t* count, size_t* elem_bytes);
+int g3d_get_array(struct g3d_ctx* ctx, int32_t which, void* host, size_t count);
+int g3d_set_array(struct g3d_ctx* ctx, int32_t which, const void* host, size_t count);
+/* Device pointer of an array (valid until the next call that reallocates; j0/jk swap each step). */
+void* g3d_device_ptr(struct g3d_ctx* ctx, int32_t which);
+
+/* ------------------------------------------------------------------ checkpoints */
+/* Binary checkpoint of the reference (src/sim_checkpoint.cpp:9-58), one rank, bit-compatible. */
+int g3d_write_checkpoint(struct g3d_ctx* ctx, const char* path);
+int g3d_read_checkpoint(struct g3d_ctx* ctx, const char* path);
+
+/* ------------------------------------------------------------------ stream, timing */
+/* The context's CUDA stream (a cudaStream_t) on which every kernel is launched. */
+void* g3d_stream(struct g3d_ctx* ctx);
+int g3d_synchronize(struct g3d_ctx* ctx);
+/* Per-kernel timing with CUDA events on the context stream: enable (1) / disable (0) and reset. */
+int g3d_profile_enable(struct g3d_ctx* ctx, int32_t on);
+/* Number of kernels timed so far; name, launches and total milliseconds of kernel k. */
+int32_t g3d_profile_count(const struct g3d_ctx* ctx);
+int g3d_profile_get(struct g3d_ctx* ctx, int32_t k, const char** name, int64_t* launches, double* total_ms);
+/* Kernel launches issued on this context since creation (all kernels, profiled or not). */
+int64_t g3d_launch_count(const struct g3d_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* G3D_H */

@@ -1,0 +1,188 @@
+"""Parity of the CUDA march (libg3d.so through the C-ABI) with the reference GEM-PIC-3D FP64 CPU path.
+
+Tolerances (FP64 plain form): spectra and particle coordinates <= 1e-10 relative L2 (the reference's own
+rounding order differs: radix-2 vs radix-8 FFT, atomics order, FMA contraction); F is float in both codes,
+so it agrees to float rounding: <= 1e-6 relative L2. Stage tests feed both sides identical inputs through
+set_array / set_particles and compare one stage at a time; run tests compare init + s-steps with the golden
+fixtures of tests/golden (made by the reference, tests/golden/make_golden.py).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SPECTRA = ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly", "jkx", "jky", "jkz"]
+TOL_SPEC = 1e-10
+TOL_F = 1e-6
+
+
+def golden_cases():
+    from g3d import configs
+    return {
+        "wake16": (configs.config1(nx=16, ny=16, nzeta=32, nmacro=3000, steps=2), 2),
+        "oblique16": (configs.config2(nx=16, ny=16, nzeta=48, nmacro=4000, steps=2, envelope=0), 2),
+    }
+
+
+def compare_state(sim, g, tag):
+    for a in SPECTRA:
+        e = rel_l2(sim.array(a), g[f"{tag}_{a}"])
+        assert e <= TOL_SPEC, (tag, a, e)
+    e = rel_l2(sim.array("F"), g[f"{tag}_F"])
+    assert e <= TOL_F, (tag, "F", e)
+    p, q = sim.host_particles(), g[f"{tag}_particles"]
+    assert np.array_equal(p["alive"], q["alive"])
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        e = rel_l2(p[f], q[f])
+        assert e <= TOL_SPEC, (tag, f, e)
+    d, dr = sim.diagnostics_sums(), g[f"{tag}_diag"]
+    for k in range(19):
+        scale = max(abs(dr[k]), 1e-300)
+        assert abs(d[k] - dr[k]) <= 1e-9 * scale + 1e-300, (tag, "diag", k, d[k], dr[k])
+
+
+@pytest.mark.parametrize("name", ["wake16", "oblique16"])
+def test_run_matches_golden(name, golden):
+    from g3d import Simulation
+    cfg, steps = golden_cases()[name]
+    g = golden(name)
+    sim = Simulation(cfg)
+    sim.load_bunch()
+    p = sim.host_particles()
+    for f in p.dtype.names:
+        assert np.array_equal(p[f], g["loaded_particles"][f]), f
+    sim.init_fields()
+    compare_state(sim, g, "init")
+    for _ in range(steps):
+        sim.step()
+    compare_state(sim, g, f"step{steps}")
+    st = sim.status()
+    assert st.istep == steps and abs(st.s - steps * cfg.params["dz"]) < 1e-12
+
+
+# ---------------------------------------------------------------- stage tests against the live reference
+ref = pytest.importorskip("ref")
+needs_ref = pytest.mark.skipif(not ref.available(), reason="reference build oracle/_ref not present")
+
+
+def pair(cfg):
+    from g3d import Simulation
+    r = ref.RefSimulation(cfg, threads=1)
+    r.load_bunch()
+    s = Simulation(cfg)
+    s.load_bunch()
+    return s, r
+
+
+def stage_cfg(k=2, **kw):
+    from g3d import configs
+    if k == 1:
+        return configs.config1(nx=32, ny=32, nzeta=64, nmacro=20000, steps=2, **kw)
+    return configs.config2(nx=32, ny=16, nzeta=96, nmacro=20000, steps=2, envelope=0, **kw)
+
+
+@needs_ref
+@pytest.mark.parametrize("k", [1, 2])
+def test_currents_stage(k):
+    s, r = pair(stage_cfg(k))
+    s.currents(); r.currents()
+    assert rel_l2(s.array("jw"), r.array("jw")) <= 1e-13
+    for a in ["jkx", "jky", "jkz"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-12, a
+
+
+@needs_ref
+@pytest.mark.parametrize("D", [0.0, 1.0, 250.0])
+def test_march_stage(D):
+    s, r = pair(stage_cfg(2))
+    r.init_fields(); r.currents()          # a physical state: the start field and currents of level s1
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly", "j0x", "j0y", "jkx", "jky", "jkz"]:
+        s.set_array(a, r.array(a))
+    s.march(D); r.march(D)
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-12, a
+
+
+@needs_ref
+def test_sponge_and_real_fields_stage():
+    s, r = pair(stage_cfg(2))
+    r.init_fields(); r.currents(); r.march(1.0)
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly", "jkz"]:
+        s.set_array(a, r.array(a))
+    st = r.status()
+    assert st.gm2_b > 0
+    # the bound field of the sponge uses beta of the bunch: take it from a co-moving field on the same particles
+    s.comoving_field()
+    for a in ["Rx", "Ry", "Ez", "Bz"]:
+        s.set_array(a, r.array(a))
+    s.sponge_and_real_fields(); r.sponge_and_real_fields()
+    for a in ["Rx", "Ry"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-12, a
+    assert rel_l2(s.array("F"), r.array("F")) <= TOL_F
+
+
+@needs_ref
+@pytest.mark.parametrize("k", [1, 2])
+def test_push_stage(k):
+    cfg = stage_cfg(k)
+    s, r = pair(cfg)
+    r.init_fields()
+    s.set_array("F", r.array("F"))
+    dz = cfg.params["dz"]
+    s.push(0.0, dz); r.push(0.0, dz)
+    p, q = s.host_particles(), r.host_particles()
+    assert np.array_equal(p["alive"], q["alive"])
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        assert rel_l2(p[f], q[f]) <= 1e-12, f
+
+
+@needs_ref
+def test_comoving_and_relax_stage():
+    s, r = pair(stage_cfg(1))
+    s.currents(); r.currents()
+    s.comoving_field(); r.comoving_field()
+    for a in ["Rx", "Ry", "Ez", "Bz"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-12, a
+    assert abs(s.status().beta_b - r.status().beta_b) <= 1e-15
+    s.relax_start_field(); r.relax_start_field()
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-11, a
+
+
+@needs_ref
+def test_shift_window_stage():
+    s, r = pair(stage_cfg(1))
+    r.init_fields(); s.init_fields()
+    s.shift_window(3, -2); r.shift_window(3, -2)
+    for a in ["Rx", "Ry", "Ez", "Bz", "j0x", "j0y"]:
+        assert rel_l2(s.array(a), r.array(a)) <= 1e-12, a
+    assert np.array_equal(s.array("F"), r.array("F")) or rel_l2(s.array("F"), r.array("F")) <= TOL_F
+    p, q = s.host_particles(), r.host_particles()
+    assert np.allclose(p["x"], q["x"], rtol=0, atol=1e-12)
+    st, rt = s.status(), r.status()
+    assert st.X0 == rt.X0 and st.Y0 == rt.Y0
+
+
+@needs_ref
+def test_checkpoint_is_read_by_the_reference(tmp_path):
+    """A checkpoint written by libg3d restarts the reference (same binary layout), and back."""
+    cfg = stage_cfg(1)
+    s, r = pair(cfg)
+    s.init_fields(); s.step()
+    path = tmp_path / "checkpoint_000001_r0000.bin"
+    s.write_checkpoint(path)
+    r.read_checkpoint(tmp_path, 1)
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly", "j0x", "j0y"]:
+        assert np.array_equal(s.array(a), r.array(a)), a
+    assert np.array_equal(s.array("F"), r.array("F"))
+    s.step(); r.step()
+    for a in ["Rx", "Ry", "Ez", "Bz"]:
+        assert rel_l2(s.array(a), r.array(a)) <= TOL_SPEC, a
+    r.write_checkpoint(tmp_path)
+    s2 = __import__("g3d").Simulation(cfg)
+    s2.read_checkpoint(tmp_path / "checkpoint_000002_r0000.bin")
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly"]:
+        assert np.array_equal(s2.array(a), r.array(a)), a
+    assert s2.status().istep == 2
