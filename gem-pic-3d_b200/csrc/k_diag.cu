@@ -91,15 +91,34 @@ __global__ void __launch_bounds__(RT) k_centroid(PartsDev P, long np, double X0,
 }
 
 // ------------------------------------------------ mean beta of the alive particles (co-moving field)
-__global__ void __launch_bounds__(RT) k_beta(PartsDev P, long np, double* __restrict__ part) {
-    double acc[2] = {0, 0};
-    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < np; i += long(gridDim.x) * RT) {
-        if (P.alive[i] != 1) continue;
-        const double px = P.px[i], py = P.py[i], pz = P.pz[i], w = P.w[i];
-        acc[0] += w * pz / sqrt(1 + px * px + py * py + pz * pz);
-        acc[1] += w;
+// The reference sums w v_z and w over the particles in array order on the host (sim_fields.cpp:45-47). The
+// mean beta enters 1 - beta^2 = gamma^-2 with a cancellation of 1 - 1/gamma^2, so the sum is taken in the
+// same order with the same IEEE operations (no FMA contraction): every term in parallel, then one warp adds
+// them in index order, 32 terms per coalesced load. Bit for bit the reference's value; used once per start.
+__global__ void k_beta_terms(PartsDev P, long np, double* __restrict__ t, double* __restrict__ w) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < np; i += long(gridDim.x) * blockDim.x) {
+        const bool al = P.alive[i] == 1;
+        const double px = P.px[i], py = P.py[i], pz = P.pz[i], wi = P.w[i];
+        const double g2 = __dadd_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(px, px)), __dmul_rn(py, py)), __dmul_rn(pz, pz));
+        t[i] = al ? __ddiv_rn(__dmul_rn(wi, pz), __dsqrt_rn(g2)) : 0.0;
+        w[i] = al ? wi : 0.0;
     }
-    block_store<2>(acc, part);
+}
+__global__ void k_seq_sum2(const double* __restrict__ t, const double* __restrict__ w, long n, const int32_t* __restrict__ alive,
+                           double* __restrict__ out) {
+    const int lane = threadIdx.x;
+    double s0 = 0, s1 = 0;
+    for (long b = 0; b < n; b += 32) {
+        const long i = b + lane;
+        const double ti = i < n ? t[i] : 0.0, wi = i < n ? w[i] : 0.0;
+        const int al = i < n ? alive[i] : 0;
+        const unsigned live = __ballot_sync(0xffffffffu, al == 1);
+        for (int k = 0; k < 32; ++k) {
+            const double a = __shfl_sync(0xffffffffu, ti, k), c = __shfl_sync(0xffffffffu, wi, k);
+            if (live >> k & 1u) { s0 = __dadd_rn(s0, a); s1 = __dadd_rn(s1, c); }
+        }
+    }
+    if (lane == 0) { out[0] = s0; out[1] = s1; }
 }
 
 template <int NV>
@@ -140,9 +159,16 @@ void launch_centroid(Ctx& c, double out[3]) {
 }
 
 void launch_beta_sums(Ctx& c, double out[2]) {
-    k_beta<<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.red.p);
-    c.check_launch("k_beta");
-    finish<2>(c, out);
+    out[0] = out[1] = 0;
+    if (c.np == 0) return;
+    DevBuf<double> tw;
+    tw.alloc(size_t(2 * c.np + 2), c.stream);
+    k_beta_terms<<<RB, RT, 0, c.stream>>>(c.parts, c.np, tw.p, tw.p + c.np);
+    c.check_launch("k_beta_terms");
+    k_seq_sum2<<<1, 32, 0, c.stream>>>(tw.p, tw.p + c.np, c.np, c.parts.alive, tw.p + 2 * c.np);
+    c.check_launch("k_seq_sum2");
+    G3D_CUDA(cudaMemcpyAsync(out, tw.p + 2 * c.np, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 }  // namespace g3d

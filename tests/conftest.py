@@ -25,6 +25,30 @@ def rel_l2(a, b):
     return d / nb if nb > 0 else d
 
 
+FIELDS = ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly"]
+CURRENTS = ["jkx", "jky", "jkz"]
+
+
+def state_errors(got, ref, names):
+    """Relative L2 errors of a set of spectra measured against the norm of the whole set (the field state
+    vector): {name: (||got - ref|| / ||ref set||, ||got - ref|| / ||ref||)}. E_z, B_z and L are gamma^-2
+    smaller than R for a relativistic bunch, so their own relative error mostly measures the cancellation
+    in them; the parity bound applies to the state norm, the component bound is a sanity check."""
+    total = np.sqrt(sum(np.linalg.norm(np.asarray(ref[n])) ** 2 for n in names))
+    out = {}
+    for n in names:
+        d = np.linalg.norm(np.asarray(got[n]) - np.asarray(ref[n]))
+        nr = np.linalg.norm(np.asarray(ref[n]))
+        out[n] = (d / total if total > 0 else d, d / nr if nr > 0 else d)
+    return out
+
+
+def assert_state(got, ref, names, tol=1e-10, comp_tol=1e-6, tag=""):
+    for n, (e_state, e_comp) in state_errors(got, ref, names).items():
+        assert e_state <= tol, (tag, n, "state-relative", e_state)
+        assert e_comp <= comp_tol, (tag, n, "component-relative", e_comp)
+
+
 @pytest.fixture(scope="session")
 def golden():
     def load(name):
