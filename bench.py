@@ -160,6 +160,24 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+# ------------------------------------------------------------------ rank aggregation
+def max_over_ranks(value, dist=None):
+    """Largest value over the ranks (device time of the slowest replica). NCCL needs a CUDA tensor,
+    gloo a CPU one."""
+    if dist is None or not dist.is_initialized():
+        return float(value)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, steps, world, ms_max):
+    """Whole-job throughput: the units every rank advanced, over the slowest rank's time."""
+    return units_per_rank * steps * world / (ms_max * 1e-3)
+
+
 # ------------------------------------------------------------------ the reference arm
 def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
@@ -228,16 +246,12 @@ def run_g3d(a):
     e1.synchronize()
     sim.synchronize()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     clk = clocks.stop()
     launches = sim.launch_count() - l0
     prof = sim.profile_results()
     sim.profile(False)
-    value = P * a.steps * world / (ms * 1e-3)
+    value = job_rate(P, a.steps, world, ms)
 
     # ---------------- roofline of the dominant kernel
     import json as _json
@@ -285,12 +299,8 @@ def run_g3d(a):
         x1.record(stream)
         x1.synchronize()
         wall = time.perf_counter() - t0
-        ems = max(x0.elapsed_time(x1), wall * 1e3)
-        if dist:
-            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": P * a.e2e_steps * world / (ems * 1e-3), "unit": UNIT,
+        ems = max_over_ranks(max(x0.elapsed_time(x1), wall * 1e3), dist)
+        e2e = {"value": job_rate(P, a.e2e_steps, world, ems), "unit": UNIT,
                "h2d_bytes_per_step": P * 104, "d2h_bytes_per_step": P * 104 + 19 * 8,
                "steps": a.e2e_steps,
                "path": "g3d_set_particles (pinned host records) -> g3d_step -> g3d_get_particles + g3d_diagnostics"}

@@ -14,6 +14,8 @@ namespace g3d {
 // (Simulation::Simulation, setup_y_fourier, setup_zeta: src/sim_setup.cpp:17-35, 63-82, 148-164).
 struct Geo {
     int nx, ny, nk, N, a, b, ns, nh;     // nh = ns + 3 planes of the raw deposit
+    int H;                               // nx/2 + 1 columns of a half spectrum (k_x = 0 .. nx/2)
+    long nkh;                            // ny * H modes of a half-spectrum plane
     int yf, zeta_uniform;
     double dx, dy, Lx, Ly;
     const double *kxd, *kxs, *filt, *maskx;
@@ -103,6 +105,8 @@ struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 struct Ctx {
     // grid (single rank: a = 0, b = ns = N)
     int nx = 0, ny = 0, N = 0, a = 0, b = 0, ns = 0, nk = 0;
+    int H = 0;                                   // nx/2 + 1: spectra are kept for k_x = 0 .. nx/2
+    long nkh = 0;                                // ny * H
     double dx = 0, dy = 0;
     bool yf = true;
     g3d_params P{};
@@ -112,14 +116,14 @@ struct Ctx {
     DevBuf<double> kxd, kxs, filt, maskx, kyd, kys, filty, masky_n, masky_h, iD, iA;
     DevBuf<double> zs, hcg, wlo, whi, wsl;
     DevBuf<cpx> twx, twy;
-    // field state (reference layouts, src/sim.hpp:265-276)
+    // field state: the reference's arrays (src/sim.hpp:265-276); spectra as half spectra [plane][j][k_x <= nx/2]
     DevBuf<cpx> Rx, Ry, Ez, Bz, Lx, Ly;          // ns planes
     DevBuf<cpx> j0x, j0y, jkx, jky, jkz;         // ns+1 half-cell planes
     DevBuf<cpx> jzg;                             // 2 ghost planes of filtered j_z (zero on one rank)
-    DevBuf<double> jw;                           // 3 x (ns+3) planes
-    DevBuf<float> F;                             // 6 x (ns+2) planes
-    DevBuf<cpx> S1, S2, S3;                      // FFT scratch, ns+1 planes each
-    DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns planes
+    DevBuf<double> jw;                           // 3 x (ns+3) real planes
+    DevBuf<float> F;                             // 6 x (ns+2) real planes
+    DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
+    DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
     // particles
     DevBuf<double> pbuf_d;                       // 11 double columns
@@ -128,6 +132,8 @@ struct Ctx {
     DevBuf<g3d_particle> pstage;                 // device staging of the 104-byte records
     PartsDev parts{};
     long np = 0, pcap = 0;
+    DevBuf<int32_t> perm;                        // particles in cell order (k_sort.cu); storage order unchanged
+    int steps_since_sort = 0;
     // reductions
     DevBuf<double> red;                          // per-block partial sums
     std::vector<double> red_h;
@@ -171,6 +177,9 @@ void launch_centroid(Ctx& c, double out[3]);
 void launch_diag(Ctx& c, double S[19]);
 double launch_field_energy(Ctx& c);
 void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy);
+void launch_half_to_full(Ctx& c, const cpx* half, cpx* full, long planes);
+void launch_full_to_half(Ctx& c, const cpx* full, cpx* half, long planes);
+void sort_particles(Ctx& c);                // refresh perm
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)
 

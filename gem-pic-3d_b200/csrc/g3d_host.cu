@@ -20,6 +20,7 @@ bool pow2_ok(int n) { return n >= 4 && n <= 512 && (n & (n - 1)) == 0; }
 Geo Ctx::geo() const {
     Geo g;
     g.nx = nx; g.ny = ny; g.nk = nk; g.N = N; g.a = a; g.b = b; g.ns = ns; g.nh = ns + 3;
+    g.H = H; g.nkh = nkh;
     g.yf = yf ? 1 : 0; g.zeta_uniform = zax.uniform;
     g.dx = dx; g.dy = dy; g.Lx = nx * dx; g.Ly = ny * dy;
     g.kxd = kxd.p; g.kxs = kxs.p; g.filt = filt.p; g.maskx = maskx.p;
@@ -79,6 +80,7 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
         if (!(G.zeta[m + 1] > G.zeta[m])) throw Error(G3D_ERR_ARG, "zeta slices must increase");
     c.P = P;
     c.N = G.nzeta; c.nx = G.nx; c.ny = G.ny; c.nk = c.nx * c.ny;
+    c.H = c.nx / 2 + 1; c.nkh = long(c.ny) * c.H;
     c.a = 0; c.ns = c.N; c.b = c.N;
     c.dx = G.Lx / c.nx;
     c.yf = true;
@@ -148,14 +150,15 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
         return t;
     };
     c.twx.upload(tw(nx), s); c.twy.upload(tw(ny), s);
-    // field buffers (reference layouts)
-    const size_t pl = size_t(c.nk), ns = size_t(c.ns);
-    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly, &c.S3}) p->alloc(ns * pl, s);
-    for (DevBuf<cpx>* p : {&c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz, &c.S1, &c.S2}) p->alloc((ns + 1) * pl, s);
-    c.jzg.alloc(2 * pl, s);
+    // field buffers: real planes of the reference layouts, spectra as half spectra
+    const size_t pl = size_t(c.nk), ph = size_t(c.nkh), ns = size_t(c.ns);
+    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly}) p->alloc(ns * ph, s);
+    for (DevBuf<cpx>* p : {&c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz}) p->alloc((ns + 1) * ph, s);
+    for (DevBuf<cpx>& w : c.W) w.alloc((ns + 1) * ph, s);
+    c.jzg.alloc(2 * ph, s);
     c.jw.alloc(3 * (ns + 3) * pl, s);
     c.F.alloc(6 * (ns + 2) * pl, s);
-    c.rscratch.alloc(ns * pl, s);
+    c.rscratch.alloc(ns * ph, s);
     c.red.alloc(size_t(297) * 17, s);
     // the plane wave (reference sim_setup.cpp:51-54; eta_c given directly)
     c.laser.on = P.laser_on; c.laser.pol = P.laser_pol; c.laser.env = P.laser_envelope;
@@ -192,7 +195,7 @@ static void set_particles(Ctx& c, const g3d_particle* v, long n) {
     if (c.pstage.n < size_t(n)) c.pstage.alloc(size_t(n) + size_t(n) / 4 + 64, c.stream);
     G3D_CUDA(cudaMemcpyAsync(c.pstage.p, v, size_t(n) * sizeof(g3d_particle), cudaMemcpyHostToDevice, c.stream));
     launch_parts_unpack(c, n);
-    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    sort_particles(c);
 }
 
 static void get_particles_into(Ctx& c, g3d_particle* out) {
@@ -310,8 +313,8 @@ static void comoving_field(Ctx& c) {
     launch_comoving(c, beta, gm2);
 }
 static void relax_start_field(Ctx& c) {
-    const size_t n = size_t(c.ns) * c.nk, nj = size_t(c.ns + 1) * c.nk;
-    cpx* dxr = c.S1.p; cpx* dyr = c.S3.p;          // R of the bunch's beta (S1 and S3 are free here)
+    const size_t n = size_t(c.ns) * c.nkh, nj = size_t(c.ns + 1) * c.nkh;
+    cpx* dxr = c.W[4].p; cpx* dyr = c.W[5].p;      // R of the bunch's beta (the co-moving solve uses W3)
     launch_copy_c(c, dxr, c.Rx.p, n);
     launch_copy_c(c, dyr, c.Ry.p, n);
     c.comoving_c_ = true; comoving_field(c); c.comoving_c_ = false;
@@ -363,6 +366,7 @@ static void init_fields(Ctx& c) {
     window_shift_post(c);
 }
 static void step(Ctx& c, bool sync) {
+    if (++c.steps_since_sort >= 16) sort_particles(c);
     window_shift_start(c);
     launch_push(c, c.s, c.s + c.P.dz);
     c.s += c.P.dz; ++c.istep;
@@ -373,22 +377,57 @@ static void step(Ctx& c, bool sync) {
 static bool finished(const Ctx& c) { return c.s >= c.P.z_end - 1e-9 || c.stop_; }
 
 // ---------------------------------------------------------------- arrays
-static void* array_ptr(Ctx& c, int which, size_t& count, size_t& eb) {
+// Storage of an array id: device pointer, element count and size of the storage, and the planes of a
+// spectrum (0 for the real arrays jw and F, which are stored in the reference layout).
+struct ArrayRef { void* p; size_t count, eb; long planes; };
+static ArrayRef array_ref(Ctx& c, int which) {
     DevBuf<cpx>* cb = nullptr;
+    long planes = c.ns;
     switch (which) {
         case G3D_A_RX: cb = &c.Rx; break; case G3D_A_RY: cb = &c.Ry; break;
         case G3D_A_EZ: cb = &c.Ez; break; case G3D_A_BZ: cb = &c.Bz; break;
         case G3D_A_LX: cb = &c.Lx; break; case G3D_A_LY: cb = &c.Ly; break;
-        case G3D_A_J0X: cb = &c.j0x; break; case G3D_A_J0Y: cb = &c.j0y; break;
-        case G3D_A_JKX: cb = c.jk_is_j0 ? &c.j0x : &c.jkx; break;
-        case G3D_A_JKY: cb = c.jk_is_j0 ? &c.j0y : &c.jky; break;
-        case G3D_A_JKZ: cb = &c.jkz; break;
-        case G3D_A_JW: count = c.jw.n; eb = sizeof(double); return c.jw.p;
-        case G3D_A_F: count = c.F.n; eb = sizeof(float); return c.F.p;
+        case G3D_A_J0X: cb = &c.j0x; planes = c.ns + 1; break;
+        case G3D_A_J0Y: cb = &c.j0y; planes = c.ns + 1; break;
+        case G3D_A_JKX: cb = c.jk_is_j0 ? &c.j0x : &c.jkx; planes = c.ns + 1; break;
+        case G3D_A_JKY: cb = c.jk_is_j0 ? &c.j0y : &c.jky; planes = c.ns + 1; break;
+        case G3D_A_JKZ: cb = &c.jkz; planes = c.ns + 1; break;
+        case G3D_A_JW: return ArrayRef{c.jw.p, c.jw.n, sizeof(double), 0};
+        case G3D_A_F: return ArrayRef{c.F.p, c.F.n, sizeof(float), 0};
         default: throw Error(G3D_ERR_ARG, "unknown array id " + std::to_string(which));
     }
-    count = cb->n; eb = sizeof(cpx);
-    return cb->p;
+    return ArrayRef{cb->p, cb->n, sizeof(cpx), planes};
+}
+// Element count of an array in the reference layout (spectra in full: planes x ny x nx).
+static size_t ref_count(Ctx& c, const ArrayRef& a) { return a.planes ? size_t(a.planes) * c.nk : a.count; }
+
+// Copy out in the reference layout (spectra expanded from the half spectrum by X(-k) = conj X(k)).
+static void get_array(Ctx& c, int which, void* host) {
+    const ArrayRef a = array_ref(c, which);
+    if (!a.planes) {
+        if (a.count) G3D_CUDA(cudaMemcpyAsync(host, a.p, a.count * a.eb, cudaMemcpyDeviceToHost, c.stream));
+    } else {
+        DevBuf<cpx> full;
+        full.alloc(ref_count(c, a), c.stream);
+        launch_half_to_full(c, static_cast<const cpx*>(a.p), full.p, a.planes);
+        G3D_CUDA(cudaMemcpyAsync(host, full.p, full.bytes(), cudaMemcpyDeviceToHost, c.stream));
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+// Copy in from the reference layout (spectra keep k_x = 0 .. nx/2: the data are the spectra of real fields).
+static void set_array(Ctx& c, int which, const void* host) {
+    const ArrayRef a = array_ref(c, which);
+    if (!a.planes) {
+        if (a.count) G3D_CUDA(cudaMemcpyAsync(a.p, host, a.count * a.eb, cudaMemcpyHostToDevice, c.stream));
+    } else {
+        DevBuf<cpx> full;
+        full.alloc(ref_count(c, a), c.stream);
+        G3D_CUDA(cudaMemcpyAsync(full.p, host, full.bytes(), cudaMemcpyHostToDevice, c.stream));
+        launch_full_to_half(c, full.p, static_cast<cpx*>(a.p), a.planes);
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    }
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 // ---------------------------------------------------------------- checkpoints (sim_checkpoint.cpp:9-58)
@@ -416,7 +455,7 @@ std::vector<T> get(FILE* f) {
     return v;
 }
 template <class T>
-std::vector<T> d2h(Ctx& c, const T* p, size_t n) {
+[[maybe_unused]] std::vector<T> d2h(Ctx& c, const T* p, size_t n) {
     std::vector<T> v(n);
     if (n) G3D_CUDA(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
@@ -436,9 +475,8 @@ static void write_checkpoint(Ctx& c, const char* path) {
     try {
         if (std::fwrite(&h, sizeof h, 1, f) != 1) throw Error(G3D_ERR_IO, "checkpoint: write error");
         for (int w : {G3D_A_RX, G3D_A_RY, G3D_A_EZ, G3D_A_BZ, G3D_A_LX, G3D_A_LY, G3D_A_J0X, G3D_A_J0Y}) {
-            size_t n, eb;
-            const cpx* p = static_cast<const cpx*>(array_ptr(c, w, n, eb));
-            const std::vector<cpx> v = d2h(c, p, n);
+            std::vector<cpx> v(ref_count(c, array_ref(c, w)));
+            get_array(c, w, v.data());
             put(f, v.data(), v.size());
         }
         for (int k = 0; k < 3; ++k) put<cpx>(f, nullptr, 0);      // js0x, js0y, js0z: no plasma
@@ -478,11 +516,11 @@ static void read_checkpoint(Ctx& c, const char* path) {
         f = nullptr;
         if (fv.size() != c.F.n) throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
         c.jk_is_j0 = false;
-        DevBuf<cpx>* dst[8] = {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly, &c.j0x, &c.j0y};
-        for (int k = 0; k < 8; ++k) {
-            if (arrays[size_t(k)].size() != dst[k]->n) throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
-            G3D_CUDA(cudaMemcpyAsync(dst[k]->p, arrays[size_t(k)].data(), dst[k]->bytes(), cudaMemcpyHostToDevice, c.stream));
-        }
+        const int ids[8] = {G3D_A_RX, G3D_A_RY, G3D_A_EZ, G3D_A_BZ, G3D_A_LX, G3D_A_LY, G3D_A_J0X, G3D_A_J0Y};
+        for (int k = 0; k < 8; ++k)
+            if (arrays[size_t(k)].size() != ref_count(c, array_ref(c, ids[k])))
+                throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
+        for (int k = 0; k < 8; ++k) set_array(c, ids[k], arrays[size_t(k)].data());
         for (int k = 8; k < 11; ++k)
             if (!arrays[size_t(k)].empty()) throw Error(G3D_ERR_IO, std::string(path) + ": streaming currents present but no plasma");
         if (!jv.empty()) throw Error(G3D_ERR_IO, std::string(path) + ": joining particles present but no plasma");
@@ -663,34 +701,31 @@ int g3d_get_status(const g3d_ctx* ctx, g3d_status* o) {
 
 int g3d_array_info(const g3d_ctx* ctx, int32_t which, size_t* count, size_t* eb) {
     return guarded(const_cast<g3d_ctx*>(ctx), [&] {
-        size_t n, e;
-        g3d::array_ptr(const_cast<g3d_ctx*>(ctx)->c, which, n, e);
-        *count = n; *eb = e;
+        Ctx& c = const_cast<g3d_ctx*>(ctx)->c;
+        const g3d::ArrayRef a = g3d::array_ref(c, which);
+        *count = g3d::ref_count(c, a); *eb = a.eb;
     });
 }
 int g3d_get_array(g3d_ctx* ctx, int32_t which, void* host, size_t count) {
     return guarded(ctx, [&] {
-        size_t n, e;
-        void* p = g3d::array_ptr(ctx->c, which, n, e);
+        Ctx& c = ctx->c;
+        const size_t n = g3d::ref_count(c, g3d::array_ref(c, which));
         if (count != n) throw Error(G3D_ERR_ARG, "count differs from the array size " + std::to_string(n));
-        if (n) G3D_CUDA(cudaMemcpyAsync(host, p, n * e, cudaMemcpyDeviceToHost, ctx->c.stream));
-        G3D_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        g3d::get_array(c, which, host);
     });
 }
 int g3d_set_array(g3d_ctx* ctx, int32_t which, const void* host, size_t count) {
     return guarded(ctx, [&] {
         Ctx& c = ctx->c;
         if (which == G3D_A_JKX || which == G3D_A_JKY || which == G3D_A_J0X || which == G3D_A_J0Y) g3d::materialize_jk(c);
-        size_t n, e;
-        void* p = g3d::array_ptr(c, which, n, e);
+        const size_t n = g3d::ref_count(c, g3d::array_ref(c, which));
         if (count != n) throw Error(G3D_ERR_ARG, "count differs from the array size " + std::to_string(n));
-        if (n) G3D_CUDA(cudaMemcpyAsync(p, host, n * e, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaStreamSynchronize(c.stream));
+        g3d::set_array(c, which, host);
     });
 }
 void* g3d_device_ptr(g3d_ctx* ctx, int32_t which) {
     void* p = nullptr;
-    guarded(ctx, [&] { size_t n, e; p = g3d::array_ptr(ctx->c, which, n, e); });
+    guarded(ctx, [&] { p = g3d::array_ref(ctx->c, which).p; });
     return p;
 }
 

@@ -1,13 +1,15 @@
-// Current deposition of the beam list, the (1,2,1)/4 zeta filter, the forward transverse FFT pair and
-// the transverse filters: Simulation::currents of the reference (src/sim_particles.cpp:56-207), Fourier y.
+// Current deposition of the beam list, the (1,2,1)/4 zeta filter, the forward transverse FFTs and the
+// transverse filters: Simulation::currents of the reference (src/sim_particles.cpp:56-207), Fourier y.
 //
-// Kernels (per call):
-//   k_deposit      one thread per particle: NGP over the zeta half-cell, TSC in x and y, FP64 atomics
-//                  into the raw current planes jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106)
-//   k_cur_cols     per (half-cell plane, tile of 8 columns): zeta filter of the raw planes (:120-138),
-//                  packing jx + i jy and jz, FFT along y of both -> S1, jkz
-//   k_cur_rows     per (half-cell plane, pairs of rows j and ny-j): FFT along x of both fields, then the
-//                  Hermitian split of jx + i jy and the cos^2 k-filters (:146-156) -> jkx, jky, jkz
+// The currents are real fields, so their spectra are Hermitian; only k_x = 0 .. nx/2 is kept (H = nx/2 + 1
+// columns, [plane][j][k_x]).
+//   k_deposit   one thread per particle: NGP over the zeta half-cell, TSC in x and y, FP64 atomics into the raw
+//               current planes jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106)
+//   k_cur_rows  per (block of rows, half-cell plane): zeta filter (sim_particles.cpp:120-138) of the three raw
+//               planes, then per row one complex FFT along x of jx + i jy, split by Hermitian symmetry into the
+//               half spectra of jx and jy, and one of jz -> three half-spectrum planes (scratch W0, W1, W2)
+//   k_cur_cols  per (half-cell plane, tile of 8 k_x columns): FFT along y, the cos^2 filters and the k_perp = 0
+//               removal (sim_particles.cpp:146-156) -> jkx, jky, jkz
 #include "g3d_ctx.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -15,9 +17,12 @@
 namespace g3d {
 
 // ---------------------------------------------------------------- deposit
-__global__ void __launch_bounds__(256) k_deposit(PartsDev P, long np, Geo g, double* __restrict__ J) {
-    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (ip >= np || P.alive[ip] != 1) return;
+__global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
+                                                double* __restrict__ J) {
+    const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const long ip = perm[t];                 // cell order: neighbouring threads add into the same lines
+    if (P.alive[ip] != 1) return;
     int m; double fz;
     g.zax.locate(P.zeta[ip], m, fz);
     const int hw = m - (g.a - 2);
@@ -44,102 +49,93 @@ __global__ void __launch_bounds__(256) k_deposit(PartsDev P, long np, Geo g, dou
         }
 }
 
-// ---------------------------------------------------------------- zeta filter + FFT along y
-// Tile of CW columns x NY rows of one half-cell plane; NY/E threads per column.
-template <int NY, int CW>
-__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const double* __restrict__ J, cpx* __restrict__ S1,
-                                                                   cpx* __restrict__ JZ, int zf) {
-    using S = FftShape<NY>;
+// ---------------------------------------------------------------- zeta filter + FFT along x (rows)
+constexpr int CUR_NT = 128;     // threads of the row kernel
+
+// One CTA = LPC rows of one half-cell plane. The filter reads the three raw planes hk, hk+1, hk+2; the CTAs
+// of neighbouring planes run together (blockIdx.x = rows is the fast index), so each raw plane comes from
+// DRAM once and from L2 for its two neighbours.
+template <int NX>
+__global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __restrict__ J, cpx* __restrict__ TX,
+                                                    cpx* __restrict__ TY, cpx* __restrict__ TZ, int zf) {
+    using S = FftShape<NX>;
+    constexpr int LPC = CUR_NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
-    cpx* s0 = sm;                    // jx + i jy
-    cpx* s1 = sm + NY * CW;          // jz
-    const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
-    const int nx = g.nx;
-    const long nk = g.nk;
-    const int hc_ = g.a - 1 + hk, hw = hk + 1;
-    const bool live = hc_ >= 0 && hc_ <= g.N - 2;
-    const double* Jp[3] = {J, J + long(g.nh) * nk, J + 2L * g.nh * nk};
-    double hm = 0, h0 = 1, hp = 0;
-    if (live && zf && !g.zeta_uniform) { hm = g.hcg[hc_ + 1]; h0 = g.hcg[hc_ + 2]; hp = g.hcg[hc_ + 3]; }
-    for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, c = e - p * CW;
-        const long i = long(p) * nx + c0 + c;
+    cpx* a0 = sm;                    // jx + i jy lines
+    cpx* a1 = sm + LPC * RS;         // jz lines
+    const int tid = threadIdx.x, r0 = blockIdx.x * LPC, hk = blockIdx.y;
+    const long nk = g.nk, cpl = long(g.nh) * nk, nkh = long(g.ny) * H;
+    const int hw = hk + 1, hc = g.a - 1 + hk;
+    const bool live = hc >= 0 && hc <= g.N - 2;
+    double wm = 0.25, w0 = 0.5, wp = 0.25, inv = 1.0;
+    if (zf && !g.zeta_uniform && live) { wm = 0.25 * g.hcg[hc + 1]; w0 = 0.5 * g.hcg[hc + 2]; wp = 0.25 * g.hcg[hc + 3]; inv = g.hcg[hc + 2]; }
+    for (int e = tid; e < LPC * NX; e += CUR_NT) {
+        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         double v[3] = {0, 0, 0};
-        if (live) {
+        if (live && row < g.ny) {
+            const long i = long(row) * NX + p;
 #pragma unroll
             for (int comp = 0; comp < 3; ++comp) {
-                const double* Jc = Jp[comp];
-                if (zf && g.zeta_uniform)
-                    v[comp] = 0.25 * Jc[(hw - 1) * nk + i] + 0.5 * Jc[hw * nk + i] + 0.25 * Jc[(hw + 1) * nk + i];
-                else if (zf)
-                    v[comp] = (0.25 * hm * Jc[(hw - 1) * nk + i] + 0.5 * h0 * Jc[hw * nk + i] + 0.25 * hp * Jc[(hw + 1) * nk + i]) / h0;
-                else
-                    v[comp] = Jc[hw * nk + i];
+                const double* Jc = J + comp * cpl + i;
+                const double jm = __ldg(Jc + (hw - 1) * nk), j0 = __ldg(Jc + hw * nk), jp = __ldg(Jc + (hw + 1) * nk);
+                if (zf && g.zeta_uniform) v[comp] = 0.25 * jm + 0.5 * j0 + 0.25 * jp;
+                else if (zf) v[comp] = (wm * jm + w0 * j0 + wp * jp) / inv;
+                else v[comp] = j0;
             }
         }
-        s0[e] = C(v[0], v[1]);
-        s1[e] = C(v[2], 0.0);
-    }
-    __syncthreads();
-    const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    cpx* o0 = S1 + long(hk) * nk;
-    cpx* o1 = JZ + long(hk) * nk;
-    for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, cc = e - p * CW;
-        const long i = long(p) * nx + c0 + cc;
-        o0[i] = s0[e];
-        o1[i] = s1[e];
-    }
-}
-
-// ---------------------------------------------------------------- FFT along x of row pairs + unpack
-// Slots 2u and 2u+1 of the CTA hold the rows j and (ny - j) % ny of one half-cell plane.
-template <int NX>
-__global__ void __launch_bounds__(128) k_cur_rows(Geo g, cpx* __restrict__ S1, cpx* __restrict__ JX, cpx* __restrict__ JY,
-                                                 cpx* __restrict__ JZ, int keep0) {
-    using S = FftShape<NX>;
-    constexpr int LPC = 128 / S::T, PPC = LPC / 2, RS = row_stride<NX>();
-    extern __shared__ cpx sm[];
-    cpx* a0 = sm;                   // jx + i jy rows
-    cpx* a1 = sm + LPC * RS;        // jz rows
-    const int hk = blockIdx.y, tid = threadIdx.x;
-    const int ny = g.ny;
-    const long nk = g.nk;
-    const long base = long(hk) * nk;
-    auto row_of = [&](int slot, bool& valid) {
-        const int jp = blockIdx.x * PPC + (slot >> 1);
-        valid = jp <= ny / 2;
-        return (slot & 1) ? (ny - jp) % ny : jp;
-    };
-    for (int e = tid; e < LPC * NX; e += 128) {
-        const int r = e / NX, p = e - r * NX;
-        bool valid;
-        const int row = row_of(r, valid);
-        cpx u0 = C(0), u1 = C(0);
-        if (valid) { const long i = base + long(row) * NX + p; u0 = S1[i]; u1 = JZ[i]; }
-        a0[r * RS + p + (p >> 3)] = u0;
-        a1[r * RS + p + (p >> 3)] = u1;
+        a0[rr * RS + p + (p >> 3)] = C(v[0], v[1]);
+        a1[rr * RS + p + (p >> 3)] = C(v[2], 0.0);
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
-    for (int e = tid; e < LPC * NX; e += 128) {
-        const int rr = e / NX, p = e - rr * NX;
-        bool valid;
-        const int row = row_of(rr, valid);
-        if (!valid) continue;
-        if ((rr & 1) && row == row_of(rr ^ 1, valid)) continue;    // a self-paired row is written once
-        const int pm = (NX - p) % NX;
-        const cpx z = a0[rr * RS + p + (p >> 3)], zm = conj(a0[(rr ^ 1) * RS + pm + (pm >> 3)]);
-        const double f = (p == 0 && row == 0 && !keep0) ? 0.0 : g.filt[p] * g.filty[row];
+    const long base = long(hk) * nkh;
+    for (int e = tid; e < LPC * H; e += CUR_NT) {
+        const int rr = e / H, kx = e - rr * H, row = r0 + rr;
+        if (row >= g.ny) continue;
+        const int km = (NX - kx) % NX;
+        const cpx z = a0[rr * RS + kx + (kx >> 3)], zm = conj(a0[rr * RS + km + (km >> 3)]);
         const cpx d = z - zm;
-        const long i = base + long(row) * NX + p;
-        JX[i] = f * (0.5 * (z + zm));
-        JY[i] = f * (0.5 * C(d.y, -d.x));
-        JZ[i] = f * a1[rr * RS + p + (p >> 3)];
+        const long o = base + long(row) * H + kx;
+        TX[o] = 0.5 * (z + zm);
+        TY[o] = 0.5 * C(d.y, -d.x);
+        TZ[o] = a1[rr * RS + kx + (kx >> 3)];
+    }
+}
+
+// ---------------------------------------------------------------- FFT along y (columns) + k-filters
+template <int NY, int CW>
+__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const cpx* __restrict__ TX, const cpx* __restrict__ TY,
+                                                                   const cpx* __restrict__ TZ, cpx* __restrict__ JX,
+                                                                   cpx* __restrict__ JY, cpx* __restrict__ JZ, int keep0) {
+    using S = FftShape<NY>;
+    extern __shared__ cpx sm[];
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * CW;
+    cpx* s2 = sm + 2 * NY * CW;
+    const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
+    const int H = g.H;
+    const long base = long(hk) * g.nkh;
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, c = e - p * CW, kx = c0 + c;
+        cpx u0 = C(0), u1 = C(0), u2 = C(0);
+        if (kx < H) { const long o = base + long(p) * H + kx; u0 = TX[o]; u1 = TY[o]; u2 = TZ[o]; }
+        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+    }
+    __syncthreads();
+    const int c = tid % CW, t = tid / CW;
+    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s2, ColAddr<CW>{c}, t, g.twy);
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, cc = e - p * CW, kx = c0 + cc;
+        if (kx >= H) continue;
+        const double f = (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p];
+        const long o = base + long(p) * H + kx;
+        JX[o] = f * s0[e];
+        JY[o] = f * s1[e];
+        JZ[o] = f * s2[e];
     }
 }
 
@@ -149,43 +145,40 @@ void launch_deposit(Ctx& c) {
     if (c.np == 0) return;
     const int tok = c.prof_begin("deposit");
     const unsigned blocks = unsigned((c.np + 255) / 256);
-    k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.np, c.geo(), c.jw.p);
+    k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p);
     c.check_launch("k_deposit");
     c.prof_end(tok);
 }
 
-template <int NY>
-static void cur_cols(Ctx& c) {
-    constexpr int CW = 8;
-    const Geo g = c.geo();
-    const int cw = c.nx < CW ? c.nx : CW;
-    if (cw != CW) throw Error(G3D_ERR_ARG, "nx must be >= 8");
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
-    auto kern = k_cur_cols<NY, CW>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const dim3 grid(unsigned(c.nx / CW), unsigned(c.ns + 1));
-    const int tok = c.prof_begin("cur_cols");
-    kern<<<grid, CW * FftShape<NY>::T, smem, c.stream>>>(g, c.jw.p, c.S1.p, c.jkz.p, c.P.zeta_filter ? 1 : 0);
-    c.check_launch("k_cur_cols");
-    c.prof_end(tok);
-}
 template <int NX>
-static void cur_rows(Ctx& c, bool keep0) {
+static void cur_rows(Ctx& c) {
     using S = FftShape<NX>;
-    constexpr int LPC = 128 / S::T, PPC = LPC / 2;
+    constexpr int LPC = CUR_NT / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
     auto kern = k_cur_rows<NX>;
     G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const dim3 grid(unsigned((c.ny / 2 + 1 + PPC - 1) / PPC), unsigned(c.ns + 1));
+    const dim3 grid(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1));
     const int tok = c.prof_begin("cur_rows");
-    kern<<<grid, 128, smem, c.stream>>>(c.geo(), c.S1.p, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0);
+    kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, c.W[0].p, c.W[1].p, c.W[2].p, c.P.zeta_filter ? 1 : 0);
     c.check_launch("k_cur_rows");
+    c.prof_end(tok);
+}
+template <int NY>
+static void cur_cols(Ctx& c, bool keep0) {
+    constexpr int CW = 8;
+    const size_t smem = size_t(3) * NY * CW * sizeof(cpx);
+    auto kern = k_cur_cols<NY, CW>;
+    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const dim3 grid(unsigned((c.H + CW - 1) / CW), unsigned(c.ns + 1));
+    const int tok = c.prof_begin("cur_cols");
+    kern<<<grid, CW * FftShape<NY>::T, smem, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0);
+    c.check_launch("k_cur_cols");
     c.prof_end(tok);
 }
 
 void launch_cur_fft(Ctx& c, bool keep0) {
-    G3D_DISPATCH_N(c.ny, NY, cur_cols<NY>(c));
-    G3D_DISPATCH_N(c.nx, NX, cur_rows<NX>(c, keep0));
+    G3D_DISPATCH_N(c.nx, NX, cur_rows<NX>(c));
+    G3D_DISPATCH_N(c.ny, NY, cur_cols<NY>(c, keep0));
 }
 
 }  // namespace g3d

@@ -1,13 +1,19 @@
 // Sponge and real-space fields (Simulation::sponge_and_real_fields, src/sim_fields.cpp:156-307, Fourier y),
-// the window shift (src/sim_setup.cpp:249-281) and small elementwise kernels.
+// the window shift (src/sim_setup.cpp:249-281), the half <-> full spectrum layouts and small elementwise kernels.
+//
+// The spectra are kept for k_x = 0 .. nx/2 (H columns): every field is real, so X(-k) = conj X(k).
+// A transverse 2-D transform is a pass along y over the H columns (k_*_cols) and a pass along x over the
+// rows (k_*_rows), where a row's other half follows from X(nx - k_x) = conj X(k_x) of the y-transformed data.
 //
 // Sponge: the radiation part R - R_b of the forward field (R_b = (1 + beta) E_perp of the slice charge,
-// psi = (rho + gamma^-2 d_zeta^2 rho / k^2) / k^2) is multiplied in real space by the separable mask
-// maskx(x) masky(y). Three kernels: k_sp_rows (bound field psi -> S2, pack R - R_b, inverse FFT along x),
-// k_sp_cols (inverse FFT along y, 1/(nx ny), mask, forward FFT along y), k_sp_rowpairs (forward FFT along
-// x, Hermitian split, + R_b).
-// Real fields: k_rf_cols packs R_x + i R_y, L_x + i L_y, E_z + i B_z and transforms them along y; k_rf_rows
-// transforms along x, normalises and writes the six float components of F.
+// psi = (rho + gamma^-2 d_zeta^2 rho / k^2) / k^2) is multiplied in real space by maskx(x) masky(y):
+//   k_sp_cols_inv  bound field psi -> W3, U = R_x - R_bx and V = R_y - R_by, inverse FFT along y
+//   k_sp_rows      per row: u + i v by one inverse FFT along x, 1/(nx ny), the mask, one forward FFT along x,
+//                  split back into the half spectra of u and v
+//   k_sp_cols_fwd  forward FFT along y, + R_b
+// Real fields: k_rf_cols transforms R_x, R_y, L_x, L_y, E_z, B_z along y (a pair per CTA); k_rf_rows rebuilds R_x + i R_y,
+// L_x + i L_y, E_z + i B_z per row, transforms along x and writes the six float components of F with the
+// reference's combinations (E_x = (r1 + l1)/2, ...).
 #include "g3d_ctx.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -18,11 +24,11 @@ namespace {
 constexpr int NT = 128;    // threads of the row kernels
 constexpr int CW = 8;      // columns per tile of the column kernels
 
-// psi of the slice charge of slice n = a + l at the mode i (reference: the Fourier-y lambda of
-// sim_fields.cpp:176-201)
+// psi of the slice charge of slice n = a + l at the half-spectrum mode i (reference: the Fourier-y lambda
+// of sim_fields.cpp:176-201)
 __device__ __forceinline__ cpx bound_psi(const Geo& g, const cpx* __restrict__ jz, const cpx* __restrict__ jg, int l, long i,
                                          double kx, double ky, double g2) {
-    const long nk = g.nk;
+    const long nk = g.nkh;
     const int n = g.a + l;
     auto half = [&](int hk) -> cpx {
         if (hk < 0) return jg[i];
@@ -44,176 +50,211 @@ __device__ __forceinline__ cpx bound_psi(const Geo& g, const cpx* __restrict__ j
     }
     return psi;
 }
-}  // namespace
 
-// ---------------------------------------------------------------- sponge, pass 1: rows (inverse x)
+// Full row z[0..NX) from the half rows A, B (k_x = 0..NX/2) of two real fields: z = A + i B with
+// A(NX - k) = conj A(k), B(NX - k) = conj B(k); stored conjugated for an inverse transform.
 template <int NX>
-__global__ void __launch_bounds__(NT) k_sp_rows(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry,
-                                               const cpx* __restrict__ jz, const cpx* __restrict__ jg, cpx* __restrict__ S1,
-                                               cpx* __restrict__ S2, double g2, double opb) {
-    using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T, RS = row_stride<NX>();
-    extern __shared__ cpx sm[];
-    const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
-    const long nk = g.nk, base = long(l) * nk;
-    for (int e = tid; e < LPC * NX; e += NT) {
-        const int r = e / NX, p = e - r * NX, row = r0 + r;
-        cpx v = C(0);
-        if (row < g.ny) {
-            const long i = long(row) * NX + p, idx = base + i;
-            const double kx = g.kxd[p], ky = g.kyd[row];
-            const cpx psi = bound_psi(g, jz, jg, l, i, kx, ky, g2);
-            S2[idx] = psi;
-            const cpx bx = -opb * ik(kx, psi), by = -opb * ik(ky, psi);
-            const cpx u = Rx[idx] - bx, w = Ry[idx] - by;
-            v = conj(C(u.x - w.y, u.y + w.x));                       // u + i w, conjugated: inverse transform
-        }
-        sm[r * RS + p + (p >> 3)] = v;
-    }
-    __syncthreads();
-    const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
-    for (int e = tid; e < LPC * NX; e += NT) {
-        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
-        if (row < g.ny) S1[base + long(row) * NX + p] = conj(sm[rr * RS + p + (p >> 3)]);
+__device__ __forceinline__ void full_row_conj(cpx* line, int p, cpx a, cpx b, bool mirror) {
+    // p in 0..NX/2: position p gets a + i b; its mirror NX - p gets conj(a) + i conj(b)
+    const cpx z = C(a.x - b.y, a.y + b.x);
+    line[p + (p >> 3)] = conj(z);
+    if (mirror) {
+        const int q = NX - p;
+        const cpx zm = C(a.x + b.y, -a.y + b.x);                     // conj(a) + i conj(b)
+        line[q + (q >> 3)] = conj(zm);
     }
 }
+}  // namespace
 
-// ---------------------------------------------------------------- sponge, pass 2: columns (inverse y, mask, forward y)
+// ---------------------------------------------------------------- sponge, pass 1: columns (psi, pack, inverse y)
 template <int NY>
-__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols(Geo g, cpx* __restrict__ S1) {
+__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry,
+                                                                      const cpx* __restrict__ jz, const cpx* __restrict__ jg,
+                                                                      cpx* __restrict__ U, cpx* __restrict__ V,
+                                                                      cpx* __restrict__ PSI, double g2, double opb) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * CW;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
-    const long nk = g.nk, base = long(l) * nk;
-    const int nx = g.nx;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
     for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, c = e - p * CW;
-        sm[e] = conj(S1[base + long(p) * nx + c0 + c]);
+        const int p = e / CW, c = e - p * CW, kxi = c0 + c;
+        cpx u = C(0), v = C(0);
+        if (kxi < H) {
+            const long i = long(p) * H + kxi, o = base + i;
+            const double kx = g.kxd[kxi], ky = g.kyd[p];
+            const cpx psi = bound_psi(g, jz, jg, l, i, kx, ky, g2);
+            PSI[o] = psi;
+            u = Rx[o] - (-opb * ik(kx, psi));
+            v = Ry[o] - (-opb * ik(ky, psi));
+        }
+        s0[e] = conj(u);
+        s1[e] = conj(v);
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(sm, ColAddr<CW>{c}, t, g.twy);
-    const double s = 1.0 / double(g.nk);
+    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
     for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, cc = e - p * CW, ixx = c0 + cc;
-        const cpx z = s * conj(sm[e]);                                 // real-space value (x and y inverse done)
-        const double mx = g.maskx[ixx];
-        sm[e] = C(mx * g.masky_n[p] * z.x, mx * g.masky_h[p] * z.y);
-    }
-    __syncthreads();
-    fft_line<NY>(sm, ColAddr<CW>{c}, t, g.twy);
-    for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, cc = e - p * CW;
-        S1[base + long(p) * nx + c0 + cc] = sm[e];
+        const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        U[o] = conj(s0[e]);
+        V[o] = conj(s1[e]);
     }
 }
 
-// ---------------------------------------------------------------- sponge, pass 3: row pairs (forward x, split, + R_b)
+// ---------------------------------------------------------------- sponge, pass 2: rows (inverse x, mask, forward x)
 template <int NX>
-__global__ void __launch_bounds__(NT) k_sp_rowpairs(Geo g, const cpx* __restrict__ S1, const cpx* __restrict__ S2,
-                                                   cpx* __restrict__ Rx, cpx* __restrict__ Ry, double opb) {
+__global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx* __restrict__ V) {
     using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T, PPC = LPC / 2, RS = row_stride<NX>();
+    constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
-    const int l = blockIdx.y, tid = threadIdx.x, ny = g.ny;
-    const long nk = g.nk, base = long(l) * nk;
-    auto row_of = [&](int slot, bool& valid) {
-        const int jp = blockIdx.x * PPC + (slot >> 1);
-        valid = jp <= ny / 2;
-        return (slot & 1) ? (ny - jp) % ny : jp;
-    };
-    for (int e = tid; e < LPC * NX; e += NT) {
-        const int r = e / NX, p = e - r * NX;
-        bool valid;
-        const int row = row_of(r, valid);
-        sm[r * RS + p + (p >> 3)] = valid ? S1[base + long(row) * NX + p] : C(0);
+    const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
+    const long base = long(l) * g.nkh;
+    for (int e = tid; e < LPC * H; e += NT) {
+        const int r = e / H, p = e - r * H, row = r0 + r;
+        cpx a = C(0), b = C(0);
+        if (row < g.ny) { const long o = base + long(row) * H + p; a = U[o]; b = V[o]; }
+        full_row_conj<NX>(sm + r * RS, p, a, b, p > 0 && p < NX / 2);
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
+    const double s = 1.0 / double(g.nk);
     for (int e = tid; e < LPC * NX; e += NT) {
-        const int rr = e / NX, p = e - rr * NX;
-        bool valid, v2;
-        const int row = row_of(rr, valid);
-        if (!valid) continue;
-        if ((rr & 1) && row == row_of(rr ^ 1, v2)) continue;
+        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
+        const int q = rr * RS + p + (p >> 3);
+        const cpx z = s * conj(sm[q]);                                  // u + i v in real space
+        const double mx = g.maskx[p];
+        const double mn = row < g.ny ? g.masky_n[row] : 0.0, mh = row < g.ny ? g.masky_h[row] : 0.0;
+        sm[q] = C(mx * mn * z.x, mx * mh * z.y);
+    }
+    __syncthreads();
+    fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
+    for (int e = tid; e < LPC * H; e += NT) {
+        const int rr = e / H, p = e - rr * H, row = r0 + rr;
+        if (row >= g.ny) continue;
         const int pm = (NX - p) % NX;
-        const cpx z = sm[rr * RS + p + (p >> 3)], zm = conj(sm[(rr ^ 1) * RS + pm + (pm >> 3)]);
+        const cpx z = sm[rr * RS + p + (p >> 3)], zm = conj(sm[rr * RS + pm + (pm >> 3)]);
         const cpx d = z - zm;
-        const long idx = base + long(row) * NX + p;
-        const cpx psi = S2[idx];
-        Rx[idx] = 0.5 * (z + zm) - opb * ik(g.kxd[p], psi);
-        Ry[idx] = 0.5 * C(d.y, -d.x) - opb * ik(g.kyd[row], psi);
+        const long o = base + long(row) * H + p;
+        U[o] = 0.5 * (z + zm);
+        V[o] = 0.5 * C(d.y, -d.x);
     }
 }
 
-// ---------------------------------------------------------------- real fields: columns (pack, inverse y)
+// ---------------------------------------------------------------- sponge, pass 3: columns (forward y, + R_b)
+template <int NY>
+__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, const cpx* __restrict__ U, const cpx* __restrict__ V,
+                                                                      const cpx* __restrict__ PSI, cpx* __restrict__ Rx,
+                                                                      cpx* __restrict__ Ry, double opb) {
+    using S = FftShape<NY>;
+    extern __shared__ cpx sm[];
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * CW;
+    const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, c = e - p * CW, kxi = c0 + c;
+        cpx u = C(0), v = C(0);
+        if (kxi < H) { const long o = base + long(p) * H + kxi; u = U[o]; v = V[o]; }
+        s0[e] = u; s1[e] = v;
+    }
+    __syncthreads();
+    const int c = tid % CW, t = tid / CW;
+    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        const cpx psi = PSI[o];
+        Rx[o] = s0[e] - opb * ik(g.kxd[kxi], psi);
+        Ry[o] = s1[e] - opb * ik(g.kyd[p], psi);
+    }
+}
+
+// ---------------------------------------------------------------- real fields: columns (inverse y of the six spectra)
+// blockIdx.z picks the pair (R_x, R_y), (L_x, L_y) or (E_z, B_z): two fields per CTA keep the shared memory small
+// enough for several CTAs per SM, so loads of one CTA overlap the transforms of another.
 template <int NY>
 __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry,
                                                                   const cpx* __restrict__ Lx, const cpx* __restrict__ Ly,
                                                                   const cpx* __restrict__ Ez, const cpx* __restrict__ Bz,
-                                                                  cpx* __restrict__ S1, cpx* __restrict__ S2, cpx* __restrict__ S3) {
+                                                                  cpx* __restrict__ W0, cpx* __restrict__ W1, cpx* __restrict__ W2,
+                                                                  cpx* __restrict__ W3, cpx* __restrict__ W4, cpx* __restrict__ W5) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
-    cpx* a0 = sm;
-    cpx* a1 = sm + NY * CW;
-    cpx* a2 = sm + 2 * NY * CW;
-    const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
-    const long nk = g.nk, base = long(l) * nk;
-    const int nx = g.nx;
+    const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    const cpx* in0 = pr == 0 ? Rx : pr == 1 ? Lx : Ez;
+    const cpx* in1 = pr == 0 ? Ry : pr == 1 ? Ly : Bz;
+    cpx* out0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
+    cpx* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * CW;
     for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, c = e - p * CW;
-        const long idx = base + long(p) * nx + c0 + c;
-        const cpx rx = Rx[idx], ry = Ry[idx], lx = Lx[idx], ly = Ly[idx], ez = Ez[idx], bz = Bz[idx];
-        a0[e] = conj(C(rx.x - ry.y, rx.y + ry.x));
-        a1[e] = conj(C(lx.x - ly.y, lx.y + ly.x));
-        a2[e] = conj(C(ez.x - bz.y, ez.y + bz.x));
+        const int p = e / CW, c = e - p * CW, kxi = c0 + c;
+        const long o = base + long(p) * H + kxi;
+        s0[e] = kxi < H ? conj(in0[o]) : C(0);
+        s1[e] = kxi < H ? conj(in1[o]) : C(0);
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(a0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(a1, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(a2, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
     for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, cc = e - p * CW;
-        const long idx = base + long(p) * nx + c0 + cc;
-        S1[idx] = a0[e]; S2[idx] = a1[e]; S3[idx] = a2[e];          // still conjugated
+        const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        out0[o] = conj(s0[e]);
+        out1[o] = conj(s1[e]);
     }
 }
 
 // ---------------------------------------------------------------- real fields: rows (inverse x, F)
 template <int NX>
-__global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ S1, const cpx* __restrict__ S2,
-                                               const cpx* __restrict__ S3, float* __restrict__ F) {
+__global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
+                                               const cpx* __restrict__ W2, const cpx* __restrict__ W3,
+                                               const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F) {
     using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T, RS = row_stride<NX>();
+    constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
     cpx* a0 = sm;
     cpx* a1 = sm + LPC * RS;
     cpx* a2 = sm + 2 * LPC * RS;
     const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
-    const long nk = g.nk, base = long(l) * nk;
-    for (int e = tid; e < LPC * NX; e += NT) {
-        const int r = e / NX, p = e - r * NX, row = r0 + r;
-        cpx u0 = C(0), u1 = C(0), u2 = C(0);
-        if (row < g.ny) { const long idx = base + long(row) * NX + p; u0 = S1[idx]; u1 = S2[idx]; u2 = S3[idx]; }
-        const int q = r * RS + p + (p >> 3);
-        a0[q] = u0; a1[q] = u1; a2[q] = u2;
+    const long base = long(l) * g.nkh;
+    for (int e = tid; e < LPC * H; e += NT) {
+        const int r = e / H, p = e - r * H, row = r0 + r;
+        cpx v[6] = {C(0), C(0), C(0), C(0), C(0), C(0)};
+        if (row < g.ny) {
+            const long o = base + long(row) * H + p;
+            v[0] = W0[o]; v[1] = W1[o]; v[2] = W2[o]; v[3] = W3[o]; v[4] = W4[o]; v[5] = W5[o];
+        }
+        const bool mirror = p > 0 && p < NX / 2;
+        full_row_conj<NX>(a0 + r * RS, p, v[0], v[1], mirror);
+        full_row_conj<NX>(a1 + r * RS, p, v[2], v[3], mirror);
+        full_row_conj<NX>(a2 + r * RS, p, v[4], v[5], mirror);
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
-    const double s = 1.0 / double(nk);
-    const long fpl = long(g.ns + 2) * nk;
+    const double s = 1.0 / double(g.nk);
+    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     for (int e = tid; e < LPC * NX; e += NT) {
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
         const int q = rr * RS + p + (p >> 3);
         const cpx z1 = s * conj(a0[q]), z2 = s * conj(a1[q]), z3 = s * conj(a2[q]);
-        const long idx = base + long(row) * NX + p;
+        const long idx = fbase + long(row) * NX + p;
         const double r1 = z1.x, r2 = z1.y, l1 = z2.x, l2 = z2.y;
         F[0 * fpl + idx] = float(0.5 * (r1 + l1));     // E_x
         F[1 * fpl + idx] = float(0.5 * (r2 + l2));     // E_y
@@ -225,76 +266,93 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ S
 }
 
 // ---------------------------------------------------------------- launchers
+template <class K>
+static void allow_smem(K kern, size_t smem) {
+    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+}
+static unsigned col_tiles(const Ctx& c) { return unsigned((c.H + CW - 1) / CW); }
+
+template <int NY>
+static void sp_cols_inv(Ctx& c) {
+    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
+    allow_smem(k_sp_cols_inv<NY>, smem);
+    const int tok = c.prof_begin("sponge_cols_inv");
+    k_sp_cols_inv<NY><<<dim3(col_tiles(c), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), c.Rx.p, c.Ry.p, c.jkz.p, c.jzg.p, c.W[0].p, c.W[1].p, c.W[3].p, c.gm2_b, 1 + c.beta_b);
+    c.check_launch("k_sp_cols_inv");
+    c.prof_end(tok);
+}
 template <int NX>
 static void sp_rows(Ctx& c) {
-    using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T;
+    constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(LPC) * row_stride<NX>() * sizeof(cpx);
-    auto kern = k_sp_rows<NX>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    allow_smem(k_sp_rows<NX>, smem);
     const int tok = c.prof_begin("sponge_rows");
-    kern<<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.jkz.p, c.jzg.p, c.S1.p, c.S2.p, c.gm2_b, 1 + c.beta_b);
+    k_sp_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p);
     c.check_launch("k_sp_rows");
     c.prof_end(tok);
 }
 template <int NY>
-static void sp_cols(Ctx& c) {
-    const size_t smem = size_t(NY) * CW * sizeof(cpx);
-    auto kern = k_sp_cols<NY>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const int tok = c.prof_begin("sponge_cols");
-    kern<<<dim3(unsigned(c.nx / CW), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(c.geo(), c.S1.p);
-    c.check_launch("k_sp_cols");
-    c.prof_end(tok);
-}
-template <int NX>
-static void sp_rowpairs(Ctx& c) {
-    using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T, PPC = LPC / 2;
-    const size_t smem = size_t(LPC) * row_stride<NX>() * sizeof(cpx);
-    auto kern = k_sp_rowpairs<NX>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    const int tok = c.prof_begin("sponge_rowpairs");
-    kern<<<dim3(unsigned((c.ny / 2 + 1 + PPC - 1) / PPC), unsigned(c.ns)), NT, smem, c.stream>>>(
-        c.geo(), c.S1.p, c.S2.p, c.Rx.p, c.Ry.p, 1 + c.beta_b);
-    c.check_launch("k_sp_rowpairs");
+static void sp_cols_fwd(Ctx& c) {
+    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
+    allow_smem(k_sp_cols_fwd<NY>, smem);
+    const int tok = c.prof_begin("sponge_cols_fwd");
+    k_sp_cols_fwd<NY><<<dim3(col_tiles(c), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), c.W[0].p, c.W[1].p, c.W[3].p, c.Rx.p, c.Ry.p, 1 + c.beta_b);
+    c.check_launch("k_sp_cols_fwd");
     c.prof_end(tok);
 }
 void launch_sponge(Ctx& c) {
-    if (c.nx < CW) throw Error(G3D_ERR_ARG, "nx must be >= 8");
+    G3D_DISPATCH_N(c.ny, NY, sp_cols_inv<NY>(c));
     G3D_DISPATCH_N(c.nx, NX, sp_rows<NX>(c));
-    G3D_DISPATCH_N(c.ny, NY, sp_cols<NY>(c));
-    G3D_DISPATCH_N(c.nx, NX, sp_rowpairs<NX>(c));
+    G3D_DISPATCH_N(c.ny, NY, sp_cols_fwd<NY>(c));
 }
 
 template <int NY>
 static void rf_cols(Ctx& c) {
-    const size_t smem = size_t(3) * NY * CW * sizeof(cpx);
-    auto kern = k_rf_cols<NY>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
+    allow_smem(k_rf_cols<NY>, smem);
     const int tok = c.prof_begin("real_cols");
-    kern<<<dim3(unsigned(c.nx / CW), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.S1.p, c.S2.p, c.S3.p);
+    k_rf_cols<NY><<<dim3(col_tiles(c), unsigned(c.ns), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p);
     c.check_launch("k_rf_cols");
     c.prof_end(tok);
 }
 template <int NX>
 static void rf_rows(Ctx& c) {
-    using S = FftShape<NX>;
-    constexpr int LPC = NT / S::T;
+    constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
-    auto kern = k_rf_rows<NX>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin("real_rows");
-    kern<<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(c.geo(), c.S1.p, c.S2.p, c.S3.p, c.F.p);
+    k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(
+        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
 void launch_real_fields(Ctx& c) {
-    if (c.nx < CW) throw Error(G3D_ERR_ARG, "nx must be >= 8");
     G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c));
     G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c));
+}
+
+// ---------------------------------------------------------------- half <-> full spectrum layouts
+// full[p][j][ix] = half[p][j][ix] (ix <= nx/2), conj(half[p][(ny - j) % ny][nx - ix]) (ix > nx/2)
+__global__ void k_half_to_full(Geo g, const cpx* __restrict__ half, cpx* __restrict__ full, long planes) {
+    const long n = planes * g.nk;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long pl = idx / g.nk, i = idx - pl * g.nk;
+        const int ixx = int(i % g.nx), j = int(i / g.nx);
+        const long hb = pl * g.nkh;
+        full[idx] = ixx <= g.nx / 2 ? half[hb + long(j) * g.H + ixx]
+                                    : conj(half[hb + long((g.ny - j) % g.ny) * g.H + (g.nx - ixx)]);
+    }
+}
+__global__ void k_full_to_half(Geo g, const cpx* __restrict__ full, cpx* __restrict__ half, long planes) {
+    const long n = planes * g.nkh;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long pl = idx / g.nkh, i = idx - pl * g.nkh;
+        const int kx = int(i % g.H), j = int(i / g.H);
+        half[idx] = full[pl * g.nk + long(j) * g.nx + kx];
+    }
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -307,6 +365,14 @@ __global__ void k_copy_c(cpx* __restrict__ y, const cpx* __restrict__ x, long n)
 static unsigned ew_blocks(long n) {
     long b = (n + 255) / 256;
     return unsigned(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+void launch_half_to_full(Ctx& c, const cpx* half, cpx* full, long planes) {
+    k_half_to_full<<<ew_blocks(planes * c.nk), 256, 0, c.stream>>>(c.geo(), half, full, planes);
+    c.check_launch("k_half_to_full");
+}
+void launch_full_to_half(Ctx& c, const cpx* full, cpx* half, long planes) {
+    k_full_to_half<<<ew_blocks(planes * c.nkh), 256, 0, c.stream>>>(c.geo(), full, half, planes);
+    c.check_launch("k_full_to_half");
 }
 void launch_zero_c(Ctx& c, cpx* p, size_t n) { if (n) G3D_CUDA(cudaMemsetAsync(p, 0, n * sizeof(cpx), c.stream)); }
 void launch_axpy_c(Ctx& c, cpx* y, const cpx* x, double a, size_t n) {
@@ -327,10 +393,10 @@ void launch_copy_c(Ctx& c, cpx* y, const cpx* x, size_t n) {
 // ---------------------------------------------------------------- window shift
 // Spectra: exact phase factor exp(i (k_x s_x + k_y s_y)) with the shift tables kxs, kys (Nyquist kept).
 __global__ void k_rotate(Geo g, cpx* __restrict__ p, long n, double sx, double sy, int nys) {
-    const long nk = g.nk;
+    const long nk = g.nkh;
     for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
         const long i = idx % nk;
-        const double ph = g.kxs[i % g.nx] * sx + (nys ? g.kys[i / g.nx] * sy : 0.0);
+        const double ph = g.kxs[i % g.H] * sx + (nys ? g.kys[i / g.H] * sy : 0.0);
         p[idx] = p[idx] * C(cos(ph), sin(ph));
     }
 }

@@ -68,9 +68,10 @@ __device__ __forceinline__ St axpy(const St& a, double h, const St& b) {
 }
 
 // RK4 from z0 to the plane s1 (reference push_one, src/sim_kernels.hpp:98-149).
-__global__ void __launch_bounds__(128) k_push(PushArgs c, PartsDev P, long np, double s0) {
-    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (ip >= np) return;
+__global__ void __launch_bounds__(128) k_push(PushArgs c, PartsDev P, const int32_t* __restrict__ perm, long np, double s0) {
+    const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const long ip = perm[t];                 // cell order: the warp's particles gather the same planes of F
     const int alive = P.alive[ip];
     if (alive != 1 && alive != 3) return;
     const double s1 = c.s1;
@@ -131,7 +132,7 @@ void launch_push(Ctx& c, double s0, double s1) {
     a.zmax = c.zeta[c.N - 1]; a.ylo = -1e300; a.yhi = 1e300; a.s1 = s1; a.vz_min = 0; a.hmin = c.hmin;
     a.freeze = c.P.freeze_bunch; a.self = c.P.self_fields;
     const int tok = c.prof_begin("push");
-    k_push<<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.parts, c.np, s0);
+    k_push<<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.parts, c.perm.p, c.np, s0);
     c.check_launch("k_push");
     c.prof_end(tok);
 }

@@ -185,6 +185,11 @@ def test_checkpoint_is_read_by_the_reference(tmp_path):
     r.write_checkpoint(tmp_path)
     s2 = __import__("g3d").Simulation(cfg)
     s2.read_checkpoint(tmp_path / "checkpoint_000002_r0000.bin")
+    # libg3d keeps k_x <= nx/2 and restores the other half by X(-k) = conj X(k); the reference's spectra obey
+    # that symmetry to rounding only (its j_z spectrum is a complex FFT of real data), so the round trip is
+    # exact in the kept half and agrees to rounding in the other
     for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly"]:
-        assert np.array_equal(s2.array(a), r.array(a)), a
+        x, y = s2.array(a).reshape(-1, cfg.ny, cfg.nx), r.array(a).reshape(-1, cfg.ny, cfg.nx)
+        assert np.array_equal(x[:, :, : cfg.nx // 2 + 1], y[:, :, : cfg.nx // 2 + 1]), a
+        assert rel_l2(x, y) <= 1e-14, a
     assert s2.status().istep == 2
