@@ -2,6 +2,7 @@
 #pragma once
 #include <array>
 #include <deque>
+#include <memory>
 #include <string>
 #include <vector>
 #include "g3d.h"
@@ -101,6 +102,8 @@ struct DevBuf {
 struct ProfEntry { std::string name; long launches = 0; double ms = 0; };
 struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 
+struct PlasmaState;               // g3d_plasma.hpp
+
 // ---------------------------------------------------------------- the context
 struct Ctx {
     // grid (single rank: a = 0, b = ns = N)
@@ -133,6 +136,9 @@ struct Ctx {
     PartsDev parts{};
     long np = 0, pcap = 0;
     DevBuf<int32_t> perm;                        // particles in cell order (k_sort.cu); storage order unchanged
+    DevBuf<uint32_t> sort_keys;                  // sort buffers, sized for the particle capacity
+    DevBuf<int32_t> sort_idx;
+    DevBuf<unsigned char> sort_tmp;
     int steps_since_sort = 0;
     // reductions
     DevBuf<double> red;                          // per-block partial sums
@@ -152,7 +158,12 @@ struct Ctx {
     std::vector<PendingEvent> pending;
     std::vector<cudaEvent_t> event_pool;
     std::string err;
+    // streaming plasma (null without plasma) and the grid lasers of the start field
+    std::unique_ptr<PlasmaState> pl;
+    std::vector<g3d_grid_laser> glasers;
 
+    Ctx();
+    ~Ctx();
     Geo geo() const;
     // kernel launch bookkeeping: call before/after each launch
     int prof_begin(const char* name);
@@ -177,9 +188,18 @@ void launch_centroid(Ctx& c, double out[3]);
 void launch_diag(Ctx& c, double S[19]);
 double launch_field_energy(Ctx& c);
 void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy);
+void launch_rotate(Ctx& c, cpx* p, size_t n, double sx, double sy, int nys);
 void launch_half_to_full(Ctx& c, const cpx* half, cpx* full, long planes);
 void launch_full_to_half(Ctx& c, const cpx* full, cpx* half, long planes);
 void sort_particles(Ctx& c);                // refresh perm
+// particles and plasma (g3d_host.cu, g3d_plasma.cu)
+void set_particles(Ctx& c, const g3d_particle* v, long n);
+std::vector<g3d_particle> get_particles(Ctx& c);
+void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions);
+void march_plasma(Ctx& c, double s0, double s1);
+void collect_restreaming(Ctx& c);
+void add_grid_lasers(Ctx& c);
+std::vector<g3d_particle> get_streaming(Ctx& c);
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)
 

@@ -5,7 +5,7 @@
 #include <complex>
 #include <cstring>
 #include <random>
-#include "g3d_ctx.hpp"
+#include "g3d_plasma.hpp"
 
 namespace g3d {
 
@@ -17,6 +17,9 @@ bool pow2_ok(int n) { return n >= 4 && n <= 512 && (n & (n - 1)) == 0; }
 }  // namespace
 
 // ---------------------------------------------------------------- context plumbing
+Ctx::Ctx() = default;
+Ctx::~Ctx() = default;
+
 Geo Ctx::geo() const {
     Geo g;
     g.nx = nx; g.ny = ny; g.nk = nk; g.N = N; g.a = a; g.b = b; g.ns = ns; g.nh = ns + 3;
@@ -165,6 +168,8 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.laser.a0 = P.a0; c.laser.kL = P.kL; c.laser.tau = P.tau; c.laser.cep = P.cep; c.laser.eta_c = P.eta_c;
     c.laser.kx = std::sin(P.theta); c.laser.kz = std::cos(P.theta);
     c.laser.flat = P.flat_length; c.laser.ramp = P.ramp_length;
+    // box origin as Simulation::init sets it (load_bunch, src/sim_bunches.cpp:216, also without bunches)
+    c.X0 = -0.5 * G.Lx; c.Y0 = -0.5 * G.Ly;
     if (P.laser_on && P.laser_envelope == G3D_ENV_FLATTOP && !(P.ramp_length > 0))
         throw Error(G3D_ERR_ARG, "flat-top envelope needs ramp_length > 0");
     G3D_CUDA(cudaStreamSynchronize(s));
@@ -188,7 +193,7 @@ static void reserve_particles(Ctx& c, long n) {
 
 // Host records (104-byte AoS) <-> device columns: one DMA of the records into a device staging buffer
 // and a transposition kernel (k_parts_unpack / k_parts_pack, k_parts.cu).
-static void set_particles(Ctx& c, const g3d_particle* v, long n) {
+void set_particles(Ctx& c, const g3d_particle* v, long n) {
     reserve_particles(c, n);
     c.np = n;
     if (!n) return;
@@ -196,6 +201,7 @@ static void set_particles(Ctx& c, const g3d_particle* v, long n) {
     G3D_CUDA(cudaMemcpyAsync(c.pstage.p, v, size_t(n) * sizeof(g3d_particle), cudaMemcpyHostToDevice, c.stream));
     launch_parts_unpack(c, n);
     sort_particles(c);
+    G3D_CUDA(cudaStreamSynchronize(c.stream));     // the caller may reuse its buffer on return
 }
 
 static void get_particles_into(Ctx& c, g3d_particle* out) {
@@ -207,7 +213,7 @@ static void get_particles_into(Ctx& c, g3d_particle* out) {
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 
-static std::vector<g3d_particle> get_particles(Ctx& c) {
+std::vector<g3d_particle> get_particles(Ctx& c) {
     std::vector<g3d_particle> out(static_cast<size_t>(c.np));
     get_particles_into(c, out.data());
     return out;
@@ -274,7 +280,9 @@ static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int c
 static void currents(Ctx& c) {
     c.jk_is_j0 = false;
     launch_deposit(c);
-    const bool keep0 = false;            // no plasma in this release: the k = 0 current is removed (sim_particles.cpp:145)
+    // with plasma the k = 0 current is kept (a 1D plasma wave, the return current), but not in the start field
+    // (sim_particles.cpp:143-145)
+    const bool keep0 = c.pl && c.pl->box_mean && !c.starting_;
     launch_cur_fft(c, keep0);
     // one rank: the filtered j_z ghosts of the neighbours are zero (exchange_jz_ghosts, sim_particles.cpp:210-226)
 }
@@ -333,6 +341,12 @@ static void shift_window(Ctx& c, int nxs, int nys) {
     materialize_jk(c);
     c.X0 += nxs * c.dx; c.Y0 += nys * c.dy;
     launch_shift(c, nxs, nys, nxs * c.dx, nys * c.dy);
+    if (c.pl) {
+        for (auto& p : c.pl->joining) { p.x -= nxs * c.dx; p.y -= nys * c.dy; }
+        launch_rotate(c, c.pl->js0x.p, c.pl->js0x.n, nxs * c.dx, nys * c.dy, nys);
+        launch_rotate(c, c.pl->js0y.p, c.pl->js0y.n, nxs * c.dx, nys * c.dy, nys);
+        launch_rotate(c, c.pl->js0z.p, c.pl->js0z.n, nxs * c.dx, nys * c.dy, nys);
+    }
 }
 static void window_shift_post(Ctx& c) {
     if (!c.P.move_x && !(c.yf && c.P.move_y)) return;
@@ -358,6 +372,7 @@ static void init_fields(Ctx& c) {
         currents(c);
         comoving_field(c);
         if (c.P.start_relax) relax_start_field(c);
+        add_grid_lasers(c);
         march(c, 0.0);
         c.starting_ = false;
         sponge_and_real_fields(c);
@@ -369,8 +384,14 @@ static void step(Ctx& c, bool sync) {
     if (++c.steps_since_sort >= 16) sort_particles(c);
     window_shift_start(c);
     launch_push(c, c.s, c.s + c.P.dz);
+    if (c.pl) collect_restreaming(c);
     c.s += c.P.dz; ++c.istep;
-    if (c.P.self_fields) solve_fields(c, 0.5 * c.P.dz);
+    if (c.P.self_fields && c.pl) {
+        currents(c);
+        march_plasma(c, c.s - c.P.dz, c.s);
+        sponge_and_real_fields(c);
+        j0_from_jk(c);
+    } else if (c.P.self_fields) solve_fields(c, 0.5 * c.P.dz);
     window_shift_post(c);
     if (sync) G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -672,6 +693,35 @@ int g3d_relax_start_field(g3d_ctx* ctx) {
     });
 }
 int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ctx, [&] { g3d::shift_window(ctx->c, nxs, nys); }); }
+int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
+    return guarded(ctx, [&] {
+        if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
+        g3d::set_plasma(ctx->c, *plasma, ions, nions);
+    });
+}
+int g3d_add_grid_laser(g3d_ctx* ctx, const g3d_grid_laser* laser) {
+    return guarded(ctx, [&] {
+        if (!laser || !(laser->waist > 0) || !(laser->tau > 0)) throw Error(G3D_ERR_ARG, "grid laser: waist and tau must be positive");
+        ctx->c.glasers.push_back(*laser);
+    });
+}
+int g3d_march_plasma(g3d_ctx* ctx, double s0, double s1) {
+    return guarded(ctx, [&] {
+        if (!ctx->c.pl) throw Error(G3D_ERR_STATE, "no plasma set (g3d_set_plasma)");
+        g3d::materialize_jk(ctx->c);
+        g3d::march_plasma(ctx->c, s0, s1);
+        G3D_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    });
+}
+int g3d_get_streaming(g3d_ctx* ctx, g3d_particle* out, int64_t capacity, int64_t* n) {
+    return guarded(ctx, [&] {
+        if (!ctx->c.pl) { if (n) *n = 0; return; }
+        const std::vector<g3d_particle> v = g3d::get_streaming(ctx->c);
+        if (n) *n = int64_t(v.size());
+        if (int64_t(v.size()) > capacity) throw Error(G3D_ERR_CAPACITY, "output capacity below the streaming particle count");
+        if (!v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(g3d_particle));
+    });
+}
 
 int g3d_diagnostics(g3d_ctx* ctx, double out[19]) {
     return guarded(ctx, [&] {

@@ -1,0 +1,463 @@
+// Host orchestration of the streaming plasma (one rank, Fourier y): set-up, the fresh plasma of a step, the
+// march half-cell by half-cell with its passes, prediction and correction, the freed electrons, trapping and
+// restreaming (src/sim_plasma.cpp:21-491, src/sim_ions.cpp:68-87, src/ionization.cpp:28-53), and the grid
+// lasers of the start field (src/sim_fields.cpp:321-374).
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include "g3d_plasma.hpp"
+
+namespace g3d {
+
+namespace {
+constexpr double c_SI = 299792458.0, e_SI = 1.602176634e-19, me_SI = 9.1093837015e-31;
+constexpr double U_H_EV = 13.605693122994, E_ATOMIC_VM = 5.14220674763e11, OMEGA_ATOMIC = 4.1341373335e16;
+}  // namespace
+
+void StrmBuf::alloc(long n, cudaStream_t s) {
+    cap = n;
+    d.alloc(size_t(n) * 10, s);
+    i.alloc(size_t(n) * 2, s);
+    u.alloc(size_t(n), s);
+    double** cols[10] = {&v.x, &v.y, &v.zeta, &v.px, &v.py, &v.pz, &v.w, &v.z, &v.q, &v.qm};
+    for (int k = 0; k < 10; ++k) *cols[k] = d.p + size_t(k) * n;
+    v.alive = i.p; v.sp = i.p + n;
+    v.id = u.p;
+}
+
+PlasmaPtrs PlasmaState::ptrs(const Ctx& c) const {
+    PlasmaPtrs p;
+    p.nkh = c.nkh;
+    p.jkx = c.jkx.p; p.jky = c.jky.p; p.jkz = c.jkz.p;
+    p.js0x = js0x.p; p.js0y = js0y.p; p.js0z = js0z.p;
+    p.jsn = jsn.p; p.sin_ = jsin.p; p.si0 = jsi0.p; p.pin = jpred.p; p.tmp = jtmp.p; p.dl = dlt.p;
+    return p;
+}
+
+// ---------------------------------------------------------------- ADK tables (src/ionization.cpp:28-53)
+// ln of omega_a C^2 (U/2U_H) (2 (U/U_H)^{3/2} E_a)^{2n*-1}, the power 2n*-1 and the exponent factor
+// -(2/3)(U/U_H)^{3/2} E_a of the ADK rate (s-states, l* = n* - 1, m = 0) in SI units
+static void adk_coefficients(double U_eV, int Zafter, double& logpre, double& power, double& expo) {
+    const double x = U_eV / U_H_EV;
+    const double nstar = Zafter / std::sqrt(x);
+    const double logC2 = 2.0 * nstar * std::log(2.0) - std::log(nstar) - std::lgamma(nstar + 1.0) - std::lgamma(nstar);
+    power = 2.0 * nstar - 1.0;
+    logpre = std::log(OMEGA_ATOMIC) + logC2 + std::log(0.5 * x) + power * std::log(2.0 * std::pow(x, 1.5) * E_ATOMIC_VM);
+    expo = -(2.0 / 3.0) * std::pow(x, 1.5) * E_ATOMIC_VM;
+}
+static double adk_raw(const AdkDev& L, double E) {
+    E = std::min(E, L.Epeak);
+    return E > 0 ? std::exp(L.logpre - L.power * std::log(E) + L.expo / E) : 0.0;
+}
+// levels Z0 .. Zmax-1 in code units; Emin: below it a level is not ionized within T with probability > 1e-10
+static std::vector<AdkDev> adk_levels(const std::vector<double>& ip_eV, int Z0, int Zmax, double E0_SI, double omega0, double T) {
+    std::vector<AdkDev> lev(size_t(std::max(Zmax, 0)), AdkDev{0, 0, 0, 1e300, 1e300});
+    for (int k = Z0; k < Zmax; ++k) {
+        AdkDev& L = lev[size_t(k)];
+        double logpre, power, expo;
+        adk_coefficients(ip_eV[size_t(k)], k + 1, logpre, power, expo);
+        L.power = power;
+        L.logpre = logpre - std::log(omega0) - power * std::log(E0_SI);
+        L.expo = expo / E0_SI;
+        L.Epeak = power > 0 ? -L.expo / power : 1e300;
+        double lo = 1e-12, hi = std::min(L.Epeak, 1e6);
+        if (adk_raw(L, hi) * T < 1e-10) L.Emin = hi;
+        else {
+            for (int it = 0; it < 200; ++it) {
+                const double mid = std::sqrt(lo * hi);
+                (adk_raw(L, mid) * T < 1e-10 ? lo : hi) = mid;
+            }
+            L.Emin = lo;
+        }
+    }
+    return lev;
+}
+
+// ---------------------------------------------------------------- set-up (setup_plasma, setup_ions)
+void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
+    if (P.ppc_x < 1 || P.ppc_y < 1) throw Error(G3D_ERR_ARG, "plasma: ppc_x, ppc_y must be >= 1");
+    if (P.iterations < 1) throw Error(G3D_ERR_ARG, "plasma: iterations must be >= 1");
+    if (!(P.vz_min > 0 && P.vz_min < P.vz_beam && P.vz_beam < 1)) throw Error(G3D_ERR_ARG, "plasma: need 0 < vz_min < vz_beam < 1");
+    if (!(P.trap_advance >= 1)) throw Error(G3D_ERR_ARG, "plasma: trap_advance must be >= 1");
+    if (!(P.n0 > 0)) throw Error(G3D_ERR_ARG, "plasma: n0 must be positive");
+    auto pl = std::make_unique<PlasmaState>();
+    pl->cfg = P;
+    if (P.n_z > 0) {
+        pl->zpts.assign(P.z_points, P.z_points + P.n_z);
+        pl->zvals.assign(P.z_values, P.z_values + P.n_z);
+    }
+    pl->cfg.z_points = nullptr; pl->cfg.z_values = nullptr;
+    pl->box_mean = P.box_mean != 0;
+    for (int k = 0; k < nions; ++k) {
+        const g3d_ion& I = ions[k];
+        IonSpec s;
+        s.mass = I.mass; s.atoms = I.atoms; s.Z0 = I.Z0; s.Zmax = I.Zmax; s.mobile = I.mobile; s.ionization = I.ionization;
+        if (I.n_ip > 0) s.ip_eV.assign(I.ip_eV, I.ip_eV + I.n_ip);
+        if (s.ionization && (int(s.ip_eV.size()) < s.Zmax || s.Zmax <= s.Z0))
+            throw Error(G3D_ERR_ARG, "ion: ionization needs Zmax > Z0 and Zmax ionization energies");
+        pl->ions.push_back(s);
+    }
+    cudaStream_t s = c.stream;
+    const size_t ph = size_t(c.nkh);
+    for (DevBuf<cpx>* b : {&pl->js0x, &pl->js0y, &pl->js0z}) b->alloc(size_t(c.ns + 1) * ph, s);
+    pl->jsr.alloc(size_t(5) * c.nk, s);
+    for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
+    pl->bk.alloc(4 * ph, s);
+    pl->nstrm_dev.alloc(1, s);
+    pl->bcnt.alloc(1, s);
+    pl->flags.alloc(1, s);
+    // ion tables on the device (setup_ions, src/sim_ions.cpp:68-87)
+    const double Lu = c.P.lambda0 / (2 * M_PI), omega0 = c_SI / Lu, E0 = me_SI * c_SI * omega0 / e_SI;
+    const double Lwin = c.zeta.back() - c.zeta.front();
+    std::vector<IonDevC> iv;
+    std::vector<AdkDev> lev;
+    for (const auto& sp : pl->ions) {
+        IonDevC d{};
+        d.mass = sp.mass; d.mobile = sp.mobile; d.ionizing = sp.ionization; d.Zmax = sp.Zmax; d.off = int(lev.size()); d.Emin = 1e300;
+        if (sp.ionization) {
+            const std::vector<AdkDev> L = adk_levels(sp.ip_eV, sp.Z0, sp.Zmax, E0, omega0, 2 * Lwin);
+            for (int k = sp.Z0; k < sp.Zmax; ++k) d.Emin = std::min(d.Emin, L[size_t(k)].Emin);
+            lev.insert(lev.end(), L.begin(), L.end());
+        }
+        iv.push_back(d);
+    }
+    if (!iv.empty()) pl->ion_dev.upload(iv, s);
+    if (!lev.empty()) pl->adk_dev.upload(lev, s);
+    G3D_CUDA(cudaStreamSynchronize(s));
+    c.pl = std::move(pl);
+}
+
+// n = n0 f(z) g(r) for r < r_max (Config::plasma_density, src/sim_config.cpp:49-66; no density function)
+static double plasma_density(const PlasmaState& P, double x, double y, double z) {
+    const double r2 = x * x + y * y;
+    if (r2 >= P.cfg.r_max * P.cfg.r_max) return 0;
+    double f = 1;
+    if (!P.zpts.empty()) {
+        if (z <= P.zpts.front()) f = P.zvals.front();
+        else if (z >= P.zpts.back()) f = P.zvals.back();
+        else {
+            size_t k = 1;
+            while (P.zpts[k] < z) ++k;
+            const double t = (z - P.zpts[k - 1]) / (P.zpts[k] - P.zpts[k - 1]);
+            f = (1 - t) * P.zvals[k - 1] + t * P.zvals[k];
+        }
+    }
+    const double g = P.cfg.parabolic ? 1 + P.cfg.channel_depth * r2 / (P.cfg.r_channel * P.cfg.r_channel) : 1.0;
+    return f * g > 0 ? P.cfg.n0 * f * g : 0.0;
+}
+
+// Fresh plasma at the front of the window in the reference's order (load_plasma, src/sim_plasma.cpp:43-90):
+// rows j, cells i, sub-cells b2, a2; the electron, then the loaded ions of every species; then the particles
+// that join the march at their zeta.
+static void load_plasma(Ctx& c, double s0, double s1) {
+    PlasmaState& P = *c.pl;
+    std::vector<g3d_particle> v;
+    long cap = 0;
+    const uint64_t id0 = uint64_t(c.istep + 1) << 32;
+    const double zmid = 0.5 * (s0 + s1), Delta = s1 - s0;
+    const int nx = c.nx, ny = c.ny, px = P.cfg.ppc_x, py = P.cfg.ppc_y;
+    const double zf = c.zeta[size_t(c.N - 1)];
+    for (int j = 0; j < ny; ++j) {
+        const double y0 = j * c.dy, hy = c.dy;
+        for (int i = 0; i < nx; ++i)
+            for (int b2 = 0; b2 < py; ++b2)
+                for (int a2 = 0; a2 < px; ++a2) {
+                    g3d_particle p{};
+                    p.x = (i + (a2 + 0.5) / px) * c.dx;
+                    p.y = y0 + (b2 + 0.5) / py * hy;
+                    const double n = plasma_density(P, p.x + c.X0, p.y + c.Y0, zmid);
+                    if (n <= 0) continue;
+                    p.w = n * c.dx * hy * Delta / (px * py);
+                    p.q = -1; p.qm = -1; p.sp = SP_PLASMA; p.alive = 1;
+                    p.zeta = zf; p.z = s0;
+                    if (P.cfg.free_electrons) { p.id = id0 + v.size(); v.push_back(p); }
+                    for (size_t k = 0; k < P.ions.size(); ++k) {
+                        const IonSpec& is = P.ions[k];
+                        if (!is.loaded()) continue;
+                        g3d_particle q = p;
+                        q.q = is.Z0; q.qm = is.Z0 / is.mass; q.w = is.atoms * p.w; q.sp = SP_ION + int(k);
+                        q.id = id0 + v.size();
+                        v.push_back(q);
+                    }
+                }
+    }
+    P.fresh_last = long(v.size());
+    for (g3d_particle p : P.joining) { p.alive = 6; v.push_back(p); }
+    P.joining.clear();
+    for (const auto& p : v)
+        if (p.sp >= SP_ION && p.sp < SP_FREED && P.ions[size_t(p.sp - SP_ION)].ionization)
+            cap += P.ions[size_t(p.sp - SP_ION)].Zmax - std::lround(p.q);
+    P.nstrm = long(v.size());
+    P.born_cap = cap;
+    const long need = long(v.size()) + cap;
+    if (P.s.cap < need) {
+        const long n = need + need / 8 + 64;
+        P.s.alloc(n, c.stream);
+        P.sbk.alloc(n, c.stream);
+    }
+    if (cap > 0 && P.bn.cap < cap) P.bn.alloc(cap, c.stream);
+    P.strm = P.s.v;
+    P.born = P.bn.v;
+    // upload as columns
+    const long n = long(v.size());
+    if (n) {
+        std::vector<double> hd(size_t(n) * 10);
+        std::vector<int32_t> hi(size_t(n) * 2);
+        std::vector<uint64_t> hu(static_cast<size_t>(n));
+        for (long k = 0; k < n; ++k) {
+            const g3d_particle& p = v[size_t(k)];
+            const double vals[10] = {p.x, p.y, p.zeta, p.px, p.py, p.pz, p.w, p.z, p.q, p.qm};
+            for (int m = 0; m < 10; ++m) hd[size_t(m) * n + k] = vals[m];
+            hi[size_t(k)] = p.alive; hi[size_t(n) + k] = p.sp; hu[size_t(k)] = p.id;
+        }
+        double* cols[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
+        for (int m = 0; m < 10; ++m)
+            G3D_CUDA(cudaMemcpyAsync(cols[m], hd.data() + size_t(m) * n, size_t(n) * 8, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.alive, hi.data(), size_t(n) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.sp, hi.data() + n, size_t(n) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.id, hu.data(), size_t(n) * 8, cudaMemcpyHostToDevice, c.stream));
+    }
+    G3D_CUDA(cudaMemcpyAsync(P.nstrm_dev.p, &P.nstrm, sizeof(long), cudaMemcpyHostToDevice, c.stream));
+    G3D_CUDA(cudaMemsetAsync(P.flags.p, 0, sizeof(int), c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+// The streaming particles back on the host (the reference's `strm` after a march).
+std::vector<g3d_particle> get_streaming(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    long n = 0;
+    G3D_CUDA(cudaMemcpyAsync(&n, P.nstrm_dev.p, sizeof(long), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    std::vector<g3d_particle> out(static_cast<size_t>(n));
+    if (!n) return out;
+    std::vector<double> hd(size_t(n) * 10);
+    std::vector<int32_t> hi(size_t(n) * 2);
+    std::vector<uint64_t> hu(static_cast<size_t>(n));
+    const double* cols[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
+    for (int m = 0; m < 10; ++m)
+        G3D_CUDA(cudaMemcpyAsync(hd.data() + size_t(m) * n, cols[m], size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data(), P.strm.alive, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data() + n, P.strm.sp, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hu.data(), P.strm.id, size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    for (long k = 0; k < n; ++k) {
+        g3d_particle& p = out[size_t(k)];
+        double* dst[10] = {&p.x, &p.y, &p.zeta, &p.px, &p.py, &p.pz, &p.w, &p.z, &p.q, &p.qm};
+        for (int m = 0; m < 10; ++m) *dst[m] = hd[size_t(m) * n + k];
+        p.alive = hi[size_t(k)]; p.sp = hi[size_t(n) + k]; p.id = hu[size_t(k)];
+    }
+    return out;
+}
+
+// ---------------------------------------------------------------- the march of a step with plasma
+static uint64_t mix64h(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+void march_plasma(Ctx& c, double s0, double s1) {
+    PlasmaState& P = *c.pl;
+    const double Delta = s1 - s0, D = 0.5 * Delta;
+    const long nkh = c.nkh;
+    const int N = c.N;
+    const int nhi = N - 2;
+    auto hpl = [&](int m) { return long(m - c.a + 1) * nkh; };
+    load_plasma(c, s0, s1);
+    const bool extrap = P.cfg.predictor_extrapolate != 0;
+    std::vector<double> cen(size_t(N - 1));
+    for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
+    cpx* pin = P.jpred.p;
+    cpx* tmp = P.jtmp.p;
+    auto copy3 = [&](cpx* dst, int m) {           // dst <- js0 of half-cell m
+        for (int k = 0; k < 3; ++k) {
+            const cpx* src = (k == 0 ? P.js0x.p : k == 1 ? P.js0y.p : P.js0z.p) + hpl(m);
+            G3D_CUDA(cudaMemcpyAsync(dst + k * nkh, src, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+        }
+    };
+    bool have_dl = false;
+    P.jpred.zero(c.stream);
+    // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
+    copy3(tmp, N - 2);
+    launch_replace(c, N - 2, pin, tmp);
+    launch_march_slice(c, D, N - 1);
+    launch_real_fields_slice(c, N - 1);
+
+    StreamArgs sa;
+    sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.X0 = c.X0; sa.Y0 = c.Y0; sa.zc = c.P.zeta_center;
+    sa.Delta = Delta; sa.s1 = s1; sa.sTrap = s1 + (P.cfg.trap_advance - 1) * Delta; sa.vz_beam = P.cfg.vz_beam;
+    sa.J = P.jsr.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p; sa.bcap = 0; sa.key = 0;
+    const bool ionz = P.born_cap > 0;
+    const uint64_t key_step = mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep));   // ion_key_step
+    const int passes = P.cfg.iterations;
+    const long nmax = P.nstrm + P.born_cap;              // upper bound of the streaming particles of this march
+    for (int n = nhi; n >= c.a; --n) {
+        const long hp = hpl(n);
+        G3D_CUDA(cudaMemcpyAsync(P.jsin.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.jsi0.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+        if (n >= 1) {                                    // start of the prediction of half-cell n-1: its level s0
+            P.jpred.zero(c.stream);
+            copy3(tmp, n - 1);
+            launch_replace(c, n - 1, pin, tmp);
+        }
+        if (passes > 1) {
+            const long o = long(n - c.a) * nkh;
+            int k = 0;
+            for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
+                G3D_CUDA(cudaMemcpyAsync(P.bk.p + (k++) * nkh, a->p + o, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+            launch_strm_copy(c, P.sbk.v, P.strm, nmax);
+        }
+        const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl) ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+        for (int pass = 0; pass < passes; ++pass) {
+            if (pass > 0) {
+                const long o = long(n - c.a) * nkh;
+                int k = 0;
+                for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
+                    G3D_CUDA(cudaMemcpyAsync(a->p + o, P.bk.p + (k++) * nkh, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+                launch_strm_copy(c, P.strm, P.sbk.v, nmax);
+            }
+            P.jsr.zero(c.stream);
+            sa.n = n;
+            if (ionz) {
+                G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
+                sa.key = mix64h(key_step ^ ((uint64_t(n) << 8) | uint64_t(pass)));   // ion_key_slice
+                sa.bcap = int(P.born_cap);
+            }
+            launch_stream(c, sa, nmax);
+            launch_stream_spectra(c);
+            launch_replace_pred(c, n, extrap ? 1 : 0, wex);
+            launch_march_slice(c, D, n);
+            launch_real_fields_slice(c, n);
+        }
+        if (ionz) launch_born_append(c);
+        // half-cell n is final: correct R at slice n+1, keep the change and the current
+        const double q = D * c.wlo_h[size_t(n + 1)];
+        launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
+        have_dl = true;
+        (void)hp;
+    }
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    int flag = 0;
+    G3D_CUDA(cudaMemcpy(&flag, P.flags.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) throw Error(G3D_ERR_CAPACITY, "ionization: list of freed electrons overflowed");
+    // trapped particles: fast ones join the beam list, slow ones stream again in the next step
+    std::vector<g3d_particle> sv = get_streaming(c);
+    std::vector<g3d_particle> add;
+    for (auto& p : sv) {
+        if (p.alive != 5) continue;
+        const double g = std::sqrt(1 + p.px * p.px + p.py * p.py + p.pz * p.pz);
+        p.z = s1;
+        if (p.pz / g >= P.cfg.vz_beam) {
+            p.alive = 1;
+            p.sp = (p.sp >= SP_FREED && p.sp < SP_INJECTED) ? p.sp - SP_FREED + SP_INJECTED : p.sp >= SP_INJECTED ? p.sp : SP_TRAPPED;
+            ++P.trapped_total;
+            add.push_back(p);
+        } else { p.alive = 6; P.joining.push_back(p); }
+    }
+    if (!add.empty()) {
+        std::vector<g3d_particle> all = get_particles(c), keep;
+        keep.reserve(all.size() + add.size());
+        for (auto& p : all) if (p.alive == 1) keep.push_back(p);
+        keep.insert(keep.end(), add.begin(), add.end());
+        set_particles(c, keep.data(), long(keep.size()));
+    }
+    // the sponge damps R - R_b with the bound field of the beam list only: jkz -= js0z
+    launch_axpy_c(c, c.jkz.p, P.js0z.p, -1.0, size_t(c.ns + 1) * c.nkh);
+}
+
+// The beam particles that became slower than vz_min stream in the current march (collect_restreaming,
+// src/sim_plasma.cpp:474-491, one rank).
+void collect_restreaming(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    std::vector<g3d_particle> all = get_particles(c), keep;
+    bool any = false;
+    for (auto& p : all) if (p.alive == 4) { any = true; break; }
+    if (!any) return;
+    for (auto& p : all) {
+        if (p.alive == 4) {
+            g3d_particle q = p; q.alive = 6; ++P.restreamed_total;
+            P.joining.push_back(q);
+        } else if (p.alive == 1) keep.push_back(p);
+    }
+    set_particles(c, keep.data(), long(keep.size()));
+}
+
+// ---------------------------------------------------------------- grid lasers (add_grid_lasers)
+// The transverse profile exp(-(x^2 + y^2) / (w^2 qb)) / qb of a paraxial beam is separable; its two real parts
+// are transformed once, and every slice adds 2 Re(c_n P) (c_n = amp env_n carrier_n) times the polarisation.
+__global__ void k_glaser_profile(Geo g, double X0, double Y0, double w2, double qr, double qi, double* __restrict__ out) {
+    const long nk = g.nk;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nk; i += long(gridDim.x) * blockDim.x) {
+        const int ix = int(i % g.nx), j = int(i / g.nx);
+        const double xp = ix * g.dx + X0, yp = j * g.dy + Y0;
+        // exp(-(r^2/w^2) / qb) / qb, qb = qr + i qi
+        const double r2 = (xp * xp + yp * yp) / w2;
+        const double d = qr * qr + qi * qi;
+        const double ir = qr / d, ii = -qi / d;                   // 1 / qb
+        const double er = -r2 * ir, ei = -r2 * ii;
+        const double m = exp(er);
+        const double pr = m * cos(ei), pi = m * sin(ei);          // exp(-r^2/(w^2 qb))
+        out[i] = pr * ir - pi * ii;                               // real part of the product with 1/qb
+        out[nk + i] = pr * ii + pi * ir;                          // imaginary part
+    }
+}
+__global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __restrict__ PI, const double* __restrict__ cre,
+                             const double* __restrict__ cim, cpx* __restrict__ Rx, cpx* __restrict__ Ry, double ax, double ay,
+                             double bx, double by) {
+    // R_x += 2 (ax (cre PR - cim PI) + bx (cim PR + cre PI)), R_y likewise with ay, by (real-valued field factors)
+    const long nk = g.nkh, n = long(g.ns) * nk;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long l = idx / nk, i = idx - l * nk;
+        const double cr = cre[l], ci = cim[l];
+        if (cr == 0 && ci == 0) continue;
+        const cpx re = cr * PR[i] - ci * PI[i];          // spectrum of Re(c P)
+        const cpx im = ci * PR[i] + cr * PI[i];          // spectrum of Im(c P)
+        Rx[idx] = Rx[idx] + 2.0 * (ax * re + bx * im);
+        Ry[idx] = Ry[idx] + 2.0 * (ay * re + by * im);
+    }
+}
+
+void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3);   // k_plasma.cu
+
+void add_grid_lasers(Ctx& c) {
+    if (c.glasers.empty()) return;
+    DevBuf<double> prof;
+    prof.alloc(size_t(3) * c.nk, c.stream);          // Re P, Im P, and a zero plane
+    DevBuf<cpx> spec, tsc;
+    spec.alloc(size_t(3) * c.nkh, c.stream);
+    tsc.alloc(size_t(3) * c.nkh, c.stream);
+    DevBuf<double> coef;
+    coef.alloc(size_t(2) * c.ns, c.stream);
+    for (const auto& Lz : c.glasers) {
+        const double amp = Lz.a0 * Lz.kL;
+        const double zR = 0.5 * Lz.kL * Lz.waist * Lz.waist;
+        const std::complex<double> qb(1.0, (0.0 - Lz.z_focus) / zR);
+        const std::complex<double> rot(std::cos(Lz.pol_angle), std::sin(Lz.pol_angle));
+        std::vector<double> cre(size_t(c.ns), 0.0), cim(size_t(c.ns), 0.0);
+        for (int n = 0; n < c.ns; ++n) {
+            const double d = c.zeta[size_t(n)] - Lz.zeta_c;
+            const double env = std::exp(-2 * std::log(2.0) * d * d / (Lz.tau * Lz.tau));
+            if (std::fabs(env) < 1e-12) continue;
+            const std::complex<double> car = std::exp(std::complex<double>(0, Lz.kL * d + Lz.cep));
+            const std::complex<double> cn = amp * env * car;
+            cre[size_t(n)] = cn.real(); cim[size_t(n)] = cn.imag();
+        }
+        k_glaser_profile<<<148 * 4, 256, 0, c.stream>>>(c.geo(), c.X0, c.Y0, Lz.waist * Lz.waist, qb.real(), qb.imag(), prof.p);
+        c.check_launch("k_glaser_profile");
+        launch_real_to_half3(c, prof.p, tsc.p, spec.p);
+        G3D_CUDA(cudaMemcpyAsync(coef.p, cre.data(), size_t(c.ns) * 8, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(coef.p + c.ns, cim.data(), size_t(c.ns) * 8, cudaMemcpyHostToDevice, c.stream));
+        // linear: ex = Re(E) cos(pol), ey = Re(E) sin(pol); circular: ex = Re E, ey = helicity Im E
+        double ax, ay, bx, by;
+        if (Lz.circular) { ax = 1; bx = 0; ay = 0; by = Lz.helicity; }
+        else { ax = rot.real(); bx = 0; ay = rot.imag(); by = 0; }
+        k_glaser_add<<<148 * 8, 256, 0, c.stream>>>(c.geo(), spec.p, spec.p + c.nkh, coef.p, coef.p + c.ns, c.Rx.p, c.Ry.p,
+                                                     ax, ay, bx, by);
+        c.check_launch("k_glaser_add");
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    }
+}
+
+}  // namespace g3d

@@ -1,0 +1,96 @@
+// State of the streaming plasma (one rank): the device structs of k_plasma.cu and the host-side state of
+// Simulation's plasma members (src/sim.hpp:292-311).
+#pragma once
+#include <memory>
+#include <vector>
+#include "g3d_ctx.hpp"
+
+namespace g3d {
+
+// species codes of the reference (src/sim.hpp:29)
+constexpr int SP_TRAPPED = 1, SP_PLASMA = 2, SP_ION = 3, SP_FREED = 50, SP_INJECTED = 100;
+
+// one ADK level in code units (reference AdkLevel, src/ionization.hpp:197)
+struct AdkDev { double logpre, power, expo, Epeak, Emin; };
+// an ion species on the device (reference IonDev, src/sim.hpp:27)
+struct IonDevC { double mass; int mobile, ionizing, Zmax, off; double Emin; };
+
+// streaming particles as structure of arrays
+struct StrmDev {
+    double *x, *y, *zeta, *px, *py, *pz, *w, *z, *q, *qm;
+    int32_t *alive, *sp;
+    uint64_t* id;
+};
+
+struct StreamArgs {
+    const float* __restrict__ F;
+    Geo g;
+    LaserDev laser;
+    double X0, Y0, zc, Delta, s1, sTrap, vz_beam;
+    int n;
+    double* J;                 // jsr: jx, jy, jz, rho-, rho+ of the half-cell (real planes)
+    const IonDevC* ions;
+    const AdkDev* adk;
+    StrmDev born;
+    int* bcnt;
+    int bcap;
+    uint64_t key;              // ion_key_slice(ion_key_step(seed, istep), n, pass)
+};
+
+struct PlasmaPtrs {
+    long nkh;
+    cpx *jkx, *jky, *jkz, *js0x, *js0y, *js0z, *jsn, *sin_, *si0, *pin, *tmp, *dl;
+};
+
+struct IonSpec {
+    double mass, atoms;
+    int Z0, Zmax, mobile, ionization;
+    std::vector<double> ip_eV;
+    bool loaded() const { return mobile || ionization; }
+};
+
+// A DevBuf-backed structure of arrays of streaming particles.
+struct StrmBuf {
+    DevBuf<double> d;          // 10 columns
+    DevBuf<int32_t> i;         // 2 columns
+    DevBuf<uint64_t> u;        // ids
+    StrmDev v{};
+    long cap = 0;
+    void alloc(long n, cudaStream_t s);
+};
+
+struct PlasmaState {
+    g3d_plasma cfg{};
+    std::vector<double> zpts, zvals;
+    std::vector<IonSpec> ions;
+    bool box_mean = true;
+    // spectra of the streaming current: level s0 per half-cell (the prediction of the next step), the current
+    // of one half-cell (jsr real, jsn spectra), the parts of jk held as predictions, backups
+    DevBuf<cpx> js0x, js0y, js0z;              // ns+1 half planes
+    DevBuf<double> jsr;                        // 5 real planes
+    DevBuf<cpx> jsn, jsin, jpred, jtmp, jsi0, dlt, tsp;   // 3 half planes each
+    DevBuf<cpx> bk;                            // 4 half planes: R_x, R_y, E_z, B_z of the slice
+    StrmBuf s, sbk, bn;                        // streaming particles, their backup, the freed electrons
+    StrmDev strm{}, born{};
+    long nstrm = 0;                            // host copy (exact at the start of the march)
+    long born_cap = 0, fresh_last = 0, trapped_total = 0, restreamed_total = 0;
+    DevBuf<long> nstrm_dev;
+    DevBuf<int> bcnt, flags;
+    DevBuf<IonDevC> ion_dev;
+    DevBuf<AdkDev> adk_dev;
+    std::vector<g3d_particle> joining;         // join the next march at their zeta
+    PlasmaPtrs ptrs(const Ctx& c) const;
+};
+
+// launchers (k_plasma.cu)
+void launch_stream(Ctx& c, const StreamArgs& a, long nmax);
+void launch_stream_spectra(Ctx& c);
+void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw);
+void launch_replace_pred(Ctx& c, int n, int extrap, double w);
+void launch_correct(Ctx& c, int n, double q, int own);
+void launch_march_slice(Ctx& c, double D, int n);
+void launch_born_append(Ctx& c);
+void launch_strm_copy(Ctx& c, const StrmDev& dst, const StrmDev& src, long nmax);
+void launch_real_fields_slice(Ctx& c, int l);
+
+}  // namespace g3d

@@ -186,10 +186,11 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
                                                                   const cpx* __restrict__ Lx, const cpx* __restrict__ Ly,
                                                                   const cpx* __restrict__ Ez, const cpx* __restrict__ Bz,
                                                                   cpx* __restrict__ W0, cpx* __restrict__ W1, cpx* __restrict__ W2,
-                                                                  cpx* __restrict__ W3, cpx* __restrict__ W4, cpx* __restrict__ W5) {
+                                                                  cpx* __restrict__ W3, cpx* __restrict__ W4, cpx* __restrict__ W5,
+                                                                  int l0) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
-    const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z;
+    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z;
     const int H = g.H;
     const long base = long(l) * g.nkh;
     const cpx* in0 = pr == 0 ? Rx : pr == 1 ? Lx : Ez;
@@ -221,14 +222,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
 template <int NX>
 __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                const cpx* __restrict__ W2, const cpx* __restrict__ W3,
-                                               const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F) {
+                                               const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F, int l0) {
     using S = FftShape<NX>;
     constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
     cpx* a0 = sm;
     cpx* a1 = sm + LPC * RS;
     cpx* a2 = sm + 2 * LPC * RS;
-    const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
+    const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
     for (int e = tid; e < LPC * H; e += NT) {
         const int r = e / H, p = e - r * H, row = r0 + r;
@@ -309,29 +310,34 @@ void launch_sponge(Ctx& c) {
 }
 
 template <int NY>
-static void rf_cols(Ctx& c) {
+static void rf_cols(Ctx& c, int l0, int nl) {
     const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
     allow_smem(k_rf_cols<NY>, smem);
-    const int tok = c.prof_begin("real_cols");
-    k_rf_cols<NY><<<dim3(col_tiles(c), unsigned(c.ns), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p);
+    const int tok = c.prof_begin(nl == 1 ? "real_cols_slice" : "real_cols");
+    k_rf_cols<NY><<<dim3(col_tiles(c), unsigned(nl), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, l0);
     c.check_launch("k_rf_cols");
     c.prof_end(tok);
 }
 template <int NX>
-static void rf_rows(Ctx& c) {
+static void rf_rows(Ctx& c, int l0, int nl) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
     allow_smem(k_rf_rows<NX>, smem);
-    const int tok = c.prof_begin("real_rows");
-    k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(
-        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p);
+    const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
+    k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
+        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
 void launch_real_fields(Ctx& c) {
-    G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c));
-    G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c));
+    G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, 0, c.ns));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, 0, c.ns));
+}
+// E and B of one slice (plane l) in real space (Simulation::real_fields_slice, src/sim_plasma.cpp:200-220)
+void launch_real_fields_slice(Ctx& c, int l) {
+    G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, l, 1));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, l, 1));
 }
 
 // ---------------------------------------------------------------- half <-> full spectrum layouts
@@ -414,6 +420,11 @@ __global__ void k_shift_parts(PartsDev P, long np, double sx, double sy) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < np; i += long(gridDim.x) * blockDim.x) {
         P.x[i] -= sx; P.y[i] -= sy;
     }
+}
+void launch_rotate(Ctx& c, cpx* p, size_t n, double sx, double sy, int nys) {
+    if (!n) return;
+    k_rotate<<<ew_blocks(long(n)), 256, 0, c.stream>>>(c.geo(), p, long(n), sx, sy, nys);
+    c.check_launch("k_rotate");
 }
 void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy) {
     const Geo g = c.geo();

@@ -1,0 +1,481 @@
+// Streaming plasma: the march of a step with plasma, half-cell by half-cell (Simulation::march_plasma,
+// src/sim_plasma.cpp:228-470, one rank, Fourier y).
+//
+// Per half-cell n (front to rear) and pass:
+//   k_stream       one thread per streaming particle: the push through the half-cell (stream_one,
+//                  src/sim_stream.hpp:104-171): mid-point gather of the grid fields + analytic wave, two relativistic
+//                  Boris pushes (a third when the particle is trapped inside the half-cell), TSC deposit of its
+//                  current and charge into the real planes jsr (stream_deposit, :33-64), ADK ionization of the ions
+//                  with the counter-based random numbers (ionize, :80-101; ionization.hpp:25-46)
+//   k_ss_rows/cols the spectra of jsr: FFT of jx + i jy and jz of one plane, the k-filters, the smoothing
+//                  1 / (1 + a^2 k_perp^2) (stream_spectra, src/sim_plasma.cpp:94-157) -> jsn (half spectrum)
+//   k_replace_pred replace the streaming part of jk(n) by jsn and, with the extrapolating predictor, of jk(n-1) by
+//                  js0(n-1) + d + w (d - dl), d = jsn - js0(n) (sim_plasma.cpp:339-351)
+//   k_march_slice  the march of the modes of slice n (march_point, src/sim_kernels.hpp:173-210)
+//   real fields of slice n: the column and row kernels of k_fields.cu on one plane
+// After the passes: k_correct (R of slice n+1 corrected for the prediction it used; dl, js0 updated,
+// sim_plasma.cpp:381-403) and k_born_append (the freed electrons join the march).
+#include "g3d_plasma.hpp"
+#include "k_fft.cuh"
+#include "k_dispatch.cuh"
+
+namespace g3d {
+
+// ---------------------------------------------------------------- relativistic Boris (sim_stream.hpp:8-18)
+__device__ __forceinline__ void boris(double& ux, double& uy, double& uz, const double E[3], const double B[3], double qm, double dt) {
+    const double qh = 0.5 * qm * dt;
+    const double umx = ux + qh * E[0], umy = uy + qh * E[1], umz = uz + qh * E[2];
+    const double gm = sqrt(1.0 + umx * umx + umy * umy + umz * umz);
+    const double tx = qh * B[0] / gm, ty = qh * B[1] / gm, tz = qh * B[2] / gm;
+    const double t2 = tx * tx + ty * ty + tz * tz;
+    const double upx = umx + (umy * tz - umz * ty), upy = umy + (umz * tx - umx * tz), upz = umz + (umx * ty - umy * tx);
+    const double sf = 2.0 / (1.0 + t2);
+    const double vx = umx + sf * (upy * tz - upz * ty), vy = umy + sf * (upz * tx - upx * tz), vz = umz + sf * (upx * ty - upy * tx);
+    ux = vx + qh * E[0]; uy = vy + qh * E[1]; uz = vz + qh * E[2];
+}
+
+// grid fields of the F planes (TSC in x, y, linear in zeta) as in the beam push
+__device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
+    E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
+    const Geo& g = c.g;
+    int n; double fz;
+    g.zax.locate(zeta, n, fz);
+    if (n == g.a - 1 && fz > 1 - 1e-9) { n = g.a; fz = 0; }
+    const int fl = n - g.a;
+    if (fl < 0 || fl > g.ns) return;
+    int ix[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    const long nk = g.nk;
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) {
+        const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
+        const float* p1 = p0 + nk;
+        double v = 0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const long k = long(jn[j]) * g.nx + ix[i];
+                v += wx[i] * wn[j] * ((1 - fz) * double(p0[k]) + fz * double(p1[k]));
+            }
+        if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+    }
+}
+__device__ __forceinline__ double wrapx(const Geo& g, double x) { return fmod(fmod(x, g.Lx) + g.Lx, g.Lx); }
+__device__ __forceinline__ double wrapy(const Geo& g, double y) { return fmod(fmod(y, g.Ly) + g.Ly, g.Ly); }
+
+// TSC deposit of f (v, 1) at (x, y) into jsr: jx, jy, jz and the charge of negative (plane 3) or positive
+// (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y)
+__device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
+    const Geo& g = c.g;
+    int ix_[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(x, g.dx, g.nx, ix_, wx);
+    const long nk = g.nk, cq = (f < 0 ? 3 : 4) * nk;
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    const double ia0 = g.iA[0];
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const long k = long(jn[v]) * g.nx + ix_[u];
+            const double w = f * wx[u] * wn[v] * ia0;
+            atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
+            atomicAdd(&c.J[cq + k], w);
+        }
+}
+
+// |E| of the grid and the wave at (x, y), lab z, slice position zeta (field_abs, sim_stream.hpp:67-74)
+__device__ __forceinline__ double field_abs(const StreamArgs& c, double x, double y, double z, double zeta) {
+    double E[3], B[3], Ee[3], Be[3];
+    sgather(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);
+    c.laser.field(x + c.X0, z, z - (zeta - c.zc), Ee, Be);
+    for (int k = 0; k < 3; ++k) E[k] += Ee[k];
+    return sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
+}
+
+// ADK rate of a level (ionization.hpp:198-202) and the counter-based random numbers (ionization.hpp:209-218)
+__device__ __forceinline__ double adk_rate(const AdkDev& L, double E) {
+    if (!(E >= L.Emin) || !(E > 0)) return 0.0;
+    E = E < L.Epeak ? E : L.Epeak;
+    return exp(L.logpre - L.power * log(E) + L.expo / E);
+}
+G3D_HD uint64_t mix64(uint64_t z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double uniform01(uint64_t key) { return double(mix64(key) >> 11) * (1.0 / 9007199254740992.0); }
+
+// Monte Carlo field ionization during dt (ionize, sim_stream.hpp:80-101): sequential levels with exponential
+// waiting times; each event frees an electron at the ion (a copy with q = -1 into the born list).
+__device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1, double E0, double dt) {
+    const int sp = S.sp[i];
+    const IonDevC& I = c.ions[sp - SP_ION];
+    if (!I.ionizing || (E1 < I.Emin && E0 < I.Emin)) return;
+    const uint64_t base = mix64(c.key ^ mix64(S.id[i]));          // ion_key_particle(key_slice, id)
+    int Z = int(floor(S.q[i] + 0.5));
+    const int Z0 = Z;
+    unsigned draw = 0;
+    double tleft = dt;
+    while (Z < I.Zmax) {
+        const AdkDev& L = c.adk[I.off + Z];
+        const double w = 0.5 * (adk_rate(L, E1) + adk_rate(L, E0));
+        if (!(w > 0)) break;
+        const double tw = -log(1.0 - uniform01(base + draw++)) / w;
+        if (tw > tleft) break;
+        tleft -= tw; ++Z;
+        const int j = atomicAdd(c.bcnt, 1);
+        if (j < c.bcap) {
+            const StrmDev& Bn = c.born;
+            Bn.x[j] = S.x[i]; Bn.y[j] = S.y[i]; Bn.zeta[j] = S.zeta[i]; Bn.px[j] = S.px[i]; Bn.py[j] = S.py[i];
+            Bn.pz[j] = S.pz[i]; Bn.w[j] = S.w[i]; Bn.z[j] = S.z[i]; Bn.q[j] = -1; Bn.qm[j] = -1;
+            Bn.alive[j] = 1; Bn.sp[j] = SP_FREED + (sp - SP_ION); Bn.id[j] = S.id[i];
+        }
+    }
+    if (Z != Z0) { S.q[i] = Z; S.qm[i] = Z / I.mass; }
+}
+
+// one streaming particle through half-cell n (stream_one, sim_stream.hpp:104-171)
+__global__ void __launch_bounds__(128) k_stream(StreamArgs c, StrmDev S, const long* __restrict__ nstrm) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= *nstrm) return;                // the launch covers the freed electrons that may join
+    const Geo& g = c.g;
+    const int n = c.n;
+    const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn;
+    int alive = S.alive[i];
+    if (alive == 6) {                 // waiting: joins the march inside the half-cell that holds its zeta
+        if (S.zeta[i] > zn) { alive = 1; S.alive[i] = 1; }
+        else return;
+    }
+    if (alive != 1) return;
+    const double zeta = S.zeta[i];
+    const double hl = zeta >= zn1 - 1e-9 * h ? h : (zeta - zn > 0 ? zeta - zn : 0.0);
+    const int sp = S.sp[i];
+    const bool ion = sp >= SP_ION && sp < SP_FREED;
+    if (ion && !c.ions[sp - SP_ION].mobile) {        // fixed ion: its charge, then the ionization
+        const double f = S.q[i] * S.w[i] * hl / (c.Delta * h * g.dx);
+        if (f != 0) sdeposit(c, S.x[i], S.y[i], f, 0, 0, 0);
+        const double E1 = field_abs(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs(c, S.x[i], S.y[i], S.z[i], zn);
+        S.zeta[i] = zn;
+        ionize(c, S, i, E1, E0, hl);
+        return;
+    }
+    const double x = S.x[i], y = S.y[i], z = S.z[i], px = S.px[i], py = S.py[i], pz = S.pz[i], qm = S.qm[i];
+    const double g0 = sqrt(1 + px * px + py * py + pz * pz);
+    const double omv0 = (1 + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
+    const double dt0 = hl / omv0;
+    const double xm = x + 0.5 * dt0 * px / g0, ym = y + 0.5 * dt0 * py / g0;
+    const double zm = z + 0.5 * dt0 * pz / g0, zetam = zeta - 0.5 * hl;
+    double E[3], B[3], Ee[3], Be[3];
+    sgather(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
+    c.laser.field(xm + c.X0, zm, zm - (zetam - c.zc), Ee, Be);
+    for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+    double ux = px, uy = py, uz = pz;
+    boris(ux, uy, uz, E, B, qm, dt0);
+    double g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
+    double dt = 2 * hl / (omv0 + (1 + ux * ux + uy * uy) / (g1 * (g1 + uz)));
+    ux = px; uy = py; uz = pz;
+    boris(ux, uy, uz, E, B, qm, dt);
+    g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
+    double vx = 0.5 * (px / g0 + ux / g1), vy = 0.5 * (py / g0 + uy / g1), vz = 0.5 * (pz / g0 + uz / g1);
+    double zeta_end = zn;
+    bool trapped = false;
+    if (z + vz * dt >= c.sTrap) {     // advanced trap_advance steps inside this half-cell: trapped
+        const double vv = vz > 1e-3 ? vz : 1e-3;
+        const double dtp = (c.sTrap - z) / vv > 0 ? (c.sTrap - z) / vv : 0.0;
+        ux = px; uy = py; uz = pz;
+        boris(ux, uy, uz, E, B, qm, dtp);
+        g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
+        vx = 0.5 * (px / g0 + ux / g1); vy = 0.5 * (py / g0 + uy / g1); vz = 0.5 * (pz / g0 + uz / g1);
+        dt = dtp;
+        zeta_end = zeta - (1 - vz) * dtp;
+        trapped = true;
+    }
+    const double xn = x + vx * dt, yn = y + vy * dt;
+    S.x[i] = xn; S.y[i] = yn;
+    S.z[i] = trapped ? c.s1 : z + vz * dt;
+    S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
+    S.zeta[i] = zeta_end;
+    const double q = S.q[i], w = S.w[i];
+    const double f = q * w * dt / (c.Delta * h * g.dx);
+    if (f != 0) sdeposit(c, 0.5 * (x + xn), 0.5 * (y + yn), f, vx, vy, vz);
+    if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
+        ionize(c, S, i, field_abs(c, xm, ym, zm, zeta), field_abs(c, xm, ym, zm, zn), dt);
+    if (trapped) {
+        S.alive[i] = 5;
+        const double vze = uz / g1;
+        if (vze >= c.vz_beam)         // joins the beam list: its beam current of level s1 from now on
+            sdeposit(c, xn, yn, q * w / (h * g.dx * vze), ux / g1, uy / g1, vze);
+    }
+}
+
+// ---------------------------------------------------------------- spectra of the streaming current
+// rows: per row, FFT along x of jx + i jy (split) and of jz -> three half rows in T0..T2
+template <int NX>
+__global__ void __launch_bounds__(128) k_ss_rows(Geo g, const double* __restrict__ J, cpx* __restrict__ T0, cpx* __restrict__ T1,
+                                                cpx* __restrict__ T2) {
+    using S = FftShape<NX>;
+    constexpr int LPC = 128 / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
+    extern __shared__ cpx sm[];
+    cpx* a0 = sm;
+    cpx* a1 = sm + LPC * RS;
+    const int tid = threadIdx.x, r0 = blockIdx.x * LPC;
+    const long nk = g.nk;
+    for (int e = tid; e < LPC * NX; e += 128) {
+        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
+        double jx = 0, jy = 0, jz = 0;
+        if (row < g.ny) { const long i = long(row) * NX + p; jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i]; }
+        a0[rr * RS + p + (p >> 3)] = C(jx, jy);
+        a1[rr * RS + p + (p >> 3)] = C(jz, 0.0);
+    }
+    __syncthreads();
+    const int r = tid / S::T, t = tid - r * S::T;
+    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
+    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    for (int e = tid; e < LPC * H; e += 128) {
+        const int rr = e / H, kx = e - rr * H, row = r0 + rr;
+        if (row >= g.ny) continue;
+        const int km = (NX - kx) % NX;
+        const cpx z = a0[rr * RS + kx + (kx >> 3)], zm = conj(a0[rr * RS + km + (km >> 3)]);
+        const cpx d = z - zm;
+        const long o = long(row) * H + kx;
+        T0[o] = 0.5 * (z + zm);
+        T1[o] = 0.5 * C(d.y, -d.x);
+        T2[o] = a1[rr * RS + kx + (kx >> 3)];
+    }
+}
+// columns: FFT along y, filters and smoothing -> jsn (3 half planes)
+template <int NY, int CW>
+__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_ss_cols(Geo g, const cpx* __restrict__ T0, const cpx* __restrict__ T1,
+                                                                  const cpx* __restrict__ T2, cpx* __restrict__ out, double a2, int keep0,
+                                                                  int filter) {
+    using S = FftShape<NY>;
+    extern __shared__ cpx sm[];
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * CW;
+    cpx* s2 = sm + 2 * NY * CW;
+    const int c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, c = e - p * CW, kx = c0 + c;
+        cpx u0 = C(0), u1 = C(0), u2 = C(0);
+        if (kx < H) { const long o = long(p) * H + kx; u0 = T0[o]; u1 = T1[o]; u2 = T2[o]; }
+        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+    }
+    __syncthreads();
+    const int c = tid % CW, t = tid / CW;
+    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    fft_line<NY>(s2, ColAddr<CW>{c}, t, g.twy);
+    const long nkh = g.nkh;
+    for (int e = tid; e < NY * CW; e += nthr) {
+        const int p = e / CW, cc = e - p * CW, kx = c0 + cc;
+        if (kx >= H) continue;
+        const double k2 = g.kxs[kx] * g.kxs[kx] + g.kys[p] * g.kys[p];
+        const double f = !filter ? 1.0 : (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p] / (1 + a2 * k2);
+        const long o = long(p) * H + kx;
+        out[o] = f * s0[e];
+        out[nkh + o] = f * s1[e];
+        out[2 * nkh + o] = f * s2[e];
+    }
+}
+
+// ---------------------------------------------------------------- elementwise steps of the half-cell
+// jk(m) += nw - old; old <- nw (the `replace` of sim_plasma.cpp:257-264), three half planes
+__global__ void k_replace(cpx* __restrict__ jx, cpx* __restrict__ jy, cpx* __restrict__ jz, cpx* __restrict__ old,
+                          const cpx* __restrict__ nw, long nkh) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        jx[i] = jx[i] + nw[i] - old[i];
+        jy[i] = jy[i] + nw[nkh + i] - old[nkh + i];
+        jz[i] = jz[i] + nw[2 * nkh + i] - old[2 * nkh + i];
+        old[i] = nw[i]; old[nkh + i] = nw[nkh + i]; old[2 * nkh + i] = nw[2 * nkh + i];
+    }
+}
+// after a pass: replace the streaming part of jk(n) by jsn (old = sin); with the extrapolating predictor and
+// n >= 1 the prediction of half-cell n-1: tmp = js0(n-1) + d + w (d - dl), d = jsn - js0(n); replace(n-1, pin, tmp)
+__global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
+    const long nkh = p.nkh;
+    const long hp = long(n + 1) * nkh, hq = long(n) * nkh;        // planes of half-cells n and n-1 (a = 0)
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        cpx u[3];
+        for (int k = 0; k < 3; ++k) u[k] = p.jsn[k * nkh + i];
+        cpx* jk[3] = {p.jkx, p.jky, p.jkz};
+        for (int k = 0; k < 3; ++k) {
+            jk[k][hp + i] = jk[k][hp + i] + u[k] - p.sin_[k * nkh + i];
+            p.sin_[k * nkh + i] = u[k];
+        }
+        if (extrap && n >= 1) {
+            const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
+            for (int k = 0; k < 3; ++k) {
+                const cpx d = u[k] - s0[k][hp + i];
+                const cpx t = s0[k][hq + i] + d + w * (d - p.dl[k * nkh + i]);
+                jk[k][hq + i] = jk[k][hq + i] + t - p.pin[k * nkh + i];
+                p.pin[k * nkh + i] = t;
+            }
+        }
+    }
+}
+// half-cell n is final (sim_plasma.cpp:381-403): R at slice n+1 corrected for the prediction it used; the
+// change s0 -> s1 kept for the extrapolation; the current kept as the prediction of the next step
+__global__ void k_correct(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ Ry, int n, double q, int own) {
+    const long nkh = p.nkh;
+    const long hp = long(n + 1) * nkh, sp1 = long(n + 1) * nkh;
+    cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        const cpx u0 = p.jsn[i], u1 = p.jsn[nkh + i], u2 = p.jsn[2 * nkh + i];
+        if (own) {
+            Rx[sp1 + i] = Rx[sp1 + i] - q * (u0 - p.si0[i]);
+            Ry[sp1 + i] = Ry[sp1 + i] - q * (u1 - p.si0[nkh + i]);
+        }
+        p.dl[i] = u0 - s0[0][hp + i]; p.dl[nkh + i] = u1 - s0[1][hp + i]; p.dl[2 * nkh + i] = u2 - s0[2][hp + i];
+        s0[0][hp + i] = u0; s0[1][hp + i] = u1; s0[2][hp + i] = u2;
+    }
+}
+// the march of slice n, all modes (march_point, sim_kernels.hpp:173-210, one rank: b = N, no boundary slice)
+__global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, cpx* __restrict__ Ez,
+                                                    cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
+                                                    const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
+                                                    const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
+                                                    const cpx* __restrict__ jkz, double D, int n) {
+    const long nk = g.nkh;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nk) return;
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
+    const long o = long(n - g.a) * nk + i, od = o, ou = o + nk;
+    const cpx Jx = wl * (j0x[od] + jkx[od]) + wu * (j0x[ou] + jkx[ou]);
+    const cpx Jy = wl * (j0y[od] + jky[od]) + wu * (j0y[ou] + jky[ou]);
+    const cpx Rsx = Rx[o] + D * (ik(kx, Ez[o]) + ik(ky, Bz[o])) - D * Jx;
+    const cpx Rsy = Ry[o] + D * (ik(ky, Ez[o]) - ik(kx, Bz[o])) - D * Jy;
+    if (n == g.N - 1) {
+        Rx[o] = Rsx; Ry[o] = Rsy; Ez[o] = C(0); Bz[o] = C(0); Lx[o] = C(0); Ly[o] = C(0);
+        return;
+    }
+    const long pp = o + nk;
+    const cpx pRx = Rx[pp], pRy = Ry[pp], pEz = Ez[pp], pBz = Bz[pp], pLx = Lx[pp], pLy = Ly[pp];
+    const double h = g.hcg[n + 2];
+    const cpx upx = jkx[ou], upy = jky[ou], upz = jkz[ou];
+    const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
+    const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
+    const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
+    const cpx Qp = -0.5 * ik(kx, pRx - pLx) + 0.5 * ik(ky, pLy - pRy);
+    const cpx SB = ik(kx, Rsy) + ik(kx, Lsy) - ik(ky, Rsx) - ik(ky, Lsx);
+    const cpx SE = -ik(kx, Rsx) + ik(kx, Lsx) + ik(ky, Lsy) - ik(ky, Rsy);
+    const double den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+    const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) / den;
+    const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) / den;
+    Ez[o] = Ezn; Bz[o] = Bzn;
+    Rx[o] = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)); Ry[o] = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
+    Lx[o] = Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)); Ly[o] = Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn));
+}
+// freed electrons join the march (appended after the streaming particles; the count stays on the device)
+__global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
+                              int* __restrict__ overflow) {
+    const int cnt = *bcnt;
+    const long base = *nstrm_dev;
+    if (cnt > bcap) { if (blockIdx.x == 0 && threadIdx.x == 0) *overflow = 1; return; }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += gridDim.x * blockDim.x) {
+        const long d = base + k;
+        S.x[d] = Bn.x[k]; S.y[d] = Bn.y[k]; S.zeta[d] = Bn.zeta[k]; S.px[d] = Bn.px[k]; S.py[d] = Bn.py[k];
+        S.pz[d] = Bn.pz[k]; S.w[d] = Bn.w[k]; S.z[d] = Bn.z[k]; S.q[d] = Bn.q[k]; S.qm[d] = Bn.qm[k];
+        S.alive[d] = Bn.alive[k]; S.sp[d] = Bn.sp[k]; S.id[d] = Bn.id[k];
+    }
+}
+__global__ void k_count_add(long* __restrict__ nstrm_dev, const int* __restrict__ bcnt, int bcap) {
+    const int cnt = *bcnt;
+    if (cnt <= bcap) *nstrm_dev += cnt;
+}
+
+// ---------------------------------------------------------------- launchers
+static unsigned ew_blocks(long n) {
+    long b = (n + 255) / 256;
+    return unsigned(b < 148 * 8 ? (b < 1 ? 1 : b) : 148 * 8);
+}
+void launch_stream(Ctx& c, const StreamArgs& a, long nmax) {
+    if (nmax <= 0) return;
+    const int tok = c.prof_begin("stream");
+    k_stream<<<unsigned((nmax + 127) / 128), 128, 0, c.stream>>>(a, c.pl->strm, c.pl->nstrm_dev.p);
+    c.check_launch("k_stream");
+    c.prof_end(tok);
+}
+// Half spectra of three real planes J[0..2] (jx, jy, jz layout) into out[0..2]; T is scratch (3 half planes).
+template <int NX>
+static void ss_rows(Ctx& c, const double* J, cpx* T) {
+    using S = FftShape<NX>;
+    constexpr int LPC = 128 / S::T;
+    const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
+    G3D_CUDA(cudaFuncSetAttribute(k_ss_rows<NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_ss_rows<NX><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh);
+    c.check_launch("k_ss_rows");
+}
+template <int NY>
+static void ss_cols(Ctx& c, const cpx* T, cpx* out, double a2, int keep0, int filter) {
+    constexpr int CW = 8;
+    const size_t smem = size_t(3) * NY * CW * sizeof(cpx);
+    G3D_CUDA(cudaFuncSetAttribute(k_ss_cols<NY, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_ss_cols<NY, CW><<<unsigned((c.H + CW - 1) / CW), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), T, T + c.nkh, T + 2 * c.nkh, out, a2, keep0, filter);
+    c.check_launch("k_ss_cols");
+}
+void launch_stream_spectra(Ctx& c) {
+    const int tok = c.prof_begin("stream_spectra");
+    PlasmaState& P = *c.pl;
+    const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
+    G3D_DISPATCH_N(c.nx, NX, ss_rows<NX>(c, P.jsr.p, P.tsp.p));
+    G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, P.tsp.p, P.jsn.p, a2, P.box_mean ? 1 : 0, 1));
+    c.prof_end(tok);
+}
+// plain transverse spectra (no filters) of three real planes: the grid-laser profile
+void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
+    G3D_DISPATCH_N(c.nx, NX, ss_rows<NX>(c, J3, T3));
+    G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
+}
+
+// copy of the streaming particles that a pass modifies (backup / restore of a half-cell's passes)
+__global__ void k_strm_copy(StrmDev d, StrmDev s, long n) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        d.x[i] = s.x[i]; d.y[i] = s.y[i]; d.zeta[i] = s.zeta[i]; d.px[i] = s.px[i]; d.py[i] = s.py[i]; d.pz[i] = s.pz[i];
+        d.z[i] = s.z[i]; d.q[i] = s.q[i]; d.qm[i] = s.qm[i]; d.alive[i] = s.alive[i];
+        d.w[i] = s.w[i]; d.sp[i] = s.sp[i]; d.id[i] = s.id[i];
+    }
+}
+void launch_strm_copy(Ctx& c, const StrmDev& dst, const StrmDev& src, long nmax) {
+    if (nmax <= 0) return;
+    const int tok = c.prof_begin("strm_copy");
+    k_strm_copy<<<ew_blocks(nmax), 256, 0, c.stream>>>(dst, src, nmax);
+    c.check_launch("k_strm_copy");
+    c.prof_end(tok);
+}
+void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw) {
+    const long h = long(m + 1) * c.nkh;
+    k_replace<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.jkx.p + h, c.jky.p + h, c.jkz.p + h, old, nw, c.nkh);
+    c.check_launch("k_replace");
+}
+void launch_replace_pred(Ctx& c, int n, int extrap, double w) {
+    const int tok = c.prof_begin("replace_pred");
+    k_replace_pred<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), n, extrap, w);
+    c.check_launch("k_replace_pred");
+    c.prof_end(tok);
+}
+void launch_correct(Ctx& c, int n, double q, int own) {
+    k_correct<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), c.Rx.p, c.Ry.p, n, q, own);
+    c.check_launch("k_correct");
+}
+void launch_march_slice(Ctx& c, double D, int n) {
+    const int tok = c.prof_begin("march_slice");
+    k_march_slice<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
+                                                                       c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D, n);
+    c.check_launch("k_march_slice");
+    c.prof_end(tok);
+}
+void launch_born_append(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    k_born_append<<<ew_blocks(P.born_cap), 256, 0, c.stream>>>(P.strm, P.born, P.bcnt.p, int(P.born_cap), P.nstrm_dev.p,
+                                                               P.flags.p);
+    c.check_launch("k_born_append");
+    k_count_add<<<1, 1, 0, c.stream>>>(P.nstrm_dev.p, P.bcnt.p, int(P.born_cap));
+    c.check_launch("k_count_add");
+}
+
+}  // namespace g3d

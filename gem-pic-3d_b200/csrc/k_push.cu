@@ -4,7 +4,7 @@
 // and y, linear in zeta between the slices; gather, sim_kernels.hpp:44-72) plus the analytic plane wave.
 // A sub-step is at most dz_push, at most push_phase of the laser phase and moves the particle by at most
 // hmin/2 in zeta. One thread per particle, FP64 arithmetic on the float field data.
-#include "g3d_ctx.hpp"
+#include "g3d_plasma.hpp"
 
 namespace g3d {
 
@@ -129,7 +129,8 @@ void launch_push(Ctx& c, double s0, double s1) {
     a.F = c.F.p; a.g = c.geo(); a.laser = c.laser;
     a.X0 = c.X0; a.Y0 = c.Y0; a.zc = c.P.zeta_center; a.dz_push = c.P.dz_push; a.push_phase = c.P.push_phase;
     a.zhand = -1e300;                                   // one rank: nothing is handed over
-    a.zmax = c.zeta[c.N - 1]; a.ylo = -1e300; a.yhi = 1e300; a.s1 = s1; a.vz_min = 0; a.hmin = c.hmin;
+    a.zmax = c.zeta[c.N - 1]; a.ylo = -1e300; a.yhi = 1e300; a.s1 = s1; a.hmin = c.hmin;
+    a.vz_min = c.pl ? c.pl->cfg.vz_min : 0;            // slower beam particles stream in the plasma march
     a.freeze = c.P.freeze_bunch; a.self = c.P.self_fields;
     const int tok = c.prof_begin("push");
     k_push<<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.parts, c.perm.p, c.np, s0);

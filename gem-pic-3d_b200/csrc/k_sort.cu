@@ -31,20 +31,23 @@ void sort_particles(Ctx& c) {
     const long n = c.np;
     if (n == 0) return;
     if (n > 0x7fffffffL) throw Error(G3D_ERR_CAPACITY, "more than 2^31 particles");
-    if (c.perm.n < size_t(n)) c.perm.alloc(size_t(c.pcap), c.stream);
-    DevBuf<uint32_t> keys;
-    keys.alloc(size_t(2 * n), c.stream);
-    DevBuf<int32_t> idx;
-    idx.alloc(size_t(n), c.stream);
+    // buffers sized for the particle capacity and kept: no allocation (and no implicit synchronisation of
+    // cudaFree) inside a step
+    if (c.perm.n < size_t(c.pcap)) {
+        c.perm.alloc(size_t(c.pcap), c.stream);
+        c.sort_keys.alloc(size_t(2 * c.pcap), c.stream);
+        c.sort_idx.alloc(size_t(c.pcap), c.stream);
+        size_t tb = 0;
+        G3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, c.sort_keys.p, c.sort_keys.p + c.pcap, c.sort_idx.p, c.perm.p,
+                                                 int(c.pcap), 0, 32, c.stream));
+        c.sort_tmp.alloc(tb, c.stream);
+    }
     const long blocks = std::min<long>((n + 255) / 256, 148 * 8);
-    k_cell_keys<<<unsigned(blocks), 256, 0, c.stream>>>(c.parts, n, c.geo(), keys.p, idx.p);
+    k_cell_keys<<<unsigned(blocks), 256, 0, c.stream>>>(c.parts, n, c.geo(), c.sort_keys.p, c.sort_idx.p);
     c.check_launch("k_cell_keys");
-    size_t tmp_bytes = 0;
-    G3D_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys.p, keys.p + n, idx.p, c.perm.p, int(n), 0, 32, c.stream));
-    DevBuf<unsigned char> tmp;
-    tmp.alloc(tmp_bytes, c.stream);
-    G3D_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, keys.p, keys.p + n, idx.p, c.perm.p, int(n), 0, 32, c.stream));
-    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    size_t tmp_bytes = c.sort_tmp.n;
+    G3D_CUDA(cub::DeviceRadixSort::SortPairs(c.sort_tmp.p, tmp_bytes, c.sort_keys.p, c.sort_keys.p + n, c.sort_idx.p, c.perm.p,
+                                             int(n), 0, 32, c.stream));
     c.steps_since_sort = 0;
 }
 

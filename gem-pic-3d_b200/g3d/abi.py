@@ -56,6 +56,28 @@ class Status(C.Structure):
                 ("istep", C.c_int64), ("np", C.c_int64), ("lost", C.c_int64), ("stop", C.c_int64)]
 
 
+class Plasma(C.Structure):
+    _fields_ = [("n0", C.c_double), ("r_max", C.c_double), ("channel_depth", C.c_double), ("r_channel", C.c_double),
+                ("smooth_length", C.c_double), ("vz_min", C.c_double), ("vz_beam", C.c_double),
+                ("trap_advance", C.c_double), ("z_points", C.POINTER(C.c_double)), ("z_values", C.POINTER(C.c_double)),
+                ("n_z", C.c_int32), ("ppc_x", C.c_int32), ("ppc_y", C.c_int32), ("iterations", C.c_int32),
+                ("predictor_extrapolate", C.c_int32), ("free_electrons", C.c_int32), ("parabolic", C.c_int32),
+                ("box_mean", C.c_int32), ("seed", C.c_uint64)]
+
+
+class Ion(C.Structure):
+    _fields_ = [("mass", C.c_double), ("atoms", C.c_double), ("ip_eV", C.POINTER(C.c_double)), ("n_ip", C.c_int32),
+                ("Z0", C.c_int32), ("Zmax", C.c_int32), ("mobile", C.c_int32), ("ionization", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class GridLaser(C.Structure):
+    _fields_ = [("a0", C.c_double), ("kL", C.c_double), ("waist", C.c_double), ("tau", C.c_double),
+                ("zeta_c", C.c_double), ("z_focus", C.c_double), ("cep", C.c_double), ("pol_angle", C.c_double),
+                ("circular", C.c_int32), ("helicity", C.c_int32)]
+
+
+assert C.sizeof(Plasma) == 120 and C.sizeof(Ion) == 48 and C.sizeof(GridLaser) == 72
 assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 120 and C.sizeof(Status) == 80
 
 _P = C.c_void_p
@@ -76,6 +98,10 @@ SIGNATURES = [
     ("g3d_load_bunches", _I, [_P, C.POINTER(Bunch), _I32]),
     ("g3d_sample_bunches", _I, [C.POINTER(Grid), C.POINTER(Params), C.POINTER(Bunch), _I32, _P, _I64,
                                 C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_D), C.POINTER(_D)]),
+    ("g3d_set_plasma", _I, [_P, C.POINTER(Plasma), C.POINTER(Ion), _I32]),
+    ("g3d_add_grid_laser", _I, [_P, C.POINTER(GridLaser)]),
+    ("g3d_march_plasma", _I, [_P, _D, _D]),
+    ("g3d_get_streaming", _I, [_P, _P, _I64, C.POINTER(_I64)]),
     ("g3d_init", _I, [_P]),
     ("g3d_step", _I, [_P]),
     ("g3d_step_async", _I, [_P]),

@@ -45,6 +45,9 @@ class RunConfig:
     params: dict = field(default_factory=dict)
     bunches: list = field(default_factory=list)
     steps: int = 10
+    plasma: dict = None              # streaming plasma (g3d_plasma keys), None: vacuum
+    ions: list = field(default_factory=list)
+    glasers: list = field(default_factory=list)
 
     @property
     def zeta(self):
@@ -73,6 +76,44 @@ class RunConfig:
                 setattr(arr[i], k, v)
         return arr, len(self.bunches)
 
+    def plasma_structs(self):
+        """(Plasma, Ion array, count, keep-alive list) or None without plasma."""
+        if self.plasma is None:
+            return None
+        d = default_plasma()
+        d.update(self.plasma)
+        keep = []
+        zp = np.ascontiguousarray(d.pop("z_points", []), dtype=np.float64)
+        zv = np.ascontiguousarray(d.pop("z_values", []), dtype=np.float64)
+        keep += [zp, zv]
+        P = abi.Plasma()
+        for k, v in d.items():
+            setattr(P, k, v)
+        P.n_z = len(zp)
+        P.z_points = zp.ctypes.data_as(abi.C.POINTER(abi.C.c_double))
+        P.z_values = zv.ctypes.data_as(abi.C.POINTER(abi.C.c_double))
+        arr = (abi.Ion * max(1, len(self.ions)))()
+        for i, ion in enumerate(self.ions):
+            ip = np.ascontiguousarray(ion.get("ip_eV", []), dtype=np.float64)
+            keep.append(ip)
+            for k in ("mass", "atoms", "Z0", "Zmax", "mobile", "ionization"):
+                setattr(arr[i], k, ion[k])
+            arr[i].n_ip = len(ip)
+            arr[i].ip_eV = ip.ctypes.data_as(abi.C.POINTER(abi.C.c_double))
+        return P, arr, len(self.ions), keep
+
+    def glaser_structs(self):
+        out = []
+        for g in self.glasers:
+            d = dict(a0=1.0, kL=1.0, waist=10.0, tau=10.0, zeta_c=0.0, z_focus=0.0, cep=0.0, pol_angle=0.0,
+                     circular=0, helicity=1)
+            d.update(g)
+            L = abi.GridLaser()
+            for k, v in d.items():
+                setattr(L, k, v)
+            out.append(L)
+        return out
+
     @property
     def grid_points(self):
         return self.nx * self.ny * self.nzeta
@@ -90,6 +131,29 @@ def default_params():
                 a0=0.0, kL=1.0, theta=0.0, tau=1.0, cep=0.0, eta_c=0.0, stop_fwhm=0.0,
                 flat_length=0.0, ramp_length=0.0, zeta_center=0.0,
                 freeze_bunch=0, start_relax=1, box_mean=1, precision=abi.G3D_FP64)
+
+
+def default_plasma():
+    """Deck defaults of the plasma and numerics keys (sim_config.cpp:167-208)."""
+    return dict(n0=0.0, r_max=1e300, channel_depth=0.0, r_channel=1.0, smooth_length=0.0, vz_min=0.8, vz_beam=0.9,
+                trap_advance=1.0, ppc_x=2, ppc_y=2, iterations=2, predictor_extrapolate=1, free_electrons=1,
+                parabolic=0, box_mean=1, seed=1)
+
+
+# Elements used by the workloads: standard atomic mass [u] and ionization energies [eV] of every charge state,
+# NIST Atomic Spectra Database (tests/test_oracle.py compares them with the reference build's table).
+ELEMENTS = {
+    "H": (1.008, [13.598434599702]),
+    "N": (14.007, [14.53413, 29.60125, 47.4453, 77.4735, 97.8901, 552.06741, 667.0461377]),
+}
+M_U_KG = 1.66053906660e-27
+
+
+def ion_species(symbol, Z0, atoms, ionization=False, mobile=True, Zmax=None):
+    mass_u, ip = ELEMENTS[symbol]
+    Zmax = (len(ip) if ionization else Z0) if Zmax is None else Zmax
+    return dict(mass=mass_u * M_U_KG / ME_SI, atoms=atoms, Z0=Z0, Zmax=Zmax, mobile=1 if mobile else 0,
+                ionization=1 if ionization else 0, ip_eV=list(ip))
 
 
 def default_bunch():
@@ -135,9 +199,70 @@ def config2(nx=128, ny=128, nzeta=1024, nmacro=1048576, steps=100, envelope=abi.
     return RunConfig("oblique plane wave on a bunch", nx, ny, nzeta, L, L, h, p, [b], steps)
 
 
+def config3(nx=256, ny=256, nzeta=2048, nmacro=4194304, steps=200, charge_pC=10.0):
+    """Laser wakefield with streaming plasma: 256x256 modes, 2048 slices (h = 0.2), n0 = 0.002 n_c with 2x2 electrons
+    per cell and mobile H+ ions, Gaussian grid laser a0 = 2, w0 = 20, tau_FWHM = 30 (1/omega0), focus at s = 0,
+    a witness bunch of 4,194,304 electrons (gamma 200, sigma_perp 1, sigma_zeta 2) 60 behind the laser peak,
+    200 s-steps of 10."""
+    lam = 0.8e-6
+    h = 0.2 * (2047 / (nzeta - 1))
+    dz = 10.0
+    L = 80.0
+    window = h * (nzeta - 1)
+    zl = 0.8 * window                      # laser peak
+    zb = zl - 60.0                         # witness centre
+    b = dict(charge_C=charge_pC * 1e-12, gamma=200.0, sigx=1.0, sigy=1.0, sigz=2.0, emitx=0.0, emity=0.0,
+             espread=0.0, zeta_center=zb, nmacro=nmacro, seed=1)
+    p = dict(lambda0=lam, dz=dz, dz_push=dz, z_end=dz * steps, sponge=0.1 * L, sponge_y=0.1 * L, zeta_center=zb,
+             move_x=0, move_y=0)
+    plasma = dict(n0=0.002, ppc_x=2, ppc_y=2, seed=1)
+    ions = [ion_species("H", 1, 1.0)]
+    gl = [dict(a0=2.0, kL=1.0, waist=20.0, tau=30.0, zeta_c=zl, z_focus=0.0)]
+    return RunConfig("laser wakefield with plasma", nx, ny, nzeta, L, L, h, p, [b], steps, plasma, ions, gl)
+
+
+def lwfa_small(nx=16, ny=16, nzeta=64, nmacro=600, steps=2, ions=True, a0=1.0, n0=0.01, ppc=2, passes=2,
+               extrapolate=1, smooth=0.0):
+    """A small laser wakefield (the structure of workload 3 at test sizes): streaming plasma with mobile H+ ions,
+    a Gaussian grid laser and a witness bunch."""
+    lam = 0.8e-6
+    L = 24.0
+    h = 0.4 * (63 / (nzeta - 1))
+    window = h * (nzeta - 1)
+    zl = 0.7 * window
+    zb = zl - 10.0
+    b = dict(charge_C=0.05e-12, gamma=50.0, sigx=1.0, sigy=1.0, sigz=1.5, emitx=0.05, emity=0.05, espread=0.0,
+             zeta_center=zb, nmacro=nmacro, seed=3)
+    p = dict(lambda0=lam, dz=2.0, dz_push=2.0, z_end=2.0 * steps, sponge=2.4, sponge_y=2.4, zeta_center=zb,
+             move_x=0, move_y=0)
+    plasma = dict(n0=n0, ppc_x=ppc, ppc_y=ppc, iterations=passes, predictor_extrapolate=extrapolate,
+                  smooth_length=smooth, seed=3)
+    ion_list = [ion_species("H", 1, 1.0)] if ions else []
+    gl = [dict(a0=a0, kL=1.0, waist=6.0, tau=6.0, zeta_c=zl, z_focus=2.0)]
+    return RunConfig("small laser wakefield", nx, ny, nzeta, L, L, h, p, [b], steps, plasma, ion_list, gl)
+
+
+def ionization_small(nx=16, ny=16, nzeta=64, steps=2, a0=2.5):
+    """Small ionization injection (the structure of workload 5 on a Fourier grid): neutral gas of atomic H (the
+    H2 of the workload at twice the density) and 1 % N, ADK ionization of every level, a grid laser."""
+    lam = 0.8e-6
+    L = 24.0
+    h = 0.4 * (63 / (nzeta - 1))
+    window = h * (nzeta - 1)
+    zl = 0.7 * window
+    p = dict(lambda0=lam, dz=2.0, dz_push=2.0, z_end=2.0 * steps, sponge=2.4, sponge_y=2.4, zeta_center=0.0,
+             move_x=0, move_y=0)
+    plasma = dict(n0=0.002, ppc_x=1, ppc_y=1, free_electrons=0, seed=7)
+    ion_list = [ion_species("H", 0, 2 * 0.99, ionization=True), ion_species("N", 0, 0.01, ionization=True)]
+    gl = [dict(a0=a0, kL=1.0, waist=6.0, tau=6.0, zeta_c=zl, z_focus=0.0)]
+    return RunConfig("small ionization injection", nx, ny, nzeta, L, L, h, p, [], steps, plasma, ion_list, gl)
+
+
 def baseline(k, **kw):
     if k == 1:
         return config1(**kw)
     if k == 2:
         return config2(**kw)
-    raise NotImplementedError(f"workload {k} needs the plasma march, which this release does not build")
+    if k == 3:
+        return config3(**kw)
+    raise NotImplementedError(f"workload {k} is not built by this release")

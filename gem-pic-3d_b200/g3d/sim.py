@@ -53,6 +53,12 @@ class Simulation:
         if rc != abi.G3D_OK:
             raise G3DError(rc, self.lib.g3d_last_error(None).decode(errors="replace"))
         self.ctx = h
+        ps = cfg.plasma_structs()
+        if ps is not None:
+            P, ions, nions, self._keep = ps
+            self._c(self.lib.g3d_set_plasma(self.ctx, C.byref(P), ions, nions))
+        for L in cfg.glaser_structs():
+            self._c(self.lib.g3d_add_grid_laser(self.ctx, C.byref(L)))
         self.N, self.nx, self.ny = cfg.nzeta, cfg.nx, cfg.ny
         self.nk = cfg.nx * cfg.ny
         self.ns = cfg.nzeta
@@ -116,6 +122,21 @@ class Simulation:
 
     def push(self, s0, s1):
         self._c(self.lib.g3d_push(self.ctx, s0, s1))
+
+    def march_plasma(self, s0, s1):
+        self._c(self.lib.g3d_march_plasma(self.ctx, s0, s1))
+
+    def streaming_particles(self):
+        n = C.c_int64()
+        self._c(self.lib.g3d_get_streaming(self.ctx, None, 0, C.byref(n))) if False else None
+        cap = 1 << 26
+        out = np.zeros(0, dtype=abi.PARTICLE_DTYPE)
+        rc = self.lib.g3d_get_streaming(self.ctx, out.ctypes.data, 0, C.byref(n))
+        if rc not in (abi.G3D_OK, abi.G3D_ERR_CAPACITY):
+            self._c(rc)
+        out = np.zeros(n.value, dtype=abi.PARTICLE_DTYPE)
+        self._c(self.lib.g3d_get_streaming(self.ctx, out.ctypes.data, n.value, C.byref(n)))
+        return out[: n.value]
 
     def comoving_field(self):
         self._c(self.lib.g3d_comoving_field(self.ctx))

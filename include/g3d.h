@@ -98,6 +98,37 @@ typedef struct g3d_bunch {
     uint64_t seed;
 } g3d_bunch;
 
+/* Streaming plasma (reference Config plasma keys, src/sim.hpp:103-116 and 129): a regular lattice of
+ * ppc_x x ppc_y electrons per transverse cell, loaded at the front of the window every s-step, with the ions
+ * of the ion blocks at the same points; n = n0 f(z) g(r) for r < r_max. */
+typedef struct g3d_plasma {
+    double n0;                  /* density [n_c] */
+    double r_max;               /* plasma only where r < r_max (1e300: everywhere) */
+    double channel_depth, r_channel;   /* parabolic: g(r) = 1 + channel_depth r^2 / r_channel^2 */
+    double smooth_length;       /* smoothing 1 / (1 + a^2 k_perp^2) of the streaming current (0: none) */
+    double vz_min, vz_beam, trap_advance;
+    const double* z_points;     /* longitudinal profile f(z): n_z points, linear between, constant beyond */
+    const double* z_values;
+    int32_t n_z, ppc_x, ppc_y, iterations;
+    int32_t predictor_extrapolate, free_electrons, parabolic, box_mean;
+    uint64_t seed;              /* random numbers of the ionization (reference: the first bunch block's seed) */
+} g3d_plasma;
+
+/* An ion species (reference Config::IonSpecies, src/sim.hpp:118-127). */
+typedef struct g3d_ion {
+    double mass;                /* [m_e] */
+    double atoms;               /* n_atom / n_e of the plasma profile */
+    const double* ip_eV;        /* ionization energies [eV]: ip_eV[k] of k -> k+1, n_ip entries */
+    int32_t n_ip, Z0, Zmax, mobile, ionization, reserved;
+} g3d_ion;
+
+/* A Gaussian laser on the grid (reference Config::GridLaser, src/sim.hpp:95-101, type = gaussian):
+ * R = 2 E_perp of a paraxial beam focused at z_focus, added at the start (Simulation::add_grid_lasers). */
+typedef struct g3d_grid_laser {
+    double a0, kL, waist, tau, zeta_c, z_focus, cep, pol_angle;
+    int32_t circular, helicity;
+} g3d_grid_laser;
+
 /* Scalars of the run (reference members s, istep, X0, Y0, beta_b, gm2_b, np, lost_total). */
 typedef struct g3d_status {
     double s, X0, Y0, beta_b, gm2_b, field_energy;
@@ -147,6 +178,11 @@ int g3d_load_bunches(struct g3d_ctx* ctx, const g3d_bunch* bunches, int32_t coun
 int g3d_sample_bunches(const g3d_grid* grid, const g3d_params* params, const g3d_bunch* bunches, int32_t count,
                        g3d_particle* out, int64_t capacity, int64_t* n, int64_t* lost, double* X0, double* Y0);
 
+/* Plasma and ion species (before g3d_init; the ion tables are built here, src/sim_ions.cpp:68-87). */
+int g3d_set_plasma(struct g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions);
+/* A grid laser, added to R by g3d_init (Simulation::add_grid_lasers, src/sim_fields.cpp:321-374). */
+int g3d_add_grid_laser(struct g3d_ctx* ctx, const g3d_grid_laser* laser);
+
 /* ------------------------------------------------------------------ the march path */
 int g3d_init(struct g3d_ctx* ctx);                  /* Simulation::init, sim_setup.cpp:178-197 (after loading) */
 int g3d_step(struct g3d_ctx* ctx);                  /* Simulation::step, sim_setup.cpp:199-217 */
@@ -159,6 +195,11 @@ int g3d_push(struct g3d_ctx* ctx, double s0, double s1);   /* Simulation::push, 
 int g3d_comoving_field(struct g3d_ctx* ctx);        /* Simulation::comoving_field, sim_fields.cpp:44-151 */
 int g3d_relax_start_field(struct g3d_ctx* ctx);     /* sim_fields.cpp:384-410 */
 int g3d_shift_window(struct g3d_ctx* ctx, int32_t nxs, int32_t nys);  /* sim_setup.cpp:249-281 */
+/* The march of a step with streaming plasma (Simulation::march_plasma, src/sim_plasma.cpp:228-470), after
+ * g3d_currents of level s1; g3d_step calls it when a plasma is set. */
+int g3d_march_plasma(struct g3d_ctx* ctx, double s0, double s1);
+/* Streaming particles of the last march (the reference's `strm`, 104-byte records). */
+int g3d_get_streaming(struct g3d_ctx* ctx, g3d_particle* out, int64_t capacity, int64_t* n);
 
 /* ------------------------------------------------------------------ diagnostics */
 /* The 19 weighted sums of Simulation::diagnostics (src/sim_output.cpp:10-26) before the

@@ -21,6 +21,11 @@ _SIGS = [
     ("ref_last_error", C.c_char_p, []),
     ("ref_set_threads", _I, [_I]),
     ("ref_create", _I, [C.POINTER(abi.Grid), C.POINTER(abi.Params), C.POINTER(abi.Bunch), _I, C.POINTER(_P)]),
+    ("ref_create2", _I, [C.POINTER(abi.Grid), C.POINTER(abi.Params), C.POINTER(abi.Bunch), _I, C.POINTER(abi.Plasma),
+                         C.POINTER(abi.Ion), _I, C.POINTER(abi.GridLaser), _I, C.POINTER(_P)]),
+    ("ref_get_streaming", _I, [_P, _P, _L, C.POINTER(_L)]),
+    ("ref_march_plasma", _I, [_P, _D, _D]),
+    ("ref_element", _I, [C.c_char_p, C.POINTER(_D), C.POINTER(_D), _I]),
     ("ref_destroy", None, [_P]),
     ("ref_load_bunches", _I, [_P]),
     ("ref_init", _I, [_P]),
@@ -52,6 +57,17 @@ _SIGS = [
 _lib = None
 
 
+def element(symbol):
+    """(mass [u], ionization energies [eV]) of an element in the reference's table."""
+    lib = load()
+    m = C.c_double()
+    ip = (C.c_double * 120)()
+    z = lib.ref_element(symbol.encode(), C.byref(m), ip, 120)
+    if z < 0:
+        raise KeyError(symbol)
+    return m.value, list(ip[:z])
+
+
 def available():
     return os.path.exists(REF_LIB)
 
@@ -80,7 +96,18 @@ class RefSimulation:
         p = cfg.params_struct()
         b, nb = cfg.bunch_structs()
         h = C.c_void_p()
-        self._c(self.lib.ref_create(C.byref(g), C.byref(p), b, nb, C.byref(h)))
+        ps = cfg.plasma_structs()
+        gls = cfg.glaser_structs()
+        if ps is None and not gls:
+            self._c(self.lib.ref_create(C.byref(g), C.byref(p), b, nb, C.byref(h)))
+        else:
+            garr = (abi.GridLaser * max(1, len(gls)))(*gls) if gls else (abi.GridLaser * 1)()
+            if ps is None:
+                self._c(self.lib.ref_create2(C.byref(g), C.byref(p), b, nb, None, None, 0, garr, len(gls), C.byref(h)))
+            else:
+                P, ions, nions, self._keep = ps
+                self._c(self.lib.ref_create2(C.byref(g), C.byref(p), b, nb, C.byref(P), ions, nions, garr, len(gls),
+                                             C.byref(h)))
         self.h = h
 
     def _c(self, rc):
@@ -133,6 +160,16 @@ class RefSimulation:
 
     def shift_window(self, nxs, nys):
         self._c(self.lib.ref_shift_window(self.h, nxs, nys))
+
+    def march_plasma(self, s0, s1):
+        self._c(self.lib.ref_march_plasma(self.h, s0, s1))
+
+    def streaming_particles(self):
+        n = C.c_long()
+        cap = 1 << 24
+        out = np.zeros(cap, dtype=abi.PARTICLE_DTYPE)
+        self._c(self.lib.ref_get_streaming(self.h, out.ctypes.data, cap, C.byref(n)))
+        return out[: n.value].copy()
 
     def set_starting(self, v):
         self._c(self.lib.ref_set_starting(self.h, 1 if v else 0))

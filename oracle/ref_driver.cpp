@@ -19,6 +19,7 @@
 #include <omp.h>
 #endif
 #include "sim.hpp"
+#include "atomic_data.hpp"
 #include "g3d.h"
 
 static_assert(sizeof(Particle) == sizeof(g3d_particle), "particle record must be the reference's 104 bytes");
@@ -102,6 +103,86 @@ int ref_create(const g3d_grid* g, const g3d_params* p, const g3d_bunch* bunches,
 }
 
 void ref_destroy(void* h) { delete static_cast<RefCtx*>(h); }
+
+// The same with a plasma, ion species and grid lasers (Config fields of src/sim.hpp:95-131).
+int ref_create2(const g3d_grid* g, const g3d_params* p, const g3d_bunch* bunches, int nb, const g3d_plasma* pl,
+                const g3d_ion* ions, int nions, const g3d_grid_laser* gl, int ngl, void** out) {
+    try {
+        void* h = nullptr;
+        // build the config as ref_create does, then add the plasma before constructing the Simulation
+        Config c = make_config(g, p);
+        c.bunches.clear();
+        for (int k = 0; k < nb; ++k) {
+            const g3d_bunch& b = bunches[k];
+            Config::Bunch u;
+            u.name = k == 0 ? "bunch" : "bunch" + std::to_string(k + 1);
+            u.q = b.q; u.charge = b.charge_C; u.gamma = b.gamma; u.sigx = b.sigx; u.sigy = b.sigy; u.sigz = b.sigz;
+            u.length = b.length; u.emitx = b.emitx; u.emity = b.emity; u.espread = b.espread;
+            u.zeta_center = b.zeta_center; u.x0 = b.x0; u.y0 = b.y0; u.nmacro = long(b.nmacro); u.seed = (unsigned long)b.seed;
+            c.bunches.push_back(u);
+        }
+        if (nb > 0) {
+            const Config::Bunch& f = c.bunches[0];
+            c.charge = f.charge; c.gamma = f.gamma; c.sigx = f.sigx; c.sigy = f.sigy; c.sigz = f.sigz; c.nmacro = f.nmacro;
+        }
+        if (pl) {
+            c.plasma_on = true;
+            c.n0 = pl->n0; c.r_max = pl->r_max; c.channel_depth = pl->channel_depth; c.r_channel = pl->r_channel;
+            c.parabolic = pl->parabolic != 0; c.smooth_length = pl->smooth_length;
+            c.pz_points.assign(pl->z_points, pl->z_points + pl->n_z);
+            c.pz_values.assign(pl->z_values, pl->z_values + pl->n_z);
+            c.ppc_x = pl->ppc_x; c.ppc_y = pl->ppc_y; c.iterations = pl->iterations;
+            c.vz_min = pl->vz_min; c.vz_beam = pl->vz_beam; c.trap_advance = pl->trap_advance;
+            c.predictor_extrapolate = pl->predictor_extrapolate != 0; c.free_electrons = pl->free_electrons != 0;
+            c.box_mean = pl->box_mean != 0;
+            c.seed = (unsigned long)pl->seed;
+        }
+        for (int k = 0; k < nions; ++k) {
+            const g3d_ion& I = ions[k];
+            Config::IonSpecies s;
+            s.name = "ion" + std::to_string(k + 1);
+            s.mass = I.mass; s.atoms = I.atoms; s.Z0 = I.Z0; s.Zmax = I.Zmax; s.mobile = I.mobile != 0;
+            s.ionization = I.ionization != 0;
+            s.ip_eV.assign(I.ip_eV, I.ip_eV + I.n_ip);
+            c.ions.push_back(s);
+        }
+        for (int k = 0; k < ngl; ++k) {
+            Config::GridLaser L;
+            L.a0 = gl[k].a0; L.kL = gl[k].kL; L.waist = gl[k].waist; L.tau = gl[k].tau; L.zeta_c = gl[k].zeta_c;
+            L.z_focus = gl[k].z_focus; L.cep = gl[k].cep; L.pol_angle = gl[k].pol_angle;
+            L.circular = gl[k].circular != 0; L.helicity = gl[k].helicity;
+            c.glasers.push_back(L);
+        }
+        auto* r = new RefCtx();
+        r->cfg = c;
+        r->sim.reset(new Simulation(r->cfg, g_comm));
+        h = r;
+        *out = h;
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// Streaming particles of the last plasma march (the reference's `strm`, nstrm records).
+int ref_get_streaming(void* h, g3d_particle* out, long cap, long* n) {
+    try {
+        Simulation& s = *static_cast<RefCtx*>(h)->sim;
+        *n = s.nstrm;
+        if (s.nstrm > cap) throw std::runtime_error("capacity");
+        if (s.nstrm) s.strm.to_host(reinterpret_cast<Particle*>(out), 0, size_t(s.nstrm));
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+int ref_march_plasma(void* h, double s0, double s1) {
+    try { static_cast<RefCtx*>(h)->sim->march_plasma(s0, s1); return 0; } catch (const std::exception& e) { return fail(e); }
+}
+// Element data of the reference's table (mass [u], ionization energies [eV]); returns Znuc or -1.
+int ref_element(const char* sym, double* mass_u, double* ip, int cap) {
+    const gem::Element* e = gem::findElement(sym);
+    if (!e) return -1;
+    *mass_u = e->mass_u;
+    for (int k = 0; k < e->Znuc && k < cap; ++k) ip[k] = e->ip_eV[size_t(k)];
+    return e->Znuc;
+}
 
 #define SIM (static_cast<RefCtx*>(h)->sim)
 #define TRY(body) try { body; return 0; } catch (const std::exception& e) { return fail(e); }

@@ -112,3 +112,12 @@ def test_flattop_envelope_is_the_derivative_of_the_potential():
         h = 1e-5
         fd = -(A(eta + h) - A(eta - h)) / (2 * h)
         assert abs(E[1][0] - fd) <= 1e-8 * max(1.0, abs(fd)), eta
+
+
+@needs_ref
+def test_element_table_matches_the_reference():
+    """The elements the workloads use carry the reference table's mass and ionization energies."""
+    for sym, (mass_u, ip) in configs.ELEMENTS.items():
+        rm, rip = ref.element(sym)
+        assert mass_u == rm, sym
+        assert ip == rip, sym

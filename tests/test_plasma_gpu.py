@@ -1,0 +1,89 @@
+"""Parity of the streaming-plasma march (libg3d.so) with the reference FP64 CPU path, small cases against the live
+reference build: init with a grid laser, then s-steps with streaming plasma (mobile ions, passes, the extrapolating
+predictor and the correction, trapping), and ADK ionization of a neutral gas.
+
+Tolerances as in test_parity_gpu.py: fields <= 1e-10 relative L2 against the field state norm (a laser-driven
+plasma is chaotic only over many steps; two steps stay at rounding level), streaming particles <= 1e-9 relative L2.
+The ionization event set must be identical: the same ions reach the same charge states, and the freed electrons
+are the same (matched by id; the order in which the GPU appends them differs).
+"""
+import numpy as np
+import pytest
+
+from conftest import CURRENTS, FIELDS, assert_state, rel_l2
+
+pytestmark = pytest.mark.gpu
+ref = pytest.importorskip("ref")
+needs_ref = pytest.mark.skipif(not ref.available(), reason="reference build oracle/_ref not present")
+
+
+def run_pair(cfg, steps):
+    from g3d import Simulation
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    return s, r
+
+
+def compare_fields(s, r, tol=1e-10, tag=""):
+    assert_state({a: s.array(a) for a in FIELDS}, {a: r.array(a) for a in FIELDS}, FIELDS, tol, comp_tol=1e-5, tag=tag)
+    assert_state({a: s.array(a) for a in CURRENTS}, {a: r.array(a) for a in CURRENTS}, CURRENTS, tol, comp_tol=1e-5, tag=tag)
+    assert rel_l2(s.array("F"), r.array("F")) <= 1e-6, tag
+
+
+def sort_by_id(p):
+    # electrons freed from one ion share its id: order them by where they are
+    return p[np.lexsort((np.round(p["x"], 6), np.round(p["zeta"], 6), p["sp"], p["id"]))]
+
+
+@needs_ref
+@pytest.mark.parametrize("ions,extrap,passes", [(True, 1, 2), (False, 0, 1), (True, 1, 3)])
+def test_lwfa_small_matches_reference(ions, extrap, passes):
+    from g3d import configs
+    cfg = configs.lwfa_small(ions=ions, extrapolate=extrap, passes=passes)
+    s, r = run_pair(cfg, 2)
+    compare_fields(s, r, tag="init")
+    for k in range(2):
+        s.step(); r.step()
+        compare_fields(s, r, tag=f"step{k + 1}")
+        ps, pr = s.streaming_particles(), r.streaming_particles()
+        assert len(ps) == len(pr)
+        assert np.array_equal(ps["alive"], pr["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+            assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f, rel_l2(ps[f], pr[f]))
+        bs, br = s.host_particles(), r.host_particles()
+        assert len(bs) == len(br)
+        for f in ["x", "y", "zeta", "px", "py", "pz"]:
+            assert rel_l2(bs[f], br[f]) <= 1e-10, (k, f)
+
+
+@needs_ref
+def test_smoothing_and_trapping_small():
+    """The smoothing 1/(1 + a^2 k^2) of the streaming current, and a driver strong enough to trap electrons."""
+    from g3d import configs
+    cfg = configs.lwfa_small(a0=3.0, n0=0.02, smooth=0.4)
+    s, r = run_pair(cfg, 2)
+    for k in range(2):
+        s.step(); r.step()
+        compare_fields(s, r, tol=1e-9, tag=f"step{k + 1}")
+    assert s.status().np == r.status().np
+
+
+@needs_ref
+def test_ionization_event_set_is_identical():
+    from g3d import configs
+    cfg = configs.ionization_small()
+    s, r = run_pair(cfg, 2)
+    for k in range(2):
+        s.step(); r.step()
+        ps, pr = sort_by_id(s.streaming_particles()), sort_by_id(r.streaming_particles())
+        assert len(ps) == len(pr), (len(ps), len(pr))
+        # the same particles (ions and the electrons they freed), the same charge states
+        assert np.array_equal(ps["id"], pr["id"]) and np.array_equal(ps["sp"], pr["sp"])
+        assert np.array_equal(ps["q"], pr["q"])
+        assert np.array_equal(ps["alive"], pr["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz"]:
+            assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f)
+    freed = ps[(ps["sp"] >= 50) & (ps["sp"] < 100)]
+    assert len(freed) > 0, "the case must ionize"
