@@ -48,6 +48,31 @@ G3D_HD cpx ik(double k, cpx z) { return make_double2(-k * z.y, k * z.x); }
 G3D_HD cpx mul_i(cpx z) { return make_double2(-z.y, z.x); }          // i z
 G3D_HD cpx mul_mi(cpx z) { return make_double2(z.y, -z.x); }         // -i z
 
+// cpxf is the FP32 complex of the mixed form (float2), with the same operators.
+typedef float2 cpxf;
+G3D_HD cpxf Cf(float r, float i = 0.0f) { return make_float2(r, i); }
+G3D_HD cpxf operator+(cpxf a, cpxf b) { return make_float2(a.x + b.x, a.y + b.y); }
+G3D_HD cpxf operator-(cpxf a, cpxf b) { return make_float2(a.x - b.x, a.y - b.y); }
+G3D_HD cpxf operator-(cpxf a) { return make_float2(-a.x, -a.y); }
+G3D_HD cpxf operator*(cpxf a, cpxf b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+G3D_HD cpxf operator*(float s, cpxf a) { return make_float2(s * a.x, s * a.y); }
+G3D_HD cpxf operator*(cpxf a, float s) { return make_float2(s * a.x, s * a.y); }
+G3D_HD cpxf operator/(cpxf a, float s) { return make_float2(a.x / s, a.y / s); }
+G3D_HD cpxf conj(cpxf a) { return make_float2(a.x, -a.y); }
+G3D_HD cpxf ik(float k, cpxf z) { return make_float2(-k * z.y, k * z.x); }
+G3D_HD cpxf mul_i(cpxf z) { return make_float2(-z.y, z.x); }
+G3D_HD cpxf mul_mi(cpxf z) { return make_float2(z.y, -z.x); }
+G3D_HD cpx to_d(cpxf a) { return make_double2(a.x, a.y); }
+G3D_HD cpxf to_f(cpx a) { return make_float2(float(a.x), float(a.y)); }
+
+// Real type of a complex type.
+template <class T> struct RealOf;
+template <> struct RealOf<double2> { typedef double type; };
+template <> struct RealOf<float2> { typedef float type; };
+template <class T> G3D_HD T mk(typename RealOf<T>::type r, typename RealOf<T>::type i);
+template <> G3D_HD double2 mk<double2>(double r, double i) { return make_double2(r, i); }
+template <> G3D_HD float2 mk<float2>(float r, float i) { return make_float2(r, i); }
+
 // ---------------------------------------------------------------- axes
 // Location of a coordinate on a grid of nodes (uniform: direct; else binary search), with the end
 // cells continued beyond the ends. Same contract as the reference's Axis::locate (src/grid.hpp:325-341).

@@ -30,31 +30,36 @@ struct FftShape {
 };
 
 // ---------------------------------------------------------------- small DFTs (forward, sign -1)
-__device__ __forceinline__ void dft2(cpx* v) {
-    const cpx a = v[0], b = v[1];
+// Generic over the complex type T (double2: the FP64 form; float2: the FP32 transforms of the mixed form).
+template <class T>
+__device__ __forceinline__ void dft2(T* v) {
+    const T a = v[0], b = v[1];
     v[0] = a + b; v[1] = a - b;
 }
-__device__ __forceinline__ void dft4(cpx* v) {
-    const cpx s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = mul_mi(v[1] - v[3]);
+template <class T>
+__device__ __forceinline__ void dft4(T* v) {
+    const T s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = mul_mi(v[1] - v[3]);
     v[0] = s02 + s13; v[1] = d02 + d13; v[2] = s02 - s13; v[3] = d02 - d13;
 }
-__device__ __forceinline__ void dft8(cpx* v) {
+template <class T>
+__device__ __forceinline__ void dft8(T* v) {
     // even / odd split into two DFT4, combined with the eighth roots of unity
-    const double r = 0.70710678118654752440;
-    const cpx a0 = v[0] + v[4], a1 = v[0] - v[4], a2 = v[2] + v[6], a3 = mul_mi(v[2] - v[6]);
-    const cpx a4 = v[1] + v[5], a5 = v[1] - v[5], a6 = v[3] + v[7], a7 = mul_mi(v[3] - v[7]);
-    const cpx b0 = a0 + a2, b2 = a0 - a2, b1 = a1 + a3, b3 = a1 - a3;
-    const cpx c0 = a4 + a6, c2 = a4 - a6, c1 = a5 + a7, c3 = a5 - a7;
-    const cpx w1 = C(r * (c1.x + c1.y), r * (c1.y - c1.x));          // exp(-i pi/4) c1
-    const cpx w2 = mul_mi(c2);                                        // -i c2
-    const cpx w3 = C(r * (c3.y - c3.x), -r * (c3.x + c3.y));         // exp(-3i pi/4) c3
+    typedef typename RealOf<T>::type Re;
+    const Re r = Re(0.70710678118654752440);
+    const T a0 = v[0] + v[4], a1 = v[0] - v[4], a2 = v[2] + v[6], a3 = mul_mi(v[2] - v[6]);
+    const T a4 = v[1] + v[5], a5 = v[1] - v[5], a6 = v[3] + v[7], a7 = mul_mi(v[3] - v[7]);
+    const T b0 = a0 + a2, b2 = a0 - a2, b1 = a1 + a3, b3 = a1 - a3;
+    const T c0 = a4 + a6, c2 = a4 - a6, c1 = a5 + a7, c3 = a5 - a7;
+    const T w1 = mk<T>(r * (c1.x + c1.y), r * (c1.y - c1.x));        // exp(-i pi/4) c1
+    const T w2 = mul_mi(c2);                                          // -i c2
+    const T w3 = mk<T>(r * (c3.y - c3.x), -r * (c3.x + c3.y));       // exp(-3i pi/4) c3
     v[0] = b0 + c0; v[4] = b0 - c0;
     v[1] = b1 + w1; v[5] = b1 - w1;
     v[2] = b2 + w2; v[6] = b2 - w2;
     v[3] = b3 + w3; v[7] = b3 - w3;
 }
-template <int R>
-__device__ __forceinline__ void dft(cpx* v) {
+template <int R, class T>
+__device__ __forceinline__ void dft(T* v) {
     if constexpr (R == 2) dft2(v);
     else if constexpr (R == 4) dft4(v);
     else dft8(v);
@@ -62,14 +67,14 @@ __device__ __forceinline__ void dft(cpx* v) {
 
 // One Stockham pass of radix R over a line. `A(p)` maps the position p of the line to its shared
 // memory index; `t` is the thread's index among the T threads of the line; tw[s] = exp(-2 pi i s / N).
-template <int N, int R, class Addr>
-__device__ __forceinline__ void fft_pass(cpx* sm, const Addr& A, int t, int L, const cpx* __restrict__ tw) {
-    constexpr int E = FftShape<N>::E, T = FftShape<N>::T, BPT = E / R;
+template <int N, int R, class Addr, class T>
+__device__ __forceinline__ void fft_pass(T* sm, const Addr& A, int t, int L, const T* __restrict__ tw) {
+    constexpr int E = FftShape<N>::E, TT = FftShape<N>::T, BPT = E / R;
     const int m = N / (L * R);
-    cpx v[E];
+    T v[E];
 #pragma unroll
     for (int u = 0; u < BPT; ++u) {
-        const int b = t + u * T, j = b / L, k = b - j * L;
+        const int b = t + u * TT, j = b / L, k = b - j * L;
 #pragma unroll
         for (int q = 0; q < R; ++q) v[u * R + q] = sm[A((q * m + j) * L + k)];
         if (L > 1) {
@@ -81,7 +86,7 @@ __device__ __forceinline__ void fft_pass(cpx* sm, const Addr& A, int t, int L, c
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < BPT; ++u) {
-        const int b = t + u * T, j = b / L, k = b - j * L;
+        const int b = t + u * TT, j = b / L, k = b - j * L;
 #pragma unroll
         for (int r = 0; r < R; ++r) sm[A((j * R + r) * L + k)] = v[u * R + r];
     }
@@ -90,8 +95,8 @@ __device__ __forceinline__ void fft_pass(cpx* sm, const Addr& A, int t, int L, c
 
 // The whole forward transform of one line in shared memory (every thread of the CTA must call it
 // the same number of times: the passes synchronise the CTA).
-template <int N, class Addr>
-__device__ __forceinline__ void fft_line(cpx* sm, const Addr& A, int t, const cpx* __restrict__ tw) {
+template <int N, class Addr, class T>
+__device__ __forceinline__ void fft_line(T* sm, const Addr& A, int t, const T* __restrict__ tw) {
     using S = FftShape<N>;
     int L = 1;
     if constexpr (S::REM > 1) { fft_pass<N, S::REM>(sm, A, t, L, tw); L *= S::REM; }
