@@ -37,12 +37,19 @@ def parse():
     ap.add_argument("--workload", type=int, default=2, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
+    ap.add_argument("--particles", type=int, default=None, help="profiling case: fewer macro-particles")
     return ap.parse_args()
 
 
-def workload(k):
+def workload(k, nzeta=None, particles=None):
     from g3d import configs
-    return configs.baseline(k)
+    kw = {}
+    if nzeta:
+        kw["nzeta"] = nzeta
+    if particles:
+        kw["nmacro"] = particles
+    return configs.baseline(k, **kw)
 
 
 def config_json(cfg, k):
@@ -51,25 +58,45 @@ def config_json(cfg, k):
             "nx": cfg.nx, "ny": cfg.ny, "nzeta": cfg.nzeta, "particles": cfg.particles,
             "grid_points": cfg.grid_points, "dz": cfg.params["dz"], "sponge": cfg.params.get("sponge", 0),
             "laser_envelope": "flattop" if cfg.params.get("laser_envelope") == 1 else "gaussian",
-            "l2": "inputs larger than L2 (field state 4.6 GB, F 0.4 GB)", "parallelism": "replicas"}
+            "l2": f"inputs larger than L2 (field state {state_bytes(cfg) / 1e9:.2f} GB, F {f_bytes(cfg) / 1e9:.2f} GB)",
+            "parallelism": "replicas"}
+
+
+def state_bytes(cfg):
+    """Device bytes of the spectral state: six fields and five current planes, half spectra of complex128."""
+    gh = (cfg.nzeta - 1) * cfg.ny * (cfg.nx // 2 + 1)
+    return 11 * 16 * gh
+
+
+def f_bytes(cfg):
+    return 6 * (cfg.nzeta + 1) * cfg.nx * cfg.ny * 4
 
 
 # ------------------------------------------------------------------ algorithmic bytes per launch (FP64)
 def algorithmic_bytes(name, cfg):
-    """Per-launch algorithmic bytes of each kernel: the per-unit figures (bytes per grid point G and per
-    beam particle P per s-step) of the reference's march, split over the kernels that do each part."""
-    G, P, nk, N = cfg.grid_points, cfg.particles, cfg.nx * cfg.ny, cfg.nzeta
+    """Per-launch algorithmic bytes of each kernel: what it must read and write once, in the layout this build keeps.
+
+    G = grid points (slices x nx x ny, each carries 6 floats of F = 24 B and 3 raw current doubles = 24 B);
+    Gh = half-spectrum points of a slice set (slices x ny x (nx/2 + 1)); a complex128 plane costs 16 B per Gh.
+    The spectra of real fields are Hermitian, so the kept half is the minimum a transform pass has to move.
+    P = beam particles: push reads x, y, zeta, px, py, pz, z, w (64 B) and writes 48 B; deposit reads 56 B."""
+    ns = cfg.nzeta - 1
+    nk = cfg.nx * cfg.ny
+    G = ns * nk
+    Gh = ns * cfg.ny * (cfg.nx // 2 + 1)
+    Gc = (ns + 1) * cfg.ny * (cfg.nx // 2 + 1)      # current planes carry one more half-cell
+    P = cfg.particles
     table = {
-        "push": 112 * P + 24 * G,          # particle read 64 + write 48; F read 24 per grid point
-        "deposit": 56 * P + 24 * G,        # particle read 56; raw current write 24 per grid point
-        "cur_cols": 24 * G + 32 * G,       # raw currents read 24; two complex planes written 32
-        "cur_rows": 32 * G + 48 * G,       # two complex planes read 32; jkx, jky, jkz written 48
-        "march": 272 * G,                  # state read 96 + j0 32 + jk 48, state write 96
-        "real_cols": 96 * G + 48 * G,      # state read 96; three complex planes written 48
-        "real_rows": 48 * G + 24 * G,      # three complex planes read 48; F written 24
-        "sponge_rows": 32 * G + 16 * G + 32 * G,   # R read 32, j_z read 16; packed R - R_b and psi written 32
-        "sponge_cols": 32 * G,             # one complex plane read and written
-        "sponge_rowpairs": 32 * G + 32 * G,        # packed plane and psi read 32; R written 32
+        "push": 112 * P + 24 * G,          # particles read 64 + written 48; F read 24 per grid point
+        "deposit": 56 * P + 24 * G,        # particles read 56; raw currents written 24 per grid point
+        "cur_rows": 24 * G + 48 * Gc,      # raw currents read 24; three complex planes written
+        "cur_cols": 48 * Gc + 48 * Gc,     # three complex planes read and written (jkx, jky, jkz)
+        "march": (9 + 6) * 16 * Gh,        # R, E_z, B_z, j0 (2), jk (3) read; R, E_z, B_z, L written
+        "sponge_cols_inv": (2 + 1 + 3) * 16 * Gh,   # R read, j_z read; U, V, psi written
+        "sponge_rows": 4 * 16 * Gh,        # U, V read and written
+        "sponge_cols_fwd": (3 + 2) * 16 * Gh,       # U, V, psi read; R written
+        "real_cols": 12 * 16 * Gh,         # six spectra read, six column transforms written
+        "real_rows": 6 * 16 * Gh + 24 * G,  # six column transforms read; F written
     }
     return table.get(name)
 
@@ -183,7 +210,7 @@ def run_reference_arm(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    cfg = workload(a.workload)
+    cfg = workload(a.workload, a.nzeta, a.particles)
     cores = host_cores()
     steps = max(1, min(a.steps, 5))
     v, why = reference_rate(cfg, steps, cores)
@@ -216,7 +243,7 @@ def run_g3d(a):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg = workload(a.workload)
+    cfg = workload(a.workload, a.nzeta, a.particles)
     sim = g3d.Simulation(cfg)
     sim.init()
     P = int(sim.status().np)
