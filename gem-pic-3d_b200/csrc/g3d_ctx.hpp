@@ -184,6 +184,7 @@ void launch_zero_c(Ctx& c, cpx* p, size_t n);
 void launch_axpy_c(Ctx& c, cpx* y, const cpx* x, double a, size_t n);   // y = y + a x
 void launch_copy_c(Ctx& c, cpx* y, const cpx* x, size_t n);
 void launch_beta_sums(Ctx& c, double out[2]);
+void launch_beta_sums_static(Ctx& c, double out[2]);
 void launch_centroid(Ctx& c, double out[3]);
 void launch_diag(Ctx& c, double S[19]);
 double launch_field_energy(Ctx& c);

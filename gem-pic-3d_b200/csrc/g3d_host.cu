@@ -685,6 +685,12 @@ int g3d_push(g3d_ctx* ctx, double s0, double s1) {
 int g3d_comoving_field(g3d_ctx* ctx) {
     return guarded(ctx, [&] { g3d::comoving_field(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
 }
+int g3d_beam_beta_sums_static(g3d_ctx* ctx, double out[2]) {
+    return guarded(ctx, [&] {
+        if (!out) throw Error(G3D_ERR_ARG, "null output");
+        g3d::launch_beta_sums_static(ctx->c, out);
+    });
+}
 int g3d_relax_start_field(g3d_ctx* ctx) {
     return guarded(ctx, [&] {
         g3d::materialize_jk(ctx->c);

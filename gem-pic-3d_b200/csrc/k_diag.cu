@@ -171,4 +171,32 @@ void launch_beta_sums(Ctx& c, double out[2]) {
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 
+// ------------------------------------------------ the same beta sums with file-scope scratch (no allocation)
+// Scratch of g3d_beam_beta_sums_static: the per-particle terms t[0..np), w[0..np) and the two sums at [2 np],
+// [2 np + 1], for at most G3D_BETA_STATIC_MAX particles (16 MiB + 16 B). It is a static device symbol of this
+// library: one copy per device, shared by every context on that device, so two calls in flight at once on one
+// device (two streams, threads or contexts) race on it. Nothing in it has to start at zero: every term below np
+// is written before the sequential sum reads it, and the two sums are stored, not accumulated.
+static __device__ __align__(256) double g_beta_scratch[2 * G3D_BETA_STATIC_MAX + 2];
+
+void launch_beta_sums_static(Ctx& c, double out[2]) {
+    if (c.np > G3D_BETA_STATIC_MAX)
+        throw Error(G3D_ERR_CAPACITY, "g3d_beam_beta_sums_static: " + std::to_string(c.np) +
+                                          " particles exceed the static scratch of G3D_BETA_STATIC_MAX = " +
+                                          std::to_string(G3D_BETA_STATIC_MAX) + "; use g3d_comoving_field");
+    out[0] = out[1] = 0;
+    if (c.np == 0) return;
+    void* sym = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&sym, g_beta_scratch);      // per device: the current one
+    if (rc != cudaSuccess)
+        throw Error(G3D_ERR_CUDA, std::string("cudaGetSymbolAddress(g_beta_scratch): ") + cudaGetErrorString(rc));
+    double* tw = static_cast<double*>(sym);
+    k_beta_terms<<<RB, RT, 0, c.stream>>>(c.parts, c.np, tw, tw + c.np);
+    c.check_launch("k_beta_terms");
+    k_seq_sum2<<<1, 32, 0, c.stream>>>(tw, tw + c.np, c.np, c.parts.alive, tw + 2 * c.np);
+    c.check_launch("k_seq_sum2");
+    G3D_CUDA(cudaMemcpyAsync(out, tw + 2 * c.np, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+
 }  // namespace g3d

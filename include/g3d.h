@@ -194,6 +194,19 @@ int g3d_sponge_and_real_fields(struct g3d_ctx* ctx);/* sim_fields.cpp:156-307 */
 int g3d_push(struct g3d_ctx* ctx, double s0, double s1);   /* Simulation::push, sim_particles.cpp:6-24 */
 int g3d_comoving_field(struct g3d_ctx* ctx);        /* Simulation::comoving_field, sim_fields.cpp:44-151 */
 int g3d_relax_start_field(struct g3d_ctx* ctx);     /* sim_fields.cpp:384-410 */
+
+/* Largest particle count g3d_beam_beta_sums_static accepts (its scratch: 2 doubles per particle, 16 MiB). */
+#define G3D_BETA_STATIC_MAX 1048576
+/* No counterpart in the reference: an added entry point that allocates no device memory. out[0] = sum of w v_z,
+ * out[1] = sum of w over the alive particles, in index order: the sums g3d_comoving_field takes the bunch's beta
+ * from (beta = out[0] / out[1]; reference sim_fields.cpp:45-51), bit for bit. Its scratch is a static device
+ * array of the library instead of a per-call buffer (g3d_comoving_field allocates 16 bytes per particle per call),
+ * for callers that must not allocate: a window state that fills the device, or an allocator the caller owns. More than
+ * G3D_BETA_STATIC_MAX particles: G3D_ERR_CAPACITY, nothing launched. The scratch is shared by every context of
+ * the process on one device, so calls on one device must not overlap in time (they would race on it). The first
+ * call on a device may load the library's device code (the address lookup of the scratch), so make it once
+ * before any stream capture. Synchronous: returns after the sums have reached `out`. */
+int g3d_beam_beta_sums_static(struct g3d_ctx* ctx, double out[2]);
 int g3d_shift_window(struct g3d_ctx* ctx, int32_t nxs, int32_t nys);  /* sim_setup.cpp:249-281 */
 /* The march of a step with streaming plasma (Simulation::march_plasma, src/sim_plasma.cpp:228-470), after
  * g3d_currents of level s1; g3d_step calls it when a plasma is set. */
