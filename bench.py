@@ -307,7 +307,7 @@ def run_g3d(a):
         host = torch.empty(P * g3d.PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
         parts = host.numpy().view(g3d.PARTICLE_DTYPE)
         parts[:] = sim.host_particles()
-        out = torch.empty_like(host)
+        out = torch.empty(P * g3d.PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
         outp = out.numpy().view(g3d.PARTICLE_DTYPE)
         lib, ctx = sim.lib, sim.ctx
         diag = (__import__("ctypes").c_double * 19)()
