@@ -24,7 +24,7 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "gem-pic-3d_b200"))
 
-METRIC = "particle-pushes/s incl. field solve (FP64 plain form)"
+METRIC = "particle-pushes/s incl. field solve, mixed vs FP64 form, 1 B200, stated error"
 UNIT = "pushes/s"
 
 
@@ -37,6 +37,8 @@ def parse():
     ap.add_argument("--workload", type=int, default=2, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: time the FP64 form, then the mixed form (the headline) and its error against FP64")
     ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
     ap.add_argument("--particles", type=int, default=None, help="profiling case: fewer macro-particles")
     return ap.parse_args()
@@ -52,9 +54,10 @@ def workload(k, nzeta=None, particles=None):
     return configs.baseline(k, **kw)
 
 
-def config_json(cfg, k):
+def config_json(cfg, k, form="fp64"):
     return {"workload": f"{k}: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, "
-                        f"{cfg.particles} macro-electrons, FP64",
+                        f"{cfg.particles} macro-electrons, {'mixed FP32/FP64' if form == 'mixed' else 'FP64'} form",
+            "form": form,
             "nx": cfg.nx, "ny": cfg.ny, "nzeta": cfg.nzeta, "particles": cfg.particles,
             "grid_points": cfg.grid_points, "dz": cfg.params["dz"], "sponge": cfg.params.get("sponge", 0),
             "laser_envelope": "flattop" if cfg.params.get("laser_envelope") == 1 else "gaussian",
@@ -73,31 +76,47 @@ def f_bytes(cfg):
 
 
 # ------------------------------------------------------------------ algorithmic bytes per launch (FP64)
-def algorithmic_bytes(name, cfg):
+def algorithmic_bytes(name, cfg, mixed=False):
     """Per-launch algorithmic bytes of each kernel: what it must read and write once, in the layout this build keeps.
 
-    G = grid points (slices x nx x ny, each carries 6 floats of F = 24 B and 3 raw current doubles = 24 B);
-    Gh = half-spectrum points of a slice set (slices x ny x (nx/2 + 1)); a complex128 plane costs 16 B per Gh.
-    The spectra of real fields are Hermitian, so the kept half is the minimum a transform pass has to move.
-    P = beam particles: push reads x, y, zeta, px, py, pz, z, w (64 B) and writes 48 B; deposit reads 56 B."""
+    G = grid points (slices x nx x ny; F carries 6 floats = 24 B, the raw currents 3 values = 24 B in FP64, 12 B
+    in the mixed form); Gh = half-spectrum points of a slice set (slices x ny x (nx/2 + 1)); a spectrum costs
+    16 B per Gh as complex128 and 8 B as complex64 (the mixed form keeps R in complex128 and the rest in
+    complex64). The spectra of real fields are Hermitian, so the kept half is the minimum a transform pass has to
+    move. P = beam particles: the push reads x, y, zeta, px, py, pz, z, w (64 B) and writes 48 B (both forms);
+    the deposit reads 56 B."""
     ns = cfg.nzeta - 1
     nk = cfg.nx * cfg.ny
     G = ns * nk
     Gh = ns * cfg.ny * (cfg.nx // 2 + 1)
     Gc = (ns + 1) * cfg.ny * (cfg.nx // 2 + 1)      # current planes carry one more half-cell
     P = cfg.particles
-    table = {
-        "push": 112 * P + 24 * G,          # particles read 64 + written 48; F read 24 per grid point
-        "deposit": 56 * P + 24 * G,        # particles read 56; raw currents written 24 per grid point
-        "cur_rows": 24 * G + 48 * Gc,      # raw currents read 24; three complex planes written
-        "cur_cols": 48 * Gc + 48 * Gc,     # three complex planes read and written (jkx, jky, jkz)
-        "march": (9 + 6) * 16 * Gh,        # R, E_z, B_z, j0 (2), jk (3) read; R, E_z, B_z, L written
-        "sponge_cols_inv": (2 + 1 + 3) * 16 * Gh,   # R read, j_z read; U, V, psi written
-        "sponge_rows": 4 * 16 * Gh,        # U, V read and written
-        "sponge_cols_fwd": (3 + 2) * 16 * Gh,       # U, V, psi read; R written
-        "real_cols": 12 * 16 * Gh,         # six spectra read, six column transforms written
-        "real_rows": 6 * 16 * Gh + 24 * G,  # six column transforms read; F written
-    }
+    if not mixed:
+        table = {
+            "push": 112 * P + 24 * G,          # particles read 64 + written 48; F read 24 per grid point
+            "deposit": 56 * P + 24 * G,        # particles read 56; raw currents written 24 per grid point
+            "cur_rows": 24 * G + 48 * Gc,      # raw currents read 24; three complex planes written
+            "cur_cols": 48 * Gc + 48 * Gc,     # three complex planes read and written (jkx, jky, jkz)
+            "march": (9 + 6) * 16 * Gh,        # R, E_z, B_z, j0 (2), jk (3) read; R, E_z, B_z, L written
+            "sponge_cols_inv": (2 + 1 + 3) * 16 * Gh,   # R read, j_z read; U, V, psi written
+            "sponge_rows": 4 * 16 * Gh,        # U, V read and written
+            "sponge_cols_fwd": (3 + 2) * 16 * Gh,       # U, V, psi read; R written
+            "real_cols": 12 * 16 * Gh,         # six spectra read, six column transforms written
+            "real_rows": 6 * 16 * Gh + 24 * G,  # six column transforms read; F written
+        }
+    else:
+        table = {
+            "push": 112 * P + 24 * G,
+            "deposit": 56 * P + 12 * G,        # FP32 raw currents
+            "cur_rows": 12 * G + 24 * Gc,
+            "cur_cols": 24 * Gc + 24 * Gc,
+            "march": (7 * 8 + 2 * 16) * Gh + (4 * 8 + 2 * 16) * Gh,   # E_z, B_z, j read, R read; E, B, L and R written
+            "sponge_cols_inv": (2 * 16 + 8 + 2 * 8) * Gh,   # R, j_z read; U, V written
+            "sponge_rows": 4 * 8 * Gh,
+            "sponge_cols_fwd": (2 * 8 + 4 * 16) * Gh,        # U, V read; R read and written (R + dR)
+            "real_cols": (2 * 16 + 4 * 8 + 6 * 8) * Gh,      # R, L, E_z, B_z read; six column transforms written
+            "real_rows": 6 * 8 * Gh + 24 * G,
+        }
     return table.get(name)
 
 
@@ -229,29 +248,16 @@ def run_reference_arm(a):
 
 
 # ------------------------------------------------------------------ our arm
-def run_g3d(a):
-    import numpy as np
+def time_form(cfg, precision, a, world, dist, local):
+    """Init, warm-up, then K device-timed steps of one form; per-kernel event times on the context stream."""
     import torch
     import g3d
-
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg = workload(a.workload, a.nzeta, a.particles)
-    sim = g3d.Simulation(cfg)
+    sim = g3d.Simulation(cfg, precision=precision)
     sim.init()
     P = int(sim.status().np)
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     for _ in range(max(a.warmup, 3)):
         sim.step()
-
-    # ---------------- timed region: K steps, per-kernel events on the same stream
     props = torch.cuda.get_device_properties(local)
     bus = getattr(props, "pci_bus_id", None)
     bus = f"{bus:02x}:00.0" if isinstance(bus, int) else None
@@ -278,59 +284,113 @@ def run_g3d(a):
     launches = sim.launch_count() - l0
     prof = sim.profile_results()
     sim.profile(False)
-    value = job_rate(P, a.steps, world, ms)
+    mixed = precision == "mixed"
+    kernels = {k: {"launches": n, "avg_ms": round(t / max(1, n), 5), "share": round(t / sum(v[1] for v in prof.values()), 4),
+                   "GB/s": (round(algorithmic_bytes(k, cfg, mixed) / (t / max(1, n) * 1e-3) / 1e9, 1)
+                            if algorithmic_bytes(k, cfg, mixed) else None)}
+               for k, (n, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+    return {"sim": sim, "P": P, "stream": stream, "ms": ms, "value": job_rate(P, a.steps, world, ms), "clk": clk,
+            "launches": launches, "prof": prof, "kernels": kernels}
 
-    # ---------------- roofline of the dominant kernel
+
+def roofline(form, cfg, workload, mixed):
     import json as _json
     peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(peaks_path):
         peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
     else:
         peak, peak_src = 6650.0, "fallback"
-    top = max(prof.items(), key=lambda kv: kv[1][1])
-    name, (n_launch, tot_ms) = top
+    name, (n_launch, tot_ms) = max(form["prof"].items(), key=lambda kv: kv[1][1])
     avg_ms = tot_ms / max(1, n_launch)
-    ab = algorithmic_bytes(name, cfg)
+    ab = algorithmic_bytes(name, cfg, mixed)
     achieved = ab / (avg_ms * 1e-3) / 1e9 if ab else None
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = _json.load(open(tpath)).get(f"{a.workload}:{name}")
-    kernels = {k: {"launches": n, "avg_ms": round(t / max(1, n), 5), "share": round(t / sum(v[1] for v in prof.values()), 4),
-                   "GB/s": (round(algorithmic_bytes(k, cfg) / (t / max(1, n) * 1e-3) / 1e9, 1)
-                            if algorithmic_bytes(k, cfg) else None)}
-               for k, (n, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
+        traffic = _json.load(open(tpath)).get(f"{workload}:{'mixed:' if mixed else ''}{name}")
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_source": peak_src,
+            "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_ms}
 
-    # ---------------- end to end through the C-ABI with host buffers
-    e2e = None
-    if a.e2e_steps > 0:
-        host = torch.empty(P * g3d.PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
-        parts = host.numpy().view(g3d.PARTICLE_DTYPE)
-        parts[:] = sim.host_particles()
-        out = torch.empty(P * g3d.PARTICLE_DTYPE.itemsize, dtype=torch.uint8, pin_memory=True)
-        outp = out.numpy().view(g3d.PARTICLE_DTYPE)
-        lib, ctx = sim.lib, sim.ctx
-        diag = (__import__("ctypes").c_double * 19)()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        x0 = torch.cuda.Event(enable_timing=True)
-        x1 = torch.cuda.Event(enable_timing=True)
-        x0.record(stream)
-        got = __import__("ctypes").c_int64()
-        for _ in range(a.e2e_steps):
-            sim._c(lib.g3d_set_particles(ctx, parts.ctypes.data, P))          # inputs: H2D from pinned memory
-            sim._c(lib.g3d_step(ctx))
-            sim._c(lib.g3d_get_particles(ctx, outp.ctypes.data, P, __import__("ctypes").byref(got)))  # result D2H
-            sim._c(lib.g3d_diagnostics(ctx, diag))
-            parts, outp = outp, parts
-        x1.record(stream)
-        x1.synchronize()
-        wall = time.perf_counter() - t0
-        ems = max_over_ranks(max(x0.elapsed_time(x1), wall * 1e3), dist)
-        e2e = {"value": job_rate(P, a.e2e_steps, world, ems), "unit": UNIT,
-               "h2d_bytes_per_step": P * 104, "d2h_bytes_per_step": P * 104 + 19 * 8,
-               "steps": a.e2e_steps,
-               "path": "g3d_set_particles (pinned host records) -> g3d_step -> g3d_get_particles + g3d_diagnostics"}
+
+def end_to_end(form, a, world, dist):
+    """The same metric through the C-ABI with host buffers: every step uploads the particle records from pinned
+    host memory (g3d_set_particles), steps (g3d_step) and reads the records and the diagnostics back."""
+    import ctypes
+    import torch
+    import g3d
+    sim, P, stream = form["sim"], form["P"], form["stream"]
+    nb = P * g3d.PARTICLE_DTYPE.itemsize
+    host = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+    parts = host.numpy().view(g3d.PARTICLE_DTYPE)
+    parts[:] = sim.host_particles()
+    out = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+    outp = out.numpy().view(g3d.PARTICLE_DTYPE)
+    lib, ctx = sim.lib, sim.ctx
+    diag = (ctypes.c_double * 19)()
+    got = ctypes.c_int64()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x0 = torch.cuda.Event(enable_timing=True)
+    x1 = torch.cuda.Event(enable_timing=True)
+    x0.record(stream)
+    for _ in range(a.e2e_steps):
+        sim._c(lib.g3d_set_particles(ctx, parts.ctypes.data, P))          # inputs: H2D from pinned memory
+        sim._c(lib.g3d_step(ctx))
+        sim._c(lib.g3d_get_particles(ctx, outp.ctypes.data, P, ctypes.byref(got)))  # result: D2H
+        sim._c(lib.g3d_diagnostics(ctx, diag))
+        parts, outp = outp, parts
+    x1.record(stream)
+    x1.synchronize()
+    wall = time.perf_counter() - t0
+    ems = max_over_ranks(max(x0.elapsed_time(x1), wall * 1e3), dist)
+    return {"value": job_rate(P, a.e2e_steps, world, ems), "unit": UNIT,
+            "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb + 19 * 8, "steps": a.e2e_steps,
+            "path": "g3d_set_particles (pinned host records) -> g3d_step -> g3d_get_particles + g3d_diagnostics"}
+
+
+def run_g3d(a):
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg = workload(a.workload, a.nzeta, a.particles)
+    forms = ["fp64", "mixed"] if a.precision == "both" else [a.precision]
+    res = {}
+    ref_state = None
+    err = None
+    for prec in forms:
+        f = time_form(cfg, prec, a, world, dist, local)
+        # the state after warm-up + K steps, for the error of the mixed form against the FP64 form
+        F = f["sim"].array("F")
+        d = f["sim"].diagnostics_sums()
+        if prec == "fp64":
+            ref_state = (F, d)
+        elif ref_state is not None:
+            F0, d0 = ref_state
+            rl = lambda x, y: float(np.linalg.norm(x.astype(np.float64) - y) / np.linalg.norm(y.astype(np.float64)))
+            err = {"F": rl(F, F0), "<p_z>": abs(d[9] / d[0] - d0[9] / d0[0]) / abs(d0[9] / d0[0]),
+                   "field_energy": abs(f["sim"].field_energy() - ref_state_energy) / abs(ref_state_energy),
+                   "after_steps": max(a.warmup, 3) + a.steps,
+                   "note": "relative L2 of the float F (all six components) and relative <p_z>, mixed vs FP64 form on the same "
+                           "inputs, same GPU"}
+        if prec == "fp64":
+            ref_state_energy = f["sim"].field_energy()
+        if prec == forms[-1] and a.e2e_steps > 0:
+            f["e2e"] = end_to_end(f, a, world, dist)
+        f["sim"].close()
+        res[prec] = f
+    head = a.precision if a.precision != "both" else "mixed"
+    H = res[head]
+    mixed = head == "mixed"
 
     # ---------------- CPU baseline on rank 0 at N = 1
     cpu = None
@@ -347,16 +407,22 @@ def run_g3d(a):
 
     if dist:
         dist.barrier()
-    sim.close()
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
-                "warmup": max(a.warmup, 3), "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bunch sampler of the reference)",
-                "config": config_json(cfg, a.workload),
-                "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak if achieved else None, "traffic": traffic,
-                             "peak_source": peak_src, "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_ms},
-                "kernels": kernels, "e2e": e2e, "gpu_launches": launches, "clocks": clk, "cpu_baseline": cpu}
+        line = {"metric": METRIC, "value": H["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+                "warmup": max(a.warmup, 3), "ms_per_step": H["ms"] / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64 (mixed form)" if mixed else "f64",
+                "data": "synthetic (seeded bunch sampler of the reference)",
+                "config": config_json(cfg, a.workload, head),
+                "roofline": roofline(H, cfg, a.workload, mixed),
+                "kernels": H["kernels"], "e2e": H.get("e2e"), "gpu_launches": H["launches"], "clocks": H["clk"],
+                "cpu_baseline": cpu}
+        if "fp64" in res and mixed:
+            F64 = res["fp64"]
+            line["fp64_form"] = {"value": F64["value"], "ms_per_step": F64["ms"] / a.steps, "dtype": "f64",
+                                 "roofline": roofline(F64, cfg, a.workload, False), "kernels": F64["kernels"],
+                                 "gpu_launches": F64["launches"], "clocks": F64["clk"]}
+            line["mixed_over_fp64"] = H["value"] / F64["value"]
+            line["mixed_error"] = err
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()

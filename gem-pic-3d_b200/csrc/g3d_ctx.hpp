@@ -104,6 +104,16 @@ struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 
 struct PlasmaState;               // g3d_plasma.hpp
 
+// Buffers of the mixed FP32/FP64 form (k_mixed.cu): complex64 half spectra of E_z, B_z, L and the currents, FP32
+// raw currents; R_x, R_y stay in Ctx::Rx, Ry (complex128), F is float in both forms.
+struct MixedBufs {
+    DevBuf<cpxf> Ez, Bz, Lx, Ly;                 // ns planes
+    DevBuf<cpxf> j0x, j0y, jkx, jky, jkz;        // ns+1 half-cell planes
+    DevBuf<cpxf> W[6];                           // transform scratch, ns+1 planes each
+    DevBuf<float> jw;                            // 3 x (ns+3) real planes
+    DevBuf<cpxf> twx, twy;                       // FP32 twiddles
+};
+
 // ---------------------------------------------------------------- the context
 struct Ctx {
     // grid (single rank: a = 0, b = ns = N)
@@ -128,6 +138,9 @@ struct Ctx {
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
+    bool mixed = false;                          // G3D_PREC_MIXED: the spectra above except Rx, Ry are not allocated
+    MixedBufs mx;
+    bool fields_ready = false;                   // init has run (the precision is fixed from then on)
     // particles
     DevBuf<double> pbuf_d;                       // 11 double columns
     DevBuf<int32_t> pbuf_i;                      // 2 int columns
@@ -193,6 +206,17 @@ void launch_rotate(Ctx& c, cpx* p, size_t n, double sx, double sy, int nys);
 void launch_half_to_full(Ctx& c, const cpx* half, cpx* full, long planes);
 void launch_full_to_half(Ctx& c, const cpx* full, cpx* half, long planes);
 void sort_particles(Ctx& c);                // refresh perm
+// the mixed form (k_mixed.cu)
+void launch_deposit_f(Ctx& c);
+void launch_cur_fft_f(Ctx& c, bool keep0);
+void launch_march_f(Ctx& c, double D);
+void launch_comoving_f(Ctx& c, double beta, double gm2);
+void launch_sponge_f(Ctx& c);
+void launch_real_fields_f(Ctx& c);
+void launch_half_to_full_f(Ctx& c, const cpxf* half, cpx* full, long planes);
+void launch_full_to_half_f(Ctx& c, const cpx* full, cpxf* half, long planes);
+void launch_rotate_f(Ctx& c, cpxf* p, size_t n, double sx, double sy, int nys);
+void launch_copy_f(Ctx& c, cpxf* y, const cpxf* x, size_t n);
 // particles and plasma (g3d_host.cu, g3d_plasma.cu)
 void set_particles(Ctx& c, const g3d_particle* v, long n);
 std::vector<g3d_particle> get_particles(Ctx& c);

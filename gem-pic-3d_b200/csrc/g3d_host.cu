@@ -20,6 +20,54 @@ bool pow2_ok(int n) { return n >= 4 && n <= 512 && (n & (n - 1)) == 0; }
 Ctx::Ctx() = default;
 Ctx::~Ctx() = default;
 
+// The spectra other than R of one form: complex128 (FP64) or complex64 (mixed), with the raw current planes
+// and the transform scratch; the other form's buffers are released.
+static void alloc_spectra(Ctx& c, bool mixed) {
+    const cudaStream_t s = c.stream;
+    const size_t pl = size_t(c.nk), ph = size_t(c.nkh), ns = size_t(c.ns);
+    if (mixed) {
+        for (DevBuf<cpx>* p : {&c.Ez, &c.Bz, &c.Lx, &c.Ly, &c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz, &c.jzg}) p->release();
+        for (DevBuf<cpx>& w : c.W) w.release();
+        c.jw.release();
+        MixedBufs& m = c.mx;
+        for (DevBuf<cpxf>* p : {&m.Ez, &m.Bz, &m.Lx, &m.Ly}) p->alloc(ns * ph, s);
+        for (DevBuf<cpxf>* p : {&m.j0x, &m.j0y, &m.jkx, &m.jky, &m.jkz}) p->alloc((ns + 1) * ph, s);
+        for (DevBuf<cpxf>& w : m.W) w.alloc((ns + 1) * ph, s);
+        m.jw.alloc(3 * (ns + 3) * pl, s);
+        auto tw = [&](int n) {
+            std::vector<cpxf> t(static_cast<size_t>(n));
+            for (int k = 0; k < n; ++k) {
+                const std::complex<double> w = std::polar(1.0, -2.0 * M_PI * k / n);
+                t[size_t(k)] = Cf(float(w.real()), float(w.imag()));
+            }
+            return t;
+        };
+        m.twx.upload(tw(c.nx), s); m.twy.upload(tw(c.ny), s);
+    } else {
+        MixedBufs& m = c.mx;
+        for (DevBuf<cpxf>* p : {&m.Ez, &m.Bz, &m.Lx, &m.Ly, &m.j0x, &m.j0y, &m.jkx, &m.jky, &m.jkz, &m.twx, &m.twy}) p->release();
+        for (DevBuf<cpxf>& w : m.W) w.release();
+        m.jw.release();
+        for (DevBuf<cpx>* p : {&c.Ez, &c.Bz, &c.Lx, &c.Ly}) p->alloc(ns * ph, s);
+        for (DevBuf<cpx>* p : {&c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz}) p->alloc((ns + 1) * ph, s);
+        for (DevBuf<cpx>& w : c.W) w.alloc((ns + 1) * ph, s);
+        c.jzg.alloc(2 * ph, s);
+        c.jw.alloc(3 * (ns + 3) * pl, s);
+    }
+    c.mixed = mixed;
+    c.jk_is_j0 = false;
+    G3D_CUDA(cudaStreamSynchronize(s));
+}
+
+static void set_precision(Ctx& c, int mode) {
+    if (mode != G3D_PREC_FP64 && mode != G3D_PREC_MIXED) throw Error(G3D_ERR_ARG, "unknown precision " + std::to_string(mode));
+    const bool mixed = mode == G3D_PREC_MIXED;
+    if (mixed == c.mixed) return;
+    if (c.fields_ready) throw Error(G3D_ERR_STATE, "the precision is set before g3d_init");
+    if (mixed && c.pl) throw Error(G3D_ERR_ARG, "the mixed form has no streaming plasma in this release");
+    alloc_spectra(c, mixed);
+}
+
 Geo Ctx::geo() const {
     Geo g;
     g.nx = nx; g.ny = ny; g.nk = nk; g.N = N; g.a = a; g.b = b; g.ns = ns; g.nh = ns + 3;
@@ -155,11 +203,8 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.twx.upload(tw(nx), s); c.twy.upload(tw(ny), s);
     // field buffers: real planes of the reference layouts, spectra as half spectra
     const size_t pl = size_t(c.nk), ph = size_t(c.nkh), ns = size_t(c.ns);
-    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.Lx, &c.Ly}) p->alloc(ns * ph, s);
-    for (DevBuf<cpx>* p : {&c.j0x, &c.j0y, &c.jkx, &c.jky, &c.jkz}) p->alloc((ns + 1) * ph, s);
-    for (DevBuf<cpx>& w : c.W) w.alloc((ns + 1) * ph, s);
-    c.jzg.alloc(2 * ph, s);
-    c.jw.alloc(3 * (ns + 3) * pl, s);
+    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry}) p->alloc(ns * ph, s);
+    alloc_spectra(c, false);
     c.F.alloc(6 * (ns + 2) * pl, s);
     c.rscratch.alloc(ns * ph, s);
     c.red.alloc(size_t(297) * 17, s);
@@ -279,29 +324,47 @@ static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int c
 // ---------------------------------------------------------------- the march path
 static void currents(Ctx& c) {
     c.jk_is_j0 = false;
-    launch_deposit(c);
+    if (!c.mixed) launch_deposit(c);
     // with plasma the k = 0 current is kept (a 1D plasma wave, the return current), but not in the start field
     // (sim_particles.cpp:143-145)
     const bool keep0 = c.pl && c.pl->box_mean && !c.starting_;
+    if (c.mixed) { launch_deposit_f(c); launch_cur_fft_f(c, keep0); return; }
     launch_cur_fft(c, keep0);
     // one rank: the filtered j_z ghosts of the neighbours are zero (exchange_jz_ghosts, sim_particles.cpp:210-226)
 }
 static void march(Ctx& c, double D) {
     if (c.jk_is_j0) throw Error(G3D_ERR_STATE, "march needs the currents of level s1 (call currents first)");
-    launch_march(c, D);
+    if (c.mixed) launch_march_f(c, D);
+    else launch_march(c, D);
 }
 static void sponge_and_real_fields(Ctx& c) {
+    if (c.mixed) {
+        if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge_f(c);
+        launch_real_fields_f(c);
+        return;
+    }
     if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge(c);
     launch_real_fields(c);
 }
 // j0 <- jk (sim_fields.cpp:313-315): the buffers are swapped; until the next deposit jk reads as j0.
 static void j0_from_jk(Ctx& c) {
-    std::swap(c.j0x.p, c.jkx.p);
-    std::swap(c.j0y.p, c.jky.p);
+    if (c.mixed) {
+        std::swap(c.mx.j0x.p, c.mx.jkx.p);
+        std::swap(c.mx.j0y.p, c.mx.jky.p);
+    } else {
+        std::swap(c.j0x.p, c.jkx.p);
+        std::swap(c.j0y.p, c.jky.p);
+    }
     c.jk_is_j0 = true;
 }
 static void materialize_jk(Ctx& c) {
     if (!c.jk_is_j0) return;
+    if (c.mixed) {
+        launch_copy_f(c, c.mx.jkx.p, c.mx.j0x.p, c.mx.jkx.n);
+        launch_copy_f(c, c.mx.jky.p, c.mx.j0y.p, c.mx.jky.n);
+        c.jk_is_j0 = false;
+        return;
+    }
     launch_copy_c(c, c.jkx.p, c.j0x.p, c.jkx.n);
     launch_copy_c(c, c.jky.p, c.j0y.p, c.jky.n);
     c.jk_is_j0 = false;
@@ -318,10 +381,30 @@ static void comoving_field(Ctx& c) {
     const double beta = c.comoving_c_ ? 1 : sums[1] > 0 ? sums[0] / sums[1] : 1;
     const double gm2 = 1 - beta * beta;
     if (!c.comoving_c_) { c.beta_b = beta; c.gm2_b = gm2; }
-    launch_comoving(c, beta, gm2);
+    if (c.mixed) launch_comoving_f(c, beta, gm2);
+    else launch_comoving(c, beta, gm2);
 }
 static void relax_start_field(Ctx& c) {
     const size_t n = size_t(c.ns) * c.nkh, nj = size_t(c.ns + 1) * c.nkh;
+    if (c.mixed) {
+        // the same three backward-Euler marches; R stays complex128, so its two copies are too
+        DevBuf<cpx> rx, ry;
+        rx.alloc(n, c.stream); ry.alloc(n, c.stream);
+        launch_copy_c(c, rx.p, c.Rx.p, n);
+        launch_copy_c(c, ry.p, c.Ry.p, n);
+        c.comoving_c_ = true; comoving_field(c); c.comoving_c_ = false;
+        launch_axpy_c(c, rx.p, c.Rx.p, -1.0, n);
+        launch_axpy_c(c, ry.p, c.Ry.p, -1.0, n);
+        const double D = 100 * c.P.dz;
+        for (int it = 0; it < 3; ++it) {
+            c.mx.Ez.zero(c.stream); c.mx.Bz.zero(c.stream); c.mx.j0x.zero(c.stream); c.mx.j0y.zero(c.stream);
+            march(c, D);
+        }
+        launch_axpy_c(c, c.Rx.p, rx.p, 1.0, n);
+        launch_axpy_c(c, c.Ry.p, ry.p, 1.0, n);
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+        return;
+    }
     cpx* dxr = c.W[4].p; cpx* dyr = c.W[5].p;      // R of the bunch's beta (the co-moving solve uses W3)
     launch_copy_c(c, dxr, c.Rx.p, n);
     launch_copy_c(c, dyr, c.Ry.p, n);
@@ -341,6 +424,8 @@ static void shift_window(Ctx& c, int nxs, int nys) {
     materialize_jk(c);
     c.X0 += nxs * c.dx; c.Y0 += nys * c.dy;
     launch_shift(c, nxs, nys, nxs * c.dx, nys * c.dy);
+    if (c.mixed && c.P.self_fields)
+        for (DevBuf<cpxf>* a : {&c.mx.Ez, &c.mx.Bz, &c.mx.j0x, &c.mx.j0y}) launch_rotate_f(c, a->p, a->n, nxs * c.dx, nys * c.dy, nys);
     if (c.pl) {
         for (auto& p : c.pl->joining) { p.x -= nxs * c.dx; p.y -= nys * c.dy; }
         launch_rotate(c, c.pl->js0x.p, c.pl->js0x.n, nxs * c.dx, nys * c.dy, nys);
@@ -367,6 +452,7 @@ static void window_shift_start(Ctx& c) {
 }
 static void init_fields(Ctx& c) {
     c.s = 0; c.istep = 0;
+    c.fields_ready = true;
     if (c.P.self_fields) {
         c.starting_ = true;
         currents(c);
@@ -398,10 +484,28 @@ static void step(Ctx& c, bool sync) {
 static bool finished(const Ctx& c) { return c.s >= c.P.z_end - 1e-9 || c.stop_; }
 
 // ---------------------------------------------------------------- arrays
-// Storage of an array id: device pointer, element count and size of the storage, and the planes of a
-// spectrum (0 for the real arrays jw and F, which are stored in the reference layout).
-struct ArrayRef { void* p; size_t count, eb; long planes; };
+// Storage of an array id: device pointer, element count and size of the storage, the planes of a spectrum
+// (0 for the real arrays jw and F, which are stored in the reference layout), and whether the storage is the
+// mixed form's (complex64 spectra, float jw) while the boundary keeps the reference's complex128 / double.
+struct ArrayRef { void* p; size_t count, eb; long planes; bool narrow; };
 static ArrayRef array_ref(Ctx& c, int which) {
+    if (c.mixed && which != G3D_A_RX && which != G3D_A_RY && which != G3D_A_F) {
+        DevBuf<cpxf>* cb = nullptr;
+        long planes = c.ns;
+        MixedBufs& m = c.mx;
+        switch (which) {
+            case G3D_A_EZ: cb = &m.Ez; break; case G3D_A_BZ: cb = &m.Bz; break;
+            case G3D_A_LX: cb = &m.Lx; break; case G3D_A_LY: cb = &m.Ly; break;
+            case G3D_A_J0X: cb = &m.j0x; planes = c.ns + 1; break;
+            case G3D_A_J0Y: cb = &m.j0y; planes = c.ns + 1; break;
+            case G3D_A_JKX: cb = c.jk_is_j0 ? &m.j0x : &m.jkx; planes = c.ns + 1; break;
+            case G3D_A_JKY: cb = c.jk_is_j0 ? &m.j0y : &m.jky; planes = c.ns + 1; break;
+            case G3D_A_JKZ: cb = &m.jkz; planes = c.ns + 1; break;
+            case G3D_A_JW: return ArrayRef{m.jw.p, m.jw.n, sizeof(double), 0, true};
+            default: throw Error(G3D_ERR_ARG, "unknown array id " + std::to_string(which));
+        }
+        return ArrayRef{cb->p, cb->n, sizeof(cpx), planes, true};
+    }
     DevBuf<cpx>* cb = nullptr;
     long planes = c.ns;
     switch (which) {
@@ -413,39 +517,55 @@ static ArrayRef array_ref(Ctx& c, int which) {
         case G3D_A_JKX: cb = c.jk_is_j0 ? &c.j0x : &c.jkx; planes = c.ns + 1; break;
         case G3D_A_JKY: cb = c.jk_is_j0 ? &c.j0y : &c.jky; planes = c.ns + 1; break;
         case G3D_A_JKZ: cb = &c.jkz; planes = c.ns + 1; break;
-        case G3D_A_JW: return ArrayRef{c.jw.p, c.jw.n, sizeof(double), 0};
-        case G3D_A_F: return ArrayRef{c.F.p, c.F.n, sizeof(float), 0};
+        case G3D_A_JW: return ArrayRef{c.jw.p, c.jw.n, sizeof(double), 0, false};
+        case G3D_A_F: return ArrayRef{c.F.p, c.F.n, sizeof(float), 0, false};
         default: throw Error(G3D_ERR_ARG, "unknown array id " + std::to_string(which));
     }
-    return ArrayRef{cb->p, cb->n, sizeof(cpx), planes};
+    return ArrayRef{cb->p, cb->n, sizeof(cpx), planes, false};
 }
 // Element count of an array in the reference layout (spectra in full: planes x ny x nx).
 static size_t ref_count(Ctx& c, const ArrayRef& a) { return a.planes ? size_t(a.planes) * c.nk : a.count; }
 
-// Copy out in the reference layout (spectra expanded from the half spectrum by X(-k) = conj X(k)).
+// Copy out in the reference layout (spectra expanded from the half spectrum by X(-k) = conj X(k); the mixed
+// form's complex64 and float values widened to complex128 and double).
 static void get_array(Ctx& c, int which, void* host) {
     const ArrayRef a = array_ref(c, which);
-    if (!a.planes) {
+    if (!a.planes && a.narrow) {
+        std::vector<float> v(a.count);
+        if (a.count) G3D_CUDA(cudaMemcpyAsync(v.data(), a.p, a.count * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+        double* out = static_cast<double*>(host);
+        for (size_t i = 0; i < a.count; ++i) out[i] = v[i];
+    } else if (!a.planes) {
         if (a.count) G3D_CUDA(cudaMemcpyAsync(host, a.p, a.count * a.eb, cudaMemcpyDeviceToHost, c.stream));
     } else {
         DevBuf<cpx> full;
         full.alloc(ref_count(c, a), c.stream);
-        launch_half_to_full(c, static_cast<const cpx*>(a.p), full.p, a.planes);
+        if (a.narrow) launch_half_to_full_f(c, static_cast<const cpxf*>(a.p), full.p, a.planes);
+        else launch_half_to_full(c, static_cast<const cpx*>(a.p), full.p, a.planes);
         G3D_CUDA(cudaMemcpyAsync(host, full.p, full.bytes(), cudaMemcpyDeviceToHost, c.stream));
         G3D_CUDA(cudaStreamSynchronize(c.stream));
     }
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
-// Copy in from the reference layout (spectra keep k_x = 0 .. nx/2: the data are the spectra of real fields).
+// Copy in from the reference layout (spectra keep k_x = 0 .. nx/2: the data are the spectra of real fields;
+// the mixed form rounds to complex64 and float).
 static void set_array(Ctx& c, int which, const void* host) {
     const ArrayRef a = array_ref(c, which);
-    if (!a.planes) {
+    if (!a.planes && a.narrow) {
+        const double* in = static_cast<const double*>(host);
+        std::vector<float> v(a.count);
+        for (size_t i = 0; i < a.count; ++i) v[i] = float(in[i]);
+        if (a.count) G3D_CUDA(cudaMemcpyAsync(a.p, v.data(), a.count * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    } else if (!a.planes) {
         if (a.count) G3D_CUDA(cudaMemcpyAsync(a.p, host, a.count * a.eb, cudaMemcpyHostToDevice, c.stream));
     } else {
         DevBuf<cpx> full;
         full.alloc(ref_count(c, a), c.stream);
         G3D_CUDA(cudaMemcpyAsync(full.p, host, full.bytes(), cudaMemcpyHostToDevice, c.stream));
-        launch_full_to_half(c, full.p, static_cast<cpx*>(a.p), a.planes);
+        if (a.narrow) launch_full_to_half_f(c, full.p, static_cast<cpxf*>(a.p), a.planes);
+        else launch_full_to_half(c, full.p, static_cast<cpx*>(a.p), a.planes);
         G3D_CUDA(cudaStreamSynchronize(c.stream));
     }
     G3D_CUDA(cudaStreamSynchronize(c.stream));
@@ -685,6 +805,7 @@ int g3d_push(g3d_ctx* ctx, double s0, double s1) {
 int g3d_comoving_field(g3d_ctx* ctx) {
     return guarded(ctx, [&] { g3d::comoving_field(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
 }
+int g3d_set_precision(g3d_ctx* ctx, int32_t mode) { return guarded(ctx, [&] { g3d::set_precision(ctx->c, mode); }); }
 int g3d_beam_beta_sums_static(g3d_ctx* ctx, double out[2]) {
     return guarded(ctx, [&] {
         if (!out) throw Error(G3D_ERR_ARG, "null output");
@@ -702,6 +823,7 @@ int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ct
 int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
     return guarded(ctx, [&] {
         if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
+        if (ctx->c.mixed) throw Error(G3D_ERR_ARG, "the mixed form has no streaming plasma in this release");
         g3d::set_plasma(ctx->c, *plasma, ions, nions);
     });
 }

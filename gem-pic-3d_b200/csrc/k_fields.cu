@@ -434,6 +434,7 @@ void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy) {
     }
     if (!c.P.self_fields) return;
     for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz, &c.j0x, &c.j0y}) {
+        if (!a->n) continue;                     // the mixed form keeps E_z, B_z, j0 in complex64 (k_mixed.cu)
         k_rotate<<<ew_blocks(long(a->n)), 256, 0, c.stream>>>(g, a->p, long(a->n), sx, sy, nys);
         c.check_launch("k_rotate");
     }

@@ -39,14 +39,26 @@ template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 }  // namespace
 
-// One thread per mode. Per slice the thread's own 16-byte loads (9 arrays) and its copies of the slice's
-// coefficients land in its column of a ring of MS slots; the recurrence itself touches only registers and
-// that ring. The denominator 1 + (h/4)(D + h/4) k_perp^2 is inverted one slice ahead, off the chain.
-__global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, cpx* __restrict__ Ez,
-                                             cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
-                                             const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
-                                             const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
-                                             const cpx* __restrict__ jkz, double D) {
+__device__ __forceinline__ cpx widen(cpx a) { return a; }
+__device__ __forceinline__ cpx widen(cpxf a) { return to_d(a); }
+template <class T> __device__ __forceinline__ T narrow(cpx a);
+template <> __device__ __forceinline__ cpx narrow<cpx>(cpx a) { return a; }
+template <> __device__ __forceinline__ cpxf narrow<cpxf>(cpx a) { return to_f(a); }
+
+// One thread per mode. Per slice the thread's own loads (9 arrays) and its copies of the slice's coefficients
+// land in its column of a ring of MS slots; the recurrence itself touches only registers and that ring. The
+// denominator 1 + (h/4)(D + h/4) k_perp^2 is inverted one slice ahead, off the chain.
+// T is the storage of E_z, B_z, L and the currents: complex128 (the FP64 form) or complex64 (the mixed form,
+// 8-byte copies into the 16-byte ring cells). R stays complex128, and the recurrence runs in FP64 in both
+// forms: its carried values (level s1 of R, L, E_z, B_z) never leave the registers, so the mixed form only
+// rounds what it stores, and the cancellations in curl R and div R that make E_z, B_z gamma^-2 small are
+// taken in FP64.
+template <class T>
+__global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
+                                             T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
+                                             const T* __restrict__ j0x, const T* __restrict__ j0y,
+                                             const T* __restrict__ jkx, const T* __restrict__ jky,
+                                             const T* __restrict__ jkz, double D) {
     extern __shared__ double ringd[];        // MS slots of [MA arrays][MT] complex, then [MC][MT] double
     const long nk = g.nkh;
     const int tid = threadIdx.x;
@@ -55,22 +67,35 @@ __global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
     const long ii = live ? i : 0;             // idle threads stream mode 0 and store nothing
     const int kxi = int(ii % g.H), j = int(ii / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
-    const cpx* src[MA] = {j0x, jkx, j0y, jky, jkz, Rx, Ry, Ez, Bz};
+    const T* srct[7] = {j0x, jkx, j0y, jky, jkz, Ez, Bz};
     auto arr = [&](int sl, int k) { return reinterpret_cast<cpx*>(ringd + size_t(sl) * SLOT) + k * MT + tid; };
     auto coef = [&](int sl, int k) { return ringd + size_t(sl) * SLOT + 2 * MA * MT + k * MT + tid; };
+    // ring cell k: j0x, jkx, j0y, jky, jkz, R_x, R_y, E_z, B_z
+    auto cell = [&](int sl, int k) -> cpx {
+        if (k == 5 || k == 6) return *arr(sl, k);
+        return widen(*reinterpret_cast<const T*>(arr(sl, k)));
+    };
     auto fetch = [&](int n) {                  // slice n (plane n - a) into its ring slot
         const int sl = (g.b - 1 - n) % MS;
         const long o = long(n - g.a) * nk + ii;
 #pragma unroll
-        for (int k = 0; k < MA; ++k) cp_async16(arr(sl, k), src[k] + o);
+        for (int k = 0; k < MA; ++k) {
+            if (k == 5) cp_async16(arr(sl, k), Rx + o);
+            else if (k == 6) cp_async16(arr(sl, k), Ry + o);
+            else {
+                const T* sp = srct[k < 5 ? k : k - 2] + o;
+                if (sizeof(T) == 16) cp_async16(arr(sl, k), sp);
+                else cp_async8(arr(sl, k), sp);
+            }
+        }
         cp_async8(coef(sl, 0), g.wlo + n);
         cp_async8(coef(sl, 1), g.whi + n);
         cp_async8(coef(sl, 2), g.hcg + n + 2);
     };
     // upper half-cell of the front slice: plane ns
     const long ou = long(g.ns) * nk + ii;
-    cpx jxu = j0x[ou] + jkx[ou], jyu = j0y[ou] + jky[ou];
-    cpx upx = jkx[ou], upy = jky[ou], upz = jkz[ou];
+    cpx jxu = widen(j0x[ou]) + widen(jkx[ou]), jyu = widen(j0y[ou]) + widen(jky[ou]);
+    cpx upx = widen(jkx[ou]), upy = widen(jky[ou]), upz = widen(jkz[ou]);
     cpx pRx = C(0), pRy = C(0), pEz = C(0), pBz = C(0), pLx = C(0), pLy = C(0);
 #pragma unroll
     for (int q = 0; q < MS; ++q) {
@@ -83,8 +108,8 @@ __global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
     for (int n = g.b - 1; n >= g.a; --n) {
         cp_wait<MS - 1>();                    // the group of slice n has landed (this thread's own copies)
         const int sl = (g.b - 1 - n) % MS;
-        const cpx dx0 = *arr(sl, 0), dxk = *arr(sl, 1), dy0 = *arr(sl, 2), dyk = *arr(sl, 3);
-        const cpx dzk = *arr(sl, 4), rx = *arr(sl, 5), ry = *arr(sl, 6), ez = *arr(sl, 7), bz = *arr(sl, 8);
+        const cpx dx0 = cell(sl, 0), dxk = cell(sl, 1), dy0 = cell(sl, 2), dyk = cell(sl, 3);
+        const cpx dzk = cell(sl, 4), rx = cell(sl, 5), ry = cell(sl, 6), ez = cell(sl, 7), bz = cell(sl, 8);
         const double wl = *coef(sl, 0), wu = *coef(sl, 1), h = *coef(sl, 2);
         if (!have_rden) rden = 1 / (1 + 0.25 * h * (D + 0.25 * h) * k2);
         // the next slice's inverse denominator, while this slice's chain runs
@@ -103,7 +128,7 @@ __global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
         if (n == g.N - 1) {          // front of the window: L = E_z = B_z = 0
             if (live) {
                 Rx[o] = Rsx; Ry[o] = Rsy;
-                Ez[o] = C(0); Bz[o] = C(0); Lx[o] = C(0); Ly[o] = C(0);
+                Ez[o] = narrow<T>(C(0)); Bz[o] = narrow<T>(C(0)); Lx[o] = narrow<T>(C(0)); Ly[o] = narrow<T>(C(0));
             }
             pRx = Rsx; pRy = Rsy; pEz = C(0); pBz = C(0); pLx = C(0); pLy = C(0);
         } else {
@@ -119,7 +144,10 @@ __global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
             const cpx nRy = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
             const cpx nLx = Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn));
             const cpx nLy = Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn));
-            if (live) { Ez[o] = Ezn; Bz[o] = Bzn; Rx[o] = nRx; Ry[o] = nRy; Lx[o] = nLx; Ly[o] = nLy; }
+            if (live) {
+                Ez[o] = narrow<T>(Ezn); Bz[o] = narrow<T>(Bzn); Rx[o] = nRx; Ry[o] = nRy;
+                Lx[o] = narrow<T>(nLx); Ly[o] = narrow<T>(nLy);
+            }
             pRx = nRx; pRy = nRy; pEz = Ezn; pBz = Bzn; pLx = nLx; pLy = nLy;
         }
         rden = rden_next;
@@ -175,10 +203,22 @@ void launch_march(Ctx& c, double D) {
     const int tok = c.prof_begin("march");
     const unsigned blocks = unsigned((c.nkh + MT - 1) / MT);
     const size_t smem = size_t(MS) * SLOT * sizeof(double);
-    G3D_CUDA(cudaFuncSetAttribute(k_march, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_march<<<blocks, MT, smem, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p,
-                                         c.jky.p, c.jkz.p, D);
+    G3D_CUDA(cudaFuncSetAttribute(k_march<cpx>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_march<cpx><<<blocks, MT, smem, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
+                                              c.jkx.p, c.jky.p, c.jkz.p, D);
     c.check_launch("k_march");
+    c.prof_end(tok);
+}
+
+void launch_march_f(Ctx& c, double D) {
+    const int tok = c.prof_begin("march");
+    const unsigned blocks = unsigned((c.nkh + MT - 1) / MT);
+    const size_t smem = size_t(MS) * SLOT * sizeof(double);
+    MixedBufs& m = c.mx;
+    G3D_CUDA(cudaFuncSetAttribute(k_march<cpxf>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_march<cpxf><<<blocks, MT, smem, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
+                                               m.jkx.p, m.jky.p, m.jkz.p, D);
+    c.check_launch("k_march_f");
     c.prof_end(tok);
 }
 

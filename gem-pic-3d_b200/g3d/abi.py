@@ -11,6 +11,7 @@ import numpy as np
 G3D_OK, G3D_ERR_CUDA, G3D_ERR_TIMEOUT, G3D_ERR_CAPACITY, G3D_ERR_ARG, G3D_ERR_STATE, G3D_ERR_IO, G3D_ERR_NODEV = range(8)
 G3D_FP64, G3D_MIXED = 0, 1
 G3D_ENV_GAUSSIAN, G3D_ENV_FLATTOP = 0, 1
+G3D_PREC_FP64, G3D_PREC_MIXED = 0, 1
 G3D_POL_S, G3D_POL_P, G3D_POL_CIRCULAR = 0, 1, 2
 
 ARRAYS = {"Rx": 0, "Ry": 1, "Ez": 2, "Bz": 3, "Lx": 4, "Ly": 5, "j0x": 6, "j0y": 7,
@@ -116,6 +117,7 @@ SIGNATURES = [
     ("g3d_diagnostics", _I, [_P, C.POINTER(_D)]),
     ("g3d_field_energy", _I, [_P, C.POINTER(_D)]),
     ("g3d_beam_beta_sums_static", _I, [_P, C.POINTER(_D)]),
+    ("g3d_set_precision", _I, [_P, _I]),
     ("g3d_get_status", _I, [_P, C.POINTER(Status)]),
     ("g3d_array_info", _I, [_P, _I32, C.POINTER(_S), C.POINTER(_S)]),
     ("g3d_get_array", _I, [_P, _I32, _P, _S]),

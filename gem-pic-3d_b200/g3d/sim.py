@@ -41,9 +41,12 @@ def sample_bunches(cfg, lib=None):
 
 
 class Simulation:
-    """One march context on the current CUDA device."""
+    """One march context on the current CUDA device. precision: "fp64" (the reference's arithmetic) or "mixed"
+    (FP32 transforms, currents and E_z/B_z/L with the FP64 accumulator R; no streaming plasma)."""
 
-    def __init__(self, cfg, lib=None):
+    def __init__(self, cfg, lib=None, precision="fp64"):
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
         self.lib = lib or abi.load_library()
         self.cfg = cfg
         g, self._zeta = cfg.grid_struct()
@@ -53,6 +56,9 @@ class Simulation:
         if rc != abi.G3D_OK:
             raise G3DError(rc, self.lib.g3d_last_error(None).decode(errors="replace"))
         self.ctx = h
+        self.precision = precision
+        if precision == "mixed":
+            self._c(self.lib.g3d_set_precision(self.ctx, abi.G3D_PREC_MIXED))
         ps = cfg.plasma_structs()
         if ps is not None:
             P, ions, nions, self._keep = ps
