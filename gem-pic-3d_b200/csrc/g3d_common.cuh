@@ -104,8 +104,24 @@ G3D_HD void tsc_weights(double xi, int idx[3], double w[3]) {
     w[2] = 0.5 * (0.5 + f) * (0.5 + f);
     idx[0] = i0 - 1; idx[1] = i0; idx[2] = i0 + 1;
 }
-// TSC on a periodic uniform grid with nodes at i*d (reference tsc, src/sim_kernels.hpp:28-31).
+// TSC on a periodic uniform grid with nodes at i*d (reference tsc, src/sim_kernels.hpp:28-31). The three
+// indices are consecutive, so one modulo wraps the first and the other two follow by a compare (the same
+// indices as wrapping each one).
 G3D_HD void tsc_periodic(double x, double d, int n, int idx[3], double w[3]) {
     tsc_weights(x / d, idx, w);
-    for (int k = 0; k < 3; ++k) idx[k] = (idx[k] % n + n) % n;
+    int b = idx[0] % n;
+    if (b < 0) b += n;
+    const int b1 = b + 1 == n ? 0 : b + 1;
+    idx[0] = b; idx[1] = b1; idx[2] = b1 + 1 == n ? 0 : b1 + 1;
 }
+
+// fmod(x, L) for L > 0, bit for bit (fmod is exact): |x| < L is x itself, L <= |x| < 2L is x -+ L (exact by
+// Sterbenz's lemma); larger |x| falls back to fmod. The periodic wrap of the reference's gather call,
+// fmod(fmod(x, L) + L, L) (src/sim_kernels.hpp), meets only the first two cases in practice.
+G3D_HD double fmod_pos(double x, double L) {
+    const double a = fabs(x);
+    if (a < L) return x;
+    if (a < 2 * L) return x > 0 ? x - L : x + L;
+    return fmod(x, L);
+}
+G3D_HD double wrap_periodic(double x, double L) { return fmod_pos(fmod_pos(x, L) + L, L); }

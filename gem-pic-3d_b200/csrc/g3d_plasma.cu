@@ -271,72 +271,110 @@ void march_plasma(Ctx& c, double s0, double s1) {
     for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
     cpx* pin = P.jpred.p;
     cpx* tmp = P.jtmp.p;
-    auto copy3 = [&](cpx* dst, int m) {           // dst <- js0 of half-cell m
-        for (int k = 0; k < 3; ++k) {
-            const cpx* src = (k == 0 ? P.js0x.p : k == 1 ? P.js0y.p : P.js0z.p) + hpl(m);
-            G3D_CUDA(cudaMemcpyAsync(dst + k * nkh, src, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-        }
-    };
-    bool have_dl = false;
-    P.jpred.zero(c.stream);
-    // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
-    copy3(tmp, N - 2);
-    launch_replace(c, N - 2, pin, tmp);
-    launch_march_slice(c, D, N - 1);
-    launch_real_fields_slice(c, N - 1);
+    // The slice loop issues some 17 operations per half-cell and pass (about 35,000 for 2,048 slices and two
+    // passes). Launched one by one, the host's launch rate would bound the march; captured into one graph they
+    // are submitted at once and run back to back. The capture replays exactly the launches below (no kernel
+    // differs); it is skipped while per-kernel events are recorded.
+    const bool graph = !c.profiling;
+    if (graph) G3D_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+    try {
+        auto copy3 = [&](cpx* dst, int m) {           // dst <- js0 of half-cell m
+            for (int k = 0; k < 3; ++k) {
+                const cpx* src = (k == 0 ? P.js0x.p : k == 1 ? P.js0y.p : P.js0z.p) + hpl(m);
+                G3D_CUDA(cudaMemcpyAsync(dst + k * nkh, src, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+            }
+        };
+        bool have_dl = false;
+        P.jpred.zero(c.stream);
+        // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
+        copy3(tmp, N - 2);
+        launch_replace(c, N - 2, pin, tmp);
+        launch_march_slice(c, D, N - 1);
+        launch_real_fields_slice(c, N - 1);
 
-    StreamArgs sa;
-    sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.X0 = c.X0; sa.Y0 = c.Y0; sa.zc = c.P.zeta_center;
-    sa.Delta = Delta; sa.s1 = s1; sa.sTrap = s1 + (P.cfg.trap_advance - 1) * Delta; sa.vz_beam = P.cfg.vz_beam;
-    sa.J = P.jsr.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p; sa.bcap = 0; sa.key = 0;
-    const bool ionz = P.born_cap > 0;
-    const uint64_t key_step = mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep));   // ion_key_step
-    const int passes = P.cfg.iterations;
-    const long nmax = P.nstrm + P.born_cap;              // upper bound of the streaming particles of this march
-    for (int n = nhi; n >= c.a; --n) {
-        const long hp = hpl(n);
-        G3D_CUDA(cudaMemcpyAsync(P.jsin.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.jsi0.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-        if (n >= 1) {                                    // start of the prediction of half-cell n-1: its level s0
-            P.jpred.zero(c.stream);
-            copy3(tmp, n - 1);
-            launch_replace(c, n - 1, pin, tmp);
-        }
-        if (passes > 1) {
-            const long o = long(n - c.a) * nkh;
-            int k = 0;
-            for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
-                G3D_CUDA(cudaMemcpyAsync(P.bk.p + (k++) * nkh, a->p + o, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-            launch_strm_copy(c, P.sbk.v, P.strm, nmax);
-        }
-        const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl) ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
-        for (int pass = 0; pass < passes; ++pass) {
-            if (pass > 0) {
+        StreamArgs sa;
+        sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.X0 = c.X0; sa.Y0 = c.Y0; sa.zc = c.P.zeta_center;
+        sa.Delta = Delta; sa.s1 = s1; sa.sTrap = s1 + (P.cfg.trap_advance - 1) * Delta; sa.vz_beam = P.cfg.vz_beam;
+        sa.J = P.jsr.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p; sa.bcap = 0; sa.key = 0;
+        const bool ionz = P.born_cap > 0;
+        const uint64_t key_step = mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep));   // ion_key_step
+        const int passes = P.cfg.iterations;
+        const long nmax = P.nstrm + P.born_cap;              // upper bound of the streaming particles of this march
+        for (int n = nhi; n >= c.a; --n) {
+            const long hp = hpl(n);
+            G3D_CUDA(cudaMemcpyAsync(P.jsin.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+            G3D_CUDA(cudaMemcpyAsync(P.jsi0.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+            if (n >= 1) {                                    // start of the prediction of half-cell n-1: its level s0
+                P.jpred.zero(c.stream);
+                copy3(tmp, n - 1);
+                launch_replace(c, n - 1, pin, tmp);
+            }
+            if (passes > 1) {
                 const long o = long(n - c.a) * nkh;
                 int k = 0;
                 for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
-                    G3D_CUDA(cudaMemcpyAsync(a->p + o, P.bk.p + (k++) * nkh, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-                launch_strm_copy(c, P.strm, P.sbk.v, nmax);
+                    G3D_CUDA(cudaMemcpyAsync(P.bk.p + (k++) * nkh, a->p + o, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+                launch_strm_copy(c, P.sbk.v, P.strm, nmax);
             }
-            P.jsr.zero(c.stream);
-            sa.n = n;
-            if (ionz) {
-                G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
-                sa.key = mix64h(key_step ^ ((uint64_t(n) << 8) | uint64_t(pass)));   // ion_key_slice
-                sa.bcap = int(P.born_cap);
+            const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl) ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+            for (int pass = 0; pass < passes; ++pass) {
+                if (pass > 0) {
+                    const long o = long(n - c.a) * nkh;
+                    int k = 0;
+                    for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
+                        G3D_CUDA(cudaMemcpyAsync(a->p + o, P.bk.p + (k++) * nkh, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
+                    launch_strm_copy(c, P.strm, P.sbk.v, nmax);
+                }
+                P.jsr.zero(c.stream);
+                sa.n = n;
+                if (ionz) {
+                    G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
+                    sa.key = mix64h(key_step ^ ((uint64_t(n) << 8) | uint64_t(pass)));   // ion_key_slice
+                    sa.bcap = int(P.born_cap);
+                }
+                launch_stream(c, sa, nmax);
+                launch_stream_spectra(c);
+                launch_replace_pred(c, n, extrap ? 1 : 0, wex);
+                launch_march_slice(c, D, n);
+                launch_real_fields_slice(c, n);
             }
-            launch_stream(c, sa, nmax);
-            launch_stream_spectra(c);
-            launch_replace_pred(c, n, extrap ? 1 : 0, wex);
-            launch_march_slice(c, D, n);
-            launch_real_fields_slice(c, n);
+            if (ionz) launch_born_append(c);
+            // half-cell n is final: correct R at slice n+1, keep the change and the current
+            const double q = D * c.wlo_h[size_t(n + 1)];
+            launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
+            have_dl = true;
+            (void)hp;
         }
-        if (ionz) launch_born_append(c);
-        // half-cell n is final: correct R at slice n+1, keep the change and the current
-        const double q = D * c.wlo_h[size_t(n + 1)];
-        launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
-        have_dl = true;
-        (void)hp;
+    } catch (...) {
+        if (graph) {
+            cudaGraph_t gr = nullptr;
+            cudaStreamEndCapture(c.stream, &gr);
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+        }
+        throw;
+    }
+    if (graph) {
+        cudaGraph_t gr = nullptr;
+        G3D_CUDA(cudaStreamEndCapture(c.stream, &gr));
+        bool updated = false;
+        if (P.loop_exec) {
+            cudaGraphExecUpdateResultInfo info;
+            updated = cudaGraphExecUpdate(P.loop_exec, gr, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(P.loop_exec);
+                P.loop_exec = nullptr;
+            }
+        }
+        if (!updated) {
+            const cudaError_t e = cudaGraphInstantiate(&P.loop_exec, gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) { P.loop_exec = nullptr; G3D_CUDA(e); }
+        } else {
+            cudaGraphDestroy(gr);
+        }
+        G3D_CUDA(cudaGraphLaunch(P.loop_exec, c.stream));
     }
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     int flag = 0;

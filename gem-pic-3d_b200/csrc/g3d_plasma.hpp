@@ -79,7 +79,13 @@ struct PlasmaState {
     DevBuf<IonDevC> ion_dev;
     DevBuf<AdkDev> adk_dev;
     std::vector<g3d_particle> joining;         // join the next march at their zeta
+    // the slice loop of a march as one CUDA graph: captured every step, the executable graph updated in place
+    cudaGraphExec_t loop_exec = nullptr;
     PlasmaPtrs ptrs(const Ctx& c) const;
+    PlasmaState() = default;
+    PlasmaState(const PlasmaState&) = delete;
+    PlasmaState& operator=(const PlasmaState&) = delete;
+    ~PlasmaState() { if (loop_exec) cudaGraphExecDestroy(loop_exec); }
 };
 
 // launchers (k_plasma.cu)

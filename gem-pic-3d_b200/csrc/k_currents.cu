@@ -69,7 +69,10 @@ __global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __rest
     const bool live = hc >= 0 && hc <= g.N - 2;
     double wm = 0.25, w0 = 0.5, wp = 0.25, inv = 1.0;
     if (zf && !g.zeta_uniform && live) { wm = 0.25 * g.hcg[hc + 1]; w0 = 0.5 * g.hcg[hc + 2]; wp = 0.25 * g.hcg[hc + 3]; inv = g.hcg[hc + 2]; }
-    for (int e = tid; e < LPC * NX; e += CUR_NT) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (LPC * NX + CUR_NT - 1) / CUR_NT; ++u_) {
+        const int e = tid + u_ * CUR_NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         double v[3] = {0, 0, 0};
         if (live && row < g.ny) {
@@ -91,7 +94,10 @@ __global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __rest
     fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
     const long base = long(hk) * nkh;
-    for (int e = tid; e < LPC * H; e += CUR_NT) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (LPC * H + CUR_NT - 1) / CUR_NT; ++u_) {
+        const int e = tid + u_ * CUR_NT;
+        if (e >= LPC * H) break;
         const int rr = e / H, kx = e - rr * H, row = r0 + rr;
         if (row >= g.ny) continue;
         const int km = (NX - kx) % NX;
@@ -117,7 +123,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
     const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(hk) * g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kx = c0 + c;
         cpx u0 = C(0), u1 = C(0), u2 = C(0);
         if (kx < H) { const long o = base + long(p) * H + kx; u0 = TX[o]; u1 = TY[o]; u2 = TZ[o]; }
@@ -128,7 +137,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
     fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
     fft_line<NY>(s2, ColAddr<CW>{c}, t, g.twy);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kx = c0 + cc;
         if (kx >= H) continue;
         const double f = (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p];

@@ -79,7 +79,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpx u = C(0), v = C(0);
         if (kxi < H) {
@@ -97,7 +100,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -114,7 +120,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx*
     extern __shared__ cpx sm[];
     const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int r = e / H, p = e - r * H, row = r0 + r;
         cpx a = C(0), b = C(0);
         if (row < g.ny) { const long o = base + long(row) * H + p; a = U[o]; b = V[o]; }
@@ -124,7 +133,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx*
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
     const double s = 1.0 / double(g.nk);
-    for (int e = tid; e < LPC * NX; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         const int q = rr * RS + p + (p >> 3);
         const cpx z = s * conj(sm[q]);                                  // u + i v in real space
@@ -134,7 +146,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx*
     }
     __syncthreads();
     fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int rr = e / H, p = e - rr * H, row = r0 + rr;
         if (row >= g.ny) continue;
         const int pm = (NX - p) % NX;
@@ -158,7 +173,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpx u = C(0), v = C(0);
         if (kxi < H) { const long o = base + long(p) * H + kxi; u = U[o]; v = V[o]; }
@@ -168,7 +186,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -199,7 +220,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
     cpx* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     cpx* s0 = sm;
     cpx* s1 = sm + NY * CW;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
         s0[e] = kxi < H ? conj(in0[o]) : C(0);
@@ -209,7 +233,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -231,7 +258,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     cpx* a2 = sm + 2 * LPC * RS;
     const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int r = e / H, p = e - r * H, row = r0 + r;
         cpx v[6] = {C(0), C(0), C(0), C(0), C(0), C(0)};
         if (row < g.ny) {
@@ -250,7 +280,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
     const double s = 1.0 / double(g.nk);
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
-    for (int e = tid; e < LPC * NX; e += NT) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
         const int q = rr * RS + p + (p >> 3);

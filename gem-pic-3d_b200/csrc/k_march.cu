@@ -20,16 +20,10 @@
 namespace g3d {
 
 namespace {
-constexpr int MT = 64;      // threads (modes) per block
-constexpr int MS = 6;       // prefetch depth in slices
 constexpr int MA = 9;       // complex arrays streamed per slice
 constexpr int MC = 3;       // per-slice coefficients streamed with them: w_lo, w_hi, h
-constexpr int SLOT = MA * MT * 2 + MC * MT;   // doubles per ring slot
+constexpr int slot_doubles(int bt) { return MA * bt + MC * bt; }   // doubles per ring slot (one value per lane)
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -39,66 +33,93 @@ template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 }  // namespace
 
-__device__ __forceinline__ cpx widen(cpx a) { return a; }
-__device__ __forceinline__ cpx widen(cpxf a) { return to_d(a); }
-template <class T> __device__ __forceinline__ T narrow(cpx a);
-template <> __device__ __forceinline__ cpx narrow<cpx>(cpx a) { return a; }
-template <> __device__ __forceinline__ cpxf narrow<cpxf>(cpx a) { return to_f(a); }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+template <class Re>
+__device__ __forceinline__ void cp_async_re(double* cell, const Re* src) {
+    if constexpr (sizeof(Re) == 8) cp_async8(cell, src);
+    else cp_async4(cell, src);
+}
+template <class Re>
+__device__ __forceinline__ double ring_re(const double* cell) {
+    if constexpr (sizeof(Re) == 8) return *cell;
+    else return double(*reinterpret_cast<const float*>(cell));
+}
 
-// One thread per mode. Per slice the thread's own loads (9 arrays) and its copies of the slice's coefficients
-// land in its column of a ring of MS slots; the recurrence itself touches only registers and that ring. The
-// denominator 1 + (h/4)(D + h/4) k_perp^2 is inverted one slice ahead, off the chain.
-// T is the storage of E_z, B_z, L and the currents: complex128 (the FP64 form) or complex64 (the mixed form,
-// 8-byte copies into the 16-byte ring cells). R stays complex128, and the recurrence runs in FP64 in both
-// forms: its carried values (level s1 of R, L, E_z, B_z) never leave the registers, so the mixed form only
-// rounds what it stores, and the cancellations in curl R and div R that make E_z, B_z gamma^-2 small are
-// taken in FP64.
-template <class T>
-__global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
+// Two lanes per mode. With E~ = i E_z and B~ = i B_z every coefficient of the march is real (i k_x, i k_y only
+// ever multiply E_z, B_z or come in pairs), so the real parts of (R, L, E~, B~) and their imaginary parts are two
+// independent real recurrences: lane c = 0 carries (Re R, Re L, -Im E_z, -Im B_z), lane c = 1 carries
+// (Im R, Im L, Re E_z, Re B_z); each lane makes the same products and sums as the component c of the complex
+// formulas (i k z contributes +-k times the other component, an exact sign change), so nothing is rounded
+// differently. The pair of a mode sits in adjacent lanes, so a warp's 8-byte loads cover 16 modes contiguously.
+// Per slice each lane streams its 9 values (R_x, R_y, E_z, B_z, j0x, j0y, jkx, jky, jkz) and the slice's
+// coefficients DEPTH slices ahead with per-thread cp.async into its own column of a shared-memory ring; the
+// recurrence touches only registers and that ring. The denominator 1 + (h/4)(D + h/4) k_perp^2 is inverted one
+// slice ahead, off the chain.
+// T is the storage of E_z, B_z, L and the currents: complex128 (the FP64 form) or complex64 (the mixed form).
+// R stays complex128 and the recurrence runs in FP64 in both forms: its carried values never leave the
+// registers, so the mixed form only rounds what it stores, and the cancellations in curl R and div R that make
+// E_z, B_z gamma^-2 small are taken in FP64.
+template <class T, int BT, int DEPTH>
+__global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
                                              T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
                                              const T* __restrict__ j0x, const T* __restrict__ j0y,
                                              const T* __restrict__ jkx, const T* __restrict__ jky,
                                              const T* __restrict__ jkz, double D) {
-    extern __shared__ double ringd[];        // MS slots of [MA arrays][MT] complex, then [MC][MT] double
+    typedef typename RealOf<T>::type Re;
+    extern __shared__ double ringd[];        // DEPTH slots of [MA arrays][BT] values, then [MC][BT] coefficients
     const long nk = g.nkh;
     const int tid = threadIdx.x;
-    const long i = long(blockIdx.x) * MT + tid;
+    const long gt = long(blockIdx.x) * BT + tid;
+    const int c = int(gt & 1);                // component of this lane
+    const long i = gt >> 1;                   // mode
     const bool live = i < nk;
-    const long ii = live ? i : 0;             // idle threads stream mode 0 and store nothing
+    const long ii = live ? i : 0;             // idle lanes stream mode 0 and store nothing
     const int kxi = int(ii % g.H), j = int(ii / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
-    const T* srct[7] = {j0x, jkx, j0y, jky, jkz, Ez, Bz};
-    auto arr = [&](int sl, int k) { return reinterpret_cast<cpx*>(ringd + size_t(sl) * SLOT) + k * MT + tid; };
-    auto coef = [&](int sl, int k) { return ringd + size_t(sl) * SLOT + 2 * MA * MT + k * MT + tid; };
-    // ring cell k: j0x, jkx, j0y, jky, jkz, R_x, R_y, E_z, B_z
-    auto cell = [&](int sl, int k) -> cpx {
-        if (k == 5 || k == 6) return *arr(sl, k);
-        return widen(*reinterpret_cast<const T*>(arr(sl, k)));
-    };
+    const double sgn = c ? 1.0 : -1.0;        // (i z)_c = sgn z_(1-c)
+    // element offsets of the own component (R, L, j_perp) and of the other one (E_z, B_z, j_z)
+    auto own = [&](long o) { return 2 * o + c; };
+    auto oth = [&](long o) { return 2 * o + 1 - c; };
+    const Re* j0xr = reinterpret_cast<const Re*>(j0x);
+    const Re* jkxr = reinterpret_cast<const Re*>(jkx);
+    const Re* j0yr = reinterpret_cast<const Re*>(j0y);
+    const Re* jkyr = reinterpret_cast<const Re*>(jky);
+    const Re* jkzr = reinterpret_cast<const Re*>(jkz);
+    Re* Ezr = reinterpret_cast<Re*>(Ez);
+    Re* Bzr = reinterpret_cast<Re*>(Bz);
+    Re* Lxr = reinterpret_cast<Re*>(Lx);
+    Re* Lyr = reinterpret_cast<Re*>(Ly);
+    double* Rxr = reinterpret_cast<double*>(Rx);
+    double* Ryr = reinterpret_cast<double*>(Ry);
+    auto cell = [&](int sl, int k) { return ringd + size_t(sl) * slot_doubles(BT) + k * BT + tid; };
+    auto coef = [&](int sl, int k) { return ringd + size_t(sl) * slot_doubles(BT) + MA * BT + k * BT + tid; };
+    // ring cells: 0 j0x, 1 jkx, 2 j0y, 3 jky (own), 4 jkz (other), 5 R_x, 6 R_y (own), 7 E_z, 8 B_z (other)
     auto fetch = [&](int n) {                  // slice n (plane n - a) into its ring slot
-        const int sl = (g.b - 1 - n) % MS;
+        const int sl = (g.b - 1 - n) % DEPTH;
         const long o = long(n - g.a) * nk + ii;
-#pragma unroll
-        for (int k = 0; k < MA; ++k) {
-            if (k == 5) cp_async16(arr(sl, k), Rx + o);
-            else if (k == 6) cp_async16(arr(sl, k), Ry + o);
-            else {
-                const T* sp = srct[k < 5 ? k : k - 2] + o;
-                if (sizeof(T) == 16) cp_async16(arr(sl, k), sp);
-                else cp_async8(arr(sl, k), sp);
-            }
-        }
+        cp_async_re(cell(sl, 0), j0xr + own(o));
+        cp_async_re(cell(sl, 1), jkxr + own(o));
+        cp_async_re(cell(sl, 2), j0yr + own(o));
+        cp_async_re(cell(sl, 3), jkyr + own(o));
+        cp_async_re(cell(sl, 4), jkzr + oth(o));
+        cp_async8(cell(sl, 5), Rxr + own(o));
+        cp_async8(cell(sl, 6), Ryr + own(o));
+        cp_async_re(cell(sl, 7), Ezr + oth(o));
+        cp_async_re(cell(sl, 8), Bzr + oth(o));
         cp_async8(coef(sl, 0), g.wlo + n);
         cp_async8(coef(sl, 1), g.whi + n);
         cp_async8(coef(sl, 2), g.hcg + n + 2);
     };
     // upper half-cell of the front slice: plane ns
     const long ou = long(g.ns) * nk + ii;
-    cpx jxu = widen(j0x[ou]) + widen(jkx[ou]), jyu = widen(j0y[ou]) + widen(jky[ou]);
-    cpx upx = widen(jkx[ou]), upy = widen(jky[ou]), upz = widen(jkz[ou]);
-    cpx pRx = C(0), pRy = C(0), pEz = C(0), pBz = C(0), pLx = C(0), pLy = C(0);
+    double jxu = double(j0xr[own(ou)]) + double(jkxr[own(ou)]), jyu = double(j0yr[own(ou)]) + double(jkyr[own(ou)]);
+    double upx = jkxr[own(ou)], upy = jkyr[own(ou)], upz = sgn * double(jkzr[oth(ou)]);
+    double pRx = 0, pRy = 0, pE = 0, pB = 0, pLx = 0, pLy = 0;    // level s1 of the slice above: R, E~, B~, L
 #pragma unroll
-    for (int q = 0; q < MS; ++q) {
+    for (int q = 0; q < DEPTH; ++q) {
         const int n = g.b - 1 - q;
         if (n >= g.a) fetch(n);
         cp_commit();                          // empty groups keep the count of groups per slice uniform
@@ -106,56 +127,59 @@ __global__ void __launch_bounds__(MT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
     double rden = 0;                          // 1 / denominator of the slice being solved
     bool have_rden = false;
     for (int n = g.b - 1; n >= g.a; --n) {
-        cp_wait<MS - 1>();                    // the group of slice n has landed (this thread's own copies)
-        const int sl = (g.b - 1 - n) % MS;
-        const cpx dx0 = cell(sl, 0), dxk = cell(sl, 1), dy0 = cell(sl, 2), dyk = cell(sl, 3);
-        const cpx dzk = cell(sl, 4), rx = cell(sl, 5), ry = cell(sl, 6), ez = cell(sl, 7), bz = cell(sl, 8);
+        cp_wait<DEPTH - 1>();                 // the group of slice n has landed (this lane's own copies)
+        const int sl = (g.b - 1 - n) % DEPTH;
+        const double dx0 = ring_re<Re>(cell(sl, 0)), dxk = ring_re<Re>(cell(sl, 1));
+        const double dy0 = ring_re<Re>(cell(sl, 2)), dyk = ring_re<Re>(cell(sl, 3));
+        const double dzk = sgn * ring_re<Re>(cell(sl, 4));
+        const double rx = *cell(sl, 5), ry = *cell(sl, 6);
+        const double e = sgn * ring_re<Re>(cell(sl, 7)), b = sgn * ring_re<Re>(cell(sl, 8));
         const double wl = *coef(sl, 0), wu = *coef(sl, 1), h = *coef(sl, 2);
         if (!have_rden) rden = 1 / (1 + 0.25 * h * (D + 0.25 * h) * k2);
         // the next slice's inverse denominator, while this slice's chain runs
         double rden_next = 0;
         if (n > g.a) {
-            cp_wait<MS - 2>();
-            const double hn = *coef((sl + 1) % MS, 2);
+            cp_wait<DEPTH - 2>();
+            const double hn = *coef((sl + 1) % DEPTH, 2);
             rden_next = 1 / (1 + 0.25 * hn * (D + 0.25 * hn) * k2);
         }
         const long o = long(n - g.a) * nk + ii;
-        const cpx jxd = dx0 + dxk, jyd = dy0 + dyk;
-        const cpx Jx = wl * jxd + wu * jxu;
-        const cpx Jy = wl * jyd + wu * jyu;
-        const cpx Rsx = rx + D * (ik(kx, ez) + ik(ky, bz)) - D * Jx;
-        const cpx Rsy = ry + D * (ik(ky, ez) - ik(kx, bz)) - D * Jy;
+        const double jxd = dx0 + dxk, jyd = dy0 + dyk;
+        const double Jx = wl * jxd + wu * jxu;
+        const double Jy = wl * jyd + wu * jyu;
+        const double Rsx = rx + D * (kx * e + ky * b) - D * Jx;
+        const double Rsy = ry + D * (ky * e - kx * b) - D * Jy;
         if (n == g.N - 1) {          // front of the window: L = E_z = B_z = 0
             if (live) {
-                Rx[o] = Rsx; Ry[o] = Rsy;
-                Ez[o] = narrow<T>(C(0)); Bz[o] = narrow<T>(C(0)); Lx[o] = narrow<T>(C(0)); Ly[o] = narrow<T>(C(0));
+                Rxr[own(o)] = Rsx; Ryr[own(o)] = Rsy;
+                Ezr[oth(o)] = Re(0); Bzr[oth(o)] = Re(0); Lxr[own(o)] = Re(0); Lyr[own(o)] = Re(0);
             }
-            pRx = Rsx; pRy = Rsy; pEz = C(0); pBz = C(0); pLx = C(0); pLy = C(0);
+            pRx = Rsx; pRy = Rsy; pE = 0; pB = 0; pLx = 0; pLy = 0;
         } else {
-            const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
-            const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
-            const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
-            const cpx Qp = -0.5 * ik(kx, pRx - pLx) + 0.5 * ik(ky, pLy - pRy);
-            const cpx SB = ik(kx, Rsy) + ik(kx, Lsy) - ik(ky, Rsx) - ik(ky, Lsx);
-            const cpx SE = -ik(kx, Rsx) + ik(kx, Lsx) + ik(ky, Lsy) - ik(ky, Rsy);
-            const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) * rden;
-            const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) * rden;
-            const cpx nRx = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn));
-            const cpx nRy = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
-            const cpx nLx = Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn));
-            const cpx nLy = Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn));
+            const double Lsx = pLx - 0.25 * h * (kx * pE - ky * pB) - 0.5 * h * upx;
+            const double Lsy = pLy - 0.25 * h * (kx * pB + ky * pE) - 0.5 * h * upy;
+            const double iCp = 0.5 * ((-kx * (pRy + pLy)) - (-ky * (pRx + pLx)));        // (i C_p)_c
+            const double iQp = -0.5 * (-kx * (pRx - pLx)) + 0.5 * (-ky * (pLy - pRy));    // (i Q_p)_c
+            const double iSB = (-kx * Rsy) + (-kx * Lsy) - (-ky * Rsx) - (-ky * Lsx);     // (i S_B)_c
+            const double iSE = (kx * Rsx) + (-kx * Lsx) + (-ky * Lsy) - (-ky * Rsy);      // (i S_E)_c
+            const double Bn = (pB - 0.5 * h * iCp - 0.25 * h * iSB) * rden;                // (i B_z)_c
+            const double En = (pE - 0.5 * h * iQp - 0.25 * h * iSE - h * upz) * rden;      // (i E_z)_c
+            const double nRx = Rsx + D * (kx * En + ky * Bn);
+            const double nRy = Rsy + D * (ky * En - kx * Bn);
+            const double nLx = Lsx - 0.25 * h * (kx * En - ky * Bn);
+            const double nLy = Lsy - 0.25 * h * (kx * Bn + ky * En);
             if (live) {
-                Ez[o] = narrow<T>(Ezn); Bz[o] = narrow<T>(Bzn); Rx[o] = nRx; Ry[o] = nRy;
-                Lx[o] = narrow<T>(nLx); Ly[o] = narrow<T>(nLy);
+                Ezr[oth(o)] = Re(sgn * En); Bzr[oth(o)] = Re(sgn * Bn); Rxr[own(o)] = nRx; Ryr[own(o)] = nRy;
+                Lxr[own(o)] = Re(nLx); Lyr[own(o)] = Re(nLy);
             }
-            pRx = nRx; pRy = nRy; pEz = Ezn; pBz = Bzn; pLx = nLx; pLy = nLy;
+            pRx = nRx; pRy = nRy; pE = En; pB = Bn; pLx = nLx; pLy = nLy;
         }
         rden = rden_next;
         have_rden = n > g.a;
         // the lower half-cell of this slice is the upper one of the next
         jxu = jxd; jyu = jyd; upx = dxk; upy = dyk; upz = dzk;
-        // refill this slot (its values are consumed above) with the slice MS below
-        const int nn = n - MS;
+        // refill this slot (its values are consumed above) with the slice DEPTH below
+        const int nn = n - DEPTH;
         if (nn >= g.a) fetch(nn);
         cp_commit();
     }
@@ -199,25 +223,36 @@ __global__ void __launch_bounds__(128) k_comoving(Geo g, const cpx* __restrict__
     }
 }
 
+// Block size and ring depth: 32 lanes per block when blocks of 64 would give fewer than two per SM (the
+// 128 x 128 grid has 8,320 half-spectrum modes, 16,640 lanes), else 64. The mixed form streams 44 bytes per lane
+// and slice instead of 72, so it keeps more slices in flight for the same bytes.
+template <class T, int BT, int DEPTH>
+static void march_launch(Ctx& c, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x, const T* j0y, const T* jkx,
+                         const T* jky, const T* jkz, double D) {
+    const unsigned blocks = unsigned((2 * c.nkh + BT - 1) / BT);
+    const size_t smem = size_t(DEPTH) * slot_doubles(BT) * sizeof(double);
+    G3D_CUDA(cudaFuncSetAttribute(k_march<T, BT, DEPTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_march<T, BT, DEPTH><<<blocks, BT, smem, c.stream>>>(c.geo(), Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
+}
+static bool narrow_blocks(const Ctx& c) { return 2 * c.nkh < 2L * 148 * 64; }
+
 void launch_march(Ctx& c, double D) {
     const int tok = c.prof_begin("march");
-    const unsigned blocks = unsigned((c.nkh + MT - 1) / MT);
-    const size_t smem = size_t(MS) * SLOT * sizeof(double);
-    G3D_CUDA(cudaFuncSetAttribute(k_march<cpx>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_march<cpx><<<blocks, MT, smem, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
-                                              c.jkx.p, c.jky.p, c.jkz.p, D);
+    if (narrow_blocks(c))
+        march_launch<cpx, 32, 6>(c, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D);
+    else
+        march_launch<cpx, 64, 6>(c, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D);
     c.check_launch("k_march");
     c.prof_end(tok);
 }
 
 void launch_march_f(Ctx& c, double D) {
     const int tok = c.prof_begin("march");
-    const unsigned blocks = unsigned((c.nkh + MT - 1) / MT);
-    const size_t smem = size_t(MS) * SLOT * sizeof(double);
     MixedBufs& m = c.mx;
-    G3D_CUDA(cudaFuncSetAttribute(k_march<cpxf>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_march<cpxf><<<blocks, MT, smem, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
-                                               m.jkx.p, m.jky.p, m.jkz.p, D);
+    if (narrow_blocks(c))
+        march_launch<cpxf, 32, 10>(c, c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p, m.jkx.p, m.jky.p, m.jkz.p, D);
+    else
+        march_launch<cpxf, 64, 10>(c, c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p, m.jkx.p, m.jky.p, m.jkz.p, D);
     c.check_launch("k_march_f");
     c.prof_end(tok);
 }

@@ -87,7 +87,10 @@ __global__ void __launch_bounds__(NT) k_cur_rows_f(Geo g, const float* __restric
     if (zf && !g.zeta_uniform && live) {
         wm = float(0.25 * g.hcg[hc + 1]); w0 = float(0.5 * g.hcg[hc + 2]); wp = float(0.25 * g.hcg[hc + 3]); inv = float(g.hcg[hc + 2]);
     }
-    for (int e = tid; e < LPC * NX; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         float v[3] = {0, 0, 0};
         if (live && row < g.ny) {
@@ -108,7 +111,10 @@ __global__ void __launch_bounds__(NT) k_cur_rows_f(Geo g, const float* __restric
     fft_line<NX>(a0, RowAddr{r * RS}, t, tw);
     fft_line<NX>(a1, RowAddr{r * RS}, t, tw);
     const long base = long(hk) * nkh;
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int rr = e / H, kx = e - rr * H, row = r0 + rr;
         if (row >= g.ny) continue;
         const int km = (NX - kx) % NX;
@@ -133,7 +139,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols_f(Geo g, cons
     cpxf* s2 = smf + 2 * NY * CW;
     const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long base = long(hk) * g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kx = c0 + c;
         cpxf u0 = Cf(0), u1 = Cf(0), u2 = Cf(0);
         if (kx < H) { const long o = base + long(p) * H + kx; u0 = TX[o]; u1 = TY[o]; u2 = TZ[o]; }
@@ -144,7 +153,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols_f(Geo g, cons
     fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
     fft_line<NY>(s2, ColAddr<CW>{c}, t, tw);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kx = c0 + cc;
         if (kx >= H) continue;
         const float f = (kx == 0 && p == 0 && !keep0) ? 0.0f : float(g.filt[kx] * g.filty[p]);
@@ -202,7 +214,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv_f(Geo g, c
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long nk = g.nkh, base = long(l) * nk;
     const int n = g.a + l;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpxf u = Cf(0), v = Cf(0);
         if (kxi < H) {
@@ -231,7 +246,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv_f(Geo g, c
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -245,7 +263,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows_f(Geo g, const cpxf* __restrict_
     extern __shared__ cpxf smf[];
     const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int r = e / H, p = e - r * H, row = r0 + r;
         cpxf a = Cf(0), b = Cf(0);
         if (row < g.ny) { const long o = base + long(row) * H + p; a = U[o]; b = V[o]; }
@@ -260,7 +281,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows_f(Geo g, const cpxf* __restrict_
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(smf, RowAddr{r * RS}, t, tw);
     const float s = 1.0f / float(g.nk);
-    for (int e = tid; e < LPC * NX; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         const int q = rr * RS + p + (p >> 3);
         const cpxf z = s * conj(smf[q]);
@@ -270,7 +294,10 @@ __global__ void __launch_bounds__(NT) k_sp_rows_f(Geo g, const cpxf* __restrict_
     }
     __syncthreads();
     fft_line<NX>(smf, RowAddr{r * RS}, t, tw);
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int rr = e / H, p = e - rr * H, row = r0 + rr;
         if (row >= g.ny) continue;
         const int pm = (NX - p) % NX;
@@ -291,7 +318,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd_f(Geo g, c
     cpxf* s1 = smf + NY * CW;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long base = long(l) * g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpxf u = Cf(0), v = Cf(0);
         if (kxi < H) { const long o = base + long(p) * H + kxi; u = U[o]; v = V[o]; }
@@ -301,7 +331,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd_f(Geo g, c
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -326,7 +359,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const
     cpxf* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     cpxf* s0 = smf;
     cpxf* s1 = smf + NY * CW;
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
         cpxf a = Cf(0), b = Cf(0);
@@ -341,7 +377,10 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const
     const int c = tid % CW, t = tid / CW;
     fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
     fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
-    for (int e = tid; e < NY * CW; e += nthr) {
+    #pragma unroll 1
+    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * CW) break;
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
@@ -360,7 +399,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
     const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
     const cpxf* in[6] = {W0, W1, W2, W3, W4, W5};
-    for (int e = tid; e < LPC * H; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * H) break;
         const int r = e / H, p = e - r * H, row = r0 + r;
         for (int f = 0; f < 3; ++f) {
             cpxf x = Cf(0), y = Cf(0);
@@ -374,7 +416,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
     for (int f = 0; f < 3; ++f) fft_line<NX>(a[f], RowAddr{r * RS}, t, tw);
     const float s = 1.0f / float(g.nk);
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
-    for (int e = tid; e < LPC * NX; e += NT) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+        const int e = tid + u_ * NT;
+        if (e >= LPC * NX) break;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
         const int q = rr * RS + p + (p >> 3);

@@ -62,8 +62,8 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
         if (comp < 3) E[comp] = v; else B[comp - 3] = v;
     }
 }
-__device__ __forceinline__ double wrapx(const Geo& g, double x) { return fmod(fmod(x, g.Lx) + g.Lx, g.Lx); }
-__device__ __forceinline__ double wrapy(const Geo& g, double y) { return fmod(fmod(y, g.Ly) + g.Ly, g.Ly); }
+__device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
+__device__ __forceinline__ double wrapy(const Geo& g, double y) { return wrap_periodic(y, g.Ly); }
 
 // TSC deposit of f (v, 1) at (x, y) into jsr: jx, jy, jz and the charge of negative (plane 3) or positive
 // (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y)

@@ -52,7 +52,7 @@ __device__ __forceinline__ bool rhs(const PushArgs& c, const St& Y, double z, do
     if (Y.pz < 0.3 * g) return false;
     const double gm = (1 + Y.px * Y.px + Y.py * Y.py) / (g + Y.pz);
     double E[3], B[3], Ee[3], Be[3];
-    gather(c, fmod(fmod(Y.x, c.g.Lx) + c.g.Lx, c.g.Lx), fmod(fmod(Y.y, c.g.Ly) + c.g.Ly, c.g.Ly), Y.zeta, E, B);
+    gather(c, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, E, B);
     c.laser.field(Y.x + c.X0, z, z - (Y.zeta - c.zc), Ee, Be);
 #pragma unroll
     for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
@@ -68,7 +68,7 @@ __device__ __forceinline__ St axpy(const St& a, double h, const St& b) {
 }
 
 // RK4 from z0 to the plane s1 (reference push_one, src/sim_kernels.hpp:98-149).
-__global__ void __launch_bounds__(128) k_push(PushArgs c, PartsDev P, const int32_t* __restrict__ perm, long np, double s0) {
+__global__ void __launch_bounds__(128, 4) k_push(PushArgs c, PartsDev P, const int32_t* __restrict__ perm, long np, double s0) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= np) return;
     const long ip = perm[t];                 // cell order: the warp's particles gather the same planes of F
@@ -103,17 +103,23 @@ __global__ void __launch_bounds__(128) k_push(PushArgs c, PartsDev P, const int3
             const double lim = c.push_phase * Y.pz / (c.laser.kL * (hl > 1e-12 ? hl : 1e-12));
             if (lim < ds) ds = (s1 - z) / ceil((s1 - z) / lim);
         }
-        St k1, k2, k3, k4;
-        if (!(rhs(c, Y, z, qm, k1) && rhs(c, axpy(Y, 0.5 * ds, k1), z + 0.5 * ds, qm, k2) &&
-              rhs(c, axpy(Y, 0.5 * ds, k2), z + 0.5 * ds, qm, k3) && rhs(c, axpy(Y, ds, k3), z + ds, qm, k4))) {
+        // k1 + 2 k2 + 2 k3 + k4 summed left to right as each stage completes (fewer live registers)
+        St k, acc;
+        bool ok = rhs(c, Y, z, qm, k);
+        acc = k;
+        ok = ok && rhs(c, axpy(Y, 0.5 * ds, k), z + 0.5 * ds, qm, k);
+        acc = axpy(acc, 2.0, k);
+        ok = ok && rhs(c, axpy(Y, 0.5 * ds, k), z + 0.5 * ds, qm, k);
+        acc = axpy(acc, 2.0, k);
+        ok = ok && rhs(c, axpy(Y, ds, k), z + ds, qm, k);
+        if (!ok) {
             P.alive[ip] = 0;
             return;
         }
+        acc = axpy(acc, 1.0, k);
         const double w = ds / 6;
-        Y.x += w * (k1.x + 2 * k2.x + 2 * k3.x + k4.x); Y.y += w * (k1.y + 2 * k2.y + 2 * k3.y + k4.y);
-        Y.zeta += w * (k1.zeta + 2 * k2.zeta + 2 * k3.zeta + k4.zeta);
-        Y.px += w * (k1.px + 2 * k2.px + 2 * k3.px + k4.px); Y.py += w * (k1.py + 2 * k2.py + 2 * k3.py + k4.py);
-        Y.pz += w * (k1.pz + 2 * k2.pz + 2 * k3.pz + k4.pz);
+        Y.x += w * acc.x; Y.y += w * acc.y; Y.zeta += w * acc.zeta;
+        Y.px += w * acc.px; Y.py += w * acc.py; Y.pz += w * acc.pz;
         z += ds;
     }
     P.x[ip] = Y.x; P.y[ip] = Y.y; P.zeta[ip] = Y.zeta; P.px[ip] = Y.px; P.py[ip] = Y.py; P.pz[ip] = Y.pz; P.z[ip] = s1;

@@ -132,14 +132,16 @@ class Simulation:
     def march_plasma(self, s0, s1):
         self._c(self.lib.g3d_march_plasma(self.ctx, s0, s1))
 
-    def streaming_particles(self):
+    def streaming_count(self):
+        """Number of streaming particles of the last march (plasma electrons and ions, no copy)."""
         n = C.c_int64()
-        self._c(self.lib.g3d_get_streaming(self.ctx, None, 0, C.byref(n))) if False else None
-        cap = 1 << 26
-        out = np.zeros(0, dtype=abi.PARTICLE_DTYPE)
-        rc = self.lib.g3d_get_streaming(self.ctx, out.ctypes.data, 0, C.byref(n))
+        rc = self.lib.g3d_get_streaming(self.ctx, None, 0, C.byref(n))
         if rc not in (abi.G3D_OK, abi.G3D_ERR_CAPACITY):
             self._c(rc)
+        return n.value
+
+    def streaming_particles(self):
+        n = C.c_int64(self.streaming_count())
         out = np.zeros(n.value, dtype=abi.PARTICLE_DTYPE)
         self._c(self.lib.g3d_get_streaming(self.ctx, out.ctypes.data, n.value, C.byref(n)))
         return out[: n.value]
