@@ -383,8 +383,6 @@ def run_g3d(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg = workload(a.workload, a.nzeta, a.particles)
     forms = ["fp64", "mixed"] if a.precision == "both" else [a.precision]
-    if cfg.plasma is not None and "mixed" in forms:
-        forms = ["fp64"]                      # the mixed form has no streaming plasma in this release
     res = {}
     ref_state = None
     err = None

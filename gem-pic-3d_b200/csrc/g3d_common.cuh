@@ -65,6 +65,13 @@ G3D_HD cpxf mul_mi(cpxf z) { return make_float2(z.y, -z.x); }
 G3D_HD cpx to_d(cpxf a) { return make_double2(a.x, a.y); }
 G3D_HD cpxf to_f(cpx a) { return make_float2(float(a.x), float(a.y)); }
 
+// Storage <-> arithmetic of the two forms: complex128 or complex64 storage, FP64 arithmetic.
+G3D_HD cpx widen(cpx a) { return a; }
+G3D_HD cpx widen(cpxf a) { return to_d(a); }
+template <class T> G3D_HD T narrow(cpx a);
+template <> G3D_HD cpx narrow<cpx>(cpx a) { return a; }
+template <> G3D_HD cpxf narrow<cpxf>(cpx a) { return to_f(a); }
+
 // Real type of a complex type.
 template <class T> struct RealOf;
 template <> struct RealOf<double2> { typedef double type; };

@@ -64,7 +64,6 @@ static void set_precision(Ctx& c, int mode) {
     const bool mixed = mode == G3D_PREC_MIXED;
     if (mixed == c.mixed) return;
     if (c.fields_ready) throw Error(G3D_ERR_STATE, "the precision is set before g3d_init");
-    if (mixed && c.pl) throw Error(G3D_ERR_ARG, "the mixed form has no streaming plasma in this release");
     alloc_spectra(c, mixed);
 }
 
@@ -823,7 +822,6 @@ int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ct
 int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
     return guarded(ctx, [&] {
         if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
-        if (ctx->c.mixed) throw Error(G3D_ERR_ARG, "the mixed form has no streaming plasma in this release");
         g3d::set_plasma(ctx->c, *plasma, ions, nions);
     });
 }

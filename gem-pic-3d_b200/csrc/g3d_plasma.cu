@@ -29,7 +29,8 @@ void StrmBuf::alloc(long n, cudaStream_t s) {
 PlasmaPtrs PlasmaState::ptrs(const Ctx& c) const {
     PlasmaPtrs p;
     p.nkh = c.nkh;
-    p.jkx = c.jkx.p; p.jky = c.jky.p; p.jkz = c.jkz.p;
+    if (c.mixed) { p.jkx = c.mx.jkx.p; p.jky = c.mx.jky.p; p.jkz = c.mx.jkz.p; }
+    else { p.jkx = c.jkx.p; p.jky = c.jky.p; p.jkz = c.jkz.p; }
     p.js0x = js0x.p; p.js0y = js0y.p; p.js0z = js0z.p;
     p.jsn = jsn.p; p.sin_ = jsin.p; p.si0 = jsi0.p; p.pin = jpred.p; p.tmp = jtmp.p; p.dl = dlt.p;
     return p;
@@ -102,6 +103,8 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     const size_t ph = size_t(c.nkh);
     for (DevBuf<cpx>* b : {&pl->js0x, &pl->js0y, &pl->js0z}) b->alloc(size_t(c.ns + 1) * ph, s);
     pl->jsr.alloc(size_t(5) * c.nk, s);
+    pl->jsrf.alloc(size_t(5) * c.nk, s);
+    pl->stepv.alloc(1, s);
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
     pl->bk.alloc(4 * ph, s);
     pl->nstrm_dev.alloc(1, s);
@@ -194,7 +197,6 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     if (P.s.cap < need) {
         const long n = need + need / 8 + 64;
         P.s.alloc(n, c.stream);
-        P.sbk.alloc(n, c.stream);
     }
     if (cap > 0 && P.bn.cap < cap) P.bn.alloc(cap, c.stream);
     P.strm = P.s.v;
@@ -258,123 +260,104 @@ static uint64_t mix64h(uint64_t z) {
     return z ^ (z >> 31);
 }
 
+static void real_fields_slice(Ctx& c, int l) {
+    if (c.mixed) launch_real_fields_slice_f(c, l);
+    else launch_real_fields_slice(c, l);
+}
+
 void march_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
     const double Delta = s1 - s0, D = 0.5 * Delta;
-    const long nkh = c.nkh;
     const int N = c.N;
     const int nhi = N - 2;
-    auto hpl = [&](int m) { return long(m - c.a + 1) * nkh; };
     load_plasma(c, s0, s1);
     const bool extrap = P.cfg.predictor_extrapolate != 0;
     std::vector<double> cen(size_t(N - 1));
     for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
-    cpx* pin = P.jpred.p;
-    cpx* tmp = P.jtmp.p;
-    // The slice loop issues some 17 operations per half-cell and pass (about 35,000 for 2,048 slices and two
-    // passes). Launched one by one, the host's launch rate would bound the march; captured into one graph they
-    // are submitted at once and run back to back. The capture replays exactly the launches below (no kernel
-    // differs); it is skipped while per-kernel events are recorded.
-    const bool graph = !c.profiling;
-    if (graph) G3D_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
-    try {
-        auto copy3 = [&](cpx* dst, int m) {           // dst <- js0 of half-cell m
-            for (int k = 0; k < 3; ++k) {
-                const cpx* src = (k == 0 ? P.js0x.p : k == 1 ? P.js0y.p : P.js0z.p) + hpl(m);
-                G3D_CUDA(cudaMemcpyAsync(dst + k * nkh, src, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-            }
-        };
+    // the values that change from step to step go to the device; the captured loop reads them there
+    const StepVals stv{s1, s1 + (P.cfg.trap_advance - 1) * Delta, c.X0, c.Y0,
+                       mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep))};   // ion_key_step
+    G3D_CUDA(cudaMemcpyAsync(P.stepv.p, &stv, sizeof(StepVals), cudaMemcpyHostToDevice, c.stream));
+    const bool ionz = P.born_cap > 0;
+    const int passes = P.cfg.iterations;
+    // The slice loop is some 20 launches per half-cell (about 41,000 for 2,048 slices and two passes). Launched
+    // one by one, the host's launch rate would bound the march; as one CUDA graph they run back to back. The
+    // graph is captured once and launched every step; it is captured again only when something it holds by value
+    // changes (a buffer moved, the capacity of the freed-electron list, the step length). While per-kernel events
+    // are recorded the loop is launched directly.
+    uint64_t key = 1469598103934665603ULL;
+    auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
+    auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
+    const PlasmaPtrs pp = P.ptrs(c);
+    mixk(ptr(c.F.p)); mixk(ptr(P.strm.x)); mixk(ptr(P.born.x)); mixk(uint64_t(P.s.cap)); mixk(uint64_t(P.born_cap));
+    mixk(uint64_t(passes)); mixk(uint64_t(c.mixed)); mixk(ptr(c.Rx.p));
+    mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
+    uint64_t dbits;
+    std::memcpy(&dbits, &Delta, sizeof dbits);
+    mixk(dbits);
+    auto issue = [&]() {
         bool have_dl = false;
-        P.jpred.zero(c.stream);
         // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
-        copy3(tmp, N - 2);
-        launch_replace(c, N - 2, pin, tmp);
+        launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
-        launch_real_fields_slice(c, N - 1);
+        real_fields_slice(c, N - 1);
 
         StreamArgs sa;
-        sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.X0 = c.X0; sa.Y0 = c.Y0; sa.zc = c.P.zeta_center;
-        sa.Delta = Delta; sa.s1 = s1; sa.sTrap = s1 + (P.cfg.trap_advance - 1) * Delta; sa.vz_beam = P.cfg.vz_beam;
-        sa.J = P.jsr.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p; sa.bcap = 0; sa.key = 0;
-        const bool ionz = P.born_cap > 0;
-        const uint64_t key_step = mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep));   // ion_key_step
-        const int passes = P.cfg.iterations;
-        const long nmax = P.nstrm + P.born_cap;              // upper bound of the streaming particles of this march
+        sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
+        sa.Delta = Delta; sa.vz_beam = P.cfg.vz_beam;
+        sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p;
+        sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
         for (int n = nhi; n >= c.a; --n) {
-            const long hp = hpl(n);
-            G3D_CUDA(cudaMemcpyAsync(P.jsin.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-            G3D_CUDA(cudaMemcpyAsync(P.jsi0.p, pin, size_t(3 * nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-            if (n >= 1) {                                    // start of the prediction of half-cell n-1: its level s0
-                P.jpred.zero(c.stream);
-                copy3(tmp, n - 1);
-                launch_replace(c, n - 1, pin, tmp);
-            }
-            if (passes > 1) {
-                const long o = long(n - c.a) * nkh;
-                int k = 0;
-                for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
-                    G3D_CUDA(cudaMemcpyAsync(P.bk.p + (k++) * nkh, a->p + o, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-                launch_strm_copy(c, P.sbk.v, P.strm, nmax);
-            }
-            const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl) ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+            // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
+            launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
+            const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl)
+                                   ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
             for (int pass = 0; pass < passes; ++pass) {
-                if (pass > 0) {
-                    const long o = long(n - c.a) * nkh;
-                    int k = 0;
-                    for (DevBuf<cpx>* a : {&c.Rx, &c.Ry, &c.Ez, &c.Bz})
-                        G3D_CUDA(cudaMemcpyAsync(a->p + o, P.bk.p + (k++) * nkh, size_t(nkh) * sizeof(cpx), cudaMemcpyDeviceToDevice, c.stream));
-                    launch_strm_copy(c, P.strm, P.sbk.v, nmax);
-                }
-                P.jsr.zero(c.stream);
+                launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
-                if (ionz) {
-                    G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
-                    sa.key = mix64h(key_step ^ ((uint64_t(n) << 8) | uint64_t(pass)));   // ion_key_slice
-                    sa.bcap = int(P.born_cap);
-                }
-                launch_stream(c, sa, nmax);
+                sa.pass = pass;
+                sa.dry = pass + 1 < passes ? 1 : 0;
+                launch_stream(c, sa);
                 launch_stream_spectra(c);
                 launch_replace_pred(c, n, extrap ? 1 : 0, wex);
                 launch_march_slice(c, D, n);
-                launch_real_fields_slice(c, n);
+                real_fields_slice(c, n);
             }
             if (ionz) launch_born_append(c);
             // half-cell n is final: correct R at slice n+1, keep the change and the current
             const double q = D * c.wlo_h[size_t(n + 1)];
             launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
             have_dl = true;
-            (void)hp;
         }
-    } catch (...) {
-        if (graph) {
+    };
+    PlasmaState::LoopGraph* hit = nullptr;
+    for (auto& l : P.loops) if (l.key == key) hit = &l;
+    if (c.profiling) {
+        issue();
+    } else if (hit) {
+        c.launches += hit->launches;
+        G3D_CUDA(cudaGraphLaunch(hit->exec, c.stream));
+    } else {
+        if (P.loops.size() >= 4) { cudaGraphExecDestroy(P.loops.front().exec); P.loops.erase(P.loops.begin()); }
+        const long l0 = c.launches;
+        G3D_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeRelaxed));
+        try {
+            issue();
+        } catch (...) {
             cudaGraph_t gr = nullptr;
             cudaStreamEndCapture(c.stream, &gr);
             if (gr) cudaGraphDestroy(gr);
             cudaGetLastError();
+            throw;
         }
-        throw;
-    }
-    if (graph) {
         cudaGraph_t gr = nullptr;
         G3D_CUDA(cudaStreamEndCapture(c.stream, &gr));
-        bool updated = false;
-        if (P.loop_exec) {
-            cudaGraphExecUpdateResultInfo info;
-            updated = cudaGraphExecUpdate(P.loop_exec, gr, &info) == cudaSuccess;
-            if (!updated) {
-                cudaGetLastError();
-                cudaGraphExecDestroy(P.loop_exec);
-                P.loop_exec = nullptr;
-            }
-        }
-        if (!updated) {
-            const cudaError_t e = cudaGraphInstantiate(&P.loop_exec, gr, 0);
-            cudaGraphDestroy(gr);
-            if (e != cudaSuccess) { P.loop_exec = nullptr; G3D_CUDA(e); }
-        } else {
-            cudaGraphDestroy(gr);
-        }
-        G3D_CUDA(cudaGraphLaunch(P.loop_exec, c.stream));
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        G3D_CUDA(e);
+        P.loops.push_back(PlasmaState::LoopGraph{key, ex, c.launches - l0});
+        G3D_CUDA(cudaGraphLaunch(ex, c.stream));
     }
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     int flag = 0;
@@ -402,7 +385,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
         set_particles(c, keep.data(), long(keep.size()));
     }
     // the sponge damps R - R_b with the bound field of the beam list only: jkz -= js0z
-    launch_axpy_c(c, c.jkz.p, P.js0z.p, -1.0, size_t(c.ns + 1) * c.nkh);
+    if (c.mixed) launch_axpy_fc(c, c.mx.jkz.p, P.js0z.p, -1.0, size_t(c.ns + 1) * c.nkh);
+    else launch_axpy_c(c, c.jkz.p, P.js0z.p, -1.0, size_t(c.ns + 1) * c.nkh);
 }
 
 // The beam particles that became slower than vz_min stream in the current march (collect_restreaming,

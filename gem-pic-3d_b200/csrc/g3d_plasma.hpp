@@ -22,24 +22,34 @@ struct StrmDev {
     uint64_t* id;
 };
 
+// The values of a march that change from step to step. The kernels read them from device memory, so the graph
+// of the slice loop, captured once, stays valid for every step.
+struct StepVals {
+    double s1, sTrap, X0, Y0;
+    uint64_t key_step;         // ion_key_step(seed, istep)
+};
+
 struct StreamArgs {
     const float* __restrict__ F;
     Geo g;
     LaserDev laser;
-    double X0, Y0, zc, Delta, s1, sTrap, vz_beam;
-    int n;
+    const StepVals* sv;
+    double zc, Delta, vz_beam;
+    int n, pass;
     double* J;                 // jsr: jx, jy, jz, rho-, rho+ of the half-cell (real planes)
+    float* Jf;                 // the same planes in FP32 (the mixed form)
     const IonDevC* ions;
     const AdkDev* adk;
     StrmDev born;
     int* bcnt;
     int bcap;
-    uint64_t key;              // ion_key_slice(ion_key_step(seed, istep), n, pass)
+    int dry;                   // a predictor pass: deposit and ionize, keep the particles as they were
 };
 
 struct PlasmaPtrs {
     long nkh;
-    cpx *jkx, *jky, *jkz, *js0x, *js0y, *js0z, *jsn, *sin_, *si0, *pin, *tmp, *dl;
+    void *jkx, *jky, *jkz;     // the window's jk: complex128, or complex64 in the mixed form
+    cpx *js0x, *js0y, *js0z, *jsn, *sin_, *si0, *pin, *tmp, *dl;
 };
 
 struct IonSpec {
@@ -68,9 +78,10 @@ struct PlasmaState {
     // of one half-cell (jsr real, jsn spectra), the parts of jk held as predictions, backups
     DevBuf<cpx> js0x, js0y, js0z;              // ns+1 half planes
     DevBuf<double> jsr;                        // 5 real planes
+    DevBuf<float> jsrf;                        // the same in FP32 (the mixed form)
     DevBuf<cpx> jsn, jsin, jpred, jtmp, jsi0, dlt, tsp;   // 3 half planes each
     DevBuf<cpx> bk;                            // 4 half planes: R_x, R_y, E_z, B_z of the slice
-    StrmBuf s, sbk, bn;                        // streaming particles, their backup, the freed electrons
+    StrmBuf s, bn;                             // streaming particles, the freed electrons
     StrmDev strm{}, born{};
     long nstrm = 0;                            // host copy (exact at the start of the march)
     long born_cap = 0, fresh_last = 0, trapped_total = 0, restreamed_total = 0;
@@ -79,24 +90,28 @@ struct PlasmaState {
     DevBuf<IonDevC> ion_dev;
     DevBuf<AdkDev> adk_dev;
     std::vector<g3d_particle> joining;         // join the next march at their zeta
-    // the slice loop of a march as one CUDA graph: captured every step, the executable graph updated in place
-    cudaGraphExec_t loop_exec = nullptr;
+    // the slice loop of a march as CUDA graphs, keyed by what they hold by value (two alternate: the j0 / jk
+    // buffers swap every step); captured again only when a buffer moved
+    struct LoopGraph { uint64_t key; cudaGraphExec_t exec; long launches; };
+    std::vector<LoopGraph> loops;
+    DevBuf<StepVals> stepv;
     PlasmaPtrs ptrs(const Ctx& c) const;
     PlasmaState() = default;
     PlasmaState(const PlasmaState&) = delete;
     PlasmaState& operator=(const PlasmaState&) = delete;
-    ~PlasmaState() { if (loop_exec) cudaGraphExecDestroy(loop_exec); }
+    ~PlasmaState() { for (auto& l : loops) cudaGraphExecDestroy(l.exec); }
 };
 
 // launchers (k_plasma.cu)
-void launch_stream(Ctx& c, const StreamArgs& a, long nmax);
+void launch_stream(Ctx& c, const StreamArgs& a);
+void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
+void launch_pass_prologue(Ctx& c, int n, int restore);
 void launch_stream_spectra(Ctx& c);
 void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw);
 void launch_replace_pred(Ctx& c, int n, int extrap, double w);
 void launch_correct(Ctx& c, int n, double q, int own);
 void launch_march_slice(Ctx& c, double D, int n);
 void launch_born_append(Ctx& c);
-void launch_strm_copy(Ctx& c, const StrmDev& dst, const StrmDev& src, long nmax);
 void launch_real_fields_slice(Ctx& c, int l);
 
 }  // namespace g3d

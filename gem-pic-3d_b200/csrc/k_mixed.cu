@@ -350,10 +350,11 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const
                                                                     const cpxf* __restrict__ Ly, const cpxf* __restrict__ Ez,
                                                                     const cpxf* __restrict__ Bz, cpxf* __restrict__ W0,
                                                                     cpxf* __restrict__ W1, cpxf* __restrict__ W2,
-                                                                    cpxf* __restrict__ W3, cpxf* __restrict__ W4, cpxf* __restrict__ W5) {
+                                                                    cpxf* __restrict__ W3, cpxf* __restrict__ W4, cpxf* __restrict__ W5,
+                                                                    int l0) {
     using S = FftShape<NY>;
     extern __shared__ cpxf smf[];
-    const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z, H = g.H;
+    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z, H = g.H;
     const long base = long(l) * g.nkh;
     cpxf* out0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
     cpxf* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
@@ -391,12 +392,12 @@ template <int NX>
 __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict__ tw, const cpxf* __restrict__ W0,
                                                  const cpxf* __restrict__ W1, const cpxf* __restrict__ W2,
                                                  const cpxf* __restrict__ W3, const cpxf* __restrict__ W4,
-                                                 const cpxf* __restrict__ W5, float* __restrict__ F) {
+                                                 const cpxf* __restrict__ W5, float* __restrict__ F, int l0) {
     using S = FftShape<NX>;
     constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpxf smf[];
     cpxf* a[3] = {smf, smf + LPC * RS, smf + 2 * LPC * RS};
-    const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
+    const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
     const cpxf* in[6] = {W0, W1, W2, W3, W4, W5};
     #pragma unroll
@@ -460,6 +461,10 @@ __global__ void k_rotate_f(Geo g, cpxf* __restrict__ p, long n, double sx, doubl
         const double ph = g.kxs[i % g.H] * sx + (nys ? g.kys[i / g.H] * sy : 0.0);
         p[idx] = to_f(to_d(p[idx]) * C(cos(ph), sin(ph)));
     }
+}
+__global__ void k_axpy_fc(cpxf* __restrict__ y, const cpx* __restrict__ x, double a, long n) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x)
+        y[i] = to_f(to_d(y[i]) + a * x[i]);
 }
 __global__ void k_copy_f(cpxf* __restrict__ y, const cpxf* __restrict__ x, long n) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) y[i] = x[i];
@@ -553,31 +558,37 @@ void launch_sponge_f(Ctx& c) {
     G3D_DISPATCH_N(c.ny, NY, sp_cols_fwd_f<NY>(c));
 }
 template <int NY>
-static void rf_cols_f(Ctx& c) {
+static void rf_cols_f(Ctx& c, int l0, int nl) {
     const size_t smem = size_t(2) * NY * CW * sizeof(cpxf);
     allow_smem(k_rf_cols_f<NY>, smem);
-    const int tok = c.prof_begin("real_cols");
+    const int tok = c.prof_begin(nl == 1 ? "real_cols_slice" : "real_cols");
     auto& m = c.mx;
-    k_rf_cols_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(c.ns), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), m.twy.p, c.Rx.p, c.Ry.p, m.Lx.p, m.Ly.p, m.Ez.p, m.Bz.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p);
+    k_rf_cols_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(nl), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), m.twy.p, c.Rx.p, c.Ry.p, m.Lx.p, m.Ly.p, m.Ez.p, m.Bz.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p,
+        l0);
     c.check_launch("k_rf_cols_f");
     c.prof_end(tok);
 }
 template <int NX>
-static void rf_rows_f(Ctx& c) {
+static void rf_rows_f(Ctx& c, int l0, int nl) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpxf);
     allow_smem(k_rf_rows_f<NX>, smem);
-    const int tok = c.prof_begin("real_rows");
+    const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     auto& m = c.mx;
-    k_rf_rows_f<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(
-        c.geo(), m.twx.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p, c.F.p);
+    k_rf_rows_f<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
+        c.geo(), m.twx.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p, c.F.p, l0);
     c.check_launch("k_rf_rows_f");
     c.prof_end(tok);
 }
 void launch_real_fields_f(Ctx& c) {
-    G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c));
-    G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c));
+    G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c, 0, c.ns));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, 0, c.ns));
+}
+// E and B of one slice (plane l) of the mixed form (the real fields of one slice of the plasma march)
+void launch_real_fields_slice_f(Ctx& c, int l) {
+    G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c, l, 1));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, l, 1));
 }
 void launch_half_to_full_f(Ctx& c, const cpxf* half, cpx* full, long planes) {
     k_half_to_full_f<<<ew_blocks(planes * c.nk), 256, 0, c.stream>>>(c.geo(), half, full, planes);
@@ -591,6 +602,11 @@ void launch_rotate_f(Ctx& c, cpxf* p, size_t n, double sx, double sy, int nys) {
     if (!n) return;
     k_rotate_f<<<ew_blocks(long(n)), 256, 0, c.stream>>>(c.geo(), p, long(n), sx, sy, nys);
     c.check_launch("k_rotate_f");
+}
+void launch_axpy_fc(Ctx& c, cpxf* y, const cpx* x, double a, size_t n) {
+    if (!n) return;
+    k_axpy_fc<<<ew_blocks(long(n)), 256, 0, c.stream>>>(y, x, a, long(n));
+    c.check_launch("k_axpy_fc");
 }
 void launch_copy_f(Ctx& c, cpxf* y, const cpxf* x, size_t n) {
     if (!n) return;

@@ -13,8 +13,11 @@
 //                  js0(n-1) + d + w (d - dl), d = jsn - js0(n) (sim_plasma.cpp:339-351)
 //   k_march_slice  the march of the modes of slice n (march_point, src/sim_kernels.hpp:173-210)
 //   real fields of slice n: the column and row kernels of k_fields.cu on one plane
+// A pass before the last (the predictor) deposits, transforms and marches like the last one but leaves the
+// particles unchanged (StreamArgs::dry), so every pass starts from the same particle state without a copy.
 // After the passes: k_correct (R of slice n+1 corrected for the prediction it used; dl, js0 updated,
 // sim_plasma.cpp:381-403) and k_born_append (the freed electrons join the march).
+#include <type_traits>
 #include "g3d_plasma.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -25,8 +28,8 @@ namespace g3d {
 __device__ __forceinline__ void boris(double& ux, double& uy, double& uz, const double E[3], const double B[3], double qm, double dt) {
     const double qh = 0.5 * qm * dt;
     const double umx = ux + qh * E[0], umy = uy + qh * E[1], umz = uz + qh * E[2];
-    const double gm = sqrt(1.0 + umx * umx + umy * umy + umz * umz);
-    const double tx = qh * B[0] / gm, ty = qh * B[1] / gm, tz = qh * B[2] / gm;
+    const double qg = qh / sqrt(1.0 + umx * umx + umy * umy + umz * umz);     // q dt / (2 m gamma-)
+    const double tx = qg * B[0], ty = qg * B[1], tz = qg * B[2];
     const double t2 = tx * tx + ty * ty + tz * tz;
     const double upx = umx + (umy * tz - umz * ty), upy = umy + (umz * tx - umx * tz), upz = umz + (umx * ty - umy * tx);
     const double sf = 2.0 / (1.0 + t2);
@@ -34,7 +37,9 @@ __device__ __forceinline__ void boris(double& ux, double& uy, double& uz, const 
     ux = vx + qh * E[0]; uy = vy + qh * E[1]; uz = vz + qh * E[2];
 }
 
-// grid fields of the F planes (TSC in x, y, linear in zeta) as in the beam push
+// grid fields of the F planes (TSC in x, y, linear in zeta) as in the beam push. F32 (the mixed form): the
+// weights and the sums in FP32; else FP64 arithmetic on the float data.
+template <bool F32>
 __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
     E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
     const Geo& g = c.g;
@@ -47,18 +52,23 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
     tsc_periodic(x, g.dx, g.nx, ix, wx);
     tsc_periodic(y, g.dy, g.ny, jn, wn);
     const long nk = g.nk;
+    typedef typename std::conditional<F32, float, double>::type R;
+    R w9[9];
+    int k9[9];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) { w9[3 * j + i] = R(wx[i] * wn[j]); k9[3 * j + i] = jn[j] * g.nx + ix[i]; }
+    // both slices summed with the TSC weights, then interpolated in zeta
+    const R f1 = R(fz), f0 = R(1 - fz);
 #pragma unroll
     for (int comp = 0; comp < 6; ++comp) {
         const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
         const float* p1 = p0 + nk;
-        double v = 0;
+        R v0 = 0, v1 = 0;
 #pragma unroll
-        for (int j = 0; j < 3; ++j)
-#pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const long k = long(jn[j]) * g.nx + ix[i];
-                v += wx[i] * wn[j] * ((1 - fz) * double(p0[k]) + fz * double(p1[k]));
-            }
+        for (int q = 0; q < 9; ++q) { v0 += w9[q] * R(p0[k9[q]]); v1 += w9[q] * R(p1[k9[q]]); }
+        const double v = double(f0 * v0 + f1 * v1);
         if (comp < 3) E[comp] = v; else B[comp - 3] = v;
     }
 }
@@ -66,7 +76,8 @@ __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_pe
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return wrap_periodic(y, g.Ly); }
 
 // TSC deposit of f (v, 1) at (x, y) into jsr: jx, jy, jz and the charge of negative (plane 3) or positive
-// (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y)
+// (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y). F32: into the FP32 planes.
+template <bool F32>
 __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
     const Geo& g = c.g;
     int ix_[3], jn[3]; double wx[3], wn[3];
@@ -80,16 +91,22 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
         for (int u = 0; u < 3; ++u) {
             const long k = long(jn[v]) * g.nx + ix_[u];
             const double w = f * wx[u] * wn[v] * ia0;
-            atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
-            atomicAdd(&c.J[cq + k], w);
+            if constexpr (F32) {
+                atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[nk + k], float(w * vy));
+                atomicAdd(&c.Jf[2 * nk + k], float(w * vz)); atomicAdd(&c.Jf[cq + k], float(w));
+            } else {
+                atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
+                atomicAdd(&c.J[cq + k], w);
+            }
         }
 }
 
 // |E| of the grid and the wave at (x, y), lab z, slice position zeta (field_abs, sim_stream.hpp:67-74)
+template <bool F32>
 __device__ __forceinline__ double field_abs(const StreamArgs& c, double x, double y, double z, double zeta) {
     double E[3], B[3], Ee[3], Be[3];
-    sgather(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);
-    c.laser.field(x + c.X0, z, z - (zeta - c.zc), Ee, Be);
+    sgather<F32>(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);
+    c.laser.field(x + c.sv->X0, z, z - (zeta - c.zc), Ee, Be);
     for (int k = 0; k < 3; ++k) E[k] += Ee[k];
     return sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
 }
@@ -114,7 +131,8 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
     const int sp = S.sp[i];
     const IonDevC& I = c.ions[sp - SP_ION];
     if (!I.ionizing || (E1 < I.Emin && E0 < I.Emin)) return;
-    const uint64_t base = mix64(c.key ^ mix64(S.id[i]));          // ion_key_particle(key_slice, id)
+    const uint64_t key = mix64(c.sv->key_step ^ ((uint64_t(c.n) << 8) | uint64_t(c.pass)));   // ion_key_slice
+    const uint64_t base = mix64(key ^ mix64(S.id[i]));            // ion_key_particle(key_slice, id)
     int Z = int(floor(S.q[i] + 0.5));
     const int Z0 = Z;
     unsigned draw = 0;
@@ -134,43 +152,53 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
             Bn.alive[j] = 1; Bn.sp[j] = SP_FREED + (sp - SP_ION); Bn.id[j] = S.id[i];
         }
     }
-    if (Z != Z0) { S.q[i] = Z; S.qm[i] = Z / I.mass; }
+    if (Z != Z0 && !c.dry) { S.q[i] = Z; S.qm[i] = Z / I.mass; }
 }
 
-// one streaming particle through half-cell n (stream_one, sim_stream.hpp:104-171)
-__global__ void __launch_bounds__(128) k_stream(StreamArgs c, StrmDev S, const long* __restrict__ nstrm) {
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= *nstrm) return;                // the launch covers the freed electrons that may join
+// The deposit of one particle in one half-cell: f (v_x, v_y, v_z, 1) at (x, y) (stream_deposit)
+struct DepReq {
+    double x, y, f, vx, vy, vz;
+    bool on;
+};
+
+// one streaming particle through half-cell n (stream_one, sim_stream.hpp:104-171); its deposit is returned to
+// the caller, the rare second deposit of a trapped particle that joins the beam list is made here. A predictor
+// pass (c.dry) computes and deposits the same but leaves the particle as it was, so every pass of a half-cell
+// starts from the same state without a copy of the particles.
+template <bool F32>
+__device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
+    DepReq d{0, 0, 0, 0, 0, 0, false};
     const Geo& g = c.g;
     const int n = c.n;
     const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn;
     int alive = S.alive[i];
     if (alive == 6) {                 // waiting: joins the march inside the half-cell that holds its zeta
-        if (S.zeta[i] > zn) { alive = 1; S.alive[i] = 1; }
-        else return;
+        if (S.zeta[i] > zn) { alive = 1; if (!c.dry) S.alive[i] = 1; }
+        else return d;
     }
-    if (alive != 1) return;
+    if (alive != 1) return d;
     const double zeta = S.zeta[i];
     const double hl = zeta >= zn1 - 1e-9 * h ? h : (zeta - zn > 0 ? zeta - zn : 0.0);
     const int sp = S.sp[i];
     const bool ion = sp >= SP_ION && sp < SP_FREED;
     if (ion && !c.ions[sp - SP_ION].mobile) {        // fixed ion: its charge, then the ionization
         const double f = S.q[i] * S.w[i] * hl / (c.Delta * h * g.dx);
-        if (f != 0) sdeposit(c, S.x[i], S.y[i], f, 0, 0, 0);
-        const double E1 = field_abs(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs(c, S.x[i], S.y[i], S.z[i], zn);
-        S.zeta[i] = zn;
+        if (f != 0) d = DepReq{S.x[i], S.y[i], f, 0, 0, 0, true};
+        const double E1 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zn);
+        if (!c.dry) S.zeta[i] = zn;
         ionize(c, S, i, E1, E0, hl);
-        return;
+        return d;
     }
     const double x = S.x[i], y = S.y[i], z = S.z[i], px = S.px[i], py = S.py[i], pz = S.pz[i], qm = S.qm[i];
-    const double g0 = sqrt(1 + px * px + py * py + pz * pz);
+    const double g0 = sqrt(1 + px * px + py * py + pz * pz), ig0 = 1 / g0;
     const double omv0 = (1 + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
     const double dt0 = hl / omv0;
-    const double xm = x + 0.5 * dt0 * px / g0, ym = y + 0.5 * dt0 * py / g0;
-    const double zm = z + 0.5 * dt0 * pz / g0, zetam = zeta - 0.5 * hl;
+    const double hd = 0.5 * dt0 * ig0;
+    const double xm = x + hd * px, ym = y + hd * py;
+    const double zm = z + hd * pz, zetam = zeta - 0.5 * hl;
     double E[3], B[3], Ee[3], Be[3];
-    sgather(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
-    c.laser.field(xm + c.X0, zm, zm - (zetam - c.zc), Ee, Be);
+    sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
+    c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
     for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
     double ux = px, uy = py, uz = pz;
     boris(ux, uy, uz, E, B, qm, dt0);
@@ -179,42 +207,63 @@ __global__ void __launch_bounds__(128) k_stream(StreamArgs c, StrmDev S, const l
     ux = px; uy = py; uz = pz;
     boris(ux, uy, uz, E, B, qm, dt);
     g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
-    double vx = 0.5 * (px / g0 + ux / g1), vy = 0.5 * (py / g0 + uy / g1), vz = 0.5 * (pz / g0 + uz / g1);
+    double ig1 = 1 / g1;
+    double vx = 0.5 * (px * ig0 + ux * ig1), vy = 0.5 * (py * ig0 + uy * ig1), vz = 0.5 * (pz * ig0 + uz * ig1);
     double zeta_end = zn;
     bool trapped = false;
-    if (z + vz * dt >= c.sTrap) {     // advanced trap_advance steps inside this half-cell: trapped
+    const double sTrap = c.sv->sTrap;
+    if (z + vz * dt >= sTrap) {       // advanced trap_advance steps inside this half-cell: trapped
         const double vv = vz > 1e-3 ? vz : 1e-3;
-        const double dtp = (c.sTrap - z) / vv > 0 ? (c.sTrap - z) / vv : 0.0;
+        const double dtp = (sTrap - z) / vv > 0 ? (sTrap - z) / vv : 0.0;
         ux = px; uy = py; uz = pz;
         boris(ux, uy, uz, E, B, qm, dtp);
         g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
-        vx = 0.5 * (px / g0 + ux / g1); vy = 0.5 * (py / g0 + uy / g1); vz = 0.5 * (pz / g0 + uz / g1);
+        ig1 = 1 / g1;
+        vx = 0.5 * (px * ig0 + ux * ig1); vy = 0.5 * (py * ig0 + uy * ig1); vz = 0.5 * (pz * ig0 + uz * ig1);
         dt = dtp;
         zeta_end = zeta - (1 - vz) * dtp;
         trapped = true;
     }
     const double xn = x + vx * dt, yn = y + vy * dt;
-    S.x[i] = xn; S.y[i] = yn;
-    S.z[i] = trapped ? c.s1 : z + vz * dt;
-    S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
-    S.zeta[i] = zeta_end;
+    if (!c.dry) {
+        S.x[i] = xn; S.y[i] = yn;
+        S.z[i] = trapped ? c.sv->s1 : z + vz * dt;
+        S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
+        S.zeta[i] = zeta_end;
+    }
     const double q = S.q[i], w = S.w[i];
     const double f = q * w * dt / (c.Delta * h * g.dx);
-    if (f != 0) sdeposit(c, 0.5 * (x + xn), 0.5 * (y + yn), f, vx, vy, vz);
+    if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, vx, vy, vz, true};
     if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
-        ionize(c, S, i, field_abs(c, xm, ym, zm, zeta), field_abs(c, xm, ym, zm, zn), dt);
+        ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), dt);
     if (trapped) {
-        S.alive[i] = 5;
-        const double vze = uz / g1;
+        if (!c.dry) S.alive[i] = 5;
+        const double vze = uz * ig1;
         if (vze >= c.vz_beam)         // joins the beam list: its beam current of level s1 from now on
-            sdeposit(c, xn, yn, q * w / (h * g.dx * vze), ux / g1, uy / g1, vze);
+            sdeposit<F32>(c, xn, yn, q * w / (h * g.dx * vze), ux * ig1, uy * ig1, vze);
+    }
+    return d;
+}
+
+// One thread per streaming particle, a fixed grid striding over their count (which freed electrons raise; it is
+// read on the device). The deposit adds go straight to global memory: without a use of the old value they are
+// fire-and-forget reductions in L2, cheaper for the SM than accumulating in shared memory the many adds that
+// neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers in FP32 arithmetic
+// and the deposit into FP32 planes; the particle state and the Boris pushes stay FP64.
+constexpr int ST_NT = 128;
+template <bool F32>
+__global__ void __launch_bounds__(ST_NT, 4) k_stream(StreamArgs c, StrmDev S, const long* __restrict__ nstrm) {
+    const long n = *nstrm;
+    for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
+        const DepReq d = stream_one<F32>(c, S, i);
+        if (d.on) sdeposit<F32>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
     }
 }
 
 // ---------------------------------------------------------------- spectra of the streaming current
 // rows: per row, FFT along x of jx + i jy (split) and of jz -> three half rows in T0..T2
-template <int NX>
-__global__ void __launch_bounds__(128) k_ss_rows(Geo g, const double* __restrict__ J, cpx* __restrict__ T0, cpx* __restrict__ T1,
+template <int NX, class JT>
+__global__ void __launch_bounds__(128) k_ss_rows(Geo g, const JT* __restrict__ J, cpx* __restrict__ T0, cpx* __restrict__ T1,
                                                 cpx* __restrict__ T2) {
     using S = FftShape<NX>;
     constexpr int LPC = 128 / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
@@ -283,26 +332,28 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_ss_cols(Geo g, const c
 
 // ---------------------------------------------------------------- elementwise steps of the half-cell
 // jk(m) += nw - old; old <- nw (the `replace` of sim_plasma.cpp:257-264), three half planes
-__global__ void k_replace(cpx* __restrict__ jx, cpx* __restrict__ jy, cpx* __restrict__ jz, cpx* __restrict__ old,
+template <class T>
+__global__ void k_replace(T* __restrict__ jx, T* __restrict__ jy, T* __restrict__ jz, cpx* __restrict__ old,
                           const cpx* __restrict__ nw, long nkh) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
-        jx[i] = jx[i] + nw[i] - old[i];
-        jy[i] = jy[i] + nw[nkh + i] - old[nkh + i];
-        jz[i] = jz[i] + nw[2 * nkh + i] - old[2 * nkh + i];
+        jx[i] = narrow<T>(widen(jx[i]) + nw[i] - old[i]);
+        jy[i] = narrow<T>(widen(jy[i]) + nw[nkh + i] - old[nkh + i]);
+        jz[i] = narrow<T>(widen(jz[i]) + nw[2 * nkh + i] - old[2 * nkh + i]);
         old[i] = nw[i]; old[nkh + i] = nw[nkh + i]; old[2 * nkh + i] = nw[2 * nkh + i];
     }
 }
 // after a pass: replace the streaming part of jk(n) by jsn (old = sin); with the extrapolating predictor and
 // n >= 1 the prediction of half-cell n-1: tmp = js0(n-1) + d + w (d - dl), d = jsn - js0(n); replace(n-1, pin, tmp)
+template <class T>
 __global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
     const long nkh = p.nkh;
     const long hp = long(n + 1) * nkh, hq = long(n) * nkh;        // planes of half-cells n and n-1 (a = 0)
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
         cpx u[3];
         for (int k = 0; k < 3; ++k) u[k] = p.jsn[k * nkh + i];
-        cpx* jk[3] = {p.jkx, p.jky, p.jkz};
+        T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
         for (int k = 0; k < 3; ++k) {
-            jk[k][hp + i] = jk[k][hp + i] + u[k] - p.sin_[k * nkh + i];
+            jk[k][hp + i] = narrow<T>(widen(jk[k][hp + i]) + u[k] - p.sin_[k * nkh + i]);
             p.sin_[k * nkh + i] = u[k];
         }
         if (extrap && n >= 1) {
@@ -310,7 +361,7 @@ __global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
             for (int k = 0; k < 3; ++k) {
                 const cpx d = u[k] - s0[k][hp + i];
                 const cpx t = s0[k][hq + i] + d + w * (d - p.dl[k * nkh + i]);
-                jk[k][hq + i] = jk[k][hq + i] + t - p.pin[k * nkh + i];
+                jk[k][hq + i] = narrow<T>(widen(jk[k][hq + i]) + t - p.pin[k * nkh + i]);
                 p.pin[k * nkh + i] = t;
             }
         }
@@ -333,29 +384,32 @@ __global__ void k_correct(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ 
     }
 }
 // the march of slice n, all modes (march_point, sim_kernels.hpp:173-210, one rank: b = N, no boundary slice)
-__global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, cpx* __restrict__ Ez,
-                                                    cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
-                                                    const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
-                                                    const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
-                                                    const cpx* __restrict__ jkz, double D, int n) {
+template <class T>
+__global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
+                                                    T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
+                                                    const T* __restrict__ j0x, const T* __restrict__ j0y,
+                                                    const T* __restrict__ jkx, const T* __restrict__ jky,
+                                                    const T* __restrict__ jkz, double D, int n) {
     const long nk = g.nkh;
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nk) return;
     const int kxi = int(i % g.H), j = int(i / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
     const long o = long(n - g.a) * nk + i, od = o, ou = o + nk;
-    const cpx Jx = wl * (j0x[od] + jkx[od]) + wu * (j0x[ou] + jkx[ou]);
-    const cpx Jy = wl * (j0y[od] + jky[od]) + wu * (j0y[ou] + jky[ou]);
-    const cpx Rsx = Rx[o] + D * (ik(kx, Ez[o]) + ik(ky, Bz[o])) - D * Jx;
-    const cpx Rsy = Ry[o] + D * (ik(ky, Ez[o]) - ik(kx, Bz[o])) - D * Jy;
+    const cpx Jx = wl * (widen(j0x[od]) + widen(jkx[od])) + wu * (widen(j0x[ou]) + widen(jkx[ou]));
+    const cpx Jy = wl * (widen(j0y[od]) + widen(jky[od])) + wu * (widen(j0y[ou]) + widen(jky[ou]));
+    const cpx ez = widen(Ez[o]), bz = widen(Bz[o]);
+    const cpx Rsx = Rx[o] + D * (ik(kx, ez) + ik(ky, bz)) - D * Jx;
+    const cpx Rsy = Ry[o] + D * (ik(ky, ez) - ik(kx, bz)) - D * Jy;
     if (n == g.N - 1) {
-        Rx[o] = Rsx; Ry[o] = Rsy; Ez[o] = C(0); Bz[o] = C(0); Lx[o] = C(0); Ly[o] = C(0);
+        Rx[o] = Rsx; Ry[o] = Rsy;
+        Ez[o] = narrow<T>(C(0)); Bz[o] = narrow<T>(C(0)); Lx[o] = narrow<T>(C(0)); Ly[o] = narrow<T>(C(0));
         return;
     }
     const long pp = o + nk;
-    const cpx pRx = Rx[pp], pRy = Ry[pp], pEz = Ez[pp], pBz = Bz[pp], pLx = Lx[pp], pLy = Ly[pp];
+    const cpx pRx = Rx[pp], pRy = Ry[pp], pEz = widen(Ez[pp]), pBz = widen(Bz[pp]), pLx = widen(Lx[pp]), pLy = widen(Ly[pp]);
     const double h = g.hcg[n + 2];
-    const cpx upx = jkx[ou], upy = jky[ou], upz = jkz[ou];
+    const cpx upx = widen(jkx[ou]), upy = widen(jky[ou]), upz = widen(jkz[ou]);
     const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
     const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
     const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
@@ -365,9 +419,10 @@ __global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx
     const double den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
     const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) / den;
     const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) / den;
-    Ez[o] = Ezn; Bz[o] = Bzn;
+    Ez[o] = narrow<T>(Ezn); Bz[o] = narrow<T>(Bzn);
     Rx[o] = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)); Ry[o] = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
-    Lx[o] = Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)); Ly[o] = Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn));
+    Lx[o] = narrow<T>(Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)));
+    Ly[o] = narrow<T>(Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn)));
 }
 // freed electrons join the march (appended after the streaming particles; the count stays on the device)
 __global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
@@ -387,26 +442,75 @@ __global__ void k_count_add(long* __restrict__ nstrm_dev, const int* __restrict_
     if (cnt <= bcap) *nstrm_dev += cnt;
 }
 
+// ---------------------------------------------------------------- per half-cell set-up, fused
+// Start of half-cell n (sim_plasma.cpp:236-262): sin <- pin and si0 <- pin (copy_in); the prediction of half-cell
+// pred_m starts from its level s0 with the prediction buffer cleared: jk(pred_m) += js0(pred_m), pin <- js0(pred_m)
+// (pred_m < 0: none); the slice's R_x, R_y, E_z, B_z saved for the passes (backup).
+template <class T>
+__global__ void k_slice_prologue(PlasmaPtrs p, cpx* __restrict__ sin_, cpx* __restrict__ si0, cpx* __restrict__ bk,
+                                 const cpx* __restrict__ Rx, const cpx* __restrict__ Ry, const T* __restrict__ Ez,
+                                 const T* __restrict__ Bz, long o, int pred_m, int copy_in, int backup) {
+    const long nkh = p.nkh;
+    const long hm = long(pred_m + 1) * nkh;
+    T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
+    const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const long q = k * nkh + i;
+            if (copy_in) { const cpx v = p.pin[q]; sin_[q] = v; si0[q] = v; }
+            if (pred_m >= 0) {
+                const cpx t = s0[k][hm + i];
+                jk[k][hm + i] = narrow<T>(widen(jk[k][hm + i]) + t);
+                p.pin[q] = t;
+            }
+        }
+        if (backup) {
+            bk[i] = Rx[o + i]; bk[nkh + i] = Ry[o + i];
+            bk[2 * nkh + i] = widen(Ez[o + i]); bk[3 * nkh + i] = widen(Bz[o + i]);
+        }
+    }
+}
+// Start of a pass: the slice restored from the backup (restore), the streaming-current planes and the count of
+// freed electrons cleared.
+template <class T, class JT>
+__global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
+                                T* __restrict__ Bz, long o, long nkh, JT* __restrict__ J, long nj, int* __restrict__ bcnt,
+                                int restore) {
+    const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x, st = long(gridDim.x) * blockDim.x;
+    if (restore)
+        for (long i = t0; i < nkh; i += st) {
+            Rx[o + i] = bk[i]; Ry[o + i] = bk[nkh + i];
+            Ez[o + i] = narrow<T>(bk[2 * nkh + i]); Bz[o + i] = narrow<T>(bk[3 * nkh + i]);
+        }
+    for (long i = t0; i < nj; i += st) J[i] = JT(0);
+    if (t0 == 0) *bcnt = 0;
+}
+
 // ---------------------------------------------------------------- launchers
 static unsigned ew_blocks(long n) {
     long b = (n + 255) / 256;
     return unsigned(b < 148 * 8 ? (b < 1 ? 1 : b) : 148 * 8);
 }
-void launch_stream(Ctx& c, const StreamArgs& a, long nmax) {
-    if (nmax <= 0) return;
+void launch_stream(Ctx& c, const StreamArgs& a) {
+    PlasmaState& P = *c.pl;
+    if (P.s.cap <= 0) return;
     const int tok = c.prof_begin("stream");
-    k_stream<<<unsigned((nmax + 127) / 128), 128, 0, c.stream>>>(a, c.pl->strm, c.pl->nstrm_dev.p);
+    const long want = (P.s.cap + ST_NT - 1) / ST_NT;
+    const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
+    if (c.mixed) k_stream<true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    else k_stream<false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
     c.check_launch("k_stream");
     c.prof_end(tok);
 }
 // Half spectra of three real planes J[0..2] (jx, jy, jz layout) into out[0..2]; T is scratch (3 half planes).
-template <int NX>
-static void ss_rows(Ctx& c, const double* J, cpx* T) {
+template <int NX, class JT>
+static void ss_rows(Ctx& c, const JT* J, cpx* T) {
     using S = FftShape<NX>;
     constexpr int LPC = 128 / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
-    G3D_CUDA(cudaFuncSetAttribute(k_ss_rows<NX>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_ss_rows<NX><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh);
+    G3D_CUDA(cudaFuncSetAttribute(k_ss_rows<NX, JT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k_ss_rows<NX, JT><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh);
     c.check_launch("k_ss_rows");
 }
 template <int NY>
@@ -422,39 +526,58 @@ void launch_stream_spectra(Ctx& c) {
     const int tok = c.prof_begin("stream_spectra");
     PlasmaState& P = *c.pl;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
-    G3D_DISPATCH_N(c.nx, NX, ss_rows<NX>(c, P.jsr.p, P.tsp.p));
+    if (c.mixed) {
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float>(c, P.jsrf.p, P.tsp.p)));
+    } else {
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p)));
+    }
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, P.tsp.p, P.jsn.p, a2, P.box_mean ? 1 : 0, 1));
     c.prof_end(tok);
 }
 // plain transverse spectra (no filters) of three real planes: the grid-laser profile
 void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
-    G3D_DISPATCH_N(c.nx, NX, ss_rows<NX>(c, J3, T3));
+    G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J3, T3)));
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
 }
 
-// copy of the streaming particles that a pass modifies (backup / restore of a half-cell's passes)
-__global__ void k_strm_copy(StrmDev d, StrmDev s, long n) {
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
-        d.x[i] = s.x[i]; d.y[i] = s.y[i]; d.zeta[i] = s.zeta[i]; d.px[i] = s.px[i]; d.py[i] = s.py[i]; d.pz[i] = s.pz[i];
-        d.z[i] = s.z[i]; d.q[i] = s.q[i]; d.qm[i] = s.qm[i]; d.alive[i] = s.alive[i];
-        d.w[i] = s.w[i]; d.sp[i] = s.sp[i]; d.id[i] = s.id[i];
-    }
+void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup) {
+    PlasmaState& P = *c.pl;
+    const long o = long(n - c.a) * c.nkh;
+    const int tok = c.prof_begin("slice_prologue");
+    if (c.mixed)
+        k_slice_prologue<cpxf><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(P.ptrs(c), P.jsin.p, P.jsi0.p, P.bk.p, c.Rx.p, c.Ry.p,
+                                                                       c.mx.Ez.p, c.mx.Bz.p, o, pred_m, copy_in, backup);
+    else
+        k_slice_prologue<cpx><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(P.ptrs(c), P.jsin.p, P.jsi0.p, P.bk.p, c.Rx.p, c.Ry.p,
+                                                                      c.Ez.p, c.Bz.p, o, pred_m, copy_in, backup);
+    c.check_launch("k_slice_prologue");
+    c.prof_end(tok);
 }
-void launch_strm_copy(Ctx& c, const StrmDev& dst, const StrmDev& src, long nmax) {
-    if (nmax <= 0) return;
-    const int tok = c.prof_begin("strm_copy");
-    k_strm_copy<<<ew_blocks(nmax), 256, 0, c.stream>>>(dst, src, nmax);
-    c.check_launch("k_strm_copy");
+void launch_pass_prologue(Ctx& c, int n, int restore) {
+    PlasmaState& P = *c.pl;
+    const long o = long(n - c.a) * c.nkh, nj = 5 * long(c.nk);
+    const int tok = c.prof_begin("pass_prologue");
+    if (c.mixed)
+        k_pass_prologue<cpxf, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.mx.Ez.p, c.mx.Bz.p, o, c.nkh,
+                                                                          P.jsrf.p, nj, P.bcnt.p, restore);
+    else
+        k_pass_prologue<cpx, double><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
+                                                                          P.jsr.p, nj, P.bcnt.p, restore);
+    c.check_launch("k_pass_prologue");
     c.prof_end(tok);
 }
 void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw) {
     const long h = long(m + 1) * c.nkh;
-    k_replace<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.jkx.p + h, c.jky.p + h, c.jkz.p + h, old, nw, c.nkh);
+    if (c.mixed)
+        k_replace<cpxf><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.mx.jkx.p + h, c.mx.jky.p + h, c.mx.jkz.p + h, old, nw, c.nkh);
+    else
+        k_replace<cpx><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.jkx.p + h, c.jky.p + h, c.jkz.p + h, old, nw, c.nkh);
     c.check_launch("k_replace");
 }
 void launch_replace_pred(Ctx& c, int n, int extrap, double w) {
     const int tok = c.prof_begin("replace_pred");
-    k_replace_pred<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), n, extrap, w);
+    if (c.mixed) k_replace_pred<cpxf><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), n, extrap, w);
+    else k_replace_pred<cpx><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), n, extrap, w);
     c.check_launch("k_replace_pred");
     c.prof_end(tok);
 }
@@ -464,8 +587,15 @@ void launch_correct(Ctx& c, int n, double q, int own) {
 }
 void launch_march_slice(Ctx& c, double D, int n) {
     const int tok = c.prof_begin("march_slice");
-    k_march_slice<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
-                                                                       c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D, n);
+    const unsigned blocks = unsigned((c.nkh + 127) / 128);
+    if (c.mixed) {
+        MixedBufs& m = c.mx;
+        k_march_slice<cpxf><<<blocks, 128, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
+                                                          m.jkx.p, m.jky.p, m.jkz.p, D, n);
+    } else {
+        k_march_slice<cpx><<<blocks, 128, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
+                                                         c.jkx.p, c.jky.p, c.jkz.p, D, n);
+    }
     c.check_launch("k_march_slice");
     c.prof_end(tok);
 }

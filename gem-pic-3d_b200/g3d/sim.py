@@ -42,7 +42,7 @@ def sample_bunches(cfg, lib=None):
 
 class Simulation:
     """One march context on the current CUDA device. precision: "fp64" (the reference's arithmetic) or "mixed"
-    (FP32 transforms, currents and E_z/B_z/L with the FP64 accumulator R; no streaming plasma)."""
+    (FP32 transforms, currents, gathers and E_z/B_z/L storage with the FP64 accumulator R and FP64 particles)."""
 
     def __init__(self, cfg, lib=None, precision="fp64"):
         if precision not in ("fp64", "mixed"):

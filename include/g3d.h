@@ -198,9 +198,9 @@ int g3d_relax_start_field(struct g3d_ctx* ctx);     /* sim_fields.cpp:384-410 */
 /* Arithmetic of the march. G3D_PREC_FP64 (default): FP64 throughout, the reference's arithmetic.
  * G3D_PREC_MIXED: no counterpart in the reference (FP64 only) - deposit (FP32 atomics), zeta filter (compensated
  * FP32 sums), transverse FFTs, the E_z/B_z/L march, the sponge and the real fields in FP32 / complex64, with FP64
- * kept for the s-level accumulator R_x, R_y and for the particles. Set before g3d_init (G3D_ERR_STATE after it);
- * not with streaming plasma (G3D_ERR_ARG). Arrays keep the reference layouts and types at the boundary
- * (g3d_get_array widens, g3d_set_array rounds). */
+ * kept for the s-level accumulator R_x, R_y and for the particles (with streaming plasma: FP32 gathers and
+ * streaming deposit, FP64 particle state and Boris pushes). Set before g3d_init (G3D_ERR_STATE after it). Arrays
+ * keep the reference layouts and types at the boundary (g3d_get_array widens, g3d_set_array rounds). */
 #define G3D_PREC_FP64  0
 #define G3D_PREC_MIXED 1
 int g3d_set_precision(struct g3d_ctx* ctx, int32_t mode);

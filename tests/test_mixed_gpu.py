@@ -107,3 +107,37 @@ def test_precision_is_fixed_after_init():
     with pytest.raises(G3DError):
         sim._c(sim.lib.g3d_set_precision(sim.ctx, abi.G3D_PREC_FP64))
     sim.close()
+
+
+def run_plasma(cfg, precision, steps):
+    from g3d import Simulation
+    sim = Simulation(cfg, precision=precision)
+    sim.init()
+    for _ in range(steps):
+        sim.step()
+    out = {a: sim.array(a) for a in FIELDS + ["F"]}
+    out["diag"] = sim.diagnostics_sums()
+    out["strm"] = sim.streaming_particles()
+    out["np"] = sim.status().np
+    sim.close()
+    return out
+
+
+@pytest.mark.parametrize("ions,passes", [(True, 2), (False, 1)])
+def test_mixed_form_plasma_error_table(ions, passes):
+    """The streaming-plasma march in the mixed form (FP32 gathers and streaming deposit, complex64 spectra, FP64
+    R and particles) against the FP64 form on the small laser-wakefield case, 3 s-steps."""
+    from g3d import configs
+    cfg = configs.lwfa_small(ions=ions, extrapolate=1, passes=passes)
+    a = run_plasma(cfg, "fp64", 3)
+    b = run_plasma(cfg, "mixed", 3)
+    table = {n: rel_l2(b[n], a[n]) for n in FIELDS + ["F"]}
+    table["state"] = stacked_error(b, a, FIELDS)
+    assert len(b["strm"]) == len(a["strm"]) and b["np"] == a["np"]
+    for f in ["x", "y", "px", "py", "pz"]:
+        table["plasma " + f] = rel_l2(b["strm"][f], a["strm"][f])
+    print(f"mixed vs FP64, plasma (ions={ions}, passes={passes}, 3 steps):", {k: f"{v:.2e}" for k, v in table.items()})
+    assert table["state"] <= TOL_FIELD
+    assert table["F"] <= TOL_FIELD
+    for f in ["x", "y", "px", "py", "pz"]:
+        assert table["plasma " + f] <= 1e-5, (f, table["plasma " + f])
