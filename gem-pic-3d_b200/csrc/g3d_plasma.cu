@@ -109,6 +109,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     pl->bk.alloc(4 * ph, s);
     pl->nstrm_dev.alloc(1, s);
     pl->bcnt.alloc(1, s);
+    pl->tally.alloc(1, s);
     pl->flags.alloc(1, s);
     // ion tables on the device (setup_ions, src/sim_ions.cpp:68-87)
     const double Lu = c.P.lambda0 / (2 * M_PI), omega0 = c_SI / Lu, E0 = me_SI * c_SI * omega0 / e_SI;
@@ -363,8 +364,11 @@ void march_plasma(Ctx& c, double s0, double s1) {
     int flag = 0;
     G3D_CUDA(cudaMemcpy(&flag, P.flags.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) throw Error(G3D_ERR_CAPACITY, "ionization: list of freed electrons overflowed");
-    // trapped particles: fast ones join the beam list, slow ones stream again in the next step
-    std::vector<g3d_particle> sv = get_streaming(c);
+    // trapped particles: fast ones join the beam list, slow ones stream again in the next step (counted on the
+    // device first: the streaming particles come to the host only when some were trapped)
+    const bool any_trapped = count_state(c, P.strm.alive, 0, P.nstrm_dev.p, 5) > 0;
+    std::vector<g3d_particle> sv;
+    if (any_trapped) sv = get_streaming(c);
     std::vector<g3d_particle> add;
     for (auto& p : sv) {
         if (p.alive != 5) continue;
@@ -393,6 +397,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
 // src/sim_plasma.cpp:474-491, one rank).
 void collect_restreaming(Ctx& c) {
     PlasmaState& P = *c.pl;
+    // counted on the device first: the whole beam list comes to the host only when a particle left it
+    if (c.np == 0 || count_state(c, c.parts.alive, c.np, nullptr, 4) == 0) return;
     std::vector<g3d_particle> all = get_particles(c), keep;
     bool any = false;
     for (auto& p : all) if (p.alive == 4) { any = true; break; }

@@ -87,6 +87,7 @@ struct PlasmaState {
     long born_cap = 0, fresh_last = 0, trapped_total = 0, restreamed_total = 0;
     DevBuf<long> nstrm_dev;
     DevBuf<int> bcnt, flags;
+    DevBuf<int> tally;                         // count of particles in a given state (count_state)
     DevBuf<IonDevC> ion_dev;
     DevBuf<AdkDev> adk_dev;
     std::vector<g3d_particle> joining;         // join the next march at their zeta
@@ -112,6 +113,8 @@ void launch_replace_pred(Ctx& c, int n, int extrap, double w);
 void launch_correct(Ctx& c, int n, double q, int own);
 void launch_march_slice(Ctx& c, double D, int n);
 void launch_born_append(Ctx& c);
+// number of particles with alive == state among n (n_dev: the count on the device instead, when not null)
+long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state);
 void launch_real_fields_slice(Ctx& c, int l);
 
 }  // namespace g3d

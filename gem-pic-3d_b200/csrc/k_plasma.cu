@@ -487,6 +487,16 @@ __global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx
     if (t0 == 0) *bcnt = 0;
 }
 
+// ---------------------------------------------------------------- count of particles in one state
+__global__ void k_count_state(const int32_t* __restrict__ alive, long n, const long* __restrict__ n_dev, int state,
+                              int* __restrict__ out) {
+    const long m = n_dev ? *n_dev : n;
+    int k = 0;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += long(gridDim.x) * blockDim.x) k += alive[i] == state;
+    for (int o = 16; o > 0; o >>= 1) k += __shfl_down_sync(0xffffffffu, k, o);
+    if ((threadIdx.x & 31) == 0 && k) atomicAdd(out, k);
+}
+
 // ---------------------------------------------------------------- launchers
 static unsigned ew_blocks(long n) {
     long b = (n + 255) / 256;
@@ -540,6 +550,16 @@ void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
 }
 
+long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state) {
+    PlasmaState& P = *c.pl;
+    G3D_CUDA(cudaMemsetAsync(P.tally.p, 0, sizeof(int), c.stream));
+    k_count_state<<<148 * 4, 256, 0, c.stream>>>(alive, n, n_dev, state, P.tally.p);
+    c.check_launch("k_count_state");
+    int h = 0;
+    G3D_CUDA(cudaMemcpyAsync(&h, P.tally.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return h;
+}
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup) {
     PlasmaState& P = *c.pl;
     const long o = long(n - c.a) * c.nkh;
