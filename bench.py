@@ -82,7 +82,7 @@ def f_bytes(cfg):
 
 
 # ------------------------------------------------------------------ algorithmic bytes per launch (FP64)
-def algorithmic_bytes(name, cfg, mixed=False):
+def algorithmic_bytes(name, cfg, mixed=False, S=0):
     """Per-launch algorithmic bytes of each kernel: what it must read and write once, in the layout this build keeps.
 
     G = grid points (slices x nx x ny; F carries 6 floats = 24 B, the raw currents 3 values = 24 B in FP64, 12 B
@@ -90,13 +90,33 @@ def algorithmic_bytes(name, cfg, mixed=False):
     16 B per Gh as complex128 and 8 B as complex64 (the mixed form keeps R in complex128 and the rest in
     complex64). The spectra of real fields are Hermitian, so the kept half is the minimum a transform pass has to
     move. P = beam particles: the push reads x, y, zeta, px, py, pz, z, w (64 B) and writes 48 B (both forms);
-    the deposit reads 56 B."""
+    the deposit reads 56 B.
+    The per-half-cell kernels of the plasma march work on one slice: nk = nx ny points, nkh = ny (nx/2 + 1) modes,
+    S = streaming particles, each read (80 B) and written (64 B) once per half-cell pass (the per-unit figure of
+    the streaming push), with the two F slices it gathers from (48 B per point) and the deposit planes (5 values
+    per point)."""
     ns = cfg.nzeta - 1
     nk = cfg.nx * cfg.ny
     G = ns * nk
     Gh = ns * cfg.ny * (cfg.nx // 2 + 1)
     Gc = (ns + 1) * cfg.ny * (cfg.nx // 2 + 1)      # current planes carry one more half-cell
     P = cfg.particles
+    nkh = cfg.ny * (cfg.nx // 2 + 1)
+    cz = 8 if mixed else 16                          # bytes of a stored spectrum value other than R
+    cr = 4 if mixed else 8                           # bytes of a raw current value
+    plasma = {
+        "stream": 144 * S + 48 * nk + 5 * cr * nk,
+        "stream_spectra": 3 * cr * nk + (2 * 48 + 3 * cz) * nkh,      # three real planes; scratch; jsn (complex128)
+        "march_slice": (4 * 16 + 10 * cz + 6 * cz) * nkh + (2 * 16 + 4 * cz) * nkh,
+        "real_cols_slice": (2 * 16 + 4 * cz + 6 * cz) * nkh,
+        "real_rows_slice": 6 * cz * nkh + 24 * nk,
+        # jsn, sin, js0 (2), dl, pin read; jk (2 half-cells) read and written; sin, pin written (3 components each)
+        "replace_pred": (6 * 48 + 2 * 3 * cz) * nkh + (2 * 3 * cz + 2 * 48) * nkh,
+        "slice_prologue": (48 + 96 + 48 + 2 * 3 * cz + 48 + 32 + 2 * cz + 64) * nkh,
+        "pass_prologue": 5 * cr * nk + 64 * nkh,
+    }
+    if name in plasma:
+        return plasma[name] if S else None
     if not mixed:
         table = {
             "push": 112 * P + 24 * G,          # particles read 64 + written 48; F read 24 per grid point
@@ -328,8 +348,8 @@ def time_form(cfg, precision, a, world, dist, local):
     sim.profile(False)
     mixed = precision == "mixed"
     kernels = {k: {"launches": n, "avg_ms": round(t / max(1, n), 5), "share": round(t / sum(v[1] for v in prof.values()), 4),
-                   "GB/s": (round(algorithmic_bytes(k, cfg, mixed) / (t / max(1, n) * 1e-3) / 1e9, 1)
-                            if algorithmic_bytes(k, cfg, mixed) else None)}
+                   "GB/s": (round(algorithmic_bytes(k, cfg, mixed, S) / (t / max(1, n) * 1e-3) / 1e9, 1)
+                            if algorithmic_bytes(k, cfg, mixed, S) else None)}
                for k, (n, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
     out = {"sim": sim, "P": P, "stream": stream, "ms": ms, "value": job_rate(P, a.steps, world, ms), "clk": clk,
            "launches": launches, "prof": prof, "kernels": kernels}
@@ -352,7 +372,7 @@ def roofline(form, cfg, workload, mixed):
         peak, peak_src = 6650.0, "fallback"
     name, (n_launch, tot_ms) = max(form["prof"].items(), key=lambda kv: kv[1][1])
     avg_ms = tot_ms / max(1, n_launch)
-    ab = algorithmic_bytes(name, cfg, mixed)
+    ab = algorithmic_bytes(name, cfg, mixed, (form.get("streaming") or {}).get("particles_per_step", 0))
     achieved = ab / (avg_ms * 1e-3) / 1e9 if ab else None
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
