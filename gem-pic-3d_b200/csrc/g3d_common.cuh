@@ -122,6 +122,19 @@ G3D_HD void tsc_periodic(double x, double d, int n, int idx[3], double w[3]) {
     idx[0] = b; idx[1] = b1; idx[2] = b1 + 1 == n ? 0 : b1 + 1;
 }
 
+// TSC on the free-hand y grid in the index coordinate xi(y) (linear within a cell): nodes at the integers,
+// half-nodes at the half-integers (stored at index j for j + 1/2); points outside 0..ny-1 are walls or beyond
+// (reference tsc_y, src/sim_kernels.hpp:34-40).
+G3D_HD void tsc_y(const AxisDev& ax, double y, int jn[3], double wn[3], int jh[3], double wh[3]) {
+    int i; double f;
+    ax.locate(y, i, f);
+    const double xi = i + f;
+    tsc_weights(xi, jn, wn);
+    tsc_weights(xi - 0.5, jh, wh);
+}
+// the components of F that live on the half-nodes of the free-hand y grid: E_y, B_x, B_z
+G3D_HD bool is_half(int comp) { return comp == 1 || comp == 3 || comp == 5; }
+
 // fmod(x, L) for L > 0, bit for bit (fmod is exact): |x| < L is x itself, L <= |x| < 2L is x -+ L (exact by
 // Sterbenz's lemma); larger |x| falls back to fmod. The periodic wrap of the reference's gather call,
 // fmod(fmod(x, L) + L, L) (src/sim_kernels.hpp), meets only the first two cases in practice.

@@ -22,6 +22,9 @@ struct Geo {
     const double *kxd, *kxs, *filt, *maskx;
     const double *kyd, *kys, *filty, *masky_n, *masky_h, *iD, *iA;
     const double *zs, *hcg, *wlo, *whi, *wsl;
+    // free-hand y (yf == 0): node positions (ny + 1), LU factors of k_x^2 - Lap_y on the nodes per (j, k_x)
+    // ([j][k_x], k_x <= nx/2), eigenvectors of -Lap_y (forward [s][j], back [j][s]) and eigenvalues [s]
+    const double *yn, *pcp, *pid, *evf, *evb, *evl;
     AxisDev zax, yax;
     const cpx *twx, *twy;               // exp(-2 pi i s / nx), exp(-2 pi i s / ny)
 };
@@ -129,6 +132,10 @@ struct Ctx {
     DevBuf<double> kxd, kxs, filt, maskx, kyd, kys, filty, masky_n, masky_h, iD, iA;
     DevBuf<double> zs, hcg, wlo, whi, wsl;
     DevBuf<cpx> twx, twy;
+    DevBuf<double> yn, pcp, pid, evf, evb, evl;  // free-hand y tables (empty for Fourier y)
+    std::vector<double> ynode_h;
+    DevBuf<cpx> fhs;                             // free-hand march scratch: 5 lines of ny x H complex
+    DevBuf<double> fhcp;                         // and the Thomas coefficients, ny x H
     // field state: the reference's arrays (src/sim.hpp:265-276); spectra as half spectra [plane][j][k_x <= nx/2]
     DevBuf<cpx> Rx, Ry, Ez, Bz, Lx, Ly;          // ns planes
     DevBuf<cpx> j0x, j0y, jkx, jky, jkz;         // ns+1 half-cell planes
@@ -189,6 +196,15 @@ struct Ctx {
 void launch_deposit(Ctx& c);
 void launch_cur_fft(Ctx& c, bool keep0);
 void launch_march(Ctx& c, double D);
+// free-hand y (k_freehand.cu)
+void launch_deposit_fh(Ctx& c);
+void launch_cur_fft_fh(Ctx& c, bool keep0);
+void launch_march_fh(Ctx& c, double D);
+void launch_sponge_fh(Ctx& c);
+void launch_real_fields_fh(Ctx& c);
+void launch_comoving_fh(Ctx& c, double beta, double gm2);
+void launch_sp_rows(Ctx& c);                // k_fields.cu
+void launch_cur_rows_to_jk(Ctx& c);         // k_currents.cu
 void launch_sponge(Ctx& c);
 void launch_real_fields(Ctx& c);
 void launch_comoving(Ctx& c, double beta, double gm2);

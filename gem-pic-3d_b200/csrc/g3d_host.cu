@@ -64,6 +64,7 @@ static void set_precision(Ctx& c, int mode) {
     const bool mixed = mode == G3D_PREC_MIXED;
     if (mixed == c.mixed) return;
     if (c.fields_ready) throw Error(G3D_ERR_STATE, "the precision is set before g3d_init");
+    if (mixed && !c.yf) throw Error(G3D_ERR_ARG, "the mixed form needs the Fourier y grid");
     alloc_spectra(c, mixed);
 }
 
@@ -76,6 +77,7 @@ Geo Ctx::geo() const {
     g.kxd = kxd.p; g.kxs = kxs.p; g.filt = filt.p; g.maskx = maskx.p;
     g.kyd = kyd.p; g.kys = kys.p; g.filty = filty.p; g.masky_n = masky_n.p; g.masky_h = masky_h.p; g.iD = iD.p; g.iA = iA.p;
     g.zs = zs.p; g.hcg = hcg.p; g.wlo = wlo.p; g.whi = whi.p; g.wsl = wsl.p;
+    g.yn = yn.p; g.pcp = pcp.p; g.pid = pid.p; g.evf = evf.p; g.evb = evb.p; g.evl = evl.p;
     g.zax = zax; g.yax = yax;
     g.twx = twx.p; g.twy = twy.p;
     return g;
@@ -118,13 +120,142 @@ void Ctx::check_launch(const char* what) {
 }
 
 // ---------------------------------------------------------------- set-up (reference sim_setup.cpp:5-164)
+// Eigenvalues and eigenvectors of a symmetric tridiagonal matrix (diagonal d, off-diagonal e[i] between i and
+// i + 1) by the implicit QL method with Wilkinson shifts (the published tql2 / tqli algorithm). On return d holds
+// the eigenvalues and z (n x n, row-major) the eigenvectors as columns: z[k n + m] is component k of vector m.
+static bool tridiagonal_eigen(std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
+    const int n = int(d.size());
+    z.assign(size_t(n) * n, 0.0);
+    for (int i = 0; i < n; ++i) z[size_t(i) * n + i] = 1;
+    e.resize(size_t(n), 0.0);
+    e[size_t(n - 1)] = 0;
+    for (int l = 0; l < n; ++l) {
+        int iter = 0, m;
+        do {
+            for (m = l; m < n - 1; ++m) {
+                const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+                if (std::fabs(e[m]) <= 1e-16 * dd) break;
+            }
+            if (m != l) {
+                if (iter++ == 100) return false;
+                double g = (d[l + 1] - d[l]) / (2 * e[l]);
+                double r = std::hypot(g, 1.0);
+                g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
+                double sn = 1, cs = 1, p = 0;
+                int i;
+                bool underflow = false;
+                for (i = m - 1; i >= l; --i) {
+                    double f = sn * e[i];
+                    const double b = cs * e[i];
+                    r = std::hypot(f, g);
+                    e[i + 1] = r;
+                    if (r == 0) { d[i + 1] -= p; e[m] = 0; underflow = true; break; }
+                    sn = f / r; cs = g / r;
+                    g = d[i + 1] - p;
+                    r = (d[i] - g) * sn + 2 * cs * b;
+                    p = sn * r;
+                    d[i + 1] = g + p;
+                    g = cs * r - b;
+                    for (int k = 0; k < n; ++k) {            // the rotation of columns i, i + 1
+                        f = z[size_t(k) * n + i + 1];
+                        z[size_t(k) * n + i + 1] = sn * z[size_t(k) * n + i] + cs * f;
+                        z[size_t(k) * n + i] = cs * z[size_t(k) * n + i] - sn * f;
+                    }
+                }
+                if (underflow) continue;
+                d[l] -= p; e[l] = g; e[m] = 0;
+            }
+        } while (m != l);
+    }
+    return true;
+}
+
+// Free-hand y (reference setup_y, src/sim_setup.cpp:84-143): nodes j = 0..ny (0 and ny are the conducting
+// walls), half-nodes j + 1/2; E_x, B_y, E_z, j_x, j_z on the nodes, E_y, B_x, B_z, j_y on the half-nodes. Cell
+// sizes Delta_j, dual sizes A_j, the sponge profile at nodes and half-nodes, the LU factors of k_x^2 - Lap_y on
+// the nodes 1..ny-1 (Dirichlet) for the bound field, and the eigenvectors of -Lap_y for the start field.
+static void setup_y_free(Ctx& c, const g3d_grid& G, const g3d_params& P, cudaStream_t s) {
+    const int ny = c.ny, H = c.H;
+    const std::vector<double> Y(G.ynode, G.ynode + ny + 1);
+    for (int j = 0; j < ny; ++j)
+        if (!(Y[size_t(j) + 1] > Y[size_t(j)])) throw Error(G3D_ERR_ARG, "ynode must increase");
+    const double Ly = Y[size_t(ny)] - Y[0];
+    c.dy = Ly / ny;
+    std::vector<double> hDel(ny), hA(ny), hiD(ny), hiA(ny), hmn(ny), hmh(ny);
+    for (int j = 0; j < ny; ++j) hDel[j] = Y[size_t(j) + 1] - Y[size_t(j)];
+    hA[0] = 0.5 * hDel[0];
+    for (int j = 1; j < ny; ++j) hA[j] = 0.5 * (hDel[j - 1] + hDel[j]);
+    auto prof = [&](double y) {
+        const double dd = 0.5 * Ly - std::fabs(y), w = P.sponge_y;
+        if (w <= 0 || dd >= w) return 1.0;
+        const double r = 1 - dd / w;
+        return 1 - P.sponge_rate * r * r;
+    };
+    for (int j = 0; j < ny; ++j) {
+        hiD[j] = 1 / hDel[j]; hiA[j] = 1 / hA[j];
+        hmn[j] = prof(Y[size_t(j)]); hmh[j] = prof(0.5 * (Y[size_t(j)] + Y[size_t(j) + 1]));
+    }
+    c.ynode_h = Y;
+    c.yn.upload(Y, s); c.iD.upload(hiD, s); c.iA.upload(hiA, s); c.masky_n.upload(hmn, s); c.masky_h.upload(hmh, s);
+    bool uni = true;
+    for (int j = 0; j < ny; ++j) uni = uni && hDel[j] == hDel[0];
+    c.yax = AxisDev{c.yn.p, ny + 1, uni ? 1 : 0, Y[0], 1 / hDel[0]};
+    // the y tables of the Fourier form are not used; zeros keep the device pointers valid
+    const std::vector<double> zero(static_cast<size_t>(ny), 0.0);
+    c.kyd.upload(zero, s); c.kys.upload(zero, s); c.filty.upload(zero, s);
+    c.kyd_h = zero;
+    // LU factors of (k_x^2 - Lap_y) on the nodes 1..ny-1, per k_x <= nx/2
+    std::vector<double> hcp(size_t(ny) * H, 0.0), hid(size_t(ny) * H, 0.0);
+    for (int i = 0; i < H; ++i) {
+        double cprev = 0;
+        const double kx = c.kxd_h[size_t(i)];
+        for (int j = 1; j < ny; ++j) {
+            const double lo = j > 1 ? -hiA[j] * hiD[j - 1] : 0, up = j < ny - 1 ? -hiA[j] * hiD[j] : 0;
+            const double den = kx * kx + hiA[j] * (hiD[j - 1] + hiD[j]) - lo * cprev;
+            hid[size_t(j) * H + i] = 1 / den;
+            hcp[size_t(j) * H + i] = cprev = up / den;
+        }
+    }
+    c.pcp.upload(hcp, s); c.pid.upload(hid, s);
+    // eigenvectors of -Lap_y on the nodes: T v = mu A v with T symmetric; S = A^-1/2 T A^-1/2 is symmetric
+    // tridiagonal with eigenvectors u, v = A^-1/2 u. Slot s = m + 1 holds eigenvalue m (slot 0 unused).
+    const int M = ny - 1;
+    std::vector<double> d(static_cast<size_t>(M)), e(static_cast<size_t>(M), 0.0), z;
+    for (int j = 1; j < ny; ++j) d[size_t(j) - 1] = hiA[j] * (hiD[j - 1] + hiD[j]);
+    for (int j = 1; j < ny - 1; ++j) e[size_t(j) - 1] = -hiD[j] / std::sqrt(hA[j] * hA[j + 1]);
+    const std::vector<double> d0 = d, e0 = e;
+    if (!tridiagonal_eigen(d, e, z)) throw Error(G3D_ERR_ARG, "eigenvectors of the y Laplacian: no convergence");
+    // self-check: |S u - mu u| relative to the largest eigenvalue
+    double emax = 0, res = 0;
+    for (int m = 0; m < M; ++m) emax = std::max(emax, std::fabs(d[size_t(m)]));
+    for (int m = 0; m < M; ++m)
+        for (int k = 0; k < M; ++k) {
+            double v = d0[size_t(k)] * z[size_t(k) * M + m] - d[size_t(m)] * z[size_t(k) * M + m];
+            if (k > 0) v += e0[size_t(k) - 1] * z[size_t(k - 1) * M + m];
+            if (k < M - 1) v += e0[size_t(k)] * z[size_t(k + 1) * M + m];
+            res = std::max(res, std::fabs(v));
+        }
+    if (!(res <= 1e-10 * emax)) throw Error(G3D_ERR_ARG, "eigenvectors of the y Laplacian: residual " + std::to_string(res / emax));
+    std::vector<double> hf(size_t(ny) * ny, 0.0), hb(size_t(ny) * ny, 0.0), hl(static_cast<size_t>(ny), 0.0);
+    for (int m = 0; m < M; ++m) {
+        hl[size_t(m) + 1] = d[size_t(m)];
+        for (int j = 1; j < ny; ++j) {
+            const double u = z[size_t(j - 1) * M + m], sq = std::sqrt(hA[j]);
+            hf[size_t(m + 1) * ny + j] = u * sq;          // coefficient = v^T A rho
+            hb[size_t(j) * ny + m + 1] = u / sq;          // value = sum v coefficient
+        }
+    }
+    c.evf.upload(hf, s); c.evb.upload(hb, s); c.evl.upload(hl, s);
+}
+
 static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
-    if (!G.y_fourier) throw Error(G3D_ERR_ARG, "free-hand y grids are not supported by this release (y_fourier = 1)");
-    if (!pow2_ok(G.nx) || !pow2_ok(G.ny) || G.nx < 8)
-        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512 and ny one in 4..512");
+    if (!G.y_fourier && !G.ynode) throw Error(G3D_ERR_ARG, "free-hand y needs the ny + 1 nodes (ynode)");
+    if (!pow2_ok(G.nx) || G.nx < 8 || (G.y_fourier && !pow2_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 4096)))
+        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512; ny one in 4..512 (Fourier y) or 3..4096 (free-hand)");
     if (G.nzeta < 4 || !G.zeta) throw Error(G3D_ERR_ARG, "nzeta must be >= 4 with a zeta table");
     if (!(G.Lx > 0) || !(G.Ly > 0)) throw Error(G3D_ERR_ARG, "Lx, Ly must be positive");
-    if (P.precision != G3D_FP64) throw Error(G3D_ERR_ARG, "only the FP64 form is built in this release");
+    if (P.precision != G3D_FP64 && P.precision != G3D_MIXED) throw Error(G3D_ERR_ARG, "precision must be G3D_FP64 or G3D_MIXED");
+    if (!G.y_fourier && P.precision == G3D_MIXED) throw Error(G3D_ERR_ARG, "the mixed form needs the Fourier y grid");
     if (!(P.dz > 0) || !(P.dz_push > 0) || !(P.lambda0 > 0)) throw Error(G3D_ERR_ARG, "dz, dz_push, lambda0 must be positive");
     for (int m = 0; m + 1 < G.nzeta; ++m)
         if (!(G.zeta[m + 1] > G.zeta[m])) throw Error(G3D_ERR_ARG, "zeta slices must increase");
@@ -155,7 +286,10 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     }
     c.kxd.upload(hkx, s); c.kxs.upload(hsx, s); c.filt.upload(hf, s); c.maskx.upload(hm, s);
     c.kxd_h = hkx;
+    c.yf = G.y_fourier != 0;
+    if (!c.yf) setup_y_free(c, G, P, s);
     // y: Fourier modes (reference setup_y_fourier, sim_setup.cpp:63-82)
+    if (c.yf) {
     c.dy = G.Ly / ny;
     std::vector<double> hky(ny), hsy(ny), hfy(ny), hmy(ny), hi(ny, 1 / c.dy);
     for (int j = 0; j < ny; ++j) {
@@ -173,6 +307,7 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.iD.upload(hi, s); c.iA.upload(hi, s);
     c.kyd_h = hky;
     c.yax = AxisDev{nullptr, ny + 1, 1, 0.0, 1 / c.dy};
+    }
     // zeta (reference setup_zeta, sim_setup.cpp:148-164)
     const int N = c.N;
     const std::vector<double>& Z = c.zeta;
@@ -213,9 +348,14 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.laser.kx = std::sin(P.theta); c.laser.kz = std::cos(P.theta);
     c.laser.flat = P.flat_length; c.laser.ramp = P.ramp_length;
     // box origin as Simulation::init sets it (load_bunch, src/sim_bunches.cpp:216, also without bunches)
-    c.X0 = -0.5 * G.Lx; c.Y0 = -0.5 * G.Ly;
+    c.X0 = -0.5 * G.Lx; c.Y0 = c.yf ? -0.5 * G.Ly : 0.0;    // free-hand y: y is the physical coordinate
     if (P.laser_on && P.laser_envelope == G3D_ENV_FLATTOP && !(P.ramp_length > 0))
         throw Error(G3D_ERR_ARG, "flat-top envelope needs ramp_length > 0");
+    if (!c.yf) {
+        c.fhs.alloc(5 * size_t(ny) * c.H, s);
+        c.fhcp.alloc(size_t(ny) * c.H, s);
+    }
+    if (P.precision == G3D_MIXED) alloc_spectra(c, true);
     G3D_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -270,7 +410,9 @@ static void sample_bunches(const g3d_grid& G, const g3d_params& P, const g3d_bun
                            std::vector<g3d_particle>& mine, long& lost, double& X0, double& Y0) {
     const double Lu = P.lambda0 / (2 * M_PI), w0 = c_SI / Lu;
     const double nc = eps0 * me_SI * w0 * w0 / (e_SI * e_SI);
-    const double yoff = 0.5 * G.Ly;                   // Fourier y: box coordinate, physical y = p.y + Y0
+    const bool yf = G.y_fourier != 0;
+    const double yoff = yf ? 0.5 * G.Ly : 0.0;        // Fourier y: box coordinate, physical y = p.y + Y0
+    const double ylo = yf ? -1e300 : G.ynode[1], yhi = yf ? 1e300 : G.ynode[G.ny - 1];   // free-hand: inside the walls
     const int N = G.nzeta;
     // the zeta axis as the set-up builds it (uniform: direct location with 1 / h)
     bool uni = true;
@@ -305,7 +447,7 @@ static void sample_bunches(const g3d_grid& G, const g3d_params& P, const g3d_bun
             p.q = B.q; p.qm = B.q; p.sp = -kb; p.z = 0;
             int hc; double f;
             zax.locate(p.zeta, hc, f);
-            if (p.zeta < 0 || hc > N - 2) { ++lost; continue; }
+            if (p.zeta < 0 || hc > N - 2 || p.y < ylo || p.y > yhi) { ++lost; continue; }
             mine.push_back(p);
         }
     }
@@ -323,20 +465,27 @@ static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int c
 // ---------------------------------------------------------------- the march path
 static void currents(Ctx& c) {
     c.jk_is_j0 = false;
-    if (!c.mixed) launch_deposit(c);
+    if (!c.mixed && c.yf) launch_deposit(c);
     // with plasma the k = 0 current is kept (a 1D plasma wave, the return current), but not in the start field
     // (sim_particles.cpp:143-145)
     const bool keep0 = c.pl && c.pl->box_mean && !c.starting_;
+    if (!c.yf) { launch_deposit_fh(c); launch_cur_fft_fh(c, keep0); return; }
     if (c.mixed) { launch_deposit_f(c); launch_cur_fft_f(c, keep0); return; }
     launch_cur_fft(c, keep0);
     // one rank: the filtered j_z ghosts of the neighbours are zero (exchange_jz_ghosts, sim_particles.cpp:210-226)
 }
 static void march(Ctx& c, double D) {
     if (c.jk_is_j0) throw Error(G3D_ERR_STATE, "march needs the currents of level s1 (call currents first)");
-    if (c.mixed) launch_march_f(c, D);
+    if (!c.yf) launch_march_fh(c, D);
+    else if (c.mixed) launch_march_f(c, D);
     else launch_march(c, D);
 }
 static void sponge_and_real_fields(Ctx& c) {
+    if (!c.yf) {
+        if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge_fh(c);
+        launch_real_fields_fh(c);
+        return;
+    }
     if (c.mixed) {
         if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge_f(c);
         launch_real_fields_f(c);
@@ -380,7 +529,8 @@ static void comoving_field(Ctx& c) {
     const double beta = c.comoving_c_ ? 1 : sums[1] > 0 ? sums[0] / sums[1] : 1;
     const double gm2 = 1 - beta * beta;
     if (!c.comoving_c_) { c.beta_b = beta; c.gm2_b = gm2; }
-    if (c.mixed) launch_comoving_f(c, beta, gm2);
+    if (!c.yf) launch_comoving_fh(c, beta, gm2);
+    else if (c.mixed) launch_comoving_f(c, beta, gm2);
     else launch_comoving(c, beta, gm2);
 }
 static void relax_start_field(Ctx& c) {
@@ -760,7 +910,8 @@ int g3d_load_bunches(g3d_ctx* ctx, const g3d_bunch* b, int32_t count) {
         if (count < 0 || (count > 0 && !b)) throw Error(G3D_ERR_ARG, "bad bunch list");
         if (count > 1) throw Error(G3D_ERR_ARG, "one bunch block per run in this release");
         Ctx& c = ctx->c;
-        const g3d_grid G{c.nx, c.ny, c.N, 1, c.nx * c.dx, c.ny * c.dy, c.zeta.data(), nullptr};
+        const g3d_grid G{c.nx, c.ny, c.N, c.yf ? 1 : 0, c.nx * c.dx, c.ny * c.dy, c.zeta.data(),
+                         c.yf ? nullptr : c.ynode_h.data()};
         g3d::load_bunches(c, G, b, count);
     });
 }
@@ -822,12 +973,14 @@ int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ct
 int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
     return guarded(ctx, [&] {
         if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
+        if (!ctx->c.yf) throw Error(G3D_ERR_ARG, "streaming plasma on the free-hand y grid is not in this release");
         g3d::set_plasma(ctx->c, *plasma, ions, nions);
     });
 }
 int g3d_add_grid_laser(g3d_ctx* ctx, const g3d_grid_laser* laser) {
     return guarded(ctx, [&] {
         if (!laser || !(laser->waist > 0) || !(laser->tau > 0)) throw Error(G3D_ERR_ARG, "grid laser: waist and tau must be positive");
+        if (!ctx->c.yf) throw Error(G3D_ERR_ARG, "grid lasers on the free-hand y grid are not in this release");
         ctx->c.glasers.push_back(*laser);
     });
 }

@@ -163,7 +163,7 @@ void launch_deposit(Ctx& c) {
 }
 
 template <int NX>
-static void cur_rows(Ctx& c) {
+static void cur_rows(Ctx& c, cpx* TX, cpx* TY, cpx* TZ) {
     using S = FftShape<NX>;
     constexpr int LPC = CUR_NT / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
@@ -171,7 +171,7 @@ static void cur_rows(Ctx& c) {
     G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     const dim3 grid(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1));
     const int tok = c.prof_begin("cur_rows");
-    kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, c.W[0].p, c.W[1].p, c.W[2].p, c.P.zeta_filter ? 1 : 0);
+    kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, TX, TY, TZ, c.P.zeta_filter ? 1 : 0);
     c.check_launch("k_cur_rows");
     c.prof_end(tok);
 }
@@ -189,8 +189,11 @@ static void cur_cols(Ctx& c, bool keep0) {
 }
 
 void launch_cur_fft(Ctx& c, bool keep0) {
-    G3D_DISPATCH_N(c.nx, NX, cur_rows<NX>(c));
+    G3D_DISPATCH_N(c.nx, NX, cur_rows<NX>(c, c.W[0].p, c.W[1].p, c.W[2].p));
     G3D_DISPATCH_N(c.ny, NY, cur_cols<NY>(c, keep0));
 }
+
+// the zeta filter and the transform along x straight into jkx, jky, jkz (free-hand y: no transform along y)
+void launch_cur_rows_to_jk(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, cur_rows<NX>(c, c.jkx.p, c.jky.p, c.jkz.p)); }
 
 }  // namespace g3d

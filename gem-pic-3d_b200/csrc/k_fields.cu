@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx*
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
     fft_line<NX>(sm, RowAddr{r * RS}, t, g.twx);
-    const double s = 1.0 / double(g.nk);
+    const double s = g.yf ? 1.0 / double(g.nk) : 1.0 / double(g.nx);   // free-hand y: rows only, 1/nx
     #pragma unroll
     for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
         const int e = tid + u_ * NT;
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
     fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
-    const double s = 1.0 / double(g.nk);
+    const double s = g.yf ? 1.0 / double(g.nk) : 1.0 / double(g.nx);   // free-hand y: rows only, 1/nx
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     #pragma unroll 1
     for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
@@ -367,6 +367,21 @@ void launch_real_fields(Ctx& c) {
     G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, 0, c.ns));
     G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, 0, c.ns));
 }
+// free-hand y: the spectra are already real in y; one inverse transform along x per row of R, L and E_z + i B_z
+template <int NX>
+static void rf_rows_direct(Ctx& c) {
+    constexpr int LPC = NT / FftShape<NX>::T;
+    const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
+    allow_smem(k_rf_rows<NX>, smem);
+    const int tok = c.prof_begin("real_rows");
+    k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), NT, smem, c.stream>>>(
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, 0);
+    c.check_launch("k_rf_rows");
+    c.prof_end(tok);
+}
+void launch_real_fields_fh(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, rf_rows_direct<NX>(c)); }
+// the sponge's row pass alone (inverse x, mask, forward x) on W0, W1: the free-hand y sponge
+void launch_sp_rows(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, sp_rows<NX>(c)); }
 // E and B of one slice (plane l) in real space (Simulation::real_fields_slice, src/sim_plasma.cpp:200-220)
 void launch_real_fields_slice(Ctx& c, int l) {
     G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, l, 1));
@@ -374,15 +389,17 @@ void launch_real_fields_slice(Ctx& c, int l) {
 }
 
 // ---------------------------------------------------------------- half <-> full spectrum layouts
-// full[p][j][ix] = half[p][j][ix] (ix <= nx/2), conj(half[p][(ny - j) % ny][nx - ix]) (ix > nx/2)
+// full[p][j][ix] = half[p][j][ix] (ix <= nx/2), conj(half[p][(ny - j) % ny][nx - ix]) (ix > nx/2; free-hand y:
+// conj(half[p][j][nx - ix]))
 __global__ void k_half_to_full(Geo g, const cpx* __restrict__ half, cpx* __restrict__ full, long planes) {
     const long n = planes * g.nk;
     for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
         const long pl = idx / g.nk, i = idx - pl * g.nk;
         const int ixx = int(i % g.nx), j = int(i / g.nx);
         const long hb = pl * g.nkh;
+        const int jm = g.yf ? (g.ny - j) % g.ny : j;      // free-hand y: y is real space, only k_x mirrors
         full[idx] = ixx <= g.nx / 2 ? half[hb + long(j) * g.H + ixx]
-                                    : conj(half[hb + long((g.ny - j) % g.ny) * g.H + (g.nx - ixx)]);
+                                    : conj(half[hb + long(jm) * g.H + (g.nx - ixx)]);
     }
 }
 __global__ void k_full_to_half(Geo g, const cpx* __restrict__ full, cpx* __restrict__ half, long planes) {

@@ -1,0 +1,411 @@
+// The march on the free-hand y grid (y_fourier = 0): x stays Fourier (half spectra k_x = 0 .. nx/2), y is a
+// table of ny + 1 nodes between conducting walls, with E_x, B_y, E_z, j_x, j_z on the nodes and E_y, B_x, B_z, j_y
+// on the half-nodes. The arrays keep the layout [plane][j][k_x] of the Fourier form, with j a point of y.
+//   k_deposit_fh    TSC in x and along the y table (nodes and half-nodes), FP64 atomics
+//                   (Simulation::currents, src/sim_particles.cpp:88-106)
+//   k_cur_lines_fh  per (half-cell, k_x) line: (1,2,1)/4 on the cell charges along y (nodes: zero at the walls;
+//                   half-nodes: mirrored), the y-mean of j_y removed at k_x = 0 (TEM), the x filter
+//                   (sim_particles.cpp:165-205); the zeta filter and the x transform are the rows kernel of
+//                   k_currents.cu
+//   k_march_fh      per k_x line, slices front to rear: the known parts of R and L, E_z on the nodes and B_z on
+//                   the half-nodes by two tridiagonal (Thomas) solves along y, then R and L (march_line,
+//                   src/sim_kernels.hpp:213-313)
+//   k_sp_psi_fh     sponge: the bound field psi = T^-1 (rho + gamma^-2 T^-1 d_zeta^2 rho), T = k_x^2 - Lap_y with
+//                   the precomputed LU factors, and R - R_b (sim_fields.cpp:199-232); then the rows kernel of
+//                   k_fields.cu (inverse x, mask, forward x) and k_sp_add_fh (+ R_b, R_x = 0 at the wall node)
+//   k_comoving_fh_* the co-moving start field in the eigenvectors of -Lap_y: projection of the charge, Thomas in
+//                   zeta per (eigenvalue, k_x), back to the nodes, R (sim_fields.cpp:44-151)
+// One thread per line; the recurrences along y and zeta are serial in the reference's order.
+#include "g3d_ctx.hpp"
+
+namespace g3d {
+
+namespace {
+__device__ __forceinline__ cpx ikx(double k, cpx z) { return ik(k, z); }     // i k_x z
+}  // namespace
+
+// ---------------------------------------------------------------- deposit
+__global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
+                                                   double* __restrict__ J) {
+    const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const long ip = perm[t];
+    if (P.alive[ip] != 1) return;
+    int m; double fz;
+    g.zax.locate(P.zeta[ip], m, fz);
+    const int hw = m - (g.a - 2);
+    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
+    const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
+    const double gm = sqrt(1 + px * px + py * py + pz * pz);
+    const double vx = px / gm, vy = py / gm, vz = pz / gm;
+    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
+    int ix[3], jn[3], jh[3]; double wx[3], wn[3], wh[3];
+    tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
+    tsc_y(g.yax, P.y[ip], jn, wn, jh, wh);
+    const long nk = g.nk, pl = long(g.nh) * nk;
+    double* J0 = J + long(hw) * nk;
+    for (int v = 0; v < 3; ++v) {
+        const bool nod = jn[v] >= 1 && jn[v] <= g.ny - 1, hal = jh[v] >= 0 && jh[v] <= g.ny - 1;
+        for (int u = 0; u < 3; ++u) {
+            if (nod) {
+                const long k = long(jn[v]) * g.nx + ix[u];
+                const double w = f * wx[u] * wn[v] * g.iA[jn[v]];
+                atomicAdd(J0 + k, w * vx / vz);
+                atomicAdd(J0 + 2 * pl + k, w);
+            }
+            if (hal) {
+                const long k = long(jh[v]) * g.nx + ix[u];
+                atomicAdd(J0 + pl + k, f * wx[u] * wh[v] * g.iD[jh[v]] * vy / vz);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- filters along the y lines of the currents
+__global__ void k_cur_lines_fh(Geo g, cpx* __restrict__ jx, cpx* __restrict__ jy, cpx* __restrict__ jz, int kf, int keep0) {
+    const long nl = long(g.ns + 1) * g.H;
+    const long line = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (line >= nl) return;
+    const int H = g.H, ny = g.ny, kxi = int(line % H);
+    const long o = (line / H) * g.nkh + kxi;         // element j at o + j H
+    const double* ia = g.iA; const double* id = g.iD;
+    const double fx = g.filt[kxi];
+    if (kf) {
+        cpx* nodal[2] = {jx, jz};
+        for (int t = 0; t < 2; ++t) {                // nodes: charges Q_j = A_j J_j, Q = 0 at the walls
+            cpx* A = nodal[t];
+            cpx qm = C(0), q0 = A[o + H] / ia[1];
+            for (int j = 1; j < ny; ++j) {
+                const cpx qp = j + 1 < ny ? A[o + long(j + 1) * H] / ia[j + 1] : C(0);
+                A[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * ia[j];
+                qm = q0; q0 = qp;
+            }
+        }
+        cpx qm = jy[o] / id[0], q0 = qm;             // half-nodes: Q_j = Delta_j J_j, mirrored at the walls
+        for (int j = 0; j < ny; ++j) {
+            const cpx qp = j + 1 < ny ? jy[o + long(j + 1) * H] / id[j + 1] : q0;
+            jy[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * id[j];
+            qm = q0; q0 = qp;
+        }
+    }
+    cpx mean = C(0);
+    if (kxi == 0 && !keep0) {
+        for (int j = 0; j < ny; ++j) mean = mean + jy[o + long(j) * H] / id[j];
+        mean = mean / (g.yn[ny] - g.yn[0]);
+    }
+    jx[o] = C(0); jz[o] = C(0);
+    for (int j = 0; j < ny; ++j) {
+        const long k = o + long(j) * H;
+        jx[k] = fx * jx[k]; jz[k] = fx * jz[k]; jy[k] = fx * (jy[k] - mean);
+    }
+}
+
+// ---------------------------------------------------------------- the march of the k_x lines
+struct FhScratch { cpx *sRx, *sRy, *sLx, *sLy, *srhs; double* scp; };
+
+__global__ void __launch_bounds__(64) k_march_fh(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, cpx* __restrict__ Ez,
+                                                cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
+                                                const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
+                                                const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
+                                                const cpx* __restrict__ jkz, FhScratch sc, double D) {
+    const int ik = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ik >= g.H) return;
+    const int ny = g.ny, H = g.H;
+    const long nk = g.nkh;
+    const double kx = g.kxd[ik], kx2 = kx * kx;
+    const double* iD = g.iD; const double* iA = g.iA;
+    auto S = [&](cpx* A, int j) -> cpx& { return A[long(j) * H + ik]; };
+    double* scp = sc.scp;
+    for (int n = g.b - 1; n >= g.a; --n) {
+        const long P0 = long(n - g.a) * nk + ik;      // slice n of the block = half-cell n-1 (current planes)
+        const long P1 = P0 + nk;                      // slice n+1 = half-cell n
+        const double wl = g.wlo[n], wu = g.whi[n];
+        // known part of R (level s0 and the currents of both levels)
+        for (int j = 0; j < ny; ++j) {
+            const long o = P0 + long(j) * H;
+            if (j == 0) S(sc.sRx, 0) = C(0);
+            else {
+                const cpx Jx = wl * (j0x[o] + jkx[o]) + wu * (j0x[o + nk] + jkx[o + nk]);
+                const cpx bm = (Bz[o] - Bz[o - H]) * iA[j];
+                S(sc.sRx, j) = Rx[o] + D * (ikx(kx, Ez[o]) + bm) - D * Jx;
+            }
+            const cpx Jy = wl * (j0y[o] + jky[o]) + wu * (j0y[o + nk] + jky[o + nk]);
+            const cpx ezu = j + 1 < ny ? Ez[o + H] : C(0);
+            S(sc.sRy, j) = Ry[o] + D * ((ezu - Ez[o]) * iD[j] - ikx(kx, Bz[o])) - D * Jy;
+        }
+        if (n == g.N - 1) {             // front of the window: L = E_z = B_z = 0
+            for (int j = 0; j < ny; ++j) {
+                const long o = P0 + long(j) * H;
+                Rx[o] = S(sc.sRx, j); Ry[o] = S(sc.sRy, j); Ez[o] = C(0); Bz[o] = C(0); Lx[o] = C(0); Ly[o] = C(0);
+            }
+            continue;
+        }
+        auto nxt = [&](const cpx* A, int j) -> cpx { return (j < 0 || j >= ny) ? C(0) : A[P1 + long(j) * H]; };
+        auto pRx = [&](int j) { return nxt(Rx, j); };
+        auto pRy = [&](int j) { return nxt(Ry, j); };
+        auto pEz = [&](int j) { return j == 0 ? C(0) : nxt(Ez, j); };
+        auto pBz = [&](int j) { return nxt(Bz, j); };
+        auto pLx = [&](int j) { return nxt(Lx, j); };
+        auto pLy = [&](int j) { return nxt(Ly, j); };
+        const double h = g.hcg[n + 2], cc = 0.25 * h * (D + 0.25 * h);
+        // known part of L
+        for (int j = 0; j < ny; ++j) {
+            const long u = P1 + long(j) * H;          // half-cell n, level s1
+            if (j == 0) S(sc.sLx, 0) = C(0);
+            else {
+                const cpx bm = (pBz(j) - pBz(j - 1)) * iA[j];
+                S(sc.sLx, j) = pLx(j) - 0.25 * h * (ikx(kx, pEz(j)) - bm) - 0.5 * h * jkx[u];
+            }
+            const cpx bp = (pEz(j + 1) - pEz(j)) * iD[j];
+            S(sc.sLy, j) = pLy(j) - 0.25 * h * (ikx(kx, pBz(j)) + bp) - 0.5 * h * jky[u];
+        }
+        // E_z on the nodes 1..ny-1 (Dirichlet at the walls)
+        double cp = 0;
+        cpx dp = C(0);
+        for (int j = 1; j < ny; ++j) {
+            const cpx Qp = 0.5 * (-(ikx(kx, pRx(j) - pLx(j))) + ((pLy(j) - pRy(j)) - (pLy(j - 1) - pRy(j - 1))) * iA[j]);
+            const cpx SE = -(ikx(kx, S(sc.sRx, j) - S(sc.sLx, j))) +
+                           ((S(sc.sLy, j) - S(sc.sRy, j)) - (S(sc.sLy, j - 1) - S(sc.sRy, j - 1))) * iA[j];
+            const cpx r = pEz(j) - 0.5 * h * Qp - 0.25 * h * SE - h * jkz[P1 + long(j) * H];
+            const double lo = j > 1 ? -cc * iA[j] * iD[j - 1] : 0, up = j < ny - 1 ? -cc * iA[j] * iD[j] : 0;
+            const double den = 1 + cc * kx2 + cc * iA[j] * (iD[j - 1] + iD[j]) - lo * cp;
+            dp = (r - lo * dp) / den;
+            cp = up / den;
+            S(sc.srhs, j) = dp; scp[long(j) * H + ik] = cp;
+        }
+        {
+            cpx next = C(0);
+            for (int j = ny - 1; j >= 1; --j) { next = S(sc.srhs, j) - scp[long(j) * H + ik] * next; Ez[P0 + long(j) * H] = next; }
+            Ez[P0] = C(0);
+        }
+        // B_z on the half-nodes 0..ny-1 (Neumann)
+        cp = 0; dp = C(0);
+        for (int j = 0; j < ny; ++j) {
+            const cpx fu = j + 1 < ny ? pRx(j + 1) + pLx(j + 1) : C(0), f0 = pRx(j) + pLx(j);
+            const cpx Cp = 0.5 * (ikx(kx, pRy(j) + pLy(j)) - (fu - f0) * iD[j]);
+            const cpx su = j + 1 < ny ? S(sc.sRx, j + 1) + S(sc.sLx, j + 1) : C(0), s0 = S(sc.sRx, j) + S(sc.sLx, j);
+            const cpx SB = ikx(kx, S(sc.sRy, j) + S(sc.sLy, j)) - (su - s0) * iD[j];
+            const cpx r = pBz(j) - 0.5 * h * Cp - 0.25 * h * SB;
+            const double al = j > 0 ? iA[j] : 0, au = j < ny - 1 ? iA[j + 1] : 0;
+            const double lo = -cc * iD[j] * al, up = -cc * iD[j] * au;
+            const double den = 1 + cc * kx2 + cc * iD[j] * (al + au) - lo * cp;
+            dp = (r - lo * dp) / den;
+            cp = up / den;
+            S(sc.srhs, j) = dp; scp[long(j) * H + ik] = cp;
+        }
+        {
+            cpx next = C(0);
+            for (int j = ny - 1; j >= 0; --j) { next = S(sc.srhs, j) - scp[long(j) * H + ik] * next; Bz[P0 + long(j) * H] = next; }
+        }
+        // R and L
+        for (int j = 0; j < ny; ++j) {
+            const long o = P0 + long(j) * H;
+            if (j == 0) { Rx[o] = C(0); Lx[o] = C(0); }
+            else {
+                const cpx bm = (Bz[o] - Bz[o - H]) * iA[j];
+                Rx[o] = S(sc.sRx, j) + D * (ikx(kx, Ez[o]) + bm);
+                Lx[o] = S(sc.sLx, j) - 0.25 * h * (ikx(kx, Ez[o]) - bm);
+            }
+            const cpx ezu = j + 1 < ny ? Ez[o + H] : C(0);
+            const cpx bp = (ezu - Ez[o]) * iD[j];
+            Ry[o] = S(sc.sRy, j) + D * (bp - ikx(kx, Bz[o]));
+            Ly[o] = S(sc.sLy, j) - 0.25 * h * (ikx(kx, Bz[o]) + bp);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- sponge
+// psi of the slice charge per (slice, k_x) line into PSI; U = R_x - R_bx, V = R_y - R_by
+__global__ void k_sp_psi_fh(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry, const cpx* __restrict__ jz,
+                            cpx* __restrict__ U, cpx* __restrict__ V, cpx* __restrict__ PSI, double g2, double opb) {
+    const long nl = long(g.ns) * g.H;
+    const long line = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (line >= nl) return;
+    const int H = g.H, ny = g.ny, kxi = int(line % H), l = int(line / H), n = g.a + l;
+    const long nk = g.nkh, o = long(l) * nk + kxi;
+    const double* ia = g.iA; const double* id = g.iD;
+    auto half = [&](int hk, long jo) -> cpx {           // half-cell plane hk = -1 .. ns+1 (no ghosts on one rank)
+        if (hk < 0 || hk > g.ns) return C(0);
+        return jz[long(hk) * nk + kxi + jo];
+    };
+    auto rho_at = [&](int dl, long jo) -> cpx {          // charge of slice n + dl at the y offset jo
+        const int nn = n + dl;
+        if (nn < 0 || nn > g.N - 1) return C(0);
+        return g.wlo[nn] * half(l + dl, jo) + g.whi[nn] * half(l + dl + 1, jo);
+    };
+    const double hm = g.hcg[n + 1], hp = g.hcg[n + 2];
+    const double cm = 2 / ((hm + hp) * hm), cp_ = 2 / ((hm + hp) * hp);
+    for (int second = 0; second < 2; ++second) {         // T^-1 of the d_zeta^2 term, then of rho + that
+        cpx dpv = C(0);
+        for (int j = 1; j < ny; ++j) {
+            const long jo = long(j) * H, k = o + jo;
+            cpx r;
+            if (!second) r = g2 * (cp_ * rho_at(1, jo) - (cm + cp_) * rho_at(0, jo) + cm * rho_at(-1, jo));
+            else r = rho_at(0, jo) + PSI[k];
+            const double lo = j > 1 ? -ia[j] * id[j - 1] : 0;
+            dpv = (r - lo * dpv) * g.pid[long(j) * H + kxi];
+            PSI[k] = dpv;
+        }
+        cpx next = C(0);
+        for (int j = ny - 1; j >= 1; --j) {
+            next = PSI[o + long(j) * H] - g.pcp[long(j) * H + kxi] * next;
+            PSI[o + long(j) * H] = next;
+        }
+    }
+    PSI[o] = C(0);
+    const double kx = g.kxd[kxi];
+    for (int j = 0; j < ny; ++j) {
+        const long k = o + long(j) * H;
+        const cpx pu = j + 1 < ny ? PSI[k + H] : C(0);
+        const cpx bx = -opb * ikx(kx, PSI[k]), by = -opb * ((pu - PSI[k]) * id[j]);
+        U[k] = Rx[k] - bx; V[k] = Ry[k] - by;
+    }
+}
+// after the mask: R = (masked R - R_b) + R_b, R_x = 0 at the wall node
+__global__ void k_sp_add_fh(Geo g, const cpx* __restrict__ U, const cpx* __restrict__ V, const cpx* __restrict__ PSI,
+                            cpx* __restrict__ Rx, cpx* __restrict__ Ry, double opb) {
+    const long n = long(g.ns) * g.nkh;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long i = idx % g.nkh;
+        const int j = int(i / g.H), kxi = int(i % g.H);
+        const cpx pu = j + 1 < g.ny ? PSI[idx + g.H] : C(0);
+        const cpx bx = -opb * ikx(g.kxd[kxi], PSI[idx]), by = -opb * ((pu - PSI[idx]) * g.iD[j]);
+        Rx[idx] = j == 0 ? C(0) : U[idx] + bx;
+        Ry[idx] = V[idx] + by;
+    }
+}
+
+// ---------------------------------------------------------------- co-moving start field
+// half-cell charges to the eigen-coefficients: E1[l][s][k_x] = sum_j evf[s][j] jz[l][j][k_x] (slot 0 stays 0)
+__global__ void k_comoving_fh_proj(Geo g, const cpx* __restrict__ jz, cpx* __restrict__ E1) {
+    const long n = long(g.ns + 1) * g.nkh;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long i = idx % g.nkh, base = idx - i;
+        const int s = int(i / g.H), kxi = int(i % g.H);
+        cpx v = C(0);
+        if (s > 0)
+            for (int j = 1; j < g.ny; ++j) v = v + g.evf[long(s) * g.ny + j] * jz[base + long(j) * g.H + kxi];
+        E1[idx] = v;
+    }
+}
+// per (eigenvalue slot, k_x): the tridiagonal system of -(k_x^2 + mu_s + gamma^-2 d_zeta^2) psi = rho along zeta
+__global__ void k_comoving_fh_thomas(Geo g, const cpx* __restrict__ E1, double* __restrict__ cpb, cpx* __restrict__ dpb,
+                                     double beta, double gm2) {
+    const long nk = g.nkh;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nk) return;
+    const int s = int(i / g.H), kxi = int(i % g.H);
+    const double kx = g.kxd[kxi], ev = g.evl[s];
+    double cprev = 0;
+    cpx dprev = C(0);
+    for (int l = 0; l < g.ns; ++l) {
+        const long o = long(l) * nk + i;
+        const int n = g.a + l;
+        const double hm = g.hcg[n + 1], hp = g.hcg[n + 2];
+        const double lo = -gm2 * 2 / ((hm + hp) * hm), up = -gm2 * 2 / ((hm + hp) * hp);
+        const double dg = kx * kx + ev + gm2 * 2 / (hm * hp);
+        if (s == 0 || dg == 0) { cpb[o] = 0; dpb[o] = C(0); continue; }
+        const cpx rhs = (1 / beta) * (g.wlo[n] * E1[o] + g.whi[n] * E1[o + nk]);
+        if (n == 0) { cprev = 0; dprev = C(0); }
+        const double den = dg - lo * cprev;
+        const double cpv = up / den;
+        const cpx dpv = (rhs - lo * dprev) / den;
+        cpb[o] = cpv; dpb[o] = dpv;
+        cprev = cpv; dprev = dpv;
+    }
+    cpx next = C(0);
+    for (int l = g.ns - 1; l >= 0; --l) {
+        const long o = long(l) * nk + i;
+        next = dpb[o] - cpb[o] * next;
+        dpb[o] = next;
+    }
+}
+// back to the nodes: psi[l][j][k_x] = sum_s evb[j][s] psi_s (psi = 0 at the wall node)
+__global__ void k_comoving_fh_back(Geo g, const cpx* __restrict__ psis, cpx* __restrict__ psi) {
+    const long n = long(g.ns) * g.nkh;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long i = idx % g.nkh, base = idx - i;
+        const int j = int(i / g.H), kxi = int(i % g.H);
+        cpx v = C(0);
+        if (j > 0)
+            for (int s = 1; s < g.ny; ++s) v = v + g.evb[long(j) * g.ny + s] * psis[base + long(s) * g.H + kxi];
+        psi[idx] = v;
+    }
+}
+// R = -(1 + beta) E_perp of psi, E_z = B_z = 0
+__global__ void k_comoving_fh_field(Geo g, const cpx* __restrict__ psi, cpx* __restrict__ Rx, cpx* __restrict__ Ry,
+                                    cpx* __restrict__ Ez, cpx* __restrict__ Bz, double beta) {
+    const long n = long(g.ns) * g.nkh;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const long i = idx % g.nkh;
+        const int j = int(i / g.H), kxi = int(i % g.H);
+        Rx[idx] = -(1 + beta) * ikx(g.kxd[kxi], psi[idx]);
+        const cpx up = j + 1 < g.ny ? psi[idx + g.H] : C(0);
+        Ry[idx] = -(1 + beta) * ((up - psi[idx]) * g.iD[j]);
+        Ez[idx] = C(0); Bz[idx] = C(0);
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static unsigned ew_blocks(long n) {
+    long b = (n + 255) / 256;
+    return unsigned(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+void launch_deposit_fh(Ctx& c) {
+    c.jw.zero(c.stream);
+    if (c.np == 0) return;
+    const int tok = c.prof_begin("deposit");
+    k_deposit_fh<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p);
+    c.check_launch("k_deposit_fh");
+    c.prof_end(tok);
+}
+void launch_cur_fft_fh(Ctx& c, bool keep0) {
+    launch_cur_rows_to_jk(c);
+    const long nl = long(c.ns + 1) * c.H;
+    const int tok = c.prof_begin("cur_lines");
+    k_cur_lines_fh<<<unsigned((nl + 127) / 128), 128, 0, c.stream>>>(c.geo(), c.jkx.p, c.jky.p, c.jkz.p, c.P.k_filter ? 1 : 0,
+                                                                      keep0 ? 1 : 0);
+    c.check_launch("k_cur_lines_fh");
+    c.prof_end(tok);
+}
+void launch_march_fh(Ctx& c, double D) {
+    const size_t ln = size_t(c.ny) * c.H;
+    FhScratch sc{c.fhs.p, c.fhs.p + ln, c.fhs.p + 2 * ln, c.fhs.p + 3 * ln, c.fhs.p + 4 * ln, c.fhcp.p};
+    const int tok = c.prof_begin("march");
+    k_march_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
+                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D);
+    c.check_launch("k_march_fh");
+    c.prof_end(tok);
+}
+void launch_sponge_fh(Ctx& c) {
+    const long nl = long(c.ns) * c.H;
+    const double opb = 1 + c.beta_b;
+    int tok = c.prof_begin("sponge_psi");
+    k_sp_psi_fh<<<unsigned((nl + 127) / 128), 128, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.jkz.p, c.W[0].p, c.W[1].p,
+                                                                   c.W[3].p, c.gm2_b, opb);
+    c.check_launch("k_sp_psi_fh");
+    c.prof_end(tok);
+    launch_sp_rows(c);
+    tok = c.prof_begin("sponge_add");
+    k_sp_add_fh<<<ew_blocks(long(c.ns) * c.nkh), 256, 0, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p, c.W[3].p, c.Rx.p, c.Ry.p, opb);
+    c.check_launch("k_sp_add_fh");
+    c.prof_end(tok);
+}
+// scratch: W0 the eigen-coefficients of the charge, W3 psi_s, W2 psi on the nodes (W4, W5 hold the copies of R
+// that relax_start_field makes around this call)
+void launch_comoving_fh(Ctx& c, double beta, double gm2) {
+    const int tok = c.prof_begin("comoving");
+    const Geo g = c.geo();
+    k_comoving_fh_proj<<<ew_blocks(long(c.ns + 1) * c.nkh), 256, 0, c.stream>>>(g, c.jkz.p, c.W[0].p);
+    c.check_launch("k_comoving_fh_proj");
+    k_comoving_fh_thomas<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(g, c.W[0].p, c.rscratch.p, c.W[3].p, beta, gm2);
+    c.check_launch("k_comoving_fh_thomas");
+    k_comoving_fh_back<<<ew_blocks(long(c.ns) * c.nkh), 256, 0, c.stream>>>(g, c.W[3].p, c.W[2].p);
+    c.check_launch("k_comoving_fh_back");
+    k_comoving_fh_field<<<ew_blocks(long(c.ns) * c.nkh), 256, 0, c.stream>>>(g, c.W[2].p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, beta);
+    c.check_launch("k_comoving_fh_field");
+    c.prof_end(tok);
+}
+
+}  // namespace g3d

@@ -29,8 +29,29 @@ __device__ __forceinline__ void gather(const PushArgs& c, double x, double y, do
     if (fl < 0 || fl > g.ns) return;
     int ix[3], jn[3]; double wx[3], wn[3];
     tsc_periodic(x, g.dx, g.nx, ix, wx);
-    tsc_periodic(y, g.dy, g.ny, jn, wn);
     const long nk = g.nk;
+    if (!g.yf) {                       // free-hand y: E_y, B_x, B_z on the half-nodes, nothing beyond the walls
+        int jh[3]; double wh[3];
+        tsc_y(g.yax, y, jn, wn, jh, wh);
+        for (int comp = 0; comp < 6; ++comp) {
+            const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
+            const float* p1 = p0 + nk;
+            const bool hf = is_half(comp);
+            const int* jj = hf ? jh : jn;
+            const double* wy = hf ? wh : wn;
+            double v = 0;
+            for (int j = 0; j < 3; ++j) {
+                if (jj[j] < 0 || jj[j] >= g.ny) continue;
+                for (int i = 0; i < 3; ++i) {
+                    const long k = long(jj[j]) * g.nx + ix[i];
+                    v += wx[i] * wy[j] * ((1 - fz) * double(__ldg(p0 + k)) + fz * double(__ldg(p1 + k)));
+                }
+            }
+            if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+        }
+        return;
+    }
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
 #pragma unroll
     for (int comp = 0; comp < 6; ++comp) {
         const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
@@ -52,7 +73,7 @@ __device__ __forceinline__ bool rhs(const PushArgs& c, const St& Y, double z, do
     if (Y.pz < 0.3 * g) return false;
     const double gm = (1 + Y.px * Y.px + Y.py * Y.py) / (g + Y.pz);
     double E[3], B[3], Ee[3], Be[3];
-    gather(c, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, E, B);
+    gather(c, wrap_periodic(Y.x, c.g.Lx), c.g.yf ? wrap_periodic(Y.y, c.g.Ly) : Y.y, Y.zeta, E, B);
     c.laser.field(Y.x + c.X0, z, z - (Y.zeta - c.zc), Ee, Be);
 #pragma unroll
     for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
@@ -135,7 +156,9 @@ void launch_push(Ctx& c, double s0, double s1) {
     a.F = c.F.p; a.g = c.geo(); a.laser = c.laser;
     a.X0 = c.X0; a.Y0 = c.Y0; a.zc = c.P.zeta_center; a.dz_push = c.P.dz_push; a.push_phase = c.P.push_phase;
     a.zhand = -1e300;                                   // one rank: nothing is handed over
-    a.zmax = c.zeta[c.N - 1]; a.ylo = -1e300; a.yhi = 1e300; a.s1 = s1; a.hmin = c.hmin;
+    a.zmax = c.zeta[c.N - 1]; a.s1 = s1; a.hmin = c.hmin;
+    a.ylo = c.yf ? -1e300 : c.ynode_h[1];              // free-hand y: lost within one cell of a wall
+    a.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
     a.vz_min = c.pl ? c.pl->cfg.vz_min : 0;            // slower beam particles stream in the plasma march
     a.freeze = c.P.freeze_bunch; a.self = c.P.self_fields;
     const int tok = c.prof_begin("push");

@@ -1,12 +1,13 @@
 """Run configurations in code units (the reference's deck keys, docs/input_deck.md, set in code the way
 the reference's tests do with `base()`, tests/test_util.hpp:36-43).
 
-`baseline(k)` builds the five benchmark workloads of this project (k = 1..5) by their sizes:
+`baseline(k)` builds the benchmark workloads of this project by their sizes:
   1  frozen-bunch wake in vacuum: 64x64 modes, 256 slices (h = 0.5), 262,144 macro-electrons, 10 s-steps
   2  oblique plane wave on a bunch: 128x128 modes, 1024 slices (h = 0.1), 1,048,576 macro-electrons,
      a0 = 0.5, p polarisation, 20 mrad, flat top 60 with sin^2 ramps 10, 100 s-steps of 2
-  3-5 plasma runs (not built by this release; `baseline` raises for them)
-Every size can be reduced with keyword overrides for tests.
+  3  laser wakefield with streaming plasma: 256x256 modes, 2048 slices, H+ ions, a grid laser, a witness bunch
+Every size can be reduced with keyword overrides for tests. `freehand_small` builds a bunch on the free-hand y grid
+(a graded table of nodes between conducting walls).
 """
 import math
 from dataclasses import dataclass, field
@@ -48,6 +49,7 @@ class RunConfig:
     plasma: dict = None              # streaming plasma (g3d_plasma keys), None: vacuum
     ions: list = field(default_factory=list)
     glasers: list = field(default_factory=list)
+    ynode: np.ndarray = None         # free-hand y: the ny + 1 nodes (walls at the ends); None: Fourier y
 
     @property
     def zeta(self):
@@ -55,9 +57,14 @@ class RunConfig:
 
     def grid_struct(self):
         z = np.ascontiguousarray(self.zeta)
-        g = abi.Grid(self.nx, self.ny, self.nzeta, 1, self.Lx, self.Ly,
-                     z.ctypes.data_as(abi.C.POINTER(abi.C.c_double)), None)
-        return g, z            # keep z alive while g is used
+        if self.ynode is None:
+            g = abi.Grid(self.nx, self.ny, self.nzeta, 1, self.Lx, self.Ly,
+                         z.ctypes.data_as(abi.C.POINTER(abi.C.c_double)), None)
+            return g, z        # keep z alive while g is used
+        y = np.ascontiguousarray(self.ynode, dtype=np.float64)
+        g = abi.Grid(self.nx, self.ny, self.nzeta, 0, self.Lx, float(y[-1] - y[0]),
+                     z.ctypes.data_as(abi.C.POINTER(abi.C.c_double)), y.ctypes.data_as(abi.C.POINTER(abi.C.c_double)))
+        return g, (z, y)
 
     def params_struct(self):
         p = abi.Params()
@@ -266,3 +273,34 @@ def baseline(k, **kw):
     if k == 3:
         return config3(**kw)
     raise NotImplementedError(f"workload {k} is not built by this release")
+
+
+def graded_ynode(half, dy0, grow, core):
+    """Nodes of a free-hand y grid symmetric about 0: cells of dy0 for |y| < core, each further cell `grow` times
+    the previous one, `half` cells on each side (the walls at the ends)."""
+    pos = [0.0]
+    d = dy0
+    for _ in range(half):
+        if pos[-1] >= core:
+            d *= grow
+        pos.append(pos[-1] + d)
+    pos = np.array(pos)
+    return np.concatenate([-pos[:0:-1], pos])
+
+
+def freehand_small(nx=16, half=12, nzeta=32, nmacro=3000, steps=2, sponge=1.5, zeta_filter=1, k_filter=1):
+    """A frozen-bunch wake on the free-hand y grid (the structure of workload 5's y grid at test sizes): 16 Fourier
+    modes in x, 2 x 12 graded cells in y between walls (0.5 near the axis, growing by 12 % per cell beyond 2.5)."""
+    lam = 0.8e-6
+    y = graded_ynode(half, 0.5, 1.12, 2.5)
+    Lx = 12.0
+    h = 0.5 * (31 / (nzeta - 1))
+    window = h * (nzeta - 1)
+    zc = 0.6 * window
+    b = dict(charge_C=0.2e-12, gamma=200.0, sigx=1.0, sigy=1.0, sigz=2.0, emitx=0.1, emity=0.1, espread=1e-3,
+             zeta_center=zc, nmacro=nmacro, seed=5)
+    p = dict(lambda0=lam, dz=3.0, dz_push=3.0, z_end=3.0 * steps, sponge=sponge, sponge_y=sponge, zeta_center=zc,
+             zeta_filter=zeta_filter, k_filter=k_filter, move_x=0, move_y=0)
+    cfg = RunConfig("frozen bunch on the free-hand y grid", nx, 2 * half, nzeta, Lx, float(y[-1] - y[0]), h, p, [b], steps)
+    cfg.ynode = y
+    return cfg

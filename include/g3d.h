@@ -63,7 +63,8 @@ typedef struct g3d_particle {
 /* Grid (reference Config grid fields, src/sim.hpp:38-44). */
 typedef struct g3d_grid {
     int32_t nx, ny, nzeta;
-    int32_t y_fourier;          /* 1: Fourier y (the only form of this release); 0: free-hand y */
+    int32_t y_fourier;          /* 1: Fourier y (periodic); 0: free-hand y between walls (the FP64 form without
+                                   streaming plasma or grid lasers in this release) */
     double Lx, Ly;
     const double* zeta;         /* nzeta slice positions, zeta[0] = 0 (rear) ... zeta[nzeta-1] = window */
     const double* ynode;        /* ny+1 node positions of the free-hand y grid, NULL for Fourier y */

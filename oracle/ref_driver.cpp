@@ -38,8 +38,16 @@ int fail(const std::exception& e) { g_err = e.what(); return G3D_ERR_ARG; }
 Config make_config(const g3d_grid* g, const g3d_params* p) {
     Config c = Config::base_units(p->lambda0);
     c.nx = g->nx; c.Lx = g->Lx;
-    if (!g->y_fourier) throw std::runtime_error("oracle driver: free-hand y needs ynode; not wired");
-    c.y_uniform(g->ny, g->Ly);
+    if (g->y_fourier) {
+        c.y_uniform(g->ny, g->Ly);
+    } else {                        // free-hand y: the node table as Config::y_table leaves it (walls at 0 and ny)
+        if (!g->ynode) throw std::runtime_error("oracle driver: free-hand y needs ynode");
+        c.ny = g->ny;
+        c.ynode.assign(g->ynode, g->ynode + g->ny + 1);
+        c.y_fourier = false; c.move_y = false;
+        c.Ly = c.ynode.back() - c.ynode.front();
+        c.y_change = 0;
+    }
     // zeta: copy the slice table; zeta_uniform when it is uniform (sim_config.cpp:14-20)
     c.nzeta = g->nzeta;
     c.zeta.assign(g->zeta, g->zeta + g->nzeta);
