@@ -203,6 +203,9 @@ void launch_march_fh(Ctx& c, double D);
 void launch_sponge_fh(Ctx& c);
 void launch_real_fields_fh(Ctx& c);
 void launch_comoving_fh(Ctx& c, double beta, double gm2);
+void launch_march_slice_fh(Ctx& c, double D, int n);
+void launch_real_fields_slice_fh(Ctx& c, int l);
+void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2);
 void launch_sp_rows(Ctx& c);                // k_fields.cu
 void launch_cur_rows_to_jk(Ctx& c);         // k_currents.cu
 void launch_sponge(Ctx& c);

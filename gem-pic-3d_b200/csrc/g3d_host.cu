@@ -973,14 +973,12 @@ int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ct
 int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
     return guarded(ctx, [&] {
         if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
-        if (!ctx->c.yf) throw Error(G3D_ERR_ARG, "streaming plasma on the free-hand y grid is not in this release");
         g3d::set_plasma(ctx->c, *plasma, ions, nions);
     });
 }
 int g3d_add_grid_laser(g3d_ctx* ctx, const g3d_grid_laser* laser) {
     return guarded(ctx, [&] {
         if (!laser || !(laser->waist > 0) || !(laser->tau > 0)) throw Error(G3D_ERR_ARG, "grid laser: waist and tau must be positive");
-        if (!ctx->c.yf) throw Error(G3D_ERR_ARG, "grid lasers on the free-hand y grid are not in this release");
         ctx->c.glasers.push_back(*laser);
     });
 }

@@ -163,7 +163,11 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     const int nx = c.nx, ny = c.ny, px = P.cfg.ppc_x, py = P.cfg.ppc_y;
     const double zf = c.zeta[size_t(c.N - 1)];
     for (int j = 0; j < ny; ++j) {
-        const double y0 = j * c.dy, hy = c.dy;
+        double y0 = j * c.dy, hy = c.dy;
+        if (!c.yf) {                                     // free-hand y: no plasma in the cells at the walls
+            if (j == 0 || j == ny - 1) continue;
+            y0 = c.ynode_h[size_t(j)]; hy = c.ynode_h[size_t(j) + 1] - c.ynode_h[size_t(j)];
+        }
         for (int i = 0; i < nx; ++i)
             for (int b2 = 0; b2 < py; ++b2)
                 for (int a2 = 0; a2 < px; ++a2) {
@@ -262,7 +266,8 @@ static uint64_t mix64h(uint64_t z) {
 }
 
 static void real_fields_slice(Ctx& c, int l) {
-    if (c.mixed) launch_real_fields_slice_f(c, l);
+    if (!c.yf) launch_real_fields_slice_fh(c, l);
+    else if (c.mixed) launch_real_fields_slice_f(c, l);
     else launch_real_fields_slice(c, l);
 }
 
@@ -308,6 +313,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.Delta = Delta; sa.vz_beam = P.cfg.vz_beam;
         sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p;
         sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
+        sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
             launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
@@ -415,26 +421,35 @@ void collect_restreaming(Ctx& c) {
 // ---------------------------------------------------------------- grid lasers (add_grid_lasers)
 // The transverse profile exp(-(x^2 + y^2) / (w^2 qb)) / qb of a paraxial beam is separable; its two real parts
 // are transformed once, and every slice adds 2 Re(c_n P) (c_n = amp env_n carrier_n) times the polarisation.
+// Free-hand y: R_x on the nodes (zero at the wall node j = 0) and R_y on the half-nodes, so the profile is taken at
+// both (planes 0, 1 and 3, 4; planes 2 and 5 stay zero) and transformed along x only.
+__device__ __forceinline__ void glaser_point(double xp, double yp, double w2, double qr, double qi, double& re, double& im) {
+    // exp(-(r^2/w^2) / qb) / qb, qb = qr + i qi
+    const double r2 = (xp * xp + yp * yp) / w2;
+    const double d = qr * qr + qi * qi;
+    const double ir = qr / d, ii = -qi / d;                   // 1 / qb
+    const double er = -r2 * ir, ei = -r2 * ii;
+    const double m = exp(er);
+    const double pr = m * cos(ei), pi = m * sin(ei);          // exp(-r^2/(w^2 qb))
+    re = pr * ir - pi * ii;                                   // real part of the product with 1/qb
+    im = pr * ii + pi * ir;                                   // imaginary part
+}
 __global__ void k_glaser_profile(Geo g, double X0, double Y0, double w2, double qr, double qi, double* __restrict__ out) {
     const long nk = g.nk;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nk; i += long(gridDim.x) * blockDim.x) {
         const int ix = int(i % g.nx), j = int(i / g.nx);
-        const double xp = ix * g.dx + X0, yp = j * g.dy + Y0;
-        // exp(-(r^2/w^2) / qb) / qb, qb = qr + i qi
-        const double r2 = (xp * xp + yp * yp) / w2;
-        const double d = qr * qr + qi * qi;
-        const double ir = qr / d, ii = -qi / d;                   // 1 / qb
-        const double er = -r2 * ir, ei = -r2 * ii;
-        const double m = exp(er);
-        const double pr = m * cos(ei), pi = m * sin(ei);          // exp(-r^2/(w^2 qb))
-        out[i] = pr * ir - pi * ii;                               // real part of the product with 1/qb
-        out[nk + i] = pr * ii + pi * ir;                          // imaginary part
+        const double xp = ix * g.dx + X0;
+        if (g.yf) { glaser_point(xp, j * g.dy + Y0, w2, qr, qi, out[i], out[nk + i]); continue; }
+        if (j == 0) { out[i] = 0; out[nk + i] = 0; }
+        else glaser_point(xp, g.yn[j], w2, qr, qi, out[i], out[nk + i]);
+        glaser_point(xp, 0.5 * (g.yn[j] + g.yn[j + 1]), w2, qr, qi, out[3 * nk + i], out[4 * nk + i]);
     }
 }
-__global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __restrict__ PI, const double* __restrict__ cre,
-                             const double* __restrict__ cim, cpx* __restrict__ Rx, cpx* __restrict__ Ry, double ax, double ay,
-                             double bx, double by) {
-    // R_x += 2 (ax (cre PR - cim PI) + bx (cim PR + cre PI)), R_y likewise with ay, by (real-valued field factors)
+__global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __restrict__ PI, const cpx* __restrict__ QR,
+                             const cpx* __restrict__ QI, const double* __restrict__ cre, const double* __restrict__ cim,
+                             cpx* __restrict__ Rx, cpx* __restrict__ Ry, double ax, double ay, double bx, double by) {
+    // R_x += 2 (ax (cre PR - cim PI) + bx (cim PR + cre PI)), R_y likewise with ay, by and the profile Q of the
+    // R_y points (real-valued field factors)
     const long nk = g.nkh, n = long(g.ns) * nk;
     for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
         const long l = idx / nk, i = idx - l * nk;
@@ -442,8 +457,9 @@ __global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __res
         if (cr == 0 && ci == 0) continue;
         const cpx re = cr * PR[i] - ci * PI[i];          // spectrum of Re(c P)
         const cpx im = ci * PR[i] + cr * PI[i];          // spectrum of Im(c P)
+        const cpx rq = cr * QR[i] - ci * QI[i], iq = ci * QR[i] + cr * QI[i];
         Rx[idx] = Rx[idx] + 2.0 * (ax * re + bx * im);
-        Ry[idx] = Ry[idx] + 2.0 * (ay * re + by * im);
+        Ry[idx] = Ry[idx] + 2.0 * (ay * rq + by * iq);
     }
 }
 
@@ -452,9 +468,10 @@ void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3);   // k_
 void add_grid_lasers(Ctx& c) {
     if (c.glasers.empty()) return;
     DevBuf<double> prof;
-    prof.alloc(size_t(3) * c.nk, c.stream);          // Re P, Im P, and a zero plane
+    prof.alloc(size_t(6) * c.nk, c.stream);          // Re P, Im P, a zero plane (free-hand y: twice)
+    G3D_CUDA(cudaMemsetAsync(prof.p, 0, size_t(6) * c.nk * sizeof(double), c.stream));
     DevBuf<cpx> spec, tsc;
-    spec.alloc(size_t(3) * c.nkh, c.stream);
+    spec.alloc(size_t(6) * c.nkh, c.stream);
     tsc.alloc(size_t(3) * c.nkh, c.stream);
     DevBuf<double> coef;
     coef.alloc(size_t(2) * c.ns, c.stream);
@@ -475,14 +492,16 @@ void add_grid_lasers(Ctx& c) {
         k_glaser_profile<<<148 * 4, 256, 0, c.stream>>>(c.geo(), c.X0, c.Y0, Lz.waist * Lz.waist, qb.real(), qb.imag(), prof.p);
         c.check_launch("k_glaser_profile");
         launch_real_to_half3(c, prof.p, tsc.p, spec.p);
+        if (!c.yf) launch_real_to_half3(c, prof.p + 3 * c.nk, tsc.p, spec.p + 3 * c.nkh);
+        const cpx* q = c.yf ? spec.p : spec.p + 3 * c.nkh;      // the profile at the points of R_y
         G3D_CUDA(cudaMemcpyAsync(coef.p, cre.data(), size_t(c.ns) * 8, cudaMemcpyHostToDevice, c.stream));
         G3D_CUDA(cudaMemcpyAsync(coef.p + c.ns, cim.data(), size_t(c.ns) * 8, cudaMemcpyHostToDevice, c.stream));
         // linear: ex = Re(E) cos(pol), ey = Re(E) sin(pol); circular: ex = Re E, ey = helicity Im E
         double ax, ay, bx, by;
         if (Lz.circular) { ax = 1; bx = 0; ay = 0; by = Lz.helicity; }
         else { ax = rot.real(); bx = 0; ay = rot.imag(); by = 0; }
-        k_glaser_add<<<148 * 8, 256, 0, c.stream>>>(c.geo(), spec.p, spec.p + c.nkh, coef.p, coef.p + c.ns, c.Rx.p, c.Ry.p,
-                                                     ax, ay, bx, by);
+        k_glaser_add<<<148 * 8, 256, 0, c.stream>>>(c.geo(), spec.p, spec.p + c.nkh, q, q + c.nkh, coef.p, coef.p + c.ns,
+                                                     c.Rx.p, c.Ry.p, ax, ay, bx, by);
         c.check_launch("k_glaser_add");
         G3D_CUDA(cudaStreamSynchronize(c.stream));
     }

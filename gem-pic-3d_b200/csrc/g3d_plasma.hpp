@@ -35,6 +35,7 @@ struct StreamArgs {
     LaserDev laser;
     const StepVals* sv;
     double zc, Delta, vz_beam;
+    double ylo, yhi;           // free-hand y: a particle beyond these (within a cell of a wall) is lost
     int n, pass;
     double* J;                 // jsr: jx, jy, jz, rho-, rho+ of the half-cell (real planes)
     float* Jf;                 // the same planes in FP32 (the mixed form)

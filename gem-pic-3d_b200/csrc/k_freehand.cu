@@ -100,6 +100,77 @@ __global__ void k_cur_lines_fh(Geo g, cpx* __restrict__ jx, cpx* __restrict__ jy
     }
 }
 
+// ---------------------------------------------------------------- filters of the streaming current along y
+// per k_x line of one half-cell (Simulation::stream_spectra, src/sim_plasma.cpp:146-180): the (1,2,1)/4 filters of
+// the cell charges as for the beam (no TEM mean removed), j_x = j_z = 0 at the wall node, the x filter, then the
+// smoothing (1 - a^2 Lap_perp)^-1: (1 + a^2 (k_x^2 - b- b+)) f = g on the nodes (f = 0 at the walls, as E_z in the
+// march) and (1 + a^2 (k_x^2 - b+ b-)) f = g on the half-nodes (as B_z), by Thomas along y
+__global__ void k_ss_lines_fh(Geo g, const cpx* __restrict__ T, cpx* __restrict__ out, cpx* __restrict__ rhs,
+                              double* __restrict__ cpv, int kf, double a2) {
+    const int kxi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kxi >= g.H) return;
+    const int H = g.H, ny = g.ny;
+    const long nkh = g.nkh;
+    cpx* ox = out; cpx* oy = out + nkh; cpx* oz = out + 2 * nkh;
+    const long o = kxi;                              // element j at o + j H
+    for (int j = 0; j < ny; ++j) {
+        const long k = o + long(j) * H;
+        ox[k] = T[k]; oy[k] = T[nkh + k]; oz[k] = T[2 * nkh + k];
+    }
+    const double* ia = g.iA; const double* id = g.iD;
+    if (kf) {
+        cpx* nodal[2] = {ox, oz};
+        for (int t = 0; t < 2; ++t) {
+            cpx* A = nodal[t];
+            cpx qm = C(0), q0 = A[o + H] / ia[1];
+            for (int j = 1; j < ny; ++j) {
+                const cpx qp = j + 1 < ny ? A[o + long(j + 1) * H] / ia[j + 1] : C(0);
+                A[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * ia[j];
+                qm = q0; q0 = qp;
+            }
+        }
+        cpx qm = oy[o] / id[0], q0 = qm;
+        for (int j = 0; j < ny; ++j) {
+            const cpx qp = j + 1 < ny ? oy[o + long(j + 1) * H] / id[j + 1] : q0;
+            oy[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * id[j];
+            qm = q0; q0 = qp;
+        }
+    }
+    const double fx = g.filt[kxi];
+    ox[o] = C(0); oz[o] = C(0);
+    for (int j = 0; j < ny; ++j) {
+        const long k = o + long(j) * H;
+        ox[k] = fx * ox[k]; oy[k] = fx * oy[k]; oz[k] = fx * oz[k];
+    }
+    if (a2 <= 0) return;
+    const double kx2 = g.kxs[kxi] * g.kxs[kxi];
+    cpx* nodal[2] = {ox, oz};
+    for (int t = 0; t < 2; ++t) {
+        cpx* A = nodal[t];
+        double cp = 0; cpx dp = C(0);
+        for (int j = 1; j < ny; ++j) {
+            const double lo = j > 1 ? -a2 * ia[j] * id[j - 1] : 0, up = j < ny - 1 ? -a2 * ia[j] * id[j] : 0;
+            const double den = 1 + a2 * kx2 + a2 * ia[j] * (id[j - 1] + id[j]) - lo * cp;
+            dp = (A[o + long(j) * H] - lo * dp) / den;
+            cp = up / den;
+            rhs[o + long(j) * H] = dp; cpv[o + long(j) * H] = cp;
+        }
+        cpx next = C(0);
+        for (int j = ny - 1; j >= 1; --j) { next = rhs[o + long(j) * H] - cpv[o + long(j) * H] * next; A[o + long(j) * H] = next; }
+    }
+    double cp = 0; cpx dp = C(0);
+    for (int j = 0; j < ny; ++j) {
+        const double al = j > 0 ? ia[j] : 0, au = j < ny - 1 ? ia[j + 1] : 0;
+        const double lo = -a2 * id[j] * al, up = -a2 * id[j] * au;
+        const double den = 1 + a2 * kx2 + a2 * id[j] * (al + au) - lo * cp;
+        dp = (oy[o + long(j) * H] - lo * dp) / den;
+        cp = up / den;
+        rhs[o + long(j) * H] = dp; cpv[o + long(j) * H] = cp;
+    }
+    cpx next = C(0);
+    for (int j = ny - 1; j >= 0; --j) { next = rhs[o + long(j) * H] - cpv[o + long(j) * H] * next; oy[o + long(j) * H] = next; }
+}
+
 // ---------------------------------------------------------------- the march of the k_x lines
 struct FhScratch { cpx *sRx, *sRy, *sLx, *sLy, *srhs; double* scp; };
 
@@ -107,7 +178,7 @@ __global__ void __launch_bounds__(64) k_march_fh(Geo g, cpx* __restrict__ Rx, cp
                                                 cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
                                                 const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
                                                 const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
-                                                const cpx* __restrict__ jkz, FhScratch sc, double D) {
+                                                const cpx* __restrict__ jkz, FhScratch sc, double D, int n_top, int n_bot) {
     const int ik = blockIdx.x * blockDim.x + threadIdx.x;
     if (ik >= g.H) return;
     const int ny = g.ny, H = g.H;
@@ -116,7 +187,7 @@ __global__ void __launch_bounds__(64) k_march_fh(Geo g, cpx* __restrict__ Rx, cp
     const double* iD = g.iD; const double* iA = g.iA;
     auto S = [&](cpx* A, int j) -> cpx& { return A[long(j) * H + ik]; };
     double* scp = sc.scp;
-    for (int n = g.b - 1; n >= g.a; --n) {
+    for (int n = n_top; n >= n_bot; --n) {
         const long P0 = long(n - g.a) * nk + ik;      // slice n of the block = half-cell n-1 (current planes)
         const long P1 = P0 + nk;                      // slice n+1 = half-cell n
         const double wl = g.wlo[n], wu = g.whi[n];
@@ -374,9 +445,26 @@ void launch_march_fh(Ctx& c, double D) {
     FhScratch sc{c.fhs.p, c.fhs.p + ln, c.fhs.p + 2 * ln, c.fhs.p + 3 * ln, c.fhs.p + 4 * ln, c.fhcp.p};
     const int tok = c.prof_begin("march");
     k_march_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
-                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D);
+                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D, c.b - 1, c.a);
     c.check_launch("k_march_fh");
     c.prof_end(tok);
+}
+// the march of the one slice n (the streaming-plasma march, Simulation::march_slice, src/sim_plasma.cpp:186-196)
+void launch_march_slice_fh(Ctx& c, double D, int n) {
+    const size_t ln = size_t(c.ny) * c.H;
+    FhScratch sc{c.fhs.p, c.fhs.p + ln, c.fhs.p + 2 * ln, c.fhs.p + 3 * ln, c.fhs.p + 4 * ln, c.fhcp.p};
+    const int tok = c.prof_begin("march_slice");
+    k_march_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
+                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D, n, n);
+    c.check_launch("k_march_fh");
+    c.prof_end(tok);
+}
+// the lines of the streaming spectra: T0..T2 (the x spectra of the rows of j_x, j_y, j_z) -> out (3 half planes)
+void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2) {
+    const size_t ln = size_t(c.ny) * c.H;
+    k_ss_lines_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), T3, out3, c.fhs.p + 4 * ln, c.fhcp.p,
+                                                                 c.P.k_filter ? 1 : 0, a2);
+    c.check_launch("k_ss_lines_fh");
 }
 void launch_sponge_fh(Ctx& c) {
     const long nl = long(c.ns) * c.H;

@@ -50,9 +50,33 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
     if (fl < 0 || fl > g.ns) return;
     int ix[3], jn[3]; double wx[3], wn[3];
     tsc_periodic(x, g.dx, g.nx, ix, wx);
-    tsc_periodic(y, g.dy, g.ny, jn, wn);
     const long nk = g.nk;
     typedef typename std::conditional<F32, float, double>::type R;
+    if (!g.yf) {                       // free-hand y: E_y, B_x, B_z on the half-nodes, nothing beyond the walls
+        int jh[3]; double wh[3];
+        tsc_y(g.yax, y, jn, wn, jh, wh);
+        const R f1 = R(fz), f0 = R(1 - fz);
+        for (int comp = 0; comp < 6; ++comp) {
+            const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
+            const float* p1 = p0 + nk;
+            const bool hf = is_half(comp);
+            const int* jj = hf ? jh : jn;
+            const double* wy = hf ? wh : wn;
+            R v0 = 0, v1 = 0;
+            for (int j = 0; j < 3; ++j) {
+                if (jj[j] < 0 || jj[j] >= g.ny) continue;
+                for (int i = 0; i < 3; ++i) {
+                    const long k = long(jj[j]) * g.nx + ix[i];
+                    const R w = R(wx[i] * wy[j]);
+                    v0 += w * R(p0[k]); v1 += w * R(p1[k]);
+                }
+            }
+            const double v = double(f0 * v0 + f1 * v1);
+            if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+        }
+        return;
+    }
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
     R w9[9];
     int k9[9];
 #pragma unroll
@@ -73,7 +97,7 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
     }
 }
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
-__device__ __forceinline__ double wrapy(const Geo& g, double y) { return wrap_periodic(y, g.Ly); }
+__device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
 // TSC deposit of f (v, 1) at (x, y) into jsr: jx, jy, jz and the charge of negative (plane 3) or positive
 // (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y). F32: into the FP32 planes.
@@ -83,6 +107,31 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
     int ix_[3], jn[3]; double wx[3], wn[3];
     tsc_periodic(x, g.dx, g.nx, ix_, wx);
     const long nk = g.nk, cq = (f < 0 ? 3 : 4) * nk;
+    if (!g.yf) {                       // free-hand y: j_x, j_z and the charges on the nodes, j_y on the half-nodes
+        int jh[3]; double wh[3];
+        tsc_y(g.yax, y, jn, wn, jh, wh);
+        for (int v = 0; v < 3; ++v) {
+            const bool nod = jn[v] >= 1 && jn[v] <= g.ny - 1, hal = jh[v] >= 0 && jh[v] <= g.ny - 1;
+            for (int u = 0; u < 3; ++u) {
+                if (nod) {
+                    const long k = long(jn[v]) * g.nx + ix_[u];
+                    const double w = f * wx[u] * wn[v] * g.iA[jn[v]];
+                    if constexpr (F32) {
+                        atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[2 * nk + k], float(w * vz)); atomicAdd(&c.Jf[cq + k], float(w));
+                    } else {
+                        atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[2 * nk + k], w * vz); atomicAdd(&c.J[cq + k], w);
+                    }
+                }
+                if (hal) {
+                    const long k = long(jh[v]) * g.nx + ix_[u];
+                    const double w = f * wx[u] * wh[v] * g.iD[jh[v]] * vy;
+                    if constexpr (F32) atomicAdd(&c.Jf[nk + k], float(w));
+                    else atomicAdd(&c.J[nk + k], w);
+                }
+            }
+        }
+        return;
+    }
     tsc_periodic(y, g.dy, g.ny, jn, wn);
     const double ia0 = g.iA[0];
 #pragma unroll
@@ -234,6 +283,10 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double q = S.q[i], w = S.w[i];
     const double f = q * w * dt / (c.Delta * h * g.dx);
     if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, vx, vy, vz, true};
+    if (!g.yf && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
+        if (!c.dry) S.alive[i] = 0;
+        return d;
+    }
     if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
         ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), dt);
     if (trapped) {
@@ -541,11 +594,14 @@ void launch_stream_spectra(Ctx& c) {
     } else {
         G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p)));
     }
-    G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, P.tsp.p, P.jsn.p, a2, P.box_mean ? 1 : 0, 1));
+    if (!c.yf) launch_ss_lines_fh(c, P.tsp.p, P.jsn.p, a2);           // free-hand y: filters along the y lines
+    else G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, P.tsp.p, P.jsn.p, a2, P.box_mean ? 1 : 0, 1));
     c.prof_end(tok);
 }
-// plain transverse spectra (no filters) of three real planes: the grid-laser profile
+// plain transverse spectra (no filters) of three real planes: the grid-laser profile (free-hand y: the x spectra
+// of the rows alone)
 void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
+    if (!c.yf) { G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J3, out3))); return; }
     G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J3, T3)));
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
 }
@@ -606,6 +662,7 @@ void launch_correct(Ctx& c, int n, double q, int own) {
     c.check_launch("k_correct");
 }
 void launch_march_slice(Ctx& c, double D, int n) {
+    if (!c.yf) { launch_march_slice_fh(c, D, n); return; }
     const int tok = c.prof_begin("march_slice");
     const unsigned blocks = unsigned((c.nkh + 127) / 128);
     if (c.mixed) {

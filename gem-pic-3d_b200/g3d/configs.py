@@ -288,6 +288,17 @@ def graded_ynode(half, dy0, grow, core):
     return np.concatenate([-pos[:0:-1], pos])
 
 
+def on_freehand_y(cfg, half=14, dy0=0.5, grow=1.15, core=2.5):
+    """The same run on a free-hand y grid between walls: 2 x `half` graded cells (dy0 for |y| < core, each further
+    cell `grow` times the previous one)."""
+    y = graded_ynode(half, dy0, grow, core)
+    cfg.ynode = y
+    cfg.ny = 2 * half
+    cfg.Ly = float(y[-1] - y[0])
+    cfg.name += " on the free-hand y grid"
+    return cfg
+
+
 def freehand_small(nx=16, half=12, nzeta=32, nmacro=3000, steps=2, sponge=1.5, zeta_filter=1, k_filter=1):
     """A frozen-bunch wake on the free-hand y grid (the structure of workload 5's y grid at test sizes): 16 Fourier
     modes in x, 2 x 12 graded cells in y between walls (0.5 near the axis, growing by 12 % per cell beyond 2.5)."""

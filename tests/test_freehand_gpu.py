@@ -121,3 +121,80 @@ def test_run_matches_reference(sponge):
             assert rel_l2(p[f], q[f]) <= 1e-10, (tag, f)
     d, dr = s.diagnostics_sums(), r.diagnostics_sums()
     assert np.allclose(d, dr, rtol=1e-9, atol=1e-300)
+
+
+def compare_plasma_state(s, r, tol, tag):
+    assert_state({a: s.array(a) for a in FIELDS}, {a: r.array(a) for a in FIELDS}, FIELDS, tol, comp_tol=1e-5, tag=tag)
+    assert_state({a: s.array(a) for a in CURRENTS}, {a: r.array(a) for a in CURRENTS}, CURRENTS, tol, comp_tol=1e-5, tag=tag)
+    assert rel_l2(s.array("F"), r.array("F")) <= 1e-6, tag
+
+
+@needs_ref
+@pytest.mark.parametrize("ions,extrap,passes,smooth", [(True, 1, 2, 0.0), (False, 0, 1, 0.0), (True, 1, 2, 0.4)])
+def test_plasma_run_matches_reference(ions, extrap, passes, smooth):
+    """The streaming-plasma march on the free-hand y grid: a grid laser on the nodes and half-nodes, the plasma
+    lattice between the wall cells, the half-node deposit and gather of the streaming particles, the filters and
+    the smoothing along y, the march of one slice by the solves along y, and the walls."""
+    from g3d import Simulation, configs
+    cfg = configs.on_freehand_y(configs.lwfa_small(ions=ions, extrapolate=extrap, passes=passes, smooth=smooth))
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    compare_plasma_state(s, r, 1e-10, "init")
+    for k in range(2):
+        s.step(); r.step()
+        compare_plasma_state(s, r, 1e-10, f"step{k + 1}")
+        ps, pr = s.streaming_particles(), r.streaming_particles()
+        assert len(ps) == len(pr)
+        assert np.array_equal(ps["alive"], pr["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+            assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f, rel_l2(ps[f], pr[f]))
+        bs, br = s.host_particles(), r.host_particles()
+        assert np.array_equal(bs["alive"], br["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz"]:
+            assert rel_l2(bs[f], br[f]) <= 1e-10, (k, f)
+    assert s.status().np == r.status().np
+
+
+@needs_ref
+def test_plasma_walls_take_the_particles_that_reach_them():
+    """A narrow free-hand grid (walls at about +-4.6) with a strong driver: streaming electrons reach the wall
+    cells and leave the march, as in the reference."""
+    from g3d import Simulation, configs
+    cfg = configs.on_freehand_y(configs.lwfa_small(a0=3.0, n0=0.02, ions=False, passes=1, extrapolate=0),
+                                half=8, dy0=0.5, grow=1.1, core=2.0)
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    for k in range(2):
+        s.step(); r.step()
+        compare_plasma_state(s, r, 1e-9, f"step{k + 1}")
+    assert s.status().np == r.status().np
+    assert s.status().lost == r.status().lost
+
+
+@needs_ref
+def test_ionization_on_the_free_hand_grid():
+    from g3d import configs
+    cfg = configs.on_freehand_y(configs.ionization_small())
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    from g3d import Simulation
+    s = Simulation(cfg)
+    s.init()
+    for k in range(2):
+        s.step(); r.step()
+        ps, pr = sort_by_id(s.streaming_particles()), sort_by_id(r.streaming_particles())
+        assert len(ps) == len(pr), (len(ps), len(pr))
+        assert np.array_equal(ps["id"], pr["id"]) and np.array_equal(ps["sp"], pr["sp"])
+        assert np.array_equal(ps["q"], pr["q"])
+        assert np.array_equal(ps["alive"], pr["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz"]:
+            assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f)
+    assert len(ps[(ps["sp"] >= 50) & (ps["sp"] < 100)]) > 0, "the case must ionize"
+
+
+def sort_by_id(p):
+    return p[np.lexsort((np.round(p["x"], 6), np.round(p["zeta"], 6), p["sp"], p["id"]))]
