@@ -146,6 +146,8 @@ struct Ctx {
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
     bool mixed = false;                          // G3D_PREC_MIXED: the spectra above except Rx, Ry are not allocated
+    bool f32s = false;                           // G3D_PREC_MIXED: FP32 gathers and deposit of the streaming plasma
+                                                 // (free-hand y: the mixed form is this alone, the spectra stay FP64)
     MixedBufs mx;
     bool fields_ready = false;                   // init has run (the precision is fixed from then on)
     // particles

@@ -55,6 +55,7 @@ static void alloc_spectra(Ctx& c, bool mixed) {
         c.jw.alloc(3 * (ns + 3) * pl, s);
     }
     c.mixed = mixed;
+    c.f32s = mixed;
     c.jk_is_j0 = false;
     G3D_CUDA(cudaStreamSynchronize(s));
 }
@@ -62,9 +63,9 @@ static void alloc_spectra(Ctx& c, bool mixed) {
 static void set_precision(Ctx& c, int mode) {
     if (mode != G3D_PREC_FP64 && mode != G3D_PREC_MIXED) throw Error(G3D_ERR_ARG, "unknown precision " + std::to_string(mode));
     const bool mixed = mode == G3D_PREC_MIXED;
-    if (mixed == c.mixed) return;
+    if (mixed == c.f32s) return;
     if (c.fields_ready) throw Error(G3D_ERR_STATE, "the precision is set before g3d_init");
-    if (mixed && !c.yf) throw Error(G3D_ERR_ARG, "the mixed form needs the Fourier y grid");
+    if (!c.yf) { c.f32s = mixed; return; }       // free-hand y: FP32 streaming plasma, FP64 spectra
     alloc_spectra(c, mixed);
 }
 
@@ -255,7 +256,6 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     if (G.nzeta < 4 || !G.zeta) throw Error(G3D_ERR_ARG, "nzeta must be >= 4 with a zeta table");
     if (!(G.Lx > 0) || !(G.Ly > 0)) throw Error(G3D_ERR_ARG, "Lx, Ly must be positive");
     if (P.precision != G3D_FP64 && P.precision != G3D_MIXED) throw Error(G3D_ERR_ARG, "precision must be G3D_FP64 or G3D_MIXED");
-    if (!G.y_fourier && P.precision == G3D_MIXED) throw Error(G3D_ERR_ARG, "the mixed form needs the Fourier y grid");
     if (!(P.dz > 0) || !(P.dz_push > 0) || !(P.lambda0 > 0)) throw Error(G3D_ERR_ARG, "dz, dz_push, lambda0 must be positive");
     for (int m = 0; m + 1 < G.nzeta; ++m)
         if (!(G.zeta[m + 1] > G.zeta[m])) throw Error(G3D_ERR_ARG, "zeta slices must increase");
@@ -355,7 +355,10 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
         c.fhs.alloc(5 * size_t(ny) * c.H, s);
         c.fhcp.alloc(size_t(ny) * c.H, s);
     }
-    if (P.precision == G3D_MIXED) alloc_spectra(c, true);
+    if (P.precision == G3D_MIXED) {
+        if (c.yf) alloc_spectra(c, true);
+        else c.f32s = true;                      // free-hand y: FP32 streaming plasma, FP64 spectra
+    }
     G3D_CUDA(cudaStreamSynchronize(s));
 }
 

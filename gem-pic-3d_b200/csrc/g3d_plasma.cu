@@ -296,7 +296,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
     mixk(ptr(c.F.p)); mixk(ptr(P.strm.x)); mixk(ptr(P.born.x)); mixk(uint64_t(P.s.cap)); mixk(uint64_t(P.born_cap));
-    mixk(uint64_t(passes)); mixk(uint64_t(c.mixed)); mixk(ptr(c.Rx.p));
+    mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
     uint64_t dbits;
     std::memcpy(&dbits, &Delta, sizeof dbits);

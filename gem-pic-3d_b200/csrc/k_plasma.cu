@@ -561,7 +561,7 @@ void launch_stream(Ctx& c, const StreamArgs& a) {
     const int tok = c.prof_begin("stream");
     const long want = (P.s.cap + ST_NT - 1) / ST_NT;
     const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
-    if (c.mixed) k_stream<true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    if (c.f32s) k_stream<true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
     else k_stream<false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
     c.check_launch("k_stream");
     c.prof_end(tok);
@@ -589,7 +589,7 @@ void launch_stream_spectra(Ctx& c) {
     const int tok = c.prof_begin("stream_spectra");
     PlasmaState& P = *c.pl;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
-    if (c.mixed) {
+    if (c.f32s) {
         G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float>(c, P.jsrf.p, P.tsp.p)));
     } else {
         G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p)));
@@ -636,6 +636,9 @@ void launch_pass_prologue(Ctx& c, int n, int restore) {
     if (c.mixed)
         k_pass_prologue<cpxf, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.mx.Ez.p, c.mx.Bz.p, o, c.nkh,
                                                                           P.jsrf.p, nj, P.bcnt.p, restore);
+    else if (c.f32s)                  // free-hand y, mixed: FP64 spectra, FP32 streaming planes
+        k_pass_prologue<cpx, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
+                                                                         P.jsrf.p, nj, P.bcnt.p, restore);
     else
         k_pass_prologue<cpx, double><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
                                                                           P.jsr.p, nj, P.bcnt.p, restore);

@@ -50,9 +50,12 @@ class RunConfig:
     ions: list = field(default_factory=list)
     glasers: list = field(default_factory=list)
     ynode: np.ndarray = None         # free-hand y: the ny + 1 nodes (walls at the ends); None: Fourier y
+    zeta_table: np.ndarray = None    # free-hand zeta: the nzeta slice positions; None: uniform steps h
 
     @property
     def zeta(self):
+        if self.zeta_table is not None:
+            return np.asarray(self.zeta_table, dtype=np.float64)
         return np.arange(self.nzeta, dtype=np.float64) * self.h
 
     def grid_struct(self):
@@ -296,6 +299,44 @@ def on_freehand_y(cfg, half=14, dy0=0.5, grow=1.15, core=2.5):
     cfg.ny = 2 * half
     cfg.Ly = float(y[-1] - y[0])
     cfg.name += " on the free-hand y grid"
+    return cfg
+
+
+def graded_zeta(window, center, h_fine, h_coarse, grow, core):
+    """Slice positions 0 .. >= window: steps of h_fine within `core` of `center`, each further step `grow` times
+    the previous one up to h_coarse."""
+    def side(length):
+        pos, d, x = [0.0], h_fine, 0.0
+        while x < length:
+            if x >= core:
+                d = min(h_coarse, d * grow)
+            x += d
+            pos.append(x)
+        return np.array(pos)
+    back = center - side(center)[::-1]          # down to <= 0
+    front = center + side(window - center)[1:]   # up to >= window
+    z = np.concatenate([back, front])
+    return z - z[0]
+
+
+def on_graded_zeta(cfg, fine=0.5, coarse=2.0, grow=1.15, core=3.0):
+    """The same run on a free-hand zeta grid: steps of fine * h within `core` of the first bunch's centre (of the
+    laser's, without a bunch), growing by `grow` per slice up to coarse * h; bunch and laser keep their distance
+    from the window front."""
+    z0 = cfg.zeta
+    window = float(z0[-1])
+    c = cfg.bunches[0]["zeta_center"] if cfg.bunches else cfg.glasers[0]["zeta_c"]
+    z = graded_zeta(window, c, fine * cfg.h, coarse * cfg.h, grow, core)
+    d = z[-1] - window                          # keep every position's distance from the front
+    for b in cfg.bunches:
+        b["zeta_center"] += d
+    for g in cfg.glasers:
+        g["zeta_c"] += d
+    if "zeta_center" in cfg.params:
+        cfg.params["zeta_center"] += d
+    cfg.zeta_table = z
+    cfg.nzeta = len(z)
+    cfg.name += " on a graded zeta grid"
     return cfg
 
 

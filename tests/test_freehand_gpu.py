@@ -198,3 +198,47 @@ def test_ionization_on_the_free_hand_grid():
 
 def sort_by_id(p):
     return p[np.lexsort((np.round(p["x"], 6), np.round(p["zeta"], 6), p["sp"], p["id"]))]
+
+
+@needs_ref
+@pytest.mark.parametrize("ygrid", ["fourier", "freehand"])
+def test_graded_zeta_frozen_bunch(ygrid):
+    """A free-hand zeta grid (steps h/2 at the bunch growing by 15 % per slice to 2h): the graded zeta filter, the
+    slice weights w_lo, w_hi of the march, the half-cell locate of the deposit and gather, the zeta terms of the
+    sponge and of the co-moving field."""
+    from g3d import Simulation, configs
+    base = configs.config1(nx=16, ny=16, nzeta=48, nmacro=3000, steps=2) if ygrid == "fourier" else case()
+    cfg = configs.on_graded_zeta(base)
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    for tag in ["init", "step1", "step2"]:
+        if tag != "init":
+            s.step(); r.step()
+        assert_state({a: s.array(a) for a in FIELDS}, {a: r.array(a) for a in FIELDS}, FIELDS, 1e-10, tag=tag)
+        assert rel_l2(s.array("F"), r.array("F")) <= 1e-6, tag
+        p, q = s.host_particles(), r.host_particles()
+        assert np.array_equal(p["alive"], q["alive"]), tag
+        for f in ["x", "y", "zeta", "px", "py", "pz"]:
+            assert rel_l2(p[f], q[f]) <= 1e-10, (tag, f)
+
+
+@needs_ref
+def test_graded_zeta_plasma_on_the_free_hand_grid():
+    """The structure of the ionization-injection workload at test size: free-hand y and zeta, streaming plasma
+    with ions and a grid laser."""
+    from g3d import Simulation, configs
+    cfg = configs.on_graded_zeta(configs.on_freehand_y(configs.lwfa_small()))
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    compare_plasma_state(s, r, 1e-10, "init")
+    for k in range(2):
+        s.step(); r.step()
+        compare_plasma_state(s, r, 1e-10, f"step{k + 1}")
+        ps, pr = s.streaming_particles(), r.streaming_particles()
+        assert len(ps) == len(pr) and np.array_equal(ps["alive"], pr["alive"])
+        for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+            assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f)

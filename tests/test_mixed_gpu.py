@@ -141,3 +141,23 @@ def test_mixed_form_plasma_error_table(ions, passes):
     assert table["F"] <= TOL_FIELD
     for f in ["x", "y", "px", "py", "pz"]:
         assert table["plasma " + f] <= 1e-5, (f, table["plasma " + f])
+
+
+def test_mixed_form_free_hand_plasma_error_table():
+    """On the free-hand y grid the mixed form is the FP32 streaming plasma (gathers and deposit) over FP64 spectra
+    (the march there is the serial solves along y per k_x line, latency-bound, not bandwidth-bound): its
+    distance from the FP64 form on the small laser wakefield on a free-hand y and zeta grid, 3 s-steps."""
+    from g3d import configs
+    cfg = configs.on_graded_zeta(configs.on_freehand_y(configs.lwfa_small(extrapolate=1, passes=2)))
+    a = run_plasma(cfg, "fp64", 3)
+    b = run_plasma(cfg, "mixed", 3)
+    table = {n: rel_l2(b[n], a[n]) for n in FIELDS + ["F"]}
+    table["state"] = stacked_error(b, a, FIELDS)
+    assert len(b["strm"]) == len(a["strm"]) and b["np"] == a["np"]
+    for f in ["x", "y", "px", "py", "pz"]:
+        table["plasma " + f] = rel_l2(b["strm"][f], a["strm"][f])
+    print("mixed vs FP64, plasma on the free-hand y and zeta grid (3 steps):", {k: f"{v:.2e}" for k, v in table.items()})
+    assert table["state"] <= TOL_FIELD
+    assert table["F"] <= TOL_FIELD
+    for f in ["x", "y", "px", "py", "pz"]:
+        assert table["plasma " + f] <= 1e-5, (f, table["plasma " + f])
