@@ -142,6 +142,10 @@ struct Ctx {
     DevBuf<cpx> jzg;                             // 2 ghost planes of filtered j_z (zero on one rank)
     DevBuf<double> jw;                           // 3 x (ns+3) real planes
     DevBuf<float> F;                             // 6 x (ns+2) real planes
+    DevBuf<double> Fd;                           // exact fields: F kept in FP64 too, gathered by the beam push
+                                                 // (the differentiable forward of the gradient check), or empty
+    DevBuf<cpx> lmode;                           // laser mode coefficients per stored mode (ny x H), or empty
+    DevBuf<cpx> lspx, lspy;                      // the grid-laser spectra added at init before the coefficients
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
@@ -247,6 +251,16 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions);
 void march_plasma(Ctx& c, double s0, double s1);
 void collect_restreaming(Ctx& c);
 void add_grid_lasers(Ctx& c);
+// the adjoint march (k_adjoint.cu)
+void launch_adj_objective(Ctx& c, double* dev_out2);
+void launch_adj_seed(Ctx& c, double W, double* lam);
+void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const* lS);
+void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D);
+void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ);
+void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const double* lJ, double* lam);
+void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
+                     double* lam, double* lF, int* err);
+void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out);
 std::vector<g3d_particle> get_streaming(Ctx& c);
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)

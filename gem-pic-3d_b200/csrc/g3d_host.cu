@@ -573,6 +573,7 @@ static void relax_start_field(Ctx& c) {
     launch_axpy_c(c, c.Ry.p, dyr, 1.0, n);
 }
 static void shift_window(Ctx& c, int nxs, int nys) {
+    if (c.Fd.p) throw Error(G3D_ERR_STATE, "exact fields need a fixed window");
     materialize_jk(c);
     c.X0 += nxs * c.dx; c.Y0 += nys * c.dy;
     launch_shift(c, nxs, nys, nxs * c.dx, nys * c.dy);
@@ -829,6 +830,134 @@ static void read_checkpoint(Ctx& c, const char* path) {
     }
 }
 
+
+// ---------------------------------------------------------------- adjoint march
+// Laser mode coefficients a(k) (per stored mode [j][k_x]) multiply every grid laser's spectrum added at init;
+// the unmultiplied spectra are kept for the gradient. Before g3d_init.
+static void set_laser_modes(Ctx& c, const double* coef) {
+    if (c.fields_ready) throw Error(G3D_ERR_STATE, "the laser mode coefficients are set before g3d_init");
+    std::vector<cpx> a(size_t(c.nkh), C(1.0));
+    if (coef)
+        for (size_t i = 0; i < a.size(); ++i) a[i] = C(coef[2 * i], coef[2 * i + 1]);
+    c.lmode.upload(a, c.stream);
+    c.lspx.alloc(size_t(c.ns) * c.nkh, c.stream);
+    c.lspy.alloc(size_t(c.ns) * c.nkh, c.stream);
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+// Exact fields: the real fields are also kept in FP64 and the beam push gathers from them (the differentiable
+// forward that central differences are taken of). Before g3d_init, FP64 form.
+static void set_exact_fields(Ctx& c, bool on) {
+    if (c.fields_ready) throw Error(G3D_ERR_STATE, "exact fields are chosen before g3d_init");
+    if (on && c.mixed) throw Error(G3D_ERR_ARG, "exact fields are an option of the FP64 form");
+    if (on) c.Fd.alloc(c.F.n, c.stream);
+    else c.Fd.release();
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+// From the start field (right after g3d_init): K s-steps forward with a checkpoint of the beam (x, y, zeta,
+// p, alive) and of the real fields at every level, J = mean p_z of the live beam, then the reverse sweep
+// (k_adjoint.cu): per step the transposed real fields, march, currents, deposit and push. Out: J, dJ/da per
+// stored laser mode [j][k_x] (complex, interleaved) and dJ/dp of every particle at s = 0 [np][3], the start
+// field held fixed (its laser part is differentiated through init's march(0)). The forward leaves the run at
+// s = K dz, as K calls of g3d_step.
+static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p) {
+    if (K < 1) throw Error(G3D_ERR_ARG, "the adjoint march needs at least one s-step");
+    if (!c.yf) throw Error(G3D_ERR_ARG, "the adjoint march needs the Fourier y grid");
+    if (c.pl) throw Error(G3D_ERR_ARG, "the adjoint march of the streaming plasma is not in this release");
+    if (c.P.sponge > 0 || c.P.sponge_y > 0) throw Error(G3D_ERR_ARG, "the adjoint march needs sponge = 0");
+    if (c.P.move_x || c.P.move_y) throw Error(G3D_ERR_ARG, "the adjoint march needs a fixed window (move_x = move_y = 0)");
+    if (c.laser.on) throw Error(G3D_ERR_ARG, "the adjoint march differentiates grid lasers, not the analytic laser");
+    if (!c.P.self_fields || c.P.freeze_bunch) throw Error(G3D_ERR_ARG, "the adjoint march needs self fields and a free bunch");
+    if (!c.fields_ready || c.istep != 0) throw Error(G3D_ERR_STATE, "the adjoint march starts right after g3d_init");
+    if (grad_modes && !c.lmode.p) throw Error(G3D_ERR_STATE, "set the laser mode coefficients (g3d_set_laser_modes) before g3d_init");
+    const long np = c.np;
+    const size_t Fn = c.F.n, ns = size_t(c.ns), nkh = size_t(c.nkh), nk = size_t(c.nk);
+    const bool ex = c.Fd.p != nullptr;
+    cudaStream_t st = c.stream;
+    DevBuf<double> X, FD;
+    DevBuf<int32_t> AL;
+    DevBuf<float> FF;
+    X.alloc(size_t(K + 1) * 6 * size_t(np), st);
+    AL.alloc(size_t(K + 1) * size_t(np), st);
+    if (ex) FD.alloc(size_t(K + 1) * Fn, st);
+    else FF.alloc(size_t(K + 1) * Fn, st);
+    std::vector<double> sl(size_t(K + 1));
+    auto save = [&](int k) {
+        double* x = X.p + size_t(k) * 6 * size_t(np);
+        double* src[6] = {c.parts.x, c.parts.y, c.parts.zeta, c.parts.px, c.parts.py, c.parts.pz};
+        if (np > 0) {
+            for (int q = 0; q < 6; ++q)
+                G3D_CUDA(cudaMemcpyAsync(x + size_t(q) * np, src[q], size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
+            G3D_CUDA(cudaMemcpyAsync(AL.p + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        if (ex) G3D_CUDA(cudaMemcpyAsync(FD.p + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+        else G3D_CUDA(cudaMemcpyAsync(FF.p + size_t(k) * Fn, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
+        sl[size_t(k)] = c.s;
+    };
+    save(0);
+    for (int k = 1; k <= K; ++k) { step(c, false); save(k); }
+    DevBuf<double> jo;
+    jo.alloc(2, st);
+    launch_adj_objective(c, jo.p);
+    double jh[2];
+    G3D_CUDA(cudaMemcpyAsync(jh, jo.p, 16, cudaMemcpyDeviceToHost, st));
+    G3D_CUDA(cudaStreamSynchronize(st));
+    if (!(jh[1] > 0)) throw Error(G3D_ERR_STATE, "the adjoint march: no live particle at the end");
+    *J = jh[0] / jh[1];
+    // the reverse sweep
+    DevBuf<cpx> lSb[6], lj0b[2], ljkb[3], Wb[6];
+    for (auto& b : lSb) b.alloc(ns * nkh, st);
+    for (auto& b : lj0b) b.alloc((ns + 1) * nkh, st);
+    for (auto& b : ljkb) b.alloc((ns + 1) * nkh, st);
+    for (auto& b : Wb) b.alloc((ns + 1) * nkh, st);
+    DevBuf<double> lF, V, lJ, lam;
+    lF.alloc(Fn, st);
+    V.alloc(3 * (ns + 1) * nk, st);
+    lJ.alloc(3 * (ns + 3) * nk, st);
+    lam.alloc(6 * size_t(np), st);
+    DevBuf<int> err;
+    err.alloc(1, st);
+    cpx* lS[6]; cpx* lj0[2]; cpx* ljk[3]; cpx* W[6];
+    for (int q = 0; q < 6; ++q) { lS[q] = lSb[q].p; W[q] = Wb[q].p; }
+    if (np > 0) launch_adj_seed(c, jh[1], lam.p);
+    for (int k = K; k >= 1; --k) {
+        if (k < K) launch_adj_real_fields(c, lF.p, W, lS);
+        for (int q = 0; q < 2; ++q) { lj0b[q].zero(st); lj0[q] = lj0b[q].p; }
+        for (int q = 0; q < 3; ++q) ljk[q] = ljkb[q].p;
+        launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);
+        launch_adj_currents(c, ljk, W, V.p, lJ.p);
+        launch_adj_deposit(c, X.p + size_t(k) * 6 * np, AL.p + size_t(k) * np, lJ.p, lam.p);
+        for (int q = 0; q < 2; ++q) std::swap(ljkb[q].p, lj0b[q].p);     // jk of level k-1 as the j0 of step k
+        ljkb[2].zero(st);
+        lF.zero(st);
+        launch_adj_push(c, ex ? nullptr : FF.p + size_t(k - 1) * Fn, ex ? FD.p + size_t(k - 1) * Fn : nullptr,
+                        X.p + size_t(k - 1) * 6 * np, AL.p + size_t(k - 1) * np, sl[size_t(k - 1)], sl[size_t(k)], lam.p, lF.p, err.p);
+    }
+    // level 0: the real fields of the start field, then init's march(0) back to R with the lasers added
+    launch_adj_real_fields(c, lF.p, W, lS);
+    for (int q = 0; q < 2; ++q) { lj0b[q].zero(st); lj0[q] = lj0b[q].p; }
+    for (int q = 0; q < 3; ++q) ljk[q] = ljkb[q].p;
+    launch_adj_march(c, lS, lj0, ljk, 0.0);
+    int eh = 0;
+    G3D_CUDA(cudaMemcpyAsync(&eh, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (grad_modes) {
+        DevBuf<cpx> gm;
+        gm.alloc(nkh, st);
+        launch_adj_lmodes(c, lS[0], lS[1], gm.p);
+        G3D_CUDA(cudaMemcpyAsync(grad_modes, gm.p, nkh * sizeof(cpx), cudaMemcpyDeviceToHost, st));
+        G3D_CUDA(cudaStreamSynchronize(st));
+    }
+    if (grad_p && np > 0) {
+        std::vector<double> h(3 * size_t(np));
+        G3D_CUDA(cudaMemcpyAsync(h.data(), lam.p + 3 * size_t(np), 3 * size_t(np) * 8, cudaMemcpyDeviceToHost, st));
+        G3D_CUDA(cudaStreamSynchronize(st));
+        for (long i = 0; i < np; ++i)
+            for (int q = 0; q < 3; ++q) grad_p[3 * i + q] = h[size_t(q) * np + i];
+    }
+    G3D_CUDA(cudaStreamSynchronize(st));
+    if (eh & 1) throw Error(G3D_ERR_STATE, "the adjoint march: a particle in the handed-over state");
+    if (eh & 2) throw Error(G3D_ERR_CAPACITY, "the adjoint march: more than 64 push sub-steps in one s-step");
+}
+
 }  // namespace g3d
 
 // ================================================================ extern "C"
@@ -1083,5 +1212,15 @@ int g3d_profile_get(g3d_ctx* ctx, int32_t k, const char** name, int64_t* launche
     });
 }
 int64_t g3d_launch_count(const g3d_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
+
+int g3d_set_laser_modes(g3d_ctx* ctx, const double* coef) { return guarded(ctx, [&] { g3d::set_laser_modes(ctx->c, coef); }); }
+int g3d_set_exact_fields(g3d_ctx* ctx, int32_t on) { return guarded(ctx, [&] { g3d::set_exact_fields(ctx->c, on != 0); }); }
+int g3d_adjoint(g3d_ctx* ctx, int32_t nsteps, double* objective, double* grad_modes, double* grad_p) {
+    return guarded(ctx, [&] {
+        if (!objective) throw Error(G3D_ERR_ARG, "g3d_adjoint: objective is required");
+        g3d::adjoint(ctx->c, nsteps, objective, grad_modes, grad_p);
+        ctx->c.prof_collect();
+    });
+}
 
 }  // extern "C"

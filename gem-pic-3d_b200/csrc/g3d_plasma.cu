@@ -447,7 +447,8 @@ __global__ void k_glaser_profile(Geo g, double X0, double Y0, double w2, double 
 }
 __global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __restrict__ PI, const cpx* __restrict__ QR,
                              const cpx* __restrict__ QI, const double* __restrict__ cre, const double* __restrict__ cim,
-                             cpx* __restrict__ Rx, cpx* __restrict__ Ry, double ax, double ay, double bx, double by) {
+                             cpx* __restrict__ Rx, cpx* __restrict__ Ry, double ax, double ay, double bx, double by,
+                             const cpx* __restrict__ lm, cpx* __restrict__ sx, cpx* __restrict__ sy) {
     // R_x += 2 (ax (cre PR - cim PI) + bx (cim PR + cre PI)), R_y likewise with ay, by and the profile Q of the
     // R_y points (real-valued field factors)
     const long nk = g.nkh, n = long(g.ns) * nk;
@@ -458,8 +459,11 @@ __global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __res
         const cpx re = cr * PR[i] - ci * PI[i];          // spectrum of Re(c P)
         const cpx im = ci * PR[i] + cr * PI[i];          // spectrum of Im(c P)
         const cpx rq = cr * QR[i] - ci * QI[i], iq = ci * QR[i] + cr * QI[i];
-        Rx[idx] = Rx[idx] + 2.0 * (ax * re + bx * im);
-        Ry[idx] = Ry[idx] + 2.0 * (ay * rq + by * iq);
+        cpx ux = 2.0 * (ax * re + bx * im), uy = 2.0 * (ay * rq + by * iq);
+        if (sx) { sx[idx] = sx[idx] + ux; sy[idx] = sy[idx] + uy; }      // kept for the laser-mode gradient
+        if (lm) { ux = lm[i] * ux; uy = lm[i] * uy; }                     // the mode coefficients
+        Rx[idx] = Rx[idx] + ux;
+        Ry[idx] = Ry[idx] + uy;
     }
 }
 
@@ -501,7 +505,7 @@ void add_grid_lasers(Ctx& c) {
         if (Lz.circular) { ax = 1; bx = 0; ay = 0; by = Lz.helicity; }
         else { ax = rot.real(); bx = 0; ay = rot.imag(); by = 0; }
         k_glaser_add<<<148 * 8, 256, 0, c.stream>>>(c.geo(), spec.p, spec.p + c.nkh, q, q + c.nkh, coef.p, coef.p + c.ns,
-                                                     c.Rx.p, c.Ry.p, ax, ay, bx, by);
+                                                     c.Rx.p, c.Ry.p, ax, ay, bx, by, c.lmode.p, c.lspx.p, c.lspy.p);
         c.check_launch("k_glaser_add");
         G3D_CUDA(cudaStreamSynchronize(c.stream));
     }

@@ -1,0 +1,630 @@
+// The adjoint march: the reverse sweep of the s-steps of the beam and its fields (Fourier y), which the reference
+// does not have. It differentiates J = mean p_z of the live beam after K s-steps with respect to the laser
+// mode coefficients of the start field and the beam momenta at s = 0. Each kernel is the transposed program of
+// one forward kernel, in reverse order; every transform, filter and march coefficient is real or a multiple of
+// i k, so the transposes are the conjugated coefficients and the inverse transforms (no normalisation).
+//   k_adj_objective  J = sum w p_z / sum w over the live particles (one CTA, fixed order)
+//   k_adj_rf_rows/cols  transposed real fields (F <- IFFT of R, L, E_z + i B_z; sim_fields.cpp:282-292): forward
+//                    transforms of the field adjoints, the half-row fold of the Hermitian rows
+//   k_adj_march      transposed per-mode march (march_point, sim_kernels.hpp:173-210), slices rear to front
+//   k_adj_cur_cols/rows, k_adj_zfilter  transposed currents (filters, transforms, the zeta filter;
+//                    sim_particles.cpp:120-156)
+//   k_adj_deposit    transposed deposit (sim_particles.cpp:88-106): a gather of the current adjoints with the
+//                    TSC weights and their derivatives
+//   k_adj_push       transposed RK4 push (push_one, sim_kernels.hpp:98-149): the sub-steps recomputed from the
+//                    level's checkpoint with the same sub-step rule (frozen schedule), then reversed stage by
+//                    stage; the gather adjoint is a deposit of the field adjoints into dJ/dF
+//   k_adj_lmodes     dJ/d(laser mode coefficient) = sum over slices of conj(laser spectrum) dJ/dR
+#include "k_push.cuh"
+#include "k_fft.cuh"
+#include "k_dispatch.cuh"
+
+namespace g3d {
+
+namespace {
+__device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     // conj(i k) z
+constexpr int ANT = 128;          // threads of the row kernels
+constexpr int ACW = 8;            // columns per tile of the column kernels
+
+// derivative of the TSC weights with respect to the index coordinate (tsc_weights of g3d_common.cuh)
+__device__ __forceinline__ void tsc_dweights(double xi, double d[3]) {
+    const double f = xi - floor(xi + 0.5);
+    d[0] = -(0.5 - f); d[1] = -2 * f; d[2] = 0.5 + f;
+}
+// d(fz)/d(zeta) of AxisDev::locate at the cell i it returned
+__device__ __forceinline__ double locate_slope(const AxisDev& ax, int i) {
+    if (ax.uniform) return ax.ih;
+    if (i < 0) return 1 / (ax.X[1] - ax.X[0]);
+    if (i >= ax.n - 1) return 1 / (ax.X[ax.n - 1] - ax.X[ax.n - 2]);
+    return 1 / (ax.X[i + 1] - ax.X[i]);
+}
+}  // namespace
+
+// ---------------------------------------------------------------- objective
+__global__ void __launch_bounds__(1024) k_adj_objective(PartsDev P, long np, double* __restrict__ out) {
+    __shared__ double s0[1024], s1[1024];
+    double a = 0, b = 0;
+    for (long i = threadIdx.x; i < np; i += 1024)
+        if (P.alive[i] == 1) { a += P.w[i] * P.pz[i]; b += P.w[i]; }
+    s0[threadIdx.x] = a; s1[threadIdx.x] = b;
+    __syncthreads();
+    for (int s = 512; s > 0; s >>= 1) {
+        if (int(threadIdx.x) < s) { s0[threadIdx.x] += s0[threadIdx.x + s]; s1[threadIdx.x] += s1[threadIdx.x + s]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[0] = s0[0]; out[1] = s1[0]; }
+}
+// dJ/d(final state): w / W on p_z of the live particles
+__global__ void k_adj_seed(PartsDev P, long np, double W, double* __restrict__ lam) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= np) return;
+    for (int k = 0; k < 5; ++k) lam[k * np + i] = 0;
+    lam[5 * np + i] = P.alive[i] == 1 ? P.w[i] / W : 0.0;
+}
+
+// ---------------------------------------------------------------- transposed real fields
+// rows: per row of slice l, Lambda_R = (lEx + lBy)/2 + i (lEy - lBx)/2, Lambda_L = (lEx - lBy)/2 + i (lEy + lBx)/2,
+// Lambda_E = lEz + i lBz; their forward transforms times 1/nk, folded onto the half rows of the two fields of
+// each pair: lA(k) = z(k) + conj z(nx-k), lB(k) = -i z(k) + i conj z(nx-k) (mirror terms for 0 < k < nx/2)
+template <int NX>
+__global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __restrict__ lF, cpx* __restrict__ W0, cpx* __restrict__ W1,
+                                                    cpx* __restrict__ W2, cpx* __restrict__ W3, cpx* __restrict__ W4,
+                                                    cpx* __restrict__ W5) {
+    using S = FftShape<NX>;
+    constexpr int LPC = ANT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
+    extern __shared__ cpx sm[];
+    cpx* a0 = sm;
+    cpx* a1 = sm + LPC * RS;
+    cpx* a2 = sm + 2 * LPC * RS;
+    const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
+    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
+    for (int e = tid; e < LPC * NX; e += ANT) {
+        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
+        double f[6] = {0, 0, 0, 0, 0, 0};
+        if (row < g.ny) {
+            const long idx = fbase + long(row) * NX + p;
+            for (int k = 0; k < 6; ++k) f[k] = lF[k * fpl + idx];
+        }
+        const int q = rr * RS + p + (p >> 3);
+        a0[q] = C(0.5 * (f[0] + f[4]), 0.5 * (f[1] - f[3]));
+        a1[q] = C(0.5 * (f[0] - f[4]), 0.5 * (f[1] + f[3]));
+        a2[q] = C(f[2], f[5]);
+    }
+    __syncthreads();
+    const int r = tid / S::T, t = tid - r * S::T;
+    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
+    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
+    const double s = 1.0 / double(g.nk);
+    const long base = long(l) * g.nkh;
+    for (int e = tid; e < LPC * H; e += ANT) {
+        const int rr = e / H, kx = e - rr * H, row = r0 + rr;
+        if (row >= g.ny) continue;
+        const bool mirror = kx > 0 && kx < NX / 2;
+        const int km = NX - kx;
+        const long o = base + long(row) * H + kx;
+        cpx* outA[3] = {W0, W2, W4};
+        cpx* outB[3] = {W1, W3, W5};
+        const cpx* a[3] = {a0, a1, a2};
+        for (int pr = 0; pr < 3; ++pr) {
+            const cpx z = s * a[pr][rr * RS + kx + (kx >> 3)];
+            cpx lA = z, lB = mul_mi(z);
+            if (mirror) {
+                const cpx zm = conj(s * a[pr][rr * RS + km + (km >> 3)]);
+                lA = lA + zm; lB = lB + mul_i(zm);
+            }
+            outA[pr][o] = lA; outB[pr][o] = lB;
+        }
+    }
+}
+// columns: forward transforms along y of the six half-row adjoints, added to the spectrum adjoints of slice l
+template <int NY>
+__global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
+                                                                      const cpx* __restrict__ W2, const cpx* __restrict__ W3,
+                                                                      const cpx* __restrict__ W4, const cpx* __restrict__ W5,
+                                                                      cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lLx,
+                                                                      cpx* __restrict__ lLy, cpx* __restrict__ lEz, cpx* __restrict__ lBz) {
+    using S = FftShape<NY>;
+    extern __shared__ cpx sm[];
+    const int l = blockIdx.y, c0 = blockIdx.x * ACW, tid = threadIdx.x, nthr = ACW * S::T, pr = blockIdx.z;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    const cpx* in0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
+    const cpx* in1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
+    cpx* out0 = pr == 0 ? lRx : pr == 1 ? lLx : lEz;
+    cpx* out1 = pr == 0 ? lRy : pr == 1 ? lLy : lBz;
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * ACW;
+    for (int e = tid; e < NY * ACW; e += nthr) {
+        const int p = e / ACW, c = e - p * ACW, kxi = c0 + c;
+        const long o = base + long(p) * H + kxi;
+        s0[e] = kxi < H ? in0[o] : C(0);
+        s1[e] = kxi < H ? in1[o] : C(0);
+    }
+    __syncthreads();
+    const int c = tid % ACW, t = tid / ACW;
+    fft_line<NY>(s0, ColAddr<ACW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<ACW>{c}, t, g.twy);
+    for (int e = tid; e < NY * ACW; e += nthr) {
+        const int p = e / ACW, cc = e - p * ACW, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        out0[o] = out0[o] + s0[e];
+        out1[o] = out1[o] + s1[e];
+    }
+}
+
+// ---------------------------------------------------------------- transposed march
+// One thread per stored mode, slices n = a .. N-1 (the reverse of the forward's N-1 .. a). The adjoints of
+// the new level at slice n (given, plus what slice n-1 passed up through the values of slice n+1 it read)
+// become the adjoints of the old level (R, E_z, B_z; the old L is not read by the forward), of j0 and of jk.
+// lj0 is zeroed by the caller; ljk holds the adjoint of jk as a j0 of the next step and is added to.
+__global__ void __launch_bounds__(128) k_adj_march(Geo g, cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lEz,
+                                                  cpx* __restrict__ lBz, cpx* __restrict__ lLx, cpx* __restrict__ lLy,
+                                                  cpx* __restrict__ lj0x, cpx* __restrict__ lj0y, cpx* __restrict__ ljkx,
+                                                  cpx* __restrict__ ljky, cpx* __restrict__ ljkz, double D) {
+    const long nk = g.nkh;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nk) return;
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
+    cpx qRx = C(0), qRy = C(0), qEz = C(0), qBz = C(0), qLx = C(0), qLy = C(0);
+    for (int n = g.a; n <= g.b - 1; ++n) {
+        const long o = long(n - g.a) * nk + i, od = o, ou = o + nk;
+        const cpx aRx = lRx[o] + qRx, aRy = lRy[o] + qRy;
+        cpx aEz = lEz[o] + qEz, aBz = lBz[o] + qBz;
+        const cpx aLx = lLx[o] + qLx, aLy = lLy[o] + qLy;
+        const double wl = g.wlo[n], wu = g.whi[n];
+        cpx lRsx, lRsy;
+        if (n == g.N - 1) {
+            lRsx = aRx; lRsy = aRy;             // E_z, B_z, L of the front slice are zero: their adjoints end here
+            qRx = qRy = qEz = qBz = qLx = qLy = C(0);
+        } else {
+            const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+            // L = Ls - (h/4)(a E_z - b B_z), (h/4)(a B_z + b E_z); R = Rs + D (a E_z + b B_z), D (b E_z - a B_z)
+            cpx lLsx = aLx, lLsy = aLy;
+            lRsx = aRx; lRsy = aRy;
+            aEz = aEz - 0.25 * h * ikc(kx, aLx) - 0.25 * h * ikc(ky, aLy) + D * ikc(kx, aRx) + D * ikc(ky, aRy);
+            aBz = aBz + 0.25 * h * ikc(ky, aLx) - 0.25 * h * ikc(kx, aLy) + D * ikc(ky, aRx) - D * ikc(kx, aRy);
+            // E_z = (pEz - h/2 Qp - h/4 SE - h upz)/den; B_z = (pBz - h/2 Cp - h/4 SB)/den
+            const cpx tE = aEz / den, tB = aBz / den;
+            cpx lpEz = tE, lpBz = tB;
+            const cpx lQp = -0.5 * h * tE, lSE = -0.25 * h * tE, lupz = -h * tE;
+            const cpx lCp = -0.5 * h * tB, lSB = -0.25 * h * tB;
+            // SE = -a Rsx + a Lsx + b Lsy - b Rsy; SB = a Rsy + a Lsy - b Rsx - b Lsx
+            lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
+            lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
+            lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
+            lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
+            // Qp = -a (pRx - pLx)/2 + b (pLy - pRy)/2; Cp = (a (pRy + pLy) - b (pRx + pLx))/2
+            cpx lpRx = -0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+            cpx lpLx = 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+            cpx lpLy = 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+            cpx lpRy = -0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+            // Lsy = pLy - (h/4)(a pBz + b pEz) - (h/2) upy; Lsx = pLx - (h/4)(a pEz - b pBz) - (h/2) upx
+            lpLy = lpLy + lLsy;
+            lpBz = lpBz - 0.25 * h * ikc(kx, lLsy) + 0.25 * h * ikc(ky, lLsx);
+            lpEz = lpEz - 0.25 * h * ikc(ky, lLsy) - 0.25 * h * ikc(kx, lLsx);
+            lpLx = lpLx + lLsx;
+            ljkx[ou] = ljkx[ou] - 0.5 * h * lLsx;
+            ljky[ou] = ljky[ou] - 0.5 * h * lLsy;
+            ljkz[ou] = ljkz[ou] + lupz;
+            qRx = lpRx; qRy = lpRy; qEz = lpEz; qBz = lpBz; qLx = lpLx; qLy = lpLy;
+        }
+        // Rsx = Rx + D (a E_z + b B_z) - D Jx; Rsy = Ry + D (b E_z - a B_z) - D Jy (old level, slice n)
+        lRx[o] = lRsx; lRy[o] = lRsy;
+        lEz[o] = D * ikc(kx, lRsx) + D * ikc(ky, lRsy);
+        lBz[o] = D * ikc(ky, lRsx) - D * ikc(kx, lRsy);
+        lLx[o] = C(0); lLy[o] = C(0);
+        const cpx lJx = -D * lRsx, lJy = -D * lRsy;
+        lj0x[od] = lj0x[od] + wl * lJx; ljkx[od] = ljkx[od] + wl * lJx;
+        lj0x[ou] = lj0x[ou] + wu * lJx; ljkx[ou] = ljkx[ou] + wu * lJx;
+        lj0y[od] = lj0y[od] + wl * lJy; ljky[od] = ljky[od] + wl * lJy;
+        lj0y[ou] = lj0y[ou] + wu * lJy; ljky[ou] = ljky[ou] + wu * lJy;
+    }
+}
+
+// ---------------------------------------------------------------- transposed currents
+// columns: per half-cell plane, the filters f(k) (zero at k = 0) and the unnormalised inverse transform along y
+template <int NY>
+__global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, const cpx* __restrict__ JX, const cpx* __restrict__ JY,
+                                                                       const cpx* __restrict__ JZ, cpx* __restrict__ TX,
+                                                                       cpx* __restrict__ TY, cpx* __restrict__ TZ) {
+    using S = FftShape<NY>;
+    extern __shared__ cpx sm[];
+    cpx* s0 = sm;
+    cpx* s1 = sm + NY * ACW;
+    cpx* s2 = sm + 2 * NY * ACW;
+    const int hk = blockIdx.y, c0 = blockIdx.x * ACW, tid = threadIdx.x, nthr = ACW * S::T;
+    const int H = g.H;
+    const long base = long(hk) * g.nkh;
+    for (int e = tid; e < NY * ACW; e += nthr) {
+        const int p = e / ACW, c = e - p * ACW, kx = c0 + c;
+        cpx u0 = C(0), u1 = C(0), u2 = C(0);
+        if (kx < H) {
+            const double f = (kx == 0 && p == 0) ? 0.0 : g.filt[kx] * g.filty[p];
+            const long o = base + long(p) * H + kx;
+            u0 = conj(f * JX[o]); u1 = conj(f * JY[o]); u2 = conj(f * JZ[o]);
+        }
+        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+    }
+    __syncthreads();
+    const int c = tid % ACW, t = tid / ACW;
+    fft_line<NY>(s0, ColAddr<ACW>{c}, t, g.twy);
+    fft_line<NY>(s1, ColAddr<ACW>{c}, t, g.twy);
+    fft_line<NY>(s2, ColAddr<ACW>{c}, t, g.twy);
+    for (int e = tid; e < NY * ACW; e += nthr) {
+        const int p = e / ACW, cc = e - p * ACW, kx = c0 + cc;
+        if (kx >= H) continue;
+        const long o = base + long(p) * H + kx;
+        TX[o] = conj(s0[e]); TY[o] = conj(s1[e]); TZ[o] = conj(s2[e]);
+    }
+}
+// rows: the transposed Hermitian split (lz(k) = (lTX + i lTY)/2, lz(nx-k) = (conj lTX + i conj lTY)/2; at
+// k = 0, nx/2: Re lTX + i Re lTY) and the unnormalised inverse transform along x: Re -> lv_x, Im -> lv_y; j_z
+// from lTZ (zero above nx/2), real part -> lv_z. Out: V [3][ns+1][ny][nx].
+template <int NX>
+__global__ void __launch_bounds__(ANT) k_adj_cur_rows(Geo g, const cpx* __restrict__ TX, const cpx* __restrict__ TY,
+                                                     const cpx* __restrict__ TZ, double* __restrict__ V) {
+    using S = FftShape<NX>;
+    constexpr int LPC = ANT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
+    extern __shared__ cpx sm[];
+    cpx* a0 = sm;
+    cpx* a1 = sm + LPC * RS;
+    const int tid = threadIdx.x, r0 = blockIdx.x * LPC, hk = blockIdx.y;
+    const long base = long(hk) * g.nkh;
+    for (int e = tid; e < LPC * NX; e += ANT) {                 // zero the rows (the mirror halves are added)
+        const int rr = e / NX, p = e - rr * NX;
+        a0[rr * RS + p + (p >> 3)] = C(0); a1[rr * RS + p + (p >> 3)] = C(0);
+    }
+    __syncthreads();
+    for (int e = tid; e < LPC * H; e += ANT) {
+        const int rr = e / H, kx = e - rr * H, row = r0 + rr;
+        if (row >= g.ny) continue;
+        const long o = base + long(row) * H + kx;
+        const cpx lx = TX[o], ly = TY[o];
+        cpx zk;
+        if (kx == 0 || kx == NX / 2) zk = C(lx.x, ly.x);
+        else {
+            zk = 0.5 * (lx + mul_i(ly));
+            const int km = NX - kx;
+            a0[rr * RS + km + (km >> 3)] = conj(0.5 * (conj(lx) + mul_i(conj(ly))));
+        }
+        a0[rr * RS + kx + (kx >> 3)] = conj(zk);
+        a1[rr * RS + kx + (kx >> 3)] = conj(TZ[o]);
+    }
+    __syncthreads();
+    const int r = tid / S::T, t = tid - r * S::T;
+    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
+    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    const long nk = g.nk, vpl = long(g.ns + 1) * nk;
+    for (int e = tid; e < LPC * NX; e += ANT) {
+        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
+        if (row >= g.ny) continue;
+        const cpx u = conj(a0[rr * RS + p + (p >> 3)]), w = conj(a1[rr * RS + p + (p >> 3)]);
+        const long idx = long(hk) * nk + long(row) * NX + p;
+        V[idx] = u.x; V[vpl + idx] = u.y; V[2 * vpl + idx] = w.x;
+    }
+}
+// the transposed zeta filter: plane hk read the raw planes hk, hk+1, hk+2 with weights (cm, c0, cp)(hk)
+__device__ __forceinline__ void zf_weights(const Geo& g, int hk, int zf, double w[3]) {
+    const int hc = g.a - 1 + hk;
+    if (hk < 0 || hk > g.ns || hc < 0 || hc > g.N - 2) { w[0] = w[1] = w[2] = 0; return; }
+    if (!zf) { w[0] = 0; w[1] = 1; w[2] = 0; return; }
+    if (g.zeta_uniform) { w[0] = 0.25; w[1] = 0.5; w[2] = 0.25; return; }
+    const double inv = g.hcg[hc + 2];
+    w[0] = 0.25 * g.hcg[hc + 1] / inv; w[1] = 0.5 * g.hcg[hc + 2] / inv; w[2] = 0.25 * g.hcg[hc + 3] / inv;
+}
+__global__ void k_adj_zfilter(Geo g, const double* __restrict__ V, double* __restrict__ lJ, int zf) {
+    const long nk = g.nk, vpl = long(g.ns + 1) * nk, jpl = long(g.nh) * nk, n = 3 * jpl;
+    for (long idx = long(blockIdx.x) * blockDim.x + threadIdx.x; idx < n; idx += long(gridDim.x) * blockDim.x) {
+        const int comp = int(idx / jpl);
+        const long r = idx - comp * jpl;
+        const int h = int(r / nk);
+        const long k = r - long(h) * nk;
+        double s = 0;
+        for (int d = 0; d < 3; ++d) {
+            const int hk = h - d;
+            if (hk < 0 || hk > g.ns) continue;
+            double w[3];
+            zf_weights(g, hk, zf, w);
+            if (w[d] != 0) s += w[d] * V[comp * vpl + long(hk) * nk + k];
+        }
+        lJ[idx] = s;
+    }
+}
+
+// ---------------------------------------------------------------- transposed deposit
+// j = f W(x, y) (p_x/p_z, p_y/p_z, 1), f = q w / (h_m dx dy), NGP in zeta (no zeta derivative)
+__global__ void __launch_bounds__(256) k_adj_deposit(PartsDev P, const double* __restrict__ X, const int32_t* __restrict__ alive,
+                                                    long np, Geo g, const double* __restrict__ lJ, double* __restrict__ lam) {
+    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ip >= np || alive[ip] != 1) return;
+    const double x = X[ip], y = X[np + ip], zeta = X[2 * np + ip], px = X[3 * np + ip], py = X[4 * np + ip], pz = X[5 * np + ip];
+    int m; double fz;
+    g.zax.locate(zeta, m, fz);
+    const int hw = m - (g.a - 2);
+    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
+    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx) * g.iA[0];
+    int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    tsc_dweights(x / g.dx, dwx);
+    tsc_dweights(y / g.dy, dwn);
+    const long nk = g.nk, pl = long(g.nh) * nk;
+    const double* J0 = lJ + long(hw) * nk;
+    const double ux = px / pz, uy = py / pz;
+    double Gx = 0, Gy = 0, Dx = 0, Dy = 0;
+    for (int v = 0; v < 3; ++v)
+        for (int u = 0; u < 3; ++u) {
+            const long k = long(jn[v]) * g.nx + ix[u];
+            const double ax = J0[k], ay = J0[pl + k], az = J0[2 * pl + k];
+            const double W = wx[u] * wn[v];
+            Gx += W * ax; Gy += W * ay;
+            const double s = ax * ux + ay * uy + az;
+            Dx += dwx[u] * wn[v] * s; Dy += wx[u] * dwn[v] * s;
+        }
+    lam[ip] += f * Dx / g.dx;
+    lam[np + ip] += f * Dy / g.dy;
+    lam[3 * np + ip] += f * Gx / pz;
+    lam[4 * np + ip] += f * Gy / pz;
+    lam[5 * np + ip] += -f * (Gx * ux + Gy * uy) / pz;
+}
+
+// ---------------------------------------------------------------- transposed push
+// The gather with its adjoint: E, B at (x, y, zeta) as the forward computes them, and for the field adjoints
+// A[6]: their deposit into dJ/dF and sum_c A_c grad(field_c).
+template <class FT>
+__device__ __forceinline__ void gather_adj(const PushArgs& c, const FT* __restrict__ Fp, double x, double y, double zeta,
+                                           const double A[6], double E[3], double B[3], double& gx, double& gy, double& gz,
+                                           double* __restrict__ lF) {
+    E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
+    gx = gy = gz = 0;
+    if (!c.self) return;
+    const Geo& g = c.g;
+    int n; double fz;
+    g.zax.locate(zeta, n, fz);
+    if (n == g.a - 1 && fz > 1 - 1e-9) { n = g.a; fz = 0; }
+    const int fl = n - g.a;
+    if (fl < 0 || fl > g.ns) return;
+    const double dfz = locate_slope(g.zax, n);
+    int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    tsc_dweights(x / g.dx, dwx);
+    tsc_dweights(y / g.dy, dwn);
+    const double idx_ = 1 / g.dx, idy = 1 / g.dy;
+    const long nk = g.nk;
+    for (int comp = 0; comp < 6; ++comp) {
+        const long off = (long(comp) * (g.ns + 2) + fl) * nk;
+        const FT* p0 = Fp + off;
+        const FT* p1 = p0 + nk;
+        double v = 0, sx = 0, sy = 0, sz = 0;
+        const double a = A[comp];
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const long k = long(jn[j]) * g.nx + ix[i];
+                const double f0 = double(p0[k]), f1 = double(p1[k]);
+                const double val = (1 - fz) * f0 + fz * f1;
+                v += wx[i] * wn[j] * val;
+                sx += dwx[i] * wn[j] * val; sy += wx[i] * dwn[j] * val; sz += wx[i] * wn[j] * (f1 - f0);
+                if (a != 0) {
+                    const double w = a * wx[i] * wn[j];
+                    atomicAdd(lF + off + k, w * (1 - fz));
+                    atomicAdd(lF + off + nk + k, w * fz);
+                }
+            }
+        if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+        gx += a * sx * idx_; gy += a * sy * idy; gz += a * sz * dfz;
+    }
+}
+// lY += d(mu . rhs)/dY at Y
+template <class FT>
+__device__ __forceinline__ void rhs_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double qm, const St& mu, St& lY,
+                                        double* __restrict__ lF) {
+    const double px = Y.px, py = Y.py, pz = Y.pz;
+    const double g = sqrt(1 + px * px + py * py + pz * pz);
+    const double gpz = g + pz, gm = (1 + px * px + py * py) / gpz, ip = 1 / pz;
+    double A[6];
+    A[0] = mu.px * qm * g * ip; A[1] = mu.py * qm * g * ip; A[2] = mu.pz * qm * g * ip;
+    A[3] = qm * ip * (mu.py * pz - mu.pz * py);
+    A[4] = qm * ip * (mu.pz * px - mu.px * pz);
+    A[5] = qm * ip * (mu.px * py - mu.py * px);
+    double E[3], B[3], gx, gy, gz;
+    gather_adj(c, Fp, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, A, E, B, gx, gy, gz, lF);
+    const double Fx = qm * (g * E[0] + py * B[2] - pz * B[1]);
+    const double Fy = qm * (g * E[1] + pz * B[0] - px * B[2]);
+    const double Fz = qm * (g * E[2] + px * B[1] - py * B[0]);
+    const double G = mu.px * E[0] + mu.py * E[1] + mu.pz * E[2];
+    const double dgx = (2 * px - gm * px / g) / gpz, dgy = (2 * py - gm * py / g) / gpz, dgz = -gm * (pz / g + 1) / gpz;
+    lY.x += gx; lY.y += gy; lY.zeta += gz;
+    lY.px += mu.x * ip - mu.zeta * ip * dgx + qm * ip * (G * px / g - mu.py * B[2] + mu.pz * B[1]);
+    lY.py += mu.y * ip - mu.zeta * ip * dgy + qm * ip * (G * py / g + mu.px * B[2] - mu.pz * B[0]);
+    lY.pz += -(mu.x * px + mu.y * py) * ip * ip - mu.zeta * ip * dgz + mu.zeta * gm * ip * ip +
+             qm * ip * (G * pz / g - mu.px * B[1] + mu.py * B[0]) - ip * ip * (mu.px * Fx + mu.py * Fy + mu.pz * Fz);
+}
+__device__ __forceinline__ St scale(const St& a, double h) { return St{h * a.x, h * a.y, h * a.zeta, h * a.px, h * a.py, h * a.pz}; }
+__device__ __forceinline__ St add(const St& a, const St& b) {
+    return St{a.x + b.x, a.y + b.y, a.zeta + b.zeta, a.px + b.px, a.py + b.py, a.pz + b.pz};
+}
+// the adjoint of one RK4 sub-step at its start state Y: lam (of the end state) -> lam (of Y)
+template <class FT>
+__device__ __forceinline__ St rk4_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double z, double ds, double qm,
+                                      const St& lam, double* __restrict__ lF) {
+    St k;
+    rhs(c, Fp, Y, z, qm, k);
+    const St Y2 = axpy(Y, 0.5 * ds, k);
+    rhs(c, Fp, Y2, z + 0.5 * ds, qm, k);
+    const St Y3 = axpy(Y, 0.5 * ds, k);
+    rhs(c, Fp, Y3, z + 0.5 * ds, qm, k);
+    const St Y4 = axpy(Y, ds, k);
+    St lY = lam;
+    St m1 = scale(lam, ds / 6), m2 = scale(lam, ds / 3), m3 = scale(lam, ds / 3);
+    const St m4 = scale(lam, ds / 6);
+    St a{0, 0, 0, 0, 0, 0};
+    rhs_adj(c, Fp, Y4, qm, m4, a, lF);                 // k4 = f(Y + ds k3)
+    lY = add(lY, a); m3 = add(m3, scale(a, ds));
+    a = St{0, 0, 0, 0, 0, 0};
+    rhs_adj(c, Fp, Y3, qm, m3, a, lF);                 // k3 = f(Y + ds/2 k2)
+    lY = add(lY, a); m2 = add(m2, scale(a, 0.5 * ds));
+    a = St{0, 0, 0, 0, 0, 0};
+    rhs_adj(c, Fp, Y2, qm, m2, a, lF);                 // k2 = f(Y + ds/2 k1)
+    lY = add(lY, a); m1 = add(m1, scale(a, 0.5 * ds));
+    a = St{0, 0, 0, 0, 0, 0};
+    rhs_adj(c, Fp, Y, qm, m1, a, lF);                  // k1 = f(Y)
+    return add(lY, a);
+}
+constexpr int ADJ_MAXSUB = 64;
+// per particle: the level's checkpoint X (x, y, zeta, px, py, pz) and alive flags; lam in/out [6][np]
+template <class FT>
+__global__ void __launch_bounds__(128) k_adj_push(PushArgs c, const FT* __restrict__ Fp, PartsDev P, const double* __restrict__ X,
+                                                 const int32_t* __restrict__ alive, long np, double s0, double* __restrict__ lam,
+                                                 double* __restrict__ lF, int* __restrict__ err) {
+    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ip >= np) return;
+    const int al = alive[ip];
+    if (al != 1) {                           // not pushed: the state passes unchanged
+        if (al == 3) atomicOr(err, 1);
+        return;
+    }
+    if (c.freeze && P.sp[ip] <= 0) return;
+    St lm{lam[ip], lam[np + ip], lam[2 * np + ip], lam[3 * np + ip], lam[4 * np + ip], lam[5 * np + ip]};
+    if (lm.x == 0 && lm.y == 0 && lm.zeta == 0 && lm.px == 0 && lm.py == 0 && lm.pz == 0) return;
+    const St Y0{X[ip], X[np + ip], X[2 * np + ip], X[3 * np + ip], X[4 * np + ip], X[5 * np + ip]};
+    const double qm = P.qm[ip], s1 = c.s1;
+    double zs[ADJ_MAXSUB], dss[ADJ_MAXSUB];
+    int nsub = 0;
+    {
+        St Y = Y0;
+        double z = s0;
+        while (z < s1 - 1e-12 * fabs(s1)) {
+            const double ds = substep(c, Y, z, s1);
+            if (nsub == ADJ_MAXSUB) { atomicOr(err, 2); return; }
+            zs[nsub] = z; dss[nsub] = ds; ++nsub;
+            if (!rk4_step(c, Fp, Y, z, ds, qm)) return;      // lost in the forward: no adjoint
+            z += ds;
+        }
+    }
+    for (int t = nsub - 1; t >= 0; --t) {
+        St Y = Y0;
+        for (int u = 0; u < t; ++u) rk4_step(c, Fp, Y, zs[u], dss[u], qm);
+        lm = rk4_adj(c, Fp, Y, zs[t], dss[t], qm, lm, lF);
+    }
+    lam[ip] = lm.x; lam[np + ip] = lm.y; lam[2 * np + ip] = lm.zeta;
+    lam[3 * np + ip] = lm.px; lam[4 * np + ip] = lm.py; lam[5 * np + ip] = lm.pz;
+}
+
+// ---------------------------------------------------------------- laser mode coefficients
+// R += a(k) s(k, l) at init: dJ/da(k) = sum_l conj(s_x) dJ/dR_x + conj(s_y) dJ/dR_y
+__global__ void k_adj_lmodes(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy, const cpx* __restrict__ sx,
+                             const cpx* __restrict__ sy, cpx* __restrict__ out) {
+    const long nk = g.nkh;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nk) return;
+    cpx s = C(0);
+    for (int l = 0; l < g.ns; ++l) {
+        const long o = long(l) * nk + i;
+        s = s + conj(sx[o]) * lRx[o] + conj(sy[o]) * lRy[o];
+    }
+    out[i] = s;
+}
+
+// ---------------------------------------------------------------- launchers
+static unsigned ew_blocks(long n) {
+    long b = (n + 255) / 256;
+    return unsigned(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+template <class K>
+static void allow_smem(K kern, size_t smem) {
+    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+}
+
+void launch_adj_objective(Ctx& c, double* dev_out2) {
+    k_adj_objective<<<1, 1024, 0, c.stream>>>(c.parts, c.np, dev_out2);
+    c.check_launch("k_adj_objective");
+}
+void launch_adj_seed(Ctx& c, double W, double* lam) {
+    k_adj_seed<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.np, W, lam);
+    c.check_launch("k_adj_seed");
+}
+template <int NX>
+static void adj_rf_rows(Ctx& c, const double* lF, cpx* const* W) {
+    constexpr int LPC = ANT / FftShape<NX>::T;
+    const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
+    allow_smem(k_adj_rf_rows<NX>, smem);
+    k_adj_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), ANT, smem, c.stream>>>(c.geo(), lF, W[0], W[1], W[2],
+                                                                                                         W[3], W[4], W[5]);
+    c.check_launch("k_adj_rf_rows");
+}
+template <int NY>
+static void adj_rf_cols(Ctx& c, cpx* const* W, cpx* const* lS) {
+    const size_t smem = size_t(2) * NY * ACW * sizeof(cpx);
+    allow_smem(k_adj_rf_cols<NY>, smem);
+    k_adj_rf_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns), 3), ACW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), W[0], W[1], W[2], W[3], W[4], W[5], lS[0], lS[1], lS[4], lS[5], lS[2], lS[3]);
+    c.check_launch("k_adj_rf_cols");
+}
+// lS = {Rx, Ry, Ez, Bz, Lx, Ly}; W: 6 half-spectrum scratch arrays of ns planes
+void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const* lS) {
+    const int tok = c.prof_begin("adj_real_fields");
+    G3D_DISPATCH_N(c.nx, NX, adj_rf_rows<NX>(c, lF, W));
+    G3D_DISPATCH_N(c.ny, NY, adj_rf_cols<NY>(c, W, lS));
+    c.prof_end(tok);
+}
+void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D) {
+    const int tok = c.prof_begin("adj_march");
+    k_adj_march<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lS[0], lS[1], lS[2], lS[3], lS[4], lS[5], lj0[0], lj0[1],
+                                                                    ljk[0], ljk[1], ljk[2], D);
+    c.check_launch("k_adj_march");
+    c.prof_end(tok);
+}
+template <int NY>
+static void adj_cur_cols(Ctx& c, cpx* const* ljk, cpx* const* T) {
+    const size_t smem = size_t(3) * NY * ACW * sizeof(cpx);
+    allow_smem(k_adj_cur_cols<NY>, smem);
+    k_adj_cur_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns + 1)), ACW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), ljk[0], ljk[1], ljk[2], T[0], T[1], T[2]);
+    c.check_launch("k_adj_cur_cols");
+}
+template <int NX>
+static void adj_cur_rows(Ctx& c, cpx* const* T, double* V) {
+    constexpr int LPC = ANT / FftShape<NX>::T;
+    const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
+    allow_smem(k_adj_cur_rows<NX>, smem);
+    k_adj_cur_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1)), ANT, smem, c.stream>>>(c.geo(), T[0], T[1], T[2], V);
+    c.check_launch("k_adj_cur_rows");
+}
+// ljk (3 half-cell spectra) -> lJ (3 x (ns+3) raw planes); T: 3 scratch arrays of ns+1 planes, V: 3 (ns+1) real planes
+void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ) {
+    const int tok = c.prof_begin("adj_currents");
+    G3D_DISPATCH_N(c.ny, NY, adj_cur_cols<NY>(c, ljk, T));
+    G3D_DISPATCH_N(c.nx, NX, adj_cur_rows<NX>(c, T, V));
+    k_adj_zfilter<<<ew_blocks(3L * (c.ns + 3) * c.nk), 256, 0, c.stream>>>(c.geo(), V, lJ, c.P.zeta_filter ? 1 : 0);
+    c.check_launch("k_adj_zfilter");
+    c.prof_end(tok);
+}
+void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const double* lJ, double* lam) {
+    if (c.np == 0) return;
+    const int tok = c.prof_begin("adj_deposit");
+    k_adj_deposit<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, X, alive, c.np, c.geo(), lJ, lam);
+    c.check_launch("k_adj_deposit");
+    c.prof_end(tok);
+}
+// the push from s0 to s1 of the level checkpointed in (X, alive) with the level's fields Ff (float) or Fd
+void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
+                     double* lam, double* lF, int* err) {
+    if (c.np == 0) return;
+    const PushArgs a = push_args(c, s1);
+    const int tok = c.prof_begin("adj_push");
+    const unsigned blocks = unsigned((c.np + 127) / 128);
+    if (Fd) k_adj_push<double><<<blocks, 128, 0, c.stream>>>(a, Fd, c.parts, X, alive, c.np, s0, lam, lF, err);
+    else k_adj_push<float><<<blocks, 128, 0, c.stream>>>(a, Ff, c.parts, X, alive, c.np, s0, lam, lF, err);
+    c.check_launch("k_adj_push");
+    c.prof_end(tok);
+}
+void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out) {
+    k_adj_lmodes<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lRx, lRy, c.lspx.p, c.lspy.p, out);
+    c.check_launch("k_adj_lmodes");
+}
+
+}  // namespace g3d

@@ -249,7 +249,8 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
 template <int NX>
 __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                const cpx* __restrict__ W2, const cpx* __restrict__ W3,
-                                               const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F, int l0) {
+                                               const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F, int l0,
+                                               double* __restrict__ Fd) {
     using S = FftShape<NX>;
     constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -296,6 +297,11 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
         F[4 * fpl + idx] = float(0.5 * (r1 - l1));     // B_y
         F[2 * fpl + idx] = float(z3.x);                // E_z
         F[5 * fpl + idx] = float(z3.y);                // B_z
+        if (Fd) {                                      // exact fields: the same values before the rounding
+            Fd[0 * fpl + idx] = 0.5 * (r1 + l1); Fd[1 * fpl + idx] = 0.5 * (r2 + l2);
+            Fd[3 * fpl + idx] = 0.5 * (l2 - r2); Fd[4 * fpl + idx] = 0.5 * (r1 - l1);
+            Fd[2 * fpl + idx] = z3.x; Fd[5 * fpl + idx] = z3.y;
+        }
     }
 }
 
@@ -359,7 +365,7 @@ static void rf_rows(Ctx& c, int l0, int nl) {
     allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0);
+        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0, c.Fd.p);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
@@ -375,7 +381,7 @@ static void rf_rows_direct(Ctx& c, int l0, int nl) {
     allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0);
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0, c.Fd.p);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }

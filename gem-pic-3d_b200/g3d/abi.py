@@ -131,6 +131,9 @@ SIGNATURES = [
     ("g3d_profile_count", _I32, [_P]),
     ("g3d_profile_get", _I, [_P, _I32, C.POINTER(C.c_char_p), C.POINTER(_I64), C.POINTER(_D)]),
     ("g3d_launch_count", _I64, [_P]),
+    ("g3d_set_laser_modes", _I, [_P, _P]),
+    ("g3d_set_exact_fields", _I, [_P, _I32]),
+    ("g3d_adjoint", _I, [_P, _I32, C.POINTER(_D), _P, _P]),
 ]
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

@@ -268,6 +268,22 @@ def ionization_small(nx=16, ny=16, nzeta=64, steps=2, a0=2.5):
     return RunConfig("small ionization injection", nx, ny, nzeta, L, L, h, p, [], steps, plasma, ion_list, gl)
 
 
+def adjoint_small(nx=16, ny=16, nzeta=64, nmacro=2000, steps=3, gamma=10.0, a0=1.0, charge_pC=0.01):
+    """The structure of the adjoint workload at test size: a witness bunch inside a Gaussian grid laser in vacuum
+    (no sponge, fixed window), h = 0.25."""
+    lam = 0.8e-6
+    L = 24.0
+    h = 0.25 * (63 / (nzeta - 1))
+    window = h * (nzeta - 1)
+    zl = 0.5 * window
+    b = dict(charge_C=charge_pC * 1e-12, gamma=gamma, sigx=1.0, sigy=1.0, sigz=1.0, emitx=0.05, emity=0.05, espread=0.0,
+             zeta_center=zl, nmacro=nmacro, seed=4)
+    p = dict(lambda0=lam, dz=1.0, dz_push=1.0, z_end=1.0 * steps, sponge=0.0, sponge_y=0.0, zeta_center=zl,
+             move_x=0, move_y=0)
+    gl = [dict(a0=a0, kL=1.0, waist=6.0, tau=4.0, zeta_c=zl, z_focus=0.0)]
+    return RunConfig("adjoint: witness bunch in a grid laser", nx, ny, nzeta, L, L, h, p, [b], steps, None, [], gl)
+
+
 def baseline(k, **kw):
     if k == 1:
         return config1(**kw)

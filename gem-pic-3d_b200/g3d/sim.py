@@ -233,3 +233,28 @@ class Simulation:
 
     def launch_count(self):
         return self.lib.g3d_launch_count(self.ctx)
+
+    # ---------------------------------------------------------------- adjoint march
+    def set_laser_modes(self, coef=None):
+        """Laser mode coefficients a[j, kx] (complex, ny x (nx/2 + 1)) multiplying the grid lasers' spectra at
+        init; None: all ones. Before init."""
+        if coef is None:
+            self._c(self.lib.g3d_set_laser_modes(self.ctx, None))
+            return
+        a = np.ascontiguousarray(np.asarray(coef, dtype=np.complex128).reshape(self.ny, self.nx // 2 + 1))
+        self._c(self.lib.g3d_set_laser_modes(self.ctx, a.ctypes.data))
+
+    def set_exact_fields(self, on=True):
+        """Keep the real fields in FP64 as well and gather the beam push from them. Before init."""
+        self._c(self.lib.g3d_set_exact_fields(self.ctx, 1 if on else 0))
+
+    def adjoint(self, nsteps, modes=True, momenta=True):
+        """From the start field: nsteps s-steps and the reverse sweep. Returns (J, dJ/da [ny, nx/2+1] complex
+        or None, dJ/dp [np, 3] or None) with J = mean p_z of the live beam."""
+        J = C.c_double()
+        gm = np.zeros((self.ny, self.nx // 2 + 1), dtype=np.complex128) if modes else None
+        n = self.status().np
+        gp = np.zeros((n, 3)) if momenta else None
+        self._c(self.lib.g3d_adjoint(self.ctx, int(nsteps), C.byref(J), gm.ctypes.data if modes else None,
+                                     gp.ctypes.data if momenta else None))
+        return J.value, gm, gp
