@@ -146,6 +146,7 @@ struct Ctx {
                                                  // (the differentiable forward of the gradient check), or empty
     DevBuf<cpx> lmode;                           // laser mode coefficients per stored mode (ny x H), or empty
     DevBuf<cpx> lspx, lspy;                      // the grid-laser spectra added at init before the coefficients
+    DevBuf<unsigned char> adjws;                 // workspace of the adjoint march, kept between calls
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped

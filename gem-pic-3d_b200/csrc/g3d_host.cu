@@ -833,9 +833,8 @@ static void read_checkpoint(Ctx& c, const char* path) {
 
 // ---------------------------------------------------------------- adjoint march
 // Laser mode coefficients a(k) (per stored mode [j][k_x]) multiply every grid laser's spectrum added at init;
-// the unmultiplied spectra are kept for the gradient. Before g3d_init.
+// the unmultiplied spectra are kept for the gradient. They take effect at the next g3d_init.
 static void set_laser_modes(Ctx& c, const double* coef) {
-    if (c.fields_ready) throw Error(G3D_ERR_STATE, "the laser mode coefficients are set before g3d_init");
     std::vector<cpx> a(size_t(c.nkh), C(1.0));
     if (coef)
         for (size_t i = 0; i < a.size(); ++i) a[i] = C(coef[2 * i], coef[2 * i + 1]);
@@ -845,9 +844,8 @@ static void set_laser_modes(Ctx& c, const double* coef) {
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 // Exact fields: the real fields are also kept in FP64 and the beam push gathers from them (the differentiable
-// forward that central differences are taken of). Before g3d_init, FP64 form.
+// forward that central differences are taken of). FP64 form; they take effect at the next g3d_init.
 static void set_exact_fields(Ctx& c, bool on) {
-    if (c.fields_ready) throw Error(G3D_ERR_STATE, "exact fields are chosen before g3d_init");
     if (on && c.mixed) throw Error(G3D_ERR_ARG, "exact fields are an option of the FP64 form");
     if (on) c.Fd.alloc(c.F.n, c.stream);
     else c.Fd.release();
@@ -858,7 +856,8 @@ static void set_exact_fields(Ctx& c, bool on) {
 // (k_adjoint.cu): per step the transposed real fields, march, currents, deposit and push. Out: J, dJ/da per
 // stored laser mode [j][k_x] (complex, interleaved) and dJ/dp of every particle at s = 0 [np][3], the start
 // field held fixed (its laser part is differentiated through init's march(0)). The forward leaves the run at
-// s = K dz, as K calls of g3d_step.
+// s = K dz, as K calls of g3d_step; g3d_set_particles + g3d_init start the next evaluation on the same context,
+// which reuses the workspace.
 static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p) {
     if (K < 1) throw Error(G3D_ERR_ARG, "the adjoint march needs at least one s-step");
     if (!c.yf) throw Error(G3D_ERR_ARG, "the adjoint march needs the Fourier y grid");
@@ -873,82 +872,87 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     const size_t Fn = c.F.n, ns = size_t(c.ns), nkh = size_t(c.nkh), nk = size_t(c.nk);
     const bool ex = c.Fd.p != nullptr;
     cudaStream_t st = c.stream;
-    DevBuf<double> X, FD;
-    DevBuf<int32_t> AL;
-    DevBuf<float> FF;
-    X.alloc(size_t(K + 1) * 6 * size_t(np), st);
-    AL.alloc(size_t(K + 1) * size_t(np), st);
-    if (ex) FD.alloc(size_t(K + 1) * Fn, st);
-    else FF.alloc(size_t(K + 1) * Fn, st);
+    // one workspace, kept between calls: the checkpoints of the K + 1 levels (beam x, y, zeta, p; alive; the real
+    // fields), the adjoints of the spectra, currents, real fields and beam, and transform scratch
+    size_t need = 0;
+    auto carve = [&](size_t bytes) { const size_t o = need; need += (bytes + 255) / 256 * 256; return o; };
+    const size_t oX = carve(size_t(K + 1) * 6 * size_t(np) * 8), oAL = carve(size_t(K + 1) * size_t(np) * 4);
+    const size_t oF = carve(size_t(K + 1) * Fn * (ex ? 8 : 4));
+    size_t oS[6], oj0[2], ojk[3], oW[6];
+    for (auto& o : oS) o = carve(ns * nkh * sizeof(cpx));
+    for (auto& o : oj0) o = carve((ns + 1) * nkh * sizeof(cpx));
+    for (auto& o : ojk) o = carve((ns + 1) * nkh * sizeof(cpx));
+    for (auto& o : oW) o = carve((ns + 1) * nkh * sizeof(cpx));
+    const size_t olF = carve(Fn * 8), oV = carve(3 * (ns + 1) * nk * 8), olJ = carve(3 * (ns + 3) * nk * 8);
+    const size_t olam = carve(6 * size_t(np) * 8), oerr = carve(sizeof(int)), ojo = carve(2 * 8), ogm = carve(nkh * sizeof(cpx));
+    if (c.adjws.n < need) c.adjws.alloc(need, st);
+    unsigned char* ws = c.adjws.p;
+    double* X = reinterpret_cast<double*>(ws + oX);
+    int32_t* AL = reinterpret_cast<int32_t*>(ws + oAL);
+    float* FF = ex ? nullptr : reinterpret_cast<float*>(ws + oF);
+    double* FD = ex ? reinterpret_cast<double*>(ws + oF) : nullptr;
+    cpx* lS[6]; cpx* lj0[2]; cpx* ljk[3]; cpx* W[6];
+    for (int q = 0; q < 6; ++q) { lS[q] = reinterpret_cast<cpx*>(ws + oS[q]); W[q] = reinterpret_cast<cpx*>(ws + oW[q]); }
+    for (int q = 0; q < 2; ++q) lj0[q] = reinterpret_cast<cpx*>(ws + oj0[q]);
+    for (int q = 0; q < 3; ++q) ljk[q] = reinterpret_cast<cpx*>(ws + ojk[q]);
+    double* lF = reinterpret_cast<double*>(ws + olF);
+    double* V = reinterpret_cast<double*>(ws + oV);
+    double* lJ = reinterpret_cast<double*>(ws + olJ);
+    double* lam = reinterpret_cast<double*>(ws + olam);
+    int* err = reinterpret_cast<int*>(ws + oerr);
+    double* jo = reinterpret_cast<double*>(ws + ojo);
+    cpx* gmd = reinterpret_cast<cpx*>(ws + ogm);
     std::vector<double> sl(size_t(K + 1));
     auto save = [&](int k) {
-        double* x = X.p + size_t(k) * 6 * size_t(np);
+        double* x = X + size_t(k) * 6 * size_t(np);
         double* src[6] = {c.parts.x, c.parts.y, c.parts.zeta, c.parts.px, c.parts.py, c.parts.pz};
         if (np > 0) {
             for (int q = 0; q < 6; ++q)
                 G3D_CUDA(cudaMemcpyAsync(x + size_t(q) * np, src[q], size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
-            G3D_CUDA(cudaMemcpyAsync(AL.p + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
+            G3D_CUDA(cudaMemcpyAsync(AL + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
         }
-        if (ex) G3D_CUDA(cudaMemcpyAsync(FD.p + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
-        else G3D_CUDA(cudaMemcpyAsync(FF.p + size_t(k) * Fn, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
+        if (ex) G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+        else G3D_CUDA(cudaMemcpyAsync(FF + size_t(k) * Fn, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
         sl[size_t(k)] = c.s;
     };
     save(0);
     for (int k = 1; k <= K; ++k) { step(c, false); save(k); }
-    DevBuf<double> jo;
-    jo.alloc(2, st);
-    launch_adj_objective(c, jo.p);
+    launch_adj_objective(c, jo);
     double jh[2];
-    G3D_CUDA(cudaMemcpyAsync(jh, jo.p, 16, cudaMemcpyDeviceToHost, st));
+    G3D_CUDA(cudaMemcpyAsync(jh, jo, 16, cudaMemcpyDeviceToHost, st));
     G3D_CUDA(cudaStreamSynchronize(st));
     if (!(jh[1] > 0)) throw Error(G3D_ERR_STATE, "the adjoint march: no live particle at the end");
     *J = jh[0] / jh[1];
     // the reverse sweep
-    DevBuf<cpx> lSb[6], lj0b[2], ljkb[3], Wb[6];
-    for (auto& b : lSb) b.alloc(ns * nkh, st);
-    for (auto& b : lj0b) b.alloc((ns + 1) * nkh, st);
-    for (auto& b : ljkb) b.alloc((ns + 1) * nkh, st);
-    for (auto& b : Wb) b.alloc((ns + 1) * nkh, st);
-    DevBuf<double> lF, V, lJ, lam;
-    lF.alloc(Fn, st);
-    V.alloc(3 * (ns + 1) * nk, st);
-    lJ.alloc(3 * (ns + 3) * nk, st);
-    lam.alloc(6 * size_t(np), st);
-    DevBuf<int> err;
-    err.alloc(1, st);
-    cpx* lS[6]; cpx* lj0[2]; cpx* ljk[3]; cpx* W[6];
-    for (int q = 0; q < 6; ++q) { lS[q] = lSb[q].p; W[q] = Wb[q].p; }
-    if (np > 0) launch_adj_seed(c, jh[1], lam.p);
+    for (int q = 0; q < 6; ++q) G3D_CUDA(cudaMemsetAsync(lS[q], 0, ns * nkh * sizeof(cpx), st));
+    for (int q = 0; q < 3; ++q) G3D_CUDA(cudaMemsetAsync(ljk[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
+    G3D_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    if (np > 0) launch_adj_seed(c, jh[1], lam);
     for (int k = K; k >= 1; --k) {
-        if (k < K) launch_adj_real_fields(c, lF.p, W, lS);
-        for (int q = 0; q < 2; ++q) { lj0b[q].zero(st); lj0[q] = lj0b[q].p; }
-        for (int q = 0; q < 3; ++q) ljk[q] = ljkb[q].p;
+        if (k < K) launch_adj_real_fields(c, lF, W, lS);
+        for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemsetAsync(lj0[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
         launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);
-        launch_adj_currents(c, ljk, W, V.p, lJ.p);
-        launch_adj_deposit(c, X.p + size_t(k) * 6 * np, AL.p + size_t(k) * np, lJ.p, lam.p);
-        for (int q = 0; q < 2; ++q) std::swap(ljkb[q].p, lj0b[q].p);     // jk of level k-1 as the j0 of step k
-        ljkb[2].zero(st);
-        lF.zero(st);
-        launch_adj_push(c, ex ? nullptr : FF.p + size_t(k - 1) * Fn, ex ? FD.p + size_t(k - 1) * Fn : nullptr,
-                        X.p + size_t(k - 1) * 6 * np, AL.p + size_t(k - 1) * np, sl[size_t(k - 1)], sl[size_t(k)], lam.p, lF.p, err.p);
+        launch_adj_currents(c, ljk, W, V, lJ);
+        launch_adj_deposit(c, X + size_t(k) * 6 * np, AL + size_t(k) * np, lJ, lam);
+        for (int q = 0; q < 2; ++q) std::swap(ljk[q], lj0[q]);           // jk of level k-1 as the j0 of step k
+        G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
+        launch_adj_push(c, ex ? nullptr : FF + size_t(k - 1) * Fn, ex ? FD + size_t(k - 1) * Fn : nullptr, X + size_t(k - 1) * 6 * np,
+                        AL + size_t(k - 1) * np, sl[size_t(k - 1)], sl[size_t(k)], lam, lF, err);
     }
     // level 0: the real fields of the start field, then init's march(0) back to R with the lasers added
-    launch_adj_real_fields(c, lF.p, W, lS);
-    for (int q = 0; q < 2; ++q) { lj0b[q].zero(st); lj0[q] = lj0b[q].p; }
-    for (int q = 0; q < 3; ++q) ljk[q] = ljkb[q].p;
+    launch_adj_real_fields(c, lF, W, lS);
+    for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemsetAsync(lj0[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
     launch_adj_march(c, lS, lj0, ljk, 0.0);
     int eh = 0;
-    G3D_CUDA(cudaMemcpyAsync(&eh, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    G3D_CUDA(cudaMemcpyAsync(&eh, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (grad_modes) {
-        DevBuf<cpx> gm;
-        gm.alloc(nkh, st);
-        launch_adj_lmodes(c, lS[0], lS[1], gm.p);
-        G3D_CUDA(cudaMemcpyAsync(grad_modes, gm.p, nkh * sizeof(cpx), cudaMemcpyDeviceToHost, st));
+        launch_adj_lmodes(c, lS[0], lS[1], gmd);
+        G3D_CUDA(cudaMemcpyAsync(grad_modes, gmd, nkh * sizeof(cpx), cudaMemcpyDeviceToHost, st));
         G3D_CUDA(cudaStreamSynchronize(st));
     }
     if (grad_p && np > 0) {
         std::vector<double> h(3 * size_t(np));
-        G3D_CUDA(cudaMemcpyAsync(h.data(), lam.p + 3 * size_t(np), 3 * size_t(np) * 8, cudaMemcpyDeviceToHost, st));
+        G3D_CUDA(cudaMemcpyAsync(h.data(), lam + 3 * size_t(np), 3 * size_t(np) * 8, cudaMemcpyDeviceToHost, st));
         G3D_CUDA(cudaStreamSynchronize(st));
         for (long i = 0; i < np; ++i)
             for (int q = 0; q < 3; ++q) grad_p[3 * i + q] = h[size_t(q) * np + i];
@@ -983,7 +987,7 @@ int guarded(g3d_ctx* ctx, Fn&& fn) {
 
 extern "C" {
 
-const char* g3d_version(void) { return "libg3d 0.1 (sm_100a, FP64 march, Fourier y)"; }
+const char* g3d_version(void) { return "libg3d 0.2 (sm_100a; FP64 and mixed forms; Fourier and free-hand y; adjoint)"; }
 
 int g3d_create(const g3d_grid* grid, const g3d_params* params, g3d_ctx** out) {
     if (!grid || !params || !out) { g3d::g_create_err = "null argument"; return G3D_ERR_ARG; }

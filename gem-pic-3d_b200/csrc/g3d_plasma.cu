@@ -470,6 +470,7 @@ __global__ void k_glaser_add(Geo g, const cpx* __restrict__ PR, const cpx* __res
 void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3);   // k_plasma.cu
 
 void add_grid_lasers(Ctx& c) {
+    if (c.lspx.p) { c.lspx.zero(c.stream); c.lspy.zero(c.stream); }
     if (c.glasers.empty()) return;
     DevBuf<double> prof;
     prof.alloc(size_t(6) * c.nk, c.stream);          // Re P, Im P, a zero plane (free-hand y: twice)

@@ -22,7 +22,6 @@
 namespace g3d {
 
 namespace {
-__device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     // conj(i k) z
 constexpr int ANT = 128;          // threads of the row kernels
 constexpr int ACW = 8;            // columns per tile of the column kernels
 
@@ -118,6 +117,7 @@ __global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __rest
     }
 }
 // columns: forward transforms along y of the six half-row adjoints, added to the spectrum adjoints of slice l
+// (R, E_z, B_z; assigned for L, whose adjoint the transposed march leaves stale)
 template <int NY>
 __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                                       const cpx* __restrict__ W2, const cpx* __restrict__ W3,
@@ -149,78 +149,152 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, co
         const int p = e / ACW, cc = e - p * ACW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        out0[o] = out0[o] + s0[e];
-        out1[o] = out1[o] + s1[e];
+        if (pr == 1) { out0[o] = s0[e]; out1[o] = s1[e]; }           // L: not an input of the forward march
+        else { out0[o] = out0[o] + s0[e]; out1[o] = out1[o] + s1[e]; }
     }
 }
 
 // ---------------------------------------------------------------- transposed march
-// One thread per stored mode, slices n = a .. N-1 (the reverse of the forward's N-1 .. a). The adjoints of
-// the new level at slice n (given, plus what slice n-1 passed up through the values of slice n+1 it read)
-// become the adjoints of the old level (R, E_z, B_z; the old L is not read by the forward), of j0 and of jk.
-// lj0 is zeroed by the caller; ljk holds the adjoint of jk as a j0 of the next step and is added to.
-__global__ void __launch_bounds__(128) k_adj_march(Geo g, cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lEz,
-                                                  cpx* __restrict__ lBz, cpx* __restrict__ lLx, cpx* __restrict__ lLy,
-                                                  cpx* __restrict__ lj0x, cpx* __restrict__ lj0y, cpx* __restrict__ ljkx,
-                                                  cpx* __restrict__ ljky, cpx* __restrict__ ljkz, double D) {
+// The transposed per-mode march in the two-lane form of the forward (k_march.cu): with E~ = i E_z, B~ = i B_z
+// every coefficient is real, so lane c = 0 carries the adjoints of (Re R, Re L, -Im E_z, -Im B_z) and lane c = 1
+// those of (Im R, Im L, Re E_z, Re B_z); each lane is the transpose of the forward lane's real recurrence. Slices
+// n = a .. N-1 (the reverse of the forward's N-1 .. a): the adjoints of the new level at slice n (given, plus what
+// slice n-1 passed up through the values of slice n+1 it read) become those of the old level (R, E_z, B_z; the
+// old L is not read by the forward, so lLx, lLy are left to the next transposed real fields, which assign
+// them) and of the currents. The two half-cells of a slice are written once each: the upper one's terms ride
+// in registers to the next slice, where it is the lower one. lj0 and ljk_z are written; ljk_x, ljk_y hold on
+// entry the adjoint of jk as the j0 of the next step and are overwritten with the total. Per
+// slice each lane streams its 8 values (the 6 adjoints of the new level, the 2 pending ones) and the slice's
+// coefficients DEPTH slices ahead into a shared-memory ring with cp.async, as the forward does.
+namespace {
+constexpr int AMA = 8, AMC = 3;
+constexpr int aslot(int bt) { return (AMA + AMC) * bt; }
+__device__ __forceinline__ void acp8(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void acommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void await_() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+}  // namespace
+
+template <int BT, int DEPTH>
+__global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lEz,
+                                                 cpx* __restrict__ lBz, cpx* __restrict__ lLx, cpx* __restrict__ lLy,
+                                                 cpx* __restrict__ lj0x, cpx* __restrict__ lj0y, cpx* __restrict__ ljkx,
+                                                 cpx* __restrict__ ljky, cpx* __restrict__ ljkz, double D) {
+    extern __shared__ double ringa[];
     const long nk = g.nkh;
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nk) return;
-    const int kxi = int(i % g.H), j = int(i / g.H);
+    const int tid = threadIdx.x;
+    const long gt = long(blockIdx.x) * BT + tid;
+    const int c = int(gt & 1);
+    const long i = gt >> 1;
+    const bool live = i < nk;
+    const long ii = live ? i : 0;
+    const int kxi = int(ii % g.H), j = int(ii / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
-    cpx qRx = C(0), qRy = C(0), qEz = C(0), qBz = C(0), qLx = C(0), qLy = C(0);
+    const double sgn = c ? 1.0 : -1.0;
+    auto own = [&](long o) { return 2 * o + c; };
+    auto oth = [&](long o) { return 2 * o + 1 - c; };
+    double* Rx = reinterpret_cast<double*>(lRx);
+    double* Ry = reinterpret_cast<double*>(lRy);
+    double* Ez = reinterpret_cast<double*>(lEz);
+    double* Bz = reinterpret_cast<double*>(lBz);
+    double* Lx = reinterpret_cast<double*>(lLx);
+    double* Ly = reinterpret_cast<double*>(lLy);
+    double* j0x = reinterpret_cast<double*>(lj0x);
+    double* j0y = reinterpret_cast<double*>(lj0y);
+    double* jkx = reinterpret_cast<double*>(ljkx);
+    double* jky = reinterpret_cast<double*>(ljky);
+    double* jkz = reinterpret_cast<double*>(ljkz);
+    auto cell = [&](int sl, int k) { return ringa + size_t(sl) * aslot(BT) + k * BT + tid; };
+    // ring cells: 0 R_x, 1 R_y, 2 L_x, 3 L_y (own), 4 E_z, 5 B_z (other), 6 jk_x, 7 jk_y pending (own); w_lo, w_hi, h
+    auto fetch = [&](int n) {
+        const int sl = (n - g.a) % DEPTH;
+        const long o = long(n - g.a) * nk + ii;
+        acp8(cell(sl, 0), Rx + own(o)); acp8(cell(sl, 1), Ry + own(o));
+        acp8(cell(sl, 2), Lx + own(o)); acp8(cell(sl, 3), Ly + own(o));
+        acp8(cell(sl, 4), Ez + oth(o)); acp8(cell(sl, 5), Bz + oth(o));
+        acp8(cell(sl, 6), jkx + own(o)); acp8(cell(sl, 7), jky + own(o));
+        acp8(cell(sl, 8), g.wlo + n); acp8(cell(sl, 9), g.whi + n); acp8(cell(sl, 10), g.hcg + n + 2);
+    };
+#pragma unroll
+    for (int q = 0; q < DEPTH; ++q) {
+        const int n = g.a + q;
+        if (n <= g.b - 1) fetch(n);
+        acommit();
+    }
+    double qRx = 0, qRy = 0, qLx = 0, qLy = 0, qE = 0, qB = 0;          // adjoints of the p-values of slice n
+    double c0x = 0, c0y = 0, ckx = 0, cky = 0, ckz = 0;                 // lower half-cell terms from slice n-1
+    double rden = 0;
+    bool have_rden = false;
     for (int n = g.a; n <= g.b - 1; ++n) {
-        const long o = long(n - g.a) * nk + i, od = o, ou = o + nk;
-        const cpx aRx = lRx[o] + qRx, aRy = lRy[o] + qRy;
-        cpx aEz = lEz[o] + qEz, aBz = lBz[o] + qBz;
-        const cpx aLx = lLx[o] + qLx, aLy = lLy[o] + qLy;
-        const double wl = g.wlo[n], wu = g.whi[n];
-        cpx lRsx, lRsy;
-        if (n == g.N - 1) {
-            lRsx = aRx; lRsy = aRy;             // E_z, B_z, L of the front slice are zero: their adjoints end here
-            qRx = qRy = qEz = qBz = qLx = qLy = C(0);
-        } else {
-            const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
-            // L = Ls - (h/4)(a E_z - b B_z), (h/4)(a B_z + b E_z); R = Rs + D (a E_z + b B_z), D (b E_z - a B_z)
-            cpx lLsx = aLx, lLsy = aLy;
-            lRsx = aRx; lRsy = aRy;
-            aEz = aEz - 0.25 * h * ikc(kx, aLx) - 0.25 * h * ikc(ky, aLy) + D * ikc(kx, aRx) + D * ikc(ky, aRy);
-            aBz = aBz + 0.25 * h * ikc(ky, aLx) - 0.25 * h * ikc(kx, aLy) + D * ikc(ky, aRx) - D * ikc(kx, aRy);
-            // E_z = (pEz - h/2 Qp - h/4 SE - h upz)/den; B_z = (pBz - h/2 Cp - h/4 SB)/den
-            const cpx tE = aEz / den, tB = aBz / den;
-            cpx lpEz = tE, lpBz = tB;
-            const cpx lQp = -0.5 * h * tE, lSE = -0.25 * h * tE, lupz = -h * tE;
-            const cpx lCp = -0.5 * h * tB, lSB = -0.25 * h * tB;
-            // SE = -a Rsx + a Lsx + b Lsy - b Rsy; SB = a Rsy + a Lsy - b Rsx - b Lsx
-            lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
-            lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
-            lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
-            lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
-            // Qp = -a (pRx - pLx)/2 + b (pLy - pRy)/2; Cp = (a (pRy + pLy) - b (pRx + pLx))/2
-            cpx lpRx = -0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
-            cpx lpLx = 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
-            cpx lpLy = 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
-            cpx lpRy = -0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
-            // Lsy = pLy - (h/4)(a pBz + b pEz) - (h/2) upy; Lsx = pLx - (h/4)(a pEz - b pBz) - (h/2) upx
-            lpLy = lpLy + lLsy;
-            lpBz = lpBz - 0.25 * h * ikc(kx, lLsy) + 0.25 * h * ikc(ky, lLsx);
-            lpEz = lpEz - 0.25 * h * ikc(ky, lLsy) - 0.25 * h * ikc(kx, lLsx);
-            lpLx = lpLx + lLsx;
-            ljkx[ou] = ljkx[ou] - 0.5 * h * lLsx;
-            ljky[ou] = ljky[ou] - 0.5 * h * lLsy;
-            ljkz[ou] = ljkz[ou] + lupz;
-            qRx = lpRx; qRy = lpRy; qEz = lpEz; qBz = lpBz; qLx = lpLx; qLy = lpLy;
+        await_<DEPTH - 1>();
+        const int sl = (n - g.a) % DEPTH;
+        const long o = long(n - g.a) * nk + ii;
+        const double ARx = *cell(sl, 0) + qRx, ARy = *cell(sl, 1) + qRy;
+        const double ALx = *cell(sl, 2) + qLx, ALy = *cell(sl, 3) + qLy;
+        double AE = sgn * *cell(sl, 4) + qE, AB = sgn * *cell(sl, 5) + qB;
+        const double pkx = *cell(sl, 6), pky = *cell(sl, 7);
+        const double wl = *cell(sl, 8), wu = *cell(sl, 9), h = *cell(sl, 10);
+        if (!have_rden) rden = 1 / (1 + 0.25 * h * (D + 0.25 * h) * k2);
+        double rden_next = 0;                 // the next slice's inverse denominator, off the chain
+        if (n < g.b - 1) {
+            await_<DEPTH - 2>();
+            const double hn = *cell((sl + 1) % DEPTH, 10);
+            rden_next = 1 / (1 + 0.25 * hn * (D + 0.25 * hn) * k2);
         }
-        // Rsx = Rx + D (a E_z + b B_z) - D Jx; Rsy = Ry + D (b E_z - a B_z) - D Jy (old level, slice n)
-        lRx[o] = lRsx; lRy[o] = lRsy;
-        lEz[o] = D * ikc(kx, lRsx) + D * ikc(ky, lRsy);
-        lBz[o] = D * ikc(ky, lRsx) - D * ikc(kx, lRsy);
-        lLx[o] = C(0); lLy[o] = C(0);
-        const cpx lJx = -D * lRsx, lJy = -D * lRsy;
-        lj0x[od] = lj0x[od] + wl * lJx; ljkx[od] = ljkx[od] + wl * lJx;
-        lj0x[ou] = lj0x[ou] + wu * lJx; ljkx[ou] = ljkx[ou] + wu * lJx;
-        lj0y[od] = lj0y[od] + wl * lJy; ljky[od] = ljky[od] + wl * lJy;
-        lj0y[ou] = lj0y[ou] + wu * lJy; ljky[ou] = ljky[ou] + wu * lJy;
+        double lRsx = ARx, lRsy = ARy;
+        double ux = 0, uy = 0, uz = 0;                                   // adjoints of jk of the upper half-cell
+        if (n == g.N - 1) {
+            qRx = qRy = qLx = qLy = qE = qB = 0;
+        } else {
+            double lLsx = ALx, lLsy = ALy;
+            AB += -0.25 * h * kx * ALy + 0.25 * h * ky * ALx - D * kx * ARy + D * ky * ARx;
+            AE += -0.25 * h * ky * ALy - 0.25 * h * kx * ALx + D * ky * ARy + D * kx * ARx;
+            const double tE = AE * rden, tB = AB * rden;
+            const double liQp = -0.5 * h * tE, liSE = -0.25 * h * tE, lupz = -h * tE;
+            const double liCp = -0.5 * h * tB, liSB = -0.25 * h * tB;
+            // iSE = kx Rsx - kx Lsx - ky Lsy + ky Rsy; iSB = -kx Rsy - kx Lsy + ky Rsx + ky Lsx
+            lRsx += kx * liSE + ky * liSB;
+            lLsx += -kx * liSE + ky * liSB;
+            lLsy += -ky * liSE - kx * liSB;
+            lRsy += ky * liSE - kx * liSB;
+            // iQp = kx (pRx - pLx)/2 - ky (pLy - pRy)/2; iCp = (-kx (pRy + pLy) + ky (pRx + pLx))/2
+            double lpRx = 0.5 * kx * liQp + 0.5 * ky * liCp;
+            double lpLx = -0.5 * kx * liQp + 0.5 * ky * liCp;
+            double lpLy = -0.5 * ky * liQp - 0.5 * kx * liCp;
+            double lpRy = 0.5 * ky * liQp - 0.5 * kx * liCp;
+            double lpE = tE, lpB = tB;
+            // Lsy = pLy - (h/4)(kx pB + ky pE) - (h/2) upy; Lsx = pLx - (h/4)(kx pE - ky pB) - (h/2) upx
+            lpLy += lLsy; lpB += -0.25 * h * kx * lLsy; lpE += -0.25 * h * ky * lLsy;
+            lpLx += lLsx; lpE += -0.25 * h * kx * lLsx; lpB += 0.25 * h * ky * lLsx;
+            ux = -0.5 * h * lLsx; uy = -0.5 * h * lLsy; uz = lupz;
+            qRx = lpRx; qRy = lpRy; qLx = lpLx; qLy = lpLy; qE = lpE; qB = lpB;
+        }
+        // Rsx = rx + D (kx e + ky b) - D Jx; Rsy = ry + D (ky e - kx b) - D Jy
+        const double le = D * kx * lRsx + D * ky * lRsy, lb = D * ky * lRsx - D * kx * lRsy;
+        const double lJx = -D * lRsx, lJy = -D * lRsy;
+        if (live) {                           // (the adjoints of the old L stay: the old L is not read)
+            Rx[own(o)] = lRsx; Ry[own(o)] = lRsy; Ez[oth(o)] = sgn * le; Bz[oth(o)] = sgn * lb;
+            // the lower half-cell (plane n - a): this slice's w_lo terms and the previous slice's upper terms
+            j0x[own(o)] = c0x + wl * lJx; j0y[own(o)] = c0y + wl * lJy;
+            jkx[own(o)] = pkx + ckx + wl * lJx; jky[own(o)] = pky + cky + wl * lJy;
+            jkz[oth(o)] = sgn * ckz;
+        }
+        rden = rden_next;
+        have_rden = n < g.b - 1;
+        c0x = wu * lJx; c0y = wu * lJy; ckx = wu * lJx + ux; cky = wu * lJy + uy; ckz = uz;
+        const int nn = n + DEPTH;
+        if (nn <= g.b - 1) fetch(nn);
+        acommit();
+    }
+    await_<0>();
+    if (live) {                                                          // the upper half-cell of the front slice
+        const long ou = long(g.ns) * nk + ii;
+        j0x[own(ou)] = c0x; j0y[own(ou)] = c0y;
+        jkx[own(ou)] = jkx[own(ou)] + ckx; jky[own(ou)] = jky[own(ou)] + cky;
+        jkz[oth(ou)] = sgn * ckz;
     }
 }
 
@@ -372,14 +446,22 @@ __global__ void __launch_bounds__(256) k_adj_deposit(PartsDev P, const double* _
 }
 
 // ---------------------------------------------------------------- transposed push
-// The gather with its adjoint: E, B at (x, y, zeta) as the forward computes them, and for the field adjoints
-// A[6]: their deposit into dJ/dF and sum_c A_c grad(field_c).
+// The stencil of one gather: the field adjoints A[6] and where they go in dJ/dF (the TSC points, the two slice
+// planes and their weights). The four stages of an RK4 sub-step usually share the stencil (a sub-step moves a
+// particle by far less than a cell), so their deposits are summed per point before the atomics.
+struct Sten {
+    double A[6], wx[3], wn[3], fz;
+    int ix[3], jn[3], fl;                     // fl < 0: nothing to deposit
+};
+// The gather with its adjoint: E, B at (x, y, zeta) as the forward computes them, sum_c A_c grad(field_c), and
+// the stencil of the field adjoints A[6].
 template <class FT>
 __device__ __forceinline__ void gather_adj(const PushArgs& c, const FT* __restrict__ Fp, double x, double y, double zeta,
                                            const double A[6], double E[3], double B[3], double& gx, double& gy, double& gz,
-                                           double* __restrict__ lF) {
+                                           Sten& st) {
     E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
     gx = gy = gz = 0;
+    st.fl = -1;
     if (!c.self) return;
     const Geo& g = c.g;
     int n; double fz;
@@ -388,40 +470,72 @@ __device__ __forceinline__ void gather_adj(const PushArgs& c, const FT* __restri
     const int fl = n - g.a;
     if (fl < 0 || fl > g.ns) return;
     const double dfz = locate_slope(g.zax, n);
-    int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
-    tsc_periodic(x, g.dx, g.nx, ix, wx);
-    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    double dwx[3], dwn[3];
+    tsc_periodic(x, g.dx, g.nx, st.ix, st.wx);
+    tsc_periodic(y, g.dy, g.ny, st.jn, st.wn);
     tsc_dweights(x / g.dx, dwx);
     tsc_dweights(y / g.dy, dwn);
     const double idx_ = 1 / g.dx, idy = 1 / g.dy;
     const long nk = g.nk;
     for (int comp = 0; comp < 6; ++comp) {
-        const long off = (long(comp) * (g.ns + 2) + fl) * nk;
-        const FT* p0 = Fp + off;
+        const FT* p0 = Fp + (long(comp) * (g.ns + 2) + fl) * nk;
         const FT* p1 = p0 + nk;
         double v = 0, sx = 0, sy = 0, sz = 0;
-        const double a = A[comp];
         for (int j = 0; j < 3; ++j)
             for (int i = 0; i < 3; ++i) {
-                const long k = long(jn[j]) * g.nx + ix[i];
+                const long k = long(st.jn[j]) * g.nx + st.ix[i];
                 const double f0 = double(p0[k]), f1 = double(p1[k]);
                 const double val = (1 - fz) * f0 + fz * f1;
-                v += wx[i] * wn[j] * val;
-                sx += dwx[i] * wn[j] * val; sy += wx[i] * dwn[j] * val; sz += wx[i] * wn[j] * (f1 - f0);
-                if (a != 0) {
-                    const double w = a * wx[i] * wn[j];
-                    atomicAdd(lF + off + k, w * (1 - fz));
-                    atomicAdd(lF + off + nk + k, w * fz);
-                }
+                v += st.wx[i] * st.wn[j] * val;
+                sx += dwx[i] * st.wn[j] * val; sy += st.wx[i] * dwn[j] * val; sz += st.wx[i] * st.wn[j] * (f1 - f0);
             }
         if (comp < 3) E[comp] = v; else B[comp - 3] = v;
-        gx += a * sx * idx_; gy += a * sy * idy; gz += a * sz * dfz;
+        gx += A[comp] * sx * idx_; gy += A[comp] * sy * idy; gz += A[comp] * sz * dfz;
+        st.A[comp] = A[comp];
+    }
+    st.fz = fz; st.fl = fl;
+}
+// the field adjoints of the stencils st[0..ns) into dJ/dF: summed per point when every stencil has the same
+// points and planes, else one by one
+__device__ __forceinline__ void flush_stencils(const Geo& g, const Sten* st, int ns, double* __restrict__ lF) {
+    const long nk = g.nk;
+    bool same = true;
+    int first = -1;
+    for (int s = 0; s < ns; ++s) {
+        if (st[s].fl < 0) continue;
+        if (first < 0) { first = s; continue; }
+        same = same && st[s].fl == st[first].fl && st[s].ix[0] == st[first].ix[0] && st[s].jn[0] == st[first].jn[0];
+    }
+    if (first < 0) return;
+    for (int s = (same ? first : 0); s < (same ? first + 1 : ns); ++s) {
+        const Sten& b = st[s];
+        if (b.fl < 0) continue;
+        for (int comp = 0; comp < 6; ++comp) {
+            const long off = (long(comp) * (g.ns + 2) + b.fl) * nk;
+            for (int j = 0; j < 3; ++j)
+                for (int i = 0; i < 3; ++i) {
+                    double c0 = 0, c1 = 0;
+                    if (same) {
+                        for (int u = 0; u < ns; ++u) {
+                            if (st[u].fl < 0) continue;
+                            const double w = st[u].A[comp] * st[u].wx[i] * st[u].wn[j];
+                            c0 += w * (1 - st[u].fz); c1 += w * st[u].fz;
+                        }
+                    } else {
+                        const double w = b.A[comp] * b.wx[i] * b.wn[j];
+                        c0 = w * (1 - b.fz); c1 = w * b.fz;
+                    }
+                    const long k = long(b.jn[j]) * g.nx + b.ix[i];
+                    if (c0 != 0) atomicAdd(lF + off + k, c0);
+                    if (c1 != 0) atomicAdd(lF + off + nk + k, c1);
+                }
+        }
     }
 }
-// lY += d(mu . rhs)/dY at Y
+// lY += d(mu . rhs)/dY at Y; the field adjoints into the stencil st
 template <class FT>
 __device__ __forceinline__ void rhs_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double qm, const St& mu, St& lY,
-                                        double* __restrict__ lF) {
+                                        Sten& st) {
     const double px = Y.px, py = Y.py, pz = Y.pz;
     const double g = sqrt(1 + px * px + py * py + pz * pz);
     const double gpz = g + pz, gm = (1 + px * px + py * py) / gpz, ip = 1 / pz;
@@ -431,7 +545,7 @@ __device__ __forceinline__ void rhs_adj(const PushArgs& c, const FT* __restrict_
     A[4] = qm * ip * (mu.pz * px - mu.px * pz);
     A[5] = qm * ip * (mu.px * py - mu.py * px);
     double E[3], B[3], gx, gy, gz;
-    gather_adj(c, Fp, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, A, E, B, gx, gy, gz, lF);
+    gather_adj(c, Fp, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, A, E, B, gx, gy, gz, st);
     const double Fx = qm * (g * E[0] + py * B[2] - pz * B[1]);
     const double Fy = qm * (g * E[1] + pz * B[0] - px * B[2]);
     const double Fz = qm * (g * E[2] + px * B[1] - py * B[0]);
@@ -461,27 +575,30 @@ __device__ __forceinline__ St rk4_adj(const PushArgs& c, const FT* __restrict__ 
     St lY = lam;
     St m1 = scale(lam, ds / 6), m2 = scale(lam, ds / 3), m3 = scale(lam, ds / 3);
     const St m4 = scale(lam, ds / 6);
+    Sten st[4];
     St a{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y4, qm, m4, a, lF);                 // k4 = f(Y + ds k3)
+    rhs_adj(c, Fp, Y4, qm, m4, a, st[3]);             // k4 = f(Y + ds k3)
     lY = add(lY, a); m3 = add(m3, scale(a, ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y3, qm, m3, a, lF);                 // k3 = f(Y + ds/2 k2)
+    rhs_adj(c, Fp, Y3, qm, m3, a, st[2]);             // k3 = f(Y + ds/2 k2)
     lY = add(lY, a); m2 = add(m2, scale(a, 0.5 * ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y2, qm, m2, a, lF);                 // k2 = f(Y + ds/2 k1)
+    rhs_adj(c, Fp, Y2, qm, m2, a, st[1]);             // k2 = f(Y + ds/2 k1)
     lY = add(lY, a); m1 = add(m1, scale(a, 0.5 * ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y, qm, m1, a, lF);                  // k1 = f(Y)
+    rhs_adj(c, Fp, Y, qm, m1, a, st[0]);              // k1 = f(Y)
+    flush_stencils(c.g, st, 4, lF);
     return add(lY, a);
 }
 constexpr int ADJ_MAXSUB = 64;
 // per particle: the level's checkpoint X (x, y, zeta, px, py, pz) and alive flags; lam in/out [6][np]
 template <class FT>
-__global__ void __launch_bounds__(128) k_adj_push(PushArgs c, const FT* __restrict__ Fp, PartsDev P, const double* __restrict__ X,
-                                                 const int32_t* __restrict__ alive, long np, double s0, double* __restrict__ lam,
-                                                 double* __restrict__ lF, int* __restrict__ err) {
-    const long ip = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (ip >= np) return;
+__global__ void __launch_bounds__(128) k_adj_push(PushArgs c, const FT* __restrict__ Fp, PartsDev P, const int32_t* __restrict__ perm,
+                                                 const double* __restrict__ X, const int32_t* __restrict__ alive, long np, double s0,
+                                                 double* __restrict__ lam, double* __restrict__ lF, int* __restrict__ err) {
+    const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const long ip = perm[t];                 // cell order: the warp's deposits into dJ/dF meet in the same lines
     const int al = alive[ip];
     if (al != 1) {                           // not pushed: the state passes unchanged
         if (al == 3) atomicOr(err, 1);
@@ -494,13 +611,15 @@ __global__ void __launch_bounds__(128) k_adj_push(PushArgs c, const FT* __restri
     const double qm = P.qm[ip], s1 = c.s1;
     double zs[ADJ_MAXSUB], dss[ADJ_MAXSUB];
     int nsub = 0;
-    {
+    {                                         // the sub-step schedule of the forward (the last one is not taken)
         St Y = Y0;
         double z = s0;
-        while (z < s1 - 1e-12 * fabs(s1)) {
+        const double zend = s1 - 1e-12 * fabs(s1);
+        while (z < zend) {
             const double ds = substep(c, Y, z, s1);
             if (nsub == ADJ_MAXSUB) { atomicOr(err, 2); return; }
             zs[nsub] = z; dss[nsub] = ds; ++nsub;
+            if (!(z + ds < zend)) break;
             if (!rk4_step(c, Fp, Y, z, ds, qm)) return;      // lost in the forward: no adjoint
             z += ds;
         }
@@ -571,10 +690,19 @@ void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const*
     G3D_DISPATCH_N(c.ny, NY, adj_rf_cols<NY>(c, W, lS));
     c.prof_end(tok);
 }
+template <int BT, int DEPTH>
+static void adj_march_launch(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D) {
+    const unsigned blocks = unsigned((2 * c.nkh + BT - 1) / BT);
+    const size_t smem = size_t(DEPTH) * aslot(BT) * sizeof(double);
+    allow_smem(k_adj_march<BT, DEPTH>, smem);
+    k_adj_march<BT, DEPTH><<<blocks, BT, smem, c.stream>>>(c.geo(), lS[0], lS[1], lS[2], lS[3], lS[4], lS[5], lj0[0], lj0[1], ljk[0],
+                                                           ljk[1], ljk[2], D);
+}
+// lS = {Rx, Ry, Ez, Bz, Lx, Ly}; ljk holds the pending adjoints of jk (x, y; z is added to)
 void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D) {
     const int tok = c.prof_begin("adj_march");
-    k_adj_march<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lS[0], lS[1], lS[2], lS[3], lS[4], lS[5], lj0[0], lj0[1],
-                                                                    ljk[0], ljk[1], ljk[2], D);
+    if (2 * c.nkh < 2L * 148 * 64) adj_march_launch<32, 6>(c, lS, lj0, ljk, D);
+    else adj_march_launch<64, 6>(c, lS, lj0, ljk, D);
     c.check_launch("k_adj_march");
     c.prof_end(tok);
 }
@@ -617,8 +745,8 @@ void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X,
     const PushArgs a = push_args(c, s1);
     const int tok = c.prof_begin("adj_push");
     const unsigned blocks = unsigned((c.np + 127) / 128);
-    if (Fd) k_adj_push<double><<<blocks, 128, 0, c.stream>>>(a, Fd, c.parts, X, alive, c.np, s0, lam, lF, err);
-    else k_adj_push<float><<<blocks, 128, 0, c.stream>>>(a, Ff, c.parts, X, alive, c.np, s0, lam, lF, err);
+    if (Fd) k_adj_push<double><<<blocks, 128, 0, c.stream>>>(a, Fd, c.parts, c.perm.p, X, alive, c.np, s0, lam, lF, err);
+    else k_adj_push<float><<<blocks, 128, 0, c.stream>>>(a, Ff, c.parts, c.perm.p, X, alive, c.np, s0, lam, lF, err);
     c.check_launch("k_adj_push");
     c.prof_end(tok);
 }

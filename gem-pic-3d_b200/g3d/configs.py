@@ -284,6 +284,24 @@ def adjoint_small(nx=16, ny=16, nzeta=64, nmacro=2000, steps=3, gamma=10.0, a0=1
     return RunConfig("adjoint: witness bunch in a grid laser", nx, ny, nzeta, L, L, h, p, [b], steps, None, [], gl)
 
 
+def config4(nx=64, ny=64, nzeta=512, nmacro=65536, steps=40, gamma=100.0, a0=1.0, charge_pC=1.0):
+    """Workload 4 without its plasma: a Gaussian grid laser (a0 1, waist 10, tau 10) and a bunch of 65,536
+    electrons (gamma 100, sigma_perp 1, sigma_zeta 1) inside the pulse, 64 x 64 modes over 40 x 40, 512 slices
+    with h = 0.25, 40 s-steps of dz = 2: the frozen-bunch/laser march the adjoint differentiates."""
+    lam = 0.8e-6
+    L = 40.0
+    h = 0.25 * (511 / (nzeta - 1))
+    window = h * (nzeta - 1)
+    zl = 0.5 * window
+    b = dict(charge_C=charge_pC * 1e-12, gamma=gamma, sigx=1.0, sigy=1.0, sigz=1.0, emitx=0.1, emity=0.1, espread=0.0,
+             zeta_center=zl, nmacro=nmacro, seed=4)
+    p = dict(lambda0=lam, dz=2.0, dz_push=2.0, z_end=2.0 * steps, sponge=0.0, sponge_y=0.0, zeta_center=zl,
+             move_x=0, move_y=0)
+    gl = [dict(a0=a0, kL=1.0, waist=10.0, tau=10.0, zeta_c=zl, z_focus=0.0)]
+    return RunConfig("frozen-bunch/laser march (workload 4 without plasma)", nx, ny, nzeta, L, L, h, p, [b], steps, None,
+                     [], gl)
+
+
 def baseline(k, **kw):
     if k == 1:
         return config1(**kw)

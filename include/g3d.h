@@ -63,8 +63,7 @@ typedef struct g3d_particle {
 /* Grid (reference Config grid fields, src/sim.hpp:38-44). */
 typedef struct g3d_grid {
     int32_t nx, ny, nzeta;
-    int32_t y_fourier;          /* 1: Fourier y (periodic); 0: free-hand y between walls (the FP64 form without
-                                   streaming plasma or grid lasers in this release) */
+    int32_t y_fourier;          /* 1: Fourier y (periodic); 0: free-hand y between walls (table ynode) */
     double Lx, Ly;
     const double* zeta;         /* nzeta slice positions, zeta[0] = 0 (rear) ... zeta[nzeta-1] = window */
     const double* ynode;        /* ny+1 node positions of the free-hand y grid, NULL for Fourier y */
@@ -262,17 +261,19 @@ int64_t g3d_launch_count(const struct g3d_ctx* ctx);
 /* ------------------------------------------------------------------ adjoint march (no reference counterpart) */
 /* Laser mode coefficients: every grid laser's R spectrum added at init (Simulation::add_grid_lasers,
  * src/sim_fields.cpp:321-373) is multiplied per stored mode by a(j, kx) = coef[2 (j H + kx)] + i coef[2 (j H + kx) + 1]
- * (ky index j = 0..ny-1, kx = 0..nx/2, H = nx/2 + 1); NULL sets every a to 1. Before g3d_init. */
+ * (ky index j = 0..ny-1, kx = 0..nx/2, H = nx/2 + 1); NULL sets every a to 1. Takes effect at the next g3d_init. */
 int g3d_set_laser_modes(struct g3d_ctx* ctx, const double* coef);
 /* Exact fields (1) or not (0): the real fields are kept in FP64 beside the float F and the beam push gathers
- * from them; the differentiable forward of which central differences are taken. FP64 form, before g3d_init. */
+ * from them; the differentiable forward of which central differences are taken. FP64 form; takes effect at the
+ * next g3d_init. */
 int g3d_set_exact_fields(struct g3d_ctx* ctx, int32_t on);
 /* The adjoint march, right after g3d_init (Fourier y, beam and grid lasers, no plasma, sponge 0, fixed window):
  * nsteps s-steps forward with per-level checkpoints of the beam and the real fields, J = sum w p_z / sum w over
  * the live beam, then the reverse sweep. Out: *objective = J; grad_modes (NULL: skipped; needs
  * g3d_set_laser_modes) = dJ/d Re a + i dJ/d Im a per stored mode, 2 ny H doubles; grad_p (NULL: skipped) =
  * dJ/d(p_x, p_y, p_z) of every particle at s = 0, 3 np doubles [particle][component], the start field held
- * fixed. The run is left at s = nsteps dz. */
+ * fixed. The run is left at s = nsteps dz; g3d_set_particles + g3d_init start the next evaluation on the same
+ * context (the checkpoint workspace is kept between calls). */
 int g3d_adjoint(struct g3d_ctx* ctx, int32_t nsteps, double* objective, double* grad_modes, double* grad_p);
 
 #ifdef __cplusplus

@@ -15,10 +15,17 @@ EPS = 1e-6
 TOL = 1e-6
 
 
-def objective(s):
-    p = s.host_particles()
+def objective(p):
     a = p["alive"] == 1
     return float(np.sum(p["w"][a] * p["pz"][a]) / np.sum(p["w"][a]))
+
+
+def central(pp, pm, eps):
+    """(J(+) - J(-)) / (2 eps) from the two final beams: the weighted sum of the per-particle differences, so that
+    the rounding of the sum of p_z ~ gamma does not enter the difference."""
+    assert np.array_equal(pp["alive"], pm["alive"])
+    a = pp["alive"] == 1
+    return float(np.sum(pp["w"][a] * (pp["pz"][a] - pm["pz"][a])) / np.sum(pp["w"][a]) / (2 * eps))
 
 
 def forward(cfg, coef=None, dp=None, exact=True, precision="fp64"):
@@ -35,9 +42,9 @@ def forward(cfg, coef=None, dp=None, exact=True, precision="fp64"):
         s.set_particles(p)
     for _ in range(cfg.steps):
         s.step()
-    J = objective(s)
+    p = s.host_particles()
     s.close()
-    return J
+    return p
 
 
 def adjoint(cfg, exact=True, precision="fp64"):
@@ -49,7 +56,7 @@ def adjoint(cfg, exact=True, precision="fp64"):
         s.set_exact_fields(True)
     s.init_fields()
     J, gm, gp = s.adjoint(cfg.steps)
-    Jh = objective(s)
+    Jh = objective(s.host_particles())
     s.close()
     return J, gm, gp, Jh
 
@@ -63,7 +70,7 @@ def test_adjoint_objective_is_the_forward_objective():
     cfg = case()
     J, gm, gp, Jh = adjoint(cfg)
     assert abs(J - Jh) <= 1e-13 * abs(J)
-    assert abs(J - forward(cfg)) <= 1e-13 * abs(J)
+    assert abs(J - objective(forward(cfg))) <= 1e-13 * abs(J)
     assert np.all(np.isfinite(gm)) and np.all(np.isfinite(gp))
 
 
@@ -74,7 +81,7 @@ def test_laser_mode_gradient_against_central_differences():
     H = cfg.nx // 2 + 1
     d = rng.standard_normal((cfg.ny, H)) + 1j * rng.standard_normal((cfg.ny, H))
     ad = float(np.real(np.sum(np.conj(gm) * d)))
-    fd = (forward(cfg, coef=1 + EPS * d) - forward(cfg, coef=1 - EPS * d)) / (2 * EPS)
+    fd = central(forward(cfg, coef=1 + EPS * d), forward(cfg, coef=1 - EPS * d), EPS)
     print(f"J = {J:.12e}, laser modes: adjoint {ad:.12e}, central difference {fd:.12e}")
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
     # the largest single component, real and imaginary parts
@@ -82,7 +89,7 @@ def test_laser_mode_gradient_against_central_differences():
     for unit in (1.0, 1j):
         e = np.zeros((cfg.ny, H), dtype=complex)
         e[j, k] = unit
-        fd1 = (forward(cfg, coef=1 + EPS * e) - forward(cfg, coef=1 - EPS * e)) / (2 * EPS)
+        fd1 = central(forward(cfg, coef=1 + EPS * e), forward(cfg, coef=1 - EPS * e), EPS)
         ad1 = float(np.real(np.conj(gm[j, k]) * unit))
         assert abs(ad1 - fd1) <= TOL * max(abs(fd1), 1e-3 * np.max(np.abs(gm))), (unit, ad1, fd1)
 
@@ -93,6 +100,6 @@ def test_momentum_gradient_against_central_differences():
     rng = np.random.default_rng(12)
     D = rng.standard_normal(gp.shape)
     ad = float(np.sum(gp * D))
-    fd = (forward(cfg, dp=EPS * D) - forward(cfg, dp=-EPS * D)) / (2 * EPS)
+    fd = central(forward(cfg, dp=EPS * D), forward(cfg, dp=-EPS * D), EPS)
     print(f"momenta: adjoint {ad:.12e}, central difference {fd:.12e}")
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
