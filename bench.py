@@ -13,7 +13,9 @@ Workload 2: the oblique plane wave on a dense bunch (128 x 128 x 1024, 1,048,576
     python bench.py [--gpus N --steps K --warmup W] [--impl g3d|reference] [--workload 2|3]
 
 Both forms are timed on the same inputs; value is the mixed form, fp64_form the FP64 form, mixed_error the
-relative L2 of F and the relative <p_z> of the mixed form against the FP64 form after the same steps.
+relative L2 of F and the relative <p_z> of the mixed form against the FP64 form after the same steps. At N = 1
+the key adjoint holds the adjoint march's cost against the forward and its agreement with central differences on
+workload 4 without its plasma (--no-adjoint skips it).
 Under torchrun (N > 1) every rank runs an independent replica (the march is one serial chain in zeta;
 replicas only), timed on the device, max over ranks; value = pushes of all ranks / that time.
 --impl reference times the reference GEM-PIC-3D CPU/OpenMP build (oracle/_ref) on the host cores.
@@ -43,6 +45,7 @@ def parse():
     ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint march check on workload 4")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time the FP64 form, then the mixed form (the headline) and its error against FP64")
     ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
@@ -486,6 +489,8 @@ def run_g3d(a):
                 "cpu_baseline": cpu}
         if "streaming" in H:
             line["streaming"] = H["streaming"]
+        if world == 1 and not a.no_adjoint:
+            line["adjoint"] = adjoint_check()
         if "fp64" in res and mixed:
             F64 = res["fp64"]
             line["fp64_form"] = {"value": F64["value"], "ms_per_step": F64["ms"] / a.steps, "dtype": "f64",
@@ -496,6 +501,84 @@ def run_g3d(a):
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def adjoint_check(eps=1e-6):
+    """The adjoint march on workload 4 without its plasma (64 x 64 x 512, 65,536 electrons, 40 s-steps): the cost
+    of one evaluation of J = mean p_z with its gradient against one forward run of the same steps (device time on
+    the context stream, the third of three repetitions on one context), and the adjoint's directional
+    derivatives (seeded random directions over the laser mode coefficients and the beam momenta) against
+    central differences of the FP64 forward with exact fields, for the FP64 and the mixed adjoint."""
+    import numpy as np
+    import torch
+    from g3d import Simulation, configs
+    cfg = configs.config4()
+    K = cfg.steps
+    H = cfg.nx // 2 + 1
+
+    def timed(sim, fn):
+        st = torch.cuda.ExternalStream(sim.stream_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sim.synchronize()
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def final(coef=None, dp=None):
+        sim = Simulation(cfg)
+        sim.load_bunch()
+        sim.set_laser_modes(coef)
+        sim.set_exact_fields(True)
+        sim.init_fields()
+        if dp is not None:
+            p = sim.host_particles()
+            p["px"] += dp[:, 0]; p["py"] += dp[:, 1]; p["pz"] += dp[:, 2]
+            sim.set_particles(p)
+        for _ in range(K):
+            sim.step_async()
+        p = sim.host_particles()
+        sim.close()
+        return p
+
+    def central(pp, pm):
+        a = pp["alive"] == 1
+        return float(np.sum(pp["w"][a] * (pp["pz"][a] - pm["pz"][a])) / np.sum(pp["w"][a]) / (2 * eps))
+
+    out = {"workload": f"4 without plasma: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, {cfg.particles} "
+                       f"macro-electrons, {K} s-steps", "objective": "mean p_z of the live beam"}
+    grads = {}
+    for form in ["fp64", "mixed"]:
+        sim = Simulation(cfg, precision=form)
+        sim.load_bunch()
+        p0 = sim.host_particles()
+        sim.set_laser_modes(None)
+        if form == "fp64":
+            sim.set_exact_fields(True)
+        tf = ta = None
+        for _ in range(3):
+            sim.set_particles(p0); sim.init_fields()
+            tf, _ = timed(sim, lambda: [sim.step_async() for _ in range(K)])
+        for _ in range(3):
+            sim.set_particles(p0); sim.init_fields()
+            ta, g = timed(sim, lambda: sim.adjoint(K))
+        grads[form] = g
+        sim.close()
+        out[form] = {"forward_ms": tf, "adjoint_ms": ta, "adjoint_over_forward": ta / tf,
+                     "note": "adjoint_ms: the forward with per-level checkpoints, J, and the reverse sweep"}
+    rng = np.random.default_rng(11)
+    d = rng.standard_normal((cfg.ny, H)) + 1j * rng.standard_normal((cfg.ny, H))
+    D = np.random.default_rng(12).standard_normal(grads["fp64"][2].shape)
+    fl = central(final(coef=1 + eps * d), final(coef=1 - eps * d))
+    fm = central(final(dp=eps * D), final(dp=-eps * D))
+    for form in ["fp64", "mixed"]:
+        J, gm, gp = grads[form]
+        al, am = float(np.real(np.sum(np.conj(gm) * d))), float(np.sum(gp * D))
+        out[form].update({"J": J, "laser_modes_rel_err": abs(al - fl) / abs(fl), "momenta_rel_err": abs(am - fm) / abs(fm)})
+    out["central_differences"] = {"eps": eps, "laser_modes": fl, "momenta": fm,
+                                  "forward": "FP64 form with exact (FP64) real fields"}
+    return out
 
 
 def main():

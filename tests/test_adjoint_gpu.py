@@ -103,3 +103,25 @@ def test_momentum_gradient_against_central_differences():
     fd = central(forward(cfg, dp=EPS * D), forward(cfg, dp=-EPS * D), EPS)
     print(f"momenta: adjoint {ad:.12e}, central difference {fd:.12e}")
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
+def test_workload4_gradients_against_central_differences():
+    """At the size of workload 4 without its plasma (64 x 64 modes x 512 slices, 65,536 electrons, gamma 100,
+    40 s-steps): the FP64 adjoint (exact fields) and the mixed adjoint (the mixed forward with the float F, the
+    reverse sweep in FP64) against central differences of the FP64 forward."""
+    from g3d import configs
+    cfg = configs.config4()
+    H = cfg.nx // 2 + 1
+    d = np.random.default_rng(11).standard_normal((cfg.ny, H)) + 1j * np.random.default_rng(13).standard_normal((cfg.ny, H))
+    fl = central(forward(cfg, coef=1 + EPS * d), forward(cfg, coef=1 - EPS * d), EPS)
+    res = {}
+    for form, kw in [("fp64", dict(exact=True)), ("mixed", dict(exact=False, precision="mixed"))]:
+        J, gm, gp, _ = adjoint(cfg, **kw)
+        if form == "fp64":
+            D = np.random.default_rng(12).standard_normal(gp.shape)
+            fm = central(forward(cfg, dp=EPS * D), forward(cfg, dp=-EPS * D), EPS)
+        al, am = float(np.real(np.sum(np.conj(gm) * d))), float(np.sum(gp * D))
+        res[form] = (abs(al - fl) / abs(fl), abs(am - fm) / abs(fm))
+    print("workload 4 without plasma, relative differences (laser modes, momenta):", res)
+    for form, (el, em) in res.items():
+        assert el <= TOL and em <= TOL, (form, el, em)
