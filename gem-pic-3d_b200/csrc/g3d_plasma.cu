@@ -104,6 +104,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     for (DevBuf<cpx>* b : {&pl->js0x, &pl->js0y, &pl->js0z}) b->alloc(size_t(c.ns + 1) * ph, s);
     pl->jsr.alloc(size_t(5) * c.nk, s);
     pl->jsrf.alloc(size_t(5) * c.nk, s);
+    if (c.yf) pl->fmid.alloc(size_t(6) * c.nk, s);      // 6 doubles or 8 floats per point
     pl->stepv.alloc(1, s);
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
     pl->bk.alloc(4 * ph, s);
@@ -314,6 +315,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p;
         sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
+        sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
             launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
@@ -326,8 +328,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
                 sa.dry = pass + 1 < passes ? 1 : 0;
                 launch_stream(c, sa);
                 launch_stream_spectra(c);
-                launch_replace_pred(c, n, extrap ? 1 : 0, wex);
-                launch_march_slice(c, D, n);
+                if (c.yf) launch_replace_march(c, D, n, extrap ? 1 : 0, wex);
+                else { launch_replace_pred(c, n, extrap ? 1 : 0, wex); launch_march_slice(c, D, n); }
                 real_fields_slice(c, n);
             }
             if (ionz) launch_born_append(c);

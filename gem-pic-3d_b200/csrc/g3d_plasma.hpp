@@ -45,6 +45,8 @@ struct StreamArgs {
     int* bcnt;
     int bcap;
     int dry;                   // a predictor pass: deposit and ionize, keep the particles as they were
+    const void* Fmid;          // Fourier y: the six fields half-way between slices n and n+1, interleaved per point
+                               // (FP32: 8 floats, FP64: 6 doubles per point), or null
 };
 
 struct PlasmaPtrs {
@@ -80,6 +82,7 @@ struct PlasmaState {
     DevBuf<cpx> js0x, js0y, js0z;              // ns+1 half planes
     DevBuf<double> jsr;                        // 5 real planes
     DevBuf<float> jsrf;                        // the same in FP32 (the mixed form)
+    DevBuf<double> fmid;                       // the fields half-way through the half-cell, interleaved per point
     DevBuf<cpx> jsn, jsin, jpred, jtmp, jsi0, dlt, tsp;   // 3 half planes each
     DevBuf<cpx> bk;                            // 4 half planes: R_x, R_y, E_z, B_z of the slice
     StrmBuf s, bn;                             // streaming particles, the freed electrons
@@ -108,6 +111,7 @@ struct PlasmaState {
 void launch_stream(Ctx& c, const StreamArgs& a);
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
 void launch_pass_prologue(Ctx& c, int n, int restore);
+void launch_replace_march(Ctx& c, double D, int n, int extrap, double w);
 void launch_stream_spectra(Ctx& c);
 void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw);
 void launch_replace_pred(Ctx& c, int n, int extrap, double w);

@@ -96,6 +96,35 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
         if (comp < 3) E[comp] = v; else B[comp - 3] = v;
     }
 }
+// The gather half-way through the half-cell (zeta = the slice midpoint, a particle crossing the whole half-cell):
+// TSC in x and y of the interleaved midpoint fields, one vector load per point (Fourier y).
+template <bool F32>
+__device__ __forceinline__ void sgather_mid(const StreamArgs& c, double x, double y, double E[3], double B[3]) {
+    const Geo& g = c.g;
+    int ix[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    typedef typename std::conditional<F32, float, double>::type R;
+    R a[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const long k = long(jn[j]) * g.nx + ix[i];
+            const R w = R(wx[i] * wn[j]);
+            if constexpr (F32) {
+                const float4* p = reinterpret_cast<const float4*>(c.Fmid) + 2 * k;
+                const float4 u = __ldg(p), v = __ldg(p + 1);
+                a[0] += w * u.x; a[1] += w * u.y; a[2] += w * u.z; a[3] += w * u.w; a[4] += w * v.x; a[5] += w * v.y;
+            } else {
+                const double2* p = reinterpret_cast<const double2*>(c.Fmid) + 3 * k;
+                const double2 u = __ldg(p), v = __ldg(p + 1), q = __ldg(p + 2);
+                a[0] += w * u.x; a[1] += w * u.y; a[2] += w * v.x; a[3] += w * v.y; a[4] += w * q.x; a[5] += w * q.y;
+            }
+        }
+    E[0] = double(a[0]); E[1] = double(a[1]); E[2] = double(a[2]);
+    B[0] = double(a[3]); B[1] = double(a[4]); B[2] = double(a[5]);
+}
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
@@ -246,7 +275,8 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double xm = x + hd * px, ym = y + hd * py;
     const double zm = z + hd * pz, zetam = zeta - 0.5 * hl;
     double E[3], B[3], Ee[3], Be[3];
-    sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
+    if (c.Fmid && zeta == zn1) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), E, B);   // the whole half-cell
+    else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
     c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
     for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
     double ux = px, uy = py, uz = pz;
@@ -398,27 +428,30 @@ __global__ void k_replace(T* __restrict__ jx, T* __restrict__ jy, T* __restrict_
 // after a pass: replace the streaming part of jk(n) by jsn (old = sin); with the extrapolating predictor and
 // n >= 1 the prediction of half-cell n-1: tmp = js0(n-1) + d + w (d - dl), d = jsn - js0(n); replace(n-1, pin, tmp)
 template <class T>
-__global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
+__device__ __forceinline__ void replace_pred_mode(const PlasmaPtrs& p, int n, int extrap, double w, long i) {
     const long nkh = p.nkh;
     const long hp = long(n + 1) * nkh, hq = long(n) * nkh;        // planes of half-cells n and n-1 (a = 0)
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
-        cpx u[3];
-        for (int k = 0; k < 3; ++k) u[k] = p.jsn[k * nkh + i];
-        T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
+    cpx u[3];
+    for (int k = 0; k < 3; ++k) u[k] = p.jsn[k * nkh + i];
+    T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
+    for (int k = 0; k < 3; ++k) {
+        jk[k][hp + i] = narrow<T>(widen(jk[k][hp + i]) + u[k] - p.sin_[k * nkh + i]);
+        p.sin_[k * nkh + i] = u[k];
+    }
+    if (extrap && n >= 1) {
+        const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
         for (int k = 0; k < 3; ++k) {
-            jk[k][hp + i] = narrow<T>(widen(jk[k][hp + i]) + u[k] - p.sin_[k * nkh + i]);
-            p.sin_[k * nkh + i] = u[k];
-        }
-        if (extrap && n >= 1) {
-            const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
-            for (int k = 0; k < 3; ++k) {
-                const cpx d = u[k] - s0[k][hp + i];
-                const cpx t = s0[k][hq + i] + d + w * (d - p.dl[k * nkh + i]);
-                jk[k][hq + i] = narrow<T>(widen(jk[k][hq + i]) + t - p.pin[k * nkh + i]);
-                p.pin[k * nkh + i] = t;
-            }
+            const cpx d = u[k] - s0[k][hp + i];
+            const cpx t = s0[k][hq + i] + d + w * (d - p.dl[k * nkh + i]);
+            jk[k][hq + i] = narrow<T>(widen(jk[k][hq + i]) + t - p.pin[k * nkh + i]);
+            p.pin[k * nkh + i] = t;
         }
     }
+}
+template <class T>
+__global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x)
+        replace_pred_mode<T>(p, n, extrap, w, i);
 }
 // half-cell n is final (sim_plasma.cpp:381-403): R at slice n+1 corrected for the prediction it used; the
 // change s0 -> s1 kept for the extrapolation; the current kept as the prediction of the next step
@@ -436,16 +469,12 @@ __global__ void k_correct(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ 
         s0[0][hp + i] = u0; s0[1][hp + i] = u1; s0[2][hp + i] = u2;
     }
 }
-// the march of slice n, all modes (march_point, sim_kernels.hpp:173-210, one rank: b = N, no boundary slice)
+// the march of slice n, one mode (march_point, sim_kernels.hpp:173-210, one rank: b = N, no boundary slice). The
+// current pointers carry no __restrict__: the fused kernel below writes jk just before.
 template <class T>
-__global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
-                                                    T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
-                                                    const T* __restrict__ j0x, const T* __restrict__ j0y,
-                                                    const T* __restrict__ jkx, const T* __restrict__ jky,
-                                                    const T* __restrict__ jkz, double D, int n) {
+__device__ __forceinline__ void march_slice_mode(const Geo& g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x,
+                                                 const T* j0y, const T* jkx, const T* jky, const T* jkz, double D, int n, long i) {
     const long nk = g.nkh;
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nk) return;
     const int kxi = int(i % g.H), j = int(i / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
     const long o = long(n - g.a) * nk + i, od = o, ou = o + nk;
@@ -476,6 +505,23 @@ __global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* __restrict__ Rx
     Rx[o] = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)); Ry[o] = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
     Lx[o] = narrow<T>(Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)));
     Ly[o] = narrow<T>(Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn)));
+}
+template <class T>
+__global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x, const T* j0y,
+                                                    const T* jkx, const T* jky, const T* jkz, double D, int n) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < g.nkh) march_slice_mode<T>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D, n, i);
+}
+// a pass's current of half-cell n in place and the prediction of n-1 (replace_pred), then the march of slice n,
+// per mode in one thread (Fourier y)
+template <class T>
+__global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly,
+                                                      const T* j0x, const T* j0y, double D, int n, int extrap, double w) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= g.nkh) return;
+    replace_pred_mode<T>(p, n, extrap, w, i);
+    march_slice_mode<T>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, static_cast<const T*>(p.jkx), static_cast<const T*>(p.jky),
+                        static_cast<const T*>(p.jkz), D, n, i);
 }
 // freed electrons join the march (appended after the streaming particles; the count stays on the device)
 __global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
@@ -524,12 +570,36 @@ __global__ void k_slice_prologue(PlasmaPtrs p, cpx* __restrict__ sin_, cpx* __re
         }
     }
 }
+// The six fields half-way between slices n and n+1 (F planes l, l+1) at point k, interleaved: FP32 (the mixed
+// form: 8 floats, the last two unused) or FP64 (6 doubles).
+struct FmidArgs {
+    const float* F;
+    long fpl, l0, nk;
+    void* out;                 // null: not used (free-hand y)
+    int f32;
+};
+__device__ __forceinline__ void fmid_point(const FmidArgs& a, long k) {
+    double v[6];
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) {
+        const float* p = a.F + comp * a.fpl + a.l0 + k;
+        v[comp] = 0.5 * (double(p[0]) + double(p[a.nk]));
+    }
+    if (a.f32) {
+        float4* o = reinterpret_cast<float4*>(a.out) + 2 * k;
+        o[0] = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+        o[1] = make_float4(float(v[4]), float(v[5]), 0.f, 0.f);
+    } else {
+        double2* o = reinterpret_cast<double2*>(a.out) + 3 * k;
+        o[0] = make_double2(v[0], v[1]); o[1] = make_double2(v[2], v[3]); o[2] = make_double2(v[4], v[5]);
+    }
+}
 // Start of a pass: the slice restored from the backup (restore), the streaming-current planes and the count of
-// freed electrons cleared.
+// freed electrons cleared, the midpoint fields of the half-cell for the streaming gather.
 template <class T, class JT>
 __global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
                                 T* __restrict__ Bz, long o, long nkh, JT* __restrict__ J, long nj, int* __restrict__ bcnt,
-                                int restore) {
+                                int restore, FmidArgs fm) {
     const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x, st = long(gridDim.x) * blockDim.x;
     if (restore)
         for (long i = t0; i < nkh; i += st) {
@@ -537,6 +607,8 @@ __global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx
             Ez[o + i] = narrow<T>(bk[2 * nkh + i]); Bz[o + i] = narrow<T>(bk[3 * nkh + i]);
         }
     for (long i = t0; i < nj; i += st) J[i] = JT(0);
+    if (fm.out)
+        for (long k = t0; k < fm.nk; k += st) fmid_point(fm, k);
     if (t0 == 0) *bcnt = 0;
 }
 
@@ -632,16 +704,18 @@ void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup) {
 void launch_pass_prologue(Ctx& c, int n, int restore) {
     PlasmaState& P = *c.pl;
     const long o = long(n - c.a) * c.nkh, nj = 5 * long(c.nk);
+    FmidArgs fm{c.F.p, long(c.ns + 2) * c.nk, long(n - c.a) * c.nk, c.nk, c.yf ? static_cast<void*>(P.fmid.p) : nullptr,
+                c.f32s ? 1 : 0};
     const int tok = c.prof_begin("pass_prologue");
     if (c.mixed)
         k_pass_prologue<cpxf, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.mx.Ez.p, c.mx.Bz.p, o, c.nkh,
-                                                                          P.jsrf.p, nj, P.bcnt.p, restore);
+                                                                          P.jsrf.p, nj, P.bcnt.p, restore, fm);
     else if (c.f32s)                  // free-hand y, mixed: FP64 spectra, FP32 streaming planes
         k_pass_prologue<cpx, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
-                                                                         P.jsrf.p, nj, P.bcnt.p, restore);
+                                                                         P.jsrf.p, nj, P.bcnt.p, restore, fm);
     else
         k_pass_prologue<cpx, double><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
-                                                                          P.jsr.p, nj, P.bcnt.p, restore);
+                                                                          P.jsr.p, nj, P.bcnt.p, restore, fm);
     c.check_launch("k_pass_prologue");
     c.prof_end(tok);
 }
@@ -677,6 +751,21 @@ void launch_march_slice(Ctx& c, double D, int n) {
                                                          c.jkx.p, c.jky.p, c.jkz.p, D, n);
     }
     c.check_launch("k_march_slice");
+    c.prof_end(tok);
+}
+void launch_replace_march(Ctx& c, double D, int n, int extrap, double w) {
+    const int tok = c.prof_begin("replace_march");
+    const unsigned blocks = unsigned((c.nkh + 127) / 128);
+    const PlasmaPtrs pp = c.pl->ptrs(c);
+    if (c.mixed) {
+        MixedBufs& m = c.mx;
+        k_replace_march<cpxf><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
+                                                            D, n, extrap, w);
+    } else {
+        k_replace_march<cpx><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
+                                                           D, n, extrap, w);
+    }
+    c.check_launch("k_replace_march");
     c.prof_end(tok);
 }
 void launch_born_append(Ctx& c) {
