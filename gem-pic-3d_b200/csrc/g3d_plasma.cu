@@ -120,6 +120,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     for (const auto& sp : pl->ions) {
         IonDevC d{};
         d.mass = sp.mass; d.mobile = sp.mobile; d.ionizing = sp.ionization; d.Zmax = sp.Zmax; d.off = int(lev.size()); d.Emin = 1e300;
+        if (sp.ionization) pl->any_ionizing = true;
         if (sp.ionization) {
             const std::vector<AdkDev> L = adk_levels(sp.ip_eV, sp.Z0, sp.Zmax, E0, omega0, 2 * Lwin);
             for (int k = sp.Z0; k < sp.Zmax; ++k) d.Emin = std::min(d.Emin, L[size_t(k)].Emin);

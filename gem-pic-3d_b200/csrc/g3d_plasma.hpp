@@ -77,6 +77,7 @@ struct PlasmaState {
     std::vector<double> zpts, zvals;
     std::vector<IonSpec> ions;
     bool box_mean = true;
+    bool any_ionizing = false;                 // some ion species ionizes (the streaming kernel's ADK path)
     // spectra of the streaming current: level s0 per half-cell (the prediction of the next step), the current
     // of one half-cell (jsr real, jsn spectra), the parts of jk held as predictions, backups
     DevBuf<cpx> js0x, js0y, js0z;              // ns+1 half planes

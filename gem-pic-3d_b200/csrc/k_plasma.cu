@@ -243,7 +243,9 @@ struct DepReq {
 // the caller, the rare second deposit of a trapped particle that joins the beam list is made here. A predictor
 // pass (c.dry) computes and deposits the same but leaves the particle as it was, so every pass of a half-cell
 // starts from the same state without a copy of the particles.
-template <bool F32>
+// ION: some species ionizes (else the field magnitudes and the ADK sampling are left out); LASER: the analytic
+// plane wave is on. Both are fixed for a run; the variants without them hold fewer registers.
+template <bool F32, bool ION, bool LASER>
 __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
     DepReq d{0, 0, 0, 0, 0, 0, false};
     const Geo& g = c.g;
@@ -262,9 +264,11 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     if (ion && !c.ions[sp - SP_ION].mobile) {        // fixed ion: its charge, then the ionization
         const double f = S.q[i] * S.w[i] * hl / (c.Delta * h * g.dx);
         if (f != 0) d = DepReq{S.x[i], S.y[i], f, 0, 0, 0, true};
-        const double E1 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zn);
         if (!c.dry) S.zeta[i] = zn;
-        ionize(c, S, i, E1, E0, hl);
+        if constexpr (ION) {
+            const double E1 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zn);
+            ionize(c, S, i, E1, E0, hl);
+        }
         return d;
     }
     const double x = S.x[i], y = S.y[i], z = S.z[i], px = S.px[i], py = S.py[i], pz = S.pz[i], qm = S.qm[i];
@@ -277,8 +281,10 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     double E[3], B[3], Ee[3], Be[3];
     if (c.Fmid && zeta == zn1) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), E, B);   // the whole half-cell
     else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
-    c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
-    for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+    if constexpr (LASER) {
+        c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
+        for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+    }
     double ux = px, uy = py, uz = pz;
     boris(ux, uy, uz, E, B, qm, dt0);
     double g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
@@ -317,8 +323,9 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         if (!c.dry) S.alive[i] = 0;
         return d;
     }
-    if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
-        ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), dt);
+    if constexpr (ION)
+        if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
+            ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), dt);
     if (trapped) {
         if (!c.dry) S.alive[i] = 5;
         const double vze = uz * ig1;
@@ -334,13 +341,26 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
 // neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers in FP32 arithmetic
 // and the deposit into FP32 planes; the particle state and the Boris pushes stay FP64.
 constexpr int ST_NT = 128;
-template <bool F32>
-__global__ void __launch_bounds__(ST_NT, 4) k_stream(StreamArgs c, StrmDev S, const long* __restrict__ nstrm) {
+#ifndef G3D_STREAM_MINB
+#define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
+#endif
+template <bool F32, bool ION, bool LASER>
+__global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c, StrmDev S,
+                                                                                       const long* __restrict__ nstrm) {
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
-        const DepReq d = stream_one<F32>(c, S, i);
+        const DepReq d = stream_one<F32, ION, LASER>(c, S, i);
         if (d.on) sdeposit<F32>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
     }
+}
+template <bool F32>
+static void stream_launch(Ctx& c, const StreamArgs& a, unsigned blocks) {
+    PlasmaState& P = *c.pl;
+    const bool ion = P.any_ionizing, las = c.laser.on != 0;
+    if (ion && las) k_stream<F32, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    else if (ion) k_stream<F32, true, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    else if (las) k_stream<F32, false, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    else k_stream<F32, false, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
 }
 
 // ---------------------------------------------------------------- spectra of the streaming current
@@ -633,8 +653,8 @@ void launch_stream(Ctx& c, const StreamArgs& a) {
     const int tok = c.prof_begin("stream");
     const long want = (P.s.cap + ST_NT - 1) / ST_NT;
     const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
-    if (c.f32s) k_stream<true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
-    else k_stream<false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    if (c.f32s) stream_launch<true>(c, a, blocks);
+    else stream_launch<false>(c, a, blocks);
     c.check_launch("k_stream");
     c.prof_end(tok);
 }
