@@ -252,6 +252,9 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions);
 void march_plasma(Ctx& c, double s0, double s1);
 void collect_restreaming(Ctx& c);
 void add_grid_lasers(Ctx& c);
+// The dynamic shared memory a kernel may use, raised to smem once per kernel and device (a host call per
+// launch would leave the GPU waiting on the host between the small per-slice kernels)
+void smem_attr(const void* kern, size_t smem);
 // the adjoint march (k_adjoint.cu)
 void launch_adj_objective(Ctx& c, double* dev_out2);
 void launch_adj_seed(Ctx& c, double W, double* lam);

@@ -1,6 +1,8 @@
 // Host side of libg3d: the context (grids, tables, buffers), the orchestration of a step, the bunch
 // loader, checkpoints and the extern "C" entry points of include/g3d.h.
 #include <algorithm>
+#include <mutex>
+#include <map>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -67,6 +69,18 @@ static void set_precision(Ctx& c, int mode) {
     if (c.fields_ready) throw Error(G3D_ERR_STATE, "the precision is set before g3d_init");
     if (!c.yf) { c.f32s = mixed; return; }       // free-hand y: FP32 streaming plasma, FP64 spectra
     alloc_spectra(c, mixed);
+}
+
+void smem_attr(const void* kern, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> have;
+    int dev = 0;
+    G3D_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& v = have[{kern, dev}];
+    if (v >= smem) return;
+    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    v = smem;
 }
 
 Geo Ctx::geo() const {

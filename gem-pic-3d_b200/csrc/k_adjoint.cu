@@ -91,9 +91,10 @@ __global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __rest
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
+    {
+        decltype(a0) const ls_[3] = {a0, a1, a2};
+        fft_lines<NX, 3>(ls_, RowAddr{r * RS}, t, g.twx);
+    }
     const double s = 1.0 / double(g.nk);
     const long base = long(l) * g.nkh;
     for (int e = tid; e < LPC * H; e += ANT) {
@@ -134,23 +135,25 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, co
     cpx* out0 = pr == 0 ? lRx : pr == 1 ? lLx : lEz;
     cpx* out1 = pr == 0 ? lRy : pr == 1 ? lLy : lBz;
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * ACW;
+    cpx* s1 = sm + ColTile<NY, ACW>::size;
     for (int e = tid; e < NY * ACW; e += nthr) {
         const int p = e / ACW, c = e - p * ACW, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
-        s0[e] = kxi < H ? in0[o] : C(0);
-        s1[e] = kxi < H ? in1[o] : C(0);
+        s0[ColTile<NY, ACW>::at(p, c)] = kxi < H ? in0[o] : C(0);
+        s1[ColTile<NY, ACW>::at(p, c)] = kxi < H ? in1[o] : C(0);
     }
     __syncthreads();
     const int c = tid % ACW, t = tid / ACW;
-    fft_line<NY>(s0, ColAddr<ACW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<ACW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, ACW>::RS}, t, g.twy);
+    }
     for (int e = tid; e < NY * ACW; e += nthr) {
         const int p = e / ACW, cc = e - p * ACW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        if (pr == 1) { out0[o] = s0[e]; out1[o] = s1[e]; }           // L: not an input of the forward march
-        else { out0[o] = out0[o] + s0[e]; out1[o] = out1[o] + s1[e]; }
+        if (pr == 1) { out0[o] = s0[ColTile<NY, ACW>::at(p, cc)]; out1[o] = s1[ColTile<NY, ACW>::at(p, cc)]; }           // L: not an input of the forward march
+        else { out0[o] = out0[o] + s0[ColTile<NY, ACW>::at(p, cc)]; out1[o] = out1[o] + s1[ColTile<NY, ACW>::at(p, cc)]; }
     }
 }
 
@@ -307,8 +310,8 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, c
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * ACW;
-    cpx* s2 = sm + 2 * NY * ACW;
+    cpx* s1 = sm + ColTile<NY, ACW>::size;
+    cpx* s2 = sm + 2 * ColTile<NY, ACW>::size;
     const int hk = blockIdx.y, c0 = blockIdx.x * ACW, tid = threadIdx.x, nthr = ACW * S::T;
     const int H = g.H;
     const long base = long(hk) * g.nkh;
@@ -320,18 +323,19 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, c
             const long o = base + long(p) * H + kx;
             u0 = conj(f * JX[o]); u1 = conj(f * JY[o]); u2 = conj(f * JZ[o]);
         }
-        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+        s0[ColTile<NY, ACW>::at(p, c)] = u0; s1[ColTile<NY, ACW>::at(p, c)] = u1; s2[ColTile<NY, ACW>::at(p, c)] = u2;
     }
     __syncthreads();
     const int c = tid % ACW, t = tid / ACW;
-    fft_line<NY>(s0, ColAddr<ACW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<ACW>{c}, t, g.twy);
-    fft_line<NY>(s2, ColAddr<ACW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[3] = {s0, s1, s2};
+        fft_lines<NY, 3>(ls_, RowAddr{c * ColTile<NY, ACW>::RS}, t, g.twy);
+    }
     for (int e = tid; e < NY * ACW; e += nthr) {
         const int p = e / ACW, cc = e - p * ACW, kx = c0 + cc;
         if (kx >= H) continue;
         const long o = base + long(p) * H + kx;
-        TX[o] = conj(s0[e]); TY[o] = conj(s1[e]); TZ[o] = conj(s2[e]);
+        TX[o] = conj(s0[ColTile<NY, ACW>::at(p, cc)]); TY[o] = conj(s1[ColTile<NY, ACW>::at(p, cc)]); TZ[o] = conj(s2[ColTile<NY, ACW>::at(p, cc)]);
     }
 }
 // rows: the transposed Hermitian split (lz(k) = (lTX + i lTY)/2, lz(nx-k) = (conj lTX + i conj lTY)/2; at
@@ -369,8 +373,10 @@ __global__ void __launch_bounds__(ANT) k_adj_cur_rows(Geo g, const cpx* __restri
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    {
+        decltype(a0) const ls_[2] = {a0, a1};
+        fft_lines<NX, 2>(ls_, RowAddr{r * RS}, t, g.twx);
+    }
     const long nk = g.nk, vpl = long(g.ns + 1) * nk;
     for (int e = tid; e < LPC * NX; e += ANT) {
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
@@ -655,7 +661,7 @@ static unsigned ew_blocks(long n) {
 }
 template <class K>
 static void allow_smem(K kern, size_t smem) {
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(kern), smem);
 }
 
 void launch_adj_objective(Ctx& c, double* dev_out2) {
@@ -677,7 +683,7 @@ static void adj_rf_rows(Ctx& c, const double* lF, cpx* const* W) {
 }
 template <int NY>
 static void adj_rf_cols(Ctx& c, cpx* const* W, cpx* const* lS) {
-    const size_t smem = size_t(2) * NY * ACW * sizeof(cpx);
+    const size_t smem = size_t(2) * ColTile<NY, ACW>::size * sizeof(cpx);
     allow_smem(k_adj_rf_cols<NY>, smem);
     k_adj_rf_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns), 3), ACW * FftShape<NY>::T, smem, c.stream>>>(
         c.geo(), W[0], W[1], W[2], W[3], W[4], W[5], lS[0], lS[1], lS[4], lS[5], lS[2], lS[3]);
@@ -708,7 +714,7 @@ void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, 
 }
 template <int NY>
 static void adj_cur_cols(Ctx& c, cpx* const* ljk, cpx* const* T) {
-    const size_t smem = size_t(3) * NY * ACW * sizeof(cpx);
+    const size_t smem = size_t(3) * ColTile<NY, ACW>::size * sizeof(cpx);
     allow_smem(k_adj_cur_cols<NY>, smem);
     k_adj_cur_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns + 1)), ACW * FftShape<NY>::T, smem, c.stream>>>(
         c.geo(), ljk[0], ljk[1], ljk[2], T[0], T[1], T[2]);

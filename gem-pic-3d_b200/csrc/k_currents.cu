@@ -91,8 +91,10 @@ __global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __rest
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    {
+        decltype(a0) const ls_[2] = {a0, a1};
+        fft_lines<NX, 2>(ls_, RowAddr{r * RS}, t, g.twx);
+    }
     const long base = long(hk) * nkh;
     #pragma unroll 1
     for (int u_ = 0; u_ < (LPC * H + CUR_NT - 1) / CUR_NT; ++u_) {
@@ -118,8 +120,8 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * CW;
-    cpx* s2 = sm + 2 * NY * CW;
+    cpx* s1 = sm + ColTile<NY, CW>::size;
+    cpx* s2 = sm + 2 * ColTile<NY, CW>::size;
     const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(hk) * g.nkh;
@@ -130,13 +132,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
         const int p = e / CW, c = e - p * CW, kx = c0 + c;
         cpx u0 = C(0), u1 = C(0), u2 = C(0);
         if (kx < H) { const long o = base + long(p) * H + kx; u0 = TX[o]; u1 = TY[o]; u2 = TZ[o]; }
-        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+        s0[ColTile<NY, CW>::at(p, c)] = u0; s1[ColTile<NY, CW>::at(p, c)] = u1; s2[ColTile<NY, CW>::at(p, c)] = u2;
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s2, ColAddr<CW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[3] = {s0, s1, s2};
+        fft_lines<NY, 3>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, g.twy);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -145,9 +148,9 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
         if (kx >= H) continue;
         const double f = (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p];
         const long o = base + long(p) * H + kx;
-        JX[o] = f * s0[e];
-        JY[o] = f * s1[e];
-        JZ[o] = f * s2[e];
+        JX[o] = f * s0[ColTile<NY, CW>::at(p, cc)];
+        JY[o] = f * s1[ColTile<NY, CW>::at(p, cc)];
+        JZ[o] = f * s2[ColTile<NY, CW>::at(p, cc)];
     }
 }
 
@@ -168,7 +171,7 @@ static void cur_rows(Ctx& c, cpx* TX, cpx* TY, cpx* TZ) {
     constexpr int LPC = CUR_NT / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
     auto kern = k_cur_rows<NX>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(kern), smem);
     const dim3 grid(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1));
     const int tok = c.prof_begin("cur_rows");
     kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, TX, TY, TZ, c.P.zeta_filter ? 1 : 0);
@@ -178,9 +181,9 @@ static void cur_rows(Ctx& c, cpx* TX, cpx* TY, cpx* TZ) {
 template <int NY>
 static void cur_cols(Ctx& c, bool keep0) {
     constexpr int CW = 8;
-    const size_t smem = size_t(3) * NY * CW * sizeof(cpx);
+    const size_t smem = size_t(3) * ColTile<NY, CW>::size * sizeof(cpx);
     auto kern = k_cur_cols<NY, CW>;
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(kern), smem);
     const dim3 grid(unsigned((c.H + CW - 1) / CW), unsigned(c.ns + 1));
     const int tok = c.prof_begin("cur_cols");
     kern<<<grid, CW * FftShape<NY>::T, smem, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0);

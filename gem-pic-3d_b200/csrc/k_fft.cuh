@@ -104,6 +104,56 @@ __device__ __forceinline__ void fft_line(T* sm, const Addr& A, int t, const T* _
     for (int s = 0; s < S::NR8; ++s) { fft_pass<N, 8>(sm, A, t, L, tw); L *= 8; }
 }
 
+// NL lines of the same shape (one addressing A, bases sm[0..NL)) transformed together: per butterfly the twiddle
+// is loaded once for all of them, the CTA synchronises once per pass for all of them, and the lines' loads and
+// DFTs interleave. Each line gets the same operations as from fft_line.
+template <int N, int R, int NL, class Addr, class T>
+__device__ __forceinline__ void fft_pass_multi(T* const* sm, const Addr& A, int t, int L, const T* __restrict__ tw) {
+    constexpr int E = FftShape<N>::E, TT = FftShape<N>::T, BPT = E / R;
+    const int m = N / (L * R);
+    T v[NL][E];
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int b = t + u * TT, j = b / L, k = b - j * L;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const int a = A((q * m + j) * L + k);
+#pragma unroll
+            for (int l = 0; l < NL; ++l) v[l][u * R + q] = sm[l][a];
+        }
+        if (L > 1) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) {
+                const T w = __ldg(&tw[q * k * m]);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) v[l][u * R + q] = v[l][u * R + q] * w;
+            }
+        }
+#pragma unroll
+        for (int l = 0; l < NL; ++l) dft<R>(&v[l][u * R]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < BPT; ++u) {
+        const int b = t + u * TT, j = b / L, k = b - j * L;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int a = A((j * R + r) * L + k);
+#pragma unroll
+            for (int l = 0; l < NL; ++l) sm[l][a] = v[l][u * R + r];
+        }
+    }
+    __syncthreads();
+}
+template <int N, int NL, class Addr, class T>
+__device__ __forceinline__ void fft_lines(T* const* sm, const Addr& A, int t, const T* __restrict__ tw) {
+    using S = FftShape<N>;
+    int L = 1;
+    if constexpr (S::REM > 1) { fft_pass_multi<N, S::REM, NL>(sm, A, t, L, tw); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR8; ++s) { fft_pass_multi<N, 8, NL>(sm, A, t, L, tw); L *= 8; }
+}
+
 // Shared-memory addressing of a row line: one padding slot per 8 values keeps the strided
 // Stockham accesses free of bank conflicts.
 struct RowAddr {
@@ -112,11 +162,13 @@ struct RowAddr {
 };
 template <int N>
 constexpr int row_stride() { return N + N / 8 + 1; }
-// Shared-memory addressing of a column line inside a tile of CW columns stored row-major.
-template <int CW>
-struct ColAddr {
-    int c;
-    __device__ __forceinline__ int operator()(int p) const { return p * CW + c; }
+// Shared-memory layout of a tile of CW columns: column c stored contiguously at c * RS with the padding of a row,
+// so that the transforms along y (RowAddr{c * RS}) read it without bank conflicts (a tile stored row-major puts a
+// column's values CW elements apart: 2- to 8-way conflicts on every pass).
+template <int N, int CW>
+struct ColTile {
+    static constexpr int RS = row_stride<N>();
+    static constexpr int size = CW * RS;           // elements per array of the tile
+    __device__ static __forceinline__ int at(int p, int c) { return c * RS + p + (p >> 3); }
 };
-
 }  // namespace g3d

@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * CW;
+    cpx* s1 = sm + ColTile<NY, CW>::size;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(l) * g.nkh;
@@ -93,13 +93,15 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
             u = Rx[o] - (-opb * ik(kx, psi));
             v = Ry[o] - (-opb * ik(ky, psi));
         }
-        s0[e] = conj(u);
-        s1[e] = conj(v);
+        s0[ColTile<NY, CW>::at(p, c)] = conj(u);
+        s1[ColTile<NY, CW>::at(p, c)] = conj(v);
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, g.twy);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -107,8 +109,8 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        U[o] = conj(s0[e]);
-        V[o] = conj(s1[e]);
+        U[o] = conj(s0[ColTile<NY, CW>::at(p, cc)]);
+        V[o] = conj(s1[ColTile<NY, CW>::at(p, cc)]);
     }
 }
 
@@ -169,7 +171,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * CW;
+    cpx* s1 = sm + ColTile<NY, CW>::size;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T;
     const int H = g.H;
     const long base = long(l) * g.nkh;
@@ -180,12 +182,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpx u = C(0), v = C(0);
         if (kxi < H) { const long o = base + long(p) * H + kxi; u = U[o]; v = V[o]; }
-        s0[e] = u; s1[e] = v;
+        s0[ColTile<NY, CW>::at(p, c)] = u; s1[ColTile<NY, CW>::at(p, c)] = v;
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, g.twy);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -194,16 +198,16 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
         const cpx psi = PSI[o];
-        Rx[o] = s0[e] - opb * ik(g.kxd[kxi], psi);
-        Ry[o] = s1[e] - opb * ik(g.kyd[p], psi);
+        Rx[o] = s0[ColTile<NY, CW>::at(p, cc)] - opb * ik(g.kxd[kxi], psi);
+        Ry[o] = s1[ColTile<NY, CW>::at(p, cc)] - opb * ik(g.kyd[p], psi);
     }
 }
 
 // ---------------------------------------------------------------- real fields: columns (inverse y of the six spectra)
 // blockIdx.z picks the pair (R_x, R_y), (L_x, L_y) or (E_z, B_z): two fields per CTA keep the shared memory small
 // enough for several CTAs per SM, so loads of one CTA overlap the transforms of another.
-template <int NY>
-__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry,
+template <int NY, int CWT>
+__global__ void __launch_bounds__(CWT * FftShape<NY>::T) k_rf_cols(Geo g, const cpx* __restrict__ Rx, const cpx* __restrict__ Ry,
                                                                   const cpx* __restrict__ Lx, const cpx* __restrict__ Ly,
                                                                   const cpx* __restrict__ Ez, const cpx* __restrict__ Bz,
                                                                   cpx* __restrict__ W0, cpx* __restrict__ W1, cpx* __restrict__ W2,
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
                                                                   int l0) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
-    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z;
+    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CWT, tid = threadIdx.x, nthr = CWT * S::T, pr = blockIdx.z;
     const int H = g.H;
     const long base = long(l) * g.nkh;
     const cpx* in0 = pr == 0 ? Rx : pr == 1 ? Lx : Ez;
@@ -219,29 +223,31 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols(Geo g, const c
     cpx* out0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
     cpx* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * CW;
+    cpx* s1 = sm + ColTile<NY, CWT>::size;
     #pragma unroll
-    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
-        if (e >= NY * CW) break;
-        const int p = e / CW, c = e - p * CW, kxi = c0 + c;
+        if (e >= NY * CWT) break;
+        const int p = e / CWT, c = e - p * CWT, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
-        s0[e] = kxi < H ? conj(in0[o]) : C(0);
-        s1[e] = kxi < H ? conj(in1[o]) : C(0);
+        s0[ColTile<NY, CWT>::at(p, c)] = kxi < H ? conj(in0[o]) : C(0);
+        s1[ColTile<NY, CWT>::at(p, c)] = kxi < H ? conj(in1[o]) : C(0);
     }
     __syncthreads();
-    const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
+    const int c = tid % CWT, t = tid / CWT;
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CWT>::RS}, t, g.twy);
+    }
     #pragma unroll
-    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
-        if (e >= NY * CW) break;
-        const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
+        if (e >= NY * CWT) break;
+        const int p = e / CWT, cc = e - p * CWT, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        out0[o] = conj(s0[e]);
-        out1[o] = conj(s1[e]);
+        out0[o] = conj(s0[ColTile<NY, CWT>::at(p, cc)]);
+        out1[o] = conj(s1[ColTile<NY, CWT>::at(p, cc)]);
     }
 }
 
@@ -276,9 +282,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a2, RowAddr{r * RS}, t, g.twx);
+    {
+        decltype(a0) const ls_[3] = {a0, a1, a2};
+        fft_lines<NX, 3>(ls_, RowAddr{r * RS}, t, g.twx);
+    }
     const double s = g.yf ? 1.0 / double(g.nk) : 1.0 / double(g.nx);   // free-hand y: rows only, 1/nx
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     #pragma unroll 1
@@ -308,13 +315,13 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
 // ---------------------------------------------------------------- launchers
 template <class K>
 static void allow_smem(K kern, size_t smem) {
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(kern), smem);
 }
 static unsigned col_tiles(const Ctx& c) { return unsigned((c.H + CW - 1) / CW); }
 
 template <int NY>
 static void sp_cols_inv(Ctx& c) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
+    const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpx);
     allow_smem(k_sp_cols_inv<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_inv");
     k_sp_cols_inv<NY><<<dim3(col_tiles(c), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
@@ -334,7 +341,7 @@ static void sp_rows(Ctx& c) {
 }
 template <int NY>
 static void sp_cols_fwd(Ctx& c) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
+    const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpx);
     allow_smem(k_sp_cols_fwd<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_fwd");
     k_sp_cols_fwd<NY><<<dim3(col_tiles(c), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
@@ -348,15 +355,21 @@ void launch_sponge(Ctx& c) {
     G3D_DISPATCH_N(c.ny, NY, sp_cols_fwd<NY>(c));
 }
 
-template <int NY>
-static void rf_cols(Ctx& c, int l0, int nl) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpx);
-    allow_smem(k_rf_cols<NY>, smem);
+// one slice (the plasma march): tiles of 2 columns, so that 3 x 65 CTAs spread the slice's latency over the SMs
+template <int NY, int CWT>
+static void rf_cols_w(Ctx& c, int l0, int nl) {
+    const size_t smem = size_t(2) * ColTile<NY, CWT>::size * sizeof(cpx);
+    allow_smem(k_rf_cols<NY, CWT>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_cols_slice" : "real_cols");
-    k_rf_cols<NY><<<dim3(col_tiles(c), unsigned(nl), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
+    k_rf_cols<NY, CWT><<<dim3(unsigned((c.H + CWT - 1) / CWT), unsigned(nl), 3), CWT * FftShape<NY>::T, smem, c.stream>>>(
         c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, l0);
     c.check_launch("k_rf_cols");
     c.prof_end(tok);
+}
+template <int NY>
+static void rf_cols(Ctx& c, int l0, int nl) {
+    if (nl == 1) rf_cols_w<NY, 2>(c, l0, nl);
+    else rf_cols_w<NY, CW>(c, l0, nl);
 }
 template <int NX>
 static void rf_rows(Ctx& c, int l0, int nl) {

@@ -231,7 +231,7 @@ static void march_launch(Ctx& c, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, c
                          const T* jky, const T* jkz, double D) {
     const unsigned blocks = unsigned((2 * c.nkh + BT - 1) / BT);
     const size_t smem = size_t(DEPTH) * slot_doubles(BT) * sizeof(double);
-    G3D_CUDA(cudaFuncSetAttribute(k_march<T, BT, DEPTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(k_march<T, BT, DEPTH>), smem);
     k_march<T, BT, DEPTH><<<blocks, BT, smem, c.stream>>>(c.geo(), Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
 }
 static bool narrow_blocks(const Ctx& c) { return 2 * c.nkh < 2L * 148 * 64; }

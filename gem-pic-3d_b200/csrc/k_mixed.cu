@@ -108,8 +108,10 @@ __global__ void __launch_bounds__(NT) k_cur_rows_f(Geo g, const float* __restric
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, tw);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, tw);
+    {
+        decltype(a0) const ls_[2] = {a0, a1};
+        fft_lines<NX, 2>(ls_, RowAddr{r * RS}, t, tw);
+    }
     const long base = long(hk) * nkh;
     #pragma unroll
     for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
@@ -135,8 +137,8 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols_f(Geo g, cons
     using S = FftShape<NY>;
     extern __shared__ cpxf smf[];
     cpxf* s0 = smf;
-    cpxf* s1 = smf + NY * CW;
-    cpxf* s2 = smf + 2 * NY * CW;
+    cpxf* s1 = smf + ColTile<NY, CW>::size;
+    cpxf* s2 = smf + 2 * ColTile<NY, CW>::size;
     const int hk = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long base = long(hk) * g.nkh;
     #pragma unroll
@@ -146,13 +148,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols_f(Geo g, cons
         const int p = e / CW, c = e - p * CW, kx = c0 + c;
         cpxf u0 = Cf(0), u1 = Cf(0), u2 = Cf(0);
         if (kx < H) { const long o = base + long(p) * H + kx; u0 = TX[o]; u1 = TY[o]; u2 = TZ[o]; }
-        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+        s0[ColTile<NY, CW>::at(p, c)] = u0; s1[ColTile<NY, CW>::at(p, c)] = u1; s2[ColTile<NY, CW>::at(p, c)] = u2;
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
-    fft_line<NY>(s2, ColAddr<CW>{c}, t, tw);
+    {
+        decltype(s0) const ls_[3] = {s0, s1, s2};
+        fft_lines<NY, 3>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, tw);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -161,7 +164,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols_f(Geo g, cons
         if (kx >= H) continue;
         const float f = (kx == 0 && p == 0 && !keep0) ? 0.0f : float(g.filt[kx] * g.filty[p]);
         const long o = base + long(p) * H + kx;
-        JX[o] = f * s0[e]; JY[o] = f * s1[e]; JZ[o] = f * s2[e];
+        JX[o] = f * s0[ColTile<NY, CW>::at(p, cc)]; JY[o] = f * s1[ColTile<NY, CW>::at(p, cc)]; JZ[o] = f * s2[ColTile<NY, CW>::at(p, cc)];
     }
 }
 
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv_f(Geo g, c
     using S = FftShape<NY>;
     extern __shared__ cpxf smf[];
     cpxf* s0 = smf;
-    cpxf* s1 = smf + NY * CW;
+    cpxf* s1 = smf + ColTile<NY, CW>::size;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long nk = g.nkh, base = long(l) * nk;
     const int n = g.a + l;
@@ -240,12 +243,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv_f(Geo g, c
             u = to_f(Rx[o] + opb * ik(kx, psi));              // R - R_b, R_b = -(1 + beta) i k psi
             v = to_f(Ry[o] + opb * ik(ky, psi));
         }
-        s0[e] = conj(u); s1[e] = conj(v);
+        s0[ColTile<NY, CW>::at(p, c)] = conj(u); s1[ColTile<NY, CW>::at(p, c)] = conj(v);
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, tw);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv_f(Geo g, c
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        U[o] = conj(s0[e]); V[o] = conj(s1[e]);
+        U[o] = conj(s0[ColTile<NY, CW>::at(p, cc)]); V[o] = conj(s1[ColTile<NY, CW>::at(p, cc)]);
     }
 }
 template <int NX>
@@ -315,7 +320,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd_f(Geo g, c
     using S = FftShape<NY>;
     extern __shared__ cpxf smf[];
     cpxf* s0 = smf;
-    cpxf* s1 = smf + NY * CW;
+    cpxf* s1 = smf + ColTile<NY, CW>::size;
     const int l = blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     const long base = long(l) * g.nkh;
     #pragma unroll
@@ -325,12 +330,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd_f(Geo g, c
         const int p = e / CW, c = e - p * CW, kxi = c0 + c;
         cpxf u = Cf(0), v = Cf(0);
         if (kxi < H) { const long o = base + long(p) * H + kxi; u = U[o]; v = V[o]; }
-        s0[e] = u; s1[e] = v;
+        s0[ColTile<NY, CW>::at(p, c)] = u; s1[ColTile<NY, CW>::at(p, c)] = v;
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, tw);
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -338,14 +345,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd_f(Geo g, c
         const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        Rx[o] = Rx[o] + to_d(s0[e]);                   // R + dR in FP64
-        Ry[o] = Ry[o] + to_d(s1[e]);
+        Rx[o] = Rx[o] + to_d(s0[ColTile<NY, CW>::at(p, cc)]);                   // R + dR in FP64
+        Ry[o] = Ry[o] + to_d(s1[ColTile<NY, CW>::at(p, cc)]);
     }
 }
 
 // ---------------------------------------------------------------- real fields (FP32 transforms of the FP64 R)
-template <int NY>
-__global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const cpxf* __restrict__ tw, const cpx* __restrict__ Rx,
+template <int NY, int CWT>
+__global__ void __launch_bounds__(CWT * FftShape<NY>::T) k_rf_cols_f(Geo g, const cpxf* __restrict__ tw, const cpx* __restrict__ Rx,
                                                                     const cpx* __restrict__ Ry, const cpxf* __restrict__ Lx,
                                                                     const cpxf* __restrict__ Ly, const cpxf* __restrict__ Ez,
                                                                     const cpxf* __restrict__ Bz, cpxf* __restrict__ W0,
@@ -354,17 +361,17 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const
                                                                     int l0) {
     using S = FftShape<NY>;
     extern __shared__ cpxf smf[];
-    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, pr = blockIdx.z, H = g.H;
+    const int l = l0 + blockIdx.y, c0 = blockIdx.x * CWT, tid = threadIdx.x, nthr = CWT * S::T, pr = blockIdx.z, H = g.H;
     const long base = long(l) * g.nkh;
     cpxf* out0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
     cpxf* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     cpxf* s0 = smf;
-    cpxf* s1 = smf + NY * CW;
+    cpxf* s1 = smf + ColTile<NY, CWT>::size;
     #pragma unroll 1
-    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
-        if (e >= NY * CW) break;
-        const int p = e / CW, c = e - p * CW, kxi = c0 + c;
+        if (e >= NY * CWT) break;
+        const int p = e / CWT, c = e - p * CWT, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
         cpxf a = Cf(0), b = Cf(0);
         if (kxi < H) {
@@ -372,20 +379,22 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_rf_cols_f(Geo g, const
             else if (pr == 1) { a = Lx[o]; b = Ly[o]; }
             else { a = Ez[o]; b = Bz[o]; }
         }
-        s0[e] = conj(a); s1[e] = conj(b);
+        s0[ColTile<NY, CWT>::at(p, c)] = conj(a); s1[ColTile<NY, CWT>::at(p, c)] = conj(b);
     }
     __syncthreads();
-    const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, tw);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, tw);
+    const int c = tid % CWT, t = tid / CWT;
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, RowAddr{c * ColTile<NY, CWT>::RS}, t, tw);
+    }
     #pragma unroll 1
-    for (int u_ = 0; u_ < (NY * CW + nthr - 1) / nthr; ++u_) {
+    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
-        if (e >= NY * CW) break;
-        const int p = e / CW, cc = e - p * CW, kxi = c0 + cc;
+        if (e >= NY * CWT) break;
+        const int p = e / CWT, cc = e - p * CWT, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        out0[o] = conj(s0[e]); out1[o] = conj(s1[e]);
+        out0[o] = conj(s0[ColTile<NY, CWT>::at(p, cc)]); out1[o] = conj(s1[ColTile<NY, CWT>::at(p, cc)]);
     }
 }
 template <int NX>
@@ -414,7 +423,7 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    for (int f = 0; f < 3; ++f) fft_line<NX>(a[f], RowAddr{r * RS}, t, tw);
+    fft_lines<NX, 3>(a, RowAddr{r * RS}, t, tw);
     const float s = 1.0f / float(g.nk);
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     #pragma unroll
@@ -477,7 +486,7 @@ static unsigned ew_blocks(long n) {
 }
 template <class K>
 static void allow_smem(K kern, size_t smem) {
-    G3D_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(kern), smem);
 }
 
 void launch_deposit_f(Ctx& c) {
@@ -501,7 +510,7 @@ static void cur_rows_f(Ctx& c) {
 }
 template <int NY>
 static void cur_cols_f(Ctx& c, bool keep0) {
-    const size_t smem = size_t(3) * NY * CW * sizeof(cpxf);
+    const size_t smem = size_t(3) * ColTile<NY, CW>::size * sizeof(cpxf);
     allow_smem(k_cur_cols_f<NY>, smem);
     const int tok = c.prof_begin("cur_cols");
     k_cur_cols_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(c.ns + 1)), CW * FftShape<NY>::T, smem, c.stream>>>(
@@ -523,7 +532,7 @@ void launch_comoving_f(Ctx& c, double beta, double gm2) {
 }
 template <int NY>
 static void sp_cols_inv_f(Ctx& c) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpxf);
+    const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpxf);
     allow_smem(k_sp_cols_inv_f<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_inv");
     k_sp_cols_inv_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
@@ -544,7 +553,7 @@ static void sp_rows_f(Ctx& c) {
 }
 template <int NY>
 static void sp_cols_fwd_f(Ctx& c) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpxf);
+    const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpxf);
     allow_smem(k_sp_cols_fwd_f<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_fwd");
     k_sp_cols_fwd_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(c.ns)), CW * FftShape<NY>::T, smem, c.stream>>>(
@@ -557,17 +566,23 @@ void launch_sponge_f(Ctx& c) {
     G3D_DISPATCH_N(c.nx, NX, sp_rows_f<NX>(c));
     G3D_DISPATCH_N(c.ny, NY, sp_cols_fwd_f<NY>(c));
 }
-template <int NY>
-static void rf_cols_f(Ctx& c, int l0, int nl) {
-    const size_t smem = size_t(2) * NY * CW * sizeof(cpxf);
-    allow_smem(k_rf_cols_f<NY>, smem);
+template <int NY, int CWT>
+static void rf_cols_fw(Ctx& c, int l0, int nl) {
+    const size_t smem = size_t(2) * ColTile<NY, CWT>::size * sizeof(cpxf);
+    allow_smem(k_rf_cols_f<NY, CWT>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_cols_slice" : "real_cols");
     auto& m = c.mx;
-    k_rf_cols_f<NY><<<dim3(unsigned((c.H + CW - 1) / CW), unsigned(nl), 3), CW * FftShape<NY>::T, smem, c.stream>>>(
+    k_rf_cols_f<NY, CWT><<<dim3(unsigned((c.H + CWT - 1) / CWT), unsigned(nl), 3), CWT * FftShape<NY>::T, smem, c.stream>>>(
         c.geo(), m.twy.p, c.Rx.p, c.Ry.p, m.Lx.p, m.Ly.p, m.Ez.p, m.Bz.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p,
         l0);
     c.check_launch("k_rf_cols_f");
     c.prof_end(tok);
+}
+// one slice (the plasma march): tiles of 2 columns, so that 3 x 65 CTAs spread the slice's latency over the SMs
+template <int NY>
+static void rf_cols_f(Ctx& c, int l0, int nl) {
+    if (nl == 1) rf_cols_fw<NY, 2>(c, l0, nl);
+    else rf_cols_fw<NY, CW>(c, l0, nl);
 }
 template <int NX>
 static void rf_rows_f(Ctx& c, int l0, int nl) {

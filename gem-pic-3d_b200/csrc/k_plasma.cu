@@ -384,8 +384,10 @@ __global__ void __launch_bounds__(128) k_ss_rows(Geo g, const JT* __restrict__ J
     }
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
-    fft_line<NX>(a0, RowAddr{r * RS}, t, g.twx);
-    fft_line<NX>(a1, RowAddr{r * RS}, t, g.twx);
+    {
+        decltype(a0) const ls_[2] = {a0, a1};
+        fft_lines<NX, 2>(ls_, RowAddr{r * RS}, t, g.twx);
+    }
     for (int e = tid; e < LPC * H; e += 128) {
         const int rr = e / H, kx = e - rr * H, row = r0 + rr;
         if (row >= g.ny) continue;
@@ -406,30 +408,41 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_ss_cols(Geo g, const c
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
-    cpx* s1 = sm + NY * CW;
-    cpx* s2 = sm + 2 * NY * CW;
+    cpx* s1 = sm + ColTile<NY, CW>::size;
+    cpx* s2 = sm + 2 * ColTile<NY, CW>::size;
     const int c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
     for (int e = tid; e < NY * CW; e += nthr) {
         const int p = e / CW, c = e - p * CW, kx = c0 + c;
         cpx u0 = C(0), u1 = C(0), u2 = C(0);
         if (kx < H) { const long o = long(p) * H + kx; u0 = T0[o]; u1 = T1[o]; u2 = T2[o]; }
-        s0[e] = u0; s1[e] = u1; s2[e] = u2;
+        s0[ColTile<NY, CW>::at(p, c)] = u0; s1[ColTile<NY, CW>::at(p, c)] = u1; s2[ColTile<NY, CW>::at(p, c)] = u2;
     }
     __syncthreads();
     const int c = tid % CW, t = tid / CW;
-    fft_line<NY>(s0, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s1, ColAddr<CW>{c}, t, g.twy);
-    fft_line<NY>(s2, ColAddr<CW>{c}, t, g.twy);
+    {
+        decltype(s0) const ls_[3] = {s0, s1, s2};
+        fft_lines<NY, 3>(ls_, RowAddr{c * ColTile<NY, CW>::RS}, t, g.twy);
+    }
     const long nkh = g.nkh;
-    for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, cc = e - p * CW, kx = c0 + cc;
+    constexpr int EPT = NY / S::T;            // elements of a thread (e = tid + u nthr)
+    double f[EPT];
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {            // the filter factors first: their loads wait for no store
+        const int e = tid + u * nthr, p = e / CW, kx = c0 + (e - p * CW);
+        f[u] = 0;
+        if (kx < H) {
+            const double k2 = g.kxs[kx] * g.kxs[kx] + g.kys[p] * g.kys[p];
+            f[u] = !filter ? 1.0 : (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p] / (1 + a2 * k2);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+        const int e = tid + u * nthr, p = e / CW, cc = e - p * CW, kx = c0 + cc;
         if (kx >= H) continue;
-        const double k2 = g.kxs[kx] * g.kxs[kx] + g.kys[p] * g.kys[p];
-        const double f = !filter ? 1.0 : (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p] / (1 + a2 * k2);
         const long o = long(p) * H + kx;
-        out[o] = f * s0[e];
-        out[nkh + o] = f * s1[e];
-        out[2 * nkh + o] = f * s2[e];
+        out[o] = f[u] * s0[ColTile<NY, CW>::at(p, cc)];
+        out[nkh + o] = f[u] * s1[ColTile<NY, CW>::at(p, cc)];
+        out[2 * nkh + o] = f[u] * s2[ColTile<NY, CW>::at(p, cc)];
     }
 }
 
@@ -533,15 +546,81 @@ __global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* Rx, cpx* Ry, T*
     if (i < g.nkh) march_slice_mode<T>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D, n, i);
 }
 // a pass's current of half-cell n in place and the prediction of n-1 (replace_pred), then the march of slice n,
-// per mode in one thread (Fourier y)
+// per mode in one thread (Fourier y, one rank: a = 0). Every load is issued before the first store, and the march
+// takes the two half-cells' new currents from registers (as stored: narrowed to T), so the thread's memory
+// requests overlap instead of following each other.
 template <class T>
-__global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly,
-                                                      const T* j0x, const T* j0y, double D, int n, int extrap, double w) {
+__global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry,
+                                                      T* __restrict__ Ez, T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
+                                                      const T* __restrict__ j0x, const T* __restrict__ j0y, double D, int n,
+                                                      int extrap, double w) {
+    const long nk = g.nkh;
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= g.nkh) return;
-    replace_pred_mode<T>(p, n, extrap, w, i);
-    march_slice_mode<T>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, static_cast<const T*>(p.jkx), static_cast<const T*>(p.jky),
-                        static_cast<const T*>(p.jkz), D, n, i);
+    if (i >= nk) return;
+    const long hp = long(n + 1) * nk + i, hq = long(n) * nk + i;      // half-cells n and n-1
+    T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
+    const bool pred = extrap && n >= 1;
+    cpx u[3], sn[3], kp[3], kq[3], s0p[3], s0q[3], dl[3], pn[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        u[k] = p.jsn[k * nk + i]; sn[k] = p.sin_[k * nk + i];
+        kp[k] = widen(jk[k][hp]); kq[k] = widen(jk[k][hq]);
+        if (pred) {
+            const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
+            s0p[k] = s0[k][hp]; s0q[k] = s0[k][hq]; dl[k] = p.dl[k * nk + i]; pn[k] = p.pin[k * nk + i];
+        }
+    }
+    // the march's own loads (slice n of level s0, slice n+1 of level s1, j0 of both half-cells)
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
+    const long o = long(n - g.a) * nk + i, ou = o + nk;
+    const cpx j0xd = widen(j0x[o]), j0xu = widen(j0x[ou]), j0yd = widen(j0y[o]), j0yu = widen(j0y[ou]);
+    const cpx rx = Rx[o], ry = Ry[o], ez = widen(Ez[o]), bz = widen(Bz[o]);
+    const bool front = n == g.N - 1;
+    cpx pRx = C(0), pRy = C(0), pEz = C(0), pBz = C(0), pLx = C(0), pLy = C(0);
+    if (!front) {
+        const long pp = o + nk;
+        pRx = Rx[pp]; pRy = Ry[pp]; pEz = widen(Ez[pp]); pBz = widen(Bz[pp]); pLx = widen(Lx[pp]); pLy = widen(Ly[pp]);
+    }
+    // replace(n, sin, jsn) and the prediction of n-1
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const T np_ = narrow<T>(kp[k] + u[k] - sn[k]);
+        jk[k][hp] = np_; kp[k] = widen(np_);
+        p.sin_[k * nk + i] = u[k];
+        if (pred) {
+            const cpx d = u[k] - s0p[k];
+            const cpx t = s0q[k] + d + w * (d - dl[k]);
+            const T nq_ = narrow<T>(kq[k] + t - pn[k]);
+            jk[k][hq] = nq_; kq[k] = widen(nq_);
+            p.pin[k * nk + i] = t;
+        }
+    }
+    // the march of slice n (march_slice_mode with the currents of half-cells n-1 = kq and n = kp)
+    const cpx Jx = wl * (j0xd + kq[0]) + wu * (j0xu + kp[0]);
+    const cpx Jy = wl * (j0yd + kq[1]) + wu * (j0yu + kp[1]);
+    const cpx Rsx = rx + D * (ik(kx, ez) + ik(ky, bz)) - D * Jx;
+    const cpx Rsy = ry + D * (ik(ky, ez) - ik(kx, bz)) - D * Jy;
+    if (front) {
+        Rx[o] = Rsx; Ry[o] = Rsy;
+        Ez[o] = narrow<T>(C(0)); Bz[o] = narrow<T>(C(0)); Lx[o] = narrow<T>(C(0)); Ly[o] = narrow<T>(C(0));
+        return;
+    }
+    const double h = g.hcg[n + 2];
+    const cpx upx = kp[0], upy = kp[1], upz = kp[2];
+    const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
+    const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
+    const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
+    const cpx Qp = -0.5 * ik(kx, pRx - pLx) + 0.5 * ik(ky, pLy - pRy);
+    const cpx SB = ik(kx, Rsy) + ik(kx, Lsy) - ik(ky, Rsx) - ik(ky, Lsx);
+    const cpx SE = -ik(kx, Rsx) + ik(kx, Lsx) + ik(ky, Lsy) - ik(ky, Rsy);
+    const double den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+    const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) / den;
+    const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) / den;
+    Ez[o] = narrow<T>(Ezn); Bz[o] = narrow<T>(Bzn);
+    Rx[o] = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)); Ry[o] = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
+    Lx[o] = narrow<T>(Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)));
+    Ly[o] = narrow<T>(Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn)));
 }
 // freed electrons join the march (appended after the streaming particles; the count stays on the device)
 __global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
@@ -664,15 +743,15 @@ static void ss_rows(Ctx& c, const JT* J, cpx* T) {
     using S = FftShape<NX>;
     constexpr int LPC = 128 / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
-    G3D_CUDA(cudaFuncSetAttribute(k_ss_rows<NX, JT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    smem_attr(reinterpret_cast<const void*>(k_ss_rows<NX, JT>), smem);
     k_ss_rows<NX, JT><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh);
     c.check_launch("k_ss_rows");
 }
 template <int NY>
 static void ss_cols(Ctx& c, const cpx* T, cpx* out, double a2, int keep0, int filter) {
-    constexpr int CW = 8;
-    const size_t smem = size_t(3) * NY * CW * sizeof(cpx);
-    G3D_CUDA(cudaFuncSetAttribute(k_ss_cols<NY, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    constexpr int CW = 2;              // one slice: 2-column tiles spread its latency over 65 SMs (measured: 8 used 17)
+    const size_t smem = size_t(3) * ColTile<NY, CW>::size * sizeof(cpx);
+    smem_attr(reinterpret_cast<const void*>(k_ss_cols<NY, CW>), smem);
     k_ss_cols<NY, CW><<<unsigned((c.H + CW - 1) / CW), CW * FftShape<NY>::T, smem, c.stream>>>(
         c.geo(), T, T + c.nkh, T + 2 * c.nkh, out, a2, keep0, filter);
     c.check_launch("k_ss_cols");
