@@ -211,6 +211,25 @@ void launch_sponge_fh(Ctx& c);
 void launch_real_fields_fh(Ctx& c);
 void launch_comoving_fh(Ctx& c, double beta, double gm2);
 void launch_march_slice_fh(Ctx& c, double D, int n);
+// The midpoint fields that the rows kernel of one slice also writes, for the streaming gather of the next pass:
+// 0.5 (F(l) + F(other)) per point, interleaved (FP32: 8 floats, FP64: 6 doubles); out null: none
+struct FmidOut {
+    void* out = nullptr;
+    int other = 0, f32 = 0;
+};
+__device__ __forceinline__ void fmid_store(const FmidOut& fm, const float* F, long fpl, long nk, long k, const float v[6]) {
+    double m[6];
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) m[comp] = 0.5 * (double(v[comp]) + double(F[comp * fpl + long(fm.other) * nk + k]));
+    if (fm.f32) {
+        float4* o = reinterpret_cast<float4*>(fm.out) + 2 * k;
+        o[0] = make_float4(float(m[0]), float(m[1]), float(m[2]), float(m[3]));
+        o[1] = make_float4(float(m[4]), float(m[5]), 0.f, 0.f);
+    } else {
+        double2* o = reinterpret_cast<double2*>(fm.out) + 3 * k;
+        o[0] = make_double2(m[0], m[1]); o[1] = make_double2(m[2], m[3]); o[2] = make_double2(m[4], m[5]);
+    }
+}
 void launch_real_fields_slice_fh(Ctx& c, int l);
 void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2);
 void launch_sp_rows(Ctx& c);                // k_fields.cu
@@ -244,7 +263,7 @@ void launch_full_to_half_f(Ctx& c, const cpx* full, cpxf* half, long planes);
 void launch_rotate_f(Ctx& c, cpxf* p, size_t n, double sx, double sy, int nys);
 void launch_copy_f(Ctx& c, cpxf* y, const cpxf* x, size_t n);
 void launch_axpy_fc(Ctx& c, cpxf* y, const cpx* x, double a, size_t n);   // y = y + a x
-void launch_real_fields_slice_f(Ctx& c, int l);
+void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm = FmidOut());
 // particles and plasma (g3d_host.cu, g3d_plasma.cu)
 void set_particles(Ctx& c, const g3d_particle* v, long n);
 std::vector<g3d_particle> get_particles(Ctx& c);

@@ -267,10 +267,18 @@ static uint64_t mix64h(uint64_t z) {
     return z ^ (z >> 31);
 }
 
-static void real_fields_slice(Ctx& c, int l) {
-    if (!c.yf) launch_real_fields_slice_fh(c, l);
-    else if (c.mixed) launch_real_fields_slice_f(c, l);
-    else launch_real_fields_slice(c, l);
+// E and B of slice l; Fourier y: with the midpoint fields of slice `target` (l for the next pass of half-cell l,
+// l - 1 for the first pass of half-cell l - 1, -1: none) for the streaming gather
+static void real_fields_slice(Ctx& c, int l, int target = -1) {
+    if (!c.yf) { launch_real_fields_slice_fh(c, l); return; }
+    FmidOut fm;
+    if (target >= c.a) {
+        fm.out = c.pl->fmid.p;
+        fm.other = (target == l ? l + 1 : l - 1) - c.a;
+        fm.f32 = c.f32s ? 1 : 0;
+    }
+    if (c.mixed) launch_real_fields_slice_f(c, l, fm);
+    else launch_real_fields_slice(c, l, fm);
 }
 
 void march_plasma(Ctx& c, double s0, double s1) {
@@ -305,10 +313,16 @@ void march_plasma(Ctx& c, double s0, double s1) {
     mixk(dbits);
     auto issue = [&]() {
         bool have_dl = false;
+        const bool fh = !c.yf;
+        // the deposit planes and the count of freed electrons start cleared (the rows kernel of every pass clears
+        // them again for the next one)
+        if (c.f32s) G3D_CUDA(cudaMemsetAsync(P.jsrf.p, 0, size_t(3) * c.nk * sizeof(float), c.stream));
+        else G3D_CUDA(cudaMemsetAsync(P.jsr.p, 0, size_t(3) * c.nk * sizeof(double), c.stream));
+        G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
         // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
         launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
-        real_fields_slice(c, N - 1);
+        real_fields_slice(c, N - 1, N - 2);
 
         StreamArgs sa;
         sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
@@ -319,24 +333,27 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
-            launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
+            // (for the half-cells below the first, fused into the correction of the half-cell above)
+            if (n == nhi) launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
             const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
             for (int pass = 0; pass < passes; ++pass) {
-                launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
+                if (fh) launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
                 sa.pass = pass;
                 sa.dry = pass + 1 < passes ? 1 : 0;
                 launch_stream(c, sa);
+                // freed electrons join the march (after the last pass's stream, before its rows kernel clears the count)
+                if (ionz && pass + 1 == passes) launch_born_append(c);
                 launch_stream_spectra(c);
-                if (c.yf) launch_replace_march(c, D, n, extrap ? 1 : 0, wex);
+                if (!fh) launch_replace_march(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
                 else { launch_replace_pred(c, n, extrap ? 1 : 0, wex); launch_march_slice(c, D, n); }
-                real_fields_slice(c, n);
+                real_fields_slice(c, n, pass + 1 < passes ? n : n - 1);
             }
-            if (ionz) launch_born_append(c);
             // half-cell n is final: correct R at slice n+1, keep the change and the current
             const double q = D * c.wlo_h[size_t(n + 1)];
-            launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
+            if (n - 1 >= c.a) launch_correct_prologue(c, n, q, n + 1 < c.b ? 1 : 0, n - 1 >= 1 ? n - 2 : -1, passes > 1 ? 1 : 0);
+            else launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
             have_dl = true;
         }
     };

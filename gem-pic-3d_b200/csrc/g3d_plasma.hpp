@@ -112,15 +112,16 @@ struct PlasmaState {
 void launch_stream(Ctx& c, const StreamArgs& a);
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
 void launch_pass_prologue(Ctx& c, int n, int restore);
-void launch_replace_march(Ctx& c, double D, int n, int extrap, double w);
+void launch_replace_march(Ctx& c, double D, int n, int extrap, double w, int restore);
 void launch_stream_spectra(Ctx& c);
 void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw);
 void launch_replace_pred(Ctx& c, int n, int extrap, double w);
 void launch_correct(Ctx& c, int n, double q, int own);
+void launch_correct_prologue(Ctx& c, int n, double q, int own, int pred_m, int backup);
 void launch_march_slice(Ctx& c, double D, int n);
 void launch_born_append(Ctx& c);
 // number of particles with alive == state among n (n_dev: the count on the device instead, when not null)
 long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state);
-void launch_real_fields_slice(Ctx& c, int l);
+void launch_real_fields_slice(Ctx& c, int l, FmidOut fm = FmidOut());
 
 }  // namespace g3d

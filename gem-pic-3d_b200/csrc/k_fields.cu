@@ -256,7 +256,7 @@ template <int NX>
 __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                const cpx* __restrict__ W2, const cpx* __restrict__ W3,
                                                const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F, int l0,
-                                               double* __restrict__ Fd) {
+                                               double* __restrict__ Fd, FmidOut fm) {
     using S = FftShape<NX>;
     constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -298,12 +298,11 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
         const cpx z1 = s * conj(a0[q]), z2 = s * conj(a1[q]), z3 = s * conj(a2[q]);
         const long idx = fbase + long(row) * NX + p;
         const double r1 = z1.x, r2 = z1.y, l1 = z2.x, l2 = z2.y;
-        F[0 * fpl + idx] = float(0.5 * (r1 + l1));     // E_x
-        F[1 * fpl + idx] = float(0.5 * (r2 + l2));     // E_y
-        F[3 * fpl + idx] = float(0.5 * (l2 - r2));     // B_x
-        F[4 * fpl + idx] = float(0.5 * (r1 - l1));     // B_y
-        F[2 * fpl + idx] = float(z3.x);                // E_z
-        F[5 * fpl + idx] = float(z3.y);                // B_z
+        const float fv[6] = {float(0.5 * (r1 + l1)), float(0.5 * (r2 + l2)), float(z3.x),    // E_x, E_y, E_z
+                             float(0.5 * (l2 - r2)), float(0.5 * (r1 - l1)), float(z3.y)};  // B_x, B_y, B_z
+#pragma unroll
+        for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
+        if (fm.out) fmid_store(fm, F, fpl, g.nk, long(row) * NX + p, fv);
         if (Fd) {                                      // exact fields: the same values before the rounding
             Fd[0 * fpl + idx] = 0.5 * (r1 + l1); Fd[1 * fpl + idx] = 0.5 * (r2 + l2);
             Fd[3 * fpl + idx] = 0.5 * (l2 - r2); Fd[4 * fpl + idx] = 0.5 * (r1 - l1);
@@ -372,13 +371,13 @@ static void rf_cols(Ctx& c, int l0, int nl) {
     else rf_cols_w<NY, CW>(c, l0, nl);
 }
 template <int NX>
-static void rf_rows(Ctx& c, int l0, int nl) {
+static void rf_rows(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
     allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0, c.Fd.p);
+        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0, c.Fd.p, fm);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
@@ -394,7 +393,7 @@ static void rf_rows_direct(Ctx& c, int l0, int nl) {
     allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0, c.Fd.p);
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0, c.Fd.p, FmidOut());
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
@@ -403,9 +402,9 @@ void launch_real_fields_slice_fh(Ctx& c, int l) { G3D_DISPATCH_N(c.nx, NX, rf_ro
 // the sponge's row pass alone (inverse x, mask, forward x) on W0, W1: the free-hand y sponge
 void launch_sp_rows(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, sp_rows<NX>(c)); }
 // E and B of one slice (plane l) in real space (Simulation::real_fields_slice, src/sim_plasma.cpp:200-220)
-void launch_real_fields_slice(Ctx& c, int l) {
+void launch_real_fields_slice(Ctx& c, int l, FmidOut fm) {
     G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, l, 1));
-    G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, l, 1));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, l, 1, fm));
 }
 
 // ---------------------------------------------------------------- half <-> full spectrum layouts

@@ -401,7 +401,7 @@ template <int NX>
 __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict__ tw, const cpxf* __restrict__ W0,
                                                  const cpxf* __restrict__ W1, const cpxf* __restrict__ W2,
                                                  const cpxf* __restrict__ W3, const cpxf* __restrict__ W4,
-                                                 const cpxf* __restrict__ W5, float* __restrict__ F, int l0) {
+                                                 const cpxf* __restrict__ W5, float* __restrict__ F, int l0, FmidOut fm) {
     using S = FftShape<NX>;
     constexpr int LPC = NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpxf smf[];
@@ -435,12 +435,11 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
         const int q = rr * RS + p + (p >> 3);
         const cpxf z1 = s * conj(a[0][q]), z2 = s * conj(a[1][q]), z3 = s * conj(a[2][q]);
         const long idx = fbase + long(row) * NX + p;
-        F[0 * fpl + idx] = 0.5f * (z1.x + z2.x);
-        F[1 * fpl + idx] = 0.5f * (z1.y + z2.y);
-        F[3 * fpl + idx] = 0.5f * (z2.y - z1.y);
-        F[4 * fpl + idx] = 0.5f * (z1.x - z2.x);
-        F[2 * fpl + idx] = z3.x;
-        F[5 * fpl + idx] = z3.y;
+        const float fv[6] = {0.5f * (z1.x + z2.x), 0.5f * (z1.y + z2.y), z3.x,      // E_x, E_y, E_z
+                             0.5f * (z2.y - z1.y), 0.5f * (z1.x - z2.x), z3.y};     // B_x, B_y, B_z
+#pragma unroll
+        for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
+        if (fm.out) fmid_store(fm, F, fpl, g.nk, long(row) * NX + p, fv);
     }
 }
 
@@ -585,14 +584,14 @@ static void rf_cols_f(Ctx& c, int l0, int nl) {
     else rf_cols_fw<NY, CW>(c, l0, nl);
 }
 template <int NX>
-static void rf_rows_f(Ctx& c, int l0, int nl) {
+static void rf_rows_f(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpxf);
     allow_smem(k_rf_rows_f<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     auto& m = c.mx;
     k_rf_rows_f<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), m.twx.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p, c.F.p, l0);
+        c.geo(), m.twx.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p, c.F.p, l0, fm);
     c.check_launch("k_rf_rows_f");
     c.prof_end(tok);
 }
@@ -601,9 +600,9 @@ void launch_real_fields_f(Ctx& c) {
     G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, 0, c.ns));
 }
 // E and B of one slice (plane l) of the mixed form (the real fields of one slice of the plasma march)
-void launch_real_fields_slice_f(Ctx& c, int l) {
+void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm) {
     G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c, l, 1));
-    G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, l, 1));
+    G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, l, 1, fm));
 }
 void launch_half_to_full_f(Ctx& c, const cpxf* half, cpx* full, long planes) {
     k_half_to_full_f<<<ew_blocks(planes * c.nk), 256, 0, c.stream>>>(c.geo(), half, full, planes);

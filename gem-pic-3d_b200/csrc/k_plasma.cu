@@ -128,15 +128,17 @@ __device__ __forceinline__ void sgather_mid(const StreamArgs& c, double x, doubl
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
-// TSC deposit of f (v, 1) at (x, y) into jsr: jx, jy, jz and the charge of negative (plane 3) or positive
-// (plane 4) particles (stream_deposit, sim_stream.hpp:33-47, Fourier y). F32: into the FP32 planes.
+// TSC deposit of f v at (x, y) into jsr: jx, jy, jz (stream_deposit, sim_stream.hpp:33-64). The reference also
+// deposits the charge of negative and positive particles into planes 3 and 4; those feed only its density
+// diagnostics (rho_lines, openPMD n_e / n_i), which this build does not write, so they are left out. F32: into the
+// FP32 planes.
 template <bool F32>
 __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
     const Geo& g = c.g;
     int ix_[3], jn[3]; double wx[3], wn[3];
     tsc_periodic(x, g.dx, g.nx, ix_, wx);
-    const long nk = g.nk, cq = (f < 0 ? 3 : 4) * nk;
-    if (!g.yf) {                       // free-hand y: j_x, j_z and the charges on the nodes, j_y on the half-nodes
+    const long nk = g.nk;
+    if (!g.yf) {                       // free-hand y: j_x, j_z on the nodes, j_y on the half-nodes
         int jh[3]; double wh[3];
         tsc_y(g.yax, y, jn, wn, jh, wh);
         for (int v = 0; v < 3; ++v) {
@@ -146,9 +148,9 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
                     const long k = long(jn[v]) * g.nx + ix_[u];
                     const double w = f * wx[u] * wn[v] * g.iA[jn[v]];
                     if constexpr (F32) {
-                        atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[2 * nk + k], float(w * vz)); atomicAdd(&c.Jf[cq + k], float(w));
+                        atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[2 * nk + k], float(w * vz));
                     } else {
-                        atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[2 * nk + k], w * vz); atomicAdd(&c.J[cq + k], w);
+                        atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[2 * nk + k], w * vz);
                     }
                 }
                 if (hal) {
@@ -171,10 +173,9 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
             const double w = f * wx[u] * wn[v] * ia0;
             if constexpr (F32) {
                 atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[nk + k], float(w * vy));
-                atomicAdd(&c.Jf[2 * nk + k], float(w * vz)); atomicAdd(&c.Jf[cq + k], float(w));
+                atomicAdd(&c.Jf[2 * nk + k], float(w * vz));
             } else {
                 atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
-                atomicAdd(&c.J[cq + k], w);
             }
         }
 }
@@ -366,8 +367,8 @@ static void stream_launch(Ctx& c, const StreamArgs& a, unsigned blocks) {
 // ---------------------------------------------------------------- spectra of the streaming current
 // rows: per row, FFT along x of jx + i jy (split) and of jz -> three half rows in T0..T2
 template <int NX, class JT>
-__global__ void __launch_bounds__(128) k_ss_rows(Geo g, const JT* __restrict__ J, cpx* __restrict__ T0, cpx* __restrict__ T1,
-                                                cpx* __restrict__ T2) {
+__global__ void __launch_bounds__(128) k_ss_rows(Geo g, JT* __restrict__ J, cpx* __restrict__ T0, cpx* __restrict__ T1,
+                                                cpx* __restrict__ T2, int clear, int* __restrict__ bcnt) {
     using S = FftShape<NX>;
     constexpr int LPC = 128 / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -378,10 +379,15 @@ __global__ void __launch_bounds__(128) k_ss_rows(Geo g, const JT* __restrict__ J
     for (int e = tid; e < LPC * NX; e += 128) {
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         double jx = 0, jy = 0, jz = 0;
-        if (row < g.ny) { const long i = long(row) * NX + p; jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i]; }
+        if (row < g.ny) {
+            const long i = long(row) * NX + p;
+            jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i];
+            if (clear) { J[i] = JT(0); J[nk + i] = JT(0); J[2 * nk + i] = JT(0); }     // for the next pass's deposit
+        }
         a0[rr * RS + p + (p >> 3)] = C(jx, jy);
         a1[rr * RS + p + (p >> 3)] = C(jz, 0.0);
     }
+    if (bcnt && blockIdx.x == 0 && tid == 0) *bcnt = 0;          // the freed electrons of the next pass
     __syncthreads();
     const int r = tid / S::T, t = tid - r * S::T;
     {
@@ -488,19 +494,21 @@ __global__ void k_replace_pred(PlasmaPtrs p, int n, int extrap, double w) {
 }
 // half-cell n is final (sim_plasma.cpp:381-403): R at slice n+1 corrected for the prediction it used; the
 // change s0 -> s1 kept for the extrapolation; the current kept as the prediction of the next step
-__global__ void k_correct(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ Ry, int n, double q, int own) {
+__device__ __forceinline__ void correct_mode(const PlasmaPtrs& p, cpx* Rx, cpx* Ry, int n, double q, int own, long i) {
     const long nkh = p.nkh;
     const long hp = long(n + 1) * nkh, sp1 = long(n + 1) * nkh;
     cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
-        const cpx u0 = p.jsn[i], u1 = p.jsn[nkh + i], u2 = p.jsn[2 * nkh + i];
-        if (own) {
-            Rx[sp1 + i] = Rx[sp1 + i] - q * (u0 - p.si0[i]);
-            Ry[sp1 + i] = Ry[sp1 + i] - q * (u1 - p.si0[nkh + i]);
-        }
-        p.dl[i] = u0 - s0[0][hp + i]; p.dl[nkh + i] = u1 - s0[1][hp + i]; p.dl[2 * nkh + i] = u2 - s0[2][hp + i];
-        s0[0][hp + i] = u0; s0[1][hp + i] = u1; s0[2][hp + i] = u2;
+    const cpx u0 = p.jsn[i], u1 = p.jsn[nkh + i], u2 = p.jsn[2 * nkh + i];
+    if (own) {
+        Rx[sp1 + i] = Rx[sp1 + i] - q * (u0 - p.si0[i]);
+        Ry[sp1 + i] = Ry[sp1 + i] - q * (u1 - p.si0[nkh + i]);
     }
+    p.dl[i] = u0 - s0[0][hp + i]; p.dl[nkh + i] = u1 - s0[1][hp + i]; p.dl[2 * nkh + i] = u2 - s0[2][hp + i];
+    s0[0][hp + i] = u0; s0[1][hp + i] = u1; s0[2][hp + i] = u2;
+}
+__global__ void k_correct(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ Ry, int n, double q, int own) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x)
+        correct_mode(p, Rx, Ry, n, q, own, i);
 }
 // the march of slice n, one mode (march_point, sim_kernels.hpp:173-210, one rank: b = N, no boundary slice). The
 // current pointers carry no __restrict__: the fused kernel below writes jk just before.
@@ -553,7 +561,7 @@ template <class T>
 __global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry,
                                                       T* __restrict__ Ez, T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
                                                       const T* __restrict__ j0x, const T* __restrict__ j0y, double D, int n,
-                                                      int extrap, double w) {
+                                                      int extrap, double w, const cpx* __restrict__ bk) {
     const long nk = g.nkh;
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nk) return;
@@ -575,7 +583,9 @@ __global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx*
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
     const long o = long(n - g.a) * nk + i, ou = o + nk;
     const cpx j0xd = widen(j0x[o]), j0xu = widen(j0x[ou]), j0yd = widen(j0y[o]), j0yu = widen(j0y[ou]);
-    const cpx rx = Rx[o], ry = Ry[o], ez = widen(Ez[o]), bz = widen(Bz[o]);
+    // level s0 of slice n: as in the arrays on the first pass, else from the backup the slice prologue took
+    const cpx rx = bk ? bk[i] : Rx[o], ry = bk ? bk[nk + i] : Ry[o];
+    const cpx ez = bk ? widen(narrow<T>(bk[2 * nk + i])) : widen(Ez[o]), bz = bk ? widen(narrow<T>(bk[3 * nk + i])) : widen(Bz[o]);
     const bool front = n == g.N - 1;
     cpx pRx = C(0), pRy = C(0), pEz = C(0), pBz = C(0), pLx = C(0), pLy = C(0);
     if (!front) {
@@ -645,60 +655,52 @@ __global__ void k_count_add(long* __restrict__ nstrm_dev, const int* __restrict_
 // pred_m starts from its level s0 with the prediction buffer cleared: jk(pred_m) += js0(pred_m), pin <- js0(pred_m)
 // (pred_m < 0: none); the slice's R_x, R_y, E_z, B_z saved for the passes (backup).
 template <class T>
-__global__ void k_slice_prologue(PlasmaPtrs p, cpx* __restrict__ sin_, cpx* __restrict__ si0, cpx* __restrict__ bk,
-                                 const cpx* __restrict__ Rx, const cpx* __restrict__ Ry, const T* __restrict__ Ez,
-                                 const T* __restrict__ Bz, long o, int pred_m, int copy_in, int backup) {
+__device__ __forceinline__ void slice_prologue_mode(const PlasmaPtrs& p, cpx* sin_, cpx* si0, cpx* bk, const cpx* Rx, const cpx* Ry,
+                                                    const T* Ez, const T* Bz, long o, int pred_m, int copy_in, int backup, long i) {
     const long nkh = p.nkh;
     const long hm = long(pred_m + 1) * nkh;
     T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
     const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const long q = k * nkh + i;
-            if (copy_in) { const cpx v = p.pin[q]; sin_[q] = v; si0[q] = v; }
-            if (pred_m >= 0) {
-                const cpx t = s0[k][hm + i];
-                jk[k][hm + i] = narrow<T>(widen(jk[k][hm + i]) + t);
-                p.pin[q] = t;
-            }
-        }
-        if (backup) {
-            bk[i] = Rx[o + i]; bk[nkh + i] = Ry[o + i];
-            bk[2 * nkh + i] = widen(Ez[o + i]); bk[3 * nkh + i] = widen(Bz[o + i]);
+    for (int k = 0; k < 3; ++k) {
+        const long q = k * nkh + i;
+        if (copy_in) { const cpx v = p.pin[q]; sin_[q] = v; si0[q] = v; }
+        if (pred_m >= 0) {
+            const cpx t = s0[k][hm + i];
+            jk[k][hm + i] = narrow<T>(widen(jk[k][hm + i]) + t);
+            p.pin[q] = t;
         }
     }
-}
-// The six fields half-way between slices n and n+1 (F planes l, l+1) at point k, interleaved: FP32 (the mixed
-// form: 8 floats, the last two unused) or FP64 (6 doubles).
-struct FmidArgs {
-    const float* F;
-    long fpl, l0, nk;
-    void* out;                 // null: not used (free-hand y)
-    int f32;
-};
-__device__ __forceinline__ void fmid_point(const FmidArgs& a, long k) {
-    double v[6];
-#pragma unroll
-    for (int comp = 0; comp < 6; ++comp) {
-        const float* p = a.F + comp * a.fpl + a.l0 + k;
-        v[comp] = 0.5 * (double(p[0]) + double(p[a.nk]));
-    }
-    if (a.f32) {
-        float4* o = reinterpret_cast<float4*>(a.out) + 2 * k;
-        o[0] = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
-        o[1] = make_float4(float(v[4]), float(v[5]), 0.f, 0.f);
-    } else {
-        double2* o = reinterpret_cast<double2*>(a.out) + 3 * k;
-        o[0] = make_double2(v[0], v[1]); o[1] = make_double2(v[2], v[3]); o[2] = make_double2(v[4], v[5]);
+    if (backup) {
+        bk[i] = Rx[o + i]; bk[nkh + i] = Ry[o + i];
+        bk[2 * nkh + i] = widen(Ez[o + i]); bk[3 * nkh + i] = widen(Bz[o + i]);
     }
 }
-// Start of a pass: the slice restored from the backup (restore), the streaming-current planes and the count of
-// freed electrons cleared, the midpoint fields of the half-cell for the streaming gather.
+template <class T>
+__global__ void k_slice_prologue(PlasmaPtrs p, cpx* __restrict__ sin_, cpx* __restrict__ si0, cpx* __restrict__ bk,
+                                 const cpx* __restrict__ Rx, const cpx* __restrict__ Ry, const T* __restrict__ Ez,
+                                 const T* __restrict__ Bz, long o, int pred_m, int copy_in, int backup) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x)
+        slice_prologue_mode<T>(p, sin_, si0, bk, Rx, Ry, Ez, Bz, o, pred_m, copy_in, backup, i);
+}
+// half-cell n final (correct) and the prologue of half-cell n-1, per mode in one thread: the correction reads si0
+// before the prologue refills it, the prologue's slice n-1 is not touched by the correction (slice n+1)
+template <class T>
+__global__ void k_correct_prologue(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ Ry, int n, double q, int own,
+                                   cpx* __restrict__ sin_, cpx* __restrict__ si0, cpx* __restrict__ bk, const T* __restrict__ Ez,
+                                   const T* __restrict__ Bz, long o_next, int pred_m, int backup) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x) {
+        correct_mode(p, Rx, Ry, n, q, own, i);
+        slice_prologue_mode<T>(p, sin_, si0, bk, Rx, Ry, Ez, Bz, o_next, pred_m, 1, backup, i);
+    }
+}
+// Start of a pass on the free-hand y grid: the slice restored from the backup (restore), the streaming-current
+// planes and the count of freed electrons cleared. (Fourier y: the fused march reads the backup, the rows kernel
+// of the spectra clears the planes and the count.)
 template <class T, class JT>
 __global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
                                 T* __restrict__ Bz, long o, long nkh, JT* __restrict__ J, long nj, int* __restrict__ bcnt,
-                                int restore, FmidArgs fm) {
+                                int restore) {
     const long t0 = long(blockIdx.x) * blockDim.x + threadIdx.x, st = long(gridDim.x) * blockDim.x;
     if (restore)
         for (long i = t0; i < nkh; i += st) {
@@ -706,8 +708,6 @@ __global__ void k_pass_prologue(const cpx* __restrict__ bk, cpx* __restrict__ Rx
             Ez[o + i] = narrow<T>(bk[2 * nkh + i]); Bz[o + i] = narrow<T>(bk[3 * nkh + i]);
         }
     for (long i = t0; i < nj; i += st) J[i] = JT(0);
-    if (fm.out)
-        for (long k = t0; k < fm.nk; k += st) fmid_point(fm, k);
     if (t0 == 0) *bcnt = 0;
 }
 
@@ -739,12 +739,12 @@ void launch_stream(Ctx& c, const StreamArgs& a) {
 }
 // Half spectra of three real planes J[0..2] (jx, jy, jz layout) into out[0..2]; T is scratch (3 half planes).
 template <int NX, class JT>
-static void ss_rows(Ctx& c, const JT* J, cpx* T) {
+static void ss_rows(Ctx& c, JT* J, cpx* T, int clear = 0, int* bcnt = nullptr) {
     using S = FftShape<NX>;
     constexpr int LPC = 128 / S::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
     smem_attr(reinterpret_cast<const void*>(k_ss_rows<NX, JT>), smem);
-    k_ss_rows<NX, JT><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh);
+    k_ss_rows<NX, JT><<<unsigned((c.ny + LPC - 1) / LPC), 128, smem, c.stream>>>(c.geo(), J, T, T + c.nkh, T + 2 * c.nkh, clear, bcnt);
     c.check_launch("k_ss_rows");
 }
 template <int NY>
@@ -761,9 +761,9 @@ void launch_stream_spectra(Ctx& c) {
     PlasmaState& P = *c.pl;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
     if (c.f32s) {
-        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float>(c, P.jsrf.p, P.tsp.p)));
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float>(c, P.jsrf.p, P.tsp.p, 1, P.bcnt.p)));
     } else {
-        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p)));
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p, 1, P.bcnt.p)));
     }
     if (!c.yf) launch_ss_lines_fh(c, P.tsp.p, P.jsn.p, a2);           // free-hand y: filters along the y lines
     else G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, P.tsp.p, P.jsn.p, a2, P.box_mean ? 1 : 0, 1));
@@ -772,8 +772,9 @@ void launch_stream_spectra(Ctx& c) {
 // plain transverse spectra (no filters) of three real planes: the grid-laser profile (free-hand y: the x spectra
 // of the rows alone)
 void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
-    if (!c.yf) { G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J3, out3))); return; }
-    G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J3, T3)));
+    double* J = const_cast<double*>(J3);      // read only: the rows kernel clears nothing here
+    if (!c.yf) { G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J, out3))); return; }
+    G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J, T3)));
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
 }
 
@@ -802,19 +803,17 @@ void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup) {
 }
 void launch_pass_prologue(Ctx& c, int n, int restore) {
     PlasmaState& P = *c.pl;
-    const long o = long(n - c.a) * c.nkh, nj = 5 * long(c.nk);
-    FmidArgs fm{c.F.p, long(c.ns + 2) * c.nk, long(n - c.a) * c.nk, c.nk, c.yf ? static_cast<void*>(P.fmid.p) : nullptr,
-                c.f32s ? 1 : 0};
+    const long o = long(n - c.a) * c.nkh, nj = 3 * long(c.nk);
     const int tok = c.prof_begin("pass_prologue");
     if (c.mixed)
         k_pass_prologue<cpxf, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.mx.Ez.p, c.mx.Bz.p, o, c.nkh,
-                                                                          P.jsrf.p, nj, P.bcnt.p, restore, fm);
+                                                                          P.jsrf.p, nj, P.bcnt.p, restore);
     else if (c.f32s)                  // free-hand y, mixed: FP64 spectra, FP32 streaming planes
         k_pass_prologue<cpx, float><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
-                                                                         P.jsrf.p, nj, P.bcnt.p, restore, fm);
+                                                                         P.jsrf.p, nj, P.bcnt.p, restore);
     else
         k_pass_prologue<cpx, double><<<ew_blocks(nj), 256, 0, c.stream>>>(P.bk.p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, o, c.nkh,
-                                                                          P.jsr.p, nj, P.bcnt.p, restore, fm);
+                                                                          P.jsr.p, nj, P.bcnt.p, restore);
     c.check_launch("k_pass_prologue");
     c.prof_end(tok);
 }
@@ -837,6 +836,20 @@ void launch_correct(Ctx& c, int n, double q, int own) {
     k_correct<<<ew_blocks(c.nkh), 256, 0, c.stream>>>(c.pl->ptrs(c), c.Rx.p, c.Ry.p, n, q, own);
     c.check_launch("k_correct");
 }
+// correct(n) and slice_prologue(n - 1, pred_m, copy_in = 1, backup) in one launch
+void launch_correct_prologue(Ctx& c, int n, double q, int own, int pred_m, int backup) {
+    PlasmaState& P = *c.pl;
+    const long o = long(n - 1 - c.a) * c.nkh;
+    const int tok = c.prof_begin("correct_prologue");
+    if (c.mixed)
+        k_correct_prologue<cpxf><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(P.ptrs(c), c.Rx.p, c.Ry.p, n, q, own, P.jsin.p, P.jsi0.p, P.bk.p,
+                                                                         c.mx.Ez.p, c.mx.Bz.p, o, pred_m, backup);
+    else
+        k_correct_prologue<cpx><<<ew_blocks(c.nkh), 256, 0, c.stream>>>(P.ptrs(c), c.Rx.p, c.Ry.p, n, q, own, P.jsin.p, P.jsi0.p, P.bk.p,
+                                                                        c.Ez.p, c.Bz.p, o, pred_m, backup);
+    c.check_launch("k_correct_prologue");
+    c.prof_end(tok);
+}
 void launch_march_slice(Ctx& c, double D, int n) {
     if (!c.yf) { launch_march_slice_fh(c, D, n); return; }
     const int tok = c.prof_begin("march_slice");
@@ -852,17 +865,18 @@ void launch_march_slice(Ctx& c, double D, int n) {
     c.check_launch("k_march_slice");
     c.prof_end(tok);
 }
-void launch_replace_march(Ctx& c, double D, int n, int extrap, double w) {
+void launch_replace_march(Ctx& c, double D, int n, int extrap, double w, int restore) {
     const int tok = c.prof_begin("replace_march");
     const unsigned blocks = unsigned((c.nkh + 127) / 128);
     const PlasmaPtrs pp = c.pl->ptrs(c);
+    const cpx* bk = restore ? c.pl->bk.p : nullptr;
     if (c.mixed) {
         MixedBufs& m = c.mx;
         k_replace_march<cpxf><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
-                                                            D, n, extrap, w);
+                                                            D, n, extrap, w, bk);
     } else {
         k_replace_march<cpx><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
-                                                           D, n, extrap, w);
+                                                           D, n, extrap, w, bk);
     }
     c.check_launch("k_replace_march");
     c.prof_end(tok);
