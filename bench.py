@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint march check on workload 4")
+    ap.add_argument("--no-error-growth", action="store_true", help="skip the mixed form's error by s-steps")
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
                     help="both: time the FP64 form, then the mixed form (the headline) and its error against FP64")
     ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
@@ -491,6 +492,8 @@ def run_g3d(a):
             line["streaming"] = H["streaming"]
         if world == 1 and not a.no_adjoint:
             line["adjoint"] = adjoint_check()
+        if world == 1 and mixed and "fp64" in res and not a.no_error_growth:
+            line["mixed_error_growth"] = error_growth(cfg)
         if "fp64" in res and mixed:
             F64 = res["fp64"]
             line["fp64_form"] = {"value": F64["value"], "ms_per_step": F64["ms"] / a.steps, "dtype": "f64",
@@ -501,6 +504,37 @@ def run_g3d(a):
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def error_growth(cfg, checkpoints=(1, 2, 4, 8)):
+    """The mixed form's distance from the FP64 form after 1, 2, 4, 8 s-steps from the same start, and the distance
+    between two FP64 runs (their deposits add in a different order) after the last: a laser-driven plasma is
+    chaotic, so a difference at rounding level grows from step to step in either form."""
+    import numpy as np
+    import g3d
+    sims = {k: g3d.Simulation(cfg, precision=("mixed" if k == "mixed" else "fp64")) for k in ("fp64", "fp64_rerun", "mixed")}
+    for sm in sims.values():
+        sm.init()
+    rl = lambda x, y: float(np.linalg.norm((x.astype(np.float64) - y).ravel()) / np.linalg.norm(y.astype(np.float64).ravel()))
+    out = {"F_mixed_vs_fp64": {}, "<p_z>_mixed_vs_fp64": {}}
+    done = 0
+    for k in checkpoints:
+        for _ in range(k - done):
+            for sm in sims.values():
+                sm.step()
+        done = k
+        F0 = sims["fp64"].array("F")
+        d0 = sims["fp64"].diagnostics_sums()
+        out["F_mixed_vs_fp64"][k] = rl(sims["mixed"].array("F"), F0)
+        d = sims["mixed"].diagnostics_sums()
+        out["<p_z>_mixed_vs_fp64"][k] = abs(d[9] / d[0] - d0[9] / d0[0]) / abs(d0[9] / d0[0])
+        if k == checkpoints[-1]:
+            out["F_fp64_rerun_vs_fp64"] = {k: rl(sims["fp64_rerun"].array("F"), F0)}
+    for sm in sims.values():
+        sm.close()
+    out["note"] = ("relative L2 of the float F (six components) by s-steps from the same start; the FP64 rerun differs from "
+                   "the FP64 run only in the order of its atomic adds")
+    return out
 
 
 def adjoint_check(eps=1e-6):
