@@ -97,8 +97,8 @@ def algorithmic_bytes(name, cfg, mixed=False, S=0):
     the deposit reads 56 B.
     The per-half-cell kernels of the plasma march work on one slice: nk = nx ny points, nkh = ny (nx/2 + 1) modes,
     S = streaming particles, each read (80 B) and written (64 B) once per half-cell pass (the per-unit figure of
-    the streaming push), with the two F slices it gathers from (48 B per point) and the deposit planes (5 values
-    per point)."""
+    the streaming push), with the midpoint fields it gathers from (6 doubles or 8 floats per point) and the three
+    deposit planes."""
     ns = cfg.nzeta - 1
     nk = cfg.nx * cfg.ny
     G = ns * nk
@@ -108,16 +108,25 @@ def algorithmic_bytes(name, cfg, mixed=False, S=0):
     nkh = cfg.ny * (cfg.nx // 2 + 1)
     cz = 8 if mixed else 16                          # bytes of a stored spectrum value other than R
     cr = 4 if mixed else 8                           # bytes of a raw current value
+    fm = 32 if mixed else 48                         # bytes of the midpoint fields per point
+    march_slice = (4 * 16 + 10 * cz + 6 * cz) * nkh + (2 * 16 + 4 * cz) * nkh
+    # jsn, sin, js0 (2), dl, pin read; jk (2 half-cells) read and written; sin, pin written (3 components each)
+    replace_pred = (6 * 48 + 2 * 3 * cz) * nkh + (2 * 3 * cz + 2 * 48) * nkh
+    slice_prologue = (48 + 96 + 48 + 2 * 3 * cz + 48 + 32 + 2 * cz + 64) * nkh
+    correct = (48 + 32 + 32 + 48 + 32 + 48 + 48) * nkh  # jsn, si0, R, js0 read; R, dl, js0 written
     plasma = {
-        "stream": 144 * S + 48 * nk + 5 * cr * nk,
-        "stream_spectra": 3 * cr * nk + (2 * 48 + 3 * cz) * nkh,      # three real planes; scratch; jsn (complex128)
-        "march_slice": (4 * 16 + 10 * cz + 6 * cz) * nkh + (2 * 16 + 4 * cz) * nkh,
+        "stream": 144 * S + fm * nk + 3 * cr * nk,
+        # three real planes read and cleared; scratch; jsn (complex128)
+        "stream_spectra": 2 * 3 * cr * nk + (2 * 48 + 3 * cz) * nkh,
+        "march_slice": march_slice,
         "real_cols_slice": (2 * 16 + 4 * cz + 6 * cz) * nkh,
-        "real_rows_slice": 6 * cz * nkh + 24 * nk,
-        # jsn, sin, js0 (2), dl, pin read; jk (2 half-cells) read and written; sin, pin written (3 components each)
-        "replace_pred": (6 * 48 + 2 * 3 * cz) * nkh + (2 * 3 * cz + 2 * 48) * nkh,
-        "slice_prologue": (48 + 96 + 48 + 2 * 3 * cz + 48 + 32 + 2 * cz + 64) * nkh,
-        "pass_prologue": 5 * cr * nk + 64 * nkh,
+        # six column transforms read, F written; the other F plane read and the midpoint fields written
+        "real_rows_slice": 6 * cz * nkh + 24 * nk + (24 + fm) * nk,
+        "replace_pred": replace_pred,
+        "replace_march": replace_pred + march_slice,
+        "slice_prologue": slice_prologue,
+        "correct_prologue": correct + slice_prologue,
+        "pass_prologue": 3 * cr * nk + 64 * nkh,
     }
     if name in plasma:
         return plasma[name] if S else None
