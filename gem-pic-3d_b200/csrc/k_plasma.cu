@@ -25,15 +25,17 @@
 namespace g3d {
 
 // ---------------------------------------------------------------- relativistic Boris (sim_stream.hpp:8-18)
-__device__ __forceinline__ void boris(double& ux, double& uy, double& uz, const double E[3], const double B[3], double qm, double dt) {
-    const double qh = 0.5 * qm * dt;
-    const double umx = ux + qh * E[0], umy = uy + qh * E[1], umz = uz + qh * E[2];
-    const double qg = qh / sqrt(1.0 + umx * umx + umy * umy + umz * umz);     // q dt / (2 m gamma-)
-    const double tx = qg * B[0], ty = qg * B[1], tz = qg * B[2];
-    const double t2 = tx * tx + ty * ty + tz * tz;
-    const double upx = umx + (umy * tz - umz * ty), upy = umy + (umz * tx - umx * tz), upz = umz + (umx * ty - umy * tx);
-    const double sf = 2.0 / (1.0 + t2);
-    const double vx = umx + sf * (upy * tz - upz * ty), vy = umy + sf * (upz * tx - upx * tz), vz = umz + sf * (upx * ty - upy * tx);
+// A: the arithmetic type of the push (double; float in the mixed form's streaming push)
+template <class A>
+__device__ __forceinline__ void boris(A& ux, A& uy, A& uz, const A E[3], const A B[3], A qm, A dt) {
+    const A qh = A(0.5) * qm * dt;
+    const A umx = ux + qh * E[0], umy = uy + qh * E[1], umz = uz + qh * E[2];
+    const A qg = qh / sqrt(A(1) + umx * umx + umy * umy + umz * umz);     // q dt / (2 m gamma-)
+    const A tx = qg * B[0], ty = qg * B[1], tz = qg * B[2];
+    const A t2 = tx * tx + ty * ty + tz * tz;
+    const A upx = umx + (umy * tz - umz * ty), upy = umy + (umz * tx - umx * tz), upz = umz + (umx * ty - umy * tx);
+    const A sf = A(2) / (A(1) + t2);
+    const A vx = umx + sf * (upy * tz - upz * ty), vy = umy + sf * (upz * tx - upx * tz), vz = umz + sf * (upx * ty - upy * tx);
     ux = vx + qh * E[0]; uy = vy + qh * E[1]; uz = vz + qh * E[2];
 }
 
@@ -272,66 +274,71 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         }
         return d;
     }
-    const double x = S.x[i], y = S.y[i], z = S.z[i], px = S.px[i], py = S.py[i], pz = S.pz[i], qm = S.qm[i];
-    const double g0 = sqrt(1 + px * px + py * py + pz * pz), ig0 = 1 / g0;
-    const double omv0 = (1 + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
-    const double dt0 = hl / omv0;
-    const double hd = 0.5 * dt0 * ig0;
-    const double xm = x + hd * px, ym = y + hd * py;
-    const double zm = z + hd * pz, zetam = zeta - 0.5 * hl;
-    double E[3], B[3], Ee[3], Be[3];
-    if (c.Fmid && zeta == zn1) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), E, B);   // the whole half-cell
-    else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, E, B);
+    // the push in A (FP32 in the mixed form: the gathered fields are FP32 already; the positions, z and zeta stay
+    // FP64 and take FP32 displacements, the momenta are kept in FP64 between half-cells)
+    typedef typename std::conditional<F32, float, double>::type A;
+    const double x = S.x[i], y = S.y[i], z = S.z[i];
+    const A px = A(S.px[i]), py = A(S.py[i]), pz = A(S.pz[i]), qm = A(S.qm[i]);
+    const A g0 = sqrt(A(1) + px * px + py * py + pz * pz), ig0 = A(1) / g0;
+    const A omv0 = (A(1) + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
+    const A dt0 = A(hl) / omv0;
+    const A hd = A(0.5) * dt0 * ig0;
+    const double xm = x + double(hd * px), ym = y + double(hd * py);
+    const double zm = z + double(hd * pz), zetam = zeta - 0.5 * hl;
+    double Ed[3], Bd[3], Ee[3], Be[3];
+    if (c.Fmid && zeta == zn1) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), Ed, Bd);   // the whole half-cell
+    else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, Ed, Bd);
     if constexpr (LASER) {
         c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
-        for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+        for (int k = 0; k < 3; ++k) { Ed[k] += Ee[k]; Bd[k] += Be[k]; }
     }
-    double ux = px, uy = py, uz = pz;
-    boris(ux, uy, uz, E, B, qm, dt0);
-    double g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
-    double dt = 2 * hl / (omv0 + (1 + ux * ux + uy * uy) / (g1 * (g1 + uz)));
+    const A E[3] = {A(Ed[0]), A(Ed[1]), A(Ed[2])}, B[3] = {A(Bd[0]), A(Bd[1]), A(Bd[2])};
+    A ux = px, uy = py, uz = pz;
+    boris<A>(ux, uy, uz, E, B, qm, dt0);
+    A g1 = sqrt(A(1) + ux * ux + uy * uy + uz * uz);
+    A dt = A(2) * A(hl) / (omv0 + (A(1) + ux * ux + uy * uy) / (g1 * (g1 + uz)));
     ux = px; uy = py; uz = pz;
-    boris(ux, uy, uz, E, B, qm, dt);
-    g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
-    double ig1 = 1 / g1;
-    double vx = 0.5 * (px * ig0 + ux * ig1), vy = 0.5 * (py * ig0 + uy * ig1), vz = 0.5 * (pz * ig0 + uz * ig1);
+    boris<A>(ux, uy, uz, E, B, qm, dt);
+    g1 = sqrt(A(1) + ux * ux + uy * uy + uz * uz);
+    A ig1 = A(1) / g1;
+    A vx = A(0.5) * (px * ig0 + ux * ig1), vy = A(0.5) * (py * ig0 + uy * ig1), vz = A(0.5) * (pz * ig0 + uz * ig1);
     double zeta_end = zn;
     bool trapped = false;
     const double sTrap = c.sv->sTrap;
-    if (z + vz * dt >= sTrap) {       // advanced trap_advance steps inside this half-cell: trapped
-        const double vv = vz > 1e-3 ? vz : 1e-3;
+    if (z + double(vz * dt) >= sTrap) {       // advanced trap_advance steps inside this half-cell: trapped
+        const double vv = double(vz) > 1e-3 ? double(vz) : 1e-3;
         const double dtp = (sTrap - z) / vv > 0 ? (sTrap - z) / vv : 0.0;
         ux = px; uy = py; uz = pz;
-        boris(ux, uy, uz, E, B, qm, dtp);
-        g1 = sqrt(1 + ux * ux + uy * uy + uz * uz);
-        ig1 = 1 / g1;
-        vx = 0.5 * (px * ig0 + ux * ig1); vy = 0.5 * (py * ig0 + uy * ig1); vz = 0.5 * (pz * ig0 + uz * ig1);
-        dt = dtp;
-        zeta_end = zeta - (1 - vz) * dtp;
+        boris<A>(ux, uy, uz, E, B, qm, A(dtp));
+        g1 = sqrt(A(1) + ux * ux + uy * uy + uz * uz);
+        ig1 = A(1) / g1;
+        vx = A(0.5) * (px * ig0 + ux * ig1); vy = A(0.5) * (py * ig0 + uy * ig1); vz = A(0.5) * (pz * ig0 + uz * ig1);
+        dt = A(dtp);
+        zeta_end = zeta - (1 - double(vz)) * dtp;
         trapped = true;
     }
-    const double xn = x + vx * dt, yn = y + vy * dt;
+    const double xn = x + double(vx * dt), yn = y + double(vy * dt);
     if (!c.dry) {
         S.x[i] = xn; S.y[i] = yn;
-        S.z[i] = trapped ? c.sv->s1 : z + vz * dt;
+        S.z[i] = trapped ? c.sv->s1 : z + double(vz * dt);
         S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
         S.zeta[i] = zeta_end;
     }
     const double q = S.q[i], w = S.w[i];
-    const double f = q * w * dt / (c.Delta * h * g.dx);
-    if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, vx, vy, vz, true};
+    const double f = q * w * double(dt) / (c.Delta * h * g.dx);
+    if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true};
     if (!g.yf && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
         if (!c.dry) S.alive[i] = 0;
         return d;
     }
     if constexpr (ION)
         if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
-            ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), dt);
+            ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), double(dt));
     if (trapped) {
         if (!c.dry) S.alive[i] = 5;
-        const double vze = uz * ig1;
+        const double vze = double(uz * ig1);
         if (vze >= c.vz_beam)         // joins the beam list: its beam current of level s1 from now on
-            sdeposit<F32>(c, xn, yn, q * w / (h * g.dx * vze), ux * ig1, uy * ig1, vze);
+            sdeposit<F32>(c, xn, yn, q * w / (h * g.dx * vze), double(ux * ig1), double(uy * ig1), vze);
     }
     return d;
 }
@@ -339,8 +346,8 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
 // One thread per streaming particle, a fixed grid striding over their count (which freed electrons raise; it is
 // read on the device). The deposit adds go straight to global memory: without a use of the old value they are
 // fire-and-forget reductions in L2, cheaper for the SM than accumulating in shared memory the many adds that
-// neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers in FP32 arithmetic
-// and the deposit into FP32 planes; the particle state and the Boris pushes stay FP64.
+// neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers, the Boris pushes and
+// the velocities in FP32 arithmetic, the deposit into FP32 planes; the particle state stays FP64.
 constexpr int ST_NT = 128;
 #ifndef G3D_STREAM_MINB
 #define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
