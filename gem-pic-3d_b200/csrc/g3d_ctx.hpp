@@ -147,6 +147,7 @@ struct Ctx {
     DevBuf<cpx> lmode;                           // laser mode coefficients per stored mode (ny x H), or empty
     DevBuf<cpx> lspx, lspy;                      // the grid-laser spectra added at init before the coefficients
     DevBuf<unsigned char> adjws;                 // workspace of the adjoint march, kept between calls
+    bool adj_after_start = false;                // dJ/dp with the start field held (G3D_ADJ_AFTER_START)
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
@@ -278,12 +279,17 @@ void smem_attr(const void* kern, size_t smem);
 void launch_adj_objective(Ctx& c, double* dev_out2);
 void launch_adj_seed(Ctx& c, double W, double* lam);
 void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const* lS);
-void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D);
+void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D, int accz = 0);
 void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ);
 void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const double* lJ, double* lam);
 void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
                      double* lam, double* lF, int* err);
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out);
+void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta,
+                         cpx* psi, double* cpf, double* cpt, cpx* dpt);
+void launch_adj_wsum(Ctx& c, const int32_t* alive, double* out);
+void launch_adj_beta(Ctx& c, const double* X, const int32_t* alive, double coef, double* lam);
+void launch_adj_widen(Ctx& c, const cpxf* a, cpx* b, long n);
 std::vector<g3d_particle> get_streaming(Ctx& c);
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)

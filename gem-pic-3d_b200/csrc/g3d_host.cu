@@ -865,11 +865,18 @@ static void set_exact_fields(Ctx& c, bool on) {
     else c.Fd.release();
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
+// What dJ/dp of the adjoint holds: through the start field (false) or with the start field held (true).
+static void set_adjoint_momenta(Ctx& c, int mode) {
+    if (mode != G3D_ADJ_THROUGH_START && mode != G3D_ADJ_AFTER_START) throw Error(G3D_ERR_ARG, "unknown adjoint momentum mode");
+    c.adj_after_start = mode == G3D_ADJ_AFTER_START;
+}
 // From the start field (right after g3d_init): K s-steps forward with a checkpoint of the beam (x, y, zeta,
 // p, alive) and of the real fields at every level, J = mean p_z of the live beam, then the reverse sweep
-// (k_adjoint.cu): per step the transposed real fields, march, currents, deposit and push. Out: J, dJ/da per
-// stored laser mode [j][k_x] (complex, interleaved) and dJ/dp of every particle at s = 0 [np][3], the start
-// field held fixed (its laser part is differentiated through init's march(0)). The forward leaves the run at
+// (k_adjoint.cu): per step the transposed real fields, march, currents, deposit and push; then init's march(0),
+// relaxation marches and co-moving fields back to the start currents and beta. Out: J, dJ/da per stored laser
+// mode [j][k_x] (complex, interleaved) and dJ/dp of every particle at s = 0 [np][3] through both the s-steps and
+// the start field the bunch made (its currents, its beta), or (G3D_ADJ_AFTER_START) through the s-steps alone, the
+// momenta then being those the start field was made with held apart from it. The forward leaves the run at
 // s = K dz, as K calls of g3d_step; g3d_set_particles + g3d_init start the next evaluation on the same context,
 // which reuses the workspace.
 static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p) {
@@ -899,6 +906,9 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     for (auto& o : oW) o = carve((ns + 1) * nkh * sizeof(cpx));
     const size_t olF = carve(Fn * 8), oV = carve(3 * (ns + 1) * nk * 8), olJ = carve(3 * (ns + 3) * nk * 8);
     const size_t olam = carve(6 * size_t(np) * 8), oerr = carve(sizeof(int)), ojo = carve(2 * 8), ogm = carve(nkh * sizeof(cpx));
+    // the start field's dependence on the bunch: j_z of the start currents, dJ/dR of the relaxation's beta part,
+    // dJ/dbeta per mode
+    const size_t ojz = carve((ns + 1) * nkh * sizeof(cpx)), odx = carve(2 * ns * nkh * sizeof(cpx)), odb = carve(nkh * 8);
     if (c.adjws.n < need) c.adjws.alloc(need, st);
     unsigned char* ws = c.adjws.p;
     double* X = reinterpret_cast<double*>(ws + oX);
@@ -916,6 +926,13 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     int* err = reinterpret_cast<int*>(ws + oerr);
     double* jo = reinterpret_cast<double*>(ws + ojo);
     cpx* gmd = reinterpret_cast<cpx*>(ws + ogm);
+    cpx* jz0 = reinterpret_cast<cpx*>(ws + ojz);
+    cpx* ldx = reinterpret_cast<cpx*>(ws + odx);
+    double* dbm = reinterpret_cast<double*>(ws + odb);
+    // the start currents' j_z (init deposited them; jkz is not swapped into j0)
+    if (c.mixed) launch_adj_widen(c, c.mx.jkz.p, jz0, long((ns + 1) * nkh));
+    else G3D_CUDA(cudaMemcpyAsync(jz0, c.jkz.p, (ns + 1) * nkh * sizeof(cpx), cudaMemcpyDeviceToDevice, st));
+    const double beta0 = c.beta_b, gm20 = c.gm2_b;
     std::vector<double> sl(size_t(K + 1));
     auto save = [&](int k) {
         double* x = X + size_t(k) * 6 * size_t(np);
@@ -963,6 +980,40 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         launch_adj_lmodes(c, lS[0], lS[1], gmd);
         G3D_CUDA(cudaMemcpyAsync(grad_modes, gmd, nkh * sizeof(cpx), cudaMemcpyDeviceToHost, st));
         G3D_CUDA(cudaStreamSynchronize(st));
+    }
+    if (grad_p && np > 0 && !c.adj_after_start) {
+        // dJ/dR before the lasers is dJ/dR of the start field R_co(beta) + (relaxed R_co(1) - R_co(1)): through the
+        // three relaxation marches (D = 100 dz; their E_z, B_z, j0 are zeroed and their E_z, B_z, L outputs unread)
+        // and the two co-moving fields, to the start currents' j_z and to beta
+        const size_t pn = ns * nkh;
+        cpx* psi = W[3]; cpx* dpt = W[4];
+        double* cpf = V; double* cpt = lF;
+        if (c.P.start_relax) {
+            for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemcpyAsync(ldx + q * pn, lS[q], pn * sizeof(cpx), cudaMemcpyDeviceToDevice, st));
+            for (int it = 0; it < 3; ++it) {
+                for (int q = 2; q < 6; ++q) G3D_CUDA(cudaMemsetAsync(lS[q], 0, pn * sizeof(cpx), st));
+                for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemsetAsync(lj0[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
+                launch_adj_march(c, lS, lj0, ljk, 100 * c.P.dz, 1);
+            }
+            // dJ/dR_co(1) = (through the marches) - dJ/dR_co(beta)
+            for (int q = 0; q < 2; ++q) launch_axpy_c(c, lS[q], ldx + q * pn, -1.0, pn);
+            launch_adj_comoving(c, lS[0], lS[1], jz0, 1.0, 0.0, ljk[2], nullptr, psi, cpf, cpt, dpt);
+            launch_adj_comoving(c, ldx, ldx + pn, jz0, beta0, gm20, ljk[2], dbm, psi, cpf, cpt, dpt);
+        } else {
+            launch_adj_comoving(c, lS[0], lS[1], jz0, beta0, gm20, ljk[2], dbm, psi, cpf, cpt, dpt);
+        }
+        // the start currents (deposit of the bunch at s = 0) and beta = sum w p_z / gamma / sum w
+        launch_adj_currents(c, ljk, W, V, lJ);
+        launch_adj_deposit(c, X, AL, lJ, lam);
+        std::vector<double> db(nkh);
+        G3D_CUDA(cudaMemcpyAsync(db.data(), dbm, nkh * 8, cudaMemcpyDeviceToHost, st));
+        launch_adj_wsum(c, AL, jo);
+        double W0 = 0;
+        G3D_CUDA(cudaMemcpyAsync(&W0, jo, 8, cudaMemcpyDeviceToHost, st));
+        G3D_CUDA(cudaStreamSynchronize(st));
+        double dbeta = 0;
+        for (double v : db) dbeta += v;
+        if (W0 > 0) launch_adj_beta(c, X, AL, dbeta / W0, lam);
     }
     if (grad_p && np > 0) {
         std::vector<double> h(3 * size_t(np));
@@ -1233,6 +1284,7 @@ int64_t g3d_launch_count(const g3d_ctx* ctx) { return ctx ? ctx->c.launches : 0;
 
 int g3d_set_laser_modes(g3d_ctx* ctx, const double* coef) { return guarded(ctx, [&] { g3d::set_laser_modes(ctx->c, coef); }); }
 int g3d_set_exact_fields(g3d_ctx* ctx, int32_t on) { return guarded(ctx, [&] { g3d::set_exact_fields(ctx->c, on != 0); }); }
+int g3d_set_adjoint_momenta(g3d_ctx* ctx, int32_t mode) { return guarded(ctx, [&] { g3d::set_adjoint_momenta(ctx->c, mode); }); }
 int g3d_adjoint(g3d_ctx* ctx, int32_t nsteps, double* objective, double* grad_modes, double* grad_p) {
     return guarded(ctx, [&] {
         if (!objective) throw Error(G3D_ERR_ARG, "g3d_adjoint: objective is required");

@@ -165,8 +165,9 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, co
 // slice n-1 passed up through the values of slice n+1 it read) become those of the old level (R, E_z, B_z; the
 // old L is not read by the forward, so lLx, lLy are left to the next transposed real fields, which assign
 // them) and of the currents. The two half-cells of a slice are written once each: the upper one's terms ride
-// in registers to the next slice, where it is the lower one. lj0 and ljk_z are written; ljk_x, ljk_y hold on
-// entry the adjoint of jk as the j0 of the next step and are overwritten with the total. Per
+// in registers to the next slice, where it is the lower one. lj0 is written; ljk_x, ljk_y hold on entry the
+// adjoint of jk as the j0 of the next step and are overwritten with the total; ljk_z is written, or added to
+// (accz: the marches of the start field's relaxation, whose j_z adjoint adds to that of init's march(0)). Per
 // slice each lane streams its 8 values (the 6 adjoints of the new level, the 2 pending ones) and the slice's
 // coefficients DEPTH slices ahead into a shared-memory ring with cp.async, as the forward does.
 namespace {
@@ -185,7 +186,7 @@ template <int BT, int DEPTH>
 __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lEz,
                                                  cpx* __restrict__ lBz, cpx* __restrict__ lLx, cpx* __restrict__ lLy,
                                                  cpx* __restrict__ lj0x, cpx* __restrict__ lj0y, cpx* __restrict__ ljkx,
-                                                 cpx* __restrict__ ljky, cpx* __restrict__ ljkz, double D) {
+                                                 cpx* __restrict__ ljky, cpx* __restrict__ ljkz, double D, int accz) {
     extern __shared__ double ringa[];
     const long nk = g.nkh;
     const int tid = threadIdx.x;
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
             // the lower half-cell (plane n - a): this slice's w_lo terms and the previous slice's upper terms
             j0x[own(o)] = c0x + wl * lJx; j0y[own(o)] = c0y + wl * lJy;
             jkx[own(o)] = pkx + ckx + wl * lJx; jky[own(o)] = pky + cky + wl * lJy;
-            jkz[oth(o)] = sgn * ckz;
+            jkz[oth(o)] = accz ? jkz[oth(o)] + sgn * ckz : sgn * ckz;
         }
         rden = rden_next;
         have_rden = n < g.b - 1;
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
         const long ou = long(g.ns) * nk + ii;
         j0x[own(ou)] = c0x; j0y[own(ou)] = c0y;
         jkx[own(ou)] = jkx[own(ou)] + ckx; jky[own(ou)] = jky[own(ou)] + cky;
-        jkz[oth(ou)] = sgn * ckz;
+        jkz[oth(ou)] = accz ? jkz[oth(ou)] + sgn * ckz : sgn * ckz;
     }
 }
 
@@ -654,6 +655,129 @@ __global__ void k_adj_lmodes(Geo g, const cpx* __restrict__ lRx, const cpx* __re
     out[i] = s;
 }
 
+// ---------------------------------------------------------------- the start field's dependence on the bunch
+// transposed co-moving field (Fourier y; k_comoving of k_march.cu, Simulation::comoving_field,
+// src/sim_fields.cpp:44-151): per mode, R = -(1 + beta) i k psi with A(gm2) psi = rhs along zeta,
+// rhs(l) = (w_lo j_z(l) + w_hi j_z(l+1)) / beta. In: dJ/dR; out: dJ/dj_z added to ljz and, when dbeta is given,
+// dJ/dbeta of the mode (through 1 + beta, 1/beta and gm2 = 1 - beta^2). Scratch per mode and slice: psi, the
+// forward Thomas factor, the transposed solve's factor and right-hand side.
+__global__ void __launch_bounds__(128) k_adj_comoving(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy,
+                                                     const cpx* __restrict__ jz, double beta, double gm2, cpx* __restrict__ ljz,
+                                                     double* __restrict__ dbeta, cpx* __restrict__ psi, double* __restrict__ cpf,
+                                                     double* __restrict__ cpt, cpx* __restrict__ dpt) {
+    const long nk = g.nkh;
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nk) return;
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], ev = ky * ky;
+    const int ns = g.ns;
+    auto coef = [&](int l, double& lo, double& up, double& dg, double& lo1, double& up1, double& dg1) {
+        const int n = g.a + l;
+        const double hm = g.hcg[n + 1], hp = g.hcg[n + 2];
+        lo1 = -2 / ((hm + hp) * hm); up1 = -2 / ((hm + hp) * hp); dg1 = 2 / (hm * hp);   // d/d(gm2)
+        lo = gm2 * lo1; up = gm2 * up1; dg = kx * kx + ev + gm2 * dg1;
+    };
+    auto rhs_at = [&](int l) {
+        const int n = g.a + l;
+        const long o = long(l) * nk + i;
+        return (1 / beta) * (g.wlo[n] * jz[o] + g.whi[n] * jz[o + nk]);
+    };
+    {
+        double lo, up, dg, a1, b1, c1;
+        coef(0, lo, up, dg, a1, b1, c1);
+        if (dg == 0) { if (dbeta) dbeta[i] = 0; return; }       // the forward leaves this mode zero
+    }
+    // forward: psi (as k_comoving)
+    double cprev = 0;
+    cpx dprev = C(0);
+    for (int l = 0; l < ns; ++l) {
+        double lo, up, dg, a1, b1, c1;
+        coef(l, lo, up, dg, a1, b1, c1);
+        const long o = long(l) * nk + i;
+        const double den = dg - lo * cprev;
+        const double cpv = up / den;
+        const cpx dpv = (rhs_at(l) - lo * dprev) / den;
+        cpf[o] = cpv; psi[o] = dpv;
+        cprev = cpv; dprev = dpv;
+    }
+    cpx next = C(0);
+    for (int l = ns - 1; l >= 0; --l) {
+        const long o = long(l) * nk + i;
+        next = psi[o] - cpf[o] * next;
+        psi[o] = next;
+    }
+    // dJ/dpsi = conj(-(1 + beta) i k) dJ/dR = (1 + beta) i k dJ/dR; A^T lrhs = lpsi (sub(l) = up(l-1), sup(l) = lo(l+1))
+    const double opb = 1 + beta;
+    double cpp = 0, upm = 0;
+    cpx dpp = C(0);
+    for (int l = 0; l < ns; ++l) {
+        double lo, up, dg, a1, b1, c1;
+        coef(l, lo, up, dg, a1, b1, c1);
+        double lon = 0;
+        if (l + 1 < ns) { double u2, d2, a2, b2, c2; coef(l + 1, lon, u2, d2, a2, b2, c2); }
+        const long o = long(l) * nk + i;
+        const cpx lpsi = opb * (ik(kx, lRx[o]) + ik(ky, lRy[o]));
+        const double sub = l > 0 ? upm : 0;
+        const double den = dg - sub * cpp;
+        const double c = lon / den;
+        const cpx d = (lpsi - sub * dpp) / den;
+        cpt[o] = c; dpt[o] = d;
+        cpp = c; dpp = d; upm = up;
+    }
+    double t1 = 0, t2 = 0, t3 = 0;
+    cpx lnext = C(0);
+    for (int l = ns - 1; l >= 0; --l) {
+        const int n = g.a + l;
+        const long o = long(l) * nk + i;
+        lnext = dpt[o] - cpt[o] * lnext;                       // dJ/drhs(l)
+        const cpx lr = lnext;
+        ljz[o] = ljz[o] + (g.wlo[n] / beta) * lr;
+        ljz[o + nk] = ljz[o + nk] + (g.whi[n] / beta) * lr;
+        if (dbeta) {
+            const cpx ps = psi[o];
+            const cpx mRx = ik(kx, ps), mRy = ik(ky, ps);      // -dR/dbeta = i k psi
+            t1 -= lRx[o].x * mRx.x + lRx[o].y * mRx.y + lRy[o].x * mRy.x + lRy[o].y * mRy.y;
+            const cpx rh = rhs_at(l);
+            t2 -= (lr.x * rh.x + lr.y * rh.y) / beta;
+            double lo, up, dg, lo1, up1, dg1;
+            coef(l, lo, up, dg, lo1, up1, dg1);
+            const cpx pm = l > 0 ? psi[o - nk] : C(0), pp = l + 1 < ns ? psi[o + nk] : C(0);
+            const cpx ap = lo1 * pm + dg1 * ps + up1 * pp;      // (dA/dgm2) psi, row l
+            t3 -= lr.x * ap.x + lr.y * ap.y;
+        }
+    }
+    if (dbeta) dbeta[i] = t1 + t2 + (-2 * beta) * t3;
+}
+// sum of w over the particles alive at a level (one CTA, fixed order)
+__global__ void __launch_bounds__(1024) k_adj_wsum(PartsDev P, const int32_t* __restrict__ alive, long np, double* __restrict__ out) {
+    __shared__ double s0[1024];
+    double a = 0;
+    for (long i = threadIdx.x; i < np; i += 1024)
+        if (alive[i] == 1) a += P.w[i];
+    s0[threadIdx.x] = a;
+    __syncthreads();
+    for (int s = 512; s > 0; s >>= 1) {
+        if (int(threadIdx.x) < s) s0[threadIdx.x] += s0[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = s0[0];
+}
+// beta = sum w p_z / gamma / sum w over the live bunch: dJ/dp += dJ/dbeta (w / W) d(p_z / gamma)/dp
+__global__ void k_adj_beta(PartsDev P, const double* __restrict__ X, const int32_t* __restrict__ alive, long np, double c,
+                           double* __restrict__ lam) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= np || alive[i] != 1) return;
+    const double px = X[3 * np + i], py = X[4 * np + i], pz = X[5 * np + i];
+    const double g = sqrt(1 + px * px + py * py + pz * pz), ig3 = 1 / (g * g * g), f = c * P.w[i];
+    lam[3 * np + i] += f * (-pz * px * ig3);
+    lam[4 * np + i] += f * (-pz * py * ig3);
+    lam[5 * np + i] += f * ((1 + px * px + py * py) * ig3);
+}
+// complex64 -> complex128 (the start currents of the mixed form for the transposed co-moving field)
+__global__ void k_adj_widen(const cpxf* __restrict__ a, cpx* __restrict__ b, long n) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = to_d(a[i]);
+}
+
 // ---------------------------------------------------------------- launchers
 static unsigned ew_blocks(long n) {
     long b = (n + 255) / 256;
@@ -697,18 +821,18 @@ void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const*
     c.prof_end(tok);
 }
 template <int BT, int DEPTH>
-static void adj_march_launch(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D) {
+static void adj_march_launch(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D, int accz) {
     const unsigned blocks = unsigned((2 * c.nkh + BT - 1) / BT);
     const size_t smem = size_t(DEPTH) * aslot(BT) * sizeof(double);
     allow_smem(k_adj_march<BT, DEPTH>, smem);
     k_adj_march<BT, DEPTH><<<blocks, BT, smem, c.stream>>>(c.geo(), lS[0], lS[1], lS[2], lS[3], lS[4], lS[5], lj0[0], lj0[1], ljk[0],
-                                                           ljk[1], ljk[2], D);
+                                                           ljk[1], ljk[2], D, accz);
 }
 // lS = {Rx, Ry, Ez, Bz, Lx, Ly}; ljk holds the pending adjoints of jk (x, y; z is added to)
-void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D) {
+void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D, int accz) {
     const int tok = c.prof_begin("adj_march");
-    if (2 * c.nkh < 2L * 148 * 64) adj_march_launch<32, 6>(c, lS, lj0, ljk, D);
-    else adj_march_launch<64, 6>(c, lS, lj0, ljk, D);
+    if (2 * c.nkh < 2L * 148 * 64) adj_march_launch<32, 6>(c, lS, lj0, ljk, D, accz);
+    else adj_march_launch<64, 6>(c, lS, lj0, ljk, D, accz);
     c.check_launch("k_adj_march");
     c.prof_end(tok);
 }
@@ -755,6 +879,24 @@ void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X,
     else k_adj_push<float><<<blocks, 128, 0, c.stream>>>(a, Ff, c.parts, c.perm.p, X, alive, c.np, s0, lam, lF, err);
     c.check_launch("k_adj_push");
     c.prof_end(tok);
+}
+void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta,
+                         cpx* psi, double* cpf, double* cpt, cpx* dpt) {
+    k_adj_comoving<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lRx, lRy, jz, beta, gm2, ljz, dbeta, psi, cpf, cpt, dpt);
+    c.check_launch("k_adj_comoving");
+}
+void launch_adj_wsum(Ctx& c, const int32_t* alive, double* out) {
+    k_adj_wsum<<<1, 1024, 0, c.stream>>>(c.parts, alive, c.np, out);
+    c.check_launch("k_adj_wsum");
+}
+void launch_adj_beta(Ctx& c, const double* X, const int32_t* alive, double coef, double* lam) {
+    if (c.np == 0) return;
+    k_adj_beta<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, X, alive, c.np, coef, lam);
+    c.check_launch("k_adj_beta");
+}
+void launch_adj_widen(Ctx& c, const cpxf* a, cpx* b, long n) {
+    k_adj_widen<<<ew_blocks(n), 256, 0, c.stream>>>(a, b, n);
+    c.check_launch("k_adj_widen");
 }
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out) {
     k_adj_lmodes<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lRx, lRy, c.lspx.p, c.lspy.p, out);

@@ -133,6 +133,7 @@ SIGNATURES = [
     ("g3d_launch_count", _I64, [_P]),
     ("g3d_set_laser_modes", _I, [_P, _P]),
     ("g3d_set_exact_fields", _I, [_P, _I32]),
+    ("g3d_set_adjoint_momenta", _I, [_P, _I32]),
     ("g3d_adjoint", _I, [_P, _I32, C.POINTER(_D), _P, _P]),
 ]
 

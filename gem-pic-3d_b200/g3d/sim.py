@@ -248,9 +248,12 @@ class Simulation:
         """Keep the real fields in FP64 as well and gather the beam push from them. Before init."""
         self._c(self.lib.g3d_set_exact_fields(self.ctx, 1 if on else 0))
 
-    def adjoint(self, nsteps, modes=True, momenta=True):
+    def adjoint(self, nsteps, modes=True, momenta=True, through_start=True):
         """From the start field: nsteps s-steps and the reverse sweep. Returns (J, dJ/da [ny, nx/2+1] complex
-        or None, dJ/dp [np, 3] or None) with J = mean p_z of the live beam."""
+        or None, dJ/dp [np, 3] or None) with J = mean p_z of the live beam and dJ/dp taken at load time, through
+        the start field the bunch makes as well as through the s-steps (through_start=False: with the start
+        field held, through the s-steps alone)."""
+        self._c(self.lib.g3d_set_adjoint_momenta(self.ctx, 0 if through_start else 1))
         J = C.c_double()
         gm = np.zeros((self.ny, self.nx // 2 + 1), dtype=np.complex128) if modes else None
         n = self.status().np

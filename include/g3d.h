@@ -267,13 +267,22 @@ int g3d_set_laser_modes(struct g3d_ctx* ctx, const double* coef);
  * from them; the differentiable forward of which central differences are taken. FP64 form; takes effect at the
  * next g3d_init. */
 int g3d_set_exact_fields(struct g3d_ctx* ctx, int32_t on);
+/* What grad_p of g3d_adjoint differentiates (no counterpart in the reference). G3D_ADJ_THROUGH_START (the default):
+ * the momenta as loaded, before g3d_init, so the derivative runs through the start field the bunch makes (its
+ * currents, its beta, the relaxation) as well as through the s-steps. G3D_ADJ_AFTER_START: the momenta right after
+ * g3d_init with the start field held, i.e. through the s-steps alone. Any other mode: G3D_ERR_ARG. */
+#define G3D_ADJ_THROUGH_START 0
+#define G3D_ADJ_AFTER_START   1
+int g3d_set_adjoint_momenta(struct g3d_ctx* ctx, int32_t mode);
 /* The adjoint march, right after g3d_init (Fourier y, beam and grid lasers, no plasma, sponge 0, fixed window):
  * nsteps s-steps forward with per-level checkpoints of the beam and the real fields, J = sum w p_z / sum w over
  * the live beam, then the reverse sweep. Out: *objective = J; grad_modes (NULL: skipped; needs
  * g3d_set_laser_modes) = dJ/d Re a + i dJ/d Im a per stored mode, 2 ny H doubles; grad_p (NULL: skipped) =
- * dJ/d(p_x, p_y, p_z) of every particle at s = 0, 3 np doubles [particle][component], the start field held
- * fixed. The run is left at s = nsteps dz; g3d_set_particles + g3d_init start the next evaluation on the same
- * context (the checkpoint workspace is kept between calls). */
+ * dJ/d(p_x, p_y, p_z) of every particle at s = 0, 3 np doubles [particle][component], through the s-steps and
+ * (unless g3d_set_adjoint_momenta chose G3D_ADJ_AFTER_START) through the start field the bunch made at g3d_init
+ * (its currents, its beta, the relaxation). The run is left at
+ * s = nsteps dz; g3d_set_particles + g3d_init start the next evaluation on the same context (the checkpoint
+ * workspace is kept between calls). */
 int g3d_adjoint(struct g3d_ctx* ctx, int32_t nsteps, double* objective, double* grad_modes, double* grad_p);
 
 #ifdef __cplusplus
