@@ -148,6 +148,10 @@ struct Ctx {
     DevBuf<cpx> lspx, lspy;                      // the grid-laser spectra added at init before the coefficients
     DevBuf<unsigned char> adjws;                 // workspace of the adjoint march, kept between calls
     bool adj_after_start = false;                // dJ/dp with the start field held (G3D_ADJ_AFTER_START)
+    // where the next real fields go instead of F / Fd (taken once by sponge_and_real_fields): the adjoint's forward
+    // writes each level's fields straight into its checkpoint
+    double* fd_next = nullptr;
+    float* f_next = nullptr;
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
@@ -285,8 +289,7 @@ void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const dou
 void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
                      double* lam, double* lF, int* err);
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out);
-void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta,
-                         cpx* psi, double* cpf, double* cpt, cpx* dpt);
+void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta);
 void launch_adj_wsum(Ctx& c, const int32_t* alive, double* out);
 void launch_adj_beta(Ctx& c, const double* X, const int32_t* alive, double coef, double* lam);
 void launch_adj_widen(Ctx& c, const cpxf* a, cpx* b, long n);

@@ -498,6 +498,8 @@ static void march(Ctx& c, double D) {
     else launch_march(c, D);
 }
 static void sponge_and_real_fields(Ctx& c) {
+    if (c.fd_next) { c.Fd.p = c.fd_next; c.fd_next = nullptr; }
+    if (c.f_next) { c.F.p = c.f_next; c.f_next = nullptr; }
     if (!c.yf) {
         if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge_fh(c);
         launch_real_fields_fh(c);
@@ -942,12 +944,26 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
                 G3D_CUDA(cudaMemcpyAsync(x + size_t(q) * np, src[q], size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
             G3D_CUDA(cudaMemcpyAsync(AL + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
         }
-        if (ex) G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
-        else G3D_CUDA(cudaMemcpyAsync(FF + size_t(k) * Fn, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
         sl[size_t(k)] = c.s;
     };
+    // the real fields of level k are written by step k straight into checkpoint k (the push of step k + 1 reads
+    // them there); the context's own F / Fd come back, with the last level's fields, when the forward is done
+    struct Own {
+        Ctx& c; double* fd; float* f;
+        ~Own() { c.Fd.p = fd; c.F.p = f; c.fd_next = nullptr; c.f_next = nullptr; }
+    } own{c, c.Fd.p, c.F.p};
+    if (ex) G3D_CUDA(cudaMemcpyAsync(FD, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+    else G3D_CUDA(cudaMemcpyAsync(FF, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
     save(0);
-    for (int k = 1; k <= K; ++k) { step(c, false); save(k); }
+    for (int k = 1; k <= K; ++k) {
+        if (ex) c.fd_next = FD + size_t(k) * Fn;
+        else c.f_next = FF + size_t(k) * Fn;
+        step(c, false);
+        save(k);
+    }
+    if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
+    else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
+    c.Fd.p = own.fd; c.F.p = own.f;
     launch_adj_objective(c, jo);
     double jh[2];
     G3D_CUDA(cudaMemcpyAsync(jh, jo, 16, cudaMemcpyDeviceToHost, st));
@@ -986,8 +1002,6 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         // three relaxation marches (D = 100 dz; their E_z, B_z, j0 are zeroed and their E_z, B_z, L outputs unread)
         // and the two co-moving fields, to the start currents' j_z and to beta
         const size_t pn = ns * nkh;
-        cpx* psi = W[3]; cpx* dpt = W[4];
-        double* cpf = V; double* cpt = lF;
         if (c.P.start_relax) {
             for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemcpyAsync(ldx + q * pn, lS[q], pn * sizeof(cpx), cudaMemcpyDeviceToDevice, st));
             for (int it = 0; it < 3; ++it) {
@@ -997,10 +1011,10 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
             }
             // dJ/dR_co(1) = (through the marches) - dJ/dR_co(beta)
             for (int q = 0; q < 2; ++q) launch_axpy_c(c, lS[q], ldx + q * pn, -1.0, pn);
-            launch_adj_comoving(c, lS[0], lS[1], jz0, 1.0, 0.0, ljk[2], nullptr, psi, cpf, cpt, dpt);
-            launch_adj_comoving(c, ldx, ldx + pn, jz0, beta0, gm20, ljk[2], dbm, psi, cpf, cpt, dpt);
+            launch_adj_comoving(c, lS[0], lS[1], jz0, 1.0, 0.0, ljk[2], nullptr);
+            launch_adj_comoving(c, ldx, ldx + pn, jz0, beta0, gm20, ljk[2], dbm);
         } else {
-            launch_adj_comoving(c, lS[0], lS[1], jz0, beta0, gm20, ljk[2], dbm, psi, cpf, cpt, dpt);
+            launch_adj_comoving(c, lS[0], lS[1], jz0, beta0, gm20, ljk[2], dbm);
         }
         // the start currents (deposit of the bunch at s = 0) and beta = sum w p_z / gamma / sum w
         launch_adj_currents(c, ljk, W, V, lJ);

@@ -1,6 +1,6 @@
 // The adjoint march: the reverse sweep of the s-steps of the beam and its fields (Fourier y), which the reference
 // does not have. It differentiates J = mean p_z of the live beam after K s-steps with respect to the laser
-// mode coefficients of the start field and the beam momenta at s = 0. Each kernel is the transposed program of
+// mode coefficients of the start field and the beam momenta at s = 0 (through the start field, or after it). Each kernel is the transposed program of
 // one forward kernel, in reverse order; every transform, filter and march coefficient is real or a multiple of
 // i k, so the transposes are the conjugated coefficients and the inverse transforms (no normalisation).
 //   k_adj_objective  J = sum w p_z / sum w over the live particles (one CTA, fixed order)
@@ -15,6 +15,10 @@
 //                    level's checkpoint with the same sub-step rule (frozen schedule), then reversed stage by
 //                    stage; the gather adjoint is a deposit of the field adjoints into dJ/dF
 //   k_adj_lmodes     dJ/d(laser mode coefficient) = sum over slices of conj(laser spectrum) dJ/dR
+//   k_adj_comoving   transposed co-moving field of the start (sim_fields.cpp:44-151): the tridiagonal solves
+//                    along zeta by parallel cyclic reduction, one CTA per mode; dJ/dj_z of the start currents
+//                    and dJ/dbeta per mode
+//   k_adj_wsum, k_adj_beta  beta = sum w p_z / gamma / sum w (sim_fields.cpp:45-51): dJ/dbeta to every particle
 #include "k_push.cuh"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -168,10 +172,11 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, co
 // in registers to the next slice, where it is the lower one. lj0 is written; ljk_x, ljk_y hold on entry the
 // adjoint of jk as the j0 of the next step and are overwritten with the total; ljk_z is written, or added to
 // (accz: the marches of the start field's relaxation, whose j_z adjoint adds to that of init's march(0)). Per
-// slice each lane streams its 8 values (the 6 adjoints of the new level, the 2 pending ones) and the slice's
-// coefficients DEPTH slices ahead into a shared-memory ring with cp.async, as the forward does.
+// slice each lane streams its 8 values (the 6 adjoints of the new level, the 2 pending ones; with accz a third,
+// j_z, so that no plain load waits inside the chain) and the slice's coefficients DEPTH slices ahead into a
+// shared-memory ring with cp.async, as the forward does.
 namespace {
-constexpr int AMA = 8, AMC = 3;
+constexpr int AMA = 9, AMC = 3;
 constexpr int aslot(int bt) { return (AMA + AMC) * bt; }
 __device__ __forceinline__ void acp8(void* smem, const void* gmem) {
     const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -212,7 +217,8 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
     double* jky = reinterpret_cast<double*>(ljky);
     double* jkz = reinterpret_cast<double*>(ljkz);
     auto cell = [&](int sl, int k) { return ringa + size_t(sl) * aslot(BT) + k * BT + tid; };
-    // ring cells: 0 R_x, 1 R_y, 2 L_x, 3 L_y (own), 4 E_z, 5 B_z (other), 6 jk_x, 7 jk_y pending (own); w_lo, w_hi, h
+    // ring cells: 0 R_x, 1 R_y, 2 L_x, 3 L_y (own), 4 E_z, 5 B_z (other), 6 jk_x, 7 jk_y pending (own); w_lo, w_hi,
+    // h; 11 jk_z pending (other; accz only)
     auto fetch = [&](int n) {
         const int sl = (n - g.a) % DEPTH;
         const long o = long(n - g.a) * nk + ii;
@@ -221,6 +227,7 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
         acp8(cell(sl, 4), Ez + oth(o)); acp8(cell(sl, 5), Bz + oth(o));
         acp8(cell(sl, 6), jkx + own(o)); acp8(cell(sl, 7), jky + own(o));
         acp8(cell(sl, 8), g.wlo + n); acp8(cell(sl, 9), g.whi + n); acp8(cell(sl, 10), g.hcg + n + 2);
+        if (accz) acp8(cell(sl, 11), jkz + oth(o));
     };
 #pragma unroll
     for (int q = 0; q < DEPTH; ++q) {
@@ -241,6 +248,7 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
         double AE = sgn * *cell(sl, 4) + qE, AB = sgn * *cell(sl, 5) + qB;
         const double pkx = *cell(sl, 6), pky = *cell(sl, 7);
         const double wl = *cell(sl, 8), wu = *cell(sl, 9), h = *cell(sl, 10);
+        const double pkz = accz ? *cell(sl, 11) : 0.0;
         if (!have_rden) rden = 1 / (1 + 0.25 * h * (D + 0.25 * h) * k2);
         double rden_next = 0;                 // the next slice's inverse denominator, off the chain
         if (n < g.b - 1) {
@@ -284,7 +292,7 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
             // the lower half-cell (plane n - a): this slice's w_lo terms and the previous slice's upper terms
             j0x[own(o)] = c0x + wl * lJx; j0y[own(o)] = c0y + wl * lJy;
             jkx[own(o)] = pkx + ckx + wl * lJx; jky[own(o)] = pky + cky + wl * lJy;
-            jkz[oth(o)] = accz ? jkz[oth(o)] + sgn * ckz : sgn * ckz;
+            jkz[oth(o)] = pkz + sgn * ckz;
         }
         rden = rden_next;
         have_rden = n < g.b - 1;
@@ -460,14 +468,16 @@ struct Sten {
     double A[6], wx[3], wn[3], fz;
     int ix[3], jn[3], fl;                     // fl < 0: nothing to deposit
 };
-// The gather with its adjoint: E, B at (x, y, zeta) as the forward computes them, sum_c A_c grad(field_c), and
-// the stencil of the field adjoints A[6].
+// The fields at one stage point with their gradients (per component: value, d/dx, d/dy, d/dzeta), gathered as
+// the forward gathers them, and the stencil the field adjoints of that point go to (A is filled by the reverse
+// chain). The forward recompute of a sub-step gathers each of its four stage points once; the reverse chain then
+// reads no memory.
+struct Gat { double F[6], dx[6], dy[6], dz[6]; };
 template <class FT>
-__device__ __forceinline__ void gather_adj(const PushArgs& c, const FT* __restrict__ Fp, double x, double y, double zeta,
-                                           const double A[6], double E[3], double B[3], double& gx, double& gy, double& gz,
-                                           Sten& st) {
-    E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
-    gx = gy = gz = 0;
+__device__ __forceinline__ void gather_grad(const PushArgs& c, const FT* __restrict__ Fp, double x, double y, double zeta, Gat& G,
+                                            Sten& st) {
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) G.F[comp] = G.dx[comp] = G.dy[comp] = G.dz[comp] = 0;
     st.fl = -1;
     if (!c.self) return;
     const Geo& g = c.g;
@@ -484,23 +494,35 @@ __device__ __forceinline__ void gather_adj(const PushArgs& c, const FT* __restri
     tsc_dweights(y / g.dy, dwn);
     const double idx_ = 1 / g.dx, idy = 1 / g.dy;
     const long nk = g.nk;
+#pragma unroll
     for (int comp = 0; comp < 6; ++comp) {
         const FT* p0 = Fp + (long(comp) * (g.ns + 2) + fl) * nk;
         const FT* p1 = p0 + nk;
         double v = 0, sx = 0, sy = 0, sz = 0;
+#pragma unroll
         for (int j = 0; j < 3; ++j)
+#pragma unroll
             for (int i = 0; i < 3; ++i) {
                 const long k = long(st.jn[j]) * g.nx + st.ix[i];
-                const double f0 = double(p0[k]), f1 = double(p1[k]);
+                const double f0 = double(__ldg(p0 + k)), f1 = double(__ldg(p1 + k));
                 const double val = (1 - fz) * f0 + fz * f1;
                 v += st.wx[i] * st.wn[j] * val;
                 sx += dwx[i] * st.wn[j] * val; sy += st.wx[i] * dwn[j] * val; sz += st.wx[i] * st.wn[j] * (f1 - f0);
             }
-        if (comp < 3) E[comp] = v; else B[comp - 3] = v;
-        gx += A[comp] * sx * idx_; gy += A[comp] * sy * idy; gz += A[comp] * sz * dfz;
-        st.A[comp] = A[comp];
+        G.F[comp] = v; G.dx[comp] = sx * idx_; G.dy[comp] = sy * idy; G.dz[comp] = sz * dfz;
     }
     st.fz = fz; st.fl = fl;
+}
+// the right-hand side of the characteristics at Y with the gathered fields (rhs of k_push.cuh, no analytic laser:
+// the adjoint march rejects it)
+__device__ __forceinline__ St rhs_g(const St& Y, double qm, const Gat& G) {
+    const double g = sqrt(1 + Y.px * Y.px + Y.py * Y.py + Y.pz * Y.pz);
+    const double gm = (1 + Y.px * Y.px + Y.py * Y.py) / (g + Y.pz);
+    const double* E = G.F;
+    const double* B = G.F + 3;
+    const double ip = 1 / Y.pz;
+    return St{Y.px * ip, Y.py * ip, -gm * ip, qm * (g * E[0] + Y.py * B[2] - Y.pz * B[1]) * ip,
+              qm * (g * E[1] + Y.pz * B[0] - Y.px * B[2]) * ip, qm * (g * E[2] + Y.px * B[1] - Y.py * B[0]) * ip};
 }
 // the field adjoints of the stencils st[0..ns) into dJ/dF: summed per point when every stencil has the same
 // points and planes, else one by one
@@ -539,10 +561,8 @@ __device__ __forceinline__ void flush_stencils(const Geo& g, const Sten* st, int
         }
     }
 }
-// lY += d(mu . rhs)/dY at Y; the field adjoints into the stencil st
-template <class FT>
-__device__ __forceinline__ void rhs_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double qm, const St& mu, St& lY,
-                                        Sten& st) {
+// lY += d(mu . rhs)/dY at Y from the gathered fields and gradients; the field adjoints A into the stencil st
+__device__ __forceinline__ void rhs_adj(const St& Y, double qm, const St& mu, const Gat& G, St& lY, Sten& st) {
     const double px = Y.px, py = Y.py, pz = Y.pz;
     const double g = sqrt(1 + px * px + py * py + pz * pz);
     const double gpz = g + pz, gm = (1 + px * px + py * py) / gpz, ip = 1 / pz;
@@ -551,49 +571,58 @@ __device__ __forceinline__ void rhs_adj(const PushArgs& c, const FT* __restrict_
     A[3] = qm * ip * (mu.py * pz - mu.pz * py);
     A[4] = qm * ip * (mu.pz * px - mu.px * pz);
     A[5] = qm * ip * (mu.px * py - mu.py * px);
-    double E[3], B[3], gx, gy, gz;
-    gather_adj(c, Fp, wrap_periodic(Y.x, c.g.Lx), wrap_periodic(Y.y, c.g.Ly), Y.zeta, A, E, B, gx, gy, gz, st);
+    double gx = 0, gy = 0, gz = 0;
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) {
+        gx += A[comp] * G.dx[comp]; gy += A[comp] * G.dy[comp]; gz += A[comp] * G.dz[comp];
+        st.A[comp] = A[comp];
+    }
+    const double* E = G.F;
+    const double* B = G.F + 3;
     const double Fx = qm * (g * E[0] + py * B[2] - pz * B[1]);
     const double Fy = qm * (g * E[1] + pz * B[0] - px * B[2]);
     const double Fz = qm * (g * E[2] + px * B[1] - py * B[0]);
-    const double G = mu.px * E[0] + mu.py * E[1] + mu.pz * E[2];
+    const double Gm = mu.px * E[0] + mu.py * E[1] + mu.pz * E[2];
     const double dgx = (2 * px - gm * px / g) / gpz, dgy = (2 * py - gm * py / g) / gpz, dgz = -gm * (pz / g + 1) / gpz;
     lY.x += gx; lY.y += gy; lY.zeta += gz;
-    lY.px += mu.x * ip - mu.zeta * ip * dgx + qm * ip * (G * px / g - mu.py * B[2] + mu.pz * B[1]);
-    lY.py += mu.y * ip - mu.zeta * ip * dgy + qm * ip * (G * py / g + mu.px * B[2] - mu.pz * B[0]);
+    lY.px += mu.x * ip - mu.zeta * ip * dgx + qm * ip * (Gm * px / g - mu.py * B[2] + mu.pz * B[1]);
+    lY.py += mu.y * ip - mu.zeta * ip * dgy + qm * ip * (Gm * py / g + mu.px * B[2] - mu.pz * B[0]);
     lY.pz += -(mu.x * px + mu.y * py) * ip * ip - mu.zeta * ip * dgz + mu.zeta * gm * ip * ip +
-             qm * ip * (G * pz / g - mu.px * B[1] + mu.py * B[0]) - ip * ip * (mu.px * Fx + mu.py * Fy + mu.pz * Fz);
+             qm * ip * (Gm * pz / g - mu.px * B[1] + mu.py * B[0]) - ip * ip * (mu.px * Fx + mu.py * Fy + mu.pz * Fz);
 }
 __device__ __forceinline__ St scale(const St& a, double h) { return St{h * a.x, h * a.y, h * a.zeta, h * a.px, h * a.py, h * a.pz}; }
 __device__ __forceinline__ St add(const St& a, const St& b) {
     return St{a.x + b.x, a.y + b.y, a.zeta + b.zeta, a.px + b.px, a.py + b.py, a.pz + b.pz};
 }
-// the adjoint of one RK4 sub-step at its start state Y: lam (of the end state) -> lam (of Y)
+// the adjoint of one RK4 sub-step at its start state Y: lam (of the end state) -> lam (of Y). The forward stages
+// are recomputed with each stage point gathered once (values and gradients); the reverse chain uses those.
 template <class FT>
-__device__ __forceinline__ St rk4_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double z, double ds, double qm,
-                                      const St& lam, double* __restrict__ lF) {
-    St k;
-    rhs(c, Fp, Y, z, qm, k);
-    const St Y2 = axpy(Y, 0.5 * ds, k);
-    rhs(c, Fp, Y2, z + 0.5 * ds, qm, k);
-    const St Y3 = axpy(Y, 0.5 * ds, k);
-    rhs(c, Fp, Y3, z + 0.5 * ds, qm, k);
-    const St Y4 = axpy(Y, ds, k);
+__device__ __forceinline__ St rk4_adj(const PushArgs& c, const FT* __restrict__ Fp, const St& Y, double ds, double qm, const St& lam,
+                                      double* __restrict__ lF) {
+    const Geo& g = c.g;
+    Gat G1, G2, G3, G4;
+    Sten st[4];
+    gather_grad(c, Fp, wrap_periodic(Y.x, g.Lx), wrap_periodic(Y.y, g.Ly), Y.zeta, G1, st[0]);
+    const St Y2 = axpy(Y, 0.5 * ds, rhs_g(Y, qm, G1));
+    gather_grad(c, Fp, wrap_periodic(Y2.x, g.Lx), wrap_periodic(Y2.y, g.Ly), Y2.zeta, G2, st[1]);
+    const St Y3 = axpy(Y, 0.5 * ds, rhs_g(Y2, qm, G2));
+    gather_grad(c, Fp, wrap_periodic(Y3.x, g.Lx), wrap_periodic(Y3.y, g.Ly), Y3.zeta, G3, st[2]);
+    const St Y4 = axpy(Y, ds, rhs_g(Y3, qm, G3));
+    gather_grad(c, Fp, wrap_periodic(Y4.x, g.Lx), wrap_periodic(Y4.y, g.Ly), Y4.zeta, G4, st[3]);
     St lY = lam;
     St m1 = scale(lam, ds / 6), m2 = scale(lam, ds / 3), m3 = scale(lam, ds / 3);
     const St m4 = scale(lam, ds / 6);
-    Sten st[4];
     St a{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y4, qm, m4, a, st[3]);             // k4 = f(Y + ds k3)
+    rhs_adj(Y4, qm, m4, G4, a, st[3]);                // k4 = f(Y + ds k3)
     lY = add(lY, a); m3 = add(m3, scale(a, ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y3, qm, m3, a, st[2]);             // k3 = f(Y + ds/2 k2)
+    rhs_adj(Y3, qm, m3, G3, a, st[2]);                // k3 = f(Y + ds/2 k2)
     lY = add(lY, a); m2 = add(m2, scale(a, 0.5 * ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y2, qm, m2, a, st[1]);             // k2 = f(Y + ds/2 k1)
+    rhs_adj(Y2, qm, m2, G2, a, st[1]);                // k2 = f(Y + ds/2 k1)
     lY = add(lY, a); m1 = add(m1, scale(a, 0.5 * ds));
     a = St{0, 0, 0, 0, 0, 0};
-    rhs_adj(c, Fp, Y, qm, m1, a, st[0]);              // k1 = f(Y)
+    rhs_adj(Y, qm, m1, G1, a, st[0]);                 // k1 = f(Y)
     flush_stencils(c.g, st, 4, lF);
     return add(lY, a);
 }
@@ -616,137 +645,226 @@ __global__ void __launch_bounds__(128) k_adj_push(PushArgs c, const FT* __restri
     if (lm.x == 0 && lm.y == 0 && lm.zeta == 0 && lm.px == 0 && lm.py == 0 && lm.pz == 0) return;
     const St Y0{X[ip], X[np + ip], X[2 * np + ip], X[3 * np + ip], X[4 * np + ip], X[5 * np + ip]};
     const double qm = P.qm[ip], s1 = c.s1;
-    double zs[ADJ_MAXSUB], dss[ADJ_MAXSUB];
+    const double zend = s1 - 1e-12 * fabs(s1);
     int nsub = 0;
-    {                                         // the sub-step schedule of the forward (the last one is not taken)
+    {                                         // the sub-step count of the forward (the last one is not taken)
         St Y = Y0;
         double z = s0;
-        const double zend = s1 - 1e-12 * fabs(s1);
         while (z < zend) {
             const double ds = substep(c, Y, z, s1);
             if (nsub == ADJ_MAXSUB) { atomicOr(err, 2); return; }
-            zs[nsub] = z; dss[nsub] = ds; ++nsub;
+            ++nsub;
             if (!(z + ds < zend)) break;
             if (!rk4_step(c, Fp, Y, z, ds, qm)) return;      // lost in the forward: no adjoint
             z += ds;
         }
     }
-    for (int t = nsub - 1; t >= 0; --t) {
+    for (int t = nsub - 1; t >= 0; --t) {     // sub-step t from its start state, the schedule recomputed as taken
         St Y = Y0;
-        for (int u = 0; u < t; ++u) rk4_step(c, Fp, Y, zs[u], dss[u], qm);
-        lm = rk4_adj(c, Fp, Y, zs[t], dss[t], qm, lm, lF);
+        double z = s0;
+        for (int u = 0; u < t; ++u) {
+            const double ds = substep(c, Y, z, s1);
+            rk4_step(c, Fp, Y, z, ds, qm);
+            z += ds;
+        }
+        lm = rk4_adj(c, Fp, Y, substep(c, Y, z, s1), qm, lm, lF);
     }
     lam[ip] = lm.x; lam[np + ip] = lm.y; lam[2 * np + ip] = lm.zeta;
     lam[3 * np + ip] = lm.px; lam[4 * np + ip] = lm.py; lam[5 * np + ip] = lm.pz;
 }
 
 // ---------------------------------------------------------------- laser mode coefficients
-// R += a(k) s(k, l) at init: dJ/da(k) = sum_l conj(s_x) dJ/dR_x + conj(s_y) dJ/dR_y
-__global__ void k_adj_lmodes(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy, const cpx* __restrict__ sx,
-                             const cpx* __restrict__ sy, cpx* __restrict__ out) {
+// R += a(k) s(k, l) at init: dJ/da(k) = sum_l conj(s_x) dJ/dR_x + conj(s_y) dJ/dR_y. A CTA takes 32 modes
+// (coalesced along k_x) x LMS slice lanes, each lane summing every LMS-th slice; the lanes are added in a fixed order.
+namespace { constexpr int LMS = 8; }
+__global__ void __launch_bounds__(32 * LMS) k_adj_lmodes(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy,
+                                                         const cpx* __restrict__ sx, const cpx* __restrict__ sy,
+                                                         cpx* __restrict__ out) {
+    __shared__ cpx part[LMS][32];
     const long nk = g.nkh;
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nk) return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const long i = long(blockIdx.x) * 32 + tx;
     cpx s = C(0);
-    for (int l = 0; l < g.ns; ++l) {
-        const long o = long(l) * nk + i;
-        s = s + conj(sx[o]) * lRx[o] + conj(sy[o]) * lRy[o];
+    if (i < nk)
+        for (int l = ty; l < g.ns; l += LMS) {
+            const long o = long(l) * nk + i;
+            s = s + conj(sx[o]) * lRx[o] + conj(sy[o]) * lRy[o];
+        }
+    part[ty][tx] = s;
+    __syncthreads();
+    if (ty == 0 && i < nk) {
+        for (int q = 1; q < LMS; ++q) s = s + part[q][tx];
+        out[i] = s;
     }
-    out[i] = s;
 }
 
 // ---------------------------------------------------------------- the start field's dependence on the bunch
 // transposed co-moving field (Fourier y; k_comoving of k_march.cu, Simulation::comoving_field,
 // src/sim_fields.cpp:44-151): per mode, R = -(1 + beta) i k psi with A(gm2) psi = rhs along zeta,
 // rhs(l) = (w_lo j_z(l) + w_hi j_z(l+1)) / beta. In: dJ/dR; out: dJ/dj_z added to ljz and, when dbeta is given,
-// dJ/dbeta of the mode (through 1 + beta, 1/beta and gm2 = 1 - beta^2). Scratch per mode and slice: psi, the
-// forward Thomas factor, the transposed solve's factor and right-hand side.
-__global__ void __launch_bounds__(128) k_adj_comoving(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy,
+// dJ/dbeta of the mode (through 1 + beta, 1/beta and gm2 = 1 - beta^2):
+//   dJ/dpsi = conj(-(1 + beta) i k) dJ/dR = (1 + beta) i k dJ/dR;  A^T dJ/drhs = dJ/dpsi;
+//   dJ/dbeta = -Re<dJ/dR, i k psi> - Re<dJ/drhs, rhs> / beta - 2 beta Re<dJ/drhs, (dA/dgm2) psi>.
+// One CTA per mode: the tridiagonal systems along zeta (A for psi, needed only for dbeta, and A^T) are solved
+// by parallel cyclic reduction in shared memory, ceil(log2 ns) halvings of the coupling distance, so a mode
+// costs a few microseconds instead of a 4 x ns-long dependent chain. The k = 0 mode is skipped: R(k = 0) =
+// -(1 + beta) i 0 psi = 0 whatever psi is, so it has no adjoint.
+namespace {
+constexpr int CMT = 256;                            // threads per mode
+// a_i x_{i-1} + b_i x_i + c_i x_{i+1} = d_i, i < n (a_0 = c_{n-1} = 0); on return d_i = x_i. Rows tid + r CMT.
+template <int RPT>
+__device__ void pcr_solve(double* a, double* b, double* c, cpx* d, int n) {
+    const int tid = threadIdx.x;
+    for (int s = 1; s < n; s <<= 1) {
+        double na[RPT], nb[RPT], nc[RPT];
+        cpx nd[RPT];
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + r * CMT;
+            if (i >= n) continue;
+            double A2 = 0, B2 = b[i], C2 = 0;
+            cpx D2 = d[i];
+            if (i - s >= 0) {
+                const double al = -a[i] / b[i - s];
+                A2 = al * a[i - s]; B2 += al * c[i - s]; D2 = D2 + al * d[i - s];
+            }
+            if (i + s < n) {
+                const double ga = -c[i] / b[i + s];
+                C2 = ga * c[i + s]; B2 += ga * a[i + s]; D2 = D2 + ga * d[i + s];
+            }
+            na[r] = A2; nb[r] = B2; nc[r] = C2; nd[r] = D2;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int i = tid + r * CMT;
+            if (i < n) { a[i] = na[r]; b[i] = nb[r]; c[i] = nc[r]; d[i] = nd[r]; }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int i = tid + r * CMT;
+        if (i < n) d[i] = (1 / b[i]) * d[i];
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ double cdot(cpx u, cpx v) { return u.x * v.x + u.y * v.y; }
+}  // namespace
+
+template <int RPT>
+__global__ void __launch_bounds__(CMT) k_adj_comoving(Geo g, const cpx* __restrict__ lRx, const cpx* __restrict__ lRy,
                                                      const cpx* __restrict__ jz, double beta, double gm2, cpx* __restrict__ ljz,
-                                                     double* __restrict__ dbeta, cpx* __restrict__ psi, double* __restrict__ cpf,
-                                                     double* __restrict__ cpt, cpx* __restrict__ dpt) {
-    const long nk = g.nkh;
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nk) return;
+                                                     double* __restrict__ dbeta) {
+    extern __shared__ double smc[];
+    const int ns = g.ns, tid = threadIdx.x;
+    cpx* d = reinterpret_cast<cpx*>(smc);
+    double* a = smc + 2 * ns;
+    double* b = a + ns;
+    double* c = b + ns;
+    const long nk = g.nkh, i = blockIdx.x;
     const int kxi = int(i % g.H), j = int(i / g.H);
-    const double kx = g.kxd[kxi], ky = g.kyd[j], ev = ky * ky;
-    const int ns = g.ns;
-    auto coef = [&](int l, double& lo, double& up, double& dg, double& lo1, double& up1, double& dg1) {
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
+    if (k2 == 0) {
+        if (dbeta && tid == 0) dbeta[i] = 0;
+        return;
+    }
+    // row l: lo(l) = gm2 lo1(l), up(l) = gm2 up1(l), dg(l) = k^2 + gm2 dg1(l) (k_comoving's coefficients)
+    auto d1 = [&](int l, double& lo1, double& up1, double& dg1) {
         const int n = g.a + l;
         const double hm = g.hcg[n + 1], hp = g.hcg[n + 2];
-        lo1 = -2 / ((hm + hp) * hm); up1 = -2 / ((hm + hp) * hp); dg1 = 2 / (hm * hp);   // d/d(gm2)
-        lo = gm2 * lo1; up = gm2 * up1; dg = kx * kx + ev + gm2 * dg1;
+        lo1 = -2 / ((hm + hp) * hm); up1 = -2 / ((hm + hp) * hp); dg1 = 2 / (hm * hp);
     };
     auto rhs_at = [&](int l) {
         const int n = g.a + l;
         const long o = long(l) * nk + i;
         return (1 / beta) * (g.wlo[n] * jz[o] + g.whi[n] * jz[o + nk]);
     };
-    {
-        double lo, up, dg, a1, b1, c1;
-        coef(0, lo, up, dg, a1, b1, c1);
-        if (dg == 0) { if (dbeta) dbeta[i] = 0; return; }       // the forward leaves this mode zero
-    }
-    // forward: psi (as k_comoving)
-    double cprev = 0;
-    cpx dprev = C(0);
-    for (int l = 0; l < ns; ++l) {
-        double lo, up, dg, a1, b1, c1;
-        coef(l, lo, up, dg, a1, b1, c1);
-        const long o = long(l) * nk + i;
-        const double den = dg - lo * cprev;
-        const double cpv = up / den;
-        const cpx dpv = (rhs_at(l) - lo * dprev) / den;
-        cpf[o] = cpv; psi[o] = dpv;
-        cprev = cpv; dprev = dpv;
-    }
-    cpx next = C(0);
-    for (int l = ns - 1; l >= 0; --l) {
-        const long o = long(l) * nk + i;
-        next = psi[o] - cpf[o] * next;
-        psi[o] = next;
-    }
-    // dJ/dpsi = conj(-(1 + beta) i k) dJ/dR = (1 + beta) i k dJ/dR; A^T lrhs = lpsi (sub(l) = up(l-1), sup(l) = lo(l+1))
-    const double opb = 1 + beta;
-    double cpp = 0, upm = 0;
-    cpx dpp = C(0);
-    for (int l = 0; l < ns; ++l) {
-        double lo, up, dg, a1, b1, c1;
-        coef(l, lo, up, dg, a1, b1, c1);
-        double lon = 0;
-        if (l + 1 < ns) { double u2, d2, a2, b2, c2; coef(l + 1, lon, u2, d2, a2, b2, c2); }
-        const long o = long(l) * nk + i;
-        const cpx lpsi = opb * (ik(kx, lRx[o]) + ik(ky, lRy[o]));
-        const double sub = l > 0 ? upm : 0;
-        const double den = dg - sub * cpp;
-        const double c = lon / den;
-        const cpx d = (lpsi - sub * dpp) / den;
-        cpt[o] = c; dpt[o] = d;
-        cpp = c; dpp = d; upm = up;
-    }
-    double t1 = 0, t2 = 0, t3 = 0;
-    cpx lnext = C(0);
-    for (int l = ns - 1; l >= 0; --l) {
-        const int n = g.a + l;
-        const long o = long(l) * nk + i;
-        lnext = dpt[o] - cpt[o] * lnext;                       // dJ/drhs(l)
-        const cpx lr = lnext;
-        ljz[o] = ljz[o] + (g.wlo[n] / beta) * lr;
-        ljz[o + nk] = ljz[o + nk] + (g.whi[n] / beta) * lr;
-        if (dbeta) {
-            const cpx ps = psi[o];
-            const cpx mRx = ik(kx, ps), mRy = ik(ky, ps);      // -dR/dbeta = i k psi
-            t1 -= lRx[o].x * mRx.x + lRx[o].y * mRx.y + lRy[o].x * mRy.x + lRy[o].y * mRy.y;
-            const cpx rh = rhs_at(l);
-            t2 -= (lr.x * rh.x + lr.y * rh.y) / beta;
-            double lo, up, dg, lo1, up1, dg1;
-            coef(l, lo, up, dg, lo1, up1, dg1);
-            const cpx pm = l > 0 ? psi[o - nk] : C(0), pp = l + 1 < ns ? psi[o + nk] : C(0);
-            const cpx ap = lo1 * pm + dg1 * ps + up1 * pp;      // (dA/dgm2) psi, row l
-            t3 -= lr.x * ap.x + lr.y * ap.y;
+    const bool tri = gm2 != 0;                       // gm2 = 0: A is the diagonal k^2
+    cpx ps[RPT];
+    if (dbeta) {                                     // psi = A^-1 rhs, kept per row in registers
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int l = tid + r * CMT;
+            if (l >= ns) continue;
+            double lo1, up1, dg1;
+            d1(l, lo1, up1, dg1);
+            a[l] = l > 0 ? gm2 * lo1 : 0; b[l] = k2 + gm2 * dg1; c[l] = l + 1 < ns ? gm2 * up1 : 0;
+            d[l] = rhs_at(l);
         }
+        __syncthreads();
+        if (tri) pcr_solve<RPT>(a, b, c, d, ns);
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int l = tid + r * CMT;
+            ps[r] = l < ns ? (tri ? d[l] : (1 / b[l]) * d[l]) : C(0);
+        }
+        __syncthreads();
     }
-    if (dbeta) dbeta[i] = t1 + t2 + (-2 * beta) * t3;
+    // A^T lrhs = lpsi: row l of A^T is (up(l-1), dg(l), lo(l+1))
+    const double opb = 1 + beta;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int l = tid + r * CMT;
+        if (l >= ns) continue;
+        double lo1, up1, dg1, lo1n = 0, up1p = 0, t0, t1;
+        d1(l, lo1, up1, dg1);
+        if (l > 0) d1(l - 1, t0, up1p, t1);
+        if (l + 1 < ns) d1(l + 1, lo1n, t0, t1);
+        a[l] = l > 0 ? gm2 * up1p : 0; b[l] = k2 + gm2 * dg1; c[l] = l + 1 < ns ? gm2 * lo1n : 0;
+        const long o = long(l) * nk + i;
+        d[l] = opb * (ik(kx, lRx[o]) + ik(ky, lRy[o]));
+    }
+    __syncthreads();
+    if (tri) pcr_solve<RPT>(a, b, c, d, ns);
+    else {
+#pragma unroll
+        for (int r = 0; r < RPT; ++r) {
+            const int l = tid + r * CMT;
+            if (l < ns) d[l] = (1 / b[l]) * d[l];
+        }
+        __syncthreads();
+    }
+    // dJ/dj_z of plane p (0 .. ns): rhs(p) reads it with w_lo(p), rhs(p - 1) with w_hi(p - 1)
+    for (int p = tid; p <= ns; p += CMT) {
+        cpx v = C(0);
+        if (p < ns) v = v + g.wlo[g.a + p] * d[p];
+        if (p > 0) v = v + g.whi[g.a + p - 1] * d[p - 1];
+        const long o = long(p) * nk + i;
+        ljz[o] = ljz[o] + (1 / beta) * v;
+    }
+    if (!dbeta) return;
+    double t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+    for (int r = 0; r < RPT; ++r) {
+        const int l = tid + r * CMT;
+        if (l >= ns) continue;
+        const long o = long(l) * nk + i;
+        t1 -= cdot(lRx[o], ik(kx, ps[r])) + cdot(lRy[o], ik(ky, ps[r]));
+        t2 -= cdot(d[l], rhs_at(l)) / beta;
+        // Re<lrhs, (dA/dgm2) psi> = sum_m Re<psi_m, up1(m-1) lrhs(m-1) + dg1(m) lrhs(m) + lo1(m+1) lrhs(m+1)>
+        double lo1, up1, dg1, lo1n = 0, up1p = 0, t0, tt;
+        d1(l, lo1, up1, dg1);
+        cpx v = dg1 * d[l];
+        if (l > 0) { d1(l - 1, t0, up1p, tt); v = v + up1p * d[l - 1]; }
+        if (l + 1 < ns) { d1(l + 1, lo1n, t0, tt); v = v + lo1n * d[l + 1]; }
+        t3 -= cdot(ps[r], v);
+    }
+    // block sums in a fixed order
+    __shared__ double red[3][CMT / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        t1 += __shfl_down_sync(0xffffffffu, t1, off);
+        t2 += __shfl_down_sync(0xffffffffu, t2, off);
+        t3 += __shfl_down_sync(0xffffffffu, t3, off);
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = t1; red[1][tid >> 5] = t2; red[2][tid >> 5] = t3; }
+    __syncthreads();
+    if (tid == 0) {
+        double s1 = 0, s2 = 0, s3 = 0;
+        for (int w = 0; w < CMT / 32; ++w) { s1 += red[0][w]; s2 += red[1][w]; s3 += red[2][w]; }
+        dbeta[i] = s1 + s2 + (-2 * beta) * s3;
+    }
 }
 // sum of w over the particles alive at a level (one CTA, fixed order)
 __global__ void __launch_bounds__(1024) k_adj_wsum(PartsDev P, const int32_t* __restrict__ alive, long np, double* __restrict__ out) {
@@ -880,9 +998,20 @@ void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X,
     c.check_launch("k_adj_push");
     c.prof_end(tok);
 }
-void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta,
-                         cpx* psi, double* cpf, double* cpt, cpx* dpt) {
-    k_adj_comoving<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lRx, lRy, jz, beta, gm2, ljz, dbeta, psi, cpf, cpt, dpt);
+template <int RPT>
+static void adj_comoving_launch(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz,
+                                double* dbeta) {
+    const size_t smem = size_t(c.ns) * (sizeof(cpx) + 3 * sizeof(double));
+    smem_attr(reinterpret_cast<const void*>(k_adj_comoving<RPT>), smem);
+    k_adj_comoving<RPT><<<unsigned(c.nkh), CMT, smem, c.stream>>>(c.geo(), lRx, lRy, jz, beta, gm2, ljz, dbeta);
+}
+void launch_adj_comoving(Ctx& c, const cpx* lRx, const cpx* lRy, const cpx* jz, double beta, double gm2, cpx* ljz, double* dbeta) {
+    const int ns = c.ns;
+    if (ns <= 2 * CMT) adj_comoving_launch<2>(c, lRx, lRy, jz, beta, gm2, ljz, dbeta);
+    else if (ns <= 4 * CMT) adj_comoving_launch<4>(c, lRx, lRy, jz, beta, gm2, ljz, dbeta);
+    else if (ns <= 8 * CMT) adj_comoving_launch<8>(c, lRx, lRy, jz, beta, gm2, ljz, dbeta);
+    else if (ns <= 16 * CMT) adj_comoving_launch<16>(c, lRx, lRy, jz, beta, gm2, ljz, dbeta);
+    else throw Error(G3D_ERR_CAPACITY, "the adjoint's co-moving field takes at most 4096 slices");
     c.check_launch("k_adj_comoving");
 }
 void launch_adj_wsum(Ctx& c, const int32_t* alive, double* out) {
@@ -899,7 +1028,7 @@ void launch_adj_widen(Ctx& c, const cpxf* a, cpx* b, long n) {
     c.check_launch("k_adj_widen");
 }
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out) {
-    k_adj_lmodes<<<unsigned((c.nkh + 127) / 128), 128, 0, c.stream>>>(c.geo(), lRx, lRy, c.lspx.p, c.lspy.p, out);
+    k_adj_lmodes<<<unsigned((c.nkh + 31) / 32), 32 * LMS, 0, c.stream>>>(c.geo(), lRx, lRy, c.lspx.p, c.lspy.p, out);
     c.check_launch("k_adj_lmodes");
 }
 

@@ -144,6 +144,46 @@ def test_start_field_part_of_the_momentum_gradient():
         assert abs(part_ad - part_fd) <= 1e-4 * abs(part_fd) + TOL * abs(f1), (k, part_ad, part_fd)
 
 
+def autograd_inputs(cfg):
+    import torch
+    from g3d.sim import sample_bunches
+    n = len(sample_bunches(cfg)[0])
+    coef = torch.zeros(cfg.ny, cfg.nx // 2 + 1, 2, dtype=torch.float64)
+    coef[..., 0] = 1
+    return coef.requires_grad_(), torch.zeros(n, 3, dtype=torch.float64, requires_grad=True)
+
+
+def test_autograd_function_backward_is_the_adjoint():
+    from g3d.autograd import MarchObjective
+    cfg = case()
+    coef, dp = autograd_inputs(cfg)
+    J, gm, gp, _ = adjoint(cfg)
+    out = MarchObjective.apply(coef, dp, cfg)
+    assert abs(out.item() - J) <= 1e-13 * abs(J)
+    (2.0 * out).backward()
+    # two runs: the gradients differ in the order of their atomic adds only
+    scale_m, scale_p = np.max(np.abs(gm)), np.max(np.abs(gp))
+    assert np.allclose(coef.grad[..., 0].numpy(), 2 * gm.real, rtol=1e-9, atol=1e-12 * scale_m)
+    assert np.allclose(coef.grad[..., 1].numpy(), 2 * gm.imag, rtol=1e-9, atol=1e-12 * scale_m)
+    assert np.allclose(dp.grad.numpy(), 2 * gp, rtol=1e-9, atol=1e-12 * scale_p)
+
+
+@pytest.mark.parametrize("through_start", [True, False])
+def test_autograd_function_passes_gradcheck(through_start):
+    """torch.autograd.gradcheck through g3d.autograd.MarchObjective, fast mode (per input one random unit
+    direction u: the central difference of the forward with step eps along u against the adjoint's
+    vector-Jacobian product along u), eps = 1e-6, relative tolerance 1e-6, no absolute tolerance."""
+    import torch
+    from g3d.autograd import MarchObjective
+    cfg = case()
+    coef, dp = autograd_inputs(cfg)
+    j0 = MarchObjective.apply(coef, dp, cfg, "fp64", True, through_start).item()
+
+    def fn(c, d):
+        return MarchObjective.apply(c, d, cfg, "fp64", True, through_start, j0)
+    assert torch.autograd.gradcheck(fn, (coef, dp), eps=EPS, atol=0.0, rtol=TOL, fast_mode=True)
+
+
 def test_adjoint_momentum_mode_is_checked():
     from g3d import Simulation
     from g3d.sim import G3DError
