@@ -144,6 +144,45 @@ def test_start_field_part_of_the_momentum_gradient():
         assert abs(part_ad - part_fd) <= 1e-4 * abs(part_fd) + TOL * abs(f1), (k, part_ad, part_fd)
 
 
+def reference_final(cfg, dp):
+    """The final beam of the reference CPU code (oracle/_ref) with dp added to the momenta as loaded."""
+    ref = pytest.importorskip("ref")
+    if not ref.available():
+        pytest.skip("reference build oracle/_ref not present")
+    r = ref.RefSimulation(cfg, threads=8)
+    try:
+        r.load_bunch()
+        p = r.host_particles()
+        p["px"] += dp[:, 0]; p["py"] += dp[:, 1]; p["pz"] += dp[:, 2]
+        r.set_particles(p)
+        r.init_fields()
+        for _ in range(cfg.steps):
+            r.step()
+        return r.host_particles()
+    finally:
+        r.close()
+
+
+@pytest.mark.parametrize("charge_pC", [0.01, 1.0])
+def test_momentum_gradient_against_central_differences_of_the_reference(charge_pC):
+    """Central differences of the reference's own CPU code (its FP64 arithmetic, its real fields rounded to float as
+    it stores them) against the adjoint of the same forward (float F, the rounding linearised as the identity).
+    The float F puts a rounding floor into the reference's difference quotient (~1e-4 at eps = 1e-6, falling with
+    eps), so eps = 3e-3, where the floor is below 1e-5 and the truncation error too. The forward here takes the same
+    difference to 1e-9: it is the reference's arithmetic."""
+    from g3d import configs
+    cfg = configs.adjoint_small(charge_pC=charge_pC)
+    _, _, gf, _ = adjoint(cfg, exact=False)
+    D = np.random.default_rng(12).standard_normal(gf.shape)
+    e = 3e-3
+    fr = central(reference_final(cfg, e * D), reference_final(cfg, -e * D), e)
+    fo = central(forward(cfg, dp=e * D, exact=False), forward(cfg, dp=-e * D, exact=False), e)
+    ad = float(np.sum(gf * D))
+    print(f"momenta, {charge_pC} pC: reference central difference {fr:.12e}, this forward's {fo:.12e}, adjoint {ad:.12e}")
+    assert abs(fo - fr) <= 1e-9 * abs(fr), (fo, fr)
+    assert abs(ad - fr) <= 1e-5 * abs(fr), (ad, fr)
+
+
 def autograd_inputs(cfg):
     import torch
     from g3d.sim import sample_bunches
