@@ -134,10 +134,9 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     c.pl = std::move(pl);
 }
 
-// n = n0 f(z) g(r) for r < r_max (Config::plasma_density, src/sim_config.cpp:49-66; no density function)
-static double plasma_density(const PlasmaState& P, double x, double y, double z) {
-    const double r2 = x * x + y * y;
-    if (r2 >= P.cfg.r_max * P.cfg.r_max) return 0;
+// n = n0 f(z) g(r) for r < r_max (Config::plasma_density, src/sim_config.cpp:49-66; no density function): f(z),
+// the longitudinal profile, here; g(r) and the cut at r_max per lattice point on the device (lattice_point).
+static double density_zfactor(const PlasmaState& P, double z) {
     double f = 1;
     if (!P.zpts.empty()) {
         if (z <= P.zpts.front()) f = P.zvals.front();
@@ -149,84 +148,80 @@ static double plasma_density(const PlasmaState& P, double x, double y, double z)
             f = (1 - t) * P.zvals[k - 1] + t * P.zvals[k];
         }
     }
-    const double g = P.cfg.parabolic ? 1 + P.cfg.channel_depth * r2 / (P.cfg.r_channel * P.cfg.r_channel) : 1.0;
-    return f * g > 0 ? P.cfg.n0 * f * g : 0.0;
+    return f;
 }
 
 // Fresh plasma at the front of the window in the reference's order (load_plasma, src/sim_plasma.cpp:43-90):
 // rows j, cells i, sub-cells b2, a2; the electron, then the loaded ions of every species; then the particles
-// that join the march at their zeta.
+// that join the march at their zeta. The lattice is built on the device (k_lattice_flags / k_lattice_fill: the
+// points of positive density counted, their particles written at the running count, ids in list order); only
+// the joining particles come from the host.
 static void load_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
-    std::vector<g3d_particle> v;
-    long cap = 0;
-    const uint64_t id0 = uint64_t(c.istep + 1) << 32;
     const double zmid = 0.5 * (s0 + s1), Delta = s1 - s0;
-    const int nx = c.nx, ny = c.ny, px = P.cfg.ppc_x, py = P.cfg.ppc_y;
-    const double zf = c.zeta[size_t(c.N - 1)];
-    for (int j = 0; j < ny; ++j) {
-        double y0 = j * c.dy, hy = c.dy;
-        if (!c.yf) {                                     // free-hand y: no plasma in the cells at the walls
-            if (j == 0 || j == ny - 1) continue;
-            y0 = c.ynode_h[size_t(j)]; hy = c.ynode_h[size_t(j) + 1] - c.ynode_h[size_t(j)];
-        }
-        for (int i = 0; i < nx; ++i)
-            for (int b2 = 0; b2 < py; ++b2)
-                for (int a2 = 0; a2 < px; ++a2) {
-                    g3d_particle p{};
-                    p.x = (i + (a2 + 0.5) / px) * c.dx;
-                    p.y = y0 + (b2 + 0.5) / py * hy;
-                    const double n = plasma_density(P, p.x + c.X0, p.y + c.Y0, zmid);
-                    if (n <= 0) continue;
-                    p.w = n * c.dx * hy * Delta / (px * py);
-                    p.q = -1; p.qm = -1; p.sp = SP_PLASMA; p.alive = 1;
-                    p.zeta = zf; p.z = s0;
-                    if (P.cfg.free_electrons) { p.id = id0 + v.size(); v.push_back(p); }
-                    for (size_t k = 0; k < P.ions.size(); ++k) {
-                        const IonSpec& is = P.ions[k];
-                        if (!is.loaded()) continue;
-                        g3d_particle q = p;
-                        q.q = is.Z0; q.qm = is.Z0 / is.mass; q.w = is.atoms * p.w; q.sp = SP_ION + int(k);
-                        q.id = id0 + v.size();
-                        v.push_back(q);
-                    }
-                }
+    LatticeArgs a{};
+    a.nx = c.nx; a.px = P.cfg.ppc_x; a.py = P.cfg.ppc_y;
+    a.j0 = c.yf ? 0 : 1;                                 // free-hand y: no plasma in the cells at the walls
+    const long nrows = c.yf ? c.ny : c.ny - 2;
+    a.electrons = P.cfg.free_electrons ? 1 : 0;
+    a.dx = c.dx; a.dy = c.dy; a.X0 = c.X0; a.Y0 = c.Y0; a.Delta = Delta;
+    a.zf = c.zeta[size_t(c.N - 1)]; a.s0 = s0;
+    a.yn = c.yf ? nullptr : c.yn.p;
+    a.f = density_zfactor(P, zmid); a.n0 = P.cfg.n0;
+    a.rmax2 = P.cfg.r_max * P.cfg.r_max;
+    a.parabolic = P.cfg.parabolic ? 1 : 0;
+    a.depth = P.cfg.channel_depth; a.rc2 = P.cfg.r_channel * P.cfg.r_channel;
+    a.id0 = uint64_t(c.istep + 1) << 32;
+    long ion_cap = 0;                                    // freed-electron capacity per point (ionizing ions)
+    for (size_t k = 0; k < P.ions.size(); ++k) {
+        const IonSpec& is = P.ions[k];
+        if (!is.loaded()) continue;
+        if (a.nion == LAT_MAXION) throw Error(G3D_ERR_ARG, "more than 8 loaded ion species");
+        a.ion_atoms[a.nion] = is.atoms; a.ion_q[a.nion] = is.Z0; a.ion_qm[a.nion] = is.Z0 / is.mass;
+        a.ion_sp[a.nion] = SP_ION + int(k);
+        ++a.nion;
+        if (is.ionization) ion_cap += is.Zmax - is.Z0;
     }
-    P.fresh_last = long(v.size());
-    for (g3d_particle p : P.joining) { p.alive = 6; v.push_back(p); }
-    P.joining.clear();
-    for (const auto& p : v)
+    a.m = a.electrons + a.nion;
+    const long npts = nrows > 0 ? nrows * c.nx * a.px * a.py : 0;
+    const long pts = (npts > 0 && a.m > 0) ? launch_lattice_count(c, a, npts) : 0;
+    const long fresh = pts * a.m;
+    long cap = pts * ion_cap;
+    for (const auto& p : P.joining)
         if (p.sp >= SP_ION && p.sp < SP_FREED && P.ions[size_t(p.sp - SP_ION)].ionization)
             cap += P.ions[size_t(p.sp - SP_ION)].Zmax - std::lround(p.q);
-    P.nstrm = long(v.size());
+    const long n = fresh + long(P.joining.size());
+    P.fresh_last = fresh;
+    P.nstrm = n;
     P.born_cap = cap;
-    const long need = long(v.size()) + cap;
-    if (P.s.cap < need) {
-        const long n = need + need / 8 + 64;
-        P.s.alloc(n, c.stream);
+    const long need = n + cap;
+    if (P.s.cap < need) {             // half again: the list grows by the joining particles for some steps, and every
+        const long nn = need + need / 2 + 64;        // move of it costs a new capture of the slice loop's graph
+        P.s.alloc(nn, c.stream);
     }
     if (cap > 0 && P.bn.cap < cap) P.bn.alloc(cap, c.stream);
     P.strm = P.s.v;
     P.born = P.bn.v;
-    // upload as columns
-    const long n = long(v.size());
-    if (n) {
-        std::vector<double> hd(size_t(n) * 10);
-        std::vector<int32_t> hi(size_t(n) * 2);
-        std::vector<uint64_t> hu(static_cast<size_t>(n));
-        for (long k = 0; k < n; ++k) {
-            const g3d_particle& p = v[size_t(k)];
+    if (fresh) launch_lattice_fill(c, a, npts, P.strm);
+    const long nj = long(P.joining.size());
+    if (nj) {                                            // the joining particles after the lattice, as columns
+        std::vector<double> hd(size_t(nj) * 10);
+        std::vector<int32_t> hi(size_t(nj) * 2);
+        std::vector<uint64_t> hu(static_cast<size_t>(nj));
+        for (long k = 0; k < nj; ++k) {
+            const g3d_particle& p = P.joining[size_t(k)];
             const double vals[10] = {p.x, p.y, p.zeta, p.px, p.py, p.pz, p.w, p.z, p.q, p.qm};
-            for (int m = 0; m < 10; ++m) hd[size_t(m) * n + k] = vals[m];
-            hi[size_t(k)] = p.alive; hi[size_t(n) + k] = p.sp; hu[size_t(k)] = p.id;
+            for (int m = 0; m < 10; ++m) hd[size_t(m) * nj + k] = vals[m];
+            hi[size_t(k)] = 6; hi[size_t(nj) + k] = p.sp; hu[size_t(k)] = p.id;
         }
         double* cols[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
         for (int m = 0; m < 10; ++m)
-            G3D_CUDA(cudaMemcpyAsync(cols[m], hd.data() + size_t(m) * n, size_t(n) * 8, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.alive, hi.data(), size_t(n) * 4, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.sp, hi.data() + n, size_t(n) * 4, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.id, hu.data(), size_t(n) * 8, cudaMemcpyHostToDevice, c.stream));
+            G3D_CUDA(cudaMemcpyAsync(cols[m] + fresh, hd.data() + size_t(m) * nj, size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.alive + fresh, hi.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.sp + fresh, hi.data() + nj, size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.id + fresh, hu.data(), size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
     }
+    P.joining.clear();
     G3D_CUDA(cudaMemcpyAsync(P.nstrm_dev.p, &P.nstrm, sizeof(long), cudaMemcpyHostToDevice, c.stream));
     G3D_CUDA(cudaMemsetAsync(P.flags.p, 0, sizeof(int), c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
@@ -249,6 +244,32 @@ std::vector<g3d_particle> get_streaming(Ctx& c) {
     G3D_CUDA(cudaMemcpyAsync(hi.data(), P.strm.alive, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaMemcpyAsync(hi.data() + n, P.strm.sp, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaMemcpyAsync(hu.data(), P.strm.id, size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    for (long k = 0; k < n; ++k) {
+        g3d_particle& p = out[size_t(k)];
+        double* dst[10] = {&p.x, &p.y, &p.zeta, &p.px, &p.py, &p.pz, &p.w, &p.z, &p.q, &p.qm};
+        for (int m = 0; m < 10; ++m) *dst[m] = hd[size_t(m) * n + k];
+        p.alive = hi[size_t(k)]; p.sp = hi[size_t(n) + k]; p.id = hu[size_t(k)];
+    }
+    return out;
+}
+
+// The trapped streaming particles (alive == 5) in list order: compacted on the device, only they come to the host.
+static std::vector<g3d_particle> trapped_particles(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    const long n = P.s.cap > 0 ? launch_compact_state(c, P.strm, P.nstrm_dev.p, P.s.cap, 5) : 0;
+    std::vector<g3d_particle> out(static_cast<size_t>(n));
+    if (!n) return out;
+    const StrmDev& T = P.tr.v;
+    std::vector<double> hd(size_t(n) * 10);
+    std::vector<int32_t> hi(size_t(n) * 2);
+    std::vector<uint64_t> hu(static_cast<size_t>(n));
+    const double* cols[10] = {T.x, T.y, T.zeta, T.px, T.py, T.pz, T.w, T.z, T.q, T.qm};
+    for (int m = 0; m < 10; ++m)
+        G3D_CUDA(cudaMemcpyAsync(hd.data() + size_t(m) * n, cols[m], size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data(), T.alive, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data() + n, T.sp, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hu.data(), T.id, size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     for (long k = 0; k < n; ++k) {
         g3d_particle& p = out[size_t(k)];
@@ -392,9 +413,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     if (flag) throw Error(G3D_ERR_CAPACITY, "ionization: list of freed electrons overflowed");
     // trapped particles: fast ones join the beam list, slow ones stream again in the next step (counted on the
     // device first: the streaming particles come to the host only when some were trapped)
-    const bool any_trapped = count_state(c, P.strm.alive, 0, P.nstrm_dev.p, 5) > 0;
-    std::vector<g3d_particle> sv;
-    if (any_trapped) sv = get_streaming(c);
+    std::vector<g3d_particle> sv = trapped_particles(c);
     std::vector<g3d_particle> add;
     for (auto& p : sv) {
         if (p.alive != 5) continue;

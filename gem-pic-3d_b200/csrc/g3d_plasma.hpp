@@ -62,6 +62,24 @@ struct IonSpec {
     bool loaded() const { return mobile || ionization; }
 };
 
+// The fresh plasma lattice of a march (Simulation::load_plasma, src/sim_plasma.cpp:43-90) as the device builds it:
+// lattice point L runs over the rows j0 .. j0 + nrows - 1, cells i, sub-cells b2, a2 (a2 fastest); a point of
+// positive density gives m particles, the electron first (when free electrons are loaded), then one per loaded ion
+// species in order. Every product, quotient and sum below is the host's, in the host's order, so the particles
+// (and whether a point has any) are bit for bit those of the reference's loader.
+constexpr int LAT_MAXION = 8;
+struct LatticeArgs {
+    int nx, px, py, j0, electrons, nion;
+    long m;
+    double dx, dy, X0, Y0, Delta, zf, s0;
+    const double* yn;                          // free-hand y: the node positions (null: rows j dy, height dy)
+    double f, n0, rmax2, depth, rc2;           // density n0 f g(r) for r^2 < rmax2, g = 1 + depth r^2 / rc2
+    int parabolic;
+    double ion_atoms[LAT_MAXION], ion_q[LAT_MAXION], ion_qm[LAT_MAXION];
+    int ion_sp[LAT_MAXION];
+    uint64_t id0;
+};
+
 // A DevBuf-backed structure of arrays of streaming particles.
 struct StrmBuf {
     DevBuf<double> d;          // 10 columns
@@ -96,6 +114,11 @@ struct PlasmaState {
     DevBuf<IonDevC> ion_dev;
     DevBuf<AdkDev> adk_dev;
     std::vector<g3d_particle> joining;         // join the next march at their zeta
+    // scratch of the lattice build and of the compaction of trapped particles: flags and their exclusive sums
+    // (one entry more than the items), the scan's temporary storage, the trapped particles in list order
+    DevBuf<int> cflag, coff;
+    DevBuf<unsigned char> ctmp;
+    StrmBuf tr;
     // the slice loop of a march as CUDA graphs, keyed by what they hold by value (two alternate: the j0 / jk
     // buffers swap every step); captured again only when a buffer moved
     struct LoopGraph { uint64_t key; cudaGraphExec_t exec; long launches; };
@@ -123,5 +146,12 @@ void launch_born_append(Ctx& c);
 // number of particles with alive == state among n (n_dev: the count on the device instead, when not null)
 long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state);
 void launch_real_fields_slice(Ctx& c, int l, FmidOut fm = FmidOut());
+// the lattice points of positive density among npts (their running count into P.coff); returns how many
+long launch_lattice_count(Ctx& c, const LatticeArgs& a, long npts);
+// the fresh particles of those points into S[0 .. count m)
+void launch_lattice_fill(Ctx& c, const LatticeArgs& a, long npts, StrmDev S);
+// the particles with alive == state among the device count n_dev of S (at most cap), in list order, into P.tr;
+// returns how many
+long launch_compact_state(Ctx& c, const StrmDev& S, const long* n_dev, long cap, int state);
 
 }  // namespace g3d

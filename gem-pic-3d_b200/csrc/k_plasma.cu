@@ -18,6 +18,7 @@
 // After the passes: k_correct (R of slice n+1 corrected for the prediction it used; dl, js0 updated,
 // sim_plasma.cpp:381-403) and k_born_append (the freed electrons join the march).
 #include <type_traits>
+#include <cub/device/device_scan.cuh>
 #include "g3d_plasma.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -728,6 +729,69 @@ __global__ void k_count_state(const int32_t* __restrict__ alive, long n, const l
     if ((threadIdx.x & 31) == 0 && k) atomicAdd(out, k);
 }
 
+// ---------------------------------------------------------------- the fresh plasma lattice
+// Lattice point L: its position (x, y), row height hy and density n with the host loader's operations, no
+// contraction into FMAs (the host code has none), so the same points get particles and the same values.
+__device__ __forceinline__ void lattice_point(const LatticeArgs& a, long L, double& x, double& y, double& hy, double& n) {
+    const int a2 = int(L % a.px);
+    long r = L / a.px;
+    const int b2 = int(r % a.py);
+    r /= a.py;
+    const int i = int(r % a.nx), j = a.j0 + int(r / a.nx);
+    double y0 = __dmul_rn(double(j), a.dy);
+    hy = a.dy;
+    if (a.yn) { y0 = a.yn[j]; hy = __dsub_rn(a.yn[j + 1], a.yn[j]); }
+    x = __dmul_rn(__dadd_rn(double(i), __ddiv_rn(__dadd_rn(double(a2), 0.5), double(a.px))), a.dx);
+    y = __dadd_rn(y0, __dmul_rn(__ddiv_rn(__dadd_rn(double(b2), 0.5), double(a.py)), hy));
+    const double xx = __dadd_rn(x, a.X0), yy = __dadd_rn(y, a.Y0);
+    const double r2 = __dadd_rn(__dmul_rn(xx, xx), __dmul_rn(yy, yy));
+    n = 0;
+    if (r2 >= a.rmax2) return;
+    const double g = a.parabolic ? __dadd_rn(1.0, __ddiv_rn(__dmul_rn(a.depth, r2), a.rc2)) : 1.0;
+    if (__dmul_rn(a.f, g) > 0) n = __dmul_rn(__dmul_rn(a.n0, a.f), g);
+}
+__global__ void k_lattice_flags(LatticeArgs a, long npts, int* __restrict__ flag) {
+    for (long L = long(blockIdx.x) * blockDim.x + threadIdx.x; L <= npts; L += long(gridDim.x) * blockDim.x) {
+        if (L == npts) { flag[L] = 0; continue; }
+        double x, y, hy, n;
+        lattice_point(a, L, x, y, hy, n);
+        flag[L] = n > 0;
+    }
+}
+__global__ void k_lattice_fill(LatticeArgs a, long npts, const int* __restrict__ off, StrmDev S) {
+    for (long L = long(blockIdx.x) * blockDim.x + threadIdx.x; L < npts; L += long(gridDim.x) * blockDim.x) {
+        double x, y, hy, n;
+        lattice_point(a, L, x, y, hy, n);
+        if (!(n > 0)) continue;
+        const double w = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(n, a.dx), hy), a.Delta), double(a.px * a.py));
+        long k = long(off[L]) * a.m;
+        auto put = [&](double ww, double q, double qm, int sp) {
+            S.x[k] = x; S.y[k] = y; S.zeta[k] = a.zf; S.px[k] = 0; S.py[k] = 0; S.pz[k] = 0;
+            S.w[k] = ww; S.z[k] = a.s0; S.q[k] = q; S.qm[k] = qm; S.alive[k] = 1; S.sp[k] = sp;
+            S.id[k] = a.id0 + uint64_t(k);
+            ++k;
+        };
+        if (a.electrons) put(w, -1, -1, SP_PLASMA);
+        for (int t = 0; t < a.nion; ++t) put(__dmul_rn(a.ion_atoms[t], w), a.ion_q[t], a.ion_qm[t], a.ion_sp[t]);
+    }
+}
+// ---------------------------------------------------------------- particles of one state, in list order
+__global__ void k_state_flags(const int32_t* __restrict__ alive, const long* __restrict__ n_dev, long cap, int state,
+                              int* __restrict__ flag) {
+    const long n = *n_dev < cap ? *n_dev : cap;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i <= cap; i += long(gridDim.x) * blockDim.x)
+        flag[i] = i < n && alive[i] == state;
+}
+__global__ void k_state_gather(StrmDev S, const int* __restrict__ flag, const int* __restrict__ off, long cap, StrmDev T) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += long(gridDim.x) * blockDim.x) {
+        if (!flag[i]) continue;
+        const long k = off[i];
+        T.x[k] = S.x[i]; T.y[k] = S.y[i]; T.zeta[k] = S.zeta[i]; T.px[k] = S.px[i]; T.py[k] = S.py[i]; T.pz[k] = S.pz[i];
+        T.w[k] = S.w[i]; T.z[k] = S.z[i]; T.q[k] = S.q[i]; T.qm[k] = S.qm[i]; T.alive[k] = S.alive[i]; T.sp[k] = S.sp[i];
+        T.id[k] = S.id[i];
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static unsigned ew_blocks(long n) {
     long b = (n + 255) / 256;
@@ -783,6 +847,49 @@ void launch_real_to_half3(Ctx& c, const double* J3, cpx* T3, cpx* out3) {
     if (!c.yf) { G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J, out3))); return; }
     G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, J, T3)));
     G3D_DISPATCH_N(c.ny, NY, ss_cols<NY>(c, T3, out3, 0.0, 1, 0));
+}
+
+// exclusive running sum of P.cflag[0 .. n] into P.coff (n + 1 entries); returns the total (a synchronisation)
+static long scan_flags(Ctx& c, long n) {
+    PlasmaState& P = *c.pl;
+    if (n + 1 > 0x7fffffffL) throw Error(G3D_ERR_CAPACITY, "more than 2^31 items in one compaction");
+    size_t tb = 0;
+    G3D_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, P.cflag.p, P.coff.p, int(n + 1), c.stream));
+    if (P.ctmp.n < tb) P.ctmp.alloc(tb, c.stream);
+    G3D_CUDA(cub::DeviceScan::ExclusiveSum(P.ctmp.p, tb, P.cflag.p, P.coff.p, int(n + 1), c.stream));
+    int h = 0;
+    G3D_CUDA(cudaMemcpyAsync(&h, P.coff.p + n, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return h;
+}
+static void reserve_flags(Ctx& c, long n) {
+    PlasmaState& P = *c.pl;
+    if (long(P.cflag.n) < n + 1) {
+        P.cflag.alloc(size_t(n + 1) + size_t(n + 1) / 8, c.stream);
+        P.coff.alloc(P.cflag.n, c.stream);
+    }
+}
+long launch_lattice_count(Ctx& c, const LatticeArgs& a, long npts) {
+    reserve_flags(c, npts);
+    k_lattice_flags<<<ew_blocks(npts + 1), 256, 0, c.stream>>>(a, npts, c.pl->cflag.p);
+    c.check_launch("k_lattice_flags");
+    return scan_flags(c, npts);
+}
+void launch_lattice_fill(Ctx& c, const LatticeArgs& a, long npts, StrmDev S) {
+    k_lattice_fill<<<ew_blocks(npts), 256, 0, c.stream>>>(a, npts, c.pl->coff.p, S);
+    c.check_launch("k_lattice_fill");
+}
+long launch_compact_state(Ctx& c, const StrmDev& S, const long* n_dev, long cap, int state) {
+    PlasmaState& P = *c.pl;
+    reserve_flags(c, cap);
+    k_state_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(S.alive, n_dev, cap, state, P.cflag.p);
+    c.check_launch("k_state_flags");
+    const long n = scan_flags(c, cap);
+    if (n == 0) return 0;
+    if (P.tr.cap < n) P.tr.alloc(n + n / 4 + 64, c.stream);
+    k_state_gather<<<ew_blocks(cap), 256, 0, c.stream>>>(S, P.cflag.p, P.coff.p, cap, P.tr.v);
+    c.check_launch("k_state_gather");
+    return n;
 }
 
 long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state) {
