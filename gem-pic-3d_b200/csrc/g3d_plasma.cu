@@ -103,7 +103,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     const size_t ph = size_t(c.nkh);
     for (DevBuf<cpx>* b : {&pl->js0x, &pl->js0y, &pl->js0z}) b->alloc(size_t(c.ns + 1) * ph, s);
     pl->jsr.alloc(size_t(5) * c.nk, s);
-    pl->jsrf.alloc(size_t(5) * c.nk, s);
+    pl->jsrf.alloc(size_t(5) * c.nk, s);               // FP32: three planes, or on the Fourier y grid (jx, jy, jz, 0) per point
     if (c.yf) pl->fmid.alloc(size_t(6) * c.nk, s);      // 6 doubles or 8 floats per point
     pl->stepv.alloc(1, s);
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
@@ -337,7 +337,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         const bool fh = !c.yf;
         // the deposit planes and the count of freed electrons start cleared (the rows kernel of every pass clears
         // them again for the next one)
-        if (c.f32s) G3D_CUDA(cudaMemsetAsync(P.jsrf.p, 0, size_t(3) * c.nk * sizeof(float), c.stream));
+        if (c.f32s) G3D_CUDA(cudaMemsetAsync(P.jsrf.p, 0, size_t(c.yf ? 4 : 3) * c.nk * sizeof(float), c.stream));
         else G3D_CUDA(cudaMemsetAsync(P.jsr.p, 0, size_t(3) * c.nk * sizeof(double), c.stream));
         G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
         // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it

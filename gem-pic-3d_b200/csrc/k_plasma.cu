@@ -134,7 +134,8 @@ __device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? 
 // TSC deposit of f v at (x, y) into jsr: jx, jy, jz (stream_deposit, sim_stream.hpp:33-64). The reference also
 // deposits the charge of negative and positive particles into planes 3 and 4; those feed only its density
 // diagnostics (rho_lines, openPMD n_e / n_i), which this build does not write, so they are left out. F32: into the
-// FP32 planes.
+// FP32 planes; on the Fourier y grid interleaved per point as (jx, jy, jz, 0), one vector atomic add per TSC
+// point instead of three (the adds into L2 bound the streaming push).
 template <bool F32>
 __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
     const Geo& g = c.g;
@@ -175,8 +176,7 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
             const long k = long(jn[v]) * g.nx + ix_[u];
             const double w = f * wx[u] * wn[v] * ia0;
             if constexpr (F32) {
-                atomicAdd(&c.Jf[k], float(w * vx)); atomicAdd(&c.Jf[nk + k], float(w * vy));
-                atomicAdd(&c.Jf[2 * nk + k], float(w * vz));
+                atomicAdd(reinterpret_cast<float4*>(c.Jf) + k, make_float4(float(w * vx), float(w * vy), float(w * vz), 0.f));
             } else {
                 atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
             }
@@ -389,8 +389,14 @@ __global__ void __launch_bounds__(128) k_ss_rows(Geo g, JT* __restrict__ J, cpx*
         double jx = 0, jy = 0, jz = 0;
         if (row < g.ny) {
             const long i = long(row) * NX + p;
-            jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i];
-            if (clear) { J[i] = JT(0); J[nk + i] = JT(0); J[2 * nk + i] = JT(0); }     // for the next pass's deposit
+            if constexpr (std::is_same<JT, float4>::value) {            // interleaved per point (FP32, Fourier y)
+                const float4 v = J[i];
+                jx = v.x; jy = v.y; jz = v.z;
+                if (clear) J[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            } else {
+                jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i];
+                if (clear) { J[i] = JT(0); J[nk + i] = JT(0); J[2 * nk + i] = JT(0); }     // for the next pass's deposit
+            }
         }
         a0[rr * RS + p + (p >> 3)] = C(jx, jy);
         a1[rr * RS + p + (p >> 3)] = C(jz, 0.0);
@@ -831,7 +837,10 @@ void launch_stream_spectra(Ctx& c) {
     const int tok = c.prof_begin("stream_spectra");
     PlasmaState& P = *c.pl;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
-    if (c.f32s) {
+    if (c.f32s && c.yf) {
+        float4* J4 = reinterpret_cast<float4*>(P.jsrf.p);
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float4>(c, J4, P.tsp.p, 1, P.bcnt.p)));
+    } else if (c.f32s) {
         G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float>(c, P.jsrf.p, P.tsp.p, 1, P.bcnt.p)));
     } else {
         G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p, 1, P.bcnt.p)));
