@@ -265,10 +265,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     cpx* a2 = sm + 2 * LPC * RS;
     const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
-    #pragma unroll 1
-    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {      // unrolled: the loads of all elements in flight
         const int e = tid + u_ * NT;
-        if (e >= LPC * H) break;
+        if (e >= LPC * H) continue;
         const int r = e / H, p = e - r * H, row = r0 + r;
         cpx v[6] = {C(0), C(0), C(0), C(0), C(0), C(0)};
         if (row < g.ny) {

@@ -367,10 +367,10 @@ __global__ void __launch_bounds__(CWT * FftShape<NY>::T) k_rf_cols_f(Geo g, cons
     cpxf* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     cpxf* s0 = smf;
     cpxf* s1 = smf + ColTile<NY, CWT>::size;
-    #pragma unroll 1
-    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * CWT + nthr - 1) / nthr; ++u_) {      // unrolled: the loads of all elements in flight
         const int e = tid + u_ * nthr;
-        if (e >= NY * CWT) break;
+        if (e >= NY * CWT) continue;
         const int p = e / CWT, c = e - p * CWT, kxi = c0 + c;
         const long o = base + long(p) * H + kxi;
         cpxf a = Cf(0), b = Cf(0);

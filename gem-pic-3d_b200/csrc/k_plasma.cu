@@ -384,22 +384,39 @@ __global__ void __launch_bounds__(128) k_ss_rows(Geo g, JT* __restrict__ J, cpx*
     cpx* a1 = sm + LPC * RS;
     const int tid = threadIdx.x, r0 = blockIdx.x * LPC;
     const long nk = g.nk;
-    for (int e = tid; e < LPC * NX; e += 128) {
-        const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
-        double jx = 0, jy = 0, jz = 0;
+    // every load first, then the clears for the next pass's deposit, then shared memory: a clear between two loads
+    // would keep the second waiting for the first (the compiler cannot move a load above a store it may alias)
+    constexpr int EPT = LPC * NX / 128;
+    double jx[EPT], jy[EPT], jz[EPT];
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+        const int e = tid + u * 128, rr = e / NX, p = e - rr * NX, row = r0 + rr;
+        jx[u] = jy[u] = jz[u] = 0;
         if (row < g.ny) {
             const long i = long(row) * NX + p;
             if constexpr (std::is_same<JT, float4>::value) {            // interleaved per point (FP32, Fourier y)
                 const float4 v = J[i];
-                jx = v.x; jy = v.y; jz = v.z;
-                if (clear) J[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                jx[u] = v.x; jy[u] = v.y; jz[u] = v.z;
             } else {
-                jx = J[i]; jy = J[nk + i]; jz = J[2 * nk + i];
-                if (clear) { J[i] = JT(0); J[nk + i] = JT(0); J[2 * nk + i] = JT(0); }     // for the next pass's deposit
+                jx[u] = J[i]; jy[u] = J[nk + i]; jz[u] = J[2 * nk + i];
             }
         }
-        a0[rr * RS + p + (p >> 3)] = C(jx, jy);
-        a1[rr * RS + p + (p >> 3)] = C(jz, 0.0);
+    }
+    if (clear) {
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+            const int e = tid + u * 128, rr = e / NX, p = e - rr * NX, row = r0 + rr;
+            if (row >= g.ny) continue;
+            const long i = long(row) * NX + p;
+            if constexpr (std::is_same<JT, float4>::value) J[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            else { J[i] = JT(0); J[nk + i] = JT(0); J[2 * nk + i] = JT(0); }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+        const int e = tid + u * 128, rr = e / NX, p = e - rr * NX;
+        a0[rr * RS + p + (p >> 3)] = C(jx[u], jy[u]);
+        a1[rr * RS + p + (p >> 3)] = C(jz[u], 0.0);
     }
     if (bcnt && blockIdx.x == 0 && tid == 0) *bcnt = 0;          // the freed electrons of the next pass
     __syncthreads();
@@ -431,8 +448,9 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_ss_cols(Geo g, const c
     cpx* s1 = sm + ColTile<NY, CW>::size;
     cpx* s2 = sm + 2 * ColTile<NY, CW>::size;
     const int c0 = blockIdx.x * CW, tid = threadIdx.x, nthr = CW * S::T, H = g.H;
-    for (int e = tid; e < NY * CW; e += nthr) {
-        const int p = e / CW, c = e - p * CW, kx = c0 + c;
+#pragma unroll
+    for (int u = 0; u < NY / S::T; ++u) {      // unrolled: the loads of all elements in flight together
+        const int e = tid + u * nthr, p = e / CW, c = e - p * CW, kx = c0 + c;
         cpx u0 = C(0), u1 = C(0), u2 = C(0);
         if (kx < H) { const long o = long(p) * H + kx; u0 = T0[o]; u1 = T1[o]; u2 = T2[o]; }
         s0[ColTile<NY, CW>::at(p, c)] = u0; s1[ColTile<NY, CW>::at(p, c)] = u1; s2[ColTile<NY, CW>::at(p, c)] = u2;
