@@ -715,15 +715,39 @@ __global__ void k_slice_prologue(PlasmaPtrs p, cpx* __restrict__ sin_, cpx* __re
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x)
         slice_prologue_mode<T>(p, sin_, si0, bk, Rx, Ry, Ez, Bz, o, pred_m, copy_in, backup, i);
 }
-// half-cell n final (correct) and the prologue of half-cell n-1, per mode in one thread: the correction reads si0
-// before the prologue refills it, the prologue's slice n-1 is not touched by the correction (slice n+1)
+// half-cell n final (correct_mode) and the prologue of half-cell n-1 (slice_prologue_mode, copy_in), per mode in
+// one thread. Every value is loaded before anything is stored: the correction reads si0 before the prologue
+// refills it, the prologue's slice n-1 and half-cell n-1 are not touched by the correction (slice n+1, half-cell
+// n), and pin and jk are each read before they are written; so the stores see the values of the sequential
+// code, and the ~26 loads of a mode wait together instead of behind stores they might alias.
 template <class T>
 __global__ void k_correct_prologue(PlasmaPtrs p, cpx* __restrict__ Rx, cpx* __restrict__ Ry, int n, double q, int own,
                                    cpx* __restrict__ sin_, cpx* __restrict__ si0, cpx* __restrict__ bk, const T* __restrict__ Ez,
                                    const T* __restrict__ Bz, long o_next, int pred_m, int backup) {
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < p.nkh; i += long(gridDim.x) * blockDim.x) {
-        correct_mode(p, Rx, Ry, n, q, own, i);
-        slice_prologue_mode<T>(p, sin_, si0, bk, Rx, Ry, Ez, Bz, o_next, pred_m, 1, backup, i);
+    const long nkh = p.nkh, hp = long(n + 1) * nkh, hm = long(pred_m + 1) * nkh;
+    cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
+    T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
+    const bool pred = pred_m >= 0;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        cpx u[3], sh[3], pn[3], t[3], jm[3], sx = C(0), sy = C(0), rx = C(0), ry = C(0);
+        cpx b0 = C(0), b1 = C(0), b2 = C(0), b3 = C(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            u[k] = p.jsn[k * nkh + i]; sh[k] = s0[k][hp + i]; pn[k] = p.pin[k * nkh + i];
+            t[k] = pred ? s0[k][hm + i] : C(0);
+            jm[k] = pred ? widen(jk[k][hm + i]) : C(0);
+        }
+        if (own) { sx = p.si0[i]; sy = p.si0[nkh + i]; rx = Rx[hp + i]; ry = Ry[hp + i]; }
+        if (backup) { b0 = Rx[o_next + i]; b1 = Ry[o_next + i]; b2 = widen(Ez[o_next + i]); b3 = widen(Bz[o_next + i]); }
+        if (own) { Rx[hp + i] = rx - q * (u[0] - sx); Ry[hp + i] = ry - q * (u[1] - sy); }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            p.dl[k * nkh + i] = u[k] - sh[k];
+            s0[k][hp + i] = u[k];
+            sin_[k * nkh + i] = pn[k]; si0[k * nkh + i] = pn[k];
+            if (pred) { jk[k][hm + i] = narrow<T>(jm[k] + t[k]); p.pin[k * nkh + i] = t[k]; }
+        }
+        if (backup) { bk[i] = b0; bk[nkh + i] = b1; bk[2 * nkh + i] = b2; bk[3 * nkh + i] = b3; }
     }
 }
 // Start of a pass on the free-hand y grid: the slice restored from the backup (restore), the streaming-current
