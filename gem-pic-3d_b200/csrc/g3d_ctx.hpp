@@ -222,10 +222,16 @@ struct FmidOut {
     void* out = nullptr;
     int other = 0, f32 = 0;
 };
-__device__ __forceinline__ void fmid_store(const FmidOut& fm, const float* F, long fpl, long nk, long k, const float v[6]) {
+// the other slice's six values at point k (loaded by the rows kernel before it stores its own slice: the other
+// slice is never this one, so the loads need not wait behind those stores)
+__device__ __forceinline__ void fmid_load(const FmidOut& fm, const float* F, long fpl, long nk, long k, float o[6]) {
+#pragma unroll
+    for (int comp = 0; comp < 6; ++comp) o[comp] = F[comp * fpl + long(fm.other) * nk + k];
+}
+__device__ __forceinline__ void fmid_store(const FmidOut& fm, long k, const float v[6], const float oth[6]) {
     double m[6];
 #pragma unroll
-    for (int comp = 0; comp < 6; ++comp) m[comp] = 0.5 * (double(v[comp]) + double(F[comp * fpl + long(fm.other) * nk + k]));
+    for (int comp = 0; comp < 6; ++comp) m[comp] = 0.5 * (double(v[comp]) + double(oth[comp]));
     if (fm.f32) {
         float4* o = reinterpret_cast<float4*>(fm.out) + 2 * k;
         o[0] = make_float4(float(m[0]), float(m[1]), float(m[2]), float(m[3]));

@@ -265,6 +265,16 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     cpx* a2 = sm + 2 * LPC * RS;
     const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
+    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
+    constexpr int EO = (LPC * NX + NT - 1) / NT;                    // output elements of a thread
+    float oth[EO][6];                                               // the midpoint fields' other slice
+    if (fm.out) {
+    #pragma unroll
+        for (int u_ = 0; u_ < EO; ++u_) {
+            const int e = tid + u_ * NT, rr = e / NX, p = e - rr * NX, row = r0 + rr;
+            if (e < LPC * NX && row < g.ny) fmid_load(fm, F, fpl, g.nk, long(row) * NX + p, oth[u_]);
+        }
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {      // unrolled: the loads of all elements in flight
         const int e = tid + u_ * NT;
@@ -287,11 +297,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
         fft_lines<NX, 3>(ls_, RowAddr{r * RS}, t, g.twx);
     }
     const double s = g.yf ? 1.0 / double(g.nk) : 1.0 / double(g.nx);   // free-hand y: rows only, 1/nx
-    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
-    #pragma unroll 1
-    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+    #pragma unroll
+    for (int u_ = 0; u_ < EO; ++u_) {
         const int e = tid + u_ * NT;
-        if (e >= LPC * NX) break;
+        if (e >= LPC * NX) continue;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
         const int q = rr * RS + p + (p >> 3);
@@ -302,7 +311,7 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
                              float(0.5 * (l2 - r2)), float(0.5 * (r1 - l1)), float(z3.y)};  // B_x, B_y, B_z
 #pragma unroll
         for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
-        if (fm.out) fmid_store(fm, F, fpl, g.nk, long(row) * NX + p, fv);
+        if (fm.out) fmid_store(fm, long(row) * NX + p, fv, oth[u_]);
         if (Fd) {                                      // exact fields: the same values before the rounding
             Fd[0 * fpl + idx] = 0.5 * (r1 + l1); Fd[1 * fpl + idx] = 0.5 * (r2 + l2);
             Fd[3 * fpl + idx] = 0.5 * (l2 - r2); Fd[4 * fpl + idx] = 0.5 * (r1 - l1);

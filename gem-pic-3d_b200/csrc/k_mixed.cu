@@ -409,6 +409,16 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
     const int l = l0 + blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
     const long base = long(l) * g.nkh;
     const cpxf* in[6] = {W0, W1, W2, W3, W4, W5};
+    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
+    constexpr int EO = (LPC * NX + NT - 1) / NT;                    // output elements of a thread
+    float oth[EO][6];                                               // the midpoint fields' other slice
+    if (fm.out) {
+    #pragma unroll
+        for (int u_ = 0; u_ < EO; ++u_) {
+            const int e = tid + u_ * NT, rr = e / NX, p = e - rr * NX, row = r0 + rr;
+            if (e < LPC * NX && row < g.ny) fmid_load(fm, F, fpl, g.nk, long(row) * NX + p, oth[u_]);
+        }
+    }
     #pragma unroll
     for (int u_ = 0; u_ < (LPC * H + NT - 1) / NT; ++u_) {
         const int e = tid + u_ * NT;
@@ -425,11 +435,10 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
     const int r = tid / S::T, t = tid - r * S::T;
     fft_lines<NX, 3>(a, RowAddr{r * RS}, t, tw);
     const float s = 1.0f / float(g.nk);
-    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     #pragma unroll
-    for (int u_ = 0; u_ < (LPC * NX + NT - 1) / NT; ++u_) {
+    for (int u_ = 0; u_ < EO; ++u_) {
         const int e = tid + u_ * NT;
-        if (e >= LPC * NX) break;
+        if (e >= LPC * NX) continue;
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
         const int q = rr * RS + p + (p >> 3);
@@ -439,7 +448,7 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
                              0.5f * (z2.y - z1.y), 0.5f * (z1.x - z2.x), z3.y};     // B_x, B_y, B_z
 #pragma unroll
         for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
-        if (fm.out) fmid_store(fm, F, fpl, g.nk, long(row) * NX + p, fv);
+        if (fm.out) fmid_store(fm, long(row) * NX + p, fv, oth[u_]);
     }
 }
 
