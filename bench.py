@@ -116,14 +116,18 @@ def algorithmic_bytes(name, cfg, mixed=False, S=0):
     correct = (48 + 32 + 32 + 48 + 32 + 48 + 48) * nkh  # jsn, si0, R, js0 read; R, dl, js0 written
     plasma = {
         "stream": 144 * S + fm * nk + 3 * cr * nk,
-        # three real planes read and cleared; scratch; jsn (complex128)
-        "stream_spectra": 2 * 3 * cr * nk + (2 * 48 + 3 * cz) * nkh,
+        # Fourier y: the rows alone: the deposit planes read and cleared (FP32: (jx, jy, jz, 0) per point), three
+        # complex128 half rows written
+        "stream_spectra": 2 * (16 if mixed else 24) * nk + 48 * nkh,
+        # the fused column work of a pass: the half rows read, jsn written, the replace and march of the slice
+        # (less its read of jsn), the six column transforms of the slice's fields written (their inputs stay in
+        # shared memory)
+        "pass_cols": 48 * nkh + 48 * nkh + replace_pred + march_slice - 48 * nkh + 6 * cz * nkh,
         "march_slice": march_slice,
         "real_cols_slice": (2 * 16 + 4 * cz + 6 * cz) * nkh,
         # six column transforms read, F written; the other F plane read and the midpoint fields written
         "real_rows_slice": 6 * cz * nkh + 24 * nk + (24 + fm) * nk,
         "replace_pred": replace_pred,
-        "replace_march": replace_pred + march_slice,
         "slice_prologue": slice_prologue,
         "correct_prologue": correct + slice_prologue,
         "pass_prologue": 3 * cr * nk + 64 * nkh,

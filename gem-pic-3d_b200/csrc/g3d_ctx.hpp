@@ -274,7 +274,7 @@ void launch_full_to_half_f(Ctx& c, const cpx* full, cpxf* half, long planes);
 void launch_rotate_f(Ctx& c, cpxf* p, size_t n, double sx, double sy, int nys);
 void launch_copy_f(Ctx& c, cpxf* y, const cpxf* x, size_t n);
 void launch_axpy_fc(Ctx& c, cpxf* y, const cpx* x, double a, size_t n);   // y = y + a x
-void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm = FmidOut());
+void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm = FmidOut(), bool cols = true);   // cols false: rows only (W given)
 // particles and plasma (g3d_host.cu, g3d_plasma.cu)
 void set_particles(Ctx& c, const g3d_particle* v, long n);
 std::vector<g3d_particle> get_particles(Ctx& c);

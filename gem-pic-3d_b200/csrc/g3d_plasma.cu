@@ -290,7 +290,7 @@ static uint64_t mix64h(uint64_t z) {
 
 // E and B of slice l; Fourier y: with the midpoint fields of slice `target` (l for the next pass of half-cell l,
 // l - 1 for the first pass of half-cell l - 1, -1: none) for the streaming gather
-static void real_fields_slice(Ctx& c, int l, int target = -1) {
+static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true) {
     if (!c.yf) { launch_real_fields_slice_fh(c, l); return; }
     FmidOut fm;
     if (target >= c.a) {
@@ -298,8 +298,8 @@ static void real_fields_slice(Ctx& c, int l, int target = -1) {
         fm.other = (target == l ? l + 1 : l - 1) - c.a;
         fm.f32 = c.f32s ? 1 : 0;
     }
-    if (c.mixed) launch_real_fields_slice_f(c, l, fm);
-    else launch_real_fields_slice(c, l, fm);
+    if (c.mixed) launch_real_fields_slice_f(c, l, fm, cols);
+    else launch_real_fields_slice(c, l, fm, cols);
 }
 
 void march_plasma(Ctx& c, double s0, double s1) {
@@ -366,10 +366,16 @@ void march_plasma(Ctx& c, double s0, double s1) {
                 launch_stream(c, sa);
                 // freed electrons join the march (after the last pass's stream, before its rows kernel clears the count)
                 if (ionz && pass + 1 == passes) launch_born_append(c);
-                launch_stream_spectra(c);
-                if (!fh) launch_replace_march(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
-                else { launch_replace_pred(c, n, extrap ? 1 : 0, wex); launch_march_slice(c, D, n); }
-                real_fields_slice(c, n, pass + 1 < passes ? n : n - 1);
+                if (!fh) {                     // rows of the current's spectra; columns, march and field columns fused
+                    launch_stream_spectra_rows(c);
+                    launch_pass_cols(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
+                    real_fields_slice(c, n, pass + 1 < passes ? n : n - 1, false);
+                } else {
+                    launch_stream_spectra(c);
+                    launch_replace_pred(c, n, extrap ? 1 : 0, wex);
+                    launch_march_slice(c, D, n);
+                    real_fields_slice(c, n, pass + 1 < passes ? n : n - 1);
+                }
             }
             // half-cell n is final: correct R at slice n+1, keep the change and the current
             const double q = D * c.wlo_h[size_t(n + 1)];

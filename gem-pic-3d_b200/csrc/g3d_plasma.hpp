@@ -135,8 +135,11 @@ struct PlasmaState {
 void launch_stream(Ctx& c, const StreamArgs& a);
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
 void launch_pass_prologue(Ctx& c, int n, int restore);
-void launch_replace_march(Ctx& c, double D, int n, int extrap, double w, int restore);
 void launch_stream_spectra(Ctx& c);
+// Fourier y: the rows of the streaming current's spectra, then the fused column work of a pass (the current's
+// y transforms and filters, the replace and march of slice n, the y transforms of slice n's fields into W)
+void launch_stream_spectra_rows(Ctx& c);
+void launch_pass_cols(Ctx& c, double D, int n, int extrap, double w, int restore);
 void launch_replace(Ctx& c, int m, cpx* old, const cpx* nw);
 void launch_replace_pred(Ctx& c, int n, int extrap, double w);
 void launch_correct(Ctx& c, int n, double q, int own);
@@ -145,7 +148,7 @@ void launch_march_slice(Ctx& c, double D, int n);
 void launch_born_append(Ctx& c);
 // number of particles with alive == state among n (n_dev: the count on the device instead, when not null)
 long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state);
-void launch_real_fields_slice(Ctx& c, int l, FmidOut fm = FmidOut());
+void launch_real_fields_slice(Ctx& c, int l, FmidOut fm = FmidOut(), bool cols = true);     // cols false: rows only (W given)
 // the lattice points of positive density among npts (their running count into P.coff); returns how many
 long launch_lattice_count(Ctx& c, const LatticeArgs& a, long npts);
 // the fresh particles of those points into S[0 .. count m)

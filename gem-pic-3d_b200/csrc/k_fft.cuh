@@ -154,6 +154,60 @@ __device__ __forceinline__ void fft_lines(T* const* sm, const Addr& A, int t, co
     for (int s = 0; s < S::NR8; ++s) { fft_pass_multi<N, 8, NL>(sm, A, t, L, tw); L *= 8; }
 }
 
+// The same transform in a CTA that has more threads than it needs: only the threads with act (t < FftShape<N>::T
+// per line set) load, compute and store; every thread of the CTA takes part in the barriers. For kernels with one
+// thread per mode of a column around the transform.
+template <int N, int R, int NL, class Addr, class T>
+__device__ __forceinline__ void fft_pass_multi_some(T* const* sm, const Addr& A, int t, int L, const T* __restrict__ tw, bool act) {
+    constexpr int E = FftShape<N>::E, TT = FftShape<N>::T, BPT = E / R;
+    const int m = N / (L * R);
+    T v[NL][E];
+    if (act) {
+#pragma unroll
+        for (int u = 0; u < BPT; ++u) {
+            const int b = t + u * TT, j = b / L, k = b - j * L;
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                const int a = A((q * m + j) * L + k);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) v[l][u * R + q] = sm[l][a];
+            }
+            if (L > 1) {
+#pragma unroll
+                for (int q = 1; q < R; ++q) {
+                    const T w = __ldg(&tw[q * k * m]);
+#pragma unroll
+                    for (int l = 0; l < NL; ++l) v[l][u * R + q] = v[l][u * R + q] * w;
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < NL; ++l) dft<R>(&v[l][u * R]);
+        }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int u = 0; u < BPT; ++u) {
+            const int b = t + u * TT, j = b / L, k = b - j * L;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int a = A((j * R + r) * L + k);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) sm[l][a] = v[l][u * R + r];
+            }
+        }
+    }
+    __syncthreads();
+}
+template <int N, int NL, class Addr, class T>
+__device__ __forceinline__ void fft_lines_some(T* const* sm, const Addr& A, int t, const T* __restrict__ tw, bool act) {
+    using S = FftShape<N>;
+    int L = 1;
+    if constexpr (S::REM > 1) { fft_pass_multi_some<N, S::REM, NL>(sm, A, t, L, tw, act); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR8; ++s) { fft_pass_multi_some<N, 8, NL>(sm, A, t, L, tw, act); L *= 8; }
+}
+
 // Shared-memory addressing of a row line: one padding slot per 8 values keeps the strided
 // Stockham accesses free of bank conflicts.
 struct RowAddr {

@@ -411,8 +411,8 @@ void launch_real_fields_slice_fh(Ctx& c, int l) { G3D_DISPATCH_N(c.nx, NX, rf_ro
 // the sponge's row pass alone (inverse x, mask, forward x) on W0, W1: the free-hand y sponge
 void launch_sp_rows(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, sp_rows<NX>(c)); }
 // E and B of one slice (plane l) in real space (Simulation::real_fields_slice, src/sim_plasma.cpp:200-220)
-void launch_real_fields_slice(Ctx& c, int l, FmidOut fm) {
-    G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, l, 1));
+void launch_real_fields_slice(Ctx& c, int l, FmidOut fm, bool cols) {
+    if (cols) G3D_DISPATCH_N(c.ny, NY, rf_cols<NY>(c, l, 1));
     G3D_DISPATCH_N(c.nx, NX, rf_rows<NX>(c, l, 1, fm));
 }
 

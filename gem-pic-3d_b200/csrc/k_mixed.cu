@@ -609,8 +609,8 @@ void launch_real_fields_f(Ctx& c) {
     G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, 0, c.ns));
 }
 // E and B of one slice (plane l) of the mixed form (the real fields of one slice of the plasma march)
-void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm) {
-    G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c, l, 1));
+void launch_real_fields_slice_f(Ctx& c, int l, FmidOut fm, bool cols) {
+    if (cols) G3D_DISPATCH_N(c.ny, NY, rf_cols_f<NY>(c, l, 1));
     G3D_DISPATCH_N(c.nx, NX, rf_rows_f<NX>(c, l, 1, fm));
 }
 void launch_half_to_full_f(Ctx& c, const cpxf* half, cpx* full, long planes) {

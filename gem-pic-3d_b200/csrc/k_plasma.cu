@@ -13,6 +13,9 @@
 //                  js0(n-1) + d + w (d - dl), d = jsn - js0(n) (sim_plasma.cpp:339-351)
 //   k_march_slice  the march of the modes of slice n (march_point, src/sim_kernels.hpp:173-210)
 //   real fields of slice n: the column and row kernels of k_fields.cu on one plane
+// On the Fourier y grid the column transform of the spectra, the replace and prediction, the slice march and the
+// column transforms of the real fields are one kernel per k_x column (k_pass_cols), between k_ss_rows and the
+// rows kernel of the real fields.
 // A pass before the last (the predictor) deposits, transforms and marches like the last one but leaves the
 // particles unchanged (StreamArgs::dry), so every pass starts from the same particle state without a copy.
 // After the passes: k_correct (R of slice n+1 corrected for the prediction it used; dl, js0 updated,
@@ -585,37 +588,49 @@ __global__ void __launch_bounds__(128) k_march_slice(Geo g, cpx* Rx, cpx* Ry, T*
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < g.nkh) march_slice_mode<T>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D, n, i);
 }
-// a pass's current of half-cell n in place and the prediction of n-1 (replace_pred), then the march of slice n,
-// per mode in one thread (Fourier y, one rank: a = 0). Every load is issued before the first store, and the march
-// takes the two half-cells' new currents from registers (as stored: narrowed to T), so the thread's memory
-// requests overlap instead of following each other.
-template <class T>
-__global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry,
-                                                      T* __restrict__ Ez, T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
-                                                      const T* __restrict__ j0x, const T* __restrict__ j0y, double D, int n,
-                                                      int extrap, double w, const cpx* __restrict__ bk) {
-    const long nk = g.nkh;
-    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= nk) return;
+// ---------------------------------------------------------------- one pass's column work, fused (Fourier y)
+// k_pass_cols: one CTA per k_x column, one thread per k_y (per mode). (1) Each thread loads what the march of its
+// mode reads (the loads of the replace and march below; they are in flight during the transform). (2) The y
+// transforms of the streaming current's three row spectra, the filters and the smoothing (k_ss_cols) -> jsn. (3)
+// Per mode the replace and the march of slice n (replace_pred_mode + march_slice_mode in one). (4) The inverse y transforms of slice n's new
+// R, L, E_z, B_z from shared memory (k_rf_cols, or k_rf_cols_f in FP32 for the mixed form) -> W, which the rows
+// kernel of the real fields takes. One launch and one pass over the spectra instead of three. The transforms
+// run on three groups of FftShape<NY>::T threads (a line or a line pair each); all threads take the barriers.
+template <int NY, class T, class WT>
+__global__ void __launch_bounds__(NY) k_pass_cols(PlasmaPtrs p, Geo g, const cpx* __restrict__ T0, const cpx* __restrict__ T1,
+                                                  const cpx* __restrict__ T2, double a2, int keep0, cpx* __restrict__ Rx,
+                                                  cpx* __restrict__ Ry, T* __restrict__ Ez, T* __restrict__ Bz, T* __restrict__ Lx,
+                                                  T* __restrict__ Ly, const T* __restrict__ j0x, const T* __restrict__ j0y,
+                                                  double D, int n, int extrap, double w, const cpx* __restrict__ bk,
+                                                  const WT* __restrict__ twi, WT* __restrict__ W0, WT* __restrict__ W1,
+                                                  WT* __restrict__ W2, WT* __restrict__ W3, WT* __restrict__ W4, WT* __restrict__ W5) {
+    using S = FftShape<NY>;
+    using Tile = ColTile<NY, 1>;
+    extern __shared__ double smp[];
+    cpx* fl[3] = {reinterpret_cast<cpx*>(smp), reinterpret_cast<cpx*>(smp) + Tile::size, reinterpret_cast<cpx*>(smp) + 2 * Tile::size};
+    WT* ib = reinterpret_cast<WT*>(reinterpret_cast<cpx*>(smp) + 3 * Tile::size);
+    const int kxi = blockIdx.x, j = threadIdx.x;
+    const long nk = g.nkh, i = long(j) * g.H + kxi;
+    // the transforms: three groups of S::T threads, one line (forward) or one line pair (inverse) each
+    const int grp = j / S::T < 2 ? j / S::T : 2, tl = j - (j / S::T) * S::T;
+    const bool act = j < 3 * S::T;
+    // (1) the march's loads
     const long hp = long(n + 1) * nk + i, hq = long(n) * nk + i;      // half-cells n and n-1
     T* jk[3] = {static_cast<T*>(p.jkx), static_cast<T*>(p.jky), static_cast<T*>(p.jkz)};
     const bool pred = extrap && n >= 1;
-    cpx u[3], sn[3], kp[3], kq[3], s0p[3], s0q[3], dl[3], pn[3];
+    cpx sn[3], kp[3], kq[3], s0p[3], s0q[3], dl[3], pn[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        u[k] = p.jsn[k * nk + i]; sn[k] = p.sin_[k * nk + i];
+        sn[k] = p.sin_[k * nk + i];
         kp[k] = widen(jk[k][hp]); kq[k] = widen(jk[k][hq]);
         if (pred) {
             const cpx* s0[3] = {p.js0x, p.js0y, p.js0z};
             s0p[k] = s0[k][hp]; s0q[k] = s0[k][hq]; dl[k] = p.dl[k * nk + i]; pn[k] = p.pin[k * nk + i];
         }
     }
-    // the march's own loads (slice n of level s0, slice n+1 of level s1, j0 of both half-cells)
-    const int kxi = int(i % g.H), j = int(i / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
     const long o = long(n - g.a) * nk + i, ou = o + nk;
     const cpx j0xd = widen(j0x[o]), j0xu = widen(j0x[ou]), j0yd = widen(j0y[o]), j0yu = widen(j0y[ou]);
-    // level s0 of slice n: as in the arrays on the first pass, else from the backup the slice prologue took
     const cpx rx = bk ? bk[i] : Rx[o], ry = bk ? bk[nk + i] : Ry[o];
     const cpx ez = bk ? widen(narrow<T>(bk[2 * nk + i])) : widen(Ez[o]), bz = bk ? widen(narrow<T>(bk[3 * nk + i])) : widen(Bz[o]);
     const bool front = n == g.N - 1;
@@ -624,7 +639,21 @@ __global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx*
         const long pp = o + nk;
         pRx = Rx[pp]; pRy = Ry[pp]; pEz = widen(Ez[pp]); pBz = widen(Bz[pp]); pLx = widen(Lx[pp]); pLy = widen(Ly[pp]);
     }
-    // replace(n, sin, jsn) and the prediction of n-1
+    const double h = front ? 0.0 : g.hcg[n + 2];
+    // (2) the current's column, transformed and filtered
+    const long ot = long(j) * g.H + kxi;
+    fl[0][Tile::at(j, 0)] = T0[ot]; fl[1][Tile::at(j, 0)] = T1[ot]; fl[2][Tile::at(j, 0)] = T2[ot];
+    __syncthreads();
+    {
+        cpx* const ls_[1] = {fl[grp]};
+        fft_lines_some<NY, 1>(ls_, RowAddr{0}, tl, g.twy, act);
+    }
+    const double k2f = g.kxs[kxi] * g.kxs[kxi] + g.kys[j] * g.kys[j];
+    const double f = (kxi == 0 && j == 0 && !keep0) ? 0.0 : g.filt[kxi] * g.filty[j] / (1 + a2 * k2f);
+    cpx u[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { u[k] = f * fl[k][Tile::at(j, 0)]; p.jsn[k * nk + i] = u[k]; }
+    // (3) replace(n, sin, jsn), the prediction of n-1, the march of slice n
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const T np_ = narrow<T>(kp[k] + u[k] - sn[k]);
@@ -638,31 +667,49 @@ __global__ void __launch_bounds__(128) k_replace_march(PlasmaPtrs p, Geo g, cpx*
             p.pin[k * nk + i] = t;
         }
     }
-    // the march of slice n (march_slice_mode with the currents of half-cells n-1 = kq and n = kp)
     const cpx Jx = wl * (j0xd + kq[0]) + wu * (j0xu + kp[0]);
     const cpx Jy = wl * (j0yd + kq[1]) + wu * (j0yu + kp[1]);
     const cpx Rsx = rx + D * (ik(kx, ez) + ik(ky, bz)) - D * Jx;
     const cpx Rsy = ry + D * (ik(ky, ez) - ik(kx, bz)) - D * Jy;
+    cpx nv[6];                                        // slice n as stored: R_x, R_y, L_x, L_y, E_z, B_z
     if (front) {
         Rx[o] = Rsx; Ry[o] = Rsy;
         Ez[o] = narrow<T>(C(0)); Bz[o] = narrow<T>(C(0)); Lx[o] = narrow<T>(C(0)); Ly[o] = narrow<T>(C(0));
-        return;
+        nv[0] = Rsx; nv[1] = Rsy;
+        nv[2] = nv[3] = nv[4] = nv[5] = widen(narrow<T>(C(0)));
+    } else {
+        const cpx upx = kp[0], upy = kp[1], upz = kp[2];
+        const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
+        const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
+        const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
+        const cpx Qp = -0.5 * ik(kx, pRx - pLx) + 0.5 * ik(ky, pLy - pRy);
+        const cpx SB = ik(kx, Rsy) + ik(kx, Lsy) - ik(ky, Rsx) - ik(ky, Lsx);
+        const cpx SE = -ik(kx, Rsx) + ik(kx, Lsx) + ik(ky, Lsy) - ik(ky, Rsy);
+        const double den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+        const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) / den;
+        const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) / den;
+        const T ezs = narrow<T>(Ezn), bzs = narrow<T>(Bzn);
+        const cpx nRx = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)), nRy = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
+        const T lxs = narrow<T>(Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)));
+        const T lys = narrow<T>(Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn)));
+        Ez[o] = ezs; Bz[o] = bzs; Rx[o] = nRx; Ry[o] = nRy; Lx[o] = lxs; Ly[o] = lys;
+        nv[0] = nRx; nv[1] = nRy; nv[2] = widen(lxs); nv[3] = widen(lys); nv[4] = widen(ezs); nv[5] = widen(bzs);
     }
-    const double h = g.hcg[n + 2];
-    const cpx upx = kp[0], upy = kp[1], upz = kp[2];
-    const cpx Lsx = pLx - 0.25 * h * (ik(kx, pEz) - ik(ky, pBz)) - 0.5 * h * upx;
-    const cpx Lsy = pLy - 0.25 * h * (ik(kx, pBz) + ik(ky, pEz)) - 0.5 * h * upy;
-    const cpx Cp = 0.5 * (ik(kx, pRy + pLy) - ik(ky, pRx + pLx));
-    const cpx Qp = -0.5 * ik(kx, pRx - pLx) + 0.5 * ik(ky, pLy - pRy);
-    const cpx SB = ik(kx, Rsy) + ik(kx, Lsy) - ik(ky, Rsx) - ik(ky, Lsx);
-    const cpx SE = -ik(kx, Rsx) + ik(kx, Lsx) + ik(ky, Lsy) - ik(ky, Rsy);
-    const double den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
-    const cpx Bzn = (pBz - 0.5 * h * Cp - 0.25 * h * SB) / den;
-    const cpx Ezn = (pEz - 0.5 * h * Qp - 0.25 * h * SE - h * upz) / den;
-    Ez[o] = narrow<T>(Ezn); Bz[o] = narrow<T>(Bzn);
-    Rx[o] = Rsx + D * (ik(kx, Ezn) + ik(ky, Bzn)); Ry[o] = Rsy + D * (ik(ky, Ezn) - ik(kx, Bzn));
-    Lx[o] = narrow<T>(Lsx - 0.25 * h * (ik(kx, Ezn) - ik(ky, Bzn)));
-    Ly[o] = narrow<T>(Lsy - 0.25 * h * (ik(kx, Bzn) + ik(ky, Ezn)));
+    // (4) the real fields' y transforms of slice n (pairs as k_rf_cols: R -> W0, W1; L -> W2, W3; E_z, B_z -> W4, W5)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if constexpr (std::is_same<WT, cpx>::value) ib[k * Tile::size + Tile::at(j, 0)] = conj(nv[k]);
+        else ib[k * Tile::size + Tile::at(j, 0)] = conj(to_f(nv[k]));
+    }
+    __syncthreads();
+    {
+        WT* const ls_[2] = {ib + (2 * grp) * Tile::size, ib + (2 * grp + 1) * Tile::size};
+        fft_lines_some<NY, 2>(ls_, RowAddr{0}, tl, twi, act);
+    }
+    WT* out[6] = {W0, W1, W2, W3, W4, W5};
+    const long ow = long(n) * nk + long(j) * g.H + kxi;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out[k][ow] = conj(ib[k * Tile::size + Tile::at(j, 0)]);
 }
 // freed electrons join the march (appended after the streaming particles; the count stays on the device)
 __global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
@@ -1030,20 +1077,45 @@ void launch_march_slice(Ctx& c, double D, int n) {
     c.check_launch("k_march_slice");
     c.prof_end(tok);
 }
-void launch_replace_march(Ctx& c, double D, int n, int extrap, double w, int restore) {
-    const int tok = c.prof_begin("replace_march");
-    const unsigned blocks = unsigned((c.nkh + 127) / 128);
-    const PlasmaPtrs pp = c.pl->ptrs(c);
-    const cpx* bk = restore ? c.pl->bk.p : nullptr;
+template <int NY>
+static void pass_cols(Ctx& c, double D, int n, int extrap, double w, int restore) {
+    PlasmaState& P = *c.pl;
+    const PlasmaPtrs pp = P.ptrs(c);
+    const cpx* bk = restore ? P.bk.p : nullptr;
+    const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
+    const int keep0 = P.box_mean ? 1 : 0;
+    const cpx* T = P.tsp.p;
+    using Tile = ColTile<NY, 1>;
     if (c.mixed) {
         MixedBufs& m = c.mx;
-        k_replace_march<cpxf><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
-                                                            D, n, extrap, w, bk);
+        const size_t smem = 3 * Tile::size * sizeof(cpx) + 6 * Tile::size * sizeof(cpxf);
+        smem_attr(reinterpret_cast<const void*>(k_pass_cols<NY, cpxf, cpxf>), smem);
+        k_pass_cols<NY, cpxf, cpxf><<<unsigned(c.H), NY, smem, c.stream>>>(
+            pp, c.geo(), T, T + c.nkh, T + 2 * c.nkh, a2, keep0, c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p,
+            D, n, extrap, w, bk, m.twy.p, m.W[0].p, m.W[1].p, m.W[2].p, m.W[3].p, m.W[4].p, m.W[5].p);
     } else {
-        k_replace_march<cpx><<<blocks, 128, 0, c.stream>>>(pp, c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
-                                                           D, n, extrap, w, bk);
+        const size_t smem = 9 * Tile::size * sizeof(cpx);
+        smem_attr(reinterpret_cast<const void*>(k_pass_cols<NY, cpx, cpx>), smem);
+        k_pass_cols<NY, cpx, cpx><<<unsigned(c.H), NY, smem, c.stream>>>(
+            pp, c.geo(), T, T + c.nkh, T + 2 * c.nkh, a2, keep0, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p,
+            D, n, extrap, w, bk, c.twy.p, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p);
     }
-    c.check_launch("k_replace_march");
+}
+void launch_pass_cols(Ctx& c, double D, int n, int extrap, double w, int restore) {
+    const int tok = c.prof_begin("pass_cols");
+    G3D_DISPATCH_N(c.ny, NY, pass_cols<NY>(c, D, n, extrap, w, restore));
+    c.check_launch("k_pass_cols");
+    c.prof_end(tok);
+}
+void launch_stream_spectra_rows(Ctx& c) {
+    const int tok = c.prof_begin("stream_spectra");
+    PlasmaState& P = *c.pl;
+    if (c.f32s) {
+        float4* J4 = reinterpret_cast<float4*>(P.jsrf.p);
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, float4>(c, J4, P.tsp.p, 1, P.bcnt.p)));
+    } else {
+        G3D_DISPATCH_N(c.nx, NX, (ss_rows<NX, double>(c, P.jsr.p, P.tsp.p, 1, P.bcnt.p)));
+    }
     c.prof_end(tok);
 }
 void launch_born_append(Ctx& c) {
