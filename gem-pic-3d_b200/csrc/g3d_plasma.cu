@@ -109,6 +109,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
     pl->bk.alloc(4 * ph, s);
     pl->nstrm_dev.alloc(1, s);
+    pl->sdev.alloc(2, s);
     pl->bcnt.alloc(1, s);
     pl->tally.alloc(1, s);
     pl->flags.alloc(1, s);
@@ -195,13 +196,15 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     P.nstrm = n;
     P.born_cap = cap;
     const long need = n + cap;
-    if (P.s.cap < need) {             // half again: the list grows by the joining particles for some steps, and every
-        const long nn = need + need / 2 + 64;        // move of it costs a new capture of the slice loop's graph
+    if (P.s.cap < need) {             // doubled: the list grows by the joining particles step after step
+        const long nn = 2 * need + 64;
         P.s.alloc(nn, c.stream);
     }
     if (cap > 0 && P.bn.cap < cap) P.bn.alloc(cap, c.stream);
     P.strm = P.s.v;
     P.born = P.bn.v;
+    P.sdh[0] = P.strm; P.sdh[1] = P.born;
+    G3D_CUDA(cudaMemcpyAsync(P.sdev.p, P.sdh, sizeof(P.sdh), cudaMemcpyHostToDevice, c.stream));
     if (fresh) launch_lattice_fill(c, a, npts, P.strm);
     const long nj = long(P.joining.size());
     if (nj) {                                            // the joining particles after the lattice, as columns
@@ -320,13 +323,14 @@ void march_plasma(Ctx& c, double s0, double s1) {
     // The slice loop is some 20 launches per half-cell (about 41,000 for 2,048 slices and two passes). Launched
     // one by one, the host's launch rate would bound the march; as one CUDA graph they run back to back. The
     // graph is captured once and launched every step; it is captured again only when something it holds by value
-    // changes (a buffer moved, the capacity of the freed-electron list, the step length). While per-kernel events
+    // changes (a buffer of the window moved, the capacity of the freed-electron list, the step length). The
+    // streaming and freed-electron lists are reached through a descriptor on the device, so they may move. While per-kernel events
     // are recorded the loop is launched directly.
     uint64_t key = 1469598103934665603ULL;
     auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
-    mixk(ptr(c.F.p)); mixk(ptr(P.strm.x)); mixk(ptr(P.born.x)); mixk(uint64_t(P.s.cap)); mixk(uint64_t(P.born_cap));
+    mixk(ptr(c.F.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
     uint64_t dbits;
@@ -348,7 +352,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         StreamArgs sa;
         sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
         sa.Delta = Delta; sa.vz_beam = P.cfg.vz_beam;
-        sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.born = P.born; sa.bcnt = P.bcnt.p;
+        sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.sd = P.sdev.p; sa.bcnt = P.bcnt.p;
         sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
         sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;

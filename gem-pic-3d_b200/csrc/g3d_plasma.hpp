@@ -41,7 +41,8 @@ struct StreamArgs {
     float* Jf;                 // the same planes in FP32 (the mixed form)
     const IonDevC* ions;
     const AdkDev* adk;
-    StrmDev born;
+    const StrmDev* sd;         // on the device: [0] the streaming particles, [1] the freed electrons (read at run
+                               // time, so that the slice loop's graph outlives a move of either list)
     int* bcnt;
     int bcap;
     int dry;                   // a predictor pass: deposit and ionize, keep the particles as they were
@@ -106,6 +107,8 @@ struct PlasmaState {
     DevBuf<cpx> bk;                            // 4 half planes: R_x, R_y, E_z, B_z of the slice
     StrmBuf s, bn;                             // streaming particles, the freed electrons
     StrmDev strm{}, born{};
+    StrmDev sdh[2]{};                          // strm and born as the kernels of the slice loop read them (sdev)
+    DevBuf<StrmDev> sdev;
     long nstrm = 0;                            // host copy (exact at the start of the march)
     long born_cap = 0, fresh_last = 0, trapped_total = 0, restreamed_total = 0;
     DevBuf<long> nstrm_dev;

@@ -231,7 +231,7 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
         tleft -= tw; ++Z;
         const int j = atomicAdd(c.bcnt, 1);
         if (j < c.bcap) {
-            const StrmDev& Bn = c.born;
+            const StrmDev Bn = c.sd[1];
             Bn.x[j] = S.x[i]; Bn.y[j] = S.y[i]; Bn.zeta[j] = S.zeta[i]; Bn.px[j] = S.px[i]; Bn.py[j] = S.py[i];
             Bn.pz[j] = S.pz[i]; Bn.w[j] = S.w[i]; Bn.z[j] = S.z[i]; Bn.q[j] = -1; Bn.qm[j] = -1;
             Bn.alive[j] = 1; Bn.sp[j] = SP_FREED + (sp - SP_ION); Bn.id[j] = S.id[i];
@@ -357,8 +357,9 @@ constexpr int ST_NT = 128;
 #define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
 #endif
 template <bool F32, bool ION, bool LASER>
-__global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c, StrmDev S,
+__global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c,
                                                                                        const long* __restrict__ nstrm) {
+    const StrmDev S = c.sd[0];
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
         const DepReq d = stream_one<F32, ION, LASER>(c, S, i);
@@ -369,10 +370,10 @@ template <bool F32>
 static void stream_launch(Ctx& c, const StreamArgs& a, unsigned blocks) {
     PlasmaState& P = *c.pl;
     const bool ion = P.any_ionizing, las = c.laser.on != 0;
-    if (ion && las) k_stream<F32, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
-    else if (ion) k_stream<F32, true, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
-    else if (las) k_stream<F32, false, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
-    else k_stream<F32, false, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.strm, P.nstrm_dev.p);
+    if (ion && las) k_stream<F32, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else if (ion) k_stream<F32, true, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else if (las) k_stream<F32, false, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else k_stream<F32, false, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
 }
 
 // ---------------------------------------------------------------- spectra of the streaming current
@@ -712,8 +713,9 @@ __global__ void __launch_bounds__(NY) k_pass_cols(PlasmaPtrs p, Geo g, const cpx
     for (int k = 0; k < 6; ++k) out[k][ow] = conj(ib[k * Tile::size + Tile::at(j, 0)]);
 }
 // freed electrons join the march (appended after the streaming particles; the count stays on the device)
-__global__ void k_born_append(StrmDev S, StrmDev Bn, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
+__global__ void k_born_append(const StrmDev* __restrict__ sd, const int* __restrict__ bcnt, int bcap, long* __restrict__ nstrm_dev,
                               int* __restrict__ overflow) {
+    const StrmDev S = sd[0], Bn = sd[1];
     const int cnt = *bcnt;
     const long base = *nstrm_dev;
     if (cnt > bcap) { if (blockIdx.x == 0 && threadIdx.x == 0) *overflow = 1; return; }
@@ -896,8 +898,8 @@ void launch_stream(Ctx& c, const StreamArgs& a) {
     PlasmaState& P = *c.pl;
     if (P.s.cap <= 0) return;
     const int tok = c.prof_begin("stream");
-    const long want = (P.s.cap + ST_NT - 1) / ST_NT;
-    const unsigned blocks = unsigned(want < 148 * 16 ? want : 148 * 16);
+    const unsigned blocks = 148 * 16;             // fixed (the kernel strides over the count on the device), so
+                                                  // that the graph of the slice loop does not depend on the list
     if (c.f32s) stream_launch<true>(c, a, blocks);
     else stream_launch<false>(c, a, blocks);
     c.check_launch("k_stream");
@@ -1120,7 +1122,7 @@ void launch_stream_spectra_rows(Ctx& c) {
 }
 void launch_born_append(Ctx& c) {
     PlasmaState& P = *c.pl;
-    k_born_append<<<ew_blocks(P.born_cap), 256, 0, c.stream>>>(P.strm, P.born, P.bcnt.p, int(P.born_cap), P.nstrm_dev.p,
+    k_born_append<<<ew_blocks(P.born_cap), 256, 0, c.stream>>>(P.sdev.p, P.bcnt.p, int(P.born_cap), P.nstrm_dev.p,
                                                                P.flags.p);
     c.check_launch("k_born_append");
     k_count_add<<<1, 1, 0, c.stream>>>(P.nstrm_dev.p, P.bcnt.p, int(P.born_cap));
