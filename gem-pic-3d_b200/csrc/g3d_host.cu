@@ -597,6 +597,7 @@ static void shift_window(Ctx& c, int nxs, int nys) {
         for (DevBuf<cpxf>* a : {&c.mx.Ez, &c.mx.Bz, &c.mx.j0x, &c.mx.j0y}) launch_rotate_f(c, a->p, a->n, nxs * c.dx, nys * c.dy, nys);
     if (c.pl) {
         for (auto& p : c.pl->joining) { p.x -= nxs * c.dx; p.y -= nys * c.dy; }
+        launch_join_shift(c, nxs * c.dx, nys * c.dy);
         launch_rotate(c, c.pl->js0x.p, c.pl->js0x.n, nxs * c.dx, nys * c.dy, nys);
         launch_rotate(c, c.pl->js0y.p, c.pl->js0y.n, nxs * c.dx, nys * c.dy, nys);
         launch_rotate(c, c.pl->js0z.p, c.pl->js0z.n, nxs * c.dx, nys * c.dy, nys);

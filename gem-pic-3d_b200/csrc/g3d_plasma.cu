@@ -112,6 +112,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     pl->sdev.alloc(2, s);
     pl->bcnt.alloc(1, s);
     pl->tally.alloc(1, s);
+    pl->ucount.alloc(1, s);
     pl->flags.alloc(1, s);
     // ion tables on the device (setup_ions, src/sim_ions.cpp:68-87)
     const double Lu = c.P.lambda0 / (2 * M_PI), omega0 = c_SI / Lu, E0 = me_SI * c_SI * omega0 / e_SI;
@@ -155,8 +156,9 @@ static double density_zfactor(const PlasmaState& P, double z) {
 // Fresh plasma at the front of the window in the reference's order (load_plasma, src/sim_plasma.cpp:43-90):
 // rows j, cells i, sub-cells b2, a2; the electron, then the loaded ions of every species; then the particles
 // that join the march at their zeta. The lattice is built on the device (k_lattice_flags / k_lattice_fill: the
-// points of positive density counted, their particles written at the running count, ids in list order); only
-// the joining particles come from the host.
+// points of positive density counted, their particles written at the running count, ids in list order); the
+// joining particles are the last march's slow trapped ones, kept on the device, then the beam particles that
+// slowed down, from the host (the order of the reference's list).
 static void load_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
     const double zmid = 0.5 * (s0 + s1), Delta = s1 - s0;
@@ -187,11 +189,12 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     const long npts = nrows > 0 ? nrows * c.nx * a.px * a.py : 0;
     const long pts = (npts > 0 && a.m > 0) ? launch_lattice_count(c, a, npts) : 0;
     const long fresh = pts * a.m;
-    long cap = pts * ion_cap;
+    long cap = pts * ion_cap + launch_join_cap(c);
     for (const auto& p : P.joining)
         if (p.sp >= SP_ION && p.sp < SP_FREED && P.ions[size_t(p.sp - SP_ION)].ionization)
             cap += P.ions[size_t(p.sp - SP_ION)].Zmax - std::lround(p.q);
-    const long n = fresh + long(P.joining.size());
+    const long jd = P.njb;                               // joining on the device (the last march's slow trapped)
+    const long n = fresh + jd + long(P.joining.size());
     P.fresh_last = fresh;
     P.nstrm = n;
     P.born_cap = cap;
@@ -206,8 +209,19 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     P.sdh[0] = P.strm; P.sdh[1] = P.born;
     G3D_CUDA(cudaMemcpyAsync(P.sdev.p, P.sdh, sizeof(P.sdh), cudaMemcpyHostToDevice, c.stream));
     if (fresh) launch_lattice_fill(c, a, npts, P.strm);
-    const long nj = long(P.joining.size());
-    if (nj) {                                            // the joining particles after the lattice, as columns
+    if (jd) {                                            // the device's joining particles after the lattice
+        const StrmDev& J = P.jb.v;
+        const double* src[10] = {J.x, J.y, J.zeta, J.px, J.py, J.pz, J.w, J.z, J.q, J.qm};
+        double* dst[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
+        for (int m = 0; m < 10; ++m)
+            G3D_CUDA(cudaMemcpyAsync(dst[m] + fresh, src[m], size_t(jd) * 8, cudaMemcpyDeviceToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.alive + fresh, J.alive, size_t(jd) * 4, cudaMemcpyDeviceToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.sp + fresh, J.sp, size_t(jd) * 4, cudaMemcpyDeviceToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.id + fresh, J.id, size_t(jd) * 8, cudaMemcpyDeviceToDevice, c.stream));
+        P.njb = 0;
+    }
+    const long nj = long(P.joining.size()), jo = fresh + jd;
+    if (nj) {                                            // then the host's (restreamed beam particles), as columns
         std::vector<double> hd(size_t(nj) * 10);
         std::vector<int32_t> hi(size_t(nj) * 2);
         std::vector<uint64_t> hu(static_cast<size_t>(nj));
@@ -219,10 +233,10 @@ static void load_plasma(Ctx& c, double s0, double s1) {
         }
         double* cols[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
         for (int m = 0; m < 10; ++m)
-            G3D_CUDA(cudaMemcpyAsync(cols[m] + fresh, hd.data() + size_t(m) * nj, size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.alive + fresh, hi.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.sp + fresh, hi.data() + nj, size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
-        G3D_CUDA(cudaMemcpyAsync(P.strm.id + fresh, hu.data(), size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
+            G3D_CUDA(cudaMemcpyAsync(cols[m] + jo, hd.data() + size_t(m) * nj, size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.alive + jo, hi.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.sp + jo, hi.data() + nj, size_t(nj) * 4, cudaMemcpyHostToDevice, c.stream));
+        G3D_CUDA(cudaMemcpyAsync(P.strm.id + jo, hu.data(), size_t(nj) * 8, cudaMemcpyHostToDevice, c.stream));
     }
     P.joining.clear();
     G3D_CUDA(cudaMemcpyAsync(P.nstrm_dev.p, &P.nstrm, sizeof(long), cudaMemcpyHostToDevice, c.stream));
@@ -257,10 +271,9 @@ std::vector<g3d_particle> get_streaming(Ctx& c) {
     return out;
 }
 
-// The trapped streaming particles (alive == 5) in list order: compacted on the device, only they come to the host.
-static std::vector<g3d_particle> trapped_particles(Ctx& c) {
+// The trapped streaming particles that join the beam (P.tr after launch_trapped_split, n of them) on the host.
+static std::vector<g3d_particle> fast_trapped(Ctx& c, long n) {
     PlasmaState& P = *c.pl;
-    const long n = P.s.cap > 0 ? launch_compact_state(c, P.strm, P.nstrm_dev.p, P.s.cap, 5) : 0;
     std::vector<g3d_particle> out(static_cast<size_t>(n));
     if (!n) return out;
     const StrmDev& T = P.tr.v;
@@ -423,18 +436,13 @@ void march_plasma(Ctx& c, double s0, double s1) {
     if (flag) throw Error(G3D_ERR_CAPACITY, "ionization: list of freed electrons overflowed");
     // trapped particles: fast ones join the beam list, slow ones stream again in the next step (counted on the
     // device first: the streaming particles come to the host only when some were trapped)
-    std::vector<g3d_particle> sv = trapped_particles(c);
-    std::vector<g3d_particle> add;
-    for (auto& p : sv) {
-        if (p.alive != 5) continue;
-        const double g = std::sqrt(1 + p.px * p.px + p.py * p.py + p.pz * p.pz);
-        p.z = s1;
-        if (p.pz / g >= P.cfg.vz_beam) {
-            p.alive = 1;
-            p.sp = (p.sp >= SP_FREED && p.sp < SP_INJECTED) ? p.sp - SP_FREED + SP_INJECTED : p.sp >= SP_INJECTED ? p.sp : SP_TRAPPED;
-            ++P.trapped_total;
-            add.push_back(p);
-        } else { p.alive = 6; P.joining.push_back(p); }
+    // (split on the device in list order, z = s1: the slow ones stay there as the next march's joining particles,
+    // alive 6; only the ones joining the beam come to the host)
+    std::vector<g3d_particle> add = fast_trapped(c, launch_trapped_split(c, s1));
+    for (auto& p : add) {
+        p.alive = 1;
+        p.sp = (p.sp >= SP_FREED && p.sp < SP_INJECTED) ? p.sp - SP_FREED + SP_INJECTED : p.sp >= SP_INJECTED ? p.sp : SP_TRAPPED;
+        ++P.trapped_total;
     }
     if (!add.empty()) {
         std::vector<g3d_particle> all = get_particles(c), keep;

@@ -116,9 +116,12 @@ struct PlasmaState {
     DevBuf<int> tally;                         // count of particles in a given state (count_state)
     DevBuf<IonDevC> ion_dev;
     DevBuf<AdkDev> adk_dev;
-    std::vector<g3d_particle> joining;         // join the next march at their zeta
+    std::vector<g3d_particle> joining;         // join the next march at their zeta (from the host: restreamed)
+    StrmBuf jb;                                // the same on the device: the slow trapped particles of the last march
+    long njb = 0;
+    DevBuf<unsigned long long> ucount;
     // scratch of the lattice build and of the compaction of trapped particles: flags and their exclusive sums
-    // (one entry more than the items), the scan's temporary storage, the trapped particles in list order
+    // (one entry more than the items), the scan's temporary storage, the trapped particles that join the beam
     DevBuf<int> cflag, coff;
     DevBuf<unsigned char> ctmp;
     StrmBuf tr;
@@ -156,8 +159,11 @@ void launch_real_fields_slice(Ctx& c, int l, FmidOut fm = FmidOut(), bool cols =
 long launch_lattice_count(Ctx& c, const LatticeArgs& a, long npts);
 // the fresh particles of those points into S[0 .. count m)
 void launch_lattice_fill(Ctx& c, const LatticeArgs& a, long npts, StrmDev S);
-// the particles with alive == state among the device count n_dev of S (at most cap), in list order, into P.tr;
-// returns how many
-long launch_compact_state(Ctx& c, const StrmDev& S, const long* n_dev, long cap, int state);
+// the trapped particles after a march: the slow ones appended to the device joining list (P.jb), the fast ones into
+// P.tr; returns how many fast ones
+long launch_trapped_split(Ctx& c, double s1);
+// the freed-electron capacity the device joining list needs (ionizing ions); its x, y moved with the window
+long launch_join_cap(Ctx& c);
+void launch_join_shift(Ctx& c, double sx, double sy);
 
 }  // namespace g3d

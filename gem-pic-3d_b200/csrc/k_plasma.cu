@@ -872,21 +872,45 @@ __global__ void k_lattice_fill(LatticeArgs a, long npts, const int* __restrict__
         for (int t = 0; t < a.nion; ++t) put(__dmul_rn(a.ion_atoms[t], w), a.ion_q[t], a.ion_qm[t], a.ion_sp[t]);
     }
 }
-// ---------------------------------------------------------------- particles of one state, in list order
-__global__ void k_state_flags(const int32_t* __restrict__ alive, const long* __restrict__ n_dev, long cap, int state,
-                              int* __restrict__ flag) {
+// ---------------------------------------------------------------- trapped particles, split on the device
+// A trapped streaming particle (alive 5) joins the beam when v_z = p_z / gamma >= vz_beam, else it streams again in
+// the next march (Simulation::march_plasma's trapping, src/sim_plasma.cpp:404-433). v_z with the host's
+// operations, so the split is the host's.
+__device__ __forceinline__ bool trapped_fast(const StrmDev& S, long i, double vzb) {
+    const double px = S.px[i], py = S.py[i], pz = S.pz[i];
+    const double g = __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(px, px)), __dmul_rn(py, py)), __dmul_rn(pz, pz)));
+    return __ddiv_rn(pz, g) >= vzb;
+}
+__global__ void k_trap_flags(StrmDev S, const long* __restrict__ n_dev, long cap, double vzb, int fast, int* __restrict__ flag) {
     const long n = *n_dev < cap ? *n_dev : cap;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i <= cap; i += long(gridDim.x) * blockDim.x)
-        flag[i] = i < n && alive[i] == state;
+        flag[i] = i < n && S.alive[i] == 5 && trapped_fast(S, i, vzb) == (fast != 0);
 }
-__global__ void k_state_gather(StrmDev S, const int* __restrict__ flag, const int* __restrict__ off, long cap, StrmDev T) {
+// the flagged particles in list order into T from T[base]: z = s1, and (slow) alive 6, waiting for their zeta
+__global__ void k_trap_gather(StrmDev S, const int* __restrict__ flag, const int* __restrict__ off, long cap, StrmDev T, long base,
+                              int slow, double s1) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += long(gridDim.x) * blockDim.x) {
         if (!flag[i]) continue;
-        const long k = off[i];
+        const long k = base + off[i];
         T.x[k] = S.x[i]; T.y[k] = S.y[i]; T.zeta[k] = S.zeta[i]; T.px[k] = S.px[i]; T.py[k] = S.py[i]; T.pz[k] = S.pz[i];
-        T.w[k] = S.w[i]; T.z[k] = S.z[i]; T.q[k] = S.q[i]; T.qm[k] = S.qm[i]; T.alive[k] = S.alive[i]; T.sp[k] = S.sp[i];
+        T.w[k] = S.w[i]; T.z[k] = s1; T.q[k] = S.q[i]; T.qm[k] = S.qm[i]; T.alive[k] = slow ? 6 : S.alive[i]; T.sp[k] = S.sp[i];
         T.id[k] = S.id[i];
     }
+}
+// the freed-electron capacity the joining ions need: sum of Zmax - round(q) over the ions of ionizing species
+__global__ void k_join_cap(StrmDev J, long n, const IonDevC* __restrict__ ions, int nion, unsigned long long* __restrict__ out) {
+    unsigned long long a = 0;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const int sp = J.sp[i];
+        if (sp >= SP_ION && sp < SP_FREED && sp - SP_ION < nion && ions[sp - SP_ION].ionizing)
+            a += (unsigned long long)(ions[sp - SP_ION].Zmax - llround(J.q[i]));
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if ((threadIdx.x & 31) == 0 && a) atomicAdd(out, a);
+}
+// x, y of the joining particles on the device moved with the window
+__global__ void k_join_shift(StrmDev J, long n, double sx, double sy) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) { J.x[i] -= sx; J.y[i] -= sy; }
 }
 
 // ---------------------------------------------------------------- launchers
@@ -979,17 +1003,66 @@ void launch_lattice_fill(Ctx& c, const LatticeArgs& a, long npts, StrmDev S) {
     k_lattice_fill<<<ew_blocks(npts), 256, 0, c.stream>>>(a, npts, c.pl->coff.p, S);
     c.check_launch("k_lattice_fill");
 }
-long launch_compact_state(Ctx& c, const StrmDev& S, const long* n_dev, long cap, int state) {
+// The trapped streaming particles after a march: the slow ones appended on the device to the joining list (P.jb,
+// P.njb), the fast ones into P.tr; returns how many fast ones.
+long launch_trapped_split(Ctx& c, double s1) {
     PlasmaState& P = *c.pl;
+    const long cap = P.s.cap;
+    if (cap <= 0) return 0;
     reserve_flags(c, cap);
-    k_state_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(S.alive, n_dev, cap, state, P.cflag.p);
-    c.check_launch("k_state_flags");
-    const long n = scan_flags(c, cap);
-    if (n == 0) return 0;
-    if (P.tr.cap < n) P.tr.alloc(n + n / 4 + 64, c.stream);
-    k_state_gather<<<ew_blocks(cap), 256, 0, c.stream>>>(S, P.cflag.p, P.coff.p, cap, P.tr.v);
-    c.check_launch("k_state_gather");
-    return n;
+    const double vzb = P.cfg.vz_beam;
+    k_trap_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(P.strm, P.nstrm_dev.p, cap, vzb, 0, P.cflag.p);
+    c.check_launch("k_trap_flags");
+    const long ns = scan_flags(c, cap);
+    if (ns > 0) {
+        if (P.jb.cap < P.njb + ns) {                     // grow, keeping the particles already there
+            StrmBuf nb;
+            nb.alloc(2 * (P.njb + ns) + 64, c.stream);
+            if (P.njb > 0) {
+                for (int m = 0; m < 10; ++m)
+                    G3D_CUDA(cudaMemcpyAsync(nb.d.p + size_t(m) * nb.cap, P.jb.d.p + size_t(m) * P.jb.cap, size_t(P.njb) * 8,
+                                             cudaMemcpyDeviceToDevice, c.stream));
+                for (int m = 0; m < 2; ++m)
+                    G3D_CUDA(cudaMemcpyAsync(nb.i.p + size_t(m) * nb.cap, P.jb.i.p + size_t(m) * P.jb.cap, size_t(P.njb) * 4,
+                                             cudaMemcpyDeviceToDevice, c.stream));
+                G3D_CUDA(cudaMemcpyAsync(nb.u.p, P.jb.u.p, size_t(P.njb) * 8, cudaMemcpyDeviceToDevice, c.stream));
+            }
+            G3D_CUDA(cudaStreamSynchronize(c.stream));
+            std::swap(P.jb.d.p, nb.d.p); std::swap(P.jb.d.n, nb.d.n);
+            std::swap(P.jb.i.p, nb.i.p); std::swap(P.jb.i.n, nb.i.n);
+            std::swap(P.jb.u.p, nb.u.p); std::swap(P.jb.u.n, nb.u.n);
+            std::swap(P.jb.v, nb.v); std::swap(P.jb.cap, nb.cap);             // nb frees the old buffers
+        }
+        k_trap_gather<<<ew_blocks(cap), 256, 0, c.stream>>>(P.strm, P.cflag.p, P.coff.p, cap, P.jb.v, P.njb, 1, s1);
+        c.check_launch("k_trap_gather");
+        P.njb += ns;
+    }
+    k_trap_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(P.strm, P.nstrm_dev.p, cap, vzb, 1, P.cflag.p);
+    c.check_launch("k_trap_flags");
+    const long nf = scan_flags(c, cap);
+    if (nf > 0) {
+        if (P.tr.cap < nf) P.tr.alloc(nf + nf / 4 + 64, c.stream);
+        k_trap_gather<<<ew_blocks(cap), 256, 0, c.stream>>>(P.strm, P.cflag.p, P.coff.p, cap, P.tr.v, 0, 0, s1);
+        c.check_launch("k_trap_gather");
+    }
+    return nf;
+}
+long launch_join_cap(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    if (P.njb == 0 || !P.any_ionizing) return 0;
+    G3D_CUDA(cudaMemsetAsync(P.ucount.p, 0, sizeof(unsigned long long), c.stream));
+    k_join_cap<<<ew_blocks(P.njb), 256, 0, c.stream>>>(P.jb.v, P.njb, P.ion_dev.p, int(P.ion_dev.n), P.ucount.p);
+    c.check_launch("k_join_cap");
+    unsigned long long h = 0;
+    G3D_CUDA(cudaMemcpyAsync(&h, P.ucount.p, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return long(h);
+}
+void launch_join_shift(Ctx& c, double sx, double sy) {
+    PlasmaState& P = *c.pl;
+    if (P.njb == 0) return;
+    k_join_shift<<<ew_blocks(P.njb), 256, 0, c.stream>>>(P.jb.v, P.njb, sx, sy);
+    c.check_launch("k_join_shift");
 }
 
 long count_state(Ctx& c, const int32_t* alive, long n, const long* n_dev, int state) {
