@@ -434,10 +434,9 @@ void march_plasma(Ctx& c, double s0, double s1) {
     int flag = 0;
     G3D_CUDA(cudaMemcpy(&flag, P.flags.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag) throw Error(G3D_ERR_CAPACITY, "ionization: list of freed electrons overflowed");
-    // trapped particles: fast ones join the beam list, slow ones stream again in the next step (counted on the
-    // device first: the streaming particles come to the host only when some were trapped)
-    // (split on the device in list order, z = s1: the slow ones stay there as the next march's joining particles,
-    // alive 6; only the ones joining the beam come to the host)
+    // trapped particles: fast ones join the beam list, slow ones stream again in the next step (split on the device
+    // in list order, z = s1: the slow ones stay there as the next march's joining particles, alive 6; only the ones
+    // joining the beam come to the host)
     std::vector<g3d_particle> add = fast_trapped(c, launch_trapped_split(c, s1));
     for (auto& p : add) {
         p.alive = 1;
