@@ -85,6 +85,26 @@ def test_plasma_channel_cutoff_and_profile_match_reference(ygrid):
 
 
 @needs_ref
+def test_window_shift_moves_the_joining_particles():
+    """A driver strong enough to trap electrons too slow to join the beam: they wait, on the device, to stream
+    again in the next march. A window shift between two steps must move them with everything else, as the
+    reference moves its joining list."""
+    from g3d import configs
+    cfg = configs.lwfa_small(a0=3.0, n0=0.02)
+    s, r = run_pair(cfg, 2)
+    s.step(); r.step()
+    s.shift_window(3, -2); r.shift_window(3, -2)
+    s.step(); r.step()
+    compare_fields(s, r, tol=1e-9, tag="after the shift")
+    ps, pr = s.streaming_particles(), r.streaming_particles()
+    fresh = cfg.nx * cfg.ny * cfg.plasma["ppc_x"] * cfg.plasma["ppc_y"] * 2
+    assert len(ps) == len(pr) > fresh, (len(ps), len(pr), fresh)        # the lattice and joining particles
+    assert np.array_equal(ps["id"], pr["id"]) and np.array_equal(ps["alive"], pr["alive"])
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        assert rel_l2(ps[f], pr[f]) <= 1e-9, (f, rel_l2(ps[f], pr[f]))
+
+
+@needs_ref
 def test_smoothing_and_trapping_small():
     """The smoothing 1/(1 + a^2 k^2) of the streaming current, and a driver strong enough to trap electrons."""
     from g3d import configs
