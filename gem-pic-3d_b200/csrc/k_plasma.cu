@@ -258,31 +258,36 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const Geo& g = c.g;
     const int n = c.n;
     const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn;
+    // The whole state is loaded at once, before any branch or store: a load behind a branch waits for the
+    // branch's own load, and a load behind a store to another array of the state (which the compiler must
+    // assume may alias it) waits for that store. Every index below the count is a valid slot of every array.
+    typedef typename std::conditional<F32, float, double>::type A;
     int alive = S.alive[i];
+    const int sp = S.sp[i];
+    const double zeta = S.zeta[i], x = S.x[i], y = S.y[i], z = S.z[i];
+    const double px_ = S.px[i], py_ = S.py[i], pz_ = S.pz[i], qm_ = S.qm[i];
+    const double qw = S.q[i] * S.w[i];
+    const double sTrap = c.sv->sTrap, s1 = c.sv->s1;
     if (alive == 6) {                 // waiting: joins the march inside the half-cell that holds its zeta
-        if (S.zeta[i] > zn) { alive = 1; if (!c.dry) S.alive[i] = 1; }
+        if (zeta > zn) { alive = 1; if (!c.dry) S.alive[i] = 1; }
         else return d;
     }
     if (alive != 1) return d;
-    const double zeta = S.zeta[i];
     const double hl = zeta >= zn1 - 1e-9 * h ? h : (zeta - zn > 0 ? zeta - zn : 0.0);
-    const int sp = S.sp[i];
     const bool ion = sp >= SP_ION && sp < SP_FREED;
     if (ion && !c.ions[sp - SP_ION].mobile) {        // fixed ion: its charge, then the ionization
-        const double f = S.q[i] * S.w[i] * hl / (c.Delta * h * g.dx);
-        if (f != 0) d = DepReq{S.x[i], S.y[i], f, 0, 0, 0, true};
+        const double f = qw * hl / (c.Delta * h * g.dx);
+        if (f != 0) d = DepReq{x, y, f, 0, 0, 0, true};
         if (!c.dry) S.zeta[i] = zn;
         if constexpr (ION) {
-            const double E1 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zeta), E0 = field_abs<F32>(c, S.x[i], S.y[i], S.z[i], zn);
+            const double E1 = field_abs<F32>(c, x, y, z, zeta), E0 = field_abs<F32>(c, x, y, z, zn);
             ionize(c, S, i, E1, E0, hl);
         }
         return d;
     }
     // the push in A (FP32 in the mixed form: the gathered fields are FP32 already; the positions, z and zeta stay
     // FP64 and take FP32 displacements, the momenta are kept in FP64 between half-cells)
-    typedef typename std::conditional<F32, float, double>::type A;
-    const double x = S.x[i], y = S.y[i], z = S.z[i];
-    const A px = A(S.px[i]), py = A(S.py[i]), pz = A(S.pz[i]), qm = A(S.qm[i]);
+    const A px = A(px_), py = A(py_), pz = A(pz_), qm = A(qm_);
     const A g0 = sqrt(A(1) + px * px + py * py + pz * pz), ig0 = A(1) / g0;
     const A omv0 = (A(1) + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
     const A dt0 = A(hl) / omv0;
@@ -308,7 +313,6 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     A vx = A(0.5) * (px * ig0 + ux * ig1), vy = A(0.5) * (py * ig0 + uy * ig1), vz = A(0.5) * (pz * ig0 + uz * ig1);
     double zeta_end = zn;
     bool trapped = false;
-    const double sTrap = c.sv->sTrap;
     if (z + double(vz * dt) >= sTrap) {       // advanced trap_advance steps inside this half-cell: trapped
         const double vv = double(vz) > 1e-3 ? double(vz) : 1e-3;
         const double dtp = (sTrap - z) / vv > 0 ? (sTrap - z) / vv : 0.0;
@@ -324,12 +328,11 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double xn = x + double(vx * dt), yn = y + double(vy * dt);
     if (!c.dry) {
         S.x[i] = xn; S.y[i] = yn;
-        S.z[i] = trapped ? c.sv->s1 : z + double(vz * dt);
+        S.z[i] = trapped ? s1 : z + double(vz * dt);
         S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
         S.zeta[i] = zeta_end;
     }
-    const double q = S.q[i], w = S.w[i];
-    const double f = q * w * double(dt) / (c.Delta * h * g.dx);
+    const double f = qw * double(dt) / (c.Delta * h * g.dx);
     if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true};
     if (!g.yf && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
         if (!c.dry) S.alive[i] = 0;
@@ -342,7 +345,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         if (!c.dry) S.alive[i] = 5;
         const double vze = double(uz * ig1);
         if (vze >= c.vz_beam)         // joins the beam list: its beam current of level s1 from now on
-            sdeposit<F32>(c, xn, yn, q * w / (h * g.dx * vze), double(ux * ig1), double(uy * ig1), vze);
+            sdeposit<F32>(c, xn, yn, qw / (h * g.dx * vze), double(ux * ig1), double(uy * ig1), vze);
     }
     return d;
 }
