@@ -227,15 +227,15 @@ def reference_config(cfg):
     return cfg
 
 
-def reference_rate(cfg, steps, threads, k=None):
+def reference_rate(cfg, steps, threads, k=None, warmup=0):
     """Reference CPU/OpenMP build on `threads` host threads: (pushes/s, description of the sample, ms per step)
     or (None, why, None).
 
-    Without plasma: init (untimed), then `steps` s-steps of the full workload. With plasma one step of the full
-    window takes minutes on a host, so the sample is one step (after an untimed init) on two shorter windows of the
-    same length and particles, 64 and 128 slices; their times fit t(N) = a + b N (the beam push and the set-up in
-    a, the half-cell march in b) and the full window's step time is t(nzeta). Pushes per step = beam particles +
-    the streaming particles of the step."""
+    Without plasma: init and `warmup` s-steps (untimed), then `steps` s-steps of the full workload. With plasma
+    one step of the full window takes minutes on a host, so the sample is run on two shorter windows of the same
+    length and particles, 64 and 128 slices: init and `warmup` s-steps (untimed), then `steps` s-steps whose mean
+    time fits t(N) = a + b N (the beam push and the set-up in a, the half-cell march in b); the full window's step
+    time is t(nzeta). Pushes per step = beam particles + the streaming particles of the last step."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import ref
     if not ref.available():
@@ -244,29 +244,35 @@ def reference_rate(cfg, steps, threads, k=None):
         r = ref.RefSimulation(reference_config(cfg), threads=threads)
         r.load_bunch()
         r.init_fields()
+        for _ in range(warmup):
+            r.step()
         t0 = time.perf_counter()
         for _ in range(steps):
             r.step()
         dt = time.perf_counter() - t0
         r.close()
-        return cfg.particles * steps / dt, (f"the full workload, init untimed then {steps} s-steps, OpenMP on "
-                                            f"{threads} threads"), dt / steps * 1e3
+        return cfg.particles * steps / dt, (f"the full workload, init and {warmup} s-steps untimed, then {steps} "
+                                            f"timed s-steps, OpenMP on {threads} threads"), dt / steps * 1e3
     pts = []
     S = 0
     for nz in (64, 128):
         c2 = reference_config(workload(k, nz, cfg.particles))
         r = ref.RefSimulation(c2, threads=threads)
         r.init()
+        for _ in range(warmup):
+            r.step()
         t0 = time.perf_counter()
-        r.step()
-        pts.append((nz, time.perf_counter() - t0))
+        for _ in range(steps):
+            r.step()
+        pts.append((nz, (time.perf_counter() - t0) / steps))
         S = len(r.streaming_particles())
         r.close()
     (n1, t1), (n2, t2) = pts
     b = (t2 - t1) / (n2 - n1)
     t_full = t1 + b * (cfg.nzeta - n1)
     return (cfg.particles + S) / t_full, (
-        f"one s-step (after an untimed init) on windows of 64 and 128 slices ({t1:.2f} s, {t2:.2f} s), "
+        f"{steps} s-step(s) after an untimed init and {warmup} untimed s-step(s), on windows of 64 and 128 slices "
+        f"({t1:.2f} s, {t2:.2f} s per step), "
         f"extrapolated linearly in the slice count to {cfg.nzeta} slices ({t_full:.1f} s per step); pushes = "
         f"{cfg.particles} beam + {S} streaming particles; OpenMP on {threads} threads"), t_full * 1e3
 
@@ -304,7 +310,8 @@ def run_reference_arm(a):
     cfg = workload(a.workload, a.nzeta, a.particles)
     cores = host_cores()
     steps = max(1, min(a.steps, 3))
-    v, why, ms = reference_rate(cfg, steps, cores, a.workload)
+    warm = max(0, min(a.warmup, 3))       # warm-up s-steps of the sample, capped so that the run ends in minutes
+    v, why, ms = reference_rate(cfg, steps, cores, a.workload, warmup=warm)
     if v is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
         return
@@ -312,7 +319,7 @@ def run_reference_arm(a):
     if cfg.params.get("laser_envelope") == 1:
         sample += " (Gaussian envelope of FWHM 60 in place of the flat top, which the reference lacks)"
     print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
-                      "steps": steps, "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                      "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                       "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bunch sampler of the reference)",
                       "config": config_json(cfg, a.workload),
                       "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
@@ -487,7 +494,7 @@ def run_g3d(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
-        v, why, _ = reference_rate(cfg, 3, cores, a.workload)
+        v, why, _ = reference_rate(cfg, 1 if cfg.plasma is not None else 3, cores, a.workload)   # ~10-30 s of host work
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": "reference OpenMP build: " + why}
 
     if dist:
