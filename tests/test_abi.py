@@ -103,3 +103,16 @@ def test_sample_bunches_rejects_bad_input():
     cfg.bunches[0]["gamma"] = 0.5
     with pytest.raises(G3DError):
         sample_bunches(cfg)
+
+
+def test_march_objective_checks_its_tensors_before_any_device_work():
+    """The autograd wrapper of the adjoint march rejects mis-shaped inputs on the host, before a context is made."""
+    import torch
+    from g3d import configs
+    from g3d.autograd import MarchObjective
+    cfg = configs.config1(nx=16, ny=16, nzeta=32, nmacro=10, steps=1)
+    dp = torch.zeros(10, 3, dtype=torch.float64)
+    with pytest.raises(ValueError, match=r"coef must be \[16, 9, 2\]"):
+        MarchObjective.apply(torch.zeros(16, 16, 2, dtype=torch.float64), dp, cfg)
+    with pytest.raises(ValueError, match=r"coef must be"):
+        MarchObjective.apply(torch.zeros(16, 9, dtype=torch.float64), dp, cfg)
