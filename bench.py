@@ -227,15 +227,32 @@ def reference_config(cfg):
     return cfg
 
 
+SAMPLE_SLICES = (256, 512)      # the reference's sample windows of a plasma workload, at the workload's own h
+
+
+def sample_config(cfg, k, n):
+    """The plasma workload k (configured as cfg) on a window of n slices at cfg's slice step h: the transverse grid,
+    plasma, ions, laser and witness unchanged, a shorter window."""
+    from g3d import configs
+    if k != 3:
+        raise ValueError(f"no sampled window for workload {k}")
+    return configs.config3(nzeta=n, h=cfg.h, nmacro=cfg.particles)
+
+
 def reference_rate(cfg, steps, threads, k=None, warmup=0):
     """Reference CPU/OpenMP build on `threads` host threads: (pushes/s, description of the sample, ms per step)
     or (None, why, None).
 
-    Without plasma: init and `warmup` s-steps (untimed), then `steps` s-steps of the full workload. With plasma
-    one step of the full window takes minutes on a host, so the sample is run on two shorter windows of the same
-    length and particles, 64 and 128 slices: init and `warmup` s-steps (untimed), then `steps` s-steps whose mean
-    time fits t(N) = a + b N (the beam push and the set-up in a, the half-cell march in b); the full window's step
-    time is t(nzeta). Pushes per step = beam particles + the streaming particles of the last step."""
+    Without plasma: init and `warmup` s-steps (untimed), then `steps` s-steps of the full workload. With plasma one
+    step of the full window takes minutes on a host (about 5 min on 8 cores for 2048 slices), so the sample is the
+    same workload on two shorter windows at the workload's own slice step h (SAMPLE_SLICES slices; the transverse
+    grid, plasma, ions, laser and witness are the workload's): init and `warmup` s-steps untimed, then `steps` timed
+    s-steps per window. The step time is t(N) = a + b N in the slice count N (the beam push and deposit of the
+    witness and the per-step set-up in a; the half-cell march of the streaming plasma, the same work per slice at a
+    fixed h, in b), fitted through the two windows and evaluated at the workload's nzeta. A fit that is not
+    increasing in N, or a non-positive step time, returns (None, why, None) rather than a number. Pushes per step =
+    beam particles + the streaming particles of the last step (loaded per step from the transverse lattice, the same
+    count at any window length)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import ref
     if not ref.available():
@@ -253,10 +270,14 @@ def reference_rate(cfg, steps, threads, k=None, warmup=0):
         r.close()
         return cfg.particles * steps / dt, (f"the full workload, init and {warmup} s-steps untimed, then {steps} "
                                             f"timed s-steps, OpenMP on {threads} threads"), dt / steps * 1e3
+    if k is None or cfg.nzeta <= SAMPLE_SLICES[-1]:
+        return None, "no sampled windows for this workload", None
     pts = []
     S = 0
-    for nz in (64, 128):
-        c2 = reference_config(workload(k, nz, cfg.particles))
+    for nz in SAMPLE_SLICES:
+        c2 = reference_config(sample_config(cfg, k, nz))
+        if c2.particles != cfg.particles or abs(c2.h - cfg.h) > 1e-12 * cfg.h:
+            return None, f"sample window of {nz} slices does not keep the workload's h and particles", None
         r = ref.RefSimulation(c2, threads=threads)
         r.init()
         for _ in range(warmup):
@@ -270,11 +291,15 @@ def reference_rate(cfg, steps, threads, k=None, warmup=0):
     (n1, t1), (n2, t2) = pts
     b = (t2 - t1) / (n2 - n1)
     t_full = t1 + b * (cfg.nzeta - n1)
+    if not (b > 0) or not (t_full > 0):
+        return None, (f"reference sample not increasing in the slice count ({n1}: {t1:.2f} s, {n2}: {t2:.2f} s per "
+                      f"step); no extrapolation"), None
     return (cfg.particles + S) / t_full, (
-        f"{steps} s-step(s) after an untimed init and {warmup} untimed s-step(s), on windows of 64 and 128 slices "
-        f"({t1:.2f} s, {t2:.2f} s per step), "
-        f"extrapolated linearly in the slice count to {cfg.nzeta} slices ({t_full:.1f} s per step); pushes = "
-        f"{cfg.particles} beam + {S} streaming particles; OpenMP on {threads} threads"), t_full * 1e3
+        f"{steps} timed s-step(s) per window after an untimed init and {warmup} untimed s-step(s), on windows of "
+        f"{n1} and {n2} slices at the workload's h = {cfg.h:g} (same 256x256 transverse grid, plasma, ions, laser and "
+        f"witness; {t1:.2f} s and {t2:.2f} s per step), t = a + b N fitted through them and evaluated at N = "
+        f"{cfg.nzeta} ({t_full:.1f} s per step); pushes = {cfg.particles} beam + {S} streaming particles; OpenMP on "
+        f"{threads} threads"), t_full * 1e3
 
 
 def host_cores():
@@ -309,8 +334,10 @@ def run_reference_arm(a):
         return
     cfg = workload(a.workload, a.nzeta, a.particles)
     cores = host_cores()
-    steps = max(1, min(a.steps, 3))
-    warm = max(0, min(a.warmup, 3))       # warm-up s-steps of the sample, capped so that the run ends in minutes
+    # per sample window: at most 1 warm-up and 2 timed s-steps, so that the arm ends in a few minutes (a 512-slice
+    # step of the laser-plasma workload takes ~45 s on 16 host cores)
+    steps = max(1, min(a.steps, 2))
+    warm = max(0, min(a.warmup, 1))
     v, why, ms = reference_rate(cfg, steps, cores, a.workload, warmup=warm)
     if v is None:
         print(json.dumps({"impl": "reference", "unavailable": why}))
@@ -494,7 +521,9 @@ def run_g3d(a):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cores = host_cores()
-        v, why, _ = reference_rate(cfg, 1 if cfg.plasma is not None else 3, cores, a.workload)   # ~10-30 s of host work
+        # the reference arm's sample with one warm-up and one timed s-step per window (about 2-3 min of host time
+        # for the laser-plasma workload on 16 cores; 3 steps of the full workload without plasma)
+        v, why, _ = reference_rate(cfg, 1 if cfg.plasma is not None else 3, cores, a.workload, warmup=1)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": "reference OpenMP build: " + why}
 
     if dist:

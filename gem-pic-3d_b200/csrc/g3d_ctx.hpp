@@ -167,6 +167,7 @@ struct Ctx {
     DevBuf<g3d_particle> pstage;                 // device staging of the 104-byte records
     PartsDev parts{};
     long np = 0, pcap = 0;
+    int nbunch = 1;                              // bunch blocks of the last g3d_load_bunches (sp = 0, -1, ...)
     DevBuf<int32_t> perm;                        // particles in cell order (k_sort.cu); storage order unchanged
     DevBuf<uint32_t> sort_keys;                  // sort buffers, sized for the particle capacity
     DevBuf<int32_t> sort_idx;
@@ -182,7 +183,8 @@ struct Ctx {
     LaserDev laser{};
     AxisDev zax{}, yax{};
     std::deque<std::array<double, 3>> cent_;     // centroid sums awaiting their step (window lag)
-    // stream, launches, profiling
+    // device, stream, launches, profiling
+    int device = 0;                              // the CUDA device current at g3d_create; every call runs on it
     cudaStream_t stream = nullptr;
     long launches = 0;
     bool profiling = false;

@@ -477,6 +477,7 @@ static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int c
     sample_bunches(G, c.P, list, count, mine, lost, c.X0, c.Y0);
     set_particles(c, mine.data(), long(mine.size()));
     c.lost_total += lost;
+    c.nbunch = count > 1 ? count : 1;
 }
 
 // ---------------------------------------------------------------- the march path
@@ -552,6 +553,38 @@ static void comoving_field(Ctx& c) {
     else if (c.mixed) launch_comoving_f(c, beta, gm2);
     else launch_comoving(c, beta, gm2);
 }
+// Several bunch blocks (reference Simulation::comoving_fields_per_bunch, src/sim_bunches.cpp:223-248): the co-moving
+// equation -(Lap_perp + gamma^-2 d_zeta^2) psi = rho is linear but its gamma is the bunch's, so each block k (the
+// particles with sp == -k, in storage order) gets its own currents and co-moving R with its own beta, and the R of
+// the blocks are summed in block order into zeroed accumulators. The currents are then those of all particles, and
+// the beta kept for the sponge's bound field is the mean over all of them. Init only: the blocks go through host
+// records.
+static void comoving_fields_per_bunch(Ctx& c) {
+    const std::vector<g3d_particle> all = get_particles(c);
+    const size_t n = size_t(c.ns) * c.nkh;
+    DevBuf<cpx> sx, sy;                          // alloc zeroes them
+    sx.alloc(n, c.stream); sy.alloc(n, c.stream);
+    std::vector<g3d_particle> one;
+    for (int k = 0; k < c.nbunch; ++k) {
+        one.clear();
+        for (const g3d_particle& p : all)
+            if (p.sp == -k) one.push_back(p);
+        set_particles(c, one.data(), long(one.size()));
+        currents(c);
+        comoving_field(c);
+        launch_axpy_c(c, sx.p, c.Rx.p, 1.0, n);
+        launch_axpy_c(c, sy.p, c.Ry.p, 1.0, n);
+    }
+    set_particles(c, all.data(), long(all.size()));
+    currents(c);
+    launch_copy_c(c, c.Rx.p, sx.p, n);
+    launch_copy_c(c, c.Ry.p, sy.p, n);
+    double sums[2];
+    launch_beta_sums(c, sums);
+    c.beta_b = sums[1] > 0 ? sums[0] / sums[1] : 1;
+    c.gm2_b = 1 - c.beta_b * c.beta_b;
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
 static void relax_start_field(Ctx& c) {
     const size_t n = size_t(c.ns) * c.nkh, nj = size_t(c.ns + 1) * c.nkh;
     if (c.mixed) {
@@ -625,8 +658,8 @@ static void init_fields(Ctx& c) {
     c.fields_ready = true;
     if (c.P.self_fields) {
         c.starting_ = true;
-        currents(c);
-        comoving_field(c);
+        if (c.nbunch > 1) comoving_fields_per_bunch(c);
+        else { currents(c); comoving_field(c); }
         if (c.P.start_relax) relax_start_field(c);
         add_grid_lasers(c);
         march(c, 0.0);
@@ -1052,6 +1085,8 @@ namespace {
 template <class Fn>
 int guarded(g3d_ctx* ctx, Fn&& fn) {
     try {
+        // every call works on the device the context was created on, whatever device the calling thread has current
+        if (ctx) G3D_CUDA(cudaSetDevice(ctx->c.device));
         fn();
         if (ctx) ctx->c.err.clear();
         return G3D_OK;
@@ -1080,6 +1115,7 @@ int g3d_create(const g3d_grid* grid, const g3d_params* params, g3d_ctx** out) {
     }
     g3d_ctx* ctx = new g3d_ctx();
     try {
+        G3D_CUDA(cudaGetDevice(&ctx->c.device));
         G3D_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         g3d::setup(ctx->c, *grid, *params);
     } catch (const Error& e) {
@@ -1098,6 +1134,7 @@ int g3d_create(const g3d_grid* grid, const g3d_params* params, g3d_ctx** out) {
 void g3d_destroy(g3d_ctx* ctx) {
     if (!ctx) return;
     Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto& pe : c.pending) { cudaEventDestroy(pe.e0); cudaEventDestroy(pe.e1); }
     for (auto e : c.event_pool) cudaEventDestroy(e);
@@ -1124,7 +1161,6 @@ int g3d_get_particles(g3d_ctx* ctx, g3d_particle* out, int64_t capacity, int64_t
 int g3d_load_bunches(g3d_ctx* ctx, const g3d_bunch* b, int32_t count) {
     return guarded(ctx, [&] {
         if (count < 0 || (count > 0 && !b)) throw Error(G3D_ERR_ARG, "bad bunch list");
-        if (count > 1) throw Error(G3D_ERR_ARG, "one bunch block per run in this release");
         Ctx& c = ctx->c;
         const g3d_grid G{c.nx, c.ny, c.N, c.yf ? 1 : 0, c.nx * c.dx, c.ny * c.dy, c.zeta.data(),
                          c.yf ? nullptr : c.ynode_h.data()};

@@ -2,6 +2,7 @@
 // march half-cell by half-cell with its passes, prediction and correction, the freed electrons, trapping and
 // restreaming (src/sim_plasma.cpp:21-491, src/sim_ions.cpp:68-87, src/ionization.cpp:28-53), and the grid
 // lasers of the start field (src/sim_fields.cpp:321-374).
+#include <cstdlib>
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -193,6 +194,12 @@ static void load_plasma(Ctx& c, double s0, double s1) {
     for (const auto& p : P.joining)
         if (p.sp >= SP_ION && p.sp < SP_FREED && P.ions[size_t(p.sp - SP_ION)].ionization)
             cap += P.ions[size_t(p.sp - SP_ION)].Zmax - std::lround(p.q);
+    // G3D_BORN_CAPACITY_LIMIT (environment, > 0): a smaller list of freed electrons than the ionization can fill, so
+    // that the overflow check (device flag -> G3D_ERR_CAPACITY) can be exercised; every write stays inside the list
+    if (const char* lim = std::getenv("G3D_BORN_CAPACITY_LIMIT")) {
+        const long l = std::atol(lim);
+        if (l > 0 && l < cap) cap = l;
+    }
     const long jd = P.njb;                               // joining on the device (the last march's slow trapped)
     const long n = fresh + jd + long(P.joining.size());
     P.fresh_last = fresh;

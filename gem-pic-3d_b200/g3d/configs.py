@@ -209,18 +209,23 @@ def config2(nx=128, ny=128, nzeta=1024, nmacro=1048576, steps=100, envelope=abi.
     return RunConfig("oblique plane wave on a bunch", nx, ny, nzeta, L, L, h, p, [b], steps)
 
 
-def config3(nx=256, ny=256, nzeta=2048, nmacro=4194304, steps=200, charge_pC=10.0):
+def config3(nx=256, ny=256, nzeta=2048, nmacro=4194304, steps=200, charge_pC=10.0, h=None):
     """Laser wakefield with streaming plasma: 256x256 modes, 2048 slices (h = 0.2), n0 = 0.002 n_c with 2x2 electrons
     per cell and mobile H+ ions, Gaussian grid laser a0 = 2, w0 = 20, tau_FWHM = 30 (1/omega0), focus at s = 0,
     a witness bunch of 4,194,304 electrons (gamma 200, sigma_perp 1, sigma_zeta 2) 60 behind the laser peak,
-    200 s-steps of 10."""
+    200 s-steps of 10.
+
+    h None: fewer slices keep the window of 409.4 (a coarser h). h given (0.2: the workload's own step): a window of
+    h (nzeta - 1), shorter with fewer slices; the laser peak then sits min(0.8 window, window - 20) from the rear and
+    the witness min(60, 0.6 x that) behind it, which is the full workload's placement at 2048 slices."""
     lam = 0.8e-6
-    h = 0.2 * (2047 / (nzeta - 1))
+    if h is None:
+        h = 0.2 * (2047 / (nzeta - 1))
     dz = 10.0
     L = 80.0
     window = h * (nzeta - 1)
-    zl = 0.8 * window                      # laser peak
-    zb = zl - 60.0                         # witness centre
+    zl = min(0.8 * window, window - 20.0)  # laser peak
+    zb = zl - min(60.0, 0.6 * zl)          # witness centre
     b = dict(charge_C=charge_pC * 1e-12, gamma=200.0, sigx=1.0, sigy=1.0, sigz=2.0, emitx=0.0, emity=0.0,
              espread=0.0, zeta_center=zb, nmacro=nmacro, seed=1)
     p = dict(lambda0=lam, dz=dz, dz_push=dz, z_end=dz * steps, sponge=0.1 * L, sponge_y=0.1 * L, zeta_center=zb,
@@ -302,6 +307,77 @@ def config4(nx=64, ny=64, nzeta=512, nmacro=65536, steps=40, gamma=100.0, a0=1.0
                      [], gl)
 
 
+def walled_ynode(half, dy0, core, grow, wall):
+    """Nodes of a free-hand y grid between conducting walls at -wall and +wall, symmetric about 0, `half` cells a
+    side: cells of dy0 for |y| < core, then cells growing by a constant ratio <= grow up to a size d, then cells of
+    d out to the wall. d (and the ratio) are found so that the cells end exactly at the wall."""
+    n_core = int(round(core / dy0))
+
+    def side(d):
+        ng = max(1, math.ceil(math.log(d / dy0) / math.log(grow) - 1e-12)) if d > dy0 else 0
+        r = (d / dy0) ** (1.0 / ng) if ng else 1.0
+        cells = [dy0] * n_core + [dy0 * r ** k for k in range(1, ng + 1)]
+        cells += [d] * (half - len(cells))
+        return cells[:half]
+    lo, hi = dy0, wall
+    for _ in range(200):                      # the outer cell size d that lands on the wall
+        mid = 0.5 * (lo + hi)
+        if sum(side(mid)) < wall:
+            lo = mid
+        else:
+            hi = mid
+    cells = np.array(side(hi))
+    cells *= wall / cells.sum()               # the last rounding: exactly at the wall
+    pos = np.concatenate([[0.0], np.cumsum(cells)])
+    return np.concatenate([-pos[:0:-1], pos])
+
+
+def stepped_zeta(nzeta, h_fine, h_coarse, ratio, fine_frac=0.2, front_frac=0.25):
+    """Slice positions of a free-hand zeta grid with nzeta slices: from the rear, coarse steps h_coarse, steps
+    shrinking by `ratio` down to h_fine, a fine region of fine_frac of the slices, steps growing back by `ratio`, and
+    coarse steps to the front (front_frac of the coarse slices in front of the fine region). Returns (zeta, start
+    and end of the fine region)."""
+    ramp = [h_fine * ratio ** k for k in range(1, 1 + math.ceil(math.log(h_coarse / h_fine) / math.log(ratio)))]
+    ramp = [min(h, h_coarse) for h in ramp]
+    n_steps = nzeta - 1
+    n_fine = max(1, int(fine_frac * n_steps))
+    n_coarse = n_steps - n_fine - 2 * len(ramp)
+    if n_coarse < 2:
+        raise ValueError("too few slices for the graded zeta grid")
+    n_front = max(1, int(front_frac * n_coarse))
+    steps = [h_coarse] * (n_coarse - n_front) + ramp[::-1] + [h_fine] * n_fine + ramp + [h_coarse] * n_front
+    z = np.concatenate([[0.0], np.cumsum(steps)])
+    f0 = n_coarse - n_front + len(ramp)
+    return z, float(z[f0]), float(z[f0 + n_fine])
+
+
+def config5(nx=256, half=96, nzeta=4096, ppc=13, steps=100, a0=2.5):
+    """Ionization injection on free-hand grids: x of 256 Fourier modes over 80; y a table between conducting walls at
+    +-40, cells of 0.1 for |y| < 4 growing by <= 15 % a cell to the outer size (2 x 96 cells, 193 nodes); zeta a table
+    of 4096 slices, h = 0.05 in the injection region (a fifth of the slices, behind the laser) grading by 5 % a slice
+    to h = 0.5 elsewhere. The gas is 99 % H2 (as atomic H at twice the density) and 1 % N, neutral, ionized by ADK
+    over all levels (NIST energies), n0 = 0.001 n_c, no free electrons; a Gaussian grid laser a0 = 2.5, w0 = 15,
+    FWHM 30, focus at s = 0, 30 behind the window front; 100 s-steps of 10. The macro-particles of a step are the
+    lattice points of the 256 x 190 cells inside the walls times ppc x ppc per cell times the two species:
+    16,440,320 at ppc = 13 (the workload's 16,777,216 rounded down to a square lattice)."""
+    lam = 0.8e-6
+    L = 80.0
+    y = walled_ynode(half, 0.1, 4.0, 1.15, 40.0)
+    z, f0, f1 = stepped_zeta(nzeta, 0.05, 0.5, 1.05)
+    window = float(z[-1])
+    zl = window - 30.0
+    p = dict(lambda0=lam, dz=10.0, dz_push=10.0, z_end=10.0 * steps, sponge=0.1 * L, sponge_y=4.0,
+             zeta_center=0.5 * (f0 + f1), move_x=0, move_y=0)
+    plasma = dict(n0=0.001, ppc_x=ppc, ppc_y=ppc, free_electrons=0, seed=5)
+    ion_list = [ion_species("H", 0, 2 * 0.99, ionization=True), ion_species("N", 0, 0.01, ionization=True)]
+    gl = [dict(a0=a0, kL=1.0, waist=15.0, tau=30.0, zeta_c=zl, z_focus=0.0)]
+    cfg = RunConfig("ionization injection on free-hand y and zeta grids", nx, 2 * half, nzeta, L, float(y[-1] - y[0]),
+                    0.05, p, [], steps, plasma, ion_list, gl)
+    cfg.ynode = y
+    cfg.zeta_table = z
+    return cfg
+
+
 def baseline(k, **kw):
     if k == 1:
         return config1(**kw)
@@ -309,6 +385,8 @@ def baseline(k, **kw):
         return config2(**kw)
     if k == 3:
         return config3(**kw)
+    if k == 5:
+        return config5(**kw)
     raise NotImplementedError(f"workload {k} is not built by this release")
 
 

@@ -8,7 +8,9 @@
  * sizes, and returns an int status (G3D_OK = 0). A non-zero status leaves a message in
  * g3d_last_error(). Calls are synchronous at the ABI: they return after the work queued on
  * the context's own CUDA stream has finished, unless the name ends in `_async`.
- * One context = one GPU = one host thread (the reference runs one host thread per rank).
+ * One context = one GPU = one host thread (the reference runs one host thread per rank). A context keeps the
+ * device that was current at g3d_create and makes it current at the start of every call that takes the context,
+ * so a caller may switch devices between calls.
  *
  * Units are the reference's code units (README.md:43-45): c = 1, lengths 1/k0, times
  * 1/omega0, momenta m c, fields m c omega0 / e, densities n_c.
@@ -31,7 +33,9 @@ typedef struct g3d_ctx g3d_ctx;
 #define G3D_OK            0
 #define G3D_ERR_CUDA      1   /* a CUDA call failed (reference: gpu_check, src/portable.hpp:43-49) */
 #define G3D_ERR_TIMEOUT   2   /* a bounded device-side wait gave up */
-#define G3D_ERR_CAPACITY  3   /* a fixed-capacity list overflowed */
+#define G3D_ERR_CAPACITY  3   /* a fixed-capacity list overflowed (the list of electrons freed by ionization is
+                                 sized for every level of every ion; the environment variable
+                                 G3D_BORN_CAPACITY_LIMIT = n > 0 caps it at n to exercise this check) */
 #define G3D_ERR_ARG       4   /* an invalid argument (sizes, grid, unknown array id) */
 #define G3D_ERR_STATE     5   /* an entry point called in the wrong state */
 #define G3D_ERR_IO        6   /* checkpoint file missing, truncated or not a checkpoint */

@@ -195,3 +195,33 @@ def test_checkpoint_is_read_by_the_reference(tmp_path):
         assert np.array_equal(x[:, :, : cfg.nx // 2 + 1], y[:, :, : cfg.nx // 2 + 1]), a
     assert_state(got, ref_, FIELDS, 1e-14, comp_tol=1e-9)
     assert s2.status().istep == 2
+
+
+@needs_ref
+def test_two_bunch_blocks_match_the_reference():
+    """A driver and a witness block with different gamma: each block gets the co-moving field of its own beta and
+    the fields are summed, while the sponge's bound field keeps the mean beta of all particles (reference
+    Simulation::comoving_fields_per_bunch, src/sim_bunches.cpp:223-248); then two s-steps."""
+    from g3d import Simulation, configs
+    cfg = configs.config1(nx=32, ny=32, nzeta=64, nmacro=20000, steps=2)
+    drv = dict(cfg.bunches[0])
+    wit = dict(drv, gamma=50.0, zeta_center=30.0, nmacro=6000, seed=7, charge_C=0.3 * drv["charge_C"])
+    cfg.bunches = [drv, wit]
+    cfg.params.update(sponge=4.0, sponge_y=4.0)
+    r = ref.RefSimulation(cfg, threads=1)
+    r.init()
+    s = Simulation(cfg)
+    s.init()
+    p, q = s.host_particles(), r.host_particles()
+    assert set(np.unique(p["sp"])) == {0, -1}
+    for f in p.dtype.names:
+        assert np.array_equal(p[f], q[f]), f
+    assert s.status().beta_b == r.status().beta_b          # the mean over both blocks, summed in the same order
+    assert_state({a: s.array(a) for a in FIELDS}, {a: r.array(a) for a in FIELDS}, FIELDS, TOL_SPEC, tag="init")
+    for _ in range(2):
+        s.step(); r.step()
+    assert_state({a: s.array(a) for a in FIELDS}, {a: r.array(a) for a in FIELDS}, FIELDS, TOL_SPEC, tag="step2")
+    p, q = s.host_particles(), r.host_particles()
+    for f in ["x", "y", "zeta", "px", "py", "pz"]:
+        assert rel_l2(p[f], q[f]) <= TOL_SPEC, f
+    assert rel_l2(s.array("F"), r.array("F")) <= TOL_F
