@@ -141,6 +141,8 @@ struct Ctx {
     DevBuf<cpx> j0x, j0y, jkx, jky, jkz;         // ns+1 half-cell planes
     DevBuf<cpx> jzg;                             // 2 ghost planes of filtered j_z (zero on one rank)
     DevBuf<double> jw;                           // 3 x (ns+3) real planes
+    DevBuf<double> depfix;                       // the fixed-point deposit's bound partials and scale (k_currents.cu)
+    double ia_max = 0;                           // the largest dual-cell factor 1/A_j, 1/Delta_j of the y grid
     DevBuf<float> F;                             // 6 x (ns+2) real planes
     DevBuf<double> Fd;                           // exact fields: F kept in FP64 too, gathered by the beam push
                                                  // (the differentiable forward of the gradient check), or empty
@@ -208,6 +210,8 @@ struct Ctx {
 
 // ---------------------------------------------------------------- launchers (k_*.cu)
 void launch_deposit(Ctx& c);
+const double* launch_deposit_scale(Ctx& c, double ia_max);   // fixed-point deposit: its scale, then the planes to doubles
+void launch_deposit_finish(Ctx& c);
 void launch_cur_fft(Ctx& c, bool keep0);
 void launch_march(Ctx& c, double D);
 // free-hand y (k_freehand.cu)

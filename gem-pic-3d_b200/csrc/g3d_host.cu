@@ -1,5 +1,6 @@
 // Host side of libg3d: the context (grids, tables, buffers), the orchestration of a step, the bunch
 // loader, checkpoints and the extern "C" entry points of include/g3d.h.
+#include <limits>
 #include <algorithm>
 #include <mutex>
 #include <map>
@@ -135,138 +136,220 @@ void Ctx::check_launch(const char* what) {
 }
 
 // ---------------------------------------------------------------- set-up (reference sim_setup.cpp:5-164)
-// Eigenvalues and eigenvectors of a symmetric tridiagonal matrix (diagonal d, off-diagonal e[i] between i and
-// i + 1) by the implicit QL method with Wilkinson shifts (the published tql2 / tqli algorithm). On return d holds
-// the eigenvalues and z (n x n, row-major) the eigenvectors as columns: z[k n + m] is component k of vector m.
-static bool tridiagonal_eigen(std::vector<double>& d, std::vector<double> e, std::vector<double>& z) {
-    const int n = int(d.size());
-    z.assign(size_t(n) * n, 0.0);
-    for (int i = 0; i < n; ++i) z[size_t(i) * n + i] = 1;
-    e.resize(size_t(n), 0.0);
-    e[size_t(n - 1)] = 0;
-    for (int l = 0; l < n; ++l) {
-        int iter = 0, m;
-        do {
-            for (m = l; m < n - 1; ++m) {
-                const double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
-                if (std::fabs(e[m]) <= 1e-16 * dd) break;
-            }
-            if (m != l) {
-                if (iter++ == 100) return false;
-                double g = (d[l + 1] - d[l]) / (2 * e[l]);
-                double r = std::hypot(g, 1.0);
-                g = d[m] - d[l] + e[l] / (g + std::copysign(r, g));
-                double sn = 1, cs = 1, p = 0;
-                int i;
-                bool underflow = false;
-                for (i = m - 1; i >= l; --i) {
-                    double f = sn * e[i];
-                    const double b = cs * e[i];
-                    r = std::hypot(f, g);
-                    e[i + 1] = r;
-                    if (r == 0) { d[i + 1] -= p; e[m] = 0; underflow = true; break; }
-                    sn = f / r; cs = g / r;
-                    g = d[i + 1] - p;
-                    r = (d[i] - g) * sn + 2 * cs * b;
-                    p = sn * r;
-                    d[i + 1] = g + p;
-                    g = cs * r - b;
-                    for (int k = 0; k < n; ++k) {            // the rotation of columns i, i + 1
-                        f = z[size_t(k) * n + i + 1];
-                        z[size_t(k) * n + i + 1] = sn * z[size_t(k) * n + i] + cs * f;
-                        z[size_t(k) * n + i] = cs * z[size_t(k) * n + i] - sn * f;
-                    }
-                }
-                if (underflow) continue;
-                d[l] -= p; e[l] = g; e[m] = 0;
-            }
-        } while (m != l);
+// Eigenpairs of a symmetric tridiagonal matrix T with diagonal t[0..n) and nonzero couplings u[i] between rows i and
+// i + 1 (an irreducible T: its eigenvalues are simple).
+//  * Eigenvalues by bisection on Sturm counts (Givens 1954; Barth, Martin & Wilkinson 1967): the number of negative
+//    pivots of the LDL^T factorisation of T - x I is the number of eigenvalues below x, so the k-th eigenvalue is
+//    bracketed inside the Gershgorin interval and halved down to the spacing of doubles.
+//  * Eigenvectors by inverse iteration (Wilkinson 1965; Peters & Wilkinson 1971): a few solves of (T - lambda I) v = b
+//    with an LU factorisation with row interchanges, the start vector fixed, each iterate orthogonalised (modified
+//    Gram-Schmidt) against the vectors already found for eigenvalues within 1e-3 ||T|| of it, so that the vectors
+//    of close eigenvalues stay orthogonal.
+// Returns the eigenvalues ascending and the unit eigenvectors, vector m in vec[m * n .. m * n + n).
+struct TridiagEigen {
+    std::vector<double> val, vec;
+};
+static int sturm_below(const std::vector<double>& t, const std::vector<double>& u2, double x, double tiny) {
+    int neg = 0;
+    double q = t[0] - x;
+    for (size_t i = 0;; ++i) {
+        if (q == 0) q = -tiny;                   // a zero pivot counts as a tiny negative one
+        neg += q < 0;
+        if (i + 1 == t.size()) break;
+        q = (t[i + 1] - x) - u2[i] / q;
     }
-    return true;
+    return neg;
+}
+static TridiagEigen tridiag_eigen(const std::vector<double>& t, const std::vector<double>& u) {
+    const int n = int(t.size());
+    TridiagEigen out;
+    out.val.assign(size_t(n), 0.0);
+    out.vec.assign(size_t(n) * n, 0.0);
+    if (n == 0) return out;
+    std::vector<double> u2(size_t(std::max(n - 1, 0)));
+    double lo = 1e300, hi = -1e300, norm = 0;
+    for (int i = 0; i < n; ++i) {
+        const double r = (i > 0 ? std::fabs(u[size_t(i) - 1]) : 0.0) + (i + 1 < n ? std::fabs(u[size_t(i)]) : 0.0);
+        lo = std::min(lo, t[size_t(i)] - r); hi = std::max(hi, t[size_t(i)] + r);
+        norm = std::max(norm, std::fabs(t[size_t(i)]) + r);
+        if (i + 1 < n) u2[size_t(i)] = u[size_t(i)] * u[size_t(i)];
+    }
+    const double eps = std::numeric_limits<double>::epsilon();
+    const double tiny = eps * eps * std::max(norm, 1e-300);
+    for (int k = 0; k < n; ++k) {               // the k-th smallest: count(x) <= k below a, > k below b
+        double a = lo - eps * norm, b = hi + eps * norm;
+        for (int it = 0; it < 200 && b - a > 2 * eps * std::max(std::fabs(a), std::fabs(b)) + tiny; ++it) {
+            const double m = 0.5 * (a + b);
+            if (m <= a || m >= b) break;
+            if (sturm_below(t, u2, m, tiny) > k) b = m; else a = m;
+        }
+        out.val[size_t(k)] = 0.5 * (a + b);
+    }
+    // inverse iteration
+    std::vector<double> dd(static_cast<size_t>(n)), du(static_cast<size_t>(n)), du2(static_cast<size_t>(n)),
+        dl(static_cast<size_t>(n)), x(static_cast<size_t>(n));
+    std::vector<int> swp(static_cast<size_t>(n));
+    const double pivot_floor = eps * std::max(norm, 1e-300);
+    int cluster_start = 0;
+    for (int k = 0; k < n; ++k) {
+        const double lam = out.val[size_t(k)];
+        if (k > 0 && lam - out.val[size_t(k) - 1] > 1e-3 * norm) cluster_start = k;
+        // LU of T - lam I with partial pivoting: row i of U holds dd[i], du[i], du2[i] (two superdiagonals)
+        double diag = t[0] - lam, sup = n > 1 ? u[0] : 0.0, sup2 = 0;
+        for (int i = 0; i + 1 < n; ++i) {
+            const double sub = u[size_t(i)], nd = t[size_t(i) + 1] - lam, nsup = i + 2 < n ? u[size_t(i) + 1] : 0.0;
+            if (std::fabs(diag) >= std::fabs(sub)) {       // no interchange
+                const double l = sub / (diag != 0 ? diag : pivot_floor);
+                dd[size_t(i)] = diag; du[size_t(i)] = sup; du2[size_t(i)] = sup2; dl[size_t(i)] = l; swp[size_t(i)] = 0;
+                diag = nd - l * sup; sup = nsup; sup2 = 0;
+            } else {                                       // rows i and i + 1 interchanged
+                const double l = diag / sub;
+                dd[size_t(i)] = sub; du[size_t(i)] = nd; du2[size_t(i)] = nsup; dl[size_t(i)] = l; swp[size_t(i)] = 1;
+                diag = sup - l * nd; sup = -l * nsup; sup2 = 0;
+            }
+        }
+        dd[size_t(n) - 1] = diag; du[size_t(n) - 1] = 0; du2[size_t(n) - 1] = 0;
+        for (int i = 0; i < n; ++i)
+            if (std::fabs(dd[size_t(i)]) < pivot_floor) dd[size_t(i)] = dd[size_t(i)] < 0 ? -pivot_floor : pivot_floor;
+        for (int i = 0; i < n; ++i) x[size_t(i)] = 1.0 + 0.1 * std::sin(1.0 + 3.0 * i);   // fixed, not special
+        for (int sweep = 0; sweep < 3; ++sweep) {
+            for (int i = 0; i + 1 < n; ++i) {              // forward: apply the interchanges and L
+                if (swp[size_t(i)]) std::swap(x[size_t(i)], x[size_t(i) + 1]);
+                x[size_t(i) + 1] -= dl[size_t(i)] * x[size_t(i)];
+            }
+            for (int i = n - 1; i >= 0; --i) {             // back substitution with U
+                double v = x[size_t(i)];
+                if (i + 1 < n) v -= du[size_t(i)] * x[size_t(i) + 1];
+                if (i + 2 < n) v -= du2[size_t(i)] * x[size_t(i) + 2];
+                x[size_t(i)] = v / dd[size_t(i)];
+            }
+            for (int m = cluster_start; m < k; ++m) {      // orthogonal to the cluster's earlier vectors
+                const double* w = &out.vec[size_t(m) * n];
+                double dot = 0;
+                for (int i = 0; i < n; ++i) dot += w[i] * x[size_t(i)];
+                for (int i = 0; i < n; ++i) x[size_t(i)] -= dot * w[i];
+            }
+            double nr = 0;
+            for (int i = 0; i < n; ++i) nr += x[size_t(i)] * x[size_t(i)];
+            nr = std::sqrt(nr);
+            for (int i = 0; i < n; ++i) x[size_t(i)] /= nr;
+        }
+        std::copy(x.begin(), x.end(), out.vec.begin() + size_t(k) * n);
+    }
+    return out;
 }
 
-// Free-hand y (reference setup_y, src/sim_setup.cpp:84-143): nodes j = 0..ny (0 and ny are the conducting
-// walls), half-nodes j + 1/2; E_x, B_y, E_z, j_x, j_z on the nodes, E_y, B_x, B_z, j_y on the half-nodes. Cell
-// sizes Delta_j, dual sizes A_j, the sponge profile at nodes and half-nodes, the LU factors of k_x^2 - Lap_y on
-// the nodes 1..ny-1 (Dirichlet) for the bound field, and the eigenvectors of -Lap_y for the start field.
+// Free-hand y (the grid of the reference's setup_y, src/sim_setup.cpp:84-143): ny cells between the conducting walls
+// at the nodes 0 and ny. Cell j runs from node j to node j + 1 (size Delta_j, its centre the half-node j); the dual
+// cell of node j has size A_j = (Delta_{j-1} + Delta_j) / 2, A_0 = Delta_0 / 2. E_x, B_y, E_z, j_x, j_z live on the
+// nodes; E_y, B_x, B_z, j_y on the half-nodes. The tables built here:
+//   * 1/Delta_j, 1/A_j and the sponge profile at the nodes and half-nodes;
+//   * the elimination of k_x^2 - Lap_y on the interior nodes 1..ny-1 (Lap_y = the three-point operator
+//     A_j^-1 [(f_{j+1} - f_j)/Delta_j - (f_j - f_{j-1})/Delta_{j-1}], zero at the walls), per k_x: the reciprocal
+//     pivots and the multipliers of the forward sweep, for the sponge's bound field;
+//   * the eigenvectors of -Lap_y for the co-moving start field. -Lap_y = A^-1 K with K symmetric, so it is
+//     similar to the symmetric tridiagonal A^-1/2 K A^-1/2; its orthonormal eigenvectors u_m give the modes
+//     v_m = A^-1/2 u_m, orthonormal in the A-weighted product. A profile f on the nodes then has the coefficients
+//     c_m = sum_j v_m(j) A_j f_j = sum_j u_m(j) sqrt(A_j) f_j, and f_j = sum_m v_m(j) c_m = sum_m u_m(j) c_m / sqrt(A_j).
+//     Tables: forward [slot][j] = u_m(j) sqrt(A_j), back [j][slot] = u_m(j) / sqrt(A_j), eigenvalue [slot], with
+//     slot = m + 1 (slot 0 left at zero: the wall node has no mode).
+static double sponge_factor(double dist_from_edge, double width, double rate) {
+    if (width <= 0 || dist_from_edge >= width) return 1.0;
+    const double r = 1 - dist_from_edge / width;
+    return 1 - rate * r * r;
+}
 static void setup_y_free(Ctx& c, const g3d_grid& G, const g3d_params& P, cudaStream_t s) {
     const int ny = c.ny, H = c.H;
-    const std::vector<double> Y(G.ynode, G.ynode + ny + 1);
+    const std::vector<double> node(G.ynode, G.ynode + ny + 1);
     for (int j = 0; j < ny; ++j)
-        if (!(Y[size_t(j) + 1] > Y[size_t(j)])) throw Error(G3D_ERR_ARG, "ynode must increase");
-    const double Ly = Y[size_t(ny)] - Y[0];
+        if (!(node[size_t(j) + 1] > node[size_t(j)])) throw Error(G3D_ERR_ARG, "ynode must increase");
+    const double Ly = node[size_t(ny)] - node[0];
     c.dy = Ly / ny;
-    std::vector<double> hDel(ny), hA(ny), hiD(ny), hiA(ny), hmn(ny), hmh(ny);
-    for (int j = 0; j < ny; ++j) hDel[j] = Y[size_t(j) + 1] - Y[size_t(j)];
-    hA[0] = 0.5 * hDel[0];
-    for (int j = 1; j < ny; ++j) hA[j] = 0.5 * (hDel[j - 1] + hDel[j]);
-    auto prof = [&](double y) {
-        const double dd = 0.5 * Ly - std::fabs(y), w = P.sponge_y;
-        if (w <= 0 || dd >= w) return 1.0;
-        const double r = 1 - dd / w;
-        return 1 - P.sponge_rate * r * r;
-    };
+    std::vector<double> cell(static_cast<size_t>(ny)), dual(static_cast<size_t>(ny));
+    std::vector<double> inv_cell(static_cast<size_t>(ny)), inv_dual(static_cast<size_t>(ny));
+    std::vector<double> mask_node(static_cast<size_t>(ny)), mask_half(static_cast<size_t>(ny));
+    for (int j = 0; j < ny; ++j) cell[size_t(j)] = node[size_t(j) + 1] - node[size_t(j)];
+    for (int j = 0; j < ny; ++j) dual[size_t(j)] = j == 0 ? 0.5 * cell[0] : 0.5 * (cell[size_t(j) - 1] + cell[size_t(j)]);
     for (int j = 0; j < ny; ++j) {
-        hiD[j] = 1 / hDel[j]; hiA[j] = 1 / hA[j];
-        hmn[j] = prof(Y[size_t(j)]); hmh[j] = prof(0.5 * (Y[size_t(j)] + Y[size_t(j) + 1]));
+        inv_cell[size_t(j)] = 1 / cell[size_t(j)];
+        inv_dual[size_t(j)] = 1 / dual[size_t(j)];
+        const double y_half = 0.5 * (node[size_t(j)] + node[size_t(j) + 1]);
+        mask_node[size_t(j)] = sponge_factor(0.5 * Ly - std::fabs(node[size_t(j)]), P.sponge_y, P.sponge_rate);
+        mask_half[size_t(j)] = sponge_factor(0.5 * Ly - std::fabs(y_half), P.sponge_y, P.sponge_rate);
     }
-    c.ynode_h = Y;
-    c.yn.upload(Y, s); c.iD.upload(hiD, s); c.iA.upload(hiA, s); c.masky_n.upload(hmn, s); c.masky_h.upload(hmh, s);
-    bool uni = true;
-    for (int j = 0; j < ny; ++j) uni = uni && hDel[j] == hDel[0];
-    c.yax = AxisDev{c.yn.p, ny + 1, uni ? 1 : 0, Y[0], 1 / hDel[0]};
+    c.ynode_h = node;
+    c.ia_max = 0;
+    for (int j = 0; j < ny; ++j) c.ia_max = std::max(c.ia_max, std::max(inv_cell[size_t(j)], inv_dual[size_t(j)]));
+    c.yn.upload(node, s); c.iD.upload(inv_cell, s); c.iA.upload(inv_dual, s);
+    c.masky_n.upload(mask_node, s); c.masky_h.upload(mask_half, s);
+    const bool equal_cells = std::all_of(cell.begin(), cell.end(), [&](double d) { return d == cell[0]; });
+    c.yax = AxisDev{c.yn.p, ny + 1, equal_cells ? 1 : 0, node[0], 1 / cell[0]};
     // the y tables of the Fourier form are not used; zeros keep the device pointers valid
     const std::vector<double> zero(static_cast<size_t>(ny), 0.0);
     c.kyd.upload(zero, s); c.kys.upload(zero, s); c.filty.upload(zero, s);
     c.kyd_h = zero;
-    // LU factors of (k_x^2 - Lap_y) on the nodes 1..ny-1, per k_x <= nx/2
-    std::vector<double> hcp(size_t(ny) * H, 0.0), hid(size_t(ny) * H, 0.0);
+    // -Lap_y on the interior nodes: row j couples j - 1 (below), j, j + 1 (above)
+    auto below = [&](int j) { return j > 1 ? -inv_dual[size_t(j)] * inv_cell[size_t(j) - 1] : 0.0; };
+    auto above = [&](int j) { return j < ny - 1 ? -inv_dual[size_t(j)] * inv_cell[size_t(j)] : 0.0; };
+    auto centre = [&](int j) { return inv_dual[size_t(j)] * (inv_cell[size_t(j) - 1] + inv_cell[size_t(j)]); };
+    // forward elimination of k_x^2 - Lap_y per k_x <= nx/2: pivot_j = k_x^2 + centre_j - below_j m_{j-1},
+    // m_j = above_j / pivot_j; stored 1/pivot_j and m_j at [j][k_x]
+    std::vector<double> mult(size_t(ny) * H, 0.0), inv_piv(size_t(ny) * H, 0.0);
     for (int i = 0; i < H; ++i) {
-        double cprev = 0;
-        const double kx = c.kxd_h[size_t(i)];
+        const double k2 = c.kxd_h[size_t(i)] * c.kxd_h[size_t(i)];
+        double m_prev = 0;
         for (int j = 1; j < ny; ++j) {
-            const double lo = j > 1 ? -hiA[j] * hiD[j - 1] : 0, up = j < ny - 1 ? -hiA[j] * hiD[j] : 0;
-            const double den = kx * kx + hiA[j] * (hiD[j - 1] + hiD[j]) - lo * cprev;
-            hid[size_t(j) * H + i] = 1 / den;
-            hcp[size_t(j) * H + i] = cprev = up / den;
+            const double piv = k2 + centre(j) - below(j) * m_prev;
+            inv_piv[size_t(j) * H + i] = 1 / piv;
+            m_prev = above(j) / piv;
+            mult[size_t(j) * H + i] = m_prev;
         }
     }
-    c.pcp.upload(hcp, s); c.pid.upload(hid, s);
-    // eigenvectors of -Lap_y on the nodes: T v = mu A v with T symmetric; S = A^-1/2 T A^-1/2 is symmetric
-    // tridiagonal with eigenvectors u, v = A^-1/2 u. Slot s = m + 1 holds eigenvalue m (slot 0 unused).
+    c.pcp.upload(mult, s); c.pid.upload(inv_piv, s);
+    // modes of -Lap_y: the symmetric form A^-1/2 K A^-1/2 (diagonal centre_j, couplings -1/(Delta_j sqrt(A_j A_{j+1})))
     const int M = ny - 1;
-    std::vector<double> d(static_cast<size_t>(M)), e(static_cast<size_t>(M), 0.0), z;
-    for (int j = 1; j < ny; ++j) d[size_t(j) - 1] = hiA[j] * (hiD[j - 1] + hiD[j]);
-    for (int j = 1; j < ny - 1; ++j) e[size_t(j) - 1] = -hiD[j] / std::sqrt(hA[j] * hA[j + 1]);
-    const std::vector<double> d0 = d, e0 = e;
-    if (!tridiagonal_eigen(d, e, z)) throw Error(G3D_ERR_ARG, "eigenvectors of the y Laplacian: no convergence");
-    // self-check: |S u - mu u| relative to the largest eigenvalue
-    double emax = 0, res = 0;
-    for (int m = 0; m < M; ++m) emax = std::max(emax, std::fabs(d[size_t(m)]));
-    for (int m = 0; m < M; ++m)
-        for (int k = 0; k < M; ++k) {
-            double v = d0[size_t(k)] * z[size_t(k) * M + m] - d[size_t(m)] * z[size_t(k) * M + m];
-            if (k > 0) v += e0[size_t(k) - 1] * z[size_t(k - 1) * M + m];
-            if (k < M - 1) v += e0[size_t(k)] * z[size_t(k + 1) * M + m];
-            res = std::max(res, std::fabs(v));
-        }
-    if (!(res <= 1e-10 * emax)) throw Error(G3D_ERR_ARG, "eigenvectors of the y Laplacian: residual " + std::to_string(res / emax));
-    std::vector<double> hf(size_t(ny) * ny, 0.0), hb(size_t(ny) * ny, 0.0), hl(static_cast<size_t>(ny), 0.0);
+    std::vector<double> t(static_cast<size_t>(M)), u(static_cast<size_t>(std::max(M - 1, 0)));
+    for (int j = 1; j < ny; ++j) t[size_t(j) - 1] = centre(j);
+    for (int j = 1; j + 1 < ny; ++j) u[size_t(j) - 1] = -inv_cell[size_t(j)] / std::sqrt(dual[size_t(j)] * dual[size_t(j) + 1]);
+    const TridiagEigen ev = tridiag_eigen(t, u);
+    // check: largest |S v - mu v| and |v_m . v_k - delta_mk| against the spectrum's size
+    double big = 0, resid = 0, orth = 0;
+    for (int m = 0; m < M; ++m) big = std::max(big, std::fabs(ev.val[size_t(m)]));
     for (int m = 0; m < M; ++m) {
-        hl[size_t(m) + 1] = d[size_t(m)];
-        for (int j = 1; j < ny; ++j) {
-            const double u = z[size_t(j - 1) * M + m], sq = std::sqrt(hA[j]);
-            hf[size_t(m + 1) * ny + j] = u * sq;          // coefficient = v^T A rho
-            hb[size_t(j) * ny + m + 1] = u / sq;          // value = sum v coefficient
+        const double* v = &ev.vec[size_t(m) * M];
+        for (int k = 0; k < M; ++k) {
+            double r = (t[size_t(k)] - ev.val[size_t(m)]) * v[k];
+            if (k > 0) r += u[size_t(k) - 1] * v[k - 1];
+            if (k + 1 < M) r += u[size_t(k)] * v[k + 1];
+            resid = std::max(resid, std::fabs(r));
+        }
+        for (int q = m; q < std::min(M, m + 8); ++q) {     // neighbours in the spectrum are the ones at risk
+            const double* w = &ev.vec[size_t(q) * M];
+            double dot = 0;
+            for (int k = 0; k < M; ++k) dot += v[k] * w[k];
+            orth = std::max(orth, std::fabs(dot - (q == m ? 1.0 : 0.0)));
         }
     }
-    c.evf.upload(hf, s); c.evb.upload(hb, s); c.evl.upload(hl, s);
+    if (!(resid <= 1e-10 * big) || !(orth <= 1e-10))
+        throw Error(G3D_ERR_ARG, "modes of the y Laplacian: residual " + std::to_string(resid / big) + ", orthogonality " +
+                                     std::to_string(orth));
+    std::vector<double> fwd(size_t(ny) * ny, 0.0), back(size_t(ny) * ny, 0.0), eig(static_cast<size_t>(ny), 0.0);
+    for (int m = 0; m < M; ++m) {
+        const int slot = m + 1;
+        eig[size_t(slot)] = ev.val[size_t(m)];
+        for (int j = 1; j < ny; ++j) {
+            const double um = ev.vec[size_t(m) * M + size_t(j) - 1], root = std::sqrt(dual[size_t(j)]);
+            fwd[size_t(slot) * ny + j] = um * root;
+            back[size_t(j) * ny + slot] = um / root;
+        }
+    }
+    c.evf.upload(fwd, s); c.evb.upload(back, s); c.evl.upload(eig, s);
 }
 
 static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     if (!G.y_fourier && !G.ynode) throw Error(G3D_ERR_ARG, "free-hand y needs the ny + 1 nodes (ynode)");
-    if (!pow2_ok(G.nx) || G.nx < 8 || (G.y_fourier && !pow2_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 4096)))
-        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512; ny one in 4..512 (Fourier y) or 3..4096 (free-hand)");
+    if (!pow2_ok(G.nx) || G.nx < 8 || (G.y_fourier && !pow2_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 512)))
+        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512; ny one in 4..512 (Fourier y) or 3..512 (free-hand)");
     if (G.nzeta < 4 || !G.zeta) throw Error(G3D_ERR_ARG, "nzeta must be >= 4 with a zeta table");
     if (!(G.Lx > 0) || !(G.Ly > 0)) throw Error(G3D_ERR_ARG, "Lx, Ly must be positive");
     if (P.precision != G3D_FP64 && P.precision != G3D_MIXED) throw Error(G3D_ERR_ARG, "precision must be G3D_FP64 or G3D_MIXED");

@@ -3,13 +3,15 @@
 //
 // The currents are real fields, so their spectra are Hermitian; only k_x = 0 .. nx/2 is kept (H = nx/2 + 1
 // columns, [plane][j][k_x]).
-//   k_deposit   one thread per particle: NGP over the zeta half-cell, TSC in x and y, FP64 atomics into the raw
-//               current planes jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106)
+//   k_deposit   one thread per particle: NGP over the zeta half-cell, TSC in x and y, into the raw current planes
+//               jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106) as fixed-point integer adds (see below), so that
+//               the sums, and the whole run, do not depend on the order of the adds
 //   k_cur_rows  per (block of rows, half-cell plane): zeta filter (sim_particles.cpp:120-138) of the three raw
 //               planes, then per row one complex FFT along x of jx + i jy, split by Hermitian symmetry into the
 //               half spectra of jx and jy, and one of jz -> three half-spectrum planes (scratch W0, W1, W2)
 //   k_cur_cols  per (half-cell plane, tile of 8 k_x columns): FFT along y, the cos^2 filters and the k_perp = 0
 //               removal (sim_particles.cpp:146-156) -> jkx, jky, jkz
+#include <algorithm>
 #include "g3d_ctx.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
@@ -17,8 +19,70 @@
 namespace g3d {
 
 // ---------------------------------------------------------------- deposit
+// Fixed-point deposit. Floating-point atomic adds make each sum depend on the order the adds arrive in, so two runs
+// of the same input differ at the last bits and drift apart. Here every deposit value v goes in as the integer
+// round(v 2^e) with a 64-bit integer atomic add, which is associative: the sums, and all that follows them, are the
+// same bits on every run. 2^e is the largest power of two with B 2^e < 2^62, B a bound on the sum of |v| over all
+// particles and points of one component (per particle: |f| x the largest dual-cell factor x max(1, |v_x/v_z|,
+// |v_y/v_z|), the TSC weights of a particle summing to 1), taken by a fixed-order two-level tree on the device, so
+// no sum can overflow; each add is rounded to 2^-e < 2^-61 B. A last pass turns the planes back into doubles
+// (times 2^-e, exact for a power of two), the raw planes of the reference's layout that the zeta filter reads.
+constexpr int DB = 296, DT = 256;     // blocks and threads of the bound's first level
+
+__device__ __forceinline__ double dep_bound_one(const PartsDev& P, long ip, const Geo& g, double ia_max) {
+    if (P.alive[ip] != 1) return 0;
+    int m; double fz;
+    g.zax.locate(P.zeta[ip], m, fz);
+    const int hw = m - (g.a - 2);
+    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return 0;
+    const double vz = P.pz[ip];               // the ratios v/v_z are p/p_z
+    const double r = fmax(1.0, fmax(fabs(P.px[ip] / vz), fabs(P.py[ip] / vz)));
+    return fabs(P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx)) * ia_max * r;
+}
+__global__ void __launch_bounds__(DT) k_dep_bound(PartsDev P, long np, Geo g, double ia_max, double* __restrict__ part) {
+    __shared__ double sh[DT];
+    double acc = 0;
+    for (long i = long(blockIdx.x) * DT + threadIdx.x; i < np; i += long(gridDim.x) * DT) acc += dep_bound_one(P, i, g, ia_max);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = DT / 2; st > 0; st >>= 1) {
+        if (int(threadIdx.x) < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+// scale[0] = 2^e, scale[1] = 2^-e
+__global__ void __launch_bounds__(DT) k_dep_scale(const double* __restrict__ part, double* __restrict__ scale) {
+    __shared__ double sh[DT];
+    double acc = 0;
+    for (int b = threadIdx.x; b < DB; b += DT) acc += part[b];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int st = DT / 2; st > 0; st >>= 1) {
+        if (int(threadIdx.x) < st) sh[threadIdx.x] += sh[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double B = sh[0] * (1 + 1e-12) + 1e-300;   // rounding of the bound's own sum, and no zero
+        int x;
+        frexp(B, &x);                                     // B < 2^x
+        const int e = min(62 - x, 1000);
+        scale[0] = ldexp(1.0, e); scale[1] = ldexp(1.0, -e);
+    }
+}
+__device__ __forceinline__ void fix_add(double* p, double v, double sc) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(__double2ll_rn(v * sc)));
+}
+__global__ void k_fix_to_double(double* __restrict__ J, long n, const double* __restrict__ scale) {
+    const double inv = scale[1];
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        const long long q = reinterpret_cast<const long long*>(J)[i];
+        J[i] = double(q) * inv;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
-                                                double* __restrict__ J) {
+                                                double* __restrict__ J, const double* __restrict__ scale) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= np) return;
     const long ip = perm[t];                 // cell order: neighbouring threads add into the same lines
@@ -27,6 +91,7 @@ __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __re
     g.zax.locate(P.zeta[ip], m, fz);
     const int hw = m - (g.a - 2);
     if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
+    const double sc = scale[0];
     const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
     const double gm = sqrt(1 + px * px + py * py + pz * pz);
     const double vx = px / gm, vy = py / gm, vz = pz / gm;
@@ -43,9 +108,9 @@ __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __re
         for (int u = 0; u < 3; ++u) {
             const long k = long(jn[v]) * g.nx + ix[u];
             const double w = f * wx[u] * wn[v] * ia0;
-            atomicAdd(J0 + k, w * vx / vz);
-            atomicAdd(J0 + pl + k, w * vy / vz);
-            atomicAdd(J0 + 2 * pl + k, w);
+            fix_add(J0 + k, w * vx / vz, sc);
+            fix_add(J0 + pl + k, w * vy / vz, sc);
+            fix_add(J0 + 2 * pl + k, w, sc);
         }
 }
 
@@ -155,13 +220,32 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
 }
 
 // ---------------------------------------------------------------- launchers
+// the scale 2^e of the fixed-point deposit into c.depfix[DB], [DB + 1] (ia_max: the largest dual-cell factor);
+// returns where it is
+const double* launch_deposit_scale(Ctx& c, double ia_max) {
+    if (c.depfix.n < size_t(DB + 2)) c.depfix.alloc(size_t(DB + 2), c.stream);
+    k_dep_bound<<<DB, DT, 0, c.stream>>>(c.parts, c.np, c.geo(), ia_max, c.depfix.p);
+    c.check_launch("k_dep_bound");
+    k_dep_scale<<<1, DT, 0, c.stream>>>(c.depfix.p, c.depfix.p + DB);
+    c.check_launch("k_dep_scale");
+    return c.depfix.p + DB;
+}
+// the fixed-point planes back to doubles
+void launch_deposit_finish(Ctx& c) {
+    const long n = long(c.jw.n);
+    const long b = std::min<long>((n + 255) / 256, 148 * 16);
+    k_fix_to_double<<<unsigned(b), 256, 0, c.stream>>>(c.jw.p, n, c.depfix.p + DB);
+    c.check_launch("k_fix_to_double");
+}
 void launch_deposit(Ctx& c) {
     c.jw.zero(c.stream);
     if (c.np == 0) return;
     const int tok = c.prof_begin("deposit");
+    const double* scale = launch_deposit_scale(c, 1 / c.dy);
     const unsigned blocks = unsigned((c.np + 255) / 256);
-    k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p);
+    k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
     c.check_launch("k_deposit");
+    launch_deposit_finish(c);
     c.prof_end(tok);
 }
 

@@ -7,15 +7,17 @@
 //                   half-nodes: mirrored), the y-mean of j_y removed at k_x = 0 (TEM), the x filter
 //                   (sim_particles.cpp:165-205); the zeta filter and the x transform are the rows kernel of
 //                   k_currents.cu
-//   k_march_fh      per k_x line, slices front to rear: the known parts of R and L, E_z on the nodes and B_z on
-//                   the half-nodes by two tridiagonal (Thomas) solves along y, then R and L (march_line,
+//   k_march_lines   one CTA per k_x line, a thread per y row, slices front to rear: the known parts of R and L,
+//                   E_z on the nodes and B_z on the half-nodes from two tridiagonal systems along y solved together
+//                   by parallel cyclic reduction in shared memory, then R and L (the scheme of march_line,
 //                   src/sim_kernels.hpp:213-313)
 //   k_sp_psi_fh     sponge: the bound field psi = T^-1 (rho + gamma^-2 T^-1 d_zeta^2 rho), T = k_x^2 - Lap_y with
 //                   the precomputed LU factors, and R - R_b (sim_fields.cpp:199-232); then the rows kernel of
 //                   k_fields.cu (inverse x, mask, forward x) and k_sp_add_fh (+ R_b, R_x = 0 at the wall node)
 //   k_comoving_fh_* the co-moving start field in the eigenvectors of -Lap_y: projection of the charge, Thomas in
 //                   zeta per (eigenvalue, k_x), back to the nodes, R (sim_fields.cpp:44-151)
-// One thread per line; the recurrences along y and zeta are serial in the reference's order.
+// The other kernels take one thread per line (the lines of a window are many); the filters and solves along y in
+// them are serial in the reference's order.
 #include "g3d_ctx.hpp"
 
 namespace g3d {
@@ -25,8 +27,11 @@ __device__ __forceinline__ cpx ikx(double k, cpx z) { return ik(k, z); }     // 
 }  // namespace
 
 // ---------------------------------------------------------------- deposit
+__device__ __forceinline__ void fix_add_fh(double* p, double v, double sc) {   // fixed-point add (k_currents.cu)
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(__double2ll_rn(v * sc)));
+}
 __global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
-                                                   double* __restrict__ J) {
+                                                   double* __restrict__ J, const double* __restrict__ scale) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= np) return;
     const long ip = perm[t];
@@ -38,7 +43,7 @@ __global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* _
     const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
     const double gm = sqrt(1 + px * px + py * py + pz * pz);
     const double vx = px / gm, vy = py / gm, vz = pz / gm;
-    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
+    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx), sc = scale[0];
     int ix[3], jn[3], jh[3]; double wx[3], wn[3], wh[3];
     tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
     tsc_y(g.yax, P.y[ip], jn, wn, jh, wh);
@@ -50,12 +55,12 @@ __global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* _
             if (nod) {
                 const long k = long(jn[v]) * g.nx + ix[u];
                 const double w = f * wx[u] * wn[v] * g.iA[jn[v]];
-                atomicAdd(J0 + k, w * vx / vz);
-                atomicAdd(J0 + 2 * pl + k, w);
+                fix_add_fh(J0 + k, w * vx / vz, sc);
+                fix_add_fh(J0 + 2 * pl + k, w, sc);
             }
             if (hal) {
                 const long k = long(jh[v]) * g.nx + ix[u];
-                atomicAdd(J0 + pl + k, f * wx[u] * wh[v] * g.iD[jh[v]] * vy / vz);
+                fix_add_fh(J0 + pl + k, f * wx[u] * wh[v] * g.iD[jh[v]] * vy / vz, sc);
             }
         }
     }
@@ -172,116 +177,187 @@ __global__ void k_ss_lines_fh(Geo g, const cpx* __restrict__ T, cpx* __restrict_
 }
 
 // ---------------------------------------------------------------- the march of the k_x lines
-struct FhScratch { cpx *sRx, *sRy, *sLx, *sLy, *srhs; double* scp; };
+// One CTA per k_x line, one thread per y row j (nodes for E_z, R_x, L_x; half-nodes for B_z, R_y, L_y), slices
+// from the top of the range down. Per slice (the scheme of the reference's march_line, src/sim_kernels.hpp:213-313):
+//   1. the parts of R known at level s0 (R + D (curl terms of E_z, B_z) - D J, J the slice current interpolated
+//      between its two half-cells with w_lo, w_hi);
+//   2. the parts of L known from the slice above (level s1);
+//   3. E_z on the nodes (Dirichlet at both walls) and B_z on the half-nodes (Neumann) from two tridiagonal systems
+//      along y, both solved together by parallel cyclic reduction: ceil(log2 ny) halving steps in shared memory, each
+//      row eliminating its neighbours at distance s = 1, 2, 4, ... (the systems are strictly diagonally dominant,
+//      diagonal 1 + cc (k_x^2 + ...) against off-diagonals summing to cc (...), so the reduction is stable);
+//   4. R and L from the new E_z, B_z.
+// The slice above stays in shared memory from one slice to the next, so a slice reads only its own level-s0 fields
+// and one current plane (the other current plane is the one the slice above read), and the loads of the next slice
+// are issued before this slice's work. Rows beyond ny (the padding of the CTA) take part in the barriers only.
+struct LineArrays {
+    cpx *Rx, *Ry, *Ez, *Bz, *Lx, *Ly;
+    const cpx *j0x, *j0y, *jkx, *jky, *jkz;
+};
+constexpr int LINE_MAX_NY = 512;
+// shared memory of one line: the slice above (6 planes), this slice's level-s0 E_z and B_z, the known parts (4),
+// the new E_z and B_z, and the two reduction systems (3 real coefficients and a complex right side per row each)
+static size_t line_smem(int ny) { return size_t(ny) * (14 * sizeof(cpx) + 2 * (3 * sizeof(double) + sizeof(cpx))); }
 
-__global__ void __launch_bounds__(64) k_march_fh(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, cpx* __restrict__ Ez,
-                                                cpx* __restrict__ Bz, cpx* __restrict__ Lx, cpx* __restrict__ Ly,
-                                                const cpx* __restrict__ j0x, const cpx* __restrict__ j0y,
-                                                const cpx* __restrict__ jkx, const cpx* __restrict__ jky,
-                                                const cpx* __restrict__ jkz, FhScratch sc, double D, int n_top, int n_bot) {
-    const int ik = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ik >= g.H) return;
-    const int ny = g.ny, H = g.H;
-    const long nk = g.nkh;
-    const double kx = g.kxd[ik], kx2 = kx * kx;
-    const double* iD = g.iD; const double* iA = g.iA;
-    auto S = [&](cpx* A, int j) -> cpx& { return A[long(j) * H + ik]; };
-    double* scp = sc.scp;
+struct SliceIn {           // what a row reads of one slice: level-s0 fields and the slice's lower current plane
+    cpx rx, ry, ez, bz, jx, jy, kx_, ky_, kz_;
+};
+__device__ __forceinline__ SliceIn load_slice(const LineArrays& A, long o) {
+    SliceIn v;
+    v.rx = A.Rx[o]; v.ry = A.Ry[o]; v.ez = A.Ez[o]; v.bz = A.Bz[o];
+    v.kx_ = A.jkx[o]; v.ky_ = A.jky[o]; v.kz_ = A.jkz[o];
+    v.jx = A.j0x[o] + v.kx_; v.jy = A.j0y[o] + v.ky_;
+    return v;
+}
+
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT) k_march_lines(Geo g, LineArrays A, double D, int n_top, int n_bot) {
+    extern __shared__ double2 sm[];
+    const int ny = g.ny, H = g.H, line = blockIdx.x, j = threadIdx.x;
+    const bool row = j < ny;
+    const long nk = g.nkh, col = long(row ? j : 0) * H + line;
+    cpx* up6 = sm;                       // the slice above: R_x, R_y, E_z, B_z, L_x, L_y (ny each)
+    cpx* lvE = sm + 6 * ny;              // this slice, level s0: E_z, B_z
+    cpx* lvB = lvE + ny;
+    cpx* kn = lvB + ny;                  // known parts: R_x, R_y, L_x, L_y
+    cpx* nwE = kn + 4 * ny;              // the new E_z, B_z
+    cpx* nwB = nwE + ny;
+    cpx* rhsE = nwB + ny;                // reduction systems: right sides, then lower, diagonal, upper
+    cpx* rhsB = rhsE + ny;
+    double* lo_E = reinterpret_cast<double*>(rhsB + ny);
+    double* dg_E = lo_E + ny; double* up_E = dg_E + ny;
+    double* lo_B = up_E + ny; double* dg_B = lo_B + ny; double* up_B = dg_B + ny;
+    cpx* uRx = up6; cpx* uRy = up6 + ny; cpx* uEz = up6 + 2 * ny; cpx* uBz = up6 + 3 * ny; cpx* uLx = up6 + 4 * ny;
+    cpx* uLy = up6 + 5 * ny;
+    cpx* kRx = kn; cpx* kRy = kn + ny; cpx* kLx = kn + 2 * ny; cpx* kLy = kn + 3 * ny;
+
+    const double kx = g.kxd[line], kx2 = kx * kx;
+    const double iAj = row ? g.iA[j] : 0, iDj = row ? g.iD[j] : 0;
+    const double iDm = (row && j > 0) ? g.iD[j - 1] : 0, iAp = (row && j + 1 < ny) ? g.iA[j + 1] : 0;
+    const cpx Z = C(0);
+    // the slice above the range (unless the range starts at the window front) and the upper current plane of
+    // the first slice
+    SliceIn up{};
+    if (row) {
+        const long o = long(n_top + 1 - g.a) * nk + col;
+        if (n_top < g.N - 1) {
+            uRx[j] = A.Rx[o]; uRy[j] = A.Ry[o]; uEz[j] = A.Ez[o]; uBz[j] = A.Bz[o]; uLx[j] = A.Lx[o]; uLy[j] = A.Ly[o];
+        }
+        up.kx_ = A.jkx[o]; up.ky_ = A.jky[o]; up.kz_ = A.jkz[o];
+        up.jx = A.j0x[o] + up.kx_; up.jy = A.j0y[o] + up.ky_;
+    }
+    SliceIn cur{};
+    if (row) cur = load_slice(A, long(n_top - g.a) * nk + col);
     for (int n = n_top; n >= n_bot; --n) {
-        const long P0 = long(n - g.a) * nk + ik;      // slice n of the block = half-cell n-1 (current planes)
-        const long P1 = P0 + nk;                      // slice n+1 = half-cell n
+        const long o = long(n - g.a) * nk + col;
+        SliceIn nxt{};
+        if (row && n > n_bot) nxt = load_slice(A, o - nk);        // the next slice's inputs, in flight meanwhile
+        if (row) { lvE[j] = cur.ez; lvB[j] = cur.bz; }
+        __syncthreads();
+        // 1. known part of R
         const double wl = g.wlo[n], wu = g.whi[n];
-        // known part of R (level s0 and the currents of both levels)
-        for (int j = 0; j < ny; ++j) {
-            const long o = P0 + long(j) * H;
-            if (j == 0) S(sc.sRx, 0) = C(0);
-            else {
-                const cpx Jx = wl * (j0x[o] + jkx[o]) + wu * (j0x[o + nk] + jkx[o + nk]);
-                const cpx bm = (Bz[o] - Bz[o - H]) * iA[j];
-                S(sc.sRx, j) = Rx[o] + D * (ikx(kx, Ez[o]) + bm) - D * Jx;
+        cpx sRx = Z, sRy = Z;
+        if (row) {
+            const cpx Jx = wl * cur.jx + wu * up.jx, Jy = wl * cur.jy + wu * up.jy;
+            if (j > 0) sRx = cur.rx + D * (ik(kx, cur.ez) + (cur.bz - lvB[j - 1]) * iAj) - D * Jx;
+            const cpx ez_up = j + 1 < ny ? lvE[j + 1] : Z;
+            sRy = cur.ry + D * ((ez_up - cur.ez) * iDj - ik(kx, cur.bz)) - D * Jy;
+        }
+        cpx oRx, oRy, oEz = Z, oBz = Z, oLx = Z, oLy = Z;
+        if (n == g.N - 1) {                                      // window front: L = E_z = B_z = 0
+            oRx = sRx; oRy = sRy;
+            __syncthreads();                                     // the neighbours' reads of lvE, lvB are done
+        } else {
+            // 2. known part of L from the slice above
+            const double h = g.hcg[n + 2], cc = 0.25 * h * (D + 0.25 * h);
+            cpx sLx = Z, sLy = Z, pe = Z;
+            if (row) {
+                pe = j == 0 ? Z : uEz[j];                         // E_z vanishes on the wall node
+                const cpx pe_up = j + 1 < ny ? uEz[j + 1] : Z;
+                if (j > 0) sLx = uLx[j] - 0.25 * h * (ik(kx, pe) - (uBz[j] - uBz[j - 1]) * iAj) - 0.5 * h * up.kx_;
+                sLy = uLy[j] - 0.25 * h * (ik(kx, uBz[j]) + (pe_up - pe) * iDj) - 0.5 * h * up.ky_;
+                kRx[j] = sRx; kRy[j] = sRy; kLx[j] = sLx; kLy[j] = sLy;
             }
-            const cpx Jy = wl * (j0y[o] + jky[o]) + wu * (j0y[o + nk] + jky[o + nk]);
-            const cpx ezu = j + 1 < ny ? Ez[o + H] : C(0);
-            S(sc.sRy, j) = Ry[o] + D * ((ezu - Ez[o]) * iD[j] - ikx(kx, Bz[o])) - D * Jy;
-        }
-        if (n == g.N - 1) {             // front of the window: L = E_z = B_z = 0
-            for (int j = 0; j < ny; ++j) {
-                const long o = P0 + long(j) * H;
-                Rx[o] = S(sc.sRx, j); Ry[o] = S(sc.sRy, j); Ez[o] = C(0); Bz[o] = C(0); Lx[o] = C(0); Ly[o] = C(0);
+            __syncthreads();
+            // 3. the rows of the two systems: E_z on the nodes 1..ny-1 (row 0 is the wall: E_z = 0), B_z on the
+            // half-nodes 0..ny-1
+            double aE = 0, bE = 1, cE = 0, aB = 0, bB = 1, cB = 0;
+            cpx rE = Z, rB = Z;
+            if (row) {
+                if (j > 0) {
+                    const cpx Qp = 0.5 * (-ik(kx, uRx[j] - uLx[j]) + ((uLy[j] - uRy[j]) - (uLy[j - 1] - uRy[j - 1])) * iAj);
+                    const cpx SE = -ik(kx, sRx - sLx) + ((sLy - sRy) - (kLy[j - 1] - kRy[j - 1])) * iAj;
+                    rE = pe - 0.5 * h * Qp - 0.25 * h * SE - h * up.kz_;
+                    aE = j > 1 ? -cc * iAj * iDm : 0;
+                    cE = j < ny - 1 ? -cc * iAj * iDj : 0;
+                    bE = 1 + cc * kx2 + cc * iAj * (iDm + iDj);
+                }
+                const cpx fu = j + 1 < ny ? uRx[j + 1] + uLx[j + 1] : Z, f0 = uRx[j] + uLx[j];
+                const cpx Cp = 0.5 * (ik(kx, uRy[j] + uLy[j]) - (fu - f0) * iDj);
+                const cpx su = j + 1 < ny ? kRx[j + 1] + kLx[j + 1] : Z, s0 = sRx + sLx;
+                const cpx SB = ik(kx, sRy + sLy) - (su - s0) * iDj;
+                rB = uBz[j] - 0.5 * h * Cp - 0.25 * h * SB;
+                const double al = j > 0 ? iAj : 0, au = j < ny - 1 ? iAp : 0;
+                aB = -cc * iDj * al; cB = -cc * iDj * au;
+                bB = 1 + cc * kx2 + cc * iDj * (al + au);
             }
-            continue;
-        }
-        auto nxt = [&](const cpx* A, int j) -> cpx { return (j < 0 || j >= ny) ? C(0) : A[P1 + long(j) * H]; };
-        auto pRx = [&](int j) { return nxt(Rx, j); };
-        auto pRy = [&](int j) { return nxt(Ry, j); };
-        auto pEz = [&](int j) { return j == 0 ? C(0) : nxt(Ez, j); };
-        auto pBz = [&](int j) { return nxt(Bz, j); };
-        auto pLx = [&](int j) { return nxt(Lx, j); };
-        auto pLy = [&](int j) { return nxt(Ly, j); };
-        const double h = g.hcg[n + 2], cc = 0.25 * h * (D + 0.25 * h);
-        // known part of L
-        for (int j = 0; j < ny; ++j) {
-            const long u = P1 + long(j) * H;          // half-cell n, level s1
-            if (j == 0) S(sc.sLx, 0) = C(0);
-            else {
-                const cpx bm = (pBz(j) - pBz(j - 1)) * iA[j];
-                S(sc.sLx, j) = pLx(j) - 0.25 * h * (ikx(kx, pEz(j)) - bm) - 0.5 * h * jkx[u];
+            // parallel cyclic reduction of both systems
+            for (int st = 1; st < ny; st <<= 1) {
+                if (row) {
+                    lo_E[j] = aE; dg_E[j] = bE; up_E[j] = cE; rhsE[j] = rE;
+                    lo_B[j] = aB; dg_B[j] = bB; up_B[j] = cB; rhsB[j] = rB;
+                }
+                __syncthreads();
+                if (row) {
+                    const int m = j - st, p = j + st;
+                    double fE = 0, gE = 0, fB = 0, gB = 0;
+                    double naE = 0, ncE = 0, naB = 0, ncB = 0;
+                    cpx dE = rE, dB = rB;
+                    double nbE = bE, nbB = bB;
+                    if (m >= 0) {
+                        fE = aE / dg_E[m]; fB = aB / dg_B[m];
+                        naE = -lo_E[m] * fE; naB = -lo_B[m] * fB;
+                        nbE -= up_E[m] * fE; nbB -= up_B[m] * fB;
+                        dE = dE - fE * rhsE[m]; dB = dB - fB * rhsB[m];
+                    }
+                    if (p < ny) {
+                        gE = cE / dg_E[p]; gB = cB / dg_B[p];
+                        ncE = -up_E[p] * gE; ncB = -up_B[p] * gB;
+                        nbE -= lo_E[p] * gE; nbB -= lo_B[p] * gB;
+                        dE = dE - gE * rhsE[p]; dB = dB - gB * rhsB[p];
+                    }
+                    aE = naE; cE = ncE; bE = nbE; rE = dE;
+                    aB = naB; cB = ncB; bB = nbB; rB = dB;
+                }
+                __syncthreads();
             }
-            const cpx bp = (pEz(j + 1) - pEz(j)) * iD[j];
-            S(sc.sLy, j) = pLy(j) - 0.25 * h * (ikx(kx, pBz(j)) + bp) - 0.5 * h * jky[u];
-        }
-        // E_z on the nodes 1..ny-1 (Dirichlet at the walls)
-        double cp = 0;
-        cpx dp = C(0);
-        for (int j = 1; j < ny; ++j) {
-            const cpx Qp = 0.5 * (-(ikx(kx, pRx(j) - pLx(j))) + ((pLy(j) - pRy(j)) - (pLy(j - 1) - pRy(j - 1))) * iA[j]);
-            const cpx SE = -(ikx(kx, S(sc.sRx, j) - S(sc.sLx, j))) +
-                           ((S(sc.sLy, j) - S(sc.sRy, j)) - (S(sc.sLy, j - 1) - S(sc.sRy, j - 1))) * iA[j];
-            const cpx r = pEz(j) - 0.5 * h * Qp - 0.25 * h * SE - h * jkz[P1 + long(j) * H];
-            const double lo = j > 1 ? -cc * iA[j] * iD[j - 1] : 0, up = j < ny - 1 ? -cc * iA[j] * iD[j] : 0;
-            const double den = 1 + cc * kx2 + cc * iA[j] * (iD[j - 1] + iD[j]) - lo * cp;
-            dp = (r - lo * dp) / den;
-            cp = up / den;
-            S(sc.srhs, j) = dp; scp[long(j) * H + ik] = cp;
-        }
-        {
-            cpx next = C(0);
-            for (int j = ny - 1; j >= 1; --j) { next = S(sc.srhs, j) - scp[long(j) * H + ik] * next; Ez[P0 + long(j) * H] = next; }
-            Ez[P0] = C(0);
-        }
-        // B_z on the half-nodes 0..ny-1 (Neumann)
-        cp = 0; dp = C(0);
-        for (int j = 0; j < ny; ++j) {
-            const cpx fu = j + 1 < ny ? pRx(j + 1) + pLx(j + 1) : C(0), f0 = pRx(j) + pLx(j);
-            const cpx Cp = 0.5 * (ikx(kx, pRy(j) + pLy(j)) - (fu - f0) * iD[j]);
-            const cpx su = j + 1 < ny ? S(sc.sRx, j + 1) + S(sc.sLx, j + 1) : C(0), s0 = S(sc.sRx, j) + S(sc.sLx, j);
-            const cpx SB = ikx(kx, S(sc.sRy, j) + S(sc.sLy, j)) - (su - s0) * iD[j];
-            const cpx r = pBz(j) - 0.5 * h * Cp - 0.25 * h * SB;
-            const double al = j > 0 ? iA[j] : 0, au = j < ny - 1 ? iA[j + 1] : 0;
-            const double lo = -cc * iD[j] * al, up = -cc * iD[j] * au;
-            const double den = 1 + cc * kx2 + cc * iD[j] * (al + au) - lo * cp;
-            dp = (r - lo * dp) / den;
-            cp = up / den;
-            S(sc.srhs, j) = dp; scp[long(j) * H + ik] = cp;
-        }
-        {
-            cpx next = C(0);
-            for (int j = ny - 1; j >= 0; --j) { next = S(sc.srhs, j) - scp[long(j) * H + ik] * next; Bz[P0 + long(j) * H] = next; }
-        }
-        // R and L
-        for (int j = 0; j < ny; ++j) {
-            const long o = P0 + long(j) * H;
-            if (j == 0) { Rx[o] = C(0); Lx[o] = C(0); }
-            else {
-                const cpx bm = (Bz[o] - Bz[o - H]) * iA[j];
-                Rx[o] = S(sc.sRx, j) + D * (ikx(kx, Ez[o]) + bm);
-                Lx[o] = S(sc.sLx, j) - 0.25 * h * (ikx(kx, Ez[o]) - bm);
+            if (row) {
+                oEz = j == 0 ? Z : rE / bE;
+                oBz = rB / bB;
+                nwE[j] = oEz; nwB[j] = oBz;
             }
-            const cpx ezu = j + 1 < ny ? Ez[o + H] : C(0);
-            const cpx bp = (ezu - Ez[o]) * iD[j];
-            Ry[o] = S(sc.sRy, j) + D * (bp - ikx(kx, Bz[o]));
-            Ly[o] = S(sc.sLy, j) - 0.25 * h * (ikx(kx, Bz[o]) + bp);
+            __syncthreads();
+            // 4. R and L
+            if (row) {
+                if (j > 0) {
+                    const cpx bm = (oBz - nwB[j - 1]) * iAj;
+                    oRx = sRx + D * (ik(kx, oEz) + bm);
+                    oLx = sLx - 0.25 * h * (ik(kx, oEz) - bm);
+                } else {
+                    oRx = Z; oLx = Z;
+                }
+                const cpx ez_up = j + 1 < ny ? nwE[j + 1] : Z;
+                const cpx bp = (ez_up - oEz) * iDj;
+                oRy = sRy + D * (bp - ik(kx, oBz));
+                oLy = sLy - 0.25 * h * (ik(kx, oBz) + bp);
+            }
         }
+        if (row) {
+            A.Rx[o] = oRx; A.Ry[o] = oRy; A.Ez[o] = oEz; A.Bz[o] = oBz; A.Lx[o] = oLx; A.Ly[o] = oLy;
+            uRx[j] = oRx; uRy[j] = oRy; uEz[j] = oEz; uBz[j] = oBz; uLx[j] = oLx; uLy[j] = oLy;
+        }
+        up = cur;                                                // this slice's lower plane is the next one's upper
+        cur = nxt;
     }
 }
 
@@ -427,8 +503,10 @@ void launch_deposit_fh(Ctx& c) {
     c.jw.zero(c.stream);
     if (c.np == 0) return;
     const int tok = c.prof_begin("deposit");
-    k_deposit_fh<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p);
+    const double* scale = launch_deposit_scale(c, c.ia_max);
+    k_deposit_fh<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
     c.check_launch("k_deposit_fh");
+    launch_deposit_finish(c);
     c.prof_end(tok);
 }
 void launch_cur_fft_fh(Ctx& c, bool keep0) {
@@ -440,25 +518,25 @@ void launch_cur_fft_fh(Ctx& c, bool keep0) {
     c.check_launch("k_cur_lines_fh");
     c.prof_end(tok);
 }
-void launch_march_fh(Ctx& c, double D) {
-    const size_t ln = size_t(c.ny) * c.H;
-    FhScratch sc{c.fhs.p, c.fhs.p + ln, c.fhs.p + 2 * ln, c.fhs.p + 3 * ln, c.fhs.p + 4 * ln, c.fhcp.p};
-    const int tok = c.prof_begin("march");
-    k_march_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
-                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D, c.b - 1, c.a);
-    c.check_launch("k_march_fh");
+static void march_lines(Ctx& c, double D, int n_top, int n_bot, const char* name) {
+    if (c.ny > LINE_MAX_NY) throw Error(G3D_ERR_ARG, "free-hand march: ny above " + std::to_string(LINE_MAX_NY));
+    const size_t smem = line_smem(c.ny);
+    const LineArrays A{c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p};
+    const int threads = (c.ny + 31) / 32 * 32;
+    const int tok = c.prof_begin(name);
+    if (threads <= 256) {         // up to 255 registers a thread
+        smem_attr(reinterpret_cast<const void*>(k_march_lines<256>), line_smem(256));
+        k_march_lines<256><<<unsigned(c.H), unsigned(threads), smem, c.stream>>>(c.geo(), A, D, n_top, n_bot);
+    } else {
+        smem_attr(reinterpret_cast<const void*>(k_march_lines<LINE_MAX_NY>), line_smem(LINE_MAX_NY));
+        k_march_lines<LINE_MAX_NY><<<unsigned(c.H), unsigned(threads), smem, c.stream>>>(c.geo(), A, D, n_top, n_bot);
+    }
+    c.check_launch("k_march_lines");
     c.prof_end(tok);
 }
+void launch_march_fh(Ctx& c, double D) { march_lines(c, D, c.b - 1, c.a, "march"); }
 // the march of the one slice n (the streaming-plasma march, Simulation::march_slice, src/sim_plasma.cpp:186-196)
-void launch_march_slice_fh(Ctx& c, double D, int n) {
-    const size_t ln = size_t(c.ny) * c.H;
-    FhScratch sc{c.fhs.p, c.fhs.p + ln, c.fhs.p + 2 * ln, c.fhs.p + 3 * ln, c.fhs.p + 4 * ln, c.fhcp.p};
-    const int tok = c.prof_begin("march_slice");
-    k_march_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p,
-                                                              c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, sc, D, n, n);
-    c.check_launch("k_march_fh");
-    c.prof_end(tok);
-}
+void launch_march_slice_fh(Ctx& c, double D, int n) { march_lines(c, D, n, n, "march_slice"); }
 // the lines of the streaming spectra: T0..T2 (the x spectra of the rows of j_x, j_y, j_z) -> out (3 half planes)
 void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2) {
     const size_t ln = size_t(c.ny) * c.H;

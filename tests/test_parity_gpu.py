@@ -225,3 +225,23 @@ def test_two_bunch_blocks_match_the_reference():
     for f in ["x", "y", "zeta", "px", "py", "pz"]:
         assert rel_l2(p[f], q[f]) <= TOL_SPEC, f
     assert rel_l2(s.array("F"), r.array("F")) <= TOL_F
+
+
+@pytest.mark.parametrize("grid", ["fourier", "freehand"])
+def test_reruns_are_bit_identical(grid):
+    """The beam deposit adds fixed-point integers (order-independent), and every reduction is a fixed-order tree,
+    so two runs of the same input give the same bits in every array, on both y grids."""
+    from g3d import Simulation, configs
+    cfg = stage_cfg(1) if grid == "fourier" else configs.freehand_small(nmacro=6000, steps=3)
+    runs = []
+    for _ in range(2):
+        s = Simulation(cfg)
+        s.init()
+        for _ in range(3):
+            s.step()
+        runs.append({a: s.array(a) for a in SPECTRA + ["F", "jw"]})
+        runs[-1]["particles"] = s.host_particles()
+        s.close()
+    a, b = runs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
