@@ -20,64 +20,67 @@ namespace g3d {
 
 // ---------------------------------------------------------------- deposit
 // Fixed-point deposit. Floating-point atomic adds make each sum depend on the order the adds arrive in, so two runs
-// of the same input differ at the last bits and drift apart. Here every deposit value v goes in as the integer
-// round(v 2^e) with a 64-bit integer atomic add, which is associative: the sums, and all that follows them, are the
-// same bits on every run. 2^e is the largest power of two with B 2^e < 2^62, B a bound on the sum of |v| over all
-// particles and points of one component (per particle: |f| x the largest dual-cell factor x max(1, |v_x/v_z|,
-// |v_y/v_z|), the TSC weights of a particle summing to 1), taken by a fixed-order two-level tree on the device, so
-// no sum can overflow; each add is rounded to 2^-e < 2^-61 B. A last pass turns the planes back into doubles
-// (times 2^-e, exact for a power of two), the raw planes of the reference's layout that the zeta filter reads.
+// of the same input differ at the last bits and drift apart. Here every deposit value v of component c goes in as
+// the integer round(v 2^e_c) with a 64-bit integer atomic add, which is associative: the sums, and all that follows
+// them, are the same bits on every run. 2^e_c is the largest power of two with B_c 2^e_c < 2^62, B_c a bound on the
+// sum of |v| over all particles and points of the component (per particle |f| x the largest dual-cell factor x
+// |v_x/v_z|, |v_y/v_z| or 1, the TSC weights of a particle summing to 1), taken by a fixed-order two-level tree on
+// the device, so no sum can overflow; each add is rounded to 2^-e_c < 2^-61 B_c, a scale of its own for each
+// component because j_x and j_y of a relativistic bunch are far below j_z. A last pass turns the planes back into
+// doubles (times 2^-e_c, exact for a power of two): the raw planes of the reference's layout that the filter reads.
 constexpr int DB = 296, DT = 256;     // blocks and threads of the bound's first level
 
-__device__ __forceinline__ double dep_bound_one(const PartsDev& P, long ip, const Geo& g, double ia_max) {
-    if (P.alive[ip] != 1) return 0;
+__device__ __forceinline__ void dep_bound_one(const PartsDev& P, long ip, const Geo& g, double ia_max, double b[3]) {
+    if (P.alive[ip] != 1) return;
     int m; double fz;
     g.zax.locate(P.zeta[ip], m, fz);
     const int hw = m - (g.a - 2);
-    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return 0;
-    const double vz = P.pz[ip];               // the ratios v/v_z are p/p_z
-    const double r = fmax(1.0, fmax(fabs(P.px[ip] / vz), fabs(P.py[ip] / vz)));
-    return fabs(P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx)) * ia_max * r;
+    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
+    const double pz = P.pz[ip];               // the ratios v/v_z are p/p_z
+    const double f = fabs(P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx)) * ia_max;
+    b[0] += f * fabs(P.px[ip] / pz); b[1] += f * fabs(P.py[ip] / pz); b[2] += f;
+}
+__device__ __forceinline__ void block_sum3(double v[3], double* __restrict__ out) {
+    __shared__ double sh[3][DT];
+    for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int st = DT / 2; st > 0; st >>= 1) {
+        if (int(threadIdx.x) < st)
+            for (int k = 0; k < 3; ++k) sh[k][threadIdx.x] += sh[k][threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 3; ++k) out[k] = sh[k][0];
 }
 __global__ void __launch_bounds__(DT) k_dep_bound(PartsDev P, long np, Geo g, double ia_max, double* __restrict__ part) {
-    __shared__ double sh[DT];
-    double acc = 0;
-    for (long i = long(blockIdx.x) * DT + threadIdx.x; i < np; i += long(gridDim.x) * DT) acc += dep_bound_one(P, i, g, ia_max);
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int st = DT / 2; st > 0; st >>= 1) {
-        if (int(threadIdx.x) < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+    double acc[3] = {0, 0, 0};
+    for (long i = long(blockIdx.x) * DT + threadIdx.x; i < np; i += long(gridDim.x) * DT) dep_bound_one(P, i, g, ia_max, acc);
+    block_sum3(acc, part + 3 * blockIdx.x);
 }
-// scale[0] = 2^e, scale[1] = 2^-e
+// scale[c] = 2^e_c, scale[3 + c] = 2^-e_c
 __global__ void __launch_bounds__(DT) k_dep_scale(const double* __restrict__ part, double* __restrict__ scale) {
-    __shared__ double sh[DT];
-    double acc = 0;
-    for (int b = threadIdx.x; b < DB; b += DT) acc += part[b];
-    sh[threadIdx.x] = acc;
+    double acc[3] = {0, 0, 0};
+    for (int b = threadIdx.x; b < DB; b += DT)
+        for (int k = 0; k < 3; ++k) acc[k] += part[3 * b + k];
+    __shared__ double tot[3];
+    block_sum3(acc, tot);
     __syncthreads();
-    for (int st = DT / 2; st > 0; st >>= 1) {
-        if (int(threadIdx.x) < st) sh[threadIdx.x] += sh[threadIdx.x + st];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        const double B = sh[0] * (1 + 1e-12) + 1e-300;   // rounding of the bound's own sum, and no zero
+    if (threadIdx.x < 3) {
+        const double B = tot[threadIdx.x] * (1 + 1e-12) + 1e-300;   // the rounding of the bound's own sum; never 0
         int x;
-        frexp(B, &x);                                     // B < 2^x
+        frexp(B, &x);                                               // B < 2^x
         const int e = min(62 - x, 1000);
-        scale[0] = ldexp(1.0, e); scale[1] = ldexp(1.0, -e);
+        scale[threadIdx.x] = ldexp(1.0, e); scale[3 + threadIdx.x] = ldexp(1.0, -e);
     }
 }
 __device__ __forceinline__ void fix_add(double* p, double v, double sc) {
     atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(__double2ll_rn(v * sc)));
 }
-__global__ void k_fix_to_double(double* __restrict__ J, long n, const double* __restrict__ scale) {
-    const double inv = scale[1];
+// pl: the values of one component (its planes)
+__global__ void k_fix_to_double(double* __restrict__ J, long n, long pl, const double* __restrict__ scale) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
         const long long q = reinterpret_cast<const long long*>(J)[i];
-        J[i] = double(q) * inv;
+        J[i] = double(q) * scale[3 + int(i / pl)];
     }
 }
 
@@ -91,7 +94,6 @@ __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __re
     g.zax.locate(P.zeta[ip], m, fz);
     const int hw = m - (g.a - 2);
     if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
-    const double sc = scale[0];
     const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
     const double gm = sqrt(1 + px * px + py * py + pz * pz);
     const double vx = px / gm, vy = py / gm, vz = pz / gm;
@@ -108,9 +110,9 @@ __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __re
         for (int u = 0; u < 3; ++u) {
             const long k = long(jn[v]) * g.nx + ix[u];
             const double w = f * wx[u] * wn[v] * ia0;
-            fix_add(J0 + k, w * vx / vz, sc);
-            fix_add(J0 + pl + k, w * vy / vz, sc);
-            fix_add(J0 + 2 * pl + k, w, sc);
+            fix_add(J0 + k, w * vx / vz, scale[0]);
+            fix_add(J0 + pl + k, w * vy / vz, scale[1]);
+            fix_add(J0 + 2 * pl + k, w, scale[2]);
         }
 }
 
@@ -220,21 +222,21 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
 }
 
 // ---------------------------------------------------------------- launchers
-// the scale 2^e of the fixed-point deposit into c.depfix[DB], [DB + 1] (ia_max: the largest dual-cell factor);
-// returns where it is
+// the scales 2^e_c, 2^-e_c of the fixed-point deposit (six values; ia_max: the largest dual-cell factor); returns
+// where they are
 const double* launch_deposit_scale(Ctx& c, double ia_max) {
-    if (c.depfix.n < size_t(DB + 2)) c.depfix.alloc(size_t(DB + 2), c.stream);
+    if (c.depfix.n < size_t(3 * DB + 6)) c.depfix.alloc(size_t(3 * DB + 6), c.stream);
     k_dep_bound<<<DB, DT, 0, c.stream>>>(c.parts, c.np, c.geo(), ia_max, c.depfix.p);
     c.check_launch("k_dep_bound");
-    k_dep_scale<<<1, DT, 0, c.stream>>>(c.depfix.p, c.depfix.p + DB);
+    k_dep_scale<<<1, DT, 0, c.stream>>>(c.depfix.p, c.depfix.p + 3 * DB);
     c.check_launch("k_dep_scale");
-    return c.depfix.p + DB;
+    return c.depfix.p + 3 * DB;
 }
 // the fixed-point planes back to doubles
 void launch_deposit_finish(Ctx& c) {
     const long n = long(c.jw.n);
     const long b = std::min<long>((n + 255) / 256, 148 * 16);
-    k_fix_to_double<<<unsigned(b), 256, 0, c.stream>>>(c.jw.p, n, c.depfix.p + DB);
+    k_fix_to_double<<<unsigned(b), 256, 0, c.stream>>>(c.jw.p, n, n / 3, c.depfix.p + 3 * DB);
     c.check_launch("k_fix_to_double");
 }
 void launch_deposit(Ctx& c) {

@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* _
     const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
     const double gm = sqrt(1 + px * px + py * py + pz * pz);
     const double vx = px / gm, vy = py / gm, vz = pz / gm;
-    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx), sc = scale[0];
+    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
     int ix[3], jn[3], jh[3]; double wx[3], wn[3], wh[3];
     tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
     tsc_y(g.yax, P.y[ip], jn, wn, jh, wh);
@@ -55,12 +55,12 @@ __global__ void __launch_bounds__(256) k_deposit_fh(PartsDev P, const int32_t* _
             if (nod) {
                 const long k = long(jn[v]) * g.nx + ix[u];
                 const double w = f * wx[u] * wn[v] * g.iA[jn[v]];
-                fix_add_fh(J0 + k, w * vx / vz, sc);
-                fix_add_fh(J0 + 2 * pl + k, w, sc);
+                fix_add_fh(J0 + k, w * vx / vz, scale[0]);
+                fix_add_fh(J0 + 2 * pl + k, w, scale[2]);
             }
             if (hal) {
                 const long k = long(jh[v]) * g.nx + ix[u];
-                fix_add_fh(J0 + pl + k, f * wx[u] * wh[v] * g.iD[jh[v]] * vy / vz, sc);
+                fix_add_fh(J0 + pl + k, f * wx[u] * wh[v] * g.iD[jh[v]] * vy / vz, scale[1]);
             }
         }
     }

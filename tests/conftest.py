@@ -44,9 +44,14 @@ def state_errors(got, ref, names):
 
 
 def assert_state(got, ref, names, tol=1e-10, comp_tol=1e-6, tag=""):
+    """The state bound on every component; the component bound only on components above 1e-12 of the state norm
+    (a component that small is rounding noise in both codes, e.g. R_y of an x-polarised laser on the free-hand
+    grid: 1.6e-11 against 5.6e4)."""
+    total = np.sqrt(sum(np.linalg.norm(np.asarray(ref[n])) ** 2 for n in names))
     for n, (e_state, e_comp) in state_errors(got, ref, names).items():
         assert e_state <= tol, (tag, n, "state-relative", e_state)
-        assert e_comp <= comp_tol, (tag, n, "component-relative", e_comp)
+        if np.linalg.norm(np.asarray(ref[n])) > 1e-12 * total:
+            assert e_comp <= comp_tol, (tag, n, "component-relative", e_comp)
 
 
 @pytest.fixture(scope="session")
