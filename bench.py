@@ -9,8 +9,10 @@ the half-cell-by-half-cell plasma march (Boris push, deposit, spectra, predictio
 slice, correction) + sponge + real fields: Simulation::step of the reference. Pushes per step = beam particles +
 streaming particles. The state (about 12 GB in FP64) is larger than L2.
 Workload 2: the oblique plane wave on a dense bunch (128 x 128 x 1024, 1,048,576 macro-electrons, no plasma).
+Workload 5: ionization injection on free-hand y and zeta grids (256 Fourier modes x 193 graded y nodes between walls,
+4096 graded slices, neutral H2 + 1 % N with ADK over every level, 16,440,320 streaming macro-particles per step).
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl g3d|reference] [--workload 2|3]
+    python bench.py [--gpus N --steps K --warmup W] [--impl g3d|reference] [--workload 1|2|3|5]
 
 Both forms are timed on the same inputs; value is the mixed form, fp64_form the FP64 form, mixed_error the
 relative L2 of F and the relative <p_z> of the mixed form against the FP64 form after the same steps. At N = 1
@@ -42,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="g3d", choices=["g3d", "reference"])
-    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3])
+    ap.add_argument("--workload", type=int, default=3, choices=[1, 2, 3, 5])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint march check on workload 4")
@@ -60,13 +62,28 @@ def workload(k, nzeta=None, particles=None):
     if nzeta:
         kw["nzeta"] = nzeta
     if particles:
-        kw["nmacro"] = particles
+        kw["ppc" if k == 5 else "nmacro"] = particles
     return configs.baseline(k, **kw)
 
 
+def lattice_particles(cfg):
+    """Streaming macro-particles loaded per step: the lattice points of the cells (inside the walls on the free-hand
+    y grid) times the species (electrons when free, and every ion species)."""
+    if cfg.plasma is None:
+        return 0
+    from g3d import configs
+    pd = configs.default_plasma()
+    pd.update(cfg.plasma)
+    rows = cfg.ny if cfg.ynode is None else cfg.ny - 2
+    species = (1 if pd["free_electrons"] else 0) + len(cfg.ions)
+    return cfg.nx * rows * pd["ppc_x"] * pd["ppc_y"] * species
+
+
 def config_json(cfg, k, form="fp64"):
+    what = (f"{cfg.particles} macro-electrons" if cfg.particles else
+            f"{lattice_particles(cfg)} streaming macro-particles per step")
     return {"workload": f"{k}: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, "
-                        f"{cfg.particles} macro-electrons, {'mixed FP32/FP64' if form == 'mixed' else 'FP64'} form",
+                        f"{what}, {'mixed FP32/FP64' if form == 'mixed' else 'FP64'} form",
             "form": form,
             "nx": cfg.nx, "ny": cfg.ny, "nzeta": cfg.nzeta, "particles": cfg.particles,
             "grid_points": cfg.grid_points, "dz": cfg.params["dz"], "sponge": cfg.params.get("sponge", 0),
@@ -270,6 +287,8 @@ def reference_rate(cfg, steps, threads, k=None, warmup=0):
         r.close()
         return cfg.particles * steps / dt, (f"the full workload, init and {warmup} s-steps untimed, then {steps} "
                                             f"timed s-steps, OpenMP on {threads} threads"), dt / steps * 1e3
+    if k == 5:
+        return reference_rate_lattice(cfg, steps, threads, warmup)
     if k is None or cfg.nzeta <= SAMPLE_SLICES[-1]:
         return None, "no sampled windows for this workload", None
     pts = []
@@ -300,6 +319,49 @@ def reference_rate(cfg, steps, threads, k=None, warmup=0):
         f"witness; {t1:.2f} s and {t2:.2f} s per step), t = a + b N fitted through them and evaluated at N = "
         f"{cfg.nzeta} ({t_full:.1f} s per step); pushes = {cfg.particles} beam + {S} streaming particles; OpenMP on "
         f"{threads} threads"), t_full * 1e3
+
+
+LATTICE_SAMPLE = (256, (1, 2))    # workload 5's reference sample: slices, and lattice points per cell along x, y
+
+
+def reference_rate_lattice(cfg, steps, threads, warmup):
+    """Workload 5 on the reference: its 16.4 M streaming macro-particles a step through 4,096 slices would take the
+    reference hours a step. The sample is the workload's grids and gas on a window of 256 graded slices with 1 x 1 and
+    2 x 2 lattice points per cell: the step time is t = a + b S in the streaming particles S of a step (the lattice and
+    the electrons freed from it; the field work of the 256 slices in a, the streaming push in b), fitted through the
+    two; the full step is then (a + b S_full) x (nzeta - 1) / 255, the work of every term growing with the half-cells
+    a particle crosses, S_full the full lattice with the same share of freed electrons as the larger sample. A fit that
+    is not increasing in S returns (None, why, None)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref
+    from g3d import configs
+    if not ref.available():
+        return None, "oracle/_ref/libg3dref.so not built", None
+    n_s, ppcs = LATTICE_SAMPLE
+    pts = []
+    for ppc in ppcs:
+        c2 = configs.config5(nzeta=n_s, ppc=ppc)
+        r = ref.RefSimulation(c2, threads=threads)
+        r.init()
+        for _ in range(warmup):
+            r.step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r.step()
+        dt = (time.perf_counter() - t0) / steps
+        pts.append((len(r.streaming_particles()), dt, lattice_particles(c2)))
+        r.close()
+    (s1, t1, _), (s2, t2, l2) = pts
+    b = (t2 - t1) / (s2 - s1)
+    S = lattice_particles(cfg) * s2 / l2          # the lattice and the electrons the gas frees, as in the sample
+    t_full = (t1 + b * (S - s1)) * (cfg.nzeta - 1) / (n_s - 1)
+    if not (b > 0) or not (t_full > 0):
+        return None, f"reference sample not increasing in the particle count ({t1:.2f} s, {t2:.2f} s)", None
+    return S / t_full, (
+        f"{steps} timed s-step(s) per sample after an untimed init and {warmup} untimed s-step(s), on a window of "
+        f"{n_s} graded slices of the workload's grids with {s1} and {s2} streaming particles a step (1 x 1 and 2 x 2 per "
+        f"cell; {t1:.2f} s and {t2:.2f} s per step), t = a + b S fitted and scaled to {S:.0f} particles and "
+        f"{cfg.nzeta} slices ({t_full:.0f} s per step); OpenMP on {threads} threads"), t_full * 1e3
 
 
 def host_cores():

@@ -376,6 +376,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
         sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;
+        sa.inv_dx = 1 / c.dx; sa.inv_dy = 1 / c.dy; sa.dep_norm = 0;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
             // (for the half-cells below the first, fused into the correction of the half-cell above)
@@ -385,6 +386,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             for (int pass = 0; pass < passes; ++pass) {
                 if (fh) launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
+                sa.dep_norm = 1 / (Delta * (c.zeta[size_t(n) + 1] - c.zeta[size_t(n)]) * c.dx);
                 sa.pass = pass;
                 sa.dry = pass + 1 < passes ? 1 : 0;
                 launch_stream(c, sa);

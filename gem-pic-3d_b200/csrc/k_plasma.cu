@@ -131,6 +131,54 @@ __device__ __forceinline__ void sgather_mid(const StreamArgs& c, double x, doubl
     E[0] = double(a[0]); E[1] = double(a[1]); E[2] = double(a[2]);
     B[0] = double(a[3]); B[1] = double(a[4]); B[2] = double(a[5]);
 }
+// The FP32 push's TSC on a periodic grid: the cell coordinate t = x / d and the nearest node in FP64 (x spans the
+// box, so the index needs the double), the offset from that node in FP32, the three weights in FP32.
+__device__ __forceinline__ void tsc_f32(double x, double inv_d, int n, int idx[3], float w[3]) {
+    const double t = x * inv_d;
+    const double c = floor(t + 0.5);
+    const float f = float(t - c);
+    w[0] = 0.5f * (0.5f - f) * (0.5f - f);
+    w[1] = 0.75f - f * f;
+    w[2] = 0.5f * (0.5f + f) * (0.5f + f);
+    int b = (int(c) - 1) % n;
+    if (b < 0) b += n;
+    const int b1 = b + 1 == n ? 0 : b + 1;
+    idx[0] = b; idx[1] = b1; idx[2] = b1 + 1 == n ? 0 : b1 + 1;
+}
+// The midpoint gather of the FP32 push (Fourier y): the interleaved midpoint fields with FP32 weights, straight into
+// the FP32 fields of the Boris push.
+__device__ __forceinline__ void sgather_mid_f32(const StreamArgs& c, double x, double y, float E[3], float B[3]) {
+    int ix[3], jn[3]; float wx[3], wn[3];
+    tsc_f32(x, c.inv_dx, c.g.nx, ix, wx);
+    tsc_f32(y, c.inv_dy, c.g.ny, jn, wn);
+    float a[6] = {0, 0, 0, 0, 0, 0};
+    const float4* F4 = reinterpret_cast<const float4*>(c.Fmid);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const long k = long(jn[j]) * c.g.nx + ix[i];
+            const float w = wx[i] * wn[j];
+            const float4 u = __ldg(F4 + 2 * k), v = __ldg(F4 + 2 * k + 1);
+            a[0] += w * u.x; a[1] += w * u.y; a[2] += w * u.z; a[3] += w * u.w; a[4] += w * v.x; a[5] += w * v.y;
+        }
+    E[0] = a[0]; E[1] = a[1]; E[2] = a[2]; B[0] = a[3]; B[1] = a[4]; B[2] = a[5];
+}
+// The FP32 push's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
+__device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, double y, float f, float vx, float vy, float vz) {
+    int ix[3], jn[3]; float wx[3], wn[3];
+    tsc_f32(x, c.inv_dx, c.g.nx, ix, wx);
+    tsc_f32(y, c.inv_dy, c.g.ny, jn, wn);
+    const float fa = f * float(c.g.iA[0]);
+    float4* J4 = reinterpret_cast<float4*>(c.Jf);
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            const float w = fa * wx[u] * wn[v];
+            atomicAdd(J4 + long(jn[v]) * c.g.nx + ix[u], make_float4(w * vx, w * vy, w * vz, 0.f));
+        }
+}
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
@@ -244,6 +292,8 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
 struct DepReq {
     double x, y, f, vx, vy, vz;
     bool on;
+    bool f32;                  // the FP32 push on the Fourier y grid: deposit with sdeposit_f32 (ff, fv)
+    float ff, fv[3];
 };
 
 // one streaming particle through half-cell n (stream_one, sim_stream.hpp:104-171); its deposit is returned to
@@ -254,7 +304,7 @@ struct DepReq {
 // plane wave is on. Both are fixed for a run; the variants without them hold fewer registers.
 template <bool F32, bool ION, bool LASER>
 __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
-    DepReq d{0, 0, 0, 0, 0, 0, false};
+    DepReq d{0, 0, 0, 0, 0, 0, false, false, 0.f, {0.f, 0.f, 0.f}};
     const Geo& g = c.g;
     const int n = c.n;
     const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn;
@@ -277,7 +327,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const bool ion = sp >= SP_ION && sp < SP_FREED;
     if (ion && !c.ions[sp - SP_ION].mobile) {        // fixed ion: its charge, then the ionization
         const double f = qw * hl / (c.Delta * h * g.dx);
-        if (f != 0) d = DepReq{x, y, f, 0, 0, 0, true};
+        if (f != 0) d = DepReq{x, y, f, 0, 0, 0, true, false, 0.f, {0.f, 0.f, 0.f}};
         if (!c.dry) S.zeta[i] = zn;
         if constexpr (ION) {
             const double E1 = field_abs<F32>(c, x, y, z, zeta), E0 = field_abs<F32>(c, x, y, z, zn);
@@ -294,14 +344,20 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const A hd = A(0.5) * dt0 * ig0;
     const double xm = x + double(hd * px), ym = y + double(hd * py);
     const double zm = z + double(hd * pz), zetam = zeta - 0.5 * hl;
-    double Ed[3], Bd[3], Ee[3], Be[3];
-    if (c.Fmid && zeta == zn1) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), Ed, Bd);   // the whole half-cell
-    else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, Ed, Bd);
-    if constexpr (LASER) {
-        c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
-        for (int k = 0; k < 3; ++k) { Ed[k] += Ee[k]; Bd[k] += Be[k]; }
+    A E[3], B[3];
+    const bool mid = c.Fmid && zeta == zn1;                       // the whole half-cell: the midpoint fields
+    if (F32 && mid && !LASER) {
+        if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy(g, ym), E, B);
+    } else {
+        double Ed[3], Bd[3], Ee[3], Be[3];
+        if (mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), Ed, Bd);
+        else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, Ed, Bd);
+        if constexpr (LASER) {
+            c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
+            for (int k = 0; k < 3; ++k) { Ed[k] += Ee[k]; Bd[k] += Be[k]; }
+        }
+        for (int k = 0; k < 3; ++k) { E[k] = A(Ed[k]); B[k] = A(Bd[k]); }
     }
-    const A E[3] = {A(Ed[0]), A(Ed[1]), A(Ed[2])}, B[3] = {A(Bd[0]), A(Bd[1]), A(Bd[2])};
     A ux = px, uy = py, uz = pz;
     boris<A>(ux, uy, uz, E, B, qm, dt0);
     A g1 = sqrt(A(1) + ux * ux + uy * uy + uz * uz);
@@ -332,8 +388,18 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         S.px[i] = ux; S.py[i] = uy; S.pz[i] = uz;
         S.zeta[i] = zeta_end;
     }
-    const double f = qw * double(dt) / (c.Delta * h * g.dx);
-    if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true};
+    if constexpr (F32) {
+        if (g.yf) {                   // FP32 deposit: the factor 1 / (Delta h dx) taken once per half-cell
+            const float ff = float(qw * c.dep_norm) * float(dt);
+            if (ff != 0.f) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), 0, 0, 0, 0, true, true, ff, {float(vx), float(vy), float(vz)}};
+        } else {
+            const double f = qw * double(dt) / (c.Delta * h * g.dx);
+            if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true, false, 0.f, {0.f, 0.f, 0.f}};
+        }
+    } else {
+        const double f = qw * double(dt) / (c.Delta * h * g.dx);
+        if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true, false, 0.f, {0.f, 0.f, 0.f}};
+    }
     if (!g.yf && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
         if (!c.dry) S.alive[i] = 0;
         return d;
@@ -366,7 +432,10 @@ __global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
         const DepReq d = stream_one<F32, ION, LASER>(c, S, i);
-        if (d.on) sdeposit<F32>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
+        if (d.on) {
+            if (F32 && d.f32) sdeposit_f32(c, d.x, d.y, d.ff, d.fv[0], d.fv[1], d.fv[2]);
+            else sdeposit<F32>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
+        }
     }
 }
 template <bool F32>
