@@ -306,6 +306,14 @@ void launch_adj_wsum(Ctx& c, const int32_t* alive, double* out);
 void launch_adj_beta(Ctx& c, const double* X, const int32_t* alive, double coef, double* lam);
 void launch_adj_widen(Ctx& c, const cpxf* a, cpx* b, long n);
 std::vector<g3d_particle> get_streaming(Ctx& c);
+// the plasma state of a checkpoint (g3d_plasma.cu): the joining list, the trapping counters, the streaming current
+// of level s0 in the reference's full layout
+std::vector<g3d_particle> get_joining(Ctx& c);
+void set_joining(Ctx& c, const std::vector<g3d_particle>& v);
+void get_plasma_counters(const Ctx& c, long& trapped, long& restreamed);
+void set_plasma_counters(Ctx& c, long trapped, long restreamed);
+std::vector<cpx> get_js0(Ctx& c, int comp);
+void set_js0(Ctx& c, int comp, const std::vector<cpx>& v);
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)
 

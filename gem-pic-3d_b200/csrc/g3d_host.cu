@@ -893,8 +893,12 @@ template <class T>
 static void write_checkpoint(Ctx& c, const char* path) {
     CkptHeader h{};
     std::memcpy(h.magic, MAGIC, 8);
-    h.ranks = 1; h.rank = 0; h.N = c.N; h.a = c.a; h.b = c.b; h.ns = c.ns; h.nk = c.nk; h.nx = c.nx; h.ny = c.ny; h.plasma = 0;
-    h.istep = c.istep; h.lost = c.lost_total; h.trapped = 0; h.restreamed = 0;
+    h.ranks = 1; h.rank = 0; h.N = c.N; h.a = c.a; h.b = c.b; h.ns = c.ns; h.nk = c.nk; h.nx = c.nx; h.ny = c.ny;
+    h.plasma = c.pl ? 1 : 0;
+    h.istep = c.istep; h.lost = c.lost_total;
+    long trapped = 0, restreamed = 0;
+    get_plasma_counters(c, trapped, restreamed);
+    h.trapped = trapped; h.restreamed = restreamed;
     h.s = c.s; h.X0 = c.X0; h.Y0 = c.Y0; h.beta_b = c.beta_b; h.gm2_b = c.gm2_b; h.stop = c.stop_; h.ncent = int(c.cent_.size());
     const std::string tmp = std::string(path) + ".tmp";
     FILE* f = std::fopen(tmp.c_str(), "wb");
@@ -906,12 +910,16 @@ static void write_checkpoint(Ctx& c, const char* path) {
             get_array(c, w, v.data());
             put(f, v.data(), v.size());
         }
-        for (int k = 0; k < 3; ++k) put<cpx>(f, nullptr, 0);      // js0x, js0y, js0z: no plasma
+        for (int k = 0; k < 3; ++k) {                              // js0x, js0y, js0z: the streaming current of s0
+            if (c.pl) { const std::vector<cpx> v = get_js0(c, k); put(f, v.data(), v.size()); }
+            else put<cpx>(f, nullptr, 0);
+        }
         const std::vector<float> fv = d2h(c, c.F.p, c.F.n);
         put(f, fv.data(), fv.size());
         const std::vector<g3d_particle> pv = get_particles(c);
         put(f, pv.data(), pv.size());
-        put<g3d_particle>(f, nullptr, 0);                          // joining: no plasma
+        if (c.pl) { const std::vector<g3d_particle> jv = get_joining(c); put(f, jv.data(), jv.size()); }
+        else put<g3d_particle>(f, nullptr, 0);                     // joining: no plasma
         for (const auto& v : c.cent_) put(f, v.data(), 3);
     } catch (...) { std::fclose(f); throw; }
     std::fclose(f);
@@ -926,7 +934,7 @@ static void read_checkpoint(Ctx& c, const char* path) {
         if (std::fread(&h, sizeof h, 1, f) != 1 || std::memcmp(h.magic, MAGIC, 8))
             throw Error(G3D_ERR_IO, std::string(path) + ": not a GEM-PIC-3D checkpoint");
         if (h.ranks != 1) throw Error(G3D_ERR_IO, std::string(path) + ": written by " + std::to_string(h.ranks) + " ranks; restart with as many");
-        if (h.N != c.N || h.a != c.a || h.b != c.b || h.nx != c.nx || h.ny != c.ny || h.plasma != 0)
+        if (h.N != c.N || h.a != c.a || h.b != c.b || h.nx != c.nx || h.ny != c.ny || h.plasma != (c.pl ? 1 : 0))
             throw Error(G3D_ERR_IO, std::string(path) + ": the grid (nx, ny, zeta slices) or the plasma differ");
         std::vector<std::vector<cpx>> arrays;
         for (int k = 0; k < 11; ++k) arrays.push_back(get<cpx>(f));
@@ -948,14 +956,21 @@ static void read_checkpoint(Ctx& c, const char* path) {
             if (arrays[size_t(k)].size() != ref_count(c, array_ref(c, ids[k])))
                 throw Error(G3D_ERR_IO, std::string(path) + ": array sizes differ from the grid");
         for (int k = 0; k < 8; ++k) set_array(c, ids[k], arrays[size_t(k)].data());
-        for (int k = 8; k < 11; ++k)
-            if (!arrays[size_t(k)].empty()) throw Error(G3D_ERR_IO, std::string(path) + ": streaming currents present but no plasma");
-        if (!jv.empty()) throw Error(G3D_ERR_IO, std::string(path) + ": joining particles present but no plasma");
+        if (!c.pl) {
+            for (int k = 8; k < 11; ++k)
+                if (!arrays[size_t(k)].empty()) throw Error(G3D_ERR_IO, std::string(path) + ": streaming currents present but no plasma");
+            if (!jv.empty()) throw Error(G3D_ERR_IO, std::string(path) + ": joining particles present but no plasma");
+        } else {
+            for (int k = 8; k < 11; ++k) set_js0(c, k - 8, arrays[size_t(k)]);
+            set_joining(c, jv);
+            set_plasma_counters(c, h.trapped, h.restreamed);
+        }
         G3D_CUDA(cudaMemcpyAsync(c.F.p, fv.data(), c.F.bytes(), cudaMemcpyHostToDevice, c.stream));
         set_particles(c, pv.data(), long(pv.size()));
         c.istep = h.istep; c.lost_total = h.lost; c.s = h.s; c.X0 = h.X0; c.Y0 = h.Y0;
         c.beta_b = h.beta_b; c.gm2_b = h.gm2_b; c.stop_ = h.stop != 0;
         c.cent_ = cent;
+        c.fields_ready = true;
         G3D_CUDA(cudaStreamSynchronize(c.stream));
     } catch (...) {
         if (f) std::fclose(f);

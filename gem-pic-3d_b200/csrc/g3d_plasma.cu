@@ -252,22 +252,19 @@ static void load_plasma(Ctx& c, double s0, double s1) {
 }
 
 // The streaming particles back on the host (the reference's `strm` after a march).
-std::vector<g3d_particle> get_streaming(Ctx& c) {
-    PlasmaState& P = *c.pl;
-    long n = 0;
-    G3D_CUDA(cudaMemcpyAsync(&n, P.nstrm_dev.p, sizeof(long), cudaMemcpyDeviceToHost, c.stream));
-    G3D_CUDA(cudaStreamSynchronize(c.stream));
+// n streaming particles of a device list as host records
+static std::vector<g3d_particle> records_of(Ctx& c, const StrmDev& S, long n) {
     std::vector<g3d_particle> out(static_cast<size_t>(n));
     if (!n) return out;
     std::vector<double> hd(size_t(n) * 10);
     std::vector<int32_t> hi(size_t(n) * 2);
     std::vector<uint64_t> hu(static_cast<size_t>(n));
-    const double* cols[10] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.px, P.strm.py, P.strm.pz, P.strm.w, P.strm.z, P.strm.q, P.strm.qm};
+    const double* cols[10] = {S.x, S.y, S.zeta, S.px, S.py, S.pz, S.w, S.z, S.q, S.qm};
     for (int m = 0; m < 10; ++m)
         G3D_CUDA(cudaMemcpyAsync(hd.data() + size_t(m) * n, cols[m], size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
-    G3D_CUDA(cudaMemcpyAsync(hi.data(), P.strm.alive, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
-    G3D_CUDA(cudaMemcpyAsync(hi.data() + n, P.strm.sp, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
-    G3D_CUDA(cudaMemcpyAsync(hu.data(), P.strm.id, size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data(), S.alive, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hi.data() + n, S.sp, size_t(n) * 4, cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaMemcpyAsync(hu.data(), S.id, size_t(n) * 8, cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     for (long k = 0; k < n; ++k) {
         g3d_particle& p = out[size_t(k)];
@@ -276,6 +273,62 @@ std::vector<g3d_particle> get_streaming(Ctx& c) {
         p.alive = hi[size_t(k)]; p.sp = hi[size_t(n) + k]; p.id = hu[size_t(k)];
     }
     return out;
+}
+
+std::vector<g3d_particle> get_streaming(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    long n = 0;
+    G3D_CUDA(cudaMemcpyAsync(&n, P.nstrm_dev.p, sizeof(long), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return records_of(c, P.strm, n);
+}
+
+// The particles that join the next march, in the order the next march appends them (the last march's slow trapped
+// ones kept on the device, then those from the host): the reference's joining list of a checkpoint.
+std::vector<g3d_particle> get_joining(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    std::vector<g3d_particle> out = records_of(c, P.jb.v, P.njb);
+    out.insert(out.end(), P.joining.begin(), P.joining.end());
+    return out;
+}
+// A checkpoint's joining list: all of it joins from the host
+void set_joining(Ctx& c, const std::vector<g3d_particle>& v) {
+    PlasmaState& P = *c.pl;
+    P.njb = 0;
+    P.joining = v;
+}
+void get_plasma_counters(const Ctx& c, long& trapped, long& restreamed) {
+    trapped = c.pl ? c.pl->trapped_total : 0;
+    restreamed = c.pl ? c.pl->restreamed_total : 0;
+}
+void set_plasma_counters(Ctx& c, long trapped, long restreamed) {
+    if (!c.pl) return;
+    c.pl->trapped_total = trapped;
+    c.pl->restreamed_total = restreamed;
+}
+// the streaming current of level s0 (ns + 1 half-cell planes) in the reference's full layout, and back
+std::vector<cpx> get_js0(Ctx& c, int comp) {
+    PlasmaState& P = *c.pl;
+    const DevBuf<cpx>& b = comp == 0 ? P.js0x : comp == 1 ? P.js0y : P.js0z;
+    const long planes = long(c.ns + 1);
+    DevBuf<cpx> full;
+    full.alloc(size_t(planes) * c.nk, c.stream);
+    launch_half_to_full(c, b.p, full.p, planes);
+    std::vector<cpx> v(size_t(planes) * c.nk);
+    G3D_CUDA(cudaMemcpyAsync(v.data(), full.p, v.size() * sizeof(cpx), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    return v;
+}
+void set_js0(Ctx& c, int comp, const std::vector<cpx>& v) {
+    PlasmaState& P = *c.pl;
+    DevBuf<cpx>& b = comp == 0 ? P.js0x : comp == 1 ? P.js0y : P.js0z;
+    const long planes = long(c.ns + 1);
+    if (v.size() != size_t(planes) * c.nk) throw Error(G3D_ERR_IO, "checkpoint: streaming current of another grid");
+    DevBuf<cpx> full;
+    full.alloc(v.size(), c.stream);
+    G3D_CUDA(cudaMemcpyAsync(full.p, v.data(), v.size() * sizeof(cpx), cudaMemcpyHostToDevice, c.stream));
+    launch_full_to_half(c, full.p, b.p, planes);
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
 
 // The trapped streaming particles that join the beam (P.tr after launch_trapped_split, n of them) on the host.

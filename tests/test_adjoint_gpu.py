@@ -183,6 +183,81 @@ def test_momentum_gradient_against_central_differences_of_the_reference(charge_p
     assert abs(ad - fr) <= 1e-5 * abs(fr), (ad, fr)
 
 
+def hermitian_direction(rng, ny, nx):
+    """A random direction over the stored modes [j][k_x], k_x = 0 .. nx/2, that keeps a real field real: on the
+    columns k_x = 0 and k_x = nx/2, whose modes j and -j are both stored, d(-j) = conj d(j) (real at j = 0, ny/2)."""
+    H = nx // 2 + 1
+    d = rng.standard_normal((ny, H)) + 1j * rng.standard_normal((ny, H))
+    for c in (0, H - 1):
+        for j in range(ny // 2 + 1):
+            m = (-j) % ny
+            if m == j:
+                d[j, c] = d[j, c].real
+            else:
+                d[m, c] = np.conj(d[j, c])
+    return d
+
+
+def full_coefficients(a_half, nx):
+    """The stored half [j][k_x <= nx/2] of the mode coefficients as a full [j][ix] array: conj a(-j, nx - ix) on the
+    other half, as the library's Hermitian storage implies."""
+    ny, H = a_half.shape
+    full = np.empty((ny, nx), dtype=np.complex128)
+    full[:, :H] = a_half
+    for ix in range(H, nx):
+        full[:, ix] = np.conj(a_half[(-np.arange(ny)) % ny, nx - ix])
+    return full
+
+
+def reference_final_modes(cfg, a_half):
+    """The final beam of the reference CPU code with every grid laser's spectrum multiplied by the coefficients a:
+    the reference's init, then its last stages after the lasers are added replayed from R + (a - 1) s, s the laser
+    spectrum added at init (R of an init with the lasers minus R of one without them). Those stages, march(0) and
+    sponge_and_real_fields without a sponge, take R as it is, and j0 = jk then, so the replay is the reference's
+    init with a (a patch of the reference's add_grid_lasers would give the same)."""
+    import copy
+    ref = pytest.importorskip("ref")
+    if not ref.available():
+        pytest.skip("reference build oracle/_ref not present")
+    assert cfg.params.get("sponge", 0) == 0
+    bare = copy.deepcopy(cfg)
+    bare.glasers = []
+    r0 = ref.RefSimulation(bare, threads=8)
+    r0.init()
+    R0 = {k: r0.array(k) for k in ("Rx", "Ry")}
+    r0.close()
+    r = ref.RefSimulation(cfg, threads=8)
+    try:
+        r.init()
+        A = np.tile(full_coefficients(a_half, cfg.nx).ravel(), cfg.nzeta)
+        for k in ("Rx", "Ry"):
+            R = r.array(k)
+            r.set_array(k, R + (A - 1) * (R - R0[k]))
+        r.march(0.0)
+        r.sponge_and_real_fields()
+        for _ in range(cfg.steps):
+            r.step()
+        return r.host_particles()
+    finally:
+        r.close()
+
+
+def test_laser_mode_gradient_against_central_differences_of_the_reference():
+    """dJ/da along a random direction against central differences of the reference's own CPU code (its float real
+    fields, so eps = 3e-3 as for the momenta), and this library's forward taking the same difference to 1e-9."""
+    from g3d import configs
+    cfg = configs.adjoint_small(charge_pC=1.0)
+    _, gm, _, _ = adjoint(cfg, exact=False)
+    d = hermitian_direction(np.random.default_rng(21), cfg.ny, cfg.nx)
+    e = 3e-3
+    fr = central(reference_final_modes(cfg, 1 + e * d), reference_final_modes(cfg, 1 - e * d), e)
+    fo = central(forward(cfg, coef=1 + e * d, exact=False), forward(cfg, coef=1 - e * d, exact=False), e)
+    ad = float(np.real(np.sum(np.conj(gm) * d)))
+    print(f"laser modes: reference central difference {fr:.12e}, this forward's {fo:.12e}, adjoint {ad:.12e}")
+    assert abs(fo - fr) <= 1e-9 * abs(fr), (fo, fr)
+    assert abs(ad - fr) <= 1e-5 * abs(fr), (ad, fr)
+
+
 def autograd_inputs(cfg):
     import torch
     from g3d.sim import sample_bunches

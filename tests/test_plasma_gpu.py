@@ -133,3 +133,34 @@ def test_ionization_event_set_is_identical():
             assert rel_l2(ps[f], pr[f]) <= 1e-9, (k, f)
     freed = ps[(ps["sp"] >= 50) & (ps["sp"] < 100)]
     assert len(freed) > 0, "the case must ionize"
+
+
+@needs_ref
+def test_plasma_checkpoint_restarts_the_reference_and_back(tmp_path):
+    """With a plasma a checkpoint also holds the streaming current of level s0 and the particles that join the next
+    march (reference src/sim_checkpoint.cpp:39-58). A driver strong enough to trap: libg3d's checkpoint after step 1
+    restarts the reference, the reference's after step 2 restarts libg3d, and each continues as the other."""
+    from g3d import Simulation, configs
+    cfg = configs.lwfa_small(a0=3.0, n0=0.02)
+    s, r = run_pair(cfg, 2)
+    s.step(); r.step()
+    s.write_checkpoint(tmp_path / "checkpoint_000001_r0000.bin")
+    r2 = ref.RefSimulation(cfg, threads=1)
+    r2.read_checkpoint(tmp_path, 1)
+    for a in ["Rx", "Ry", "Ez", "Bz", "Lx", "Ly", "j0x", "j0y"]:
+        assert np.array_equal(s.array(a), r2.array(a)), a
+    s.step(); r2.step()
+    compare_fields(s, r2, tol=1e-9, tag="reference from libg3d's checkpoint")
+    ps, pr = s.streaming_particles(), r2.streaming_particles()
+    fresh = cfg.nx * cfg.ny * cfg.plasma["ppc_x"] * cfg.plasma["ppc_y"] * 2
+    assert len(ps) == len(pr) > fresh and np.array_equal(ps["id"], pr["id"])      # the joining particles came along
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        assert rel_l2(ps[f], pr[f]) <= 1e-9, f
+    r2.write_checkpoint(tmp_path)
+    s2 = Simulation(cfg)
+    s2.read_checkpoint(tmp_path / "checkpoint_000002_r0000.bin")
+    s2.step(); r2.step()
+    compare_fields(s2, r2, tol=1e-9, tag="libg3d from the reference's checkpoint")
+    assert s2.status().istep == r2.status().istep == 3
+    for sim in (s, s2, r, r2):
+        sim.close()
