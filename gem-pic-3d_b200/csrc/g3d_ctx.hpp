@@ -75,6 +75,16 @@ struct LaserDev {
     }
 };
 
+// External magnetic elements on the device (k_external.cuh): the undulators and magnets of g3d_set_external and
+// the taper table of the undulators.
+struct ExtDev {
+    int nu, nm;
+    const g3d_undulator* u;
+    const g3d_magnet* m;
+    const double* kt;
+    G3D_HD bool any() const { return nu > 0 || nm > 0; }
+};
+
 // ---------------------------------------------------------------- device buffers
 template <class T>
 struct DevBuf {
@@ -197,6 +207,11 @@ struct Ctx {
     // streaming plasma (null without plasma) and the grid lasers of the start field
     std::unique_ptr<PlasmaState> pl;
     std::vector<g3d_grid_laser> glasers;
+    // external magnetic elements (g3d_set_external)
+    DevBuf<g3d_undulator> und;
+    DevBuf<g3d_magnet> mag;
+    DevBuf<double> ktab;
+    ExtDev ext{0, 0, nullptr, nullptr, nullptr};
 
     Ctx();
     ~Ctx();

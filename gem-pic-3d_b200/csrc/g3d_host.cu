@@ -1022,6 +1022,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     if (c.laser.on) throw Error(G3D_ERR_ARG, "the adjoint march differentiates grid lasers, not the analytic laser");
     if (!c.P.self_fields || c.P.freeze_bunch) throw Error(G3D_ERR_ARG, "the adjoint march needs self fields and a free bunch");
     if (!c.fields_ready || c.istep != 0) throw Error(G3D_ERR_STATE, "the adjoint march starts right after g3d_init");
+    if (c.ext.any()) throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate external elements");
     if (grad_modes && !c.lmode.p) throw Error(G3D_ERR_STATE, "set the laser mode coefficients (g3d_set_laser_modes) before g3d_init");
     const long np = c.np;
     const size_t Fn = c.F.n, ns = size_t(c.ns), nkh = size_t(c.nkh), nk = size_t(c.nk);
@@ -1330,6 +1331,27 @@ int g3d_add_grid_laser(g3d_ctx* ctx, const g3d_grid_laser* laser) {
     return guarded(ctx, [&] {
         if (!laser || !(laser->waist > 0) || !(laser->tau > 0)) throw Error(G3D_ERR_ARG, "grid laser: waist and tau must be positive");
         ctx->c.glasers.push_back(*laser);
+    });
+}
+int g3d_set_external(g3d_ctx* ctx, const g3d_undulator* u, int32_t nu, const g3d_magnet* m, int32_t nm, const double* kt,
+                     int32_t nkt) {
+    return guarded(ctx, [&] {
+        if (nu < 0 || nm < 0 || nkt < 0 || (nu && !u) || (nm && !m) || (nkt && !kt))
+            throw Error(G3D_ERR_ARG, "g3d_set_external: bad element arrays");
+        for (int k = 0; k < nu; ++k) {
+            const g3d_undulator& U = u[k];
+            if (!(U.ku > 0) || !(U.z1 > U.z0) || U.ramp < 0 || (U.nk > 0 && (U.nk < 2 || U.koff < 0 || U.koff + U.nk > nkt || !(U.dzk > 0))))
+                throw Error(G3D_ERR_ARG, "g3d_set_external: undulator " + std::to_string(k) + " (period, extent, ramp or taper table)");
+        }
+        for (int k = 0; k < nm; ++k)
+            if (m[k].kind < 0 || m[k].kind > 2 || !(m[k].z1 > m[k].z0) || m[k].ramp < 0 || !(m[k].dsmax > 0))
+                throw Error(G3D_ERR_ARG, "g3d_set_external: magnet " + std::to_string(k) + " (kind, extent, ramp or dsmax)");
+        Ctx& c = ctx->c;
+        c.und.upload(std::vector<g3d_undulator>(u, u + nu), c.stream);
+        c.mag.upload(std::vector<g3d_magnet>(m, m + nm), c.stream);
+        c.ktab.upload(std::vector<double>(kt, kt + nkt), c.stream);
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+        c.ext = g3d::ExtDev{nu, nm, c.und.p, c.mag.p, c.ktab.p};
     });
 }
 int g3d_march_plasma(g3d_ctx* ctx, double s0, double s1) {

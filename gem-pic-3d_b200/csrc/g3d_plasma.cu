@@ -404,6 +404,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
     mixk(ptr(c.F.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
+    mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
     uint64_t dbits;
@@ -430,6 +431,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
         sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;
         sa.inv_dx = 1 / c.dx; sa.inv_dy = 1 / c.dy; sa.dep_norm = 0;
+        sa.ext = c.ext;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
             // (for the half-cells below the first, fused into the correction of the half-cell above)

@@ -23,6 +23,7 @@
 #include <type_traits>
 #include <cub/device/device_scan.cuh>
 #include "g3d_plasma.hpp"
+#include "k_external.cuh"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
 
@@ -346,7 +347,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double zm = z + double(hd * pz), zetam = zeta - 0.5 * hl;
     A E[3], B[3];
     const bool mid = c.Fmid && zeta == zn1;                       // the whole half-cell: the midpoint fields
-    if (F32 && mid && !LASER) {
+    if (F32 && mid && !LASER && !c.ext.any()) {
         if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy(g, ym), E, B);
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
@@ -356,6 +357,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
             c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
             for (int k = 0; k < 3; ++k) { Ed[k] += Ee[k]; Bd[k] += Be[k]; }
         }
+        if (c.ext.any()) add_external(c.ext, xm + c.sv->X0, ym + c.sv->Y0, zm, Bd);   // sim_stream.hpp:133
         for (int k = 0; k < 3; ++k) { E[k] = A(Ed[k]); B[k] = A(Bd[k]); }
     }
     A ux = px, uy = py, uz = pz;

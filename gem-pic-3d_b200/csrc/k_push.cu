@@ -58,6 +58,7 @@ PushArgs push_args(Ctx& c, double s1) {
     a.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
     a.vz_min = c.pl ? c.pl->cfg.vz_min : 0;            // slower beam particles stream in the plasma march
     a.freeze = c.P.freeze_bunch; a.self = c.P.self_fields;
+    a.ext = c.ext;
     return a;
 }
 void launch_push(Ctx& c, double s0, double s1) {

@@ -5,6 +5,7 @@
 // reference's F) or double (the exact fields of the gradient check).
 #pragma once
 #include "g3d_plasma.hpp"
+#include "k_external.cuh"
 
 namespace g3d {
 
@@ -15,6 +16,7 @@ struct PushArgs {
     LaserDev laser;
     double X0, Y0, zc, dz_push, push_phase, zhand, zmax, ylo, yhi, s1, vz_min, hmin;
     int freeze, self;
+    ExtDev ext;                           // external magnetic elements (none: nu = nm = 0)
 };
 
 struct St { double x, y, zeta, px, py, pz; };
@@ -83,6 +85,7 @@ __device__ __forceinline__ bool rhs(const PushArgs& c, const FT* __restrict__ Fp
     c.laser.field(Y.x + c.X0, z, z - (Y.zeta - c.zc), Ee, Be);
 #pragma unroll
     for (int k = 0; k < 3; ++k) { E[k] += Ee[k]; B[k] += Be[k]; }
+    if (c.ext.any()) add_external(c.ext, Y.x + c.X0, Y.y + c.Y0, z, B);
     const double ip = 1 / Y.pz;
     d.x = Y.px * ip; d.y = Y.py * ip; d.zeta = -gm * ip;
     d.px = qm * (g * E[0] + Y.py * B[2] - Y.pz * B[1]) * ip;
@@ -105,6 +108,7 @@ __device__ __forceinline__ double substep(const PushArgs& c, const St& Y, double
         const double lim = c.push_phase * Y.pz / (c.laser.kL * (hl > 1e-12 ? hl : 1e-12));
         if (lim < ds) ds = (s1 - z) / ceil((s1 - z) / lim);
     }
+    if (c.ext.any()) ds = external_step(c.ext, z, ds);       // the external elements resolved
     return ds;
 }
 __device__ __forceinline__ St axpy(const St& a, double h, const St& b) {
@@ -117,13 +121,16 @@ __device__ __forceinline__ St axpy(const St& a, double h, const St& b) {
 template <class FT>
 __device__ __forceinline__ bool rk4_step(const PushArgs& c, const FT* __restrict__ Fp, St& Y, double z, double ds, double qm) {
     St k, acc;
-    bool ok = rhs(c, Fp, Y, z, qm, k);
+    // with external elements the first and last stages take the field just inside the sub-step, which ends on the
+    // elements' breakpoints, where the field or its derivative jumps
+    const double e = c.ext.any() ? 1e-9 * ds : 0.0;
+    bool ok = rhs(c, Fp, Y, z + e, qm, k);
     acc = k;
     ok = ok && rhs(c, Fp, axpy(Y, 0.5 * ds, k), z + 0.5 * ds, qm, k);
     acc = axpy(acc, 2.0, k);
     ok = ok && rhs(c, Fp, axpy(Y, 0.5 * ds, k), z + 0.5 * ds, qm, k);
     acc = axpy(acc, 2.0, k);
-    ok = ok && rhs(c, Fp, axpy(Y, ds, k), z + ds, qm, k);
+    ok = ok && rhs(c, Fp, axpy(Y, ds, k), z + ds - e, qm, k);
     if (!ok) return false;
     acc = axpy(acc, 1.0, k);
     const double w = ds / 6;

@@ -78,7 +78,18 @@ class GridLaser(C.Structure):
                 ("circular", C.c_int32), ("helicity", C.c_int32)]
 
 
+class Undulator(C.Structure):
+    _fields_ = [("helical", C.c_int32), ("focusing", C.c_int32), ("ku", C.c_double), ("B0", C.c_double), ("z0", C.c_double),
+                ("z1", C.c_double), ("ramp", C.c_double), ("nk", C.c_int32), ("koff", C.c_int32), ("dzk", C.c_double)]
+
+
+class Magnet(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("z0", C.c_double), ("z1", C.c_double), ("g", C.c_double),
+                ("R", C.c_double), ("ramp", C.c_double), ("dsmax", C.c_double)]
+
+
 assert C.sizeof(Plasma) == 120 and C.sizeof(Ion) == 48 and C.sizeof(GridLaser) == 72
+assert C.sizeof(Undulator) == 64 and C.sizeof(Magnet) == 56
 assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 120 and C.sizeof(Status) == 80
 
 _P = C.c_void_p
@@ -101,6 +112,7 @@ SIGNATURES = [
                                 C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_D), C.POINTER(_D)]),
     ("g3d_set_plasma", _I, [_P, C.POINTER(Plasma), C.POINTER(Ion), _I32]),
     ("g3d_add_grid_laser", _I, [_P, C.POINTER(GridLaser)]),
+    ("g3d_set_external", _I, [_P, C.POINTER(Undulator), _I32, C.POINTER(Magnet), _I32, C.POINTER(_D), _I32]),
     ("g3d_march_plasma", _I, [_P, _D, _D]),
     ("g3d_get_streaming", _I, [_P, _P, _I64, C.POINTER(_I64)]),
     ("g3d_init", _I, [_P]),

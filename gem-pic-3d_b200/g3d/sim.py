@@ -65,9 +65,26 @@ class Simulation:
             self._c(self.lib.g3d_set_plasma(self.ctx, C.byref(P), ions, nions))
         for L in cfg.glaser_structs():
             self._c(self.lib.g3d_add_grid_laser(self.ctx, C.byref(L)))
+        if getattr(cfg, "undulators", None) or getattr(cfg, "magnets", None):
+            self.set_external(cfg.undulators, cfg.magnets, getattr(cfg, "ktab", None))
         self.N, self.nx, self.ny = cfg.nzeta, cfg.nx, cfg.ny
         self.nk = cfg.nx * cfg.ny
         self.ns = cfg.nzeta
+
+    def set_external(self, undulators=(), magnets=(), ktab=None):
+        """External magnetic elements (dicts of the g3d_undulator / g3d_magnet fields, code units; ktab: the taper
+        table of the undulators); none removes them (reference src/external.hpp)."""
+        U = (abi.Undulator * max(1, len(undulators)))()
+        for k, u in enumerate(undulators):
+            for f, v in u.items():
+                setattr(U[k], f, v)
+        M = (abi.Magnet * max(1, len(magnets)))()
+        for k, m in enumerate(magnets):
+            for f, v in m.items():
+                setattr(M[k], f, v)
+        kt = np.ascontiguousarray(ktab if ktab is not None else [], dtype=np.float64)
+        self._c(self.lib.g3d_set_external(self.ctx, U, len(undulators), M, len(magnets),
+                                          kt.ctypes.data_as(C.POINTER(C.c_double)), len(kt)))
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -4,8 +4,8 @@
 //
 //   g3dshim::Setup      the g3d structs of a run, built from a reference Config by setup_from (params_from.cpp),
 //                       which maps every deck key the march uses and rejects, with std::runtime_error, the ones
-//                       the library does not run (external elements, bunch files and profile functions, laser files,
-//                       density functions, beamlet noise)
+//                       the library does not run (chicanes, bunch files and profile functions, laser files, density
+//                       functions, beamlet noise)
 //   g3dshim::Simulation the reference's method names (init, step, finished, solve_fields, currents, march, push,
 //                       shift_window, host_particles, set_particles, write/read_checkpoint, diagnostics sums), each
 //                       a call of the C-ABI whose non-zero status becomes a std::runtime_error with the library's
@@ -32,6 +32,9 @@ struct Setup {
     std::vector<g3d_ion> ions;
     std::vector<std::vector<double>> ion_ip;
     std::vector<g3d_grid_laser> lasers;
+    std::vector<g3d_undulator> undulators;
+    std::vector<g3d_magnet> magnets;
+    std::vector<double> ktab;
     int precision = G3D_PREC_FP64;
 };
 
@@ -60,6 +63,10 @@ public:
                 check(g3d_set_plasma(ctx_, &p, ions.data(), int32_t(ions.size())), ctx_, "g3d_set_plasma");
             }
             for (const g3d_grid_laser& L : s_.lasers) check(g3d_add_grid_laser(ctx_, &L), ctx_, "g3d_add_grid_laser");
+            if (!s_.undulators.empty() || !s_.magnets.empty())
+                check(g3d_set_external(ctx_, s_.undulators.data(), int32_t(s_.undulators.size()), s_.magnets.data(),
+                                       int32_t(s_.magnets.size()), s_.ktab.data(), int32_t(s_.ktab.size())),
+                      ctx_, "g3d_set_external");
         } catch (...) {
             g3d_destroy(ctx_);
             throw;

@@ -45,9 +45,11 @@ Setup setup_from(const Config& c) {
     p.zeta_center = c.zeta_center;
     p.freeze_bunch = c.freeze_bunch; p.start_relax = c.start_relax; p.box_mean = c.box_mean;
     p.precision = G3D_FP64;
-    // external elements: not on the march path of this library
-    if (!c.undulators.empty()) refuse("undulator blocks");
-    if (!c.magnets.empty()) refuse("quadrupole, plasma_lens or solenoid blocks");
+    // external elements (src/external.hpp: the same fields, code units) and their taper table
+    for (const Undulator& U : c.undulators)
+        s.undulators.push_back(g3d_undulator{U.helical, U.focusing, U.ku, U.B0, U.z0, U.z1, U.ramp, U.nk, U.koff, U.dzk});
+    for (const Magnet& M : c.magnets) s.magnets.push_back(g3d_magnet{M.kind, 0, M.z0, M.z1, M.g, M.R, M.ramp, M.dsmax});
+    s.ktab = c.ktab;
     if (!c.chicanes.empty()) refuse("chicane blocks");
     // bunch blocks: the built-in Gaussian / flat-top profiles with random shot noise
     for (const Config::Bunch& B : c.bunch_list()) {

@@ -133,6 +133,24 @@ typedef struct g3d_grid_laser {
     int32_t circular, helicity;
 } g3d_grid_laser;
 
+/* External magnetic elements acting on the particles (reference struct Undulator / Magnet, src/external.hpp:15-30; the
+ * deck blocks undulator, quadrupole, plasma_lens, solenoid, as Config::parse_external builds them,
+ * src/sim_external.cpp:5-85). Code units: B in m omega0 / e, lengths 1/k0, z the lab position. Undulator: B0 = K k_u,
+ * linear ramps of `ramp` at both ends between z0 and z1; planar (B_y, with natural focusing B_y cosh, B_z sinh) or
+ * helical (B_x, B_y); nk > 0: a taper, B0(z0 + j dzk) = ktab[koff + j]. Magnet kind 0 quadrupole (gradient g),
+ * 1 plasma lens (gradient g inside radius R), 2 solenoid (field g, linear fringes of `ramp`); dsmax the longest push
+ * sub-step inside it. */
+typedef struct g3d_undulator {
+    int32_t helical, focusing;
+    double ku, B0, z0, z1, ramp;
+    int32_t nk, koff;
+    double dzk;
+} g3d_undulator;
+typedef struct g3d_magnet {
+    int32_t kind, reserved;
+    double z0, z1, g, R, ramp, dsmax;
+} g3d_magnet;
+
 /* Scalars of the run (reference members s, istep, X0, Y0, beta_b, gm2_b, np, lost_total). */
 typedef struct g3d_status {
     double s, X0, Y0, beta_b, gm2_b, field_energy;
@@ -186,6 +204,12 @@ int g3d_sample_bunches(const g3d_grid* grid, const g3d_params* params, const g3d
 int g3d_set_plasma(struct g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions);
 /* A grid laser, added to R by g3d_init (Simulation::add_grid_lasers, src/sim_fields.cpp:321-374). */
 int g3d_add_grid_laser(struct g3d_ctx* ctx, const g3d_grid_laser* laser);
+/* The external elements of the run (replaces any set before; nu = nm = 0 removes them). Their fields are added to the
+ * gathered fields of the beam push and of the streaming push at the lab position, and the beam push's sub-steps end on
+ * their breakpoints (reference add_external / external_step, src/external.hpp:40-92, used at
+ * src/sim_kernels.hpp:88 and :126-133 and src/sim_stream.hpp:133). The adjoint march rejects a run with them. */
+int g3d_set_external(struct g3d_ctx* ctx, const g3d_undulator* undulators, int32_t nu, const g3d_magnet* magnets,
+                     int32_t nm, const double* ktab, int32_t nktab);
 
 /* ------------------------------------------------------------------ the march path */
 int g3d_init(struct g3d_ctx* ctx);                  /* Simulation::init, sim_setup.cpp:178-197 (after loading) */

@@ -7,7 +7,7 @@ import subprocess
 
 import pytest
 
-from test_shim_gpu import L, SHIM, lwfa_deck, wake_deck
+from test_shim_gpu import L, SHIM, external_deck, lwfa_deck, wake_deck
 
 needs_shim = pytest.mark.skipif(not os.path.exists(SHIM), reason="g3d_run not built (it needs the reference's sources)")
 
@@ -39,8 +39,15 @@ def test_what_the_library_does_not_run_is_refused(extra, key, tmp_path):
 
 
 @needs_shim
-def test_external_elements_are_refused(tmp_path):
-    text = wake_deck(tmp_path / "out") + "solenoid {\n  z_start = 1 um\n  z_end = 2 um\n  B = 1 T\n}\n"
+def test_external_elements_map(tmp_path):
+    r = check(external_deck(tmp_path / "out"), tmp_path)
+    assert r.returncode == 0, r.stderr
+    for name in ("undulator", "quadrupole", "plasma lens", "solenoid"):
+        assert name in r.stdout, name
+
+
+@needs_shim
+def test_chicanes_are_refused(tmp_path):
+    text = wake_deck(tmp_path / "out") + "chicane {\n  z = 1 um\n  r56 = 0.1 um\n  gamma = 1000\n}\n"
     r = check(text, tmp_path)
-    assert r.returncode == 2, (r.stdout[-300:], r.stderr)
-    assert "libg3d does not run" in r.stderr or "solenoid" in r.stderr, r.stderr
+    assert r.returncode == 2 and "libg3d does not run" in r.stderr and "chicane" in r.stderr, r.stderr

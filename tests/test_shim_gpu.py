@@ -117,6 +117,37 @@ output {{
 """
 
 
+def external_deck(out):
+    """The vacuum wake with a lower-gamma bunch through an undulator, a quadrupole, a plasma lens and a solenoid
+    (reference src/external.hpp) along the run's 2 um of z."""
+    text = wake_deck(out).replace("  gamma = 1000\n", "  gamma = 50\n", 1)
+    return text + """undulator {
+  period = 1.5 um
+  K = 0.3
+  z_start = 0.05 um
+  periods = 1
+  ramp_periods = 0
+}
+quadrupole {
+  z_start = 0.3 um
+  length = 0.5 um
+  gradient = 2e5 T/m
+}
+plasma_lens {
+  z_start = 0.85 um
+  length = 0.4 um
+  gradient = 3e5 T/m
+  radius = 0.1 um
+}
+solenoid {
+  z_start = 1.3 um
+  length = 0.5 um
+  field = 3e3 T
+  ramp = 0.1 um
+}
+"""
+
+
 def run(cmd, cwd):
     return subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
 
@@ -193,3 +224,24 @@ def test_laser_wakefield_deck_matches_the_reference_cli(tmp_path):
     a, b = diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt")
     assert a.shape[0] >= 3
     diag_close(a, b, "lwfa")
+
+
+@needs_both
+def test_external_elements_deck_matches_the_reference_cli(tmp_path):
+    """Undulator, quadrupole, plasma lens and solenoid fields in the push and its sub-steps ending on their
+    breakpoints: the checkpoint after step 3 and diag.txt as for the plain wake."""
+    ref_dir, our_dir = tmp_path / "ref", tmp_path / "g3d"
+    for d, exe in ((ref_dir, REF_CLI), (our_dir, SHIM)):
+        d.mkdir()
+        deck = d / "ext.deck"
+        deck.write_text(external_deck(d / "out"))
+        r = run([exe, str(deck)], d)
+        assert r.returncode == 0, (exe, r.stdout[-2000:], r.stderr[-2000:])
+    a = read_checkpoint(our_dir / "out" / "checkpoint_000003_r0000.bin")
+    b = read_checkpoint(ref_dir / "out" / "checkpoint_000003_r0000.bin")
+    assert_state({k: a[k] for k in FIELDS}, {k: b[k] for k in FIELDS}, FIELDS, 1e-10, tag="checkpoint")
+    p, q = a["particles"], b["particles"]
+    assert len(p) == len(q)
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        assert rel_l2(p[f], q[f]) <= 1e-10, f
+    diag_close(diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt"), "external")
