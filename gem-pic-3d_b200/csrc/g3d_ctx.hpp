@@ -212,6 +212,7 @@ struct Ctx {
     DevBuf<g3d_magnet> mag;
     DevBuf<double> ktab;
     ExtDev ext{0, 0, nullptr, nullptr, nullptr};
+    std::vector<g3d_chicane> chicanes;           // thin chicanes (g3d_set_chicanes)
 
     Ctx();
     ~Ctx();

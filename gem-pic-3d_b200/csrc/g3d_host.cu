@@ -704,6 +704,59 @@ static void relax_start_field(Ctx& c) {
     launch_axpy_c(c, c.Rx.p, dxr, 1.0, n);
     launch_axpy_c(c, c.Ry.p, dyr, 1.0, n);
 }
+// The thin chicanes passed in the step s0 -> s1 (reference Simulation::apply_chicanes, src/sim_external.cpp:108-151):
+// every live beam particle moves in zeta by r56 (gamma / gamma_ref - 1) - delay, those leaving the window are lost;
+// R keeps its radiation and trades the beam's co-moving field of the old positions for that of the new ones (each
+// made as at the start: per bunch block, relaxed, vacuum); E_z, B_z, L, the real fields and j0 follow as at the start.
+static void apply_chicanes(Ctx& c, double s0, double s1) {
+    for (const g3d_chicane& ch : c.chicanes) {
+        if (!(ch.z > s0 && ch.z <= s1)) continue;
+        const size_t n = size_t(c.ns) * c.nkh;
+        DevBuf<cpx> keep_x, keep_y, old_x, old_y;
+        auto comoving_into = [&](DevBuf<cpx>& rx, DevBuf<cpx>& ry) {
+            c.starting_ = true;                          // vacuum at the chicane: no k_perp = 0 current
+            if (c.nbunch > 1) comoving_fields_per_bunch(c);
+            else { currents(c); comoving_field(c); }
+            if (c.P.start_relax) relax_start_field(c);
+            c.starting_ = false;
+            rx.alloc(n, c.stream); ry.alloc(n, c.stream);
+            launch_copy_c(c, rx.p, c.Rx.p, n);
+            launch_copy_c(c, ry.p, c.Ry.p, n);
+        };
+        if (c.P.self_fields) {
+            keep_x.alloc(n, c.stream); keep_y.alloc(n, c.stream);
+            launch_copy_c(c, keep_x.p, c.Rx.p, n);
+            launch_copy_c(c, keep_y.p, c.Ry.p, n);
+            comoving_into(old_x, old_y);
+        }
+        const std::vector<g3d_particle> all = get_particles(c);
+        std::vector<g3d_particle> kept;
+        kept.reserve(all.size());
+        const double zmax = c.zeta[size_t(c.N) - 1];
+        for (g3d_particle p : all) {
+            if (p.alive != 1) continue;
+            const double g = std::sqrt(1 + p.px * p.px + p.py * p.py + p.pz * p.pz);
+            p.zeta += ch.r56 * (g / ch.gamma_ref - 1) - ch.delay;
+            if (p.zeta < 0 || p.zeta >= zmax) { ++c.lost_total; continue; }
+            kept.push_back(p);
+        }
+        set_particles(c, kept.data(), long(kept.size()));
+        if (!c.P.self_fields) continue;
+        DevBuf<cpx> new_x, new_y;
+        comoving_into(new_x, new_y);
+        // R = (R before + new) - old, in that order
+        launch_axpy_c(c, keep_x.p, new_x.p, 1.0, n);
+        launch_axpy_c(c, keep_x.p, old_x.p, -1.0, n);
+        launch_axpy_c(c, keep_y.p, new_y.p, 1.0, n);
+        launch_axpy_c(c, keep_y.p, old_y.p, -1.0, n);
+        launch_copy_c(c, c.Rx.p, keep_x.p, n);
+        launch_copy_c(c, c.Ry.p, keep_y.p, n);
+        march(c, 0.0);                                   // E_z, B_z, L of R, as at the start
+        sponge_and_real_fields(c);
+        j0_from_jk(c);
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+    }
+}
 static void shift_window(Ctx& c, int nxs, int nys) {
     if (c.Fd.p) throw Error(G3D_ERR_STATE, "exact fields need a fixed window");
     materialize_jk(c);
@@ -764,6 +817,7 @@ static void step(Ctx& c, bool sync) {
         sponge_and_real_fields(c);
         j0_from_jk(c);
     } else if (c.P.self_fields) solve_fields(c, 0.5 * c.P.dz);
+    if (!c.chicanes.empty()) apply_chicanes(c, c.s - c.P.dz, c.s);
     window_shift_post(c);
     if (sync) G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -1022,7 +1076,8 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     if (c.laser.on) throw Error(G3D_ERR_ARG, "the adjoint march differentiates grid lasers, not the analytic laser");
     if (!c.P.self_fields || c.P.freeze_bunch) throw Error(G3D_ERR_ARG, "the adjoint march needs self fields and a free bunch");
     if (!c.fields_ready || c.istep != 0) throw Error(G3D_ERR_STATE, "the adjoint march starts right after g3d_init");
-    if (c.ext.any()) throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate external elements");
+    if (c.ext.any() || !c.chicanes.empty())
+        throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate external elements or chicanes");
     if (grad_modes && !c.lmode.p) throw Error(G3D_ERR_STATE, "set the laser mode coefficients (g3d_set_laser_modes) before g3d_init");
     const long np = c.np;
     const size_t Fn = c.F.n, ns = size_t(c.ns), nkh = size_t(c.nkh), nk = size_t(c.nk);
@@ -1352,6 +1407,14 @@ int g3d_set_external(g3d_ctx* ctx, const g3d_undulator* u, int32_t nu, const g3d
         c.ktab.upload(std::vector<double>(kt, kt + nkt), c.stream);
         G3D_CUDA(cudaStreamSynchronize(c.stream));
         c.ext = g3d::ExtDev{nu, nm, c.und.p, c.mag.p, c.ktab.p};
+    });
+}
+int g3d_set_chicanes(g3d_ctx* ctx, const g3d_chicane* ch, int32_t n) {
+    return guarded(ctx, [&] {
+        if (n < 0 || (n && !ch)) throw Error(G3D_ERR_ARG, "g3d_set_chicanes: bad chicane array");
+        for (int k = 0; k < n; ++k)
+            if (!(ch[k].gamma_ref > 1)) throw Error(G3D_ERR_ARG, "g3d_set_chicanes: the reference gamma must be > 1");
+        ctx->c.chicanes.assign(ch, ch + n);
     });
 }
 int g3d_march_plasma(g3d_ctx* ctx, double s0, double s1) {

@@ -89,7 +89,11 @@ class Magnet(C.Structure):
 
 
 assert C.sizeof(Plasma) == 120 and C.sizeof(Ion) == 48 and C.sizeof(GridLaser) == 72
-assert C.sizeof(Undulator) == 64 and C.sizeof(Magnet) == 56
+class Chicane(C.Structure):
+    _fields_ = [("z", C.c_double), ("r56", C.c_double), ("delay", C.c_double), ("gamma_ref", C.c_double)]
+
+
+assert C.sizeof(Undulator) == 64 and C.sizeof(Magnet) == 56 and C.sizeof(Chicane) == 32
 assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 120 and C.sizeof(Status) == 80
 
 _P = C.c_void_p
@@ -113,6 +117,7 @@ SIGNATURES = [
     ("g3d_set_plasma", _I, [_P, C.POINTER(Plasma), C.POINTER(Ion), _I32]),
     ("g3d_add_grid_laser", _I, [_P, C.POINTER(GridLaser)]),
     ("g3d_set_external", _I, [_P, C.POINTER(Undulator), _I32, C.POINTER(Magnet), _I32, C.POINTER(_D), _I32]),
+    ("g3d_set_chicanes", _I, [_P, C.POINTER(Chicane), _I32]),
     ("g3d_march_plasma", _I, [_P, _D, _D]),
     ("g3d_get_streaming", _I, [_P, _P, _I64, C.POINTER(_I64)]),
     ("g3d_init", _I, [_P]),

@@ -86,6 +86,14 @@ class Simulation:
         self._c(self.lib.g3d_set_external(self.ctx, U, len(undulators), M, len(magnets),
                                           kt.ctypes.data_as(C.POINTER(C.c_double)), len(kt)))
 
+    def set_chicanes(self, chicanes=()):
+        """Thin chicanes: dicts of z, r56, delay, gamma_ref (code units); none removes them."""
+        A = (abi.Chicane * max(1, len(chicanes)))()
+        for k, ch in enumerate(chicanes):
+            for f, v in ch.items():
+                setattr(A[k], f, v)
+        self._c(self.lib.g3d_set_chicanes(self.ctx, A, len(chicanes)))
+
     def close(self):
         if getattr(self, "ctx", None):
             self.lib.g3d_destroy(self.ctx)

@@ -4,8 +4,8 @@
 //
 //   g3dshim::Setup      the g3d structs of a run, built from a reference Config by setup_from (params_from.cpp),
 //                       which maps every deck key the march uses and rejects, with std::runtime_error, the ones
-//                       the library does not run (chicanes, bunch files and profile functions, laser files, density
-//                       functions, beamlet noise)
+//                       the library does not run (bunch files and profile functions, laser files, density functions,
+//                       beamlet noise)
 //   g3dshim::Simulation the reference's method names (init, step, finished, solve_fields, currents, march, push,
 //                       shift_window, host_particles, set_particles, write/read_checkpoint, diagnostics sums), each
 //                       a call of the C-ABI whose non-zero status becomes a std::runtime_error with the library's
@@ -35,6 +35,7 @@ struct Setup {
     std::vector<g3d_undulator> undulators;
     std::vector<g3d_magnet> magnets;
     std::vector<double> ktab;
+    std::vector<g3d_chicane> chicanes;
     int precision = G3D_PREC_FP64;
 };
 
@@ -67,6 +68,8 @@ public:
                 check(g3d_set_external(ctx_, s_.undulators.data(), int32_t(s_.undulators.size()), s_.magnets.data(),
                                        int32_t(s_.magnets.size()), s_.ktab.data(), int32_t(s_.ktab.size())),
                       ctx_, "g3d_set_external");
+            if (!s_.chicanes.empty())
+                check(g3d_set_chicanes(ctx_, s_.chicanes.data(), int32_t(s_.chicanes.size())), ctx_, "g3d_set_chicanes");
         } catch (...) {
             g3d_destroy(ctx_);
             throw;

@@ -50,7 +50,7 @@ Setup setup_from(const Config& c) {
         s.undulators.push_back(g3d_undulator{U.helical, U.focusing, U.ku, U.B0, U.z0, U.z1, U.ramp, U.nk, U.koff, U.dzk});
     for (const Magnet& M : c.magnets) s.magnets.push_back(g3d_magnet{M.kind, 0, M.z0, M.z1, M.g, M.R, M.ramp, M.dsmax});
     s.ktab = c.ktab;
-    if (!c.chicanes.empty()) refuse("chicane blocks");
+    for (const Config::Chicane& ch : c.chicanes) s.chicanes.push_back(g3d_chicane{ch.z, ch.r56, ch.delay, ch.gamma_ref});
     // bunch blocks: the built-in Gaussian / flat-top profiles with random shot noise
     for (const Config::Bunch& B : c.bunch_list()) {
         if (B.from_file) refuse("bunch.file (" + B.name + ")");

@@ -151,6 +151,12 @@ typedef struct g3d_magnet {
     double z0, z1, g, R, ramp, dsmax;
 } g3d_magnet;
 
+/* A thin chicane at the lab position z (reference Config::Chicane, src/sim.hpp; deck block chicane, code units): every
+ * beam particle moves in zeta by r56 (gamma / gamma_ref - 1) - delay. */
+typedef struct g3d_chicane {
+    double z, r56, delay, gamma_ref;
+} g3d_chicane;
+
 /* Scalars of the run (reference members s, istep, X0, Y0, beta_b, gm2_b, np, lost_total). */
 typedef struct g3d_status {
     double s, X0, Y0, beta_b, gm2_b, field_energy;
@@ -210,6 +216,12 @@ int g3d_add_grid_laser(struct g3d_ctx* ctx, const g3d_grid_laser* laser);
  * src/sim_kernels.hpp:88 and :126-133 and src/sim_stream.hpp:133). The adjoint march rejects a run with them. */
 int g3d_set_external(struct g3d_ctx* ctx, const g3d_undulator* undulators, int32_t nu, const g3d_magnet* magnets,
                      int32_t nm, const double* ktab, int32_t nktab);
+/* The thin chicanes of the run (replaces any set before; n = 0 removes them). A step that passes one (s0 < z <= s1)
+ * ends with it (reference Simulation::apply_chicanes, src/sim_external.cpp:108-151): the beam's co-moving field of
+ * the old positions is taken out of R and that of the new positions put in (vacuum at the chicane; the radiation in
+ * the window stays), particles leaving the window are lost, and E_z, B_z, L and the real fields follow from R as at
+ * the start. */
+int g3d_set_chicanes(struct g3d_ctx* ctx, const g3d_chicane* chicanes, int32_t n);
 
 /* ------------------------------------------------------------------ the march path */
 int g3d_init(struct g3d_ctx* ctx);                  /* Simulation::init, sim_setup.cpp:178-197 (after loading) */

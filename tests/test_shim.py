@@ -7,7 +7,7 @@ import subprocess
 
 import pytest
 
-from test_shim_gpu import L, SHIM, external_deck, lwfa_deck, wake_deck
+from test_shim_gpu import L, SHIM, chicane_deck, external_deck, lwfa_deck, wake_deck
 
 needs_shim = pytest.mark.skipif(not os.path.exists(SHIM), reason="g3d_run not built (it needs the reference's sources)")
 
@@ -47,7 +47,6 @@ def test_external_elements_map(tmp_path):
 
 
 @needs_shim
-def test_chicanes_are_refused(tmp_path):
-    text = wake_deck(tmp_path / "out") + "chicane {\n  z = 1 um\n  r56 = 0.1 um\n  gamma = 1000\n}\n"
-    r = check(text, tmp_path)
-    assert r.returncode == 2 and "libg3d does not run" in r.stderr and "chicane" in r.stderr, r.stderr
+def test_chicanes_map(tmp_path):
+    r = check(chicane_deck(tmp_path / "out"), tmp_path)
+    assert r.returncode == 0 and "chicane at z" in r.stdout, r.stderr

@@ -148,6 +148,18 @@ solenoid {
 """
 
 
+def chicane_deck(out):
+    """The two-bunch wake with an energy spread through a thin chicane inside the second step."""
+    text = wake_deck(out).replace("  gamma = 1000\n", "  gamma = 1000\n  energy_spread = 0.01\n", 1)
+    return text + f"""chicane {{
+  z = {L(7)}
+  r56 = {L(200)}
+  delay = {L(2)}
+  gamma = 990
+}}
+"""
+
+
 def run(cmd, cwd):
     return subprocess.run(cmd, cwd=cwd, capture_output=True, text=True, timeout=600)
 
@@ -245,3 +257,24 @@ def test_external_elements_deck_matches_the_reference_cli(tmp_path):
     for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
         assert rel_l2(p[f], q[f]) <= 1e-10, f
     diag_close(diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt"), "external")
+
+
+@needs_both
+def test_chicane_deck_matches_the_reference_cli(tmp_path):
+    """A thin chicane passed in step 2: the beam moved in zeta by its energy, its co-moving field traded, E_z, B_z, L
+    and the real fields rebuilt; the checkpoint after step 3 and diag.txt as for the plain wake."""
+    ref_dir, our_dir = tmp_path / "ref", tmp_path / "g3d"
+    for d, exe in ((ref_dir, REF_CLI), (our_dir, SHIM)):
+        d.mkdir()
+        deck = d / "chicane.deck"
+        deck.write_text(chicane_deck(d / "out"))
+        r = run([exe, str(deck)], d)
+        assert r.returncode == 0, (exe, r.stdout[-2000:], r.stderr[-2000:])
+    a = read_checkpoint(our_dir / "out" / "checkpoint_000003_r0000.bin")
+    b = read_checkpoint(ref_dir / "out" / "checkpoint_000003_r0000.bin")
+    assert_state({k: a[k] for k in FIELDS}, {k: b[k] for k in FIELDS}, FIELDS, 1e-10, tag="checkpoint")
+    p, q = a["particles"], b["particles"]
+    assert len(p) == len(q)
+    for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
+        assert rel_l2(p[f], q[f]) <= 1e-10, f
+    diag_close(diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt"), "chicane")
