@@ -529,26 +529,52 @@ static void sample_bunches(const g3d_grid& G, const g3d_params& P, const g3d_bun
         const double Ne = B.charge_C / e_SI;
         const double W = (B.nmacro > 0 ? Ne / double(B.nmacro) : 0) / (nc * std::pow(Lu, 3));
         const double p0 = std::sqrt(B.gamma * B.gamma - 1);
+        // Fawley's beamlets (shot_noise = fawley): groups of M particles sharing a draw
+        const int M = B.beamlet > 1 ? B.beamlet : 1;
+        if (M > 1 && (M < 3 || B.nmacro % M || !(B.noise_lambda > 0)))
+            throw Error(G3D_ERR_ARG, "Fawley shot noise needs beamlet >= 3 dividing the macroparticles and noise_lambda > 0");
+        const long groups = B.nmacro / M;
+        const double Ne_group = groups > 0 ? Ne / double(groups) : 0;
+        std::vector<double> dz(static_cast<size_t>(M), 0.0), dth(static_cast<size_t>(M));
         mine.reserve(mine.size() + size_t(B.nmacro));
-        for (long ib = 0; ib < B.nmacro; ++ib) {
+        for (long ib = 0; ib < groups; ++ib) {
             const double x = B.x0 + B.sigx * Gs(rng);
             const double y = B.y0 + B.sigy * Gs(rng);
             const double z = B.length > 0 ? B.length * U(rng) : B.sigz * Gs(rng);
             const double px = B.sigx > 0 ? B.emitx / B.sigx * Gs(rng) : 0;
             const double py = B.sigy > 0 ? B.emity / B.sigy * Gs(rng) : 0;
             const double pz = p0 * (1 + B.espread * Gs(rng));
-            const double g = std::sqrt(1 + px * px + py * py + pz * pz);
-            const double vx = px / g, vy = py / g, vz = pz / g;
-            const double zz = z;
-            g3d_particle p{};
-            p.x = x - vx * zz / vz + 0.5 * G.Lx; p.y = y - vy * zz / vz + yoff;
-            p.zeta = B.zeta_center + zz / vz;
-            p.px = px; p.py = py; p.pz = pz; p.w = W; p.alive = 1;
-            p.q = B.q; p.qm = B.q; p.sp = -kb; p.z = 0;
-            int hc; double f;
-            zax.locate(p.zeta, hc, f);
-            if (p.zeta < 0 || hc > N - 2 || p.y < ylo || p.y > yhi) { ++lost; continue; }
-            mine.push_back(p);
+            if (M > 1) {
+                // M particles evenly spaced in the phase theta = 2 pi z / noise_lambda from a random theta0, each
+                // displaced by sum_h Re(c_h e^{-i h theta_j}), c_h = -2 i b_h / h with b_h the bunching factor of
+                // Ne_group random electrons at harmonic h (complex Gaussian of variance 1 / Ne_group), h < M / 2
+                using cplx = std::complex<double>;
+                const cplx I(0, 1);
+                const double th0 = 2 * M_PI * std::uniform_real_distribution<double>(0, 1)(rng);
+                std::fill(dth.begin(), dth.end(), 0.0);
+                for (int hh = 1; 2 * hh < M; ++hh) {
+                    const double gi = Gs(rng);               // the imaginary part is drawn first (the reference's order)
+                    const double gr = Gs(rng);
+                    const cplx bh = std::sqrt(0.5 / Ne_group) * cplx(gr, gi);
+                    const cplx ch = -2.0 * I * bh / double(hh);
+                    for (int j = 0; j < M; ++j) dth[size_t(j)] += std::real(ch * std::exp(-I * double(hh) * (th0 + 2 * M_PI * j / M)));
+                }
+                for (int j = 0; j < M; ++j) dz[size_t(j)] = B.noise_lambda * ((th0 + 2 * M_PI * j / M + dth[size_t(j)]) / (2 * M_PI) - 0.5);
+            }
+            for (int j = 0; j < M; ++j) {
+                const double g = std::sqrt(1 + px * px + py * py + pz * pz);
+                const double vx = px / g, vy = py / g, vz = pz / g;
+                const double zz = z + dz[size_t(j)];
+                g3d_particle p{};
+                p.x = x - vx * zz / vz + 0.5 * G.Lx; p.y = y - vy * zz / vz + yoff;
+                p.zeta = B.zeta_center + zz / vz;
+                p.px = px; p.py = py; p.pz = pz; p.w = W; p.alive = 1;
+                p.q = B.q; p.qm = B.q; p.sp = -kb; p.z = 0;
+                int hc; double f;
+                zax.locate(p.zeta, hc, f);
+                if (p.zeta < 0 || hc > N - 2 || p.y < ylo || p.y > yhi) { ++lost; continue; }
+                mine.push_back(p);
+            }
         }
     }
     X0 = -0.5 * G.Lx; Y0 = -yoff;

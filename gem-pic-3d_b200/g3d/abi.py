@@ -48,7 +48,8 @@ class Bunch(C.Structure):
     _fields_ = [("charge_C", C.c_double), ("gamma", C.c_double), ("sigx", C.c_double), ("sigy", C.c_double),
                 ("sigz", C.c_double), ("length", C.c_double), ("emitx", C.c_double), ("emity", C.c_double),
                 ("espread", C.c_double), ("zeta_center", C.c_double), ("x0", C.c_double), ("y0", C.c_double),
-                ("q", C.c_double), ("nmacro", C.c_int64), ("seed", C.c_uint64)]
+                ("q", C.c_double), ("nmacro", C.c_int64), ("seed", C.c_uint64), ("beamlet", C.c_int32),
+                ("reserved", C.c_int32), ("noise_lambda", C.c_double)]
 
 
 class Status(C.Structure):
@@ -94,7 +95,7 @@ class Chicane(C.Structure):
 
 
 assert C.sizeof(Undulator) == 64 and C.sizeof(Magnet) == 56 and C.sizeof(Chicane) == 32
-assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 120 and C.sizeof(Status) == 80
+assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 136 and C.sizeof(Status) == 80
 
 _P = C.c_void_p
 _D = C.c_double

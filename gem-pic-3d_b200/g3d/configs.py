@@ -168,7 +168,7 @@ def ion_species(symbol, Z0, atoms, ionization=False, mobile=True, Zmax=None):
 
 def default_bunch():
     return dict(charge_C=0.0, gamma=2.0, sigx=1.0, sigy=1.0, sigz=1.0, length=0.0, emitx=0.0, emity=0.0,
-                espread=0.0, zeta_center=0.0, x0=0.0, y0=0.0, q=-1.0, nmacro=0, seed=1)
+                espread=0.0, zeta_center=0.0, x0=0.0, y0=0.0, q=-1.0, nmacro=0, seed=1, beamlet=0, noise_lambda=0.0)
 
 
 def config1(nx=64, ny=64, nzeta=256, nmacro=262144, steps=10):

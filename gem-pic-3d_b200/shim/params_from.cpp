@@ -56,11 +56,12 @@ Setup setup_from(const Config& c) {
         if (B.from_file) refuse("bunch.file (" + B.name + ")");
         if (!B.profile_z.empty() || !B.gamma_fn.empty() || !B.profile_r.empty() || !B.ux_fn.empty() || !B.uy_fn.empty())
             refuse("bunch profile functions (" + B.name + ")");
-        if (B.noise != "random") refuse("bunch.shot_noise = " + B.noise + " (" + B.name + ")");
+        if (B.noise != "random" && B.noise != "fawley") refuse("bunch.shot_noise = " + B.noise + " (" + B.name + ")");
         g3d_bunch b{};
         b.charge_C = B.charge; b.gamma = B.gamma; b.sigx = B.sigx; b.sigy = B.sigy; b.sigz = B.sigz; b.length = B.length;
         b.emitx = B.emitx; b.emity = B.emity; b.espread = B.espread; b.zeta_center = B.zeta_center;
         b.x0 = B.x0; b.y0 = B.y0; b.q = B.q; b.nmacro = B.nmacro; b.seed = B.seed;
+        if (B.noise == "fawley") { b.beamlet = B.beamlet; b.noise_lambda = B.noise_lambda; }
         if (c.bunches.empty() && b.nmacro == 0) continue;      // no bunch block in the deck: no bunch
         s.bunches.push_back(b);
     }

@@ -100,6 +100,11 @@ typedef struct g3d_bunch {
     double q;                   /* charge number: -1 electrons, +1 positrons */
     int64_t nmacro;
     uint64_t seed;
+    /* shot noise: beamlet <= 1 random (the default); beamlet = M >= 3: Fawley's beamlets (Phys. Rev. ST Accel.
+     * Beams 5, 070701 (2002); deck shot_noise = fawley): nmacro / M groups of M particles spread evenly over
+     * noise_lambda, displaced so that their bunching at the harmonics h < M/2 is that of the real electrons */
+    int32_t beamlet, reserved;
+    double noise_lambda;
 } g3d_bunch;
 
 /* Streaming plasma (reference Config plasma keys, src/sim.hpp:103-116 and 129): a regular lattice of

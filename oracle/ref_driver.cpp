@@ -97,6 +97,7 @@ int ref_create(const g3d_grid* g, const g3d_params* p, const g3d_bunch* bunches,
             u.q = b.q; u.charge = b.charge_C; u.gamma = b.gamma; u.sigx = b.sigx; u.sigy = b.sigy; u.sigz = b.sigz;
             u.length = b.length; u.emitx = b.emitx; u.emity = b.emity; u.espread = b.espread;
             u.zeta_center = b.zeta_center; u.x0 = b.x0; u.y0 = b.y0; u.nmacro = long(b.nmacro); u.seed = (unsigned long)b.seed;
+            if (b.beamlet > 1) { u.noise = "fawley"; u.beamlet = b.beamlet; u.noise_lambda = b.noise_lambda; }
             r->cfg.bunches.push_back(u);
         }
         if (nb > 0) {
@@ -127,6 +128,7 @@ int ref_create2(const g3d_grid* g, const g3d_params* p, const g3d_bunch* bunches
             u.q = b.q; u.charge = b.charge_C; u.gamma = b.gamma; u.sigx = b.sigx; u.sigy = b.sigy; u.sigz = b.sigz;
             u.length = b.length; u.emitx = b.emitx; u.emity = b.emity; u.espread = b.espread;
             u.zeta_center = b.zeta_center; u.x0 = b.x0; u.y0 = b.y0; u.nmacro = long(b.nmacro); u.seed = (unsigned long)b.seed;
+            if (b.beamlet > 1) { u.noise = "fawley"; u.beamlet = b.beamlet; u.noise_lambda = b.noise_lambda; }
             c.bunches.push_back(u);
         }
         if (nb > 0) {

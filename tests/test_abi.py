@@ -116,3 +116,34 @@ def test_march_objective_checks_its_tensors_before_any_device_work():
         MarchObjective.apply(torch.zeros(16, 16, 2, dtype=torch.float64), dp, cfg)
     with pytest.raises(ValueError, match=r"coef must be"):
         MarchObjective.apply(torch.zeros(16, 9, dtype=torch.float64), dp, cfg)
+
+
+@pytest.mark.parametrize("beamlet", [4, 7])
+def test_fawley_beamlets_match_the_reference_loader(beamlet):
+    """Shot noise by Fawley's beamlets (Phys. Rev. ST Accel. Beams 5, 070701 (2002); the deck's shot_noise = fawley):
+    the host sampler, without a device, against the reference build's loader, bit for bit."""
+    ref = pytest.importorskip("ref")
+    if not ref.available():
+        pytest.skip("reference build oracle/_ref not present")
+    from g3d import configs, sample_bunches
+    cfg = configs.config2(nx=16, ny=16, nzeta=48, nmacro=4200, steps=2, envelope=0)
+    cfg.bunches[0].update(beamlet=beamlet, noise_lambda=0.35)
+    got, lost, _, _ = sample_bunches(cfg)
+    r = ref.RefSimulation(cfg, threads=1)
+    r.load_bunch()
+    want = r.host_particles()
+    r.close()
+    assert len(got) == len(want) > 4000 - 200
+    for f in want.dtype.names:
+        assert np.array_equal(got[f], want[f]), f
+    # the groups: each draws one position and momentum, M phases spread over the wavelength
+    z = got["zeta"][:beamlet]
+    assert np.all(got["px"][:beamlet] == got["px"][0]) and np.ptp(z) > 0
+
+
+def test_fawley_beamlets_need_a_divisible_count():
+    from g3d import G3DError, configs, sample_bunches
+    cfg = configs.config1(nx=16, ny=16, nzeta=32, nmacro=1001)
+    cfg.bunches[0].update(beamlet=4, noise_lambda=0.5)
+    with pytest.raises(G3DError):
+        sample_bunches(cfg)

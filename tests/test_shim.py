@@ -29,13 +29,26 @@ def test_supported_decks_map(which, tmp_path):
 
 @needs_shim
 @pytest.mark.parametrize("extra,key", [
-    (f"  shot_noise = fawley\n  noise_wavelength = {L(1)}\n", "shot_noise"),
     ("  ux_function = 0.001\n", "profile functions"),
 ])
 def test_what_the_library_does_not_run_is_refused(extra, key, tmp_path):
     text = wake_deck(tmp_path / "out").replace("  seed = 3\n", "  seed = 3\n" + extra, 1)
     r = check(text, tmp_path)
     assert r.returncode == 2 and "libg3d does not run" in r.stderr and key in r.stderr, (r.stdout[-500:], r.stderr)
+
+
+@needs_shim
+def test_a_plasma_density_function_is_refused(tmp_path):
+    text = lwfa_deck(tmp_path / "out").replace("  ppc_y = 2\n", "  ppc_y = 2\n  density_function = 1 + 0.1 * r\n", 1)
+    r = check(text, tmp_path)
+    assert r.returncode == 2 and "libg3d does not run" in r.stderr and "density_function" in r.stderr, r.stderr
+
+
+@needs_shim
+def test_fawley_shot_noise_maps(tmp_path):
+    text = wake_deck(tmp_path / "out").replace("  seed = 3\n", f"  seed = 3\n  shot_noise = fawley\n  noise_wavelength = {L(1)}\n", 1)
+    r = check(text, tmp_path)
+    assert r.returncode == 0 and "fawley" in r.stdout, r.stderr
 
 
 @needs_shim
