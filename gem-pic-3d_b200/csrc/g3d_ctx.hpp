@@ -187,6 +187,7 @@ struct Ctx {
     int steps_since_sort = 0;
     // reductions
     DevBuf<double> red;                          // per-block partial sums
+    DevBuf<double> momw;                         // the beam moments' partial sums, totals and means
     std::vector<double> red_h;
     // scalars (reference members)
     double s = 0, X0 = 0, Y0 = 0, beta_b = 1, gm2_b = 0, field_energy = 0, hmin = 1e300;
@@ -277,6 +278,8 @@ void launch_copy_c(Ctx& c, cpx* y, const cpx* x, size_t n);
 void launch_beta_sums(Ctx& c, double out[2]);
 void launch_beta_sums_static(Ctx& c, double out[2]);
 void launch_centroid(Ctx& c, double out[3]);
+int beam_groups(const Ctx& c);              // beam species: bunch blocks, trapped, injected per ion species
+void launch_beam_moments(Ctx& c, double* s1, double* s2);
 void launch_diag(Ctx& c, double S[19]);
 double launch_field_energy(Ctx& c);
 void launch_shift(Ctx& c, int nxs, int nys, double sx, double sy);

@@ -1476,6 +1476,15 @@ int g3d_diagnostics(g3d_ctx* ctx, double out[19]) {
         std::memcpy(out, S, sizeof S);
     });
 }
+int g3d_beam_moments(g3d_ctx* ctx, int32_t capacity, double* s1, double* s2, int32_t* ngroups) {
+    return guarded(ctx, [&] {
+        const int G = g3d::beam_groups(ctx->c);
+        if (ngroups) *ngroups = G;
+        if (!s1 || !s2) throw Error(G3D_ERR_ARG, "g3d_beam_moments: null output");
+        if (capacity < G) throw Error(G3D_ERR_CAPACITY, "g3d_beam_moments: capacity below the " + std::to_string(G) + " beam species");
+        g3d::launch_beam_moments(ctx->c, s1, s2);
+    });
+}
 int g3d_field_energy(g3d_ctx* ctx, double* out) {
     return guarded(ctx, [&] { *out = ctx->c.P.self_fields ? g3d::launch_field_energy(ctx->c) : 0; });
 }

@@ -5,7 +5,7 @@
 // fixed-order two-level tree: a persistent grid of RB blocks accumulates grid-stride partial sums,
 // each block reduces them in shared memory, and one block sums the block results in index order. The
 // result depends only on the input, never on the thread schedule, so reruns are bit-identical.
-#include "g3d_ctx.hpp"
+#include "g3d_plasma.hpp"
 
 namespace g3d {
 
@@ -121,6 +121,46 @@ __global__ void k_seq_sum2(const double* __restrict__ t, const double* __restric
     if (lane == 0) { out[0] = s0; out[1] = s1; }
 }
 
+// ------------------------------------------------ moments of the beam species (bunches.txt)
+// group of a beam particle: bunch block k (sp = -k) -> k, trapped plasma electrons -> nbunch, electrons injected
+// from ion species m (sp = 100 + m) -> nbunch + 1 + m (the reference's Config::beam_index); -1: none
+constexpr int MOM_G = 16, MOM_NV = 8 * MOM_G;
+__device__ __forceinline__ int beam_group(int sp, int nbunch, int ngroups) {
+    const int g = sp <= 0 ? -sp : (sp >= 100 ? nbunch + 1 + (sp - 100) : nbunch);
+    return g < ngroups ? g : -1;
+}
+__device__ __forceinline__ void beam_values(const PartsDev& P, long i, double X0, double Y0, double v[6]) {
+    const double px = P.px[i], py = P.py[i], pz = P.pz[i];
+    v[0] = P.x[i] + X0; v[1] = P.y[i] + Y0; v[2] = P.zeta[i]; v[3] = px; v[4] = py;
+    v[5] = sqrt(1 + px * px + py * py + pz * pz);
+}
+// first pass: w, count and w v per group; second pass (mean given): the centred second moments
+template <int PASS>
+__global__ void __launch_bounds__(RT) k_moments(PartsDev P, long np, double X0, double Y0, int nbunch, int ngroups,
+                                               const double* __restrict__ mean, double* __restrict__ part) {
+    double acc[MOM_NV];
+    for (int v = 0; v < MOM_NV; ++v) acc[v] = 0;
+    for (long i = long(blockIdx.x) * RT + threadIdx.x; i < np; i += long(gridDim.x) * RT) {
+        if (P.alive[i] != 1) continue;
+        const int g = beam_group(P.sp[i], nbunch, ngroups);
+        if (g < 0) continue;
+        double v[6];
+        beam_values(P, i, X0, Y0, v);
+        const double w = P.w[i];
+        double* a = acc + 8 * g;
+        if (PASS == 1) {
+            a[0] += w; a[1] += 1;
+            for (int k = 0; k < 6; ++k) a[2 + k] += w * v[k];
+        } else {
+            double d[6];
+            for (int k = 0; k < 6; ++k) d[k] = v[k] - mean[6 * g + k];
+            a[0] += w * d[0] * d[0]; a[1] += w * d[1] * d[1]; a[2] += w * d[2] * d[2]; a[3] += w * d[3] * d[3];
+            a[4] += w * d[4] * d[4]; a[5] += w * d[0] * d[3]; a[6] += w * d[1] * d[4]; a[7] += w * d[5] * d[5];
+        }
+    }
+    block_store<MOM_NV>(acc, part);
+}
+
 template <int NV>
 void finish(Ctx& c, double* out) {
     k_final<NV><<<1, RT, 0, c.stream>>>(c.red.p, RB, c.red.p + RB * NV);
@@ -150,6 +190,36 @@ double launch_field_energy(Ctx& c) {
     c.prof_end(tok);
     finish<1>(c, r);
     return r[0] * c.dx;
+}
+
+int beam_groups(const Ctx& c) { return c.nbunch + 1 + (c.pl ? int(c.pl->ions.size()) : 0); }
+void launch_beam_moments(Ctx& c, double* s1, double* s2) {
+    const int G = beam_groups(c);
+    if (G > MOM_G) throw Error(G3D_ERR_CAPACITY, "beam moments: more than " + std::to_string(MOM_G) + " beam species");
+    if (c.momw.n < size_t(RB + 2) * MOM_NV) c.momw.alloc(size_t(RB + 2) * MOM_NV, c.stream);
+    double* part = c.momw.p;
+    double* tot = part + size_t(RB) * MOM_NV;
+    double* mean = tot + MOM_NV;
+    std::vector<double> r(MOM_NV), mh(MOM_NV, 0.0);
+    k_moments<1><<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.X0, c.Y0, c.nbunch, G, mean, part);
+    c.check_launch("k_moments");
+    k_final<MOM_NV><<<1, RT, 0, c.stream>>>(part, RB, tot);
+    c.check_launch("k_final");
+    G3D_CUDA(cudaMemcpyAsync(r.data(), tot, MOM_NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    for (int g = 0; g < G; ++g) {
+        for (int k = 0; k < 8; ++k) s1[8 * g + k] = r[size_t(8 * g + k)];
+        for (int k = 0; k < 6; ++k) mh[size_t(6 * g + k)] = r[size_t(8 * g)] > 0 ? r[size_t(8 * g + 2 + k)] / r[size_t(8 * g)] : 0;
+    }
+    G3D_CUDA(cudaMemcpyAsync(mean, mh.data(), MOM_NV * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    k_moments<2><<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.X0, c.Y0, c.nbunch, G, mean, part);
+    c.check_launch("k_moments");
+    k_final<MOM_NV><<<1, RT, 0, c.stream>>>(part, RB, tot);
+    c.check_launch("k_final");
+    G3D_CUDA(cudaMemcpyAsync(r.data(), tot, MOM_NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    for (int g = 0; g < G; ++g)
+        for (int k = 0; k < 8; ++k) s2[8 * g + k] = r[size_t(8 * g + k)];
 }
 
 void launch_centroid(Ctx& c, double out[3]) {

@@ -134,6 +134,7 @@ SIGNATURES = [
     ("g3d_shift_window", _I, [_P, _I32, _I32]),
     ("g3d_diagnostics", _I, [_P, C.POINTER(_D)]),
     ("g3d_field_energy", _I, [_P, C.POINTER(_D)]),
+    ("g3d_beam_moments", _I, [_P, _I32, C.POINTER(_D), C.POINTER(_D), C.POINTER(_I32)]),
     ("g3d_beam_beta_sums_static", _I, [_P, C.POINTER(_D)]),
     ("g3d_set_precision", _I, [_P, _I]),
     ("g3d_get_status", _I, [_P, C.POINTER(Status)]),

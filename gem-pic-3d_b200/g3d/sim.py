@@ -186,6 +186,16 @@ class Simulation:
         self._c(self.lib.g3d_diagnostics(self.ctx, out))
         return np.array(out[:], dtype=np.float64)
 
+    def beam_moments(self):
+        """(s1, s2): per beam species [G, 8] the first sums and the centred second sums of bunches.txt."""
+        cap = 16
+        s1 = (C.c_double * (8 * cap))()
+        s2 = (C.c_double * (8 * cap))()
+        G = C.c_int32()
+        self._c(self.lib.g3d_beam_moments(self.ctx, cap, s1, s2, C.byref(G)))
+        n = 8 * G.value
+        return np.array(s1[:n]).reshape(-1, 8), np.array(s2[:n]).reshape(-1, 8)
+
     def field_energy(self):
         v = C.c_double()
         self._c(self.lib.g3d_field_energy(self.ctx, C.byref(v)))

@@ -4,7 +4,8 @@
 //
 //   g3d_run deck [--check] [--restart latest|STEP] [--precision fp64|mixed] [block.key=value ...]
 //
-// Written to output.dir: diag.txt (the reference's columns, every output.every steps and the last), checkpoints
+// Written to output.dir: diag.txt and bunches.txt (the reference's columns, every output.every steps and the last;
+// the beam moments from the device), checkpoints
 // every output.checkpoint_every steps in the reference's layout and name (checkpoint_NNNNNN_r0000.bin; without a
 // plasma: the library checkpoints no streaming state), and
 // "done: N steps, X s" on stdout. Field files, particle dumps, frames, openPMD and the other output groups of the
@@ -76,6 +77,37 @@ void diag_line(FILE* f, const Config& c, g3dshim::Simulation& sim, bool header) 
         if (out) { std::fputs(line, out); std::fflush(out); }
 }
 
+// bunches.txt: per output step one line per beam species (the reference's columns: N, Q [pC], E [MeV], dE/E,
+// sig_x, sig_y, eps_nx, eps_ny [um], <zeta>, sig_z [um], <x>, <y> [um]) from the device moments
+void bunches_lines(FILE* f, const Config& c, g3dshim::Simulation& sim, bool header) {
+    if (!f) return;
+    if (header)
+        std::fprintf(f, "# step  z[mm]  bunch  N  Q[pC]  E[MeV]  dE/E(rms)  sig_x[um]  sig_y[um]  eps_nx[um]  eps_ny[um]  "
+                        "<zeta>[um]  sig_z[um]  <x>[um]  <y>[um]    (trapped = self-injected plasma electrons, inj_<ion> "
+                        "= from field ionization)\n");
+    std::vector<double> s1, s2;
+    sim.beam_moments(s1, s2);
+    const g3d_status st = sim.status();
+    const double pC = c.nc * std::pow(c.Lu, 3) * kE * 1e12, um = c.Lu * 1e6;
+    const std::vector<std::string> names = c.beam_names();
+    for (size_t g = 0; g < names.size() && 8 * g < s1.size(); ++g) {
+        const double* a = &s1[8 * g];
+        const double* b = &s2[8 * g];
+        const double w = a[0];
+        auto mean = [&](int k) { return w > 0 ? a[2 + k] / w : 0.0; };
+        auto var = [&](int k) { return w > 0 ? b[k] / w : 0.0; };
+        const double gm = mean(5);
+        const double ex = std::sqrt(std::max(0.0, var(0) * var(3) - var(5) * var(5)));
+        const double ey = std::sqrt(std::max(0.0, var(1) * var(4) - var(6) * var(6)));
+        std::fprintf(f, "%6ld %10.5f %-12s", long(st.istep), st.s * c.Lu * 1e3, names[g].c_str());
+        std::fprintf(f, " %10ld %12.6f %13.6f %10.3e %10.5f %10.5f %10.5f %10.5f %11.4f %10.4f %11.5f %11.5f\n", long(a[1]),
+                     w * pC, w > 0 ? (gm - 1) * 0.51099895 : 0.0, gm > 0 ? std::sqrt(var(7)) / gm : 0.0,
+                     std::sqrt(var(0)) * um, std::sqrt(var(1)) * um, ex * um, ey * um, mean(2) * um, std::sqrt(var(2)) * um,
+                     mean(0) * um, mean(1) * um);
+    }
+    std::fflush(f);
+}
+
 std::string checkpoint_name(const std::string& dir, long step) {
     char fn[64];
     std::snprintf(fn, sizeof fn, "/checkpoint_%06ld_r0000.bin", step);
@@ -133,19 +165,21 @@ int main(int argc, char** argv) {
         }
         FILE* f = open_table(c.dir + "/diag.txt", rs);
         if (!f) throw std::runtime_error("cannot write " + c.dir + "/diag.txt");
-        if (rs < 0) diag_line(f, c, sim, true);
+        FILE* fb = open_table(c.dir + "/bunches.txt", rs);
+        if (rs < 0) { diag_line(f, c, sim, true); bunches_lines(fb, c, sim, true); }
         const auto t0 = std::chrono::steady_clock::now();
         long steps = 0;
         long istep = sim.status().istep;
         while (!sim.finished()) {
             sim.step();
             ++steps; ++istep;
-            if (c.every > 0 && istep % c.every == 0) diag_line(f, c, sim, false);
+            if (c.every > 0 && istep % c.every == 0) { diag_line(f, c, sim, false); bunches_lines(fb, c, sim, false); }
             if (c.checkpoint_every > 0 && istep % c.checkpoint_every == 0 && !setup.plasma_on)
                 sim.write_checkpoint(checkpoint_name(c.dir, istep));
         }
-        if (c.every <= 0 || istep % c.every) diag_line(f, c, sim, false);
+        if (c.every <= 0 || istep % c.every) { diag_line(f, c, sim, false); bunches_lines(fb, c, sim, false); }
         std::fclose(f);
+        if (fb) std::fclose(fb);
         const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::printf("done: %ld steps, %.1f s\n", istep, sec);
         (void)steps;

@@ -114,6 +114,13 @@ public:
         check(g3d_diagnostics(ctx_, S.data()), ctx_, "diagnostics");
         return S;
     }
+    // the first and the centred second moments of the beam species (bunches.txt), [group][8] each
+    void beam_moments(std::vector<double>& s1, std::vector<double>& s2) {
+        s1.assign(16 * 8, 0.0); s2.assign(16 * 8, 0.0);
+        int32_t G = 0;
+        check(g3d_beam_moments(ctx_, 16, s1.data(), s2.data(), &G), ctx_, "beam_moments");
+        s1.resize(size_t(G) * 8); s2.resize(size_t(G) * 8);
+    }
     g3d_status status() const {
         g3d_status st{};
         check(g3d_get_status(ctx_, &st), ctx_, "status");

@@ -275,6 +275,13 @@ int g3d_get_streaming(struct g3d_ctx* ctx, g3d_particle* out, int64_t capacity, 
  * Y^2, zeta^2, px, py, pz, gamma, p.khat, pz^2, eta), S[14] their count, S[15] field energy
  * (code units), S[16] lost particles, S[17] count and S[18] charge of trapped particles. */
 int g3d_diagnostics(struct g3d_ctx* ctx, double out[19]);
+/* Moments of the beam species for bunches.txt (Simulation::write_bunches, src/sim_bunch_diag.cpp:42-80), on the
+ * device in a fixed order, two passes (the second moments centred on the first's means). Groups g: the bunch blocks
+ * 0 .. nbunch-1, then the trapped plasma electrons, then the electrons injected from each ion species (the reference's
+ * beam_index); *ngroups = their number, at most 16 (G3D_ERR_CAPACITY if above `capacity`). Per group, of the alive
+ * particles with v = (x, y, zeta, u_x, u_y, gamma), x and y physical: s1[8 g ..] = sum w, count, sum w v[0..5];
+ * s2[8 g ..] = sum w d0^2, w d1^2, w d2^2, w d3^2, w d4^2, w d0 d3, w d1 d4, w d5^2 with d = v - mean. */
+int g3d_beam_moments(struct g3d_ctx* ctx, int32_t capacity, double* s1, double* s2, int32_t* ngroups);
 /* Field energy of the slices in code units (Simulation::local_field_energy, sim_output.cpp:55-77). */
 int g3d_field_energy(struct g3d_ctx* ctx, double* out);
 int g3d_get_status(const struct g3d_ctx* ctx, g3d_status* out);

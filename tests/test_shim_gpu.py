@@ -189,6 +189,27 @@ def diag_rows(path):
     return np.array([[float(v) for v in line.split()] for line in open(path) if line.strip() and line[0] != "#"])
 
 
+def bunches_rows(path):
+    """bunches.txt as {species: rows of numbers (step, z, N, Q, ...)}"""
+    out = {}
+    for line in open(path):
+        if not line.strip() or line[0] == "#":
+            continue
+        f = line.split()
+        out.setdefault(f[2], []).append([float(v) for v in f[:2] + f[3:]])
+    return {k: np.array(v) for k, v in out.items()}
+
+
+def bunches_close(a, b, tag):
+    assert sorted(a) == sorted(b), (tag, sorted(a), sorted(b))
+    for k in a:
+        x, y = a[k], b[k]
+        assert x.shape == y.shape, (tag, k, x.shape, y.shape)
+        tol = 3e-4 * np.maximum(np.abs(x), np.abs(y)) + 2e-5
+        bad = np.argwhere(np.abs(x - y) > tol)
+        assert len(bad) == 0, (tag, k, [(int(i), int(j), x[i, j], y[i, j]) for i, j in bad[:5]])
+
+
 def diag_close(a, b, tag):
     """Every column to its printed digits: within a few units of the last digit of either side. With mobile ions the
     reference adds a 22nd column, the largest ion density on the axis, from charge planes this library does not
@@ -222,6 +243,7 @@ def test_vacuum_wake_deck_matches_the_reference_cli(tmp_path):
     for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
         assert rel_l2(p[f], q[f]) <= 1e-10, f
     diag_close(diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt"), "wake")
+    bunches_close(bunches_rows(our_dir / "out" / "bunches.txt"), bunches_rows(ref_dir / "out" / "bunches.txt"), "wake")
 
 
 @needs_both
@@ -236,6 +258,7 @@ def test_laser_wakefield_deck_matches_the_reference_cli(tmp_path):
     a, b = diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt")
     assert a.shape[0] >= 3
     diag_close(a, b, "lwfa")
+    bunches_close(bunches_rows(our_dir / "out" / "bunches.txt"), bunches_rows(ref_dir / "out" / "bunches.txt"), "lwfa")
 
 
 @needs_both
