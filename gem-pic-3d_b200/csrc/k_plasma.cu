@@ -46,7 +46,7 @@ __device__ __forceinline__ void boris(A& ux, A& uy, A& uz, const A E[3], const A
 
 // grid fields of the F planes (TSC in x, y, linear in zeta) as in the beam push. F32 (the mixed form): the
 // weights and the sums in FP32; else FP64 arithmetic on the float data.
-template <bool F32>
+template <bool F32, int NC = 6>
 __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
     E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
     const Geo& g = c.g;
@@ -63,7 +63,7 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
         int jh[3]; double wh[3];
         tsc_y(g.yax, y, jn, wn, jh, wh);
         const R f1 = R(fz), f0 = R(1 - fz);
-        for (int comp = 0; comp < 6; ++comp) {
+        for (int comp = 0; comp < NC; ++comp) {
             const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
             const float* p1 = p0 + nk;
             const bool hf = is_half(comp);
@@ -93,7 +93,7 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
     // both slices summed with the TSC weights, then interpolated in zeta
     const R f1 = R(fz), f0 = R(1 - fz);
 #pragma unroll
-    for (int comp = 0; comp < 6; ++comp) {
+    for (int comp = 0; comp < NC; ++comp) {
         const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
         const float* p1 = p0 + nk;
         R v0 = 0, v1 = 0;
@@ -239,7 +239,7 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
 template <bool F32>
 __device__ __forceinline__ double field_abs(const StreamArgs& c, double x, double y, double z, double zeta) {
     double E[3], B[3], Ee[3], Be[3];
-    sgather<F32>(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);
+    sgather<F32, 3>(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);      // |E| needs the electric field only
     c.laser.field(x + c.sv->X0, z, z - (zeta - c.zc), Ee, Be);
     for (int k = 0; k < 3; ++k) E[k] += Ee[k];
     return sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
@@ -347,7 +347,11 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double zm = z + double(hd * pz), zetam = zeta - 0.5 * hl;
     A E[3], B[3];
     const bool mid = c.Fmid && zeta == zn1;                       // the whole half-cell: the midpoint fields
-    if (F32 && mid && !LASER && !c.ext.any()) {
+    if (qm_ == 0) {
+        // a neutral atom: the Boris pushes below leave u exactly as it is whatever the (finite) fields, so they
+        // are not gathered (the gas of an ionization-injection run is mostly neutral until the laser arrives)
+        for (int k = 0; k < 3; ++k) { E[k] = A(0); B[k] = A(0); }
+    } else if (F32 && mid && !LASER && !c.ext.any()) {
         if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy(g, ym), E, B);
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
