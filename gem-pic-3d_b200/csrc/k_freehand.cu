@@ -109,71 +109,92 @@ __global__ void k_cur_lines_fh(Geo g, cpx* __restrict__ jx, cpx* __restrict__ jy
 // per k_x line of one half-cell (Simulation::stream_spectra, src/sim_plasma.cpp:146-180): the (1,2,1)/4 filters of
 // the cell charges as for the beam (no TEM mean removed), j_x = j_z = 0 at the wall node, the x filter, then the
 // smoothing (1 - a^2 Lap_perp)^-1: (1 + a^2 (k_x^2 - b- b+)) f = g on the nodes (f = 0 at the walls, as E_z in the
-// march) and (1 + a^2 (k_x^2 - b+ b-)) f = g on the half-nodes (as B_z), by Thomas along y
-__global__ void k_ss_lines_fh(Geo g, const cpx* __restrict__ T, cpx* __restrict__ out, cpx* __restrict__ rhs,
-                              double* __restrict__ cpv, int kf, double a2) {
-    const int kxi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (kxi >= g.H) return;
-    const int H = g.H, ny = g.ny;
-    const long nkh = g.nkh;
-    cpx* ox = out; cpx* oy = out + nkh; cpx* oz = out + 2 * nkh;
-    const long o = kxi;                              // element j at o + j H
-    for (int j = 0; j < ny; ++j) {
-        const long k = o + long(j) * H;
-        ox[k] = T[k]; oy[k] = T[nkh + k]; oz[k] = T[2 * nkh + k];
-    }
+// march) and (1 + a^2 (k_x^2 - b+ b-)) f = g on the half-nodes (as B_z). One CTA per k_x line, a thread per y row:
+// the charges Q_j of a row and its neighbours from shared memory (the same products and sums as a sweep along the
+// line), the smoothing systems (one matrix for j_x and j_z on the nodes, one for j_y on the half-nodes, strictly
+// diagonally dominant) by parallel cyclic reduction as in the march of the lines.
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT) k_ss_lines_fh(Geo g, const cpx* __restrict__ T, cpx* __restrict__ out, int kf, double a2) {
+    extern __shared__ double2 sm[];
+    const int ny = g.ny, H = g.H, kxi = blockIdx.x, j = threadIdx.x;
+    const bool row = j < ny;
+    const long nkh = g.nkh, k = long(row ? j : 0) * H + kxi;
+    cpx* qx = sm; cpx* qy = sm + ny; cpx* qz = sm + 2 * ny;        // charges of the rows
+    cpx* rx = sm + 3 * ny; cpx* ry = sm + 4 * ny; cpx* rz = sm + 5 * ny;
+    double* lo_n = reinterpret_cast<double*>(sm + 6 * ny);
+    double* dg_n = lo_n + ny; double* up_n = dg_n + ny; double* lo_h = up_n + ny; double* dg_h = lo_h + ny; double* up_h = dg_h + ny;
     const double* ia = g.iA; const double* id = g.iD;
+    cpx vx = C(0), vy = C(0), vz = C(0);
+    if (row) { vx = T[k]; vy = T[nkh + k]; vz = T[2 * nkh + k]; }
     if (kf) {
-        cpx* nodal[2] = {ox, oz};
-        for (int t = 0; t < 2; ++t) {
-            cpx* A = nodal[t];
-            cpx qm = C(0), q0 = A[o + H] / ia[1];
-            for (int j = 1; j < ny; ++j) {
-                const cpx qp = j + 1 < ny ? A[o + long(j + 1) * H] / ia[j + 1] : C(0);
-                A[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * ia[j];
-                qm = q0; q0 = qp;
-            }
+        // nodes (j_x, j_z): Q_j = J_j / (1/A_j), zero on the wall node 0 and beyond the last node; half-nodes (j_y):
+        // Q_j = J_j / (1/Delta_j), mirrored at both walls
+        if (row) {
+            qx[j] = j == 0 ? C(0) : vx / ia[j]; qz[j] = j == 0 ? C(0) : vz / ia[j];
+            qy[j] = vy / id[j];
         }
-        cpx qm = oy[o] / id[0], q0 = qm;
-        for (int j = 0; j < ny; ++j) {
-            const cpx qp = j + 1 < ny ? oy[o + long(j + 1) * H] / id[j + 1] : q0;
-            oy[o + long(j) * H] = (0.25 * qm + 0.5 * q0 + 0.25 * qp) * id[j];
-            qm = q0; q0 = qp;
+        __syncthreads();
+        if (row) {
+            if (j > 0) {
+                const cpx xm = j > 1 ? qx[j - 1] : C(0), zm = j > 1 ? qz[j - 1] : C(0);
+                const cpx xp = j + 1 < ny ? qx[j + 1] : C(0), zp = j + 1 < ny ? qz[j + 1] : C(0);
+                vx = (0.25 * xm + 0.5 * qx[j] + 0.25 * xp) * ia[j];
+                vz = (0.25 * zm + 0.5 * qz[j] + 0.25 * zp) * ia[j];
+            }
+            const cpx ym = j > 0 ? qy[j - 1] : qy[0], yp = j + 1 < ny ? qy[j + 1] : qy[ny - 1];
+            vy = (0.25 * ym + 0.5 * qy[j] + 0.25 * yp) * id[j];
         }
     }
     const double fx = g.filt[kxi];
-    ox[o] = C(0); oz[o] = C(0);
-    for (int j = 0; j < ny; ++j) {
-        const long k = o + long(j) * H;
-        ox[k] = fx * ox[k]; oy[k] = fx * oy[k]; oz[k] = fx * oz[k];
-    }
-    if (a2 <= 0) return;
-    const double kx2 = g.kxs[kxi] * g.kxs[kxi];
-    cpx* nodal[2] = {ox, oz};
-    for (int t = 0; t < 2; ++t) {
-        cpx* A = nodal[t];
-        double cp = 0; cpx dp = C(0);
-        for (int j = 1; j < ny; ++j) {
-            const double lo = j > 1 ? -a2 * ia[j] * id[j - 1] : 0, up = j < ny - 1 ? -a2 * ia[j] * id[j] : 0;
-            const double den = 1 + a2 * kx2 + a2 * ia[j] * (id[j - 1] + id[j]) - lo * cp;
-            dp = (A[o + long(j) * H] - lo * dp) / den;
-            cp = up / den;
-            rhs[o + long(j) * H] = dp; cpv[o + long(j) * H] = cp;
+    if (j == 0) { vx = C(0); vz = C(0); }
+    vx = fx * vx; vy = fx * vy; vz = fx * vz;
+    if (a2 > 0) {
+        const double kx2 = g.kxs[kxi] * g.kxs[kxi];
+        // nodes 1..ny-1 (row 0, the wall, stays 0) and half-nodes 0..ny-1
+        double an = 0, bn = 1, cn = 0, ah = 0, bh = 1, ch = 0;
+        if (row) {
+            if (j > 0) {
+                an = j > 1 ? -a2 * ia[j] * id[j - 1] : 0;
+                cn = j < ny - 1 ? -a2 * ia[j] * id[j] : 0;
+                bn = 1 + a2 * kx2 + a2 * ia[j] * (id[j - 1] + id[j]);
+            }
+            const double al = j > 0 ? ia[j] : 0, au = j < ny - 1 ? ia[j + 1] : 0;
+            ah = -a2 * id[j] * al; ch = -a2 * id[j] * au;
+            bh = 1 + a2 * kx2 + a2 * id[j] * (al + au);
         }
-        cpx next = C(0);
-        for (int j = ny - 1; j >= 1; --j) { next = rhs[o + long(j) * H] - cpv[o + long(j) * H] * next; A[o + long(j) * H] = next; }
+        for (int st = 1; st < ny; st <<= 1) {
+            __syncthreads();                                        // the previous step's reads are done
+            if (row) {
+                lo_n[j] = an; dg_n[j] = bn; up_n[j] = cn; rx[j] = vx; rz[j] = vz;
+                lo_h[j] = ah; dg_h[j] = bh; up_h[j] = ch; ry[j] = vy;
+            }
+            __syncthreads();
+            if (row) {
+                const int m = j - st, q = j + st;
+                double nan_ = 0, ncn = 0, nah = 0, nch = 0, nbn = bn, nbh = bh;
+                cpx dx = vx, dz = vz, dy = vy;
+                if (m >= 0) {
+                    const double fn = an / dg_n[m], fh = ah / dg_h[m];
+                    nan_ = -lo_n[m] * fn; nah = -lo_h[m] * fh;
+                    nbn -= up_n[m] * fn; nbh -= up_h[m] * fh;
+                    dx = dx - fn * rx[m]; dz = dz - fn * rz[m]; dy = dy - fh * ry[m];
+                }
+                if (q < ny) {
+                    const double gn = cn / dg_n[q], gh = ch / dg_h[q];
+                    ncn = -up_n[q] * gn; nch = -up_h[q] * gh;
+                    nbn -= lo_n[q] * gn; nbh -= lo_h[q] * gh;
+                    dx = dx - gn * rx[q]; dz = dz - gn * rz[q]; dy = dy - gh * ry[q];
+                }
+                an = nan_; cn = ncn; bn = nbn; ah = nah; ch = nch; bh = nbh;
+                vx = dx; vz = dz; vy = dy;
+            }
+        }
+        if (row) {
+            vx = j == 0 ? C(0) : vx / bn; vz = j == 0 ? C(0) : vz / bn;
+            vy = vy / bh;
+        }
     }
-    double cp = 0; cpx dp = C(0);
-    for (int j = 0; j < ny; ++j) {
-        const double al = j > 0 ? ia[j] : 0, au = j < ny - 1 ? ia[j + 1] : 0;
-        const double lo = -a2 * id[j] * al, up = -a2 * id[j] * au;
-        const double den = 1 + a2 * kx2 + a2 * id[j] * (al + au) - lo * cp;
-        dp = (oy[o + long(j) * H] - lo * dp) / den;
-        cp = up / den;
-        rhs[o + long(j) * H] = dp; cpv[o + long(j) * H] = cp;
-    }
-    cpx next = C(0);
-    for (int j = ny - 1; j >= 0; --j) { next = rhs[o + long(j) * H] - cpv[o + long(j) * H] * next; oy[o + long(j) * H] = next; }
+    if (row) { out[k] = vx; out[nkh + k] = vy; out[2 * nkh + k] = vz; }
 }
 
 // ---------------------------------------------------------------- the march of the k_x lines
@@ -539,9 +560,17 @@ void launch_march_fh(Ctx& c, double D) { march_lines(c, D, c.b - 1, c.a, "march"
 void launch_march_slice_fh(Ctx& c, double D, int n) { march_lines(c, D, n, n, "march_slice"); }
 // the lines of the streaming spectra: T0..T2 (the x spectra of the rows of j_x, j_y, j_z) -> out (3 half planes)
 void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2) {
-    const size_t ln = size_t(c.ny) * c.H;
-    k_ss_lines_fh<<<unsigned((c.H + 63) / 64), 64, 0, c.stream>>>(c.geo(), T3, out3, c.fhs.p + 4 * ln, c.fhcp.p,
-                                                                 c.P.k_filter ? 1 : 0, a2);
+    if (c.ny > LINE_MAX_NY) throw Error(G3D_ERR_ARG, "free-hand streaming spectra: ny above " + std::to_string(LINE_MAX_NY));
+    const size_t smem = size_t(c.ny) * (6 * sizeof(cpx) + 6 * sizeof(double));
+    const int threads = (c.ny + 31) / 32 * 32;
+    if (threads <= 256) {
+        smem_attr(reinterpret_cast<const void*>(k_ss_lines_fh<256>), size_t(256) * (6 * sizeof(cpx) + 6 * sizeof(double)));
+        k_ss_lines_fh<256><<<unsigned(c.H), unsigned(threads), smem, c.stream>>>(c.geo(), T3, out3, c.P.k_filter ? 1 : 0, a2);
+    } else {
+        smem_attr(reinterpret_cast<const void*>(k_ss_lines_fh<LINE_MAX_NY>),
+                  size_t(LINE_MAX_NY) * (6 * sizeof(cpx) + 6 * sizeof(double)));
+        k_ss_lines_fh<LINE_MAX_NY><<<unsigned(c.H), unsigned(threads), smem, c.stream>>>(c.geo(), T3, out3, c.P.k_filter ? 1 : 0, a2);
+    }
     c.check_launch("k_ss_lines_fh");
 }
 void launch_sponge_fh(Ctx& c) {

@@ -243,19 +243,27 @@ def reference_final_modes(cfg, a_half):
 
 
 def test_laser_mode_gradient_against_central_differences_of_the_reference():
-    """dJ/da along a random direction against central differences of the reference's own CPU code (its float real
-    fields, so eps = 3e-3 as for the momenta), and this library's forward taking the same difference to 1e-9."""
+    """dJ/da along a random direction against central differences of the reference's own CPU code, and this
+    library's forward taking the same differences to 1e-9 (measured 1e-12: they are the reference's arithmetic).
+    The reference keeps the real fields in float, and their rounding reaches J: its difference quotients for the laser
+    modes scatter by ~1e-4 relative at steps of 1e-3 (measured: 1.00907e-3 and 1.00916e-3 at eps = 4e-3 and 2e-3),
+    more than their truncation error, so the adjoint is held to 5e-4 of their Richardson extrapolation
+    (4 D(eps/2) - D(eps)) / 3 here; the same adjoint matches the central differences of the forward with FP64 real
+    fields to 1e-6 (test_laser_mode_gradient_against_central_differences)."""
     from g3d import configs
     cfg = configs.adjoint_small(charge_pC=1.0)
     _, gm, _, _ = adjoint(cfg, exact=False)
     d = hermitian_direction(np.random.default_rng(21), cfg.ny, cfg.nx)
-    e = 3e-3
-    fr = central(reference_final_modes(cfg, 1 + e * d), reference_final_modes(cfg, 1 - e * d), e)
-    fo = central(forward(cfg, coef=1 + e * d, exact=False), forward(cfg, coef=1 - e * d, exact=False), e)
+    quot = {}
+    for e in (4e-3, 2e-3):
+        fr = central(reference_final_modes(cfg, 1 + e * d), reference_final_modes(cfg, 1 - e * d), e)
+        fo = central(forward(cfg, coef=1 + e * d, exact=False), forward(cfg, coef=1 - e * d, exact=False), e)
+        assert abs(fo - fr) <= 1e-9 * abs(fr), (e, fo, fr)
+        quot[e] = fr
+    rich = (4 * quot[2e-3] - quot[4e-3]) / 3
     ad = float(np.real(np.sum(np.conj(gm) * d)))
-    print(f"laser modes: reference central difference {fr:.12e}, this forward's {fo:.12e}, adjoint {ad:.12e}")
-    assert abs(fo - fr) <= 1e-9 * abs(fr), (fo, fr)
-    assert abs(ad - fr) <= 1e-5 * abs(fr), (ad, fr)
+    print(f"laser modes: reference central differences {quot}, extrapolated {rich:.12e}, adjoint {ad:.12e}")
+    assert abs(ad - rich) <= 5e-4 * abs(rich), (ad, rich)
 
 
 def autograd_inputs(cfg):
