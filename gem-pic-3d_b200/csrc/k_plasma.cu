@@ -46,7 +46,7 @@ __device__ __forceinline__ void boris(A& ux, A& uy, A& uz, const A E[3], const A
 
 // grid fields of the F planes (TSC in x, y, linear in zeta) as in the beam push. F32 (the mixed form): the
 // weights and the sums in FP32; else FP64 arithmetic on the float data.
-template <bool F32, int NC = 6>
+template <bool F32, bool YF, int NC = 6>
 __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
     E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
     const Geo& g = c.g;
@@ -59,22 +59,25 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
     tsc_periodic(x, g.dx, g.nx, ix, wx);
     const long nk = g.nk;
     typedef typename std::conditional<F32, float, double>::type R;
-    if (!g.yf) {                       // free-hand y: E_y, B_x, B_z on the half-nodes, nothing beyond the walls
+    if constexpr (!YF) {               // free-hand y: E_y, B_x, B_z on the half-nodes, nothing beyond the walls
         int jh[3]; double wh[3];
         tsc_y(g.yax, y, jn, wn, jh, wh);
         const R f1 = R(fz), f0 = R(1 - fz);
+#pragma unroll
         for (int comp = 0; comp < NC; ++comp) {
             const float* p0 = c.F + (long(comp) * (g.ns + 2) + fl) * nk;
             const float* p1 = p0 + nk;
             const bool hf = is_half(comp);
-            const int* jj = hf ? jh : jn;
-            const double* wy = hf ? wh : wn;
             R v0 = 0, v1 = 0;
+#pragma unroll
             for (int j = 0; j < 3; ++j) {
-                if (jj[j] < 0 || jj[j] >= g.ny) continue;
+                const int jy = hf ? jh[j] : jn[j];
+                const double wy = hf ? wh[j] : wn[j];
+                if (jy < 0 || jy >= g.ny) continue;
+#pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    const long k = long(jj[j]) * g.nx + ix[i];
-                    const R w = R(wx[i] * wy[j]);
+                    const long k = long(jy) * g.nx + ix[i];
+                    const R w = R(wx[i] * wy);
                     v0 += w * R(p0[k]); v1 += w * R(p1[k]);
                 }
             }
@@ -181,24 +184,27 @@ __device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, doub
         }
 }
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
-__device__ __forceinline__ double wrapy(const Geo& g, double y) { return g.yf ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
+template <bool YF>
+__device__ __forceinline__ double wrapy(const Geo& g, double y) { return YF ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
 // TSC deposit of f v at (x, y) into jsr: jx, jy, jz (stream_deposit, sim_stream.hpp:33-64). The reference also
 // deposits the charge of negative and positive particles into planes 3 and 4; those feed only its density
 // diagnostics (rho_lines, openPMD n_e / n_i), which this build does not write, so they are left out. F32: into the
 // FP32 planes; on the Fourier y grid interleaved per point as (jx, jy, jz, 0), one vector atomic add per TSC
 // point instead of three (the adds into L2 bound the streaming push).
-template <bool F32>
+template <bool F32, bool YF>
 __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
     const Geo& g = c.g;
     int ix_[3], jn[3]; double wx[3], wn[3];
     tsc_periodic(x, g.dx, g.nx, ix_, wx);
     const long nk = g.nk;
-    if (!g.yf) {                       // free-hand y: j_x, j_z on the nodes, j_y on the half-nodes
+    if constexpr (!YF) {               // free-hand y: j_x, j_z on the nodes, j_y on the half-nodes
         int jh[3]; double wh[3];
         tsc_y(g.yax, y, jn, wn, jh, wh);
+#pragma unroll
         for (int v = 0; v < 3; ++v) {
             const bool nod = jn[v] >= 1 && jn[v] <= g.ny - 1, hal = jh[v] >= 0 && jh[v] <= g.ny - 1;
+#pragma unroll
             for (int u = 0; u < 3; ++u) {
                 if (nod) {
                     const long k = long(jn[v]) * g.nx + ix_[u];
@@ -236,10 +242,10 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
 }
 
 // |E| of the grid and the wave at (x, y), lab z, slice position zeta (field_abs, sim_stream.hpp:67-74)
-template <bool F32>
+template <bool F32, bool YF>
 __device__ __forceinline__ double field_abs(const StreamArgs& c, double x, double y, double z, double zeta) {
     double E[3], B[3], Ee[3], Be[3];
-    sgather<F32, 3>(c, wrapx(c.g, x), wrapy(c.g, y), zeta, E, B);      // |E| needs the electric field only
+    sgather<F32, YF, 3>(c, wrapx(c.g, x), wrapy<YF>(c.g, y), zeta, E, B);      // |E| needs the electric field only
     c.laser.field(x + c.sv->X0, z, z - (zeta - c.zc), Ee, Be);
     for (int k = 0; k < 3; ++k) E[k] += Ee[k];
     return sqrt(E[0] * E[0] + E[1] * E[1] + E[2] * E[2]);
@@ -303,7 +309,7 @@ struct DepReq {
 // starts from the same state without a copy of the particles.
 // ION: some species ionizes (else the field magnitudes and the ADK sampling are left out); LASER: the analytic
 // plane wave is on. Both are fixed for a run; the variants without them hold fewer registers.
-template <bool F32, bool ION, bool LASER>
+template <bool F32, bool ION, bool LASER, bool YF>
 __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
     DepReq d{0, 0, 0, 0, 0, 0, false, false, 0.f, {0.f, 0.f, 0.f}};
     const Geo& g = c.g;
@@ -331,7 +337,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         if (f != 0) d = DepReq{x, y, f, 0, 0, 0, true, false, 0.f, {0.f, 0.f, 0.f}};
         if (!c.dry) S.zeta[i] = zn;
         if constexpr (ION) {
-            const double E1 = field_abs<F32>(c, x, y, z, zeta), E0 = field_abs<F32>(c, x, y, z, zn);
+            const double E1 = field_abs<F32, YF>(c, x, y, z, zeta), E0 = field_abs<F32, YF>(c, x, y, z, zn);
             ionize(c, S, i, E1, E0, hl);
         }
         return d;
@@ -351,12 +357,12 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         // a neutral atom: the Boris pushes below leave u exactly as it is whatever the (finite) fields, so they
         // are not gathered (the gas of an ionization-injection run is mostly neutral until the laser arrives)
         for (int k = 0; k < 3; ++k) { E[k] = A(0); B[k] = A(0); }
-    } else if (F32 && mid && !LASER && !c.ext.any()) {
-        if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy(g, ym), E, B);
+    } else if (F32 && YF && mid && !LASER && !c.ext.any()) {
+        if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy<YF>(g, ym), E, B);
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
-        if (mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy(g, ym), Ed, Bd);
-        else sgather<F32>(c, wrapx(g, xm), wrapy(g, ym), zetam, Ed, Bd);
+        if (mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy<YF>(g, ym), Ed, Bd);
+        else sgather<F32, YF>(c, wrapx(g, xm), wrapy<YF>(g, ym), zetam, Ed, Bd);
         if constexpr (LASER) {
             c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
             for (int k = 0; k < 3; ++k) { Ed[k] += Ee[k]; Bd[k] += Be[k]; }
@@ -395,7 +401,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         S.zeta[i] = zeta_end;
     }
     if constexpr (F32) {
-        if (g.yf) {                   // FP32 deposit: the factor 1 / (Delta h dx) taken once per half-cell
+        if constexpr (YF) {           // FP32 deposit: the factor 1 / (Delta h dx) taken once per half-cell
             const float ff = float(qw * c.dep_norm) * float(dt);
             if (ff != 0.f) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), 0, 0, 0, 0, true, true, ff, {float(vx), float(vy), float(vz)}};
         } else {
@@ -406,18 +412,18 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         const double f = qw * double(dt) / (c.Delta * h * g.dx);
         if (f != 0) d = DepReq{0.5 * (x + xn), 0.5 * (y + yn), f, double(vx), double(vy), double(vz), true, false, 0.f, {0.f, 0.f, 0.f}};
     }
-    if (!g.yf && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
+    if (!YF && (yn < c.ylo || yn > c.yhi)) {        // free-hand y: reached the cell at a wall
         if (!c.dry) S.alive[i] = 0;
         return d;
     }
     if constexpr (ION)
         if (ion && !trapped && c.ions[sp - SP_ION].ionizing)
-            ionize(c, S, i, field_abs<F32>(c, xm, ym, zm, zeta), field_abs<F32>(c, xm, ym, zm, zn), double(dt));
+            ionize(c, S, i, field_abs<F32, YF>(c, xm, ym, zm, zeta), field_abs<F32, YF>(c, xm, ym, zm, zn), double(dt));
     if (trapped) {
         if (!c.dry) S.alive[i] = 5;
         const double vze = double(uz * ig1);
         if (vze >= c.vz_beam)         // joins the beam list: its beam current of level s1 from now on
-            sdeposit<F32>(c, xn, yn, qw / (h * g.dx * vze), double(ux * ig1), double(uy * ig1), vze);
+            sdeposit<F32, YF>(c, xn, yn, qw / (h * g.dx * vze), double(ux * ig1), double(uy * ig1), vze);
     }
     return d;
 }
@@ -431,27 +437,34 @@ constexpr int ST_NT = 128;
 #ifndef G3D_STREAM_MINB
 #define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
 #endif
-template <bool F32, bool ION, bool LASER>
+// YF: the Fourier y grid (true) or the free-hand one, fixed for a run, so that each variant holds only its own grid's
+// gathers and deposits (fewer registers and no local arrays).
+template <bool F32, bool ION, bool LASER, bool YF>
 __global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c,
                                                                                        const long* __restrict__ nstrm) {
     const StrmDev S = c.sd[0];
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
-        const DepReq d = stream_one<F32, ION, LASER>(c, S, i);
+        const DepReq d = stream_one<F32, ION, LASER, YF>(c, S, i);
         if (d.on) {
-            if (F32 && d.f32) sdeposit_f32(c, d.x, d.y, d.ff, d.fv[0], d.fv[1], d.fv[2]);
-            else sdeposit<F32>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
+            if (F32 && YF && d.f32) sdeposit_f32(c, d.x, d.y, d.ff, d.fv[0], d.fv[1], d.fv[2]);
+            else sdeposit<F32, YF>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
         }
     }
 }
-template <bool F32>
-static void stream_launch(Ctx& c, const StreamArgs& a, unsigned blocks) {
+template <bool F32, bool YF>
+static void stream_launch_y(Ctx& c, const StreamArgs& a, unsigned blocks) {
     PlasmaState& P = *c.pl;
     const bool ion = P.any_ionizing, las = c.laser.on != 0;
-    if (ion && las) k_stream<F32, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
-    else if (ion) k_stream<F32, true, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
-    else if (las) k_stream<F32, false, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
-    else k_stream<F32, false, false><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    if (ion && las) k_stream<F32, true, true, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else if (ion) k_stream<F32, true, false, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else if (las) k_stream<F32, false, true, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+    else k_stream<F32, false, false, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+}
+template <bool F32>
+static void stream_launch(Ctx& c, const StreamArgs& a, unsigned blocks) {
+    if (c.yf) stream_launch_y<F32, true>(c, a, blocks);
+    else stream_launch_y<F32, false>(c, a, blocks);
 }
 
 // ---------------------------------------------------------------- spectra of the streaming current
