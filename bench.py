@@ -18,8 +18,10 @@ Both forms are timed on the same inputs; value is the mixed form, fp64_form the 
 relative L2 of F and the relative <p_z> of the mixed form against the FP64 form after the same steps. At N = 1
 the key adjoint holds the adjoint march's cost against the forward and its agreement with central differences on
 workload 4 without its plasma (--no-adjoint skips it).
-Under torchrun (N > 1) every rank runs an independent replica (the march is one serial chain in zeta;
-replicas only), timed on the device, max over ranks; value = pushes of all ranks / that time.
+Under torchrun (N > 1), workloads 3 and 5 (streaming plasma: one serial chain of half-cells) run an independent
+replica per rank (scaling weak); workloads 1 and 2 (no plasma) run ONE window sharded over the ranks in zeta slabs,
+the march on mode pencils through NCCL all-to-alls (FP64 form, scaling strong; --replicas keeps replicas). Timed on
+the device, max over ranks; value = pushes of all ranks / that time.
 --impl reference times the reference GEM-PIC-3D CPU/OpenMP build (oracle/_ref) on the host cores.
 """
 import argparse
@@ -53,7 +55,13 @@ def parse():
                     help="both: time the FP64 form, then the mixed form (the headline) and its error against FP64")
     ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
     ap.add_argument("--particles", type=int, default=None, help="profiling case: fewer macro-particles")
+    ap.add_argument("--replicas", action="store_true", help="N > 1 on workloads 1-2: replicas instead of one sharded run")
     return ap.parse_args()
+
+
+def sharded(a, world):
+    """One window over the ranks (zeta slabs, mode pencils): workloads without plasma on more than one GPU."""
+    return world > 1 and a.workload in (1, 2) and not a.replicas
 
 
 def workload(k, nzeta=None, particles=None):
@@ -79,7 +87,7 @@ def lattice_particles(cfg):
     return cfg.nx * rows * pd["ppc_x"] * pd["ppc_y"] * species
 
 
-def config_json(cfg, k, form="fp64"):
+def config_json(cfg, k, form="fp64", parallelism="replicas"):
     what = (f"{cfg.particles} macro-electrons" if cfg.particles else
             f"{lattice_particles(cfg)} streaming macro-particles per step")
     return {"workload": f"{k}: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, "
@@ -89,7 +97,7 @@ def config_json(cfg, k, form="fp64"):
             "grid_points": cfg.grid_points, "dz": cfg.params["dz"], "sponge": cfg.params.get("sponge", 0),
             "laser_envelope": "flattop" if cfg.params.get("laser_envelope") == 1 else "gaussian",
             "l2": f"inputs larger than L2 (field state {state_bytes(cfg) / 1e9:.2f} GB, F {f_bytes(cfg) / 1e9:.2f} GB)",
-            "parallelism": "replicas"}
+            "parallelism": parallelism}
 
 
 def state_bytes(cfg):
@@ -425,7 +433,11 @@ def time_form(cfg, precision, a, world, dist, local):
     """Init, warm-up, then K device-timed steps of one form; per-kernel event times on the context stream."""
     import torch
     import g3d
-    sim = g3d.Simulation(cfg, precision=precision)
+    comm = None
+    if sharded(a, world):
+        from g3d import shard
+        comm = shard.RankComm(device=f"cuda:{local}")
+    sim = g3d.Simulation(cfg, precision=precision, comm=comm)
     sim.init()
     stream = torch.cuda.ExternalStream(sim.stream_ptr())
     for _ in range(min_warmup(a)):
@@ -433,6 +445,10 @@ def time_form(cfg, precision, a, world, dist, local):
     # pushes per step: the beam list, plus with plasma the streaming particles that cross the window in one march
     S = sim.streaming_count() if cfg.plasma is not None else 0
     P = int(sim.status().np) + S
+    if comm is not None:                       # a sharded run: the pushes of all ranks, as one replica's
+        t = torch.tensor([float(P)], device=f"cuda:{local}")
+        dist.all_reduce(t)
+        P = int(t.item())
     props = torch.cuda.get_device_properties(local)
     bus = getattr(props, "pci_bus_id", None)
     bus = f"{bus:02x}:00.0" if isinstance(bus, int) else None
@@ -469,8 +485,11 @@ def time_form(cfg, precision, a, world, dist, local):
                    "GB/s": (round(algorithmic_bytes(k, cfg, mixed, S) / (t / max(1, n) * 1e-3) / 1e9, 1)
                             if algorithmic_bytes(k, cfg, mixed, S) else None)}
                for k, (n, t) in sorted(prof.items(), key=lambda kv: -kv[1][1])}
-    out = {"sim": sim, "P": P, "stream": stream, "ms": ms, "value": job_rate(P, a.steps, world, ms), "clk": clk,
-           "launches": launches, "prof": prof, "kernels": kernels}
+    reps = 1 if comm is not None else world
+    out = {"sim": sim, "P": P, "stream": stream, "ms": ms, "value": job_rate(P, a.steps, reps, ms), "clk": clk,
+           "launches": launches, "prof": prof, "kernels": kernels, "reps": reps}
+    if comm is not None:
+        out["comm_calls"] = comm.calls
     if S:
         from g3d import configs
         pd = configs.default_plasma()
@@ -536,7 +555,7 @@ def end_to_end(form, a, world, dist):
     x1.synchronize()
     wall = time.perf_counter() - t0
     ems = max_over_ranks(max(x0.elapsed_time(x1), wall * 1e3), dist)
-    return {"value": job_rate(P, a.e2e_steps, world, ems), "unit": UNIT,
+    return {"value": job_rate(P, a.e2e_steps, form.get("reps", world), ems), "unit": UNIT,
             "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb + 19 * 8, "steps": a.e2e_steps,
             "path": "g3d_set_particles (pinned host records) -> g3d_step -> g3d_get_particles + g3d_diagnostics"}
 
@@ -556,13 +575,15 @@ def run_g3d(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg = workload(a.workload, a.nzeta, a.particles)
     forms = ["fp64", "mixed"] if a.precision == "both" else [a.precision]
+    if sharded(a, world):
+        forms = ["fp64"]                        # a sharded run is FP64
     res = {}
     ref_state = None
     err = None
     for prec in forms:
         f = time_form(cfg, prec, a, world, dist, local)
         # the state after warm-up + K steps, for the error of the mixed form against the FP64 form
-        F = f["sim"].array("F")
+        F = f["sim"].array("F") if len(forms) > 1 else None
         d = f["sim"].diagnostics_sums()
         if prec == "fp64":
             ref_state = (F, d)
@@ -597,10 +618,13 @@ def run_g3d(a):
         dist.barrier()
     if rank == 0:
         line = {"metric": METRIC, "value": H["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
-                "warmup": min_warmup(a), "ms_per_step": H["ms"] / a.steps, "higher_is_better": True, "scaling": "weak",
+                "warmup": min_warmup(a), "ms_per_step": H["ms"] / a.steps, "higher_is_better": True,
+                "scaling": "strong" if sharded(a, world) else "weak",
                 "vs_baseline": None, "dtype": "f32+f64 (mixed form)" if mixed else "f64",
                 "data": "synthetic (seeded bunch sampler of the reference)",
-                "config": config_json(cfg, a.workload, head),
+                "config": config_json(cfg, a.workload, head,
+                                      f"zeta slabs x mode pencils over {world} ranks (NCCL all-to-all)"
+                                      if sharded(a, world) else "replicas"),
                 "roofline": roofline(H, cfg, a.workload, mixed),
                 "kernels": H["kernels"], "e2e": H.get("e2e"), "gpu_launches": H["launches"], "clocks": H["clk"],
                 "cpu_baseline": cpu}

@@ -17,6 +17,7 @@ struct Geo {
     int nx, ny, nk, N, a, b, ns, nh;     // nh = ns + 3 planes of the raw deposit
     int H;                               // nx/2 + 1 columns of a half spectrum (k_x = 0 .. nx/2)
     long nkh;                            // ny * H modes of a half-spectrum plane
+    long m0;                             // the first mode of the planes (a mode pencil of a sharded run; else 0)
     int yf, zeta_uniform;
     double dx, dy, Lx, Ly;
     const double *kxd, *kxs, *filt, *maskx;
@@ -116,6 +117,7 @@ struct ProfEntry { std::string name; long launches = 0; double ms = 0; };
 struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 
 struct PlasmaState;               // g3d_plasma.hpp
+struct Shard;                     // g3d_shard.cu
 
 // Buffers of the mixed FP32/FP64 form (k_mixed.cu): complex64 half spectra of E_z, B_z, L and the currents, FP32
 // raw currents; R_x, R_y stay in Ctx::Rx, Ry (complex128), F is float in both forms.
@@ -214,6 +216,16 @@ struct Ctx {
     DevBuf<double> ktab;
     ExtDev ext{0, 0, nullptr, nullptr, nullptr};
     std::vector<g3d_chicane> chicanes;           // thin chicanes (g3d_set_chicanes)
+    // a sharded run (g3d_set_ranks, g3d_shard.cu): this rank's slab and mode pencil, the caller's collectives
+    int rank = 0, world = 1;
+    g3d_comm_fn comm_fn = nullptr;
+    void* comm_user = nullptr;
+    std::unique_ptr<Shard> sh;
+    bool sharded() const { return world > 1; }
+    // sums `count` values at the device pointer `data` across the ranks (nothing on one rank)
+    void all_sum(void* data, long count, int kind);
+    // the all-to-all of device buffers with host byte counts per rank
+    void all_to_all(const void* send, const int64_t* send_bytes, void* recv, const int64_t* recv_bytes);
 
     Ctx();
     ~Ctx();
@@ -272,6 +284,19 @@ void launch_sponge(Ctx& c);
 void launch_real_fields(Ctx& c);
 void launch_comoving(Ctx& c, double beta, double gm2);
 void launch_push(Ctx& c, double s0, double s1);
+void launch_push_range(Ctx& c, double s0, double s1, long i0, long n);
+void launch_march_pencil(Ctx& c, const Geo& g, cpx* const* p, double D);
+void launch_comoving_pencil(Ctx& c, const Geo& g, const cpx* jz, double* cpb, cpx* dpb, cpx* const* out, double beta, double gm2);
+void realloc_slab(Ctx& c);                        // the field buffers of the slab [a, b) (g3d_host.cu)
+void reserve_particles(Ctx& c, long n);           // particle columns for n (contents not kept when they move)
+// a sharded run (g3d_shard.cu)
+void shard_raw_halo(Ctx& c);
+void shard_jz_ghosts(Ctx& c);
+void shard_field_ghosts(Ctx& c);
+void shard_march(Ctx& c, double D);
+void shard_comoving(Ctx& c, double beta, double gm2);
+void shard_exchange_particles(Ctx& c, double s1);
+bool shard_owns(const Ctx& c, double zeta);
 void launch_zero_c(Ctx& c, cpx* p, size_t n);
 void launch_axpy_c(Ctx& c, cpx* y, const cpx* x, double a, size_t n);   // y = y + a x
 void launch_copy_c(Ctx& c, cpx* y, const cpx* x, size_t n);

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <random>
 #include "g3d_plasma.hpp"
+#include "g3d_shard.hpp"
 
 namespace g3d {
 
@@ -87,7 +88,7 @@ void smem_attr(const void* kern, size_t smem) {
 Geo Ctx::geo() const {
     Geo g;
     g.nx = nx; g.ny = ny; g.nk = nk; g.N = N; g.a = a; g.b = b; g.ns = ns; g.nh = ns + 3;
-    g.H = H; g.nkh = nkh;
+    g.H = H; g.nkh = nkh; g.m0 = 0;
     g.yf = yf ? 1 : 0; g.zeta_uniform = zax.uniform;
     g.dx = dx; g.dy = dy; g.Lx = nx * dx; g.Ly = ny * dy;
     g.kxd = kxd.p; g.kxs = kxs.p; g.filt = filt.p; g.maskx = maskx.p;
@@ -346,6 +347,16 @@ static void setup_y_free(Ctx& c, const g3d_grid& G, const g3d_params& P, cudaStr
     c.evf.upload(fwd, s); c.evb.upload(back, s); c.evl.upload(eig, s);
 }
 
+// field buffers of the slab [a, b): real planes of the reference layouts, spectra as half spectra (FP64 form)
+void realloc_slab(Ctx& c) {
+    const cudaStream_t s = c.stream;
+    const size_t pl = size_t(c.nk), ph = size_t(c.nkh), ns = size_t(c.ns);
+    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry}) p->alloc(ns * ph, s);
+    alloc_spectra(c, false);
+    c.F.alloc(6 * (ns + 2) * pl, s);
+    c.rscratch.alloc(ns * ph, s);
+}
+
 static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     if (!G.y_fourier && !G.ynode) throw Error(G3D_ERR_ARG, "free-hand y needs the ny + 1 nodes (ynode)");
     if (!pow2_ok(G.nx) || G.nx < 8 || (G.y_fourier && !pow2_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 512)))
@@ -432,12 +443,7 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
         return t;
     };
     c.twx.upload(tw(nx), s); c.twy.upload(tw(ny), s);
-    // field buffers: real planes of the reference layouts, spectra as half spectra
-    const size_t pl = size_t(c.nk), ph = size_t(c.nkh), ns = size_t(c.ns);
-    for (DevBuf<cpx>* p : {&c.Rx, &c.Ry}) p->alloc(ns * ph, s);
-    alloc_spectra(c, false);
-    c.F.alloc(6 * (ns + 2) * pl, s);
-    c.rscratch.alloc(ns * ph, s);
+    realloc_slab(c);
     c.red.alloc(size_t(297) * 17, s);
     // the plane wave (reference sim_setup.cpp:51-54; eta_c given directly)
     c.laser.on = P.laser_on; c.laser.pol = P.laser_pol; c.laser.env = P.laser_envelope;
@@ -460,7 +466,7 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
 }
 
 // ---------------------------------------------------------------- particles
-static void reserve_particles(Ctx& c, long n) {
+void reserve_particles(Ctx& c, long n) {
     if (n <= c.pcap && c.pcap <= 2 * n + 1024) return;
     const long cap = n + n / 4 + 64;
     c.pbuf_d.alloc(size_t(cap) * 11, c.stream);
@@ -584,8 +590,14 @@ static void load_bunches(Ctx& c, const g3d_grid& G, const g3d_bunch* list, int c
     std::vector<g3d_particle> mine;
     long lost = 0;
     sample_bunches(G, c.P, list, count, mine, lost, c.X0, c.Y0);
+    if (c.sharded()) {                               // every rank samples the beam and keeps the particles of its slab
+        std::vector<g3d_particle> own;
+        for (const g3d_particle& p : mine)
+            if (shard_owns(c, p.zeta)) own.push_back(p);
+        mine.swap(own);
+    }
     set_particles(c, mine.data(), long(mine.size()));
-    c.lost_total += lost;
+    c.lost_total += c.rank == 0 ? lost : 0;          // every rank samples the same beam: its losses count once
     c.nbunch = count > 1 ? count : 1;
 }
 
@@ -599,12 +611,14 @@ static void currents(Ctx& c) {
     if (!c.yf) { launch_deposit_fh(c); launch_cur_fft_fh(c, keep0); return; }
     if (c.mixed) { launch_deposit_f(c); launch_cur_fft_f(c, keep0); return; }
     launch_cur_fft(c, keep0);
+    if (c.sharded()) shard_jz_ghosts(c);
     // one rank: the filtered j_z ghosts of the neighbours are zero (exchange_jz_ghosts, sim_particles.cpp:210-226)
 }
 static void march(Ctx& c, double D) {
     if (c.jk_is_j0) throw Error(G3D_ERR_STATE, "march needs the currents of level s1 (call currents first)");
     if (!c.yf) launch_march_fh(c, D);
     else if (c.mixed) launch_march_f(c, D);
+    else if (c.sharded()) shard_march(c, D);
     else launch_march(c, D);
 }
 static void sponge_and_real_fields(Ctx& c) {
@@ -622,6 +636,7 @@ static void sponge_and_real_fields(Ctx& c) {
     }
     if (c.P.sponge > 0 || c.P.sponge_y > 0) launch_sponge(c);
     launch_real_fields(c);
+    if (c.sharded()) shard_field_ghosts(c);
 }
 // j0 <- jk (sim_fields.cpp:313-315): the buffers are swapped; until the next deposit jk reads as j0.
 static void j0_from_jk(Ctx& c) {
@@ -660,6 +675,7 @@ static void comoving_field(Ctx& c) {
     if (!c.comoving_c_) { c.beta_b = beta; c.gm2_b = gm2; }
     if (!c.yf) launch_comoving_fh(c, beta, gm2);
     else if (c.mixed) launch_comoving_f(c, beta, gm2);
+    else if (c.sharded()) shard_comoving(c, beta, gm2);
     else launch_comoving(c, beta, gm2);
 }
 // Several bunch blocks (reference Simulation::comoving_fields_per_bunch, src/sim_bunches.cpp:223-248): the co-moving
@@ -835,6 +851,7 @@ static void step(Ctx& c, bool sync) {
     if (++c.steps_since_sort >= 16) sort_particles(c);
     window_shift_start(c);
     launch_push(c, c.s, c.s + c.P.dz);
+    if (c.sharded()) shard_exchange_particles(c, c.s + c.P.dz);
     if (c.pl) collect_restreaming(c);
     c.s += c.P.dz; ++c.istep;
     if (c.P.self_fields && c.pl) {
@@ -1102,6 +1119,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     if (c.laser.on) throw Error(G3D_ERR_ARG, "the adjoint march differentiates grid lasers, not the analytic laser");
     if (!c.P.self_fields || c.P.freeze_bunch) throw Error(G3D_ERR_ARG, "the adjoint march needs self fields and a free bunch");
     if (!c.fields_ready || c.istep != 0) throw Error(G3D_ERR_STATE, "the adjoint march starts right after g3d_init");
+    if (c.world > 1) throw Error(G3D_ERR_STATE, "the adjoint march of a sharded run is not built");
     if (c.ext.any() || !c.chicanes.empty())
         throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate external elements or chicanes");
     if (grad_modes && !c.lmode.p) throw Error(G3D_ERR_STATE, "set the laser mode coefficients (g3d_set_laser_modes) before g3d_init");
@@ -1271,10 +1289,10 @@ int guarded(g3d_ctx* ctx, Fn&& fn) {
         if (ctx) ctx->c.err.clear();
         return G3D_OK;
     } catch (const Error& e) {
-        if (ctx) ctx->c.err = e.what();
+        (ctx ? ctx->c.err : g3d::g_create_err) = e.what();
         return e.code;
     } catch (const std::exception& e) {
-        if (ctx) ctx->c.err = e.what();
+        (ctx ? ctx->c.err : g3d::g_create_err) = e.what();
         return G3D_ERR_ARG;
     }
 }
@@ -1387,7 +1405,12 @@ int g3d_push(g3d_ctx* ctx, double s0, double s1) {
 int g3d_comoving_field(g3d_ctx* ctx) {
     return guarded(ctx, [&] { g3d::comoving_field(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
 }
-int g3d_set_precision(g3d_ctx* ctx, int32_t mode) { return guarded(ctx, [&] { g3d::set_precision(ctx->c, mode); }); }
+int g3d_set_precision(g3d_ctx* ctx, int32_t mode) {
+    return guarded(ctx, [&] {
+        if (ctx->c.sharded() && mode != G3D_PREC_FP64) throw Error(G3D_ERR_STATE, "a sharded run is FP64");
+        g3d::set_precision(ctx->c, mode);
+    });
+}
 int g3d_beam_beta_sums_static(g3d_ctx* ctx, double out[2]) {
     return guarded(ctx, [&] {
         if (!out) throw Error(G3D_ERR_ARG, "null output");
@@ -1405,6 +1428,7 @@ int g3d_shift_window(g3d_ctx* ctx, int32_t nxs, int32_t nys) { return guarded(ct
 int g3d_set_plasma(g3d_ctx* ctx, const g3d_plasma* plasma, const g3d_ion* ions, int32_t nions) {
     return guarded(ctx, [&] {
         if (!plasma || nions < 0 || (nions > 0 && !ions)) throw Error(G3D_ERR_ARG, "bad plasma arguments");
+        if (ctx->c.world > 1) throw Error(G3D_ERR_STATE, "a sharded run has no plasma");
         g3d::set_plasma(ctx->c, *plasma, ions, nions);
     });
 }
@@ -1435,9 +1459,41 @@ int g3d_set_external(g3d_ctx* ctx, const g3d_undulator* u, int32_t nu, const g3d
         c.ext = g3d::ExtDev{nu, nm, c.und.p, c.mag.p, c.ktab.p};
     });
 }
+int g3d_set_ranks(g3d_ctx* ctx, int32_t rank, int32_t world, g3d_comm_fn comm, void* user) {
+    return guarded(ctx, [&] { g3d::set_ranks(ctx->c, rank, world, comm, user); });
+}
+int g3d_shard_layout(int32_t nzeta, int64_t nkh, int32_t rank, int32_t world, int64_t out[4]) {
+    return guarded(nullptr, [&] {
+        if (!out || rank < 0 || rank >= world) throw Error(G3D_ERR_ARG, "g3d_shard_layout: bad arguments");
+        const g3d::ShardLayout L(nzeta, long(nkh), world);
+        out[0] = L.a[size_t(rank)]; out[1] = L.a[size_t(rank)] + L.ns[size_t(rank)];
+        out[2] = L.m0[size_t(rank)]; out[3] = L.m0[size_t(rank)] + L.mq[size_t(rank)];
+    });
+}
+int g3d_shard_transpose_plan(int32_t nzeta, int64_t nkh, int32_t rank, int32_t world, const int32_t* kinds, int32_t narrays,
+                             int32_t to_pencil, int64_t elem_bytes, g3d_block* pack, int32_t pack_cap, int32_t* npack,
+                             g3d_block* unpack, int32_t unpack_cap, int32_t* nunpack, int64_t* send_bytes,
+                             int64_t* recv_bytes) {
+    return guarded(nullptr, [&] {
+        if (!npack || !nunpack || !send_bytes || !recv_bytes || rank < 0 || rank >= world)
+            throw Error(G3D_ERR_ARG, "g3d_shard_transpose_plan: bad arguments");
+        const g3d::ShardLayout L(nzeta, long(nkh), world);
+        g3d::ShardPlan pl;
+        g3d::shard_plan(L, rank, kinds, narrays, to_pencil != 0, long(elem_bytes), pl);
+        *npack = int32_t(pl.pack.size()); *nunpack = int32_t(pl.unpack.size());
+        std::copy(pl.send_bytes.begin(), pl.send_bytes.end(), send_bytes);
+        std::copy(pl.recv_bytes.begin(), pl.recv_bytes.end(), recv_bytes);
+        if (int64_t(pl.pack.size()) > pack_cap || int64_t(pl.unpack.size()) > unpack_cap || (!pack && !pl.pack.empty()) ||
+            (!unpack && !pl.unpack.empty()))
+            throw Error(G3D_ERR_CAPACITY, "g3d_shard_transpose_plan: more blocks than the capacity");
+        std::copy(pl.pack.begin(), pl.pack.end(), pack);
+        std::copy(pl.unpack.begin(), pl.unpack.end(), unpack);
+    });
+}
 int g3d_set_chicanes(g3d_ctx* ctx, const g3d_chicane* ch, int32_t n) {
     return guarded(ctx, [&] {
         if (n < 0 || (n && !ch)) throw Error(G3D_ERR_ARG, "g3d_set_chicanes: bad chicane array");
+        if (n && ctx->c.sharded()) throw Error(G3D_ERR_STATE, "g3d_set_chicanes: a sharded run has no chicanes");
         for (int k = 0; k < n; ++k)
             if (!(ch[k].gamma_ref > 1)) throw Error(G3D_ERR_ARG, "g3d_set_chicanes: the reference gamma must be > 1");
         ctx->c.chicanes.assign(ch, ch + n);
@@ -1468,6 +1524,14 @@ int g3d_diagnostics(g3d_ctx* ctx, double out[19]) {
         g3d::launch_diag(c, S);
         S[15] = c.P.self_fields ? g3d::launch_field_energy(c) : 0;
         S[16] = double(c.lost_total);
+        if (c.sharded()) {                               // the particles lost on every rank
+            g3d::DevBuf<double> lost;
+            lost.alloc(1, c.stream);
+            G3D_CUDA(cudaMemcpyAsync(lost.p, &S[16], sizeof(double), cudaMemcpyHostToDevice, c.stream));
+            c.all_sum(lost.p, 1, G3D_SUM_F64);
+            G3D_CUDA(cudaMemcpyAsync(&S[16], lost.p, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+            G3D_CUDA(cudaStreamSynchronize(c.stream));
+        }
         c.field_energy = S[15];
         // stop condition of the analytic laser (sim_output.cpp:30-31)
         const double w = S[0] > 0 ? S[0] : 1;
@@ -1526,8 +1590,18 @@ void* g3d_device_ptr(g3d_ctx* ctx, int32_t which) {
     return p;
 }
 
-int g3d_write_checkpoint(g3d_ctx* ctx, const char* path) { return guarded(ctx, [&] { g3d::write_checkpoint(ctx->c, path); }); }
-int g3d_read_checkpoint(g3d_ctx* ctx, const char* path) { return guarded(ctx, [&] { g3d::read_checkpoint(ctx->c, path); }); }
+int g3d_write_checkpoint(g3d_ctx* ctx, const char* path) {
+    return guarded(ctx, [&] {
+        if (ctx->c.world > 1) throw Error(G3D_ERR_STATE, "checkpoints of a sharded run are not written");
+        g3d::write_checkpoint(ctx->c, path);
+    });
+}
+int g3d_read_checkpoint(g3d_ctx* ctx, const char* path) {
+    return guarded(ctx, [&] {
+        if (ctx->c.world > 1) throw Error(G3D_ERR_STATE, "checkpoints of a sharded run are not read");
+        g3d::read_checkpoint(ctx->c, path);
+    });
+}
 
 void* g3d_stream(g3d_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
 int g3d_synchronize(g3d_ctx* ctx) {
@@ -1552,7 +1626,12 @@ int g3d_profile_get(g3d_ctx* ctx, int32_t k, const char** name, int64_t* launche
 int64_t g3d_launch_count(const g3d_ctx* ctx) { return ctx ? ctx->c.launches : 0; }
 
 int g3d_set_laser_modes(g3d_ctx* ctx, const double* coef) { return guarded(ctx, [&] { g3d::set_laser_modes(ctx->c, coef); }); }
-int g3d_set_exact_fields(g3d_ctx* ctx, int32_t on) { return guarded(ctx, [&] { g3d::set_exact_fields(ctx->c, on != 0); }); }
+int g3d_set_exact_fields(g3d_ctx* ctx, int32_t on) {
+    return guarded(ctx, [&] {
+        if (on && ctx->c.sharded()) throw Error(G3D_ERR_STATE, "g3d_set_exact_fields: not in a sharded run");
+        g3d::set_exact_fields(ctx->c, on != 0);
+    });
+}
 int g3d_set_adjoint_momenta(g3d_ctx* ctx, int32_t mode) { return guarded(ctx, [&] { g3d::set_adjoint_momenta(ctx->c, mode); }); }
 int g3d_adjoint(g3d_ctx* ctx, int32_t nsteps, double* objective, double* grad_modes, double* grad_p) {
     return guarded(ctx, [&] {

@@ -607,7 +607,7 @@ void add_grid_lasers(Ctx& c) {
         const std::complex<double> rot(std::cos(Lz.pol_angle), std::sin(Lz.pol_angle));
         std::vector<double> cre(size_t(c.ns), 0.0), cim(size_t(c.ns), 0.0);
         for (int n = 0; n < c.ns; ++n) {
-            const double d = c.zeta[size_t(n)] - Lz.zeta_c;
+            const double d = c.zeta[size_t(c.a + n)] - Lz.zeta_c;
             const double env = std::exp(-2 * std::log(2.0) * d * d / (Lz.tau * Lz.tau));
             if (std::fabs(env) < 1e-12) continue;
             const std::complex<double> car = std::exp(std::complex<double>(0, Lz.kL * d + Lz.cep));

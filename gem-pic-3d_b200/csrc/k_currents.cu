@@ -57,14 +57,15 @@ __global__ void __launch_bounds__(DT) k_dep_bound(PartsDev P, long np, Geo g, do
     for (long i = long(blockIdx.x) * DT + threadIdx.x; i < np; i += long(gridDim.x) * DT) dep_bound_one(P, i, g, ia_max, acc);
     block_sum3(acc, part + 3 * blockIdx.x);
 }
-// scale[c] = 2^e_c, scale[3 + c] = 2^-e_c
-__global__ void __launch_bounds__(DT) k_dep_scale(const double* __restrict__ part, double* __restrict__ scale) {
+// the bound's three totals into tot[0..2]
+__global__ void __launch_bounds__(DT) k_dep_total(const double* __restrict__ part, double* __restrict__ tot) {
     double acc[3] = {0, 0, 0};
     for (int b = threadIdx.x; b < DB; b += DT)
         for (int k = 0; k < 3; ++k) acc[k] += part[3 * b + k];
-    __shared__ double tot[3];
     block_sum3(acc, tot);
-    __syncthreads();
+}
+// scale[c] = 2^e_c, scale[3 + c] = 2^-e_c from the totals
+__global__ void k_dep_scale(const double* __restrict__ tot, double* __restrict__ scale) {
     if (threadIdx.x < 3) {
         const double B = tot[threadIdx.x] * (1 + 1e-12) + 1e-300;   // the rounding of the bound's own sum; never 0
         int x;
@@ -225,10 +226,14 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
 // the scales 2^e_c, 2^-e_c of the fixed-point deposit (six values; ia_max: the largest dual-cell factor); returns
 // where they are
 const double* launch_deposit_scale(Ctx& c, double ia_max) {
-    if (c.depfix.n < size_t(3 * DB + 6)) c.depfix.alloc(size_t(3 * DB + 6), c.stream);
+    if (c.depfix.n < size_t(3 * DB + 9)) c.depfix.alloc(size_t(3 * DB + 9), c.stream);
+    double* tot = c.depfix.p + 3 * DB + 6;
     k_dep_bound<<<DB, DT, 0, c.stream>>>(c.parts, c.np, c.geo(), ia_max, c.depfix.p);
     c.check_launch("k_dep_bound");
-    k_dep_scale<<<1, DT, 0, c.stream>>>(c.depfix.p, c.depfix.p + 3 * DB);
+    k_dep_total<<<1, DT, 0, c.stream>>>(c.depfix.p, tot);
+    c.check_launch("k_dep_total");
+    c.all_sum(tot, 3, G3D_SUM_F64);                      // a sharded run: the bound of every rank's particles
+    k_dep_scale<<<1, 32, 0, c.stream>>>(tot, c.depfix.p + 3 * DB);
     c.check_launch("k_dep_scale");
     return c.depfix.p + 3 * DB;
 }
@@ -241,13 +246,16 @@ void launch_deposit_finish(Ctx& c) {
 }
 void launch_deposit(Ctx& c) {
     c.jw.zero(c.stream);
-    if (c.np == 0) return;
+    if (c.np == 0 && !c.sharded()) return;           // a sharded rank without particles still takes part in the sums
     const int tok = c.prof_begin("deposit");
     const double* scale = launch_deposit_scale(c, 1 / c.dy);
-    const unsigned blocks = unsigned((c.np + 255) / 256);
-    k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
-    c.check_launch("k_deposit");
+    if (c.np > 0) {
+        const unsigned blocks = unsigned((c.np + 255) / 256);
+        k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
+        c.check_launch("k_deposit");
+    }
     launch_deposit_finish(c);
+    if (c.sharded()) shard_raw_halo(c);
     c.prof_end(tok);
 }
 

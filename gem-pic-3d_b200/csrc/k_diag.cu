@@ -161,10 +161,12 @@ __global__ void __launch_bounds__(RT) k_moments(PartsDev P, long np, double X0, 
     block_store<MOM_NV>(acc, part);
 }
 
+// `sum`: a sum over the particles, which a sharded run adds across the ranks
 template <int NV>
-void finish(Ctx& c, double* out) {
+void finish(Ctx& c, double* out, bool sum) {
     k_final<NV><<<1, RT, 0, c.stream>>>(c.red.p, RB, c.red.p + RB * NV);
     c.check_launch("k_final");
+    if (sum) c.all_sum(c.red.p + RB * NV, NV, G3D_SUM_F64);
     G3D_CUDA(cudaMemcpyAsync(out, c.red.p + RB * NV, NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }
@@ -177,7 +179,7 @@ void launch_diag(Ctx& c, double S[19]) {
     k_diag<<<RB, RT, 0, c.stream>>>(c.parts, c.np, d, c.red.p);
     c.check_launch("k_diag");
     c.prof_end(tok);
-    finish<NDIAG>(c, r);
+    finish<NDIAG>(c, r, true);
     for (int k = 0; k < 15; ++k) S[k] = r[k];
     S[17] = r[15]; S[18] = r[16];
 }
@@ -188,7 +190,7 @@ double launch_field_energy(Ctx& c) {
     k_energy<<<RB, RT, 0, c.stream>>>(c.geo(), c.F.p, c.red.p);
     c.check_launch("k_energy");
     c.prof_end(tok);
-    finish<1>(c, r);
+    finish<1>(c, r, true);                    // a sharded run: the energies of the slabs
     return r[0] * c.dx;
 }
 
@@ -205,6 +207,7 @@ void launch_beam_moments(Ctx& c, double* s1, double* s2) {
     c.check_launch("k_moments");
     k_final<MOM_NV><<<1, RT, 0, c.stream>>>(part, RB, tot);
     c.check_launch("k_final");
+    c.all_sum(tot, MOM_NV, G3D_SUM_F64);
     G3D_CUDA(cudaMemcpyAsync(r.data(), tot, MOM_NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     for (int g = 0; g < G; ++g) {
@@ -216,6 +219,7 @@ void launch_beam_moments(Ctx& c, double* s1, double* s2) {
     c.check_launch("k_moments");
     k_final<MOM_NV><<<1, RT, 0, c.stream>>>(part, RB, tot);
     c.check_launch("k_final");
+    c.all_sum(tot, MOM_NV, G3D_SUM_F64);
     G3D_CUDA(cudaMemcpyAsync(r.data(), tot, MOM_NV * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
     for (int g = 0; g < G; ++g)
@@ -225,18 +229,21 @@ void launch_beam_moments(Ctx& c, double* s1, double* s2) {
 void launch_centroid(Ctx& c, double out[3]) {
     k_centroid<<<RB, RT, 0, c.stream>>>(c.parts, c.np, c.X0, c.Y0, c.red.p);
     c.check_launch("k_centroid");
-    finish<3>(c, out);
+    finish<3>(c, out, true);
 }
 
 void launch_beta_sums(Ctx& c, double out[2]) {
     out[0] = out[1] = 0;
-    if (c.np == 0) return;
+    if (c.np == 0 && !c.sharded()) return;
     DevBuf<double> tw;
-    tw.alloc(size_t(2 * c.np + 2), c.stream);
-    k_beta_terms<<<RB, RT, 0, c.stream>>>(c.parts, c.np, tw.p, tw.p + c.np);
-    c.check_launch("k_beta_terms");
-    k_seq_sum2<<<1, 32, 0, c.stream>>>(tw.p, tw.p + c.np, c.np, c.parts.alive, tw.p + 2 * c.np);
-    c.check_launch("k_seq_sum2");
+    tw.alloc(size_t(2 * c.np + 2), c.stream);                       // zeroed: a rank without particles adds 0
+    if (c.np > 0) {
+        k_beta_terms<<<RB, RT, 0, c.stream>>>(c.parts, c.np, tw.p, tw.p + c.np);
+        c.check_launch("k_beta_terms");
+        k_seq_sum2<<<1, 32, 0, c.stream>>>(tw.p, tw.p + c.np, c.np, c.parts.alive, tw.p + 2 * c.np);
+        c.check_launch("k_seq_sum2");
+    }
+    c.all_sum(tw.p + 2 * c.np, 2, G3D_SUM_F64);   // a sharded run: the ranks' sums in rank order of the reducer
     G3D_CUDA(cudaMemcpyAsync(out, tw.p + 2 * c.np, 2 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     G3D_CUDA(cudaStreamSynchronize(c.stream));
 }

@@ -522,11 +522,13 @@ static unsigned ew_blocks(long n) {
 
 void launch_deposit_fh(Ctx& c) {
     c.jw.zero(c.stream);
-    if (c.np == 0) return;
+    if (c.np == 0 && !c.sharded()) return;
     const int tok = c.prof_begin("deposit");
     const double* scale = launch_deposit_scale(c, c.ia_max);
-    k_deposit_fh<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
-    c.check_launch("k_deposit_fh");
+    if (c.np > 0) {
+        k_deposit_fh<<<unsigned((c.np + 255) / 256), 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
+        c.check_launch("k_deposit_fh");
+    }
     launch_deposit_finish(c);
     c.prof_end(tok);
 }

@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
     const long i = gt >> 1;                   // mode
     const bool live = i < nk;
     const long ii = live ? i : 0;             // idle lanes stream mode 0 and store nothing
-    const int kxi = int(ii % g.H), j = int(ii / g.H);
+    const int kxi = int((g.m0 + ii) % g.H), j = int((g.m0 + ii) / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky;
     const double sgn = c ? 1.0 : -1.0;        // (i z)_c = sgn z_(1-c)
     // element offsets of the own component (R, L, j_perp) and of the other one (E_z, B_z, j_z)
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(128) k_comoving(Geo g, const cpx* __restrict__
     const long nk = g.nkh;
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= nk) return;
-    const int kxi = int(i % g.H), j = int(i / g.H);
+    const int kxi = int((g.m0 + i) % g.H), j = int((g.m0 + i) / g.H);
     const double kx = g.kxd[kxi], ky = g.kyd[j];
     const double ev = ky * ky;                      // Fourier y: the eigenvalue of -Lap_y is k_y^2
     double cprev = 0;
@@ -227,21 +227,32 @@ __global__ void __launch_bounds__(128) k_comoving(Geo g, const cpx* __restrict__
 // 128 x 128 grid has 8,320 half-spectrum modes, 16,640 lanes), else 64. The mixed form streams 44 bytes per lane
 // and slice instead of 72, so it keeps more slices in flight for the same bytes.
 template <class T, int BT, int DEPTH>
-static void march_launch(Ctx& c, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x, const T* j0y, const T* jkx,
-                         const T* jky, const T* jkz, double D) {
-    const unsigned blocks = unsigned((2 * c.nkh + BT - 1) / BT);
+static void march_launch(Ctx& c, const Geo& g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x, const T* j0y,
+                         const T* jkx, const T* jky, const T* jkz, double D) {
+    const unsigned blocks = unsigned((2 * g.nkh + BT - 1) / BT);
+    if (blocks == 0) return;
     const size_t smem = size_t(DEPTH) * slot_doubles(BT) * sizeof(double);
     smem_attr(reinterpret_cast<const void*>(k_march<T, BT, DEPTH>), smem);
-    k_march<T, BT, DEPTH><<<blocks, BT, smem, c.stream>>>(c.geo(), Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
+    k_march<T, BT, DEPTH><<<blocks, BT, smem, c.stream>>>(g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
 }
-static bool narrow_blocks(const Ctx& c) { return 2 * c.nkh < 2L * 148 * 64; }
+template <class T, int DEPTH>
+static void march_any(Ctx& c, const Geo& g, cpx* Rx, cpx* Ry, T* Ez, T* Bz, T* Lx, T* Ly, const T* j0x, const T* j0y,
+                      const T* jkx, const T* jky, const T* jkz, double D) {
+    if (2 * g.nkh < 2L * 148 * 64) march_launch<T, 32, DEPTH>(c, g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
+    else march_launch<T, 64, DEPTH>(c, g, Rx, Ry, Ez, Bz, Lx, Ly, j0x, j0y, jkx, jky, jkz, D);
+}
 
 void launch_march(Ctx& c, double D) {
     const int tok = c.prof_begin("march");
-    if (narrow_blocks(c))
-        march_launch<cpx, 32, 6>(c, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D);
-    else
-        march_launch<cpx, 64, 6>(c, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D);
+    march_any<cpx, 6>(c, c.geo(), c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p, D);
+    c.check_launch("k_march");
+    c.prof_end(tok);
+}
+// the march of a mode pencil (a sharded run): all N slices of the modes [g.m0, g.m0 + g.nkh), arrays in the order
+// R_x, R_y, E_z, B_z, L_x, L_y, j0x, j0y, jkx, jky, jkz
+void launch_march_pencil(Ctx& c, const Geo& g, cpx* const* p, double D) {
+    const int tok = c.prof_begin("march");
+    march_any<cpx, 6>(c, g, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9], p[10], D);
     c.check_launch("k_march");
     c.prof_end(tok);
 }
@@ -249,20 +260,26 @@ void launch_march(Ctx& c, double D) {
 void launch_march_f(Ctx& c, double D) {
     const int tok = c.prof_begin("march");
     MixedBufs& m = c.mx;
-    if (narrow_blocks(c))
-        march_launch<cpxf, 32, 10>(c, c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p, m.jkx.p, m.jky.p, m.jkz.p, D);
-    else
-        march_launch<cpxf, 64, 10>(c, c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p, m.jkx.p, m.jky.p, m.jkz.p, D);
+    march_any<cpxf, 10>(c, c.geo(), c.Rx.p, c.Ry.p, m.Ez.p, m.Bz.p, m.Lx.p, m.Ly.p, m.j0x.p, m.j0y.p, m.jkx.p, m.jky.p, m.jkz.p, D);
     c.check_launch("k_march_f");
     c.prof_end(tok);
 }
 
-void launch_comoving(Ctx& c, double beta, double gm2) {
+static void comoving_launch(Ctx& c, const Geo& g, const cpx* jz, double* cpb, cpx* dpb, cpx* Rx, cpx* Ry, cpx* Ez, cpx* Bz,
+                            double beta, double gm2) {
     const int tok = c.prof_begin("comoving");
-    const unsigned blocks = unsigned((c.nkh + 127) / 128);
-    k_comoving<<<blocks, 128, 0, c.stream>>>(c.geo(), c.jkz.p, c.rscratch.p, c.W[3].p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, beta, gm2);
+    const unsigned blocks = unsigned((g.nkh + 127) / 128);
+    if (blocks) k_comoving<<<blocks, 128, 0, c.stream>>>(g, jz, cpb, dpb, Rx, Ry, Ez, Bz, beta, gm2);
     c.check_launch("k_comoving");
     c.prof_end(tok);
+}
+void launch_comoving(Ctx& c, double beta, double gm2) {
+    comoving_launch(c, c.geo(), c.jkz.p, c.rscratch.p, c.W[3].p, c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, beta, gm2);
+}
+// the co-moving solve of a mode pencil: j_z (N + 1 half cells) in, R_x, R_y, E_z, B_z (N slices) out
+void launch_comoving_pencil(Ctx& c, const Geo& g, const cpx* jz, double* cpb, cpx* dpb, cpx* const* out, double beta,
+                            double gm2) {
+    comoving_launch(c, g, jz, cpb, dpb, out[0], out[1], out[2], out[3], beta, gm2);
 }
 
 }  // namespace g3d

@@ -9,12 +9,13 @@
 namespace g3d {
 
 // RK4 from z0 to the plane s1 (reference push_one, src/sim_kernels.hpp:98-149).
+// perm: the particles in cell order, or null for the particles [i0, i0 + np) in storage order
 template <class FT>
 __global__ void __launch_bounds__(128, 4) k_push(PushArgs c, const FT* __restrict__ Fp, PartsDev P, const int32_t* __restrict__ perm,
-                                                long np, double s0) {
+                                                long i0, long np, double s0) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= np) return;
-    const long ip = perm[t];                 // cell order: the warp's particles gather the same planes of F
+    const long ip = perm ? perm[t] : i0 + t;     // cell order: the warp's particles gather the same planes of F
     const int alive = P.alive[ip];
     if (alive != 1 && alive != 3) return;
     const double s1 = c.s1;
@@ -52,7 +53,8 @@ PushArgs push_args(Ctx& c, double s1) {
     PushArgs a;
     a.F = c.F.p; a.Fd = c.Fd.p; a.g = c.geo(); a.laser = c.laser;
     a.X0 = c.X0; a.Y0 = c.Y0; a.zc = c.P.zeta_center; a.dz_push = c.P.dz_push; a.push_phase = c.P.push_phase;
-    a.zhand = -1e300;                                   // one rank: nothing is handed over
+    // a sharded run: particles below zeta[a + 1] go to the rank below (sim_particles.cpp:10); rank 0 keeps all
+    a.zhand = c.sharded() && c.rank > 0 ? c.zeta[size_t(c.a) + 1] : -1e300;
     a.zmax = c.zeta[c.N - 1]; a.s1 = s1; a.hmin = c.hmin;
     a.ylo = c.yf ? -1e300 : c.ynode_h[1];              // free-hand y: lost within one cell of a wall
     a.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
@@ -61,14 +63,17 @@ PushArgs push_args(Ctx& c, double s1) {
     a.ext = c.ext;
     return a;
 }
-void launch_push(Ctx& c, double s0, double s1) {
-    if (c.np == 0) return;
+static void push_launch(Ctx& c, double s0, double s1, const int32_t* perm, long i0, long n) {
+    if (n <= 0) return;
     const PushArgs a = push_args(c, s1);
     const int tok = c.prof_begin("push");
-    if (c.Fd.p) k_push<double><<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.Fd.p, c.parts, c.perm.p, c.np, s0);
-    else k_push<float><<<unsigned((c.np + 127) / 128), 128, 0, c.stream>>>(a, c.F.p, c.parts, c.perm.p, c.np, s0);
+    if (c.Fd.p) k_push<double><<<unsigned((n + 127) / 128), 128, 0, c.stream>>>(a, c.Fd.p, c.parts, perm, i0, n, s0);
+    else k_push<float><<<unsigned((n + 127) / 128), 128, 0, c.stream>>>(a, c.F.p, c.parts, perm, i0, n, s0);
     c.check_launch("k_push");
     c.prof_end(tok);
 }
+void launch_push(Ctx& c, double s0, double s1) { push_launch(c, s0, s1, c.perm.p, 0, c.np); }
+// the particles [i0, i0 + n) in storage order (those adopted from the rank above finish their push)
+void launch_push_range(Ctx& c, double s0, double s1, long i0, long n) { push_launch(c, s0, s1, nullptr, i0, n); }
 
 }  // namespace g3d

@@ -94,6 +94,25 @@ class Chicane(C.Structure):
     _fields_ = [("z", C.c_double), ("r56", C.c_double), ("delay", C.c_double), ("gamma_ref", C.c_double)]
 
 
+class CommOp(C.Structure):
+    """struct g3d_comm_op: one collective the library asks of the caller (a sharded run)."""
+    _fields_ = [("op", C.c_int32), ("kind", C.c_int32), ("count", C.c_int64), ("data", C.c_void_p),
+                ("send", C.c_void_p), ("send_bytes", C.POINTER(C.c_int64)), ("recv", C.c_void_p),
+                ("recv_bytes", C.POINTER(C.c_int64))]
+
+
+class Block(C.Structure):
+    """struct g3d_block: one copy of a slab <-> pencil transpose."""
+    _fields_ = [("src", C.c_int64), ("dst", C.c_int64), ("rows", C.c_int64), ("cols", C.c_int64),
+                ("src_stride", C.c_int64), ("dst_stride", C.c_int64), ("src_array", C.c_int32), ("dst_array", C.c_int32)]
+
+
+G3D_COMM_SUM, G3D_COMM_ALLTOALL = 0, 1
+G3D_SUM_F64, G3D_SUM_I64 = 0, 1
+G3D_SLAB_NODES, G3D_SLAB_HALF = 0, 1
+COMM_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(CommOp))
+
+assert C.sizeof(CommOp) == 56 and C.sizeof(Block) == 56
 assert C.sizeof(Undulator) == 64 and C.sizeof(Magnet) == 56 and C.sizeof(Chicane) == 32
 assert C.sizeof(Grid) == 48 and C.sizeof(Params) == 200 and C.sizeof(Bunch) == 136 and C.sizeof(Status) == 80
 
@@ -119,6 +138,11 @@ SIGNATURES = [
     ("g3d_add_grid_laser", _I, [_P, C.POINTER(GridLaser)]),
     ("g3d_set_external", _I, [_P, C.POINTER(Undulator), _I32, C.POINTER(Magnet), _I32, C.POINTER(_D), _I32]),
     ("g3d_set_chicanes", _I, [_P, C.POINTER(Chicane), _I32]),
+    ("g3d_set_ranks", _I, [_P, _I32, _I32, COMM_FN, _P]),
+    ("g3d_shard_layout", _I, [_I32, _I64, _I32, _I32, C.POINTER(_I64)]),
+    ("g3d_shard_transpose_plan", _I, [_I32, _I64, _I32, _I32, C.POINTER(_I32), _I32, _I32, _I64, C.POINTER(Block), _I32,
+                                      C.POINTER(_I32), C.POINTER(Block), _I32, C.POINTER(_I32), C.POINTER(_I64),
+                                      C.POINTER(_I64)]),
     ("g3d_march_plasma", _I, [_P, _D, _D]),
     ("g3d_get_streaming", _I, [_P, _P, _I64, C.POINTER(_I64)]),
     ("g3d_init", _I, [_P]),

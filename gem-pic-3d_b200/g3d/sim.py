@@ -44,7 +44,9 @@ class Simulation:
     """One march context on the current CUDA device. precision: "fp64" (the reference's arithmetic) or "mixed"
     (FP32 transforms, currents, gathers and E_z/B_z/L storage with the FP64 accumulator R and FP64 particles)."""
 
-    def __init__(self, cfg, lib=None, precision="fp64"):
+    def __init__(self, cfg, lib=None, precision="fp64", comm=None):
+        """comm: a shard.RankComm for a run sharded over the ranks of a process group (zeta slabs; FP64, Fourier y,
+        no plasma), or None for the whole window on this device."""
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
         self.lib = lib or abi.load_library()
@@ -57,6 +59,14 @@ class Simulation:
             raise G3DError(rc, self.lib.g3d_last_error(None).decode(errors="replace"))
         self.ctx = h
         self.precision = precision
+        self.comm = comm
+        self.a = 0
+        self.ns = cfg.nzeta
+        if comm is not None:
+            self._c(self.lib.g3d_set_ranks(self.ctx, comm.rank, comm.world, comm.fn, None))
+            from . import shard
+            self.a, b, _, _ = shard.layout(cfg.nzeta, cfg.ny * (cfg.nx // 2 + 1), comm.rank, comm.world, self.lib)
+            self.ns = b - self.a
         if precision == "mixed":
             self._c(self.lib.g3d_set_precision(self.ctx, abi.G3D_PREC_MIXED))
         ps = cfg.plasma_structs()
@@ -69,7 +79,6 @@ class Simulation:
             self.set_external(cfg.undulators, cfg.magnets, getattr(cfg, "ktab", None))
         self.N, self.nx, self.ny = cfg.nzeta, cfg.nx, cfg.ny
         self.nk = cfg.nx * cfg.ny
-        self.ns = cfg.nzeta
 
     def set_external(self, undulators=(), magnets=(), ktab=None):
         """External magnetic elements (dicts of the g3d_undulator / g3d_magnet fields, code units; ktab: the taper
@@ -106,6 +115,9 @@ class Simulation:
             pass
 
     def _c(self, rc):
+        if rc != abi.G3D_OK and getattr(self, "comm", None) is not None and self.comm.error is not None:
+            err, self.comm.error = self.comm.error, None
+            raise G3DError(rc, f"{self.lib.g3d_last_error(self.ctx).decode(errors='replace')}: {err!r}") from err
         _check(self.lib, self.ctx, rc)
 
     # ------------------------------------------------------------ particles

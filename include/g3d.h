@@ -228,6 +228,66 @@ int g3d_set_external(struct g3d_ctx* ctx, const g3d_undulator* undulators, int32
  * the start. */
 int g3d_set_chicanes(struct g3d_ctx* ctx, const g3d_chicane* chicanes, int32_t n);
 
+/* ------------------------------------------------------------------ sharded runs (zeta slabs over ranks)
+ * The reference's MPI zeta decomposition (Simulation::Simulation, src/sim_setup.cpp:9-15; Comm, src/comm.hpp:11-46)
+ * with its march over the ranks replaced by a transpose: rank r of `world` holds the slices [a, b) of the window
+ * (the reference's split: N / world each, the first N % world ranks one more, at least 4) and its beam particles
+ * (zeta >= zeta[a + 1] below the next rank's bound; rank 0 everything below), and pushes, deposits, transforms,
+ * sponges and turns into real fields only those. The march and the co-moving solve, serial in zeta but independent
+ * per mode, run on mode pencils: before them an all-to-all moves the slab's planes of the modes [m0, m1) of every
+ * rank to that rank, which then holds all N slices of its modes; after them a second all-to-all moves the results
+ * back. Between neighbours, as in the reference: the three top raw current half-cells go up (sim_particles.cpp:
+ * 108-119), the filtered j_z ghost half-cells both ways (:210-226), the two lowest real-field slices down
+ * (sim_fields.cpp:295-306), and the particles that crossed below zeta[a + 1] down, which finish their push there
+ * (sim_particles.cpp:28-48). Sums over the ranks: the deposit's bound (its fixed-point scale is then global, so the
+ * current planes are those of one rank holding every particle), the beta sums, the centroid, the diagnostics (the
+ * field energy of the slabs and the particles lost in the exchange included) and the beam moments.
+ *
+ * The library does no communication itself: it calls the caller's `comm` function on the context's thread, its stream
+ * synchronized, with DEVICE buffers (G3D_COMM_SUM: `count` values at `data` replaced by their sum over the ranks,
+ * `kind` G3D_SUM_F64 or G3D_SUM_I64; G3D_COMM_ALLTOALL: `send` holds world blocks of send_bytes[q] bytes, the q-th for
+ * rank q, and `recv` receives world blocks of recv_bytes[r] bytes, the r-th from rank r; host count arrays). It
+ * returns 0, or non-zero to fail the call with G3D_ERR_CUDA. Every rank makes the same calls in the same order, so
+ * the library's collectives match. g3d_set_ranks comes after g3d_create and before particles are loaded; the run
+ * must be FP64 with Fourier y and without plasma, chicanes, checkpoints or the adjoint march (G3D_ERR_STATE). What
+ * stays this rank's own: the arrays of g3d_get_array (this slab's planes), g3d_get_particles, g3d_set_particles (the
+ * caller gives this rank's particles), g3d_get_status and g3d_beam_beta_sums_static. */
+#define G3D_COMM_SUM 0
+#define G3D_COMM_ALLTOALL 1
+#define G3D_SUM_F64 0
+#define G3D_SUM_I64 1
+typedef struct g3d_comm_op {
+    int32_t op, kind;                            /* G3D_COMM_*, G3D_SUM_* */
+    int64_t count;                               /* G3D_COMM_SUM: values at data */
+    void* data;
+    const void* send;                            /* G3D_COMM_ALLTOALL */
+    const int64_t* send_bytes;                   /* [world] */
+    void* recv;
+    const int64_t* recv_bytes;                   /* [world] */
+} g3d_comm_op;
+typedef int (*g3d_comm_fn)(void* user, const g3d_comm_op* op);
+int g3d_set_ranks(struct g3d_ctx* ctx, int32_t rank, int32_t world, g3d_comm_fn comm, void* user);
+/* The partition, host arithmetic only: out = {a, b, m0, m1}, the slab [a, b) of the nzeta slices and the pencil
+ * [m0, m1) of the nkh = ny (nx/2 + 1) stored modes of rank `rank` of `world` (G3D_ERR_ARG below 4 slices a rank). */
+int g3d_shard_layout(int32_t nzeta, int64_t nkh, int32_t rank, int32_t world, int64_t out[4]);
+/* One copy of a transpose: `rows` rows of `cols` elements from src (row stride src_stride) to dst (dst_stride),
+ * offsets in elements; an array index of -1 is the send (pack) or receive (unpack) buffer, else the index into the
+ * list of arrays given to g3d_shard_transpose_plan. */
+typedef struct g3d_block {
+    int64_t src, dst, rows, cols, src_stride, dst_stride;
+    int32_t src_array, dst_array;
+} g3d_block;
+#define G3D_SLAB_NODES 0                          /* a slab array of ns planes (slices a .. b-1) */
+#define G3D_SLAB_HALF 1                           /* of ns + 1 half-cell planes (a - 1/2 .. b - 1/2) */
+/* The plan of the slab -> pencil transpose (to_pencil = 1) or back (0) of `narrays` arrays of the given kinds, on rank
+ * `rank`: the copies into the send buffer (pack), the copies out of the receive buffer (unpack) and the byte counts of
+ * the all-to-all for an element of elem_bytes. A pencil array holds N (nodes) or N + 1 (half cells) planes of m1 - m0
+ * modes. A plan with more blocks than the capacity fails with G3D_ERR_CAPACITY and sets the counts. */
+int g3d_shard_transpose_plan(int32_t nzeta, int64_t nkh, int32_t rank, int32_t world, const int32_t* kinds, int32_t narrays,
+                             int32_t to_pencil, int64_t elem_bytes, g3d_block* pack, int32_t pack_cap, int32_t* npack,
+                             g3d_block* unpack, int32_t unpack_cap, int32_t* nunpack, int64_t* send_bytes,
+                             int64_t* recv_bytes);
+
 /* ------------------------------------------------------------------ the march path */
 int g3d_init(struct g3d_ctx* ctx);                  /* Simulation::init, sim_setup.cpp:178-197 (after loading) */
 int g3d_step(struct g3d_ctx* ctx);                  /* Simulation::step, sim_setup.cpp:199-217 */
