@@ -49,8 +49,8 @@ struct StreamArgs {
     const void* Fmid;          // Fourier y: the six fields half-way between slices n and n+1, interleaved per point
                                // (FP32: 8 floats, FP64: 6 doubles per point), or null
     ExtDev ext;                // external magnetic elements (none: nu = nm = 0)
-    double inv_dx, inv_dy;     // 1/dx, 1/dy (the FP32 push's cell coordinates)
-    double dep_norm;           // 1 / (Delta h_n dx): the deposit factor of half-cell n per unit of q w dt (FP32 push)
+    double inv_dx, inv_dy;     // 1/dx, 1/dy (the mixed form's FP32 gathers and deposit)
+    double dep_norm;           // 1 / (Delta h_n dx): the deposit factor of half-cell n per unit of q w dt (the mixed form's FP32 deposit)
 };
 
 struct PlasmaPtrs {

@@ -30,7 +30,7 @@
 namespace g3d {
 
 // ---------------------------------------------------------------- relativistic Boris (sim_stream.hpp:8-18)
-// A: the arithmetic type of the push (double; float in the mixed form's streaming push)
+// A: the arithmetic type of the push (double in both forms)
 template <class A>
 __device__ __forceinline__ void boris(A& ux, A& uy, A& uz, const A E[3], const A B[3], A qm, A dt) {
     const A qh = A(0.5) * qm * dt;
@@ -135,7 +135,7 @@ __device__ __forceinline__ void sgather_mid(const StreamArgs& c, double x, doubl
     E[0] = double(a[0]); E[1] = double(a[1]); E[2] = double(a[2]);
     B[0] = double(a[3]); B[1] = double(a[4]); B[2] = double(a[5]);
 }
-// The FP32 push's TSC on a periodic grid: the cell coordinate t = x / d and the nearest node in FP64 (x spans the
+// The mixed form's TSC on a periodic grid: the cell coordinate t = x / d and the nearest node in FP64 (x spans the
 // box, so the index needs the double), the offset from that node in FP32, the three weights in FP32.
 __device__ __forceinline__ void tsc_f32(double x, double inv_d, int n, int idx[3], float w[3]) {
     const double t = x * inv_d;
@@ -149,7 +149,7 @@ __device__ __forceinline__ void tsc_f32(double x, double inv_d, int n, int idx[3
     const int b1 = b + 1 == n ? 0 : b + 1;
     idx[0] = b; idx[1] = b1; idx[2] = b1 + 1 == n ? 0 : b1 + 1;
 }
-// The midpoint gather of the FP32 push (Fourier y): the interleaved midpoint fields with FP32 weights, straight into
+// The mixed form's midpoint gather (Fourier y): the interleaved midpoint fields with FP32 weights, straight into
 // the FP32 fields of the Boris push.
 __device__ __forceinline__ void sgather_mid_f32(const StreamArgs& c, double x, double y, float E[3], float B[3]) {
     int ix[3], jn[3]; float wx[3], wn[3];
@@ -168,7 +168,7 @@ __device__ __forceinline__ void sgather_mid_f32(const StreamArgs& c, double x, d
         }
     E[0] = a[0]; E[1] = a[1]; E[2] = a[2]; B[0] = a[3]; B[1] = a[4]; B[2] = a[5];
 }
-// The FP32 push's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
+// The mixed form's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
 __device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, double y, float f, float vx, float vy, float vz) {
     int ix[3], jn[3]; float wx[3], wn[3];
     tsc_f32(x, c.inv_dx, c.g.nx, ix, wx);
@@ -299,7 +299,7 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
 struct DepReq {
     double x, y, f, vx, vy, vz;
     bool on;
-    bool f32;                  // the FP32 push on the Fourier y grid: deposit with sdeposit_f32 (ff, fv)
+    bool f32;                  // the mixed form on the Fourier y grid: deposit with sdeposit_f32 (ff, fv)
     float ff, fv[3];
 };
 
@@ -318,7 +318,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     // The whole state is loaded at once, before any branch or store: a load behind a branch waits for the
     // branch's own load, and a load behind a store to another array of the state (which the compiler must
     // assume may alias it) waits for that store. Every index below the count is a valid slot of every array.
-    typedef typename std::conditional<F32, float, double>::type A;
+    typedef double A;     // the push arithmetic: FP64 in both forms (the mixed form's FP32 push gave 3-4x its F error)
     int alive = S.alive[i];
     const int sp = S.sp[i];
     const double zeta = S.zeta[i], x = S.x[i], y = S.y[i], z = S.z[i];
@@ -342,8 +342,9 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         }
         return d;
     }
-    // the push in A (FP32 in the mixed form: the gathered fields are FP32 already; the positions, z and zeta stay
-    // FP64 and take FP32 displacements, the momenta are kept in FP64 between half-cells)
+    // the push in FP64 in both forms: the mixed form gathers FP32 fields and deposits into FP32 planes, but its Boris
+    // steps, gamma, 1 - v_z and velocities are FP64 (measured on the laser-plasma workload: FP32 arithmetic here put
+    // 3-4x more error into F over 1-5 s-steps, for 2.6 % less time in this kernel)
     const A px = A(px_), py = A(py_), pz = A(pz_), qm = A(qm_);
     const A g0 = sqrt(A(1) + px * px + py * py + pz * pz), ig0 = A(1) / g0;
     const A omv0 = (A(1) + px * px + py * py) / (g0 * (g0 + pz));     // 1 - v_z, no cancellation
@@ -358,7 +359,11 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         // are not gathered (the gas of an ionization-injection run is mostly neutral until the laser arrives)
         for (int k = 0; k < 3; ++k) { E[k] = A(0); B[k] = A(0); }
     } else if (F32 && YF && mid && !LASER && !c.ext.any()) {
-        if constexpr (F32) sgather_mid_f32(c, wrapx(g, xm), wrapy<YF>(g, ym), E, B);
+        if constexpr (F32) {
+            float Ef[3], Bf[3];
+            sgather_mid_f32(c, wrapx(g, xm), wrapy<YF>(g, ym), Ef, Bf);
+            for (int k = 0; k < 3; ++k) { E[k] = A(Ef[k]); B[k] = A(Bf[k]); }
+        }
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
         if (mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy<YF>(g, ym), Ed, Bd);
@@ -431,8 +436,8 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
 // One thread per streaming particle, a fixed grid striding over their count (which freed electrons raise; it is
 // read on the device). The deposit adds go straight to global memory: without a use of the old value they are
 // fire-and-forget reductions in L2, cheaper for the SM than accumulating in shared memory the many adds that
-// neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers, the Boris pushes and
-// the velocities in FP32 arithmetic, the deposit into FP32 planes; the particle state stays FP64.
+// neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers in FP32 from FP32 field
+// planes, the deposit into FP32 planes; the push arithmetic and the particle state stay FP64.
 constexpr int ST_NT = 128;
 #ifndef G3D_STREAM_MINB
 #define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
