@@ -440,7 +440,10 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
 // planes, the deposit into FP32 planes; the push arithmetic and the particle state stay FP64.
 constexpr int ST_NT = 128;
 #ifndef G3D_STREAM_MINB
-#define G3D_STREAM_MINB 6          // resident CTAs per SM the register budget of the plain variant is sized for (measured: 6 beats 4 and 8)
+// resident CTAs per SM the register budget of the plain variant is sized for: 5 (96 registers) against 6 (80) gave
+// 55.8 against 57.8 us per launch in the mixed form and 89.7 against 91.8 us in the FP64 form (laser-plasma workload,
+// one box); 4, 7 and 8 were slower
+#define G3D_STREAM_MINB 5
 #endif
 // YF: the Fourier y grid (true) or the free-hand one, fixed for a run, so that each variant holds only its own grid's
 // gathers and deposits (fewer registers and no local arrays).
