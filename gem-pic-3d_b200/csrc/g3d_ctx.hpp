@@ -7,6 +7,7 @@
 #include <vector>
 #include "g3d.h"
 #include "g3d_common.cuh"
+#include "k_tma.cuh"
 
 namespace g3d {
 
@@ -117,6 +118,28 @@ struct ProfEntry { std::string name; long launches = 0; double ms = 0; };
 struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 
 struct PlasmaState;               // g3d_plasma.hpp
+// Tensor maps of a TMA column kernel over a set of buffers (k_tma.cuh), rebuilt when the buffers move
+struct TmaCache {
+    bool valid = false;
+    const void* base[6] = {};
+    long rows = 0;
+    TileMaps maps{};
+    // the maps of n arrays [rows][H] for 8-column tiles of ny rows; false where the TMA path does not apply
+    bool get(const cpx* const* p, int n, long H, long rows_, int ny) {
+        bool same = valid && rows == rows_;
+        for (int k = 0; k < n && same; ++k) same = base[k] == p[k];
+        if (same) return true;
+        valid = false;
+        if (ny > 256 || n > 6) return false;
+        for (int k = 0; k < n; ++k) {
+            if (!tma_map_columns(&maps.m[k], p[k], H, rows_, ny)) return false;
+            base[k] = p[k];
+        }
+        rows = rows_;
+        valid = true;
+        return true;
+    }
+};
 struct Shard;                     // g3d_shard.cu
 
 // Buffers of the mixed FP32/FP64 form (k_mixed.cu): complex64 half spectra of E_z, B_z, L and the currents, FP32
@@ -168,6 +191,11 @@ struct Ctx {
     float* f_next = nullptr;
     DevBuf<cpx> W[6];                            // half-spectrum scratch, ns+1 planes each
     DevBuf<double> rscratch;                     // real scratch (Thomas coefficients), ns half planes
+    // TMA tile loads of the whole-window column transforms (k_tma.cuh): on unless G3D_NO_TMA is set; the error word
+    // of their bounded waits (bit 1: a tile never landed)
+    bool use_tma = true;
+    TmaCache tma_rf, tma_cur, tma_spi, tma_spf;
+    DevBuf<int> kerr;
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
     bool mixed = false;                          // G3D_PREC_MIXED: the spectra above except Rx, Ry are not allocated
     bool f32s = false;                           // G3D_PREC_MIXED: FP32 gathers and deposit of the streaming plasma

@@ -6,6 +6,7 @@
 #include <map>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include "g3d_plasma.hpp"
@@ -445,6 +446,8 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.twx.upload(tw(nx), s); c.twy.upload(tw(ny), s);
     realloc_slab(c);
     c.red.alloc(size_t(297) * 17, s);
+    c.kerr.alloc(1, s);
+    c.use_tma = std::getenv("G3D_NO_TMA") == nullptr;
     // the plane wave (reference sim_setup.cpp:51-54; eta_c given directly)
     c.laser.on = P.laser_on; c.laser.pol = P.laser_pol; c.laser.env = P.laser_envelope;
     c.laser.a0 = P.a0; c.laser.kL = P.kL; c.laser.tau = P.tau; c.laser.cep = P.cep; c.laser.eta_c = P.eta_c;
@@ -831,6 +834,7 @@ static void window_shift_start(Ctx& c) {
     const int nys = c.yf && c.P.move_y ? int(std::lround((v[1] / v[2] - (c.Y0 + 0.5 * Ly)) / c.dy)) : 0;
     if (std::abs(nxs) >= 2 || std::abs(nys) >= 2) shift_window(c, nxs, nys);
 }
+static void check_kernel_errors(Ctx& c);
 static void init_fields(Ctx& c) {
     c.s = 0; c.istep = 0;
     c.fields_ready = true;
@@ -862,9 +866,18 @@ static void step(Ctx& c, bool sync) {
     } else if (c.P.self_fields) solve_fields(c, 0.5 * c.P.dz);
     if (!c.chicanes.empty()) apply_chicanes(c, c.s - c.P.dz, c.s);
     window_shift_post(c);
-    if (sync) G3D_CUDA(cudaStreamSynchronize(c.stream));
+    if (sync) check_kernel_errors(c);
 }
 static bool finished(const Ctx& c) { return c.s >= c.P.z_end - 1e-9 || c.stop_; }
+// the error word of the kernels' bounded waits (after the stream is synchronized): G3D_ERR_TIMEOUT, reset
+static void check_kernel_errors(Ctx& c) {
+    int e = 0;
+    G3D_CUDA(cudaMemcpyAsync(&e, c.kerr.p, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    if (e == 0) return;
+    G3D_CUDA(cudaMemsetAsync(c.kerr.p, 0, sizeof(int), c.stream));
+    throw Error(G3D_ERR_TIMEOUT, "a tile load of the TMA column transforms did not land within its bounded wait");
+}
 
 // ---------------------------------------------------------------- arrays
 // Storage of an array id: device pointer, element count and size of the storage, the planes of a spectrum
@@ -1386,18 +1399,18 @@ int g3d_sample_bunches(const g3d_grid* grid, const g3d_params* params, const g3d
         return e.code;
     }
 }
-int g3d_init(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::init_fields(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); }); }
+int g3d_init(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::init_fields(ctx->c); g3d::check_kernel_errors(ctx->c); }); }
 int g3d_step(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::step(ctx->c, true); ctx->c.prof_collect(); }); }
 int g3d_step_async(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::step(ctx->c, false); }); }
 int g3d_solve_fields(g3d_ctx* ctx, double D) {
-    return guarded(ctx, [&] { g3d::solve_fields(ctx->c, D); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+    return guarded(ctx, [&] { g3d::solve_fields(ctx->c, D); g3d::check_kernel_errors(ctx->c); });
 }
 int g3d_currents(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::currents(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); }); }
 int g3d_march(g3d_ctx* ctx, double D) {
     return guarded(ctx, [&] { g3d::materialize_jk(ctx->c); g3d::march(ctx->c, D); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
 }
 int g3d_sponge_and_real_fields(g3d_ctx* ctx) {
-    return guarded(ctx, [&] { g3d::sponge_and_real_fields(ctx->c); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
+    return guarded(ctx, [&] { g3d::sponge_and_real_fields(ctx->c); g3d::check_kernel_errors(ctx->c); });
 }
 int g3d_push(g3d_ctx* ctx, double s0, double s1) {
     return guarded(ctx, [&] { g3d::launch_push(ctx->c, s0, s1); G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); });
@@ -1605,7 +1618,7 @@ int g3d_read_checkpoint(g3d_ctx* ctx, const char* path) {
 
 void* g3d_stream(g3d_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
 int g3d_synchronize(g3d_ctx* ctx) {
-    return guarded(ctx, [&] { G3D_CUDA(cudaStreamSynchronize(ctx->c.stream)); ctx->c.prof_collect(); });
+    return guarded(ctx, [&] { g3d::check_kernel_errors(ctx->c); ctx->c.prof_collect(); });
 }
 int g3d_profile_enable(g3d_ctx* ctx, int32_t on) {
     return guarded(ctx, [&] {

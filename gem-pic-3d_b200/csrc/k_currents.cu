@@ -15,6 +15,7 @@
 #include "g3d_ctx.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
+#include "k_tma.cuh"
 
 namespace g3d {
 
@@ -222,6 +223,44 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
     }
 }
 
+// The same with the tiles of TX, TY, TZ (maps 0, 1, 2) loaded by the TMA (k_tma.cuh): row-major 8-column tiles,
+// transformed along their columns (stride 8).
+template <int NY>
+__global__ void __launch_bounds__(8 * FftShape<NY>::T) k_cur_cols_tma(Geo g, const __grid_constant__ TileMaps maps,
+                                                                     cpx* __restrict__ JX, cpx* __restrict__ JY,
+                                                                     cpx* __restrict__ JZ, int keep0, int* __restrict__ err) {
+    using S = FftShape<NY>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int ok;
+    const int hk = blockIdx.y, c0 = blockIdx.x * 8, tid = threadIdx.x, nthr = 8 * S::T;
+    const int H = g.H;
+    const long base = long(hk) * g.nkh;
+    cpx* s0 = reinterpret_cast<cpx*>(smraw + ((128 - (smem_addr(smraw) & 127)) & 127));
+    cpx* s1 = s0 + NY * 8;
+    cpx* s2 = s1 + NY * 8;
+    const int idx[3] = {0, 1, 2};
+    cpx* const dst[3] = {s0, s1, s2};
+    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, hk * g.ny, &bar, &ok, err)) return;
+    const int c = tid % 8, t = tid / 8;
+    {
+        decltype(s0) const ls_[3] = {s0, s1, s2};
+        fft_lines<NY, 3>(ls_, TileCol{c}, t, g.twy);
+    }
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * 8) break;
+        const int p = e / 8, cc = e - p * 8, kx = c0 + cc;
+        if (kx >= H) continue;
+        const double f = (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p];
+        const long o = base + long(p) * H + kx;
+        JX[o] = f * s0[e];
+        JY[o] = f * s1[e];
+        JZ[o] = f * s2[e];
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 // the scales 2^e_c, 2^-e_c of the fixed-point deposit (six values; ia_max: the largest dual-cell factor); returns
 // where they are
@@ -272,9 +311,26 @@ static void cur_rows(Ctx& c, cpx* TX, cpx* TY, cpx* TZ) {
     c.check_launch("k_cur_rows");
     c.prof_end(tok);
 }
+// the tensor maps of TX, TY, TZ (the transform scratch W0..W2, ns + 1 planes), made once per set of buffers
+static bool cur_maps(Ctx& c) {
+    const cpx* p[3] = {c.W[0].p, c.W[1].p, c.W[2].p};
+    return c.tma_cur.get(p, 3, c.H, long(c.ns + 1) * c.ny, c.ny);
+}
 template <int NY>
 static void cur_cols(Ctx& c, bool keep0) {
     constexpr int CW = 8;
+    if constexpr (NY <= 256) {
+        if (c.use_tma && cur_maps(c)) {
+            const size_t smem = size_t(3) * NY * 8 * sizeof(cpx) + 128;
+            smem_attr(reinterpret_cast<const void*>(k_cur_cols_tma<NY>), smem);
+            const int tok = c.prof_begin("cur_cols");
+            k_cur_cols_tma<NY><<<dim3(unsigned((c.H + 7) / 8), unsigned(c.ns + 1)), 8 * FftShape<NY>::T, smem, c.stream>>>(
+                c.geo(), c.tma_cur.maps, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0, c.kerr.p);
+            c.check_launch("k_cur_cols_tma");
+            c.prof_end(tok);
+            return;
+        }
+    }
     const size_t smem = size_t(3) * ColTile<NY, CW>::size * sizeof(cpx);
     auto kern = k_cur_cols<NY, CW>;
     smem_attr(reinterpret_cast<const void*>(kern), smem);

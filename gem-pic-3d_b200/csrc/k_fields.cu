@@ -17,6 +17,7 @@
 #include "g3d_ctx.hpp"
 #include "k_fft.cuh"
 #include "k_dispatch.cuh"
+#include "k_tma.cuh"
 
 namespace g3d {
 
@@ -114,6 +115,60 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_inv(Geo g, con
     }
 }
 
+// The same with the tiles of R_x, R_y (maps 0, 1) loaded by the TMA (k_tma.cuh); psi per element as above.
+template <int NY>
+__global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_inv_tma(Geo g, const __grid_constant__ TileMaps maps,
+                                                                        const cpx* __restrict__ jz, const cpx* __restrict__ jg,
+                                                                        cpx* __restrict__ U, cpx* __restrict__ V,
+                                                                        cpx* __restrict__ PSI, double g2, double opb,
+                                                                        int* __restrict__ err) {
+    using S = FftShape<NY>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int ok;
+    const int l = blockIdx.y, c0 = blockIdx.x * 8, tid = threadIdx.x, nthr = 8 * S::T;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    cpx* s0 = reinterpret_cast<cpx*>(smraw + ((128 - (smem_addr(smraw) & 127)) & 127));
+    cpx* s1 = s0 + NY * 8;
+    const int idx[2] = {0, 1};
+    cpx* const dst[2] = {s0, s1};
+    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * 8) break;
+        const int p = e / 8, c = e - p * 8, kxi = c0 + c;
+        cpx u = C(0), v = C(0);
+        if (kxi < H) {
+            const long i = long(p) * H + kxi, o = base + i;
+            const double kx = g.kxd[kxi], ky = g.kyd[p];
+            const cpx psi = bound_psi(g, jz, jg, l, i, kx, ky, g2);
+            PSI[o] = psi;
+            u = s0[e] - (-opb * ik(kx, psi));
+            v = s1[e] - (-opb * ik(ky, psi));
+        }
+        s0[e] = conj(u);
+        s1[e] = conj(v);
+    }
+    __syncthreads();
+    const int c = tid % 8, t = tid / 8;
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, TileCol{c}, t, g.twy);
+    }
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * 8) break;
+        const int p = e / 8, cc = e - p * 8, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        U[o] = conj(s0[e]);
+        V[o] = conj(s1[e]);
+    }
+}
+
 // ---------------------------------------------------------------- sponge, pass 2: rows (inverse x, mask, forward x)
 template <int NX>
 __global__ void __launch_bounds__(NT) k_sp_rows(Geo g, cpx* __restrict__ U, cpx* __restrict__ V) {
@@ -203,6 +258,42 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
     }
 }
 
+// The same with the tiles of U, V, PSI (maps 0, 1, 2) loaded by the TMA (k_tma.cuh).
+template <int NY>
+__global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_fwd_tma(Geo g, const __grid_constant__ TileMaps maps,
+                                                                        cpx* __restrict__ Rx, cpx* __restrict__ Ry, double opb,
+                                                                        int* __restrict__ err) {
+    using S = FftShape<NY>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int ok;
+    const int l = blockIdx.y, c0 = blockIdx.x * 8, tid = threadIdx.x, nthr = 8 * S::T;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    cpx* s0 = reinterpret_cast<cpx*>(smraw + ((128 - (smem_addr(smraw) & 127)) & 127));
+    cpx* s1 = s0 + NY * 8;
+    cpx* s2 = s1 + NY * 8;
+    const int idx[3] = {0, 1, 2};
+    cpx* const dst[3] = {s0, s1, s2};
+    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    const int c = tid % 8, t = tid / 8;
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, TileCol{c}, t, g.twy);
+    }
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * 8) break;
+        const int p = e / 8, cc = e - p * 8, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        const cpx psi = s2[e];
+        Rx[o] = s0[e] - opb * ik(g.kxd[kxi], psi);
+        Ry[o] = s1[e] - opb * ik(g.kyd[p], psi);
+    }
+}
+
 // ---------------------------------------------------------------- real fields: columns (inverse y of the six spectra)
 // blockIdx.z picks the pair (R_x, R_y), (L_x, L_y) or (E_z, B_z): two fields per CTA keep the shared memory small
 // enough for several CTAs per SM, so loads of one CTA overlap the transforms of another.
@@ -248,6 +339,48 @@ __global__ void __launch_bounds__(CWT * FftShape<NY>::T) k_rf_cols(Geo g, const 
         const long o = base + long(p) * H + kxi;
         out0[o] = conj(s0[ColTile<NY, CWT>::at(p, cc)]);
         out1[o] = conj(s1[ColTile<NY, CWT>::at(p, cc)]);
+    }
+}
+
+// The same transforms of the whole window with the tiles loaded by the TMA (k_tma.cuh): the 8-column tiles of the
+// pair land row-major in shared memory, are conjugated in place, transformed along their columns (stride 8) and
+// written back conjugated; maps 0..5 are R_x, R_y, L_x, L_y, E_z, B_z.
+template <int NY>
+__global__ void __launch_bounds__(8 * FftShape<NY>::T) k_rf_cols_tma(Geo g, const __grid_constant__ TileMaps maps,
+                                                                    cpx* __restrict__ W0, cpx* __restrict__ W1,
+                                                                    cpx* __restrict__ W2, cpx* __restrict__ W3,
+                                                                    cpx* __restrict__ W4, cpx* __restrict__ W5, int l0,
+                                                                    int* __restrict__ err) {
+    using S = FftShape<NY>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int ok;
+    const int l = l0 + blockIdx.y, c0 = blockIdx.x * 8, tid = threadIdx.x, nthr = 8 * S::T, pr = blockIdx.z;
+    const int H = g.H;
+    const long base = long(l) * g.nkh;
+    cpx* s0 = reinterpret_cast<cpx*>(smraw + ((128 - (smem_addr(smraw) & 127)) & 127));
+    cpx* s1 = s0 + NY * 8;
+    cpx* out0 = pr == 0 ? W0 : pr == 1 ? W2 : W4;
+    cpx* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
+    const int idx[2] = {2 * pr, 2 * pr + 1};
+    cpx* const dst[2] = {s0, s1};
+    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    for (int e = tid; e < NY * 8; e += nthr) { s0[e] = conj(s0[e]); s1[e] = conj(s1[e]); }
+    __syncthreads();
+    const int c = tid % 8, t = tid / 8;
+    {
+        decltype(s0) const ls_[2] = {s0, s1};
+        fft_lines<NY, 2>(ls_, TileCol{c}, t, g.twy);
+    }
+    #pragma unroll
+    for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
+        const int e = tid + u_ * nthr;
+        if (e >= NY * 8) break;
+        const int p = e / 8, cc = e - p * 8, kxi = c0 + cc;
+        if (kxi >= H) continue;
+        const long o = base + long(p) * H + kxi;
+        out0[o] = conj(s0[e]);
+        out1[o] = conj(s1[e]);
     }
 }
 
@@ -329,6 +462,19 @@ static unsigned col_tiles(const Ctx& c) { return unsigned((c.H + CW - 1) / CW); 
 
 template <int NY>
 static void sp_cols_inv(Ctx& c) {
+    if constexpr (NY <= 256) {
+        const cpx* p[2] = {c.Rx.p, c.Ry.p};
+        if (c.use_tma && c.tma_spi.get(p, 2, c.H, long(c.ns) * c.ny, c.ny)) {
+            const size_t smem = size_t(2) * NY * 8 * sizeof(cpx) + 128;
+            allow_smem(k_sp_cols_inv_tma<NY>, smem);
+            const int tok = c.prof_begin("sponge_cols_inv");
+            k_sp_cols_inv_tma<NY><<<dim3(col_tiles(c), unsigned(c.ns)), 8 * FftShape<NY>::T, smem, c.stream>>>(
+                c.geo(), c.tma_spi.maps, c.jkz.p, c.jzg.p, c.W[0].p, c.W[1].p, c.W[3].p, c.gm2_b, 1 + c.beta_b, c.kerr.p);
+            c.check_launch("k_sp_cols_inv_tma");
+            c.prof_end(tok);
+            return;
+        }
+    }
     const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpx);
     allow_smem(k_sp_cols_inv<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_inv");
@@ -349,6 +495,19 @@ static void sp_rows(Ctx& c) {
 }
 template <int NY>
 static void sp_cols_fwd(Ctx& c) {
+    if constexpr (NY <= 256) {
+        const cpx* p[3] = {c.W[0].p, c.W[1].p, c.W[3].p};
+        if (c.use_tma && c.tma_spf.get(p, 3, c.H, long(c.ns) * c.ny, c.ny)) {
+            const size_t smem = size_t(3) * NY * 8 * sizeof(cpx) + 128;
+            allow_smem(k_sp_cols_fwd_tma<NY>, smem);
+            const int tok = c.prof_begin("sponge_cols_fwd");
+            k_sp_cols_fwd_tma<NY><<<dim3(col_tiles(c), unsigned(c.ns)), 8 * FftShape<NY>::T, smem, c.stream>>>(
+                c.geo(), c.tma_spf.maps, c.Rx.p, c.Ry.p, 1 + c.beta_b, c.kerr.p);
+            c.check_launch("k_sp_cols_fwd_tma");
+            c.prof_end(tok);
+            return;
+        }
+    }
     const size_t smem = size_t(2) * ColTile<NY, CW>::size * sizeof(cpx);
     allow_smem(k_sp_cols_fwd<NY>, smem);
     const int tok = c.prof_begin("sponge_cols_fwd");
@@ -374,10 +533,28 @@ static void rf_cols_w(Ctx& c, int l0, int nl) {
     c.check_launch("k_rf_cols");
     c.prof_end(tok);
 }
+// the tensor maps of R_x, R_y, L_x, L_y, E_z, B_z for tiles of 8 columns x ny rows, made once per set of buffers;
+// false where the TMA path does not apply (ny > 256, or the encoder is unavailable)
+static bool rf_maps(Ctx& c) {
+    const cpx* p[6] = {c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p};
+    return c.tma_rf.get(p, 6, c.H, long(c.ns) * c.ny, c.ny);
+}
+template <int NY>
+static void rf_cols_tma(Ctx& c, int l0, int nl) {
+    const size_t smem = size_t(2) * NY * 8 * sizeof(cpx) + 128;
+    allow_smem(k_rf_cols_tma<NY>, smem);
+    const int tok = c.prof_begin("real_cols");
+    k_rf_cols_tma<NY><<<dim3(unsigned((c.H + 7) / 8), unsigned(nl), 3), 8 * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), c.tma_rf.maps, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, l0, c.kerr.p);
+    c.check_launch("k_rf_cols_tma");
+    c.prof_end(tok);
+}
 template <int NY>
 static void rf_cols(Ctx& c, int l0, int nl) {
     if (nl == 1) rf_cols_w<NY, 2>(c, l0, nl);
-    else rf_cols_w<NY, CW>(c, l0, nl);
+    else if (c.use_tma && rf_maps(c)) {
+        if constexpr (NY <= 256) rf_cols_tma<NY>(c, l0, nl);
+    } else rf_cols_w<NY, CW>(c, l0, nl);
 }
 template <int NX>
 static void rf_rows(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {

@@ -245,3 +245,25 @@ def test_reruns_are_bit_identical(grid):
     a, b = runs
     for k in a:
         assert np.array_equal(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("ny", [32, 128])
+def test_tma_column_tiles_give_the_plain_loads_bits(ny, monkeypatch):
+    """The column transforms of the whole window (currents, real fields) load their 8-column tiles with the TMA;
+    with G3D_NO_TMA set at creation they use per-thread loads into the padded tiles. The arithmetic is the same, so
+    every array is the same bits after the start field and three s-steps (ny = 128: the workload-2 tile height)."""
+    from g3d import Simulation, configs
+    cfg = configs.config2(nx=32, ny=ny, nzeta=64, nmacro=20000, steps=3, envelope=0)
+    runs = []
+    for plain in (False, True):
+        if plain:
+            monkeypatch.setenv("G3D_NO_TMA", "1")
+        s = Simulation(cfg)
+        s.init()
+        for _ in range(3):
+            s.step()
+        runs.append({a: s.array(a) for a in SPECTRA + ["F"]})
+        s.close()
+    a, b = runs
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
