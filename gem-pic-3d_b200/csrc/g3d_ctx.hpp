@@ -118,6 +118,15 @@ struct ProfEntry { std::string name; long launches = 0; double ms = 0; };
 struct PendingEvent { int entry; cudaEvent_t e0, e1; };
 
 struct PlasmaState;               // g3d_plasma.hpp
+// The slabs of a sharded run's ranks as one GPU sees them (g3d_shard.cu, the peer march of k_march.cu): each rank's
+// first slice, slice count and its 11 slab arrays (R_x, R_y, E_z, B_z, L_x, L_y, j0x, j0y, jkx, jky, jkz) mapped here
+constexpr int SHARD_PEER_MAX = 8;
+struct SlabPeers {
+    int P = 0;
+    int a[SHARD_PEER_MAX] = {}, ns[SHARD_PEER_MAX] = {};
+    long nkh = 0;
+    void* arr[SHARD_PEER_MAX][11] = {};
+};
 // Tensor maps of a TMA column kernel over a set of buffers (k_tma.cuh), rebuilt when the buffers move
 struct TmaCache {
     bool valid = false;
@@ -314,6 +323,7 @@ void launch_comoving(Ctx& c, double beta, double gm2);
 void launch_push(Ctx& c, double s0, double s1);
 void launch_push_range(Ctx& c, double s0, double s1, long i0, long n);
 void launch_march_pencil(Ctx& c, const Geo& g, cpx* const* p, double D);
+void launch_march_peer(Ctx& c, const Geo& g, const SlabPeers& sp, double D);
 void launch_comoving_pencil(Ctx& c, const Geo& g, const cpx* jz, double* cpb, cpx* dpb, cpx* const* out, double beta, double gm2);
 void realloc_slab(Ctx& c);                        // the field buffers of the slab [a, b) (g3d_host.cu)
 void reserve_particles(Ctx& c, long n);           // particle columns for n (contents not kept when they move)

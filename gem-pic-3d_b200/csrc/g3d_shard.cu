@@ -17,6 +17,8 @@
 // through the caller's function (g3d_set_ranks): sums and all-to-alls of device buffers, every rank calling the same
 // collectives in the same order. Neighbour exchanges are all-to-alls with zero bytes for the other ranks.
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <cub/device/device_select.cuh>
 #include "g3d_shard.hpp"
 
@@ -226,6 +228,7 @@ long select_flagged(Ctx& c, const g3d_particle* in, const unsigned char* flags, 
 }  // namespace
 
 // ---------------------------------------------------------------- set-up
+static void setup_peers(Ctx& c, Shard& S);
 void set_ranks(Ctx& c, int rank, int world, g3d_comm_fn comm, void* user) {
     if (world < 1 || rank < 0 || rank >= world) throw Error(G3D_ERR_ARG, "g3d_set_ranks: rank must be in [0, world)");
     if (world > 1 && !comm) throw Error(G3D_ERR_ARG, "g3d_set_ranks: several ranks need a communication function");
@@ -264,8 +267,80 @@ void set_ranks(Ctx& c, int rank, int world, g3d_comm_fn comm, void* user) {
     S->cnt.alloc(2, c.stream);
     S->hv.alloc(size_t(world), c.stream);
     S->nsel.alloc(1, c.stream);
+    S->one.alloc(1, c.stream);
     c.sh = std::move(S);
+    setup_peers(c, *c.sh);
     G3D_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+Shard::~Shard() {
+    for (void* p : opened) cudaIpcCloseMemHandle(p);          // nothing to report from a destructor
+}
+
+// every rank has reached this point with its stream drained (a sum of nothing over the ranks)
+static void shard_barrier(Ctx& c) {
+    Shard& S = *c.sh;
+    c.all_sum(S.one.p, 1, G3D_SUM_I64);
+}
+// Map every rank's slab arrays into this GPU's address space (CUDA IPC handles exchanged by the all-to-all): the
+// fused march then reads and writes them directly. All ranks agree on the outcome (a failure anywhere is summed),
+// so either every rank marches over peer memory or every rank uses the transposes.
+static void setup_peers(Ctx& c, Shard& S) {
+    const int P = c.world, r = c.rank;
+    const bool want = P <= SHARD_PEER_MAX && std::getenv("G3D_SHARD_TRANSPOSE") == nullptr;
+    cpx* mine[11] = {c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.Lx.p, c.Ly.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p};
+    std::vector<cudaIpcMemHandle_t> h(11);
+    int64_t fail = want ? 0 : 1;
+    for (int k = 0; k < 11 && !fail; ++k)
+        if (cudaIpcGetMemHandle(&h[size_t(k)], mine[k]) != cudaSuccess) { fail = 1; cudaGetLastError(); }
+    auto agree = [&](int64_t f) {                // the sum of the ranks' failure flags
+        G3D_CUDA(cudaMemcpyAsync(S.one.p, &f, sizeof(f), cudaMemcpyHostToDevice, c.stream));
+        c.all_sum(S.one.p, 1, G3D_SUM_I64);
+        int64_t t = 0;
+        G3D_CUDA(cudaMemcpyAsync(&t, S.one.p, sizeof(t), cudaMemcpyDeviceToHost, c.stream));
+        G3D_CUDA(cudaMemsetAsync(S.one.p, 0, sizeof(int64_t), c.stream));
+        G3D_CUDA(cudaStreamSynchronize(c.stream));
+        return t;
+    };
+    if (agree(fail) != 0) return;
+    const size_t hb = 11 * sizeof(cudaIpcMemHandle_t);
+    std::vector<unsigned char> send(size_t(P) * hb), recv(size_t(P) * hb);
+    for (int q = 0; q < P; ++q) std::memcpy(send.data() + size_t(q) * hb, h.data(), hb);
+    DevBuf<unsigned char> ds, dr;
+    ds.upload(send, c.stream);
+    dr.alloc(size_t(P) * hb, c.stream);
+    const std::vector<int64_t> bytes(static_cast<size_t>(P), static_cast<int64_t>(hb));
+    c.all_to_all(ds.p, bytes.data(), dr.p, bytes.data());
+    G3D_CUDA(cudaMemcpyAsync(recv.data(), dr.p, recv.size(), cudaMemcpyDeviceToHost, c.stream));
+    G3D_CUDA(cudaStreamSynchronize(c.stream));
+    SlabPeers sp;
+    sp.P = P;
+    sp.nkh = c.nkh;
+    for (int q = 0; q < P; ++q) {
+        sp.a[q] = S.L.a[size_t(q)];
+        sp.ns[q] = S.L.ns[size_t(q)];
+        for (int k = 0; k < 11; ++k) {
+            if (q == r) { sp.arr[q][k] = mine[k]; continue; }
+            cudaIpcMemHandle_t hq;
+            std::memcpy(&hq, recv.data() + size_t(q) * hb + size_t(k) * sizeof(cudaIpcMemHandle_t), sizeof(hq));
+            void* p = nullptr;
+            if (fail == 0 && cudaIpcOpenMemHandle(&p, hq, cudaIpcMemLazyEnablePeerAccess) == cudaSuccess) {
+                S.opened.push_back(p);
+                sp.arr[q][k] = p;
+            } else {
+                fail = 1;
+                cudaGetLastError();
+            }
+        }
+    }
+    if (agree(fail) != 0) {
+        for (void* p : S.opened) cudaIpcCloseMemHandle(p);
+        S.opened.clear();
+        return;
+    }
+    S.peers = sp;
+    S.orig_j0x = c.j0x.p;
+    S.peer = true;
 }
 
 bool shard_owns(const Ctx& c, double zeta) {
@@ -280,6 +355,16 @@ bool shard_owns(const Ctx& c, double zeta) {
 // ---------------------------------------------------------------- the march and the co-moving solve on pencils
 void shard_march(Ctx& c, double D) {
     Shard& S = *c.sh;
+    if (S.peer) {
+        // j0 and jk trade buffers after every field solve, on every rank alike: the peers' current roles follow ours
+        SlabPeers sp = S.peers;
+        if (c.j0x.p != S.orig_j0x)
+            for (int q = 0; q < sp.P; ++q) { std::swap(sp.arr[q][6], sp.arr[q][8]); std::swap(sp.arr[q][7], sp.arr[q][9]); }
+        shard_barrier(c);                        // every slab's inputs are complete
+        launch_march_peer(c, S.pencil, sp, D);
+        shard_barrier(c);                        // every rank's march has written its modes into every slab
+        return;
+    }
     cpx* slab_in[9] = {c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p, c.j0x.p, c.j0y.p, c.jkx.p, c.jky.p, c.jkz.p};
     cpx* pen_in[9] = {S.pen[0].p, S.pen[1].p, S.pen[2].p, S.pen[3].p, S.pen[6].p, S.pen[7].p, S.pen[8].p, S.pen[9].p, S.pen[10].p};
     transpose(c, S.march_in, slab_in, 9, pen_in, 9);

@@ -42,7 +42,15 @@ struct Shard {
     DevBuf<int> nsel;
     DevBuf<unsigned char> cubtmp;
     DevBuf<g3d_particle> stage2, handrec;
+    // the fused march over peer memory: every rank's slab arrays mapped here (CUDA IPC), as set up (j0 and jk in
+    // their first roles); off when a rank cannot map them, above SHARD_PEER_MAX ranks or with G3D_SHARD_TRANSPOSE
+    bool peer = false;
+    SlabPeers peers;
+    const void* orig_j0x = nullptr;
+    std::vector<void*> opened;                  // the peers' mappings, closed with the shard
+    DevBuf<int64_t> one;                        // the barrier's value
     explicit Shard(const ShardLayout& l) : L(l) {}
+    ~Shard();
 };
 
 void set_ranks(Ctx& c, int rank, int world, g3d_comm_fn comm, void* user);

@@ -62,13 +62,20 @@ __device__ __forceinline__ double ring_re(const double* cell) {
 // R stays complex128 and the recurrence runs in FP64 in both forms: its carried values never leave the
 // registers, so the mixed form only rounds what it stores, and the cancellations in curl R and div R that make
 // E_z, B_z gamma^-2 small are taken in FP64.
-template <class T, int BT, int DEPTH>
+//
+// PEER (a sharded run with the ranks' slab buffers mapped into this GPU's address space, g3d_shard.cu): the lanes of
+// the modes [g.m0, g.m0 + g.nkh) fetch slice n straight from the slab of the rank that holds it and store its results
+// there, so the transposes before and after the march are this kernel's own loads and stores over NVLink (peer
+// loads through the cp.async ring, plain peer stores) instead of an all-to-all and two copies; the pointer arguments
+// are unused then.
+template <class T, int BT, int DEPTH, bool PEER = false>
 __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* __restrict__ Ry, T* __restrict__ Ez,
                                              T* __restrict__ Bz, T* __restrict__ Lx, T* __restrict__ Ly,
                                              const T* __restrict__ j0x, const T* __restrict__ j0y,
                                              const T* __restrict__ jkx, const T* __restrict__ jky,
-                                             const T* __restrict__ jkz, double D) {
+                                             const T* __restrict__ jkz, double D, SlabPeers sp = SlabPeers()) {
     typedef typename RealOf<T>::type Re;
+    static_assert(!PEER || sizeof(Re) == 8, "the peer march is the FP64 form's");
     extern __shared__ double ringd[];        // DEPTH slots of [MA arrays][BT] values, then [MC][BT] coefficients
     const long nk = g.nkh;
     const int tid = threadIdx.x;
@@ -97,26 +104,56 @@ __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
     auto cell = [&](int sl, int k) { return ringd + size_t(sl) * slot_doubles(BT) + k * BT + tid; };
     auto coef = [&](int sl, int k) { return ringd + size_t(sl) * slot_doubles(BT) + MA * BT + k * BT + tid; };
     // ring cells: 0 j0x, 1 jkx, 2 j0y, 3 jky (own), 4 jkz (other), 5 R_x, 6 R_y (own), 7 E_z, 8 B_z (other)
+    // PEER: the slab arrays of the rank holding slice n (R_x, R_y, E_z, B_z, L_x, L_y, j0x, j0y, jkx, jky, jkz) and the
+    // element offset of this lane's mode in its plane
+    auto peer = [&](int n, long& o) -> double* const* {
+        int r = 0;
+        while (r + 1 < sp.P && n >= sp.a[r + 1]) ++r;
+        o = long(n - sp.a[r]) * sp.nkh + g.m0 + ii;
+        return reinterpret_cast<double* const*>(sp.arr[r]);
+    };
     auto fetch = [&](int n) {                  // slice n (plane n - a) into its ring slot
         const int sl = (g.b - 1 - n) % DEPTH;
-        const long o = long(n - g.a) * nk + ii;
-        cp_async_re(cell(sl, 0), j0xr + own(o));
-        cp_async_re(cell(sl, 1), jkxr + own(o));
-        cp_async_re(cell(sl, 2), j0yr + own(o));
-        cp_async_re(cell(sl, 3), jkyr + own(o));
-        cp_async_re(cell(sl, 4), jkzr + oth(o));
-        cp_async8(cell(sl, 5), Rxr + own(o));
-        cp_async8(cell(sl, 6), Ryr + own(o));
-        cp_async_re(cell(sl, 7), Ezr + oth(o));
-        cp_async_re(cell(sl, 8), Bzr + oth(o));
+        if constexpr (PEER) {
+            long o;
+            double* const* q = peer(n, o);
+            cp_async8(cell(sl, 0), q[6] + own(o));
+            cp_async8(cell(sl, 1), q[8] + own(o));
+            cp_async8(cell(sl, 2), q[7] + own(o));
+            cp_async8(cell(sl, 3), q[9] + own(o));
+            cp_async8(cell(sl, 4), q[10] + oth(o));
+            cp_async8(cell(sl, 5), q[0] + own(o));
+            cp_async8(cell(sl, 6), q[1] + own(o));
+            cp_async8(cell(sl, 7), q[2] + oth(o));
+            cp_async8(cell(sl, 8), q[3] + oth(o));
+        } else {
+            const long o = long(n - g.a) * nk + ii;
+            cp_async_re(cell(sl, 0), j0xr + own(o));
+            cp_async_re(cell(sl, 1), jkxr + own(o));
+            cp_async_re(cell(sl, 2), j0yr + own(o));
+            cp_async_re(cell(sl, 3), jkyr + own(o));
+            cp_async_re(cell(sl, 4), jkzr + oth(o));
+            cp_async8(cell(sl, 5), Rxr + own(o));
+            cp_async8(cell(sl, 6), Ryr + own(o));
+            cp_async_re(cell(sl, 7), Ezr + oth(o));
+            cp_async_re(cell(sl, 8), Bzr + oth(o));
+        }
         cp_async8(coef(sl, 0), g.wlo + n);
         cp_async8(coef(sl, 1), g.whi + n);
         cp_async8(coef(sl, 2), g.hcg + n + 2);
     };
-    // upper half-cell of the front slice: plane ns
-    const long ou = long(g.ns) * nk + ii;
-    double jxu = double(j0xr[own(ou)]) + double(jkxr[own(ou)]), jyu = double(j0yr[own(ou)]) + double(jkyr[own(ou)]);
-    double upx = jkxr[own(ou)], upy = jkyr[own(ou)], upz = sgn * double(jkzr[oth(ou)]);
+    // upper half-cell of the front slice: plane ns (PEER: the top rank's last half-cell plane)
+    const Re* uj0x = j0xr; const Re* ujkx = jkxr; const Re* uj0y = j0yr; const Re* ujky = jkyr; const Re* ujkz = jkzr;
+    long ou = long(g.ns) * nk + ii;
+    if constexpr (PEER) {
+        const int r = sp.P - 1;
+        ou = long(sp.ns[r]) * sp.nkh + g.m0 + ii;
+        uj0x = static_cast<const Re*>(sp.arr[r][6]); uj0y = static_cast<const Re*>(sp.arr[r][7]);
+        ujkx = static_cast<const Re*>(sp.arr[r][8]); ujky = static_cast<const Re*>(sp.arr[r][9]);
+        ujkz = static_cast<const Re*>(sp.arr[r][10]);
+    }
+    double jxu = double(uj0x[own(ou)]) + double(ujkx[own(ou)]), jyu = double(uj0y[own(ou)]) + double(ujky[own(ou)]);
+    double upx = ujkx[own(ou)], upy = ujky[own(ou)], upz = sgn * double(ujkz[oth(ou)]);
     double pRx = 0, pRy = 0, pE = 0, pB = 0, pLx = 0, pLy = 0;    // level s1 of the slice above: R, E~, B~, L
 #pragma unroll
     for (int q = 0; q < DEPTH; ++q) {
@@ -143,7 +180,13 @@ __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
             const double hn = *coef((sl + 1) % DEPTH, 2);
             rden_next = 1 / (1 + 0.25 * hn * (D + 0.25 * hn) * k2);
         }
-        const long o = long(n - g.a) * nk + ii;
+        long o = long(n - g.a) * nk + ii;
+        Re* sEz = Ezr; Re* sBz = Bzr; Re* sLx = Lxr; Re* sLy = Lyr;
+        double* sRx = Rxr; double* sRy = Ryr;
+        if constexpr (PEER) {                  // the results go to the slab of the rank holding slice n
+            double* const* q = peer(n, o);
+            sRx = q[0]; sRy = q[1]; sEz = q[2]; sBz = q[3]; sLx = q[4]; sLy = q[5];
+        }
         const double jxd = dx0 + dxk, jyd = dy0 + dyk;
         const double Jx = wl * jxd + wu * jxu;
         const double Jy = wl * jyd + wu * jyu;
@@ -151,8 +194,8 @@ __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
         const double Rsy = ry + D * (ky * e - kx * b) - D * Jy;
         if (n == g.N - 1) {          // front of the window: L = E_z = B_z = 0
             if (live) {
-                Rxr[own(o)] = Rsx; Ryr[own(o)] = Rsy;
-                Ezr[oth(o)] = Re(0); Bzr[oth(o)] = Re(0); Lxr[own(o)] = Re(0); Lyr[own(o)] = Re(0);
+                sRx[own(o)] = Rsx; sRy[own(o)] = Rsy;
+                sEz[oth(o)] = Re(0); sBz[oth(o)] = Re(0); sLx[own(o)] = Re(0); sLy[own(o)] = Re(0);
             }
             pRx = Rsx; pRy = Rsy; pE = 0; pB = 0; pLx = 0; pLy = 0;
         } else {
@@ -169,8 +212,8 @@ __global__ void __launch_bounds__(BT) k_march(Geo g, cpx* __restrict__ Rx, cpx* 
             const double nLx = Lsx - 0.25 * h * (kx * En - ky * Bn);
             const double nLy = Lsy - 0.25 * h * (kx * Bn + ky * En);
             if (live) {
-                Ezr[oth(o)] = Re(sgn * En); Bzr[oth(o)] = Re(sgn * Bn); Rxr[own(o)] = nRx; Ryr[own(o)] = nRy;
-                Lxr[own(o)] = Re(nLx); Lyr[own(o)] = Re(nLy);
+                sEz[oth(o)] = Re(sgn * En); sBz[oth(o)] = Re(sgn * Bn); sRx[own(o)] = nRx; sRy[own(o)] = nRy;
+                sLx[own(o)] = Re(nLx); sLy[own(o)] = Re(nLy);
             }
             pRx = nRx; pRy = nRy; pE = En; pB = Bn; pLx = nLx; pLy = nLy;
         }
@@ -254,6 +297,25 @@ void launch_march_pencil(Ctx& c, const Geo& g, cpx* const* p, double D) {
     const int tok = c.prof_begin("march");
     march_any<cpx, 6>(c, g, p[0], p[1], p[2], p[3], p[4], p[5], p[6], p[7], p[8], p[9], p[10], D);
     c.check_launch("k_march");
+    c.prof_end(tok);
+}
+
+// the fused transpose and march of a sharded run: the modes of this rank's pencil, every slice read from and written to
+// the slab of the rank that holds it (sp: the slabs' mapped buffers)
+void launch_march_peer(Ctx& c, const Geo& g, const SlabPeers& sp, double D) {
+    const int tok = c.prof_begin("march_peer");
+    if (2 * g.nkh < 2L * 148 * 64) {
+        const unsigned blocks = unsigned((2 * g.nkh + 31) / 32);
+        const size_t smem = size_t(6) * slot_doubles(32) * sizeof(double);
+        smem_attr(reinterpret_cast<const void*>(k_march<cpx, 32, 6, true>), smem);
+        if (blocks) k_march<cpx, 32, 6, true><<<blocks, 32, smem, c.stream>>>(g, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, D, sp);
+    } else {
+        const unsigned blocks = unsigned((2 * g.nkh + 63) / 64);
+        const size_t smem = size_t(6) * slot_doubles(64) * sizeof(double);
+        smem_attr(reinterpret_cast<const void*>(k_march<cpx, 64, 6, true>), smem);
+        k_march<cpx, 64, 6, true><<<blocks, 64, smem, c.stream>>>(g, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, D, sp);
+    }
+    c.check_launch("k_march_peer");
     c.prof_end(tok);
 }
 

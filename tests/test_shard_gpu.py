@@ -39,13 +39,15 @@ def _cases():
     }
 
 
-def _rank(rank, world, port, name, out):
+def _rank(rank, world, port, name, mode, out):
     import sys
     repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, os.path.join(repo, "gem-pic-3d_b200"))
     import torch
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    if mode == "transpose":
+        os.environ["G3D_SHARD_TRANSPOSE"] = "1"
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         torch.cuda.set_device(0)
@@ -69,6 +71,7 @@ def _rank(rank, world, port, name, out):
         np0 = sh.status().np
         full.init_fields()
         sh.init_fields()
+        sh.profile(True)
         res = []
         for step in range(cfg.steps + 1):
             if step:
@@ -104,7 +107,7 @@ def _rank(rank, world, port, name, out):
             d_full, d_sh = full.diagnostics_sums(), sh.diagnostics_sums()
             err["diag"] = max(abs(d_sh[k] - d_full[k]) / max(abs(d_full[k]), 1e-300) for k in range(16))
             res.append(err)
-        out[rank] = (res, np0, sh.status().np, comm.calls)
+        out[rank] = (res, np0, sh.status().np, comm.calls, sorted(sh.profile_results()))
         full.close()
         sh.close()
     finally:
@@ -117,14 +120,21 @@ def dist_all_ids(dist, ids):
     return np.concatenate([np.asarray(g, dtype=np.int64) for g in got])
 
 
-@pytest.mark.parametrize("name,world", [("laser_bunch", 2), ("laser_bunch", 3), ("oblique16", 2)])
-def test_sharded_run_matches_the_whole_window(name, world):
+@pytest.mark.parametrize("name,world,mode", [("laser_bunch", 2, "peer"), ("laser_bunch", 3, "peer"), ("oblique16", 2, "peer"),
+                                             ("laser_bunch", 2, "transpose"), ("laser_bunch", 3, "transpose")])
+def test_sharded_run_matches_the_whole_window(name, world, mode):
+    """mode peer: the march reads and writes the other ranks' slabs through CUDA IPC mappings (one fused kernel);
+    transpose (G3D_SHARD_TRANSPOSE): the all-to-all transposes around the pencil march."""
     port = _free_port()
     out = mp.get_context("spawn").Manager().dict()
-    mp.start_processes(_rank, args=(world, port, name, out), nprocs=world, start_method="spawn", join=True)
+    mp.start_processes(_rank, args=(world, port, name, mode, out), nprocs=world, start_method="spawn", join=True)
     handed = 0
     for r in range(world):
-        res, np0, np_end, calls = out[r]
+        res, np0, np_end, calls, kernels = out[r]
+        if mode == "peer":
+            assert "march_peer" in kernels and "shard_transpose" not in kernels, kernels
+        else:
+            assert "shard_transpose" in kernels and "march_peer" not in kernels, kernels
         handed += max(0, np0 - np_end) if r > 0 else 0
         assert calls > 0
         for s, e in enumerate(res):
