@@ -185,6 +185,7 @@ struct Ctx {
     DevBuf<cpx> j0x, j0y, jkx, jky, jkz;         // ns+1 half-cell planes
     DevBuf<cpx> jzg;                             // 2 ghost planes of filtered j_z (zero on one rank)
     DevBuf<double> jw;                           // 3 x (ns+3) real planes
+    bool jw_fixed = false;                       // jw holds the fixed-point deposit's integers (Fourier y, FP64)
     DevBuf<double> depfix;                       // the fixed-point deposit's bound partials and scale (k_currents.cu)
     double ia_max = 0;                           // the largest dual-cell factor 1/A_j, 1/Delta_j of the y grid
     DevBuf<float> F;                             // 6 x (ns+2) real planes

@@ -913,7 +913,9 @@ static ArrayRef array_ref(Ctx& c, int which) {
         case G3D_A_JKX: cb = c.jk_is_j0 ? &c.j0x : &c.jkx; planes = c.ns + 1; break;
         case G3D_A_JKY: cb = c.jk_is_j0 ? &c.j0y : &c.jky; planes = c.ns + 1; break;
         case G3D_A_JKZ: cb = &c.jkz; planes = c.ns + 1; break;
-        case G3D_A_JW: return ArrayRef{c.jw.p, c.jw.n, sizeof(double), 0, false};
+        case G3D_A_JW:
+            if (c.jw_fixed) launch_deposit_finish(c);   // the reference's doubles at the boundary
+            return ArrayRef{c.jw.p, c.jw.n, sizeof(double), 0, false};
         case G3D_A_F: return ArrayRef{c.F.p, c.F.n, sizeof(float), 0, false};
         default: throw Error(G3D_ERR_ARG, "unknown array id " + std::to_string(which));
     }

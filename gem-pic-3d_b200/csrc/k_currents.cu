@@ -5,10 +5,12 @@
 // columns, [plane][j][k_x]).
 //   k_deposit   one thread per particle: NGP over the zeta half-cell, TSC in x and y, into the raw current planes
 //               jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106) as fixed-point integer adds (see below), so that
-//               the sums, and the whole run, do not depend on the order of the adds
+//               the sums, and the whole run, do not depend on the order of the adds; the lanes of a warp that hit
+//               the same point add their integers in the warp first (one atomic per point and warp)
 //   k_cur_rows  per (block of rows, half-cell plane): zeta filter (sim_particles.cpp:120-138) of the three raw
-//               planes, then per row one complex FFT along x of jx + i jy, split by Hermitian symmetry into the
-//               half spectra of jx and jy, and one of jz -> three half-spectrum planes (scratch W0, W1, W2)
+//               planes (read as the deposit's integers and scaled to doubles on the way in), then per row one
+//               complex FFT along x of jx + i jy, split by Hermitian symmetry into the half spectra of jx and jy,
+//               and one of jz -> three half-spectrum planes (scratch W0, W1, W2)
 //   k_cur_cols  per (half-cell plane, tile of 8 k_x columns): FFT along y, the cos^2 filters and the k_perp = 0
 //               removal (sim_particles.cpp:146-156) -> jkx, jky, jkz
 #include <algorithm>
@@ -75,9 +77,6 @@ __global__ void k_dep_scale(const double* __restrict__ tot, double* __restrict__
         scale[threadIdx.x] = ldexp(1.0, e); scale[3 + threadIdx.x] = ldexp(1.0, -e);
     }
 }
-__device__ __forceinline__ void fix_add(double* p, double v, double sc) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(__double2ll_rn(v * sc)));
-}
 // pl: the values of one component (its planes)
 __global__ void k_fix_to_double(double* __restrict__ J, long n, long pl, const double* __restrict__ scale) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
@@ -86,35 +85,67 @@ __global__ void k_fix_to_double(double* __restrict__ J, long n, long pl, const d
     }
 }
 
+// The sum of a 64-bit integer over the lanes of grp (exact, modulo 2^64 as the atomic adds are): three 21-bit
+// chunks summed by the warp's integer reduction (each chunk sum < 2^27), put back together.
+__device__ __forceinline__ unsigned long long group_sum(unsigned grp, unsigned long long u) {
+    const unsigned long long s0 = __reduce_add_sync(grp, unsigned(u & 0x1FFFFFull));
+    const unsigned long long s1 = __reduce_add_sync(grp, unsigned((u >> 21) & 0x1FFFFFull));
+    const unsigned long long s2 = __reduce_add_sync(grp, unsigned(u >> 42));
+    return s0 + (s1 << 21) + (s2 << 42);
+}
+
+// One thread per particle in cell order. The lanes of a warp that add into the same point (a sorted bunch puts many
+// in one cell) first sum their integers in the warp and one of them adds the sum: the same total as their separate
+// adds, since integer addition is exact, with up to 32 times fewer atomics on the contended points. Every lane takes
+// part in the warp steps (a lane without a particle has a key of its own and adds nothing).
 __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
                                                 double* __restrict__ J, const double* __restrict__ scale) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= np) return;
-    const long ip = perm[t];                 // cell order: neighbouring threads add into the same lines
-    if (P.alive[ip] != 1) return;
-    int m; double fz;
-    g.zax.locate(P.zeta[ip], m, fz);
-    const int hw = m - (g.a - 2);
-    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
-    const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
-    const double gm = sqrt(1 + px * px + py * py + pz * pz);
-    const double vx = px / gm, vy = py / gm, vz = pz / gm;
-    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
-    int ix[3], jn[3]; double wx[3], wn[3];
-    tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
-    tsc_periodic(P.y[ip], g.dy, g.ny, jn, wn);
+    const int lane = int(threadIdx.x & 31);
+    bool ok = t < np;
+    long ip = 0;
+    if (ok) { ip = perm[t]; ok = P.alive[ip] == 1; }      // cell order: neighbouring threads add into the same lines
+    int m = 0, hw = 0;
+    double fz;
+    if (ok) {
+        g.zax.locate(P.zeta[ip], m, fz);
+        hw = m - (g.a - 2);
+        ok = !(hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2);
+    }
+    double vx = 0, vy = 0, vz = 1, f = 0;
+    int ix[3] = {0, 0, 0}, jn[3] = {0, 0, 0};
+    double wx[3] = {0, 0, 0}, wn[3] = {0, 0, 0};
+    if (ok) {
+        const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
+        const double gm = sqrt(1 + px * px + py * py + pz * pz);
+        vx = px / gm; vy = py / gm; vz = pz / gm;
+        f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
+        tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
+        tsc_periodic(P.y[ip], g.dy, g.ny, jn, wn);
+    }
     const double ia0 = g.iA[0];
     const long nk = g.nk, pl = long(g.nh) * nk;
-    double* J0 = J + long(hw) * nk;
+    unsigned long long* J0 = reinterpret_cast<unsigned long long*>(J) + long(hw) * nk;
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const long k = long(jn[v]) * g.nx + ix[u];
             const double w = f * wx[u] * wn[v] * ia0;
-            fix_add(J0 + k, w * vx / vz, scale[0]);
-            fix_add(J0 + pl + k, w * vy / vz, scale[1]);
-            fix_add(J0 + 2 * pl + k, w, scale[2]);
+            unsigned long long q0 = 0, q1 = 0, q2 = 0;
+            if (ok) {
+                q0 = static_cast<unsigned long long>(__double2ll_rn(w * vx / vz * scale[0]));
+                q1 = static_cast<unsigned long long>(__double2ll_rn(w * vy / vz * scale[1]));
+                q2 = static_cast<unsigned long long>(__double2ll_rn(w * scale[2]));
+            }
+            const unsigned long long key = ok ? static_cast<unsigned long long>(long(hw) * nk + k) : ~static_cast<unsigned long long>(lane);
+            const unsigned grp = __match_any_sync(0xffffffffu, key);
+            q0 = group_sum(grp, q0); q1 = group_sum(grp, q1); q2 = group_sum(grp, q2);
+            if (ok && lane == __ffs(grp) - 1) {
+                atomicAdd(J0 + k, q0);
+                atomicAdd(J0 + pl + k, q1);
+                atomicAdd(J0 + 2 * pl + k, q2);
+            }
         }
 }
 
@@ -124,9 +155,13 @@ constexpr int CUR_NT = 128;     // threads of the row kernel
 // One CTA = LPC rows of one half-cell plane. The filter reads the three raw planes hk, hk+1, hk+2; the CTAs
 // of neighbouring planes run together (blockIdx.x = rows is the fast index), so each raw plane comes from
 // DRAM once and from L2 for its two neighbours.
+// iscale (the fixed-point deposit's 2^-e_c per component, or null): the raw planes still hold the deposit's 64-bit
+// integers, turned into doubles here as they are read (the same product as k_fix_to_double, without its pass over
+// the planes)
 template <int NX>
 __global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __restrict__ J, cpx* __restrict__ TX,
-                                                    cpx* __restrict__ TY, cpx* __restrict__ TZ, int zf) {
+                                                    cpx* __restrict__ TY, cpx* __restrict__ TZ, int zf,
+                                                    const double* __restrict__ iscale) {
     using S = FftShape<NX>;
     constexpr int LPC = CUR_NT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -149,7 +184,15 @@ __global__ void __launch_bounds__(CUR_NT) k_cur_rows(Geo g, const double* __rest
 #pragma unroll
             for (int comp = 0; comp < 3; ++comp) {
                 const double* Jc = J + comp * cpl + i;
-                const double jm = __ldg(Jc + (hw - 1) * nk), j0 = __ldg(Jc + hw * nk), jp = __ldg(Jc + (hw + 1) * nk);
+                double jm, j0, jp;
+                if (iscale) {
+                    const long long* Qc = reinterpret_cast<const long long*>(Jc);
+                    const double sc = iscale[comp];
+                    jm = double(__ldg(Qc + (hw - 1) * nk)) * sc; j0 = double(__ldg(Qc + hw * nk)) * sc;
+                    jp = double(__ldg(Qc + (hw + 1) * nk)) * sc;
+                } else {
+                    jm = __ldg(Jc + (hw - 1) * nk); j0 = __ldg(Jc + hw * nk); jp = __ldg(Jc + (hw + 1) * nk);
+                }
                 if (zf && g.zeta_uniform) v[comp] = 0.25 * jm + 0.5 * j0 + 0.25 * jp;
                 else if (zf) v[comp] = (wm * jm + w0 * j0 + wp * jp) / inv;
                 else v[comp] = j0;
@@ -276,8 +319,9 @@ const double* launch_deposit_scale(Ctx& c, double ia_max) {
     c.check_launch("k_dep_scale");
     return c.depfix.p + 3 * DB;
 }
-// the fixed-point planes back to doubles
+// the fixed-point planes back to doubles (the free-hand deposit, and the raw planes read through the ABI)
 void launch_deposit_finish(Ctx& c) {
+    c.jw_fixed = false;
     const long n = long(c.jw.n);
     const long b = std::min<long>((n + 255) / 256, 148 * 16);
     k_fix_to_double<<<unsigned(b), 256, 0, c.stream>>>(c.jw.p, n, n / 3, c.depfix.p + 3 * DB);
@@ -285,6 +329,7 @@ void launch_deposit_finish(Ctx& c) {
 }
 void launch_deposit(Ctx& c) {
     c.jw.zero(c.stream);
+    c.jw_fixed = false;                              // zero planes read the same either way
     if (c.np == 0 && !c.sharded()) return;           // a sharded rank without particles still takes part in the sums
     const int tok = c.prof_begin("deposit");
     const double* scale = launch_deposit_scale(c, 1 / c.dy);
@@ -293,8 +338,8 @@ void launch_deposit(Ctx& c) {
         k_deposit<<<blocks, 256, 0, c.stream>>>(c.parts, c.perm.p, c.np, c.geo(), c.jw.p, scale);
         c.check_launch("k_deposit");
     }
-    launch_deposit_finish(c);
-    if (c.sharded()) shard_raw_halo(c);
+    c.jw_fixed = true;                               // k_cur_rows turns the integers into doubles as it reads them
+    if (c.sharded()) shard_raw_halo(c);              // integer planes of one global scale: copied as they are
     c.prof_end(tok);
 }
 
@@ -307,7 +352,8 @@ static void cur_rows(Ctx& c, cpx* TX, cpx* TY, cpx* TZ) {
     smem_attr(reinterpret_cast<const void*>(kern), smem);
     const dim3 grid(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1));
     const int tok = c.prof_begin("cur_rows");
-    kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, TX, TY, TZ, c.P.zeta_filter ? 1 : 0);
+    kern<<<grid, CUR_NT, smem, c.stream>>>(c.geo(), c.jw.p, TX, TY, TZ, c.P.zeta_filter ? 1 : 0,
+                                           c.jw_fixed ? c.depfix.p + 3 * DB + 3 : nullptr);
     c.check_launch("k_cur_rows");
     c.prof_end(tok);
 }
