@@ -5,8 +5,7 @@
 // columns, [plane][j][k_x]).
 //   k_deposit   one thread per particle: NGP over the zeta half-cell, TSC in x and y, into the raw current planes
 //               jw [3][ns+3][ny][nx] (sim_particles.cpp:66-106) as fixed-point integer adds (see below), so that
-//               the sums, and the whole run, do not depend on the order of the adds; the lanes of a warp that hit
-//               the same point add their integers in the warp first (one atomic per point and warp)
+//               the sums, and the whole run, do not depend on the order of the adds
 //   k_cur_rows  per (block of rows, half-cell plane): zeta filter (sim_particles.cpp:120-138) of the three raw
 //               planes (read as the deposit's integers and scaled to doubles on the way in), then per row one
 //               complex FFT along x of jx + i jy, split by Hermitian symmetry into the half spectra of jx and jy,
@@ -85,67 +84,42 @@ __global__ void k_fix_to_double(double* __restrict__ J, long n, long pl, const d
     }
 }
 
-// The sum of a 64-bit integer over the lanes of grp (exact, modulo 2^64 as the atomic adds are): three 21-bit
-// chunks summed by the warp's integer reduction (each chunk sum < 2^27), put back together.
-__device__ __forceinline__ unsigned long long group_sum(unsigned grp, unsigned long long u) {
-    const unsigned long long s0 = __reduce_add_sync(grp, unsigned(u & 0x1FFFFFull));
-    const unsigned long long s1 = __reduce_add_sync(grp, unsigned((u >> 21) & 0x1FFFFFull));
-    const unsigned long long s2 = __reduce_add_sync(grp, unsigned(u >> 42));
-    return s0 + (s1 << 21) + (s2 << 42);
+__device__ __forceinline__ void fix_add(double* p, double v, double sc) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p), static_cast<unsigned long long>(__double2ll_rn(v * sc)));
 }
 
-// One thread per particle in cell order. The lanes of a warp that add into the same point (a sorted bunch puts many
-// in one cell) first sum their integers in the warp and one of them adds the sum: the same total as their separate
-// adds, since integer addition is exact, with up to 32 times fewer atomics on the contended points. Every lane takes
-// part in the warp steps (a lane without a particle has a key of its own and adds nothing).
+// One thread per particle in cell order, 27 integer atomics each. (Summing the lanes of a warp that hit the same point
+// first, with match-any and the warp's integer reductions, made this kernel 4x slower on the dense bunch of the
+// oblique-wave workload: the integer adds in L2 are not what bounds it.)
 __global__ void __launch_bounds__(256) k_deposit(PartsDev P, const int32_t* __restrict__ perm, long np, Geo g,
                                                 double* __restrict__ J, const double* __restrict__ scale) {
     const long t = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int lane = int(threadIdx.x & 31);
-    bool ok = t < np;
-    long ip = 0;
-    if (ok) { ip = perm[t]; ok = P.alive[ip] == 1; }      // cell order: neighbouring threads add into the same lines
-    int m = 0, hw = 0;
-    double fz;
-    if (ok) {
-        g.zax.locate(P.zeta[ip], m, fz);
-        hw = m - (g.a - 2);
-        ok = !(hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2);
-    }
-    double vx = 0, vy = 0, vz = 1, f = 0;
-    int ix[3] = {0, 0, 0}, jn[3] = {0, 0, 0};
-    double wx[3] = {0, 0, 0}, wn[3] = {0, 0, 0};
-    if (ok) {
-        const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
-        const double gm = sqrt(1 + px * px + py * py + pz * pz);
-        vx = px / gm; vy = py / gm; vz = pz / gm;
-        f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
-        tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
-        tsc_periodic(P.y[ip], g.dy, g.ny, jn, wn);
-    }
+    if (t >= np) return;
+    const long ip = perm[t];                 // cell order: neighbouring threads add into the same lines
+    if (P.alive[ip] != 1) return;
+    int m; double fz;
+    g.zax.locate(P.zeta[ip], m, fz);
+    const int hw = m - (g.a - 2);
+    if (hw < 0 || hw >= g.nh || m < 0 || m > g.N - 2) return;
+    const double px = P.px[ip], py = P.py[ip], pz = P.pz[ip];
+    const double gm = sqrt(1 + px * px + py * py + pz * pz);
+    const double vx = px / gm, vy = py / gm, vz = pz / gm;
+    const double f = P.q[ip] * P.w[ip] / (g.hcg[m + 2] * g.dx);
+    int ix[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(P.x[ip], g.dx, g.nx, ix, wx);
+    tsc_periodic(P.y[ip], g.dy, g.ny, jn, wn);
     const double ia0 = g.iA[0];
     const long nk = g.nk, pl = long(g.nh) * nk;
-    unsigned long long* J0 = reinterpret_cast<unsigned long long*>(J) + long(hw) * nk;
+    double* J0 = J + long(hw) * nk;
 #pragma unroll
     for (int v = 0; v < 3; ++v)
 #pragma unroll
         for (int u = 0; u < 3; ++u) {
             const long k = long(jn[v]) * g.nx + ix[u];
             const double w = f * wx[u] * wn[v] * ia0;
-            unsigned long long q0 = 0, q1 = 0, q2 = 0;
-            if (ok) {
-                q0 = static_cast<unsigned long long>(__double2ll_rn(w * vx / vz * scale[0]));
-                q1 = static_cast<unsigned long long>(__double2ll_rn(w * vy / vz * scale[1]));
-                q2 = static_cast<unsigned long long>(__double2ll_rn(w * scale[2]));
-            }
-            const unsigned long long key = ok ? static_cast<unsigned long long>(long(hw) * nk + k) : ~static_cast<unsigned long long>(lane);
-            const unsigned grp = __match_any_sync(0xffffffffu, key);
-            q0 = group_sum(grp, q0); q1 = group_sum(grp, q1); q2 = group_sum(grp, q2);
-            if (ok && lane == __ffs(grp) - 1) {
-                atomicAdd(J0 + k, q0);
-                atomicAdd(J0 + pl + k, q1);
-                atomicAdd(J0 + 2 * pl + k, q2);
-            }
+            fix_add(J0 + k, w * vx / vz, scale[0]);
+            fix_add(J0 + pl + k, w * vy / vz, scale[1]);
+            fix_add(J0 + 2 * pl + k, w, scale[2]);
         }
 }
 
