@@ -2,10 +2,13 @@
 // y axis lookup, TSC weights, and the error plumbing of the C-ABI.
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #define G3D_HD __host__ __device__ __forceinline__
 
@@ -87,6 +90,11 @@ struct AxisDev {
     const double* X;            // nodes (device), n of them
     int n, uniform;
     double x0, ih;
+    // a non-uniform axis on the device: bins of width <= its smallest cell from X[0], bins[b] the last node at or
+    // below the bin's start, so a point's cell is one table load and a step or two away (null: a binary search)
+    const int* bins = nullptr;
+    int nb = 0;
+    double bih = 0;
     G3D_HD void locate(double x, int& i, double& f) const {
         if (uniform) { const double t = (x - x0) * ih; i = int(floor(t)); f = t - i; return; }
         if (x < X[0]) { const double t = (x - X[0]) / (X[1] - X[0]); i = int(floor(t)); f = t - i; return; }
@@ -95,11 +103,38 @@ struct AxisDev {
             const int k = int(floor(t));
             i = n - 1 + k; f = t - k; return;
         }
-        int lo = 0, hi = n - 1;
-        while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (X[m] <= x) lo = m; else hi = m; }
+        int lo;
+        if (bins) {            // the same cell as the search below: the one lo with X[lo] <= x < X[lo + 1]
+            int b = int((x - X[0]) * bih);
+            b = b < 0 ? 0 : (b >= nb ? nb - 1 : b);
+            lo = bins[b];
+            while (lo > 0 && X[lo] > x) --lo;
+            while (lo < n - 2 && X[lo + 1] <= x) ++lo;
+        } else {
+            lo = 0;
+            int hi = n - 1;
+            while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (X[m] <= x) lo = m; else hi = m; }
+        }
         i = lo; f = (x - X[lo]) / (X[lo + 1] - X[lo]);
     }
 };
+// the bin table of a non-uniform axis (host): nb bins of width <= its smallest cell
+inline std::vector<int> axis_bins(const std::vector<double>& X, double& bih) {
+    const size_t n = X.size();
+    double hmin = 1e300;
+    for (size_t k = 0; k + 1 < n; ++k) hmin = std::min(hmin, X[k + 1] - X[k]);
+    const double span = X[n - 1] - X[0];
+    const long nb = std::max<long>(1, std::min<long>(long(std::ceil(span / hmin)) + 1, 1L << 22));
+    bih = double(nb) / span;
+    std::vector<int> bins(size_t(nb), 0);
+    int lo = 0;
+    for (long b = 0; b < nb; ++b) {
+        const double start = X[0] + double(b) / bih;
+        while (lo + 2 < int(n) && X[size_t(lo) + 1] <= start) ++lo;
+        bins[size_t(b)] = lo;
+    }
+    return bins;
+}
 
 // Quadratic (TSC) weights of the three points around the nearest integer of the index coordinate
 // (reference tsc_index, src/sim_kernels.hpp:21-26).

@@ -175,6 +175,7 @@ struct Ctx {
     // tables
     DevBuf<double> kxd, kxs, filt, maskx, kyd, kys, filty, masky_n, masky_h, iD, iA;
     DevBuf<double> zs, hcg, wlo, whi, wsl;
+    DevBuf<int> zbins, ybins;                    // bin tables of the graded zeta axis and the free-hand y axis
     DevBuf<cpx> twx, twy;
     DevBuf<double> yn, pcp, pid, evf, evb, evl;  // free-hand y tables (empty for Fourier y)
     std::vector<double> ynode_h;

@@ -286,6 +286,10 @@ static void setup_y_free(Ctx& c, const g3d_grid& G, const g3d_params& P, cudaStr
     c.masky_n.upload(mask_node, s); c.masky_h.upload(mask_half, s);
     const bool equal_cells = std::all_of(cell.begin(), cell.end(), [&](double d) { return d == cell[0]; });
     c.yax = AxisDev{c.yn.p, ny + 1, equal_cells ? 1 : 0, node[0], 1 / cell[0]};
+    if (!equal_cells) {
+        c.ybins.upload(axis_bins(node, c.yax.bih), s);
+        c.yax.bins = c.ybins.p; c.yax.nb = int(c.ybins.n);
+    }
     // the y tables of the Fourier form are not used; zeros keep the device pointers valid
     const std::vector<double> zero(static_cast<size_t>(ny), 0.0);
     c.kyd.upload(zero, s); c.kys.upload(zero, s); c.filty.upload(zero, s);
@@ -435,6 +439,10 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.zs.upload(Z, s); c.hcg.upload(g, s); c.wlo.upload(lo, s); c.whi.upload(hi2, s); c.wsl.upload(ws, s);
     c.hcg_h = g; c.wlo_h = lo; c.whi_h = hi2; c.wsl_h = ws;
     c.zax = AxisDev{c.zs.p, N, uni ? 1 : 0, 0.0, 1 / hh[0]};
+    if (!uni) {
+        c.zbins.upload(axis_bins(Z, c.zax.bih), s);
+        c.zax.bins = c.zbins.p; c.zax.nb = int(c.zbins.n);
+    }
     c.hmin = 1e300;
     for (int m = 0; m + 1 < N; ++m) c.hmin = std::min(c.hmin, Z[m + 1] - Z[m]);
     // twiddles exp(-2 pi i s / n)
