@@ -295,6 +295,7 @@ void launch_march_slice_fh(Ctx& c, double D, int n);
 struct FmidOut {
     void* out = nullptr;
     int other = 0, f32 = 0;
+    int fh = 0;               // free-hand y (FP32): per point (E_x, E_z, B_y, 0) of the node row, (E_y, B_x, B_z, 0) of the half-node row
 };
 // the other slice's six values at point k (loaded by the rows kernel before it stores its own slice: the other
 // slice is never this one, so the loads need not wait behind those stores)
@@ -306,7 +307,11 @@ __device__ __forceinline__ void fmid_store(const FmidOut& fm, long k, const floa
     double m[6];
 #pragma unroll
     for (int comp = 0; comp < 6; ++comp) m[comp] = 0.5 * (double(v[comp]) + double(oth[comp]));
-    if (fm.f32) {
+    if (fm.fh) {
+        float4* o = reinterpret_cast<float4*>(fm.out) + 2 * k;
+        o[0] = make_float4(float(m[0]), float(m[2]), float(m[4]), 0.f);
+        o[1] = make_float4(float(m[1]), float(m[3]), float(m[5]), 0.f);
+    } else if (fm.f32) {
         float4* o = reinterpret_cast<float4*>(fm.out) + 2 * k;
         o[0] = make_float4(float(m[0]), float(m[1]), float(m[2]), float(m[3]));
         o[1] = make_float4(float(m[4]), float(m[5]), 0.f, 0.f);
@@ -315,7 +320,7 @@ __device__ __forceinline__ void fmid_store(const FmidOut& fm, long k, const floa
         o[0] = make_double2(m[0], m[1]); o[1] = make_double2(m[2], m[3]); o[2] = make_double2(m[4], m[5]);
     }
 }
-void launch_real_fields_slice_fh(Ctx& c, int l);
+void launch_real_fields_slice_fh(Ctx& c, int l, FmidOut fm = FmidOut());
 void launch_ss_lines_fh(Ctx& c, const cpx* T3, cpx* out3, double a2);
 void launch_sp_rows(Ctx& c);                // k_fields.cu
 void launch_cur_rows_to_jk(Ctx& c);         // k_currents.cu

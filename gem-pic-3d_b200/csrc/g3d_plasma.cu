@@ -105,7 +105,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     for (DevBuf<cpx>* b : {&pl->js0x, &pl->js0y, &pl->js0z}) b->alloc(size_t(c.ns + 1) * ph, s);
     pl->jsr.alloc(size_t(5) * c.nk, s);
     pl->jsrf.alloc(size_t(5) * c.nk, s);               // FP32: three planes, or on the Fourier y grid (jx, jy, jz, 0) per point
-    if (c.yf) pl->fmid.alloc(size_t(6) * c.nk, s);      // 6 doubles or 8 floats per point
+    if (c.yf || c.f32s) pl->fmid.alloc(size_t(6) * c.nk, s);      // 6 doubles or 8 floats per point
     pl->stepv.alloc(1, s);
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
     pl->bk.alloc(4 * ph, s);
@@ -367,13 +367,14 @@ static uint64_t mix64h(uint64_t z) {
 // E and B of slice l; Fourier y: with the midpoint fields of slice `target` (l for the next pass of half-cell l,
 // l - 1 for the first pass of half-cell l - 1, -1: none) for the streaming gather
 static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true) {
-    if (!c.yf) { launch_real_fields_slice_fh(c, l); return; }
     FmidOut fm;
-    if (target >= c.a) {
+    if (target >= c.a && (c.yf || c.f32s) && c.pl->fmid.p) {   // free-hand y: the mixed form's FP32 gather only
         fm.out = c.pl->fmid.p;
         fm.other = (target == l ? l + 1 : l - 1) - c.a;
         fm.f32 = c.f32s ? 1 : 0;
+        fm.fh = c.yf ? 0 : 1;
     }
+    if (!c.yf) { launch_real_fields_slice_fh(c, l, fm); return; }
     if (c.mixed) launch_real_fields_slice_f(c, l, fm, cols);
     else launch_real_fields_slice(c, l, fm, cols);
 }
@@ -429,7 +430,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.J = P.jsr.p; sa.Jf = P.jsrf.p; sa.ions = P.ion_dev.p; sa.adk = P.adk_dev.p; sa.sd = P.sdev.p; sa.bcnt = P.bcnt.p;
         sa.bcap = ionz ? int(P.born_cap) : 0; sa.dry = 0; sa.n = 0; sa.pass = 0;
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
-        sa.Fmid = c.yf ? static_cast<const void*>(P.fmid.p) : nullptr;
+        sa.Fmid = c.yf || c.f32s ? static_cast<const void*>(P.fmid.p) : nullptr;   // null if never allocated
         sa.inv_dx = 1 / c.dx; sa.inv_dy = 1 / c.dy; sa.dep_norm = 0;
         sa.ext = c.ext;
         for (int n = nhi; n >= c.a; --n) {

@@ -573,18 +573,18 @@ void launch_real_fields(Ctx& c) {
 }
 // free-hand y: the spectra are already real in y; one inverse transform along x per row of R, L and E_z + i B_z
 template <int NX>
-static void rf_rows_direct(Ctx& c, int l0, int nl) {
+static void rf_rows_direct(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
     allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
     k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0, c.Fd.p, FmidOut());
+        c.geo(), c.Rx.p, c.Ry.p, c.Lx.p, c.Ly.p, c.Ez.p, c.Bz.p, c.F.p, l0, c.Fd.p, fm);
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }
 void launch_real_fields_fh(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, rf_rows_direct<NX>(c, 0, c.ns)); }
-void launch_real_fields_slice_fh(Ctx& c, int l) { G3D_DISPATCH_N(c.nx, NX, rf_rows_direct<NX>(c, l, 1)); }
+void launch_real_fields_slice_fh(Ctx& c, int l, FmidOut fm) { G3D_DISPATCH_N(c.nx, NX, rf_rows_direct<NX>(c, l, 1, fm)); }
 // the sponge's row pass alone (inverse x, mask, forward x) on W0, W1: the free-hand y sponge
 void launch_sp_rows(Ctx& c) { G3D_DISPATCH_N(c.nx, NX, sp_rows<NX>(c)); }
 // E and B of one slice (plane l) in real space (Simulation::real_fields_slice, src/sim_plasma.cpp:200-220)

@@ -168,6 +168,35 @@ __device__ __forceinline__ void sgather_mid_f32(const StreamArgs& c, double x, d
         }
     E[0] = a[0]; E[1] = a[1]; E[2] = a[2]; B[0] = a[3]; B[1] = a[4]; B[2] = a[5];
 }
+// The mixed form's midpoint gather on the free-hand y grid: per TSC point one float4 of the node row (E_x, E_z, B_y)
+// and one of the half-node row (E_y, B_x, B_z) of the interleaved midpoint fields, rows beyond the walls left out
+// (as sgather does); the weights as in sgather's FP32 form (FP64 TSC weights, their products rounded to FP32).
+__device__ __forceinline__ void sgather_mid_fh_f32(const StreamArgs& c, double x, double y, float E[3], float B[3]) {
+    const Geo& g = c.g;
+    int ix[3], jn[3], jh[3]; double wx[3], wn[3], wh[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_y(g.yax, y, jn, wn, jh, wh);
+    float a[6] = {0, 0, 0, 0, 0, 0};
+    const float4* F4 = reinterpret_cast<const float4*>(c.Fmid);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const bool nod = jn[j] >= 0 && jn[j] < g.ny, hal = jh[j] >= 0 && jh[j] < g.ny;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (nod) {
+                const float w = float(wx[i] * wn[j]);
+                const float4 u = __ldg(F4 + 2 * (long(jn[j]) * g.nx + ix[i]));
+                a[0] += w * u.x; a[2] += w * u.y; a[4] += w * u.z;
+            }
+            if (hal) {
+                const float w = float(wx[i] * wh[j]);
+                const float4 v = __ldg(F4 + 2 * (long(jh[j]) * g.nx + ix[i]) + 1);
+                a[1] += w * v.x; a[3] += w * v.y; a[5] += w * v.z;
+            }
+        }
+    }
+    E[0] = a[0]; E[1] = a[1]; E[2] = a[2]; B[0] = a[3]; B[1] = a[4]; B[2] = a[5];
+}
 // The mixed form's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
 __device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, double y, float f, float vx, float vy, float vz) {
     int ix[3], jn[3]; float wx[3], wn[3];
@@ -358,15 +387,16 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
         // a neutral atom: the Boris pushes below leave u exactly as it is whatever the (finite) fields, so they
         // are not gathered (the gas of an ionization-injection run is mostly neutral until the laser arrives)
         for (int k = 0; k < 3; ++k) { E[k] = A(0); B[k] = A(0); }
-    } else if (F32 && YF && mid && !LASER && !c.ext.any()) {
+    } else if (F32 && mid && !LASER && !c.ext.any()) {
         if constexpr (F32) {
             float Ef[3], Bf[3];
-            sgather_mid_f32(c, wrapx(g, xm), wrapy<YF>(g, ym), Ef, Bf);
+            if constexpr (YF) sgather_mid_f32(c, wrapx(g, xm), wrapy<YF>(g, ym), Ef, Bf);
+            else sgather_mid_fh_f32(c, wrapx(g, xm), ym, Ef, Bf);
             for (int k = 0; k < 3; ++k) { E[k] = A(Ef[k]); B[k] = A(Bf[k]); }
         }
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
-        if (mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy<YF>(g, ym), Ed, Bd);
+        if (YF && mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy<YF>(g, ym), Ed, Bd);   // free-hand: Fmid is FP32-only
         else sgather<F32, YF>(c, wrapx(g, xm), wrapy<YF>(g, ym), zetam, Ed, Bd);
         if constexpr (LASER) {
             c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
