@@ -207,6 +207,9 @@ struct Ctx {
     bool use_tma = true;
     TmaCache tma_rf, tma_cur, tma_spi, tma_spf;
     DevBuf<int> kerr;
+    long tma_polls = 1L << 24;
+    unsigned tma_extra = 0;
+    TmaWait tma_wait() { return TmaWait{kerr.p, tma_polls, tma_extra}; }
     bool jk_is_j0 = false;                       // after solve_fields jk == j0: the j0/jk buffers were swapped
     bool mixed = false;                          // G3D_PREC_MIXED: the spectra above except Rx, Ry are not allocated
     bool f32s = false;                           // G3D_PREC_MIXED: FP32 gathers and deposit of the streaming plasma

@@ -456,6 +456,8 @@ static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     c.red.alloc(size_t(297) * 17, s);
     c.kerr.alloc(1, s);
     c.use_tma = std::getenv("G3D_NO_TMA") == nullptr;
+    if (const char* v = std::getenv("G3D_TMA_POLLS")) c.tma_polls = std::max(1L, std::atol(v));
+    if (const char* v = std::getenv("G3D_TMA_EXTRA_BYTES")) c.tma_extra = unsigned(std::min(4096L, std::max(0L, std::atol(v))));
     // the plane wave (reference sim_setup.cpp:51-54; eta_c given directly)
     c.laser.on = P.laser_on; c.laser.pol = P.laser_pol; c.laser.env = P.laser_envelope;
     c.laser.a0 = P.a0; c.laser.kL = P.kL; c.laser.tau = P.tau; c.laser.cep = P.cep; c.laser.eta_c = P.eta_c;

@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_cur_cols(Geo g, const 
 template <int NY>
 __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_cur_cols_tma(Geo g, const __grid_constant__ TileMaps maps,
                                                                      cpx* __restrict__ JX, cpx* __restrict__ JY,
-                                                                     cpx* __restrict__ JZ, int keep0, int* __restrict__ err) {
+                                                                     cpx* __restrict__ JZ, int keep0, TmaWait wt) {
     using S = FftShape<NY>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_cur_cols_tma(Geo g, con
     cpx* s2 = s1 + NY * 8;
     const int idx[3] = {0, 1, 2};
     cpx* const dst[3] = {s0, s1, s2};
-    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, hk * g.ny, &bar, &ok, err)) return;
+    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, hk * g.ny, &bar, &ok, wt)) return;
     const int c = tid % 8, t = tid / 8;
     {
         decltype(s0) const ls_[3] = {s0, s1, s2};
@@ -345,7 +345,7 @@ static void cur_cols(Ctx& c, bool keep0) {
             smem_attr(reinterpret_cast<const void*>(k_cur_cols_tma<NY>), smem);
             const int tok = c.prof_begin("cur_cols");
             k_cur_cols_tma<NY><<<dim3(unsigned((c.H + 7) / 8), unsigned(c.ns + 1)), 8 * FftShape<NY>::T, smem, c.stream>>>(
-                c.geo(), c.tma_cur.maps, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0, c.kerr.p);
+                c.geo(), c.tma_cur.maps, c.jkx.p, c.jky.p, c.jkz.p, keep0 ? 1 : 0, c.tma_wait());
             c.check_launch("k_cur_cols_tma");
             c.prof_end(tok);
             return;

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_inv_tma(Geo g, 
                                                                         const cpx* __restrict__ jz, const cpx* __restrict__ jg,
                                                                         cpx* __restrict__ U, cpx* __restrict__ V,
                                                                         cpx* __restrict__ PSI, double g2, double opb,
-                                                                        int* __restrict__ err) {
+                                                                        TmaWait wt) {
     using S = FftShape<NY>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_inv_tma(Geo g, 
     cpx* s1 = s0 + NY * 8;
     const int idx[2] = {0, 1};
     cpx* const dst[2] = {s0, s1};
-    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, wt)) return;
     #pragma unroll
     for (int u_ = 0; u_ < (NY * 8 + nthr - 1) / nthr; ++u_) {
         const int e = tid + u_ * nthr;
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(CW * FftShape<NY>::T) k_sp_cols_fwd(Geo g, con
 template <int NY>
 __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_fwd_tma(Geo g, const __grid_constant__ TileMaps maps,
                                                                         cpx* __restrict__ Rx, cpx* __restrict__ Ry, double opb,
-                                                                        int* __restrict__ err) {
+                                                                        TmaWait wt) {
     using S = FftShape<NY>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_sp_cols_fwd_tma(Geo g, 
     cpx* s2 = s1 + NY * 8;
     const int idx[3] = {0, 1, 2};
     cpx* const dst[3] = {s0, s1, s2};
-    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    if (!tma_tiles<NY>(maps, idx, 3, dst, c0, l * g.ny, &bar, &ok, wt)) return;
     const int c = tid % 8, t = tid / 8;
     {
         decltype(s0) const ls_[2] = {s0, s1};
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_rf_cols_tma(Geo g, cons
                                                                     cpx* __restrict__ W0, cpx* __restrict__ W1,
                                                                     cpx* __restrict__ W2, cpx* __restrict__ W3,
                                                                     cpx* __restrict__ W4, cpx* __restrict__ W5, int l0,
-                                                                    int* __restrict__ err) {
+                                                                    TmaWait wt) {
     using S = FftShape<NY>;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_rf_cols_tma(Geo g, cons
     cpx* out1 = pr == 0 ? W1 : pr == 1 ? W3 : W5;
     const int idx[2] = {2 * pr, 2 * pr + 1};
     cpx* const dst[2] = {s0, s1};
-    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, err)) return;
+    if (!tma_tiles<NY>(maps, idx, 2, dst, c0, l * g.ny, &bar, &ok, wt)) return;
     for (int e = tid; e < NY * 8; e += nthr) { s0[e] = conj(s0[e]); s1[e] = conj(s1[e]); }
     __syncthreads();
     const int c = tid % 8, t = tid / 8;
@@ -469,7 +469,7 @@ static void sp_cols_inv(Ctx& c) {
             allow_smem(k_sp_cols_inv_tma<NY>, smem);
             const int tok = c.prof_begin("sponge_cols_inv");
             k_sp_cols_inv_tma<NY><<<dim3(col_tiles(c), unsigned(c.ns)), 8 * FftShape<NY>::T, smem, c.stream>>>(
-                c.geo(), c.tma_spi.maps, c.jkz.p, c.jzg.p, c.W[0].p, c.W[1].p, c.W[3].p, c.gm2_b, 1 + c.beta_b, c.kerr.p);
+                c.geo(), c.tma_spi.maps, c.jkz.p, c.jzg.p, c.W[0].p, c.W[1].p, c.W[3].p, c.gm2_b, 1 + c.beta_b, c.tma_wait());
             c.check_launch("k_sp_cols_inv_tma");
             c.prof_end(tok);
             return;
@@ -502,7 +502,7 @@ static void sp_cols_fwd(Ctx& c) {
             allow_smem(k_sp_cols_fwd_tma<NY>, smem);
             const int tok = c.prof_begin("sponge_cols_fwd");
             k_sp_cols_fwd_tma<NY><<<dim3(col_tiles(c), unsigned(c.ns)), 8 * FftShape<NY>::T, smem, c.stream>>>(
-                c.geo(), c.tma_spf.maps, c.Rx.p, c.Ry.p, 1 + c.beta_b, c.kerr.p);
+                c.geo(), c.tma_spf.maps, c.Rx.p, c.Ry.p, 1 + c.beta_b, c.tma_wait());
             c.check_launch("k_sp_cols_fwd_tma");
             c.prof_end(tok);
             return;
@@ -545,7 +545,7 @@ static void rf_cols_tma(Ctx& c, int l0, int nl) {
     allow_smem(k_rf_cols_tma<NY>, smem);
     const int tok = c.prof_begin("real_cols");
     k_rf_cols_tma<NY><<<dim3(unsigned((c.H + 7) / 8), unsigned(nl), 3), 8 * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), c.tma_rf.maps, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, l0, c.kerr.p);
+        c.geo(), c.tma_rf.maps, c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, l0, c.tma_wait());
     c.check_launch("k_rf_cols_tma");
     c.prof_end(tok);
 }

@@ -19,6 +19,14 @@ namespace g3d {
 struct TileMaps {                                  // up to six tensor maps of one kernel (kernel parameter)
     CUtensorMap m[6];
 };
+// The bound of a kernel's tile waits: the error word, the polls of the barrier before giving up (2^24 unless
+// G3D_TMA_POLLS sets it), and bytes the barrier expects beyond the tiles (0; G3D_TMA_EXTRA_BYTES > 0 makes every wait
+// run out, for the test of the timeout path: the tiles land, the barrier's phase never completes).
+struct TmaWait {
+    int* err;
+    long polls;
+    unsigned extra;
+};
 
 // ---------------------------------------------------------------- host
 inline PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
@@ -78,15 +86,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
 // unit wrote are visible to it). On a timeout the error word gets bit 1 and every thread returns false.
 template <int NY>
 __device__ __forceinline__ bool tma_tiles(const TileMaps& maps, const int* idx, int n, cpx* const* dst, int c0, int y,
-                                          uint64_t* bar, int* ok, int* err) {
+                                          uint64_t* bar, int* ok, const TmaWait& w) {
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        mbar_expect_tx(bar, unsigned(n) * NY * 8 * sizeof(cpx));
+        mbar_expect_tx(bar, unsigned(n) * NY * 8 * sizeof(cpx) + w.extra);
         for (int k = 0; k < n; ++k) tma_load_2d(dst[k], &maps.m[idx[k]], bar, 2 * c0, y);
         bool done = false;
-        for (long it = 0; it < (1L << 24) && !done; ++it) done = mbar_try_wait(bar, 0);
+        for (long it = 0; it < w.polls && !done; ++it) done = mbar_try_wait(bar, 0);
         *ok = done ? 1 : 0;
-        if (!done) atomicOr(err, 1);
+        if (!done) atomicOr(w.err, 1);
     }
     __syncthreads();
     if (*ok == 0) return false;

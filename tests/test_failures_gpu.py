@@ -13,7 +13,7 @@ from conftest import REPO, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-G3D_ERR_CAPACITY, G3D_ERR_ARG, G3D_ERR_IO = 3, 4, 6
+G3D_ERR_TIMEOUT, G3D_ERR_CAPACITY, G3D_ERR_ARG, G3D_ERR_IO = 2, 3, 4, 6
 
 
 def small():
@@ -105,3 +105,36 @@ def test_freed_electron_overflow_gives_capacity_error():
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert f"code {G3D_ERR_CAPACITY}" in out.stdout and "overflowed" in out.stdout, out.stdout
+
+
+TIMEOUT_SCRIPT = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+from g3d import G3DError, Simulation, configs
+cfg = configs.config2(nx=16, ny=16, nzeta=32, nmacro=2000, steps=1, envelope=0)
+sim = Simulation(cfg)
+try:
+    sim.init()
+    print("no error")
+except G3DError as e:
+    print("code", e.code, str(e))
+sim.close()
+"""
+
+
+def test_tma_tile_wait_that_runs_out_gives_timeout():
+    """The TMA column kernels wait for their tiles on an mbarrier with a bounded number of polls. With the barrier
+    told to expect 16 bytes more than the tiles bring (G3D_TMA_EXTRA_BYTES, read at creation) its phase never
+    completes: every wait gives up after G3D_TMA_POLLS polls, sets the error word and returns, and the call reports
+    G3D_ERR_TIMEOUT. The tiles themselves land (no copy is left in flight) and the GPU stays usable: a context made
+    afterwards in this process, without the settings, runs the same start field and step."""
+    env = dict(os.environ, G3D_TMA_EXTRA_BYTES="16", G3D_TMA_POLLS="2000")
+    out = subprocess.run([sys.executable, "-c", TIMEOUT_SCRIPT, os.path.join(REPO, "gem-pic-3d_b200")], env=env,
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert f"code {G3D_ERR_TIMEOUT}" in out.stdout and "bounded wait" in out.stdout, out.stdout
+    from g3d import Simulation, configs
+    sim = Simulation(configs.config2(nx=16, ny=16, nzeta=32, nmacro=2000, steps=1, envelope=0))
+    sim.init()
+    sim.step()
+    sim.close()
