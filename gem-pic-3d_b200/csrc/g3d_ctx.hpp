@@ -195,6 +195,7 @@ struct Ctx {
     DevBuf<cpx> lmode;                           // laser mode coefficients per stored mode (ny x H), or empty
     DevBuf<cpx> lspx, lspy;                      // the grid-laser spectra added at init before the coefficients
     DevBuf<unsigned char> adjws;                 // workspace of the adjoint march, kept between calls
+    DevBuf<unsigned char> adjrec;                // the adjoint's record of one plasma march, kept between calls
     bool adj_after_start = false;                // dJ/dp with the start field held (G3D_ADJ_AFTER_START)
     // where the next real fields go instead of F / Fd (taken once by sponge_and_real_fields): the adjoint's forward
     // writes each level's fields straight into its checkpoint
@@ -388,8 +389,11 @@ void launch_adj_objective(Ctx& c, double* dev_out2);
 void launch_adj_seed(Ctx& c, double W, double* lam);
 void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const* lS);
 void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, double D, int accz = 0);
-void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ);
+void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ, bool keep0 = false);
 void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const double* lJ, double* lam);
+// one slice of the streaming-plasma march (k_adjoint.cu): the transposed real fields and current spectra
+void launch_adj_real_fields_slice(Ctx& c, const double* lF, long fpl, cpx* const* W, cpx* const* lsl);
+void launch_adj_stream_spectra(Ctx& c, cpx* const* ljsn, cpx* const* T, double* lJ, bool keep0, double a2);
 void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
                      double* lam, double* lF, int* err);
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out);

@@ -1127,7 +1127,9 @@ static void set_adjoint_momenta(Ctx& c, int mode) {
     c.adj_after_start = mode == G3D_ADJ_AFTER_START;
 }
 // From the start field (right after g3d_init): K s-steps forward with a checkpoint of the beam (x, y, zeta,
-// p, alive) and of the real fields at every level, J = mean p_z of the live beam, then the reverse sweep
+// p, alive) and of the real fields at every level (with a streaming plasma also the spectra R, E_z, B_z, j0 and the
+// streaming current js0: each step is run again from its level in the reverse sweep, with the march recorded, and
+// its march transposed, k_adj_plasma.cu), J = mean p_z of the live beam, then the reverse sweep
 // (k_adjoint.cu): per step the transposed real fields, march, currents, deposit and push; then init's march(0),
 // relaxation marches and co-moving fields back to the start currents and beta. Out: J, dJ/da per stored laser
 // mode [j][k_x] (complex, interleaved) and dJ/dp of every particle at s = 0 [np][3] through both the s-steps and
@@ -1138,7 +1140,14 @@ static void set_adjoint_momenta(Ctx& c, int mode) {
 static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p) {
     if (K < 1) throw Error(G3D_ERR_ARG, "the adjoint march needs at least one s-step");
     if (!c.yf) throw Error(G3D_ERR_ARG, "the adjoint march needs the Fourier y grid");
-    if (c.pl) throw Error(G3D_ERR_ARG, "the adjoint march of the streaming plasma is not in this release");
+    const bool plasma = c.pl != nullptr;
+    if (plasma) {
+        if (c.mixed || !c.Fd.p)
+            throw Error(G3D_ERR_ARG, "the adjoint of the streaming plasma differentiates the FP64 form with exact fields (g3d_set_exact_fields)");
+        if (c.pl->any_ionizing) throw Error(G3D_ERR_ARG, "the adjoint march does not differentiate ionization");
+        if (c.pl->njb || !c.pl->joining.empty())
+            throw Error(G3D_ERR_STATE, "the adjoint march starts with no particle waiting to join the streaming plasma");
+    }
     if (c.P.sponge > 0 || c.P.sponge_y > 0) throw Error(G3D_ERR_ARG, "the adjoint march needs sponge = 0");
     if (c.P.move_x || c.P.move_y) throw Error(G3D_ERR_ARG, "the adjoint march needs a fixed window (move_x = move_y = 0)");
     if (c.laser.on) throw Error(G3D_ERR_ARG, "the adjoint march differentiates grid lasers, not the analytic laser");
@@ -1168,6 +1177,12 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     // the start field's dependence on the bunch: j_z of the start currents, dJ/dR of the relaxation's beta part,
     // dJ/dbeta per mode
     const size_t ojz = carve((ns + 1) * nkh * sizeof(cpx)), odx = carve(2 * ns * nkh * sizeof(cpx)), odb = carve(nkh * 8);
+    // with a streaming plasma: per level the spectra R_x, R_y, E_z, B_z, j0 (x, y) and js0 (x, y, z); the adjoints of
+    // js0 and of one slice's values, the adjoint's carried planes and one plane each of transform scratch
+    const size_t lv = plasma ? size_t(K + 1) : 0, hp = (ns + 1) * nkh;
+    const size_t oSP = carve(lv * 4 * ns * nkh * sizeof(cpx)), oJ0 = carve(lv * 2 * hp * sizeof(cpx)), oJS = carve(lv * 3 * hp * sizeof(cpx));
+    const size_t ojs0 = carve(plasma ? 3 * hp * sizeof(cpx) : 0), osl = carve(plasma ? 31 * nkh * sizeof(cpx) : 0);
+    const size_t oFa = carve(plasma ? 21 * nk * 8 : 0);
     if (c.adjws.n < need) c.adjws.alloc(need, st);
     unsigned char* ws = c.adjws.p;
     double* X = reinterpret_cast<double*>(ws + oX);
@@ -1188,11 +1203,49 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     cpx* jz0 = reinterpret_cast<cpx*>(ws + ojz);
     cpx* ldx = reinterpret_cast<cpx*>(ws + odx);
     double* dbm = reinterpret_cast<double*>(ws + odb);
+    cpx* SP = reinterpret_cast<cpx*>(ws + oSP);
+    cpx* J0 = reinterpret_cast<cpx*>(ws + oJ0);
+    cpx* JS = reinterpret_cast<cpx*>(ws + oJS);
+    AdjPlasmaPtrs ap{};
+    AdjPlasmaWs aw{};
+    if (plasma) {
+        ap.nkh = long(nkh);
+        for (int q = 0; q < 6; ++q) ap.lS[q] = lS[q];
+        cpx* js = reinterpret_cast<cpx*>(ws + ojs0);
+        for (int q = 0; q < 3; ++q) ap.ljs0[q] = js + q * hp;
+        cpx* sl0 = reinterpret_cast<cpx*>(ws + osl);           // 31 planes: lsl 6, lold 4, ljsnA 3, ljsn 3, ldl 3, lsi0 6, W 6
+        for (int q = 0; q < 6; ++q) ap.lsl[q] = sl0 + q * nkh;
+        ap.lold = sl0 + 6 * nkh; ap.ljsnA = sl0 + 10 * nkh; ap.ljsn = sl0 + 13 * nkh; ap.ldl = sl0 + 16 * nkh;
+        ap.lsi0[0] = sl0 + 19 * nkh; ap.lsi0[1] = sl0 + 22 * nkh;
+        for (int q = 0; q < 6; ++q) aw.Wsc[q] = sl0 + (25 + q) * nkh;
+        for (int q = 0; q < 3; ++q) aw.Tsc[q] = W[q] ;                // the currents' scratch is free during the march
+        double* fa = reinterpret_cast<double*>(ws + oFa);      // 21 real planes: lFup 2 x 6, lFcur 6, ljsr 3
+        aw.lFup[0] = fa; aw.lFup[1] = fa + 6 * nk; aw.lFcur = fa + 12 * nk; aw.ljsr = fa + 18 * nk;
+    }
     // the start currents' j_z (init deposited them; jkz is not swapped into j0)
     if (c.mixed) launch_adj_widen(c, c.mx.jkz.p, jz0, long((ns + 1) * nkh));
     else G3D_CUDA(cudaMemcpyAsync(jz0, c.jkz.p, (ns + 1) * nkh * sizeof(cpx), cudaMemcpyDeviceToDevice, st));
     const double beta0 = c.beta_b, gm20 = c.gm2_b;
     std::vector<double> sl(size_t(K + 1));
+    // the plasma state of a level: the spectra R_x, R_y, E_z, B_z (the march reads their old values), j0 x, y, js0
+    auto plasma_state = [&](int k, bool out) {
+        cpx* sp_[4] = {c.Rx.p, c.Ry.p, c.Ez.p, c.Bz.p};
+        cpx* j0_[2] = {c.j0x.p, c.j0y.p};
+        cpx* js_[3] = {c.pl->js0x.p, c.pl->js0y.p, c.pl->js0z.p};
+        const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+        for (int q = 0; q < 4; ++q) {
+            cpx* ck = SP + (size_t(k) * 4 + q) * ns * nkh;
+            G3D_CUDA(cudaMemcpyAsync(out ? ck : sp_[q], out ? sp_[q] : ck, ns * nkh * sizeof(cpx), d2d, st));
+        }
+        for (int q = 0; q < 2; ++q) {
+            cpx* ck = J0 + (size_t(k) * 2 + q) * hp;
+            G3D_CUDA(cudaMemcpyAsync(out ? ck : j0_[q], out ? j0_[q] : ck, hp * sizeof(cpx), d2d, st));
+        }
+        for (int q = 0; q < 3; ++q) {
+            cpx* ck = JS + (size_t(k) * 3 + q) * hp;
+            G3D_CUDA(cudaMemcpyAsync(out ? ck : js_[q], out ? js_[q] : ck, hp * sizeof(cpx), d2d, st));
+        }
+    };
     auto save = [&](int k) {
         double* x = X + size_t(k) * 6 * size_t(np);
         double* src[6] = {c.parts.x, c.parts.y, c.parts.zeta, c.parts.px, c.parts.py, c.parts.pz};
@@ -1201,10 +1254,29 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
                 G3D_CUDA(cudaMemcpyAsync(x + size_t(q) * np, src[q], size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
             G3D_CUDA(cudaMemcpyAsync(AL + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
         }
+        if (plasma) plasma_state(k, true);
         sl[size_t(k)] = c.s;
     };
+    // back to level k (the beam, the exact real fields, the plasma state, s), to run step k + 1 again
+    auto restore = [&](int k) {
+        const double* x = X + size_t(k) * 6 * size_t(np);
+        double* dst[6] = {c.parts.x, c.parts.y, c.parts.zeta, c.parts.px, c.parts.py, c.parts.pz};
+        if (np > 0) {
+            for (int q = 0; q < 6; ++q)
+                G3D_CUDA(cudaMemcpyAsync(dst[q], x + size_t(q) * np, size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
+            G3D_CUDA(cudaMemcpyAsync(c.parts.alive, AL + size_t(k) * np, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
+        }
+        G3D_CUDA(cudaMemcpyAsync(c.Fd.p, FD + size_t(k) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
+        plasma_state(k, false);
+        c.jk_is_j0 = true;
+        c.s = sl[size_t(k)];
+        c.istep = k;
+    };
+    long tr0 = 0, rs0 = 0, npl_max = 0;
+    if (plasma) get_plasma_counters(c, tr0, rs0);
     // the real fields of level k are written by step k straight into checkpoint k (the push of step k + 1 reads
-    // them there); the context's own F / Fd come back, with the last level's fields, when the forward is done
+    // them there; with a plasma they are copied there after the step); the context's own F / Fd come back, with the
+    // last level's fields, when the forward is done
     struct Own {
         Ctx& c; double* fd; float* f;
         ~Own() { c.Fd.p = fd; c.F.p = f; c.fd_next = nullptr; c.f_next = nullptr; }
@@ -1213,10 +1285,33 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     else G3D_CUDA(cudaMemcpyAsync(FF, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
     save(0);
     for (int k = 1; k <= K; ++k) {
-        if (ex) c.fd_next = FD + size_t(k) * Fn;
-        else c.f_next = FF + size_t(k) * Fn;
-        step(c, false);
+        // with a plasma the march writes the real fields slice by slice into the context's F during the step, so
+        // the step keeps its own F and the level is copied after it (the level before must stay as it was)
+        if (plasma) {
+            step(c, false);
+            G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+            npl_max = std::max(npl_max, c.pl->nstrm);
+        } else {
+            if (ex) c.fd_next = FD + size_t(k) * Fn;
+            else c.f_next = FF + size_t(k) * Fn;
+            step(c, false);
+        }
         save(k);
+    }
+    if (plasma) {
+        long tr = 0, rs = 0;
+        get_plasma_counters(c, tr, rs);
+        if (tr != tr0 || rs != rs0 || c.pl->njb || !c.pl->joining.empty())
+            throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate trapping or restreaming, and the forward had some");
+        // the record of one march: the particles entering every half-cell, the exact fields of every slice and pass
+        const size_t passes = size_t(c.pl->cfg.iterations);
+        const size_t rx = ns * 5 * size_t(npl_max) * 8, rf = ns * passes * 6 * nk * 8, rl = 5 * size_t(npl_max) * 8;
+        const size_t r1 = (rx + 255) / 256 * 256, r2 = (rf + 255) / 256 * 256;
+        if (c.adjrec.n < r1 + r2 + rl) c.adjrec.alloc(r1 + r2 + rl, st);
+        aw.np = npl_max; aw.rs = npl_max;
+        aw.rec_x = reinterpret_cast<double*>(c.adjrec.p);
+        aw.rec_f = reinterpret_cast<double*>(c.adjrec.p + r1);
+        aw.lam = reinterpret_cast<double*>(c.adjrec.p + r1 + r2);
     }
     if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
     else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
@@ -1232,14 +1327,34 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     for (int q = 0; q < 3; ++q) G3D_CUDA(cudaMemsetAsync(ljk[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
     G3D_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
     if (np > 0) launch_adj_seed(c, jh[1], lam);
+    if (plasma) G3D_CUDA(cudaMemsetAsync(ap.ljs0[0], 0, 3 * hp * sizeof(cpx), st));
     for (int k = K; k >= 1; --k) {
         if (k < K) launch_adj_real_fields(c, lF, W, lS);
         for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemsetAsync(lj0[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
-        launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);
-        launch_adj_currents(c, ljk, W, V, lJ);
+        if (plasma) {
+            // step k again from level k-1 with its march recorded, then the march transposed; the level k-1 fields'
+            // adjoint takes the reads of the streaming pushes, then those of the beam push
+            restore(k - 1);
+            PlasmaState& Pl = *c.pl;
+            Pl.rec_x = aw.rec_x; Pl.rec_f = aw.rec_f; Pl.rec_np = aw.np;
+            struct Unrec { PlasmaState& P; ~Unrec() { P.rec_x = nullptr; P.rec_f = nullptr; P.rec_np = 0; } } unrec{Pl};
+            step(c, false);
+            if (Pl.nstrm > aw.np) throw Error(G3D_ERR_STATE, "the adjoint march: the plasma of a step grew when run again");
+            G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
+            G3D_CUDA(cudaMemsetAsync(ljk[2], 0, (ns + 1) * nkh * sizeof(cpx), st));
+            for (int q = 0; q < 2; ++q) ap.lj0[q] = lj0[q];
+            for (int q = 0; q < 3; ++q) ap.ljk[q] = ljk[q];
+            AdjPlasmaWs awk = aw;
+            awk.np = Pl.nstrm;
+            adjoint_march_plasma(c, awk, ap, FD + size_t(k - 1) * Fn, lF, sl[size_t(k - 1)], sl[size_t(k)]);
+            launch_adj_currents(c, ljk, W, V, lJ, Pl.box_mean);
+        } else {
+            launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);
+            launch_adj_currents(c, ljk, W, V, lJ);
+        }
         launch_adj_deposit(c, X + size_t(k) * 6 * np, AL + size_t(k) * np, lJ, lam);
         for (int q = 0; q < 2; ++q) std::swap(ljk[q], lj0[q]);           // jk of level k-1 as the j0 of step k
-        G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
+        if (!plasma) G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
         launch_adj_push(c, ex ? nullptr : FF + size_t(k - 1) * Fn, ex ? FD + size_t(k - 1) * Fn : nullptr, X + size_t(k - 1) * 6 * np,
                         AL + size_t(k - 1) * np, sl[size_t(k - 1)], sl[size_t(k)], lam, lF, err);
     }
@@ -1292,6 +1407,10 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         G3D_CUDA(cudaStreamSynchronize(st));
         for (long i = 0; i < np; ++i)
             for (int q = 0; q < 3; ++q) grad_p[3 * i + q] = h[size_t(q) * np + i];
+    }
+    if (plasma) {                                     // the run as the forward left it, at level K
+        restore(K);
+        launch_d2f(c, c.Fd.p, c.F.p, long(Fn));
     }
     G3D_CUDA(cudaStreamSynchronize(st));
     if (eh & 1) throw Error(G3D_ERR_STATE, "the adjoint march: a particle in the handed-over state");

@@ -379,6 +379,22 @@ static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true) 
     else launch_real_fields_slice(c, l, fm, cols);
 }
 
+// The adjoint's record of a march (PlasmaState::rec_x, rec_f): the exact fields of slice l after pass p, the particles
+// entering half-cell n
+static void record_fields(Ctx& c, int l, int p) {
+    PlasmaState& P = *c.pl;
+    const size_t nk = size_t(c.nk), fpl = size_t(c.ns + 2) * nk;
+    double* dst = P.rec_f + 6 * nk * (size_t(P.cfg.iterations) * size_t(l) + size_t(p));
+    G3D_CUDA(cudaMemcpy2DAsync(dst, nk * 8, c.Fd.p + size_t(l - c.a) * nk, fpl * 8, nk * 8, 6, cudaMemcpyDeviceToDevice, c.stream));
+}
+static void record_particles(Ctx& c, int n) {
+    PlasmaState& P = *c.pl;
+    const size_t np = size_t(P.rec_np);
+    const double* src[5] = {P.strm.x, P.strm.y, P.strm.px, P.strm.py, P.strm.pz};
+    for (int q = 0; q < 5; ++q)
+        G3D_CUDA(cudaMemcpyAsync(P.rec_x + (5 * size_t(n) + q) * np, src[q], size_t(P.nstrm) * 8, cudaMemcpyDeviceToDevice, c.stream));
+}
+
 void march_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
     const double Delta = s1 - s0, D = 0.5 * Delta;
@@ -423,6 +439,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
         real_fields_slice(c, N - 1, N - 2);
+        if (P.rec_f) record_fields(c, N - 1, passes - 1);
 
         StreamArgs sa;
         sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
@@ -439,6 +456,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             if (n == nhi) launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
             const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+            if (P.rec_x) record_particles(c, n);
             for (int pass = 0; pass < passes; ++pass) {
                 if (fh) launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
@@ -452,6 +470,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
                     launch_stream_spectra_rows(c);
                     launch_pass_cols(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
                     real_fields_slice(c, n, pass + 1 < passes ? n : n - 1, false);
+                    if (P.rec_f) record_fields(c, n, pass);
                 } else {
                     launch_stream_spectra(c);
                     launch_replace_pred(c, n, extrap ? 1 : 0, wex);
@@ -468,7 +487,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     };
     PlasmaState::LoopGraph* hit = nullptr;
     for (auto& l : P.loops) if (l.key == key) hit = &l;
-    if (c.profiling) {
+    if (c.profiling || P.rec_x) {
         issue();
     } else if (hit) {
         c.launches += hit->launches;

@@ -133,12 +133,44 @@ struct PlasmaState {
     struct LoopGraph { uint64_t key; cudaGraphExec_t exec; long launches; };
     std::vector<LoopGraph> loops;
     DevBuf<StepVals> stepv;
+    // recording for the adjoint march (null: off; the slice loop then runs without its graph): the streaming particles
+    // entering every half-cell n (x, y, p_x, p_y, p_z; rec_np each, at rec_x + 5 rec_np n) and the exact real fields of
+    // every slice n after every pass p (6 planes of nk, at rec_f + 6 nk (P n + p))
+    double* rec_x = nullptr;
+    double* rec_f = nullptr;
+    long rec_np = 0;
     PlasmaPtrs ptrs(const Ctx& c) const;
     PlasmaState() = default;
     PlasmaState(const PlasmaState&) = delete;
     PlasmaState& operator=(const PlasmaState&) = delete;
     ~PlasmaState() { for (auto& l : loops) cudaGraphExecDestroy(l.exec); }
 };
+
+// The adjoint of one march (k_adj_plasma.cu). The adjoint arrays of the window (device, half spectra):
+struct AdjPlasmaPtrs {
+    long nkh;
+    cpx* lS[6];                // the spectra {R_x, R_y, E_z, B_z, L_x, L_y}, ns planes
+    cpx* lj0[2];               // j0 x, y (ns + 1 planes)
+    cpx* ljk[3];               // the beam current's jk x, y, z (ns + 1 planes)
+    cpx* ljs0[3];              // js0 (ns + 1 planes)
+    cpx* lsl[6];               // one slice: the adjoint of its values in one pass (one plane each)
+    cpx *lold, *ljsnA, *ljsn, *ldl;      // 4, 3, 3, 3 planes
+    cpx* lsi0[2];              // 3 planes each, by the parity of the half-cell
+};
+// ... and its scratch: the record of the forward march (PlasmaState::rec_x, rec_f), np streaming particles recorded
+// with the stride rs (rs >= np)
+struct AdjPlasmaWs {
+    long np, rs;
+    double *rec_x, *rec_f;
+    double *lFup[2], *lFcur;   // 6 real planes each: the adjoints of a slice's real fields
+    double* ljsr;              // 3 real planes: the adjoint of a pass's streaming deposit
+    double* lam;               // 5 rs: the adjoint of the streaming particles' state
+    cpx* Wsc[6];               // one plane each of transform scratch
+    cpx* Tsc[3];
+};
+void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
+                          double s1);
+void launch_d2f(Ctx& c, const double* a, float* b, long n);     // b = float(a)
 
 // launchers (k_plasma.cu)
 void launch_stream(Ctx& c, const StreamArgs& a);

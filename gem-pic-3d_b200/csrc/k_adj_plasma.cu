@@ -1,0 +1,350 @@
+// The adjoint of the streaming-plasma march of one s-step (one rank, Fourier y, FP64 form with exact real fields),
+// which the reference does not have: the transpose of march_plasma (g3d_plasma.cu; src/sim_plasma.cpp:228-470) with
+// its discrete events frozen (the adjoint admits a march with no trapping, no restreaming and no ionization).
+//
+// The forward, per half-cell n from the front (N-2) to the rear (0) and pass p (the last one moves the particles):
+//   jsr(p)   = deposit(push(X_n, fields of slice n+1 and of slice n as pass p sees it: level s0 for p = 0, else the
+//              slice as pass p-1 left it))
+//   jsn(p)   = S(jsr(p))                                  the spectra, filters and smoothing
+//   jk(n)    = b(n) + jsn(p); jk(n-1) = b(n-1) + pred(p), pred(p) = js0(n-1) + (1+w)(jsn(p) - js0(n)) - w dl
+//              (extrapolating predictor; else pred = js0(n-1)); b the beam current
+//   slice n  = M_n(old R, E_z, B_z of slice n; jk(n-1), jk(n), j0(n-1), j0(n); slice n+1 as solved)
+//   F_n(p+1) = RF(slice n)                                the slice's real fields
+// then R(n+1) -= q (jsn - si0) with si0 the prediction slice n+1 was solved with; dl = jsn - js0(n); js0(n) = jsn.
+// The reverse runs n = 0 .. N-2 and the passes P-1 .. 0, each line transposed (complex coefficients conjugated), and
+// ends with the front slice N-1. Kernels:
+//   k_adjp_correct  the correction, dl and js0 of half-cell n (one thread per mode)
+//   k_adjp_march    the transposed slice march of one pass with the replace and the prediction (one thread per mode)
+//   k_adjp_stream   the transposed push and deposit of every streaming particle in one pass (k_adj_stream.cuh)
+// and the transposed real fields and current spectra of one slice (k_adjoint.cu).
+#include "g3d_plasma.hpp"
+#include "k_adj_stream.cuh"
+
+namespace g3d {
+
+namespace {
+// d(TSC weights)/d(index coordinate) (tsc_weights of g3d_common.cuh)
+__device__ __forceinline__ void tsc_slopes(double xi, double d[3]) {
+    const double f = xi - floor(xi + 0.5);
+    d[0] = -(0.5 - f); d[1] = -2 * f; d[2] = 0.5 + f;
+}
+__device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     // conj(i k) z
+}  // namespace
+
+// ---------------------------------------------------------------- the correction of half-cell n
+// R(n+1) -= q (jsn - si0): dJ/djsn = -q dJ/dR(n+1), dJ/dsi0 = q dJ/dR(n+1) (to the last pass of half-cell n+1, which
+// made that prediction); dl(n-1) = jsn - js0(n): dJ/djsn += dJ/ddl, dJ/djs0_old(n) = -dJ/ddl; js0_new(n) = jsn and
+// jk(n) = b(n) + jsn as the next step's j0: dJ/djsn += dJ/djs0_new(n) + dJ/dj0_next(n) (x, y)
+__global__ void k_adjp_correct(AdjPlasmaPtrs a, int n, double q, int par) {
+    const long nkh = a.nkh;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        const long pl = long(n + 1) * nkh + i;      // slice n+1 of the spectra, half-cell n of the current planes
+        const cpx lr[3] = {a.lS[0][pl], a.lS[1][pl], C(0)};
+        cpx* so = a.lsi0[par];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const cpx d = a.ldl[k * nkh + i];
+            cpx u = -q * lr[k] + d + a.ljs0[k][pl];
+            if (k < 2) u = u + a.ljk[k][pl];
+            a.ljsnA[k * nkh + i] = u;
+            so[k * nkh + i] = q * lr[k];
+            a.ljs0[k][pl] = -d;
+            a.ldl[k * nkh + i] = C(0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- the transposed slice march of one pass
+// march_slice_mode (k_plasma.cu; march_point, src/sim_kernels.hpp:173-210) transposed line by line: the adjoints of
+// the slice's new values (the slice's real fields of this pass, plus for the last pass what later reads of the slice
+// left in lS) go to the old R, E_z, B_z of the slice (summed over the passes in lold; the first pass writes them
+// into lS, L's old value being unread), the new values of slice n+1 (lS, added), j0 and the beam part of jk (added),
+// the streaming current of the pass (ljsn) and, through the prediction of half-cell n-1, js0 and dl.
+// front: the front slice (L = E_z = B_z = 0), solved once with the prediction js0(N-2).
+__global__ void k_adjp_march(Geo g, AdjPlasmaPtrs a, int n, double D, int last, int first, int multi, int extrap, double w,
+                             int par_prev, int front) {
+    const long nkh = a.nkh;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
+        const int kxi = int(i % g.H), j = int(i / g.H);
+        const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
+        const long o = long(n - g.a) * nkh + i, od = o, ou = o + nkh;
+        cpx ln[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ln[k] = a.lsl[k][i] + (last ? a.lS[k][o] : C(0));
+        cpx lRsx, lRsy, lup[3] = {C(0), C(0), C(0)};
+        if (front) {
+            lRsx = ln[0]; lRsy = ln[1];
+        } else {
+            const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+            // L_x = Ls_x - h/4 (a E - b B), L_y = Ls_y - h/4 (a B + b E)
+            cpx lLsx = ln[4], lLsy = ln[5];
+            cpx lEn = ln[2] - 0.25 * h * ikc(kx, ln[4]) - 0.25 * h * ikc(ky, ln[5]);
+            cpx lBn = ln[3] + 0.25 * h * ikc(ky, ln[4]) - 0.25 * h * ikc(kx, ln[5]);
+            // R_x = Rs_x + D (a E + b B), R_y = Rs_y + D (b E - a B)
+            lRsx = ln[0]; lRsy = ln[1];
+            lEn = lEn + D * ikc(kx, ln[0]) + D * ikc(ky, ln[1]);
+            lBn = lBn + D * ikc(ky, ln[0]) - D * ikc(kx, ln[1]);
+            // E = (pE - h/2 Qp - h/4 SE - h up_z) / den, B = (pB - h/2 Cp - h/4 SB) / den
+            const cpx le = lEn / den, lb = lBn / den;
+            cpx lpE = le, lpB = lb;
+            const cpx lQp = -0.5 * h * le, lSE = -0.25 * h * le, lCp = -0.5 * h * lb, lSB = -0.25 * h * lb;
+            lup[2] = -h * le;
+            // SE = -a Rs_x + a Ls_x + b Ls_y - b Rs_y; SB = a Rs_y + a Ls_y - b Rs_x - b Ls_x
+            lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
+            lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
+            lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
+            lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
+            // Qp = -1/2 a (pR_x - pL_x) + 1/2 b (pL_y - pR_y); Cp = 1/2 (a (pR_y + pL_y) - b (pR_x + pL_x))
+            cpx lpRx = -0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+            cpx lpLx = 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+            cpx lpRy = -0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+            cpx lpLy = 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+            // Ls_x = pL_x - h/4 (a pE - b pB) - h/2 up_x; Ls_y = pL_y - h/4 (a pB + b pE) - h/2 up_y
+            lpLx = lpLx + lLsx;
+            lpLy = lpLy + lLsy;
+            lpE = lpE - 0.25 * h * ikc(kx, lLsx) - 0.25 * h * ikc(ky, lLsy);
+            lpB = lpB + 0.25 * h * ikc(ky, lLsx) - 0.25 * h * ikc(kx, lLsy);
+            lup[0] = -0.5 * h * lLsx;
+            lup[1] = -0.5 * h * lLsy;
+            const long pp = o + nkh;                // slice n+1 as this march read it
+            a.lS[0][pp] = a.lS[0][pp] + lpRx; a.lS[1][pp] = a.lS[1][pp] + lpRy;
+            a.lS[2][pp] = a.lS[2][pp] + lpE; a.lS[3][pp] = a.lS[3][pp] + lpB;
+            a.lS[4][pp] = a.lS[4][pp] + lpLx; a.lS[5][pp] = a.lS[5][pp] + lpLy;
+        }
+        // Rs_x = R_x + D (a E + b B) - D J_x, Rs_y = R_y + D (b E - a B) - D J_y (the old level of slice n)
+        const cpx lo[4] = {lRsx, lRsy, D * ikc(kx, lRsx) + D * ikc(ky, lRsy), D * ikc(ky, lRsx) - D * ikc(kx, lRsy)};
+        const cpx lJx = -D * lRsx, lJy = -D * lRsy;
+        // J = wl (j0 + jk)(n-1) + wu (j0 + jk)(n)
+        a.lj0[0][od] = a.lj0[0][od] + wl * lJx; a.lj0[0][ou] = a.lj0[0][ou] + wu * lJx;
+        a.lj0[1][od] = a.lj0[1][od] + wl * lJy; a.lj0[1][ou] = a.lj0[1][ou] + wu * lJy;
+        const cpx lkd[3] = {wl * lJx, wl * lJy, C(0)};
+        const cpx lku[3] = {wu * lJx + lup[0], wu * lJy + lup[1], lup[2]};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { a.ljk[k][od] = a.ljk[k][od] + lkd[k]; a.ljk[k][ou] = a.ljk[k][ou] + lku[k]; }
+        const cpx* si = a.lsi0[par_prev];
+        if (front) {
+            // jk(N-2) = b + js0(N-2), the prediction slice N-1 is solved with (and corrected for: si0(N-2))
+#pragma unroll
+            for (int k = 0; k < 3; ++k) a.ljs0[k][od] = a.ljs0[k][od] + lkd[k] + si[k * nkh + i];
+        } else {
+            cpx ls[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ls[k] = (last ? a.ljsnA[k * nkh + i] : C(0)) + lku[k];
+            if (n >= 1) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const cpx lp = lkd[k] + (last ? si[k * nkh + i] : C(0));      // dJ/dpred of half-cell n-1
+                    a.ljs0[k][od] = a.ljs0[k][od] + lp;
+                    if (extrap) {
+                        ls[k] = ls[k] + (1 + w) * lp;
+                        a.ljs0[k][ou] = a.ljs0[k][ou] - (1 + w) * lp;
+                        a.ldl[k * nkh + i] = a.ldl[k * nkh + i] - w * lp;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) a.ljsn[k * nkh + i] = ls[k];
+        }
+        // the old R_x, R_y, E_z, B_z of slice n: summed over the passes, written by the first
+        if (first) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a.lS[k][o] = (multi ? a.lold[k * nkh + i] : C(0)) + lo[k];
+            a.lS[4][o] = C(0); a.lS[5][o] = C(0);
+        } else if (last) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = lo[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = a.lold[k * nkh + i] + lo[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- the transposed streaming push of one pass
+// The midpoint fields (Fa + Fb) / 2 of the recorded slices n and n+1 gathered with TSC (sgather_mid of k_plasma.cu);
+// the adjoint deposits half of each field adjoint into lFa and lFb and returns dJ/d(position)
+struct MidGat {
+    const Geo* g;
+    const double *Fa, *Fb;
+    long sa, sb;
+    double *lFa, *lFb;
+    long lsa, lsb;
+    __device__ void gather(double xm, double ym, double E[3], double B[3]) const {
+        int ix[3], jn[3]; double wx[3], wn[3];
+        tsc_periodic(wrap_periodic(xm, g->Lx), g->dx, g->nx, ix, wx);
+        tsc_periodic(wrap_periodic(ym, g->Ly), g->dy, g->ny, jn, wn);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            double v = 0;
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii) {
+                    const long k = long(jn[jj]) * g->nx + ix[ii];
+                    v += wx[ii] * wn[jj] * (0.5 * (Fa[c * sa + k] + Fb[c * sb + k]));
+                }
+            if (c < 3) E[c] = v; else B[c - 3] = v;
+        }
+    }
+    __device__ void adjoint(double xm, double ym, const double lE[3], const double lB[3], double& lxm, double& lym) const {
+        const double xw = wrap_periodic(xm, g->Lx), yw = wrap_periodic(ym, g->Ly);
+        int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
+        tsc_periodic(xw, g->dx, g->nx, ix, wx);
+        tsc_periodic(yw, g->dy, g->ny, jn, wn);
+        tsc_slopes(xw / g->dx, dwx);
+        tsc_slopes(yw / g->dy, dwn);
+        double sx = 0, sy = 0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double l = c < 3 ? lE[c] : lB[c - 3];
+            double vx = 0, vy = 0;
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii) {
+                    const long k = long(jn[jj]) * g->nx + ix[ii];
+                    const double m = 0.5 * (Fa[c * sa + k] + Fb[c * sb + k]);
+                    vx += dwx[ii] * wn[jj] * m; vy += wx[ii] * dwn[jj] * m;
+                    if (l != 0) {
+                        const double u = 0.5 * l * wx[ii] * wn[jj];
+                        atomicAdd(lFa + c * lsa + k, u);
+                        atomicAdd(lFb + c * lsb + k, u);
+                    }
+                }
+            sx += l * vx; sy += l * vy;
+        }
+        lxm += sx / g->dx;
+        lym += sy / g->dy;
+    }
+};
+// the current adjoints lJ (3 real planes) gathered with the deposit's TSC weights and 1/A (sdeposit of k_plasma.cu)
+struct DepGat {
+    const Geo* g;
+    const double* lJ;
+    __device__ void gather(double xd, double yd, double G[3], double Dx[3], double Dy[3]) const {
+        int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
+        tsc_periodic(xd, g->dx, g->nx, ix, wx);
+        tsc_periodic(yd, g->dy, g->ny, jn, wn);
+        tsc_slopes(xd / g->dx, dwx);
+        tsc_slopes(yd / g->dy, dwn);
+        const double ia = g->iA[0], sx = ia / g->dx, sy = ia / g->dy;
+        const long nk = g->nk;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            double v = 0, vx = 0, vy = 0;
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                for (int ii = 0; ii < 3; ++ii) {
+                    const double l = lJ[c * nk + long(jn[jj]) * g->nx + ix[ii]];
+                    v += wx[ii] * wn[jj] * l; vx += dwx[ii] * wn[jj] * l; vy += wx[ii] * dwn[jj] * l;
+                }
+            G[c] = ia * v; Dx[c] = sx * vx; Dy[c] = sy * vy;
+        }
+    }
+};
+// One thread per streaming particle of the recorded list: the state entering half-cell n (rec), the pass's current
+// adjoints lJ and, for the last pass, the adjoint of the state it leaves with (lam, replaced by the adjoint of the
+// state it enters with; earlier passes add to it: they deposit from the same state). Fixed ions carry no current
+// and do not move; particles of no charge deposit nothing.
+template <bool LAST>
+__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, StrmDev S, const IonDevC* __restrict__ ions, long np, long rs,
+                                                     const double* __restrict__ rec, int n, double Delta, const double* Fa, long sa,
+                                                     const double* Fb, long sb, double* lFa, long lsa, double* lFb, long lsb,
+                                                     const double* __restrict__ lJ, double* __restrict__ lam) {
+    const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= np || S.alive[i] != 1) return;
+    const int sp = S.sp[i];
+    if (sp >= SP_ION && sp < SP_FREED && !ions[sp - SP_ION].mobile) return;
+    const double qw = S.q[i] * S.w[i];
+    if (qw == 0) return;
+    const double h = g.zs[n + 1] - g.zs[n], fscale = 1 / (Delta * h * g.dx);
+    const double p[3] = {rec[2 * rs + i], rec[3 * rs + i], rec[4 * rs + i]};
+    double lout[5] = {0, 0, 0, 0, 0};
+    if (LAST)
+        for (int k = 0; k < 5; ++k) lout[k] = lam[k * rs + i];
+    MidGat gat{&g, Fa, Fb, sa, sb, lFa, lFb, lsa, lsb};
+    DepGat dep{&g, lJ};
+    double lin[5];
+    stream_push_reverse(rec[i], rec[rs + i], p, S.qm[i], qw, h, fscale, gat, dep, lout, lin);
+    for (int k = 0; k < 5; ++k) lam[k * rs + i] = LAST ? lin[k] : lam[k * rs + i] + lin[k];
+}
+
+// ---------------------------------------------------------------- the reverse of one march
+static unsigned mode_blocks(long n) {
+    const long b = (n + 127) / 128;
+    return unsigned(b < 1 ? 1 : b);
+}
+
+// The transpose of march_plasma(s0, s1) for the step whose forward was recorded into w.rec_x, w.rec_f. On entry lS holds
+// the adjoints of the step's final spectra, ljk (x, y) those of jk as the next step's j0 (ljk z zero), ljs0 those of
+// the step's final js0, lj0 zeros; lF (the level s0 real fields' adjoint, whole window) receives the reads of the
+// level s0 fields. On exit lS holds the adjoints of the level s0 spectra, lj0 of j0, ljk of the beam current of the
+// step (x, y, z), ljs0 of the level s0 streaming current. Fprev: the level s0 exact real fields.
+void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
+                          double s1) {
+    PlasmaState& P = *c.pl;
+    const int N = c.N, passes = P.cfg.iterations;
+    const double Delta = s1 - s0, D = 0.5 * Delta;
+    const long nkh = c.nkh, nk = c.nk, fpl = long(c.ns + 2) * nk, np = w.np, rs = w.rs;
+    const bool extrap = P.cfg.predictor_extrapolate != 0, keep0 = P.box_mean;
+    const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
+    cudaStream_t st = c.stream;
+    std::vector<double> cen(size_t(N - 1));
+    for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
+    G3D_CUDA(cudaMemsetAsync(a.ldl, 0, 3 * nkh * sizeof(cpx), st));
+    G3D_CUDA(cudaMemsetAsync(w.lFup[0], 0, 6 * nk * 8, st));
+    if (rs) G3D_CUDA(cudaMemsetAsync(w.lam, 0, 5 * size_t(rs) * 8, st));
+    const StrmDev S = P.strm;
+    const double* Fnext = nullptr;
+    int cur = 0;
+    const unsigned mb = mode_blocks(nkh), pb = unsigned((np + 127) / 128);
+    for (int n = c.a; n <= N - 2; ++n) {
+        k_adjp_correct<<<mb, 128, 0, st>>>(a, n, D * c.wlo_h[size_t(n + 1)], n & 1);
+        c.check_launch("k_adjp_correct");
+        G3D_CUDA(cudaMemsetAsync(w.lFup[cur ^ 1], 0, 6 * nk * 8, st));
+        // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
+        const double wex = (n >= 1 && n + 1 <= N - 2)
+                               ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+        Fnext = w.rec_f + 6 * nk * (size_t(passes) * size_t(n + 1) + size_t(passes - 1));
+        for (int p = passes - 1; p >= 0; --p) {
+            launch_adj_real_fields_slice(c, p == passes - 1 ? w.lFup[cur] : w.lFcur, nk, w.Wsc, a.lsl);
+            k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, n, D, p == passes - 1 ? 1 : 0, p == 0 ? 1 : 0, passes > 1 ? 1 : 0,
+                                              extrap ? 1 : 0, wex, (n - 1) & 1, 0);
+            c.check_launch("k_adjp_march");
+            cpx* js3[3] = {a.ljsn, a.ljsn + nkh, a.ljsn + 2 * nkh};
+            launch_adj_stream_spectra(c, js3, w.Tsc, w.ljsr, keep0, a2);
+            if (p >= 1) G3D_CUDA(cudaMemsetAsync(w.lFcur, 0, 6 * nk * 8, st));
+            if (!np) continue;
+            const double* Fa = p == 0 ? Fprev + size_t(n - c.a) * nk : w.rec_f + 6 * nk * (size_t(passes) * size_t(n) + size_t(p - 1));
+            const long sa = p == 0 ? fpl : nk;
+            double* lFa = p == 0 ? lF + size_t(n - c.a) * nk : w.lFcur;
+            const long lsa = p == 0 ? fpl : nk;
+            const double* rec = w.rec_x + 5 * size_t(rs) * size_t(n);
+            if (p == passes - 1)
+                k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, n, Delta, Fa, sa, Fnext, nk, lFa, lsa,
+                                                        w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
+            else
+                k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, n, Delta, Fa, sa, Fnext, nk, lFa, lsa,
+                                                         w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
+            c.check_launch("k_adjp_stream");
+        }
+        cur ^= 1;
+    }
+    // the front slice N-1: its real fields (read by half-cell N-2), then its march with the prediction js0(N-2)
+    launch_adj_real_fields_slice(c, w.lFup[cur], nk, w.Wsc, a.lsl);
+    k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, 1, 1, 0, 0, 0.0, (N - 2) & 1, 1);
+    c.check_launch("k_adjp_march");
+}
+
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long n) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = float(a[i]);
+}
+void launch_d2f(Ctx& c, const double* a, float* b, long n) {
+    if (n <= 0) return;
+    const long bl = (n + 255) / 256;
+    k_d2f<<<unsigned(bl < 148 * 16 ? bl : 148 * 16), 256, 0, c.stream>>>(a, b, n);
+    c.check_launch("k_d2f");
+}
+
+}  // namespace g3d

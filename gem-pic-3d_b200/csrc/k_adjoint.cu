@@ -72,7 +72,7 @@ __global__ void k_adj_seed(PartsDev P, long np, double W, double* __restrict__ l
 template <int NX>
 __global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __restrict__ lF, cpx* __restrict__ W0, cpx* __restrict__ W1,
                                                     cpx* __restrict__ W2, cpx* __restrict__ W3, cpx* __restrict__ W4,
-                                                    cpx* __restrict__ W5) {
+                                                    cpx* __restrict__ W5, long fpl) {
     using S = FftShape<NX>;
     constexpr int LPC = ANT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __rest
     cpx* a1 = sm + LPC * RS;
     cpx* a2 = sm + 2 * LPC * RS;
     const int l = blockIdx.y, r0 = blockIdx.x * LPC, tid = threadIdx.x;
-    const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
+    const long fbase = long(l) * g.nk;
     for (int e = tid; e < LPC * NX; e += ANT) {
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         double f[6] = {0, 0, 0, 0, 0, 0};
@@ -122,13 +122,15 @@ __global__ void __launch_bounds__(ANT) k_adj_rf_rows(Geo g, const double* __rest
     }
 }
 // columns: forward transforms along y of the six half-row adjoints, added to the spectrum adjoints of slice l
-// (R, E_z, B_z; assigned for L, whose adjoint the transposed march leaves stale)
+// (R, E_z, B_z; assigned for L, whose adjoint the transposed march leaves stale), or all six assigned (`assign`: one
+// slice of the streaming-plasma march, whose slice fields are read by nothing but its own real fields)
 template <int NY>
 __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                                       const cpx* __restrict__ W2, const cpx* __restrict__ W3,
                                                                       const cpx* __restrict__ W4, const cpx* __restrict__ W5,
                                                                       cpx* __restrict__ lRx, cpx* __restrict__ lRy, cpx* __restrict__ lLx,
-                                                                      cpx* __restrict__ lLy, cpx* __restrict__ lEz, cpx* __restrict__ lBz) {
+                                                                      cpx* __restrict__ lLy, cpx* __restrict__ lEz, cpx* __restrict__ lBz,
+                                                                      int assign) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     const int l = blockIdx.y, c0 = blockIdx.x * ACW, tid = threadIdx.x, nthr = ACW * S::T, pr = blockIdx.z;
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_rf_cols(Geo g, co
         const int p = e / ACW, cc = e - p * ACW, kxi = c0 + cc;
         if (kxi >= H) continue;
         const long o = base + long(p) * H + kxi;
-        if (pr == 1) { out0[o] = s0[ColTile<NY, ACW>::at(p, cc)]; out1[o] = s1[ColTile<NY, ACW>::at(p, cc)]; }           // L: not an input of the forward march
+        if (pr == 1 || assign) { out0[o] = s0[ColTile<NY, ACW>::at(p, cc)]; out1[o] = s1[ColTile<NY, ACW>::at(p, cc)]; }   // L: not an input of the forward march
         else { out0[o] = out0[o] + s0[ColTile<NY, ACW>::at(p, cc)]; out1[o] = out1[o] + s1[ColTile<NY, ACW>::at(p, cc)]; }
     }
 }
@@ -311,11 +313,14 @@ __global__ void __launch_bounds__(BT) k_adj_march(Geo g, cpx* __restrict__ lRx, 
 }
 
 // ---------------------------------------------------------------- transposed currents
-// columns: per half-cell plane, the filters f(k) (zero at k = 0) and the unnormalised inverse transform along y
+// columns: per half-cell plane, the filters f(k) (zero at k = 0 unless keep0: the box mean of a run with plasma) with
+// the smoothing 1 / (1 + a2 k_perp^2) (a2 > 0: the streaming current's spectra, k_ss_cols) and the unnormalised
+// inverse transform along y
 template <int NY>
 __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, const cpx* __restrict__ JX, const cpx* __restrict__ JY,
                                                                        const cpx* __restrict__ JZ, cpx* __restrict__ TX,
-                                                                       cpx* __restrict__ TY, cpx* __restrict__ TZ) {
+                                                                       cpx* __restrict__ TY, cpx* __restrict__ TZ, int keep0,
+                                                                       double a2) {
     using S = FftShape<NY>;
     extern __shared__ cpx sm[];
     cpx* s0 = sm;
@@ -328,7 +333,8 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, c
         const int p = e / ACW, c = e - p * ACW, kx = c0 + c;
         cpx u0 = C(0), u1 = C(0), u2 = C(0);
         if (kx < H) {
-            const double f = (kx == 0 && p == 0) ? 0.0 : g.filt[kx] * g.filty[p];
+            const double k2 = g.kxs[kx] * g.kxs[kx] + g.kys[p] * g.kys[p];
+            const double f = (kx == 0 && p == 0 && !keep0) ? 0.0 : g.filt[kx] * g.filty[p] / (1 + a2 * k2);
             const long o = base + long(p) * H + kx;
             u0 = conj(f * JX[o]); u1 = conj(f * JY[o]); u2 = conj(f * JZ[o]);
         }
@@ -352,7 +358,7 @@ __global__ void __launch_bounds__(ACW * FftShape<NY>::T) k_adj_cur_cols(Geo g, c
 // from lTZ (zero above nx/2), real part -> lv_z. Out: V [3][ns+1][ny][nx].
 template <int NX>
 __global__ void __launch_bounds__(ANT) k_adj_cur_rows(Geo g, const cpx* __restrict__ TX, const cpx* __restrict__ TY,
-                                                     const cpx* __restrict__ TZ, double* __restrict__ V) {
+                                                     const cpx* __restrict__ TZ, double* __restrict__ V, long vpl) {
     using S = FftShape<NX>;
     constexpr int LPC = ANT / S::T, RS = row_stride<NX>(), H = NX / 2 + 1;
     extern __shared__ cpx sm[];
@@ -386,7 +392,7 @@ __global__ void __launch_bounds__(ANT) k_adj_cur_rows(Geo g, const cpx* __restri
         decltype(a0) const ls_[2] = {a0, a1};
         fft_lines<NX, 2>(ls_, RowAddr{r * RS}, t, g.twx);
     }
-    const long nk = g.nk, vpl = long(g.ns + 1) * nk;
+    const long nk = g.nk;
     for (int e = tid; e < LPC * NX; e += ANT) {
         const int rr = e / NX, p = e - rr * NX, row = r0 + rr;
         if (row >= g.ny) continue;
@@ -920,7 +926,8 @@ static void adj_rf_rows(Ctx& c, const double* lF, cpx* const* W) {
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
     allow_smem(k_adj_rf_rows<NX>, smem);
     k_adj_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns)), ANT, smem, c.stream>>>(c.geo(), lF, W[0], W[1], W[2],
-                                                                                                         W[3], W[4], W[5]);
+                                                                                                         W[3], W[4], W[5],
+                                                                                                         long(c.ns + 2) * c.nk);
     c.check_launch("k_adj_rf_rows");
 }
 template <int NY>
@@ -928,7 +935,7 @@ static void adj_rf_cols(Ctx& c, cpx* const* W, cpx* const* lS) {
     const size_t smem = size_t(2) * ColTile<NY, ACW>::size * sizeof(cpx);
     allow_smem(k_adj_rf_cols<NY>, smem);
     k_adj_rf_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns), 3), ACW * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), W[0], W[1], W[2], W[3], W[4], W[5], lS[0], lS[1], lS[4], lS[5], lS[2], lS[3]);
+        c.geo(), W[0], W[1], W[2], W[3], W[4], W[5], lS[0], lS[1], lS[4], lS[5], lS[2], lS[3], 0);
     c.check_launch("k_adj_rf_cols");
 }
 // lS = {Rx, Ry, Ez, Bz, Lx, Ly}; W: 6 half-spectrum scratch arrays of ns planes
@@ -936,6 +943,55 @@ void launch_adj_real_fields(Ctx& c, const double* lF, cpx* const* W, cpx* const*
     const int tok = c.prof_begin("adj_real_fields");
     G3D_DISPATCH_N(c.nx, NX, adj_rf_rows<NX>(c, lF, W));
     G3D_DISPATCH_N(c.ny, NY, adj_rf_cols<NY>(c, W, lS));
+    c.prof_end(tok);
+}
+// One slice of the streaming-plasma march: the transposed real fields of lF (6 planes of one slice, component stride
+// fpl) assigned to the slice's spectrum adjoints lsl = {Rx, Ry, Ez, Bz, Lx, Ly} (one plane each); W: 6 planes of scratch
+template <int NX>
+static void adj_rf_rows_slice(Ctx& c, const double* lF, long fpl, cpx* const* W) {
+    constexpr int LPC = ANT / FftShape<NX>::T;
+    const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
+    allow_smem(k_adj_rf_rows<NX>, smem);
+    k_adj_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), 1u), ANT, smem, c.stream>>>(c.geo(), lF, W[0], W[1], W[2], W[3],
+                                                                                          W[4], W[5], fpl);
+    c.check_launch("k_adj_rf_rows");
+}
+template <int NY>
+static void adj_rf_cols_slice(Ctx& c, cpx* const* W, cpx* const* lsl) {
+    const size_t smem = size_t(2) * ColTile<NY, ACW>::size * sizeof(cpx);
+    allow_smem(k_adj_rf_cols<NY>, smem);
+    k_adj_rf_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), 1u, 3u), ACW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), W[0], W[1], W[2], W[3], W[4], W[5], lsl[0], lsl[1], lsl[4], lsl[5], lsl[2], lsl[3], 1);
+    c.check_launch("k_adj_rf_cols");
+}
+void launch_adj_real_fields_slice(Ctx& c, const double* lF, long fpl, cpx* const* W, cpx* const* lsl) {
+    const int tok = c.prof_begin("adj_real_fields_slice");
+    G3D_DISPATCH_N(c.nx, NX, adj_rf_rows_slice<NX>(c, lF, fpl, W));
+    G3D_DISPATCH_N(c.ny, NY, adj_rf_cols_slice<NY>(c, W, lsl));
+    c.prof_end(tok);
+}
+// The transposed spectra of one half-cell's streaming current (k_ss_rows + the column part of k_pass_cols): ljsn (3 half
+// planes) -> lJ (3 real planes, component stride nk); T: 3 planes of scratch
+template <int NY>
+static void adj_ss_cols(Ctx& c, cpx* const* ljsn, cpx* const* T, bool keep0, double a2) {
+    const size_t smem = size_t(3) * ColTile<NY, ACW>::size * sizeof(cpx);
+    allow_smem(k_adj_cur_cols<NY>, smem);
+    k_adj_cur_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), 1u), ACW * FftShape<NY>::T, smem, c.stream>>>(
+        c.geo(), ljsn[0], ljsn[1], ljsn[2], T[0], T[1], T[2], keep0 ? 1 : 0, a2);
+    c.check_launch("k_adj_cur_cols");
+}
+template <int NX>
+static void adj_ss_rows(Ctx& c, cpx* const* T, double* lJ) {
+    constexpr int LPC = ANT / FftShape<NX>::T;
+    const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
+    allow_smem(k_adj_cur_rows<NX>, smem);
+    k_adj_cur_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), 1u), ANT, smem, c.stream>>>(c.geo(), T[0], T[1], T[2], lJ, long(c.nk));
+    c.check_launch("k_adj_cur_rows");
+}
+void launch_adj_stream_spectra(Ctx& c, cpx* const* ljsn, cpx* const* T, double* lJ, bool keep0, double a2) {
+    const int tok = c.prof_begin("adj_stream_spectra");
+    G3D_DISPATCH_N(c.ny, NY, adj_ss_cols<NY>(c, ljsn, T, keep0, a2));
+    G3D_DISPATCH_N(c.nx, NX, adj_ss_rows<NX>(c, T, lJ));
     c.prof_end(tok);
 }
 template <int BT, int DEPTH>
@@ -955,11 +1011,11 @@ void launch_adj_march(Ctx& c, cpx* const* lS, cpx* const* lj0, cpx* const* ljk, 
     c.prof_end(tok);
 }
 template <int NY>
-static void adj_cur_cols(Ctx& c, cpx* const* ljk, cpx* const* T) {
+static void adj_cur_cols(Ctx& c, cpx* const* ljk, cpx* const* T, bool keep0) {
     const size_t smem = size_t(3) * ColTile<NY, ACW>::size * sizeof(cpx);
     allow_smem(k_adj_cur_cols<NY>, smem);
     k_adj_cur_cols<NY><<<dim3(unsigned((c.H + ACW - 1) / ACW), unsigned(c.ns + 1)), ACW * FftShape<NY>::T, smem, c.stream>>>(
-        c.geo(), ljk[0], ljk[1], ljk[2], T[0], T[1], T[2]);
+        c.geo(), ljk[0], ljk[1], ljk[2], T[0], T[1], T[2], keep0 ? 1 : 0, 0.0);
     c.check_launch("k_adj_cur_cols");
 }
 template <int NX>
@@ -967,13 +1023,15 @@ static void adj_cur_rows(Ctx& c, cpx* const* T, double* V) {
     constexpr int LPC = ANT / FftShape<NX>::T;
     const size_t smem = size_t(2) * LPC * row_stride<NX>() * sizeof(cpx);
     allow_smem(k_adj_cur_rows<NX>, smem);
-    k_adj_cur_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1)), ANT, smem, c.stream>>>(c.geo(), T[0], T[1], T[2], V);
+    k_adj_cur_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(c.ns + 1)), ANT, smem, c.stream>>>(c.geo(), T[0], T[1], T[2], V,
+                                                                                                          long(c.ns + 1) * c.nk);
     c.check_launch("k_adj_cur_rows");
 }
-// ljk (3 half-cell spectra) -> lJ (3 x (ns+3) raw planes); T: 3 scratch arrays of ns+1 planes, V: 3 (ns+1) real planes
-void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ) {
+// ljk (3 half-cell spectra) -> lJ (3 x (ns+3) raw planes); T: 3 scratch arrays of ns+1 planes, V: 3 (ns+1) real planes;
+// keep0: the k_perp = 0 current kept (the steps of a run with plasma and box_mean, currents() of g3d_host.cu)
+void launch_adj_currents(Ctx& c, cpx* const* ljk, cpx* const* T, double* V, double* lJ, bool keep0) {
     const int tok = c.prof_begin("adj_currents");
-    G3D_DISPATCH_N(c.ny, NY, adj_cur_cols<NY>(c, ljk, T));
+    G3D_DISPATCH_N(c.ny, NY, adj_cur_cols<NY>(c, ljk, T, keep0));
     G3D_DISPATCH_N(c.nx, NX, adj_cur_rows<NX>(c, T, V));
     k_adj_zfilter<<<ew_blocks(3L * (c.ns + 3) * c.nk), 256, 0, c.stream>>>(c.geo(), V, lJ, c.P.zeta_filter ? 1 : 0);
     c.check_launch("k_adj_zfilter");

@@ -385,7 +385,9 @@ __global__ void __launch_bounds__(8 * FftShape<NY>::T) k_rf_cols_tma(Geo g, cons
 }
 
 // ---------------------------------------------------------------- real fields: rows (inverse x, F)
-template <int NX>
+// XM (exact fields with midpoint fields, FP64 Fourier y): the midpoint fields from the FP64 values of both slices
+// (Fd), so that the streaming push of the exact forward gathers unrounded fields like the beam push does
+template <int NX, bool XM = false>
 __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
                                                const cpx* __restrict__ W2, const cpx* __restrict__ W3,
                                                const cpx* __restrict__ W4, const cpx* __restrict__ W5, float* __restrict__ F, int l0,
@@ -400,12 +402,19 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
     const long base = long(l) * g.nkh;
     const long fpl = long(g.ns + 2) * g.nk, fbase = long(l) * g.nk;
     constexpr int EO = (LPC * NX + NT - 1) / NT;                    // output elements of a thread
-    float oth[EO][6];                                               // the midpoint fields' other slice
+    float oth[XM ? 1 : EO][6];                                      // the midpoint fields' other slice
+    double othd[XM ? EO : 1][6];
     if (fm.out) {
     #pragma unroll
         for (int u_ = 0; u_ < EO; ++u_) {
             const int e = tid + u_ * NT, rr = e / NX, p = e - rr * NX, row = r0 + rr;
-            if (e < LPC * NX && row < g.ny) fmid_load(fm, F, fpl, g.nk, long(row) * NX + p, oth[u_]);
+            if (e >= LPC * NX || row >= g.ny) continue;
+            if constexpr (XM) {
+#pragma unroll
+                for (int comp = 0; comp < 6; ++comp) othd[u_][comp] = Fd[comp * fpl + long(fm.other) * g.nk + long(row) * NX + p];
+            } else {
+                fmid_load(fm, F, fpl, g.nk, long(row) * NX + p, oth[u_]);
+            }
         }
     }
     #pragma unroll
@@ -444,7 +453,15 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
                              float(0.5 * (l2 - r2)), float(0.5 * (r1 - l1)), float(z3.y)};  // B_x, B_y, B_z
 #pragma unroll
         for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
-        if (fm.out) fmid_store(fm, long(row) * NX + p, fv, oth[u_]);
+        if constexpr (XM) {
+            const double dv[6] = {0.5 * (r1 + l1), 0.5 * (r2 + l2), z3.x, 0.5 * (l2 - r2), 0.5 * (r1 - l1), z3.y};
+            double2* o = reinterpret_cast<double2*>(fm.out) + 3 * (long(row) * NX + p);
+            o[0] = make_double2(0.5 * (dv[0] + othd[u_][0]), 0.5 * (dv[1] + othd[u_][1]));
+            o[1] = make_double2(0.5 * (dv[2] + othd[u_][2]), 0.5 * (dv[3] + othd[u_][3]));
+            o[2] = make_double2(0.5 * (dv[4] + othd[u_][4]), 0.5 * (dv[5] + othd[u_][5]));
+        } else if (fm.out) {
+            fmid_store(fm, long(row) * NX + p, fv, oth[u_]);
+        }
         if (Fd) {                                      // exact fields: the same values before the rounding
             Fd[0 * fpl + idx] = 0.5 * (r1 + l1); Fd[1 * fpl + idx] = 0.5 * (r2 + l2);
             Fd[3 * fpl + idx] = 0.5 * (l2 - r2); Fd[4 * fpl + idx] = 0.5 * (r1 - l1);
@@ -560,10 +577,17 @@ template <int NX>
 static void rf_rows(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {
     constexpr int LPC = NT / FftShape<NX>::T;
     const size_t smem = size_t(3) * LPC * row_stride<NX>() * sizeof(cpx);
-    allow_smem(k_rf_rows<NX>, smem);
     const int tok = c.prof_begin(nl == 1 ? "real_rows_slice" : "real_rows");
-    k_rf_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl)), NT, smem, c.stream>>>(
-        c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0, c.Fd.p, fm);
+    const dim3 grid(unsigned((c.ny + LPC - 1) / LPC), unsigned(nl));
+    if (c.Fd.p && fm.out && !fm.f32 && !fm.fh) {       // exact fields: unrounded midpoint fields
+        allow_smem(k_rf_rows<NX, true>, smem);
+        k_rf_rows<NX, true><<<grid, NT, smem, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p,
+                                                          l0, c.Fd.p, fm);
+    } else {
+        allow_smem(k_rf_rows<NX>, smem);
+        k_rf_rows<NX><<<grid, NT, smem, c.stream>>>(c.geo(), c.W[0].p, c.W[1].p, c.W[2].p, c.W[3].p, c.W[4].p, c.W[5].p, c.F.p, l0,
+                                                    c.Fd.p, fm);
+    }
     c.check_launch("k_rf_rows");
     c.prof_end(tok);
 }

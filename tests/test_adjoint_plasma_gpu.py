@@ -1,0 +1,102 @@
+"""The adjoint march with a streaming plasma (the structure of workload 4: a witness bunch inside a Gaussian grid
+laser in a plasma with mobile H+ ions) against central finite differences of the forward. The reference has no
+adjoint. The forward is the FP64 form with exact fields: the real fields kept in FP64 and gathered by the beam push
+and, through the midpoint fields, by the streaming push, so that J = mean p_z of the live beam after K s-steps is a
+smooth function of the laser mode coefficients and of the beam momenta. The plasma couples both ways: the beam's
+current and the laser drive the plasma, whose current enters the fields the beam feels. The adjoint runs each
+s-step again from its level checkpoint with the march recorded and transposes the march half-cell by half-cell
+(passes, prediction, correction, the Boris pushes and deposits of every streaming particle).
+
+Bound: relative difference <= 1e-6 between the adjoint's directional derivative and the central difference
+(eps = 1e-6), as for the adjoint without plasma.
+"""
+import numpy as np
+import pytest
+
+from test_adjoint_gpu import EPS, TOL, adjoint, central, forward, hermitian_direction, objective
+
+pytestmark = pytest.mark.gpu
+
+
+def case(**kw):
+    from g3d import configs
+    return configs.adjoint_plasma_small(**kw)
+
+
+def test_plasma_adjoint_objective_and_the_run_it_leaves():
+    """J is the forward's J, and the run is left at s = K dz as K steps leave it (the adjoint runs the steps again
+    from their levels)."""
+    from g3d import Simulation
+    cfg = case()
+    s = Simulation(cfg)
+    s.load_bunch()
+    s.set_laser_modes(None)
+    s.set_exact_fields(True)
+    s.init_fields()
+    J, gm, gp = s.adjoint(cfg.steps)
+    assert s.streaming_count() > 0
+    p = s.host_particles()
+    F = s.array("F")
+    rx = s.array("Rx")
+    s.close()
+    assert np.all(np.isfinite(gm)) and np.all(np.isfinite(gp))
+    assert abs(J - objective(p)) <= 1e-13 * abs(J)
+    # the same run without the adjoint
+    s = Simulation(cfg)
+    s.load_bunch()
+    s.set_laser_modes(None)
+    s.set_exact_fields(True)
+    s.init_fields()
+    for _ in range(cfg.steps):
+        s.step()
+    p2, F2, rx2 = s.host_particles(), s.array("F"), s.array("Rx")
+    s.close()
+    assert abs(J - objective(p2)) <= 1e-12 * abs(J)
+    assert np.linalg.norm(F - F2) <= 1e-6 * np.linalg.norm(F2)
+    assert np.linalg.norm(rx - rx2) <= 1e-10 * np.linalg.norm(rx2)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(passes=1), dict(extrapolate=0, smooth=0.5), dict(ions=False, passes=3)],
+                         ids=["two-passes", "one-pass", "previous-smoothed", "electrons-three-passes"])
+def test_plasma_laser_mode_gradient_against_central_differences(kw):
+    cfg = case(**kw)
+    J, gm, gp, _ = adjoint(cfg)
+    d = hermitian_direction(np.random.default_rng(31), cfg.ny, cfg.nx)
+    ad = float(np.real(np.sum(np.conj(gm) * d)))
+    fd = central(forward(cfg, coef=1 + EPS * d), forward(cfg, coef=1 - EPS * d), EPS)
+    print(f"{kw}: J = {J:.12e}, laser modes: adjoint {ad:.12e}, central difference {fd:.12e}")
+    assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
+@pytest.mark.parametrize("through_start", [True, False])
+def test_plasma_momentum_gradient_against_central_differences(through_start):
+    cfg = case(charge_pC=1.0)
+    J, gm, gp, _ = adjoint(cfg, through_start=through_start)
+    D = np.random.default_rng(32).standard_normal(gp.shape)
+    ad = float(np.sum(gp * D))
+    fd = central(forward(cfg, dp=EPS * D, through_start=through_start),
+                 forward(cfg, dp=-EPS * D, through_start=through_start), EPS)
+    print(f"momenta (through the start field: {through_start}): adjoint {ad:.12e}, central difference {fd:.12e}")
+    assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
+def test_plasma_adjoint_refuses_what_it_does_not_differentiate():
+    """The mixed form and ionization are refused with G3D_ERR_ARG before anything runs."""
+    from g3d import G3DError, Simulation, configs
+    cfg = case()
+    s = Simulation(cfg, precision="mixed")
+    s.load_bunch()
+    s.set_laser_modes(None)
+    s.init_fields()
+    with pytest.raises(G3DError):
+        s.adjoint(cfg.steps)
+    s.close()
+    ion = configs.ionization_small()
+    ion.params.update(sponge=0.0, sponge_y=0.0)
+    s = Simulation(ion)
+    s.set_laser_modes(None)
+    s.set_exact_fields(True)
+    s.init_fields()
+    with pytest.raises(G3DError):
+        s.adjoint(1, momenta=False)
+    s.close()
