@@ -1246,7 +1246,10 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
             G3D_CUDA(cudaMemcpyAsync(out ? ck : js_[q], out ? js_[q] : ck, hp * sizeof(cpx), d2d, st));
         }
     };
+    // the particles waiting to join the streaming plasma at each level (slow trapped ones of the step before; few)
+    std::vector<std::vector<g3d_particle>> joins(plasma ? size_t(K + 1) : 0);
     auto save = [&](int k) {
+        if (plasma) joins[size_t(k)] = get_joining(c);
         double* x = X + size_t(k) * 6 * size_t(np);
         double* src[6] = {c.parts.x, c.parts.y, c.parts.zeta, c.parts.px, c.parts.py, c.parts.pz};
         if (np > 0) {
@@ -1268,6 +1271,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         }
         G3D_CUDA(cudaMemcpyAsync(c.Fd.p, FD + size_t(k) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
         plasma_state(k, false);
+        set_joining(c, joins[size_t(k)]);
         c.jk_is_j0 = true;
         c.s = sl[size_t(k)];
         c.istep = k;
@@ -1301,17 +1305,22 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     if (plasma) {
         long tr = 0, rs = 0;
         get_plasma_counters(c, tr, rs);
-        if (tr != tr0 || rs != rs0 || c.pl->njb || !c.pl->joining.empty())
-            throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate trapping or restreaming, and the forward had some");
-        // the record of one march: the particles entering every half-cell, the exact fields of every slice and pass
-        const size_t passes = size_t(c.pl->cfg.iterations);
-        const size_t rx = ns * 5 * size_t(npl_max) * 8, rf = ns * passes * 6 * nk * 8, rl = 5 * size_t(npl_max) * 8;
-        const size_t r1 = (rx + 255) / 256 * 256, r2 = (rf + 255) / 256 * 256;
-        if (c.adjrec.n < r1 + r2 + rl) c.adjrec.alloc(r1 + r2 + rl, st);
+        if (tr != tr0 || rs != rs0)
+            throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate particles that join the beam (fast trapped or "
+                                       "restreamed ones), and the forward had some");
+        // the record of one march: the particles entering every half-cell (state and alive), the exact fields of every
+        // slice and pass; the adjoints of the streaming particles and of the joining ones carried between steps
+        const size_t passes = size_t(c.pl->cfg.iterations), m = size_t(npl_max);
+        const size_t sz[5] = {ns * 7 * m * 8, ns * passes * 6 * nk * 8, (ns + 1) * m * 4, 7 * m * 8, 7 * m * 8};
+        size_t off[5], tot = 0;
+        for (int q = 0; q < 5; ++q) { off[q] = tot; tot += (sz[q] + 255) / 256 * 256; }
+        if (c.adjrec.n < tot) c.adjrec.alloc(tot, st);
         aw.np = npl_max; aw.rs = npl_max;
-        aw.rec_x = reinterpret_cast<double*>(c.adjrec.p);
-        aw.rec_f = reinterpret_cast<double*>(c.adjrec.p + r1);
-        aw.lam = reinterpret_cast<double*>(c.adjrec.p + r1 + r2);
+        aw.rec_x = reinterpret_cast<double*>(c.adjrec.p + off[0]);
+        aw.rec_f = reinterpret_cast<double*>(c.adjrec.p + off[1]);
+        aw.rec_a = reinterpret_cast<int32_t*>(c.adjrec.p + off[2]);
+        aw.lam = reinterpret_cast<double*>(c.adjrec.p + off[3]);
+        aw.jl = reinterpret_cast<double*>(c.adjrec.p + off[4]);
     }
     if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
     else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
@@ -1336,10 +1345,18 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
             // adjoint takes the reads of the streaming pushes, then those of the beam push
             restore(k - 1);
             PlasmaState& Pl = *c.pl;
-            Pl.rec_x = aw.rec_x; Pl.rec_f = aw.rec_f; Pl.rec_np = aw.np;
-            struct Unrec { PlasmaState& P; ~Unrec() { P.rec_x = nullptr; P.rec_f = nullptr; P.rec_np = 0; } } unrec{Pl};
+            Pl.rec_x = aw.rec_x; Pl.rec_f = aw.rec_f; Pl.rec_a = aw.rec_a; Pl.rec_np = aw.rs;
+            struct Unrec { PlasmaState& P; ~Unrec() { P.rec_x = nullptr; P.rec_f = nullptr; P.rec_a = nullptr; P.rec_np = 0; } } unrec{Pl};
+            const long tr1 = Pl.trapped_total;
             step(c, false);
-            if (Pl.nstrm > aw.np) throw Error(G3D_ERR_STATE, "the adjoint march: the plasma of a step grew when run again");
+            if (Pl.nstrm > aw.rs || Pl.trapped_total != tr1)
+                throw Error(G3D_ERR_STATE, "the adjoint march: a step run again from its level did not repeat its plasma");
+            // the streaming particles' adjoints after the march: the slow trapped ones are the next march's joining ones
+            G3D_CUDA(cudaMemsetAsync(aw.lam, 0, 7 * size_t(aw.rs) * 8, st));
+            const long njl = k < K ? long(joins[size_t(k)].size()) : 0;
+            const long nslow = launch_join_adjoint_in(c, aw.jl, njl, aw.lam, aw.rs);
+            if (k < K && nslow != njl)
+                throw Error(G3D_ERR_STATE, "the adjoint march: the trapped particles of a step run again differ from its forward");
             G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
             G3D_CUDA(cudaMemsetAsync(ljk[2], 0, (ns + 1) * nkh * sizeof(cpx), st));
             for (int q = 0; q < 2; ++q) ap.lj0[q] = lj0[q];
@@ -1347,6 +1364,8 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
             AdjPlasmaWs awk = aw;
             awk.np = Pl.nstrm;
             adjoint_march_plasma(c, awk, ap, FD + size_t(k - 1) * Fn, lF, sl[size_t(k - 1)], sl[size_t(k)]);
+            // the joining particles of this march (after its fresh plasma) pass their adjoints to the march before
+            launch_join_adjoint_out(c, aw.lam, aw.rs, Pl.fresh_last, long(joins[size_t(k - 1)].size()), aw.jl);
             launch_adj_currents(c, ljk, W, V, lJ, Pl.box_mean);
         } else {
             launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);

@@ -390,9 +390,13 @@ static void record_fields(Ctx& c, int l, int p) {
 static void record_particles(Ctx& c, int n) {
     PlasmaState& P = *c.pl;
     const size_t np = size_t(P.rec_np);
-    const double* src[5] = {P.strm.x, P.strm.y, P.strm.px, P.strm.py, P.strm.pz};
-    for (int q = 0; q < 5; ++q)
-        G3D_CUDA(cudaMemcpyAsync(P.rec_x + (5 * size_t(n) + q) * np, src[q], size_t(P.nstrm) * 8, cudaMemcpyDeviceToDevice, c.stream));
+    if (n >= 0) {
+        const double* src[7] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.z, P.strm.px, P.strm.py, P.strm.pz};
+        for (int q = 0; q < 7; ++q)
+            G3D_CUDA(cudaMemcpyAsync(P.rec_x + (7 * size_t(n) + q) * np, src[q], size_t(P.nstrm) * 8, cudaMemcpyDeviceToDevice,
+                                     c.stream));
+    }
+    G3D_CUDA(cudaMemcpyAsync(P.rec_a + size_t(n + 1) * np, P.strm.alive, size_t(P.nstrm) * 4, cudaMemcpyDeviceToDevice, c.stream));
 }
 
 void march_plasma(Ctx& c, double s0, double s1) {
@@ -420,7 +424,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
-    mixk(ptr(c.F.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
+    mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
@@ -449,6 +453,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.ylo = c.yf ? -1e300 : c.ynode_h[1]; sa.yhi = c.yf ? 1e300 : c.ynode_h[size_t(c.ny) - 1];
         sa.Fmid = c.yf || c.f32s ? static_cast<const void*>(P.fmid.p) : nullptr;   // null if never allocated
         sa.inv_dx = 1 / c.dx; sa.inv_dy = 1 / c.dy; sa.dep_norm = 0;
+        sa.Fd = c.mixed ? nullptr : c.Fd.p;
         sa.ext = c.ext;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
@@ -484,6 +489,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             else launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
             have_dl = true;
         }
+        if (P.rec_x) record_particles(c, -1);            // the states after the last half-cell
     };
     PlasmaState::LoopGraph* hit = nullptr;
     for (auto& l : P.loops) if (l.key == key) hit = &l;

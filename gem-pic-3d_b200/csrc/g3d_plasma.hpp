@@ -51,6 +51,8 @@ struct StreamArgs {
     ExtDev ext;                // external magnetic elements (none: nu = nm = 0)
     double inv_dx, inv_dy;     // 1/dx, 1/dy (the mixed form's FP32 gathers and deposit)
     double dep_norm;           // 1 / (Delta h_n dx): the deposit factor of half-cell n per unit of q w dt (the mixed form's FP32 deposit)
+    const double* Fd;          // exact fields (FP64 form, Fourier y, no ionization, no analytic wave): the F planes in FP64 for
+                               // the gather of a particle that starts inside the half-cell (null: the float planes F)
 };
 
 struct PlasmaPtrs {
@@ -134,10 +136,12 @@ struct PlasmaState {
     std::vector<LoopGraph> loops;
     DevBuf<StepVals> stepv;
     // recording for the adjoint march (null: off; the slice loop then runs without its graph): the streaming particles
-    // entering every half-cell n (x, y, p_x, p_y, p_z; rec_np each, at rec_x + 5 rec_np n) and the exact real fields of
-    // every slice n after every pass p (6 planes of nk, at rec_f + 6 nk (P n + p))
+    // entering every half-cell n (x, y, zeta, z, p_x, p_y, p_z; rec_np each, at rec_x + 7 rec_np n) with their state
+    // alive (at rec_a + rec_np (n + 1); after the last half-cell at rec_a), and the exact real fields of every slice n
+    // after every pass p (6 planes of nk, at rec_f + 6 nk (P n + p))
     double* rec_x = nullptr;
     double* rec_f = nullptr;
+    int32_t* rec_a = nullptr;
     long rec_np = 0;
     PlasmaPtrs ptrs(const Ctx& c) const;
     PlasmaState() = default;
@@ -157,19 +161,27 @@ struct AdjPlasmaPtrs {
     cpx *lold, *ljsnA, *ljsn, *ldl;      // 4, 3, 3, 3 planes
     cpx* lsi0[2];              // 3 planes each, by the parity of the half-cell
 };
-// ... and its scratch: the record of the forward march (PlasmaState::rec_x, rec_f), np streaming particles recorded
-// with the stride rs (rs >= np)
+// ... and its scratch: the record of the forward march (PlasmaState::rec_x, rec_f, rec_a), np streaming particles
+// recorded with the stride rs (rs >= np)
 struct AdjPlasmaWs {
     long np, rs;
     double *rec_x, *rec_f;
+    int32_t* rec_a;
     double *lFup[2], *lFcur;   // 6 real planes each: the adjoints of a slice's real fields
     double* ljsr;              // 3 real planes: the adjoint of a pass's streaming deposit
-    double* lam;               // 5 rs: the adjoint of the streaming particles' state
+    double* lam;               // 7 rs: the adjoint of the streaming particles' state (x, y, zeta, z, p)
+    double* jl;                // 7 rs: the adjoint of the state of the joining particles carried to the step before
     cpx* Wsc[6];               // one plane each of transform scratch
     cpx* Tsc[3];
 };
 void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
                           double s1);
+// The slow trapped particles of the march just run (alive 5, v_z below vz_beam) in list order: they join the next
+// march after its fresh plasma. launch_join_adjoint_out copies the adjoint of the state of the next march's joining
+// particles (lam from index fresh, n of them) to jl; launch_join_adjoint_in puts jl onto those particles of this march
+// (lam, 7 components of stride rs). Both return how many particles they moved.
+long launch_join_adjoint_out(Ctx& c, const double* lam, long rs, long fresh, long n, double* jl);
+long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, long rs);
 void launch_d2f(Ctx& c, const double* a, float* b, long n);     // b = float(a)
 
 // launchers (k_plasma.cu)

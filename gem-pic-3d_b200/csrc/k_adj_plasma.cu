@@ -161,18 +161,22 @@ __global__ void k_adjp_march(Geo g, AdjPlasmaPtrs a, int n, double D, int last, 
 }
 
 // ---------------------------------------------------------------- the transposed streaming push of one pass
-// The midpoint fields (Fa + Fb) / 2 of the recorded slices n and n+1 gathered with TSC (sgather_mid of k_plasma.cu);
-// the adjoint deposits half of each field adjoint into lFa and lFb and returns dJ/d(position)
-struct MidGat {
+// The fields of the recorded slices n (Fa, as pass p read it) and n+1 (Fb) at (xm, ym, zetam): TSC in x and y, linear
+// in zeta between the two slices (fz = (zetam - zn) / h; 1/2 for a particle crossing the whole half-cell, whose gather
+// the forward takes from the midpoint fields (Fa + Fb) / 2). The adjoint deposits the field adjoints into lFa, lFb
+// with the same weights and adds dJ/d(position).
+struct SliceGat {
     const Geo* g;
     const double *Fa, *Fb;
     long sa, sb;
     double *lFa, *lFb;
     long lsa, lsb;
-    __device__ void gather(double xm, double ym, double E[3], double B[3]) const {
+    double zn, ih;
+    __device__ void gather(double xm, double ym, double zetam, double E[3], double B[3]) const {
         int ix[3], jn[3]; double wx[3], wn[3];
         tsc_periodic(wrap_periodic(xm, g->Lx), g->dx, g->nx, ix, wx);
         tsc_periodic(wrap_periodic(ym, g->Ly), g->dy, g->ny, jn, wn);
+        const double fz = (zetam - zn) * ih;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             double v = 0;
@@ -181,40 +185,41 @@ struct MidGat {
 #pragma unroll
                 for (int ii = 0; ii < 3; ++ii) {
                     const long k = long(jn[jj]) * g->nx + ix[ii];
-                    v += wx[ii] * wn[jj] * (0.5 * (Fa[c * sa + k] + Fb[c * sb + k]));
+                    v += wx[ii] * wn[jj] * ((1 - fz) * Fa[c * sa + k] + fz * Fb[c * sb + k]);
                 }
             if (c < 3) E[c] = v; else B[c - 3] = v;
         }
     }
-    __device__ void adjoint(double xm, double ym, const double lE[3], const double lB[3], double& lxm, double& lym) const {
-        const double xw = wrap_periodic(xm, g->Lx), yw = wrap_periodic(ym, g->Ly);
+    __device__ void adjoint(double xm, double ym, double zetam, const double lE[3], const double lB[3], double& lxm, double& lym,
+                            double& lzm) const {
+        const double xw = wrap_periodic(xm, g->Lx), yw = wrap_periodic(ym, g->Ly), fz = (zetam - zn) * ih;
         int ix[3], jn[3]; double wx[3], wn[3], dwx[3], dwn[3];
         tsc_periodic(xw, g->dx, g->nx, ix, wx);
         tsc_periodic(yw, g->dy, g->ny, jn, wn);
         tsc_slopes(xw / g->dx, dwx);
         tsc_slopes(yw / g->dy, dwn);
-        double sx = 0, sy = 0;
+        double sx = 0, sy = 0, sz = 0;
 #pragma unroll
         for (int c = 0; c < 6; ++c) {
             const double l = c < 3 ? lE[c] : lB[c - 3];
-            double vx = 0, vy = 0;
+            double vx = 0, vy = 0, vz = 0;
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj)
 #pragma unroll
                 for (int ii = 0; ii < 3; ++ii) {
                     const long k = long(jn[jj]) * g->nx + ix[ii];
-                    const double m = 0.5 * (Fa[c * sa + k] + Fb[c * sb + k]);
-                    vx += dwx[ii] * wn[jj] * m; vy += wx[ii] * dwn[jj] * m;
+                    const double a = Fa[c * sa + k], b = Fb[c * sb + k], m = (1 - fz) * a + fz * b, w = wx[ii] * wn[jj];
+                    vx += dwx[ii] * wn[jj] * m; vy += wx[ii] * dwn[jj] * m; vz += w * (b - a);
                     if (l != 0) {
-                        const double u = 0.5 * l * wx[ii] * wn[jj];
-                        atomicAdd(lFa + c * lsa + k, u);
-                        atomicAdd(lFb + c * lsb + k, u);
+                        atomicAdd(lFa + c * lsa + k, (1 - fz) * l * w);
+                        atomicAdd(lFb + c * lsb + k, fz * l * w);
                     }
                 }
-            sx += l * vx; sy += l * vy;
+            sx += l * vx; sy += l * vy; sz += l * vz;
         }
         lxm += sx / g->dx;
         lym += sy / g->dy;
+        lzm += sz * ih;
     }
 };
 // the current adjoints lJ (3 real planes) gathered with the deposit's TSC weights and 1/A (sdeposit of k_plasma.cu)
@@ -243,31 +248,41 @@ struct DepGat {
         }
     }
 };
-// One thread per streaming particle of the recorded list: the state entering half-cell n (rec), the pass's current
-// adjoints lJ and, for the last pass, the adjoint of the state it leaves with (lam, replaced by the adjoint of the
-// state it enters with; earlier passes add to it: they deposit from the same state). Fixed ions carry no current
+// One thread per streaming particle of the recorded list: the state entering half-cell n (rec: x, y, zeta, z, p_x,
+// p_y, p_z of stride rs), its state alive before (ae) and after (ax) the half-cell, the pass's current adjoints lJ
+// and, for the last pass, the adjoint of the state it leaves with (lam, replaced by the adjoint of the state it
+// enters with; the earlier passes add to it: they deposit from the same state). A particle takes part as the forward
+// let it (alive, or waiting and reached by the half-cell; then from its zeta: a partial path); the last pass keeps
+// the forward's trapping event (ax = 5), an earlier one decides it as the forward did. Fixed ions carry no current
 // and do not move; particles of no charge deposit nothing.
 template <bool LAST>
 __global__ void __launch_bounds__(128) k_adjp_stream(Geo g, StrmDev S, const IonDevC* __restrict__ ions, long np, long rs,
-                                                     const double* __restrict__ rec, int n, double Delta, const double* Fa, long sa,
-                                                     const double* Fb, long sb, double* lFa, long lsa, double* lFb, long lsb,
-                                                     const double* __restrict__ lJ, double* __restrict__ lam) {
+                                                     const double* __restrict__ rec, const int32_t* __restrict__ ae,
+                                                     const int32_t* __restrict__ ax, int n, double Delta, double sTrap,
+                                                     const double* Fa, long sa, const double* Fb, long sb, double* lFa, long lsa,
+                                                     double* lFb, long lsb, const double* __restrict__ lJ, double* __restrict__ lam) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= np || S.alive[i] != 1) return;
+    if (i >= np) return;
+    const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn, zeta = rec[2 * rs + i];
+    const int a_in = ae[i];
+    if (!(a_in == 1 || (a_in == 6 && zeta > zn))) return;
     const int sp = S.sp[i];
     if (sp >= SP_ION && sp < SP_FREED && !ions[sp - SP_ION].mobile) return;
     const double qw = S.q[i] * S.w[i];
     if (qw == 0) return;
-    const double h = g.zs[n + 1] - g.zs[n], fscale = 1 / (Delta * h * g.dx);
-    const double p[3] = {rec[2 * rs + i], rec[3 * rs + i], rec[4 * rs + i]};
-    double lout[5] = {0, 0, 0, 0, 0};
+    StreamCase K;
+    K.zn = zn; K.h = h; K.fscale = 1 / (Delta * h * g.dx); K.sTrap = sTrap;
+    K.partial = zeta < zn1 - 1e-9 * h;
+    K.trap = LAST ? (ax[i] == 5 ? 1 : 0) : 2;
+    const double p[3] = {rec[4 * rs + i], rec[5 * rs + i], rec[6 * rs + i]};
+    double lout[7] = {0, 0, 0, 0, 0, 0, 0};
     if (LAST)
-        for (int k = 0; k < 5; ++k) lout[k] = lam[k * rs + i];
-    MidGat gat{&g, Fa, Fb, sa, sb, lFa, lFb, lsa, lsb};
+        for (int k = 0; k < 7; ++k) lout[k] = lam[k * rs + i];
+    SliceGat gat{&g, Fa, Fb, sa, sb, lFa, lFb, lsa, lsb, zn, 1 / h};
     DepGat dep{&g, lJ};
-    double lin[5];
-    stream_push_reverse(rec[i], rec[rs + i], p, S.qm[i], qw, h, fscale, gat, dep, lout, lin);
-    for (int k = 0; k < 5; ++k) lam[k * rs + i] = LAST ? lin[k] : lam[k * rs + i] + lin[k];
+    double lin[7];
+    stream_push_reverse(rec[i], rec[rs + i], zeta, rec[3 * rs + i], p, S.qm[i], qw, K, gat, dep, lout, lin);
+    for (int k = 0; k < 7; ++k) lam[k * rs + i] = LAST ? lin[k] : lam[k * rs + i] + lin[k];
 }
 
 // ---------------------------------------------------------------- the reverse of one march
@@ -276,11 +291,13 @@ static unsigned mode_blocks(long n) {
     return unsigned(b < 1 ? 1 : b);
 }
 
-// The transpose of march_plasma(s0, s1) for the step whose forward was recorded into w.rec_x, w.rec_f. On entry lS holds
-// the adjoints of the step's final spectra, ljk (x, y) those of jk as the next step's j0 (ljk z zero), ljs0 those of
-// the step's final js0, lj0 zeros; lF (the level s0 real fields' adjoint, whole window) receives the reads of the
+// The transpose of march_plasma(s0, s1) for the step whose forward was recorded into w.rec_x, w.rec_f, w.rec_a. On entry
+// lS holds the adjoints of the step's final spectra, ljk (x, y) those of jk as the next step's j0 (ljk z zero), ljs0
+// those of the step's final js0, lj0 zeros, w.lam those of the streaming particles' states after the march (the slow
+// trapped ones join the next march); lF (the level s0 real fields' adjoint, whole window) receives the reads of the
 // level s0 fields. On exit lS holds the adjoints of the level s0 spectra, lj0 of j0, ljk of the beam current of the
-// step (x, y, z), ljs0 of the level s0 streaming current. Fprev: the level s0 exact real fields.
+// step (x, y, z), ljs0 of the level s0 streaming current, w.lam of the streaming particles' states at the start.
+// Fprev: the level s0 exact real fields.
 void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
                           double s1) {
     PlasmaState& P = *c.pl;
@@ -294,7 +311,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
     for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
     G3D_CUDA(cudaMemsetAsync(a.ldl, 0, 3 * nkh * sizeof(cpx), st));
     G3D_CUDA(cudaMemsetAsync(w.lFup[0], 0, 6 * nk * 8, st));
-    if (rs) G3D_CUDA(cudaMemsetAsync(w.lam, 0, 5 * size_t(rs) * 8, st));
+    const double sTrap = s1 + (P.cfg.trap_advance - 1) * Delta;
     const StrmDev S = P.strm;
     const double* Fnext = nullptr;
     int cur = 0;
@@ -320,13 +337,15 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
             const long sa = p == 0 ? fpl : nk;
             double* lFa = p == 0 ? lF + size_t(n - c.a) * nk : w.lFcur;
             const long lsa = p == 0 ? fpl : nk;
-            const double* rec = w.rec_x + 5 * size_t(rs) * size_t(n);
+            const double* rec = w.rec_x + 7 * size_t(rs) * size_t(n);
+            const int32_t* ae = w.rec_a + size_t(rs) * size_t(n + 1);
+            const int32_t* ax = w.rec_a + size_t(rs) * size_t(n);
             if (p == passes - 1)
-                k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, n, Delta, Fa, sa, Fnext, nk, lFa, lsa,
-                                                        w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
+                k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, ae, ax, n, Delta, sTrap, Fa, sa, Fnext,
+                                                        nk, lFa, lsa, w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
             else
-                k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, n, Delta, Fa, sa, Fnext, nk, lFa, lsa,
-                                                         w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
+                k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, ae, ax, n, Delta, sTrap, Fa, sa, Fnext,
+                                                         nk, lFa, lsa, w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
             c.check_launch("k_adjp_stream");
         }
         cur ^= 1;

@@ -106,6 +106,33 @@ __device__ __forceinline__ void sgather(const StreamArgs& c, double x, double y,
         if (comp < 3) E[comp] = v; else B[comp - 3] = v;
     }
 }
+// The exact fields (the FP64 planes Fd of the FP64 form) at (x, y, zeta), TSC in x and y, linear in zeta: the gather of
+// a particle that starts inside the half-cell when the fields are kept exact (a variant of its own, k_stream's EX)
+__device__ __forceinline__ void sgather_exact(const StreamArgs& c, double x, double y, double zeta, double E[3], double B[3]) {
+    E[0] = E[1] = E[2] = B[0] = B[1] = B[2] = 0;
+    const Geo& g = c.g;
+    int n; double fz;
+    g.zax.locate(zeta, n, fz);
+    if (n == g.a - 1 && fz > 1 - 1e-9) { n = g.a; fz = 0; }
+    const int fl = n - g.a;
+    if (fl < 0 || fl > g.ns) return;
+    int ix[3], jn[3]; double wx[3], wn[3];
+    tsc_periodic(x, g.dx, g.nx, ix, wx);
+    tsc_periodic(y, g.dy, g.ny, jn, wn);
+    const long nk = g.nk;
+    for (int comp = 0; comp < 6; ++comp) {
+        const double* p0 = c.Fd + (long(comp) * (g.ns + 2) + fl) * nk;
+        const double* p1 = p0 + nk;
+        double v0 = 0, v1 = 0;
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                const long k = long(jn[j]) * g.nx + ix[i];
+                v0 += wx[i] * wn[j] * p0[k]; v1 += wx[i] * wn[j] * p1[k];
+            }
+        const double v = (1 - fz) * v0 + fz * v1;
+        if (comp < 3) E[comp] = v; else B[comp - 3] = v;
+    }
+}
 // The gather half-way through the half-cell (zeta = the slice midpoint, a particle crossing the whole half-cell):
 // TSC in x and y of the interleaved midpoint fields, one vector load per point (Fourier y).
 template <bool F32>
@@ -338,7 +365,8 @@ struct DepReq {
 // starts from the same state without a copy of the particles.
 // ION: some species ionizes (else the field magnitudes and the ADK sampling are left out); LASER: the analytic
 // plane wave is on. Both are fixed for a run; the variants without them hold fewer registers.
-template <bool F32, bool ION, bool LASER, bool YF>
+// EX: exact fields (FP64 form, Fourier y, neither ionization nor the analytic wave): the gathers from the FP64 planes.
+template <bool F32, bool ION, bool LASER, bool YF, bool EX = false>
 __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
     DepReq d{0, 0, 0, 0, 0, 0, false, false, 0.f, {0.f, 0.f, 0.f}};
     const Geo& g = c.g;
@@ -397,6 +425,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     } else {
         double Ed[3], Bd[3], Ee[3], Be[3];
         if (YF && mid) sgather_mid<F32>(c, wrapx(g, xm), wrapy<YF>(g, ym), Ed, Bd);   // free-hand: Fmid is FP32-only
+        else if (EX) sgather_exact(c, wrapx(g, xm), wrapy<YF>(g, ym), zetam, Ed, Bd);
         else sgather<F32, YF>(c, wrapx(g, xm), wrapy<YF>(g, ym), zetam, Ed, Bd);
         if constexpr (LASER) {
             c.laser.field(xm + c.sv->X0, zm, zm - (zetam - c.zc), Ee, Be);
@@ -477,13 +506,13 @@ constexpr int ST_NT = 128;
 #endif
 // YF: the Fourier y grid (true) or the free-hand one, fixed for a run, so that each variant holds only its own grid's
 // gathers and deposits (fewer registers and no local arrays).
-template <bool F32, bool ION, bool LASER, bool YF>
+template <bool F32, bool ION, bool LASER, bool YF, bool EX = false>
 __global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c,
                                                                                        const long* __restrict__ nstrm) {
     const StrmDev S = c.sd[0];
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
-        const DepReq d = stream_one<F32, ION, LASER, YF>(c, S, i);
+        const DepReq d = stream_one<F32, ION, LASER, YF, EX>(c, S, i);
         if (d.on) {
             if (F32 && YF && d.f32) sdeposit_f32(c, d.x, d.y, d.ff, d.fv[0], d.fv[1], d.fv[2]);
             else sdeposit<F32, YF>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
@@ -494,6 +523,12 @@ template <bool F32, bool YF>
 static void stream_launch_y(Ctx& c, const StreamArgs& a, unsigned blocks) {
     PlasmaState& P = *c.pl;
     const bool ion = P.any_ionizing, las = c.laser.on != 0;
+    if constexpr (!F32 && YF) {
+        if (a.Fd && !ion && !las) {
+            k_stream<false, false, false, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+            return;
+        }
+    }
     if (ion && las) k_stream<F32, true, true, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
     else if (ion) k_stream<F32, true, false, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
     else if (las) k_stream<F32, false, true, YF><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
@@ -1175,6 +1210,43 @@ long launch_trapped_split(Ctx& c, double s1) {
         c.check_launch("k_trap_gather");
     }
     return nf;
+}
+// The adjoint march across steps: the slow trapped particles of a march (in list order, as launch_trapped_split takes
+// them) are the next march's joining particles (its list from index fresh). Their state adjoints (7 components of
+// stride rs: x, y, zeta, z, p_x, p_y, p_z) go from the next march's list to this one's.
+__global__ void k_join_adj_out(const double* __restrict__ lam, long rs, long fresh, long n, double* __restrict__ jl) {
+    for (long j = long(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += long(gridDim.x) * blockDim.x)
+        for (int q = 0; q < 7; ++q) jl[q * n + j] = lam[q * rs + fresh + j];
+}
+__global__ void k_join_adj_in(const int* __restrict__ flag, const int* __restrict__ off, long cap, const double* __restrict__ jl,
+                              long njl, double* __restrict__ lam, long rs) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += long(gridDim.x) * blockDim.x) {
+        if (!flag[i]) continue;
+        const long j = off[i];
+        if (j >= njl) continue;
+        for (int q = 0; q < 7; ++q) lam[q * rs + i] = jl[q * njl + j];
+    }
+}
+long launch_join_adjoint_out(Ctx& c, const double* lam, long rs, long fresh, long n, double* jl) {
+    if (n <= 0) return 0;
+    k_join_adj_out<<<ew_blocks(n), 256, 0, c.stream>>>(lam, rs, fresh, n, jl);
+    c.check_launch("k_join_adj_out");
+    return n;
+}
+long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, long rs) {
+    PlasmaState& P = *c.pl;
+    const long cap = P.s.cap;
+    if (cap <= 0) return 0;
+    reserve_flags(c, cap);
+    k_trap_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(P.strm, P.nstrm_dev.p, cap, P.cfg.vz_beam, 0, P.cflag.p);
+    c.check_launch("k_trap_flags");
+    const long ns = scan_flags(c, cap);
+    if (ns > 0 && njl > 0 && rs >= std::min<long>(cap, P.nstrm)) {
+        k_join_adj_in<<<ew_blocks(std::min<long>(cap, rs)), 256, 0, c.stream>>>(P.cflag.p, P.coff.p, std::min<long>(cap, rs), jl, njl,
+                                                                               lam, rs);
+        c.check_launch("k_join_adj_in");
+    }
+    return ns;
 }
 long launch_join_cap(Ctx& c) {
     PlasmaState& P = *c.pl;

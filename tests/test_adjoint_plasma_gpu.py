@@ -80,6 +80,36 @@ def test_plasma_momentum_gradient_against_central_differences(through_start):
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
 
 
+@pytest.mark.parametrize("what", ["laser modes", "momenta"])
+def test_plasma_gradients_with_trapped_electrons(what):
+    """At a0 = 1 about 130 plasma electrons a step advance a whole step in z inside the window: the forward traps them
+    (they stop inside their half-cell) and they join the next step's march at their zeta, in its partial half-cell.
+    The adjoint keeps these events as the forward took them and differentiates the trapped pushes (the third Boris
+    push over dtp = (s1 - z) / v_z, the stop in zeta) and the joining paths across the steps."""
+    from g3d import Simulation
+    cfg = case(a0=1.0, charge_pC=1.0)
+    s = Simulation(cfg)
+    s.load_bunch()
+    s.set_exact_fields(True)
+    s.init_fields()
+    s.step()
+    trapped = int(np.sum(s.streaming_particles()["alive"] == 5))
+    s.close()
+    assert trapped > 0
+    J, gm, gp, _ = adjoint(cfg)
+    rng = np.random.default_rng(33)
+    if what == "laser modes":
+        d = hermitian_direction(rng, cfg.ny, cfg.nx)
+        ad = float(np.real(np.sum(np.conj(gm) * d)))
+        fd = central(forward(cfg, coef=1 + EPS * d), forward(cfg, coef=1 - EPS * d), EPS)
+    else:
+        D = rng.standard_normal(gp.shape)
+        ad = float(np.sum(gp * D))
+        fd = central(forward(cfg, dp=EPS * D), forward(cfg, dp=-EPS * D), EPS)
+    print(f"trapping, {what}: J = {J:.12e}, adjoint {ad:.12e}, central difference {fd:.12e}")
+    assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
 def test_plasma_adjoint_refuses_what_it_does_not_differentiate():
     """The mixed form and ionization are refused with G3D_ERR_ARG before anything runs."""
     from g3d import G3DError, Simulation, configs
