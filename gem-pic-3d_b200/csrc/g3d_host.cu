@@ -1311,9 +1311,9 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         // the record of one march: the particles entering every half-cell (state and alive), the exact fields of every
         // slice and pass; the adjoints of the streaming particles and of the joining ones carried between steps
         const size_t passes = size_t(c.pl->cfg.iterations), m = size_t(npl_max);
-        const size_t sz[5] = {ns * 7 * m * 8, ns * passes * 6 * nk * 8, (ns + 1) * m * 4, 7 * m * 8, 7 * m * 8};
-        size_t off[5], tot = 0;
-        for (int q = 0; q < 5; ++q) { off[q] = tot; tot += (sz[q] + 255) / 256 * 256; }
+        const size_t sz[6] = {ns * 7 * m * 8, ns * passes * 6 * nk * 8, (ns + 1) * m * 4, 7 * m * 8, 7 * m * 8, sizeof(AdjStepDev)};
+        size_t off[6], tot = 0;
+        for (int q = 0; q < 6; ++q) { off[q] = tot; tot += (sz[q] + 255) / 256 * 256; }
         if (c.adjrec.n < tot) c.adjrec.alloc(tot, st);
         aw.np = npl_max; aw.rs = npl_max;
         aw.rec_x = reinterpret_cast<double*>(c.adjrec.p + off[0]);
@@ -1321,6 +1321,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         aw.rec_a = reinterpret_cast<int32_t*>(c.adjrec.p + off[2]);
         aw.lam = reinterpret_cast<double*>(c.adjrec.p + off[3]);
         aw.jl = reinterpret_cast<double*>(c.adjrec.p + off[4]);
+        aw.stepd = reinterpret_cast<AdjStepDev*>(c.adjrec.p + off[5]);
     }
     if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
     else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));

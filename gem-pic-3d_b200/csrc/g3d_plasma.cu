@@ -387,17 +387,7 @@ static void record_fields(Ctx& c, int l, int p) {
     double* dst = P.rec_f + 6 * nk * (size_t(P.cfg.iterations) * size_t(l) + size_t(p));
     G3D_CUDA(cudaMemcpy2DAsync(dst, nk * 8, c.Fd.p + size_t(l - c.a) * nk, fpl * 8, nk * 8, 6, cudaMemcpyDeviceToDevice, c.stream));
 }
-static void record_particles(Ctx& c, int n) {
-    PlasmaState& P = *c.pl;
-    const size_t np = size_t(P.rec_np);
-    if (n >= 0) {
-        const double* src[7] = {P.strm.x, P.strm.y, P.strm.zeta, P.strm.z, P.strm.px, P.strm.py, P.strm.pz};
-        for (int q = 0; q < 7; ++q)
-            G3D_CUDA(cudaMemcpyAsync(P.rec_x + (7 * size_t(n) + q) * np, src[q], size_t(P.nstrm) * 8, cudaMemcpyDeviceToDevice,
-                                     c.stream));
-    }
-    G3D_CUDA(cudaMemcpyAsync(P.rec_a + size_t(n + 1) * np, P.strm.alive, size_t(P.nstrm) * 4, cudaMemcpyDeviceToDevice, c.stream));
-}
+static void record_particles(Ctx& c, int n) { launch_record_particles(c, n); }
 
 void march_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
@@ -424,7 +414,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
-    mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
+    mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(ptr(P.rec_x)); mixk(ptr(P.rec_f)); mixk(ptr(P.rec_a)); mixk(uint64_t(P.rec_np)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
@@ -493,7 +483,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
     };
     PlasmaState::LoopGraph* hit = nullptr;
     for (auto& l : P.loops) if (l.key == key) hit = &l;
-    if (c.profiling || P.rec_x) {
+    if (c.profiling) {
         issue();
     } else if (hit) {
         c.launches += hit->launches;

@@ -134,6 +134,8 @@ struct PlasmaState {
     // buffers swap every step); captured again only when a buffer moved
     struct LoopGraph { uint64_t key; cudaGraphExec_t exec; long launches; };
     std::vector<LoopGraph> loops;
+    // the reverse of a march (the adjoint, k_adj_plasma.cu) as a CUDA graph, keyed like the loops
+    struct AdjGraph { uint64_t key = 0; cudaGraphExec_t exec = nullptr; } adjg;
     DevBuf<StepVals> stepv;
     // recording for the adjoint march (null: off; the slice loop then runs without its graph): the streaming particles
     // entering every half-cell n (x, y, zeta, z, p_x, p_y, p_z; rec_np each, at rec_x + 7 rec_np n) with their state
@@ -147,10 +149,19 @@ struct PlasmaState {
     PlasmaState() = default;
     PlasmaState(const PlasmaState&) = delete;
     PlasmaState& operator=(const PlasmaState&) = delete;
-    ~PlasmaState() { for (auto& l : loops) cudaGraphExecDestroy(l.exec); }
+    ~PlasmaState() {
+        for (auto& l : loops) cudaGraphExecDestroy(l.exec);
+        if (adjg.exec) cudaGraphExecDestroy(adjg.exec);
+    }
 };
 
-// The adjoint of one march (k_adj_plasma.cu). The adjoint arrays of the window (device, half spectra):
+// The adjoint of one march (k_adj_plasma.cu). The values of a step its kernels read from device memory:
+struct AdjStepDev {
+    const double* Fprev;       // the exact real fields of level s0
+    double sTrap;
+    long np;                   // the streaming particles of the march
+};
+// The adjoint arrays of the window (device, half spectra):
 struct AdjPlasmaPtrs {
     long nkh;
     cpx* lS[6];                // the spectra {R_x, R_y, E_z, B_z, L_x, L_y}, ns planes
@@ -171,6 +182,7 @@ struct AdjPlasmaWs {
     double* ljsr;              // 3 real planes: the adjoint of a pass's streaming deposit
     double* lam;               // 7 rs: the adjoint of the streaming particles' state (x, y, zeta, z, p)
     double* jl;                // 7 rs: the adjoint of the state of the joining particles carried to the step before
+    AdjStepDev* stepd;         // the values of the step (device)
     cpx* Wsc[6];               // one plane each of transform scratch
     cpx* Tsc[3];
 };
@@ -185,6 +197,7 @@ long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, lon
 void launch_d2f(Ctx& c, const double* a, float* b, long n);     // b = float(a)
 
 // launchers (k_plasma.cu)
+void launch_record_particles(Ctx& c, int n);     // the adjoint's record of the particles entering half-cell n
 void launch_stream(Ctx& c, const StreamArgs& a);
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
 void launch_pass_prologue(Ctx& c, int n, int restore);

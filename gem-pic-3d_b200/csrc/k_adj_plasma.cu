@@ -17,6 +17,7 @@
 //   k_adjp_march    the transposed slice march of one pass with the replace and the prediction (one thread per mode)
 //   k_adjp_stream   the transposed push and deposit of every streaming particle in one pass (k_adj_stream.cuh)
 // and the transposed real fields and current spectra of one slice (k_adjoint.cu).
+#include <cstring>
 #include "g3d_plasma.hpp"
 #include "k_adj_stream.cuh"
 
@@ -35,8 +36,10 @@ __device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     //
 // R(n+1) -= q (jsn - si0): dJ/djsn = -q dJ/dR(n+1), dJ/dsi0 = q dJ/dR(n+1) (to the last pass of half-cell n+1, which
 // made that prediction); dl(n-1) = jsn - js0(n): dJ/djsn += dJ/ddl, dJ/djs0_old(n) = -dJ/ddl; js0_new(n) = jsn and
 // jk(n) = b(n) + jsn as the next step's j0: dJ/djsn += dJ/djs0_new(n) + dJ/dj0_next(n) (x, y)
-__global__ void k_adjp_correct(AdjPlasmaPtrs a, int n, double q, int par) {
+__global__ void k_adjp_correct(AdjPlasmaPtrs a, int n, double q, int par, double* __restrict__ zero6, long nk) {
     const long nkh = a.nkh;
+    // the field adjoint of slice n+1 that this half-cell's pushes read: cleared for them
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < 6 * nk; i += long(gridDim.x) * blockDim.x) zero6[i] = 0;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
         const long pl = long(n + 1) * nkh + i;      // slice n+1 of the spectra, half-cell n of the current planes
         const cpx lr[3] = {a.lS[0][pl], a.lS[1][pl], C(0)};
@@ -61,9 +64,13 @@ __global__ void k_adjp_correct(AdjPlasmaPtrs a, int n, double q, int par) {
 // into lS, L's old value being unread), the new values of slice n+1 (lS, added), j0 and the beam part of jk (added),
 // the streaming current of the pass (ljsn) and, through the prediction of half-cell n-1, js0 and dl.
 // front: the front slice (L = E_z = B_z = 0), solved once with the prediction js0(N-2).
+// zero6 (not null): the field adjoint of slice n that this pass's pushes read (cleared: the transposed real fields of the
+// pass have taken it in)
 __global__ void k_adjp_march(Geo g, AdjPlasmaPtrs a, int n, double D, int last, int first, int multi, int extrap, double w,
-                             int par_prev, int front) {
+                             int par_prev, int front, double* __restrict__ zero6) {
     const long nkh = a.nkh;
+    if (zero6)
+        for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < 6 * long(g.nk); i += long(gridDim.x) * blockDim.x) zero6[i] = 0;
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
         const int kxi = int(i % g.H), j = int(i / g.H);
         const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
@@ -255,14 +262,22 @@ struct DepGat {
 // let it (alive, or waiting and reached by the half-cell; then from its zeta: a partial path); the last pass keeps
 // the forward's trapping event (ax = 5), an earlier one decides it as the forward did. Fixed ions carry no current
 // and do not move; particles of no charge deposit nothing.
+// The values of the step (the list and its count, sTrap, the level s0 fields) come from device memory (AdjStepDev), so
+// that the reverse of a march runs as one graph for every step. prev: Fa is slice n of the level s0 fields, st->Fprev +
+// off; else the given planes Fa.
 template <bool LAST>
-__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, StrmDev S, const IonDevC* __restrict__ ions, long np, long rs,
-                                                     const double* __restrict__ rec, const int32_t* __restrict__ ae,
-                                                     const int32_t* __restrict__ ax, int n, double Delta, double sTrap,
-                                                     const double* Fa, long sa, const double* Fb, long sb, double* lFa, long lsa,
-                                                     double* lFb, long lsb, const double* __restrict__ lJ, double* __restrict__ lam) {
+__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, const StrmDev* __restrict__ sd, const IonDevC* __restrict__ ions,
+                                                     const AdjStepDev* __restrict__ st, long rs, const double* __restrict__ rec,
+                                                     const int32_t* __restrict__ ae, const int32_t* __restrict__ ax, int n,
+                                                     double Delta, int prev, long off, const double* Fa, long sa, const double* Fb, long sb,
+                                                     double* lFa, long lsa, double* lFb, long lsb, const double* __restrict__ lJ,
+                                                     double* __restrict__ lam) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long np = st->np;
     if (i >= np) return;
+    const StrmDev S = sd[0];
+    const double sTrap = st->sTrap;
+    if (prev) Fa = st->Fprev + off;
     const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn, zeta = rec[2 * rs + i];
     const int a_in = ae[i];
     if (!(a_in == 1 || (a_in == 6 && zeta > zn))) return;
@@ -297,63 +312,102 @@ static unsigned mode_blocks(long n) {
 // trapped ones join the next march); lF (the level s0 real fields' adjoint, whole window) receives the reads of the
 // level s0 fields. On exit lS holds the adjoints of the level s0 spectra, lj0 of j0, ljk of the beam current of the
 // step (x, y, z), ljs0 of the level s0 streaming current, w.lam of the streaming particles' states at the start.
-// Fprev: the level s0 exact real fields.
+// Fprev: the level s0 exact real fields. The half-cell loop (some 13 launches a half-cell) runs as one CUDA graph,
+// captured at the first step and launched for the others: what changes from step to step (the particle count, sTrap,
+// Fprev) is read by the kernels from w.stepd.
 void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
                           double s1) {
     PlasmaState& P = *c.pl;
     const int N = c.N, passes = P.cfg.iterations;
     const double Delta = s1 - s0, D = 0.5 * Delta;
-    const long nkh = c.nkh, nk = c.nk, fpl = long(c.ns + 2) * nk, np = w.np, rs = w.rs;
+    const long nkh = c.nkh, nk = c.nk, fpl = long(c.ns + 2) * nk, rs = w.rs;
     const bool extrap = P.cfg.predictor_extrapolate != 0, keep0 = P.box_mean;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
     cudaStream_t st = c.stream;
-    std::vector<double> cen(size_t(N - 1));
-    for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
-    G3D_CUDA(cudaMemsetAsync(a.ldl, 0, 3 * nkh * sizeof(cpx), st));
-    G3D_CUDA(cudaMemsetAsync(w.lFup[0], 0, 6 * nk * 8, st));
-    const double sTrap = s1 + (P.cfg.trap_advance - 1) * Delta;
-    const StrmDev S = P.strm;
-    const double* Fnext = nullptr;
-    int cur = 0;
-    const unsigned mb = mode_blocks(nkh), pb = unsigned((np + 127) / 128);
-    for (int n = c.a; n <= N - 2; ++n) {
-        k_adjp_correct<<<mb, 128, 0, st>>>(a, n, D * c.wlo_h[size_t(n + 1)], n & 1);
-        c.check_launch("k_adjp_correct");
-        G3D_CUDA(cudaMemsetAsync(w.lFup[cur ^ 1], 0, 6 * nk * 8, st));
-        // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
-        const double wex = (n >= 1 && n + 1 <= N - 2)
-                               ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
-        Fnext = w.rec_f + 6 * nk * (size_t(passes) * size_t(n + 1) + size_t(passes - 1));
-        for (int p = passes - 1; p >= 0; --p) {
-            launch_adj_real_fields_slice(c, p == passes - 1 ? w.lFup[cur] : w.lFcur, nk, w.Wsc, a.lsl);
-            k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, n, D, p == passes - 1 ? 1 : 0, p == 0 ? 1 : 0, passes > 1 ? 1 : 0,
-                                              extrap ? 1 : 0, wex, (n - 1) & 1, 0);
-            c.check_launch("k_adjp_march");
-            cpx* js3[3] = {a.ljsn, a.ljsn + nkh, a.ljsn + 2 * nkh};
-            launch_adj_stream_spectra(c, js3, w.Tsc, w.ljsr, keep0, a2);
-            if (p >= 1) G3D_CUDA(cudaMemsetAsync(w.lFcur, 0, 6 * nk * 8, st));
-            if (!np) continue;
-            const double* Fa = p == 0 ? Fprev + size_t(n - c.a) * nk : w.rec_f + 6 * nk * (size_t(passes) * size_t(n) + size_t(p - 1));
-            const long sa = p == 0 ? fpl : nk;
-            double* lFa = p == 0 ? lF + size_t(n - c.a) * nk : w.lFcur;
-            const long lsa = p == 0 ? fpl : nk;
-            const double* rec = w.rec_x + 7 * size_t(rs) * size_t(n);
-            const int32_t* ae = w.rec_a + size_t(rs) * size_t(n + 1);
-            const int32_t* ax = w.rec_a + size_t(rs) * size_t(n);
-            if (p == passes - 1)
-                k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, ae, ax, n, Delta, sTrap, Fa, sa, Fnext,
-                                                        nk, lFa, lsa, w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
-            else
-                k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), S, P.ion_dev.p, np, rs, rec, ae, ax, n, Delta, sTrap, Fa, sa, Fnext,
-                                                         nk, lFa, lsa, w.lFup[cur ^ 1], nk, w.ljsr, w.lam);
-            c.check_launch("k_adjp_stream");
+    const AdjStepDev sv{Fprev, s1 + (P.cfg.trap_advance - 1) * Delta, w.np};
+    G3D_CUDA(cudaMemcpyAsync(w.stepd, &sv, sizeof sv, cudaMemcpyHostToDevice, st));
+    auto issue = [&]() {
+        std::vector<double> cen(size_t(N - 1));
+        for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
+        G3D_CUDA(cudaMemsetAsync(a.ldl, 0, 3 * nkh * sizeof(cpx), st));
+        G3D_CUDA(cudaMemsetAsync(w.lFup[0], 0, 6 * nk * 8, st));
+        int cur = 0;
+        const unsigned mb = mode_blocks(nkh), pb = unsigned((rs + 127) / 128);
+        for (int n = c.a; n <= N - 2; ++n) {
+            k_adjp_correct<<<mb, 128, 0, st>>>(a, n, D * c.wlo_h[size_t(n + 1)], n & 1, w.lFup[cur ^ 1], nk);
+            c.check_launch("k_adjp_correct");
+            // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
+            const double wex = (n >= 1 && n + 1 <= N - 2)
+                                   ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
+            const double* Fnext = w.rec_f + 6 * nk * (size_t(passes) * size_t(n + 1) + size_t(passes - 1));
+            for (int p = passes - 1; p >= 0; --p) {
+                launch_adj_real_fields_slice(c, p == passes - 1 ? w.lFup[cur] : w.lFcur, nk, w.Wsc, a.lsl);
+                k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, n, D, p == passes - 1 ? 1 : 0, p == 0 ? 1 : 0, passes > 1 ? 1 : 0,
+                                                  extrap ? 1 : 0, wex, (n - 1) & 1, 0, p >= 1 ? w.lFcur : nullptr);
+                c.check_launch("k_adjp_march");
+                cpx* js3[3] = {a.ljsn, a.ljsn + nkh, a.ljsn + 2 * nkh};
+                launch_adj_stream_spectra(c, js3, w.Tsc, w.ljsr, keep0, a2);
+                if (!rs) continue;
+                const double* Fa = p == 0 ? nullptr : w.rec_f + 6 * nk * (size_t(passes) * size_t(n) + size_t(p - 1));
+                const long sa = p == 0 ? fpl : nk, off = long(n - c.a) * nk;
+                double* lFa = p == 0 ? lF + off : w.lFcur;
+                const long lsa = p == 0 ? fpl : nk;
+                const double* rec = w.rec_x + 7 * size_t(rs) * size_t(n);
+                const int32_t* ae = w.rec_a + size_t(rs) * size_t(n + 1);
+                const int32_t* ax = w.rec_a + size_t(rs) * size_t(n);
+                if (p == passes - 1)
+                    k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), P.sdev.p, P.ion_dev.p, w.stepd, rs, rec, ae, ax, n, Delta,
+                                                            p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
+                                                            w.ljsr, w.lam);
+                else
+                    k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), P.sdev.p, P.ion_dev.p, w.stepd, rs, rec, ae, ax, n, Delta,
+                                                             p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
+                                                             w.ljsr, w.lam);
+                c.check_launch("k_adjp_stream");
+            }
+            cur ^= 1;
         }
-        cur ^= 1;
+        // the front slice N-1: its real fields (read by half-cell N-2), then its march with the prediction js0(N-2)
+        launch_adj_real_fields_slice(c, w.lFup[cur], nk, w.Wsc, a.lsl);
+        k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, 1, 1, 0, 0, 0.0, (N - 2) & 1, 1, nullptr);
+        c.check_launch("k_adjp_march");
+    };
+    // what the graph holds by value: the arrays, the grid and the step length
+    uint64_t key = 1469598103934665603ULL;
+    auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
+    auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
+    for (int q = 0; q < 6; ++q) { mixk(ptr(a.lS[q])); mixk(ptr(a.lsl[q])); mixk(ptr(w.Wsc[q])); }
+    for (int q = 0; q < 3; ++q) { mixk(ptr(a.ljk[q])); mixk(ptr(a.ljs0[q])); mixk(ptr(w.Tsc[q])); }
+    for (int q = 0; q < 2; ++q) { mixk(ptr(a.lj0[q])); mixk(ptr(a.lsi0[q])); mixk(ptr(w.lFup[q])); }
+    mixk(ptr(a.lold)); mixk(ptr(a.ljsnA)); mixk(ptr(a.ljsn)); mixk(ptr(a.ldl)); mixk(ptr(w.lFcur)); mixk(ptr(w.ljsr));
+    mixk(ptr(w.lam)); mixk(ptr(w.rec_x)); mixk(ptr(w.rec_f)); mixk(ptr(w.rec_a)); mixk(ptr(w.stepd)); mixk(ptr(lF));
+    mixk(ptr(P.sdev.p)); mixk(uint64_t(rs)); mixk(uint64_t(passes)); mixk(uint64_t(extrap) | uint64_t(keep0) << 1);
+    uint64_t bits;
+    std::memcpy(&bits, &Delta, sizeof bits); mixk(bits);
+    std::memcpy(&bits, &a2, sizeof bits); mixk(bits);
+    if (c.profiling) { issue(); return; }
+    if (!P.adjg.exec || P.adjg.key != key) {
+        if (P.adjg.exec) { cudaGraphExecDestroy(P.adjg.exec); P.adjg.exec = nullptr; }
+        G3D_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        try {
+            issue();
+        } catch (...) {
+            cudaGraph_t gr = nullptr;
+            cudaStreamEndCapture(st, &gr);
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            throw;
+        }
+        cudaGraph_t gr = nullptr;
+        G3D_CUDA(cudaStreamEndCapture(st, &gr));
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&ex, gr, 0);
+        cudaGraphDestroy(gr);
+        G3D_CUDA(e);
+        P.adjg.exec = ex;
+        P.adjg.key = key;
     }
-    // the front slice N-1: its real fields (read by half-cell N-2), then its march with the prediction js0(N-2)
-    launch_adj_real_fields_slice(c, w.lFup[cur], nk, w.Wsc, a.lsl);
-    k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, 1, 1, 0, 0, 0.0, (N - 2) & 1, 1);
-    c.check_launch("k_adjp_march");
+    G3D_CUDA(cudaGraphLaunch(P.adjg.exec, st));
 }
 
 __global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long n) {

@@ -1248,6 +1248,28 @@ long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, lon
     }
     return ns;
 }
+// The adjoint's record of the particles entering half-cell n (n < 0: only their states alive after the last one): the
+// seven state columns and alive of every streaming particle, the count read on the device, so that the recording
+// slice loop can run as a graph
+__global__ void k_rec_particles(const StrmDev* __restrict__ sd, const long* __restrict__ n_dev, long rs, double* __restrict__ rec,
+                                int32_t* __restrict__ ra) {
+    const StrmDev S = sd[0];
+    const long n = *n_dev < rs ? *n_dev : rs;
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
+        if (rec) {
+            rec[i] = S.x[i]; rec[rs + i] = S.y[i]; rec[2 * rs + i] = S.zeta[i]; rec[3 * rs + i] = S.z[i];
+            rec[4 * rs + i] = S.px[i]; rec[5 * rs + i] = S.py[i]; rec[6 * rs + i] = S.pz[i];
+        }
+        ra[i] = S.alive[i];
+    }
+}
+void launch_record_particles(Ctx& c, int n) {
+    PlasmaState& P = *c.pl;
+    const size_t rs = size_t(P.rec_np);
+    double* rec = n >= 0 ? P.rec_x + 7 * rs * size_t(n) : nullptr;
+    k_rec_particles<<<ew_blocks(long(rs)), 256, 0, c.stream>>>(P.sdev.p, P.nstrm_dev.p, long(rs), rec, P.rec_a + size_t(n + 1) * rs);
+    c.check_launch("k_rec_particles");
+}
 long launch_join_cap(Ctx& c) {
     PlasmaState& P = *c.pl;
     if (P.njb == 0 || !P.any_ionizing) return 0;
