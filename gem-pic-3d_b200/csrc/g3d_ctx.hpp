@@ -394,6 +394,8 @@ void launch_adj_deposit(Ctx& c, const double* X, const int32_t* alive, const dou
 // one slice of the streaming-plasma march (k_adjoint.cu): the transposed real fields and current spectra
 void launch_adj_real_fields_slice(Ctx& c, const double* lF, long fpl, cpx* const* W, cpx* const* lsl);
 void launch_adj_stream_spectra(Ctx& c, cpx* const* ljsn, cpx* const* T, double* lJ, bool keep0, double a2);
+void launch_adj_rf_rows_slice(Ctx& c, const double* lF, long fpl, cpx* const* W);   // the rows half of each
+void launch_adj_ss_rows(Ctx& c, cpx* const* T, double* lJ);
 void launch_adj_push(Ctx& c, const float* Ff, const double* Fd, const double* X, const int32_t* alive, double s0, double s1,
                      double* lam, double* lF, int* err);
 void launch_adj_lmodes(Ctx& c, const cpx* lRx, const cpx* lRy, cpx* out);

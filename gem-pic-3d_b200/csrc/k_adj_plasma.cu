@@ -13,13 +13,17 @@
 // then R(n+1) -= q (jsn - si0) with si0 the prediction slice n+1 was solved with; dl = jsn - js0(n); js0(n) = jsn.
 // The reverse runs n = 0 .. N-2 and the passes P-1 .. 0, each line transposed (complex coefficients conjugated), and
 // ends with the front slice N-1. Kernels:
-//   k_adjp_correct  the correction, dl and js0 of half-cell n (one thread per mode)
-//   k_adjp_march    the transposed slice march of one pass with the replace and the prediction (one thread per mode)
-//   k_adjp_stream   the transposed push and deposit of every streaming particle in one pass (k_adj_stream.cuh)
-// and the transposed real fields and current spectra of one slice (k_adjoint.cu).
+//   k_adjp_pass_cols  one pass's column work: the columns of the transposed real fields of slice n, the transposed
+//                     correction (last pass), the transposed slice march with the replace and the prediction, the
+//                     columns of the transposed current spectra (one CTA per k_x column, one thread per mode)
+//   k_adjp_stream     the transposed push and deposit of every streaming particle in one pass (k_adj_stream.cuh)
+// and the rows of the transposed real fields and current spectra of one slice (k_adjoint.cu): four launches a pass,
+// as the forward's four.
 #include <cstring>
 #include "g3d_plasma.hpp"
 #include "k_adj_stream.cuh"
+#include "k_fft.cuh"
+#include "k_dispatch.cuh"
 
 namespace g3d {
 
@@ -32,139 +36,210 @@ __device__ __forceinline__ void tsc_slopes(double xi, double d[3]) {
 __device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     // conj(i k) z
 }  // namespace
 
-// ---------------------------------------------------------------- the correction of half-cell n
+// ---------------------------------------------------------------- the correction of half-cell n (one mode)
 // R(n+1) -= q (jsn - si0): dJ/djsn = -q dJ/dR(n+1), dJ/dsi0 = q dJ/dR(n+1) (to the last pass of half-cell n+1, which
 // made that prediction); dl(n-1) = jsn - js0(n): dJ/djsn += dJ/ddl, dJ/djs0_old(n) = -dJ/ddl; js0_new(n) = jsn and
-// jk(n) = b(n) + jsn as the next step's j0: dJ/djsn += dJ/djs0_new(n) + dJ/dj0_next(n) (x, y)
-__global__ void k_adjp_correct(AdjPlasmaPtrs a, int n, double q, int par, double* __restrict__ zero6, long nk) {
+// jk(n) = b(n) + jsn as the next step's j0: dJ/djsn += dJ/djs0_new(n) + dJ/dj0_next(n) (x, y). jA: dJ/djsn out.
+__device__ __forceinline__ void adj_correct_mode(const AdjPlasmaPtrs& a, int n, double q, int par, long i, cpx jA[3]) {
     const long nkh = a.nkh;
-    // the field adjoint of slice n+1 that this half-cell's pushes read: cleared for them
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < 6 * nk; i += long(gridDim.x) * blockDim.x) zero6[i] = 0;
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
-        const long pl = long(n + 1) * nkh + i;      // slice n+1 of the spectra, half-cell n of the current planes
-        const cpx lr[3] = {a.lS[0][pl], a.lS[1][pl], C(0)};
-        cpx* so = a.lsi0[par];
+    const long pl = long(n + 1) * nkh + i;          // slice n+1 of the spectra, half-cell n of the current planes
+    const cpx lr[3] = {a.lS[0][pl], a.lS[1][pl], C(0)};
+    cpx* so = a.lsi0[par];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const cpx d = a.ldl[k * nkh + i];
-            cpx u = -q * lr[k] + d + a.ljs0[k][pl];
-            if (k < 2) u = u + a.ljk[k][pl];
-            a.ljsnA[k * nkh + i] = u;
-            so[k * nkh + i] = q * lr[k];
-            a.ljs0[k][pl] = -d;
-            a.ldl[k * nkh + i] = C(0);
-        }
+    for (int k = 0; k < 3; ++k) {
+        const cpx d = a.ldl[k * nkh + i];
+        cpx u = -q * lr[k] + d + a.ljs0[k][pl];
+        if (k < 2) u = u + a.ljk[k][pl];
+        jA[k] = u;
+        so[k * nkh + i] = q * lr[k];
+        a.ljs0[k][pl] = -d;
+        a.ldl[k * nkh + i] = C(0);
     }
 }
 
-// ---------------------------------------------------------------- the transposed slice march of one pass
+// ---------------------------------------------------------------- the transposed slice march of one pass (one mode)
 // march_slice_mode (k_plasma.cu; march_point, src/sim_kernels.hpp:173-210) transposed line by line: the adjoints of
-// the slice's new values (the slice's real fields of this pass, plus for the last pass what later reads of the slice
-// left in lS) go to the old R, E_z, B_z of the slice (summed over the passes in lold; the first pass writes them
-// into lS, L's old value being unread), the new values of slice n+1 (lS, added), j0 and the beam part of jk (added),
-// the streaming current of the pass (ljsn) and, through the prediction of half-cell n-1, js0 and dl.
-// front: the front slice (L = E_z = B_z = 0), solved once with the prediction js0(N-2).
-// zero6 (not null): the field adjoint of slice n that this pass's pushes read (cleared: the transposed real fields of the
-// pass have taken it in)
-__global__ void k_adjp_march(Geo g, AdjPlasmaPtrs a, int n, double D, int last, int first, int multi, int extrap, double w,
-                             int par_prev, int front, double* __restrict__ zero6) {
+// the slice's new values (lsl: those of the slice's real fields of this pass, plus for the last pass what later reads of
+// the slice left in lS) go to the old R, E_z, B_z of the slice (summed over the passes in lold; the first pass writes
+// them into lS, L's old value being unread), the new values of slice n+1 (lS, added), j0 and the beam part of jk
+// (added), the streaming current of the pass (ls out, with jA of the correction for the last pass) and, through the
+// prediction of half-cell n-1, js0 and dl. front: the front slice (L = E_z = B_z = 0), solved once with the prediction
+// js0(N-2).
+__device__ __forceinline__ void adj_march_mode(const Geo& g, const AdjPlasmaPtrs& a, int n, double D, int last, int first, int multi,
+                                               int extrap, double w, int par_prev, int front, long i, const cpx lsl[6],
+                                               const cpx jA[3], cpx ls[3]) {
     const long nkh = a.nkh;
-    if (zero6)
-        for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < 6 * long(g.nk); i += long(gridDim.x) * blockDim.x) zero6[i] = 0;
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < nkh; i += long(gridDim.x) * blockDim.x) {
-        const int kxi = int(i % g.H), j = int(i / g.H);
-        const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
-        const long o = long(n - g.a) * nkh + i, od = o, ou = o + nkh;
-        cpx ln[6];
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
+    const long o = long(n - g.a) * nkh + i, od = o, ou = o + nkh;
+    cpx ln[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) ln[k] = a.lsl[k][i] + (last ? a.lS[k][o] : C(0));
-        cpx lRsx, lRsy, lup[3] = {C(0), C(0), C(0)};
-        if (front) {
-            lRsx = ln[0]; lRsy = ln[1];
-        } else {
-            const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
-            // L_x = Ls_x - h/4 (a E - b B), L_y = Ls_y - h/4 (a B + b E)
-            cpx lLsx = ln[4], lLsy = ln[5];
-            cpx lEn = ln[2] - 0.25 * h * ikc(kx, ln[4]) - 0.25 * h * ikc(ky, ln[5]);
-            cpx lBn = ln[3] + 0.25 * h * ikc(ky, ln[4]) - 0.25 * h * ikc(kx, ln[5]);
-            // R_x = Rs_x + D (a E + b B), R_y = Rs_y + D (b E - a B)
-            lRsx = ln[0]; lRsy = ln[1];
-            lEn = lEn + D * ikc(kx, ln[0]) + D * ikc(ky, ln[1]);
-            lBn = lBn + D * ikc(ky, ln[0]) - D * ikc(kx, ln[1]);
-            // E = (pE - h/2 Qp - h/4 SE - h up_z) / den, B = (pB - h/2 Cp - h/4 SB) / den
-            const cpx le = lEn / den, lb = lBn / den;
-            cpx lpE = le, lpB = lb;
-            const cpx lQp = -0.5 * h * le, lSE = -0.25 * h * le, lCp = -0.5 * h * lb, lSB = -0.25 * h * lb;
-            lup[2] = -h * le;
-            // SE = -a Rs_x + a Ls_x + b Ls_y - b Rs_y; SB = a Rs_y + a Ls_y - b Rs_x - b Ls_x
-            lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
-            lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
-            lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
-            lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
-            // Qp = -1/2 a (pR_x - pL_x) + 1/2 b (pL_y - pR_y); Cp = 1/2 (a (pR_y + pL_y) - b (pR_x + pL_x))
-            cpx lpRx = -0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
-            cpx lpLx = 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
-            cpx lpRy = -0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
-            cpx lpLy = 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
-            // Ls_x = pL_x - h/4 (a pE - b pB) - h/2 up_x; Ls_y = pL_y - h/4 (a pB + b pE) - h/2 up_y
-            lpLx = lpLx + lLsx;
-            lpLy = lpLy + lLsy;
-            lpE = lpE - 0.25 * h * ikc(kx, lLsx) - 0.25 * h * ikc(ky, lLsy);
-            lpB = lpB + 0.25 * h * ikc(ky, lLsx) - 0.25 * h * ikc(kx, lLsy);
-            lup[0] = -0.5 * h * lLsx;
-            lup[1] = -0.5 * h * lLsy;
-            const long pp = o + nkh;                // slice n+1 as this march read it
-            a.lS[0][pp] = a.lS[0][pp] + lpRx; a.lS[1][pp] = a.lS[1][pp] + lpRy;
-            a.lS[2][pp] = a.lS[2][pp] + lpE; a.lS[3][pp] = a.lS[3][pp] + lpB;
-            a.lS[4][pp] = a.lS[4][pp] + lpLx; a.lS[5][pp] = a.lS[5][pp] + lpLy;
-        }
-        // Rs_x = R_x + D (a E + b B) - D J_x, Rs_y = R_y + D (b E - a B) - D J_y (the old level of slice n)
-        const cpx lo[4] = {lRsx, lRsy, D * ikc(kx, lRsx) + D * ikc(ky, lRsy), D * ikc(ky, lRsx) - D * ikc(kx, lRsy)};
-        const cpx lJx = -D * lRsx, lJy = -D * lRsy;
-        // J = wl (j0 + jk)(n-1) + wu (j0 + jk)(n)
-        a.lj0[0][od] = a.lj0[0][od] + wl * lJx; a.lj0[0][ou] = a.lj0[0][ou] + wu * lJx;
-        a.lj0[1][od] = a.lj0[1][od] + wl * lJy; a.lj0[1][ou] = a.lj0[1][ou] + wu * lJy;
-        const cpx lkd[3] = {wl * lJx, wl * lJy, C(0)};
-        const cpx lku[3] = {wu * lJx + lup[0], wu * lJy + lup[1], lup[2]};
+    for (int k = 0; k < 6; ++k) ln[k] = lsl[k] + (last ? a.lS[k][o] : C(0));
+    cpx lRsx, lRsy, lup[3] = {C(0), C(0), C(0)};
+    if (front) {
+        lRsx = ln[0]; lRsy = ln[1];
+    } else {
+        const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+        // L_x = Ls_x - h/4 (a E - b B), L_y = Ls_y - h/4 (a B + b E)
+        cpx lLsx = ln[4], lLsy = ln[5];
+        cpx lEn = ln[2] - 0.25 * h * ikc(kx, ln[4]) - 0.25 * h * ikc(ky, ln[5]);
+        cpx lBn = ln[3] + 0.25 * h * ikc(ky, ln[4]) - 0.25 * h * ikc(kx, ln[5]);
+        // R_x = Rs_x + D (a E + b B), R_y = Rs_y + D (b E - a B)
+        lRsx = ln[0]; lRsy = ln[1];
+        lEn = lEn + D * ikc(kx, ln[0]) + D * ikc(ky, ln[1]);
+        lBn = lBn + D * ikc(ky, ln[0]) - D * ikc(kx, ln[1]);
+        // E = (pE - h/2 Qp - h/4 SE - h up_z) / den, B = (pB - h/2 Cp - h/4 SB) / den
+        const cpx le = lEn / den, lb = lBn / den;
+        cpx lpE = le, lpB = lb;
+        const cpx lQp = -0.5 * h * le, lSE = -0.25 * h * le, lCp = -0.5 * h * lb, lSB = -0.25 * h * lb;
+        lup[2] = -h * le;
+        // SE = -a Rs_x + a Ls_x + b Ls_y - b Rs_y; SB = a Rs_y + a Ls_y - b Rs_x - b Ls_x
+        lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
+        lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
+        lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
+        lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
+        // Qp = -1/2 a (pR_x - pL_x) + 1/2 b (pL_y - pR_y); Cp = 1/2 (a (pR_y + pL_y) - b (pR_x + pL_x))
+        cpx lpRx = -0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+        cpx lpLx = 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+        cpx lpRy = -0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+        cpx lpLy = 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+        // Ls_x = pL_x - h/4 (a pE - b pB) - h/2 up_x; Ls_y = pL_y - h/4 (a pB + b pE) - h/2 up_y
+        lpLx = lpLx + lLsx;
+        lpLy = lpLy + lLsy;
+        lpE = lpE - 0.25 * h * ikc(kx, lLsx) - 0.25 * h * ikc(ky, lLsy);
+        lpB = lpB + 0.25 * h * ikc(ky, lLsx) - 0.25 * h * ikc(kx, lLsy);
+        lup[0] = -0.5 * h * lLsx;
+        lup[1] = -0.5 * h * lLsy;
+        const long pp = o + nkh;                    // slice n+1 as this march read it
+        a.lS[0][pp] = a.lS[0][pp] + lpRx; a.lS[1][pp] = a.lS[1][pp] + lpRy;
+        a.lS[2][pp] = a.lS[2][pp] + lpE; a.lS[3][pp] = a.lS[3][pp] + lpB;
+        a.lS[4][pp] = a.lS[4][pp] + lpLx; a.lS[5][pp] = a.lS[5][pp] + lpLy;
+    }
+    // Rs_x = R_x + D (a E + b B) - D J_x, Rs_y = R_y + D (b E - a B) - D J_y (the old level of slice n)
+    const cpx lo[4] = {lRsx, lRsy, D * ikc(kx, lRsx) + D * ikc(ky, lRsy), D * ikc(ky, lRsx) - D * ikc(kx, lRsy)};
+    const cpx lJx = -D * lRsx, lJy = -D * lRsy;
+    // J = wl (j0 + jk)(n-1) + wu (j0 + jk)(n)
+    a.lj0[0][od] = a.lj0[0][od] + wl * lJx; a.lj0[0][ou] = a.lj0[0][ou] + wu * lJx;
+    a.lj0[1][od] = a.lj0[1][od] + wl * lJy; a.lj0[1][ou] = a.lj0[1][ou] + wu * lJy;
+    const cpx lkd[3] = {wl * lJx, wl * lJy, C(0)};
+    const cpx lku[3] = {wu * lJx + lup[0], wu * lJy + lup[1], lup[2]};
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { a.ljk[k][od] = a.ljk[k][od] + lkd[k]; a.ljk[k][ou] = a.ljk[k][ou] + lku[k]; }
-        const cpx* si = a.lsi0[par_prev];
-        if (front) {
-            // jk(N-2) = b + js0(N-2), the prediction slice N-1 is solved with (and corrected for: si0(N-2))
+    for (int k = 0; k < 3; ++k) { a.ljk[k][od] = a.ljk[k][od] + lkd[k]; a.ljk[k][ou] = a.ljk[k][ou] + lku[k]; }
+    const cpx* si = a.lsi0[par_prev];
+    if (front) {
+        // jk(N-2) = b + js0(N-2), the prediction slice N-1 is solved with (and corrected for: si0(N-2))
 #pragma unroll
-            for (int k = 0; k < 3; ++k) a.ljs0[k][od] = a.ljs0[k][od] + lkd[k] + si[k * nkh + i];
-        } else {
-            cpx ls[3];
+        for (int k = 0; k < 3; ++k) { a.ljs0[k][od] = a.ljs0[k][od] + lkd[k] + si[k * nkh + i]; ls[k] = C(0); }
+    } else {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) ls[k] = (last ? a.ljsnA[k * nkh + i] : C(0)) + lku[k];
-            if (n >= 1) {
+        for (int k = 0; k < 3; ++k) ls[k] = (last ? jA[k] : C(0)) + lku[k];
+        if (n >= 1) {
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const cpx lp = lkd[k] + (last ? si[k * nkh + i] : C(0));      // dJ/dpred of half-cell n-1
-                    a.ljs0[k][od] = a.ljs0[k][od] + lp;
-                    if (extrap) {
-                        ls[k] = ls[k] + (1 + w) * lp;
-                        a.ljs0[k][ou] = a.ljs0[k][ou] - (1 + w) * lp;
-                        a.ldl[k * nkh + i] = a.ldl[k * nkh + i] - w * lp;
-                    }
+            for (int k = 0; k < 3; ++k) {
+                const cpx lp = lkd[k] + (last ? si[k * nkh + i] : C(0));      // dJ/dpred of half-cell n-1
+                a.ljs0[k][od] = a.ljs0[k][od] + lp;
+                if (extrap) {
+                    ls[k] = ls[k] + (1 + w) * lp;
+                    a.ljs0[k][ou] = a.ljs0[k][ou] - (1 + w) * lp;
+                    a.ldl[k * nkh + i] = a.ldl[k * nkh + i] - w * lp;
                 }
             }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) a.ljsn[k * nkh + i] = ls[k];
-        }
-        // the old R_x, R_y, E_z, B_z of slice n: summed over the passes, written by the first
-        if (first) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a.lS[k][o] = (multi ? a.lold[k * nkh + i] : C(0)) + lo[k];
-            a.lS[4][o] = C(0); a.lS[5][o] = C(0);
-        } else if (last) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = lo[k];
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = a.lold[k * nkh + i] + lo[k];
         }
     }
+    // the old R_x, R_y, E_z, B_z of slice n: summed over the passes, written by the first
+    if (first) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.lS[k][o] = (multi ? a.lold[k * nkh + i] : C(0)) + lo[k];
+        a.lS[4][o] = C(0); a.lS[5][o] = C(0);
+    } else if (last) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = lo[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = a.lold[k * nkh + i] + lo[k];
+    }
+}
+// the front slice's march alone (its slice adjoints in a.lsl)
+__global__ void k_adjp_march_front(Geo g, AdjPlasmaPtrs a, int n, double D, int par_prev) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < a.nkh; i += long(gridDim.x) * blockDim.x) {
+        cpx lsl[6], jA[3] = {C(0), C(0), C(0)}, ls[3];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) lsl[k] = a.lsl[k][i];
+        adj_march_mode(g, a, n, D, 1, 1, 0, 0, 0.0, par_prev, 1, i, lsl, jA, ls);
+    }
+}
+
+// ---------------------------------------------------------------- one pass's column work, fused
+// k_adjp_pass_cols: the transpose of k_pass_cols (k_plasma.cu) and of the correction, one CTA per k_x column and one
+// thread per k_y. (1) The y transforms of the six half-row adjoints of slice n's real fields (the column half of the
+// transposed real fields, k_adj_rf_cols) give the adjoints of the slice's values of this pass. (2) The last pass: the
+// transposed correction of half-cell n (adj_correct_mode). (3) The transposed march of the mode (adj_march_mode) gives
+// the adjoint of the pass's streaming current. (4) Its filters and inverse y transforms (the column half of the
+// transposed current spectra, k_adj_cur_cols) into T, which the rows kernel turns into the current's real adjoint.
+// zero_a, zero_b (nullable, nzero values each): field adjoints cleared for the pushes of this pass.
+template <int NY>
+__global__ void __launch_bounds__(NY) k_adjp_pass_cols(Geo g, AdjPlasmaPtrs a, const cpx* __restrict__ W0, const cpx* __restrict__ W1,
+                                                       const cpx* __restrict__ W2, const cpx* __restrict__ W3,
+                                                       const cpx* __restrict__ W4, const cpx* __restrict__ W5, cpx* __restrict__ T0,
+                                                       cpx* __restrict__ T1, cpx* __restrict__ T2, int n, double D, double q, int last,
+                                                       int first, int multi, int extrap, double w, int par, int par_prev,
+                                                       double* __restrict__ zero_a, double* __restrict__ zero_b, long nzero, int keep0,
+                                                       double a2) {
+    using S = FftShape<NY>;
+    using Tile = ColTile<NY, 1>;
+    extern __shared__ double smp[];
+    cpx* tl[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) tl[k] = reinterpret_cast<cpx*>(smp) + k * Tile::size;
+    const int kxi = blockIdx.x, j = threadIdx.x;
+    const long i = long(j) * g.H + kxi;
+    for (long e = long(blockIdx.x) * NY + j; e < nzero; e += long(gridDim.x) * NY) {
+        if (zero_a) zero_a[e] = 0;
+        if (zero_b) zero_b[e] = 0;
+    }
+    const int grp = j / S::T < 2 ? j / S::T : 2, tt = j - (j / S::T) * S::T;
+    const bool act = j < 3 * S::T;
+    // (1) the half-row adjoints of the column, transformed along y in pairs (R, L, E_z + i B_z as k_adj_rf_cols)
+    const cpx* Win[6] = {W0, W1, W2, W3, W4, W5};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) tl[k][Tile::at(j, 0)] = Win[k][i];
+    __syncthreads();
+    {
+        cpx* const ls_[2] = {tl[2 * grp], tl[2 * grp + 1]};
+        fft_lines_some<NY, 2>(ls_, RowAddr{0}, tt, g.twy, act);
+    }
+    __syncthreads();
+    const cpx lsl[6] = {tl[0][Tile::at(j, 0)], tl[1][Tile::at(j, 0)], tl[4][Tile::at(j, 0)], tl[5][Tile::at(j, 0)],
+                        tl[2][Tile::at(j, 0)], tl[3][Tile::at(j, 0)]};              // {R_x, R_y, E_z, B_z, L_x, L_y}
+    // (2), (3)
+    cpx jA[3] = {C(0), C(0), C(0)}, ls[3];
+    if (last) adj_correct_mode(a, n, q, par, i, jA);
+    adj_march_mode(g, a, n, D, last, first, multi, extrap, w, par_prev, 0, i, lsl, jA, ls);
+    // (4) the filters and the inverse transforms along y (conjugate, forward, conjugate)
+    const double k2f = g.kxs[kxi] * g.kxs[kxi] + g.kys[j] * g.kys[j];
+    const double f = (kxi == 0 && j == 0 && !keep0) ? 0.0 : g.filt[kxi] * g.filty[j] / (1 + a2 * k2f);
+    __syncthreads();                                  // every thread has read its slice adjoints from the tiles
+#pragma unroll
+    for (int k = 0; k < 3; ++k) tl[k][Tile::at(j, 0)] = conj(f * ls[k]);
+    __syncthreads();
+    {
+        cpx* const ls_[1] = {tl[grp]};
+        fft_lines_some<NY, 1>(ls_, RowAddr{0}, tt, g.twy, act);
+    }
+    __syncthreads();
+    T0[i] = conj(tl[0][Tile::at(j, 0)]);
+    T1[i] = conj(tl[1][Tile::at(j, 0)]);
+    T2[i] = conj(tl[2][Tile::at(j, 0)]);
+}
+template <int NY>
+static void adjp_pass_cols(Ctx& c, const AdjPlasmaPtrs& a, const AdjPlasmaWs& w, int n, double D, double q, int last, int first,
+                           int multi, int extrap, double wex, double* zero_a, double* zero_b, bool keep0, double a2) {
+    using Tile = ColTile<NY, 1>;
+    const size_t smem = 6 * Tile::size * sizeof(cpx);
+    smem_attr(reinterpret_cast<const void*>(k_adjp_pass_cols<NY>), smem);
+    k_adjp_pass_cols<NY><<<unsigned(c.H), NY, smem, c.stream>>>(c.geo(), a, w.Wsc[0], w.Wsc[1], w.Wsc[2], w.Wsc[3], w.Wsc[4], w.Wsc[5],
+                                                               w.Tsc[0], w.Tsc[1], w.Tsc[2], n, D, q, last, first, multi, extrap, wex,
+                                                               n & 1, (n - 1) & 1, zero_a, zero_b, 6 * long(c.nk), keep0 ? 1 : 0, a2);
 }
 
 // ---------------------------------------------------------------- the transposed streaming push of one pass
@@ -334,19 +409,23 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
         int cur = 0;
         const unsigned mb = mode_blocks(nkh), pb = unsigned((rs + 127) / 128);
         for (int n = c.a; n <= N - 2; ++n) {
-            k_adjp_correct<<<mb, 128, 0, st>>>(a, n, D * c.wlo_h[size_t(n + 1)], n & 1, w.lFup[cur ^ 1], nk);
-            c.check_launch("k_adjp_correct");
+            int tok = 0;
             // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
             const double wex = (n >= 1 && n + 1 <= N - 2)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
             const double* Fnext = w.rec_f + 6 * nk * (size_t(passes) * size_t(n + 1) + size_t(passes - 1));
+            const double q = D * c.wlo_h[size_t(n + 1)];
             for (int p = passes - 1; p >= 0; --p) {
-                launch_adj_real_fields_slice(c, p == passes - 1 ? w.lFup[cur] : w.lFcur, nk, w.Wsc, a.lsl);
-                k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, n, D, p == passes - 1 ? 1 : 0, p == 0 ? 1 : 0, passes > 1 ? 1 : 0,
-                                                  extrap ? 1 : 0, wex, (n - 1) & 1, 0, p >= 1 ? w.lFcur : nullptr);
-                c.check_launch("k_adjp_march");
-                cpx* js3[3] = {a.ljsn, a.ljsn + nkh, a.ljsn + 2 * nkh};
-                launch_adj_stream_spectra(c, js3, w.Tsc, w.ljsr, keep0, a2);
+                // the rows of the transposed real fields of slice n, the fused column work, the rows of the transposed
+                // current spectra, the transposed pushes
+                launch_adj_rf_rows_slice(c, p == passes - 1 ? w.lFup[cur] : w.lFcur, nk, w.Wsc);
+                tok = c.prof_begin("adj_plasma_pass_cols");
+                G3D_DISPATCH_N(c.ny, NY, adjp_pass_cols<NY>(c, a, w, n, D, q, p == passes - 1 ? 1 : 0, p == 0 ? 1 : 0,
+                                                          passes > 1 ? 1 : 0, extrap ? 1 : 0, wex, p >= 1 ? w.lFcur : nullptr,
+                                                          p == passes - 1 ? w.lFup[cur ^ 1] : nullptr, keep0, a2));
+                c.check_launch("k_adjp_pass_cols");
+                c.prof_end(tok);
+                launch_adj_ss_rows(c, w.Tsc, w.ljsr);
                 if (!rs) continue;
                 const double* Fa = p == 0 ? nullptr : w.rec_f + 6 * nk * (size_t(passes) * size_t(n) + size_t(p - 1));
                 const long sa = p == 0 ? fpl : nk, off = long(n - c.a) * nk;
@@ -355,6 +434,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
                 const double* rec = w.rec_x + 7 * size_t(rs) * size_t(n);
                 const int32_t* ae = w.rec_a + size_t(rs) * size_t(n + 1);
                 const int32_t* ax = w.rec_a + size_t(rs) * size_t(n);
+                tok = c.prof_begin("adj_plasma_stream");
                 if (p == passes - 1)
                     k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), P.sdev.p, P.ion_dev.p, w.stepd, rs, rec, ae, ax, n, Delta,
                                                             p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
@@ -364,13 +444,14 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
                                                              p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
                                                              w.ljsr, w.lam);
                 c.check_launch("k_adjp_stream");
+                c.prof_end(tok);
             }
             cur ^= 1;
         }
         // the front slice N-1: its real fields (read by half-cell N-2), then its march with the prediction js0(N-2)
         launch_adj_real_fields_slice(c, w.lFup[cur], nk, w.Wsc, a.lsl);
-        k_adjp_march<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, 1, 1, 0, 0, 0.0, (N - 2) & 1, 1, nullptr);
-        c.check_launch("k_adjp_march");
+        k_adjp_march_front<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, (N - 2) & 1);
+        c.check_launch("k_adjp_march_front");
     };
     // what the graph holds by value: the arrays, the grid and the step length
     uint64_t key = 1469598103934665603ULL;

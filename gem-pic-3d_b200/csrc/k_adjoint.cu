@@ -988,6 +988,16 @@ static void adj_ss_rows(Ctx& c, cpx* const* T, double* lJ) {
     k_adj_cur_rows<NX><<<dim3(unsigned((c.ny + LPC - 1) / LPC), 1u), ANT, smem, c.stream>>>(c.geo(), T[0], T[1], T[2], lJ, long(c.nk));
     c.check_launch("k_adj_cur_rows");
 }
+void launch_adj_rf_rows_slice(Ctx& c, const double* lF, long fpl, cpx* const* W) {
+    const int tok = c.prof_begin("adj_rf_rows_slice");
+    G3D_DISPATCH_N(c.nx, NX, adj_rf_rows_slice<NX>(c, lF, fpl, W));
+    c.prof_end(tok);
+}
+void launch_adj_ss_rows(Ctx& c, cpx* const* T, double* lJ) {
+    const int tok = c.prof_begin("adj_ss_rows");
+    G3D_DISPATCH_N(c.nx, NX, adj_ss_rows<NX>(c, T, lJ));
+    c.prof_end(tok);
+}
 void launch_adj_stream_spectra(Ctx& c, cpx* const* ljsn, cpx* const* T, double* lJ, bool keep0, double a2) {
     const int tok = c.prof_begin("adj_stream_spectra");
     G3D_DISPATCH_N(c.ny, NY, adj_ss_cols<NY>(c, ljsn, T, keep0, a2));
