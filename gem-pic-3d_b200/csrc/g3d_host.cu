@@ -1278,6 +1278,69 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     };
     long tr0 = 0, rs0 = 0, npl_max = 0;
     if (plasma) get_plasma_counters(c, tr0, rs0);
+    // The record of the marches (k_adj_plasma.cu): kept from the forward for every step when it fits in half of the free
+    // device memory (stride rs: twice the fresh plasma's most particles, room for the joining ones), else, or when a
+    // march outgrows rs, or with G3D_ADJ_RECOMPUTE set, each step is run again from its level in the reverse sweep with
+    // one march's record (the checkpoints of the levels are the only memory that grows with K).
+    struct RecInfo { RecDev rec; long np, fresh; };
+    std::vector<RecInfo> recinfo(plasma ? size_t(K + 1) : 0);
+    bool stored = false, overflow = false;
+    size_t step_bytes = 0, common = 0;
+    long rs_rec = 0;
+    int k_cur = 0;
+    auto rup = [](size_t b) { return (b + 255) / 256 * 256; };
+    auto rec_bytes = [&](long rs) {
+        const size_t passes = size_t(c.pl->cfg.iterations);
+        return rup((ns + 1) * 7 * size_t(rs) * 8) + rup(ns * passes * 6 * nk * 8) + rup((ns + 1) * size_t(rs) * 4) + rup(2 * size_t(rs) * 8);
+    };
+    auto carve_rec = [&](unsigned char* base, long rs) {
+        const size_t passes = size_t(c.pl->cfg.iterations);
+        RecDev r{};
+        size_t o = 0;
+        r.x = reinterpret_cast<double*>(base + o); o += rup((ns + 1) * 7 * size_t(rs) * 8);
+        r.f = reinterpret_cast<double*>(base + o); o += rup(ns * passes * 6 * nk * 8);
+        r.a = reinterpret_cast<int32_t*>(base + o); o += rup((ns + 1) * size_t(rs) * 4);
+        r.q = reinterpret_cast<double*>(base + o);
+        r.rs = rs;
+        return r;
+    };
+    // lam, jl (7 rs each) and the step's values after the records
+    auto carve_common = [&](unsigned char* base, long rs) {
+        aw.lam = reinterpret_cast<double*>(base);
+        aw.jl = reinterpret_cast<double*>(base + rup(7 * size_t(rs) * 8));
+        aw.stepd = reinterpret_cast<AdjStepDev*>(base + 2 * rup(7 * size_t(rs) * 8));
+    };
+    struct RecOff {
+        PlasmaState* P;
+        ~RecOff() { if (P) { P->rec_on = false; P->rec_step = nullptr; } }
+    } rec_off{plasma ? c.pl.get() : nullptr};
+    if (plasma) {
+        PlasmaState& Pl = *c.pl;
+        if (!Pl.recd.p) Pl.recd.alloc(1, st);
+        long m = Pl.cfg.free_electrons ? 1 : 0;
+        for (const auto& is : Pl.ions) m += is.loaded() ? 1 : 0;
+        const long fresh_bound = long(c.yf ? c.ny : c.ny - 2) * c.nx * Pl.cfg.ppc_x * Pl.cfg.ppc_y * m;
+        rs_rec = 2 * fresh_bound + 1024;
+        step_bytes = rec_bytes(rs_rec);
+        common = 2 * rup(7 * size_t(rs_rec) * 8) + rup(sizeof(AdjStepDev));
+        size_t fr = 0, tot = 0;
+        G3D_CUDA(cudaMemGetInfo(&fr, &tot));
+        const size_t have = c.adjrec.n >= size_t(K) * step_bytes + common ? c.adjrec.n : 0;
+        stored = !std::getenv("G3D_ADJ_RECOMPUTE") && (have || size_t(K) * step_bytes + common <= fr / 2);
+        if (stored) {
+            if (c.adjrec.n < size_t(K) * step_bytes + common) c.adjrec.alloc(size_t(K) * step_bytes + common, st);
+            carve_common(c.adjrec.p + size_t(K) * step_bytes, rs_rec);
+            Pl.rec_on = true;
+            Pl.rec_step = [&](long nstrm, long fresh) {
+                if (nstrm > rs_rec || k_cur < 1 || k_cur > K) { overflow = true; return false; }
+                RecInfo& ri = recinfo[size_t(k_cur)];
+                ri.rec = carve_rec(c.adjrec.p + size_t(k_cur - 1) * step_bytes, rs_rec);
+                ri.np = nstrm; ri.fresh = fresh;
+                G3D_CUDA(cudaMemcpyAsync(c.pl->recd.p, &ri.rec, sizeof(RecDev), cudaMemcpyHostToDevice, c.stream));
+                return true;
+            };
+        }
+    }
     // the real fields of level k are written by step k straight into checkpoint k (the push of step k + 1 reads
     // them there; with a plasma they are copied there after the step); the context's own F / Fd come back, with the
     // last level's fields, when the forward is done
@@ -1292,6 +1355,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         // with a plasma the march writes the real fields slice by slice into the context's F during the step, so
         // the step keeps its own F and the level is copied after it (the level before must stay as it was)
         if (plasma) {
+            k_cur = k;
             step(c, false);
             G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
             npl_max = std::max(npl_max, c.pl->nstrm);
@@ -1308,20 +1372,22 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         if (tr != tr0 || rs != rs0)
             throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate particles that join the beam (fast trapped or "
                                        "restreamed ones), and the forward had some");
-        // the record of one march: the particles entering every half-cell (state and alive), the exact fields of every
-        // slice and pass; the adjoints of the streaming particles and of the joining ones carried between steps
-        const size_t passes = size_t(c.pl->cfg.iterations), m = size_t(npl_max);
-        const size_t sz[6] = {ns * 7 * m * 8, ns * passes * 6 * nk * 8, (ns + 1) * m * 4, 7 * m * 8, 7 * m * 8, sizeof(AdjStepDev)};
-        size_t off[6], tot = 0;
-        for (int q = 0; q < 6; ++q) { off[q] = tot; tot += (sz[q] + 255) / 256 * 256; }
-        if (c.adjrec.n < tot) c.adjrec.alloc(tot, st);
-        aw.np = npl_max; aw.rs = npl_max;
-        aw.rec_x = reinterpret_cast<double*>(c.adjrec.p + off[0]);
-        aw.rec_f = reinterpret_cast<double*>(c.adjrec.p + off[1]);
-        aw.rec_a = reinterpret_cast<int32_t*>(c.adjrec.p + off[2]);
-        aw.lam = reinterpret_cast<double*>(c.adjrec.p + off[3]);
-        aw.jl = reinterpret_cast<double*>(c.adjrec.p + off[4]);
-        aw.stepd = reinterpret_cast<AdjStepDev*>(c.adjrec.p + off[5]);
+        c.pl->rec_on = false;
+        if (!stored || overflow) {                    // one march's record, filled by running each step again
+            stored = false;
+            const long rs = npl_max;
+            const size_t need = rec_bytes(rs) + 2 * rup(7 * size_t(rs) * 8) + rup(sizeof(AdjStepDev));
+            if (c.adjrec.n < need) c.adjrec.alloc(need, st);
+            const RecDev one = carve_rec(c.adjrec.p, rs);
+            carve_common(c.adjrec.p + rec_bytes(rs), rs);
+            c.pl->rec_step = [&, one](long nstrm, long fresh) {
+                if (nstrm > one.rs) return false;
+                RecInfo& ri = recinfo[size_t(k_cur)];
+                ri.rec = one; ri.np = nstrm; ri.fresh = fresh;
+                G3D_CUDA(cudaMemcpyAsync(c.pl->recd.p, &ri.rec, sizeof(RecDev), cudaMemcpyHostToDevice, c.stream));
+                return true;
+            };
+        }
     }
     if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
     else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
@@ -1342,31 +1408,36 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         if (k < K) launch_adj_real_fields(c, lF, W, lS);
         for (int q = 0; q < 2; ++q) G3D_CUDA(cudaMemsetAsync(lj0[q], 0, (ns + 1) * nkh * sizeof(cpx), st));
         if (plasma) {
-            // step k again from level k-1 with its march recorded, then the march transposed; the level k-1 fields'
-            // adjoint takes the reads of the streaming pushes, then those of the beam push
-            restore(k - 1);
             PlasmaState& Pl = *c.pl;
-            Pl.rec_x = aw.rec_x; Pl.rec_f = aw.rec_f; Pl.rec_a = aw.rec_a; Pl.rec_np = aw.rs;
-            struct Unrec { PlasmaState& P; ~Unrec() { P.rec_x = nullptr; P.rec_f = nullptr; P.rec_a = nullptr; P.rec_np = 0; } } unrec{Pl};
-            const long tr1 = Pl.trapped_total;
-            step(c, false);
-            if (Pl.nstrm > aw.rs || Pl.trapped_total != tr1)
-                throw Error(G3D_ERR_STATE, "the adjoint march: a step run again from its level did not repeat its plasma");
+            if (!stored) {
+                // step k again from level k-1 with its march recorded
+                restore(k - 1);
+                k_cur = k;
+                const long tr1 = Pl.trapped_total;
+                Pl.rec_on = true;
+                step(c, false);
+                Pl.rec_on = false;
+                if (Pl.nstrm > npl_max || Pl.trapped_total != tr1)
+                    throw Error(G3D_ERR_STATE, "the adjoint march: a step run again from its level did not repeat its plasma");
+            }
+            const RecInfo& ri = recinfo[size_t(k)];
             // the streaming particles' adjoints after the march: the slow trapped ones are the next march's joining ones
-            G3D_CUDA(cudaMemsetAsync(aw.lam, 0, 7 * size_t(aw.rs) * 8, st));
+            G3D_CUDA(cudaMemsetAsync(aw.lam, 0, 7 * size_t(ri.rec.rs) * 8, st));
             const long njl = k < K ? long(joins[size_t(k)].size()) : 0;
-            const long nslow = launch_join_adjoint_in(c, aw.jl, njl, aw.lam, aw.rs);
+            const long nslow = launch_join_adjoint_in(c, ri.rec, ri.np, aw.jl, njl, aw.lam);
             if (k < K && nslow != njl)
-                throw Error(G3D_ERR_STATE, "the adjoint march: the trapped particles of a step run again differ from its forward");
+                throw Error(G3D_ERR_STATE, "the adjoint march: the trapped particles of a step differ from those joining the next");
+            // the march transposed; the level k-1 fields' adjoint takes the reads of the streaming pushes, then those of
+            // the beam push
             G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
             G3D_CUDA(cudaMemsetAsync(ljk[2], 0, (ns + 1) * nkh * sizeof(cpx), st));
             for (int q = 0; q < 2; ++q) ap.lj0[q] = lj0[q];
             for (int q = 0; q < 3; ++q) ap.ljk[q] = ljk[q];
             AdjPlasmaWs awk = aw;
-            awk.np = Pl.nstrm;
+            awk.np = ri.np; awk.fresh = ri.fresh; awk.rec = ri.rec;
             adjoint_march_plasma(c, awk, ap, FD + size_t(k - 1) * Fn, lF, sl[size_t(k - 1)], sl[size_t(k)]);
             // the joining particles of this march (after its fresh plasma) pass their adjoints to the march before
-            launch_join_adjoint_out(c, aw.lam, aw.rs, Pl.fresh_last, long(joins[size_t(k - 1)].size()), aw.jl);
+            launch_join_adjoint_out(c, aw.lam, ri.rec.rs, ri.fresh, long(joins[size_t(k - 1)].size()), aw.jl);
             launch_adj_currents(c, ljk, W, V, lJ, Pl.box_mean);
         } else {
             launch_adj_march(c, lS, lj0, ljk, 0.5 * c.P.dz);

@@ -379,16 +379,6 @@ static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true) 
     else launch_real_fields_slice(c, l, fm, cols);
 }
 
-// The adjoint's record of a march (PlasmaState::rec_x, rec_f): the exact fields of slice l after pass p, the particles
-// entering half-cell n
-static void record_fields(Ctx& c, int l, int p) {
-    PlasmaState& P = *c.pl;
-    const size_t nk = size_t(c.nk), fpl = size_t(c.ns + 2) * nk;
-    double* dst = P.rec_f + 6 * nk * (size_t(P.cfg.iterations) * size_t(l) + size_t(p));
-    G3D_CUDA(cudaMemcpy2DAsync(dst, nk * 8, c.Fd.p + size_t(l - c.a) * nk, fpl * 8, nk * 8, 6, cudaMemcpyDeviceToDevice, c.stream));
-}
-static void record_particles(Ctx& c, int n) { launch_record_particles(c, n); }
-
 void march_plasma(Ctx& c, double s0, double s1) {
     PlasmaState& P = *c.pl;
     const double Delta = s1 - s0, D = 0.5 * Delta;
@@ -414,7 +404,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto mixk = [&](uint64_t v) { key = (key ^ v) * 1099511628211ULL; };
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
-    mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(ptr(P.rec_x)); mixk(ptr(P.rec_f)); mixk(ptr(P.rec_a)); mixk(uint64_t(P.rec_np)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
+    const bool rec = P.rec_on && P.rec_step && P.rec_step(P.nstrm, P.fresh_last);   // the adjoint's record of this march
+    mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(uint64_t(rec)); mixk(ptr(P.recd.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
     mixk(ptr(pp.jkx)); mixk(ptr(pp.jky)); mixk(ptr(c.mixed ? static_cast<const void*>(c.mx.j0x.p) : c.j0x.p));
@@ -433,7 +424,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
         real_fields_slice(c, N - 1, N - 2);
-        if (P.rec_f) record_fields(c, N - 1, passes - 1);
+        if (rec) launch_record_fields(c, N - 1, passes - 1);
 
         StreamArgs sa;
         sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
@@ -451,7 +442,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             if (n == nhi) launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
             const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
-            if (P.rec_x) record_particles(c, n);
+            if (rec) launch_record_particles(c, n);
             for (int pass = 0; pass < passes; ++pass) {
                 if (fh) launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
@@ -465,7 +456,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
                     launch_stream_spectra_rows(c);
                     launch_pass_cols(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
                     real_fields_slice(c, n, pass + 1 < passes ? n : n - 1, false);
-                    if (P.rec_f) record_fields(c, n, pass);
+                    if (rec) launch_record_fields(c, n, pass);
                 } else {
                     launch_stream_spectra(c);
                     launch_replace_pred(c, n, extrap ? 1 : 0, wex);
@@ -479,7 +470,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             else launch_correct(c, n, q, n + 1 < c.b ? 1 : 0);
             have_dl = true;
         }
-        if (P.rec_x) record_particles(c, -1);            // the states after the last half-cell
+        if (rec) launch_record_particles(c, -1);         // the states after the last half-cell
     };
     PlasmaState::LoopGraph* hit = nullptr;
     for (auto& l : P.loops) if (l.key == key) hit = &l;

@@ -1,6 +1,7 @@
 // State of the streaming plasma (one rank): the device structs of k_plasma.cu and the host-side state of
 // Simulation's plasma members (src/sim.hpp:292-311).
 #pragma once
+#include <functional>
 #include <memory>
 #include <vector>
 #include "g3d_ctx.hpp"
@@ -53,6 +54,19 @@ struct StreamArgs {
     double dep_norm;           // 1 / (Delta h_n dx): the deposit factor of half-cell n per unit of q w dt (the mixed form's FP32 deposit)
     const double* Fd;          // exact fields (FP64 form, Fourier y, no ionization, no analytic wave): the F planes in FP64 for
                                // the gather of a particle that starts inside the half-cell (null: the float planes F)
+};
+
+// The adjoint's record of one march, written by the recording slice loop (device pointers; rs the stride of a particle
+// column): x the streaming particles' states (x, y, zeta, z, p_x, p_y, p_z) entering half-cell n at slot n + 1 and
+// after the last half-cell at slot 0 (7 rs each); a their states alive at the same slots (rs each); q their q w (0 for a
+// fixed ion, which carries no current) and q/m (2 rs); f the exact real fields of slice l after pass p (6 planes of nk
+// at 6 nk (P l + p)).
+struct RecDev {
+    double* x;
+    double* f;
+    int32_t* a;
+    double* q;
+    long rs;
 };
 
 struct PlasmaPtrs {
@@ -137,14 +151,12 @@ struct PlasmaState {
     // the reverse of a march (the adjoint, k_adj_plasma.cu) as a CUDA graph, keyed like the loops
     struct AdjGraph { uint64_t key = 0; cudaGraphExec_t exec = nullptr; } adjg;
     DevBuf<StepVals> stepv;
-    // recording for the adjoint march (null: off; the slice loop then runs without its graph): the streaming particles
-    // entering every half-cell n (x, y, zeta, z, p_x, p_y, p_z; rec_np each, at rec_x + 7 rec_np n) with their state
-    // alive (at rec_a + rec_np (n + 1); after the last half-cell at rec_a), and the exact real fields of every slice n
-    // after every pass p (6 planes of nk, at rec_f + 6 nk (P n + p))
-    double* rec_x = nullptr;
-    double* rec_f = nullptr;
-    int32_t* rec_a = nullptr;
-    long rec_np = 0;
+    // recording for the adjoint march: when rec_on, march_plasma calls rec_step(nstrm, fresh) after loading its plasma
+    // (it points recd at this march's record, or returns false: no record for this march) and the slice loop writes the
+    // record through recd (RecDev), so one graph serves every march
+    bool rec_on = false;
+    std::function<bool(long, long)> rec_step;
+    DevBuf<RecDev> recd;
     PlasmaPtrs ptrs(const Ctx& c) const;
     PlasmaState() = default;
     PlasmaState(const PlasmaState&) = delete;
@@ -160,6 +172,7 @@ struct AdjStepDev {
     const double* Fprev;       // the exact real fields of level s0
     double sTrap;
     long np;                   // the streaming particles of the march
+    RecDev rec;                // the march's record
 };
 // The adjoint arrays of the window (device, half spectra):
 struct AdjPlasmaPtrs {
@@ -172,32 +185,31 @@ struct AdjPlasmaPtrs {
     cpx *lold, *ljsnA, *ljsn, *ldl;      // 4, 3, 3, 3 planes
     cpx* lsi0[2];              // 3 planes each, by the parity of the half-cell
 };
-// ... and its scratch: the record of the forward march (PlasmaState::rec_x, rec_f, rec_a), np streaming particles
-// recorded with the stride rs (rs >= np)
+// ... and its scratch: the march's record (rec, np streaming particles, fresh of them the fresh plasma, the rest joining)
 struct AdjPlasmaWs {
-    long np, rs;
-    double *rec_x, *rec_f;
-    int32_t* rec_a;
+    long np, fresh;
+    RecDev rec;
     double *lFup[2], *lFcur;   // 6 real planes each: the adjoints of a slice's real fields
     double* ljsr;              // 3 real planes: the adjoint of a pass's streaming deposit
-    double* lam;               // 7 rs: the adjoint of the streaming particles' state (x, y, zeta, z, p)
-    double* jl;                // 7 rs: the adjoint of the state of the joining particles carried to the step before
+    double* lam;               // 7 rec.rs: the adjoint of the streaming particles' state (x, y, zeta, z, p)
+    double* jl;                // 7 rec.rs: the adjoint of the state of the joining particles carried to the step before
     AdjStepDev* stepd;         // the values of the step (device)
     cpx* Wsc[6];               // one plane each of transform scratch
     cpx* Tsc[3];
 };
 void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, const double* Fprev, double* lF, double s0,
                           double s1);
-// The slow trapped particles of the march just run (alive 5, v_z below vz_beam) in list order: they join the next
-// march after its fresh plasma. launch_join_adjoint_out copies the adjoint of the state of the next march's joining
-// particles (lam from index fresh, n of them) to jl; launch_join_adjoint_in puts jl onto those particles of this march
-// (lam, 7 components of stride rs). Both return how many particles they moved.
+// The slow trapped particles of a march (alive 5 after it, v_z below vz_beam) in list order: they join the next march
+// after its fresh plasma. launch_join_adjoint_out copies the adjoint of the state of the next march's joining particles
+// (lam from index fresh, n of them) to jl; launch_join_adjoint_in puts jl onto those particles of the march recorded in
+// rec (np of them; lam, 7 components of stride rec.rs). Both return how many particles they moved.
 long launch_join_adjoint_out(Ctx& c, const double* lam, long rs, long fresh, long n, double* jl);
-long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, long rs);
+long launch_join_adjoint_in(Ctx& c, const RecDev& rec, long np, const double* jl, long njl, double* lam);
 void launch_d2f(Ctx& c, const double* a, float* b, long n);     // b = float(a)
 
 // launchers (k_plasma.cu)
-void launch_record_particles(Ctx& c, int n);     // the adjoint's record of the particles entering half-cell n
+void launch_record_particles(Ctx& c, int n);     // the adjoint's record of the particles entering half-cell n (-1: after)
+void launch_record_fields(Ctx& c, int l, int p); // ... of the exact real fields of slice l after pass p
 void launch_stream(Ctx& c, const StreamArgs& a);
 void launch_slice_prologue(Ctx& c, int n, int pred_m, int copy_in, int backup);
 void launch_pass_prologue(Ctx& c, int n, int restore);

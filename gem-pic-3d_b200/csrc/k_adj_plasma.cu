@@ -36,27 +36,6 @@ __device__ __forceinline__ void tsc_slopes(double xi, double d[3]) {
 __device__ __forceinline__ cpx ikc(double k, cpx z) { return ik(-k, z); }     // conj(i k) z
 }  // namespace
 
-// ---------------------------------------------------------------- the correction of half-cell n (one mode)
-// R(n+1) -= q (jsn - si0): dJ/djsn = -q dJ/dR(n+1), dJ/dsi0 = q dJ/dR(n+1) (to the last pass of half-cell n+1, which
-// made that prediction); dl(n-1) = jsn - js0(n): dJ/djsn += dJ/ddl, dJ/djs0_old(n) = -dJ/ddl; js0_new(n) = jsn and
-// jk(n) = b(n) + jsn as the next step's j0: dJ/djsn += dJ/djs0_new(n) + dJ/dj0_next(n) (x, y). jA: dJ/djsn out.
-__device__ __forceinline__ void adj_correct_mode(const AdjPlasmaPtrs& a, int n, double q, int par, long i, cpx jA[3]) {
-    const long nkh = a.nkh;
-    const long pl = long(n + 1) * nkh + i;          // slice n+1 of the spectra, half-cell n of the current planes
-    const cpx lr[3] = {a.lS[0][pl], a.lS[1][pl], C(0)};
-    cpx* so = a.lsi0[par];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const cpx d = a.ldl[k * nkh + i];
-        cpx u = -q * lr[k] + d + a.ljs0[k][pl];
-        if (k < 2) u = u + a.ljk[k][pl];
-        jA[k] = u;
-        so[k * nkh + i] = q * lr[k];
-        a.ljs0[k][pl] = -d;
-        a.ldl[k * nkh + i] = C(0);
-    }
-}
-
 // ---------------------------------------------------------------- the transposed slice march of one pass (one mode)
 // march_slice_mode (k_plasma.cu; march_point, src/sim_kernels.hpp:173-210) transposed line by line: the adjoints of
 // the slice's new values (lsl: those of the slice's real fields of this pass, plus for the last pass what later reads of
@@ -159,6 +138,117 @@ __device__ __forceinline__ void adj_march_mode(const Geo& g, const AdjPlasmaPtrs
         for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = a.lold[k * nkh + i] + lo[k];
     }
 }
+// One pass of half-cell n for one mode, as adj_march_mode with, for the last pass, the transposed correction of the
+// half-cell first: R(n+1) -= q (jsn - si0) gives dJ/djsn = -q dJ/dR(n+1) and dJ/dsi0 = q dJ/dR(n+1) (for the last pass
+// of half-cell n+1, which made that prediction); dl(n-1) = jsn - js0(n) gives dJ/djsn += dJ/ddl, dJ/djs0_old(n) =
+// -dJ/ddl; js0_new(n) = jsn and jk(n) = b(n) + jsn as the next step's j0 give dJ/djsn += dJ/djs0_new(n) +
+// dJ/dj0_next(n) (x, y). Every value of the mode is loaded before anything is stored (the stores would otherwise keep
+// the later loads waiting: the compiler cannot prove the arrays distinct), then the same arithmetic as
+// adj_march_mode runs on registers.
+__device__ __forceinline__ void adj_pass_mode(const Geo& g, const AdjPlasmaPtrs& a, int n, double D, double q, int last, int first,
+                                              int multi, int extrap, double w, int par, int par_prev, long i, const cpx lsl[6],
+                                              cpx ls[3]) {
+    const long nkh = a.nkh;
+    const int kxi = int(i % g.H), j = int(i / g.H);
+    const double kx = g.kxd[kxi], ky = g.kyd[j], k2 = kx * kx + ky * ky, wl = g.wlo[n], wu = g.whi[n];
+    const long o = long(n - g.a) * nkh + i, od = o, ou = o + nkh;     // ou: slice n+1 of the spectra, half-cell n
+    const double h = g.hcg[n + 2], den = 1 + 0.25 * h * (D + 0.25 * h) * k2;
+    const bool pred = n >= 1;
+    // loads
+    cpx sN[6], sP[6], j0d[2], j0u[2], kd[3], ku[3], s0d[3], s0u[3], dl[3], si[3], old[4];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) { sN[k] = last ? a.lS[k][o] : C(0); sP[k] = a.lS[k][ou]; }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) { j0d[k] = a.lj0[k][od]; j0u[k] = a.lj0[k][ou]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        kd[k] = a.ljk[k][od]; ku[k] = a.ljk[k][ou]; s0d[k] = a.ljs0[k][od]; s0u[k] = a.ljs0[k][ou];
+        dl[k] = a.ldl[k * nkh + i];
+        si[k] = last && pred ? a.lsi0[par_prev][k * nkh + i] : C(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) old[k] = multi && !last ? a.lold[k * nkh + i] : C(0);
+    // the correction (last pass)
+    cpx jA[3] = {C(0), C(0), C(0)}, so[3] = {C(0), C(0), C(0)};
+    if (last) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const cpx lr = k < 2 ? sP[k] : C(0);
+            jA[k] = -q * lr + dl[k] + s0u[k] + (k < 2 ? ku[k] : C(0));
+            so[k] = q * lr;
+            s0u[k] = -dl[k];
+            dl[k] = C(0);
+        }
+    }
+    // the march (adj_march_mode's arithmetic)
+    cpx ln[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ln[k] = lsl[k] + sN[k];
+    cpx lLsx = ln[4], lLsy = ln[5];
+    cpx lEn = ln[2] - 0.25 * h * ikc(kx, ln[4]) - 0.25 * h * ikc(ky, ln[5]);
+    cpx lBn = ln[3] + 0.25 * h * ikc(ky, ln[4]) - 0.25 * h * ikc(kx, ln[5]);
+    cpx lRsx = ln[0], lRsy = ln[1];
+    lEn = lEn + D * ikc(kx, ln[0]) + D * ikc(ky, ln[1]);
+    lBn = lBn + D * ikc(ky, ln[0]) - D * ikc(kx, ln[1]);
+    const cpx le = lEn / den, lb = lBn / den;
+    cpx lpE = le, lpB = lb;
+    const cpx lQp = -0.5 * h * le, lSE = -0.25 * h * le, lCp = -0.5 * h * lb, lSB = -0.25 * h * lb;
+    cpx lup[3];
+    lup[2] = -h * le;
+    lRsx = lRsx - ikc(kx, lSE) - ikc(ky, lSB);
+    lRsy = lRsy - ikc(ky, lSE) + ikc(kx, lSB);
+    lLsx = lLsx + ikc(kx, lSE) - ikc(ky, lSB);
+    lLsy = lLsy + ikc(ky, lSE) + ikc(kx, lSB);
+    sP[0] = sP[0] - 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp);
+    sP[4] = sP[4] + 0.5 * ikc(kx, lQp) - 0.5 * ikc(ky, lCp) + lLsx;
+    sP[1] = sP[1] - 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp);
+    sP[5] = sP[5] + 0.5 * ikc(ky, lQp) + 0.5 * ikc(kx, lCp) + lLsy;
+    lpE = lpE - 0.25 * h * ikc(kx, lLsx) - 0.25 * h * ikc(ky, lLsy);
+    lpB = lpB + 0.25 * h * ikc(ky, lLsx) - 0.25 * h * ikc(kx, lLsy);
+    sP[2] = sP[2] + lpE;
+    sP[3] = sP[3] + lpB;
+    lup[0] = -0.5 * h * lLsx;
+    lup[1] = -0.5 * h * lLsy;
+    const cpx lo[4] = {lRsx, lRsy, D * ikc(kx, lRsx) + D * ikc(ky, lRsy), D * ikc(ky, lRsx) - D * ikc(kx, lRsy)};
+    const cpx lJx = -D * lRsx, lJy = -D * lRsy;
+    j0d[0] = j0d[0] + wl * lJx; j0u[0] = j0u[0] + wu * lJx;
+    j0d[1] = j0d[1] + wl * lJy; j0u[1] = j0u[1] + wu * lJy;
+    const cpx lkd[3] = {wl * lJx, wl * lJy, C(0)};
+    const cpx lku[3] = {wu * lJx + lup[0], wu * lJy + lup[1], lup[2]};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        kd[k] = kd[k] + lkd[k]; ku[k] = ku[k] + lku[k];
+        ls[k] = jA[k] + lku[k];
+        if (pred) {
+            const cpx lp = lkd[k] + si[k];                  // dJ/dpred of half-cell n-1
+            s0d[k] = s0d[k] + lp;
+            if (extrap) {
+                ls[k] = ls[k] + (1 + w) * lp;
+                s0u[k] = s0u[k] - (1 + w) * lp;
+                dl[k] = dl[k] - w * lp;
+            }
+        }
+    }
+    // stores
+#pragma unroll
+    for (int k = 0; k < 6; ++k) a.lS[k][ou] = sP[k];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) { a.lj0[k][od] = j0d[k]; a.lj0[k][ou] = j0u[k]; }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        a.ljk[k][od] = kd[k]; a.ljk[k][ou] = ku[k]; a.ljs0[k][od] = s0d[k]; a.ljs0[k][ou] = s0u[k];
+        a.ldl[k * nkh + i] = dl[k];
+        if (last) a.lsi0[par][k * nkh + i] = so[k];
+    }
+    if (first) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.lS[k][o] = old[k] + lo[k];
+        a.lS[4][o] = C(0); a.lS[5][o] = C(0);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a.lold[k * nkh + i] = old[k] + lo[k];
+    }
+}
 // the front slice's march alone (its slice adjoints in a.lsl)
 __global__ void k_adjp_march_front(Geo g, AdjPlasmaPtrs a, int n, double D, int par_prev) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < a.nkh; i += long(gridDim.x) * blockDim.x) {
@@ -172,9 +262,9 @@ __global__ void k_adjp_march_front(Geo g, AdjPlasmaPtrs a, int n, double D, int 
 // ---------------------------------------------------------------- one pass's column work, fused
 // k_adjp_pass_cols: the transpose of k_pass_cols (k_plasma.cu) and of the correction, one CTA per k_x column and one
 // thread per k_y. (1) The y transforms of the six half-row adjoints of slice n's real fields (the column half of the
-// transposed real fields, k_adj_rf_cols) give the adjoints of the slice's values of this pass. (2) The last pass: the
-// transposed correction of half-cell n (adj_correct_mode). (3) The transposed march of the mode (adj_march_mode) gives
-// the adjoint of the pass's streaming current. (4) Its filters and inverse y transforms (the column half of the
+// transposed real fields, k_adj_rf_cols) give the adjoints of the slice's values of this pass. (2), (3) The last pass:
+// the transposed correction of half-cell n; the transposed march of the mode (both in adj_pass_mode), which gives the
+// adjoint of the pass's streaming current. (4) Its filters and inverse y transforms (the column half of the
 // transposed current spectra, k_adj_cur_cols) into T, which the rows kernel turns into the current's real adjoint.
 // zero_a, zero_b (nullable, nzero values each): field adjoints cleared for the pushes of this pass.
 template <int NY>
@@ -212,9 +302,8 @@ __global__ void __launch_bounds__(NY) k_adjp_pass_cols(Geo g, AdjPlasmaPtrs a, c
     const cpx lsl[6] = {tl[0][Tile::at(j, 0)], tl[1][Tile::at(j, 0)], tl[4][Tile::at(j, 0)], tl[5][Tile::at(j, 0)],
                         tl[2][Tile::at(j, 0)], tl[3][Tile::at(j, 0)]};              // {R_x, R_y, E_z, B_z, L_x, L_y}
     // (2), (3)
-    cpx jA[3] = {C(0), C(0), C(0)}, ls[3];
-    if (last) adj_correct_mode(a, n, q, par, i, jA);
-    adj_march_mode(g, a, n, D, last, first, multi, extrap, w, par_prev, 0, i, lsl, jA, ls);
+    cpx ls[3];
+    adj_pass_mode(g, a, n, D, q, last, first, multi, extrap, w, par, par_prev, i, lsl, ls);
     // (4) the filters and the inverse transforms along y (conjugate, forward, conjugate)
     const double k2f = g.kxs[kxi] * g.kxs[kxi] + g.kys[j] * g.kys[j];
     const double f = (kxi == 0 && j == 0 && !keep0) ? 0.0 : g.filt[kxi] * g.filty[j] / (1 + a2 * k2f);
@@ -330,48 +419,47 @@ struct DepGat {
         }
     }
 };
-// One thread per streaming particle of the recorded list: the state entering half-cell n (rec: x, y, zeta, z, p_x,
-// p_y, p_z of stride rs), its state alive before (ae) and after (ax) the half-cell, the pass's current adjoints lJ
-// and, for the last pass, the adjoint of the state it leaves with (lam, replaced by the adjoint of the state it
-// enters with; the earlier passes add to it: they deposit from the same state). A particle takes part as the forward
-// let it (alive, or waiting and reached by the half-cell; then from its zeta: a partial path); the last pass keeps
-// the forward's trapping event (ax = 5), an earlier one decides it as the forward did. Fixed ions carry no current
-// and do not move; particles of no charge deposit nothing.
-// The values of the step (the list and its count, sTrap, the level s0 fields) come from device memory (AdjStepDev), so
-// that the reverse of a march runs as one graph for every step. prev: Fa is slice n of the level s0 fields, st->Fprev +
-// off; else the given planes Fa.
+// One thread per streaming particle of the recorded march (st->rec: the state entering half-cell n, its states alive
+// before and after the half-cell, q w and q/m), the pass's current adjoints lJ and, for the last pass, the adjoint of the
+// state it leaves with (lam, replaced by the adjoint of the state it enters with; the earlier passes add to it: they
+// deposit from the same state). A particle takes part as the forward let it (alive, or waiting and reached by the
+// half-cell; then from its zeta: a partial path); the last pass keeps the forward's trapping event (alive 5 after the
+// half-cell), an earlier one decides it as the forward did. Particles of no charge (and fixed ions) deposit nothing.
+// The fields the pushes read: slice n as pass p saw it (the level s0 fields st->Fprev for p = 0, else the record) and
+// slice n+1 as solved (the record); their adjoints go to lF (p = 0; the level s0 fields' adjoint, whole window) or lFcur,
+// and to lFnext. Everything that changes from step to step is read from st, so that the reverse of a march runs as one
+// graph for every step.
 template <bool LAST>
-__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, const StrmDev* __restrict__ sd, const IonDevC* __restrict__ ions,
-                                                     const AdjStepDev* __restrict__ st, long rs, const double* __restrict__ rec,
-                                                     const int32_t* __restrict__ ae, const int32_t* __restrict__ ax, int n,
-                                                     double Delta, int prev, long off, const double* Fa, long sa, const double* Fb, long sb,
-                                                     double* lFa, long lsa, double* lFb, long lsb, const double* __restrict__ lJ,
+__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, const AdjStepDev* __restrict__ st, int n, int p, int passes, double Delta,
+                                                     double* lF, double* lFcur, double* lFnext, const double* __restrict__ lJ,
                                                      double* __restrict__ lam) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
-    const long np = st->np;
-    if (i >= np) return;
-    const StrmDev S = sd[0];
-    const double sTrap = st->sTrap;
-    if (prev) Fa = st->Fprev + off;
+    if (i >= st->np) return;
+    const RecDev R = st->rec;
+    const long rs = R.rs, nk = g.nk;
+    const double* rec = R.x + 7 * rs * long(n + 1);
     const double zn = g.zs[n], zn1 = g.zs[n + 1], h = zn1 - zn, zeta = rec[2 * rs + i];
-    const int a_in = ae[i];
+    const int a_in = R.a[rs * long(n + 1) + i];
     if (!(a_in == 1 || (a_in == 6 && zeta > zn))) return;
-    const int sp = S.sp[i];
-    if (sp >= SP_ION && sp < SP_FREED && !ions[sp - SP_ION].mobile) return;
-    const double qw = S.q[i] * S.w[i];
+    const double qw = R.q[i];
     if (qw == 0) return;
     StreamCase K;
-    K.zn = zn; K.h = h; K.fscale = 1 / (Delta * h * g.dx); K.sTrap = sTrap;
+    K.zn = zn; K.h = h; K.fscale = 1 / (Delta * h * g.dx); K.sTrap = st->sTrap;
     K.partial = zeta < zn1 - 1e-9 * h;
-    K.trap = LAST ? (ax[i] == 5 ? 1 : 0) : 2;
-    const double p[3] = {rec[4 * rs + i], rec[5 * rs + i], rec[6 * rs + i]};
+    K.trap = LAST ? (R.a[rs * long(n) + i] == 5 ? 1 : 0) : 2;
+    const long fpl = long(g.ns + 2) * nk, off = long(n - g.a) * nk;
+    const double* Fa = p == 0 ? st->Fprev + off : R.f + 6 * nk * (long(passes) * n + p - 1);
+    const double* Fb = R.f + 6 * nk * (long(passes) * (n + 1) + passes - 1);
+    double* lFa = p == 0 ? lF + off : lFcur;
+    const long sa = p == 0 ? fpl : nk;
+    const double pp[3] = {rec[4 * rs + i], rec[5 * rs + i], rec[6 * rs + i]};
     double lout[7] = {0, 0, 0, 0, 0, 0, 0};
     if (LAST)
         for (int k = 0; k < 7; ++k) lout[k] = lam[k * rs + i];
-    SliceGat gat{&g, Fa, Fb, sa, sb, lFa, lFb, lsa, lsb, zn, 1 / h};
+    SliceGat gat{&g, Fa, Fb, sa, nk, lFa, lFnext, sa, nk, zn, 1 / h};
     DepGat dep{&g, lJ};
     double lin[7];
-    stream_push_reverse(rec[i], rec[rs + i], zeta, rec[3 * rs + i], p, S.qm[i], qw, K, gat, dep, lout, lin);
+    stream_push_reverse(rec[i], rec[rs + i], zeta, rec[3 * rs + i], pp, R.q[rs + i], qw, K, gat, dep, lout, lin);
     for (int k = 0; k < 7; ++k) lam[k * rs + i] = LAST ? lin[k] : lam[k * rs + i] + lin[k];
 }
 
@@ -381,7 +469,7 @@ static unsigned mode_blocks(long n) {
     return unsigned(b < 1 ? 1 : b);
 }
 
-// The transpose of march_plasma(s0, s1) for the step whose forward was recorded into w.rec_x, w.rec_f, w.rec_a. On entry
+// The transpose of march_plasma(s0, s1) for the step whose forward was recorded into w.rec. On entry
 // lS holds the adjoints of the step's final spectra, ljk (x, y) those of jk as the next step's j0 (ljk z zero), ljs0
 // those of the step's final js0, lj0 zeros, w.lam those of the streaming particles' states after the march (the slow
 // trapped ones join the next march); lF (the level s0 real fields' adjoint, whole window) receives the reads of the
@@ -395,11 +483,11 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
     PlasmaState& P = *c.pl;
     const int N = c.N, passes = P.cfg.iterations;
     const double Delta = s1 - s0, D = 0.5 * Delta;
-    const long nkh = c.nkh, nk = c.nk, fpl = long(c.ns + 2) * nk, rs = w.rs;
+    const long nkh = c.nkh, nk = c.nk, rs = w.rec.rs;
     const bool extrap = P.cfg.predictor_extrapolate != 0, keep0 = P.box_mean;
     const double a2 = P.cfg.smooth_length * P.cfg.smooth_length;
     cudaStream_t st = c.stream;
-    const AdjStepDev sv{Fprev, s1 + (P.cfg.trap_advance - 1) * Delta, w.np};
+    const AdjStepDev sv{Fprev, s1 + (P.cfg.trap_advance - 1) * Delta, w.np, w.rec};
     G3D_CUDA(cudaMemcpyAsync(w.stepd, &sv, sizeof sv, cudaMemcpyHostToDevice, st));
     auto issue = [&]() {
         std::vector<double> cen(size_t(N - 1));
@@ -413,7 +501,6 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
             // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
             const double wex = (n >= 1 && n + 1 <= N - 2)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
-            const double* Fnext = w.rec_f + 6 * nk * (size_t(passes) * size_t(n + 1) + size_t(passes - 1));
             const double q = D * c.wlo_h[size_t(n + 1)];
             for (int p = passes - 1; p >= 0; --p) {
                 // the rows of the transposed real fields of slice n, the fused column work, the rows of the transposed
@@ -427,21 +514,12 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
                 c.prof_end(tok);
                 launch_adj_ss_rows(c, w.Tsc, w.ljsr);
                 if (!rs) continue;
-                const double* Fa = p == 0 ? nullptr : w.rec_f + 6 * nk * (size_t(passes) * size_t(n) + size_t(p - 1));
-                const long sa = p == 0 ? fpl : nk, off = long(n - c.a) * nk;
-                double* lFa = p == 0 ? lF + off : w.lFcur;
-                const long lsa = p == 0 ? fpl : nk;
-                const double* rec = w.rec_x + 7 * size_t(rs) * size_t(n);
-                const int32_t* ae = w.rec_a + size_t(rs) * size_t(n + 1);
-                const int32_t* ax = w.rec_a + size_t(rs) * size_t(n);
                 tok = c.prof_begin("adj_plasma_stream");
                 if (p == passes - 1)
-                    k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), P.sdev.p, P.ion_dev.p, w.stepd, rs, rec, ae, ax, n, Delta,
-                                                            p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
+                    k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
                                                             w.ljsr, w.lam);
                 else
-                    k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), P.sdev.p, P.ion_dev.p, w.stepd, rs, rec, ae, ax, n, Delta,
-                                                             p == 0 ? 1 : 0, off, Fa, sa, Fnext, nk, lFa, lsa, w.lFup[cur ^ 1], nk,
+                    k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
                                                              w.ljsr, w.lam);
                 c.check_launch("k_adjp_stream");
                 c.prof_end(tok);
@@ -461,8 +539,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
     for (int q = 0; q < 3; ++q) { mixk(ptr(a.ljk[q])); mixk(ptr(a.ljs0[q])); mixk(ptr(w.Tsc[q])); }
     for (int q = 0; q < 2; ++q) { mixk(ptr(a.lj0[q])); mixk(ptr(a.lsi0[q])); mixk(ptr(w.lFup[q])); }
     mixk(ptr(a.lold)); mixk(ptr(a.ljsnA)); mixk(ptr(a.ljsn)); mixk(ptr(a.ldl)); mixk(ptr(w.lFcur)); mixk(ptr(w.ljsr));
-    mixk(ptr(w.lam)); mixk(ptr(w.rec_x)); mixk(ptr(w.rec_f)); mixk(ptr(w.rec_a)); mixk(ptr(w.stepd)); mixk(ptr(lF));
-    mixk(ptr(P.sdev.p)); mixk(uint64_t(rs)); mixk(uint64_t(passes)); mixk(uint64_t(extrap) | uint64_t(keep0) << 1);
+    mixk(ptr(w.lam)); mixk(ptr(w.stepd)); mixk(ptr(lF)); mixk(uint64_t(rs)); mixk(uint64_t(passes)); mixk(uint64_t(extrap) | uint64_t(keep0) << 1);
     uint64_t bits;
     std::memcpy(&bits, &Delta, sizeof bits); mixk(bits);
     std::memcpy(&bits, &a2, sizeof bits); mixk(bits);

@@ -1218,6 +1218,19 @@ __global__ void k_join_adj_out(const double* __restrict__ lam, long rs, long fre
     for (long j = long(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += long(gridDim.x) * blockDim.x)
         for (int q = 0; q < 7; ++q) jl[q * n + j] = lam[q * rs + fresh + j];
 }
+// the slow trapped particles of a recorded march: alive 5 after it and v_z of their final momenta below vzb (the
+// operations of trapped_fast)
+__global__ void k_join_flags(RecDev R, long np, double vzb, int* __restrict__ flag) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i <= np; i += long(gridDim.x) * blockDim.x) {
+        bool f = false;
+        if (i < np && R.a[i] == 5) {
+            const double px = R.x[4 * R.rs + i], py = R.x[5 * R.rs + i], pz = R.x[6 * R.rs + i];
+            const double g = __dsqrt_rn(__dadd_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(px, px)), __dmul_rn(py, py)), __dmul_rn(pz, pz)));
+            f = !(__ddiv_rn(pz, g) >= vzb);
+        }
+        flag[i] = f ? 1 : 0;
+    }
+}
 __global__ void k_join_adj_in(const int* __restrict__ flag, const int* __restrict__ off, long cap, const double* __restrict__ jl,
                               long njl, double* __restrict__ lam, long rs) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < cap; i += long(gridDim.x) * blockDim.x) {
@@ -1233,43 +1246,61 @@ long launch_join_adjoint_out(Ctx& c, const double* lam, long rs, long fresh, lon
     c.check_launch("k_join_adj_out");
     return n;
 }
-long launch_join_adjoint_in(Ctx& c, const double* jl, long njl, double* lam, long rs) {
+long launch_join_adjoint_in(Ctx& c, const RecDev& rec, long np, const double* jl, long njl, double* lam) {
     PlasmaState& P = *c.pl;
-    const long cap = P.s.cap;
-    if (cap <= 0) return 0;
-    reserve_flags(c, cap);
-    k_trap_flags<<<ew_blocks(cap + 1), 256, 0, c.stream>>>(P.strm, P.nstrm_dev.p, cap, P.cfg.vz_beam, 0, P.cflag.p);
-    c.check_launch("k_trap_flags");
-    const long ns = scan_flags(c, cap);
-    if (ns > 0 && njl > 0 && rs >= std::min<long>(cap, P.nstrm)) {
-        k_join_adj_in<<<ew_blocks(std::min<long>(cap, rs)), 256, 0, c.stream>>>(P.cflag.p, P.coff.p, std::min<long>(cap, rs), jl, njl,
-                                                                               lam, rs);
+    if (np <= 0) return 0;
+    reserve_flags(c, np);
+    k_join_flags<<<ew_blocks(np + 1), 256, 0, c.stream>>>(rec, np, P.cfg.vz_beam, P.cflag.p);
+    c.check_launch("k_join_flags");
+    const long ns = scan_flags(c, np);
+    if (ns > 0 && njl > 0) {
+        k_join_adj_in<<<ew_blocks(np), 256, 0, c.stream>>>(P.cflag.p, P.coff.p, np, jl, njl, lam, rec.rs);
         c.check_launch("k_join_adj_in");
     }
     return ns;
 }
-// The adjoint's record of the particles entering half-cell n (n < 0: only their states alive after the last one): the
-// seven state columns and alive of every streaming particle, the count read on the device, so that the recording
-// slice loop can run as a graph
-__global__ void k_rec_particles(const StrmDev* __restrict__ sd, const long* __restrict__ n_dev, long rs, double* __restrict__ rec,
-                                int32_t* __restrict__ ra) {
+// The adjoint's record of the particles entering half-cell n (n < 0: after the last one, with their charges): the
+// seven state columns and alive of every streaming particle at slot n + 1 of the record that rd points at; the count
+// read on the device, so that the recording slice loop can run as a graph
+__global__ void k_rec_particles(const StrmDev* __restrict__ sd, const long* __restrict__ n_dev, const RecDev* __restrict__ rd, int n,
+                                const IonDevC* __restrict__ ions) {
     const StrmDev S = sd[0];
-    const long n = *n_dev < rs ? *n_dev : rs;
-    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) {
-        if (rec) {
-            rec[i] = S.x[i]; rec[rs + i] = S.y[i]; rec[2 * rs + i] = S.zeta[i]; rec[3 * rs + i] = S.z[i];
-            rec[4 * rs + i] = S.px[i]; rec[5 * rs + i] = S.py[i]; rec[6 * rs + i] = S.pz[i];
+    const RecDev R = *rd;
+    const long rs = R.rs, m = *n_dev < rs ? *n_dev : rs;
+    double* x = R.x + 7 * rs * long(n + 1);
+    int32_t* a = R.a + rs * long(n + 1);
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += long(gridDim.x) * blockDim.x) {
+        x[i] = S.x[i]; x[rs + i] = S.y[i]; x[2 * rs + i] = S.zeta[i]; x[3 * rs + i] = S.z[i];
+        x[4 * rs + i] = S.px[i]; x[5 * rs + i] = S.py[i]; x[6 * rs + i] = S.pz[i];
+        a[i] = S.alive[i];
+        if (n < 0) {
+            const int sp = S.sp[i];
+            const bool fixed = sp >= SP_ION && sp < SP_FREED && !ions[sp - SP_ION].mobile;
+            R.q[i] = fixed ? 0.0 : S.q[i] * S.w[i];
+            R.q[rs + i] = S.qm[i];
         }
-        ra[i] = S.alive[i];
     }
 }
 void launch_record_particles(Ctx& c, int n) {
     PlasmaState& P = *c.pl;
-    const size_t rs = size_t(P.rec_np);
-    double* rec = n >= 0 ? P.rec_x + 7 * rs * size_t(n) : nullptr;
-    k_rec_particles<<<ew_blocks(long(rs)), 256, 0, c.stream>>>(P.sdev.p, P.nstrm_dev.p, long(rs), rec, P.rec_a + size_t(n + 1) * rs);
+    k_rec_particles<<<ew_blocks(P.s.cap), 256, 0, c.stream>>>(P.sdev.p, P.nstrm_dev.p, P.recd.p, n, P.ion_dev.p);
     c.check_launch("k_rec_particles");
 }
+// ... and of the exact real fields of slice l after pass p
+__global__ void k_rec_fields(const RecDev* __restrict__ rd, const double* __restrict__ Fd, long fpl, long nk, long l, int passes, int p) {
+    double* f = rd->f + 6 * nk * (long(passes) * l + p);
+    for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < 6 * nk; e += long(gridDim.x) * blockDim.x) {
+        const long comp = e / nk, k = e - comp * nk;
+        f[e] = Fd[comp * fpl + l * nk + k];
+    }
+}
+void launch_record_fields(Ctx& c, int l, int p) {
+    PlasmaState& P = *c.pl;
+    k_rec_fields<<<ew_blocks(6L * c.nk), 256, 0, c.stream>>>(P.recd.p, c.Fd.p, long(c.ns + 2) * c.nk, long(c.nk), long(l - c.a),
+                                                            P.cfg.iterations, p);
+    c.check_launch("k_rec_fields");
+}
+
 long launch_join_cap(Ctx& c) {
     PlasmaState& P = *c.pl;
     if (P.njb == 0 || !P.any_ionizing) return 0;

@@ -110,6 +110,18 @@ def test_plasma_gradients_with_trapped_electrons(what):
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
 
 
+def test_plasma_adjoint_stored_and_recomputed_records_agree(monkeypatch):
+    """The march records kept from the forward (the default when they fit) and those made by running every step again
+    from its level checkpoint (G3D_ADJ_RECOMPUTE) give the same gradients, with trapped electrons joining later steps."""
+    cfg = case(a0=1.0, charge_pC=1.0)
+    J1, gm1, gp1, _ = adjoint(cfg)
+    monkeypatch.setenv("G3D_ADJ_RECOMPUTE", "1")
+    J2, gm2, gp2, _ = adjoint(cfg)
+    assert J1 == J2
+    assert np.linalg.norm(gm1 - gm2) <= 1e-10 * np.linalg.norm(gm1)
+    assert np.linalg.norm(gp1 - gp2) <= 1e-10 * np.linalg.norm(gp1)
+
+
 def test_plasma_adjoint_refuses_what_it_does_not_differentiate():
     """The mixed form and ionization are refused with G3D_ERR_ARG before anything runs."""
     from g3d import G3DError, Simulation, configs
