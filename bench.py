@@ -765,7 +765,89 @@ def adjoint_check(eps=1e-6):
         "note": "momenta: as loaded, through the start field (timed adjoint); momenta_after_start: right after init "
                 "with the start field held. The first takes eps = 1e-4: the bunch's beta, bit for bit the "
                 "reference's sum of w p_z / gamma, rounds at ~1e-14, which a step of 1e-6 does not clear"}
+    out["with_plasma"] = plasma_adjoint_check(eps, timed, central)
     return out
+
+
+def plasma_adjoint_check(eps, timed, central):
+    """Workload 4 as specified, with its streaming plasma (0.005 n_c, 2 x 2 per cell, two passes): the adjoint's cost
+    against the forward (FP64 form with exact fields; the march records kept from the forward, and with every step run
+    again from its level checkpoint), the trapped plasma electrons of the forward, and the directional derivatives
+    against central differences of the forward."""
+    import os
+    import numpy as np
+    from g3d import Simulation, configs
+    cfg = configs.config4(plasma=True)
+    K = cfg.steps
+    H = cfg.nx // 2 + 1
+    sim = Simulation(cfg)
+    sim.load_bunch()
+    p0 = sim.host_particles()
+    sim.set_laser_modes(None)
+    sim.set_exact_fields(True)
+    trapped = []
+    for _ in range(3):
+        sim.set_particles(p0); sim.init_fields()
+        tf, _ = timed(sim, lambda: [sim.step_async() for _ in range(K)])
+    sim.set_particles(p0); sim.init_fields()
+    for _ in range(K):
+        sim.step()
+        trapped.append(int(np.sum(sim.streaming_particles()["alive"] == 5)))
+    times = {}
+    for mode in ("stored", "recompute"):
+        if mode == "recompute":
+            os.environ["G3D_ADJ_RECOMPUTE"] = "1"
+        try:
+            for _ in range(2):
+                sim.set_particles(p0); sim.init_fields()
+                ta, g = timed(sim, lambda: sim.adjoint(K))
+        finally:
+            os.environ.pop("G3D_ADJ_RECOMPUTE", None)
+        times[mode] = ta
+        if mode == "stored":
+            grads = g
+    sim.set_particles(p0); sim.init_fields()
+    ga = sim.adjoint(K, modes=False, through_start=False)[2]
+    sim.close()
+
+    def final(coef=None, dp=None, through_start=True):
+        s = Simulation(cfg)
+        s.load_bunch()
+
+        def perturb():
+            p = s.host_particles()
+            p["px"] += dp[:, 0]; p["py"] += dp[:, 1]; p["pz"] += dp[:, 2]
+            s.set_particles(p)
+        if dp is not None and through_start:
+            perturb()
+        s.set_laser_modes(coef)
+        s.set_exact_fields(True)
+        s.init_fields()
+        if dp is not None and not through_start:
+            perturb()
+        for _ in range(K):
+            s.step_async()
+        p = s.host_particles()
+        s.close()
+        return p
+    J, gm, gp = grads
+    d = np.random.default_rng(11).standard_normal((cfg.ny, H)) + 1j * np.random.default_rng(12).standard_normal((cfg.ny, H))
+    D = np.random.default_rng(13).standard_normal(gp.shape)
+    fl = central(final(coef=1 + eps * d), final(coef=1 - eps * d))
+    fa = central(final(dp=eps * D, through_start=False), final(dp=-eps * D, through_start=False))
+    e4 = 1e-4
+    fm = central(final(dp=e4 * D), final(dp=-e4 * D), e4)
+    al, am, aa = float(np.real(np.sum(np.conj(gm) * d))), float(np.sum(gp * D)), float(np.sum(ga * D))
+    return {"workload": f"4: {cfg.name}, {cfg.nx}x{cfg.ny} modes x {cfg.nzeta} slices, {cfg.particles} macro-electrons, "
+                        f"plasma n0 0.005 n_c at 2x2 per cell, {K} s-steps", "form": "fp64 (exact fields)",
+            "forward_ms": tf, "adjoint_ms": times["stored"], "adjoint_over_forward": times["stored"] / tf,
+            "adjoint_recompute_ms": times["recompute"], "adjoint_recompute_over_forward": times["recompute"] / tf,
+            "trapped_plasma_electrons_per_step": {"max": max(trapped), "total": sum(trapped)},
+            "J": J, "laser_modes_rel_err": abs(al - fl) / abs(fl), "momenta_rel_err": abs(am - fm) / abs(fm),
+            "momenta_after_start_rel_err": abs(aa - fa) / abs(fa),
+            "central_differences": {"laser_modes": fl, "momenta": fm, "momenta_after_start": fa, "eps": eps, "eps_momenta": e4},
+            "note": "adjoint_ms: the forward keeping each march's record, J and the reverse sweep; adjoint_recompute_ms: "
+                    "the forward with level checkpoints only, each step run again in the reverse sweep"}
 
 
 def main():

@@ -429,8 +429,9 @@ struct DepGat {
 // slice n+1 as solved (the record); their adjoints go to lF (p = 0; the level s0 fields' adjoint, whole window) or lFcur,
 // and to lFnext. Everything that changes from step to step is read from st, so that the reverse of a march runs as one
 // graph for every step.
+constexpr int ADJ_ST_NT = 32;      // one warp a CTA: the few thousand particles of a march spread over every SM
 template <bool LAST>
-__global__ void __launch_bounds__(128) k_adjp_stream(Geo g, const AdjStepDev* __restrict__ st, int n, int p, int passes, double Delta,
+__global__ void __launch_bounds__(ADJ_ST_NT) k_adjp_stream(Geo g, const AdjStepDev* __restrict__ st, int n, int p, int passes, double Delta,
                                                      double* lF, double* lFcur, double* lFnext, const double* __restrict__ lJ,
                                                      double* __restrict__ lam) {
     const long i = long(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -495,7 +496,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
         G3D_CUDA(cudaMemsetAsync(a.ldl, 0, 3 * nkh * sizeof(cpx), st));
         G3D_CUDA(cudaMemsetAsync(w.lFup[0], 0, 6 * nk * 8, st));
         int cur = 0;
-        const unsigned mb = mode_blocks(nkh), pb = unsigned((rs + 127) / 128);
+        const unsigned pb = unsigned((rs + ADJ_ST_NT - 1) / ADJ_ST_NT);
         for (int n = c.a; n <= N - 2; ++n) {
             int tok = 0;
             // the forward's weight of the extrapolation (none for the first half-cell, N-2, which has no change dl yet)
@@ -516,10 +517,10 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
                 if (!rs) continue;
                 tok = c.prof_begin("adj_plasma_stream");
                 if (p == passes - 1)
-                    k_adjp_stream<true><<<pb, 128, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
+                    k_adjp_stream<true><<<pb, ADJ_ST_NT, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
                                                             w.ljsr, w.lam);
                 else
-                    k_adjp_stream<false><<<pb, 128, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
+                    k_adjp_stream<false><<<pb, ADJ_ST_NT, 0, st>>>(c.geo(), w.stepd, n, p, passes, Delta, lF, w.lFcur, w.lFup[cur ^ 1],
                                                              w.ljsr, w.lam);
                 c.check_launch("k_adjp_stream");
                 c.prof_end(tok);
@@ -528,7 +529,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
         }
         // the front slice N-1: its real fields (read by half-cell N-2), then its march with the prediction js0(N-2)
         launch_adj_real_fields_slice(c, w.lFup[cur], nk, w.Wsc, a.lsl);
-        k_adjp_march_front<<<mb, 128, 0, st>>>(c.geo(), a, N - 1, D, (N - 2) & 1);
+        k_adjp_march_front<<<mode_blocks(nkh), 128, 0, st>>>(c.geo(), a, N - 1, D, (N - 2) & 1);
         c.check_launch("k_adjp_march_front");
     };
     // what the graph holds by value: the arrays, the grid and the step length
