@@ -300,6 +300,10 @@ struct FmidOut {
     void* out = nullptr;
     int other = 0, f32 = 0;
     int fh = 0;               // free-hand y (FP32): per point (E_x, E_z, B_y, 0) of the node row, (E_y, B_x, B_z, 0) of the half-node row
+    // the adjoint's record of the slice's exact fields (the exact midpoint variant only): the device address of the
+    // record's field array and the offset of this slice and pass in it (6 planes of nk)
+    double* const* rec_f = nullptr;
+    long rec_off = 0;
 };
 // the other slice's six values at point k (loaded by the rows kernel before it stores its own slice: the other
 // slice is never this one, so the loads need not wait behind those stores)

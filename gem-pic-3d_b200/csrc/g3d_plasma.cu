@@ -366,8 +366,12 @@ static uint64_t mix64h(uint64_t z) {
 
 // E and B of slice l; Fourier y: with the midpoint fields of slice `target` (l for the next pass of half-cell l,
 // l - 1 for the first pass of half-cell l - 1, -1: none) for the streaming gather
-static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true) {
+static void real_fields_slice(Ctx& c, int l, int target = -1, bool cols = true, long rec_slot = -1) {
     FmidOut fm;
+    if (rec_slot >= 0) {                              // the adjoint's record of the slice (exact fields)
+        fm.rec_f = &c.pl->recd.p->f;
+        fm.rec_off = 6 * long(c.nk) * rec_slot;
+    }
     if (target >= c.a && (c.yf || c.f32s) && c.pl->fmid.p) {   // free-hand y: the mixed form's FP32 gather only
         fm.out = c.pl->fmid.p;
         fm.other = (target == l ? l + 1 : l - 1) - c.a;
@@ -405,6 +409,10 @@ void march_plasma(Ctx& c, double s0, double s1) {
     auto ptr = [](const void* q) { return uint64_t(reinterpret_cast<uintptr_t>(q)); };
     const PlasmaPtrs pp = P.ptrs(c);
     const bool rec = P.rec_on && P.rec_step && P.rec_step(P.nstrm, P.fresh_last);   // the adjoint's record of this march
+    // the record written by the kernels that hold the values (the exact streaming variant and the exact midpoint rows),
+    // else by copy kernels of its own
+    const bool exact_fourier = !c.mixed && c.yf && c.Fd.p;
+    const bool rec_x = rec && exact_fourier && !P.any_ionizing && !c.laser.on, rec_fld = rec && exact_fourier;
     mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(uint64_t(rec)); mixk(ptr(P.recd.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));
@@ -423,8 +431,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
         // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
         launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
-        real_fields_slice(c, N - 1, N - 2);
-        if (rec) launch_record_fields(c, N - 1, passes - 1);
+        real_fields_slice(c, N - 1, N - 2, true, rec_fld ? long(passes) * (N - 1) + passes - 1 : -1);
+        if (rec && !rec_fld) launch_record_fields(c, N - 1, passes - 1);
 
         StreamArgs sa;
         sa.F = c.F.p; sa.g = c.geo(); sa.laser = c.laser; sa.sv = P.stepv.p; sa.zc = c.P.zeta_center;
@@ -435,6 +443,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.Fmid = c.yf || c.f32s ? static_cast<const void*>(P.fmid.p) : nullptr;   // null if never allocated
         sa.inv_dx = 1 / c.dx; sa.inv_dy = 1 / c.dy; sa.dep_norm = 0;
         sa.Fd = c.mixed ? nullptr : c.Fd.p;
+        sa.recd = rec_x ? P.recd.p : nullptr;
         sa.ext = c.ext;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
@@ -442,7 +451,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
             if (n == nhi) launch_slice_prologue(c, n, n >= 1 ? n - 1 : -1, 1, passes > 1 ? 1 : 0);
             const double wex = (n >= 1 && n + 1 <= N - 2 && have_dl)
                                    ? (cen[size_t(n)] - cen[size_t(n - 1)]) / (cen[size_t(n + 1)] - cen[size_t(n)]) : 0.0;
-            if (rec) launch_record_particles(c, n);
+            if (rec && !rec_x) launch_record_particles(c, n);
             for (int pass = 0; pass < passes; ++pass) {
                 if (fh) launch_pass_prologue(c, n, pass > 0 ? 1 : 0);
                 sa.n = n;
@@ -455,8 +464,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
                 if (!fh) {                     // rows of the current's spectra; columns, march and field columns fused
                     launch_stream_spectra_rows(c);
                     launch_pass_cols(c, D, n, extrap ? 1 : 0, wex, pass > 0 ? 1 : 0);
-                    real_fields_slice(c, n, pass + 1 < passes ? n : n - 1, false);
-                    if (rec) launch_record_fields(c, n, pass);
+                    real_fields_slice(c, n, pass + 1 < passes ? n : n - 1, false, rec_fld ? long(passes) * n + pass : -1);
+                    if (rec && !rec_fld) launch_record_fields(c, n, pass);
                 } else {
                     launch_stream_spectra(c);
                     launch_replace_pred(c, n, extrap ? 1 : 0, wex);

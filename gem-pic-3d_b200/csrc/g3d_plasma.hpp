@@ -54,6 +54,8 @@ struct StreamArgs {
     double dep_norm;           // 1 / (Delta h_n dx): the deposit factor of half-cell n per unit of q w dt (the mixed form's FP32 deposit)
     const double* Fd;          // exact fields (FP64 form, Fourier y, no ionization, no analytic wave): the F planes in FP64 for
                                // the gather of a particle that starts inside the half-cell (null: the float planes F)
+    const struct RecDev* recd; // the same variant, recording for the adjoint: the state of every particle entering half-cell n
+                               // (pass 0) into the record (null: none)
 };
 
 // The adjoint's record of one march, written by the recording slice loop (device pointers; rs the stride of a particle

@@ -455,6 +455,11 @@ __global__ void __launch_bounds__(NT) k_rf_rows(Geo g, const cpx* __restrict__ W
         for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
         if constexpr (XM) {
             const double dv[6] = {0.5 * (r1 + l1), 0.5 * (r2 + l2), z3.x, 0.5 * (l2 - r2), 0.5 * (r1 - l1), z3.y};
+            if (fm.rec_f) {                            // the adjoint's record of the slice
+                double* R = *fm.rec_f + fm.rec_off + long(row) * NX + p;
+#pragma unroll
+                for (int comp = 0; comp < 6; ++comp) R[comp * g.nk] = dv[comp];
+            }
             double2* o = reinterpret_cast<double2*>(fm.out) + 3 * (long(row) * NX + p);
             o[0] = make_double2(0.5 * (dv[0] + othd[u_][0]), 0.5 * (dv[1] + othd[u_][1]));
             o[1] = make_double2(0.5 * (dv[2] + othd[u_][2]), 0.5 * (dv[3] + othd[u_][3]));

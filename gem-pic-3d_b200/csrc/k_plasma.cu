@@ -382,6 +382,15 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double px_ = S.px[i], py_ = S.py[i], pz_ = S.pz[i], qm_ = S.qm[i];
     const double qw = S.q[i] * S.w[i];
     const double sTrap = c.sv->sTrap, s1 = c.sv->s1;
+    if constexpr (EX) {
+        if (c.recd && c.pass == 0) {                 // the adjoint's record: the state entering half-cell n
+            const RecDev R = *c.recd;
+            double* xr = R.x + 7 * R.rs * long(n + 1) + i;
+            xr[0] = x; xr[R.rs] = y; xr[2 * R.rs] = zeta; xr[3 * R.rs] = z;
+            xr[4 * R.rs] = px_; xr[5 * R.rs] = py_; xr[6 * R.rs] = pz_;
+            R.a[R.rs * long(n + 1) + i] = alive;
+        }
+    }
     if (alive == 6) {                 // waiting: joins the march inside the half-cell that holds its zeta
         if (zeta > zn) { alive = 1; if (!c.dry) S.alive[i] = 1; }
         else return d;
