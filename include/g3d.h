@@ -376,8 +376,9 @@ int64_t g3d_launch_count(const struct g3d_ctx* ctx);
  * (ky index j = 0..ny-1, kx = 0..nx/2, H = nx/2 + 1); NULL sets every a to 1. Takes effect at the next g3d_init. */
 int g3d_set_laser_modes(struct g3d_ctx* ctx, const double* coef);
 /* Exact fields (1) or not (0): the real fields are kept in FP64 beside the float F and the beam push gathers
- * from them; the differentiable forward of which central differences are taken. FP64 form; takes effect at the
- * next g3d_init. */
+ * from them (and, with a streaming plasma on the Fourier y grid, the streaming push: its midpoint fields and the
+ * gathers of particles joining inside a half-cell); the differentiable forward of which central differences are
+ * taken. FP64 form; takes effect at the next g3d_init. */
 int g3d_set_exact_fields(struct g3d_ctx* ctx, int32_t on);
 /* What grad_p of g3d_adjoint differentiates (no counterpart in the reference). G3D_ADJ_THROUGH_START (the default):
  * the momenta as loaded, before g3d_init, so the derivative runs through the start field the bunch makes (its
@@ -386,9 +387,15 @@ int g3d_set_exact_fields(struct g3d_ctx* ctx, int32_t on);
 #define G3D_ADJ_THROUGH_START 0
 #define G3D_ADJ_AFTER_START   1
 int g3d_set_adjoint_momenta(struct g3d_ctx* ctx, int32_t mode);
-/* The adjoint march, right after g3d_init (Fourier y, beam and grid lasers, no plasma, sponge 0, fixed window):
+/* The adjoint march, right after g3d_init (Fourier y, beam and grid lasers, sponge 0, fixed window):
  * nsteps s-steps forward with per-level checkpoints of the beam and the real fields, J = sum w p_z / sum w over
- * the live beam, then the reverse sweep. Out: *objective = J; grad_modes (NULL: skipped; needs
+ * the live beam, then the reverse sweep. With a streaming plasma (FP64 form with exact fields, no ionization, no
+ * analytic laser): the levels also keep the spectra, j0, js0 and the particles waiting to join the plasma, each
+ * march is recorded (its particles entering every half-cell, the slices' fields after every pass) and transposed;
+ * the records of all steps are kept when they fit in half the free device memory, else (or with the environment
+ * variable G3D_ADJ_RECOMPUTE set) each step is run again from its level in the reverse sweep. Trapping is kept as
+ * the forward took it (slow trapped electrons joining later marches are differentiated); a forward in which a
+ * particle joins the beam (fast trapped or restreamed) gives G3D_ERR_STATE. Out: *objective = J; grad_modes (NULL: skipped; needs
  * g3d_set_laser_modes) = dJ/d Re a + i dJ/d Im a per stored mode, 2 ny H doubles; grad_p (NULL: skipped) =
  * dJ/d(p_x, p_y, p_z) of every particle at s = 0, 3 np doubles [particle][component], through the s-steps and
  * (unless g3d_set_adjoint_momenta chose G3D_ADJ_AFTER_START) through the start field the bunch made at g3d_init
