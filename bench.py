@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--nzeta", type=int, default=None, help="profiling case: fewer slices (same window)")
     ap.add_argument("--particles", type=int, default=None, help="profiling case: fewer macro-particles")
     ap.add_argument("--replicas", action="store_true", help="N > 1 on workloads 1-2: replicas instead of one sharded run")
+    ap.add_argument("--adjoint-plasma", type=int, default=0, metavar="K",
+                    help="profiling case: only one adjoint evaluation of workload 4 with its plasma over K s-steps (after "
+                         "one untimed evaluation), printing its device time")
     return ap.parse_args()
 
 
@@ -850,9 +853,36 @@ def plasma_adjoint_check(eps, timed, central):
                     "the forward with level checkpoints only, each step run again in the reverse sweep"}
 
 
+def adjoint_plasma_case(K):
+    """One evaluation of the plasma adjoint on workload 4 (64 x 64 x 512, 65,536 electrons, plasma 0.005 n_c at 2 x 2 per
+    cell) over K s-steps, after an untimed one on the same context: a case for the profiler."""
+    import torch
+    from g3d import Simulation, configs
+    cfg = configs.config4(plasma=True, steps=K)
+    sim = Simulation(cfg)
+    sim.load_bunch()
+    p0 = sim.host_particles()
+    sim.set_laser_modes(None)
+    sim.set_exact_fields(True)
+    st = torch.cuda.ExternalStream(sim.stream_ptr())
+    for rep in range(2):
+        sim.set_particles(p0)
+        sim.init_fields()
+        sim.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        J, _, _ = sim.adjoint(K)
+        e1.record(st)
+        torch.cuda.synchronize()
+    sim.close()
+    print(json.dumps({"case": f"plasma adjoint, workload 4, {K} s-steps", "J": J, "adjoint_ms": e0.elapsed_time(e1)}))
+
+
 def main():
     a = parse()
-    if a.impl == "reference":
+    if a.adjoint_plasma:
+        adjoint_plasma_case(a.adjoint_plasma)
+    elif a.impl == "reference":
         run_reference_arm(a)
     else:
         run_g3d(a)
