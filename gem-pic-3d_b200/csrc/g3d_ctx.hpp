@@ -383,6 +383,7 @@ void set_particles(Ctx& c, const g3d_particle* v, long n);
 std::vector<g3d_particle> get_particles(Ctx& c);
 void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions);
 void march_plasma(Ctx& c, double s0, double s1);
+void reset_plasma_march(Ctx& c);   // g3d_init: no streaming current of level s0, no particle waiting to join
 void collect_restreaming(Ctx& c);
 void add_grid_lasers(Ctx& c);
 // The dynamic shared memory a kernel may use, raised to smem once per kernel and device (a host call per

@@ -848,6 +848,7 @@ static void check_kernel_errors(Ctx& c);
 static void init_fields(Ctx& c) {
     c.s = 0; c.istep = 0;
     c.fields_ready = true;
+    if (c.pl) reset_plasma_march(c);                 // a run starts with no streaming current and no waiting particle
     if (c.P.self_fields) {
         c.starting_ = true;
         if (c.nbunch > 1) comoving_fields_per_bunch(c);

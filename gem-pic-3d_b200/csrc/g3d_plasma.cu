@@ -275,6 +275,15 @@ static std::vector<g3d_particle> records_of(Ctx& c, const StrmDev& S, long n) {
     return out;
 }
 
+// The start of a run (g3d_init): the streaming current of level s0 is zero and no particle waits to join the march, as
+// in a new Simulation (src/sim_setup.cpp), also when the context ran before.
+void reset_plasma_march(Ctx& c) {
+    PlasmaState& P = *c.pl;
+    for (DevBuf<cpx>* b : {&P.js0x, &P.js0y, &P.js0z}) G3D_CUDA(cudaMemsetAsync(b->p, 0, b->bytes(), c.stream));
+    P.njb = 0;
+    P.joining.clear();
+}
+
 std::vector<g3d_particle> get_streaming(Ctx& c) {
     PlasmaState& P = *c.pl;
     long n = 0;

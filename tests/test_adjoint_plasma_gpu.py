@@ -122,6 +122,28 @@ def test_plasma_adjoint_stored_and_recomputed_records_agree(monkeypatch):
     assert np.linalg.norm(gp1 - gp2) <= 1e-10 * np.linalg.norm(gp1)
 
 
+def test_plasma_second_evaluation_on_the_same_context():
+    """g3d_set_particles + g3d_init start the next evaluation on the same context: the plasma starts afresh (no
+    streaming current of a level before, no trapped electron waiting from the last run), so the second evaluation
+    after a run that trapped electrons is the first one again."""
+    from g3d import Simulation
+    cfg = case(a0=1.0, charge_pC=1.0, steps=1)
+    s = Simulation(cfg)
+    s.load_bunch()
+    p0 = s.host_particles()
+    s.set_laser_modes(None)
+    s.set_exact_fields(True)
+    out = []
+    for _ in range(2):
+        s.set_particles(p0)
+        s.init_fields()
+        out.append(s.adjoint(cfg.steps))
+    s.close()
+    assert out[0][0] == out[1][0]
+    for k in (1, 2):
+        assert np.linalg.norm(out[0][k] - out[1][k]) <= 1e-12 * np.linalg.norm(out[0][k])
+
+
 def test_plasma_adjoint_refuses_what_it_does_not_differentiate():
     """The mixed form and ionization are refused with G3D_ERR_ARG before anything runs."""
     from g3d import G3DError, Simulation, configs
