@@ -243,6 +243,8 @@ struct Ctx {
     std::deque<std::array<double, 3>> cent_;     // centroid sums awaiting their step (window lag)
     // device, stream, launches, profiling
     int device = 0;                              // the CUDA device current at g3d_create; every call runs on it
+    std::shared_ptr<void> ckjob;                 // the asynchronous checkpoint in flight (g3d_host.cu), or none
+    DevBuf<unsigned char> ckpt_snap;             // its device copy of the state, kept for the next one
     cudaStream_t stream = nullptr;
     long launches = 0;
     bool profiling = false;

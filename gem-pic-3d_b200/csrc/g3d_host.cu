@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <random>
+#include <thread>
 #include "g3d_plasma.hpp"
 #include "g3d_shard.hpp"
 
@@ -1013,7 +1014,9 @@ template <class T>
 }
 }  // namespace
 
+static void checkpoint_wait(Ctx& c);
 static void write_checkpoint(Ctx& c, const char* path) {
+    checkpoint_wait(c);
     CkptHeader h{};
     std::memcpy(h.magic, MAGIC, 8);
     h.ranks = 1; h.rank = 0; h.N = c.N; h.a = c.a; h.b = c.b; h.ns = c.ns; h.nk = c.nk; h.nx = c.nx; h.ny = c.ny;
@@ -1049,7 +1052,214 @@ static void write_checkpoint(Ctx& c, const char* path) {
     if (std::rename(tmp.c_str(), path) != 0) throw Error(G3D_ERR_IO, std::string("cannot rename to ") + path);
 }
 
+// ---------------------------------------------------------------- asynchronous checkpoints
+// The checkpoint above stops the caller until the file is written: the arrays go to the host one by one with the
+// stream drained. The asynchronous one copies the state on the device, on the context's stream (so the next calls
+// may change the state at once), and a host thread of the library waits for that copy, brings it to the host plane by
+// plane, expands the half spectra to the reference's full layout on the host (as k_half_to_full does) and writes the
+// same file while the march goes on. One job per context; a new one, the synchronous checkpoints, g3d_checkpoint_wait
+// and g3d_destroy wait for the one in flight.
+struct CkptJob {
+    std::thread th;
+    int code = G3D_OK;
+    std::string msg;
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ready = nullptr;
+    ~CkptJob() {
+        if (th.joinable()) th.join();
+        if (ready) cudaEventDestroy(ready);
+        if (s2) cudaStreamDestroy(s2);
+    }
+};
+// the job in flight ends; its outcome (the error of a failed write is thrown here, once)
+static void checkpoint_wait(Ctx& c) {
+    if (!c.ckjob) return;
+    CkptJob& j = *static_cast<CkptJob*>(c.ckjob.get());
+    if (j.th.joinable()) j.th.join();
+    const int code = j.code;
+    const std::string msg = j.msg;
+    c.ckjob.reset();
+    if (code != G3D_OK) throw Error(code, msg);
+}
+
+static void write_checkpoint_async(Ctx& c, const char* path) {
+    checkpoint_wait(c);
+    auto job = std::make_shared<CkptJob>();
+    CkptJob& J = *job;
+    cudaStream_t st = c.stream;
+    // what the file holds, in its order: the spectra, js0, F, the particles, the joining list, the centroid history
+    struct Seg { size_t off, bytes; long planes; bool narrow; };
+    std::vector<Seg> spec;
+    size_t tot = 0;
+    auto add = [&](size_t bytes) { const size_t o = tot; tot += (bytes + 255) / 256 * 256; return o; };
+    const int ws[8] = {G3D_A_RX, G3D_A_RY, G3D_A_EZ, G3D_A_BZ, G3D_A_LX, G3D_A_LY, G3D_A_J0X, G3D_A_J0Y};
+    std::vector<ArrayRef> refs;
+    for (int w : ws) {
+        const ArrayRef a = array_ref(c, w);
+        const size_t b = a.count * (a.narrow ? sizeof(cpxf) : sizeof(cpx));
+        spec.push_back(Seg{add(b), b, a.planes, a.narrow});
+        refs.push_back(a);
+    }
+    const bool pl = c.pl != nullptr;
+    const size_t hb = size_t(c.ns + 1) * c.nkh * sizeof(cpx);
+    size_t ojs[3] = {0, 0, 0};
+    if (pl) for (int k = 0; k < 3; ++k) ojs[k] = add(hb);
+    const size_t oF = add(c.F.n * sizeof(float));
+    const long np = c.np;
+    const size_t oP = add(size_t(np) * sizeof(g3d_particle));
+    const long njb = pl ? c.pl->njb : 0;
+    const size_t oJ = add(size_t(njb) * (10 * 8 + 2 * 4 + 8));
+    if (c.ckpt_snap.n < tot) c.ckpt_snap.alloc(tot, st);
+    unsigned char* S = c.ckpt_snap.p;
+    for (size_t q = 0; q < spec.size(); ++q)
+        if (spec[q].bytes) G3D_CUDA(cudaMemcpyAsync(S + spec[q].off, refs[q].p, spec[q].bytes, cudaMemcpyDeviceToDevice, st));
+    if (pl) {
+        const cpx* js[3] = {c.pl->js0x.p, c.pl->js0y.p, c.pl->js0z.p};
+        for (int k = 0; k < 3; ++k) G3D_CUDA(cudaMemcpyAsync(S + ojs[k], js[k], hb, cudaMemcpyDeviceToDevice, st));
+    }
+    if (c.F.n) G3D_CUDA(cudaMemcpyAsync(S + oF, c.F.p, c.F.n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    if (np) {
+        if (c.pstage.n < size_t(np)) c.pstage.alloc(size_t(np) + size_t(np) / 4 + 64, st);
+        launch_parts_pack(c, np);
+        G3D_CUDA(cudaMemcpyAsync(S + oP, c.pstage.p, size_t(np) * sizeof(g3d_particle), cudaMemcpyDeviceToDevice, st));
+    }
+    if (njb) {                                        // the device joining list as columns: 10 doubles, alive, sp, id
+        const StrmDev& V = c.pl->jb.v;
+        const double* dc[10] = {V.x, V.y, V.zeta, V.px, V.py, V.pz, V.w, V.z, V.q, V.qm};
+        unsigned char* o = S + oJ;
+        for (int m = 0; m < 10; ++m, o += size_t(njb) * 8) G3D_CUDA(cudaMemcpyAsync(o, dc[m], size_t(njb) * 8, cudaMemcpyDeviceToDevice, st));
+        G3D_CUDA(cudaMemcpyAsync(o, V.alive, size_t(njb) * 4, cudaMemcpyDeviceToDevice, st)); o += size_t(njb) * 4;
+        G3D_CUDA(cudaMemcpyAsync(o, V.sp, size_t(njb) * 4, cudaMemcpyDeviceToDevice, st)); o += size_t(njb) * 4;
+        G3D_CUDA(cudaMemcpyAsync(o, V.id, size_t(njb) * 8, cudaMemcpyDeviceToDevice, st));
+    }
+    G3D_CUDA(cudaEventCreateWithFlags(&J.ready, cudaEventDisableTiming));
+    G3D_CUDA(cudaEventRecord(J.ready, st));
+    G3D_CUDA(cudaStreamCreateWithFlags(&J.s2, cudaStreamNonBlocking));
+    // the host values of the header and the rest, as they are now
+    CkptHeader h{};
+    std::memcpy(h.magic, MAGIC, 8);
+    h.ranks = 1; h.rank = 0; h.N = c.N; h.a = c.a; h.b = c.b; h.ns = c.ns; h.nk = c.nk; h.nx = c.nx; h.ny = c.ny;
+    h.plasma = pl ? 1 : 0;
+    h.istep = c.istep; h.lost = c.lost_total;
+    long trapped = 0, restreamed = 0;
+    get_plasma_counters(c, trapped, restreamed);
+    h.trapped = trapped; h.restreamed = restreamed;
+    h.s = c.s; h.X0 = c.X0; h.Y0 = c.Y0; h.beta_b = c.beta_b; h.gm2_b = c.gm2_b; h.stop = c.stop_; h.ncent = int(c.cent_.size());
+    std::vector<std::array<double, 3>> cent(c.cent_.begin(), c.cent_.end());
+    std::vector<g3d_particle> joining_host = pl ? c.pl->joining : std::vector<g3d_particle>();
+    const int dev = c.device, nx = c.nx, ny = c.ny, H = c.H, yf = c.yf ? 1 : 0;
+    const long nkh = c.nkh, nk = c.nk, fn = long(c.F.n);
+    const std::string out = path;
+    J.th = std::thread([&J, S, spec, ojs, oF, oP, oJ, np, njb, pl, h, cent, joining_host, dev, nx, ny, H, yf, nkh, nk, fn, hb, out]() {
+        FILE* f = nullptr;
+        const std::string tmp = out + ".tmp";
+        try {
+            G3D_CUDA(cudaSetDevice(dev));
+            G3D_CUDA(cudaEventSynchronize(J.ready));
+            f = std::fopen(tmp.c_str(), "wb");
+            if (!f) throw Error(G3D_ERR_IO, "cannot write " + tmp);
+            auto wr = [&](const void* p, size_t b) {
+                if (b && std::fwrite(p, 1, b, f) != b) throw Error(G3D_ERR_IO, "checkpoint: write error");
+            };
+            auto d2h = [&](void* dst, const unsigned char* src, size_t b) {
+                if (!b) return;
+                G3D_CUDA(cudaMemcpyAsync(dst, src, b, cudaMemcpyDeviceToHost, J.s2));
+                G3D_CUDA(cudaStreamSynchronize(J.s2));
+            };
+            wr(&h, sizeof h);
+            // the spectra: per plane the half spectrum widened and expanded to the full layout (k_half_to_full)
+            std::vector<cpx> half(static_cast<size_t>(nkh)), full(static_cast<size_t>(nk));
+            std::vector<cpxf> halff(static_cast<size_t>(nkh));
+            auto expand = [&](const std::vector<cpx>& hv) {
+                for (int j = 0; j < ny; ++j) {
+                    const int jm = yf ? (ny - j) % ny : j;
+                    for (int ix = 0; ix < nx; ++ix) {
+                        const cpx v = ix <= nx / 2 ? hv[size_t(j) * H + ix] : conj(hv[size_t(jm) * H + (nx - ix)]);
+                        full[size_t(j) * nx + ix] = v;
+                    }
+                }
+            };
+            for (const Seg& g : spec) {
+                const uint64_t cnt = uint64_t(g.planes) * uint64_t(nk);
+                wr(&cnt, sizeof cnt);
+                for (long q = 0; q < g.planes; ++q) {
+                    if (g.narrow) {
+                        d2h(halff.data(), S + g.off + size_t(q) * nkh * sizeof(cpxf), size_t(nkh) * sizeof(cpxf));
+                        for (long i = 0; i < nkh; ++i) half[size_t(i)] = to_d(halff[size_t(i)]);
+                    } else {
+                        d2h(half.data(), S + g.off + size_t(q) * nkh * sizeof(cpx), size_t(nkh) * sizeof(cpx));
+                    }
+                    expand(half);
+                    wr(full.data(), size_t(nk) * sizeof(cpx));
+                }
+            }
+            for (int k = 0; k < 3; ++k) {                 // js0: the streaming current of s0, full layout
+                const uint64_t cnt = pl ? uint64_t(hb / sizeof(cpx) / nkh) * uint64_t(nk) : 0;
+                wr(&cnt, sizeof cnt);
+                for (uint64_t q = 0; pl && q < uint64_t(hb / sizeof(cpx) / nkh); ++q) {
+                    d2h(half.data(), S + ojs[k] + size_t(q) * nkh * sizeof(cpx), size_t(nkh) * sizeof(cpx));
+                    expand(half);
+                    wr(full.data(), size_t(nk) * sizeof(cpx));
+                }
+            }
+            {                                             // F, in chunks
+                const uint64_t cnt = uint64_t(fn);
+                wr(&cnt, sizeof cnt);
+                std::vector<float> buf(size_t(1) << 22);
+                for (long o = 0; o < fn; o += long(buf.size())) {
+                    const size_t m = size_t(std::min<long>(long(buf.size()), fn - o));
+                    d2h(buf.data(), S + oF + size_t(o) * sizeof(float), m * sizeof(float));
+                    wr(buf.data(), m * sizeof(float));
+                }
+            }
+            {                                             // the particles
+                const uint64_t cnt = uint64_t(np);
+                wr(&cnt, sizeof cnt);
+                std::vector<g3d_particle> buf(size_t(1) << 16);
+                for (long o = 0; o < np; o += long(buf.size())) {
+                    const size_t m = size_t(std::min<long>(long(buf.size()), np - o));
+                    d2h(buf.data(), S + oP + size_t(o) * sizeof(g3d_particle), m * sizeof(g3d_particle));
+                    wr(buf.data(), m * sizeof(g3d_particle));
+                }
+            }
+            if (pl) {                                     // the joining list: the device's, then the host's
+                std::vector<unsigned char> raw(size_t(njb) * (10 * 8 + 2 * 4 + 8));
+                d2h(raw.data(), S + oJ, raw.size());
+                std::vector<g3d_particle> jv(static_cast<size_t>(njb));
+                const double* dc = reinterpret_cast<const double*>(raw.data());
+                const int32_t* ic = reinterpret_cast<const int32_t*>(raw.data() + size_t(njb) * 80);
+                const uint64_t* uc = reinterpret_cast<const uint64_t*>(raw.data() + size_t(njb) * 88);
+                for (long k = 0; k < njb; ++k) {
+                    g3d_particle& p = jv[size_t(k)];
+                    double* dst[10] = {&p.x, &p.y, &p.zeta, &p.px, &p.py, &p.pz, &p.w, &p.z, &p.q, &p.qm};
+                    for (int m = 0; m < 10; ++m) *dst[m] = dc[size_t(m) * njb + k];
+                    p.alive = ic[k]; p.sp = ic[njb + k]; p.id = uc[k];
+                }
+                jv.insert(jv.end(), joining_host.begin(), joining_host.end());
+                const uint64_t cnt = jv.size();
+                wr(&cnt, sizeof cnt);
+                wr(jv.data(), jv.size() * sizeof(g3d_particle));
+            } else {
+                const uint64_t cnt = 0;
+                wr(&cnt, sizeof cnt);
+            }
+            for (const auto& v : cent) { const uint64_t cnt = 3; wr(&cnt, sizeof cnt); wr(v.data(), 3 * sizeof(double)); }
+            if (std::fclose(f) != 0) { f = nullptr; throw Error(G3D_ERR_IO, "checkpoint: write error"); }
+            f = nullptr;
+            if (std::rename(tmp.c_str(), out.c_str()) != 0) throw Error(G3D_ERR_IO, "cannot rename to " + out);
+        } catch (const Error& e) {
+            if (f) std::fclose(f);
+            J.code = e.code; J.msg = e.what();
+        } catch (const std::exception& e) {
+            if (f) std::fclose(f);
+            J.code = G3D_ERR_IO; J.msg = e.what();
+        }
+    });
+    c.ckjob = job;
+}
+
 static void read_checkpoint(Ctx& c, const char* path) {
+    checkpoint_wait(c);
     FILE* f = std::fopen(path, "rb");
     if (!f) throw Error(G3D_ERR_IO, std::string("cannot read ") + path);
     try {
@@ -1569,6 +1779,7 @@ void g3d_destroy(g3d_ctx* ctx) {
     if (!ctx) return;
     Ctx& c = ctx->c;
     cudaSetDevice(c.device);
+    c.ckjob.reset();                 // an asynchronous checkpoint in flight ends first (its error is dropped)
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto& pe : c.pending) { cudaEventDestroy(pe.e0); cudaEventDestroy(pe.e1); }
     for (auto e : c.event_pool) cudaEventDestroy(e);
@@ -1826,6 +2037,14 @@ void* g3d_device_ptr(g3d_ctx* ctx, int32_t which) {
     return p;
 }
 
+int g3d_write_checkpoint_async(g3d_ctx* ctx, const char* path) {
+    return guarded(ctx, [&] {
+        if (!path) throw Error(G3D_ERR_ARG, "g3d_write_checkpoint_async: no path");
+        if (ctx->c.world > 1) throw Error(G3D_ERR_STATE, "checkpoints of a sharded run are not built");
+        g3d::write_checkpoint_async(ctx->c, path);
+    });
+}
+int g3d_checkpoint_wait(g3d_ctx* ctx) { return guarded(ctx, [&] { g3d::checkpoint_wait(ctx->c); }); }
 int g3d_write_checkpoint(g3d_ctx* ctx, const char* path) {
     return guarded(ctx, [&] {
         if (ctx->c.world > 1) throw Error(G3D_ERR_STATE, "checkpoints of a sharded run are not written");

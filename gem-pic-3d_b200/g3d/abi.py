@@ -168,6 +168,8 @@ SIGNATURES = [
     ("g3d_device_ptr", _P, [_P, _I32]),
     ("g3d_write_checkpoint", _I, [_P, C.c_char_p]),
     ("g3d_read_checkpoint", _I, [_P, C.c_char_p]),
+    ("g3d_write_checkpoint_async", _I, [_P, C.c_char_p]),
+    ("g3d_checkpoint_wait", _I, [_P]),
     ("g3d_stream", _P, [_P]),
     ("g3d_synchronize", _I, [_P]),
     ("g3d_profile_enable", _I, [_P, _I32]),

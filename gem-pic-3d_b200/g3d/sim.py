@@ -260,6 +260,14 @@ class Simulation:
     def read_checkpoint(self, path):
         self._c(self.lib.g3d_read_checkpoint(self.ctx, str(path).encode()))
 
+    def write_checkpoint_async(self, path):
+        """The checkpoint of write_checkpoint, written by a host thread of the library while the run goes on (the
+        state copied on the device first); checkpoint_wait() returns when the file is complete."""
+        self._c(self.lib.g3d_write_checkpoint_async(self.ctx, str(path).encode()))
+
+    def checkpoint_wait(self):
+        self._c(self.lib.g3d_checkpoint_wait(self.ctx))
+
     # ------------------------------------------------------------ stream, timing
     def stream_ptr(self):
         return self.lib.g3d_stream(self.ctx)

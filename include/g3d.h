@@ -357,6 +357,15 @@ void* g3d_device_ptr(struct g3d_ctx* ctx, int32_t which);
 /* Binary checkpoint of the reference (src/sim_checkpoint.cpp:9-58), one rank, bit-compatible. */
 int g3d_write_checkpoint(struct g3d_ctx* ctx, const char* path);
 int g3d_read_checkpoint(struct g3d_ctx* ctx, const char* path);
+/* Asynchronous checkpoint, the same file as g3d_write_checkpoint (no counterpart in the reference, whose checkpoint
+ * stops the run while it is written): the state is copied on the device on the context's stream, so the calls that
+ * follow (g3d_step ...) may change it at once, and a host thread of the library brings the copy to the host and writes
+ * the file (path + ".tmp", renamed to path when complete) while the march goes on. The copy takes device memory of about
+ * the state's size, kept for the next checkpoint. One at a time per context: a second call, g3d_write_checkpoint,
+ * g3d_read_checkpoint and g3d_checkpoint_wait wait for the one in flight; g3d_checkpoint_wait (and the next of these
+ * calls) returns its outcome (G3D_ERR_IO if the file could not be written); g3d_destroy waits for it too. */
+int g3d_write_checkpoint_async(struct g3d_ctx* ctx, const char* path);
+int g3d_checkpoint_wait(struct g3d_ctx* ctx);
 
 /* ------------------------------------------------------------------ stream, timing */
 /* The context's CUDA stream (a cudaStream_t) on which every kernel is launched. */
