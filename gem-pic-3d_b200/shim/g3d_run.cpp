@@ -6,8 +6,9 @@
 //
 // Written to output.dir: diag.txt and bunches.txt (the reference's columns, every output.every steps and the last;
 // the beam moments from the device), checkpoints
-// every output.checkpoint_every steps in the reference's layout and name (checkpoint_NNNNNN_r0000.bin; without a
-// plasma: the library checkpoints no streaming state), and
+// every output.checkpoint_every steps in the reference's layout and name (checkpoint_NNNNNN_r0000.bin, with the streaming
+// plasma's state; written by the library's host thread while the next steps run, the last one waited for before
+// "done"), and
 // "done: N steps, X s" on stdout. Field files, particle dumps, frames, openPMD and the other output groups of the
 // reference are not written, nor diag.txt's last column with mobile ions (the ion density on the axis, from charge
 // planes the library does not deposit). A deck key the library does not run stops it before any device work; exit codes as the
@@ -174,9 +175,10 @@ int main(int argc, char** argv) {
             sim.step();
             ++steps; ++istep;
             if (c.every > 0 && istep % c.every == 0) { diag_line(f, c, sim, false); bunches_lines(fb, c, sim, false); }
-            if (c.checkpoint_every > 0 && istep % c.checkpoint_every == 0 && !setup.plasma_on)
-                sim.write_checkpoint(checkpoint_name(c.dir, istep));
+            if (c.checkpoint_every > 0 && istep % c.checkpoint_every == 0)
+                sim.write_checkpoint_async(checkpoint_name(c.dir, istep));
         }
+        sim.checkpoint_wait();
         if (c.every <= 0 || istep % c.every) { diag_line(f, c, sim, false); bunches_lines(fb, c, sim, false); }
         std::fclose(f);
         if (fb) std::fclose(fb);

@@ -97,6 +97,11 @@ public:
     void shift_window(int nxs, int nys) { check(g3d_shift_window(ctx_, nxs, nys), ctx_, "shift_window"); }
     void write_checkpoint(const std::string& path) { check(g3d_write_checkpoint(ctx_, path.c_str()), ctx_, "write_checkpoint"); }
     void read_checkpoint(const std::string& path) { check(g3d_read_checkpoint(ctx_, path.c_str()), ctx_, "read_checkpoint"); }
+    // the same file written by the library's host thread while the run goes on; checkpoint_wait returns when it is done
+    void write_checkpoint_async(const std::string& path) {
+        check(g3d_write_checkpoint_async(ctx_, path.c_str()), ctx_, "write_checkpoint_async");
+    }
+    void checkpoint_wait() { check(g3d_checkpoint_wait(ctx_), ctx_, "checkpoint_wait"); }
     std::vector<g3d_particle> host_particles() {
         const int64_t n = status().np;
         std::vector<g3d_particle> v(size_t(n > 0 ? n : 0));

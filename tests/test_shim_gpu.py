@@ -111,6 +111,7 @@ bunch {{
 output {{
   dir = {out}
   every = 1
+  checkpoint_every = 2
   fields = none
   particles = false
 }}
@@ -258,6 +259,14 @@ def test_laser_wakefield_deck_matches_the_reference_cli(tmp_path):
     a, b = diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt")
     assert a.shape[0] >= 3
     diag_close(a, b, "lwfa")
+    # the checkpoint after step 2, with the streaming plasma's state (written here while the run went on)
+    ca = read_checkpoint(our_dir / "out" / "checkpoint_000002_r0000.bin")
+    cb = read_checkpoint(ref_dir / "out" / "checkpoint_000002_r0000.bin")
+    assert_state({k: ca[k] for k in FIELDS}, {k: cb[k] for k in FIELDS}, FIELDS, 1e-10, tag="checkpoint")
+    for k in ("js0x", "js0y", "js0z"):
+        assert rel_l2(ca[k], cb[k]) <= 1e-9, k
+    assert rel_l2(ca["F"], cb["F"]) <= 1e-6
+    assert len(ca["particles"]) == len(cb["particles"])
     bunches_close(bunches_rows(our_dir / "out" / "bunches.txt"), bunches_rows(ref_dir / "out" / "bunches.txt"), "lwfa")
 
 
