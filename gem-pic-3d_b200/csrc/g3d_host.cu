@@ -1353,8 +1353,9 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     if (!c.yf) throw Error(G3D_ERR_ARG, "the adjoint march needs the Fourier y grid");
     const bool plasma = c.pl != nullptr;
     if (plasma) {
-        if (c.mixed || !c.Fd.p)
-            throw Error(G3D_ERR_ARG, "the adjoint of the streaming plasma differentiates the FP64 form with exact fields (g3d_set_exact_fields)");
+        if (!c.mixed && !c.Fd.p)
+            throw Error(G3D_ERR_ARG, "the FP64 form's adjoint of the streaming plasma differentiates the forward with exact fields "
+                                     "(g3d_set_exact_fields)");
         if (c.pl->any_ionizing) throw Error(G3D_ERR_ARG, "the adjoint march does not differentiate ionization");
         if (c.pl->njb || !c.pl->joining.empty())
             throw Error(G3D_ERR_STATE, "the adjoint march starts with no particle waiting to join the streaming plasma");
@@ -1371,13 +1372,14 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     const long np = c.np;
     const size_t Fn = c.F.n, ns = size_t(c.ns), nkh = size_t(c.nkh), nk = size_t(c.nk);
     const bool ex = c.Fd.p != nullptr;
+    const bool fdl = ex || plasma;                   // the levels' real fields in FP64 (the mixed form's float F widened)
     cudaStream_t st = c.stream;
     // one workspace, kept between calls: the checkpoints of the K + 1 levels (beam x, y, zeta, p; alive; the real
     // fields), the adjoints of the spectra, currents, real fields and beam, and transform scratch
     size_t need = 0;
     auto carve = [&](size_t bytes) { const size_t o = need; need += (bytes + 255) / 256 * 256; return o; };
     const size_t oX = carve(size_t(K + 1) * 6 * size_t(np) * 8), oAL = carve(size_t(K + 1) * size_t(np) * 4);
-    const size_t oF = carve(size_t(K + 1) * Fn * (ex ? 8 : 4));
+    const size_t oF = carve(size_t(K + 1) * Fn * (fdl ? 8 : 4));
     size_t oS[6], oj0[2], ojk[3], oW[6];
     for (auto& o : oS) o = carve(ns * nkh * sizeof(cpx));
     for (auto& o : oj0) o = carve((ns + 1) * nkh * sizeof(cpx));
@@ -1398,8 +1400,8 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
     unsigned char* ws = c.adjws.p;
     double* X = reinterpret_cast<double*>(ws + oX);
     int32_t* AL = reinterpret_cast<int32_t*>(ws + oAL);
-    float* FF = ex ? nullptr : reinterpret_cast<float*>(ws + oF);
-    double* FD = ex ? reinterpret_cast<double*>(ws + oF) : nullptr;
+    float* FF = fdl ? nullptr : reinterpret_cast<float*>(ws + oF);
+    double* FD = fdl ? reinterpret_cast<double*>(ws + oF) : nullptr;
     cpx* lS[6]; cpx* lj0[2]; cpx* ljk[3]; cpx* W[6];
     for (int q = 0; q < 6; ++q) { lS[q] = reinterpret_cast<cpx*>(ws + oS[q]); W[q] = reinterpret_cast<cpx*>(ws + oW[q]); }
     for (int q = 0; q < 2; ++q) lj0[q] = reinterpret_cast<cpx*>(ws + oj0[q]);
@@ -1468,7 +1470,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
                 G3D_CUDA(cudaMemcpyAsync(x + size_t(q) * np, src[q], size_t(np) * 8, cudaMemcpyDeviceToDevice, st));
             G3D_CUDA(cudaMemcpyAsync(AL + size_t(k) * np, c.parts.alive, size_t(np) * 4, cudaMemcpyDeviceToDevice, st));
         }
-        if (plasma) plasma_state(k, true);
+        if (plasma && !c.mixed) plasma_state(k, true);   // the mixed form keeps the records: no step is run again
         sl[size_t(k)] = c.s;
     };
     // back to level k (the beam, the exact real fields, the plasma state, s), to run step k + 1 again
@@ -1560,6 +1562,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         ~Own() { c.Fd.p = fd; c.F.p = f; c.fd_next = nullptr; c.f_next = nullptr; }
     } own{c, c.Fd.p, c.F.p};
     if (ex) G3D_CUDA(cudaMemcpyAsync(FD, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+    else if (fdl) launch_f2d(c, c.F.p, FD, long(Fn));
     else G3D_CUDA(cudaMemcpyAsync(FF, c.F.p, Fn * 4, cudaMemcpyDeviceToDevice, st));
     save(0);
     for (int k = 1; k <= K; ++k) {
@@ -1568,7 +1571,8 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         if (plasma) {
             k_cur = k;
             step(c, false);
-            G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+            if (ex) G3D_CUDA(cudaMemcpyAsync(FD + size_t(k) * Fn, c.Fd.p, Fn * 8, cudaMemcpyDeviceToDevice, st));
+            else launch_f2d(c, c.F.p, FD + size_t(k) * Fn, long(Fn));
             npl_max = std::max(npl_max, c.pl->nstrm);
         } else {
             if (ex) c.fd_next = FD + size_t(k) * Fn;
@@ -1584,6 +1588,9 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
             throw Error(G3D_ERR_STATE, "the adjoint march does not differentiate particles that join the beam (fast trapped or "
                                        "restreamed ones), and the forward had some");
         c.pl->rec_on = false;
+        if (c.mixed && (!stored || overflow))
+            throw Error(G3D_ERR_CAPACITY, "the mixed form's adjoint of the streaming plasma keeps the records of every step, and "
+                                          "they do not fit in half the free device memory (or G3D_ADJ_RECOMPUTE is set)");
         if (!stored || overflow) {                    // one march's record, filled by running each step again
             stored = false;
             const long rs = npl_max;
@@ -1601,7 +1608,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         }
     }
     if (ex) G3D_CUDA(cudaMemcpyAsync(own.fd, FD + size_t(K) * Fn, Fn * 8, cudaMemcpyDeviceToDevice, st));
-    else G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
+    else if (!fdl) G3D_CUDA(cudaMemcpyAsync(own.f, FF + size_t(K) * Fn, Fn * 4, cudaMemcpyDeviceToDevice, st));
     c.Fd.p = own.fd; c.F.p = own.f;
     launch_adj_objective(c, jo);
     double jh[2];
@@ -1657,7 +1664,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         launch_adj_deposit(c, X + size_t(k) * 6 * np, AL + size_t(k) * np, lJ, lam);
         for (int q = 0; q < 2; ++q) std::swap(ljk[q], lj0[q]);           // jk of level k-1 as the j0 of step k
         if (!plasma) G3D_CUDA(cudaMemsetAsync(lF, 0, Fn * 8, st));
-        launch_adj_push(c, ex ? nullptr : FF + size_t(k - 1) * Fn, ex ? FD + size_t(k - 1) * Fn : nullptr, X + size_t(k - 1) * 6 * np,
+        launch_adj_push(c, fdl ? nullptr : FF + size_t(k - 1) * Fn, fdl ? FD + size_t(k - 1) * Fn : nullptr, X + size_t(k - 1) * 6 * np,
                         AL + size_t(k - 1) * np, sl[size_t(k - 1)], sl[size_t(k)], lam, lF, err);
     }
     // level 0: the real fields of the start field, then init's march(0) back to R with the lasers added
@@ -1710,7 +1717,7 @@ static void adjoint(Ctx& c, int K, double* J, double* grad_modes, double* grad_p
         for (long i = 0; i < np; ++i)
             for (int q = 0; q < 3; ++q) grad_p[3 * i + q] = h[size_t(q) * np + i];
     }
-    if (plasma) {                                     // the run as the forward left it, at level K
+    if (plasma && !stored) {                          // the run as the forward left it, at level K
         restore(K);
         launch_d2f(c, c.Fd.p, c.F.p, long(Fn));
     }

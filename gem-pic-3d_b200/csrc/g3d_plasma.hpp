@@ -208,6 +208,7 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
 long launch_join_adjoint_out(Ctx& c, const double* lam, long rs, long fresh, long n, double* jl);
 long launch_join_adjoint_in(Ctx& c, const RecDev& rec, long np, const double* jl, long njl, double* lam);
 void launch_d2f(Ctx& c, const double* a, float* b, long n);     // b = float(a)
+void launch_f2d(Ctx& c, const float* a, double* b, long n);     // b = double(a)
 
 // launchers (k_plasma.cu)
 void launch_record_particles(Ctx& c, int n);     // the adjoint's record of the particles entering half-cell n (-1: after)

@@ -569,6 +569,15 @@ void adjoint_march_plasma(Ctx& c, const AdjPlasmaWs& w, const AdjPlasmaPtrs& a, 
     G3D_CUDA(cudaGraphLaunch(P.adjg.exec, st));
 }
 
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, long n) {
+    for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = double(a[i]);
+}
+void launch_f2d(Ctx& c, const float* a, double* b, long n) {
+    if (n <= 0) return;
+    const long bl = (n + 255) / 256;
+    k_f2d<<<unsigned(bl < 148 * 16 ? bl : 148 * 16), 256, 0, c.stream>>>(a, b, n);
+    c.check_launch("k_f2d");
+}
 __global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long n) {
     for (long i = long(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += long(gridDim.x) * blockDim.x) b[i] = float(a[i]);
 }

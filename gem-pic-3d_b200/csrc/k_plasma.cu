@@ -1295,18 +1295,23 @@ void launch_record_particles(Ctx& c, int n) {
     k_rec_particles<<<ew_blocks(P.s.cap), 256, 0, c.stream>>>(P.sdev.p, P.nstrm_dev.p, P.recd.p, n, P.ion_dev.p);
     c.check_launch("k_rec_particles");
 }
-// ... and of the exact real fields of slice l after pass p
-__global__ void k_rec_fields(const RecDev* __restrict__ rd, const double* __restrict__ Fd, long fpl, long nk, long l, int passes, int p) {
+// ... and of the real fields of slice l after pass p (the exact FP64 planes, or the float F of the mixed form widened)
+template <class FT>
+__global__ void k_rec_fields(const RecDev* __restrict__ rd, const FT* __restrict__ Fd, long fpl, long nk, long l, int passes, int p) {
     double* f = rd->f + 6 * nk * (long(passes) * l + p);
     for (long e = long(blockIdx.x) * blockDim.x + threadIdx.x; e < 6 * nk; e += long(gridDim.x) * blockDim.x) {
         const long comp = e / nk, k = e - comp * nk;
-        f[e] = Fd[comp * fpl + l * nk + k];
+        f[e] = double(Fd[comp * fpl + l * nk + k]);
     }
 }
 void launch_record_fields(Ctx& c, int l, int p) {
     PlasmaState& P = *c.pl;
-    k_rec_fields<<<ew_blocks(6L * c.nk), 256, 0, c.stream>>>(P.recd.p, c.Fd.p, long(c.ns + 2) * c.nk, long(c.nk), long(l - c.a),
-                                                            P.cfg.iterations, p);
+    if (c.Fd.p)
+        k_rec_fields<double><<<ew_blocks(6L * c.nk), 256, 0, c.stream>>>(P.recd.p, c.Fd.p, long(c.ns + 2) * c.nk, long(c.nk),
+                                                                        long(l - c.a), P.cfg.iterations, p);
+    else
+        k_rec_fields<float><<<ew_blocks(6L * c.nk), 256, 0, c.stream>>>(P.recd.p, c.F.p, long(c.ns + 2) * c.nk, long(c.nk),
+                                                                       long(l - c.a), P.cfg.iterations, p);
     c.check_launch("k_rec_fields");
 }
 
