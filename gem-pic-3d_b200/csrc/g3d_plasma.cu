@@ -420,8 +420,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
     const bool rec = P.rec_on && P.rec_step && P.rec_step(P.nstrm, P.fresh_last);   // the adjoint's record of this march
     // the record written by the kernels that hold the values (the exact streaming variant and the exact midpoint rows),
     // else by copy kernels of its own
-    const bool exact_fourier = !c.mixed && c.yf && c.Fd.p;
-    const bool rec_x = rec && exact_fourier && !P.any_ionizing && !c.laser.on, rec_fld = rec && exact_fourier;
+    const bool rec_fourier = c.yf && (c.mixed || c.Fd.p);        // the exact FP64 forward or the mixed one
+    const bool rec_x = rec && rec_fourier && !P.any_ionizing && !c.laser.on, rec_fld = rec && rec_fourier;
     mixk(ptr(c.F.p)); mixk(ptr(c.Fd.p)); mixk(uint64_t(rec)); mixk(ptr(P.recd.p)); mixk(uint64_t(P.s.cap > 0)); mixk(uint64_t(P.born_cap));
     mixk(ptr(c.ext.u)); mixk(ptr(c.ext.m)); mixk(ptr(c.ext.kt)); mixk(uint64_t(c.ext.nu) << 32 | uint64_t(c.ext.nm));
     mixk(uint64_t(passes)); mixk(uint64_t(c.mixed) | uint64_t(c.f32s) << 1); mixk(ptr(c.Rx.p));

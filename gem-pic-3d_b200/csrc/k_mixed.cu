@@ -449,6 +449,11 @@ __global__ void __launch_bounds__(NT) k_rf_rows_f(Geo g, const cpxf* __restrict_
 #pragma unroll
         for (int comp = 0; comp < 6; ++comp) F[comp * fpl + idx] = fv[comp];
         if (fm.out) fmid_store(fm, long(row) * NX + p, fv, oth[u_]);
+        if (fm.rec_f) {                                // the adjoint's record of the slice (widened)
+            double* R = *fm.rec_f + fm.rec_off + long(row) * NX + p;
+#pragma unroll
+            for (int comp = 0; comp < 6; ++comp) R[comp * g.nk] = double(fv[comp]);
+        }
     }
 }
 

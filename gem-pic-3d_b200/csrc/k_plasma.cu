@@ -366,7 +366,8 @@ struct DepReq {
 // ION: some species ionizes (else the field magnitudes and the ADK sampling are left out); LASER: the analytic
 // plane wave is on. Both are fixed for a run; the variants without them hold fewer registers.
 // EX: exact fields (FP64 form, Fourier y, neither ionization nor the analytic wave): the gathers from the FP64 planes.
-template <bool F32, bool ION, bool LASER, bool YF, bool EX = false>
+// REC: the variant that writes the adjoint's record (c.recd, first pass), launched only when recording.
+template <bool F32, bool ION, bool LASER, bool YF, bool EX = false, bool REC = false>
 __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev& S, long i) {
     DepReq d{0, 0, 0, 0, 0, 0, false, false, 0.f, {0.f, 0.f, 0.f}};
     const Geo& g = c.g;
@@ -382,7 +383,7 @@ __device__ __forceinline__ DepReq stream_one(const StreamArgs& c, const StrmDev&
     const double px_ = S.px[i], py_ = S.py[i], pz_ = S.pz[i], qm_ = S.qm[i];
     const double qw = S.q[i] * S.w[i];
     const double sTrap = c.sv->sTrap, s1 = c.sv->s1;
-    if constexpr (EX) {
+    if constexpr (REC) {
         if (c.recd && c.pass == 0) {                 // the adjoint's record: the state entering half-cell n
             const RecDev R = *c.recd;
             double* xr = R.x + 7 * R.rs * long(n + 1) + i;
@@ -515,13 +516,13 @@ constexpr int ST_NT = 128;
 #endif
 // YF: the Fourier y grid (true) or the free-hand one, fixed for a run, so that each variant holds only its own grid's
 // gathers and deposits (fewer registers and no local arrays).
-template <bool F32, bool ION, bool LASER, bool YF, bool EX = false>
+template <bool F32, bool ION, bool LASER, bool YF, bool EX = false, bool REC = false>
 __global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c,
                                                                                        const long* __restrict__ nstrm) {
     const StrmDev S = c.sd[0];
     const long n = *nstrm;
     for (long i = long(blockIdx.x) * ST_NT + threadIdx.x; i < n; i += long(gridDim.x) * ST_NT) {
-        const DepReq d = stream_one<F32, ION, LASER, YF, EX>(c, S, i);
+        const DepReq d = stream_one<F32, ION, LASER, YF, EX, REC>(c, S, i);
         if (d.on) {
             if (F32 && YF && d.f32) sdeposit_f32(c, d.x, d.y, d.ff, d.fv[0], d.fv[1], d.fv[2]);
             else sdeposit<F32, YF>(c, d.x, d.y, d.f, d.vx, d.vy, d.vz);
@@ -533,8 +534,14 @@ static void stream_launch_y(Ctx& c, const StreamArgs& a, unsigned blocks) {
     PlasmaState& P = *c.pl;
     const bool ion = P.any_ionizing, las = c.laser.on != 0;
     if constexpr (!F32 && YF) {
-        if (a.Fd && !ion && !las) {
-            k_stream<false, false, false, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+        if (a.Fd && !ion && !las) {                  // exact fields (the adjoint's forward, writing its record when asked)
+            k_stream<false, false, false, true, true, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
+            return;
+        }
+    }
+    if constexpr (F32 && YF) {
+        if (a.recd && !ion && !las) {                // the mixed form's forward of the adjoint, writing its record
+            k_stream<true, false, false, true, false, true><<<blocks, ST_NT, 0, c.stream>>>(a, P.nstrm_dev.p);
             return;
         }
     }
