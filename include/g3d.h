@@ -398,11 +398,12 @@ int g3d_set_exact_fields(struct g3d_ctx* ctx, int32_t on);
 int g3d_set_adjoint_momenta(struct g3d_ctx* ctx, int32_t mode);
 /* The adjoint march, right after g3d_init (Fourier y, beam and grid lasers, sponge 0, fixed window):
  * nsteps s-steps forward with per-level checkpoints of the beam and the real fields, J = sum w p_z / sum w over
- * the live beam, then the reverse sweep. With a streaming plasma (FP64 form with exact fields, no ionization, no
- * analytic laser): the levels also keep the spectra, j0, js0 and the particles waiting to join the plasma, each
- * march is recorded (its particles entering every half-cell, the slices' fields after every pass) and transposed;
- * the records of all steps are kept when they fit in half the free device memory, else (or with the environment
- * variable G3D_ADJ_RECOMPUTE set) each step is run again from its level in the reverse sweep. Trapping is kept as
+ * the live beam, then the reverse sweep. With a streaming plasma (the FP64 form with exact fields or the mixed form; no
+ * ionization, no analytic laser): the levels also keep the spectra, j0, js0 and the particles waiting to join the
+ * plasma, each march is recorded (its particles entering every half-cell, the slices' fields after every pass) and
+ * transposed; the records of all steps are kept when they fit in half the free device memory, else (or with the
+ * environment variable G3D_ADJ_RECOMPUTE set) each step is run again from its level in the reverse sweep (the FP64
+ * form only: the mixed form then gives G3D_ERR_CAPACITY). Trapping is kept as
  * the forward took it (slow trapped electrons joining later marches are differentiated); a forward in which a
  * particle joins the beam (fast trapped or restreamed) gives G3D_ERR_STATE. Out: *objective = J; grad_modes (NULL: skipped; needs
  * g3d_set_laser_modes) = dJ/d Re a + i dJ/d Im a per stored mode, 2 ny H doubles; grad_p (NULL: skipped) =
