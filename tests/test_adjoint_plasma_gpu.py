@@ -13,7 +13,7 @@ Bound: relative difference <= 1e-6 between the adjoint's directional derivative 
 import numpy as np
 import pytest
 
-from test_adjoint_gpu import EPS, TOL, adjoint, central, forward, hermitian_direction, objective
+from test_adjoint_gpu import EPS, TOL, adjoint, autograd_inputs, central, forward, hermitian_direction, objective
 
 pytestmark = pytest.mark.gpu
 
@@ -161,6 +161,21 @@ def test_mixed_plasma_adjoint_against_central_differences_of_the_fp64_forward(a0
     print(f"mixed, a0 {a0}: laser modes {abs(al - fl) / abs(fl):.3e}, momenta {abs(am - fm) / abs(fm):.3e}")
     assert abs(al - fl) <= TOL * abs(fl), (al, fl)
     assert abs(am - fm) <= TOL * abs(fm), (am, fm)
+
+
+def test_autograd_gradcheck_with_trapped_electrons():
+    """torch.autograd.gradcheck through g3d.autograd.MarchObjective on the plasma case with trapping (fast mode: per
+    input one random direction, central difference at eps = 1e-6 against the adjoint's vector-Jacobian product,
+    relative tolerance 1e-6, no absolute tolerance)."""
+    import torch
+    from g3d.autograd import MarchObjective
+    cfg = case(a0=1.0, charge_pC=1.0)
+    coef, dp = autograd_inputs(cfg)
+    j0 = MarchObjective.apply(coef, dp, cfg, "fp64", True, True).item()
+
+    def fn(c, d):
+        return MarchObjective.apply(c, d, cfg, "fp64", True, True, j0)
+    assert torch.autograd.gradcheck(fn, (coef, dp), eps=EPS, atol=0.0, rtol=TOL, fast_mode=True)
 
 
 def test_plasma_adjoint_refuses_what_it_does_not_differentiate():
