@@ -20,6 +20,8 @@ constexpr double c_SI = 299792458.0, e_SI = 1.602176634e-19, me_SI = 9.109383701
 thread_local std::string g_create_err;
 
 bool pow2_ok(int n) { return n >= 4 && n <= 512 && (n & (n - 1)) == 0; }
+// the transverse sizes the transforms take: a power of two in 4..512, or three times one in 24..384 (k_fft.cuh)
+bool fft_size_ok(int n) { return pow2_ok(n) || (n % 3 == 0 && n >= 24 && n <= 384 && ((n / 3) & (n / 3 - 1)) == 0); }
 }  // namespace
 
 // ---------------------------------------------------------------- context plumbing
@@ -365,8 +367,9 @@ void realloc_slab(Ctx& c) {
 
 static void setup(Ctx& c, const g3d_grid& G, const g3d_params& P) {
     if (!G.y_fourier && !G.ynode) throw Error(G3D_ERR_ARG, "free-hand y needs the ny + 1 nodes (ynode)");
-    if (!pow2_ok(G.nx) || G.nx < 8 || (G.y_fourier && !pow2_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 512)))
-        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512; ny one in 4..512 (Fourier y) or 3..512 (free-hand)");
+    if (!fft_size_ok(G.nx) || G.nx < 8 || (G.y_fourier && !fft_size_ok(G.ny)) || (!G.y_fourier && (G.ny < 3 || G.ny > 512)))
+        throw Error(G3D_ERR_ARG, "nx must be a power of two in 8..512 or three times one in 24..384; ny likewise (4..512, Fourier y) "
+                                 "or 3..512 (free-hand)");
     if (G.nzeta < 4 || !G.zeta) throw Error(G3D_ERR_ARG, "nzeta must be >= 4 with a zeta table");
     if (!(G.Lx > 0) || !(G.Ly > 0)) throw Error(G3D_ERR_ARG, "Lx, Ly must be positive");
     if (P.precision != G3D_FP64 && P.precision != G3D_MIXED) throw Error(G3D_ERR_ARG, "precision must be G3D_FP64 or G3D_MIXED");

@@ -339,7 +339,7 @@ static bool cur_maps(Ctx& c) {
 template <int NY>
 static void cur_cols(Ctx& c, bool keep0) {
     constexpr int CW = 8;
-    if constexpr (NY <= 256) {
+    if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) {
         if (c.use_tma && cur_maps(c)) {
             const size_t smem = size_t(3) * NY * 8 * sizeof(cpx) + 128;
             smem_attr(reinterpret_cast<const void*>(k_cur_cols_tma<NY>), smem);

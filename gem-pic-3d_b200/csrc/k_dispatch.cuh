@@ -1,4 +1,5 @@
-// Run-time dispatch of a power-of-two transform length onto the compile-time FFT kernels.
+// Run-time dispatch of a transform length (a power of two in 4..512, or three times one in 24..384) onto the
+// compile-time FFT kernels.
 #pragma once
 
 #define G3D_CASE_N(VAL, NAME, ...) \
@@ -17,5 +18,10 @@
         G3D_CASE_N(128, NAME, __VA_ARGS__)                                                             \
         G3D_CASE_N(256, NAME, __VA_ARGS__)                                                             \
         G3D_CASE_N(512, NAME, __VA_ARGS__)                                                             \
-        default: throw ::g3d::Error(G3D_ERR_ARG, "transverse sizes must be powers of two in 4..512"); \
+        G3D_CASE_N(24, NAME, __VA_ARGS__)                                                              \
+        G3D_CASE_N(48, NAME, __VA_ARGS__)                                                              \
+        G3D_CASE_N(96, NAME, __VA_ARGS__)                                                              \
+        G3D_CASE_N(192, NAME, __VA_ARGS__)                                                             \
+        G3D_CASE_N(384, NAME, __VA_ARGS__)                                                             \
+        default: throw ::g3d::Error(G3D_ERR_ARG, "transverse sizes must be powers of two in 4..512 or three times one in 24..384"); \
     }

@@ -1,13 +1,15 @@
-// Hand-written batched FFT of power-of-two lengths 4..512 on lines held in shared memory.
+// Hand-written batched FFT of lengths 4..512 that are powers of two or three times a power of two (24..384), on lines
+// held in shared memory.
 //
 // Algorithm: self-sorting Stockham, decimation in time. A length-N transform is a sequence of passes
 // with radices R (the product of the radices of the earlier passes is L, m = N / (L R)); butterfly
 // b = j L + k of a pass reads x[(q m + j) L + k], q < R, multiplies by exp(-2 pi i q k / (L R)), takes the
 // length-R DFT and writes y[(j R + r) L + k], r < R. The passes here are one radix-2 or radix-4 pass
 // (when log2 N is not a multiple of 3; it comes first, where the twiddles are all 1) followed by radix-8
-// passes. Every thread owns E = min(N, 8) values of a line in registers during a pass; a line is worked
-// by N / E threads. The pass reads its inputs, synchronises the CTA, writes its outputs and synchronises
-// again, so a line is transformed in place.
+// passes. A length 3 * 2^k takes a radix-3 pass first, then a radix-2 pass when k is odd, then radix-4 passes.
+// Every thread owns E values of a line in registers during a pass (min(N, 8) for a power of two, 12 for three times
+// one); a line is worked by N / E threads. The pass reads its inputs, synchronises the CTA, writes its outputs and
+// synchronises again, so a line is transformed in place.
 //
 // The forward transform has the sign -1 and is unnormalised; the inverse is taken as
 // conj(forward(conj(x))) by the callers, who also apply the 1/N factors (the reference's convention,
@@ -18,15 +20,21 @@
 namespace g3d {
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+constexpr bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+// the transform lengths of the library: powers of two in 4..512, three times a power of two in 24..384
+constexpr bool fft_length_ok(int n) { return (is_pow2(n) && n >= 4 && n <= 512) || (n % 3 == 0 && is_pow2(n / 3) && n >= 24 && n <= 384); }
 
 template <int N>
 struct FftShape {
-    static_assert(N >= 4 && N <= 512 && (N & (N - 1)) == 0, "FFT length must be a power of two in 4..512");
-    static constexpr int E = N < 8 ? N : 8;                 // values per thread
+    static_assert(fft_length_ok(N), "FFT length must be a power of two in 4..512 or three times one in 24..384");
+    static constexpr bool P3 = !is_pow2(N);                 // a radix-3 pass first
+    static constexpr int B = P3 ? N / 3 : N;                // the power-of-two part
+    static constexpr int LOG = ilog2(B);
+    static constexpr int E = P3 ? 12 : (N < 8 ? N : 8);     // values per thread
     static constexpr int T = N / E;                         // threads per line
-    static constexpr int LOG = ilog2(N);
-    static constexpr int REM = N < 8 ? N : (1 << (LOG % 3));   // radix of the first pass (1: none)
-    static constexpr int NR8 = N < 8 ? 0 : LOG / 3;            // radix-8 passes
+    static constexpr int REM = P3 ? ((LOG & 1) ? 2 : 1) : (N < 8 ? N : (1 << (LOG % 3)));   // radix of the next pass (1: none)
+    static constexpr int NR8 = P3 ? 0 : (N < 8 ? 0 : LOG / 3);   // radix-8 passes (powers of two)
+    static constexpr int NR4 = P3 ? LOG / 2 : 0;                 // radix-4 passes (three times a power of two)
 };
 
 // ---------------------------------------------------------------- small DFTs (forward, sign -1)
@@ -35,6 +43,16 @@ template <class T>
 __device__ __forceinline__ void dft2(T* v) {
     const T a = v[0], b = v[1];
     v[0] = a + b; v[1] = a - b;
+}
+// length 3: with w = exp(-2 pi i / 3) = -1/2 - i sqrt(3)/2, y1,2 = a - (b + c)/2 -+ i (sqrt(3)/2) (b - c)
+template <class T>
+__device__ __forceinline__ void dft3(T* v) {
+    typedef typename RealOf<T>::type Re;
+    const Re h = Re(0.86602540378443864676);                 // sqrt(3) / 2
+    const T s = v[1] + v[2], d = v[1] - v[2];
+    const T m = mk<T>(v[0].x - Re(0.5) * s.x, v[0].y - Re(0.5) * s.y);
+    const T r = mk<T>(h * d.y, -h * d.x);                    // -i (sqrt(3)/2) (b - c)
+    v[0] = v[0] + s; v[1] = m + r; v[2] = m - r;
 }
 template <class T>
 __device__ __forceinline__ void dft4(T* v) {
@@ -61,6 +79,7 @@ __device__ __forceinline__ void dft8(T* v) {
 template <int R, class T>
 __device__ __forceinline__ void dft(T* v) {
     if constexpr (R == 2) dft2(v);
+    else if constexpr (R == 3) dft3(v);
     else if constexpr (R == 4) dft4(v);
     else dft8(v);
 }
@@ -99,7 +118,10 @@ template <int N, class Addr, class T>
 __device__ __forceinline__ void fft_line(T* sm, const Addr& A, int t, const T* __restrict__ tw) {
     using S = FftShape<N>;
     int L = 1;
+    if constexpr (S::P3) { fft_pass<N, 3>(sm, A, t, L, tw); L *= 3; }
     if constexpr (S::REM > 1) { fft_pass<N, S::REM>(sm, A, t, L, tw); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR4; ++s) { fft_pass<N, 4>(sm, A, t, L, tw); L *= 4; }
 #pragma unroll
     for (int s = 0; s < S::NR8; ++s) { fft_pass<N, 8>(sm, A, t, L, tw); L *= 8; }
 }
@@ -149,7 +171,10 @@ template <int N, int NL, class Addr, class T>
 __device__ __forceinline__ void fft_lines(T* const* sm, const Addr& A, int t, const T* __restrict__ tw) {
     using S = FftShape<N>;
     int L = 1;
+    if constexpr (S::P3) { fft_pass_multi<N, 3, NL>(sm, A, t, L, tw); L *= 3; }
     if constexpr (S::REM > 1) { fft_pass_multi<N, S::REM, NL>(sm, A, t, L, tw); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR4; ++s) { fft_pass_multi<N, 4, NL>(sm, A, t, L, tw); L *= 4; }
 #pragma unroll
     for (int s = 0; s < S::NR8; ++s) { fft_pass_multi<N, 8, NL>(sm, A, t, L, tw); L *= 8; }
 }
@@ -203,7 +228,10 @@ template <int N, int NL, class Addr, class T>
 __device__ __forceinline__ void fft_lines_some(T* const* sm, const Addr& A, int t, const T* __restrict__ tw, bool act) {
     using S = FftShape<N>;
     int L = 1;
+    if constexpr (S::P3) { fft_pass_multi_some<N, 3, NL>(sm, A, t, L, tw, act); L *= 3; }
     if constexpr (S::REM > 1) { fft_pass_multi_some<N, S::REM, NL>(sm, A, t, L, tw, act); L *= S::REM; }
+#pragma unroll
+    for (int s = 0; s < S::NR4; ++s) { fft_pass_multi_some<N, 4, NL>(sm, A, t, L, tw, act); L *= 4; }
 #pragma unroll
     for (int s = 0; s < S::NR8; ++s) { fft_pass_multi_some<N, 8, NL>(sm, A, t, L, tw, act); L *= 8; }
 }

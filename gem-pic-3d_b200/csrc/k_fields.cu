@@ -484,7 +484,7 @@ static unsigned col_tiles(const Ctx& c) { return unsigned((c.H + CW - 1) / CW); 
 
 template <int NY>
 static void sp_cols_inv(Ctx& c) {
-    if constexpr (NY <= 256) {
+    if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) {
         const cpx* p[2] = {c.Rx.p, c.Ry.p};
         if (c.use_tma && c.tma_spi.get(p, 2, c.H, long(c.ns) * c.ny, c.ny)) {
             const size_t smem = size_t(2) * NY * 8 * sizeof(cpx) + 128;
@@ -517,7 +517,7 @@ static void sp_rows(Ctx& c) {
 }
 template <int NY>
 static void sp_cols_fwd(Ctx& c) {
-    if constexpr (NY <= 256) {
+    if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) {
         const cpx* p[3] = {c.W[0].p, c.W[1].p, c.W[3].p};
         if (c.use_tma && c.tma_spf.get(p, 3, c.H, long(c.ns) * c.ny, c.ny)) {
             const size_t smem = size_t(3) * NY * 8 * sizeof(cpx) + 128;
@@ -575,7 +575,7 @@ template <int NY>
 static void rf_cols(Ctx& c, int l0, int nl) {
     if (nl == 1) rf_cols_w<NY, 2>(c, l0, nl);
     else if (c.use_tma && rf_maps(c)) {
-        if constexpr (NY <= 256) rf_cols_tma<NY>(c, l0, nl);
+        if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) rf_cols_tma<NY>(c, l0, nl);
     } else rf_cols_w<NY, CW>(c, l0, nl);
 }
 template <int NX>

@@ -74,7 +74,7 @@ def test_create_reports_missing_device_or_bad_grid():
     from g3d import abi, configs
     lib = abi.load_library()
     cfg = configs.config1(nx=16, ny=16, nzeta=8, nmacro=10)
-    cfg.nx = 12                                 # not a power of two
+    cfg.nx = 12                                 # neither a power of two in 8..512 nor three times one in 24..384
     g, z = cfg.grid_struct()
     p = cfg.params_struct()
     h = C.c_void_p()
