@@ -573,10 +573,11 @@ static void rf_cols_tma(Ctx& c, int l0, int nl) {
 }
 template <int NY>
 static void rf_cols(Ctx& c, int l0, int nl) {
-    if (nl == 1) rf_cols_w<NY, 2>(c, l0, nl);
-    else if (c.use_tma && rf_maps(c)) {
-        if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) rf_cols_tma<NY>(c, l0, nl);
-    } else rf_cols_w<NY, CW>(c, l0, nl);
+    if (nl == 1) { rf_cols_w<NY, 2>(c, l0, nl); return; }
+    if constexpr (NY <= 256 && (NY & (NY - 1)) == 0) {
+        if (c.use_tma && rf_maps(c)) { rf_cols_tma<NY>(c, l0, nl); return; }
+    }
+    rf_cols_w<NY, CW>(c, l0, nl);
 }
 template <int NX>
 static void rf_rows(Ctx& c, int l0, int nl, FmidOut fm = FmidOut()) {
