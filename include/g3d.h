@@ -189,7 +189,9 @@ typedef struct g3d_status {
 
 /* ------------------------------------------------------------------ lifetime */
 /* Creates a context on the current CUDA device: device buffers of the reference layouts,
- * k-tables, zeta weights. Replaces Simulation::Simulation (src/sim_setup.cpp:5-60). */
+ * k-tables, zeta weights. Replaces Simulation::Simulation (src/sim_setup.cpp:5-60). Transverse
+ * sizes: nx a power of two in 8..512 or three times one in 24..384; ny the same (from 4) with
+ * Fourier y, 3..512 with free-hand y; any other size is G3D_ERR_ARG. */
 int g3d_create(const g3d_grid* grid, const g3d_params* params, struct g3d_ctx** out);
 void g3d_destroy(struct g3d_ctx* ctx);
 /* Message of the last failed call on this context (or of the last failed g3d_create when
