@@ -900,6 +900,11 @@ static void check_kernel_errors(Ctx& c) {
 // mixed form's (complex64 spectra, float jw) while the boundary keeps the reference's complex128 / double.
 struct ArrayRef { void* p; size_t count, eb; long planes; bool narrow; };
 static ArrayRef array_ref(Ctx& c, int which) {
+    if (which == G3D_A_RHO_E || which == G3D_A_RHO_I) {            // the density lines of the plasma march
+        const size_t nl = size_t(c.N) * size_t(c.nx + c.ny);
+        if (!c.pl || (which == G3D_A_RHO_I && !c.pl->ion_lines)) return ArrayRef{nullptr, 0, sizeof(double), 0, false};
+        return ArrayRef{c.pl->rhol.p + (which == G3D_A_RHO_I ? nl : 0), nl, sizeof(double), 0, false};
+    }
     if (c.mixed && which != G3D_A_RX && which != G3D_A_RY && which != G3D_A_F) {
         DevBuf<cpxf>* cb = nullptr;
         long planes = c.ns;

@@ -99,6 +99,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
         if (s.ionization && (int(s.ip_eV.size()) < s.Zmax || s.Zmax <= s.Z0))
             throw Error(G3D_ERR_ARG, "ion: ionization needs Zmax > Z0 and Zmax ionization energies");
         pl->ions.push_back(s);
+        if (s.loaded()) pl->ion_lines = true;
     }
     cudaStream_t s = c.stream;
     const size_t ph = size_t(c.nkh);
@@ -106,6 +107,7 @@ void set_plasma(Ctx& c, const g3d_plasma& P, const g3d_ion* ions, int nions) {
     pl->jsr.alloc(size_t(5) * c.nk, s);
     pl->jsrf.alloc(size_t(5) * c.nk, s);               // FP32: three planes, or on the Fourier y grid (jx, jy, jz, 0) per point
     if (c.yf || c.f32s) pl->fmid.alloc(size_t(6) * c.nk, s);      // 6 doubles or 8 floats per point
+    pl->rhol.alloc(size_t(pl->ion_lines ? 2 : 1) * size_t(c.N) * size_t(c.nx + c.ny), s);
     pl->stepv.alloc(1, s);
     for (DevBuf<cpx>* b : {&pl->jsn, &pl->jsin, &pl->jpred, &pl->jtmp, &pl->jsi0, &pl->dlt, &pl->tsp}) b->alloc(3 * ph, s);
     pl->bk.alloc(4 * ph, s);
@@ -402,8 +404,11 @@ void march_plasma(Ctx& c, double s0, double s1) {
     std::vector<double> cen(size_t(N - 1));
     for (int m = 0; m < N - 1; ++m) cen[size_t(m)] = 0.5 * (c.zeta[size_t(m)] + c.zeta[size_t(m + 1)]);
     // the values that change from step to step go to the device; the captured loop reads them there
+    // the box column and row through the axis (src/sim_plasma.cpp:364-366)
+    const int i0 = ((int(std::lround(-c.X0 / c.dx)) % c.nx) + c.nx) % c.nx;
+    const int j0 = c.yf ? ((int(std::lround(-c.Y0 / c.dy)) % c.ny) + c.ny) % c.ny : c.ny / 2;
     const StepVals stv{s1, s1 + (P.cfg.trap_advance - 1) * Delta, c.X0, c.Y0,
-                       mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep))};   // ion_key_step
+                       mix64h(P.cfg.seed * 0x9E3779B97F4A7C15ULL + uint64_t(c.istep)), i0, j0};   // ion_key_step
     G3D_CUDA(cudaMemcpyAsync(P.stepv.p, &stv, sizeof(StepVals), cudaMemcpyHostToDevice, c.stream));
     const bool ionz = P.born_cap > 0;
     const int passes = P.cfg.iterations;
@@ -437,6 +442,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         if (c.f32s) G3D_CUDA(cudaMemsetAsync(P.jsrf.p, 0, size_t(c.yf ? 4 : 3) * c.nk * sizeof(float), c.stream));
         else G3D_CUDA(cudaMemsetAsync(P.jsr.p, 0, size_t(3) * c.nk * sizeof(double), c.stream));
         G3D_CUDA(cudaMemsetAsync(P.bcnt.p, 0, sizeof(int), c.stream));
+        G3D_CUDA(cudaMemsetAsync(P.rhol.p, 0, P.rhol.n * sizeof(double), c.stream));
         // front: half-cell N-2 predicted with its value of level s0; the front slice solved with it
         launch_slice_prologue(c, N - 1, N - 2, 0, 0);
         launch_march_slice(c, D, N - 1);
@@ -454,6 +460,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         sa.Fd = c.mixed ? nullptr : c.Fd.p;
         sa.recd = rec_x ? P.recd.p : nullptr;
         sa.ext = c.ext;
+        const long nl = long(c.nx) + c.ny;
         for (int n = nhi; n >= c.a; --n) {
             // sin, si0 <- pin; the prediction of half-cell n-1 from its level s0; the slice saved for the passes
             // (for the half-cells below the first, fused into the correction of the half-cell above)
@@ -467,6 +474,8 @@ void march_plasma(Ctx& c, double s0, double s1) {
                 sa.dep_norm = 1 / (Delta * (c.zeta[size_t(n) + 1] - c.zeta[size_t(n)]) * c.dx);
                 sa.pass = pass;
                 sa.dry = pass + 1 < passes ? 1 : 0;
+                sa.rl[0] = sa.dry ? nullptr : P.rhol.p + long(n) * nl;
+                sa.rl[1] = sa.dry || !P.ion_lines ? nullptr : P.rhol.p + (long(N) + n) * nl;
                 launch_stream(c, sa);
                 // freed electrons join the march (after the last pass's stream, before its rows kernel clears the count)
                 if (ionz && pass + 1 == passes) launch_born_append(c);

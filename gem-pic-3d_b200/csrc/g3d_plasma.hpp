@@ -28,6 +28,7 @@ struct StrmDev {
 struct StepVals {
     double s1, sTrap, X0, Y0;
     uint64_t key_step;         // ion_key_step(seed, istep)
+    int i0, j0;                // the box column and row through the axis x = 0, y = 0 (the density lines)
 };
 
 struct StreamArgs {
@@ -56,6 +57,8 @@ struct StreamArgs {
                                // the gather of a particle that starts inside the half-cell (null: the float planes F)
     const struct RecDev* recd; // the same variant, recording for the adjoint: the state of every particle entering half-cell n
                                // (pass 0) into the record (null: none)
+    double* rl[2];             // the last pass: the charge of the negative [0] and the positive [1] particles on the lines
+                               // through the axis of half-cell n (row j0: nx values, column i0: ny values), or null
 };
 
 // The adjoint's record of one march, written by the recording slice loop (device pointers; rs the stride of a particle
@@ -124,6 +127,10 @@ struct PlasmaState {
     DevBuf<double> jsr;                        // 5 real planes
     DevBuf<float> jsrf;                        // the same in FP32 (the mixed form)
     DevBuf<double> fmid;                       // the fields half-way through the half-cell, interleaved per point
+    // the charge of the streaming particles of every half-cell n on the lines through the axis [N][nx + ny] (row j0,
+    // column i0), deposited by the last pass: the negative particles, then (ion_lines) the positive ones
+    DevBuf<double> rhol;
+    bool ion_lines = false;                    // some ion species is loaded (mobile or ionizing)
     DevBuf<cpx> jsn, jsin, jpred, jtmp, jsi0, dlt, tsp;   // 3 half planes each
     DevBuf<cpx> bk;                            // 4 half planes: R_x, R_y, E_z, B_z of the slice
     StrmBuf s, bn;                             // streaming particles, the freed electrons

@@ -224,6 +224,27 @@ __device__ __forceinline__ void sgather_mid_fh_f32(const StreamArgs& c, double x
     }
     E[0] = a[0]; E[1] = a[1]; E[2] = a[2]; B[0] = a[3]; B[1] = a[4]; B[2] = a[5];
 }
+// The charge of a particle's TSC points on the lines through the axis of half-cell n (the density lines,
+// src/sim_plasma.cpp:363-374, of the charge planes that stream_deposit fills, src/sim_stream.hpp:33-64): the points of
+// row j0 at their column, those of column i0 at nx + their row. W(u, v) is the charge of point (ix[u], jn[v]); a point
+// with jn[v] < 0 has none. Negative particles go to rl[0], positive ones to rl[1] (null: not recorded).
+template <typename T, typename Wf>
+__device__ __forceinline__ void sdeposit_lines(const StreamArgs& c, T f, const int ix[3], const int jn[3], Wf W) {
+    double* rl = c.rl[f < T(0) ? 0 : 1];
+    if (!rl) return;
+    const int i0 = c.sv->i0, j0 = c.sv->j0;
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+        if (jn[v] == j0)
+#pragma unroll
+            for (int u = 0; u < 3; ++u) atomicAdd(rl + ix[u], double(W(u, v)));
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+        if (ix[u] == i0)
+#pragma unroll
+            for (int v = 0; v < 3; ++v)
+                if (jn[v] >= 0) atomicAdd(rl + c.g.nx + jn[v], double(W(u, v)));
+}
 // The mixed form's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
 __device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, double y, float f, float vx, float vy, float vz) {
     int ix[3], jn[3]; float wx[3], wn[3];
@@ -238,16 +259,18 @@ __device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, doub
             const float w = fa * wx[u] * wn[v];
             atomicAdd(J4 + long(jn[v]) * c.g.nx + ix[u], make_float4(w * vx, w * vy, w * vz, 0.f));
         }
+    sdeposit_lines(c, f, ix, jn, [&](int u, int v) { return fa * wx[u] * wn[v]; });
 }
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
 template <bool YF>
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return YF ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
 
 // TSC deposit of f v at (x, y) into jsr: jx, jy, jz (stream_deposit, sim_stream.hpp:33-64). The reference also
-// deposits the charge of negative and positive particles into planes 3 and 4; those feed only its density
-// diagnostics (rho_lines, openPMD n_e / n_i), which this build does not write, so they are left out. F32: into the
-// FP32 planes; on the Fourier y grid interleaved per point as (jx, jy, jz, 0), one vector atomic add per TSC
-// point instead of three (the adds into L2 bound the streaming push).
+// deposits the charge of negative and positive particles into whole planes 3 and 4, of which it keeps only the lines
+// through the axis (rho_lines; openPMD n_e / n_i, not written here, take the planes): the last pass adds the charge of
+// the points on those lines alone (sdeposit_lines). F32: into the FP32 planes; on the Fourier y grid interleaved per
+// point as (jx, jy, jz, 0), one vector atomic add per TSC point instead of three (the adds into L2 bound the
+// streaming push).
 template <bool F32, bool YF>
 __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y, double f, double vx, double vy, double vz) {
     const Geo& g = c.g;
@@ -279,6 +302,10 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
                 }
             }
         }
+        int jl[3];                     // the charge lives on the inner nodes 1 .. ny - 1
+#pragma unroll
+        for (int v = 0; v < 3; ++v) jl[v] = jn[v] >= 1 && jn[v] <= g.ny - 1 ? jn[v] : -1;
+        sdeposit_lines(c, f, ix_, jl, [&](int u, int v) { return f * wx[u] * wn[v] * g.iA[jl[v]]; });
         return;
     }
     tsc_periodic(y, g.dy, g.ny, jn, wn);
@@ -295,6 +322,7 @@ __device__ __forceinline__ void sdeposit(const StreamArgs& c, double x, double y
                 atomicAdd(&c.J[k], w * vx); atomicAdd(&c.J[nk + k], w * vy); atomicAdd(&c.J[2 * nk + k], w * vz);
             }
         }
+    sdeposit_lines(c, f, ix_, jn, [&](int u, int v) { return f * wx[u] * wn[v] * ia0; });
 }
 
 // |E| of the grid and the wave at (x, y), lab z, slice position zeta (field_abs, sim_stream.hpp:67-74)

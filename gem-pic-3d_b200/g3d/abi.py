@@ -15,7 +15,7 @@ G3D_PREC_FP64, G3D_PREC_MIXED = 0, 1
 G3D_POL_S, G3D_POL_P, G3D_POL_CIRCULAR = 0, 1, 2
 
 ARRAYS = {"Rx": 0, "Ry": 1, "Ez": 2, "Bz": 3, "Lx": 4, "Ly": 5, "j0x": 6, "j0y": 7,
-          "jkx": 8, "jky": 9, "jkz": 10, "jw": 11, "F": 12}
+          "jkx": 8, "jky": 9, "jkz": 10, "jw": 11, "F": 12, "rho_lines": 13, "rho_lines_i": 14}
 
 PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("zeta", "<f8"), ("px", "<f8"), ("py", "<f8"),
                            ("pz", "<f8"), ("w", "<f8"), ("rem", "<f8"), ("z", "<f8"), ("q", "<f8"),

@@ -9,10 +9,10 @@
 // every output.checkpoint_every steps in the reference's layout and name (checkpoint_NNNNNN_r0000.bin, with the streaming
 // plasma's state; written by the library's host thread while the next steps run, the last one waited for before
 // "done"), and
-// "done: N steps, X s" on stdout. Field files, particle dumps, frames, openPMD and the other output groups of the
-// reference are not written, nor diag.txt's last column with mobile ions (the ion density on the axis, from charge
-// planes the library does not deposit). A deck key the library does not run stops it before any device work; exit codes as the
-// reference's: 0 done, 2 error.
+// "done: N steps, X s" on stdout. With loaded ions diag.txt has the reference's last column, the largest ion charge
+// density on the axis (from the library's density lines). Field files, particle dumps, frames, openPMD and the other
+// output groups of the reference are not written. A deck key the library does not run stops it before any device
+// work; exit codes as the reference's: 0 done, 2 error.
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -50,7 +50,7 @@ void diag_line(FILE* f, const Config& c, g3dshim::Simulation& sim, bool header) 
         for (FILE* out : {f, stdout})
             if (out) std::fprintf(out, "# step  z[mm]  N_alive  <x>[um] <y>[um] <zeta>[um]  rms_x rms_y rms_zeta[um]  <px> <py> "
                                        "<pz> <gamma> <p.khat>  rms_pz  eta_rel[FWHM] a_env  W_field[J] W_kin[J]  N_trapped "
-                                       "Q_trapped[pC]\n");
+                                       "Q_trapped[pC]%s\n", c.mobile_ions() ? "  max_Zni/n0(axis)" : "");
     const std::vector<double> S = sim.diagnostics_sums();
     const g3d_status st = sim.status();
     const double w = S[0] > 0 ? S[0] : 1;
@@ -74,6 +74,15 @@ void diag_line(FILE* f, const Config& c, g3dshim::Simulation& sim, bool header) 
                   long(st.istep), st.s * c.Lu * 1e3, long(S[14]), mean(1) * um, mean(2) * um, mean(3) * um,
                   spread(1, 4) * um, spread(2, 5) * um, spread(3, 6) * um, mean(7), mean(8), mean(9), mean(10), mean(11),
                   spread(9, 12), eta_rel, a_env, W_field, W_kin, long(S[17]), Q_tr);
+    if (c.mobile_ions()) {             // the largest ion charge density on the axis (src/sim_output.cpp:44-51)
+        const std::vector<double> rl = sim.real_array(G3D_A_RHO_I);
+        const int nx = c.nx, ny = c.ny, N = int(rl.size() / size_t(nx + ny));
+        const int i0 = ((int(std::lround(-st.X0 / (c.Lx / nx))) % nx) + nx) % nx;
+        double mx = 0;
+        for (int n = 0; n + 1 < N; ++n) mx = std::max(mx, rl[size_t(n) * size_t(nx + ny) + size_t(i0)] / c.n0);
+        const size_t l = std::strlen(line);
+        std::snprintf(line + l - 1, sizeof line - l + 1, " %11.4e\n", mx);
+    }
     for (FILE* out : {f, stdout})
         if (out) { std::fputs(line, out); std::fflush(out); }
 }

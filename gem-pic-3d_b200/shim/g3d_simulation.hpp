@@ -126,6 +126,15 @@ public:
         check(g3d_beam_moments(ctx_, 16, s1.data(), s2.data(), &G), ctx_, "beam_moments");
         s1.resize(size_t(G) * 8); s2.resize(size_t(G) * 8);
     }
+    // a real array of the reference layout (jw, the density lines rho_lines / rho_lines_i) as doubles
+    std::vector<double> real_array(int32_t which) {
+        size_t n = 0, eb = 0;
+        check(g3d_array_info(ctx_, which, &n, &eb), ctx_, "array_info");
+        if (eb != sizeof(double)) throw std::runtime_error("real_array: not an array of doubles");
+        std::vector<double> v(n);
+        check(g3d_get_array(ctx_, which, v.data(), n), ctx_, "get_array");
+        return v;
+    }
     g3d_status status() const {
         g3d_status st{};
         check(g3d_get_status(ctx_, &st), ctx_, "status");

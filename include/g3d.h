@@ -171,7 +171,11 @@ typedef struct g3d_status {
 /* Array ids for g3d_array_info / g3d_get_array / g3d_set_array / g3d_device_ptr.
  * Layouts are the reference's (src/sim.hpp:265-301): spectra [l][j][ix] complex128
  * (l = slice 0..N-1 or half-cell plane 0..N), jw [comp][hw][j][ix] double (3 x (N+3) planes),
- * F [comp][fl][j][ix] float (6 x (N+2) planes). */
+ * F [comp][fl][j][ix] float (6 x (N+2) planes). The density lines rho_lines and rho_lines_i
+ * (src/sim.hpp:299-301) are [n][nx + ny] double: the charge of the negative (RHO_E) and of the
+ * positive (RHO_I) streaming particles of half-cell n in its last pass on the row through the axis
+ * (nx values) and on the column through it (ny values); 0 elements without a plasma, and RHO_I
+ * without a loaded ion species. */
 #define G3D_A_RX   0
 #define G3D_A_RY   1
 #define G3D_A_EZ   2
@@ -185,7 +189,9 @@ typedef struct g3d_status {
 #define G3D_A_JKZ  10
 #define G3D_A_JW   11
 #define G3D_A_F    12
-#define G3D_A_COUNT 13
+#define G3D_A_RHO_E 13
+#define G3D_A_RHO_I 14
+#define G3D_A_COUNT 15
 
 /* ------------------------------------------------------------------ lifetime */
 /* Creates a context on the current CUDA device: device buffers of the reference layouts,

@@ -273,6 +273,8 @@ static int array_of(Simulation& s, int which, Buf<cpx>** c, Buf<double>** d, Buf
         case G3D_A_JKZ: *c = &s.jkz; break;
         case G3D_A_JW: *d = &s.jw; break;
         case G3D_A_F: *f = &s.F; break;
+        case G3D_A_RHO_E: *d = &s.rho_lines; break;
+        case G3D_A_RHO_I: *d = &s.rho_lines_i; break;
         default: return -1;
     }
     return 0;
