@@ -255,7 +255,7 @@ def test_laser_wakefield_deck_matches_the_reference_cli(tmp_path):
         r = run([exe, str(deck)], d)
         assert r.returncode == 0, (exe, r.stdout[-2000:], r.stderr[-2000:])
     a, b = diag_rows(our_dir / "out" / "diag.txt"), diag_rows(ref_dir / "out" / "diag.txt")
-    assert a.shape[0] >= 3 and a.shape[1] == 22 and np.all(a[:, 21] > 0)
+    assert a.shape[0] >= 3 and a.shape[1] == 22 and np.all(a[1:, 21] > 0)      # no march before the first step
     diag_close(a, b, "lwfa")
     # the checkpoint after step 2, with the streaming plasma's state (written here while the run went on)
     ca = read_checkpoint(our_dir / "out" / "checkpoint_000002_r0000.bin")
