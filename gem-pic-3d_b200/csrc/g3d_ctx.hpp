@@ -230,6 +230,8 @@ struct Ctx {
     DevBuf<int32_t> sort_idx;
     DevBuf<unsigned char> sort_tmp;
     int steps_since_sort = 0;
+    DevBuf<int32_t> jflag, joff;                 // the join of trapped particles: live flags of the list, their sums
+    DevBuf<unsigned char> jtmp;
     // reductions
     DevBuf<double> red;                          // per-block partial sums
     DevBuf<double> momw;                         // the beam moments' partial sums, totals and means
@@ -421,6 +423,8 @@ std::vector<cpx> get_js0(Ctx& c, int comp);
 void set_js0(Ctx& c, int comp, const std::vector<cpx>& v);
 void launch_parts_unpack(Ctx& c, long n);   // pstage (records) -> parts (columns)
 void launch_parts_pack(Ctx& c, long n);     // parts (columns) -> pstage (records)
+// the live particles (alive 1) of the list in order, then the na records `add` (host): false when the capacity is short
+bool beam_keep_live_and_append(Ctx& c, const g3d_particle* add, long na);
 
 }  // namespace g3d
 

@@ -541,7 +541,7 @@ void march_plasma(Ctx& c, double s0, double s1) {
         p.sp = (p.sp >= SP_FREED && p.sp < SP_INJECTED) ? p.sp - SP_FREED + SP_INJECTED : p.sp >= SP_INJECTED ? p.sp : SP_TRAPPED;
         ++P.trapped_total;
     }
-    if (!add.empty()) {
+    if (!add.empty() && !beam_keep_live_and_append(c, add.data(), long(add.size()))) {   // short of capacity: on the host
         std::vector<g3d_particle> all = get_particles(c), keep;
         keep.reserve(all.size() + add.size());
         for (auto& p : all) if (p.alive == 1) keep.push_back(p);
