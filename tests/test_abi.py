@@ -38,6 +38,18 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= exported
 
 
+def test_array_ids_match_the_header():
+    """The Python mirror's array names map to the ids include/g3d.h defines, and cover all of them."""
+    from g3d import abi
+    text = open(HEADER).read()
+    ids = {m.group(1): int(m.group(2)) for m in re.finditer(r"^#define G3D_A_(\w+)\s+(\d+)", text, flags=re.M)}
+    count = ids.pop("COUNT")
+    assert sorted(abi.ARRAYS.values()) == sorted(ids.values()) == list(range(count))
+    names = {"RX": "Rx", "RY": "Ry", "EZ": "Ez", "BZ": "Bz", "LX": "Lx", "LY": "Ly", "J0X": "j0x", "J0Y": "j0y",
+             "JKX": "jkx", "JKY": "jky", "JKZ": "jkz", "JW": "jw", "F": "F", "RHO_E": "rho_lines", "RHO_I": "rho_lines_i"}
+    assert {names[k]: v for k, v in ids.items()} == abi.ARRAYS
+
+
 def test_version_string():
     from g3d import abi
     assert b"sm_100a" in abi.load_library().g3d_version()
