@@ -102,6 +102,11 @@ def test_window_shift_moves_the_joining_particles():
     assert np.array_equal(ps["id"], pr["id"]) and np.array_equal(ps["alive"], pr["alive"])
     for f in ["x", "y", "zeta", "px", "py", "pz", "z"]:
         assert rel_l2(ps[f], pr[f]) <= 1e-9, (f, rel_l2(ps[f], pr[f]))
+    # the density lines through the axis follow the shifted window origin
+    for a in ["rho_lines", "rho_lines_i"]:
+        x, y = s.array(a), r.array(a)
+        assert x.size == y.size > 0 and np.abs(y).max() > 0, a
+        assert rel_l2(x, y) <= 1e-9, (a, rel_l2(x, y))
 
 
 @needs_ref
