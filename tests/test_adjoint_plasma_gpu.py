@@ -13,7 +13,8 @@ Bound: relative difference <= 1e-6 between the adjoint's directional derivative 
 import numpy as np
 import pytest
 
-from test_adjoint_gpu import EPS, TOL, adjoint, autograd_inputs, central, forward, hermitian_direction, objective
+from test_adjoint_gpu import (EPS, TOL, adjoint, autograd_inputs, central, forward, hermitian_direction, objective,
+                              reference_final, reference_final_modes)
 
 pytestmark = pytest.mark.gpu
 
@@ -78,6 +79,38 @@ def test_plasma_momentum_gradient_against_central_differences(through_start):
                  forward(cfg, dp=-EPS * D, through_start=through_start), EPS)
     print(f"momenta (through the start field: {through_start}): adjoint {ad:.12e}, central difference {fd:.12e}")
     assert abs(ad - fd) <= TOL * abs(fd), (ad, fd)
+
+
+@pytest.mark.parametrize("what", ["momenta", "laser modes"])
+def test_plasma_gradients_against_central_differences_of_the_reference(what):
+    """The plasma adjoint (FP64, exact fields) against central differences of the reference's own CPU code with its
+    streaming plasma, whose real fields are rounded to float as it stores them: the float rounding puts a floor into
+    its difference quotients, so the steps are those of the adjoint without plasma (3e-3 for the momenta; for the
+    laser modes the Richardson extrapolation of 4e-3 and 2e-3), and this library's forward with float fields takes
+    the same differences to 1e-7 (its arithmetic is the reference's; its atomic adds run in another order)."""
+    cfg = case(charge_pC=1.0)
+    J, gm, gp, _ = adjoint(cfg)
+    if what == "momenta":
+        D = np.random.default_rng(41).standard_normal(gp.shape)
+        e = 3e-3
+        fr = central(reference_final(cfg, e * D), reference_final(cfg, -e * D), e)
+        fo = central(forward(cfg, dp=e * D, exact=False), forward(cfg, dp=-e * D, exact=False), e)
+        ad = float(np.sum(gp * D))
+        print(f"plasma, momenta: reference central difference {fr:.12e}, this forward's {fo:.12e}, adjoint {ad:.12e}")
+        assert abs(fo - fr) <= 1e-7 * abs(fr), (fo, fr)
+        assert abs(ad - fr) <= 1e-4 * abs(fr), (ad, fr)
+        return
+    d = hermitian_direction(np.random.default_rng(42), cfg.ny, cfg.nx)
+    quot = {}
+    for e in (4e-3, 2e-3):
+        fr = central(reference_final_modes(cfg, 1 + e * d), reference_final_modes(cfg, 1 - e * d), e)
+        fo = central(forward(cfg, coef=1 + e * d, exact=False), forward(cfg, coef=1 - e * d, exact=False), e)
+        assert abs(fo - fr) <= 1e-7 * abs(fr), (e, fo, fr)
+        quot[e] = fr
+    rich = (4 * quot[2e-3] - quot[4e-3]) / 3
+    ad = float(np.real(np.sum(np.conj(gm) * d)))
+    print(f"plasma, laser modes: reference central differences {quot}, extrapolated {rich:.12e}, adjoint {ad:.12e}")
+    assert abs(ad - rich) <= 5e-4 * abs(rich), (ad, rich)
 
 
 @pytest.mark.parametrize("what", ["laser modes", "momenta"])
