@@ -245,22 +245,6 @@ __device__ __forceinline__ void sdeposit_lines(const StreamArgs& c, T f, const i
             for (int v = 0; v < 3; ++v)
                 if (jn[v] >= 0) atomicAdd(rl + c.g.nx + jn[v], double(W(u, v)));
 }
-// The mixed form's deposit on the Fourier y grid: f (v_x, v_y, v_z) at (x, y), FP32 weights, one vector add per point.
-__device__ __forceinline__ void sdeposit_f32(const StreamArgs& c, double x, double y, float f, float vx, float vy, float vz) {
-    int ix[3], jn[3]; float wx[3], wn[3];
-    tsc_f32(x, c.inv_dx, c.g.nx, ix, wx);
-    tsc_f32(y, c.inv_dy, c.g.ny, jn, wn);
-    const float fa = f * float(c.g.iA[0]);
-    float4* J4 = reinterpret_cast<float4*>(c.Jf);
-#pragma unroll
-    for (int v = 0; v < 3; ++v)
-#pragma unroll
-        for (int u = 0; u < 3; ++u) {
-            const float w = fa * wx[u] * wn[v];
-            atomicAdd(J4 + long(jn[v]) * c.g.nx + ix[u], make_float4(w * vx, w * vy, w * vz, 0.f));
-        }
-    sdeposit_lines(c, f, ix, jn, [&](int u, int v) { return fa * wx[u] * wn[v]; });
-}
 __device__ __forceinline__ double wrapx(const Geo& g, double x) { return wrap_periodic(x, g.Lx); }
 template <bool YF>
 __device__ __forceinline__ double wrapy(const Geo& g, double y) { return YF ? wrap_periodic(y, g.Ly) : y; }   // free-hand: walls
@@ -383,7 +367,7 @@ __device__ void ionize(const StreamArgs& c, const StrmDev& S, long i, double E1,
 struct DepReq {
     double x, y, f, vx, vy, vz;
     bool on;
-    bool f32;                  // the mixed form on the Fourier y grid: deposit with sdeposit_f32 (ff, fv)
+    bool f32;                  // the mixed form on the Fourier y grid: FP32 deposit weights from ff, fv (sdeposit_warp)
     float ff, fv[3];
 };
 
