@@ -596,16 +596,21 @@ __device__ __forceinline__ void sdeposit_warp(const StreamArgs& c, const DepReq&
 // neighbouring lattice particles make to the same points. F32 (the mixed form): the gathers in FP32 from FP32 field
 // planes, the deposit into FP32 planes; the push arithmetic and the particle state stay FP64.
 constexpr int ST_NT = 128;
+// Resident CTAs per SM the register budget of the plain variant is sized for, by form. With the per-thread deposit,
+// 5 (96 registers) against 6 (80) gave 55.8 against 57.8 us per launch in the mixed form and 89.7 against 91.8 us in
+// the FP64 form (laser-plasma workload, one box); 4, 7 and 8 were slower. With the warp-summed deposit the mixed form
+// prefers 6 (47.1 and 46.6 against 47.7 and 48.9 us, 4: 52.6) and the FP64 form keeps 5 (66.5 against 66.8 at 6, 71.4
+// at 4; 256 x 256 x 128 case, all builds alternated in one call).
 #ifndef G3D_STREAM_MINB
-// resident CTAs per SM the register budget of the plain variant is sized for: 5 (96 registers) against 6 (80) gave
-// 55.8 against 57.8 us per launch in the mixed form and 89.7 against 91.8 us in the FP64 form (laser-plasma workload,
-// one box); 4, 7 and 8 were slower
 #define G3D_STREAM_MINB 5
+#endif
+#ifndef G3D_STREAM_MINB_F32
+#define G3D_STREAM_MINB_F32 6
 #endif
 // YF: the Fourier y grid (true) or the free-hand one, fixed for a run, so that each variant holds only its own grid's
 // gathers and deposits (fewer registers and no local arrays).
 template <bool F32, bool ION, bool LASER, bool YF, bool EX = false, bool REC = false>
-__global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : G3D_STREAM_MINB) k_stream(StreamArgs c,
+__global__ void __launch_bounds__(ST_NT, (ION || LASER) ? 4 : F32 ? G3D_STREAM_MINB_F32 : G3D_STREAM_MINB) k_stream(StreamArgs c,
                                                                                        const long* __restrict__ nstrm) {
     const StrmDev S = c.sd[0];
     const long n = *nstrm;
